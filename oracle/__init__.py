@@ -1,0 +1,91 @@
+"""ORACLE -- test infrastructure only.
+
+CPU FP64 restatement of the reference's hot-path operators (see the header of
+oracle_trisk.cpp and oracle_elliptic.cpp for the reference routines followed,
+file:line).  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg import this package, and only as the checker.  The product library never
+links or calls it.
+
+Parity status: unpinned against the reference binary (the reference is Fortran
+and no Fortran compiler exists in the build container); pinned instead by the
+properties the reference relies on (conservation, identities, analytic cases),
+checked in tests/test_oracle.py.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int64)
+
+
+class orc_level(C.Structure):
+    _fields_ = [("n", C.c_int), ("P", C.c_int), ("NN", C.c_int64),
+                ("len", _dp), ("pedlen", _dp), ("part", _dp), ("hex_inv", _dp), ("triarea", _dp), ("coriolis", _dp),
+                ("halo_node", _ip), ("n_halo_node", C.c_int64), ("halo_edge", _ip), ("n_halo_edge", C.c_int64)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing; run `make -C oracle`")
+        L = C.CDLL(LIB_PATH)
+        L.orc_trend.argtypes = [C.POINTER(orc_level), C.c_int, C.c_double, C.c_double, C.c_double] + [_dp] * 9
+        L.orc_trend.restype = C.c_int
+        L.orc_rk4.argtypes = [C.POINTER(orc_level), C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                              C.c_int] + [_dp] * 6
+        L.orc_rk4.restype = C.c_int
+        if hasattr(L, "orc_elliptic_apply"):
+            from . import elliptic as _e  # noqa: F401  (binds its own signatures)
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+class _Level:
+    """Keeps the numpy arrays alive for the lifetime of the ctypes struct."""
+
+    def __init__(self, g):
+        self.keep = [np.ascontiguousarray(x) for x in
+                     (g.len, g.pedlen, g.part, g.hex_inv, g.triarea, g.coriolis)]
+        self.hn = np.ascontiguousarray(g.halo_node, dtype=np.int64)
+        self.he = np.ascontiguousarray(g.halo_edge, dtype=np.int64)
+        k = self.keep
+        self.s = orc_level(g.n, g.P, g.NN, _d(k[0]), _d(k[1]), _d(k[2]), _d(k[3]), _d(k[4]), _d(k[5]),
+                           self.hn.ctypes.data_as(_ip), len(self.hn), self.he.ctypes.data_as(_ip), len(self.he))
+
+
+def trend(g, nz, ph, state):
+    """One evaluation of trend_ml on a uniform level.  Returns (dmass, dtemp, dvelo, state_after_halo)."""
+    lv = _Level(g)
+    m, t, v = (np.ascontiguousarray(state[k]).copy() for k in ("mass", "temp", "velo"))
+    dm, dt, dv = np.zeros_like(m), np.zeros_like(t), np.zeros_like(v)
+    rc = lib().orc_trend(C.byref(lv.s), nz, ph.grav, ph.ref_density, ph.p_top, _d(m), _d(t), _d(v),
+                         _d(np.ascontiguousarray(state["mean_m"])), _d(np.ascontiguousarray(state["mean_t"])),
+                         _d(np.ascontiguousarray(state["topo"])), _d(dm), _d(dt), _d(dv))
+    assert rc == 0
+    return dm, dt, dv, dict(mass=m, temp=t, velo=v)
+
+
+def rk4(g, nz, ph, state, dt, nsteps):
+    """nsteps RK4 steps on a uniform level; returns the new (mass, temp, velo)."""
+    lv = _Level(g)
+    m, t, v = (np.ascontiguousarray(state[k]).copy() for k in ("mass", "temp", "velo"))
+    rc = lib().orc_rk4(C.byref(lv.s), nz, ph.grav, ph.ref_density, ph.p_top, float(dt), int(nsteps), _d(m), _d(t),
+                       _d(v), _d(np.ascontiguousarray(state["mean_m"])), _d(np.ascontiguousarray(state["mean_t"])),
+                       _d(np.ascontiguousarray(state["topo"])))
+    assert rc == 0
+    return m, t, v

@@ -1,0 +1,122 @@
+"""ctypes bindings of libwtgpu.so (the C-ABI declared in include/wavetrisk_gpu.h).
+
+The shared library is built in-tree by ``wavetrisk_hydrostatic_b200.build``.
+Loading fails loudly when it is missing: there is no Python or CPU fallback
+for any device entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwtgpu.so")
+
+WT_OK = 0
+WT_ERR_ARG = -1
+WT_ERR_CUDA = -2
+WT_ERR_ALLOC = -3
+WT_ERR_NONFINITE = -4
+WT_ERR_NOT_CONVERGED = -5
+WT_ERR_TIMEOUT = -6
+WT_ERR_STATE = -7
+WT_ERR_NO_DEVICE = -8
+
+STATUS_NAMES = {
+    WT_OK: "WT_OK", WT_ERR_ARG: "WT_ERR_ARG", WT_ERR_CUDA: "WT_ERR_CUDA", WT_ERR_ALLOC: "WT_ERR_ALLOC",
+    WT_ERR_NONFINITE: "WT_ERR_NONFINITE", WT_ERR_NOT_CONVERGED: "WT_ERR_NOT_CONVERGED",
+    WT_ERR_TIMEOUT: "WT_ERR_TIMEOUT", WT_ERR_STATE: "WT_ERR_STATE", WT_ERR_NO_DEVICE: "WT_ERR_NO_DEVICE",
+}
+
+
+class WtError(RuntimeError):
+    def __init__(self, where: str, code: int):
+        super().__init__(f"{where} failed: {STATUS_NAMES.get(code, code)}")
+        self.code = code
+
+
+class wt_level_dims(C.Structure):
+    _fields_ = [("n", C.c_int), ("P", C.c_int), ("NN", C.c_int64),
+                ("n_halo_node", C.c_int64), ("n_halo_edge", C.c_int64)]
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int64)
+
+
+class wt_level_desc(C.Structure):
+    _fields_ = [("level", C.c_int), ("n", C.c_int), ("P", C.c_int), ("NN", C.c_int64),
+                ("len", _dp), ("pedlen", _dp), ("part", _dp), ("hex_inv", _dp), ("triarea", _dp),
+                ("coriolis", _dp), ("overl_a", _dp), ("topo", _dp),
+                ("halo_node", _ip), ("n_halo_node", C.c_int64),
+                ("halo_edge", _ip), ("n_halo_edge", C.c_int64)]
+
+
+class wt_grid_desc(C.Structure):
+    _fields_ = [("level_start", C.c_int), ("level_end", C.c_int), ("nz", C.c_int),
+                ("grav", C.c_double), ("ref_density", C.c_double), ("p_top", C.c_double),
+                ("levels", C.POINTER(wt_level_desc))]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libwtgpu.so once; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; run wavetrisk_hydrostatic_b200.build.build()")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.wt_grid_build.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(vp)]
+        L.wt_grid_build.restype = C.c_int
+        L.wt_grid_free.argtypes = [vp]
+        L.wt_grid_free.restype = None
+        L.wt_grid_level_dims.argtypes = [vp, C.c_int, C.POINTER(wt_level_dims)]
+        L.wt_grid_level_dims.restype = C.c_int
+        L.wt_grid_copy.argtypes = [vp, C.c_int, C.c_char_p, vp]
+        L.wt_grid_copy.restype = C.c_int
+        for name, args in _DEVICE_SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.wt_stream.argtypes = [vp]
+        L.wt_stream.restype = vp
+        _lib = L
+    return _lib
+
+
+_vp = C.c_void_p
+_DEVICE_SIGS = {
+    "wt_create": [C.POINTER(wt_grid_desc), C.POINTER(_vp)],
+    "wt_destroy": [_vp],
+    "wt_status": [_vp],
+    "wt_synchronize": [_vp],
+    "wt_upload_state": [_vp, _dp, _dp, _dp, _dp, _dp],
+    "wt_download_state": [_vp, _dp, _dp, _dp],
+    "wt_trend": [_vp],
+    "wt_download_trend": [_vp, _dp, _dp, _dp],
+    "wt_rk4_step": [_vp, C.c_double, C.c_int],
+    "wt_rk4_step_host": [_vp, C.c_double, C.c_int, _dp, _dp, _dp],
+}
+
+
+def check(where: str, code: int) -> None:
+    if code != WT_OK:
+        raise WtError(where, code)
+
+
+def dptr(a):
+    """Pointer to a C-contiguous float64 numpy array (or NULL for None)."""
+    if a is None:
+        return C.cast(None, _dp)
+    assert a.dtype.kind == "f" and a.dtype.itemsize == 8 and a.flags["C_CONTIGUOUS"], "need contiguous float64"
+    return a.ctypes.data_as(_dp)
+
+
+def iptr(a):
+    if a is None:
+        return C.cast(None, _ip)
+    assert a.dtype.kind == "i" and a.dtype.itemsize == 8 and a.flags["C_CONTIGUOUS"], "need contiguous int64"
+    return a.ctypes.data_as(_ip)

@@ -1,0 +1,94 @@
+"""Seeded synthetic initial states for the benchmark and test workloads.
+
+The reference builds initial conditions in its test-case modules
+(test/seamount/test_case_module.f90: init_mean :381-412, init_sol :341-379):
+sol_mean holds the layer mass rho0*dz and Theta = rho0*dz*(1 - rho/rho0);
+sol holds the perturbation (the free surface rho0*eta in the top layer).
+Velocities are edge-normal components of an analytic zonal jet
+(proj_vel, src/sphere.f90:330).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .grid import DG, RT, UP, LevelGeom, halo_edges, halo_nodes
+
+
+@dataclass
+class OceanParams:
+    grav: float = 9.80616          # grav_accel default, src/shared.f90:386
+    ref_density: float = 1028.0    # ref_density_water, src/shared.f90:407
+    p_top: float = 0.0
+    depth: float = 4000.0
+
+
+def _neighbours(g: LevelGeom):
+    d, i, j = g.ij()
+    ok = (i + 1 < g.n + 2) & (j + 1 < g.n + 2)
+    E = np.where(ok, g.idx(d, np.minimum(i + 1, g.n + 1), j), 0)
+    N = np.where(ok, g.idx(d, i, np.minimum(j + 1, g.n + 1)), 0)
+    NE = np.where(ok, g.idx(d, np.minimum(i + 1, g.n + 1), np.minimum(j + 1, g.n + 1)), 0)
+    return E, N, NE
+
+
+def _proj_jet(p, q, u0, lat0, width):
+    """Edge-normal velocity of u = u0 sech^2((lat-lat0)/width) along p->q at its midpoint."""
+    m = p + q
+    nrm = np.linalg.norm(m, axis=0)
+    nrm = np.where(nrm == 0, 1.0, nrm)
+    m = m / nrm
+    lat = np.arcsin(np.clip(m[2], -1, 1))
+    lon = np.arctan2(m[1], m[0])
+    u = u0 / np.cosh((lat - lat0) / width) ** 2
+    ez = np.stack([-np.sin(lon), np.cos(lon), np.zeros_like(lon)])
+    v = q - p
+    vn = np.linalg.norm(v, axis=0)
+    vn = np.where(vn == 0, 1.0, vn)
+    return u * np.einsum("ij,ij->j", ez, v / vn)
+
+
+def jet_state(g: LevelGeom, nz: int, seed: int = 0, ph: OceanParams | None = None,
+              u0: float = 1.0, eta_amp: float = 1e-3, rho_bottom: float = 1027.0, rho_top: float = 1024.0):
+    """Uniform-level layered ocean state: flat bottom, linear layer densities, zonal
+    jet at 45N in the top layer decaying linearly to 0 at the bottom, seeded white
+    noise free surface.  Returns dict of float64 arrays in the C-ABI layout."""
+    ph = ph or OceanParams()
+    NN = g.NN
+    rng = np.random.default_rng(seed)
+    dz = ph.depth / nz
+    rho = rho_bottom + (rho_top - rho_bottom) * np.arange(nz) / max(nz - 1, 1)   # k=1 is the bottom layer
+    mean_m = np.empty((nz, NN))
+    mean_t = np.empty((nz, NN))
+    for k in range(nz):
+        mean_m[k] = ph.ref_density * dz
+        mean_t[k] = mean_m[k] * (1.0 - rho[k] / ph.ref_density)
+    topo = np.full(NN, -ph.depth)
+    eta = np.zeros(NN)
+    own = g.owned
+    eta[own] = eta_amp * rng.standard_normal(int(own.sum()))
+    npole, spole = g.pole_ids()
+    pole_eta = eta_amp * rng.standard_normal(2)
+    d, i, j = g.ij()
+    eta[(d >= 5) & (i == 0) & (j == g.n)] = pole_eta[0]
+    eta[(d < 5) & (i == g.n) & (j == 0)] = pole_eta[1]
+    halo_nodes(g, eta)
+    mass = np.zeros((nz, NN))
+    temp = np.zeros((nz, NN))
+    mass[nz - 1] = ph.ref_density * eta
+    velo = np.zeros((nz, 3 * NN))
+    E, N, NE = _neighbours(g)
+    p = g.node
+    ujet = np.zeros(3 * NN)
+    sel = own
+    ujet[RT * NN:(RT + 1) * NN][sel] = _proj_jet(p[:, sel], p[:, E[sel]], u0, np.pi / 4, np.pi / 36)
+    ujet[DG * NN:(DG + 1) * NN][sel] = _proj_jet(p[:, NE[sel]], p[:, sel], u0, np.pi / 4, np.pi / 36)
+    ujet[UP * NN:(UP + 1) * NN][sel] = _proj_jet(p[:, sel], p[:, N[sel]], u0, np.pi / 4, np.pi / 36)
+    for k in range(nz):
+        velo[k] = ujet * (k / max(nz - 1, 1))
+    for k in range(nz):
+        halo_nodes(g, mass[k])
+        halo_nodes(g, temp[k])
+        halo_edges(g, velo[k])
+    return dict(mass=mass, temp=temp, velo=velo, mean_m=mean_m, mean_t=mean_t, topo=topo)

@@ -1,0 +1,301 @@
+// C-ABI implementation: device context, state upload/download, the trend and
+// the RK4 stepper (one captured CUDA graph per step).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/wavetrisk_gpu.h"
+#include "trisk_kernels.cuh"
+#include "wt_handle.cuh"
+
+using namespace wtk;
+
+namespace {
+
+constexpr int TPB = 256;
+
+inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+}  // namespace
+
+int wt_handle_fail(const char* where, cudaError_t e) {
+  std::fprintf(stderr, "wavetrisk_gpu: %s: %s\n", where, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? WT_ERR_ALLOC : WT_ERR_CUDA;
+}
+
+#define CK(x)                                         \
+  do {                                                \
+    cudaError_t e_ = (x);                             \
+    if (e_ != cudaSuccess) return wt_handle_fail(#x, e_); \
+  } while (0)
+
+static int dev_copy(double** dst, const double* src, int64_t count) {
+  CK(cudaMalloc(dst, count * sizeof(double)));
+  if (src)
+    CK(cudaMemcpy(*dst, src, count * sizeof(double), cudaMemcpyHostToDevice));
+  else
+    CK(cudaMemset(*dst, 0, count * sizeof(double)));
+  return WT_OK;
+}
+
+static int dev_zero(double** dst, int64_t count) { return dev_copy(dst, nullptr, count); }
+
+extern "C" {
+
+int wt_create(const wt_grid_desc* desc, wt_handle** out) {
+  if (!desc || !out || !desc->levels || desc->nz < 1 || desc->level_end < desc->level_start) return WT_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return WT_ERR_NO_DEVICE;
+  wt_handle* h = new wt_handle();
+  h->nz = desc->nz;
+  h->ph = Phys{desc->grav, desc->ref_density, desc->p_top};
+  h->level_start = desc->level_start;
+  h->level_end = desc->level_end;
+  const int nlev = desc->level_end - desc->level_start + 1;
+  h->lev.resize(nlev);
+  int rc = WT_OK;
+  for (int q = 0; q < nlev && rc == WT_OK; ++q) {
+    const wt_level_desc& ld = desc->levels[q];
+    DevLevel& D = h->lev[q];
+    if (ld.n != (1 << ld.level) || ld.P != ld.n + 4 || ld.NN != (int64_t)10 * ld.P * ld.P) { rc = WT_ERR_ARG; break; }
+    if (ld.NN >= (int64_t)1 << 31) { rc = WT_ERR_ARG; break; }
+    D.level = ld.level;
+    D.n = ld.n;
+    D.P = ld.P;
+    D.NN = ld.NN;
+    const int64_t NN = ld.NN;
+    if ((rc = dev_copy(&D.len, ld.len, 3 * NN))) break;
+    if ((rc = dev_copy(&D.pedlen, ld.pedlen, 3 * NN))) break;
+    if ((rc = dev_copy(&D.part, ld.part, 6 * NN))) break;
+    if ((rc = dev_copy(&D.hex_inv, ld.hex_inv, NN))) break;
+    if ((rc = dev_copy(&D.triarea, ld.triarea, 2 * NN))) break;
+    if ((rc = dev_copy(&D.coriolis, ld.coriolis, 2 * NN))) break;
+    if ((rc = dev_copy(&D.overl_a, ld.overl_a, 4 * NN))) break;
+    if ((rc = dev_copy(&D.topo, ld.topo, NN))) break;
+    std::vector<int2> hn(ld.n_halo_node);
+    for (int64_t k = 0; k < ld.n_halo_node; ++k) {
+      int64_t a = ld.halo_node[2 * k], b = ld.halo_node[2 * k + 1];
+      if (a < 0 || b < 0 || a >= NN || b >= NN) { rc = WT_ERR_ARG; break; }
+      hn[k] = make_int2((int)a, (int)b);
+    }
+    if (rc) break;
+    std::vector<int3> he(ld.n_halo_edge);
+    for (int64_t k = 0; k < ld.n_halo_edge; ++k) {
+      int64_t a = ld.halo_edge[3 * k], b = ld.halo_edge[3 * k + 1], s = ld.halo_edge[3 * k + 2];
+      if (a < 0 || b < 0 || a >= 3 * NN || b >= 3 * NN) { rc = WT_ERR_ARG; break; }
+      he[k] = make_int3((int)a, (int)b, (int)s);
+    }
+    if (rc) break;
+    D.n_hn = (int)hn.size();
+    D.n_he = (int)he.size();
+    cudaError_t e;
+    if ((e = cudaMalloc(&D.hn, sizeof(int2) * std::max<size_t>(1, hn.size()))) != cudaSuccess) { rc = wt_handle_fail("halo", e); break; }
+    if ((e = cudaMalloc(&D.he, sizeof(int3) * std::max<size_t>(1, he.size()))) != cudaSuccess) { rc = wt_handle_fail("halo", e); break; }
+    cudaMemcpy(D.hn, hn.data(), sizeof(int2) * hn.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(D.he, he.data(), sizeof(int3) * he.size(), cudaMemcpyHostToDevice);
+  }
+  if (rc == WT_OK) {
+    // Prognostic state and RK/trend work arrays on level_end.
+    DevLevel& D = h->top();
+    const int64_t NN = D.NN, nn = (int64_t)h->nz * NN, ne = 3 * nn;
+    double** node_arrays[] = {&h->mass, &h->temp, &h->mean_m, &h->mean_t, &h->m1, &h->t1, &h->dm, &h->dt,
+                              &h->bern, &h->phik, &h->pterm};
+    for (double** p : node_arrays)
+      if ((rc = dev_zero(p, nn))) break;
+    double** edge_arrays[] = {&h->velo, &h->v1, &h->dv, &h->qe, &h->hfm, &h->hft};
+    if (rc == WT_OK)
+      for (double** p : edge_arrays)
+        if ((rc = dev_zero(p, ne))) break;
+    if (rc == WT_OK) {
+      cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+      if (e != cudaSuccess) rc = wt_handle_fail("stream", e);
+    }
+  }
+  if (rc != WT_OK) {
+    wt_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return WT_OK;
+}
+
+int wt_destroy(wt_handle* h) {
+  if (!h) return WT_OK;
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  for (auto& D : h->lev) D.release();
+  double* arrays[] = {h->mass, h->temp, h->velo, h->mean_m, h->mean_t, h->m1, h->t1, h->v1, h->dm, h->dt, h->dv,
+                      h->qe, h->hfm, h->hft, h->bern, h->phik, h->pterm};
+  for (double* p : arrays)
+    if (p) cudaFree(p);
+  h->release_extra();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return WT_OK;
+}
+
+void* wt_stream(wt_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+int wt_synchronize(wt_handle* h) {
+  if (!h) return WT_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_status(wt_handle* h) {
+  if (!h) return WT_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaGetLastError());
+  return h->sticky;
+}
+
+int wt_upload_state(wt_handle* h, const double* mass, const double* temp, const double* velo, const double* mean_m,
+                    const double* mean_t) {
+  if (!h || !mass || !temp || !velo) return WT_ERR_ARG;
+  const int64_t nn = (int64_t)h->nz * h->top().NN;
+  CK(cudaMemcpyAsync(h->mass, mass, nn * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->temp, temp, nn * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->velo, velo, 3 * nn * 8, cudaMemcpyHostToDevice, h->stream));
+  if (mean_m) CK(cudaMemcpyAsync(h->mean_m, mean_m, nn * 8, cudaMemcpyHostToDevice, h->stream));
+  if (mean_t) CK(cudaMemcpyAsync(h->mean_t, mean_t, nn * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
+  return WT_OK;
+}
+
+int wt_download_state(wt_handle* h, double* mass, double* temp, double* velo) {
+  if (!h || !mass || !temp || !velo) return WT_ERR_ARG;
+  const int64_t nn = (int64_t)h->nz * h->top().NN;
+  CK(cudaMemcpyAsync(mass, h->mass, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(temp, h->temp, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(velo, h->velo, 3 * nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+}  // extern "C"
+
+// Launch sequence of one trend evaluation of state (m, t, v); MODE_RK writes
+// dst = base + hstep * trend, MODE_TREND writes the trends into h->dm/dt/dv.
+static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode, const double* bm, const double* bt,
+                        const double* bv, double* om, double* ot, double* ov, double hstep, bool halo_first) {
+  DevLevel& D = h->top();
+  LevelDev L = D.view();
+  const int nz = h->nz;
+  cudaStream_t s = h->stream;
+  if (halo_first) {
+    int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * nz;
+    k_halo_state<<<blocks_for(nt), TPB, 0, s>>>(nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, m, t, v);
+  }
+  const int mm = D.n + 1;
+  k_column<<<blocks_for(10 * mm * mm, 128), 128, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm);
+  Step1Out so{h->qe, h->hfm, h->hft, h->bern};
+  k_step1<<<blocks_for((int64_t)10 * mm * mm * nz), TPB, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
+  k_post_step1<<<blocks_for(40 * nz, 64), 64, 0, s>>>(L, nz, m, v, h->mean_m, h->qe);
+  k_halo_flux<<<blocks_for((int64_t)2 * D.n_he * nz), TPB, 0, s>>>(nz, D.NN, D.he, D.n_he, h->hfm, h->hft);
+  TrendIO io{};
+  io.mass = m; io.temp = t; io.mean_m = h->mean_m; io.mean_t = h->mean_t; io.qe = h->qe; io.hfm = h->hfm;
+  io.hft = h->hft; io.bern = h->bern; io.phik = h->phik;
+  io.base_m = bm; io.base_t = bt; io.base_v = bv; io.dst_m = om; io.dst_t = ot; io.dst_v = ov; io.h = hstep;
+  io.dm = h->dm; io.dtt = h->dt; io.dv = h->dv;
+  int64_t nt = D.NN * nz;
+  if (mode == MODE_RK)
+    k_trend<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+  else
+    k_trend<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+  CK(cudaGetLastError());
+  return WT_OK;
+}
+
+extern "C" {
+
+int wt_trend(wt_handle* h) {
+  if (!h) return WT_ERR_ARG;
+  int rc = launch_trend(h, h->mass, h->temp, h->velo, MODE_TREND, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                        0.0, true);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_download_trend(wt_handle* h, double* dmass, double* dtemp, double* dvelo) {
+  if (!h || !dmass || !dtemp || !dvelo) return WT_ERR_ARG;
+  const int64_t nn = (int64_t)h->nz * h->top().NN;
+  CK(cudaMemcpyAsync(dmass, h->dm, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(dtemp, h->dt, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(dvelo, h->dv, 3 * nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+// One RK4 step (src/time_integr.f90:78-103): four trend evaluations, each
+// fused with its sub-step, each followed by the ghost copy of WT_after_step.
+static int record_rk4(wt_handle* h, double dt) {
+  DevLevel& D = h->top();
+  const int nz = h->nz;
+  const double hs[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
+  for (int stage = 0; stage < 4; ++stage) {
+    double* qm = stage == 0 ? h->mass : h->m1;
+    double* qt = stage == 0 ? h->temp : h->t1;
+    double* qv = stage == 0 ? h->velo : h->v1;
+    double* om = stage == 3 ? h->mass : h->m1;
+    double* ot = stage == 3 ? h->temp : h->t1;
+    double* ov = stage == 3 ? h->velo : h->v1;
+    int rc = launch_trend(h, qm, qt, qv, MODE_RK, h->mass, h->temp, h->velo, om, ot, ov, hs[stage], false);
+    if (rc) return rc;
+    int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * nz;
+    k_halo_state<<<blocks_for(nt), TPB, 0, h->stream>>>(nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, om, ot, ov);
+  }
+  CK(cudaGetLastError());
+  return WT_OK;
+}
+
+int wt_rk4_step(wt_handle* h, double dt, int nsteps) {
+  if (!h || nsteps < 0) return WT_ERR_ARG;
+  if (nsteps == 0) return WT_OK;
+  if (!h->state_halo_done) {
+    // the reference's trend_ml starts with update_bdry of the state
+    DevLevel& D = h->top();
+    int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * h->nz;
+    k_halo_state<<<blocks_for(nt), TPB, 0, h->stream>>>(h->nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, h->mass, h->temp, h->velo);
+    h->state_halo_done = true;
+  }
+  if (!h->graph_exec || h->graph_dt != dt) {
+    if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = record_rk4(h, dt);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return wt_handle_fail("capture", e);
+    CK(cudaGraphInstantiate(&h->graph_exec, g, 0));
+    cudaGraphDestroy(g);
+    h->graph_dt = dt;
+  }
+  for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(h->graph_exec, h->stream));
+  CK(cudaGetLastError());
+  return WT_OK;
+}
+
+int wt_rk4_step_host(wt_handle* h, double dt, int nsteps, double* mass, double* temp, double* velo) {
+  if (!h || !mass || !temp || !velo) return WT_ERR_ARG;
+  const int64_t nn = (int64_t)h->nz * h->top().NN;
+  CK(cudaMemcpyAsync(h->mass, mass, nn * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->temp, temp, nn * 8, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->velo, velo, 3 * nn * 8, cudaMemcpyHostToDevice, h->stream));
+  h->state_halo_done = false;
+  int rc = wt_rk4_step(h, dt, nsteps);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(mass, h->mass, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(temp, h->temp, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(velo, h->velo, 3 * nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+}  // extern "C"
+
+void wt_handle::release_extra() {}

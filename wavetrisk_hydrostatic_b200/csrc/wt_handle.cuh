@@ -1,0 +1,55 @@
+// Device context behind the opaque wt_handle of the C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "trisk_kernels.cuh"
+
+struct DevLevel {
+  int level = 0, n = 0, P = 0;
+  int64_t NN = 0;
+  double *len = nullptr, *pedlen = nullptr, *part = nullptr, *hex_inv = nullptr, *triarea = nullptr,
+         *coriolis = nullptr, *overl_a = nullptr, *topo = nullptr;
+  int2* hn = nullptr;
+  int3* he = nullptr;
+  int n_hn = 0, n_he = 0;
+  wtk::LevelDev view() const { return wtk::LevelDev{n, P, NN, len, pedlen, part, hex_inv, triarea, coriolis, topo}; }
+  void release() {
+    double* a[] = {len, pedlen, part, hex_inv, triarea, coriolis, overl_a, topo};
+    for (double* p : a)
+      if (p) cudaFree(p);
+    if (hn) cudaFree(hn);
+    if (he) cudaFree(he);
+    len = pedlen = part = hex_inv = triarea = coriolis = overl_a = topo = nullptr;
+    hn = nullptr;
+    he = nullptr;
+  }
+};
+
+struct wt_handle {
+  int nz = 0, level_start = 0, level_end = 0;
+  wtk::Phys ph{};
+  std::vector<DevLevel> lev;
+  cudaStream_t stream = nullptr;
+  // prognostic state (level_end) and RK4 stage copy
+  double *mass = nullptr, *temp = nullptr, *velo = nullptr, *mean_m = nullptr, *mean_t = nullptr;
+  double *m1 = nullptr, *t1 = nullptr, *v1 = nullptr;
+  // trend output (wt_trend) and operator work arrays
+  double *dm = nullptr, *dt = nullptr, *dv = nullptr;
+  double *qe = nullptr, *hfm = nullptr, *hft = nullptr, *bern = nullptr, *phik = nullptr, *pterm = nullptr;
+  bool state_halo_done = false;
+  cudaGraphExec_t graph_exec = nullptr;
+  double graph_dt = 0.0;
+  int sticky = 0;  // WT_OK or the first error seen by a device-side check
+
+  // elliptic solver state (allocated by wt_elliptic_setup)
+  void* ell = nullptr;
+  void release_extra();
+
+  DevLevel& top() { return lev.back(); }
+  DevLevel& at(int l) { return lev[l - level_start]; }
+};
+
+int wt_handle_fail(const char* where, cudaError_t e);

@@ -1,0 +1,350 @@
+"""Benchmark: simulated days per wall-clock hour of the TRiSK RK4 stepper.
+
+Workload (N=1): uniform icosahedral J5 grid (10,242 cells, 30,720 edges),
+8 Boussinesq layers, flat 4000 m bottom, zonal jet + seeded white-noise free
+surface, explicit RK4 with dt = 300 s (the reference's time_step ->
+dt_step => RK4 -> trend_ml path).  A "step" is one RK4 step (four trend
+evaluations, four fused sub-steps, four ghost copies).  With --gpus N>1 every
+rank advances its own ensemble member (independent seeds, no collective):
+weak scaling, value = member-days per hour summed over ranks.
+
+--impl reference times the CPU restatement of the reference's path (the
+reference is Fortran; no Fortran compiler exists on the build or GPU hosts)
+on the host cores, OpenMP over the 10 lozenge domains.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 300.0
+DAY = 86400.0
+
+
+def sim_days_per_hour(steps, seconds):
+    return (steps * DT / DAY) / (seconds / 3600.0)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--level", type=int, default=5)
+    p.add_argument("--nz", type=int, default=8)
+    p.add_argument("--no-extra", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = [n for q, n in enumerate(names) if any(r[4 + q].lower().startswith("active") for r in rows)]
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allreduce_max(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ---------------------------------------------------------------- ours ----
+def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=True, kernels=True):
+    import numpy as np
+    import torch
+
+    from wavetrisk_hydrostatic_b200 import Grid, OceanParams, jet_state
+    from wavetrisk_hydrostatic_b200 import _native as Nt
+    from wavetrisk_hydrostatic_b200.model import TriskModel
+
+    g = Grid(level, level, radius=6371e3).level(level)
+    ph = OceanParams()
+    st = jet_state(g, nz, seed=seed, ph=ph)
+    model = TriskModel(g, nz, st["topo"], ph)
+    model.upload(st)
+    stream = torch.cuda.ExternalStream(model.stream, device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # 256 MB > 126 MB L2
+    for _ in range(warmup):
+        model.rk4(DT, 1)
+    model.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for s in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(s))           # L2 flush between timed steps, outside the timed region
+        ev[s][0].record(stream)
+        model.rk4(DT, 1)
+        ev[s][1].record(stream)
+    model.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    out = {"ms_total": ms, "ms_per_step": ms / steps}
+
+    if kernels:
+        # Per-kernel launch durations of the same stepper, launched kernel by kernel
+        # with CUDA events on the handle's stream (same steps, no graph).
+        kt = (Nt.C.c_double * 16)()
+        nk = Nt.C.c_int(0)
+        Nt.check("wt_profile_rk4", Nt.lib().wt_profile_rk4(model.h, DT, steps, kt, Nt.C.byref(nk)))
+        names = ["halo_state", "column", "step1", "post_step1", "halo_flux", "trend_rk"]
+        out["kernel_ms_per_launch"] = {names[k]: kt[k] for k in range(min(nk.value, len(names)))}
+
+    if e2e:
+        NN = g.NN
+        pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+        m, t, v = pin((nz, NN)), pin((nz, NN)), pin((nz, 3 * NN))
+        m[:] = st["mass"]; t[:] = st["temp"]; v[:] = st["velo"]
+        model.rk4_host(DT, 1, m, t, v)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            model.rk4_host(DT, 1, m, t, v)
+        t1 = time.perf_counter()
+        out["e2e_s"] = t1 - t0
+        out["h2d_bytes_per_step"] = int(m.nbytes + t.nbytes + v.nbytes)
+        out["d2h_bytes_per_step"] = int(m.nbytes + t.nbytes + v.nbytes)
+    out["NN"] = g.NN
+    out["cells"] = 10 * 4 ** level + 2
+    model.close()
+    return out
+
+
+def algorithmic_bytes_trend_rk(cells, nz):
+    """Compulsory bytes of one k_trend launch (MODE_RK) per node-layer: reads
+    mass, temp, mean_m, mean_t, qe(3), hflux_m(3), hflux_t(3), bernoulli, Phi,
+    base mass/temp/velo(3) = 20 words; writes dest mass/temp/velo(3) = 5 words;
+    geometry len(3), part(6), hex_inv once per node (amortised over nz)."""
+    return cells * (nz * 25 * 8 + 10 * 8)
+
+
+def bench_ours(args):
+    import torch
+
+    world, rank, local, pg = dist_init(args)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    barrier(pg)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    torch.cuda.synchronize(device)
+    barrier(pg)
+    r = run_case(args.level, args.nz, args.steps, args.warmup, seed=1000 + rank, device=device)
+    torch.cuda.synchronize(device)
+    barrier(pg)
+    clocks = sampler.stop() if sampler else None
+    ms_max = allreduce_max(pg, r["ms_total"], device)
+    e2e_max = allreduce_max(pg, r["e2e_s"], device)
+    value = world * sim_days_per_hour(args.steps, ms_max / 1e3)
+    e2e_value = world * sim_days_per_hour(args.steps, e2e_max)
+
+    extra = []
+    if not args.no_extra and rank == 0 and world == 1:
+        for (lv, nz, steps) in [(7, 16, 20), (8, 32, 5)]:
+            rr = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False)
+            kt = rr["kernel_ms_per_launch"]
+            ab = algorithmic_bytes_trend_rk(rr["NN"], nz)
+            extra.append({
+                "workload": f"uniform J{lv} ({rr['cells']} cells), {nz} layers, RK4 dt=300 s",
+                "ms_per_step": rr["ms_per_step"], "value": sim_days_per_hour(steps, rr["ms_total"] / 1e3),
+                "kernel_ms_per_launch": kt,
+                "trend_rk_GBps": ab / (kt["trend_rk"] / 1e3) / 1e9,
+            })
+
+    if rank == 0:
+        kt = r["kernel_ms_per_launch"]
+        dom = max(kt, key=lambda k: kt[k])
+        ab = algorithmic_bytes_trend_rk(r["NN"], args.nz)
+        ach = ab / (kt["trend_rk"] / 1e3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "trend_rk_traffic.json")
+        if os.path.exists(tf):
+            try:
+                traffic = json.load(open(tf)).get(f"J{args.level}_nz{args.nz}")
+            except Exception:
+                traffic = None
+        cpu = cpu_baseline(args, quick=True)
+        line = {
+            "metric": "sim-days/hour",
+            "value": value,
+            "unit": "simulated days per wall-clock hour",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded jet + white-noise free surface)",
+            "config": {
+                "workload": f"uniform J{args.level} icosahedral grid ({r['cells']} cells), {args.nz} Boussinesq layers, "
+                            f"flat 4000 m bottom, explicit RK4 dt=300 s",
+                "level": args.level, "layers": args.nz, "dt_s": DT,
+                "parallelism": f"replicas x{world} (independent ensemble members)" if world > 1 else "single GPU",
+                "l2": "flushed (256 MB write) between timed steps, outside the timed region",
+            },
+            "e2e": {"value": e2e_value, "unit": "simulated days per wall-clock hour",
+                    "h2d_bytes_per_step": r["h2d_bytes_per_step"], "d2h_bytes_per_step": r["d2h_bytes_per_step"],
+                    "path": "wt_rk4_step_host (C-ABI), pinned host buffers, state copied in and out every step"},
+            "gpu_launches": 24 * args.steps,
+            "roofline": {"bound": "hbm", "kernel": "trend_rk", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                         "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
+                         "dominant_kernel_by_time": dom, "kernel_ms_per_launch": kt},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        if extra:
+            line["extra"] = extra
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+# ----------------------------------------------------------- reference ----
+def cpu_baseline(args, quick=False):
+    """Times the CPU restatement (oracle) on a bounded sample of the workload."""
+    import numpy as np
+
+    import oracle
+    from wavetrisk_hydrostatic_b200 import Grid, OceanParams, jet_state
+
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    g = Grid(args.level, args.level, radius=6371e3).level(args.level)
+    ph = OceanParams()
+    st = jet_state(g, args.nz, seed=1, ph=ph)
+    oracle.rk4(g, args.nz, ph, st, DT, 1)
+    budget = args.cpu_seconds if not quick else min(args.cpu_seconds, 10.0)
+    steps, t_used = 0, 0.0
+    cur = st
+    while t_used < budget:
+        t0 = time.perf_counter()
+        m, t, v = oracle.rk4(g, args.nz, ph, cur, DT, 1)
+        t_used += time.perf_counter() - t0
+        cur = dict(st, mass=m, temp=t, velo=v)
+        steps += 1
+    return {"value": sim_days_per_hour(steps, t_used), "unit": "simulated days per wall-clock hour",
+            "cores": oracle.get_threads(), "kind": "port",
+            "sample": f"{steps} RK4 steps of the same workload ({t_used:.1f} s of CPU time)"}
+
+
+def bench_reference(args):
+    world, rank, local, pg = dist_init(args)
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    steps = max(1, args.steps)
+    cb = cpu_baseline(args)
+    line = {
+        "impl": "reference",
+        "metric": "sim-days/hour",
+        "value": cb["value"],
+        "unit": cb["unit"],
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded jet + white-noise free surface)",
+        "config": {"workload": f"uniform J{args.level} icosahedral grid, {args.nz} Boussinesq layers, explicit RK4 dt=300 s",
+                   "note": "CPU restatement of the reference path (no Fortran compiler on the host)"},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_ours(args)
+
+
+if __name__ == "__main__":
+    main()

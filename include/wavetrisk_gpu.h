@@ -109,6 +109,63 @@ int wt_rk4_step(wt_handle* h, double dt, int nsteps);
 /* Same, through host buffers: uploads the state, steps, downloads it. */
 int wt_rk4_step_host(wt_handle* h, double dt, int nsteps, double* mass, double* temp, double* velo);
 
+/* Measurement aid: the same RK4 steps launched kernel by kernel with CUDA
+ * events around every launch; ms_per_launch[0..5] = average duration of the
+ * ghost copy, column, step1, pentagon fix, flux ghost copy and trend+sub-step
+ * kernels.  No reference counterpart (the reference times whole steps). */
+int wt_profile_rk4(wt_handle* h, double dt, int nsteps, double* ms_per_launch, int* nkernels);
+
+/* ------------------------------------------------------------ elliptic ---- */
+/* Barotropic free-surface solve L(eta) = f with
+ *   L(q) = theta1 theta2 dt^2 div(g (|H| phi + eta_old) grad q) - q
+ * (elliptic_lo, src/barotropic_2d.f90:187-250; phi = 1, eta_old = 0) on the
+ * uniform hierarchy level_start..level_end of the handle.  Fields u (solution,
+ * initial guess) and f (right-hand side) are multi-level: the levels' NN-node
+ * arrays concatenated from level_start to level_end. */
+enum { WT_SOLVER_FMG = 0, WT_SOLVER_SRJ = 1, WT_SOLVER_MIXED_IR = 2 };
+
+typedef struct {
+  int method;                 /* WT_SOLVER_*                                         */
+  /* src/lin_solve.f90:11-26 module parameters (reference defaults in brackets)     */
+  int coarse_iter;            /* [50]  BiCGSTAB iterations on level_start           */
+  int max_vcycle;             /* [3]                                                 */
+  int pre_iter, down_iter, up_iter, post_iter;   /* [2, 2, 2, 4]                    */
+  int max_srj_iter;           /* [200]                                               */
+  double fine_tol, coarse_tol;/* [1e-3, 1e-3]                                        */
+  /* WT_SOLVER_MIXED_IR: FP64 refinement around FP32 V-cycles (down/up_iter sweeps,
+   * coarse_iter Jacobi sweeps on level_start); stop at ir_tol or ir_max.           */
+  double ir_tol;
+  int ir_max;
+} wt_solver_opts;
+
+typedef struct {
+  double nrm_res_init[16];    /* per level: initial ||f - L u|| / ||f||             */
+  double nrm_res_final[16];   /* per level: final normalised residual               */
+  int iterations[16];         /* per level: V-cycles / SRJ sweeps / BiCGSTAB its    */
+  int outer_iterations;       /* refinement steps (WT_SOLVER_MIXED_IR)              */
+  double true_rel_residual;   /* FP64 ||f - L u|| / ||f|| on level_end after solve  */
+  double ms;                  /* host wall time of the solve                         */
+} wt_solver_report;
+
+/* Builds the operator tables (replaces the per-call coefficient work of
+ * elliptic_lo / elliptic_lo_diag); allocates all solver work arrays once. */
+int wt_elliptic_setup(wt_handle* h, double dt, double theta1, double theta2, int domain_level);
+int wt_elliptic_upload(wt_handle* h, const double* u, const double* f);   /* either may be NULL */
+int wt_elliptic_download(wt_handle* h, double* u, double* f);             /* either may be NULL */
+/* f(level) = L(u(level)) on [0, n]^2 of one level (elliptic_lo). */
+int wt_elliptic_apply(wt_handle* h, int level);
+/* f on coarser levels from f on level_end by successive restriction
+ * (forward_scalar_transform, src/wavelet.f90:105-155). */
+int wt_elliptic_restrict(wt_handle* h);
+/* u on level fine from u on fine-1 (prolong, src/lin_solve.f90:243). */
+int wt_elliptic_prolong(wt_handle* h, int fine);
+/* l2 (src/lin_solve.f90:433) of u (which = 0) or f (which = 1) on one level. */
+int wt_elliptic_l2(wt_handle* h, int level, int which, double* out);
+/* Replaces elliptic_solver => FMG | SRJ (src/init.f90:127, src/lin_solve.f90:33,142)
+ * on the resident u, f.  Returns WT_ERR_NOT_CONVERGED when the mixed solver
+ * stops at ir_max above ir_tol. */
+int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report* rep);
+
 /* Raw stream of the handle (cudaStream_t), for event timing by the caller. */
 void* wt_stream(wt_handle* h);
 

@@ -89,3 +89,17 @@ def rk4(g, nz, ph, state, dt, nsteps):
                        _d(np.ascontiguousarray(state["topo"])))
     assert rc == 0
     return m, t, v
+
+
+def set_threads(n: int) -> None:
+    """Worker threads of the oracle (parallel over the 10 lozenge domains)."""
+    L = lib()
+    L.orc_set_threads.argtypes = [C.c_int]
+    L.orc_set_threads.restype = None
+    L.orc_set_threads(int(n))
+
+
+def get_threads() -> int:
+    L = lib()
+    L.orc_get_threads.restype = C.c_int
+    return int(L.orc_get_threads())

@@ -27,6 +27,10 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
+#include <thread>
 
 namespace {
 
@@ -47,6 +51,64 @@ struct Lev {
 struct Phys { double grav, ref_density, p_top; };
 
 inline double interp(double a, double b) { return 0.5 * (a + b); }   // src/utils.f90:528
+
+// Minimal persistent worker pool: run(fn) calls fn(d) for d = 0..9 (the ten
+// lozenge domains) spread over the workers and returns when all are done.
+// Results do not depend on the thread count (no cross-domain reductions).
+class Pool {
+ public:
+  void set_threads(int n) {
+    stop();
+    n = n < 1 ? 1 : (n > 10 ? 10 : n);
+    nthreads_ = n;
+    for (int t = 1; t < n; ++t) workers_.emplace_back([this, t] { loop(t); });
+  }
+  int threads() const { return nthreads_; }
+  void run(const std::function<void(int)>& fn) {
+    if (nthreads_ <= 1) { for (int d = 0; d < 10; ++d) fn(d); return; }
+    {
+      std::unique_lock<std::mutex> lk(m_);
+      fn_ = &fn; pending_ = nthreads_ - 1; ++gen_;
+    }
+    cv_.notify_all();
+    for (int d = 0; d < 10; d += nthreads_) fn(d);
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+  }
+  ~Pool() { stop(); }
+ private:
+  void loop(int t) {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(int)>* fn;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return quit_ || gen_ != seen; });
+        if (quit_) return;
+        seen = gen_; fn = fn_;
+      }
+      for (int d = t; d < 10; d += nthreads_) (*fn)(d);
+      std::unique_lock<std::mutex> lk(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  void stop() {
+    { std::unique_lock<std::mutex> lk(m_); quit_ = true; }
+    cv_.notify_all();
+    for (auto& w : workers_) w.join();
+    workers_.clear();
+    quit_ = false;
+    nthreads_ = 1;
+  }
+  std::vector<std::thread> workers_;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)>* fn_ = nullptr;
+  uint64_t gen_ = 0;
+  int pending_ = 0, nthreads_ = 1;
+  bool quit_ = false;
+};
+Pool& pool() { static Pool p; return p; }
 
 struct Ctx {
   const Lev& L;
@@ -354,13 +416,23 @@ void trend_ml(const Lev& L, const Phys& ph, int nz, double* mass, double* temp, 
   for (int k = 0; k < nz; ++k) {
     halo_nodes(L, mass + k * NN);
     halo_nodes(L, temp + k * NN);
-    for (int e = 0; e < 3; ++e) (void)e;
     halo_edges(L, velo + k * 3 * NN);
   }
-  Ctx c(L, ph);
+  // Every lozenge is an independent domain between ghost copies (the
+  // reference's MPI decomposition); the per-lozenge loops run in parallel.
+  auto ctx = [&](int d) {
+    Ctx c(L, ph);
+    c.d = d;
+    c.qe = w.qe.data(); c.vort = w.vort.data(); c.ke = w.ke.data(); c.bernoulli = w.bernoulli.data();
+    c.exner = w.exner.data(); c.hflux_m = w.hflux_m.data(); c.hflux_t = w.hflux_t.data(); c.geopot = w.geopot.data();
+    c.geopot_lower = w.geopot_lower.data(); c.press = w.press.data(); c.press_lower = w.press_lower.data();
+    c.surf_press = w.surf_press.data(); c.topo = topo;
+    return c;
+  };
   // zero_float_field over [-(BDRY-1), BDRY] (src/utils.f90:1217)
-  for (int k = 0; k < nz; ++k)
-    for (c.d = 0; c.d < 10; ++c.d)
+  pool().run([&](int d) {
+    Ctx c = ctx(d);
+    for (int k = 0; k < nz; ++k)
       for (int j = -1; j <= n + 1; ++j)
         for (int i = -1; i <= n + 1; ++i) {
           int64_t id = c.id(i, j);
@@ -368,13 +440,14 @@ void trend_ml(const Lev& L, const Phys& ph, int nz, double* mass, double* temp, 
           dtemp[k * NN + id] = 0.0;
           for (int e = 0; e < 3; ++e) dvelo[k * 3 * NN + e * NN + id] = 0.0;
         }
-  // cal_surf_press
-  for (c.d = 0; c.d < 10; ++c.d)
+  });
+  // cal_surf_press: set_surf_geopot over [-1, n+1]; column_mass over [0, n]
+  for (int64_t id = 0; id < NN; ++id) w.surf_press[id] = 0.0;
+  pool().run([&](int d) {
+    Ctx c = ctx(d);
     for (int j = -1; j <= n + 1; ++j)
       for (int i = -1; i <= n + 1; ++i) w.geopot[c.id(i, j)] = ph.grav * topo[c.id(i, j)];
-  std::fill(w.surf_press.begin(), w.surf_press.end(), 0.0);
-  for (int k = 0; k < nz; ++k)
-    for (c.d = 0; c.d < 10; ++c.d)
+    for (int k = 0; k < nz; ++k)
       for (int j = 0; j <= n; ++j)
         for (int i = 0; i <= n; ++i) {
           int64_t id = c.id(i, j);
@@ -382,19 +455,17 @@ void trend_ml(const Lev& L, const Phys& ph, int nz, double* mass, double* temp, 
           double rho_dz_theta = mean_t[k * NN + id] + temp[k * NN + id];
           w.surf_press[id] = w.surf_press[id] + (rho_dz - rho_dz_theta);
         }
+  });
   for (int64_t id = 0; id < NN; ++id) {
     w.surf_press[id] = ph.grav * w.surf_press[id] + ph.p_top;
     w.press_lower[id] = w.surf_press[id];
   }
-  c.qe = w.qe.data(); c.vort = w.vort.data(); c.ke = w.ke.data(); c.bernoulli = w.bernoulli.data();
-  c.exner = w.exner.data(); c.hflux_m = w.hflux_m.data(); c.hflux_t = w.hflux_t.data(); c.geopot = w.geopot.data();
-  c.geopot_lower = w.geopot_lower.data(); c.press = w.press.data(); c.press_lower = w.press_lower.data();
-  c.surf_press = w.surf_press.data(); c.topo = topo;
   for (int k = 0; k < nz; ++k) {
-    c.mass = mass + k * NN; c.temp = temp + k * NN; c.velo = velo + k * 3 * NN;
-    c.mean_m = mean_m + k * NN; c.mean_t = mean_t + k * NN;
     // basic_operators: integrate_pressure_up then step1, per lozenge; post_step1 at the corners
-    for (c.d = 0; c.d < 10; ++c.d) {
+    pool().run([&](int d) {
+      Ctx c = ctx(d);
+      c.mass = mass + k * NN; c.temp = temp + k * NN; c.velo = velo + k * 3 * NN;
+      c.mean_m = mean_m + k * NN; c.mean_t = mean_t + k * NN;
       for (int j = 0; j <= n; ++j)
         for (int i = 0; i <= n; ++i) {
           int64_t id = c.id(i, j);
@@ -408,20 +479,22 @@ void trend_ml(const Lev& L, const Phys& ph, int nz, double* mass, double* temp, 
         }
       step1(c);
       for (int corner = 5; corner <= 8; ++corner) post_step1(c, corner);   // apply_to_penta_d order NE..NW
-    }
+    });
     // cal_scalar_trend: update_bdry(horiz_flux) then scalar_trend over [0, n]
     halo_edges(L, w.hflux_m.data());
     halo_edges(L, w.hflux_t.data());
-    for (c.d = 0; c.d < 10; ++c.d)
+    double* dv = dvelo + k * 3 * NN;
+    pool().run([&](int d) {
+      Ctx c = ctx(d);
+      c.mass = mass + k * NN; c.temp = temp + k * NN; c.velo = velo + k * 3 * NN;
+      c.mean_m = mean_m + k * NN; c.mean_t = mean_t + k * NN;
       for (int j = 0; j <= n; ++j)
         for (int i = 0; i <= n; ++i) {
           int64_t id = c.id(i, j);
           dmass[k * NN + id] = -divg(c, w.hflux_m.data(), i, j);
           dtemp[k * NN + id] = -divg(c, w.hflux_t.data(), i, j);
         }
-    // velocity_trend_source (du_source) then velocity_trend_grad (du_grad) on owned nodes
-    double* dv = dvelo + k * 3 * NN;
-    for (c.d = 0; c.d < 10; ++c.d)
+      // velocity_trend_source (du_source) then velocity_trend_grad (du_grad) on owned nodes
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
           int64_t id = c.id(i, j);
@@ -429,7 +502,6 @@ void trend_ml(const Lev& L, const Phys& ph, int nz, double* mass, double* temp, 
           Qperp(c, i, j, Q);
           for (int e = 0; e < 3; ++e) dv[e * NN + id] = -Q[e] + 0.0 * L.len[e * NN + id];
         }
-    for (c.d = 0; c.d < 10; ++c.d)
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
           int64_t id = c.id(i, j), idE = c.id(i + 1, j), idN = c.id(i, j + 1), idNE = c.id(i + 1, j + 1);
@@ -450,6 +522,7 @@ void trend_ml(const Lev& L, const Phys& ph, int nz, double* mass, double* temp, 
           for (int e = 0; e < 3; ++e)
             dv[e * NN + id] = dv[e * NN + id] / L.len[e * NN + id] - gradB[e] - theta_e[e] * gradE[e];
         }
+    });
   }
 }
 
@@ -460,6 +533,10 @@ void rk_sub_step(int64_t count, const double* sol, const double* trend, double h
 }  // namespace
 
 extern "C" {
+
+void orc_set_threads(int n) { pool().set_threads(n); }
+
+int orc_get_threads(void) { return pool().threads(); }
 
 struct orc_level {
   int n, P;

@@ -58,6 +58,17 @@ class wt_grid_desc(C.Structure):
                 ("levels", C.POINTER(wt_level_desc))]
 
 
+class wt_solver_opts(C.Structure):
+    _fields_ = [("method", C.c_int), ("coarse_iter", C.c_int), ("max_vcycle", C.c_int), ("pre_iter", C.c_int),
+                ("down_iter", C.c_int), ("up_iter", C.c_int), ("post_iter", C.c_int), ("max_srj_iter", C.c_int),
+                ("fine_tol", C.c_double), ("coarse_tol", C.c_double), ("ir_tol", C.c_double), ("ir_max", C.c_int)]
+
+
+class wt_solver_report(C.Structure):
+    _fields_ = [("nrm_res_init", C.c_double * 16), ("nrm_res_final", C.c_double * 16), ("iterations", C.c_int * 16),
+                ("outer_iterations", C.c_int), ("true_rel_residual", C.c_double), ("ms", C.c_double)]
+
+
 _lib = None
 
 
@@ -99,6 +110,15 @@ _DEVICE_SIGS = {
     "wt_download_trend": [_vp, _dp, _dp, _dp],
     "wt_rk4_step": [_vp, C.c_double, C.c_int],
     "wt_rk4_step_host": [_vp, C.c_double, C.c_int, _dp, _dp, _dp],
+    "wt_profile_rk4": [_vp, C.c_double, C.c_int, _dp, C.POINTER(C.c_int)],
+    "wt_elliptic_setup": [_vp, C.c_double, C.c_double, C.c_double, C.c_int],
+    "wt_elliptic_upload": [_vp, _dp, _dp],
+    "wt_elliptic_download": [_vp, _dp, _dp],
+    "wt_elliptic_apply": [_vp, C.c_int],
+    "wt_elliptic_restrict": [_vp],
+    "wt_elliptic_prolong": [_vp, C.c_int],
+    "wt_elliptic_l2": [_vp, C.c_int, C.c_int, _dp],
+    "wt_elliptic_solve": [_vp, C.POINTER(wt_solver_opts), C.POINTER(wt_solver_report)],
 }
 
 

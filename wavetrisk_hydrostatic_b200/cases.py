@@ -92,3 +92,55 @@ def jet_state(g: LevelGeom, nz: int, seed: int = 0, ph: OceanParams | None = Non
         halo_nodes(g, temp[k])
         halo_edges(g, velo[k])
     return dict(mass=mass, temp=temp, velo=velo, mean_m=mean_m, mean_t=mean_t, topo=topo)
+
+
+def bathymetry(g: LevelGeom, seed: int = 0, lmax: int = 32, nterms: int = 160,
+               hmin: float = 500.0, hmax: float = 5000.0, _cache: dict = {}) -> np.ndarray:
+    """Smooth seeded random depth H in [hmin, hmax] m: a sum of zonal harmonics
+    P_l(x.a_q) of degree l <= lmax about random axes a_q with amplitude ~ l^-2
+    (every term is a spherical harmonic of degree l).  Returns topography = -H
+    at every node of the level (ghosts from their own coordinates)."""
+    from scipy.special import eval_legendre
+
+    key = (seed, lmax, nterms)
+    if key not in _cache:
+        rng = np.random.default_rng(seed)
+        ax = rng.standard_normal((nterms, 3))
+        ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+        deg = rng.integers(1, lmax + 1, nterms)
+        amp = rng.standard_normal(nterms) / deg.astype(float) ** 2
+        _cache[key] = (ax, deg, amp)
+    ax, deg, amp = _cache[key]
+    x = g.node
+    r = np.linalg.norm(x, axis=0)
+    ok = r > 0
+    u = np.zeros_like(x)
+    u[:, ok] = x[:, ok] / r[ok]
+    h = np.zeros(g.NN)
+    for a, l, c in zip(ax, deg, amp):
+        h += c * eval_legendre(int(l), np.clip(a @ u, -1.0, 1.0))
+    lo, hi = -sum(abs(amp)), sum(abs(amp))   # level-independent normalisation
+    H = hmin + (hmax - hmin) * (h - lo) / (hi - lo)
+    H[~ok] = hmin
+    return -H
+
+
+def elliptic_rhs(g: LevelGeom, seed: int = 0) -> np.ndarray:
+    """Seeded N(0,1) right-hand side on the owned nodes and poles of level g,
+    minus its area-weighted mean, copied to the ghosts."""
+    rng = np.random.default_rng(seed)
+    f = np.zeros(g.NN)
+    own = g.owned.copy()
+    npole, spole = g.pole_ids()
+    d, i, j = g.ij()
+    f[own] = rng.standard_normal(int(own.sum()))
+    pv = rng.standard_normal(2)
+    f[(d >= 5) & (i == 0) & (j == g.n)] = pv[0]
+    f[(d < 5) & (i == g.n) & (j == 0)] = pv[1]
+    area = np.where(g.hex_inv > 0, 1.0 / np.where(g.hex_inv > 0, g.hex_inv, 1.0), 0.0)
+    sel = own.copy()
+    sel[npole] = sel[spole] = True
+    mean = (f[sel] * area[sel]).sum() / area[sel].sum()
+    f[sel | ((d >= 5) & (i == 0) & (j == g.n)) | ((d < 5) & (i == g.n) & (j == 0))] -= mean
+    halo_nodes(g, f)
+    return f

@@ -12,26 +12,9 @@
 #pragma once
 #include <cstdint>
 
+#include "trisk_types.cuh"
+
 namespace wtk {
-
-enum { RT = 0, DG = 1, UP = 2 };
-enum { LORT = 0, UPLT = 1 };
-
-struct LevelDev {
-  int n, P;
-  int64_t NN;
-  const double* __restrict__ len;      // 3*NN
-  const double* __restrict__ pedlen;   // 3*NN
-  const double* __restrict__ part;     // 6*NN
-  const double* __restrict__ hex_inv;  // NN
-  const double* __restrict__ triarea;  // 2*NN
-  const double* __restrict__ coriolis; // 2*NN
-  const double* __restrict__ topo;     // NN
-};
-
-struct Phys {
-  double grav, ref_density, p_top;
-};
 
 __device__ __forceinline__ double interp(double a, double b) { return 0.5 * (a + b); }  // src/utils.f90:528
 

@@ -178,34 +178,75 @@ int wt_download_state(wt_handle* h, double* mass, double* temp, double* velo) {
 
 }  // extern "C"
 
+// Optional per-launch timing (wt_profile_rk4): events recorded around each
+// kernel on the handle's stream.
+struct KTimer {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> ids;
+  cudaStream_t s = nullptr;
+  void begin(int) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    ev.push_back(e);
+  }
+  void end(int id) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    ev.push_back(e);
+    ids.push_back(id);
+  }
+  ~KTimer() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+#define TB(id) \
+  if (tm) tm->begin(id)
+#define TE(id) \
+  if (tm) tm->end(id)
+
 // Launch sequence of one trend evaluation of state (m, t, v); MODE_RK writes
 // dst = base + hstep * trend, MODE_TREND writes the trends into h->dm/dt/dv.
 static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode, const double* bm, const double* bt,
-                        const double* bv, double* om, double* ot, double* ov, double hstep, bool halo_first) {
+                        const double* bv, double* om, double* ot, double* ov, double hstep, bool halo_first,
+                        KTimer* tm = nullptr) {
   DevLevel& D = h->top();
   LevelDev L = D.view();
   const int nz = h->nz;
   cudaStream_t s = h->stream;
   if (halo_first) {
     int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * nz;
+    TB(0);
     k_halo_state<<<blocks_for(nt), TPB, 0, s>>>(nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, m, t, v);
+    TE(0);
   }
   const int mm = D.n + 1;
+  TB(1);
   k_column<<<blocks_for(10 * mm * mm, 128), 128, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm);
+  TE(1);
   Step1Out so{h->qe, h->hfm, h->hft, h->bern};
+  TB(2);
   k_step1<<<blocks_for((int64_t)10 * mm * mm * nz), TPB, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
+  TE(2);
+  TB(3);
   k_post_step1<<<blocks_for(40 * nz, 64), 64, 0, s>>>(L, nz, m, v, h->mean_m, h->qe);
+  TE(3);
+  TB(4);
   k_halo_flux<<<blocks_for((int64_t)2 * D.n_he * nz), TPB, 0, s>>>(nz, D.NN, D.he, D.n_he, h->hfm, h->hft);
+  TE(4);
   TrendIO io{};
   io.mass = m; io.temp = t; io.mean_m = h->mean_m; io.mean_t = h->mean_t; io.qe = h->qe; io.hfm = h->hfm;
   io.hft = h->hft; io.bern = h->bern; io.phik = h->phik;
   io.base_m = bm; io.base_t = bt; io.base_v = bv; io.dst_m = om; io.dst_t = ot; io.dst_v = ov; io.h = hstep;
   io.dm = h->dm; io.dtt = h->dt; io.dv = h->dv;
   int64_t nt = D.NN * nz;
+  TB(5);
   if (mode == MODE_RK)
     k_trend<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
   else
     k_trend<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+  TE(5);
   CK(cudaGetLastError());
   return WT_OK;
 }
@@ -233,7 +274,7 @@ int wt_download_trend(wt_handle* h, double* dmass, double* dtemp, double* dvelo)
 
 // One RK4 step (src/time_integr.f90:78-103): four trend evaluations, each
 // fused with its sub-step, each followed by the ghost copy of WT_after_step.
-static int record_rk4(wt_handle* h, double dt) {
+static int record_rk4(wt_handle* h, double dt, KTimer* tm = nullptr) {
   DevLevel& D = h->top();
   const int nz = h->nz;
   const double hs[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
@@ -244,10 +285,12 @@ static int record_rk4(wt_handle* h, double dt) {
     double* om = stage == 3 ? h->mass : h->m1;
     double* ot = stage == 3 ? h->temp : h->t1;
     double* ov = stage == 3 ? h->velo : h->v1;
-    int rc = launch_trend(h, qm, qt, qv, MODE_RK, h->mass, h->temp, h->velo, om, ot, ov, hs[stage], false);
+    int rc = launch_trend(h, qm, qt, qv, MODE_RK, h->mass, h->temp, h->velo, om, ot, ov, hs[stage], false, tm);
     if (rc) return rc;
     int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * nz;
+    TB(0);
     k_halo_state<<<blocks_for(nt), TPB, 0, h->stream>>>(nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, om, ot, ov);
+    TE(0);
   }
   CK(cudaGetLastError());
   return WT_OK;
@@ -280,6 +323,32 @@ int wt_rk4_step(wt_handle* h, double dt, int nsteps) {
   return WT_OK;
 }
 
+// Same steps as wt_rk4_step, launched kernel by kernel (no graph) with CUDA
+// events around every launch; ms_per_launch[k] receives the average duration
+// of kernel k (0 halo_state, 1 column, 2 step1, 3 post_step1, 4 halo_flux,
+// 5 trend_rk) and *nkernels the number of kernel kinds.
+int wt_profile_rk4(wt_handle* h, double dt, int nsteps, double* ms_per_launch, int* nkernels) {
+  if (!h || nsteps < 1 || !ms_per_launch || !nkernels) return WT_ERR_ARG;
+  KTimer tm;
+  tm.s = h->stream;
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = record_rk4(h, dt, &tm);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  double tot[8] = {0};
+  int cnt[8] = {0};
+  for (size_t q = 0; q < tm.ids.size(); ++q) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, tm.ev[2 * q], tm.ev[2 * q + 1]));
+    tot[tm.ids[q]] += ms;
+    cnt[tm.ids[q]] += 1;
+  }
+  for (int k = 0; k < 6; ++k) ms_per_launch[k] = cnt[k] ? tot[k] / cnt[k] : 0.0;
+  *nkernels = 6;
+  return WT_OK;
+}
+
 int wt_rk4_step_host(wt_handle* h, double dt, int nsteps, double* mass, double* temp, double* velo) {
   if (!h || !mass || !temp || !velo) return WT_ERR_ARG;
   const int64_t nn = (int64_t)h->nz * h->top().NN;
@@ -297,5 +366,3 @@ int wt_rk4_step_host(wt_handle* h, double dt, int nsteps, double* mass, double* 
 }
 
 }  // extern "C"
-
-void wt_handle::release_extra() {}

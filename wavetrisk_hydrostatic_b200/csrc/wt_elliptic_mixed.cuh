@@ -1,0 +1,157 @@
+// Mixed precision solve: FP64 iterative refinement on the finest level around
+// FP32 multigrid V-cycles (Jacobi smoothing, lifted-wavelet restriction and
+// interpolation, Jacobi sweeps on the coarsest level).  The outer residual
+// f - L(u) and the correction u += c stay FP64; the V-cycle solves
+// L c = r approximately in FP32.  Included by wt_elliptic.cu only.
+#pragma once
+
+namespace {
+
+template <class T>
+__device__ __forceinline__ T rdwT(const EllLev& L, const T* __restrict__ f, int d, int i, int j) {
+  if (i < -2 || j < -2 || i > L.n + 1 || j > L.n + 1) return T(0);
+  return f[L.nsrc[nidx(L, d, i, j)]];
+}
+__device__ __forceinline__ float oaf(const EllLev& L, int d, int i, int j, int k) {
+  if (i < -2 || j < -2 || i > L.n + 1 || j > L.n + 1) return 0.f;
+  return (float)L.oa[(int64_t)(k - 1) * L.NN + nidx(L, d, i, j)];
+}
+__device__ __forceinline__ float interp_node32(const EllLev& F, const float* s, int d, int i, int j, int i1, int j1,
+                                               int i2, int j2, int i3, int j3, int i4, int j4) {
+  return (oaf(F, d, i, j, 1) * rdwT(F, s, d, i1, j1) + oaf(F, d, i, j, 2) * rdwT(F, s, d, i2, j2) +
+          oaf(F, d, i, j, 3) * rdwT(F, s, d, i3, j3) + oaf(F, d, i, j, 4) * rdwT(F, s, d, i4, j4)) *
+         F.hinvf[nidx(F, d, i, j)];
+}
+
+// FP32 restriction of a residual (wavelets + lifting) from level c+1 to c.
+__global__ void k_wc_compute32(EllLev C, EllLev F, const float* __restrict__ s, float* __restrict__ wc) {
+  const int m = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  int d, ip, jp;
+  decode(C, t, d, ip, jp, m);
+  const int i = 2 * ip, j = 2 * jp;
+  wc[nidx(F, d, i + 1, j)] = rdwT(F, s, d, i + 1, j) - interp_node32(F, s, d, i + 1, j, i, j, i + 2, j, i + 2, j + 2, i, j - 2);
+  wc[nidx(F, d, i + 1, j + 1)] =
+      rdwT(F, s, d, i + 1, j + 1) - interp_node32(F, s, d, i + 1, j + 1, i + 2, j + 2, i, j, i + 2, j, i, j + 2);
+  wc[nidx(F, d, i, j + 1)] = rdwT(F, s, d, i, j + 1) - interp_node32(F, s, d, i, j + 1, i, j, i, j + 2, i - 2, j, i + 2, j + 2);
+}
+
+__global__ void k_restrict32(EllLev C, EllLev F, const float* __restrict__ sf, const float* __restrict__ wc,
+                             float* __restrict__ sc) {
+  const int m = C.n + 1;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  int d, ip, jp;
+  decode(C, t, d, ip, jp, m);
+  const int64_t kp = nidx(C, d, ip, jp);
+  if (C.nsrc[kp] != kp) return;
+  const int i = 2 * ip, j = 2 * jp;
+#define W(a, b, k) (rdwT(F, wc, d, i + (a), j + (b)) * oaf(F, d, i + (a), j + (b), k))
+  const float sum = W(1, 0, 1) + W(1, 1, 2) + W(2, 1, 3) + W(1, 2, 4) + W(0, 1, 1) + W(-1, 0, 2) + W(-1, 1, 3) +
+                    W(-2, -1, 4) + W(-1, -1, 1) + W(0, -1, 2) + W(-1, -2, 3) + W(1, -1, 4);
+#undef W
+  sc[kp] = sf[nidx(F, d, i, j)] + sum * C.hinvf[kp];
+}
+
+// Interpolation of a coarse correction onto level f (zero wavelets): even
+// children copy the parent, odd children interpolate.  acc: add into dst.
+__global__ void k_interp_even32(EllLev C, EllLev F, const float* __restrict__ sc, float* __restrict__ sf) {
+  const int m = C.n + 1;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  int d, ip, jp;
+  decode(C, t, d, ip, jp, m);
+  const int64_t kc = nidx(F, d, 2 * ip, 2 * jp);
+  if (F.nsrc[kc] != kc) return;
+  sf[kc] = sc[C.nsrc[nidx(C, d, ip, jp)]];
+}
+__global__ void k_interp_odd32(EllLev C, EllLev F, float* __restrict__ s) {
+  const int m = C.n;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  int d, ip, jp;
+  decode(C, t, d, ip, jp, m);
+  const int i = 2 * ip, j = 2 * jp;
+  float a = interp_node32(F, s, d, i + 1, j, i, j, i + 2, j, i + 2, j + 2, i, j - 2);
+  float b = interp_node32(F, s, d, i + 1, j + 1, i + 2, j + 2, i, j, i + 2, j, i, j + 2);
+  float c = interp_node32(F, s, d, i, j + 1, i, j, i, j + 2, i - 2, j, i + 2, j + 2);
+  s[nidx(F, d, i + 1, j)] = a;
+  s[nidx(F, d, i + 1, j + 1)] = b;
+  s[nidx(F, d, i, j + 1)] = c;
+}
+
+__global__ void k_add32(int64_t n, float* __restrict__ a, const float* __restrict__ b) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) a[t] += b[t];
+}
+__global__ void k_d2f(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) b[t] = (float)a[t];
+}
+// u += (double) c  on the whole level (ghost copies are refreshed by reads via nsrc)
+__global__ void k_axpy_f2d(int64_t n, double* __restrict__ u, const float* __restrict__ c) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) u[t] = u[t] + (double)c[t];
+}
+
+void jacobi32(Ell& E, MField& u, MField& f, int l, int iters, float w = 1.f) {
+  EllLev V = E.view(l);
+  unsigned g = nb(10 * E.m(l) * E.m(l));
+  for (int it = 0; it < iters; ++it) {
+    k_ell_op32<OP_JACOBI><<<g, TPB, 0, E.s()>>>(V, u.lvf[l - E.ls], f.lvf[l - E.ls], E.t32.lvf[l - E.ls], w);
+    std::swap(u.lvf[l - E.ls], E.t32.lvf[l - E.ls]);
+  }
+}
+
+// One FP32 V-cycle for L c = r on levels ls..le, c returned in E.c32 (level le).
+void vcycle32(Ell& E, const wt_solver_opts& o) {
+  for (int j = E.ls; j <= E.le; ++j) cudaMemsetAsync(E.c32.lvf[j - E.ls], 0, 4 * E.L[j - E.ls].NN, E.s());
+  for (int j = E.le; j >= E.ls + 1; --j) {
+    jacobi32(E, E.c32, E.r32, j, o.down_iter);
+    EllLev V = E.view(j);
+    unsigned g = nb(10 * E.m(j) * E.m(j));
+    // residual r - L c into t32 (level j), then restrict it into r32 at level j-1
+    k_ell_op32<OP_RESID><<<g, TPB, 0, E.s()>>>(V, E.c32.lvf[j - E.ls], E.r32.lvf[j - E.ls], E.u32.lvf[j - E.ls], 1.f);
+    EllLev C = E.view(j - 1), F = E.view(j);
+    int n = E.L[j - 1 - E.ls].n;
+    cudaMemsetAsync(E.f32.lvf[j - E.ls], 0, 4 * E.L[j - E.ls].NN, E.s());
+    k_wc_compute32<<<nb(10 * n * n), TPB, 0, E.s()>>>(C, F, E.u32.lvf[j - E.ls], E.f32.lvf[j - E.ls]);
+    k_restrict32<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, E.u32.lvf[j - E.ls], E.f32.lvf[j - E.ls],
+                                                                 E.r32.lvf[j - 1 - E.ls]);
+  }
+  jacobi32(E, E.c32, E.r32, E.ls, o.coarse_iter);
+  for (int j = E.ls + 1; j <= E.le; ++j) {
+    EllLev C = E.view(j - 1), F = E.view(j);
+    int n = E.L[j - 1 - E.ls].n;
+    k_interp_even32<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, E.c32.lvf[j - 1 - E.ls], E.u32.lvf[j - E.ls]);
+    k_interp_odd32<<<nb(10 * n * n), TPB, 0, E.s()>>>(C, F, E.u32.lvf[j - E.ls]);
+    int64_t NN = E.L[j - E.ls].NN;
+    k_add32<<<nb(NN), TPB, 0, E.s()>>>(NN, E.c32.lvf[j - E.ls], E.u32.lvf[j - E.ls]);
+    jacobi32(E, E.c32, E.r32, j, o.up_iter);
+  }
+}
+
+int mixed_ir(Ell& E, const wt_solver_opts& o, wt_solver_report& rep) {
+  const int l = E.le, q = l - E.ls;
+  const int64_t NN = E.L[q].NN;
+  double nf = l2(E, l, E.f.lv[q]);
+  if (nf == 0.0) nf = 1.0;
+  int it;
+  double err = 0.0;
+  for (it = 0; it <= o.ir_max; ++it) {
+    op(E, OP_RESID, l, E.u.lv[q], E.f.lv[q], E.res.lv[q]);
+    err = l2(E, l, E.res.lv[q]) / nf;
+    if (it == 0) rep.nrm_res_init[q] = err;
+    if (err <= o.ir_tol || it == o.ir_max) break;
+    k_d2f<<<nb(NN), TPB, 0, E.s()>>>(NN, E.res.lv[q], E.r32.lvf[q]);
+    vcycle32(E, o);
+    k_axpy_f2d<<<nb(NN), TPB, 0, E.s()>>>(NN, E.u.lv[q], E.c32.lvf[q]);
+  }
+  rep.outer_iterations = it;
+  rep.nrm_res_final[q] = err;
+  rep.iterations[q] = it;
+  return err <= o.ir_tol ? WT_OK : WT_ERR_NOT_CONVERGED;
+}
+
+}  // namespace

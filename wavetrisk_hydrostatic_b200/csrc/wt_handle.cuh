@@ -5,7 +5,7 @@
 #include <cstdint>
 #include <vector>
 
-#include "trisk_kernels.cuh"
+#include "trisk_types.cuh"
 
 struct DevLevel {
   int level = 0, n = 0, P = 0;

@@ -115,3 +115,64 @@ class TriskModel(DeviceGrid):
 
     def synchronize(self) -> None:
         N.check("wt_synchronize", N.lib().wt_synchronize(self.h))
+
+
+def solver_opts(method: str = "fmg", tol: float = 1e-10, **kw):
+    """wt_solver_opts with the reference's defaults (src/lin_solve.f90:11-26),
+    tolerances set to tol.  method: 'fmg', 'srj' or 'mixed'."""
+    o = N.wt_solver_opts()
+    o.method = {"fmg": 0, "srj": 1, "mixed": 2}[method]
+    o.coarse_iter, o.max_vcycle = 50, 3
+    o.pre_iter, o.down_iter, o.up_iter, o.post_iter = 2, 2, 2, 4
+    o.max_srj_iter = 200
+    o.fine_tol = o.coarse_tol = tol
+    o.ir_tol, o.ir_max = tol, 60
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class EllipticSolver(DeviceGrid):
+    """Barotropic free-surface solve on a uniform hierarchy (elliptic_solver)."""
+
+    def __init__(self, levels: list[LevelGeom], topos: list[np.ndarray], ph: OceanParams | None = None,
+                 dt: float = 600.0, theta1: float = 1.0, theta2: float = 1.0, domain_level: int = 2):
+        super().__init__(levels, topos, 1, ph)
+        self.offsets = np.cumsum([0] + [g.NN for g in levels])
+        N.check("wt_elliptic_setup", N.lib().wt_elliptic_setup(self.h, dt, theta1, theta2, domain_level))
+
+    def field(self) -> np.ndarray:
+        return np.zeros(int(self.offsets[-1]))
+
+    def level_view(self, a: np.ndarray, q: int) -> np.ndarray:
+        return a[self.offsets[q]:self.offsets[q + 1]]
+
+    def upload(self, u=None, f=None):
+        N.check("wt_elliptic_upload", N.lib().wt_elliptic_upload(self.h, N.dptr(u), N.dptr(f)))
+
+    def download(self):
+        u, f = self.field(), self.field()
+        N.check("wt_elliptic_download", N.lib().wt_elliptic_download(self.h, N.dptr(u), N.dptr(f)))
+        return u, f
+
+    def apply(self, level: int) -> None:
+        N.check("wt_elliptic_apply", N.lib().wt_elliptic_apply(self.h, level))
+
+    def restrict(self) -> None:
+        N.check("wt_elliptic_restrict", N.lib().wt_elliptic_restrict(self.h))
+
+    def prolong(self, fine: int) -> None:
+        N.check("wt_elliptic_prolong", N.lib().wt_elliptic_prolong(self.h, fine))
+
+    def l2(self, level: int, which: int = 1) -> float:
+        v = C.c_double()
+        N.check("wt_elliptic_l2", N.lib().wt_elliptic_l2(self.h, level, which, C.byref(v)))
+        return v.value
+
+    def solve(self, opts) -> "N.wt_solver_report":
+        rep = N.wt_solver_report()
+        rc = N.lib().wt_elliptic_solve(self.h, C.byref(opts), C.byref(rep))
+        if rc not in (N.WT_OK, N.WT_ERR_NOT_CONVERGED):
+            N.check("wt_elliptic_solve", rc)
+        rep.status = rc
+        return rep

@@ -5,6 +5,11 @@
 // (E = +1, N = +P, NE = P+1, W = -1, S = -P, SW = -P-1, SE = 1-P, NW = P-1):
 // the kernels never branch on patch or boundary-patch membership.
 //
+// Ghost cells of the prognostic state and of the mass flux are not copied:
+// threads near a lozenge border read them through the level's remap tables
+// (nsrc, esrc), which name the node or signed edge the reference's
+// update_bdry copies there.  Threads in the interior read directly.
+//
 // Floating point follows the reference expression by expression (operand order
 // and parenthesisation of src/ops.f90); the file is compiled with --fmad=false
 // so that no multiply-add is contracted, which keeps every result bit-identical
@@ -22,9 +27,26 @@ __device__ __forceinline__ int64_t nid(const LevelDev& L, int d, int i, int j) {
   return ((int64_t)d * L.P + (j + 2)) * L.P + (i + 2);
 }
 
+// Readers of the state through the ghost remap.
+struct Rd {
+  const LevelDev& L;
+  bool direct;
+  __device__ __forceinline__ double n(const double* __restrict__ f, int64_t x) const {
+    return direct ? f[x] : f[L.nsrc[x]];
+  }
+  // edge field with planes of NN: slot = e*NN + x
+  __device__ __forceinline__ double e(const double* __restrict__ f, int64_t slot) const {
+    if (direct) return f[slot];
+    const int c = L.esrc[slot];
+    const double v = f[c >> 1];
+    return (c & 1) ? -v : v;
+  }
+};
+
 // --------------------------------------------------------------------------
 // Ghost copy (cp_bdry_inside, src/comm.f90:785-808) of the layered state:
-// node entries for mass and temp, signed edge entries for velocity.
+// node entries for mass and temp, signed edge entries for velocity.  Used to
+// hand the host a state whose ghosts hold their copies.
 __global__ void k_halo_state(int nz, int64_t NN, const int2* __restrict__ hn, int n_hn, const int3* __restrict__ he,
                              int n_he, double* __restrict__ mass, double* __restrict__ temp, double* __restrict__ velo) {
   const int per_layer = 2 * n_hn + n_he;
@@ -44,53 +66,137 @@ __global__ void k_halo_state(int nz, int64_t NN, const int2* __restrict__ hn, in
   }
 }
 
-// Ghost copy of the two horizontal flux fields (update_bdry(horiz_flux),
-// src/multi_level.f90:110) for all layers.
-__global__ void k_halo_flux(int nz, int64_t NN, const int3* __restrict__ he, int n_he, double* __restrict__ hfm,
-                            double* __restrict__ hft) {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)2 * n_he * nz) return;
-  int k = (int)(t / (2 * n_he));
-  int r = (int)(t - (int64_t)k * 2 * n_he);
-  double* f = (r < n_he ? hfm : hft) + (int64_t)k * 3 * NN;
-  int3 e = he[r % n_he];
-  double v = f[e.y];
-  f[e.x] = e.z < 0 ? -v : v;
-}
-
 // --------------------------------------------------------------------------
 // Column pass: cal_surf_press/column_mass (src/ops.f90:1023-1072) and
 // integrate_pressure_up (src/ops.f90:1094-1131), incompressible case, for every
 // node (i, j) in [0, n]^2 of every lozenge.  Writes the layer geopotential
 // Phi_k = interp(geopot, geopot_lower) and press/(rho0*phi).
-__global__ void k_column(LevelDev L, Phys ph, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
-                         const double* __restrict__ mean_m, const double* __restrict__ mean_t,
-                         double* __restrict__ phik, double* __restrict__ pterm) {
+__global__ void __launch_bounds__(128) k_column(LevelDev L, Phys ph, int nz, const double* __restrict__ mass,
+                                                const double* __restrict__ temp, const double* __restrict__ mean_m,
+                                                const double* __restrict__ mean_t, double* __restrict__ phik,
+                                                double* __restrict__ pterm) {
   const int m = L.n + 1;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 10 * m * m) return;
   int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
-  int64_t id = nid(L, d, i, j);
+  const int64_t id = nid(L, d, i, j);
+  const int64_t src = (i < L.n && j < L.n) ? id : (int64_t)L.nsrc[id];
   double sp = 0.0;
   for (int k = 0; k < nz; ++k) {
-    int64_t o = (int64_t)k * L.NN + id;
-    double rho_dz = mean_m[o] + mass[o];
-    double rho_dz_theta = mean_t[o] + temp[o];
+    const int64_t o = (int64_t)k * L.NN;
+    double rho_dz = mean_m[o + id] + mass[o + src];
+    double rho_dz_theta = mean_t[o + id] + temp[o + src];
     sp = sp + (rho_dz - rho_dz_theta);
   }
   double p_lower = ph.grav * sp + ph.p_top;
   double geopot = ph.grav * L.topo[id];
   for (int k = 0; k < nz; ++k) {
-    int64_t o = (int64_t)k * L.NN + id;
-    double rho_dz = mean_m[o] + mass[o];
-    double rho_dz_theta = mean_t[o] + temp[o];
+    const int64_t o = (int64_t)k * L.NN;
+    double rho_dz = mean_m[o + id] + mass[o + src];
+    double rho_dz_theta = mean_t[o + id] + temp[o + src];
     double geopot_lower = geopot;
     double p_upper = p_lower - ph.grav * (rho_dz - rho_dz_theta);
     double press = interp(p_lower, p_upper);
     geopot = geopot_lower + ph.grav * rho_dz / (ph.ref_density * 1.0);
     p_lower = p_upper;
-    phik[o] = interp(geopot, geopot_lower);
-    pterm[o] = press / (ph.ref_density * 1.0);
+    phik[o + id] = interp(geopot, geopot_lower);
+    pterm[o + id] = press / (ph.ref_density * 1.0);
+  }
+}
+
+struct Step1Out {
+  double* __restrict__ qe;    // [nz][3][NN]
+  double* __restrict__ hfm;   // [nz][3][NN]
+  double* __restrict__ hft;   // [nz][3][NN]
+  double* __restrict__ bern;  // [nz][NN]
+};
+
+// post_step1 (src/ops.f90:526-737): PV of the merged triangle at a pentagon
+// corner.  Run by the thread that owns the corrected edges; the vorticity the
+// reference reads back from its vort array is re-formed from the same
+// circulation sum its last writer used, divided by the same triangle area.
+__device__ __noinline__ void post_corner(const LevelDev& L, int c, int d, int64_t ko, const double* __restrict__ mass,
+                                         const double* __restrict__ velo, const double* __restrict__ mean_m,
+                                         double* __restrict__ qe) {
+  const int n = L.n;
+  const int64_t NN = L.NN;
+  const Rd R{L, false};
+  const double* v = velo + 3 * ko;
+  auto rho = [&](int64_t x) { return R.n(mass + ko, x) + mean_m[ko + x]; };
+  auto pr = [&](int e, int64_t x) { return R.e(v, (int64_t)e * NN + x) * L.len[(int64_t)e * NN + x]; };
+  auto part = [&](int64_t x, int kk) { return L.part[(int64_t)(kk - 1) * NN + x]; };
+  auto tri = [&](int tt, int64_t x) { return L.triarea[(int64_t)tt * NN + x]; };
+  auto cor = [&](int tt, int64_t x) { return L.coriolis[(int64_t)tt * NN + x]; };
+  auto I = [&](int i, int j) { return nid(L, d, i, j); };
+  double* q = qe + 3 * ko;
+  if (c == 0) {  // IJPLUS (north-east corner)
+    int64_t id = I(n, n), idN = I(n, n + 1), idE = I(n + 1, n), idS = I(n, n - 1), idW = I(n - 1, n);
+    double r0 = rho(id), rN = rho(idN), rE = rho(idE), rS = rho(idS), rW = rho(idW);
+    double circ_LORT = pr(RT, id) - pr(RT, idN) - pr(UP, id);
+    double vW = (pr(RT, idW) + pr(UP, id) + pr(DG, idW)) / tri(LORT, idW);
+    double vS = -(pr(DG, idS) + pr(UP, idS) + pr(RT, id)) / tri(UPLT, idS);
+    double circ_W_LORT = vW * tri(LORT, idW);
+    double circ_S_UPLT = vS * tri(UPLT, idS);
+    double pm1 = rE * part(idE, 3) + r0 * (part(id, 1) + part(id, 2)) + rN * part(idN, 6);
+    double pm2 = rW * part(idW, 1) + r0 * part(id, 3) + rN * part(idN, 5);
+    double pm3 = rS * part(idS, 2) + rE * part(idE, 4) + r0 * part(id, 6);
+    double pv_LORT = (cor(LORT, id) + circ_LORT) / pm1;
+    double pv_W_LORT = (cor(LORT, idW) + circ_W_LORT) / pm2;
+    double pv_S_UPLT = (cor(UPLT, idS) + circ_S_UPLT) / pm3;
+    double pv_UPLT = pv_LORT;
+    q[(int64_t)RT * NN + id] = interp(pv_LORT, pv_S_UPLT);
+    q[(int64_t)UP * NN + id] = interp(pv_UPLT, pv_W_LORT);
+  } else if (c == 1) {  // IPLUSJMINUS (south-east corner)
+    int64_t id = I(n, 0), idE = I(n + 1, 0), idS = I(n, -1), idW = I(n - 1, 0), idNE = I(n + 1, 1), idSW = I(n - 1, -1);
+    double r0 = rho(id), rE = rho(idE), rS = rho(idS), rW = rho(idW), rNE = rho(idNE), rSW = rho(idSW);
+    double circ_SW_LORT = -pr(RT, id) + pr(RT, idSW) + pr(DG, idSW);
+    double vL = (pr(RT, id) + pr(UP, idE) + pr(DG, id)) / tri(LORT, id);
+    double vU = -(pr(RT, idW) + pr(DG, idSW) + pr(UP, idSW)) / tri(UPLT, idSW);
+    double circ_LORT = vL * tri(LORT, id);
+    double circ_SW_UPLT = vU * tri(UPLT, idSW);
+    double pm1 = rSW * part(idSW, 1) + rS * part(idS, 3) + r0 * (part(id, 5) + part(id, 6));
+    double pm2 = r0 * part(id, 1) + rE * part(idE, 3) + rNE * part(idNE, 5);
+    double pm3 = rSW * part(idSW, 2) + r0 * part(id, 4) + rW * part(idW, 6);
+    double pv_SW_LORT = (cor(LORT, idSW) + circ_SW_LORT) / pm1;
+    double pv_LORT = (cor(LORT, id) + circ_LORT) / pm2;
+    double pv_SW_UPLT = (cor(UPLT, idSW) + circ_SW_UPLT) / pm3;
+    double pv_S_UPLT = pv_SW_LORT;
+    q[(int64_t)RT * NN + id] = interp(pv_S_UPLT, pv_LORT);
+    q[(int64_t)DG * NN + idSW] = interp(pv_SW_LORT, pv_SW_UPLT);
+  } else if (c == 2) {  // IJMINUS (south-west corner)
+    int64_t id = I(0, 0), idN = I(0, 1), idE = I(1, 0), idS = I(0, -1), idW = I(-1, 0), idSW = I(-1, -1);
+    double r0 = rho(id), rN = rho(idN), rE = rho(idE), rS = rho(idS), rW = rho(idW);
+    double circ_SW_LORT = pr(UP, idS) - pr(RT, idW) + pr(RT, idSW);
+    double vW = (pr(RT, idW) + pr(UP, id) + pr(DG, idW)) / tri(LORT, idW);
+    double vS = -(pr(RT, id) + pr(DG, idS) + pr(UP, idS)) / tri(UPLT, idS);
+    double circ_W_LORT = vW * tri(LORT, idW);
+    double circ_S_UPLT = vS * tri(UPLT, idS);
+    double pm1 = rW * part(idW, 6) + r0 * (part(id, 4) + part(id, 5)) + rS * part(idS, 3);
+    double pm2 = rW * part(idW, 1) + r0 * part(id, 3) + rN * part(idN, 5);
+    double pm3 = rS * part(idS, 2) + rE * part(idE, 4) + r0 * part(id, 6);
+    double pv_W_LORT = (cor(LORT, idW) + circ_W_LORT) / pm1;
+    double pv_SW_LORT = (cor(LORT, idSW) + circ_SW_LORT) / pm2;
+    double pv_S_UPLT = (cor(UPLT, idS) + circ_S_UPLT) / pm3;
+    double pv_SW_UPLT = pv_SW_LORT;
+    q[(int64_t)RT * NN + idW] = interp(pv_W_LORT, pv_SW_UPLT);
+    q[(int64_t)UP * NN + idS] = interp(pv_S_UPLT, pv_SW_LORT);
+  } else {  // IMINUSJPLUS (north-west corner)
+    int64_t id = I(0, n), idN = I(0, n + 1), idS = I(0, n - 1), idW = I(-1, n), idNE = I(1, n + 1), idSW = I(-1, n - 1);
+    double r0 = rho(id), rN = rho(idN), rS = rho(idS), rW = rho(idW), rNE = rho(idNE), rSW = rho(idSW);
+    double circ_SW_UPLT = pr(UP, id) - pr(DG, idSW) - pr(UP, idSW);
+    double vU = -(pr(DG, id) + pr(UP, id) + pr(RT, idN)) / tri(UPLT, id);
+    double vL = (pr(RT, idSW) + pr(UP, idS) + pr(DG, idSW)) / tri(LORT, idSW);
+    double circ_UPLT = vU * tri(UPLT, id);
+    double circ_SW_LORT = vL * tri(LORT, idSW);
+    double pm1 = rSW * part(idSW, 2) + r0 * (part(id, 3) + part(id, 4)) + rW * part(idW, 6);
+    double pm2 = r0 * part(id, 2) + rNE * part(idNE, 4) + rN * part(idN, 6);
+    double pm3 = rSW * part(idSW, 1) + rS * part(idS, 3) + r0 * part(id, 5);
+    double pv_SW_UPLT = (cor(UPLT, idSW) + circ_SW_UPLT) / pm1;
+    double pv_UPLT = (cor(UPLT, id) + circ_UPLT) / pm2;
+    double pv_SW_LORT = (cor(LORT, idSW) + circ_SW_LORT) / pm3;
+    double pv_W_LORT = pv_SW_UPLT;
+    q[(int64_t)UP * NN + id] = interp(pv_W_LORT, pv_UPLT);
+    q[(int64_t)DG * NN + idSW] = interp(pv_SW_LORT, pv_SW_UPLT);
   }
 }
 
@@ -100,18 +206,12 @@ __global__ void k_column(LevelDev L, Phys ph, int nz, const double* __restrict__
 // kinetic energy and the Bernoulli function.  comp_SW runs where i == 0 or
 // j == 0, as at the reference's south and west domain boundaries.  Each edge
 // has exactly one writer, chosen so that the stored value is the one the
-// reference's sequential sweep leaves behind.
-struct Step1Out {
-  double* __restrict__ qe;    // [nz][3][NN]
-  double* __restrict__ hfm;   // [nz][3][NN]
-  double* __restrict__ hft;   // [nz][3][NN]
-  double* __restrict__ bern;  // [nz][NN]
-};
-
-__global__ void k_step1(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
-                        const double* __restrict__ velo, const double* __restrict__ mean_m,
-                        const double* __restrict__ mean_t, const double* __restrict__ phik,
-                        const double* __restrict__ pterm, Step1Out out) {
+// reference's sequential sweep leaves behind; the four corner threads then
+// apply post_step1.
+__global__ void __launch_bounds__(256, 2)
+    k_step1(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
+            const double* __restrict__ velo, const double* __restrict__ mean_m, const double* __restrict__ mean_t,
+            const double* __restrict__ phik, const double* __restrict__ pterm, Step1Out out) {
   const int m = L.n + 1;
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)10 * m * m * nz) return;
@@ -125,6 +225,7 @@ __global__ void k_step1(LevelDev L, int nz, const double* __restrict__ mass, con
   const int64_t id = nid(L, d, i, j);
   const int64_t idN = id + P, idE = id + 1, idS = id - P, idW = id - 1, idNE = id + P + 1, idSW = id - P - 1;
   const int64_t ko = (int64_t)k * NN;
+  const Rd R{L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2};
   const double* Mm = mass + ko;
   const double* Mt = temp + ko;
   const double* Am = mean_m + ko;
@@ -140,12 +241,10 @@ __global__ void k_step1(LevelDev L, int nz, const double* __restrict__ mass, con
 #define E3(e, x) ((int64_t)(e) * NN + (x))
 #define PART(x, kk) part[(int64_t)((kk) - 1) * NN + (x)]
 
-  const double r0 = Mm[id] + Am[id], rN = Mm[idN] + Am[idN], rE = Mm[idE] + Am[idE], rS = Mm[idS] + Am[idS],
-               rW = Mm[idW] + Am[idW], rNE = Mm[idNE] + Am[idNE];
-  const double t0 = Mt[id] + At[id], tN = Mt[idN] + At[idN], tE = Mt[idE] + At[idE], tNE = Mt[idNE] + At[idNE];
-
-  const double vRT = v[E3(RT, id)], vDG = v[E3(DG, id)], vUP = v[E3(UP, id)];
-  const double vRT_W = v[E3(RT, idW)], vDG_SW = v[E3(DG, idSW)], vUP_S = v[E3(UP, idS)];
+  const double r0 = R.n(Mm, id) + Am[id], rN = R.n(Mm, idN) + Am[idN], rE = R.n(Mm, idE) + Am[idE],
+               rS = R.n(Mm, idS) + Am[idS], rW = R.n(Mm, idW) + Am[idW], rNE = R.n(Mm, idNE) + Am[idNE];
+  const double vRT = R.e(v, E3(RT, id)), vDG = R.e(v, E3(DG, id)), vUP = R.e(v, E3(UP, id));
+  const double vRT_W = R.e(v, E3(RT, idW)), vDG_SW = R.e(v, E3(DG, idSW)), vUP_S = R.e(v, E3(UP, idS));
   const double u_dual_RT = vRT * ped[E3(RT, id)];
   const double u_dual_DG = vDG * ped[E3(DG, id)];
   const double u_dual_UP = vUP * ped[E3(UP, id)];
@@ -154,30 +253,26 @@ __global__ void k_step1(LevelDev L, int nz, const double* __restrict__ mass, con
   const double u_dual_UP_S = vUP_S * ped[E3(UP, idS)];
 
   const double u_prim_RT = vRT * len[E3(RT, id)];
-  const double u_prim_RT_N = v[E3(RT, idN)] * len[E3(RT, idN)];
   const double u_prim_RT_W = vRT_W * len[E3(RT, idW)];
   const double u_prim_DG = vDG * len[E3(DG, id)];
-  const double u_prim_DG_S = v[E3(DG, idS)] * len[E3(DG, idS)];
   const double u_prim_DG_SW = vDG_SW * len[E3(DG, idSW)];
-  const double u_prim_DG_W = v[E3(DG, idW)] * len[E3(DG, idW)];
   const double u_prim_UP = vUP * len[E3(UP, id)];
-  const double u_prim_UP_E = v[E3(UP, idE)] * len[E3(UP, idE)];
   const double u_prim_UP_S = vUP_S * len[E3(UP, idS)];
+  const double u_prim_DG_W = R.e(v, E3(DG, idW)) * len[E3(DG, idW)];
+  const double u_prim_UP_E = R.e(v, E3(UP, idE)) * len[E3(UP, idE)];
 
   const double circ_LORT = u_prim_RT + u_prim_UP_E + u_prim_DG;
-  const double circ_UPLT = -(u_prim_DG + u_prim_UP + u_prim_RT_N);
   const double circ_W_LORT = u_prim_RT_W + u_prim_UP + u_prim_DG_W;
+  const double pv_LORT = (cor[E3(LORT, id)] + circ_LORT) / (r0 * PART(id, 1) + rE * PART(idE, 3) + rNE * PART(idNE, 5));
+  const double pv_W_LORT =
+      (cor[E3(LORT, idW)] + circ_W_LORT) / (rW * PART(idW, 1) + r0 * PART(id, 3) + rN * PART(idN, 5));
+  const double u_prim_RT_N = R.e(v, E3(RT, idN)) * len[E3(RT, idN)];
+  const double circ_UPLT = -(u_prim_DG + u_prim_UP + u_prim_RT_N);
+  const double pv_UPLT = (cor[E3(UPLT, id)] + circ_UPLT) / (r0 * PART(id, 2) + rNE * PART(idNE, 4) + rN * PART(idN, 6));
+  const double u_prim_DG_S = R.e(v, E3(DG, idS)) * len[E3(DG, idS)];
   const double circ_S_UPLT = -(u_prim_RT + u_prim_DG_S + u_prim_UP_S);
-
-  const double pm1 = r0 * PART(id, 1) + rE * PART(idE, 3) + rNE * PART(idNE, 5);
-  const double pm2 = r0 * PART(id, 2) + rNE * PART(idNE, 4) + rN * PART(idN, 6);
-  const double pm3 = rW * PART(idW, 1) + r0 * PART(id, 3) + rN * PART(idN, 5);
-  const double pm4 = rS * PART(idS, 2) + rE * PART(idE, 4) + r0 * PART(id, 6);
-
-  const double pv_LORT = (cor[E3(LORT, id)] + circ_LORT) / pm1;
-  const double pv_UPLT = (cor[E3(UPLT, id)] + circ_UPLT) / pm2;
-  const double pv_W_LORT = (cor[E3(LORT, idW)] + circ_W_LORT) / pm3;
-  const double pv_S_UPLT = (cor[E3(UPLT, idS)] + circ_S_UPLT) / pm4;
+  const double pv_S_UPLT =
+      (cor[E3(UPLT, idS)] + circ_S_UPLT) / (rS * PART(idS, 2) + rE * PART(idE, 4) + r0 * PART(id, 6));
 
   qe[E3(RT, id)] = interp(pv_S_UPLT, pv_LORT);
   qe[E3(DG, id)] = interp(pv_UPLT, pv_LORT);
@@ -193,15 +288,19 @@ __global__ void k_step1(LevelDev L, int nz, const double* __restrict__ mass, con
   hfm[E3(RT, id)] = u_dual_RT * interp(r0, rE) + 0.0;
   hfm[E3(DG, id)] = u_dual_DG * interp(r0, rNE) + 0.0;
   hfm[E3(UP, id)] = u_dual_UP * interp(r0, rN) + 0.0;
-  hft[E3(RT, id)] = u_dual_RT * interp(t0, tE) + 0.0;
-  hft[E3(DG, id)] = u_dual_DG * interp(t0, tNE) + 0.0;
-  hft[E3(UP, id)] = u_dual_UP * interp(t0, tN) + 0.0;
+  {
+    const double t0 = R.n(Mt, id) + At[id];
+    hft[E3(RT, id)] = u_dual_RT * interp(t0, R.n(Mt, idE) + At[idE]) + 0.0;
+    hft[E3(DG, id)] = u_dual_DG * interp(t0, R.n(Mt, idNE) + At[idNE]) + 0.0;
+    hft[E3(UP, id)] = u_dual_UP * interp(t0, R.n(Mt, idN) + At[idN]) + 0.0;
+  }
 
   if (i == 0 || j == 0) {  // comp_SW
-    const double rSW = Mm[idSW] + Am[idSW];
-    const double tS = Mt[idS] + At[idS], tW = Mt[idW] + At[idW], tSW = Mt[idSW] + At[idSW];
-    const double u_prim_RT_SW = v[E3(RT, idSW)] * len[E3(RT, idSW)];
-    const double u_prim_UP_SW = v[E3(UP, idSW)] * len[E3(UP, idSW)];
+    const double rSW = R.n(Mm, idSW) + Am[idSW];
+    const double t0 = R.n(Mt, id) + At[id];
+    const double tS = R.n(Mt, idS) + At[idS], tW = R.n(Mt, idW) + At[idW], tSW = R.n(Mt, idSW) + At[idSW];
+    const double u_prim_RT_SW = R.e(v, E3(RT, idSW)) * len[E3(RT, idSW)];
+    const double u_prim_UP_SW = R.e(v, E3(UP, idSW)) * len[E3(UP, idSW)];
     const double circ_SW_LORT = u_prim_RT_SW + u_prim_UP_S + u_prim_DG_SW;
     const double circ_SW_UPLT = -(u_prim_RT_W + u_prim_DG_SW + u_prim_UP_SW);
     const double qm1 = rSW * PART(idSW, 1) + rS * PART(idS, 3) + r0 * PART(id, 5);
@@ -224,102 +323,11 @@ __global__ void k_step1(LevelDev L, int nz, const double* __restrict__ mass, con
   }
 #undef E3
 #undef PART
-}
-
-// --------------------------------------------------------------------------
-// post_step1 (src/ops.f90:526-737): PV of the merged triangle at the four
-// pentagon corners of every lozenge.  The vorticity that the reference reads
-// back from its vort array is re-formed here from the same circulation sum that
-// its last writer used, divided by the same triangle area.  Thread = (corner,
-// lozenge, layer).
-__global__ void k_post_step1(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ velo,
-                             const double* __restrict__ mean_m, double* __restrict__ qe_all) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 40 * nz) return;
-  const int k = t / 40, c = (t % 40) / 10, d = t % 10;
-  const int n = L.n;
-  const int64_t NN = L.NN, ko = (int64_t)k * NN;
-  const double* v = velo + 3 * ko;
-  double* qe = qe_all + 3 * ko;
-  auto rho = [&](int64_t x) { return mass[ko + x] + mean_m[ko + x]; };
-  auto pr = [&](int e, int64_t x) { return v[(int64_t)e * NN + x] * L.len[(int64_t)e * NN + x]; };
-  auto part = [&](int64_t x, int kk) { return L.part[(int64_t)(kk - 1) * NN + x]; };
-  auto tri = [&](int tt, int64_t x) { return L.triarea[(int64_t)tt * NN + x]; };
-  auto cor = [&](int tt, int64_t x) { return L.coriolis[(int64_t)tt * NN + x]; };
-  auto I = [&](int i, int j) { return nid(L, d, i, j); };
-  if (c == 0) {  // IJPLUS (north-east corner)
-    int64_t id = I(n, n), idN = I(n, n + 1), idE = I(n + 1, n), idS = I(n, n - 1), idW = I(n - 1, n);
-    double r0 = rho(id), rN = rho(idN), rE = rho(idE), rS = rho(idS), rW = rho(idW);
-    double circ_LORT = pr(RT, id) - pr(RT, idN) - pr(UP, id);
-    // vort(LORT(W)) last written by comput(n-1,n): RT + UP_E + DG;  vort(UPLT(S)) by comput(n,n-1): -(DG + UP + RT_N)
-    double vW = (pr(RT, idW) + pr(UP, id) + pr(DG, idW)) / tri(LORT, idW);
-    double vS = -(pr(DG, idS) + pr(UP, idS) + pr(RT, id)) / tri(UPLT, idS);
-    double circ_W_LORT = vW * tri(LORT, idW);
-    double circ_S_UPLT = vS * tri(UPLT, idS);
-    double pm1 = rE * part(idE, 3) + r0 * (part(id, 1) + part(id, 2)) + rN * part(idN, 6);
-    double pm2 = rW * part(idW, 1) + r0 * part(id, 3) + rN * part(idN, 5);
-    double pm3 = rS * part(idS, 2) + rE * part(idE, 4) + r0 * part(id, 6);
-    double pv_LORT = (cor(LORT, id) + circ_LORT) / pm1;
-    double pv_W_LORT = (cor(LORT, idW) + circ_W_LORT) / pm2;
-    double pv_S_UPLT = (cor(UPLT, idS) + circ_S_UPLT) / pm3;
-    double pv_UPLT = pv_LORT;
-    qe[(int64_t)RT * NN + id] = interp(pv_LORT, pv_S_UPLT);
-    qe[(int64_t)UP * NN + id] = interp(pv_UPLT, pv_W_LORT);
-  } else if (c == 1) {  // IPLUSJMINUS (south-east corner)
-    int64_t id = I(n, 0), idE = I(n + 1, 0), idS = I(n, -1), idW = I(n - 1, 0), idNE = I(n + 1, 1), idSW = I(n - 1, -1);
-    double r0 = rho(id), rE = rho(idE), rS = rho(idS), rW = rho(idW), rNE = rho(idNE), rSW = rho(idSW);
-    double circ_SW_LORT = -pr(RT, id) + pr(RT, idSW) + pr(DG, idSW);
-    // vort(LORT(id)) from comput(n,0); vort(UPLT(SW)) from comp_SW(n,0): -(RT_W + DG_SW + UP_SW)
-    double vL = (pr(RT, id) + pr(UP, idE) + pr(DG, id)) / tri(LORT, id);
-    double vU = -(pr(RT, idW) + pr(DG, idSW) + pr(UP, idSW)) / tri(UPLT, idSW);
-    double circ_LORT = vL * tri(LORT, id);
-    double circ_SW_UPLT = vU * tri(UPLT, idSW);
-    double pm1 = rSW * part(idSW, 1) + rS * part(idS, 3) + r0 * (part(id, 5) + part(id, 6));
-    double pm2 = r0 * part(id, 1) + rE * part(idE, 3) + rNE * part(idNE, 5);
-    double pm3 = rSW * part(idSW, 2) + r0 * part(id, 4) + rW * part(idW, 6);
-    double pv_SW_LORT = (cor(LORT, idSW) + circ_SW_LORT) / pm1;
-    double pv_LORT = (cor(LORT, id) + circ_LORT) / pm2;
-    double pv_SW_UPLT = (cor(UPLT, idSW) + circ_SW_UPLT) / pm3;
-    double pv_S_UPLT = pv_SW_LORT;
-    qe[(int64_t)RT * NN + id] = interp(pv_S_UPLT, pv_LORT);
-    qe[(int64_t)DG * NN + idSW] = interp(pv_SW_LORT, pv_SW_UPLT);
-  } else if (c == 2) {  // IJMINUS (south-west corner)
-    int64_t id = I(0, 0), idN = I(0, 1), idE = I(1, 0), idS = I(0, -1), idW = I(-1, 0), idSW = I(-1, -1);
-    double r0 = rho(id), rN = rho(idN), rE = rho(idE), rS = rho(idS), rW = rho(idW);
-    double circ_SW_LORT = pr(UP, idS) - pr(RT, idW) + pr(RT, idSW);
-    // vort(LORT(W)) from comput(0,0): RT_W + UP + DG_W;  vort(UPLT(S)): -(RT + DG_S + UP_S)
-    double vW = (pr(RT, idW) + pr(UP, id) + pr(DG, idW)) / tri(LORT, idW);
-    double vS = -(pr(RT, id) + pr(DG, idS) + pr(UP, idS)) / tri(UPLT, idS);
-    double circ_W_LORT = vW * tri(LORT, idW);
-    double circ_S_UPLT = vS * tri(UPLT, idS);
-    double pm1 = rW * part(idW, 6) + r0 * (part(id, 4) + part(id, 5)) + rS * part(idS, 3);
-    double pm2 = rW * part(idW, 1) + r0 * part(id, 3) + rN * part(idN, 5);
-    double pm3 = rS * part(idS, 2) + rE * part(idE, 4) + r0 * part(id, 6);
-    double pv_W_LORT = (cor(LORT, idW) + circ_W_LORT) / pm1;
-    double pv_SW_LORT = (cor(LORT, idSW) + circ_SW_LORT) / pm2;
-    double pv_S_UPLT = (cor(UPLT, idS) + circ_S_UPLT) / pm3;
-    double pv_SW_UPLT = pv_SW_LORT;
-    qe[(int64_t)RT * NN + idW] = interp(pv_W_LORT, pv_SW_UPLT);
-    qe[(int64_t)UP * NN + idS] = interp(pv_S_UPLT, pv_SW_LORT);
-  } else {  // IMINUSJPLUS (north-west corner)
-    int64_t id = I(0, n), idN = I(0, n + 1), idS = I(0, n - 1), idW = I(-1, n), idNE = I(1, n + 1), idSW = I(-1, n - 1);
-    double r0 = rho(id), rN = rho(idN), rS = rho(idS), rW = rho(idW), rNE = rho(idNE), rSW = rho(idSW);
-    double circ_SW_UPLT = pr(UP, id) - pr(DG, idSW) - pr(UP, idSW);
-    // vort(UPLT(id)) from comput(0,n): -(DG + UP + RT_N);  vort(LORT(SW)) from comput(0,n-1): RT_W + UP + DG_W
-    double vU = -(pr(DG, id) + pr(UP, id) + pr(RT, idN)) / tri(UPLT, id);
-    double vL = (pr(RT, idSW) + pr(UP, idS) + pr(DG, idSW)) / tri(LORT, idSW);
-    double circ_UPLT = vU * tri(UPLT, id);
-    double circ_SW_LORT = vL * tri(LORT, idSW);
-    double pm1 = rSW * part(idSW, 2) + r0 * (part(id, 3) + part(id, 4)) + rW * part(idW, 6);
-    double pm2 = r0 * part(id, 2) + rNE * part(idNE, 4) + rN * part(idN, 6);
-    double pm3 = rSW * part(idSW, 1) + rS * part(idS, 3) + r0 * part(id, 5);
-    double pv_SW_UPLT = (cor(UPLT, idSW) + circ_SW_UPLT) / pm1;
-    double pv_UPLT = (cor(UPLT, id) + circ_UPLT) / pm2;
-    double pv_SW_LORT = (cor(LORT, idSW) + circ_SW_LORT) / pm3;
-    double pv_W_LORT = pv_SW_UPLT;
-    qe[(int64_t)UP * NN + id] = interp(pv_W_LORT, pv_UPLT);
-    qe[(int64_t)DG * NN + idSW] = interp(pv_SW_LORT, pv_SW_UPLT);
-  }
+  // post_step1 at the pentagon corners, by the thread that wrote those edges
+  if (i == L.n && j == L.n) post_corner(L, 0, d, ko, mass, velo, mean_m, out.qe);
+  if (i == L.n && j == 0) post_corner(L, 1, d, ko, mass, velo, mean_m, out.qe);
+  if (i == 0 && j == 0) post_corner(L, 2, d, ko, mass, velo, mean_m, out.qe);
+  if (i == 0 && j == L.n) post_corner(L, 3, d, ko, mass, velo, mean_m, out.qe);
 }
 
 // --------------------------------------------------------------------------
@@ -327,9 +335,10 @@ __global__ void k_post_step1(LevelDev L, int nz, const double* __restrict__ mass
 //   scalar_trend  dscalar = -div(h_flux) on [0, n]^2          (src/ops.f90:739)
 //   du_source     dvelo   = -Qperp on owned nodes [0, n)^2    (src/ops.f90:757,834)
 //   du_grad       dvelo   = dvelo/len - grad B - theta_e grad Exner  (src/ops.f90:787)
-// For MODE_RK every node of the padded level (all layers) is written as
-//   dest = base + h * trend   (trend = 0 where the reference leaves it zero).
-// For MODE_TREND the trends themselves are written on the same node set.
+// Mass fluxes at ghost edges are read from their source edges (the
+// reference's update_bdry(horiz_flux)).  For MODE_RK every node of the padded
+// level (all layers) is written as dest = base + h * trend (trend = 0 where
+// the reference leaves it zero); MODE_TREND writes the trends themselves.
 enum { MODE_TREND = 0, MODE_RK = 1 };
 
 struct TrendIO {
@@ -367,7 +376,7 @@ __device__ __forceinline__ void weights5(const LevelDev& L, int64_t id, int offs
 }
 
 template <int MODE>
-__global__ void k_trend(LevelDev L, int nz, TrendIO io) {
+__global__ void __launch_bounds__(256, 2) k_trend(LevelDev L, int nz, TrendIO io) {
   const int P = L.P;
   const int64_t NN = L.NN;
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -380,6 +389,7 @@ __global__ void k_trend(LevelDev L, int nz, TrendIO io) {
   const int j = r / P - 2, i = r % P - 2;
   const int n = L.n;
   const int64_t ko = (int64_t)k * NN;
+  const Rd R{L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2};
   double dms = 0.0, dts = 0.0, dv0 = 0.0, dv1 = 0.0, dv2 = 0.0;
   const bool scal = (i >= 0 && j >= 0 && i <= n && j <= n);
   const bool own = (i >= 0 && j >= 0 && i < n && j < n);
@@ -388,10 +398,10 @@ __global__ void k_trend(LevelDev L, int nz, TrendIO io) {
     const double* fm = io.hfm + 3 * ko;
     const double* ft = io.hft + 3 * ko;
     double hinv = L.hex_inv[id];
-    double divm = (fm[RT * NN + id] - fm[RT * NN + idW] + fm[DG * NN + idSW] - fm[DG * NN + id] + fm[UP * NN + id] -
-                   fm[UP * NN + idS]) * hinv;
-    double divt = (ft[RT * NN + id] - ft[RT * NN + idW] + ft[DG * NN + idSW] - ft[DG * NN + id] + ft[UP * NN + id] -
-                   ft[UP * NN + idS]) * hinv;
+    double divm = (R.e(fm, RT * NN + id) - R.e(fm, RT * NN + idW) + R.e(fm, DG * NN + idSW) - R.e(fm, DG * NN + id) +
+                   R.e(fm, UP * NN + id) - R.e(fm, UP * NN + idS)) * hinv;
+    double divt = (R.e(ft, RT * NN + id) - R.e(ft, RT * NN + idW) + R.e(ft, DG * NN + idSW) - R.e(ft, DG * NN + id) +
+                   R.e(ft, UP * NN + id) - R.e(ft, UP * NN + idS)) * hinv;
     dms = -divm;
     dts = -divt;
   }
@@ -400,7 +410,7 @@ __global__ void k_trend(LevelDev L, int nz, TrendIO io) {
     const double* qe = io.qe + 3 * ko;
     const int64_t idNW = id + P - 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idE = id + 1, idSW = id - P - 1,
                   idS = id - P, idSE = id - P + 1;
-#define TQ(e1, n1, q0, w) (hm[(int64_t)(e1) * NN + (n1)] * interp(qe[(int64_t)(e1) * NN + (n1)], (q0)) * (w))
+#define TQ(e1, n1, q0, w) (R.e(hm, (int64_t)(e1) * NN + (n1)) * interp(qe[(int64_t)(e1) * NN + (n1)], (q0)) * (w))
     double w1[5], w2[5];
     double q0 = qe[RT * NN + id];
     weights5(L, id, 0, w1);
@@ -426,10 +436,10 @@ __global__ void k_trend(LevelDev L, int nz, TrendIO io) {
     const double* mt = io.temp + ko;
     const double* am = io.mean_m + ko;
     const double* at = io.mean_t + ko;
-    double th0 = (at[id] + mt[id]) / (am[id] + mm[id]);
-    double thE = (at[idE] + mt[idE]) / (am[idE] + mm[idE]);
-    double thNE = (at[idNE] + mt[idNE]) / (am[idNE] + mm[idNE]);
-    double thN = (at[idN] + mt[idN]) / (am[idN] + mm[idN]);
+    double th0 = (at[id] + R.n(mt, id)) / (am[id] + R.n(mm, id));
+    double thE = (at[idE] + R.n(mt, idE)) / (am[idE] + R.n(mm, idE));
+    double thNE = (at[idNE] + R.n(mt, idNE)) / (am[idNE] + R.n(mm, idNE));
+    double thN = (at[idN] + R.n(mt, idN)) / (am[idN] + R.n(mm, idN));
     const double* B = io.bern + ko;
     const double* F = io.phik + ko;   // exner = -Phi_k (src/ops.f90:358)
     const double lRT = L.len[RT * NN + id], lDG = L.len[DG * NN + id], lUP = L.len[UP * NN + id];

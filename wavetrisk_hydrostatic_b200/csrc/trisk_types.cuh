@@ -17,6 +17,10 @@ struct LevelDev {
   const double* __restrict__ triarea;  // 2*NN
   const double* __restrict__ coriolis; // 2*NN
   const double* __restrict__ topo;     // NN
+  // Ghost remaps (cp_bdry_inside, src/comm.f90:785): node x reads x' = nsrc[x];
+  // edge slot e reads slot esrc[e] >> 1, negated when esrc[e] & 1.
+  const int* __restrict__ nsrc;        // NN
+  const int* __restrict__ esrc;        // 3*NN
 };
 
 struct Phys {

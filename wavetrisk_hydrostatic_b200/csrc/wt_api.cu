@@ -97,6 +97,16 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
     if ((e = cudaMalloc(&D.he, sizeof(int3) * std::max<size_t>(1, he.size()))) != cudaSuccess) { rc = wt_handle_fail("halo", e); break; }
     cudaMemcpy(D.hn, hn.data(), sizeof(int2) * hn.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(D.he, he.data(), sizeof(int3) * he.size(), cudaMemcpyHostToDevice);
+    // read remaps: a ghost reads the node / signed edge its copy entry names
+    std::vector<int> nsrc(NN), esrc(3 * NN);
+    for (int64_t k = 0; k < NN; ++k) nsrc[k] = (int)k;
+    for (auto& x : hn) nsrc[x.x] = x.y;
+    for (int64_t k = 0; k < 3 * NN; ++k) esrc[k] = (int)(2 * k);
+    for (auto& x : he) esrc[x.x] = 2 * x.y + (x.z < 0 ? 1 : 0);
+    if ((e = cudaMalloc(&D.nsrc, sizeof(int) * NN)) != cudaSuccess) { rc = wt_handle_fail("remap", e); break; }
+    if ((e = cudaMalloc(&D.esrc, sizeof(int) * 3 * NN)) != cudaSuccess) { rc = wt_handle_fail("remap", e); break; }
+    cudaMemcpy(D.nsrc, nsrc.data(), sizeof(int) * NN, cudaMemcpyHostToDevice);
+    cudaMemcpy(D.esrc, esrc.data(), sizeof(int) * 3 * NN, cudaMemcpyHostToDevice);
   }
   if (rc == WT_OK) {
     // Prognostic state and RK/trend work arrays on level_end.
@@ -169,6 +179,12 @@ int wt_upload_state(wt_handle* h, const double* mass, const double* temp, const 
 int wt_download_state(wt_handle* h, double* mass, double* temp, double* velo) {
   if (!h || !mass || !temp || !velo) return WT_ERR_ARG;
   const int64_t nn = (int64_t)h->nz * h->top().NN;
+  {
+    // ghosts are read through remaps on the device; fill them for the host
+    DevLevel& D = h->top();
+    int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * h->nz;
+    k_halo_state<<<blocks_for(nt), TPB, 0, h->stream>>>(h->nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, h->mass, h->temp, h->velo);
+  }
   CK(cudaMemcpyAsync(mass, h->mass, nn * 8, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(temp, h->temp, nn * 8, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(velo, h->velo, 3 * nn * 8, cudaMemcpyDeviceToHost, h->stream));
@@ -215,12 +231,7 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   LevelDev L = D.view();
   const int nz = h->nz;
   cudaStream_t s = h->stream;
-  if (halo_first) {
-    int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * nz;
-    TB(0);
-    k_halo_state<<<blocks_for(nt), TPB, 0, s>>>(nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, m, t, v);
-    TE(0);
-  }
+  (void)halo_first;
   const int mm = D.n + 1;
   TB(1);
   k_column<<<blocks_for(10 * mm * mm, 128), 128, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm);
@@ -229,12 +240,6 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   TB(2);
   k_step1<<<blocks_for((int64_t)10 * mm * mm * nz), TPB, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
   TE(2);
-  TB(3);
-  k_post_step1<<<blocks_for(40 * nz, 64), 64, 0, s>>>(L, nz, m, v, h->mean_m, h->qe);
-  TE(3);
-  TB(4);
-  k_halo_flux<<<blocks_for((int64_t)2 * D.n_he * nz), TPB, 0, s>>>(nz, D.NN, D.he, D.n_he, h->hfm, h->hft);
-  TE(4);
   TrendIO io{};
   io.mass = m; io.temp = t; io.mean_m = h->mean_m; io.mean_t = h->mean_t; io.qe = h->qe; io.hfm = h->hfm;
   io.hft = h->hft; io.bern = h->bern; io.phik = h->phik;
@@ -287,10 +292,6 @@ static int record_rk4(wt_handle* h, double dt, KTimer* tm = nullptr) {
     double* ov = stage == 3 ? h->velo : h->v1;
     int rc = launch_trend(h, qm, qt, qv, MODE_RK, h->mass, h->temp, h->velo, om, ot, ov, hs[stage], false, tm);
     if (rc) return rc;
-    int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * nz;
-    TB(0);
-    k_halo_state<<<blocks_for(nt), TPB, 0, h->stream>>>(nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, om, ot, ov);
-    TE(0);
   }
   CK(cudaGetLastError());
   return WT_OK;
@@ -299,13 +300,6 @@ static int record_rk4(wt_handle* h, double dt, KTimer* tm = nullptr) {
 int wt_rk4_step(wt_handle* h, double dt, int nsteps) {
   if (!h || nsteps < 0) return WT_ERR_ARG;
   if (nsteps == 0) return WT_OK;
-  if (!h->state_halo_done) {
-    // the reference's trend_ml starts with update_bdry of the state
-    DevLevel& D = h->top();
-    int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * h->nz;
-    k_halo_state<<<blocks_for(nt), TPB, 0, h->stream>>>(h->nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, h->mass, h->temp, h->velo);
-    h->state_halo_done = true;
-  }
   if (!h->graph_exec || h->graph_dt != dt) {
     if (h->graph_exec) { cudaGraphExecDestroy(h->graph_exec); h->graph_exec = nullptr; }
     cudaGraph_t g;
@@ -345,7 +339,7 @@ int wt_profile_rk4(wt_handle* h, double dt, int nsteps, double* ms_per_launch, i
     cnt[tm.ids[q]] += 1;
   }
   for (int k = 0; k < 6; ++k) ms_per_launch[k] = cnt[k] ? tot[k] / cnt[k] : 0.0;
-  *nkernels = 6;
+  *nkernels = 6;   // kinds 0 (ghost copy), 3, 4 are no longer launched by the stepper
   return WT_OK;
 }
 

@@ -167,15 +167,13 @@ extern "C" int wt_elliptic_setup(wt_handle* h, double dt, double theta1, double 
     }
     if ((rc = dalloc(*E, &X.Ie, 3 * NN))) break;
     if ((rc = dalloc(*E, &X.diag, NN))) break;
-    if ((rc = dalloc(*E, &X.nsrc, NN))) break;
-    if ((rc = dalloc(*E, &X.esrc, 3 * NN))) break;
+    X.nsrc = D.nsrc;
+    X.esrc = D.esrc;
     if ((rc = dalloc(*E, &X.Kf, 3 * NN))) break;
     if ((rc = dalloc(*E, &X.hinvf, NN))) break;
     if ((rc = dalloc(*E, &X.diagf, NN))) break;
     cudaMemcpy(X.Ie, Ie.data(), 8 * 3 * NN, cudaMemcpyHostToDevice);
     cudaMemcpy(X.diag, diag.data(), 8 * NN, cudaMemcpyHostToDevice);
-    cudaMemcpy(X.nsrc, nsrc.data(), 4 * NN, cudaMemcpyHostToDevice);
-    cudaMemcpy(X.esrc, esrc.data(), 4 * 3 * NN, cudaMemcpyHostToDevice);
     cudaMemcpy(X.Kf, Kf.data(), 4 * 3 * NN, cudaMemcpyHostToDevice);
     cudaMemcpy(X.hinvf, hinvf.data(), 4 * NN, cudaMemcpyHostToDevice);
     cudaMemcpy(X.diagf, diagf.data(), 4 * NN, cudaMemcpyHostToDevice);

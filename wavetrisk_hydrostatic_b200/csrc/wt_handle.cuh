@@ -15,13 +15,20 @@ struct DevLevel {
   int2* hn = nullptr;
   int3* he = nullptr;
   int n_hn = 0, n_he = 0;
-  wtk::LevelDev view() const { return wtk::LevelDev{n, P, NN, len, pedlen, part, hex_inv, triarea, coriolis, topo}; }
+  int* nsrc = nullptr;  // node read remap (ghost -> source node)
+  int* esrc = nullptr;  // signed edge read remap: source slot * 2 + negate
+  wtk::LevelDev view() const {
+    return wtk::LevelDev{n, P, NN, len, pedlen, part, hex_inv, triarea, coriolis, topo, nsrc, esrc};
+  }
   void release() {
     double* a[] = {len, pedlen, part, hex_inv, triarea, coriolis, overl_a, topo};
     for (double* p : a)
       if (p) cudaFree(p);
     if (hn) cudaFree(hn);
     if (he) cudaFree(he);
+    if (nsrc) cudaFree(nsrc);
+    if (esrc) cudaFree(esrc);
+    nsrc = esrc = nullptr;
     len = pedlen = part = hex_inv = triarea = coriolis = overl_a = topo = nullptr;
     hn = nullptr;
     he = nullptr;

@@ -122,7 +122,7 @@ int wt_profile_rk4(wt_handle* h, double dt, int nsteps, double* ms_per_launch, i
  * uniform hierarchy level_start..level_end of the handle.  Fields u (solution,
  * initial guess) and f (right-hand side) are multi-level: the levels' NN-node
  * arrays concatenated from level_start to level_end. */
-enum { WT_SOLVER_FMG = 0, WT_SOLVER_SRJ = 1, WT_SOLVER_MIXED_IR = 2 };
+enum { WT_SOLVER_FMG = 0, WT_SOLVER_SRJ = 1, WT_SOLVER_MIXED_IR = 2, WT_SOLVER_MG64 = 3 };
 
 typedef struct {
   int method;                 /* WT_SOLVER_*                                         */
@@ -133,7 +133,8 @@ typedef struct {
   int max_srj_iter;           /* [200]                                               */
   double fine_tol, coarse_tol;/* [1e-3, 1e-3]                                        */
   /* WT_SOLVER_MIXED_IR: FP64 refinement around FP32 V-cycles (down/up_iter sweeps,
-   * coarse_iter Jacobi sweeps on level_start); stop at ir_tol or ir_max.           */
+   * coarse_iter Jacobi sweeps on level_start); stop at ir_tol or ir_max.
+   * WT_SOLVER_MG64: the same cycle entirely in FP64 (precision-matched baseline). */
   double ir_tol;
   int ir_max;
 } wt_solver_opts;

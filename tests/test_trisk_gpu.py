@@ -86,3 +86,21 @@ def test_mass_conserved_over_steps():
     assert abs(total(out["mass"]) / m0 - 1) < 1e-13
     assert np.isfinite(out["velo"]).all()
     model.close()
+
+
+def test_rk4_is_deterministic():
+    # a stage never writes the array it reads at neighbouring nodes
+    g = Grid(4, 4, radius=6371e3).level(4)
+    nz = 3
+    ph = OceanParams()
+    st = jet_state(g, nz, seed=11, ph=ph)
+    outs = []
+    for _ in range(3):
+        m = TriskModel(g, nz, st["topo"], ph)
+        m.upload(st)
+        m.rk4(300.0, 3)
+        outs.append(m.download())
+        m.close()
+    for o in outs[1:]:
+        for k in ("mass", "temp", "velo"):
+            assert np.array_equal(o[k], outs[0][k])

@@ -112,11 +112,11 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
     // Prognostic state and RK/trend work arrays on level_end.
     DevLevel& D = h->top();
     const int64_t NN = D.NN, nn = (int64_t)h->nz * NN, ne = 3 * nn;
-    double** node_arrays[] = {&h->mass, &h->temp, &h->mean_m, &h->mean_t, &h->m1, &h->t1, &h->dm, &h->dt,
-                              &h->bern, &h->phik, &h->pterm};
+    double** node_arrays[] = {&h->mass, &h->temp, &h->mean_m, &h->mean_t, &h->m1, &h->t1, &h->m2, &h->t2,
+                              &h->dm, &h->dt, &h->bern, &h->phik, &h->pterm};
     for (double** p : node_arrays)
       if ((rc = dev_zero(p, nn))) break;
-    double** edge_arrays[] = {&h->velo, &h->v1, &h->dv, &h->qe, &h->hfm, &h->hft};
+    double** edge_arrays[] = {&h->velo, &h->v1, &h->v2, &h->dv, &h->qe, &h->hfm, &h->hft};
     if (rc == WT_OK)
       for (double** p : edge_arrays)
         if ((rc = dev_zero(p, ne))) break;
@@ -137,8 +137,8 @@ int wt_destroy(wt_handle* h) {
   if (!h) return WT_OK;
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   for (auto& D : h->lev) D.release();
-  double* arrays[] = {h->mass, h->temp, h->velo, h->mean_m, h->mean_t, h->m1, h->t1, h->v1, h->dm, h->dt, h->dv,
-                      h->qe, h->hfm, h->hft, h->bern, h->phik, h->pterm};
+  double* arrays[] = {h->mass, h->temp, h->velo, h->mean_m, h->mean_t, h->m1, h->t1, h->v1, h->m2, h->t2, h->v2,
+                      h->dm, h->dt, h->dv, h->qe, h->hfm, h->hft, h->bern, h->phik, h->pterm};
   for (double* p : arrays)
     if (p) cudaFree(p);
   h->release_extra();
@@ -245,12 +245,12 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   io.hft = h->hft; io.bern = h->bern; io.phik = h->phik;
   io.base_m = bm; io.base_t = bt; io.base_v = bv; io.dst_m = om; io.dst_t = ot; io.dst_v = ov; io.h = hstep;
   io.dm = h->dm; io.dtt = h->dt; io.dv = h->dv;
-  int64_t nt = D.NN * nz;
+  int64_t nt = 3 * D.NN * nz;
   TB(5);
   if (mode == MODE_RK)
-    k_trend<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+    k_trend_e<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
   else
-    k_trend<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+    k_trend_e<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
   TE(5);
   CK(cudaGetLastError());
   return WT_OK;
@@ -283,13 +283,21 @@ static int record_rk4(wt_handle* h, double dt, KTimer* tm = nullptr) {
   DevLevel& D = h->top();
   const int nz = h->nz;
   const double hs[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
+  // Stage states ping-pong between two buffers: k_trend reads the stage state at
+  // neighbouring nodes while it writes the next one, so they must differ (the
+  // reference finishes the whole trend before RK_sub_step).  The last stage
+  // writes the solution in place, which it reads only at each thread's own node.
+  double* SM[3] = {h->mass, h->m1, h->m2};
+  double* ST[3] = {h->temp, h->t1, h->t2};
+  double* SV[3] = {h->velo, h->v1, h->v2};
+  const int qi[4] = {0, 1, 2, 1}, oi[4] = {1, 2, 1, 0};
   for (int stage = 0; stage < 4; ++stage) {
-    double* qm = stage == 0 ? h->mass : h->m1;
-    double* qt = stage == 0 ? h->temp : h->t1;
-    double* qv = stage == 0 ? h->velo : h->v1;
-    double* om = stage == 3 ? h->mass : h->m1;
-    double* ot = stage == 3 ? h->temp : h->t1;
-    double* ov = stage == 3 ? h->velo : h->v1;
+    double* qm = SM[qi[stage]];
+    double* qt = ST[qi[stage]];
+    double* qv = SV[qi[stage]];
+    double* om = SM[oi[stage]];
+    double* ot = ST[oi[stage]];
+    double* ov = SV[oi[stage]];
     int rc = launch_trend(h, qm, qt, qv, MODE_RK, h->mass, h->temp, h->velo, om, ot, ov, hs[stage], false, tm);
     if (rc) return rc;
   }
@@ -352,6 +360,11 @@ int wt_rk4_step_host(wt_handle* h, double dt, int nsteps, double* mass, double* 
   h->state_halo_done = false;
   int rc = wt_rk4_step(h, dt, nsteps);
   if (rc) return rc;
+  {
+    DevLevel& D = h->top();
+    int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * h->nz;
+    k_halo_state<<<blocks_for(nt), TPB, 0, h->stream>>>(h->nz, D.NN, D.hn, D.n_hn, D.he, D.n_he, h->mass, h->temp, h->velo);
+  }
   CK(cudaMemcpyAsync(mass, h->mass, nn * 8, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(temp, h->temp, nn * 8, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(velo, h->velo, 3 * nn * 8, cudaMemcpyDeviceToHost, h->stream));

@@ -126,21 +126,12 @@ extern "C" int wt_elliptic_setup(wt_handle* h, double dt, double theta1, double 
     X.NN = D.NN;
     X.nd = std::max(1, D.n >> domain_level);
     const int64_t NN = D.NN;
-    // host copies of the level tables needed to build the remaps and coefficients
-    std::vector<int2> hn(D.n_hn);
-    std::vector<int3> he(D.n_he);
-    cudaMemcpy(hn.data(), D.hn, sizeof(int2) * D.n_hn, cudaMemcpyDeviceToHost);
-    cudaMemcpy(he.data(), D.he, sizeof(int3) * D.n_he, cudaMemcpyDeviceToHost);
+    // host copies of the level tables needed to build the operator coefficients
     std::vector<double> topo(NN), len(3 * NN), ped(3 * NN), hinv(NN);
     cudaMemcpy(topo.data(), D.topo, 8 * NN, cudaMemcpyDeviceToHost);
     cudaMemcpy(len.data(), D.len, 8 * 3 * NN, cudaMemcpyDeviceToHost);
     cudaMemcpy(ped.data(), D.pedlen, 8 * 3 * NN, cudaMemcpyDeviceToHost);
     cudaMemcpy(hinv.data(), D.hex_inv, 8 * NN, cudaMemcpyDeviceToHost);
-    std::vector<int> nsrc(NN), esrc(3 * NN);
-    for (int64_t k = 0; k < NN; ++k) nsrc[k] = (int)k;
-    for (auto& e : hn) nsrc[e.x] = e.y;
-    for (int64_t k = 0; k < 3 * NN; ++k) esrc[k] = (int)(k * 2);
-    for (auto& e : he) esrc[e.x] = e.y * 2 + (e.z < 0 ? 1 : 0);
     // csq = g (|H| phi + eta_old) with phi = 1, eta_old = 0 (src/ops.f90:203-208)
     auto csq = [&](int64_t k) { return g * (std::fabs(topo[k]) * 1.0 + 0.0); };
     std::vector<double> Ie(3 * NN, 0.0), diag(NN, 0.0);
@@ -493,6 +484,7 @@ int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report
   if (opts->method == WT_SOLVER_FMG) fmg(E, *opts, *rep);
   else if (opts->method == WT_SOLVER_SRJ) srj(E, *opts, *rep);
   else if (opts->method == WT_SOLVER_MIXED_IR) rc = mixed_ir(E, *opts, *rep);
+  else if (opts->method == WT_SOLVER_MG64) rc = mixed_ir(E, *opts, *rep, true);
   else return WT_ERR_ARG;
   CKE(cudaStreamSynchronize(E.s()));
   auto t1 = std::chrono::steady_clock::now();

@@ -132,7 +132,39 @@ void vcycle32(Ell& E, const wt_solver_opts& o) {
   }
 }
 
-int mixed_ir(Ell& E, const wt_solver_opts& o, wt_solver_report& rep) {
+// The same V-cycle in FP64 (WT_SOLVER_MG64): the precision-matched baseline of
+// the mixed solver, with the reference's FP64 kernels.
+void vcycle64(Ell& E, const wt_solver_opts& o) {
+  for (int j = E.ls; j <= E.le; ++j) zero_level(E, j, E.corr.lv[j - E.ls]);
+  for (int j = E.le; j >= E.ls + 1; --j) {
+    jacobi(E, E.corr, E.res, j, o.down_iter);
+    op(E, OP_RESID, j, E.corr.lv[j - E.ls], E.res.lv[j - E.ls], E.au.lv[j - E.ls]);
+    EllLev C = E.view(j - 1), F = E.view(j);
+    int n = E.L[j - 1 - E.ls].n;
+    zero_level(E, j, E.wc_temp.lv[j - E.ls]);
+    k_wc_compute<<<nb(10 * n * n), TPB, 0, E.s()>>>(C, F, E.au.lv[j - E.ls], E.wc_temp.lv[j - E.ls]);
+    k_restrict<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, E.au.lv[j - E.ls], E.wc_temp.lv[j - E.ls],
+                                                                E.res.lv[j - 1 - E.ls]);
+  }
+  jacobi(E, E.corr, E.res, E.ls, o.coarse_iter);
+  for (int j = E.ls + 1; j <= E.le; ++j) {
+    EllLev C = E.view(j - 1), F = E.view(j);
+    int n = E.L[j - 1 - E.ls].n;
+    zero_level(E, j, E.wc_mass.lv[j - E.ls]);
+    k_prolong_even<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, E.corr.lv[j - 1 - E.ls], E.wc_mass.lv[j - E.ls],
+                                                                    E.pf.lv[j - E.ls]);
+    k_prolong_odd<<<nb(10 * n * n), TPB, 0, E.s()>>>(C, F, E.pf.lv[j - E.ls], E.wc_mass.lv[j - E.ls]);
+    lc(E, j, E.corr.lv[j - E.ls], 1.0, E.corr.lv[j - E.ls], 1.0, E.pf.lv[j - E.ls]);
+    jacobi(E, E.corr, E.res, j, o.up_iter);
+  }
+}
+
+__global__ void k_axpy_d(int64_t n, double* __restrict__ u, const double* __restrict__ c) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) u[t] = u[t] + c[t];
+}
+
+int mixed_ir(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, bool fp64 = false) {
   const int l = E.le, q = l - E.ls;
   const int64_t NN = E.L[q].NN;
   double nf = l2(E, l, E.f.lv[q]);
@@ -144,9 +176,14 @@ int mixed_ir(Ell& E, const wt_solver_opts& o, wt_solver_report& rep) {
     err = l2(E, l, E.res.lv[q]) / nf;
     if (it == 0) rep.nrm_res_init[q] = err;
     if (err <= o.ir_tol || it == o.ir_max) break;
-    k_d2f<<<nb(NN), TPB, 0, E.s()>>>(NN, E.res.lv[q], E.r32.lvf[q]);
-    vcycle32(E, o);
-    k_axpy_f2d<<<nb(NN), TPB, 0, E.s()>>>(NN, E.u.lv[q], E.c32.lvf[q]);
+    if (fp64) {
+      vcycle64(E, o);
+      k_axpy_d<<<nb(NN), TPB, 0, E.s()>>>(NN, E.u.lv[q], E.corr.lv[q]);
+    } else {
+      k_d2f<<<nb(NN), TPB, 0, E.s()>>>(NN, E.res.lv[q], E.r32.lvf[q]);
+      vcycle32(E, o);
+      k_axpy_f2d<<<nb(NN), TPB, 0, E.s()>>>(NN, E.u.lv[q], E.c32.lvf[q]);
+    }
   }
   rep.outer_iterations = it;
   rep.nrm_res_final[q] = err;

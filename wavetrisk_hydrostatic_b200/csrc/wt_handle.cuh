@@ -43,6 +43,7 @@ struct wt_handle {
   // prognostic state (level_end) and RK4 stage copy
   double *mass = nullptr, *temp = nullptr, *velo = nullptr, *mean_m = nullptr, *mean_t = nullptr;
   double *m1 = nullptr, *t1 = nullptr, *v1 = nullptr;
+  double *m2 = nullptr, *t2 = nullptr, *v2 = nullptr;  // second stage buffer: a stage never writes what it reads
   // trend output (wt_trend) and operator work arrays
   double *dm = nullptr, *dt = nullptr, *dv = nullptr;
   double *qe = nullptr, *hfm = nullptr, *hft = nullptr, *bern = nullptr, *phik = nullptr, *pterm = nullptr;

@@ -119,9 +119,10 @@ class TriskModel(DeviceGrid):
 
 def solver_opts(method: str = "fmg", tol: float = 1e-10, **kw):
     """wt_solver_opts with the reference's defaults (src/lin_solve.f90:11-26),
-    tolerances set to tol.  method: 'fmg', 'srj' or 'mixed'."""
+    tolerances set to tol.  method: 'fmg', 'srj' (the reference's solvers),
+    'mixed' (FP32 V-cycles in FP64 refinement) or 'mg64' (same cycle in FP64)."""
     o = N.wt_solver_opts()
-    o.method = {"fmg": 0, "srj": 1, "mixed": 2}[method]
+    o.method = {"fmg": 0, "srj": 1, "mixed": 2, "mg64": 3}[method]
     o.coarse_iter, o.max_vcycle = 50, 3
     o.pre_iter, o.down_iter, o.up_iter, o.post_iter = 2, 2, 2, 4
     o.max_srj_iter = 200

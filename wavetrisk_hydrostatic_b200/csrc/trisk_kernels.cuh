@@ -29,15 +29,17 @@ __device__ __forceinline__ int64_t nid(const LevelDev& L, int d, int i, int j) {
 
 // Readers of the state through the ghost remap.
 struct Rd {
-  const LevelDev& L;
+  const int* __restrict__ nsrc;
+  const int* __restrict__ esrc;
   bool direct;
+  __device__ __forceinline__ Rd(const LevelDev& L, bool dir) : nsrc(L.nsrc), esrc(L.esrc), direct(dir) {}
   __device__ __forceinline__ double n(const double* __restrict__ f, int64_t x) const {
-    return direct ? f[x] : f[L.nsrc[x]];
+    return f[direct ? x : (int64_t)__ldg(nsrc + x)];
   }
   // edge field with planes of NN: slot = e*NN + x
   __device__ __forceinline__ double e(const double* __restrict__ f, int64_t slot) const {
     if (direct) return f[slot];
-    const int c = L.esrc[slot];
+    const int c = __ldg(esrc + slot);
     const double v = f[c >> 1];
     return (c & 1) ? -v : v;
   }
@@ -115,12 +117,12 @@ struct Step1Out {
 // corner.  Run by the thread that owns the corrected edges; the vorticity the
 // reference reads back from its vort array is re-formed from the same
 // circulation sum its last writer used, divided by the same triangle area.
-__device__ __noinline__ void post_corner(const LevelDev& L, int c, int d, int64_t ko, const double* __restrict__ mass,
+__device__ __noinline__ void post_corner(const LevelDev L, int c, int d, int64_t ko, const double* __restrict__ mass,
                                          const double* __restrict__ velo, const double* __restrict__ mean_m,
                                          double* __restrict__ qe) {
   const int n = L.n;
   const int64_t NN = L.NN;
-  const Rd R{L, false};
+  const Rd R(L, false);
   const double* v = velo + 3 * ko;
   auto rho = [&](int64_t x) { return R.n(mass + ko, x) + mean_m[ko + x]; };
   auto pr = [&](int e, int64_t x) { return R.e(v, (int64_t)e * NN + x) * L.len[(int64_t)e * NN + x]; };
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(256, 2)
   const int64_t id = nid(L, d, i, j);
   const int64_t idN = id + P, idE = id + 1, idS = id - P, idW = id - 1, idNE = id + P + 1, idSW = id - P - 1;
   const int64_t ko = (int64_t)k * NN;
-  const Rd R{L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2};
+  const Rd R(L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2);
   const double* Mm = mass + ko;
   const double* Mt = temp + ko;
   const double* Am = mean_m + ko;
@@ -389,7 +391,7 @@ __global__ void __launch_bounds__(256, 2) k_trend(LevelDev L, int nz, TrendIO io
   const int j = r / P - 2, i = r % P - 2;
   const int n = L.n;
   const int64_t ko = (int64_t)k * NN;
-  const Rd R{L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2};
+  const Rd R(L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2);
   double dms = 0.0, dts = 0.0, dv0 = 0.0, dv1 = 0.0, dv2 = 0.0;
   const bool scal = (i >= 0 && j >= 0 && i <= n && j <= n);
   const bool own = (i >= 0 && j >= 0 && i < n && j < n);
@@ -489,7 +491,7 @@ __global__ void __launch_bounds__(256, 3) k_trend_e(LevelDev L, int nz, TrendIO 
   const int j = r / P - 2, i = r % P - 2;
   const int n = L.n;
   const int64_t ko = (int64_t)k * NN;
-  const Rd R{L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2};
+  const Rd R(L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2);
   if (e == RT) {
     double dms = 0.0, dts = 0.0;
     if (i >= 0 && j >= 0 && i <= n && j <= n) {

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -55,6 +56,7 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
   h->ph = Phys{desc->grav, desc->ref_density, desc->p_top};
   h->level_start = desc->level_start;
   h->level_end = desc->level_end;
+  if (const char* tv = std::getenv("WAVETRISK_TREND_KERNEL")) h->trend_variant = (std::strcmp(tv, "edge") == 0) ? 1 : 0;
   const int nlev = desc->level_end - desc->level_start + 1;
   h->lev.resize(nlev);
   int rc = WT_OK;
@@ -245,12 +247,20 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   io.hft = h->hft; io.bern = h->bern; io.phik = h->phik;
   io.base_m = bm; io.base_t = bt; io.base_v = bv; io.dst_m = om; io.dst_t = ot; io.dst_v = ov; io.h = hstep;
   io.dm = h->dm; io.dtt = h->dt; io.dv = h->dv;
-  int64_t nt = 3 * D.NN * nz;
   TB(5);
-  if (mode == MODE_RK)
-    k_trend_e<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
-  else
-    k_trend_e<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+  if (h->trend_variant == 1) {
+    int64_t nt = 3 * D.NN * nz;
+    if (mode == MODE_RK)
+      k_trend_e<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+    else
+      k_trend_e<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+  } else {
+    int64_t nt = D.NN * nz;
+    if (mode == MODE_RK)
+      k_trend<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+    else
+      k_trend<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+  }
   TE(5);
   CK(cudaGetLastError());
   return WT_OK;

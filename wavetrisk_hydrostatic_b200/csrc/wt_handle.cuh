@@ -51,6 +51,7 @@ struct wt_handle {
   cudaGraphExec_t graph_exec = nullptr;
   double graph_dt = 0.0;
   int sticky = 0;  // WT_OK or the first error seen by a device-side check
+  int trend_variant = 0;  // 0: thread per node (k_trend), 1: thread per edge (k_trend_e)
 
   // elliptic solver state (allocated by wt_elliptic_setup)
   void* ell = nullptr;

@@ -167,6 +167,25 @@ int wt_elliptic_l2(wt_handle* h, int level, int which, double* out);
  * stops at ir_max above ir_tol. */
 int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report* rep);
 
+/* ------------------------------------------------------ no allocation ---- */
+/* Weighted l2 norm of one level (the solver's l2, src/lin_solve.f90:433-464)
+ * for callers that cannot allocate device memory: a host loop running inside
+ * a memory pool it does not control, or a code that must not grow its device
+ * footprint after start-up.  No reference counterpart: the reference never
+ * allocates device memory at all.
+ *   field  : device pointer, NN = 10*(2^level + 4)^2 doubles, padded layout;
+ *   nsrc   : device pointer to the level's ghost remap (NN ints), or NULL when
+ *            the ghosts of field already hold their copies;
+ *   result : device pointer to one double, written asynchronously on stream
+ *            (a cudaStream_t, or NULL for the default stream).
+ * Allocates nothing: the block partial sums live in a fixed device array of
+ * 4096 doubles, so level must be <= 8 (WT_ERR_ARG beyond).  Every call on a
+ * device shares that array: calls that overlap on the GPU race.  The first
+ * call on each device looks the array's address up (cudaGetSymbolAddress);
+ * make that first call before any stream capture. */
+int wt_elliptic_l2_noalloc(int level, int domain_level, const int* nsrc, const double* field, double* result,
+                           void* stream);
+
 /* Raw stream of the handle (cudaStream_t), for event timing by the caller. */
 void* wt_stream(wt_handle* h);
 

@@ -73,14 +73,13 @@ __global__ void k_halo_state(int nz, int64_t NN, const int2* __restrict__ hn, in
 // integrate_pressure_up (src/ops.f90:1094-1131), incompressible case, for every
 // node (i, j) in [0, n]^2 of every lozenge.  Writes the layer geopotential
 // Phi_k = interp(geopot, geopot_lower) and press/(rho0*phi).
-__global__ void __launch_bounds__(128) k_column(LevelDev L, Phys ph, int nz, const double* __restrict__ mass,
+__global__ void __launch_bounds__(256) k_column(LevelDev L, Phys ph, int nz, const double* __restrict__ mass,
                                                 const double* __restrict__ temp, const double* __restrict__ mean_m,
                                                 const double* __restrict__ mean_t, double* __restrict__ phik,
                                                 double* __restrict__ pterm) {
-  const int m = L.n + 1;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 10 * m * m) return;
-  int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
+  // 2-D tiles: blockIdx.z = lozenge, x/y tile the (i, j) range [0, n]^2
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, d = blockIdx.z;
+  if (i > L.n || j > L.n) return;
   const int64_t id = nid(L, d, i, j);
   const int64_t src = (i < L.n && j < L.n) ? id : (int64_t)L.nsrc[id];
   double sp = 0.0;
@@ -214,14 +213,10 @@ __global__ void __launch_bounds__(256, 2)
     k_step1(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
             const double* __restrict__ velo, const double* __restrict__ mean_m, const double* __restrict__ mean_t,
             const double* __restrict__ phik, const double* __restrict__ pterm, Step1Out out) {
-  const int m = L.n + 1;
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)10 * m * m * nz) return;
-  int k = (int)(t / (10 * m * m));
-  int r = (int)(t - (int64_t)k * 10 * m * m);
-  int d = r / (m * m);
-  r -= d * m * m;
-  int j = r / m, i = r - j * m;
+  // 2-D tiles over [0, n]^2; blockIdx.z = layer * 10 + lozenge
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z / 10, d = blockIdx.z - 10 * k;
+  if (i > L.n || j > L.n) return;
   const int64_t NN = L.NN;
   const int P = L.P;
   const int64_t id = nid(L, d, i, j);
@@ -381,14 +376,12 @@ template <int MODE>
 __global__ void __launch_bounds__(256, 2) k_trend(LevelDev L, int nz, TrendIO io) {
   const int P = L.P;
   const int64_t NN = L.NN;
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= NN * nz) return;
-  const int k = (int)(t / NN);
-  const int64_t id = t - (int64_t)k * NN;
-  const int pp = P * P;
-  const int d = (int)(id / pp);
-  const int r = (int)(id - (int64_t)d * pp);
-  const int j = r / P - 2, i = r % P - 2;
+  // 2-D tiles over the padded range [-2, n+1]^2; blockIdx.z = layer * 10 + lozenge
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x, jp = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ip >= P || jp >= P) return;
+  const int k = blockIdx.z / 10, d = blockIdx.z - 10 * k;
+  const int i = ip - 2, j = jp - 2;
+  const int64_t id = ((int64_t)d * P + jp) * P + ip;
   const int n = L.n;
   const int64_t ko = (int64_t)k * NN;
   const Rd R(L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2);

@@ -235,12 +235,16 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   cudaStream_t s = h->stream;
   (void)halo_first;
   const int mm = D.n + 1;
+  const dim3 tile(32, 8);
+  const dim3 g_nodes((mm + 31) / 32, (mm + 7) / 8, 10);
+  const dim3 g_layers((mm + 31) / 32, (mm + 7) / 8, 10 * nz);
+  const dim3 g_padded((D.P + 31) / 32, (D.P + 7) / 8, 10 * nz);
   TB(1);
-  k_column<<<blocks_for(10 * mm * mm, 128), 128, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm);
+  k_column<<<g_nodes, tile, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm);
   TE(1);
   Step1Out so{h->qe, h->hfm, h->hft, h->bern};
   TB(2);
-  k_step1<<<blocks_for((int64_t)10 * mm * mm * nz), TPB, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
+  k_step1<<<g_layers, tile, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
   TE(2);
   TrendIO io{};
   io.mass = m; io.temp = t; io.mean_m = h->mean_m; io.mean_t = h->mean_t; io.qe = h->qe; io.hfm = h->hfm;
@@ -255,11 +259,10 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
     else
       k_trend_e<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
   } else {
-    int64_t nt = D.NN * nz;
     if (mode == MODE_RK)
-      k_trend<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+      k_trend<MODE_RK><<<g_padded, tile, 0, s>>>(L, nz, io);
     else
-      k_trend<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
+      k_trend<MODE_TREND><<<g_padded, tile, 0, s>>>(L, nz, io);
   }
   TE(5);
   CK(cudaGetLastError());

@@ -51,6 +51,8 @@ struct Ell {
   MField u32, f32, r32, c32, t32;  // FP32 V-cycle work
   double* partial = nullptr;
   double* scal = nullptr;  // device scalars
+  cudaGraphExec_t cycle_exec[2] = {nullptr, nullptr};  // captured correction cycles (FP32, FP64)
+  int cycle_key[2] = {-1, -1};
   int nbmax = 0;
   std::vector<void*> allocs;
 
@@ -94,6 +96,8 @@ int alloc_field(Ell& E, MField& F, bool fp32 = false) {
 // ---------------------------------------------------------------- setup ----
 static void ell_free(Ell* E) {
   if (!E) return;
+  for (auto& ex : E->cycle_exec)
+    if (ex) cudaGraphExecDestroy(ex);
   for (void* p : E->allocs) cudaFree(p);
   delete E;
 }

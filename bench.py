@@ -3,14 +3,19 @@
 Workload (N=1): uniform icosahedral J5 grid (10,242 cells, 30,720 edges),
 8 Boussinesq layers, flat 4000 m bottom, zonal jet + seeded white-noise free
 surface, explicit RK4 with dt = 300 s (the reference's time_step ->
-dt_step => RK4 -> trend_ml path).  A "step" is one RK4 step (four trend
-evaluations, four fused sub-steps, four ghost copies).  With --gpus N>1 every
-rank advances its own ensemble member (independent seeds, no collective):
-weak scaling, value = member-days per hour summed over ranks.
+dt_step => RK4 -> trend_ml path).  A "step" is one RK4 step: four trend
+evaluations, each fused with its sub-step (3 kernels per stage, ghosts read
+through remap tables).  With --gpus N>1 every rank advances its own ensemble
+member (independent seeds, no collective): weak scaling, value = member-days
+per hour summed over ranks.
 
 --impl reference times the CPU restatement of the reference's path (the
 reference is Fortran; no Fortran compiler exists on the build or GPU hosts)
-on the host cores, OpenMP over the 10 lozenge domains.
+on the host cores, one worker thread per lozenge domain up to the core count.
+
+--kernels-only times the device-resident stepper alone on --level/--nz (no
+CPU baseline, host-buffer path or extra workloads); it is the small case the
+kernel profiles are captured on.
 """
 from __future__ import annotations
 
@@ -43,6 +48,7 @@ def parse():
     p.add_argument("--nz", type=int, default=8)
     p.add_argument("--no-extra", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--kernels-only", action="store_true")
     return p.parse_args()
 
 
@@ -179,12 +185,58 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
     return out
 
 
-def algorithmic_bytes_trend_rk(cells, nz):
-    """Compulsory bytes of one k_trend launch (MODE_RK) per node-layer: reads
-    mass, temp, mean_m, mean_t, qe(3), hflux_m(3), hflux_t(3), bernoulli, Phi,
-    base mass/temp/velo(3) = 20 words; writes dest mass/temp/velo(3) = 5 words;
-    geometry len(3), part(6), hex_inv once per node (amortised over nz)."""
-    return cells * (nz * 25 * 8 + 10 * 8)
+def elliptic_case(lmax, repeats=3):
+    """Free-surface solve on the uniform hierarchy J5..lmax to relative residual
+    1e-10: the reference's FMG and SRJ, the FP64 V-cycle in FP64 refinement
+    (plain FP64 multigrid) and FP32 V-cycles in FP64 refinement.  Best of
+    `repeats` device-timed solves (the report's ms) from a zero first guess."""
+    import numpy as np
+
+    from wavetrisk_hydrostatic_b200 import Grid
+    from wavetrisk_hydrostatic_b200.cases import bathymetry, elliptic_rhs
+    from wavetrisk_hydrostatic_b200.model import EllipticSolver, solver_opts
+
+    g = Grid(5, lmax, radius=6371e3)
+    levels = [g.level(l) for l in range(5, lmax + 1)]
+    S = EllipticSolver(levels, [bathymetry(lv, seed=1) for lv in levels])
+    off = S.offsets
+    f = np.zeros(off[-1])
+    f[off[-2]:off[-1]] = elliptic_rhs(levels[-1], seed=2)
+    S.upload(f=f)
+    S.restrict()
+    _, fr = S.download()
+    out = {"workload": f"Helmholtz free-surface solve, uniform J{lmax} ({10 * 4 ** lmax + 2} cells), "
+                       f"hierarchy J5..J{lmax}, seeded bathymetry 500-5000 m, dt 600 s, rel. residual 1e-10"}
+    methods = [("fmg", solver_opts("fmg", 1e-10, max_vcycle=50, coarse_iter=300)),
+               ("srj", solver_opts("srj", 1e-10, max_srj_iter=4000, coarse_iter=300)),
+               ("mg64", solver_opts("mg64", 1e-10, down_iter=2, up_iter=2, coarse_iter=20)),
+               ("mixed", solver_opts("mixed", 1e-10, down_iter=2, up_iter=2, coarse_iter=20))]
+    for name, o in methods:
+        best, rep = None, None
+        for _ in range(repeats):
+            S.upload(u=np.zeros(off[-1]), f=fr)
+            rep = S.solve(o)
+            best = rep.ms if best is None else min(best, rep.ms)
+        out[name] = {"ms": best, "rel_residual": rep.true_rel_residual, "status": rep.status,
+                     "outer_iterations": rep.outer_iterations}
+    out["mixed_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["mixed"]["ms"]
+    out["mixed_speedup_vs_fmg"] = out["fmg"]["ms"] / out["mixed"]["ms"]
+    S.close()
+    return out
+
+
+def algorithmic_bytes_trend_rk(level, nz):
+    """Compulsory bytes of one k_trend launch (MODE_RK).  Node-layers of the
+    computed range [0, n]^2 read theta, qe(3), hflux_mass(3), hflux_Theta(3),
+    Bernoulli, Phi and the base mass/temp/velo(3) = 17 words and write the
+    stage's mass/temp/velo(3) = 5 words; node-layers of the padded ring only
+    read and write the 5 base words; geometry len(3), part(6) and hex_inv is
+    read once per node of [0, n]^2."""
+    n = 2 ** level
+    P = n + 4
+    inner = 10 * (n + 1) ** 2
+    ring = 10 * P * P - inner
+    return nz * (inner * 22 * 8 + ring * 10 * 8) + inner * 10 * 8
 
 
 def bench_ours(args):
@@ -221,18 +273,20 @@ def bench_ours(args):
         for (lv, nz, steps) in [(7, 16, 20), (8, 32, 5)]:
             rr = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False)
             kt = rr["kernel_ms_per_launch"]
-            ab = algorithmic_bytes_trend_rk(rr["NN"], nz)
+            ab = algorithmic_bytes_trend_rk(lv, nz)
             extra.append({
                 "workload": f"uniform J{lv} ({rr['cells']} cells), {nz} layers, RK4 dt=300 s",
                 "ms_per_step": rr["ms_per_step"], "value": sim_days_per_hour(steps, rr["ms_total"] / 1e3),
                 "kernel_ms_per_launch": kt,
                 "trend_rk_GBps": ab / (kt["trend_rk"] / 1e3) / 1e9,
             })
+        for lmax in (6, 7, 8):
+            extra.append(elliptic_case(lmax))
 
     if rank == 0:
         kt = r["kernel_ms_per_launch"]
         dom = max(kt, key=lambda k: kt[k])
-        ab = algorithmic_bytes_trend_rk(r["NN"], args.nz)
+        ab = algorithmic_bytes_trend_rk(args.level, args.nz)
         ach = ab / (kt["trend_rk"] / 1e3) / 1e9
         traffic = None
         tf = os.path.join(ROOT, "profiles", "trend_rk_traffic.json")
@@ -338,10 +392,24 @@ def bench_reference(args):
         pg.destroy_process_group()
 
 
+def bench_kernels(args):
+    import torch
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    r = run_case(args.level, args.nz, args.steps, args.warmup, seed=1, device=device, e2e=False, kernels=False)
+    print(json.dumps({"workload": f"uniform J{args.level} ({r['cells']} cells), {args.nz} layers, RK4 dt=300 s",
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                      "value": sim_days_per_hour(args.steps, r["ms_total"] / 1e3),
+                      "unit": "simulated days per wall-clock hour"}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         bench_reference(args)
+    elif args.kernels_only:
+        bench_kernels(args)
     else:
         bench_ours(args)
 

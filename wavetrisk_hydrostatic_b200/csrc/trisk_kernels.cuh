@@ -27,17 +27,37 @@ __device__ __forceinline__ int64_t nid(const LevelDev& L, int d, int i, int j) {
   return ((int64_t)d * L.P + (j + 2)) * L.P + (i + 2);
 }
 
+// Block-to-work mapping of the layer kernels: block b covers NODE_TILE
+// consecutive padded nodes of layer b % nz, so the nz blocks of one node chunk
+// are dispatched back to back and read that chunk's level geometry from L2
+// instead of DRAM.  Offsets inside one layer are 32-bit (the context rejects
+// levels with 6*NN >= 2^31).
+constexpr int NODE_TILE = 256;
+
+__device__ __forceinline__ bool layer_node(const LevelDev& L, int nz, int& k, int& id, int& i, int& j) {
+  const int chunk = blockIdx.x / nz;
+  k = blockIdx.x - chunk * nz;
+  id = chunk * NODE_TILE + threadIdx.x;
+  if (id >= L.NN) return false;
+  const int pp = L.P * L.P;
+  const int r = id - (id / pp) * pp;
+  const int jp = r / L.P;
+  j = jp - 2;
+  i = r - jp * L.P - 2;
+  return true;
+}
+
 // Readers of the state through the ghost remap.
 struct Rd {
   const int* __restrict__ nsrc;
   const int* __restrict__ esrc;
   bool direct;
   __device__ __forceinline__ Rd(const LevelDev& L, bool dir) : nsrc(L.nsrc), esrc(L.esrc), direct(dir) {}
-  __device__ __forceinline__ double n(const double* __restrict__ f, int64_t x) const {
-    return f[direct ? x : (int64_t)__ldg(nsrc + x)];
+  __device__ __forceinline__ double n(const double* __restrict__ f, int x) const {
+    return f[direct ? x : __ldg(nsrc + x)];
   }
   // edge field with planes of NN: slot = e*NN + x
-  __device__ __forceinline__ double e(const double* __restrict__ f, int64_t slot) const {
+  __device__ __forceinline__ double e(const double* __restrict__ f, int slot) const {
     if (direct) return f[slot];
     const int c = __ldg(esrc + slot);
     const double v = f[c >> 1];
@@ -73,15 +93,15 @@ __global__ void k_halo_state(int nz, int64_t NN, const int2* __restrict__ hn, in
 // integrate_pressure_up (src/ops.f90:1094-1131), incompressible case, for every
 // node (i, j) in [0, n]^2 of every lozenge.  Writes the layer geopotential
 // Phi_k = interp(geopot, geopot_lower) and press/(rho0*phi).
-__global__ void __launch_bounds__(256) k_column(LevelDev L, Phys ph, int nz, const double* __restrict__ mass,
-                                                const double* __restrict__ temp, const double* __restrict__ mean_m,
-                                                const double* __restrict__ mean_t, double* __restrict__ phik,
-                                                double* __restrict__ pterm) {
-  // 2-D tiles: blockIdx.z = lozenge, x/y tile the (i, j) range [0, n]^2
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, d = blockIdx.z;
-  if (i > L.n || j > L.n) return;
-  const int64_t id = nid(L, d, i, j);
-  const int64_t src = (i < L.n && j < L.n) ? id : (int64_t)L.nsrc[id];
+__global__ void __launch_bounds__(NODE_TILE) k_column(LevelDev L, Phys ph, int nz, const double* __restrict__ mass,
+                                                      const double* __restrict__ temp, const double* __restrict__ mean_m,
+                                                      const double* __restrict__ mean_t, double* __restrict__ phik,
+                                                      double* __restrict__ pterm) {
+  // one thread per padded node, all layers
+  int k0, id, i, j;
+  if (!layer_node(L, 1, k0, id, i, j)) return;
+  if (i < 0 || j < 0 || i > L.n || j > L.n) return;
+  const int src = (i < L.n && j < L.n) ? id : L.nsrc[id];
   double sp = 0.0;
   for (int k = 0; k < nz; ++k) {
     const int64_t o = (int64_t)k * L.NN;
@@ -110,6 +130,7 @@ struct Step1Out {
   double* __restrict__ hfm;   // [nz][3][NN]
   double* __restrict__ hft;   // [nz][3][NN]
   double* __restrict__ bern;  // [nz][NN]
+  double* __restrict__ theta; // [nz][NN]
 };
 
 // post_step1 (src/ops.f90:526-737): PV of the merged triangle at a pentagon
@@ -208,38 +229,39 @@ __device__ __noinline__ void post_corner(const LevelDev L, int c, int d, int64_t
 // j == 0, as at the reference's south and west domain boundaries.  Each edge
 // has exactly one writer, chosen so that the stored value is the one the
 // reference's sequential sweep leaves behind; the four corner threads then
-// apply post_step1.
-__global__ void __launch_bounds__(256, 2)
+// apply post_step1.  The node's potential temperature Theta/rho
+// (src/ops.f90:798, theta_e's node factor) is stored for the velocity trend.
+__global__ void __launch_bounds__(NODE_TILE, 3)
     k_step1(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
             const double* __restrict__ velo, const double* __restrict__ mean_m, const double* __restrict__ mean_t,
             const double* __restrict__ phik, const double* __restrict__ pterm, Step1Out out) {
-  // 2-D tiles over [0, n]^2; blockIdx.z = layer * 10 + lozenge
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = blockIdx.z / 10, d = blockIdx.z - 10 * k;
-  if (i > L.n || j > L.n) return;
-  const int64_t NN = L.NN;
+  int k, id, i, j;
+  if (!layer_node(L, nz, k, id, i, j)) return;
+  if (i < 0 || j < 0 || i > L.n || j > L.n) return;
+  const int NN = L.NN;
   const int P = L.P;
-  const int64_t id = nid(L, d, i, j);
-  const int64_t idN = id + P, idE = id + 1, idS = id - P, idW = id - 1, idNE = id + P + 1, idSW = id - P - 1;
+  const int idN = id + P, idE = id + 1, idS = id - P, idW = id - 1, idNE = id + P + 1, idSW = id - P - 1;
   const int64_t ko = (int64_t)k * NN;
   const Rd R(L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2);
-  const double* Mm = mass + ko;
-  const double* Mt = temp + ko;
-  const double* Am = mean_m + ko;
-  const double* At = mean_t + ko;
-  const double* v = velo + 3 * ko;
-  double* qe = out.qe + 3 * ko;
-  double* hfm = out.hfm + 3 * ko;
-  double* hft = out.hft + 3 * ko;
-  const double* len = L.len;
-  const double* ped = L.pedlen;
-  const double* part = L.part;
-  const double* cor = L.coriolis;
-#define E3(e, x) ((int64_t)(e) * NN + (x))
-#define PART(x, kk) part[(int64_t)((kk) - 1) * NN + (x)]
+  const double* __restrict__ Mm = mass + ko;
+  const double* __restrict__ Mt = temp + ko;
+  const double* __restrict__ Am = mean_m + ko;
+  const double* __restrict__ At = mean_t + ko;
+  const double* __restrict__ v = velo + 3 * ko;
+  double* __restrict__ qe = out.qe + 3 * ko;
+  double* __restrict__ hfm = out.hfm + 3 * ko;
+  double* __restrict__ hft = out.hft + 3 * ko;
+  const double* __restrict__ len = L.len;
+  const double* __restrict__ ped = L.pedlen;
+  const double* __restrict__ part = L.part;
+  const double* __restrict__ cor = L.coriolis;
+#define E3(e, x) ((e) * NN + (x))
+#define PART(x, kk) part[((kk) - 1) * NN + (x)]
 
   const double r0 = R.n(Mm, id) + Am[id], rN = R.n(Mm, idN) + Am[idN], rE = R.n(Mm, idE) + Am[idE],
                rS = R.n(Mm, idS) + Am[idS], rW = R.n(Mm, idW) + Am[idW], rNE = R.n(Mm, idNE) + Am[idNE];
+  const double t0 = R.n(Mt, id) + At[id];
+  out.theta[ko + id] = t0 / r0;
   const double vRT = R.e(v, E3(RT, id)), vDG = R.e(v, E3(DG, id)), vUP = R.e(v, E3(UP, id));
   const double vRT_W = R.e(v, E3(RT, idW)), vDG_SW = R.e(v, E3(DG, idSW)), vUP_S = R.e(v, E3(UP, idS));
   const double u_dual_RT = vRT * ped[E3(RT, id)];
@@ -285,16 +307,12 @@ __global__ void __launch_bounds__(256, 2)
   hfm[E3(RT, id)] = u_dual_RT * interp(r0, rE) + 0.0;
   hfm[E3(DG, id)] = u_dual_DG * interp(r0, rNE) + 0.0;
   hfm[E3(UP, id)] = u_dual_UP * interp(r0, rN) + 0.0;
-  {
-    const double t0 = R.n(Mt, id) + At[id];
-    hft[E3(RT, id)] = u_dual_RT * interp(t0, R.n(Mt, idE) + At[idE]) + 0.0;
-    hft[E3(DG, id)] = u_dual_DG * interp(t0, R.n(Mt, idNE) + At[idNE]) + 0.0;
-    hft[E3(UP, id)] = u_dual_UP * interp(t0, R.n(Mt, idN) + At[idN]) + 0.0;
-  }
+  hft[E3(RT, id)] = u_dual_RT * interp(t0, R.n(Mt, idE) + At[idE]) + 0.0;
+  hft[E3(DG, id)] = u_dual_DG * interp(t0, R.n(Mt, idNE) + At[idNE]) + 0.0;
+  hft[E3(UP, id)] = u_dual_UP * interp(t0, R.n(Mt, idN) + At[idN]) + 0.0;
 
   if (i == 0 || j == 0) {  // comp_SW
     const double rSW = R.n(Mm, idSW) + Am[idSW];
-    const double t0 = R.n(Mt, id) + At[id];
     const double tS = R.n(Mt, idS) + At[idS], tW = R.n(Mt, idW) + At[idW], tSW = R.n(Mt, idSW) + At[idSW];
     const double u_prim_RT_SW = R.e(v, E3(RT, idSW)) * len[E3(RT, idSW)];
     const double u_prim_UP_SW = R.e(v, E3(UP, idSW)) * len[E3(UP, idSW)];
@@ -321,10 +339,11 @@ __global__ void __launch_bounds__(256, 2)
 #undef E3
 #undef PART
   // post_step1 at the pentagon corners, by the thread that wrote those edges
-  if (i == L.n && j == L.n) post_corner(L, 0, d, ko, mass, velo, mean_m, out.qe);
-  if (i == L.n && j == 0) post_corner(L, 1, d, ko, mass, velo, mean_m, out.qe);
-  if (i == 0 && j == 0) post_corner(L, 2, d, ko, mass, velo, mean_m, out.qe);
-  if (i == 0 && j == L.n) post_corner(L, 3, d, ko, mass, velo, mean_m, out.qe);
+  if ((i == 0 || i == L.n) && (j == 0 || j == L.n)) {
+    const int d = id / (P * P);
+    const int c = (i == L.n) ? (j == L.n ? 0 : 1) : (j == 0 ? 2 : 3);
+    post_corner(L, c, d, ko, mass, velo, mean_m, out.qe);
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -339,10 +358,7 @@ __global__ void __launch_bounds__(256, 2)
 enum { MODE_TREND = 0, MODE_RK = 1 };
 
 struct TrendIO {
-  const double* __restrict__ mass;   // stage state q (for theta)
-  const double* __restrict__ temp;
-  const double* __restrict__ mean_m;
-  const double* __restrict__ mean_t;
+  const double* __restrict__ theta;  // Theta/rho of the stage state at [0, n]^2 (k_step1)
   const double* __restrict__ qe;
   const double* __restrict__ hfm;
   const double* __restrict__ hft;
@@ -356,15 +372,15 @@ struct TrendIO {
   double* dm; double* dtt; double* dv;
 };
 
-__device__ __forceinline__ void weights5(const LevelDev& L, int64_t id, int offs, double w[5]) {  // get_weights
-  const int64_t NN = L.NN;
-  double acc = L.part[(int64_t)offs * NN + id];
+__device__ __forceinline__ void weights5(const LevelDev& L, int id, int offs, double w[5]) {  // get_weights
+  const int NN = L.NN;
+  double acc = L.part[offs * NN + id];
   double hinv = L.hex_inv[id];
   double wgt[5];
   wgt[0] = acc;
 #pragma unroll
   for (int q = 2; q <= 5; ++q) {
-    acc = acc + L.part[(int64_t)((q + offs - 1) % 6) * NN + id];
+    acc = acc + L.part[((q + offs - 1) % 6) * NN + id];
     wgt[q - 1] = acc;
   }
 #pragma unroll
@@ -373,15 +389,11 @@ __device__ __forceinline__ void weights5(const LevelDev& L, int64_t id, int offs
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256, 2) k_trend(LevelDev L, int nz, TrendIO io) {
+__global__ void __launch_bounds__(NODE_TILE, 3) k_trend(LevelDev L, int nz, TrendIO io) {
+  int k, id, i, j;
+  if (!layer_node(L, nz, k, id, i, j)) return;
   const int P = L.P;
-  const int64_t NN = L.NN;
-  // 2-D tiles over the padded range [-2, n+1]^2; blockIdx.z = layer * 10 + lozenge
-  const int ip = blockIdx.x * blockDim.x + threadIdx.x, jp = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ip >= P || jp >= P) return;
-  const int k = blockIdx.z / 10, d = blockIdx.z - 10 * k;
-  const int i = ip - 2, j = jp - 2;
-  const int64_t id = ((int64_t)d * P + jp) * P + ip;
+  const int NN = L.NN;
   const int n = L.n;
   const int64_t ko = (int64_t)k * NN;
   const Rd R(L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2);
@@ -389,175 +401,74 @@ __global__ void __launch_bounds__(256, 2) k_trend(LevelDev L, int nz, TrendIO io
   const bool scal = (i >= 0 && j >= 0 && i <= n && j <= n);
   const bool own = (i >= 0 && j >= 0 && i < n && j < n);
   if (scal) {
-    const int64_t idW = id - 1, idS = id - P, idSW = id - P - 1;
-    const double* fm = io.hfm + 3 * ko;
-    const double* ft = io.hft + 3 * ko;
-    double hinv = L.hex_inv[id];
-    double divm = (R.e(fm, RT * NN + id) - R.e(fm, RT * NN + idW) + R.e(fm, DG * NN + idSW) - R.e(fm, DG * NN + id) +
-                   R.e(fm, UP * NN + id) - R.e(fm, UP * NN + idS)) * hinv;
-    double divt = (R.e(ft, RT * NN + id) - R.e(ft, RT * NN + idW) + R.e(ft, DG * NN + idSW) - R.e(ft, DG * NN + id) +
-                   R.e(ft, UP * NN + id) - R.e(ft, UP * NN + idS)) * hinv;
+    const int idW = id - 1, idS = id - P, idSW = id - P - 1;
+    const double* __restrict__ fm = io.hfm + 3 * ko;
+    const double* __restrict__ ft = io.hft + 3 * ko;
+    const double hinv = L.hex_inv[id];
+    const double divm = (R.e(fm, RT * NN + id) - R.e(fm, RT * NN + idW) + R.e(fm, DG * NN + idSW) -
+                         R.e(fm, DG * NN + id) + R.e(fm, UP * NN + id) - R.e(fm, UP * NN + idS)) * hinv;
+    const double divt = (R.e(ft, RT * NN + id) - R.e(ft, RT * NN + idW) + R.e(ft, DG * NN + idSW) -
+                         R.e(ft, DG * NN + id) + R.e(ft, UP * NN + id) - R.e(ft, UP * NN + idS)) * hinv;
     dms = -divm;
     dts = -divt;
   }
   if (own) {
-    const double* hm = io.hfm + 3 * ko;
-    const double* qe = io.qe + 3 * ko;
-    const int64_t idNW = id + P - 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idE = id + 1, idSW = id - P - 1,
-                  idS = id - P, idSE = id - P + 1;
-#define TQ(e1, n1, q0, w) (R.e(hm, (int64_t)(e1) * NN + (n1)) * interp(qe[(int64_t)(e1) * NN + (n1)], (q0)) * (w))
+    const double* __restrict__ hm = io.hfm + 3 * ko;
+    const double* __restrict__ qe = io.qe + 3 * ko;
+    const int idNW = id + P - 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idE = id + 1, idSW = id - P - 1,
+              idS = id - P, idSE = id - P + 1;
+#define TQ(e1, n1, q0, w) (R.e(hm, (e1) * NN + (n1)) * interp(qe[(e1) * NN + (n1)], (q0)) * (w))
     double w1[5], w2[5];
     double q0 = qe[RT * NN + id];
     weights5(L, id, 0, w1);
     weights5(L, idE, 3, w2);
-    double Q0 = TQ(DG, id, q0, w1[0]) + TQ(UP, id, q0, w1[1]) + TQ(RT, idW, q0, w1[2]) + TQ(DG, idSW, q0, w1[3]) +
-                TQ(UP, idS, q0, w1[4]) + TQ(DG, idS, q0, w2[0]) + TQ(UP, idSE, q0, w2[1]) + TQ(RT, idE, q0, w2[2]) +
-                TQ(DG, idE, q0, w2[3]) + TQ(UP, idE, q0, w2[4]);
+    const double Q0 = TQ(DG, id, q0, w1[0]) + TQ(UP, id, q0, w1[1]) + TQ(RT, idW, q0, w1[2]) +
+                      TQ(DG, idSW, q0, w1[3]) + TQ(UP, idS, q0, w1[4]) + TQ(DG, idS, q0, w2[0]) +
+                      TQ(UP, idSE, q0, w2[1]) + TQ(RT, idE, q0, w2[2]) + TQ(DG, idE, q0, w2[3]) +
+                      TQ(UP, idE, q0, w2[4]);
     q0 = qe[DG * NN + id];
     weights5(L, id, 1, w1);
     weights5(L, idNE, 4, w2);
-    double Q1 = TQ(UP, id, q0, w1[0]) + TQ(RT, idW, q0, w1[1]) + TQ(DG, idSW, q0, w1[2]) + TQ(UP, idS, q0, w1[3]) +
-                TQ(RT, id, q0, w1[4]) + TQ(UP, idE, q0, w2[0]) + TQ(RT, idNE, q0, w2[1]) + TQ(DG, idNE, q0, w2[2]) +
-                TQ(UP, idNE, q0, w2[3]) + TQ(RT, idN, q0, w2[4]);
+    const double Q1 = TQ(UP, id, q0, w1[0]) + TQ(RT, idW, q0, w1[1]) + TQ(DG, idSW, q0, w1[2]) +
+                      TQ(UP, idS, q0, w1[3]) + TQ(RT, id, q0, w1[4]) + TQ(UP, idE, q0, w2[0]) +
+                      TQ(RT, idNE, q0, w2[1]) + TQ(DG, idNE, q0, w2[2]) + TQ(UP, idNE, q0, w2[3]) +
+                      TQ(RT, idN, q0, w2[4]);
     q0 = qe[UP * NN + id];
     weights5(L, id, 2, w1);
     weights5(L, idN, 5, w2);
-    double Q2 = TQ(RT, idW, q0, w1[0]) + TQ(DG, idSW, q0, w1[1]) + TQ(UP, idS, q0, w1[2]) + TQ(RT, id, q0, w1[3]) +
-                TQ(DG, id, q0, w1[4]) + TQ(RT, idN, q0, w2[0]) + TQ(DG, idN, q0, w2[1]) + TQ(UP, idN, q0, w2[2]) +
-                TQ(RT, idNW, q0, w2[3]) + TQ(DG, idW, q0, w2[4]);
+    const double Q2 = TQ(RT, idW, q0, w1[0]) + TQ(DG, idSW, q0, w1[1]) + TQ(UP, idS, q0, w1[2]) +
+                      TQ(RT, id, q0, w1[3]) + TQ(DG, id, q0, w1[4]) + TQ(RT, idN, q0, w2[0]) +
+                      TQ(DG, idN, q0, w2[1]) + TQ(UP, idN, q0, w2[2]) + TQ(RT, idNW, q0, w2[3]) +
+                      TQ(DG, idW, q0, w2[4]);
 #undef TQ
     // du_grad
-    const double* mm = io.mass + ko;
-    const double* mt = io.temp + ko;
-    const double* am = io.mean_m + ko;
-    const double* at = io.mean_t + ko;
-    double th0 = (at[id] + R.n(mt, id)) / (am[id] + R.n(mm, id));
-    double thE = (at[idE] + R.n(mt, idE)) / (am[idE] + R.n(mm, idE));
-    double thNE = (at[idNE] + R.n(mt, idNE)) / (am[idNE] + R.n(mm, idNE));
-    double thN = (at[idN] + R.n(mt, idN)) / (am[idN] + R.n(mm, idN));
-    const double* B = io.bern + ko;
-    const double* F = io.phik + ko;   // exner = -Phi_k (src/ops.f90:358)
+    const double* __restrict__ th = io.theta + ko;
+    const double th0 = th[id], thE = th[idE], thNE = th[idNE], thN = th[idN];
+    const double* __restrict__ B = io.bern + ko;
+    const double* __restrict__ F = io.phik + ko;  // exner = -Phi_k (src/ops.f90:358)
     const double lRT = L.len[RT * NN + id], lDG = L.len[DG * NN + id], lUP = L.len[UP * NN + id];
-    double gB0 = (B[idE] - B[id]) / lRT, gB1 = (B[id] - B[idNE]) / lDG, gB2 = (B[idN] - B[id]) / lUP;
-    double xE = -F[idE], x0 = -F[id], xNE = -F[idNE], xN = -F[idN];
-    double gE0 = (xE - x0) / lRT, gE1 = (x0 - xNE) / lDG, gE2 = (xN - x0) / lUP;
+    const double gB0 = (B[idE] - B[id]) / lRT, gB1 = (B[id] - B[idNE]) / lDG, gB2 = (B[idN] - B[id]) / lUP;
+    const double xE = -F[idE], x0 = -F[id], xNE = -F[idNE], xN = -F[idN];
+    const double gE0 = (xE - x0) / lRT, gE1 = (x0 - xNE) / lDG, gE2 = (xN - x0) / lUP;
     dv0 = (-Q0 + 0.0 * lRT) / lRT - gB0 - interp(th0, thE) * gE0;
     dv1 = (-Q1 + 0.0 * lDG) / lDG - gB1 - interp(th0, thNE) * gE1;
     dv2 = (-Q2 + 0.0 * lUP) / lUP - gB2 - interp(th0, thN) * gE2;
   }
+  const int64_t vo = 3 * ko + id;
   if (MODE == MODE_RK) {
     const double h = io.h;
     io.dst_m[ko + id] = io.base_m[ko + id] + h * dms;
     io.dst_t[ko + id] = io.base_t[ko + id] + h * dts;
-    const int64_t vo = 3 * ko + id;
     io.dst_v[vo] = io.base_v[vo] + h * dv0;
     io.dst_v[vo + NN] = io.base_v[vo + NN] + h * dv1;
     io.dst_v[vo + 2 * NN] = io.base_v[vo + 2 * NN] + h * dv2;
   } else {
     io.dm[ko + id] = dms;
     io.dtt[ko + id] = dts;
-    const int64_t vo = 3 * ko + id;
     io.dv[vo] = dv0;
     io.dv[vo + NN] = dv1;
     io.dv[vo + 2 * NN] = dv2;
   }
-}
-
-
-// Same trends and sub-step with one thread per edge (e, node, layer): the
-// velocity trend of one edge per thread, and the node's scalar trends on the RT
-// thread.  Three times the threads of k_trend with a third of the live state
-// each; identical arithmetic.
-template <int MODE>
-__global__ void __launch_bounds__(256, 3) k_trend_e(LevelDev L, int nz, TrendIO io) {
-  const int P = L.P;
-  const int64_t NN = L.NN;
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 3 * NN * nz) return;
-  const int k = (int)(t / (3 * NN));
-  const int64_t rr = t - (int64_t)k * 3 * NN;
-  const int e = (int)(rr / NN);
-  const int64_t id = rr - (int64_t)e * NN;
-  const int pp = P * P;
-  const int d = (int)(id / pp);
-  const int r = (int)(id - (int64_t)d * pp);
-  const int j = r / P - 2, i = r % P - 2;
-  const int n = L.n;
-  const int64_t ko = (int64_t)k * NN;
-  const Rd R(L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2);
-  if (e == RT) {
-    double dms = 0.0, dts = 0.0;
-    if (i >= 0 && j >= 0 && i <= n && j <= n) {
-      const int64_t idW = id - 1, idS = id - P, idSW = id - P - 1;
-      const double* fm = io.hfm + 3 * ko;
-      const double* ft = io.hft + 3 * ko;
-      const double hinv = L.hex_inv[id];
-      const double divm = (R.e(fm, RT * NN + id) - R.e(fm, RT * NN + idW) + R.e(fm, DG * NN + idSW) -
-                           R.e(fm, DG * NN + id) + R.e(fm, UP * NN + id) - R.e(fm, UP * NN + idS)) * hinv;
-      const double divt = (R.e(ft, RT * NN + id) - R.e(ft, RT * NN + idW) + R.e(ft, DG * NN + idSW) -
-                           R.e(ft, DG * NN + id) + R.e(ft, UP * NN + id) - R.e(ft, UP * NN + idS)) * hinv;
-      dms = -divm;
-      dts = -divt;
-    }
-    if (MODE == MODE_RK) {
-      io.dst_m[ko + id] = io.base_m[ko + id] + io.h * dms;
-      io.dst_t[ko + id] = io.base_t[ko + id] + io.h * dts;
-    } else {
-      io.dm[ko + id] = dms;
-      io.dtt[ko + id] = dts;
-    }
-  }
-  double dv = 0.0;
-  if (i >= 0 && j >= 0 && i < n && j < n) {
-    const double* hm = io.hfm + 3 * ko;
-    const double* qe = io.qe + 3 * ko;
-    const int64_t idNW = id + P - 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idE = id + 1, idSW = id - P - 1,
-                  idS = id - P, idSE = id - P + 1;
-#define TQ(e1, n1, w) (R.e(hm, (int64_t)(e1) * NN + (n1)) * interp(qe[(int64_t)(e1) * NN + (n1)], q0) * (w))
-    double w1[5], w2[5];
-    const double q0 = qe[(int64_t)e * NN + id];
-    double Q;
-    int64_t idB;  // far node of the edge
-    if (e == RT) {
-      weights5(L, id, 0, w1);
-      weights5(L, idE, 3, w2);
-      Q = TQ(DG, id, w1[0]) + TQ(UP, id, w1[1]) + TQ(RT, idW, w1[2]) + TQ(DG, idSW, w1[3]) + TQ(UP, idS, w1[4]) +
-          TQ(DG, idS, w2[0]) + TQ(UP, idSE, w2[1]) + TQ(RT, idE, w2[2]) + TQ(DG, idE, w2[3]) + TQ(UP, idE, w2[4]);
-      idB = idE;
-    } else if (e == DG) {
-      weights5(L, id, 1, w1);
-      weights5(L, idNE, 4, w2);
-      Q = TQ(UP, id, w1[0]) + TQ(RT, idW, w1[1]) + TQ(DG, idSW, w1[2]) + TQ(UP, idS, w1[3]) + TQ(RT, id, w1[4]) +
-          TQ(UP, idE, w2[0]) + TQ(RT, idNE, w2[1]) + TQ(DG, idNE, w2[2]) + TQ(UP, idNE, w2[3]) + TQ(RT, idN, w2[4]);
-      idB = idNE;
-    } else {
-      weights5(L, id, 2, w1);
-      weights5(L, idN, 5, w2);
-      Q = TQ(RT, idW, w1[0]) + TQ(DG, idSW, w1[1]) + TQ(UP, idS, w1[2]) + TQ(RT, id, w1[3]) + TQ(DG, id, w1[4]) +
-          TQ(RT, idN, w2[0]) + TQ(DG, idN, w2[1]) + TQ(UP, idN, w2[2]) + TQ(RT, idNW, w2[3]) + TQ(DG, idW, w2[4]);
-      idB = idN;
-    }
-#undef TQ
-    const double* mm = io.mass + ko;
-    const double* mt = io.temp + ko;
-    const double* am = io.mean_m + ko;
-    const double* at = io.mean_t + ko;
-    const double th0 = (at[id] + R.n(mt, id)) / (am[id] + R.n(mm, id));
-    const double thB = (at[idB] + R.n(mt, idB)) / (am[idB] + R.n(mm, idB));
-    const double* B = io.bern + ko;
-    const double* F = io.phik + ko;
-    const double le = L.len[(int64_t)e * NN + id];
-    // gradi_e orientation: RT and UP point from id to the far node, DG from the far node to id
-    const double gB = (e == DG) ? (B[id] - B[idB]) / le : (B[idB] - B[id]) / le;
-    const double x0 = -F[id], xB = -F[idB];
-    const double gE = (e == DG) ? (x0 - xB) / le : (xB - x0) / le;
-    dv = (-Q + 0.0 * le) / le - gB - interp(th0, thB) * gE;
-  }
-  const int64_t vo = 3 * ko + (int64_t)e * NN + id;
-  if (MODE == MODE_RK)
-    io.dst_v[vo] = io.base_v[vo] + io.h * dv;
-  else
-    io.dv[vo] = dv;
 }
 
 }  // namespace wtk

@@ -9,7 +9,7 @@ enum { LORT = 0, UPLT = 1 };
 
 struct LevelDev {
   int n, P;
-  int64_t NN;
+  int NN;  // 10*P*P; 6*NN < 2^31, so offsets inside one layer fit an int
   const double* __restrict__ len;      // 3*NN
   const double* __restrict__ pedlen;   // 3*NN
   const double* __restrict__ part;     // 6*NN

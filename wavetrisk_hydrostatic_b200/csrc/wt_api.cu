@@ -56,7 +56,6 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
   h->ph = Phys{desc->grav, desc->ref_density, desc->p_top};
   h->level_start = desc->level_start;
   h->level_end = desc->level_end;
-  if (const char* tv = std::getenv("WAVETRISK_TREND_KERNEL")) h->trend_variant = (std::strcmp(tv, "edge") == 0) ? 1 : 0;
   const int nlev = desc->level_end - desc->level_start + 1;
   h->lev.resize(nlev);
   int rc = WT_OK;
@@ -64,7 +63,7 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
     const wt_level_desc& ld = desc->levels[q];
     DevLevel& D = h->lev[q];
     if (ld.n != (1 << ld.level) || ld.P != ld.n + 4 || ld.NN != (int64_t)10 * ld.P * ld.P) { rc = WT_ERR_ARG; break; }
-    if (ld.NN >= (int64_t)1 << 31) { rc = WT_ERR_ARG; break; }
+    if (6 * ld.NN >= (int64_t)1 << 31) { rc = WT_ERR_ARG; break; }  // 32-bit offsets inside one layer
     D.level = ld.level;
     D.n = ld.n;
     D.P = ld.P;
@@ -115,7 +114,7 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
     DevLevel& D = h->top();
     const int64_t NN = D.NN, nn = (int64_t)h->nz * NN, ne = 3 * nn;
     double** node_arrays[] = {&h->mass, &h->temp, &h->mean_m, &h->mean_t, &h->m1, &h->t1, &h->m2, &h->t2,
-                              &h->dm, &h->dt, &h->bern, &h->phik, &h->pterm};
+                              &h->dm, &h->dt, &h->bern, &h->phik, &h->pterm, &h->theta};
     for (double** p : node_arrays)
       if ((rc = dev_zero(p, nn))) break;
     double** edge_arrays[] = {&h->velo, &h->v1, &h->v2, &h->dv, &h->qe, &h->hfm, &h->hft};
@@ -140,7 +139,7 @@ int wt_destroy(wt_handle* h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   for (auto& D : h->lev) D.release();
   double* arrays[] = {h->mass, h->temp, h->velo, h->mean_m, h->mean_t, h->m1, h->t1, h->v1, h->m2, h->t2, h->v2,
-                      h->dm, h->dt, h->dv, h->qe, h->hfm, h->hft, h->bern, h->phik, h->pterm};
+                      h->dm, h->dt, h->dv, h->qe, h->hfm, h->hft, h->bern, h->phik, h->pterm, h->theta};
   for (double* p : arrays)
     if (p) cudaFree(p);
   h->release_extra();
@@ -234,36 +233,24 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   const int nz = h->nz;
   cudaStream_t s = h->stream;
   (void)halo_first;
-  const int mm = D.n + 1;
-  const dim3 tile(32, 8);
-  const dim3 g_nodes((mm + 31) / 32, (mm + 7) / 8, 10);
-  const dim3 g_layers((mm + 31) / 32, (mm + 7) / 8, 10 * nz);
-  const dim3 g_padded((D.P + 31) / 32, (D.P + 7) / 8, 10 * nz);
+  // block b: layer b % nz of node chunk b / nz (layer_node in trisk_kernels.cuh)
+  const unsigned chunks = blocks_for(D.NN, NODE_TILE);
   TB(1);
-  k_column<<<g_nodes, tile, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm);
+  k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm);
   TE(1);
-  Step1Out so{h->qe, h->hfm, h->hft, h->bern};
+  Step1Out so{h->qe, h->hfm, h->hft, h->bern, h->theta};
   TB(2);
-  k_step1<<<g_layers, tile, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
+  k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
   TE(2);
   TrendIO io{};
-  io.mass = m; io.temp = t; io.mean_m = h->mean_m; io.mean_t = h->mean_t; io.qe = h->qe; io.hfm = h->hfm;
-  io.hft = h->hft; io.bern = h->bern; io.phik = h->phik;
+  io.theta = h->theta; io.qe = h->qe; io.hfm = h->hfm; io.hft = h->hft; io.bern = h->bern; io.phik = h->phik;
   io.base_m = bm; io.base_t = bt; io.base_v = bv; io.dst_m = om; io.dst_t = ot; io.dst_v = ov; io.h = hstep;
   io.dm = h->dm; io.dtt = h->dt; io.dv = h->dv;
   TB(5);
-  if (h->trend_variant == 1) {
-    int64_t nt = 3 * D.NN * nz;
-    if (mode == MODE_RK)
-      k_trend_e<MODE_RK><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
-    else
-      k_trend_e<MODE_TREND><<<blocks_for(nt), TPB, 0, s>>>(L, nz, io);
-  } else {
-    if (mode == MODE_RK)
-      k_trend<MODE_RK><<<g_padded, tile, 0, s>>>(L, nz, io);
-    else
-      k_trend<MODE_TREND><<<g_padded, tile, 0, s>>>(L, nz, io);
-  }
+  if (mode == MODE_RK)
+    k_trend<MODE_RK><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
+  else
+    k_trend<MODE_TREND><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
   TE(5);
   CK(cudaGetLastError());
   return WT_OK;
@@ -291,10 +278,9 @@ int wt_download_trend(wt_handle* h, double* dmass, double* dtemp, double* dvelo)
 }
 
 // One RK4 step (src/time_integr.f90:78-103): four trend evaluations, each
-// fused with its sub-step, each followed by the ghost copy of WT_after_step.
+// fused with its sub-step.  WT_after_step on a uniform level is the ghost copy,
+// which the kernels replace by reading ghosts through the remap tables.
 static int record_rk4(wt_handle* h, double dt, KTimer* tm = nullptr) {
-  DevLevel& D = h->top();
-  const int nz = h->nz;
   const double hs[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
   // Stage states ping-pong between two buffers: k_trend reads the stage state at
   // neighbouring nodes while it writes the next one, so they must differ (the

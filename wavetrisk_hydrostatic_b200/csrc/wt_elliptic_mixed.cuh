@@ -96,56 +96,6 @@ __global__ void k_axpy_f2d(int64_t n, double* __restrict__ u, const float* __res
 }
 
 
-// Coarsest-level Jacobi sweeps in one thread block (the level is small: J5 has
-// 10*33^2 nodes), so the whole coarse solve is one launch with __syncthreads
-// between sweeps instead of one launch per sweep.  Ping-pong between c and t;
-// the result is left in c.
-template <class T>
-__global__ void __launch_bounds__(1024) k_coarse_jacobi(EllLev L, T* __restrict__ c, const T* __restrict__ r,
-                                                        T* __restrict__ t, int iters, double cf) {
-  const int m = L.n + 1;
-  const int total = 10 * m * m;
-  T* a = c;
-  T* b = t;
-  for (int it = 0; it < iters; ++it) {
-    for (int q = threadIdx.x; q < total; q += blockDim.x) {
-      int d, i, j;
-      decode(L, q, d, i, j, m);
-      const int64_t id = nidx(L, d, i, j);
-      if (L.nsrc[id] != id) continue;
-      const int64_t NN = L.NN, P = L.P;
-      T lq;
-      if constexpr (sizeof(T) == 4) {
-        const float div = (flux32(L, (const float*)a, RT * NN + id) - flux32(L, (const float*)a, RT * NN + id - 1) +
-                           flux32(L, (const float*)a, DG * NN + id - P - 1) - flux32(L, (const float*)a, DG * NN + id) +
-                           flux32(L, (const float*)a, UP * NN + id) - flux32(L, (const float*)a, UP * NN + id - P)) *
-                          L.hinvf[id];
-        lq = div - a[id];
-        b[id] = a[id] + (r[id] - lq) / L.diagf[id];
-      } else {
-        const double div = (ell_flux(L, (const double*)a, RT * NN + id) - ell_flux(L, (const double*)a, RT * NN + id - 1) +
-                            ell_flux(L, (const double*)a, DG * NN + id - P - 1) - ell_flux(L, (const double*)a, DG * NN + id) +
-                            ell_flux(L, (const double*)a, UP * NN + id) - ell_flux(L, (const double*)a, UP * NN + id - P)) *
-                           L.hinv[id];
-        lq = cf * div - a[id];
-        b[id] = a[id] + 1.0 * (r[id] - lq) / L.diag[id];
-      }
-    }
-    __syncthreads();
-    T* x = a;
-    a = b;
-    b = x;
-  }
-  if (a != c) {
-    for (int q = threadIdx.x; q < total; q += blockDim.x) {
-      int d, i, j;
-      decode(L, q, d, i, j, m);
-      const int64_t id = nidx(L, d, i, j);
-      c[id] = a[id];
-    }
-  }
-}
-
 void jacobi32(Ell& E, MField& u, MField& f, int l, int iters, float w = 1.f) {
   EllLev V = E.view(l);
   unsigned g = nb(10 * E.m(l) * E.m(l));
@@ -171,8 +121,7 @@ void vcycle32(Ell& E, const wt_solver_opts& o) {
     k_restrict32<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, E.u32.lvf[j - E.ls], E.f32.lvf[j - E.ls],
                                                                  E.r32.lvf[j - 1 - E.ls]);
   }
-  k_coarse_jacobi<float><<<1, 1024, 0, E.s()>>>(E.view(E.ls), E.c32.lvf[0], E.r32.lvf[0], E.t32.lvf[0],
-                                                 o.coarse_iter, E.cf);
+  jacobi32(E, E.c32, E.r32, E.ls, o.coarse_iter);
   for (int j = E.ls + 1; j <= E.le; ++j) {
     EllLev C = E.view(j - 1), F = E.view(j);
     int n = E.L[j - 1 - E.ls].n;
@@ -198,8 +147,7 @@ void vcycle64(Ell& E, const wt_solver_opts& o) {
     k_restrict<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, E.au.lv[j - E.ls], E.wc_temp.lv[j - E.ls],
                                                                 E.res.lv[j - 1 - E.ls]);
   }
-  k_coarse_jacobi<double><<<1, 1024, 0, E.s()>>>(E.view(E.ls), E.corr.lv[0], E.res.lv[0], E.tmp.lv[0],
-                                                  o.coarse_iter, E.cf);
+  jacobi(E, E.corr, E.res, E.ls, o.coarse_iter);
   for (int j = E.ls + 1; j <= E.le; ++j) {
     EllLev C = E.view(j - 1), F = E.view(j);
     int n = E.L[j - 1 - E.ls].n;

@@ -18,7 +18,7 @@ struct DevLevel {
   int* nsrc = nullptr;  // node read remap (ghost -> source node)
   int* esrc = nullptr;  // signed edge read remap: source slot * 2 + negate
   wtk::LevelDev view() const {
-    return wtk::LevelDev{n, P, NN, len, pedlen, part, hex_inv, triarea, coriolis, topo, nsrc, esrc};
+    return wtk::LevelDev{n, P, (int)NN, len, pedlen, part, hex_inv, triarea, coriolis, topo, nsrc, esrc};
   }
   void release() {
     double* a[] = {len, pedlen, part, hex_inv, triarea, coriolis, overl_a, topo};
@@ -47,11 +47,11 @@ struct wt_handle {
   // trend output (wt_trend) and operator work arrays
   double *dm = nullptr, *dt = nullptr, *dv = nullptr;
   double *qe = nullptr, *hfm = nullptr, *hft = nullptr, *bern = nullptr, *phik = nullptr, *pterm = nullptr;
+  double* theta = nullptr;  // Theta/rho of the stage state, written by k_step1
   bool state_halo_done = false;
   cudaGraphExec_t graph_exec = nullptr;
   double graph_dt = 0.0;
   int sticky = 0;  // WT_OK or the first error seen by a device-side check
-  int trend_variant = 0;  // 0: thread per node (k_trend), 1: thread per edge (k_trend_e)
 
   // elliptic solver state (allocated by wt_elliptic_setup)
   void* ell = nullptr;

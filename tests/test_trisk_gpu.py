@@ -104,3 +104,27 @@ def test_rk4_is_deterministic():
     for o in outs[1:]:
         for k in ("mass", "temp", "velo"):
             assert np.array_equal(o[k], outs[0][k])
+
+
+@pytest.mark.parametrize("level,nz", [(4, 2), (5, 8), (7, 2)])
+def test_trend_kernel_variants_agree(level, nz, monkeypatch):
+    """The TMA-staged trend kernel (default) and the L1 variant
+    (WAVETRISK_TREND_KERNEL=plain) give identical RK4 states, and both match
+    the oracle."""
+    g = Grid(level, level, radius=6371e3).level(level)
+    ph = OceanParams()
+    st = jet_state(g, nz, seed=3 + level, ph=ph)
+    outs = []
+    for variant in ("tma", "plain"):
+        monkeypatch.setenv("WAVETRISK_TREND_KERNEL", variant)
+        model = TriskModel(g, nz, st["topo"], ph)
+        model.upload(st)
+        model.rk4(300.0, 2)
+        outs.append(model.download())
+        assert model.status() == 0
+        model.close()
+    for key in ("mass", "temp", "velo"):
+        assert np.array_equal(outs[0][key], outs[1][key])
+    m, t, v = oracle.rk4(g, nz, ph, st, 300.0, 2)
+    assert rel(outs[0]["mass"], m) <= TOL
+    assert rel(outs[0]["velo"], v) <= TOL

@@ -1,5 +1,7 @@
 // Plain data types shared by the TRiSK kernels and the device context.
 #pragma once
+#include <cuda.h>
+
 #include <cstdint>
 
 namespace wtk {
@@ -21,6 +23,22 @@ struct LevelDev {
   // edge slot e reads slot esrc[e] >> 1, negated when esrc[e] & 1.
   const int* __restrict__ nsrc;        // NN
   const int* __restrict__ esrc;        // 3*NN
+};
+
+// Tensor maps of one handle's trend inputs, dims (x = P, y = P, lozenge = 10,
+// plane); consumed by the TMA-staged trend kernel.
+struct TrendMaps {
+  CUtensorMap hfm, hft, qe;       // plane = 3*layer + edge orientation
+  CUtensorMap theta, bern, phik;  // plane = layer
+  CUtensorMap part;               // plane = area part 0..5
+  CUtensorMap hinv;               // one plane
+};
+
+// Tensor maps of the step1 inputs for one stage state buffer.
+struct Step1Maps {
+  CUtensorMap mass, temp, velo;  // plane = layer (velo: 3*layer + edge orientation)
+  CUtensorMap mean_m, mean_t;    // plane = layer
+  CUtensorMap len, ped, part, cor;  // plane = edge orientation / area part / triangle
 };
 
 struct Phys {

@@ -1,6 +1,7 @@
 // C-ABI implementation: device context, state upload/download, the trend and
 // the RK4 stepper (one captured CUDA graph per step).
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -10,6 +11,7 @@
 
 #include "../../include/wavetrisk_gpu.h"
 #include "trisk_kernels.cuh"
+#include "trisk_tma.cuh"
 #include "wt_handle.cuh"
 
 using namespace wtk;
@@ -43,6 +45,55 @@ static int dev_copy(double** dst, const double* src, int64_t count) {
 }
 
 static int dev_zero(double** dst, int64_t count) { return dev_copy(dst, nullptr, count); }
+
+// Tensor maps of the trend inputs on the top level: dims (P, P, 10 lozenges,
+// planes), boxes of TB_X x TB_Y nodes.  The encoder is taken from the driver
+// through the runtime, so the library does not link libcuda directly.
+static int make_trend_maps(wt_handle* h) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
+      std::fprintf(stderr, "wavetrisk_gpu: cuTensorMapEncodeTiled unavailable\n");
+      return WT_ERR_CUDA;
+    }
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const DevLevel& D = h->top();
+  auto mk = [&](CUtensorMap* m, const double* base, int planes) {
+    const cuuint64_t dims[4] = {(cuuint64_t)D.P, (cuuint64_t)D.P, 10, (cuuint64_t)planes};
+    const cuuint64_t strides[3] = {(cuuint64_t)D.P * 8, (cuuint64_t)D.P * D.P * 8, (cuuint64_t)D.NN * 8};
+    const cuuint32_t box[4] = {(cuuint32_t)TB_X, (cuuint32_t)TB_Y, 1, 1};
+    const cuuint32_t elem[4] = {1, 1, 1, 1};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(base), dims, strides, box, elem,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  TrendMaps& M = h->maps;
+  const int nz = h->nz;
+  bool ok = mk(&M.hfm, h->hfm, 3 * nz) && mk(&M.hft, h->hft, 3 * nz) && mk(&M.qe, h->qe, 3 * nz) &&
+                  mk(&M.theta, h->theta, nz) && mk(&M.bern, h->bern, nz) && mk(&M.phik, h->phik, nz) &&
+                  mk(&M.part, D.part, 6) && mk(&M.hinv, D.hex_inv, 1);
+  double* SM[3] = {h->mass, h->m1, h->m2};
+  double* ST[3] = {h->temp, h->t1, h->t2};
+  double* SV[3] = {h->velo, h->v1, h->v2};
+  for (int b = 0; b < 3 && ok; ++b) {
+    Step1Maps& S = h->s1maps[b];
+    ok = mk(&S.mass, SM[b], nz) && mk(&S.temp, ST[b], nz) && mk(&S.velo, SV[b], 3 * nz) && mk(&S.mean_m, h->mean_m, nz) &&
+         mk(&S.mean_t, h->mean_t, nz) && mk(&S.len, D.len, 3) && mk(&S.ped, D.pedlen, 3) && mk(&S.part, D.part, 6) &&
+         mk(&S.cor, D.coriolis, 2);
+  }
+  if (!ok) {
+    std::fprintf(stderr, "wavetrisk_gpu: tensor map encoding failed\n");
+    return WT_ERR_CUDA;
+  }
+  CK(cudaFuncSetAttribute(k_step1_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, STEP1_TMA_SMEM));
+  CK(cudaFuncSetAttribute(k_trend_tma<MODE_RK>, cudaFuncAttributeMaxDynamicSharedMemorySize, TREND_TMA_SMEM));
+  CK(cudaFuncSetAttribute(k_trend_tma<MODE_TREND>, cudaFuncAttributeMaxDynamicSharedMemorySize, TREND_TMA_SMEM));
+  return WT_OK;
+}
 
 extern "C" {
 
@@ -110,6 +161,16 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
     cudaMemcpy(D.esrc, esrc.data(), sizeof(int) * 3 * NN, cudaMemcpyHostToDevice);
   }
   if (rc == WT_OK) {
+    // Kernel pair: TMA-staged tiles from n = 64 up; below that the 32-wide tiles
+    // are mostly empty (n + 1 = 33 nodes per row at J5) and the L1 kernels are
+    // faster.  WAVETRISK_TREND_KERNEL=tma|plain forces either pair.
+    h->trend_variant = (h->top().n >= 64) ? 0 : 1;
+    if (const char* tv = std::getenv("WAVETRISK_TREND_KERNEL")) {
+      if (std::strcmp(tv, "tma") == 0) h->trend_variant = 0;
+      if (std::strcmp(tv, "plain") == 0) h->trend_variant = 1;
+    }
+  }
+  if (rc == WT_OK) {
     // Prognostic state and RK/trend work arrays on level_end.
     DevLevel& D = h->top();
     const int64_t NN = D.NN, nn = (int64_t)h->nz * NN, ne = 3 * nn;
@@ -125,6 +186,12 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
       cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
       if (e != cudaSuccess) rc = wt_handle_fail("stream", e);
     }
+    if (rc == WT_OK) {
+      cudaError_t e = cudaMalloc(&h->dflag, sizeof(int));
+      if (e == cudaSuccess) e = cudaMemset(h->dflag, 0, sizeof(int));
+      if (e != cudaSuccess) rc = wt_handle_fail("flag", e);
+    }
+    if (rc == WT_OK) rc = make_trend_maps(h);
   }
   if (rc != WT_OK) {
     wt_destroy(h);
@@ -143,6 +210,7 @@ int wt_destroy(wt_handle* h) {
   for (double* p : arrays)
     if (p) cudaFree(p);
   h->release_extra();
+  if (h->dflag) cudaFree(h->dflag);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return WT_OK;
@@ -160,6 +228,11 @@ int wt_status(wt_handle* h) {
   if (!h) return WT_ERR_ARG;
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaGetLastError());
+  if (h->dflag && h->sticky == WT_OK) {
+    int f = 0;
+    CK(cudaMemcpy(&f, h->dflag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) h->sticky = WT_ERR_TIMEOUT;
+  }
   return h->sticky;
 }
 
@@ -240,17 +313,34 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   TE(1);
   Step1Out so{h->qe, h->hfm, h->hft, h->bern, h->theta};
   TB(2);
-  k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
+  if (h->trend_variant == 0) {
+    const int sb = (m == h->m1) ? 1 : (m == h->m2) ? 2 : 0;  // which state buffer the stage reads
+    const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;
+    const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
+    k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, s>>>(L, nz, nbx, nby, m, t, v, h->mean_m, h->phik, h->pterm, so,
+                                                           h->dflag, h->s1maps[sb]);
+  } else {
+    k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
+  }
   TE(2);
   TrendIO io{};
   io.theta = h->theta; io.qe = h->qe; io.hfm = h->hfm; io.hft = h->hft; io.bern = h->bern; io.phik = h->phik;
   io.base_m = bm; io.base_t = bt; io.base_v = bv; io.dst_m = om; io.dst_t = ot; io.dst_v = ov; io.h = hstep;
   io.dm = h->dm; io.dtt = h->dt; io.dv = h->dv;
   TB(5);
-  if (mode == MODE_RK)
-    k_trend<MODE_RK><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
-  else
-    k_trend<MODE_TREND><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
+  if (h->trend_variant == 0) {
+    const int nbx = (D.P + TT_X - 1) / TT_X, nby = (D.P + TT_Y - 1) / TT_Y;
+    const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
+    if (mode == MODE_RK)
+      k_trend_tma<MODE_RK><<<nblk, TT_X * TT_Y, TREND_TMA_SMEM, s>>>(L, nz, nbx, nby, io, h->dflag, h->maps);
+    else
+      k_trend_tma<MODE_TREND><<<nblk, TT_X * TT_Y, TREND_TMA_SMEM, s>>>(L, nz, nbx, nby, io, h->dflag, h->maps);
+  } else {
+    if (mode == MODE_RK)
+      k_trend<MODE_RK><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
+    else
+      k_trend<MODE_TREND><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
+  }
   TE(5);
   CK(cudaGetLastError());
   return WT_OK;

@@ -48,6 +48,10 @@ struct wt_handle {
   double *dm = nullptr, *dt = nullptr, *dv = nullptr;
   double *qe = nullptr, *hfm = nullptr, *hft = nullptr, *bern = nullptr, *phik = nullptr, *pterm = nullptr;
   double* theta = nullptr;  // Theta/rho of the stage state, written by k_step1
+  wtk::TrendMaps maps{};    // tensor maps of the trend inputs (TMA-staged trend kernel)
+  wtk::Step1Maps s1maps[3]{};  // step1 input maps for the state buffers (mass,temp,velo), (m1,t1,v1), (m2,t2,v2)
+  int* dflag = nullptr;     // device error flag: 1 = a kernel's staged copies did not complete
+  int trend_variant = 0;    // 0: TMA-staged k_step1_tma/k_trend_tma, 1: k_step1/k_trend (loads through L1)
   bool state_halo_done = false;
   cudaGraphExec_t graph_exec = nullptr;
   double graph_dt = 0.0;

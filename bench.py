@@ -1,8 +1,10 @@
 """Benchmark: simulated days per wall-clock hour of the TRiSK RK4 stepper.
 
-Workload (N=1): uniform icosahedral J5 grid (10,242 cells, 30,720 edges),
-8 Boussinesq layers, flat 4000 m bottom, zonal jet + seeded white-noise free
-surface, explicit RK4 with dt = 300 s (the reference's time_step ->
+Workload (N=1): uniform icosahedral J7 grid (163,842 cells, 491,520 edges),
+16 Boussinesq layers -- the adaptive J4..J7, 16-layer run with every point
+active (wavelet adaptivity is not part of this stepper yet) -- flat 4000 m
+bottom, zonal jet + seeded white-noise free surface, explicit RK4 with
+dt = 300 s (the reference's time_step ->
 dt_step => RK4 -> trend_ml path).  A "step" is one RK4 step: four trend
 evaluations, each fused with its sub-step (3 kernels per stage, ghosts read
 through remap tables).  With --gpus N>1 every rank advances its own ensemble
@@ -44,8 +46,8 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--level", type=int, default=5)
-    p.add_argument("--nz", type=int, default=8)
+    p.add_argument("--level", type=int, default=7)
+    p.add_argument("--nz", type=int, default=16)
     p.add_argument("--no-extra", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--kernels-only", action="store_true")
@@ -225,6 +227,19 @@ def elliptic_case(lmax, repeats=3):
     return out
 
 
+def workload_config(args, world=1):
+    cells = 10 * 4 ** args.level + 2
+    return {
+        "workload": f"uniform J{args.level} icosahedral grid ({cells} cells), {args.nz} Boussinesq layers, "
+                    f"flat 4000 m bottom, explicit RK4 dt=300 s"
+                    + (" (the adaptive J4..J7 16-layer run with every point active)"
+                       if (args.level, args.nz) == (7, 16) else ""),
+        "level": args.level, "layers": args.nz, "dt_s": DT,
+        "parallelism": f"replicas x{world} (independent ensemble members)" if world > 1 else "single GPU",
+        "l2": "flushed (256 MB write) between timed steps, outside the timed region",
+    }
+
+
 def algorithmic_bytes_trend_rk(level, nz):
     """Compulsory bytes of one k_trend launch (MODE_RK).  Node-layers of the
     computed range [0, n]^2 read theta, qe(3), hflux_mass(3), hflux_Theta(3),
@@ -270,7 +285,7 @@ def bench_ours(args):
 
     extra = []
     if not args.no_extra and rank == 0 and world == 1:
-        for (lv, nz, steps) in [(7, 16, 20), (8, 32, 5)]:
+        for (lv, nz, steps) in [(5, 8, 100), (8, 32, 10)]:
             rr = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False)
             kt = rr["kernel_ms_per_launch"]
             ab = algorithmic_bytes_trend_rk(lv, nz)
@@ -279,6 +294,7 @@ def bench_ours(args):
                 "ms_per_step": rr["ms_per_step"], "value": sim_days_per_hour(steps, rr["ms_total"] / 1e3),
                 "kernel_ms_per_launch": kt,
                 "trend_rk_GBps": ab / (kt["trend_rk"] / 1e3) / 1e9,
+                "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,
             })
         for lmax in (6, 7, 8):
             extra.append(elliptic_case(lmax))
@@ -309,13 +325,7 @@ def bench_ours(args):
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic (seeded jet + white-noise free surface)",
-            "config": {
-                "workload": f"uniform J{args.level} icosahedral grid ({r['cells']} cells), {args.nz} Boussinesq layers, "
-                            f"flat 4000 m bottom, explicit RK4 dt=300 s",
-                "level": args.level, "layers": args.nz, "dt_s": DT,
-                "parallelism": f"replicas x{world} (independent ensemble members)" if world > 1 else "single GPU",
-                "l2": "flushed (256 MB write) between timed steps, outside the timed region",
-            },
+            "config": workload_config(args, world),
             "e2e": {"value": e2e_value, "unit": "simulated days per wall-clock hour",
                     "h2d_bytes_per_step": r["h2d_bytes_per_step"], "d2h_bytes_per_step": r["d2h_bytes_per_step"],
                     "path": "wt_rk4_step_host (C-ABI), pinned host buffers, state copied in and out every step"},
@@ -382,8 +392,8 @@ def bench_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded jet + white-noise free surface)",
-        "config": {"workload": f"uniform J{args.level} icosahedral grid, {args.nz} Boussinesq layers, explicit RK4 dt=300 s",
-                   "note": "CPU restatement of the reference path (no Fortran compiler on the host)"},
+        "config": dict(workload_config(args, world),
+                       note="CPU restatement of the reference path (no Fortran compiler on the host)"),
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

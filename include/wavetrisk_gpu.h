@@ -71,6 +71,8 @@ typedef struct {
   int64_t n_halo_node;
   const int64_t *halo_edge;    /* 3*n_halo_edge (dst, src, sign)              */
   int64_t n_halo_edge;
+  const double *iu_wgt;        /* 9*NN  I_u_wgt%enc (outer velocity weights, set_WT_wgts,
+                                  src/wavelet.f90:1567-1705); NULL on level_start */
 } wt_level_desc;
 
 typedef struct {
@@ -185,6 +187,45 @@ int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report
  * make that first call before any stream capture. */
 int wt_elliptic_l2_noalloc(int level, int domain_level, const int* nsrc, const double* field, double* result,
                            void* stream);
+
+/* ------------------------------------------------------------ wavelets ---- */
+/* Multi-level fields of the prognostic variables on the hierarchy
+ * [level_start, level_end] of the handle, every layer.  The reference keeps
+ * them in sol(v,k) and wav_coeff(v,k) (src/shared.f90) with the masks mask_n,
+ * mask_e of each domain (src/domain.f90).  Level level_end's scaling fields are
+ * the stepper's state (wt_upload_state/wt_rk4_step). */
+enum {
+  WT_FIELD_MASS = 0, WT_FIELD_TEMP = 1, WT_FIELD_VELO = 2,   /* scaling: [nz][NN], [nz][NN], [nz][3*NN] doubles */
+  WT_WAVE_MASS = 3, WT_WAVE_TEMP = 4, WT_WAVE_VELO = 5,      /* wavelet coefficients, same shapes            */
+  WT_MASK_NODE = 6, WT_MASK_EDGE = 7                         /* int32 [NN], [3*NN]                           */
+};
+/* Mask values (src/shared.f90:58-73). */
+enum { WT_MASK_ZERO = 0, WT_MASK_TRSK = 2, WT_MASK_ADJZONE = 8, WT_MASK_RESTRCT = 12, WT_MASK_TOLRNZ = 16,
+       WT_MASK_FROZEN = 32 };
+
+/* Allocates the coarse-level scaling fields, the wavelet fields (zero) and the
+ * masks (TOLRNZ: every point active) of every level.  Needs iu_wgt on every
+ * level above level_start. */
+int wt_wavelet_setup(wt_handle* h);
+/* Host <-> device copy of one field of one level (host layout as the device's).
+ * Downloads of scaling and wavelet fields first give ghosts their copies. */
+int wt_upload_field(wt_handle* h, int level, int field, const void* src);
+int wt_download_field(wt_handle* h, int level, int field, void* dst);
+/* forward_wavelet_transform(scaling, wavelet, level_start+1) (src/wavelet.f90:20-98):
+ * scalar and velocity wavelets of levels > level_start, coarse scaling by
+ * lifting (scalars) and averaging (velocity). */
+int wt_forward_wt(wt_handle* h);
+/* inverse_wavelet_transform(wavelet, scaling, level_start) (src/wavelet.f90:208-296). */
+int wt_inverse_wt(wt_handle* h);
+/* The threshold pass of mask_active (src/mask.f90:17-38, mask_tol_vars :102-156):
+ * level_end on nodes [0, n], coarser levels on [-1, n+1].  threshold is
+ * [3][nz] (mass, Theta, velocity per layer), as threshold(v, k). */
+int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill);
+/* compress_wavelets (src/adapt.f90:79-103): zero the wavelets of inactive points. */
+int wt_compress(wt_handle* h);
+/* WT_after_step (src/adapt.f90:234-283): wavelets of the current scaling fields,
+ * compression, inverse transform. */
+int wt_wt_after_step(wt_handle* h);
 
 /* Raw stream of the handle (cudaStream_t), for event timing by the caller. */
 void* wt_stream(wt_handle* h);

@@ -1,0 +1,93 @@
+"""ORACLE (test infrastructure only): bindings of oracle_wavelet.cpp.
+
+`Hierarchy` holds, for every level of a uniform hierarchy, the scaling and
+wavelet fields of layer mass, potential temperature and velocity (all layers)
+and the node/edge masks, as numpy arrays in the padded lozenge layout, and runs
+the reference's forward/inverse wavelet transforms, mask_tol_vars, compression
+and WT_after_step on them in place."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _dp, _ip, lib
+
+FROZEN, TOLRNZ, ADJZONE, ZERO = 32, 16, 8, 0
+_i32p = C.POINTER(C.c_int32)
+
+
+class orc_wlevel(C.Structure):
+    _fields_ = [("level", C.c_int), ("n", C.c_int), ("P", C.c_int), ("NN", C.c_int64),
+                ("len", _dp), ("triarea", _dp), ("hex_inv", _dp), ("overl_a", _dp), ("iu_wgt", _dp),
+                ("halo_node", _ip), ("n_halo_node", C.c_int64), ("halo_edge", _ip), ("n_halo_edge", C.c_int64),
+                ("mask_n", _i32p), ("mask_e", _i32p),
+                ("s_m", _dp), ("s_t", _dp), ("s_v", _dp), ("w_m", _dp), ("w_t", _dp), ("w_v", _dp)]
+
+
+def _bind():
+    L = lib()
+    P = C.POINTER(orc_wlevel)
+    for name in ("orc_wt_forward", "orc_wt_inverse", "orc_compress", "orc_wt_after_step"):
+        getattr(L, name).argtypes = [P, C.c_int, C.c_int, C.c_int]
+    L.orc_mask_tol.argtypes = [P, C.c_int, C.c_int, C.c_int, _dp, C.c_int]
+    return L
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class Hierarchy:
+    """Fields of levels levels[0].level .. levels[-1].level with nz layers."""
+
+    FIELDS = ("s_m", "s_t", "s_v", "w_m", "w_t", "w_v")
+
+    def __init__(self, levels, nz):
+        self.L = _bind()
+        self.levels = levels
+        self.nz = nz
+        self.ls, self.le = levels[0].level, levels[-1].level
+        self.arr = (orc_wlevel * len(levels))()
+        self.keep = []
+        self.f = []
+        for q, g in enumerate(levels):
+            geo = [np.ascontiguousarray(x, dtype=np.float64) for x in (g.len, g.triarea, g.hex_inv, g.overl_a)]
+            iu = np.ascontiguousarray(g.iu_wgt if g.iu_wgt is not None else np.zeros((9, g.NN)), dtype=np.float64)
+            hn = np.ascontiguousarray(g.halo_node, dtype=np.int64)
+            he = np.ascontiguousarray(g.halo_edge, dtype=np.int64)
+            fl = {
+                "mask_n": np.full(g.NN, TOLRNZ, dtype=np.int32),
+                "mask_e": np.full(3 * g.NN, TOLRNZ, dtype=np.int32),
+                "s_m": np.zeros((nz, g.NN)), "s_t": np.zeros((nz, g.NN)), "s_v": np.zeros((nz, 3 * g.NN)),
+                "w_m": np.zeros((nz, g.NN)), "w_t": np.zeros((nz, g.NN)), "w_v": np.zeros((nz, 3 * g.NN)),
+            }
+            self.keep += geo + [iu, hn, he]
+            self.f.append(fl)
+            self.arr[q] = orc_wlevel(g.level, g.n, g.P, g.NN, *[_p(x) for x in geo], _p(iu),
+                                     _p(hn, _ip), len(hn), _p(he, _ip), len(he),
+                                     _p(fl["mask_n"], _i32p), _p(fl["mask_e"], _i32p),
+                                     *[_p(fl[k]) for k in self.FIELDS])
+
+    def field(self, level, name):
+        """The numpy array of `name` (s_m, s_t, s_v, w_m, w_t, w_v, mask_n, mask_e) at `level`, by reference."""
+        return self.f[level - self.ls][name]
+
+    def set(self, level, name, value):
+        self.f[level - self.ls][name][...] = value
+
+    def forward(self):
+        self.L.orc_wt_forward(self.arr, self.ls, self.le, self.nz)
+
+    def inverse(self):
+        self.L.orc_wt_inverse(self.arr, self.ls, self.le, self.nz)
+
+    def mask_tol(self, threshold, level_fill):
+        thr = np.ascontiguousarray(threshold, dtype=np.float64).reshape(3, self.nz)
+        self.L.orc_mask_tol(self.arr, self.ls, self.le, self.nz, _p(thr), int(level_fill))
+
+    def compress(self):
+        self.L.orc_compress(self.arr, self.ls, self.le, self.nz)
+
+    def wt_after_step(self):
+        self.L.orc_wt_after_step(self.arr, self.ls, self.le, self.nz)

@@ -49,7 +49,7 @@ class wt_level_desc(C.Structure):
                 ("len", _dp), ("pedlen", _dp), ("part", _dp), ("hex_inv", _dp), ("triarea", _dp),
                 ("coriolis", _dp), ("overl_a", _dp), ("topo", _dp),
                 ("halo_node", _ip), ("n_halo_node", C.c_int64),
-                ("halo_edge", _ip), ("n_halo_edge", C.c_int64)]
+                ("halo_edge", _ip), ("n_halo_edge", C.c_int64), ("iu_wgt", _dp)]
 
 
 class wt_grid_desc(C.Structure):
@@ -119,6 +119,14 @@ _DEVICE_SIGS = {
     "wt_elliptic_prolong": [_vp, C.c_int],
     "wt_elliptic_l2": [_vp, C.c_int, C.c_int, _dp],
     "wt_elliptic_solve": [_vp, C.POINTER(wt_solver_opts), C.POINTER(wt_solver_report)],
+    "wt_wavelet_setup": [_vp],
+    "wt_upload_field": [_vp, C.c_int, C.c_int, _vp],
+    "wt_download_field": [_vp, C.c_int, C.c_int, _vp],
+    "wt_forward_wt": [_vp],
+    "wt_inverse_wt": [_vp],
+    "wt_mask_tol_vars": [_vp, _dp, C.c_int],
+    "wt_compress": [_vp],
+    "wt_wt_after_step": [_vp],
 }
 
 

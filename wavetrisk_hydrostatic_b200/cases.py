@@ -144,3 +144,34 @@ def elliptic_rhs(g: LevelGeom, seed: int = 0) -> np.ndarray:
     f[sel | ((d >= 5) & (i == 0) & (j == g.n)) | ((d < 5) & (i == g.n) & (j == 0))] -= mean
     halo_nodes(g, f)
     return f
+
+
+def solid_body_rotation(u0: float = 1.0):
+    """Tangent field of a rigid rotation about the polar axis, u0 at the equator:
+    U(x) = u0 (-y, x, 0) / |x|, for x of shape (3, N)."""
+    def U(x):
+        r = np.linalg.norm(x, axis=0)
+        r = np.where(r == 0, 1.0, r)
+        return u0 * np.stack([-x[1], x[0], np.zeros_like(x[0])]) / r
+    return U
+
+
+def edge_velocity(g: LevelGeom, U) -> np.ndarray:
+    """Velocity components of the tangent field U along every owned edge
+    (endpoint 1 -> endpoint 2 of end_pt, src/shared.f90:287-292) at the edge
+    midpoint, ghosts by the level's copy table; (3*NN,) in the C-ABI layout."""
+    NN = g.NN
+    E, N, NE = _neighbours(g)
+    sel = g.owned
+    ids = np.nonzero(sel)[0]
+    p = g.node
+    v = np.zeros(3 * NN)
+    for e, (a, b) in ((RT, (ids, E[sel])), (DG, (NE[sel], ids)), (UP, (ids, N[sel]))):
+        pa, pb = p[:, a], p[:, b]
+        m = pa + pb
+        m = m / np.linalg.norm(m, axis=0) * np.linalg.norm(pa, axis=0)
+        t = pb - pa
+        t = t / np.linalg.norm(t, axis=0)
+        v[e * NN + ids] = np.einsum("ij,ij->j", U(m), t)
+    halo_edges(g, v)
+    return v

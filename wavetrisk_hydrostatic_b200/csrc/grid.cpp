@@ -6,6 +6,7 @@
 #include "grid.hpp"
 
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <functional>
 #include <stdexcept>
@@ -575,6 +576,197 @@ void overlap_areas(Level& Pa, Level& L) {
       }
 }
 
+// ---- outer velocity interpolation weights I_u_wgt -------------------------
+// set_WT_wgts / outer_velo_weights (src/wavelet.f90:1567-1705) with the
+// helpers local_coord (:1500), coords_to_rowd (:1769), coord2local (:1749),
+// normalize2 (:1477), normalize_Coord and direction (src/sphere.f90:7,256).
+
+inline Coord normalize_coord(Coord c) {
+  const double nrm = std::sqrt(sq(c.x) + sq(c.y) + sq(c.z));
+  if (nrm >= eps()) return C(c.x / nrm, c.y / nrm, c.z / nrm);
+  return C(0.0, 0.0, 0.0);
+}
+inline Coord direction(Coord a, Coord b) { return normalize_coord(vector(a, b)); }
+
+struct Row6 { double v[6]; };
+inline Row6 operator-(const Row6& a, const Row6& b) {
+  Row6 r;
+  for (int k = 0; k < 6; ++k) r.v[k] = a.v[k] - b.v[k];
+  return r;
+}
+
+inline Row6 coords_to_rowd(Coord midpt, Coord dirvec, Coord x, Coord y) {
+  const double q0 = inner(dirvec, x), q1 = inner(dirvec, y);
+  const double nrm = std::sqrt(sq(q0) + sq(q1));
+  const double u = q0 / nrm, v = q1 / nrm;
+  const double x0 = inner(midpt, x), x1 = inner(midpt, y);
+  return Row6{{u, u * x0, u * x1, v, v * x0, v * x1}};
+}
+
+// Vendored DGESV path for a 6x6 system (src/dgesv.f90: DGETRF -> DGETF2 since
+// ILAENV's block size exceeds 6, then DGETRS), with the reference BLAS loops of
+// IDAMAX, DSWAP, DSCAL, DGER and DTRSM.  a is column-major: a[c*6 + r].  On a
+// singular factor b is left as DGESV leaves it (unsolved).
+bool dgesv6(double a[36], double b[6]) {
+  auto A = [&](int r, int c) -> double& { return a[c * 6 + r]; };
+  const double sfmin = std::numeric_limits<double>::min();  // DLAMCH('S')
+  int ipiv[6];
+  int info = 0;
+  for (int j = 0; j < 6; ++j) {
+    int jp = j;
+    double dmax = std::fabs(A(j, j));
+    for (int i = j + 1; i < 6; ++i)
+      if (std::fabs(A(i, j)) > dmax) { dmax = std::fabs(A(i, j)); jp = i; }
+    ipiv[j] = jp;
+    if (A(jp, j) != 0.0) {
+      if (jp != j)
+        for (int c = 0; c < 6; ++c) std::swap(A(j, c), A(jp, c));
+      if (j < 5) {
+        if (std::fabs(A(j, j)) >= sfmin) {
+          const double r = 1.0 / A(j, j);
+          for (int i = j + 1; i < 6; ++i) A(i, j) = r * A(i, j);
+        } else {
+          for (int i = j + 1; i < 6; ++i) A(i, j) = A(i, j) / A(j, j);
+        }
+      }
+    } else if (info == 0) {
+      info = j + 1;
+    }
+    if (j < 5)
+      for (int c = j + 1; c < 6; ++c)
+        if (A(j, c) != 0.0) {
+          const double temp = -1.0 * A(j, c);
+          for (int i = j + 1; i < 6; ++i) A(i, c) = A(i, c) + A(i, j) * temp;
+        }
+  }
+  if (info != 0) return false;
+  for (int i = 0; i < 6; ++i)
+    if (ipiv[i] != i) std::swap(b[i], b[ipiv[i]]);
+  for (int k = 0; k < 6; ++k)
+    if (b[k] != 0.0)
+      for (int i = k + 1; i < 6; ++i) b[i] = b[i] - b[k] * A(i, k);
+  for (int k = 5; k >= 0; --k)
+    if (b[k] != 0.0) {
+      b[k] = b[k] / A(k, k);
+      for (int i = 0; i < k; ++i) b[i] = b[i] - b[k] * A(i, k);
+    }
+  return true;
+}
+
+// Stencil tables of src/shared.f90:287-324 (0-based edge index, k = 0, 1).
+const int END_PT[3][2][2] = {{{0, 0}, {1, 0}}, {{1, 1}, {0, 0}}, {{0, 0}, {0, 1}}};
+const int OPP_NO[3][2][2] = {{{0, -1}, {1, 1}}, {{0, 1}, {1, 0}}, {{1, 1}, {-1, 0}}};
+const int HEX_SIDES[10][3] = {{0, 0, RT},  {0, 0, DG},   {0, 0, UP}, {-1, 0, RT}, {-1, -1, DG},
+                              {0, -1, UP}, {0, 0, RT},   {0, 0, DG}, {0, 0, UP},  {-1, 0, RT}};
+const int HEX_S_OFFS[3] = {2, 0, 4};
+const double IU_BASE[9] = {16.0 / 16.0, -1.0 / 16.0, 1.0 / 16.0, 1.0 / 16.0, -1.0 / 16.0,
+                           -1.0 / 16.0, -1.0 / 16.0, 1.0 / 16.0, 1.0 / 16.0};
+
+struct OuterWeights {
+  const Grid& g;
+  const Level& Pa;
+  int d;
+  Coord x, y;
+  int bad = 0;  // reads of undefined node coordinates
+
+  Coord node(int i, int j) {
+    if (!Pa.in(i, j) || !Pa.valid[Pa.id(d, i, j)]) { ++bad; return C(0.0, 0.0, 0.0); }
+    return Pa.node[Pa.id(d, i, j)];
+  }
+  // get_coord: the pentagon corners take the node the reference's boundary
+  // patches hold there (nidx of IMINUS/JMINUS/JPLUS/IPLUS/IJPLUS).
+  Coord get_coord(int i, int j, int e) {
+    const int n = Pa.n;
+    if (i == -1) {
+      if (j == -1 && g.penta[d][SOUTHWEST]) {
+        if (e == RT) return node(-1, 0);
+        if (e == UP) return node(0, -1);
+        ++bad;  // the reference returns an undefined value here; never reached
+        return C(0.0, 0.0, 0.0);
+      }
+      if (j == n && g.penta[d][NORTHWEST]) return node(0, n + 1);
+      return node(i, j);
+    }
+    if (i == n && j == -1 && g.penta[d][SOUTHEAST]) return node(n + 1, 0);
+    if (i == n + 1 && j == n + 1 && g.penta[d][NORTHEAST]) return node(n + 1, n);
+    return node(i, j);
+  }
+  Row6 row(int i0, int j0, const int* off1, const int* off2, int e00) {
+    const int i = i0 + off1[0] + off2[0], j = j0 + off1[1] + off2[1], e = off2[2];
+    const Coord p1 = get_coord(i + END_PT[e][0][0], j + END_PT[e][0][1], e00);
+    const Coord p2 = get_coord(i + END_PT[e][1][0], j + END_PT[e][1][1], e00);
+    return coords_to_rowd(mid_pt(p1, p2), vector(p1, p2), x, y);
+  }
+  // outer_velo_weights(dom, p, i0, j0, e0): 9 entries of I_u_wgt%enc.
+  void compute(int i0, int j0, int e0, double out[9]) {
+    const int n = Pa.n;
+    (void)n;
+    const Coord mid = Pa.midpt[(int64_t)e0 * Pa.NN + Pa.id(d, i0, j0)];
+    const Coord e1 = Pa.node[Pa.id(d, i0 + END_PT[e0][0][0], j0 + END_PT[e0][0][1])];
+    const Coord e2 = Pa.node[Pa.id(d, i0 + END_PT[e0][1][0], j0 + END_PT[e0][1][1])];
+    x = direction(e1, e2);
+    y = normalize_coord(cross(x, mid));
+    double w[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const int hs = HEX_S_OFFS[e0];
+    const int zero2[2] = {0, 0};
+    const int self3[3] = {0, 0, e0};
+    for (int k = 1; k <= 2; ++k) {
+      const int* ep_k = END_PT[e0][k - 1];
+      const int* ep_o = END_PT[e0][2 - k];  // end_pt(:, -k+3)
+      const int* op_k = OPP_NO[e0][k - 1];
+      const int s = 3 * k - 3;
+      Row6 G[6];
+      G[0] = row(i0, j0, zero2, self3, e0);
+      G[1] = row(i0, j0, ep_o, HEX_SIDES[hs + 2 + s], e0);
+      G[2] = row(i0, j0, ep_k, HEX_SIDES[(hs + 3) - s], e0);
+      G[3] = row(i0, j0, op_k, HEX_SIDES[hs + 1 + s], e0) - row(i0, j0, ep_k, HEX_SIDES[hs + 2 + s], e0);
+      G[4] = row(i0, j0, ep_o, HEX_SIDES[(hs + 3) - s], e0) - row(i0, j0, op_k, HEX_SIDES[(hs + 4) - s], e0);
+      G[5] = row(i0, j0, ep_k, HEX_SIDES[(hs + 5) - s], e0) - row(i0, j0, ep_o, HEX_SIDES[hs + 0 + s], e0);
+      double a[36];
+      for (int c = 0; c < 6; ++c)
+        for (int r = 0; r < 6; ++r) a[c * 6 + r] = G[c].v[r];
+      const Coord n1 = Pa.node[Pa.id(d, i0 + END_PT[e0][0][0], j0 + END_PT[e0][0][1])];
+      const Coord n2 = Pa.node[Pa.id(d, i0 + END_PT[e0][1][0], j0 + END_PT[e0][1][1])];
+      Row6 bb = coords_to_rowd(mid_pt(mid, n2), vector(n1, n2), x, y);
+      double b[6];
+      for (int r = 0; r < 6; ++r) b[r] = bb.v[r];
+      dgesv6(a, b);
+      w[0] = w[0] + b[0];
+      w[2 * k - 1] = w[2 * k - 1] + b[1];
+      w[2 * k] = w[2 * k] + b[2];
+      w[2 * k + 3] = b[3];
+      w[2 * k + 4] = b[4];
+      w[-2 * k + 5] = w[-2 * k + 5] + b[5];
+      w[-2 * k + 6] = w[-2 * k + 6] - b[5];
+    }
+    for (int q = 0; q < 9; ++q) out[q] = 0.5 * w[q] - IU_BASE[q];
+  }
+};
+
+// set_WT_wgts over the parents [0, n_par)^2 of every lozenge
+// (apply_interscale_to_patch3(..., 0, 0) in refine_patch2): RT weights at the
+// child (2i+1, 2j), DG at (2i, 2j), UP at (2i, 2j+1).  Other nodes, ghosts
+// included, keep zero weights, as in the reference's extend(I_u_wgt, 0).
+void velo_weights(const Grid& g, const Level& Pa, Level& L) {
+  L.iu_wgt.assign((size_t)9 * L.NN, 0.0);
+  int bad = 0;
+  for (int d = 0; d < N_LOZ; ++d) {
+    OuterWeights W{g, Pa, d, C(0, 0, 0), C(0, 0, 0)};
+    for (int jp = 0; jp < Pa.n; ++jp)
+      for (int ip = 0; ip < Pa.n; ++ip) {
+        const int tgt[3][2] = {{2 * ip + 1, 2 * jp}, {2 * ip, 2 * jp}, {2 * ip, 2 * jp + 1}};
+        for (int e = 0; e < 3; ++e) {
+          double w[9];
+          W.compute(ip, jp, e, w);
+          const int64_t id = L.id(d, tgt[e][0], tgt[e][1]);
+          for (int q = 0; q < 9; ++q) L.iu_wgt[(int64_t)q * L.NN + id] = w[q];
+        }
+      }
+    bad += W.bad;
+  }
+  if (bad) std::fprintf(stderr, "wtg: %d undefined node reads in velocity weights (level %d)\n", bad, L.l);
+}
+
 // comm_nodes9(get_areas, set_areas) + area_post_comm (src/refine_patch.f90:436-486)
 void comm_areas(const Grid& g, Level& L) {
   for (auto& h : L.halo_node) {
@@ -619,7 +811,10 @@ void build_grid(Grid& g, int min_level, int max_level, int domain_level, double 
       coords_child(g, g.at(l - 1), L);
     }
     geometry(g, L);
-    if (l > min_level - 1) overlap_areas(g.at(l - 1), L);
+    if (l > min_level - 1) {
+      overlap_areas(g.at(l - 1), L);
+      velo_weights(g, g.at(l - 1), L);
+    }
     comm_areas(g, L);
   }
   // Strip the temporary sign encoding of node entries (kept only for the area swap).

@@ -41,6 +41,7 @@ struct Level {
   std::vector<double> triarea, coriolis;  // [2*NN]
   std::vector<double> overl_a;            // [4*NN]  Overl_Area%a
   std::vector<double> overl_split;        // [2*NN]  Overl_Area%split
+  std::vector<double> iu_wgt;             // [9*NN]  I_u_wgt%enc (k at k*NN + node); levels > min_level-1
   std::vector<uint8_t> valid;             // [NN] 1 where node coordinates are defined
   std::vector<HaloNode> halo_node;
   std::vector<HaloEdge> halo_edge;

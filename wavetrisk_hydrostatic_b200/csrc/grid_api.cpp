@@ -69,6 +69,10 @@ int wt_grid_copy(const wt_grid* gh, int level, const char* name, void* dst) {
   else if (!std::strcmp(name, "coriolis")) cp(L.coriolis);
   else if (!std::strcmp(name, "overl_a")) cp(L.overl_a);
   else if (!std::strcmp(name, "overl_split")) cp(L.overl_split);
+  else if (!std::strcmp(name, "iu_wgt")) {
+    if (L.iu_wgt.empty()) return WT_ERR_ARG;
+    cp(L.iu_wgt);
+  }
   else if (!std::strcmp(name, "halo_node")) {
     int64_t* o = static_cast<int64_t*>(dst);
     for (size_t k = 0; k < L.halo_node.size(); ++k) { o[2 * k] = L.halo_node[k].dst; o[2 * k + 1] = L.halo_node[k].src; }

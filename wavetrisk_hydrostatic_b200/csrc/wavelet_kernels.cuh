@@ -1,0 +1,452 @@
+// Wavelet transform kernels for the prognostic variables (layer mass,
+// potential temperature, velocity) on a uniform hierarchy of padded lozenge
+// levels, the threshold mask and compression.
+//
+// Each kernel is one interscale (parent level l, child level l+1) or onescale
+// pass of the reference's drivers (src/wavelet.f90, src/adapt.f90,
+// src/mask.f90), one thread per (layer, lozenge, node) of the pass's range.
+// Ghost values are read through the level's remap tables (the node or signed
+// edge that update_bdry copies there); masks and weights are read as stored.
+// Floating point keeps the reference's operand order (compiled with
+// --fmad=false).
+#pragma once
+#include <cstdint>
+
+namespace wtw {
+
+enum { RT = 0, DG = 1, UP = 2 };
+enum { LORT = 0, UPLT = 1 };
+constexpr int FROZEN = 32, TOLRNZ = 16, ADJZONE = 8, ZERO = 0;
+
+// One level of the hierarchy on the device.
+struct WLev {
+  int n, P, NN;
+  const double* __restrict__ len;   // 3*NN
+  const double* __restrict__ tri;   // 2*NN
+  const double* __restrict__ hinv;  // NN
+  const double* __restrict__ oa;    // 4*NN overlap areas
+  const double* __restrict__ iu;    // 9*NN outer velocity weights (null on the coarsest level)
+  const int* __restrict__ nsrc;     // node remap
+  const int* __restrict__ esrc;     // signed edge remap
+  int* mask_n;                      // NN
+  int* mask_e;                      // 3*NN
+  double *sm, *st, *sv;             // scaling: [nz][NN], [nz][NN], [nz][3*NN]
+  double *wm, *wt, *wv;             // wavelets, same shapes
+};
+
+__constant__ int c_end_pt[3][2][2] = {{{0, 0}, {1, 0}}, {{1, 1}, {0, 0}}, {{0, 0}, {0, 1}}};
+__constant__ int c_opp_no[3][2][2] = {{{0, -1}, {1, 1}}, {{0, 1}, {1, 0}}, {{1, 1}, {-1, 0}}};
+__constant__ int c_hex_sides[10][3] = {{0, 0, RT},  {0, 0, DG}, {0, 0, UP}, {-1, 0, RT}, {-1, -1, DG},
+                                       {0, -1, UP}, {0, 0, RT}, {0, 0, DG}, {0, 0, UP},  {-1, 0, RT}};
+__constant__ int c_hex_s_offs[3] = {2, 0, 4};
+// Iu_Base_Wgt (src/wavelet.f90:1764)
+__constant__ double c_iu_base[9] = {16.0 / 16.0, -1.0 / 16.0, 1.0 / 16.0, 1.0 / 16.0, -1.0 / 16.0,
+                                    -1.0 / 16.0, -1.0 / 16.0, 1.0 / 16.0, 1.0 / 16.0};
+
+__device__ __forceinline__ int nid(const WLev& L, int d, int i, int j) { return (d * L.P + j + 2) * L.P + i + 2; }
+__device__ __forceinline__ bool inr(const WLev& L, int i, int j) {
+  return i >= -2 && j >= -2 && i < L.n + 2 && j < L.n + 2;
+}
+// node field (one layer) through the ghost remap; 0 outside the padded array
+__device__ __forceinline__ double rn(const WLev& L, const double* __restrict__ f, int d, int i, int j) {
+  if (!inr(L, i, j)) return 0.0;
+  return f[__ldg(L.nsrc + nid(L, d, i, j))];
+}
+// edge field (one layer, planes of NN) through the signed ghost remap
+__device__ __forceinline__ double re(const WLev& L, const double* __restrict__ f, int e, int d, int i, int j) {
+  if (!inr(L, i, j)) return 0.0;
+  const int c = __ldg(L.esrc + e * L.NN + nid(L, d, i, j));
+  const double v = f[c >> 1];
+  return (c & 1) ? -v : v;
+}
+__device__ __forceinline__ double oa(const WLev& L, int d, int i, int j, int k) {
+  return inr(L, i, j) ? L.oa[(k - 1) * L.NN + nid(L, d, i, j)] : 0.0;
+}
+__device__ __forceinline__ double hv(const WLev& L, int d, int i, int j) {
+  return inr(L, i, j) ? L.hinv[nid(L, d, i, j)] : 0.0;
+}
+__device__ __forceinline__ double ln(const WLev& L, int e, int d, int i, int j) {
+  return inr(L, i, j) ? L.len[e * L.NN + nid(L, d, i, j)] : 0.0;
+}
+__device__ __forceinline__ double ta(const WLev& L, int t, int d, int i, int j) {
+  return inr(L, i, j) ? L.tri[t * L.NN + nid(L, d, i, j)] : 0.0;
+}
+__device__ __forceinline__ double iw(const WLev& L, int q, int d, int i, int j) {
+  return (L.iu && inr(L, i, j)) ? L.iu[q * L.NN + nid(L, d, i, j)] : 0.0;
+}
+__device__ __forceinline__ int mn(const WLev& L, int d, int i, int j) {
+  return inr(L, i, j) ? L.mask_n[nid(L, d, i, j)] : ZERO;
+}
+__device__ __forceinline__ int me(const WLev& L, int e, int d, int i, int j) {
+  return inr(L, i, j) ? L.mask_e[e * L.NN + nid(L, d, i, j)] : ZERO;
+}
+
+// Thread -> (layer k, lozenge d, i, j) over [0, m)^2, layer fastest across blocks.
+__device__ __forceinline__ bool decode(int nz, int m, int& k, int& d, int& i, int& j) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t per = (int64_t)10 * m * m;
+  if (t >= per * nz) return false;
+  k = (int)(t / per);
+  int r = (int)(t - (int64_t)k * per);
+  d = r / (m * m);
+  r -= d * m * m;
+  j = r / m;
+  i = r - j * m;
+  return true;
+}
+
+// Interp_node (src/wavelet.f90:1487-1498)
+__device__ __forceinline__ double interp_node(const WLev& C, const double* s, int d, int i, int j, int i1, int j1,
+                                              int i2, int j2, int i3, int j3, int i4, int j4) {
+  return (oa(C, d, i, j, 1) * rn(C, s, d, i1, j1) + oa(C, d, i, j, 2) * rn(C, s, d, i2, j2) +
+          oa(C, d, i, j, 3) * rn(C, s, d, i3, j3) + oa(C, d, i, j, 4) * rn(C, s, d, i4, j4)) *
+         hv(C, d, i, j);
+}
+
+// Compute_scalar_wavelets (src/wavelet.f90:642-670), parents [0, np)^2, both scalars.
+__global__ void k_scalar_wc(WLev C, int np, int nz) {
+  int k, d, ip, jp;
+  if (!decode(nz, np, k, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  for (int v = 0; v < 2; ++v) {
+    const double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+    double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+    if (mn(C, d, i + 1, j) >= ADJZONE)
+      wc[nid(C, d, i + 1, j)] = rn(C, s, d, i + 1, j) - interp_node(C, s, d, i + 1, j, i, j, i + 2, j, i + 2, j + 2, i, j - 2);
+    if (mn(C, d, i + 1, j + 1) >= ADJZONE)
+      wc[nid(C, d, i + 1, j + 1)] =
+          rn(C, s, d, i + 1, j + 1) - interp_node(C, s, d, i + 1, j + 1, i + 2, j + 2, i, j, i + 2, j, i, j + 2);
+    if (mn(C, d, i, j + 1) >= ADJZONE)
+      wc[nid(C, d, i, j + 1)] = rn(C, s, d, i, j + 1) - interp_node(C, s, d, i, j + 1, i, j, i, j + 2, i - 2, j, i + 2, j + 2);
+  }
+}
+
+// Restrict_scalar (parents [0, np]^2, src/wavelet.f90:520-569) and
+// Restrict_velo (parents [0, np)^2, :1154-1174).
+__global__ void k_restrict(WLev Pa, WLev C, int nz) {
+  const int np = Pa.n;
+  int k, d, ip, jp;
+  if (!decode(nz, np + 1, k, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  if (mn(C, d, i, j) != 0) {
+    for (int v = 0; v < 2; ++v) {
+      const double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+      const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+      double* sp = (v == 0 ? Pa.sm : Pa.st) + (int64_t)k * Pa.NN;
+      const double sum =
+          rn(C, wc, d, i + 1, j) * oa(C, d, i + 1, j, 1) + rn(C, wc, d, i + 1, j + 1) * oa(C, d, i + 1, j + 1, 2) +
+          rn(C, wc, d, i + 2, j + 1) * oa(C, d, i + 2, j + 1, 3) + rn(C, wc, d, i + 1, j + 2) * oa(C, d, i + 1, j + 2, 4) +
+          rn(C, wc, d, i, j + 1) * oa(C, d, i, j + 1, 1) + rn(C, wc, d, i - 1, j) * oa(C, d, i - 1, j, 2) +
+          rn(C, wc, d, i - 1, j + 1) * oa(C, d, i - 1, j + 1, 3) + rn(C, wc, d, i - 2, j - 1) * oa(C, d, i - 2, j - 1, 4) +
+          rn(C, wc, d, i - 1, j - 1) * oa(C, d, i - 1, j - 1, 1) + rn(C, wc, d, i, j - 1) * oa(C, d, i, j - 1, 2) +
+          rn(C, wc, d, i - 1, j - 2) * oa(C, d, i - 1, j - 2, 3) + rn(C, wc, d, i + 1, j - 1) * oa(C, d, i + 1, j - 1, 4);
+      sp[nid(Pa, d, ip, jp)] = rn(C, s, d, i, j) + sum * hv(Pa, d, ip, jp);
+    }
+  }
+  if (ip < np && jp < np) {
+    const double* v = C.sv + (int64_t)k * 3 * C.NN;
+    double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+    const int x = nid(Pa, d, ip, jp);
+    if (me(C, RT, d, i, j) > 0) vp[RT * Pa.NN + x] = 0.5 * (re(C, v, RT, d, i, j) + re(C, v, RT, d, i + 1, j));
+    if (me(C, DG, d, i, j) > 0) vp[DG * Pa.NN + x] = 0.5 * (re(C, v, DG, d, i + 1, j + 1) + re(C, v, DG, d, i, j));
+    if (me(C, UP, d, i, j) > 0) vp[UP * Pa.NN + x] = 0.5 * (re(C, v, UP, d, i, j) + re(C, v, UP, d, i, j + 1));
+  }
+}
+
+// Interp_outer_velo (src/wavelet.f90:1064-1094): child weights at (ic, jc).
+__device__ double interp_outer(const WLev& Pa, const WLev& C, const double* vp, int d, int ip, int jp, int ic, int jc,
+                               int e) {
+  const int hs = c_hex_s_offs[e];
+  auto ved = [&](const int* off, int col) {
+    return re(Pa, vp, c_hex_sides[col][2], d, ip + off[0] + c_hex_sides[col][0], jp + off[1] + c_hex_sides[col][1]);
+  };
+  const int* e1 = c_end_pt[e][0];
+  const int* e2 = c_end_pt[e][1];
+  const int* o1 = c_opp_no[e][0];
+  const int* o2 = c_opp_no[e][1];
+  double t[9];
+  t[0] = re(Pa, vp, e, d, ip, jp);
+  t[1] = ved(e2, hs + 2);
+  t[2] = ved(e1, hs + 3);
+  t[3] = ved(e1, hs + 5);
+  t[4] = ved(e2, hs + 0);
+  t[5] = ved(o1, hs + 1) - ved(e1, hs + 2);
+  t[6] = ved(e2, hs + 3) - ved(o1, hs + 4);
+  t[7] = ved(o2, hs + 4) - ved(e2, hs + 5);
+  t[8] = ved(e1, hs + 0) - ved(o2, hs + 1);
+  double sum = 0.0;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) sum = sum + (c_iu_base[q] + iw(C, q, d, ic, jc)) * t[q];
+  return sum;
+}
+
+// Interp_inner_velo (src/wavelet.f90:1005-1062)
+__device__ void interp_inner(const WLev& Pa, const WLev& C, const double* vp, const double* v, int d, int ip, int jp,
+                             double u[6]) {
+  double curl[2];
+#pragma unroll
+  for (int t = LORT; t <= UPLT; ++t) {
+    const int i1 = ip - t + 1, j1 = jp, i2 = ip, j2 = jp + t;
+    curl[t] = (re(Pa, vp, DG, d, ip, jp) * ln(Pa, DG, d, ip, jp) + re(Pa, vp, UP, d, i1, j1) * ln(Pa, UP, d, i1, j1) +
+               re(Pa, vp, RT, d, i2, j2) * ln(Pa, RT, d, i2, j2)) /
+              ta(Pa, t, d, ip, jp);
+  }
+  const int i = 2 * ip, j = 2 * jp;
+  auto pr = [&](int e, int a, int b) { return re(C, v, e, d, a, b) * ln(C, e, d, a, b); };
+  u[0] = (ta(C, LORT, d, i, j) * curl[LORT] - pr(RT, i, j) - pr(DG, i, j)) / ln(C, UP, d, i + 1, j);
+  u[1] = (ta(C, LORT, d, i + 1, j) * curl[LORT] - pr(RT, i + 1, j) - pr(UP, i + 2, j)) / ln(C, DG, d, i + 1, j);
+  u[2] = (ta(C, LORT, d, i + 1, j + 1) * curl[LORT] - pr(DG, i + 1, j + 1) - pr(UP, i + 2, j + 1)) /
+         ln(C, RT, d, i + 1, j + 1);
+  u[3] = (ta(C, UPLT, d, i, j) * curl[UPLT] - pr(UP, i, j) - pr(DG, i, j)) / ln(C, RT, d, i, j + 1);
+  u[4] = (ta(C, UPLT, d, i, j + 1) * curl[UPLT] - pr(UP, i, j + 1) - pr(RT, i, j + 2)) / ln(C, DG, d, i, j + 1);
+  u[5] = (ta(C, UPLT, d, i + 1, j + 1) * curl[UPLT] - pr(DG, i + 1, j + 1) - pr(RT, i + 1, j + 2)) /
+         ln(C, UP, d, i + 1, j + 1);
+}
+
+__device__ __forceinline__ double& ee(const WLev& L, double* f, int e, int d, int i, int j) {
+  return f[e * L.NN + nid(L, d, i, j)];
+}
+
+// Compute_velo_wavelets (src/wavelet.f90:672-710), parents [0, np)^2.
+__global__ void k_velo_wc(WLev Pa, WLev C, int nz) {
+  int k, d, ip, jp;
+  if (!decode(nz, Pa.n, k, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+  const double* v = C.sv + (int64_t)k * 3 * C.NN;
+  double* wc = C.wv + (int64_t)k * 3 * C.NN;
+  for (int e = 0; e < 3; ++e) {
+    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
+    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
+    if (me(C, e, d, a2, b2) < ADJZONE) continue;
+    const double u = interp_outer(Pa, C, vp, d, ip, jp, a2, b2, e);
+    const double w = re(C, v, e, d, a2, b2) - u;
+    ee(C, wc, e, d, a2, b2) = w;
+    ee(C, wc, e, d, a1, b1) = -w;
+  }
+  double u[6];
+  interp_inner(Pa, C, vp, v, d, ip, jp, u);
+  if (me(C, UP, d, i + 1, j) >= ADJZONE) ee(C, wc, UP, d, i + 1, j) = re(C, v, UP, d, i + 1, j) - u[0];
+  if (me(C, DG, d, i + 1, j) >= ADJZONE) ee(C, wc, DG, d, i + 1, j) = re(C, v, DG, d, i + 1, j) - u[1];
+  if (me(C, RT, d, i + 1, j + 1) >= ADJZONE) ee(C, wc, RT, d, i + 1, j + 1) = re(C, v, RT, d, i + 1, j + 1) - u[2];
+  if (me(C, RT, d, i, j + 1) >= ADJZONE) ee(C, wc, RT, d, i, j + 1) = re(C, v, RT, d, i, j + 1) - u[3];
+  if (me(C, DG, d, i, j + 1) >= ADJZONE) ee(C, wc, DG, d, i, j + 1) = re(C, v, DG, d, i, j + 1) - u[4];
+  if (me(C, UP, d, i + 1, j + 1) >= ADJZONE) ee(C, wc, UP, d, i + 1, j + 1) = re(C, v, UP, d, i + 1, j + 1) - u[5];
+}
+
+// velo_interp_penta_corr (src/wavelet.f90:927-952) at the south-west corner.
+__device__ void penta_corr(const WLev& Pa, const WLev& C, const double* vp, int d, double u[2]) {
+  u[0] = (c_iu_base[8] + iw(C, 8, d, 0, 1)) *
+         ((-re(Pa, vp, UP, d, 0, -1) - (-re(Pa, vp, RT, d, -1, -1))) - (re(Pa, vp, DG, d, -1, -1) - re(Pa, vp, UP, d, -1, -1)));
+  u[1] = (c_iu_base[5] + iw(C, 5, d, 1, 0)) *
+         (re(Pa, vp, RT, d, -1, -1) + re(Pa, vp, RT, d, -1, 0) - (re(Pa, vp, RT, d, -1, -1) - re(Pa, vp, DG, d, -1, -1)));
+}
+
+// Pentagon corrections at the lozenge corners, in the reference's corner
+// order (NE, SE, SW, NW), one thread per (layer, lozenge):
+// reconstruct == 0: Compute_velo_wavelets_penta on the wavelets
+// (src/wavelet.f90:712-781); reconstruct == 1: Reconstruct_velo_penta on the
+// child velocity (:1096-1152).
+__global__ void k_velo_penta(WLev Pa, WLev C, int nz, int reconstruct) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * nz) return;
+  const int k = t / 10, d = t - 10 * k;
+  const int np = Pa.n, nc = C.n;
+  const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+  if (!reconstruct) {
+    double* wc = C.wv + (int64_t)k * 3 * C.NN;
+    {  // SE
+      const double vv = (c_iu_base[6] + iw(C, 6, d, nc - 1, 0)) * (re(Pa, vp, RT, d, np, 0) + re(Pa, vp, UP, d, np, -1));
+      if (me(C, RT, d, nc - 2, 0) >= ADJZONE) {
+        ee(C, wc, RT, d, nc - 2, 0) = ee(C, wc, RT, d, nc - 2, 0) - vv;
+        ee(C, wc, RT, d, nc - 1, 0) = ee(C, wc, RT, d, nc - 1, 0) + vv;
+      }
+    }
+    {  // SW
+      double u[2];
+      penta_corr(Pa, C, vp, d, u);
+      if (me(C, UP, d, 0, 0) >= ADJZONE) {
+        ee(C, wc, UP, d, 0, 0) = ee(C, wc, UP, d, 0, 0) + u[0];
+        ee(C, wc, UP, d, 0, 1) = ee(C, wc, UP, d, 0, 1) - u[0];
+      }
+      if (me(C, RT, d, 0, 0) >= ADJZONE) {
+        ee(C, wc, RT, d, 0, 0) = ee(C, wc, RT, d, 0, 0) + u[1];
+        ee(C, wc, RT, d, 1, 0) = ee(C, wc, RT, d, 1, 0) - u[1];
+      }
+    }
+    {  // NW
+      const double vv = -(c_iu_base[7] + iw(C, 7, d, 0, nc - 1)) * (re(Pa, vp, UP, d, 0, np) + re(Pa, vp, RT, d, -1, np));
+      if (me(C, UP, d, 0, nc - 2) >= ADJZONE) {
+        ee(C, wc, UP, d, 0, nc - 2) = ee(C, wc, UP, d, 0, nc - 2) - vv;
+        ee(C, wc, UP, d, 0, nc - 1) = ee(C, wc, UP, d, 0, nc - 1) + vv;
+      }
+    }
+  } else {
+    double* v = C.sv + (int64_t)k * 3 * C.NN;
+    {  // SE
+      const double vv = -(c_iu_base[6] + iw(C, 6, d, nc - 1, 0)) * (re(Pa, vp, RT, d, np, 0) + re(Pa, vp, UP, d, np, -1));
+      ee(C, v, RT, d, nc - 2, 0) = ee(C, v, RT, d, nc - 2, 0) - vv;
+      ee(C, v, RT, d, nc - 1, 0) = ee(C, v, RT, d, nc - 1, 0) + vv;
+    }
+    {  // SW
+      double u[2];
+      penta_corr(Pa, C, vp, d, u);
+      ee(C, v, UP, d, 0, 0) = ee(C, v, UP, d, 0, 0) - u[0];
+      ee(C, v, UP, d, 0, 1) = ee(C, v, UP, d, 0, 1) + u[0];
+      ee(C, v, RT, d, 0, 0) = ee(C, v, RT, d, 0, 0) - u[1];
+      ee(C, v, RT, d, 1, 0) = ee(C, v, RT, d, 1, 0) + u[1];
+    }
+    {  // NW
+      const double vv = (c_iu_base[7] + iw(C, 7, d, 0, nc - 1)) * (re(Pa, vp, UP, d, 0, np) + re(Pa, vp, RT, d, -1, np));
+      ee(C, v, UP, d, 0, nc - 2) = ee(C, v, UP, d, 0, nc - 2) - vv;
+      ee(C, v, UP, d, 0, nc - 1) = ee(C, v, UP, d, 0, nc - 1) + vv;
+    }
+  }
+}
+
+// Prolong_scalar (src/wavelet.f90:571-612), parents [0, np]^2: eleven of the
+// twelve lifting terms, as the reference sums them.
+__global__ void k_prolong(WLev Pa, WLev C, int nz) {
+  const int np = Pa.n;
+  int k, d, ip, jp;
+  if (!decode(nz, np + 1, k, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  if (mn(C, d, i, j) == FROZEN) return;
+  for (int v = 0; v < 2; ++v) {
+    const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+    const double* sp = (v == 0 ? Pa.sm : Pa.st) + (int64_t)k * Pa.NN;
+    double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+    const double sum =
+        rn(C, wc, d, i + 1, j) * oa(C, d, i + 1, j, 1) + rn(C, wc, d, i + 1, j + 1) * oa(C, d, i + 1, j + 1, 2) +
+        rn(C, wc, d, i + 2, j + 1) * oa(C, d, i + 2, j + 1, 3) + rn(C, wc, d, i, j + 1) * oa(C, d, i, j + 1, 1) +
+        rn(C, wc, d, i - 1, j) * oa(C, d, i - 1, j, 2) + rn(C, wc, d, i - 1, j + 1) * oa(C, d, i - 1, j + 1, 3) +
+        rn(C, wc, d, i - 2, j - 1) * oa(C, d, i - 2, j - 1, 4) + rn(C, wc, d, i - 1, j - 1) * oa(C, d, i - 1, j - 1, 1) +
+        rn(C, wc, d, i, j - 1) * oa(C, d, i, j - 1, 2) + rn(C, wc, d, i - 1, j - 2) * oa(C, d, i - 1, j - 2, 3) +
+        rn(C, wc, d, i + 1, j - 1) * oa(C, d, i + 1, j - 1, 4);
+    s[nid(C, d, i, j)] = rn(Pa, sp, d, ip, jp) - sum * hv(Pa, d, ip, jp);
+  }
+}
+
+// Reconstruct_outer_velo (src/wavelet.f90:954-976), parents [0, np]^2.
+__global__ void k_recon_outer(WLev Pa, WLev C, int nz) {
+  int k, d, ip, jp;
+  if (!decode(nz, Pa.n + 1, k, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+  const double* wc = C.wv + (int64_t)k * 3 * C.NN;
+  double* v = C.sv + (int64_t)k * 3 * C.NN;
+  for (int e = 0; e < 3; ++e) {
+    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
+    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
+    const double u = interp_outer(Pa, C, vp, d, ip, jp, a2, b2, e);
+    const double v2 = u + re(C, wc, e, d, a2, b2);
+    ee(C, v, e, d, a2, b2) = v2;
+    ee(C, v, e, d, a1, b1) = 2.0 * re(Pa, vp, e, d, ip, jp) - v2;
+  }
+}
+
+// Reconstruct_scalar (src/wavelet.f90:614-640), parents [0, np)^2.
+__global__ void k_recon_scalar(WLev C, int np, int nz) {
+  int k, d, ip, jp;
+  if (!decode(nz, np, k, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  for (int v = 0; v < 2; ++v) {
+    const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+    double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+    const double a = interp_node(C, s, d, i + 1, j, i, j, i + 2, j, i + 2, j + 2, i, j - 2) + rn(C, wc, d, i + 1, j);
+    const double b = interp_node(C, s, d, i + 1, j + 1, i + 2, j + 2, i, j, i + 2, j, i, j + 2) + rn(C, wc, d, i + 1, j + 1);
+    const double c = interp_node(C, s, d, i, j + 1, i, j, i, j + 2, i - 2, j, i + 2, j + 2) + rn(C, wc, d, i, j + 1);
+    s[nid(C, d, i + 1, j)] = a;
+    s[nid(C, d, i + 1, j + 1)] = b;
+    s[nid(C, d, i, j + 1)] = c;
+  }
+}
+
+// Reconstruct_inner_velo (src/wavelet.f90:978-1003), parents [0, np)^2.
+__global__ void k_recon_inner(WLev Pa, WLev C, int nz) {
+  int k, d, ip, jp;
+  if (!decode(nz, Pa.n, k, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+  const double* wc = C.wv + (int64_t)k * 3 * C.NN;
+  double* v = C.sv + (int64_t)k * 3 * C.NN;
+  double u[6];
+  interp_inner(Pa, C, vp, v, d, ip, jp, u);
+  ee(C, v, UP, d, i + 1, j) = u[0] + re(C, wc, UP, d, i + 1, j);
+  ee(C, v, DG, d, i + 1, j) = u[1] + re(C, wc, DG, d, i + 1, j);
+  ee(C, v, RT, d, i + 1, j + 1) = u[2] + re(C, wc, RT, d, i + 1, j + 1);
+  ee(C, v, RT, d, i, j + 1) = u[3] + re(C, wc, RT, d, i, j + 1);
+  ee(C, v, DG, d, i, j + 1) = u[4] + re(C, wc, DG, d, i, j + 1);
+  ee(C, v, UP, d, i + 1, j + 1) = u[5] + re(C, wc, UP, d, i + 1, j + 1);
+}
+
+// mask_tol_vars (src/mask.f90:102-156) on nodes [st, n-1+en]^2 of one level,
+// all layers per thread.  thr[v*nz + k]: v = 0 mass, 1 Theta, 2 velocity.
+__global__ void k_mask_tol(WLev L, int nz, int st, int en, const double* __restrict__ thr, int below_fill) {
+  const int m = L.n + en - st;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)10 * m * m) return;
+  const int d = (int)(t / ((int64_t)m * m));
+  int r = (int)(t - (int64_t)d * m * m);
+  const int j = r / m + st, i = r % m + st;
+  if (!inr(L, i, j)) return;
+  const int x = nid(L, d, i, j);
+  if (L.mask_n[x] == FROZEN) return;
+  bool active = false;
+  for (int k = 0; k < nz; ++k) {
+    const double wm = rn(L, L.wm + (int64_t)k * L.NN, d, i, j), wt = rn(L, L.wt + (int64_t)k * L.NN, d, i, j);
+    if (fabs(wm) >= thr[0 * nz + k] || below_fill) active = true;
+    if (fabs(wt) >= thr[1 * nz + k] || below_fill) active = true;
+  }
+  if (active)
+    L.mask_n[x] = TOLRNZ;
+  else if (L.mask_n[x] > ADJZONE)
+    L.mask_n[x] = ADJZONE;
+  for (int e = 0; e < 3; ++e) {
+    active = false;
+    for (int k = 0; k < nz; ++k)
+      if (fabs(re(L, L.wv + (int64_t)k * 3 * L.NN, e, d, i, j)) >= thr[2 * nz + k] || below_fill) active = true;
+    int& me_ = L.mask_e[e * L.NN + x];
+    if (active)
+      me_ = TOLRNZ;
+    else if (me_ > ADJZONE)
+      me_ = ADJZONE;
+  }
+}
+
+// compress_scalar on nodes [0, n]^2 and compress_vector on [0, n)^2
+// (src/adapt.f90:79-232) of one level, one thread per (layer, node).
+__global__ void k_compress(WLev L, int nz) {
+  int k, d, i, j;
+  if (!decode(nz, L.n + 1, k, d, i, j)) return;
+  const int x = nid(L, d, i, j);
+  if (L.mask_n[x] < ADJZONE) {
+    L.wm[(int64_t)k * L.NN + x] = 0.0;
+    L.wt[(int64_t)k * L.NN + x] = 0.0;
+  }
+  if (i < L.n && j < L.n)
+    for (int e = 0; e < 3; ++e)
+      if (L.mask_e[e * L.NN + x] < ADJZONE) L.wv[(int64_t)k * 3 * L.NN + e * L.NN + x] = 0.0;
+}
+
+// Ghost copy of one level's layered node and edge fields (for host downloads).
+__global__ void k_halo_level(int nz, int NN, const int2* __restrict__ hn, int n_hn, const int3* __restrict__ he, int n_he,
+                             double* a, double* b, double* v) {
+  const int per = 2 * n_hn + n_he;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)per * nz) return;
+  const int k = (int)(t / per);
+  const int r = (int)(t - (int64_t)k * per);
+  if (r < 2 * n_hn) {
+    const int2 e = hn[r % n_hn];
+    double* f = (r < n_hn ? a : b) + (int64_t)k * NN;
+    f[e.x] = f[e.y];
+  } else {
+    const int3 e = he[r - 2 * n_hn];
+    double* f = v + (int64_t)k * 3 * NN;
+    const double x = f[e.y];
+    f[e.x] = e.z < 0 ? -x : x;
+  }
+}
+
+}  // namespace wtw

@@ -128,6 +128,7 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
     if ((rc = dev_copy(&D.coriolis, ld.coriolis, 2 * NN))) break;
     if ((rc = dev_copy(&D.overl_a, ld.overl_a, 4 * NN))) break;
     if ((rc = dev_copy(&D.topo, ld.topo, NN))) break;
+    if (ld.iu_wgt && (rc = dev_copy(&D.iu_wgt, ld.iu_wgt, 9 * NN))) break;
     std::vector<int2> hn(ld.n_halo_node);
     for (int64_t k = 0; k < ld.n_halo_node; ++k) {
       int64_t a = ld.halo_node[2 * k], b = ld.halo_node[2 * k + 1];

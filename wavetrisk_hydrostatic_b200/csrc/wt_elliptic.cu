@@ -105,6 +105,7 @@ static void ell_free(Ell* E) {
 void wt_handle::release_extra() {
   if (ell) ell_free(static_cast<Ell*>(ell));
   ell = nullptr;
+  wt_wavelet_release(this);
 }
 
 extern "C" int wt_elliptic_setup(wt_handle* h, double dt, double theta1, double theta2, int domain_level) {

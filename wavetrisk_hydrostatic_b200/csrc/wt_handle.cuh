@@ -12,6 +12,7 @@ struct DevLevel {
   int64_t NN = 0;
   double *len = nullptr, *pedlen = nullptr, *part = nullptr, *hex_inv = nullptr, *triarea = nullptr,
          *coriolis = nullptr, *overl_a = nullptr, *topo = nullptr;
+  double* iu_wgt = nullptr;  // 9*NN outer velocity weights (levels above level_start)
   int2* hn = nullptr;
   int3* he = nullptr;
   int n_hn = 0, n_he = 0;
@@ -21,7 +22,7 @@ struct DevLevel {
     return wtk::LevelDev{n, P, (int)NN, len, pedlen, part, hex_inv, triarea, coriolis, topo, nsrc, esrc};
   }
   void release() {
-    double* a[] = {len, pedlen, part, hex_inv, triarea, coriolis, overl_a, topo};
+    double* a[] = {len, pedlen, part, hex_inv, triarea, coriolis, overl_a, topo, iu_wgt};
     for (double* p : a)
       if (p) cudaFree(p);
     if (hn) cudaFree(hn);
@@ -29,7 +30,7 @@ struct DevLevel {
     if (nsrc) cudaFree(nsrc);
     if (esrc) cudaFree(esrc);
     nsrc = esrc = nullptr;
-    len = pedlen = part = hex_inv = triarea = coriolis = overl_a = topo = nullptr;
+    len = pedlen = part = hex_inv = triarea = coriolis = overl_a = topo = iu_wgt = nullptr;
     hn = nullptr;
     he = nullptr;
   }
@@ -59,6 +60,8 @@ struct wt_handle {
 
   // elliptic solver state (allocated by wt_elliptic_setup)
   void* ell = nullptr;
+  // multi-level wavelet fields and masks (allocated by wt_wavelet_setup)
+  void* wav = nullptr;
   void release_extra();
 
   DevLevel& top() { return lev.back(); }
@@ -66,3 +69,4 @@ struct wt_handle {
 };
 
 int wt_handle_fail(const char* where, cudaError_t e);
+void wt_wavelet_release(wt_handle* h);

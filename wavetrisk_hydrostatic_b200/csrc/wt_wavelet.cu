@@ -1,0 +1,277 @@
+// C-ABI of the wavelet transforms, threshold mask and compression of the
+// prognostic variables on the handle's uniform hierarchy.  The launch order of
+// each entry point follows the reference driver named in its comment; ghost
+// copies (update_bdry) are replaced by the kernels' remapped reads.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "../../include/wavetrisk_gpu.h"
+#include "wavelet_kernels.cuh"
+#include "wt_handle.cuh"
+
+using namespace wtw;
+
+namespace {
+
+constexpr int TPB = 256;
+inline unsigned nb(int64_t n) { return (unsigned)((n + TPB - 1) / TPB); }
+
+struct WavLevel {
+  double *sm = nullptr, *st = nullptr, *sv = nullptr;  // scaling (owned below level_end)
+  double *wm = nullptr, *wt = nullptr, *wv = nullptr;
+  int *mask_n = nullptr, *mask_e = nullptr;
+  bool own_scaling = false;
+};
+
+struct WavCtx {
+  std::vector<WavLevel> L;
+  double* thr = nullptr;  // [3][nz] thresholds
+  std::vector<void*> allocs;
+  template <class T>
+  cudaError_t alloc(T** p, size_t count) {
+    cudaError_t e = cudaMalloc(p, count * sizeof(T));
+    if (e == cudaSuccess) allocs.push_back(*p);
+    return e;
+  }
+};
+
+WavCtx* ctx(wt_handle* h) { return static_cast<WavCtx*>(h->wav); }
+
+WLev view(wt_handle* h, int l) {
+  const DevLevel& D = h->at(l);
+  WavLevel& W = ctx(h)->L[l - h->level_start];
+  WLev v;
+  v.n = D.n;
+  v.P = D.P;
+  v.NN = (int)D.NN;
+  v.len = D.len;
+  v.tri = D.triarea;
+  v.hinv = D.hex_inv;
+  v.oa = D.overl_a;
+  v.iu = D.iu_wgt;
+  v.nsrc = D.nsrc;
+  v.esrc = D.esrc;
+  v.mask_n = W.mask_n;
+  v.mask_e = W.mask_e;
+  v.sm = W.sm;
+  v.st = W.st;
+  v.sv = W.sv;
+  v.wm = W.wm;
+  v.wt = W.wt;
+  v.wv = W.wv;
+  return v;
+}
+
+int fail(const char* where, cudaError_t e) { return wt_handle_fail(where, e); }
+
+#define CKW(x)                                  \
+  do {                                          \
+    cudaError_t e_ = (x);                       \
+    if (e_ != cudaSuccess) return fail(#x, e_); \
+  } while (0)
+
+int ready(wt_handle* h) {
+  if (!h) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  return WT_OK;
+}
+
+void zero_wavelets(wt_handle* h) {
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    const DevLevel& D = h->at(l);
+    WavLevel& W = ctx(h)->L[l - h->level_start];
+    const size_t nn = (size_t)h->nz * D.NN * sizeof(double);
+    cudaMemsetAsync(W.wm, 0, nn, h->stream);
+    cudaMemsetAsync(W.wt, 0, nn, h->stream);
+    cudaMemsetAsync(W.wv, 0, 3 * nn, h->stream);
+  }
+}
+
+// Scalar wavelets of level l+1 (Compute_scalar_wavelets over parents [0, n_l)).
+void launch_scalar_wc(wt_handle* h, int l) {
+  const int np = h->at(l).n, nz = h->nz;
+  k_scalar_wc<<<nb((int64_t)nz * 10 * np * np), TPB, 0, h->stream>>>(view(h, l + 1), np, nz);
+}
+
+// Velocity wavelets of level l+1 and the pentagon corrections.
+void launch_velo_wc(wt_handle* h, int l) {
+  const int np = h->at(l).n, nz = h->nz;
+  k_velo_wc<<<nb((int64_t)nz * 10 * np * np), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), nz);
+  k_velo_penta<<<nb(10 * nz), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), nz, 0);
+}
+
+// inverse_wavelet_transform (src/wavelet.f90:208-296) from level_start.
+void inverse(wt_handle* h) {
+  const int nz = h->nz;
+  for (int l = h->level_start; l <= h->level_end - 1; ++l) {
+    const int np = h->at(l).n;
+    const WLev P = view(h, l), C = view(h, l + 1);
+    const int64_t par1 = (int64_t)nz * 10 * (np + 1) * (np + 1), par0 = (int64_t)nz * 10 * np * np;
+    k_prolong<<<nb(par1), TPB, 0, h->stream>>>(P, C, nz);
+    k_recon_outer<<<nb(par1), TPB, 0, h->stream>>>(P, C, nz);
+    k_velo_penta<<<nb(10 * nz), TPB, 0, h->stream>>>(P, C, nz, 1);
+    k_recon_scalar<<<nb(par0), TPB, 0, h->stream>>>(C, np, nz);
+    k_recon_inner<<<nb(par0), TPB, 0, h->stream>>>(P, C, nz);
+  }
+}
+
+void compress(wt_handle* h) {
+  const int nz = h->nz;
+  for (int l = h->level_start + 1; l <= h->level_end; ++l) {
+    const int n = h->at(l).n;
+    k_compress<<<nb((int64_t)nz * 10 * (n + 1) * (n + 1)), TPB, 0, h->stream>>>(view(h, l), nz);
+  }
+}
+
+}  // namespace
+
+void wt_wavelet_release(wt_handle* h) {
+  if (!h || !h->wav) return;
+  for (void* p : ctx(h)->allocs) cudaFree(p);
+  delete ctx(h);
+  h->wav = nullptr;
+}
+
+extern "C" {
+
+int wt_wavelet_setup(wt_handle* h) {
+  if (!h || h->lev.empty()) return WT_ERR_ARG;
+  for (int l = h->level_start + 1; l <= h->level_end; ++l)
+    if (!h->at(l).iu_wgt) return WT_ERR_ARG;
+  wt_wavelet_release(h);
+  WavCtx* W = new WavCtx();
+  h->wav = W;
+  const int nz = h->nz;
+  W->L.resize(h->level_end - h->level_start + 1);
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    const DevLevel& D = h->at(l);
+    WavLevel& V = W->L[l - h->level_start];
+    const size_t nn = (size_t)nz * D.NN;
+    if (l == h->level_end) {
+      V.sm = h->mass;
+      V.st = h->temp;
+      V.sv = h->velo;
+    } else {
+      V.own_scaling = true;
+      CKW(W->alloc(&V.sm, nn));
+      CKW(W->alloc(&V.st, nn));
+      CKW(W->alloc(&V.sv, 3 * nn));
+      CKW(cudaMemsetAsync(V.sm, 0, nn * 8, h->stream));
+      CKW(cudaMemsetAsync(V.st, 0, nn * 8, h->stream));
+      CKW(cudaMemsetAsync(V.sv, 0, 3 * nn * 8, h->stream));
+    }
+    CKW(W->alloc(&V.wm, nn));
+    CKW(W->alloc(&V.wt, nn));
+    CKW(W->alloc(&V.wv, 3 * nn));
+    CKW(W->alloc(&V.mask_n, (size_t)D.NN));
+    CKW(W->alloc(&V.mask_e, (size_t)3 * D.NN));
+    std::vector<int> tol(3 * D.NN, WT_MASK_TOLRNZ);
+    CKW(cudaMemcpy(V.mask_n, tol.data(), D.NN * sizeof(int), cudaMemcpyHostToDevice));
+    CKW(cudaMemcpy(V.mask_e, tol.data(), 3 * D.NN * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  CKW(W->alloc(&W->thr, (size_t)3 * nz));
+  zero_wavelets(h);
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
+  if (int rc = ready(h)) return rc;
+  if (!src || level < h->level_start || level > h->level_end || field < 0 || field > WT_MASK_EDGE) return WT_ERR_ARG;
+  const DevLevel& D = h->at(level);
+  WavLevel& V = ctx(h)->L[level - h->level_start];
+  const size_t nn = (size_t)h->nz * D.NN;
+  void* dst[8] = {V.sm, V.st, V.sv, V.wm, V.wt, V.wv, V.mask_n, V.mask_e};
+  const size_t bytes[8] = {nn * 8, nn * 8, 3 * nn * 8, nn * 8, nn * 8, 3 * nn * 8, D.NN * 4, 3 * D.NN * 4};
+  CKW(cudaMemcpyAsync(dst[field], src, bytes[field], cudaMemcpyHostToDevice, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  if (level == h->level_end && field <= WT_FIELD_VELO) h->state_halo_done = false;
+  return WT_OK;
+}
+
+int wt_download_field(wt_handle* h, int level, int field, void* dst) {
+  if (int rc = ready(h)) return rc;
+  if (!dst || level < h->level_start || level > h->level_end || field < 0 || field > WT_MASK_EDGE) return WT_ERR_ARG;
+  const DevLevel& D = h->at(level);
+  WavLevel& V = ctx(h)->L[level - h->level_start];
+  const size_t nn = (size_t)h->nz * D.NN;
+  if (field <= WT_WAVE_VELO) {
+    const bool wav = field >= WT_WAVE_MASS;
+    const int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * h->nz;
+    k_halo_level<<<nb(nt), TPB, 0, h->stream>>>(h->nz, (int)D.NN, D.hn, D.n_hn, D.he, D.n_he, wav ? V.wm : V.sm,
+                                                 wav ? V.wt : V.st, wav ? V.wv : V.sv);
+    CKW(cudaGetLastError());
+  }
+  const void* src[8] = {V.sm, V.st, V.sv, V.wm, V.wt, V.wv, V.mask_n, V.mask_e};
+  const size_t bytes[8] = {nn * 8, nn * 8, 3 * nn * 8, nn * 8, nn * 8, 3 * nn * 8, D.NN * 4, 3 * D.NN * 4};
+  CKW(cudaMemcpyAsync(dst, src[field], bytes[field], cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+// forward_wavelet_transform (src/wavelet.f90:20-98) with jmin_in = level_start+1.
+int wt_forward_wt(wt_handle* h) {
+  if (int rc = ready(h)) return rc;
+  const int nz = h->nz;
+  zero_wavelets(h);
+  for (int l = h->level_end - 1; l >= h->level_start; --l) {
+    const int np = h->at(l).n;
+    launch_scalar_wc(h, l);
+    k_restrict<<<nb((int64_t)nz * 10 * (np + 1) * (np + 1)), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), nz);
+  }
+  for (int l = h->level_end - 1; l >= h->level_start; --l) launch_velo_wc(h, l);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_inverse_wt(wt_handle* h) {
+  if (int rc = ready(h)) return rc;
+  inverse(h);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill) {
+  if (int rc = ready(h)) return rc;
+  if (!threshold) return WT_ERR_ARG;
+  const int nz = h->nz;
+  WavCtx* W = ctx(h);
+  CKW(cudaMemcpyAsync(W->thr, threshold, 3 * nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  for (int l = h->level_end; l >= h->level_start; --l) {
+    const int st = (l == h->level_end) ? 0 : -1, en = (l == h->level_end) ? 1 : 2;
+    const int m = h->at(l).n + en - st;
+    k_mask_tol<<<nb((int64_t)10 * m * m), TPB, 0, h->stream>>>(view(h, l), nz, st, en, W->thr, l < level_fill ? 1 : 0);
+  }
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_compress(wt_handle* h) {
+  if (int rc = ready(h)) return rc;
+  compress(h);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_wt_after_step(wt_handle* h) {
+  if (int rc = ready(h)) return rc;
+  zero_wavelets(h);
+  for (int l = h->level_start; l <= h->level_end - 1; ++l) {
+    launch_scalar_wc(h, l);
+    launch_velo_wc(h, l);
+  }
+  compress(h);
+  inverse(h);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
+  return WT_OK;
+}
+
+}  // extern "C"

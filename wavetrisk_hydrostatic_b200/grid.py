@@ -36,6 +36,7 @@ class LevelGeom:
     ccentre: np.ndarray       # (2, 3, NN)
     halo_node: np.ndarray     # (n_halo_node, 2) int64
     halo_edge: np.ndarray     # (n_halo_edge, 3) int64
+    iu_wgt: np.ndarray | None = None   # (9, NN) outer velocity weights I_u_wgt (levels above min_level-1)
     _owned: np.ndarray | None = field(default=None, repr=False)
 
     def idx(self, d, i, j):
@@ -107,6 +108,7 @@ class Grid:
             overl_split=get("overl_split", (2, NN)), ccentre=get("ccentre", (2, 3, NN)),
             halo_node=get("halo_node", (dims.n_halo_node, 2), np.int64),
             halo_edge=get("halo_edge", (dims.n_halo_edge, 3), np.int64),
+            iu_wgt=get("iu_wgt", (9, NN)) if l > self.min_level - 1 else None,
         )
         self._levels[l] = g
         return g

@@ -40,8 +40,11 @@ class _LevelDescs:
             hn = np.ascontiguousarray(g.halo_node, dtype=np.int64)
             he = np.ascontiguousarray(g.halo_edge, dtype=np.int64)
             self.keep += bufs + [hn, he]
+            iu = _c(g.iu_wgt) if (g.iu_wgt is not None and q > 0) else None
+            if iu is not None:
+                self.keep.append(iu)
             arr[q] = N.wt_level_desc(g.level, g.n, g.P, g.NN, *[N.dptr(b) for b in bufs],
-                                     N.iptr(hn), len(hn), N.iptr(he), len(he))
+                                     N.iptr(hn), len(hn), N.iptr(he), len(he), N.dptr(iu))
         self.arr = arr
 
 
@@ -115,6 +118,57 @@ class TriskModel(DeviceGrid):
 
     def synchronize(self) -> None:
         N.check("wt_synchronize", N.lib().wt_synchronize(self.h))
+
+
+class WaveletHierarchy(DeviceGrid):
+    """Layer mass, potential temperature and velocity on every level of a
+    uniform hierarchy, their wavelet coefficients and the node/edge masks, with
+    the reference's forward_wavelet_transform, inverse_wavelet_transform,
+    mask_tol_vars, compress_wavelets and WT_after_step (src/wavelet.f90,
+    src/mask.f90, src/adapt.f90).  Level level_end's scaling fields are the
+    stepper's state."""
+
+    FIELDS = {"mass": 0, "temp": 1, "velo": 2, "wc_mass": 3, "wc_temp": 4, "wc_velo": 5, "mask_n": 6, "mask_e": 7}
+
+    def __init__(self, levels: list[LevelGeom], topos: list[np.ndarray], nz: int, ph: OceanParams | None = None):
+        super().__init__(levels, topos, nz, ph)
+        self.ls, self.le = levels[0].level, levels[-1].level
+        N.check("wt_wavelet_setup", N.lib().wt_wavelet_setup(self.h))
+
+    def _shape(self, level, name):
+        NN = self.levels[level - self.ls].NN
+        if name == "mask_n":
+            return (NN,), np.int32
+        if name == "mask_e":
+            return (3 * NN,), np.int32
+        return (self.nz, (3 if name.endswith("velo") else 1) * NN), np.float64
+
+    def upload(self, level: int, name: str, a: np.ndarray) -> None:
+        shape, dt = self._shape(level, name)
+        buf = np.ascontiguousarray(np.broadcast_to(a, shape), dtype=dt)
+        N.check("wt_upload_field", N.lib().wt_upload_field(self.h, level, self.FIELDS[name], buf.ctypes.data))
+
+    def download(self, level: int, name: str) -> np.ndarray:
+        shape, dt = self._shape(level, name)
+        buf = np.empty(shape, dtype=dt)
+        N.check("wt_download_field", N.lib().wt_download_field(self.h, level, self.FIELDS[name], buf.ctypes.data))
+        return buf
+
+    def forward(self) -> None:
+        N.check("wt_forward_wt", N.lib().wt_forward_wt(self.h))
+
+    def inverse(self) -> None:
+        N.check("wt_inverse_wt", N.lib().wt_inverse_wt(self.h))
+
+    def mask_tol_vars(self, threshold: np.ndarray, level_fill: int) -> None:
+        thr = _c(np.asarray(threshold).reshape(3, self.nz))
+        N.check("wt_mask_tol_vars", N.lib().wt_mask_tol_vars(self.h, N.dptr(thr), int(level_fill)))
+
+    def compress(self) -> None:
+        N.check("wt_compress", N.lib().wt_compress(self.h))
+
+    def wt_after_step(self) -> None:
+        N.check("wt_wt_after_step", N.lib().wt_wt_after_step(self.h))
 
 
 def solver_opts(method: str = "fmg", tol: float = 1e-10, **kw):

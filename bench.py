@@ -17,7 +17,8 @@ on the host cores, one worker thread per lozenge domain up to the core count.
 
 --kernels-only times the device-resident stepper alone on --level/--nz (no
 CPU baseline, host-buffer path or extra workloads); it is the small case the
-kernel profiles are captured on.
+kernel profiles are captured on.  --wavelets-only does the same for the
+wavelet transforms on the hierarchy --level-2 .. --level.
 """
 from __future__ import annotations
 
@@ -51,6 +52,7 @@ def parse():
     p.add_argument("--no-extra", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--kernels-only", action="store_true")
+    p.add_argument("--wavelets-only", action="store_true")
     return p.parse_args()
 
 
@@ -240,6 +242,47 @@ def workload_config(args, world=1):
     }
 
 
+def wavelet_case(lmin, lmax, nz, repeats=5, device=None):
+    """Wavelet transforms of the layered state on the uniform hierarchy
+    lmin..lmax: forward_wavelet_transform, inverse_wavelet_transform and
+    WT_after_step (wavelets + compression + inverse).  CUDA-event time on the
+    handle's stream, best of `repeats`.  Algorithmic bytes of WT_after_step per
+    node-layer of the levels above lmin: read scaling and write wavelets of
+    5 words, read wavelets and read/write scaling of 5 words = 20 words."""
+    import numpy as np
+    import torch
+
+    from wavetrisk_hydrostatic_b200 import Grid
+    from wavetrisk_hydrostatic_b200.cases import edge_velocity, jet_state, solid_body_rotation
+    from wavetrisk_hydrostatic_b200.model import WaveletHierarchy
+
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    H = WaveletHierarchy(levels, [np.full(g.NN, -4000.0) for g in levels], nz)
+    g = levels[-1]
+    st = jet_state(g, nz, seed=3)
+    H.upload(lmax, "mass", st["mass"])
+    H.upload(lmax, "temp", st["temp"])
+    H.upload(lmax, "velo", st["velo"] + edge_velocity(g, solid_body_rotation(0.1))[None, :])
+    stream = torch.cuda.ExternalStream(H.stream, device=device)
+    out = {"workload": f"wavelet transforms, uniform J{lmin}..J{lmax} hierarchy, {nz} layers (mass, Theta, velocity)"}
+    for name, fn in (("forward_ms", H.forward), ("inverse_ms", H.inverse), ("wt_after_step_ms", H.wt_after_step)):
+        best = None
+        for _ in range(repeats):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            t = a.elapsed_time(b)
+            best = t if best is None else min(best, t)
+        out[name] = best
+    cells = sum(10 * 4 ** l for l in range(lmin + 1, lmax + 1))
+    out["wt_after_step_GBps"] = cells * nz * 20 * 8 / (out["wt_after_step_ms"] / 1e3) / 1e9
+    H.close()
+    return out
+
+
 def algorithmic_bytes_trend_rk(level, nz):
     """Compulsory bytes of one k_trend launch (MODE_RK).  Node-layers of the
     computed range [0, n]^2 read theta, qe(3), hflux_mass(3), hflux_Theta(3),
@@ -298,6 +341,8 @@ def bench_ours(args):
             })
         for lmax in (6, 7, 8):
             extra.append(elliptic_case(lmax))
+        for (lmin, lmax, nzw) in ((5, 7, 16), (5, 8, 32)):
+            extra.append(wavelet_case(lmin, lmax, nzw, device=device))
 
     if rank == 0:
         kt = r["kernel_ms_per_launch"]
@@ -414,12 +459,23 @@ def bench_kernels(args):
                       "unit": "simulated days per wall-clock hour"}), flush=True)
 
 
+def bench_wavelets(args):
+    import torch
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    print(json.dumps(wavelet_case(args.level - 2, args.level, args.nz, repeats=max(1, args.steps), device=device)),
+          flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         bench_reference(args)
     elif args.kernels_only:
         bench_kernels(args)
+    elif args.wavelets_only:
+        bench_wavelets(args)
     else:
         bench_ours(args)
 

@@ -207,7 +207,11 @@ __device__ __forceinline__ double& ee(const WLev& L, double* f, int e, int d, in
   return f[e * L.NN + nid(L, d, i, j)];
 }
 
-// Compute_velo_wavelets (src/wavelet.f90:672-710), parents [0, np)^2.
+__device__ void penta_compute(const WLev& Pa, const WLev& C, const double* vp, double* wc, int d, int ip, int jp);
+__device__ void penta_reconstruct(const WLev& Pa, const WLev& C, const double* vp, double* v, int d, int ip, int jp);
+
+// Compute_velo_wavelets (src/wavelet.f90:672-710), parents [0, np)^2, then the
+// pentagon corrections of the corner parents.
 __global__ void k_velo_wc(WLev Pa, WLev C, int nz) {
   int k, d, ip, jp;
   if (!decode(nz, Pa.n, k, d, ip, jp)) return;
@@ -232,6 +236,7 @@ __global__ void k_velo_wc(WLev Pa, WLev C, int nz) {
   if (me(C, RT, d, i, j + 1) >= ADJZONE) ee(C, wc, RT, d, i, j + 1) = re(C, v, RT, d, i, j + 1) - u[3];
   if (me(C, DG, d, i, j + 1) >= ADJZONE) ee(C, wc, DG, d, i, j + 1) = re(C, v, DG, d, i, j + 1) - u[4];
   if (me(C, UP, d, i + 1, j + 1) >= ADJZONE) ee(C, wc, UP, d, i + 1, j + 1) = re(C, v, UP, d, i + 1, j + 1) - u[5];
+  if ((ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1)) penta_compute(Pa, C, vp, wc, d, ip, jp);
 }
 
 // velo_interp_penta_corr (src/wavelet.f90:927-952) at the south-west corner.
@@ -242,65 +247,61 @@ __device__ void penta_corr(const WLev& Pa, const WLev& C, const double* vp, int 
          (re(Pa, vp, RT, d, -1, -1) + re(Pa, vp, RT, d, -1, 0) - (re(Pa, vp, RT, d, -1, -1) - re(Pa, vp, DG, d, -1, -1)));
 }
 
-// Pentagon corrections at the lozenge corners, in the reference's corner
-// order (NE, SE, SW, NW), one thread per (layer, lozenge):
-// reconstruct == 0: Compute_velo_wavelets_penta on the wavelets
-// (src/wavelet.f90:712-781); reconstruct == 1: Reconstruct_velo_penta on the
-// child velocity (:1096-1152).
-__global__ void k_velo_penta(WLev Pa, WLev C, int nz, int reconstruct) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 10 * nz) return;
-  const int k = t / 10, d = t - 10 * k;
+// Pentagon corrections at the lozenge corners, in the reference's corner order
+// (NE, SE, SW, NW).  Each touches only child edges of one parent's outer pairs,
+// so the thread of that parent applies it right after writing them: SE by
+// parent (np-1, 0), SW by (0, 0), NW by (0, np-1).
+// Compute_velo_wavelets_penta (src/wavelet.f90:712-781), on the wavelets.
+__device__ void penta_compute(const WLev& Pa, const WLev& C, const double* vp, double* wc, int d, int ip, int jp) {
   const int np = Pa.n, nc = C.n;
-  const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
-  if (!reconstruct) {
-    double* wc = C.wv + (int64_t)k * 3 * C.NN;
-    {  // SE
-      const double vv = (c_iu_base[6] + iw(C, 6, d, nc - 1, 0)) * (re(Pa, vp, RT, d, np, 0) + re(Pa, vp, UP, d, np, -1));
-      if (me(C, RT, d, nc - 2, 0) >= ADJZONE) {
-        ee(C, wc, RT, d, nc - 2, 0) = ee(C, wc, RT, d, nc - 2, 0) - vv;
-        ee(C, wc, RT, d, nc - 1, 0) = ee(C, wc, RT, d, nc - 1, 0) + vv;
-      }
+  if (ip == np - 1 && jp == 0) {  // SE (IPLUSJMINUS)
+    const double vv = (c_iu_base[6] + iw(C, 6, d, nc - 1, 0)) * (re(Pa, vp, RT, d, np, 0) + re(Pa, vp, UP, d, np, -1));
+    if (me(C, RT, d, nc - 2, 0) >= ADJZONE) {
+      ee(C, wc, RT, d, nc - 2, 0) = ee(C, wc, RT, d, nc - 2, 0) - vv;
+      ee(C, wc, RT, d, nc - 1, 0) = ee(C, wc, RT, d, nc - 1, 0) + vv;
     }
-    {  // SW
-      double u[2];
-      penta_corr(Pa, C, vp, d, u);
-      if (me(C, UP, d, 0, 0) >= ADJZONE) {
-        ee(C, wc, UP, d, 0, 0) = ee(C, wc, UP, d, 0, 0) + u[0];
-        ee(C, wc, UP, d, 0, 1) = ee(C, wc, UP, d, 0, 1) - u[0];
-      }
-      if (me(C, RT, d, 0, 0) >= ADJZONE) {
-        ee(C, wc, RT, d, 0, 0) = ee(C, wc, RT, d, 0, 0) + u[1];
-        ee(C, wc, RT, d, 1, 0) = ee(C, wc, RT, d, 1, 0) - u[1];
-      }
+  }
+  if (ip == 0 && jp == 0) {  // SW (IJMINUS)
+    double u[2];
+    penta_corr(Pa, C, vp, d, u);
+    if (me(C, UP, d, 0, 0) >= ADJZONE) {
+      ee(C, wc, UP, d, 0, 0) = ee(C, wc, UP, d, 0, 0) + u[0];
+      ee(C, wc, UP, d, 0, 1) = ee(C, wc, UP, d, 0, 1) - u[0];
     }
-    {  // NW
-      const double vv = -(c_iu_base[7] + iw(C, 7, d, 0, nc - 1)) * (re(Pa, vp, UP, d, 0, np) + re(Pa, vp, RT, d, -1, np));
-      if (me(C, UP, d, 0, nc - 2) >= ADJZONE) {
-        ee(C, wc, UP, d, 0, nc - 2) = ee(C, wc, UP, d, 0, nc - 2) - vv;
-        ee(C, wc, UP, d, 0, nc - 1) = ee(C, wc, UP, d, 0, nc - 1) + vv;
-      }
+    if (me(C, RT, d, 0, 0) >= ADJZONE) {
+      ee(C, wc, RT, d, 0, 0) = ee(C, wc, RT, d, 0, 0) + u[1];
+      ee(C, wc, RT, d, 1, 0) = ee(C, wc, RT, d, 1, 0) - u[1];
     }
-  } else {
-    double* v = C.sv + (int64_t)k * 3 * C.NN;
-    {  // SE
-      const double vv = -(c_iu_base[6] + iw(C, 6, d, nc - 1, 0)) * (re(Pa, vp, RT, d, np, 0) + re(Pa, vp, UP, d, np, -1));
-      ee(C, v, RT, d, nc - 2, 0) = ee(C, v, RT, d, nc - 2, 0) - vv;
-      ee(C, v, RT, d, nc - 1, 0) = ee(C, v, RT, d, nc - 1, 0) + vv;
+  }
+  if (ip == 0 && jp == np - 1) {  // NW (IMINUSJPLUS)
+    const double vv = -(c_iu_base[7] + iw(C, 7, d, 0, nc - 1)) * (re(Pa, vp, UP, d, 0, np) + re(Pa, vp, RT, d, -1, np));
+    if (me(C, UP, d, 0, nc - 2) >= ADJZONE) {
+      ee(C, wc, UP, d, 0, nc - 2) = ee(C, wc, UP, d, 0, nc - 2) - vv;
+      ee(C, wc, UP, d, 0, nc - 1) = ee(C, wc, UP, d, 0, nc - 1) + vv;
     }
-    {  // SW
-      double u[2];
-      penta_corr(Pa, C, vp, d, u);
-      ee(C, v, UP, d, 0, 0) = ee(C, v, UP, d, 0, 0) - u[0];
-      ee(C, v, UP, d, 0, 1) = ee(C, v, UP, d, 0, 1) + u[0];
-      ee(C, v, RT, d, 0, 0) = ee(C, v, RT, d, 0, 0) - u[1];
-      ee(C, v, RT, d, 1, 0) = ee(C, v, RT, d, 1, 0) + u[1];
-    }
-    {  // NW
-      const double vv = (c_iu_base[7] + iw(C, 7, d, 0, nc - 1)) * (re(Pa, vp, UP, d, 0, np) + re(Pa, vp, RT, d, -1, np));
-      ee(C, v, UP, d, 0, nc - 2) = ee(C, v, UP, d, 0, nc - 2) - vv;
-      ee(C, v, UP, d, 0, nc - 1) = ee(C, v, UP, d, 0, nc - 1) + vv;
-    }
+  }
+}
+
+// Reconstruct_velo_penta (src/wavelet.f90:1096-1152), on the child velocity.
+__device__ void penta_reconstruct(const WLev& Pa, const WLev& C, const double* vp, double* v, int d, int ip, int jp) {
+  const int np = Pa.n, nc = C.n;
+  if (ip == np - 1 && jp == 0) {  // SE
+    const double vv = -(c_iu_base[6] + iw(C, 6, d, nc - 1, 0)) * (re(Pa, vp, RT, d, np, 0) + re(Pa, vp, UP, d, np, -1));
+    ee(C, v, RT, d, nc - 2, 0) = ee(C, v, RT, d, nc - 2, 0) - vv;
+    ee(C, v, RT, d, nc - 1, 0) = ee(C, v, RT, d, nc - 1, 0) + vv;
+  }
+  if (ip == 0 && jp == 0) {  // SW
+    double u[2];
+    penta_corr(Pa, C, vp, d, u);
+    ee(C, v, UP, d, 0, 0) = ee(C, v, UP, d, 0, 0) - u[0];
+    ee(C, v, UP, d, 0, 1) = ee(C, v, UP, d, 0, 1) + u[0];
+    ee(C, v, RT, d, 0, 0) = ee(C, v, RT, d, 0, 0) - u[1];
+    ee(C, v, RT, d, 1, 0) = ee(C, v, RT, d, 1, 0) + u[1];
+  }
+  if (ip == 0 && jp == np - 1) {  // NW
+    const double vv = (c_iu_base[7] + iw(C, 7, d, 0, nc - 1)) * (re(Pa, vp, UP, d, 0, np) + re(Pa, vp, RT, d, -1, np));
+    ee(C, v, UP, d, 0, nc - 2) = ee(C, v, UP, d, 0, nc - 2) - vv;
+    ee(C, v, UP, d, 0, nc - 1) = ee(C, v, UP, d, 0, nc - 1) + vv;
   }
 }
 
@@ -327,7 +328,8 @@ __global__ void k_prolong(WLev Pa, WLev C, int nz) {
   }
 }
 
-// Reconstruct_outer_velo (src/wavelet.f90:954-976), parents [0, np]^2.
+// Reconstruct_outer_velo (src/wavelet.f90:954-976), parents [0, np]^2, then
+// Reconstruct_velo_penta by the corner parents.
 __global__ void k_recon_outer(WLev Pa, WLev C, int nz) {
   int k, d, ip, jp;
   if (!decode(nz, Pa.n + 1, k, d, ip, jp)) return;
@@ -343,6 +345,7 @@ __global__ void k_recon_outer(WLev Pa, WLev C, int nz) {
     ee(C, v, e, d, a2, b2) = v2;
     ee(C, v, e, d, a1, b1) = 2.0 * re(Pa, vp, e, d, ip, jp) - v2;
   }
+  if ((ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1)) penta_reconstruct(Pa, C, vp, v, d, ip, jp);
 }
 
 // Reconstruct_scalar (src/wavelet.f90:614-640), parents [0, np)^2.

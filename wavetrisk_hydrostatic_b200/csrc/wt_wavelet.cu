@@ -95,11 +95,10 @@ void launch_scalar_wc(wt_handle* h, int l) {
   k_scalar_wc<<<nb((int64_t)nz * 10 * np * np), TPB, 0, h->stream>>>(view(h, l + 1), np, nz);
 }
 
-// Velocity wavelets of level l+1 and the pentagon corrections.
+// Velocity wavelets of level l+1 (pentagon corrections included).
 void launch_velo_wc(wt_handle* h, int l) {
   const int np = h->at(l).n, nz = h->nz;
   k_velo_wc<<<nb((int64_t)nz * 10 * np * np), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), nz);
-  k_velo_penta<<<nb(10 * nz), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), nz, 0);
 }
 
 // inverse_wavelet_transform (src/wavelet.f90:208-296) from level_start.
@@ -111,7 +110,6 @@ void inverse(wt_handle* h) {
     const int64_t par1 = (int64_t)nz * 10 * (np + 1) * (np + 1), par0 = (int64_t)nz * 10 * np * np;
     k_prolong<<<nb(par1), TPB, 0, h->stream>>>(P, C, nz);
     k_recon_outer<<<nb(par1), TPB, 0, h->stream>>>(P, C, nz);
-    k_velo_penta<<<nb(10 * nz), TPB, 0, h->stream>>>(P, C, nz, 1);
     k_recon_scalar<<<nb(par0), TPB, 0, h->stream>>>(C, np, nz);
     k_recon_inner<<<nb(par0), TPB, 0, h->stream>>>(P, C, nz);
   }
@@ -184,7 +182,7 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
   WavLevel& V = ctx(h)->L[level - h->level_start];
   const size_t nn = (size_t)h->nz * D.NN;
   void* dst[8] = {V.sm, V.st, V.sv, V.wm, V.wt, V.wv, V.mask_n, V.mask_e};
-  const size_t bytes[8] = {nn * 8, nn * 8, 3 * nn * 8, nn * 8, nn * 8, 3 * nn * 8, D.NN * 4, 3 * D.NN * 4};
+  const size_t bytes[8] = {nn * 8, nn * 8, 3 * nn * 8, nn * 8, nn * 8, 3 * nn * 8, (size_t)D.NN * 4, (size_t)3 * D.NN * 4};
   CKW(cudaMemcpyAsync(dst[field], src, bytes[field], cudaMemcpyHostToDevice, h->stream));
   CKW(cudaStreamSynchronize(h->stream));
   if (level == h->level_end && field <= WT_FIELD_VELO) h->state_halo_done = false;
@@ -205,7 +203,7 @@ int wt_download_field(wt_handle* h, int level, int field, void* dst) {
     CKW(cudaGetLastError());
   }
   const void* src[8] = {V.sm, V.st, V.sv, V.wm, V.wt, V.wv, V.mask_n, V.mask_e};
-  const size_t bytes[8] = {nn * 8, nn * 8, 3 * nn * 8, nn * 8, nn * 8, 3 * nn * 8, D.NN * 4, 3 * D.NN * 4};
+  const size_t bytes[8] = {nn * 8, nn * 8, 3 * nn * 8, nn * 8, nn * 8, 3 * nn * 8, (size_t)D.NN * 4, (size_t)3 * D.NN * 4};
   CKW(cudaMemcpyAsync(dst, src[field], bytes[field], cudaMemcpyDeviceToHost, h->stream));
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;

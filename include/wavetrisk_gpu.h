@@ -227,6 +227,22 @@ int wt_compress(wt_handle* h);
  * compression, inverse transform. */
 int wt_wt_after_step(wt_handle* h);
 
+/* ---------------------------------------------------------- barotropic ---- */
+/* The free-surface pieces of the mode-split step on level_end, around the
+ * elliptic solve (eta_update / u_update, src/barotropic_2d.f90:118-149).
+ * eta is the free surface sol(S_MASS, zlevels+1); div_old the flux divergence
+ * of the previous step, trend(S_TEMP, zlevels+1); both NN doubles. */
+int wt_barotropic_upload(wt_handle* h, const double* eta, const double* div_old);  /* either may be NULL */
+/* flux_divergence (src/barotropic_2d.f90:326-366: step1 itype 4, the
+ * vertically summed mass flux of the resident state, and cal_div) and
+ * rhs_elliptic (:151-185): rhs = -eta + dt (theta2 div + (1-theta2) div_old) / rho0. */
+int wt_rhs_elliptic(wt_handle* h, double dt, double theta2);
+/* grad_eta (src/barotropic_2d.f90:455-474: step1 itype 3, g grad eta) and
+ * u_update (:131-149): velo_k -= theta1 dt grad eta on every layer. */
+int wt_u_update(wt_handle* h, double dt, double theta1);
+/* div_flux (NN), rhs (NN), grad (3*NN); any may be NULL. */
+int wt_barotropic_download(wt_handle* h, double* div_flux, double* rhs, double* grad);
+
 /* Raw stream of the handle (cudaStream_t), for event timing by the caller. */
 void* wt_stream(wt_handle* h);
 

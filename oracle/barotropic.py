@@ -1,0 +1,52 @@
+"""ORACLE (test infrastructure only): bindings of oracle_barotropic.cpp."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _dp, _ip, lib
+
+
+class orc_blevel(C.Structure):
+    _fields_ = [("n", C.c_int), ("P", C.c_int), ("NN", C.c_int64), ("len", _dp), ("pedlen", _dp), ("hex_inv", _dp),
+                ("halo_node", _ip), ("n_halo_node", C.c_int64), ("halo_edge", _ip), ("n_halo_edge", C.c_int64)]
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class _Level:
+    def __init__(self, g):
+        self.keep = [_c(g.len), _c(g.pedlen), _c(g.hex_inv), np.ascontiguousarray(g.halo_node, dtype=np.int64),
+                     np.ascontiguousarray(g.halo_edge, dtype=np.int64)]
+        ln, pl, hi, hn, he = self.keep
+        self.s = orc_blevel(g.n, g.P, g.NN, _p(ln), _p(pl), _p(hi), _p(hn, _ip), len(hn), _p(he, _ip), len(he))
+
+
+def rhs_elliptic(g, nz, mass, mean_m, velo, eta, div_old, dt, theta2, rho0):
+    """flux_divergence + rhs_elliptic on one level: returns (hflux, div, rhs)."""
+    L = lib()
+    lv = _Level(g)
+    hflux, div, rhs = np.zeros(3 * g.NN), np.zeros(g.NN), np.zeros(g.NN)
+    bufs = [_c(mass), _c(mean_m), _c(velo), _c(eta), _c(div_old)]
+    L.orc_rhs_elliptic.argtypes = [C.POINTER(orc_blevel), C.c_int] + [_dp] * 5 + [C.c_double] * 3 + [_dp] * 3
+    L.orc_rhs_elliptic(C.byref(lv.s), nz, *[_p(b) for b in bufs], dt, theta2, rho0, _p(hflux), _p(div), _p(rhs))
+    return hflux, div, rhs
+
+
+def u_update(g, nz, grav, eta, velo, dt, theta1):
+    """grad_eta + u_update on one level: returns (velo, grad)."""
+    L = lib()
+    lv = _Level(g)
+    v = _c(velo).copy()
+    grad = np.zeros(3 * g.NN)
+    e = _c(eta)
+    L.orc_u_update.argtypes = [C.POINTER(orc_blevel), C.c_int, C.c_double, _dp, C.c_double, C.c_double, _dp, _dp]
+    L.orc_u_update(C.byref(lv.s), nz, grav, _p(e), dt, theta1, _p(v), _p(grad))
+    return v, grad

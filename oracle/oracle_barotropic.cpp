@@ -1,0 +1,164 @@
+// ORACLE (test infrastructure only): CPU FP64 restatement of the barotropic
+// pieces of the reference's mode-split step on one uniform level of padded
+// lozenge arrays.  Imported only by tests/.
+//
+// Routines, op for op:
+//   flux_divergence (one level)               src/barotropic_2d.f90:326-366
+//   step1 itype 4 (comput :229-244, comp_SW :420-437)    src/ops.f90
+//   cal_div, div                              src/ops.f90:1325-1355
+//   rhs_elliptic, cal_rhs_elliptic            src/barotropic_2d.f90:151-185
+//   grad_eta (one level)                      src/barotropic_2d.f90:455-474
+//   step1 itype 3 (comput :225-228, comp_SW :416-419), porosity 1   src/ops.f90
+//   u_update                                  src/barotropic_2d.f90:131-149
+// step1 visits nodes [0, n]^2 of each lozenge and runs comp_SW on the south
+// and west borders; update_bdry is the level's ghost copy.  u_update is
+// applied to the edges grad_eta writes (the reference's element range also
+// covers ghost edges, which the next ghost copy overwrites).
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+extern "C" {
+struct orc_blevel {
+  int n, P;
+  int64_t NN;
+  const double *len, *pedlen, *hex_inv;
+  const int64_t* hn;
+  int64_t nhn;
+  const int64_t* he;
+  int64_t nhe;
+};
+}
+
+namespace {
+
+enum { RT = 0, DG = 1, UP = 2 };
+
+inline double interp(double a, double b) { return 0.5 * (a + b); }
+
+struct B {
+  const orc_blevel& L;
+  int64_t id(int d, int i, int j) const { return ((int64_t)d * L.P + j + 2) * L.P + i + 2; }
+  void halo_n(double* f) const {
+    for (int64_t q = 0; q < L.nhn; ++q) f[L.hn[2 * q]] = f[L.hn[2 * q + 1]];
+  }
+  void halo_e(double* f) const {
+    for (int64_t q = 0; q < L.nhe; ++q) {
+      const double v = f[L.he[3 * q + 1]];
+      f[L.he[3 * q]] = L.he[3 * q + 2] < 0 ? -v : v;
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int orc_rhs_elliptic(const orc_blevel* Lp, int nz, const double* mass, const double* mean_m, const double* velo,
+                     const double* eta, const double* div_old, double dt, double theta2, double rho0, double* hflux,
+                     double* div, double* rhs) {
+  const orc_blevel& L = *Lp;
+  B b{L};
+  const int64_t NN = L.NN;
+  const int P = L.P;
+  std::vector<double> m(mass, mass + nz * NN), v(velo, velo + 3 * nz * NN), e(eta, eta + NN), dold(div_old, div_old + NN);
+  for (int k = 0; k < nz; ++k) {
+    b.halo_n(m.data() + k * NN);
+    b.halo_e(v.data() + 3 * k * NN);
+  }
+  b.halo_n(e.data());
+  b.halo_n(dold.data());
+  std::memset(hflux, 0, 3 * NN * sizeof(double));
+  // step1 itype 4
+  for (int d = 0; d < 10; ++d)
+    for (int j = 0; j <= L.n; ++j)
+      for (int i = 0; i <= L.n; ++i) {
+        const int64_t id = b.id(d, i, j);
+        const int64_t idE = id + 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idS = id - P, idSW = id - P - 1;
+        double f[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < nz; ++k) {
+          const double* M = m.data() + k * NN;
+          const double* A = mean_m + k * NN;
+          const double* V = v.data() + 3 * k * NN;
+          const double dz0 = M[id] + A[id];
+          double dz = interp(dz0, M[idE] + A[idE]);
+          f[RT] = f[RT] + V[RT * NN + id] * dz;
+          dz = interp(dz0, M[idNE] + A[idNE]);
+          f[DG] = f[DG] + V[DG * NN + id] * dz;
+          dz = interp(dz0, M[idN] + A[idN]);
+          f[UP] = f[UP] + V[UP * NN + id] * dz;
+        }
+        for (int q = 0; q < 3; ++q) hflux[q * NN + id] = f[q] * L.pedlen[q * NN + id];
+        if (i == 0 || j == 0) {  // comp_SW
+          double g[3] = {0.0, 0.0, 0.0};
+          for (int k = 0; k < nz; ++k) {
+            const double* M = m.data() + k * NN;
+            const double* A = mean_m + k * NN;
+            const double* V = v.data() + 3 * k * NN;
+            const double dz0 = M[id] + A[id];
+            double dz = interp(dz0, M[idW] + A[idW]);
+            g[0] = g[0] + V[RT * NN + idW] * dz;
+            dz = interp(dz0, M[idSW] + A[idSW]);
+            g[1] = g[1] + V[DG * NN + idSW] * dz;
+            dz = interp(dz0, M[idS] + A[idS]);
+            g[2] = g[2] + V[UP * NN + idS] * dz;
+          }
+          hflux[RT * NN + idW] = g[0] * L.pedlen[RT * NN + idW];
+          hflux[DG * NN + idSW] = g[1] * L.pedlen[DG * NN + idSW];
+          hflux[UP * NN + idS] = g[2] * L.pedlen[UP * NN + idS];
+        }
+      }
+  b.halo_e(hflux);
+  std::memset(div, 0, NN * sizeof(double));
+  for (int d = 0; d < 10; ++d)
+    for (int j = 0; j <= L.n; ++j)
+      for (int i = 0; i <= L.n; ++i) {
+        const int64_t id = b.id(d, i, j);
+        div[id] = (hflux[RT * NN + id] - hflux[RT * NN + id - 1] + hflux[DG * NN + id - P - 1] - hflux[DG * NN + id] +
+                   hflux[UP * NN + id] - hflux[UP * NN + id - P]) *
+                  L.hex_inv[id];
+      }
+  b.halo_n(div);
+  std::memset(rhs, 0, NN * sizeof(double));
+  for (int d = 0; d < 10; ++d)
+    for (int j = 0; j <= L.n; ++j)
+      for (int i = 0; i <= L.n; ++i) {
+        const int64_t id = b.id(d, i, j);
+        rhs[id] = -e[id] + dt * (theta2 * div[id] + (1.0 - theta2) * dold[id]) / rho0;
+      }
+  return 0;
+}
+
+int orc_u_update(const orc_blevel* Lp, int nz, double grav, const double* eta, double dt, double theta1, double* velo,
+                 double* grad) {
+  const orc_blevel& L = *Lp;
+  B b{L};
+  const int64_t NN = L.NN;
+  const int P = L.P;
+  std::vector<double> e(eta, eta + NN);
+  b.halo_n(e.data());
+  std::memset(grad, 0, 3 * NN * sizeof(double));
+  std::vector<char> written(3 * NN, 0);
+  for (int d = 0; d < 10; ++d)
+    for (int j = 0; j <= L.n; ++j)
+      for (int i = 0; i <= L.n; ++i) {
+        const int64_t id = b.id(d, i, j);
+        grad[RT * NN + id] = grav * (e[id + 1] / 1.0 - e[id] / 1.0) / L.len[RT * NN + id];
+        grad[DG * NN + id] = grav * (e[id] / 1.0 - e[id + P + 1] / 1.0) / L.len[DG * NN + id];
+        grad[UP * NN + id] = grav * (e[id + P] / 1.0 - e[id] / 1.0) / L.len[UP * NN + id];
+        written[RT * NN + id] = written[DG * NN + id] = written[UP * NN + id] = 1;
+        if (i == 0 || j == 0) {  // comp_SW
+          grad[RT * NN + id - 1] = -(grav * (e[id - 1] / 1.0 - e[id] / 1.0) / L.len[RT * NN + id - 1]);
+          grad[DG * NN + id - P - 1] = -(grav * (e[id] / 1.0 - e[id - P - 1] / 1.0) / L.len[DG * NN + id - P - 1]);
+          grad[UP * NN + id - P] = -(grav * (e[id - P] / 1.0 - e[id] / 1.0) / L.len[UP * NN + id - P]);
+          written[RT * NN + id - 1] = written[DG * NN + id - P - 1] = written[UP * NN + id - P] = 1;
+        }
+      }
+  const double s = theta1 * dt;
+  for (int k = 0; k < nz; ++k)
+    for (int64_t x = 0; x < 3 * NN; ++x)
+      if (written[x]) velo[3 * k * NN + x] = velo[3 * k * NN + x] - s * grad[x];
+  return 0;
+}
+
+}  // extern "C"

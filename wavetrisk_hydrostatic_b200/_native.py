@@ -127,6 +127,10 @@ _DEVICE_SIGS = {
     "wt_mask_tol_vars": [_vp, _dp, C.c_int],
     "wt_compress": [_vp],
     "wt_wt_after_step": [_vp],
+    "wt_barotropic_upload": [_vp, _dp, _dp],
+    "wt_rhs_elliptic": [_vp, C.c_double, C.c_double],
+    "wt_u_update": [_vp, C.c_double, C.c_double],
+    "wt_barotropic_download": [_vp, _dp, _dp, _dp],
 }
 
 

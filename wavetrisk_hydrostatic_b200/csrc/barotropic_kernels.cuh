@@ -1,0 +1,157 @@
+// Barotropic pieces of the mode-split step on one uniform level
+// (src/barotropic_2d.f90): the vertically summed mass flux and its divergence
+// (flux_divergence, step1 itype 4), the right-hand side of the free-surface
+// equation (rhs_elliptic), the external pressure gradient (grad_eta, step1
+// itype 3) and the velocity update with it (u_update).
+//
+// Every edge flux is a function of the edge alone, so the south/west-border
+// formulas of comp_SW (src/ops.f90:420-445) are written to the ghost edges
+// they own, every edge is written by exactly one thread (the reference's
+// repeated writes carry identical bits), and every other ghost edge is read
+// through the level's remap.
+// Operand order follows the reference; compiled with --fmad=false.
+#pragma once
+#include <cstdint>
+
+#include "trisk_read.cuh"
+
+namespace wtb {
+
+using wtk::DG;
+using wtk::interp;
+using wtk::LevelDev;
+using wtk::Rd;
+using wtk::RT;
+using wtk::UP;
+
+// step1 itype 4 (src/ops.f90:229-244, comp_SW :420-437): h_flux = pedlen *
+// sum_k u_k interp(rho dz_k) at the edges of nodes [0, n]^2 and, on the
+// south/west borders, at the ghost edges comp_SW writes.
+__global__ void k_flux_sum(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ mean_m,
+                           const double* __restrict__ velo, double* __restrict__ hflux) {
+  const int m = L.n + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  const int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
+  const int P = L.P, NN = L.NN;
+  const int id = (d * P + j + 2) * P + i + 2;
+  const int idE = id + 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idS = id - P, idSW = id - P - 1;
+  const Rd R(L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2);
+  double fRT = 0.0, fDG = 0.0, fUP = 0.0;
+  for (int k = 0; k < nz; ++k) {
+    const int64_t ko = (int64_t)k * NN;
+    const double* Mm = mass + ko;
+    const double* Am = mean_m + ko;
+    const double* v = velo + 3 * ko;
+    const double dz0 = R.n(Mm, id) + Am[id];
+    double dz = interp(dz0, R.n(Mm, idE) + Am[idE]);
+    fRT = fRT + R.e(v, RT * NN + id) * dz;
+    dz = interp(dz0, R.n(Mm, idNE) + Am[idNE]);
+    fDG = fDG + R.e(v, DG * NN + id) * dz;
+    dz = interp(dz0, R.n(Mm, idN) + Am[idN]);
+    fUP = fUP + R.e(v, UP * NN + id) * dz;
+  }
+  hflux[RT * NN + id] = fRT * L.pedlen[RT * NN + id];
+  hflux[DG * NN + id] = fDG * L.pedlen[DG * NN + id];
+  hflux[UP * NN + id] = fUP * L.pedlen[UP * NN + id];
+  if (i == 0 || j == 0) {  // comp_SW
+    double gW = 0.0, gSW = 0.0, gS = 0.0;
+    for (int k = 0; k < nz; ++k) {
+      const int64_t ko = (int64_t)k * NN;
+      const double* Mm = mass + ko;
+      const double* Am = mean_m + ko;
+      const double* v = velo + 3 * ko;
+      const double dz0 = R.n(Mm, id) + Am[id];
+      double dz = interp(dz0, R.n(Mm, idW) + Am[idW]);
+      gW = gW + R.e(v, RT * NN + idW) * dz;
+      dz = interp(dz0, R.n(Mm, idSW) + Am[idSW]);
+      gSW = gSW + R.e(v, DG * NN + idSW) * dz;
+      dz = interp(dz0, R.n(Mm, idS) + Am[idS]);
+      gS = gS + R.e(v, UP * NN + idS) * dz;
+    }
+    // Edges an interior node also produces, bit-identically, are left to it:
+    // RT of (i-1, 0) when i > 0 and UP of (0, j-1) when j > 0.
+    if (i == 0) hflux[RT * NN + idW] = gW * L.pedlen[RT * NN + idW];
+    hflux[DG * NN + idSW] = gSW * L.pedlen[DG * NN + idSW];
+    if (!(i == 0 && j > 0)) hflux[UP * NN + idS] = gS * L.pedlen[UP * NN + idS];
+  }
+}
+
+// cal_div (src/ops.f90:1325-1355) at nodes [0, n]^2:
+//   div = hex_inv * (F_RT - F_RT,W + F_DG,SW - F_DG + F_UP - F_UP,S)
+__global__ void k_div(LevelDev L, const double* __restrict__ hflux, double* __restrict__ div) {
+  const int m = L.n + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  const int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
+  const int P = L.P, NN = L.NN;
+  const int id = (d * P + j + 2) * P + i + 2;
+  const Rd R(L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2);
+  div[id] = (R.e(hflux, RT * NN + id) - R.e(hflux, RT * NN + id - 1) + R.e(hflux, DG * NN + id - P - 1) -
+             R.e(hflux, DG * NN + id) + R.e(hflux, UP * NN + id) - R.e(hflux, UP * NN + id - P)) *
+            L.hex_inv[id];
+}
+
+// cal_rhs_elliptic (src/barotropic_2d.f90:167-184) at nodes [0, n]^2, after
+// flux_divergence's ghost copy of div (read through the remap):
+//   rhs = -eta + dt (theta2 div + (1 - theta2) div_old) / rho0
+__global__ void k_rhs(LevelDev L, const double* __restrict__ div, const double* __restrict__ eta,
+                      const double* __restrict__ div_old, double dt, double theta2, double rho0,
+                      double* __restrict__ rhs) {
+  const int m = L.n + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  const int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
+  const int id = (d * L.P + j + 2) * L.P + i + 2;
+  const Rd R(L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2);
+  rhs[id] = -R.n(eta, id) + dt * (theta2 * R.n(div, id) + (1.0 - theta2) * R.n(div_old, id)) / rho0;
+}
+
+// step1 itype 3 (src/ops.f90:225-228, comp_SW :416-419) with porosity 1,
+// h_flux = g (eta_far - eta_near) / len, and u_update
+// (src/barotropic_2d.f90:131-149): velo_k -= theta1 dt h_flux on every layer.
+__global__ void k_grad_eta_update(LevelDev L, int nz, double grav, const double* __restrict__ eta, double scale,
+                                  double* __restrict__ grad, double* __restrict__ velo) {
+  const int m = L.n + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  const int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
+  const int P = L.P, NN = L.NN;
+  const int id = (d * P + j + 2) * P + i + 2;
+  const Rd R(L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2);
+  const double e0 = R.n(eta, id) / 1.0;
+  int slot[6];
+  double g[6];
+  int ne = 3;
+  slot[0] = RT * NN + id;
+  g[0] = grav * (R.n(eta, id + 1) / 1.0 - e0) / L.len[slot[0]];
+  slot[1] = DG * NN + id;
+  g[1] = grav * (e0 - R.n(eta, id + P + 1) / 1.0) / L.len[slot[1]];
+  slot[2] = UP * NN + id;
+  g[2] = grav * (R.n(eta, id + P) / 1.0 - e0) / L.len[slot[2]];
+  if (i == 0 || j == 0) {  // comp_SW
+    if (i == 0) {
+      slot[ne] = RT * NN + id - 1;
+      g[ne] = -grav * (R.n(eta, id - 1) / 1.0 - e0) / L.len[slot[ne]];
+      ++ne;
+    }
+    slot[ne] = DG * NN + id - P - 1;
+    g[ne] = -grav * (e0 - R.n(eta, id - P - 1) / 1.0) / L.len[slot[ne]];
+    ++ne;
+    // UP of (0, j-1) is the own edge of that node (same value): updated once, there
+    if (!(i == 0 && j > 0)) {
+      slot[ne] = UP * NN + id - P;
+      g[ne] = -grav * (R.n(eta, id - P) / 1.0 - e0) / L.len[slot[ne]];
+      ++ne;
+    }
+  }
+  for (int q = 0; q < ne; ++q) {
+    grad[slot[q]] = g[q];
+    for (int k = 0; k < nz; ++k) {
+      double* v = velo + (int64_t)k * 3 * NN;
+      v[slot[q]] = v[slot[q]] - scale * g[q];
+    }
+  }
+}
+
+}  // namespace wtb

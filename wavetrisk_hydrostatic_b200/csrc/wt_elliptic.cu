@@ -106,6 +106,7 @@ void wt_handle::release_extra() {
   if (ell) ell_free(static_cast<Ell*>(ell));
   ell = nullptr;
   wt_wavelet_release(this);
+  wt_barotropic_release(this);
 }
 
 extern "C" int wt_elliptic_setup(wt_handle* h, double dt, double theta1, double theta2, int domain_level) {

@@ -62,6 +62,8 @@ struct wt_handle {
   void* ell = nullptr;
   // multi-level wavelet fields and masks (allocated by wt_wavelet_setup)
   void* wav = nullptr;
+  // free-surface fields of the barotropic step (allocated on first use)
+  void* baro = nullptr;
   void release_extra();
 
   DevLevel& top() { return lev.back(); }
@@ -70,3 +72,4 @@ struct wt_handle {
 
 int wt_handle_fail(const char* where, cudaError_t e);
 void wt_wavelet_release(wt_handle* h);
+void wt_barotropic_release(wt_handle* h);

@@ -119,6 +119,25 @@ class TriskModel(DeviceGrid):
     def synchronize(self) -> None:
         N.check("wt_synchronize", N.lib().wt_synchronize(self.h))
 
+    # -- barotropic pieces of the mode-split step (src/barotropic_2d.f90) --
+    def barotropic_upload(self, eta: np.ndarray | None = None, div_old: np.ndarray | None = None) -> None:
+        N.check("wt_barotropic_upload", N.lib().wt_barotropic_upload(
+            self.h, N.dptr(None if eta is None else _c(eta)), N.dptr(None if div_old is None else _c(div_old))))
+
+    def rhs_elliptic(self, dt: float, theta2: float = 1.0):
+        """flux_divergence + rhs_elliptic of the resident state: returns (div_flux, rhs)."""
+        N.check("wt_rhs_elliptic", N.lib().wt_rhs_elliptic(self.h, float(dt), float(theta2)))
+        div, rhs = np.empty(self.g.NN), np.empty(self.g.NN)
+        N.check("wt_barotropic_download", N.lib().wt_barotropic_download(self.h, N.dptr(div), N.dptr(rhs), None))
+        return div, rhs
+
+    def u_update(self, dt: float, theta1: float = 1.0) -> np.ndarray:
+        """grad_eta + u_update on the resident velocity: returns grad eta (3*NN)."""
+        N.check("wt_u_update", N.lib().wt_u_update(self.h, float(dt), float(theta1)))
+        grad = np.empty(3 * self.g.NN)
+        N.check("wt_barotropic_download", N.lib().wt_barotropic_download(self.h, None, None, N.dptr(grad)))
+        return grad
+
 
 class WaveletHierarchy(DeviceGrid):
     """Layer mass, potential temperature and velocity on every level of a

@@ -221,6 +221,19 @@ int wt_inverse_wt(wt_handle* h);
  * level_end on nodes [0, n], coarser levels on [-1, n+1].  threshold is
  * [3][nz] (mass, Theta, velocity per layer), as threshold(v, k). */
 int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill);
+/* adapt's mask sequence (src/adapt.f90:14-65) on the dense hierarchy, without
+ * the tree surgery that the host keeps: init_masks_zero, mask_active
+ * (mask_tol_vars + mask_parent_nodes/edges), mask_adj_same_scale,
+ * mask_restrict_same_scale (levels < max_level), mask_adj_finer_scale,
+ * complete_masks and mask_trsk (src/mask.f90), with comm_masks between sweeps
+ * as the serial build does.  child_required (may be NULL) receives
+ * check_child_required (src/refine_patch.f90:289-327) for every parent patch
+ * of side patch_size and child quadrant (NE, SE, SW, NW) of levels
+ * level_start .. level_end-1, level by level, lozenge-major:
+ * sum_l 10 * (n_l / patch_size)^2 * 4 bytes.  Exact when every patch of the
+ * hierarchy exists (a fully refined tree). */
+int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max_level, int patch_size,
+                  unsigned char* child_required);
 /* compress_wavelets (src/adapt.f90:79-103): zero the wavelets of inactive points. */
 int wt_compress(wt_handle* h);
 /* WT_after_step (src/adapt.f90:234-283): wavelets of the current scaling fields,

@@ -16,6 +16,14 @@
 //   mask_tol_vars                                         src/mask.f90:102-156
 //   compress_wavelets, compress_scalar, compress_vector   src/adapt.f90:79-232
 //   WT_after_step                                         src/adapt.f90:234-283
+//   adapt's mask sequence without tree surgery            src/adapt.f90:14-65
+//     init_masks_zero, mask_active, mask_adj_same_scale, mask_restrict_same_scale,
+//     mask_adj_finer_scale, complete_masks, mask_trsk      src/mask.f90:7-100,734-768
+//     mask_parent_nodes/edges, mask_adj_same_scale_nodes_edges, mask_restrict_flux,
+//     mask_adj_child, mask_edges_consist(2), mask_edges_if_both_nodes,
+//     mask_nodes_if_all_edges, prolong_node_adjzone, div_grad_stencil  src/mask.f90:158-867
+//     comm_masks (serial comm_masks_mpi)                  src/comm.f90:531-553
+//   check_child_required                                  src/refine_patch.f90:289-327
 // Iteration sets are those of apply_interscale_d (parents [0, n_par)),
 // apply_interscale_d with +1 (parents [0, n_par], "+1 to include poles"),
 // apply_interscale_d2 (parents [0, n_par]: every child patch is extended) and
@@ -33,7 +41,7 @@ namespace {
 enum { RT = 0, DG = 1, UP = 2 };
 enum { LORT = 0, UPLT = 1 };
 constexpr int H = 2;
-constexpr int FROZEN = 32, TOLRNZ = 16, ADJZONE = 8, ZERO = 0;
+constexpr int FROZEN = 32, TOLRNZ = 16, ADJSPACE = 14, RESTRCT = 12, ADJZONE = 8, TRSK = 2, ZERO = 0;
 
 // Stencil tables of src/shared.f90:287-324 (0-based edge index, k = 0, 1).
 const int END_PT[3][2][2] = {{{0, 0}, {1, 0}}, {{1, 1}, {0, 0}}, {{0, 0}, {0, 1}}};
@@ -513,6 +521,329 @@ struct W {
       }
   }
 
+  // ---- masks (one level; out-of-array reads are ZERO, writes are skipped)
+  static void at_least(int32_t* m, int64_t x, int typ) {
+    if (m[x] < typ) m[x] = typ;
+  }
+  static void sn(orc_wlevel& g, int d, int i, int j, int typ) {
+    if (in(g, i, j)) at_least(g.mask_n, id(g, d, i, j), typ);
+  }
+  static void se(orc_wlevel& g, int e, int d, int i, int j, int typ) {
+    if (in(g, i, j)) at_least(g.mask_e, (int64_t)e * g.NN + id(g, d, i, j), typ);
+  }
+  // serial comm_masks_mpi: every level's node and edge masks to their ghost copies
+  void comm_masks() {
+    for (int l = ls; l <= le; ++l) {
+      orc_wlevel& g = L(l);
+      for (int64_t q = 0; q < g.nhn; ++q) g.mask_n[g.hn[2 * q]] = g.mask_n[g.hn[2 * q + 1]];
+      for (int64_t q = 0; q < g.nhe; ++q) g.mask_e[g.he[3 * q]] = g.mask_e[g.he[3 * q + 1]];
+    }
+  }
+  void init_masks_zero() {
+    for (int l = ls + 1; l <= le; ++l) {
+      orc_wlevel& g = L(l);
+      for (int64_t x = 0; x < g.NN; ++x) g.mask_n[x] = ZERO;
+      for (int64_t x = 0; x < 3 * g.NN; ++x) g.mask_e[x] = ZERO;
+    }
+  }
+  void mask_parent_nodes(int l) {  // parents [0, np]
+    orc_wlevel& Pa = L(l);
+    orc_wlevel& C = L(l + 1);
+    for (int d = 0; d < 10; ++d)
+      for (int jp = 0; jp <= Pa.n; ++jp)
+        for (int ip = 0; ip <= Pa.n; ++ip) {
+          const int i = 2 * ip, j = 2 * jp;
+          if (mn(C, d, i + 1, j) == TOLRNZ || mn(C, d, i + 1, j + 1) == TOLRNZ || mn(C, d, i, j + 1) == TOLRNZ ||
+              mn(C, d, i - 1, j) == TOLRNZ || mn(C, d, i - 1, j - 1) == TOLRNZ || mn(C, d, i, j - 1) == TOLRNZ) {
+            sn(Pa, d, ip, jp, TOLRNZ);
+            sn(C, d, i, j, TOLRNZ);
+          }
+        }
+  }
+  void mask_parent_edges(int l) {  // parents [0, np)
+    orc_wlevel& Pa = L(l);
+    orc_wlevel& C = L(l + 1);
+    for (int d = 0; d < 10; ++d)
+      for (int jp = 0; jp < Pa.n; ++jp)
+        for (int ip = 0; ip < Pa.n; ++ip) {
+          const int i = 2 * ip, j = 2 * jp;
+          auto T = [&](int e, int a, int b) { return me(C, e, d, a, b) == TOLRNZ; };
+          if (T(RT, i, j) || T(RT, i + 1, j) || T(DG, i, j - 1) || T(DG, i + 1, j) || T(UP, i + 1, j) || T(UP, i + 1, j - 1))
+            se(Pa, RT, d, ip, jp, TOLRNZ);
+          if (T(RT, i, j + 1) || T(RT, i + 1, j + 1) || T(DG, i, j) || T(DG, i + 1, j + 1) || T(UP, i + 1, j + 1) ||
+              T(UP, i + 1, j))
+            se(Pa, DG, d, ip, jp, TOLRNZ);
+          if (T(RT, i, j + 1) || T(RT, i - 1, j + 1) || T(DG, i, j + 1) || T(DG, i - 1, j) || T(UP, i, j) || T(UP, i, j + 1))
+            se(Pa, UP, d, ip, jp, TOLRNZ);
+        }
+  }
+  void mask_adj_same_scale(int l) {  // nodes [0, n]
+    orc_wlevel& g = L(l);
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j <= g.n; ++j)
+        for (int i = 0; i <= g.n; ++i) {
+          if (mn(g, d, i + 1, j) == TOLRNZ || mn(g, d, i + 1, j + 1) == TOLRNZ || mn(g, d, i, j + 1) == TOLRNZ ||
+              mn(g, d, i - 1, j) == TOLRNZ || mn(g, d, i - 1, j - 1) == TOLRNZ || mn(g, d, i, j - 1) == TOLRNZ)
+            sn(g, d, i, j, ADJSPACE);
+          auto T = [&](int e, int a, int b) { return me(g, e, d, a, b) == TOLRNZ; };
+          if (T(DG, i, j) || T(UP, i, j - 1) || T(DG, i, j - 1) || T(UP, i + 1, j)) se(g, RT, d, i, j, ADJSPACE);
+          if (T(UP, i, j) || T(RT, i, j) || T(UP, i + 1, j) || T(RT, i, j + 1)) se(g, DG, d, i, j, ADJSPACE);
+          if (T(DG, i, j) || T(RT, i - 1, j) || T(DG, i - 1, j) || T(RT, i, j + 1)) se(g, UP, d, i, j, ADJSPACE);
+        }
+  }
+  void mask_restrict_flux(int l) {  // nodes [0, n)
+    orc_wlevel& g = L(l);
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j < g.n; ++j)
+        for (int i = 0; i < g.n; ++i) {
+          if (mn(g, d, i, j) >= ADJSPACE) {
+            se(g, RT, d, i, j, RESTRCT);
+            se(g, DG, d, i, j, RESTRCT);
+            se(g, UP, d, i, j, RESTRCT);
+          } else {
+            if (mn(g, d, i + 1, j) >= ADJSPACE) se(g, RT, d, i, j, RESTRCT);
+            if (mn(g, d, i + 1, j + 1) >= ADJSPACE) se(g, DG, d, i, j, RESTRCT);
+            if (mn(g, d, i, j + 1) >= ADJSPACE) se(g, UP, d, i, j, RESTRCT);
+          }
+        }
+  }
+  void mask_adj_child(int l) {  // parents [0, np]
+    orc_wlevel& Pa = L(l);
+    orc_wlevel& C = L(l + 1);
+    for (int d = 0; d < 10; ++d)
+      for (int jp = 0; jp <= Pa.n; ++jp)
+        for (int ip = 0; ip <= Pa.n; ++ip) {
+          const int i = 2 * ip, j = 2 * jp;
+          auto PE = [&](int e, int a, int b, int typ) { return me(Pa, e, d, a, b) >= typ; };
+          if (mn(Pa, d, ip, jp) >= TOLRNZ) {
+            const int nb[13][2] = {{0, 0},  {1, 0},  {1, 1},  {0, 1},  {-1, 0}, {-1, -1}, {0, -1},
+                                   {-1, 1}, {1, -1}, {2, 1},  {1, 2},  {-1, -2}, {-2, -1}};
+            for (auto& q : nb) sn(C, d, i + q[0], j + q[1], ADJZONE);
+            se(Pa, UP, d, ip, jp, RESTRCT);
+            se(Pa, DG, d, ip, jp, RESTRCT);
+            se(Pa, RT, d, ip, jp, RESTRCT);
+          } else {
+            if (mn(Pa, d, ip, jp + 1) >= TOLRNZ) {
+              sn(C, d, i, j + 1, ADJZONE);
+              se(Pa, UP, d, ip, jp, RESTRCT);
+            }
+            if (mn(Pa, d, ip + 1, jp + 1) >= TOLRNZ) {
+              sn(C, d, i + 1, j + 1, ADJZONE);
+              se(Pa, DG, d, ip, jp, RESTRCT);
+            }
+            if (mn(Pa, d, ip + 1, jp) >= TOLRNZ) {
+              sn(C, d, i + 1, j, ADJZONE);
+              se(Pa, RT, d, ip, jp, RESTRCT);
+            }
+          }
+          if (PE(UP, ip, jp, TOLRNZ)) {
+            sn(C, d, i, j + 1, ADJZONE);
+            if (PE(UP, ip, jp - 1, TOLRNZ)) sn(C, d, i, j, ADJZONE);
+          }
+          if (PE(DG, ip, jp, TOLRNZ)) {
+            sn(C, d, i + 1, j + 1, ADJZONE);
+            if (PE(DG, ip - 1, jp - 1, TOLRNZ)) sn(C, d, i, j, ADJZONE);
+          }
+          if (PE(RT, ip, jp, TOLRNZ)) {
+            sn(C, d, i + 1, j, ADJZONE);
+            if (PE(RT, ip - 1, jp, TOLRNZ)) sn(C, d, i, j, ADJZONE);
+          }
+          if (PE(UP, ip, jp, TOLRNZ) || PE(DG, ip, jp, TOLRNZ) || PE(RT, ip - 1, jp, TOLRNZ) || PE(DG, ip - 1, jp, TOLRNZ) ||
+              PE(RT, ip, jp + 1, TOLRNZ)) {
+            se(C, UP, d, i, j, ADJZONE);
+            se(C, UP, d, i, j + 1, ADJZONE);
+          }
+          if (PE(DG, ip, jp, TOLRNZ) || PE(UP, ip, jp, TOLRNZ) || PE(RT, ip, jp, TOLRNZ) || PE(UP, ip + 1, jp, TOLRNZ) ||
+              PE(RT, ip, jp + 1, TOLRNZ)) {
+            se(C, DG, d, i, j, ADJZONE);
+            se(C, DG, d, i + 1, j + 1, ADJZONE);
+          }
+          if (PE(RT, ip, jp, TOLRNZ) || PE(DG, ip, jp, TOLRNZ) || PE(UP, ip, jp - 1, TOLRNZ) || PE(DG, ip, jp - 1, TOLRNZ) ||
+              PE(UP, ip + 1, jp, TOLRNZ)) {
+            se(C, RT, d, i, j, ADJZONE);
+            se(C, RT, d, i + 1, j, ADJZONE);
+          }
+          if (PE(UP, ip, jp, TOLRNZ) || PE(DG, ip, jp, TOLRNZ) || PE(RT, ip, jp + 1, TOLRNZ)) {
+            se(C, RT, d, i, j + 1, ADJZONE);
+            se(C, DG, d, i, j + 1, ADJZONE);
+            se(C, UP, d, i + 1, j + 1, ADJZONE);
+          }
+          if (PE(RT, ip, jp, TOLRNZ) || PE(DG, ip, jp, TOLRNZ) || PE(UP, ip + 1, jp, TOLRNZ)) {
+            se(C, UP, d, i + 1, j, ADJZONE);
+            se(C, DG, d, i + 1, j, ADJZONE);
+            se(C, RT, d, i + 1, j + 1, ADJZONE);
+          }
+          if (PE(RT, ip, jp, ADJSPACE) || PE(DG, ip, jp, ADJSPACE) || PE(UP, ip, jp, ADJSPACE) ||
+              PE(RT, ip - 1, jp, ADJSPACE) || PE(DG, ip - 1, jp - 1, ADJSPACE) || PE(UP, ip, jp - 1, ADJSPACE))
+            sn(Pa, d, ip, jp, RESTRCT);
+        }
+  }
+  void mask_edges_if_both_nodes(int l) {  // nodes [0, n)
+    orc_wlevel& g = L(l);
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j < g.n; ++j)
+        for (int i = 0; i < g.n; ++i)
+          if (mn(g, d, i, j) >= ADJZONE) {
+            if (mn(g, d, i + 1, j) >= ADJZONE) se(g, RT, d, i, j, ADJZONE);
+            if (mn(g, d, i + 1, j + 1) >= ADJZONE) se(g, DG, d, i, j, ADJZONE);
+            if (mn(g, d, i, j + 1) >= ADJZONE) se(g, UP, d, i, j, ADJZONE);
+          }
+  }
+  void mask_edges_consist(int l) {  // parents [0, np]
+    orc_wlevel& Pa = L(l);
+    orc_wlevel& C = L(l + 1);
+    for (int d = 0; d < 10; ++d)
+      for (int jp = 0; jp <= Pa.n; ++jp)
+        for (int ip = 0; ip <= Pa.n; ++ip) {
+          const int i = 2 * ip, j = 2 * jp;
+          auto A = [&](int e, int a, int b) { return me(C, e, d, a, b) >= ADJZONE; };
+          if (A(RT, i, j) || A(RT, i + 1, j) || A(DG, i, j - 1) || A(DG, i + 1, j) || A(UP, i + 1, j - 1) || A(UP, i + 1, j)) {
+            se(C, RT, d, i, j, ADJZONE);
+            se(C, RT, d, i + 1, j, ADJZONE);
+            se(Pa, RT, d, ip, jp, ADJZONE);
+          }
+          if (A(RT, i, j + 1) || A(RT, i + 1, j + 1) || A(DG, i, j) || A(DG, i + 1, j + 1) || A(UP, i + 1, j) ||
+              A(UP, i + 1, j + 1)) {
+            se(C, DG, d, i, j, ADJZONE);
+            se(C, DG, d, i + 1, j + 1, ADJZONE);
+            se(Pa, DG, d, ip, jp, ADJZONE);
+          }
+          if (A(RT, i - 1, j + 1) || A(RT, i, j + 1) || A(DG, i - 1, j) || A(DG, i, j + 1) || A(UP, i, j) || A(UP, i, j + 1)) {
+            se(C, UP, d, i, j, ADJZONE);
+            se(C, UP, d, i, j + 1, ADJZONE);
+            se(Pa, UP, d, ip, jp, ADJZONE);
+          }
+        }
+  }
+  void mask_edges_consist2(int l) {  // parents [0, np)
+    orc_wlevel& Pa = L(l);
+    orc_wlevel& C = L(l + 1);
+    for (int d = 0; d < 10; ++d)
+      for (int jp = 0; jp < Pa.n; ++jp)
+        for (int ip = 0; ip < Pa.n; ++ip) {
+          const int i = 2 * ip, j = 2 * jp;
+          auto A = [&](int e, int a, int b) { return me(C, e, d, i + a, j + b) >= ADJZONE; };
+          if (A(RT, -2, -2) || A(RT, 0, -2) || A(RT, 0, 2) || A(RT, 2, 2) || A(DG, -2, -2) || A(DG, 0, -2) || A(DG, 0, 0) ||
+              A(DG, 2, 0) || A(UP, 0, -2) || A(UP, 2, -2) || A(UP, 0, 0) || A(UP, 2, 0))
+            se(Pa, RT, d, ip, jp, ADJZONE);
+          if (A(RT, -2, 0) || A(RT, 0, 0) || A(RT, 0, 2) || A(RT, 2, 2) || A(DG, 0, -2) || A(DG, -2, 0) || A(DG, 2, 0) ||
+              A(DG, 0, 2) || A(UP, 0, -2) || A(UP, 0, 0) || A(UP, 2, 0) || A(UP, 2, 2))
+            se(Pa, DG, d, ip, jp, ADJZONE);
+          if (A(RT, 0, 0) || A(RT, 0, 2) || A(RT, -2, 0) || A(RT, -2, 2) || A(DG, 0, 2) || A(DG, 0, 0) || A(DG, -2, -2) ||
+              A(DG, -2, 0) || A(UP, 2, 0) || A(UP, 2, 2) || A(UP, -2, -2) || A(UP, -2, 0))
+            se(Pa, UP, d, ip, jp, ADJZONE);
+        }
+  }
+  void mask_nodes_if_all_edges(int l) {  // nodes [0, n]
+    orc_wlevel& g = L(l);
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j <= g.n; ++j)
+        for (int i = 0; i <= g.n; ++i)
+          if (me(g, RT, d, i, j) >= ADJZONE && me(g, DG, d, i, j) >= ADJZONE && me(g, UP, d, i, j) >= ADJZONE &&
+              me(g, RT, d, i - 1, j) >= ADJZONE && me(g, DG, d, i - 1, j - 1) >= ADJZONE && me(g, UP, d, i, j - 1) >= ADJZONE)
+            sn(g, d, i, j, ADJZONE);
+  }
+  void prolong_node_adjzone(int l) {  // parents [0, np]
+    orc_wlevel& Pa = L(l);
+    orc_wlevel& C = L(l + 1);
+    for (int d = 0; d < 10; ++d)
+      for (int jp = 0; jp <= Pa.n; ++jp)
+        for (int ip = 0; ip <= Pa.n; ++ip)
+          if (mn(C, d, 2 * ip, 2 * jp) >= ADJZONE) sn(Pa, d, ip, jp, ADJZONE);
+  }
+  void mask_node_trsk(int l) {  // nodes [-2, n+1]: div_grad_stencil (no Laplacian diffusion)
+    orc_wlevel& g = L(l);
+    for (int d = 0; d < 10; ++d)
+      for (int j = -2; j <= g.n + 1; ++j)
+        for (int i = -2; i <= g.n + 1; ++i)
+          if (mn(g, d, i, j) >= ADJZONE) {
+            const int nb[7][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}, {-1, 0}, {-1, -1}, {0, -1}};
+            for (auto& q : nb) sn(g, d, i + q[0], j + q[1], TRSK);
+            se(g, RT, d, i, j, TRSK);
+            se(g, DG, d, i, j, TRSK);
+            se(g, UP, d, i, j, TRSK);
+            se(g, RT, d, i - 1, j, TRSK);
+            se(g, DG, d, i - 1, j - 1, TRSK);
+            se(g, UP, d, i, j - 1, TRSK);
+          }
+  }
+  // check_child_required for every parent patch of level l (patch side ps) and
+  // child quadrant c = 0 NE, 1 SE, 2 SW, 3 NW (chd_offs).
+  void child_required(int l, int ps, uint8_t* out) {
+    const orc_wlevel& g = L(l);
+    const int np = g.n / ps;
+    const int offs[4][2] = {{ps / 2, ps / 2}, {ps / 2, 0}, {0, 0}, {0, ps / 2}};
+    int64_t o = 0;
+    for (int d = 0; d < 10; ++d)
+      for (int pj = 0; pj < np; ++pj)
+        for (int pi = 0; pi < np; ++pi)
+          for (int c = 0; c < 4; ++c) {
+            bool req = false;
+            for (int jj = -2; jj <= ps / 2 + 1 && !req; ++jj)
+              for (int ii = -2; ii <= ps / 2 + 1 && !req; ++ii) {
+                const int i = pi * ps + offs[c][0] + ii, j = pj * ps + offs[c][1] + jj;
+                req = mn(g, d, i, j) >= ADJZONE || me(g, RT, d, i, j) >= RESTRCT || me(g, DG, d, i, j) >= RESTRCT ||
+                      me(g, UP, d, i, j) >= RESTRCT;
+              }
+            out[o++] = req ? 1 : 0;
+          }
+  }
+  // adapt (src/adapt.f90:14-65) without tree surgery: every patch exists.
+  void mask_build(const double* thr, int level_fill, int max_level, int ps, uint8_t* required) {
+    init_masks_zero();
+    // mask_active
+    for (int l = ls; l <= le; ++l) {
+      halo_scalars(l, true);
+      halo_velo(l, true);
+    }
+    mask_tol(le, 0, 1, thr, level_fill);
+    comm_masks();
+    for (int l = le - 1; l >= ls; --l) {
+      mask_tol(l, -1, 2, thr, level_fill);
+      mask_parent_nodes(l);
+      mask_parent_edges(l);
+      comm_masks();
+    }
+    comm_masks();
+    for (int l = ls; l <= le; ++l) mask_adj_same_scale(l);
+    comm_masks();
+    for (int l = ls; l <= (le < max_level - 1 ? le : max_level - 1); ++l) mask_restrict_flux(l);
+    comm_masks();
+    if (required) {
+      uint8_t* o = required;
+      for (int l = ls; l <= le - 1; ++l) {
+        child_required(l, ps, o);
+        o += (int64_t)10 * (L(l).n / ps) * (L(l).n / ps) * 4;
+      }
+    }
+    comm_masks();  // post_refine
+    for (int l = le - 1; l >= ls; --l) {
+      mask_adj_child(l);
+      mask_edges_if_both_nodes(l + 1);
+    }
+    comm_masks();
+    // complete_masks
+    for (int l = le - 1; l >= ls + 1; --l) {
+      mask_edges_consist(l);
+      comm_masks();
+      mask_edges_consist2(l);
+      comm_masks();
+    }
+    if (ls < le) {
+      mask_edges_consist(ls);
+      comm_masks();
+      comm_masks();
+    }
+    for (int l = le - 1; l >= ls + 1; --l) {
+      mask_nodes_if_all_edges(l + 1);
+      prolong_node_adjzone(l);
+    }
+    if (ls + 1 <= le) mask_nodes_if_all_edges(ls + 1);
+    comm_masks();
+    // mask_trsk
+    for (int l = ls; l <= le; ++l) mask_node_trsk(l);
+  }
+
   void wt_after_step() {
     zero_wavelets();
     for (int l = ls; l <= le; ++l) {
@@ -556,6 +887,13 @@ int orc_mask_tol(orc_wlevel* lv, int ls, int le, int nz, const double* threshold
   }
   w.mask_tol(le, 0, 1, threshold, level_fill);
   for (int l = le - 1; l >= ls; --l) w.mask_tol(l, -1, 2, threshold, level_fill);
+  return 0;
+}
+
+int orc_mask_build(orc_wlevel* lv, int ls, int le, int nz, const double* threshold, int level_fill, int max_level,
+                   int patch_size, uint8_t* child_required) {
+  W w{lv, ls, le, nz};
+  w.mask_build(threshold, level_fill, max_level, patch_size, child_required);
   return 0;
 }
 

@@ -31,6 +31,7 @@ def _bind():
     for name in ("orc_wt_forward", "orc_wt_inverse", "orc_compress", "orc_wt_after_step"):
         getattr(L, name).argtypes = [P, C.c_int, C.c_int, C.c_int]
     L.orc_mask_tol.argtypes = [P, C.c_int, C.c_int, C.c_int, _dp, C.c_int]
+    L.orc_mask_build.argtypes = [P, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p]
     return L
 
 
@@ -85,6 +86,16 @@ class Hierarchy:
     def mask_tol(self, threshold, level_fill):
         thr = np.ascontiguousarray(threshold, dtype=np.float64).reshape(3, self.nz)
         self.L.orc_mask_tol(self.arr, self.ls, self.le, self.nz, _p(thr), int(level_fill))
+
+    def mask_build(self, threshold, level_fill, max_level, patch_size=0):
+        thr = np.ascontiguousarray(threshold, dtype=np.float64).reshape(3, self.nz)
+        out = None
+        if patch_size > 0:
+            n = sum(10 * (g.n // patch_size) ** 2 * 4 for g in self.levels[:-1])
+            out = np.zeros(n, dtype=np.uint8)
+        self.L.orc_mask_build(self.arr, self.ls, self.le, self.nz, _p(thr), int(level_fill), int(max_level),
+                              int(patch_size), None if out is None else out.ctypes.data)
+        return out
 
     def compress(self):
         self.L.orc_compress(self.arr, self.ls, self.le, self.nz)

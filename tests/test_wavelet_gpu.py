@@ -139,3 +139,22 @@ def test_compress_and_wt_after_step_match_oracle():
     _compare(levels, orc, dev, NAMES)
     assert dev.status() == 0
     dev.close()
+
+
+@pytest.mark.parametrize("level_fill,scale", [(3, 0.3), (0, 0.05), (4, 1.0)])
+def test_mask_build_matches_oracle_exactly(level_fill, scale):
+    """adapt's mask sequence: every node and edge mask of every level (ghost
+    slots included) and every check_child_required flag equal the oracle's."""
+    levels, orc, dev = _setup(3, 5, 2)
+    _random_fine(levels, orc, dev, 2, seed=61)
+    orc.forward()
+    dev.forward()
+    thr = np.full((3, 2), scale)
+    rq_o = orc.mask_build(thr, level_fill, 6, patch_size=4)
+    rq_d = dev.mask_build(thr, level_fill, 6, patch_size=4)
+    for g in levels:
+        for name in ("mask_n", "mask_e"):
+            assert np.array_equal(dev.download(g.level, name), orc.field(g.level, name)), (g.level, name)
+    assert np.array_equal(rq_d, rq_o)
+    assert rq_o.sum() > 0
+    dev.close()

@@ -126,6 +126,7 @@ _DEVICE_SIGS = {
     "wt_inverse_wt": [_vp],
     "wt_mask_tol_vars": [_vp, _dp, C.c_int],
     "wt_compress": [_vp],
+    "wt_mask_build": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "wt_wt_after_step": [_vp],
     "wt_barotropic_upload": [_vp, _dp, _dp],
     "wt_rhs_elliptic": [_vp, C.c_double, C.c_double],

@@ -453,3 +453,272 @@ __global__ void k_halo_level(int nz, int NN, const int2* __restrict__ hn, int n_
 }
 
 }  // namespace wtw
+
+// ---------------------------------------------------------------------------
+// adapt's mask sequence (src/adapt.f90:14-65, src/mask.f90) on the dense
+// hierarchy.  Each sweep is one kernel over the reference's iteration range;
+// set_at_least is an atomic max.  Within every sweep the conditions read
+// values the sweep cannot change (they test == TOLRNZ, >= TOLRNZ or
+// >= ADJSPACE while the sweep writes lower values, or they read mask classes
+// the sweep does not write), so the parallel sweep equals the sequential one.
+namespace wtw {
+
+constexpr int ADJSPACE = 14, RESTRCT = 12, TRSK = 2;
+
+__device__ __forceinline__ void sat(int* m, int x, int typ) {
+  if (m[x] < typ) atomicMax(m + x, typ);
+}
+__device__ __forceinline__ void sn(const WLev& g, int d, int i, int j, int typ) {
+  if (inr(g, i, j)) sat(g.mask_n, nid(g, d, i, j), typ);
+}
+__device__ __forceinline__ void se(const WLev& g, int e, int d, int i, int j, int typ) {
+  if (inr(g, i, j)) sat(g.mask_e, e * g.NN + nid(g, d, i, j), typ);
+}
+// thread -> (lozenge, i, j) over [st, m-1+st]^2
+__device__ __forceinline__ bool node_of(int m, int st, int& d, int& i, int& j) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return false;
+  d = t / (m * m);
+  const int r = t - d * m * m;
+  j = r / m + st;
+  i = r % m + st;
+  return true;
+}
+
+// serial comm_masks_mpi (src/comm.f90:531-553): node and edge masks to their
+// ghost copies (the tables have no chains, so the copy order is immaterial).
+__global__ void k_mask_halo(WLev g, const int2* __restrict__ hn, int n_hn, const int3* __restrict__ he, int n_he) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n_hn) {
+    g.mask_n[hn[t].x] = g.mask_n[hn[t].y];
+  } else if (t < n_hn + n_he) {
+    const int3 e = he[t - n_hn];
+    g.mask_e[e.x] = g.mask_e[e.y];
+  }
+}
+
+__global__ void k_mask_zero(WLev g) {  // init_masks_zero on one level
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < g.NN) g.mask_n[t] = ZERO;
+  if (t < 3 * g.NN) g.mask_e[t] = ZERO;
+}
+
+// mask_parent_nodes (parents [0, np]) and mask_parent_edges (parents [0, np))
+__global__ void k_mask_parent(WLev Pa, WLev C) {
+  int d, ip, jp;
+  if (!node_of(Pa.n + 1, 0, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  if (mn(C, d, i + 1, j) == TOLRNZ || mn(C, d, i + 1, j + 1) == TOLRNZ || mn(C, d, i, j + 1) == TOLRNZ ||
+      mn(C, d, i - 1, j) == TOLRNZ || mn(C, d, i - 1, j - 1) == TOLRNZ || mn(C, d, i, j - 1) == TOLRNZ) {
+    sn(Pa, d, ip, jp, TOLRNZ);
+    sn(C, d, i, j, TOLRNZ);
+  }
+  if (ip == Pa.n || jp == Pa.n) return;
+  auto T = [&](int e, int a, int b) { return me(C, e, d, a, b) == TOLRNZ; };
+  if (T(RT, i, j) || T(RT, i + 1, j) || T(DG, i, j - 1) || T(DG, i + 1, j) || T(UP, i + 1, j) || T(UP, i + 1, j - 1))
+    se(Pa, RT, d, ip, jp, TOLRNZ);
+  if (T(RT, i, j + 1) || T(RT, i + 1, j + 1) || T(DG, i, j) || T(DG, i + 1, j + 1) || T(UP, i + 1, j + 1) || T(UP, i + 1, j))
+    se(Pa, DG, d, ip, jp, TOLRNZ);
+  if (T(RT, i, j + 1) || T(RT, i - 1, j + 1) || T(DG, i, j + 1) || T(DG, i - 1, j) || T(UP, i, j) || T(UP, i, j + 1))
+    se(Pa, UP, d, ip, jp, TOLRNZ);
+}
+
+// mask_adj_same_scale_nodes_edges, nodes [0, n]
+__global__ void k_mask_adj_same(WLev g) {
+  int d, i, j;
+  if (!node_of(g.n + 1, 0, d, i, j)) return;
+  if (mn(g, d, i + 1, j) == TOLRNZ || mn(g, d, i + 1, j + 1) == TOLRNZ || mn(g, d, i, j + 1) == TOLRNZ ||
+      mn(g, d, i - 1, j) == TOLRNZ || mn(g, d, i - 1, j - 1) == TOLRNZ || mn(g, d, i, j - 1) == TOLRNZ)
+    sn(g, d, i, j, ADJSPACE);
+  auto T = [&](int e, int a, int b) { return me(g, e, d, a, b) == TOLRNZ; };
+  if (T(DG, i, j) || T(UP, i, j - 1) || T(DG, i, j - 1) || T(UP, i + 1, j)) se(g, RT, d, i, j, ADJSPACE);
+  if (T(UP, i, j) || T(RT, i, j) || T(UP, i + 1, j) || T(RT, i, j + 1)) se(g, DG, d, i, j, ADJSPACE);
+  if (T(DG, i, j) || T(RT, i - 1, j) || T(DG, i - 1, j) || T(RT, i, j + 1)) se(g, UP, d, i, j, ADJSPACE);
+}
+
+// mask_restrict_flux, nodes [0, n)
+__global__ void k_mask_restrict_flux(WLev g) {
+  int d, i, j;
+  if (!node_of(g.n, 0, d, i, j)) return;
+  if (mn(g, d, i, j) >= ADJSPACE) {
+    se(g, RT, d, i, j, RESTRCT);
+    se(g, DG, d, i, j, RESTRCT);
+    se(g, UP, d, i, j, RESTRCT);
+  } else {
+    if (mn(g, d, i + 1, j) >= ADJSPACE) se(g, RT, d, i, j, RESTRCT);
+    if (mn(g, d, i + 1, j + 1) >= ADJSPACE) se(g, DG, d, i, j, RESTRCT);
+    if (mn(g, d, i, j + 1) >= ADJSPACE) se(g, UP, d, i, j, RESTRCT);
+  }
+}
+
+// mask_adj_child, parents [0, np]
+__global__ void k_mask_adj_child(WLev Pa, WLev C) {
+  int d, ip, jp;
+  if (!node_of(Pa.n + 1, 0, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  auto PE = [&](int e, int a, int b, int typ) { return me(Pa, e, d, a, b) >= typ; };
+  if (mn(Pa, d, ip, jp) >= TOLRNZ) {
+    const int nb[13][2] = {{0, 0},  {1, 0},  {1, 1}, {0, 1}, {-1, 0},  {-1, -1}, {0, -1},
+                           {-1, 1}, {1, -1}, {2, 1}, {1, 2}, {-1, -2}, {-2, -1}};
+    for (int q = 0; q < 13; ++q) sn(C, d, i + nb[q][0], j + nb[q][1], ADJZONE);
+    se(Pa, UP, d, ip, jp, RESTRCT);
+    se(Pa, DG, d, ip, jp, RESTRCT);
+    se(Pa, RT, d, ip, jp, RESTRCT);
+  } else {
+    if (mn(Pa, d, ip, jp + 1) >= TOLRNZ) {
+      sn(C, d, i, j + 1, ADJZONE);
+      se(Pa, UP, d, ip, jp, RESTRCT);
+    }
+    if (mn(Pa, d, ip + 1, jp + 1) >= TOLRNZ) {
+      sn(C, d, i + 1, j + 1, ADJZONE);
+      se(Pa, DG, d, ip, jp, RESTRCT);
+    }
+    if (mn(Pa, d, ip + 1, jp) >= TOLRNZ) {
+      sn(C, d, i + 1, j, ADJZONE);
+      se(Pa, RT, d, ip, jp, RESTRCT);
+    }
+  }
+  if (PE(UP, ip, jp, TOLRNZ)) {
+    sn(C, d, i, j + 1, ADJZONE);
+    if (PE(UP, ip, jp - 1, TOLRNZ)) sn(C, d, i, j, ADJZONE);
+  }
+  if (PE(DG, ip, jp, TOLRNZ)) {
+    sn(C, d, i + 1, j + 1, ADJZONE);
+    if (PE(DG, ip - 1, jp - 1, TOLRNZ)) sn(C, d, i, j, ADJZONE);
+  }
+  if (PE(RT, ip, jp, TOLRNZ)) {
+    sn(C, d, i + 1, j, ADJZONE);
+    if (PE(RT, ip - 1, jp, TOLRNZ)) sn(C, d, i, j, ADJZONE);
+  }
+  if (PE(UP, ip, jp, TOLRNZ) || PE(DG, ip, jp, TOLRNZ) || PE(RT, ip - 1, jp, TOLRNZ) || PE(DG, ip - 1, jp, TOLRNZ) ||
+      PE(RT, ip, jp + 1, TOLRNZ)) {
+    se(C, UP, d, i, j, ADJZONE);
+    se(C, UP, d, i, j + 1, ADJZONE);
+  }
+  if (PE(DG, ip, jp, TOLRNZ) || PE(UP, ip, jp, TOLRNZ) || PE(RT, ip, jp, TOLRNZ) || PE(UP, ip + 1, jp, TOLRNZ) ||
+      PE(RT, ip, jp + 1, TOLRNZ)) {
+    se(C, DG, d, i, j, ADJZONE);
+    se(C, DG, d, i + 1, j + 1, ADJZONE);
+  }
+  if (PE(RT, ip, jp, TOLRNZ) || PE(DG, ip, jp, TOLRNZ) || PE(UP, ip, jp - 1, TOLRNZ) || PE(DG, ip, jp - 1, TOLRNZ) ||
+      PE(UP, ip + 1, jp, TOLRNZ)) {
+    se(C, RT, d, i, j, ADJZONE);
+    se(C, RT, d, i + 1, j, ADJZONE);
+  }
+  if (PE(UP, ip, jp, TOLRNZ) || PE(DG, ip, jp, TOLRNZ) || PE(RT, ip, jp + 1, TOLRNZ)) {
+    se(C, RT, d, i, j + 1, ADJZONE);
+    se(C, DG, d, i, j + 1, ADJZONE);
+    se(C, UP, d, i + 1, j + 1, ADJZONE);
+  }
+  if (PE(RT, ip, jp, TOLRNZ) || PE(DG, ip, jp, TOLRNZ) || PE(UP, ip + 1, jp, TOLRNZ)) {
+    se(C, UP, d, i + 1, j, ADJZONE);
+    se(C, DG, d, i + 1, j, ADJZONE);
+    se(C, RT, d, i + 1, j + 1, ADJZONE);
+  }
+  if (PE(RT, ip, jp, ADJSPACE) || PE(DG, ip, jp, ADJSPACE) || PE(UP, ip, jp, ADJSPACE) || PE(RT, ip - 1, jp, ADJSPACE) ||
+      PE(DG, ip - 1, jp - 1, ADJSPACE) || PE(UP, ip, jp - 1, ADJSPACE))
+    sn(Pa, d, ip, jp, RESTRCT);
+}
+
+// mask_edges_if_both_nodes, nodes [0, n)
+__global__ void k_mask_edges_both(WLev g) {
+  int d, i, j;
+  if (!node_of(g.n, 0, d, i, j)) return;
+  if (mn(g, d, i, j) >= ADJZONE) {
+    if (mn(g, d, i + 1, j) >= ADJZONE) se(g, RT, d, i, j, ADJZONE);
+    if (mn(g, d, i + 1, j + 1) >= ADJZONE) se(g, DG, d, i, j, ADJZONE);
+    if (mn(g, d, i, j + 1) >= ADJZONE) se(g, UP, d, i, j, ADJZONE);
+  }
+}
+
+// mask_edges_consist, parents [0, np]
+__global__ void k_mask_edges_consist(WLev Pa, WLev C) {
+  int d, ip, jp;
+  if (!node_of(Pa.n + 1, 0, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  auto A = [&](int e, int a, int b) { return me(C, e, d, a, b) >= ADJZONE; };
+  if (A(RT, i, j) || A(RT, i + 1, j) || A(DG, i, j - 1) || A(DG, i + 1, j) || A(UP, i + 1, j - 1) || A(UP, i + 1, j)) {
+    se(C, RT, d, i, j, ADJZONE);
+    se(C, RT, d, i + 1, j, ADJZONE);
+    se(Pa, RT, d, ip, jp, ADJZONE);
+  }
+  if (A(RT, i, j + 1) || A(RT, i + 1, j + 1) || A(DG, i, j) || A(DG, i + 1, j + 1) || A(UP, i + 1, j) || A(UP, i + 1, j + 1)) {
+    se(C, DG, d, i, j, ADJZONE);
+    se(C, DG, d, i + 1, j + 1, ADJZONE);
+    se(Pa, DG, d, ip, jp, ADJZONE);
+  }
+  if (A(RT, i - 1, j + 1) || A(RT, i, j + 1) || A(DG, i - 1, j) || A(DG, i, j + 1) || A(UP, i, j) || A(UP, i, j + 1)) {
+    se(C, UP, d, i, j, ADJZONE);
+    se(C, UP, d, i, j + 1, ADJZONE);
+    se(Pa, UP, d, ip, jp, ADJZONE);
+  }
+}
+
+// mask_edges_consist2, parents [0, np)
+__global__ void k_mask_edges_consist2(WLev Pa, WLev C) {
+  int d, ip, jp;
+  if (!node_of(Pa.n, 0, d, ip, jp)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  auto A = [&](int e, int a, int b) { return me(C, e, d, i + a, j + b) >= ADJZONE; };
+  if (A(RT, -2, -2) || A(RT, 0, -2) || A(RT, 0, 2) || A(RT, 2, 2) || A(DG, -2, -2) || A(DG, 0, -2) || A(DG, 0, 0) ||
+      A(DG, 2, 0) || A(UP, 0, -2) || A(UP, 2, -2) || A(UP, 0, 0) || A(UP, 2, 0))
+    se(Pa, RT, d, ip, jp, ADJZONE);
+  if (A(RT, -2, 0) || A(RT, 0, 0) || A(RT, 0, 2) || A(RT, 2, 2) || A(DG, 0, -2) || A(DG, -2, 0) || A(DG, 2, 0) ||
+      A(DG, 0, 2) || A(UP, 0, -2) || A(UP, 0, 0) || A(UP, 2, 0) || A(UP, 2, 2))
+    se(Pa, DG, d, ip, jp, ADJZONE);
+  if (A(RT, 0, 0) || A(RT, 0, 2) || A(RT, -2, 0) || A(RT, -2, 2) || A(DG, 0, 2) || A(DG, 0, 0) || A(DG, -2, -2) ||
+      A(DG, -2, 0) || A(UP, 2, 0) || A(UP, 2, 2) || A(UP, -2, -2) || A(UP, -2, 0))
+    se(Pa, UP, d, ip, jp, ADJZONE);
+}
+
+// mask_nodes_if_all_edges, nodes [0, n]
+__global__ void k_mask_nodes_all(WLev g) {
+  int d, i, j;
+  if (!node_of(g.n + 1, 0, d, i, j)) return;
+  if (me(g, RT, d, i, j) >= ADJZONE && me(g, DG, d, i, j) >= ADJZONE && me(g, UP, d, i, j) >= ADJZONE &&
+      me(g, RT, d, i - 1, j) >= ADJZONE && me(g, DG, d, i - 1, j - 1) >= ADJZONE && me(g, UP, d, i, j - 1) >= ADJZONE)
+    sn(g, d, i, j, ADJZONE);
+}
+
+// prolong_node_adjzone, parents [0, np]
+__global__ void k_mask_prolong_adj(WLev Pa, WLev C) {
+  int d, ip, jp;
+  if (!node_of(Pa.n + 1, 0, d, ip, jp)) return;
+  if (mn(C, d, 2 * ip, 2 * jp) >= ADJZONE) sn(Pa, d, ip, jp, ADJZONE);
+}
+
+// mask_node_trsk with div_grad_stencil (no Laplacian diffusion), nodes [-2, n+1]
+__global__ void k_mask_trsk(WLev g) {
+  int d, i, j;
+  if (!node_of(g.n + 4, -2, d, i, j)) return;
+  if (mn(g, d, i, j) < ADJZONE) return;
+  const int nb[7][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}, {-1, 0}, {-1, -1}, {0, -1}};
+  for (int q = 0; q < 7; ++q) sn(g, d, i + nb[q][0], j + nb[q][1], TRSK);
+  se(g, RT, d, i, j, TRSK);
+  se(g, DG, d, i, j, TRSK);
+  se(g, UP, d, i, j, TRSK);
+  se(g, RT, d, i - 1, j, TRSK);
+  se(g, DG, d, i - 1, j - 1, TRSK);
+  se(g, UP, d, i, j - 1, TRSK);
+}
+
+// check_child_required (src/refine_patch.f90:289-327): one flag per (lozenge,
+// parent patch of side ps, child quadrant c = 0 NE, 1 SE, 2 SW, 3 NW).
+__global__ void k_child_required(WLev g, int ps, unsigned char* __restrict__ out) {
+  const int np = g.n / ps;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * np * np * 4) return;
+  const int c = t % 4, r = t / 4;
+  const int pi = r % np, pj = (r / np) % np, d = r / (np * np);
+  const int ox = (c == 0 || c == 1) ? ps / 2 : 0, oy = (c == 0 || c == 3) ? ps / 2 : 0;
+  bool req = false;
+  for (int jj = -2; jj <= ps / 2 + 1 && !req; ++jj)
+    for (int ii = -2; ii <= ps / 2 + 1 && !req; ++ii) {
+      const int i = pi * ps + ox + ii, j = pj * ps + oy + jj;
+      req = mn(g, d, i, j) >= ADJZONE || me(g, RT, d, i, j) >= RESTRCT || me(g, DG, d, i, j) >= RESTRCT ||
+            me(g, UP, d, i, j) >= RESTRCT;
+    }
+  out[t] = req ? 1 : 0;
+}
+
+}  // namespace wtw

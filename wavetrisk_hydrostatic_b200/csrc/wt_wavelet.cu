@@ -4,6 +4,7 @@
 // copies (update_bdry) are replaced by the kernels' remapped reads.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <vector>
 
@@ -246,6 +247,92 @@ int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill) {
   }
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+namespace {
+void comm_masks(wt_handle* h) {
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    const DevLevel& D = h->at(l);
+    k_mask_halo<<<nb(D.n_hn + D.n_he), TPB, 0, h->stream>>>(view(h, l), D.hn, D.n_hn, D.he, D.n_he);
+  }
+}
+inline unsigned nodes_blocks(int m) { return nb((int64_t)10 * m * m); }
+}  // namespace
+
+// adapt (src/adapt.f90:14-65) without tree surgery, on the dense hierarchy.
+int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max_level, int patch_size,
+                  unsigned char* child_required) {
+  if (int rc = ready(h)) return rc;
+  const int ls = h->level_start, le = h->level_end, nz = h->nz;
+  if (!threshold) return WT_ERR_ARG;
+  if (child_required && (patch_size < 2 || (patch_size & 1) || h->at(ls).n % patch_size)) return WT_ERR_ARG;
+  WavCtx* W = ctx(h);
+  cudaStream_t s = h->stream;
+  CKW(cudaMemcpyAsync(W->thr, threshold, 3 * nz * sizeof(double), cudaMemcpyHostToDevice, s));
+  for (int l = ls + 1; l <= le; ++l) k_mask_zero<<<nb(3 * h->at(l).NN), TPB, 0, s>>>(view(h, l));
+  // mask_active
+  auto tol = [&](int l, int st, int en) {
+    const int m = h->at(l).n + en - st;
+    k_mask_tol<<<nb((int64_t)10 * m * m), TPB, 0, s>>>(view(h, l), nz, st, en, W->thr, l < level_fill ? 1 : 0);
+  };
+  tol(le, 0, 1);
+  comm_masks(h);
+  for (int l = le - 1; l >= ls; --l) {
+    tol(l, -1, 2);
+    k_mask_parent<<<nodes_blocks(h->at(l).n + 1), TPB, 0, s>>>(view(h, l), view(h, l + 1));
+    comm_masks(h);
+  }
+  comm_masks(h);
+  for (int l = ls; l <= le; ++l) k_mask_adj_same<<<nodes_blocks(h->at(l).n + 1), TPB, 0, s>>>(view(h, l));
+  comm_masks(h);
+  for (int l = ls; l <= std::min(le, max_level - 1); ++l)
+    k_mask_restrict_flux<<<nodes_blocks(h->at(l).n), TPB, 0, s>>>(view(h, l));
+  comm_masks(h);
+  unsigned char* dreq = nullptr;
+  int64_t nreq = 0;
+  if (child_required) {
+    for (int l = ls; l <= le - 1; ++l) nreq += (int64_t)10 * (h->at(l).n / patch_size) * (h->at(l).n / patch_size) * 4;
+    if (nreq > 0) {
+      CKW(cudaMalloc(&dreq, nreq));
+      int64_t o = 0;
+      for (int l = ls; l <= le - 1; ++l) {
+        const int64_t cnt = (int64_t)10 * (h->at(l).n / patch_size) * (h->at(l).n / patch_size) * 4;
+        k_child_required<<<nb(cnt), TPB, 0, s>>>(view(h, l), patch_size, dreq + o);
+        o += cnt;
+      }
+    }
+  }
+  comm_masks(h);  // post_refine
+  for (int l = le - 1; l >= ls; --l) {
+    k_mask_adj_child<<<nodes_blocks(h->at(l).n + 1), TPB, 0, s>>>(view(h, l), view(h, l + 1));
+    k_mask_edges_both<<<nodes_blocks(h->at(l + 1).n), TPB, 0, s>>>(view(h, l + 1));
+  }
+  comm_masks(h);
+  // complete_masks
+  for (int l = le - 1; l >= ls + 1; --l) {
+    k_mask_edges_consist<<<nodes_blocks(h->at(l).n + 1), TPB, 0, s>>>(view(h, l), view(h, l + 1));
+    comm_masks(h);
+    k_mask_edges_consist2<<<nodes_blocks(h->at(l).n), TPB, 0, s>>>(view(h, l), view(h, l + 1));
+    comm_masks(h);
+  }
+  if (ls < le) {
+    k_mask_edges_consist<<<nodes_blocks(h->at(ls).n + 1), TPB, 0, s>>>(view(h, ls), view(h, ls + 1));
+    comm_masks(h);
+  }
+  for (int l = le - 1; l >= ls + 1; --l) {
+    k_mask_nodes_all<<<nodes_blocks(h->at(l + 1).n + 1), TPB, 0, s>>>(view(h, l + 1));
+    k_mask_prolong_adj<<<nodes_blocks(h->at(l).n + 1), TPB, 0, s>>>(view(h, l), view(h, l + 1));
+  }
+  if (ls + 1 <= le) k_mask_nodes_all<<<nodes_blocks(h->at(ls + 1).n + 1), TPB, 0, s>>>(view(h, ls + 1));
+  comm_masks(h);
+  // mask_trsk
+  for (int l = ls; l <= le; ++l) k_mask_trsk<<<nodes_blocks(h->at(l).n + 4), TPB, 0, s>>>(view(h, l));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && dreq) e = cudaMemcpy(child_required, dreq, nreq, cudaMemcpyDeviceToHost);
+  if (dreq) cudaFree(dreq);
+  if (e != cudaSuccess) return fail("mask_build", e);
   return WT_OK;
 }
 

@@ -183,6 +183,18 @@ class WaveletHierarchy(DeviceGrid):
         thr = _c(np.asarray(threshold).reshape(3, self.nz))
         N.check("wt_mask_tol_vars", N.lib().wt_mask_tol_vars(self.h, N.dptr(thr), int(level_fill)))
 
+    def mask_build(self, threshold: np.ndarray, level_fill: int, max_level: int, patch_size: int = 0):
+        """adapt's mask sequence; returns the check_child_required flags (uint8)
+        of every parent patch and child quadrant when patch_size > 0."""
+        thr = _c(np.asarray(threshold).reshape(3, self.nz))
+        out = None
+        if patch_size > 0:
+            n = sum(10 * (g.n // patch_size) ** 2 * 4 for g in self.levels[:-1])
+            out = np.zeros(n, dtype=np.uint8)
+        N.check("wt_mask_build", N.lib().wt_mask_build(self.h, N.dptr(thr), int(level_fill), int(max_level),
+                                                       int(patch_size), None if out is None else out.ctypes.data))
+        return out
+
     def compress(self) -> None:
         N.check("wt_compress", N.lib().wt_compress(self.h))
 

@@ -253,6 +253,13 @@ int wt_rhs_elliptic(wt_handle* h, double dt, double theta2);
 /* grad_eta (src/barotropic_2d.f90:455-474: step1 itype 3, g grad eta) and
  * u_update (:131-149): velo_k -= theta1 dt grad eta on every layer. */
 int wt_u_update(wt_handle* h, double dt, double theta1);
+/* step1 with itype 1 (scalar gradient flux), 5 (u pedlen), 6 (surface pressure
+ * flux) or 7 (mass flux) on one layer of the resident state
+ * (src/ops.f90:198-262, comp_SW :396-455): flux (3*NN host doubles) at the
+ * edges of nodes [0, n]^2 and the south/west ghost edges; scalar (NN host
+ * doubles) is the node field of itypes 1 and 6 (NULL otherwise).  Uses the
+ * barotropic work buffers, so it overwrites the last rhs and grad. */
+int wt_step1_flux(wt_handle* h, int itype, int layer, const double* scalar, double* flux);
 /* div_flux (NN), rhs (NN), grad (3*NN); any may be NULL. */
 int wt_barotropic_download(wt_handle* h, double* div_flux, double* rhs, double* grad);
 

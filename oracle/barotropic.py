@@ -50,3 +50,16 @@ def u_update(g, nz, grav, eta, velo, dt, theta1):
     L.orc_u_update.argtypes = [C.POINTER(orc_blevel), C.c_int, C.c_double, _dp, C.c_double, C.c_double, _dp, _dp]
     L.orc_u_update(C.byref(lv.s), nz, grav, _p(e), dt, theta1, _p(v), _p(grad))
     return v, grad
+
+
+def step1_flux(g, itype, velo, mass, mean_m, scalar=None):
+    """step1 itype 1, 5, 6 or 7 on one layer: returns the edge flux (3*NN)."""
+    L = lib()
+    lv = _Level(g)
+    flux = np.zeros(3 * g.NN)
+    bufs = [None if scalar is None else _c(scalar), _c(velo), _c(mass), _c(mean_m)]
+    L.orc_step1_flux.argtypes = [C.POINTER(orc_blevel), C.c_int, _dp, _dp, _dp, _dp, _dp]
+    L.orc_step1_flux.restype = C.c_int
+    rc = L.orc_step1_flux(C.byref(lv.s), int(itype), *[None if b is None else _p(b) for b in bufs], _p(flux))
+    assert rc == 0
+    return flux

@@ -10,6 +10,7 @@
 //   grad_eta (one level)                      src/barotropic_2d.f90:455-474
 //   step1 itype 3 (comput :225-228, comp_SW :416-419), porosity 1   src/ops.f90
 //   u_update                                  src/barotropic_2d.f90:131-149
+//   step1 itypes 1, 5, 6, 7 (comput :198-262, comp_SW :396-455)     src/ops.f90
 // step1 visits nodes [0, n]^2 of each lozenge and runs comp_SW on the south
 // and west borders; update_bdry is the level's ghost copy.  u_update is
 // applied to the edges grad_eta writes (the reference's element range also
@@ -158,6 +159,73 @@ int orc_u_update(const orc_blevel* Lp, int nz, double grav, const double* eta, d
   for (int k = 0; k < nz; ++k)
     for (int64_t x = 0; x < 3 * NN; ++x)
       if (written[x]) velo[3 * k * NN + x] = velo[3 * k * NN + x] - s * grad[x];
+  return 0;
+}
+
+// One layer: s (NN, itypes 1 and 6), v (3*NN), mass, mean_m (NN); flux (3*NN out).
+int orc_step1_flux(const orc_blevel* Lp, int itype, const double* s_in, const double* v_in, const double* m_in,
+                   const double* mean_m, double* flux) {
+  const orc_blevel& L = *Lp;
+  B b{L};
+  const int64_t NN = L.NN;
+  const int P = L.P;
+  std::vector<double> s(NN, 0.0), v(v_in, v_in + 3 * NN), m(m_in, m_in + NN);
+  if (s_in) s.assign(s_in, s_in + NN);
+  b.halo_n(s.data());
+  b.halo_n(m.data());
+  b.halo_e(v.data());
+  std::memset(flux, 0, 3 * NN * sizeof(double));
+  const double* ped = L.pedlen;
+  const double* len = L.len;
+  for (int d = 0; d < 10; ++d)
+    for (int j = 0; j <= L.n; ++j)
+      for (int i = 0; i <= L.n; ++i) {
+        const int64_t id = b.id(d, i, j);
+        const int64_t idE = id + 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idS = id - P, idSW = id - P - 1;
+        const int64_t rt = RT * NN + id, dg = DG * NN + id, up = UP * NN + id;
+        const int64_t wrt = RT * NN + idW, swdg = DG * NN + idSW, sup = UP * NN + idS;
+        const bool sw = (i == 0 || j == 0);
+        if (itype == 1) {
+          flux[rt] = (s[idE] - s[id]) / len[rt] * ped[rt];
+          flux[dg] = (s[id] - s[idNE]) / len[dg] * ped[dg];
+          flux[up] = (s[idN] - s[id]) / len[up] * ped[up];
+          if (sw) {
+            flux[wrt] = -((s[idW] - s[id]) / len[wrt] * ped[wrt]);
+            flux[swdg] = -((s[id] - s[idSW]) / len[swdg] * ped[swdg]);
+            flux[sup] = -((s[idS] - s[id]) / len[sup] * ped[sup]);
+          }
+        } else if (itype == 5) {
+          flux[rt] = v[rt] * ped[rt];
+          flux[dg] = v[dg] * ped[dg];
+          flux[up] = v[up] * ped[up];
+          if (sw) {
+            flux[wrt] = v[wrt] * ped[wrt];
+            flux[swdg] = v[swdg] * ped[swdg];
+            flux[sup] = v[sup] * ped[sup];
+          }
+        } else if (itype == 6) {
+          flux[rt] = (s[idE] - s[id]) * v[rt] * ped[rt] / 4.0;
+          flux[dg] = (s[id] - s[idNE]) * v[dg] * ped[dg] / 4.0;
+          flux[up] = (s[idN] - s[id]) * v[up] * ped[up] / 4.0;
+          if (sw) {
+            flux[wrt] = -((s[idW] - s[id]) * v[wrt] * ped[wrt] / 4.0);
+            flux[swdg] = -((s[id] - s[idSW]) * v[swdg] * ped[swdg] / 4.0);
+            flux[sup] = -((s[idS] - s[id]) * v[sup] * ped[sup] / 4.0);
+          }
+        } else if (itype == 7) {
+          const double dz0 = m[id] + mean_m[id];
+          flux[rt] = v[rt] * ped[rt] * interp(dz0, m[idE] + mean_m[idE]);
+          flux[dg] = v[dg] * ped[dg] * interp(dz0, m[idNE] + mean_m[idNE]);
+          flux[up] = v[up] * ped[up] * interp(dz0, m[idN] + mean_m[idN]);
+          if (sw) {
+            flux[wrt] = v[wrt] * ped[wrt] * interp(dz0, m[idW] + mean_m[idW]);
+            flux[swdg] = v[swdg] * ped[swdg] * interp(dz0, m[idSW] + mean_m[idSW]);
+            flux[sup] = v[sup] * ped[sup] * interp(dz0, m[idS] + mean_m[idS]);
+          }
+        } else {
+          return -1;
+        }
+      }
   return 0;
 }
 

@@ -50,3 +50,22 @@ def test_rhs_elliptic_and_u_update_match_oracle(level, nz):
     halo_edges(g, ov)        # u_update leaves the ghosts stale; the next update_bdry copies them
     assert rel(v[:, e], ov[:, e]) <= TOL
     model.close()
+
+
+@pytest.mark.parametrize("itype", [1, 5, 6, 7])
+def test_step1_flux_itypes_match_oracle(itype):
+    level, nz = 5, 2
+    g = Grid(level, level, radius=6371e3).level(level)
+    ph = OceanParams()
+    st = jet_state(g, nz, seed=9, ph=ph)
+    s = np.random.default_rng(itype).standard_normal(g.NN)
+    halo_nodes(g, s)
+    model = TriskModel(g, nz, st["topo"], ph)
+    model.upload(st)
+    k = nz - 1
+    f = model.step1_flux(itype, k, s if itype in (1, 6) else None)
+    of = ob.step1_flux(g, itype, st["velo"][k], st["mass"][k], st["mean_m"][k], s if itype in (1, 6) else None)
+    own = np.nonzero(g.owned)[0]
+    e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+    assert rel(f[e], of[e]) <= TOL
+    model.close()

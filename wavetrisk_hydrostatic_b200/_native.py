@@ -132,6 +132,7 @@ _DEVICE_SIGS = {
     "wt_rhs_elliptic": [_vp, C.c_double, C.c_double],
     "wt_u_update": [_vp, C.c_double, C.c_double],
     "wt_barotropic_download": [_vp, _dp, _dp, _dp],
+    "wt_step1_flux": [_vp, C.c_int, C.c_int, _dp, _dp],
 }
 
 

@@ -155,3 +155,70 @@ __global__ void k_grad_eta_update(LevelDev L, int nz, double grav, const double*
 }
 
 }  // namespace wtb
+
+namespace wtb {
+
+// step1 itypes 1, 5, 6, 7 (src/ops.f90:198-201, 245-262; comp_SW :396-401,
+// 438-455) on one layer, at the edges of nodes [0, n]^2 and at the
+// south/west ghost edges comp_SW owns (once each, as in k_flux_sum):
+//   1  scalar gradient flux   (s_far - s_near) / len * pedlen
+//   5  divu flux              u * pedlen
+//   6  surface pressure flux  (s_far - s_near) * u * pedlen / 4
+//   7  mass flux              u * pedlen * interp(rho dz)
+template <int ITYPE>
+__global__ void k_step1_flux(LevelDev L, const double* __restrict__ s, const double* __restrict__ v,
+                             const double* __restrict__ mass, const double* __restrict__ mean_m,
+                             double* __restrict__ hflux) {
+  const int m = L.n + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  const int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
+  const int P = L.P, NN = L.NN;
+  const int id = (d * P + j + 2) * P + i + 2;
+  const Rd R(L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2);
+  // comput: edge e of node id towards node nb; the scalar difference is
+  // s(nb) - s(id) for RT and UP, s(id) - s(nb) for DG
+  auto comput = [&](int e, int nb) {
+    const int slot = e * NN + id;
+    if (ITYPE == 1) {
+      const double dsc = (e == DG) ? R.n(s, id) - R.n(s, nb) : R.n(s, nb) - R.n(s, id);
+      hflux[slot] = dsc / L.len[slot] * L.pedlen[slot];
+    } else if (ITYPE == 5) {
+      hflux[slot] = R.e(v, slot) * L.pedlen[slot];
+    } else if (ITYPE == 6) {
+      const double dsc = (e == DG) ? R.n(s, id) - R.n(s, nb) : R.n(s, nb) - R.n(s, id);
+      hflux[slot] = dsc * R.e(v, slot) * L.pedlen[slot] / 4.0;
+    } else {
+      const double dz0 = R.n(mass, id) + mean_m[id];
+      const double dz = interp(dz0, R.n(mass, nb) + mean_m[nb]);
+      hflux[slot] = R.e(v, slot) * L.pedlen[slot] * dz;
+    }
+  };
+  comput(RT, id + 1);
+  comput(DG, id + P + 1);
+  comput(UP, id + P);
+  if (!(i == 0 || j == 0)) return;
+  // comp_SW: edge e of the ghost node g, which joins g and id; the scalar
+  // difference is -(s(g) - s(id)) for RT and UP, -(s(id) - s(g)) for DG
+  auto comp_sw = [&](int e, int g) {
+    const int slot = e * NN + g;
+    if (ITYPE == 1) {
+      const double dsc = (e == DG) ? R.n(s, id) - R.n(s, g) : R.n(s, g) - R.n(s, id);
+      hflux[slot] = -(dsc / L.len[slot] * L.pedlen[slot]);
+    } else if (ITYPE == 5) {
+      hflux[slot] = R.e(v, slot) * L.pedlen[slot];
+    } else if (ITYPE == 6) {
+      const double dsc = (e == DG) ? R.n(s, id) - R.n(s, g) : R.n(s, g) - R.n(s, id);
+      hflux[slot] = -(dsc * R.e(v, slot) * L.pedlen[slot] / 4.0);
+    } else {
+      const double dz0 = R.n(mass, id) + mean_m[id];
+      const double dz = interp(dz0, R.n(mass, g) + mean_m[g]);
+      hflux[slot] = R.e(v, slot) * L.pedlen[slot] * dz;
+    }
+  };
+  if (i == 0) comp_sw(RT, id - 1);
+  comp_sw(DG, id - P - 1);
+  if (!(i == 0 && j > 0)) comp_sw(UP, id - P);
+}
+
+}  // namespace wtb

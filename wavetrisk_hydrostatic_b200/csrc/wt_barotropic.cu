@@ -94,6 +94,34 @@ int wt_u_update(wt_handle* h, double dt, double theta1) {
   return WT_OK;
 }
 
+int wt_step1_flux(wt_handle* h, int itype, int layer, const double* scalar, double* flux) {
+  if (!h || !flux || layer < 0 || layer >= h->nz) return WT_ERR_ARG;
+  if (itype != 1 && itype != 5 && itype != 6 && itype != 7) return WT_ERR_ARG;
+  if ((itype == 1 || itype == 6) && !scalar) return WT_ERR_ARG;
+  if (int rc = ensure(h)) return rc;
+  BaroCtx* B = static_cast<BaroCtx*>(h->baro);
+  const DevLevel& D = h->top();
+  const wtk::LevelDev L = D.view();
+  const size_t NN = (size_t)D.NN;
+  const int64_t ko = (int64_t)layer * D.NN;
+  if (scalar) CKB(cudaMemcpyAsync(B->rhs, scalar, NN * 8, cudaMemcpyHostToDevice, h->stream));
+  CKB(cudaMemsetAsync(B->grad, 0, 3 * NN * 8, h->stream));
+  const int m = D.n + 1;
+  const double* v = h->velo + 3 * ko;
+  const double* ms = h->mass + ko;
+  const double* mm = h->mean_m + ko;
+  switch (itype) {
+    case 1: wtb::k_step1_flux<1><<<nb(10 * m * m), TPB, 0, h->stream>>>(L, B->rhs, v, ms, mm, B->grad); break;
+    case 5: wtb::k_step1_flux<5><<<nb(10 * m * m), TPB, 0, h->stream>>>(L, B->rhs, v, ms, mm, B->grad); break;
+    case 6: wtb::k_step1_flux<6><<<nb(10 * m * m), TPB, 0, h->stream>>>(L, B->rhs, v, ms, mm, B->grad); break;
+    default: wtb::k_step1_flux<7><<<nb(10 * m * m), TPB, 0, h->stream>>>(L, B->rhs, v, ms, mm, B->grad); break;
+  }
+  CKB(cudaGetLastError());
+  CKB(cudaMemcpyAsync(flux, B->grad, 3 * NN * 8, cudaMemcpyDeviceToHost, h->stream));
+  CKB(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
 int wt_barotropic_download(wt_handle* h, double* div_flux, double* rhs, double* grad) {
   if (!h) return WT_ERR_ARG;
   if (!h->baro) return WT_ERR_STATE;

@@ -139,6 +139,17 @@ class TriskModel(DeviceGrid):
         return grad
 
 
+def _step1_flux(model, itype: int, layer: int = 0, scalar: np.ndarray | None = None) -> np.ndarray:
+    flux = np.empty(3 * model.g.NN)
+    N.check("wt_step1_flux", N.lib().wt_step1_flux(model.h, int(itype), int(layer),
+                                                   N.dptr(None if scalar is None else _c(scalar)), N.dptr(flux)))
+    return flux
+
+
+TriskModel.step1_flux = _step1_flux
+TriskModel.step1_flux.__doc__ = """step1 itype 1, 5, 6 or 7 on one layer of the resident state: edge flux (3*NN)."""
+
+
 class WaveletHierarchy(DeviceGrid):
     """Layer mass, potential temperature and velocity on every level of a
     uniform hierarchy, their wavelet coefficients and the node/edge masks, with

@@ -73,6 +73,9 @@ typedef struct {
   int64_t n_halo_edge;
   const double *iu_wgt;        /* 9*NN  I_u_wgt%enc (outer velocity weights, set_WT_wgts,
                                   src/wavelet.f90:1567-1705); NULL on level_start */
+  const double *overl_split;   /* 2*NN  Overl_Area%split; may be NULL          */
+  const double *rf_wgt;        /* 3*NN  R_F_wgt%enc (flux-restriction weights, set_RF_wgts,
+                                  src/wavelet.f90:1512-1540,1176-1360); NULL on level_start */
 } wt_level_desc;
 
 typedef struct {
@@ -197,7 +200,12 @@ int wt_elliptic_l2_noalloc(int level, int domain_level, const int* nsrc, const d
 enum {
   WT_FIELD_MASS = 0, WT_FIELD_TEMP = 1, WT_FIELD_VELO = 2,   /* scaling: [nz][NN], [nz][NN], [nz][3*NN] doubles */
   WT_WAVE_MASS = 3, WT_WAVE_TEMP = 4, WT_WAVE_VELO = 5,      /* wavelet coefficients, same shapes            */
-  WT_MASK_NODE = 6, WT_MASK_EDGE = 7                         /* int32 [NN], [3*NN]                           */
+  WT_MASK_NODE = 6, WT_MASK_EDGE = 7,                        /* int32 [NN], [3*NN]                           */
+  /* Work fields of the multi-level trend (allocated on first use, zero):
+   * a node scalar (Bernoulli or Exner), the scalar trend dscalar, the
+   * horizontal flux h_flux and the velocity trend dvelo of every layer. */
+  WT_WORK_SCALAR = 8, WT_WORK_DSCALAR = 9,                   /* [nz][NN] doubles                             */
+  WT_WORK_FLUX = 10, WT_WORK_DVELO = 11                      /* [nz][3*NN] doubles                           */
 };
 /* Mask values (src/shared.f90:58-73). */
 enum { WT_MASK_ZERO = 0, WT_MASK_TRSK = 2, WT_MASK_ADJZONE = 8, WT_MASK_RESTRCT = 12, WT_MASK_TOLRNZ = 16,
@@ -240,6 +248,24 @@ int wt_compress(wt_handle* h);
  * compression, inverse transform. */
 int wt_wt_after_step(wt_handle* h);
 
+/* ------------------------------------------------ compute-or-restrict ---- */
+/* The coarse-level restrictions of the multi-level trend (trend_ml,
+ * src/multi_level.f90:5-43) from level+1 to `level`, level_start <= level <
+ * level_end, every layer, on the work fields.
+ * scalar_cpt_restr (src/multi_level.f90:311-345): the node scalar of parents
+ * [0, n]^2 with mask_n >= RESTRCT is sub-sampled from the child. */
+int wt_restrict_scalar(wt_handle* h, int level);
+/* flux_cpt_restr (src/multi_level.f90:394-659): the flux of the edges of
+ * parents [0, n)^2 with mask_e >= RESTRCT is the conservative restriction of
+ * the child's flux and dscalar (interp_flux with R_F_wgt, part_coarse_flux and
+ * coarse_flux with the overlap areas).  Needs rf_wgt and overl_split of
+ * level+1. */
+int wt_restrict_flux(wt_handle* h, int level);
+/* The restriction of u_source_cpt_restr (src/multi_level.f90:365-392): the
+ * velocity trend of parent edges whose first child edge has mask_e >= ADJZONE
+ * is the sum of the two child edges; the others keep the parent's value. */
+int wt_restrict_u_source(wt_handle* h, int level);
+
 /* ---------------------------------------------------------- barotropic ---- */
 /* The free-surface pieces of the mode-split step on level_end, around the
  * elliptic solve (eta_update / u_update, src/barotropic_2d.f90:118-149).
@@ -260,6 +286,12 @@ int wt_u_update(wt_handle* h, double dt, double theta1);
  * doubles) is the node field of itypes 1 and 6 (NULL otherwise).  Uses the
  * barotropic work buffers, so it overwrites the last rhs and grad. */
 int wt_step1_flux(wt_handle* h, int itype, int layer, const double* scalar, double* flux);
+/* step1 itype 8 (src/ops.f90:256-271, comp_SW :460-471) and post_vort
+ * (:1159-1228): the vorticity (circulation / triangle area) of one layer of the
+ * resident velocity on the triangles the reference's loop over nodes [0, n]^2
+ * writes, pentagon corners included.  vort: 2*NN host doubles (LORT plane,
+ * UPLT plane); other triangles 0. */
+int wt_step1_vort(wt_handle* h, int layer, double* vort);
 /* div_flux (NN), rhs (NN), grad (3*NN); any may be NULL. */
 int wt_barotropic_download(wt_handle* h, double* div_flux, double* rhs, double* grad);
 

@@ -63,3 +63,16 @@ def step1_flux(g, itype, velo, mass, mean_m, scalar=None):
     rc = L.orc_step1_flux(C.byref(lv.s), int(itype), *[None if b is None else _p(b) for b in bufs], _p(flux))
     assert rc == 0
     return flux
+
+
+def step1_vort(g, velo):
+    """step1 itype 8 + post_vort on one layer's velocity: vorticity (2*NN, LORT then UPLT)."""
+    L = lib()
+    lv = _Level(g)
+    vort = np.zeros(2 * g.NN)
+    tri = _c(g.triarea)
+    L.orc_step1_vort.argtypes = [C.POINTER(orc_blevel), _dp, _dp, _dp]
+    L.orc_step1_vort.restype = C.c_int
+    rc = L.orc_step1_vort(C.byref(lv.s), _p(tri), _p(_c(velo)), _p(vort))
+    assert rc == 0
+    return vort

@@ -11,6 +11,9 @@
 //   step1 itype 3 (comput :225-228, comp_SW :416-419), porosity 1   src/ops.f90
 //   u_update                                  src/barotropic_2d.f90:131-149
 //   step1 itypes 1, 5, 6, 7 (comput :198-262, comp_SW :396-455)     src/ops.f90
+//   step1 itype 8 (comput :256-271, comp_SW :460-471) + post_vort :1159-1228
+//     in the reference's visiting order for a patch covering the lozenge:
+//     nodes [0, n)^2 row by row, the north row and (n, n), the east column.
 // step1 visits nodes [0, n]^2 of each lozenge and runs comp_SW on the south
 // and west borders; update_bdry is the level's ghost copy.  u_update is
 // applied to the edges grad_eta writes (the reference's element range also
@@ -226,6 +229,71 @@ int orc_step1_flux(const orc_blevel* Lp, int itype, const double* s_in, const do
           return -1;
         }
       }
+  return 0;
+}
+
+// One layer's velocity v (3*NN) -> vort (2*NN, LORT plane then UPLT plane).
+int orc_step1_vort(const orc_blevel* Lp, const double* triarea, const double* v_in, double* vort) {
+  const orc_blevel& L = *Lp;
+  B b{L};
+  const int64_t NN = L.NN;
+  const int P = L.P, n = L.n;
+  std::vector<double> v(v_in, v_in + 3 * NN);
+  b.halo_e(v.data());
+  std::memset(vort, 0, 2 * NN * sizeof(double));
+  auto up = [&](int e, int64_t x) { return v[e * NN + x] * L.len[e * NN + x]; };
+  auto put = [&](int t, int64_t x, double c) { vort[t * NN + x] = c / triarea[t * NN + x]; };
+  enum { LORT = 0, UPLT = 1 };
+  for (int d = 0; d < 10; ++d) {
+    auto node = [&](int i, int j) {
+      const int64_t id = b.id(d, i, j);
+      const int64_t idN = id + P, idE = id + 1, idS = id - P, idW = id - 1, idSW = id - P - 1;
+      // comput
+      const double u_RT = up(RT, id), u_RT_N = up(RT, idN), u_RT_W = up(RT, idW);
+      const double u_DG = up(DG, id), u_DG_S = up(DG, idS), u_DG_W = up(DG, idW);
+      const double u_UP = up(UP, id), u_UP_E = up(UP, idE), u_UP_S = up(UP, idS);
+      const double c_LORT = u_RT + u_UP_E + u_DG;
+      const double c_UPLT = -(u_DG + u_UP + u_RT_N);
+      const double c_W_LORT = u_RT_W + u_UP + u_DG_W;
+      const double c_S_UPLT = -(u_RT + u_DG_S + u_UP_S);
+      put(LORT, id, c_LORT);
+      put(UPLT, id, c_UPLT);
+      put(LORT, idW, c_W_LORT);
+      put(UPLT, idS, c_S_UPLT);
+      if (i == 0 || j == 0) {  // comp_SW
+        const double w_RT_W = up(RT, idW), w_RT_SW = up(RT, idSW), w_DG_SW = up(DG, idSW);
+        const double w_UP_S = up(UP, idS), w_UP_SW = up(UP, idSW);
+        put(LORT, idSW, w_RT_SW + w_UP_S + w_DG_SW);
+        put(UPLT, idSW, -(w_RT_W + w_DG_SW + w_UP_SW));
+      }
+    };
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) node(i, j);
+    for (int i = 0; i < n; ++i) node(i, n);
+    node(n, n);
+    for (int j = 0; j < n; ++j) node(n, j);
+    // post_vort at the four pentagon corners
+    {
+      const int64_t idS = b.id(d, 0, -1), idSW = b.id(d, -1, -1), idW = b.id(d, -1, 0);
+      put(LORT, idSW, up(UP, idS) - up(RT, idW) + up(RT, idSW));
+      vort[UPLT * NN + idSW] = vort[LORT * NN + idSW];
+    }
+    {
+      const int64_t id = b.id(d, n, 0), idS = b.id(d, n, -1), idSW = b.id(d, n - 1, -1);
+      put(LORT, idSW, -up(RT, id) + up(RT, idSW) + up(DG, idSW));
+      vort[UPLT * NN + idS] = vort[LORT * NN + idSW];
+    }
+    {
+      const int64_t id = b.id(d, 0, n), idSW = b.id(d, -1, n - 1), idW = b.id(d, -1, n);
+      put(UPLT, idSW, up(UP, id) - up(DG, idSW) - up(UP, idSW));
+      vort[LORT * NN + idW] = vort[UPLT * NN + idSW];
+    }
+    {
+      const int64_t id = b.id(d, n, n), idN = b.id(d, n, n + 1);
+      put(LORT, id, up(RT, id) - up(RT, idN) - up(UP, id));
+      vort[UPLT * NN + id] = vort[LORT * NN + id];
+    }
+  }
   return 0;
 }
 

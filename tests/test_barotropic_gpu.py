@@ -69,3 +69,23 @@ def test_step1_flux_itypes_match_oracle(itype):
     e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
     assert rel(f[e], of[e]) <= TOL
     model.close()
+
+
+@pytest.mark.parametrize("level", [4, 6])
+def test_step1_vorticity_matches_oracle_exactly(level):
+    """itype 8 + post_vort: every triangle the reference's loop writes, the
+    pentagon corners and the UPLT values written twice included, bit for bit."""
+    nz = 2
+    g = Grid(level, level, radius=6371e3).level(level)
+    ph = OceanParams()
+    st = jet_state(g, nz, seed=level, ph=ph)
+    st["velo"] = st["velo"] + np.random.default_rng(level).standard_normal(st["velo"].shape)
+    halo_edges(g, st["velo"])
+    model = TriskModel(g, nz, st["topo"], ph)
+    model.upload(st)
+    for k in range(nz):
+        v = model.step1_vort(k)
+        ov = ob.step1_vort(g, st["velo"][k])
+        assert np.count_nonzero(ov) > 0
+        assert np.array_equal(v, ov), (k, np.abs(v - ov).max())
+    model.close()

@@ -49,7 +49,8 @@ class wt_level_desc(C.Structure):
                 ("len", _dp), ("pedlen", _dp), ("part", _dp), ("hex_inv", _dp), ("triarea", _dp),
                 ("coriolis", _dp), ("overl_a", _dp), ("topo", _dp),
                 ("halo_node", _ip), ("n_halo_node", C.c_int64),
-                ("halo_edge", _ip), ("n_halo_edge", C.c_int64), ("iu_wgt", _dp)]
+                ("halo_edge", _ip), ("n_halo_edge", C.c_int64), ("iu_wgt", _dp),
+                ("overl_split", _dp), ("rf_wgt", _dp)]
 
 
 class wt_grid_desc(C.Structure):
@@ -128,6 +129,10 @@ _DEVICE_SIGS = {
     "wt_compress": [_vp],
     "wt_mask_build": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "wt_wt_after_step": [_vp],
+    "wt_step1_vort": [_vp, C.c_int, _dp],
+    "wt_restrict_scalar": [_vp, C.c_int],
+    "wt_restrict_flux": [_vp, C.c_int],
+    "wt_restrict_u_source": [_vp, C.c_int],
     "wt_barotropic_upload": [_vp, _dp, _dp],
     "wt_rhs_elliptic": [_vp, C.c_double, C.c_double],
     "wt_u_update": [_vp, C.c_double, C.c_double],

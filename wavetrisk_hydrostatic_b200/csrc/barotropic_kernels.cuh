@@ -18,6 +18,8 @@
 namespace wtb {
 
 using wtk::DG;
+using wtk::LORT;
+using wtk::UPLT;
 using wtk::interp;
 using wtk::LevelDev;
 using wtk::Rd;
@@ -219,6 +221,70 @@ __global__ void k_step1_flux(LevelDev L, const double* __restrict__ s, const dou
   if (i == 0) comp_sw(RT, id - 1);
   comp_sw(DG, id - P - 1);
   if (!(i == 0 && j > 0)) comp_sw(UP, id - P);
+}
+
+// step1 itype 8, vorticity of one layer's velocity (src/ops.f90:256-271,
+// comp_SW :460-471), with post_vort's pentagon values (src/ops.f90:1159-1228).
+// The reference's loop writes most triangles twice; the two LORT expressions
+// are the same sum, the two UPLT ones are not (own: -(DG + UP + RT_N), from
+// the node above: -(RT_N + DG + UP)).  The reference visits the nodes
+// [0, n)^2 row by row, then the north row (i < n, n) and (n, n), then the
+// east column (n, j < n), so the node-above form lands last except on the top
+// row and at (n, n-1).  Here each triangle has one writer that evaluates the
+// expression that lands last: thread (i, j) in [0, n]^2 writes LORT(i, j) and
+// UPLT(i, j); thread (0, j) also writes
+// LORT(-1, j) and UPLT(-1, j-1), thread (i, 0) LORT(i-1, -1) and UPLT(i, -1);
+// the four lozenge-corner threads write the pentagon values instead.
+__global__ void k_step1_vort(LevelDev L, const double* __restrict__ v, double* __restrict__ vort) {
+  const int n = L.n, m = n + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  const int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
+  const int P = L.P, NN = L.NN;
+  const int id = (d * P + j + 2) * P + i + 2;
+  const Rd R(L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2);
+  auto up = [&](int e, int x) { const int slot = e * NN + x; return R.e(v, slot) * L.len[slot]; };
+  auto lort = [&](int x) { return up(RT, x) + up(UP, x + 1) + up(DG, x); };
+  auto uplt_n = [&](int x) { return -(up(RT, x + P) + up(DG, x) + up(UP, x)); };  // written from the node above
+  auto put = [&](int tri, int x, double c) { vort[tri * NN + x] = c / L.triarea[tri * NN + x]; };
+  const int idW = id - 1, idS = id - P, idSW = id - P - 1;
+  if (i == n && j == n) {  // IJPLUS
+    const double c = up(RT, id) - up(RT, id + P) - up(UP, id);
+    put(LORT, id, c);
+    vort[UPLT * NN + id] = vort[LORT * NN + id];
+    return;
+  }
+  put(LORT, id, lort(id));
+  if (j < n && !(i == n && j == n - 1)) put(UPLT, id, uplt_n(id));
+  else put(UPLT, id, -(up(DG, id) + up(UP, id) + up(RT, id + P)));
+  if (i == 0 && j == 0) {  // IJMINUS
+    const double c = up(UP, idS) - up(RT, idW) + up(RT, idSW);
+    put(LORT, idSW, c);
+    vort[UPLT * NN + idSW] = vort[LORT * NN + idSW];
+    put(LORT, idW, lort(idW));
+    put(UPLT, idS, uplt_n(idS));
+    return;
+  }
+  if (i == 0 && j == n) {  // IMINUSJPLUS
+    const double c = up(UP, id) - up(DG, idSW) - up(UP, idSW);
+    put(UPLT, idSW, c);
+    vort[LORT * NN + idW] = vort[UPLT * NN + idSW];
+    return;
+  }
+  if (i == n && j == 0) {  // IPLUSJMINUS
+    const double c = -up(RT, id) + up(RT, idSW) + up(DG, idSW);
+    put(LORT, idSW, c);
+    vort[UPLT * NN + idS] = vort[LORT * NN + idSW];
+    return;
+  }
+  if (i == 0) {
+    put(LORT, idW, lort(idW));
+    put(UPLT, idSW, uplt_n(idSW));
+  }
+  if (j == 0) {
+    put(LORT, idSW, lort(idSW));
+    put(UPLT, idS, uplt_n(idS));
+  }
 }
 
 }  // namespace wtb

@@ -5,7 +5,9 @@
 // file is compiled with -ffp-contract=off (no FMA contraction).
 #include "grid.hpp"
 
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <limits>
 #include <cstdio>
 #include <functional>
@@ -513,9 +515,13 @@ const int bfly_tri[3][4][3] = {  // [e][k][:]
     {{0, 0, LORT}, {0, 1, LORT}, {-1, 0, UPLT}, {-1, -1, UPLT}}};
 const int adj_tri[3][2][3] = {{{0, -1, UPLT}, {0, 0, LORT}}, {{0, 0, UPLT}, {0, 0, LORT}}, {{0, 0, UPLT}, {-1, 0, LORT}}};
 
-void get_overl_areas(Level& Pa, Level& L, int d, int ip, int jp, int ic, int jc, int e, double area[8]) {
+enum { INSIDE = 0, OUTER1 = 1, OUTER2 = 2 };  // src/shared.f90:65-67
+
+// typ[0..1] is the reference's typ(1:2): how the two coarse dual edges cross the child hexagon.
+void get_overl_areas(Level& Pa, Level& L, int d, int ip, int jp, int ic, int jc, int e, double area[8], int typ[2]) {
   Acc P{Pa, d}, Cc{L, d};
   for (int k = 0; k < 8; ++k) area[k] = 0.0;
+  typ[0] = typ[1] = 0;
   Coord hex[6];
   for (int i = 0; i < 6; ++i) {
     const int* t = no_adj_tri[i + hex_s_offs[-e + 2]];
@@ -540,6 +546,7 @@ void get_overl_areas(Level& Pa, Level& L, int d, int ip, int jp, int ic, int jc,
       area[i + 1] = area[i + 3] + area[i + 5];
       area[i - 1] = area[i - 1] + triarea(hex[3 * i - 3], ip0, pt) + triarea(ip0, pt, tri[1][i - 1]);
       area[-i + 2] = area[-i + 2] + triarea(ip1, hex[3 * i - 1], pt) + triarea(tri[1][i - 1], pt, ip1);
+      typ[-i + 2] = INSIDE;
     } else if (!d0 && !d1) {
       area[i + 1] = 0.0;
       arc_inters(tri[1][0], tri[1][1], hex[3 * i - 3], hex[3 * i - 2], ip0, d0);
@@ -547,9 +554,11 @@ void get_overl_areas(Level& Pa, Level& L, int d, int ip, int jp, int ic, int jc,
       if (!d0 && d1) {
         area[i - 1] = area[i - 1] + triarea(hex[3 * i - 3], hex[3 * i - 2], pt) + triarea(hex[3 * i - 2], ip1, pt);
         area[-i + 2] = area[-i + 2] + triarea(ip1, hex[3 * i - 1], pt);
+        typ[-i + 2] = OUTER2;
       } else if (d0 && !d1) {
         area[i - 1] = area[i - 1] + triarea(hex[3 * i - 3], ip0, pt);
         area[-i + 2] = area[-i + 2] + triarea(hex[3 * i - 2], hex[3 * i - 1], pt) + triarea(ip0, hex[3 * i - 2], pt);
+        typ[-i + 2] = OUTER1;
       } else {
         std::fprintf(stderr, "wtg: overlap area case A at d=%d (%d,%d)\n", d, ic, jc);
       }
@@ -567,7 +576,8 @@ void overlap_areas(Level& Pa, Level& L) {
         const int ce[3][2] = {{ic + 1, jc}, {ic + 1, jc + 1}, {ic, jc + 1}};
         for (int e = 0; e < 3; ++e) {
           double area[8];
-          get_overl_areas(Pa, L, d, ip, jp, ce[e][0], ce[e][1], e, area);
+          int typ[2];
+          get_overl_areas(Pa, L, d, ip, jp, ce[e][0], ce[e][1], e, area, typ);
           int64_t id = L.id(d, ce[e][0], ce[e][1]);
           for (int k = 0; k < 4; ++k) L.overl_a[k * L.NN + id] = area[k];
           L.overl_split[id] = area[4];
@@ -767,6 +777,181 @@ void velo_weights(const Grid& g, const Level& Pa, Level& L) {
   if (bad) std::fprintf(stderr, "wtg: %d undefined node reads in velocity weights (level %d)\n", bad, L.l);
 }
 
+// ---- flux-restriction weights R_F_wgt ----------------------------------------
+// set_RF_wgts / basic_F_restr_wgt (src/wavelet.f90:1512-1540, 1176-1360) with
+// get_indices' stencil naming (src/shared.f90:84-112) and nghb_pt (:285).
+// R_F_wgt lives on the child level (3 components, component c at c*NN + node)
+// and is not ghost-copied.  Two parents write some slots (RT k=1 of (i,j) and
+// UP k=1 of (i+1,j) describe the same coarse LORT triangle; UP k=0 of (i,j)
+// and RT k=0 of (i,j+1) the same UPLT triangle); the last write wins, in the
+// order lozenge, j, i, then RT before UP, i.e. the reference's loop order for a
+// patch covering the whole lozenge.
+enum { S_UZM = 0, S_UPZ, S_UMZ, S_UZP, S_VMM, S_VPM, S_VMP, S_VPP, S_WMM, S_WPM, S_WMP, S_WPP, S_WMMM, S_WPPP,
+       S_VMPP, S_VPMM };
+const int NGHB_PT[10][2] = {{1, 0}, {1, 1}, {0, 1}, {-1, 0}, {-1, -1}, {0, -1}, {1, 0}, {1, 1}, {0, 1}, {-1, 0}};
+
+struct RFWeights {
+  const Level& Pa;
+  Level& L;
+  int d;
+  Coord x, y;
+  int bad = 0;  // reads outside the padded child level
+  double conflict = 0.0;  // largest change of a slot by a second writer
+
+  Coord node(int i, int j) {
+    if (!L.in(i, j)) { ++bad; return C(0.0, 0.0, 0.0); }
+    return L.node[L.id(d, i, j)];
+  }
+  Coord cc(int i, int j, const int* t) {
+    const int ii = i + t[0], jj = j + t[1];
+    if (!L.in(ii, jj)) { ++bad; return C(0.0, 0.0, 0.0); }
+    return L.ccentre[(int64_t)t[2] * L.NN + L.id(d, ii, jj)];
+  }
+  // coords_to_row (:1336-1359): row of the flux at edge ije, scaled by its dual length.
+  Row6 row(const int* ije) {
+    const int i = ije[0], j = ije[1], e = ije[2];
+    const Coord p1 = node(i + END_PT[e][0][0], j + END_PT[e][0][1]);
+    const Coord p2 = node(i + END_PT[e][1][0], j + END_PT[e][1][1]);
+    const double ped = dist(cc(i, j, adj_tri[e][0]), cc(i, j, adj_tri[e][1]));
+    Row6 r = coords_to_rowd(mid_pt(p1, p2), vector(p1, p2), x, y);
+    for (int q = 0; q < 6; ++q) r.v[q] = r.v[q] * ped;
+    return r;
+  }
+  // interp_F_wgts (:1288-1321)
+  void interp(int k1, const int* lcsd, Coord endpt_o, int ije[16][3], const int st[9], double w[6]) {
+    const Coord c = cc(lcsd[0], lcsd[1], adj_tri[lcsd[2]][1 - k1]);
+    const Coord m = L.in(lcsd[0], lcsd[1]) ? L.midpt[(int64_t)lcsd[2] * L.NN + L.id(d, lcsd[0], lcsd[1])]
+                                           : C(0.0, 0.0, 0.0);
+    x = direction(c, m);
+    y = normalize_coord(cross(x, c));
+    Row6 G[6];
+    G[0] = row(ije[st[0]]);
+    G[1] = row(ije[st[1]]);
+    G[2] = row(ije[st[2]]);
+    G[3] = row(ije[st[3]]) - row(ije[st[4]]);
+    G[4] = row(ije[st[5]]) - row(ije[st[6]]);
+    G[5] = row(ije[st[7]]) - row(ije[st[8]]);
+    double a[36];
+    for (int col = 0; col < 6; ++col)
+      for (int r = 0; r < 6; ++r) a[col * 6 + r] = G[col].v[r];
+    // coords_to_row_perp (:1323-1334)
+    const Coord mid = mid_pt(c, endpt_o);
+    const Coord dir = cross(vector(c, endpt_o), mid);
+    Row6 b = coords_to_rowd(mid, dir, x, y);
+    const double dd = dist(c, endpt_o);
+    for (int q = 0; q < 6; ++q) w[q] = b.v[q] * dd;
+    dgesv6(a, w);
+  }
+  void store(int i, int j, const double* v) {
+    if (!L.in(i, j)) { ++bad; return; }
+    const int64_t id = L.id(d, i, j);
+    for (int c = 0; c < 3; ++c) {
+      double& s = L.rf_wgt[(int64_t)c * L.NN + id];
+      if (L.rf_set[id]) conflict = std::max(conflict, std::fabs(s - v[c]));
+      s = v[c];
+    }
+    L.rf_set[id] = 1;
+  }
+  // basic_F_restr_wgt for parent (ip, jp), edge e in {RT, UP}, overlap types typ[0..1].
+  void compute(int ip, int jp, int e, const int typ[2]) {
+    const int i0 = 2 * ip, j0 = 2 * jp;
+    int enc[4][2];
+    int i, j;
+    if (e == UP) {
+      const int t[4][2] = {{i0 - 2, j0}, {i0 - 2, j0 + 1}, {i0 + 1, j0}, {i0 + 1, j0 + 1}};
+      std::memcpy(enc, t, sizeof t);
+      i = i0;
+      j = j0 + 1;
+    } else {
+      const int t[4][2] = {{i0, j0}, {i0, j0 + 1}, {i0 + 1, j0 - 2}, {i0 + 1, j0 - 1}};
+      std::memcpy(enc, t, sizeof t);
+      i = i0 + 1;
+      j = j0;
+    }
+    const int hs = HEX_S_OFFS[e];
+    int ije[16][3];
+    auto set = [&](int s, int bi, int bj, const int* h) { ije[s][0] = bi + h[0]; ije[s][1] = bj + h[1]; ije[s][2] = h[2]; };
+    set(S_UMZ, i, j, HEX_SIDES[hs + 1]);
+    set(S_UPZ, i, j, HEX_SIDES[hs + 4]);
+    set(S_WMP, i, j, HEX_SIDES[hs + 0]);
+    set(S_VPP, i, j, HEX_SIDES[hs + 5]);
+    set(S_WPM, i, j, HEX_SIDES[hs + 3]);
+    set(S_VMM, i, j, HEX_SIDES[hs + 2]);
+    const int mp[2] = {i + NGHB_PT[hs + 0][0], j + NGHB_PT[hs + 0][1]};
+    const int pp[2] = {i + NGHB_PT[hs + 5][0], j + NGHB_PT[hs + 5][1]};
+    const int pm[2] = {i + NGHB_PT[hs + 3][0], j + NGHB_PT[hs + 3][1]};
+    const int mm[2] = {i + NGHB_PT[hs + 2][0], j + NGHB_PT[hs + 2][1]};
+    set(S_VMP, mp[0], mp[1], HEX_SIDES[hs + 2]);
+    set(S_VMPP, mp[0], mp[1], HEX_SIDES[hs + 5]);
+    set(S_UZP, mp[0], mp[1], HEX_SIDES[hs + 4]);
+    set(S_WPPP, pp[0], pp[1], HEX_SIDES[hs + 0]);
+    set(S_WPP, pp[0], pp[1], HEX_SIDES[hs + 3]);
+    set(S_VPM, pm[0], pm[1], HEX_SIDES[hs + 5]);
+    set(S_VPMM, pm[0], pm[1], HEX_SIDES[hs + 2]);
+    set(S_UZM, pm[0], pm[1], HEX_SIDES[hs + 1]);
+    set(S_WMMM, mm[0], mm[1], HEX_SIDES[hs + 3]);
+    set(S_WMM, mm[0], mm[1], HEX_SIDES[hs + 0]);
+    static const int ST1[9] = {S_VPP, S_WMP, S_UZP, S_UPZ, S_WPP, S_VMP, S_UMZ, S_WPPP, S_VMPP};
+    static const int ST0[9] = {S_VMM, S_WPM, S_UZM, S_UMZ, S_WMM, S_VPM, S_UPZ, S_WMMM, S_VPMM};
+    for (int k = 1; k >= 0; --k) {
+      const int* ta = adj_tri[e][k];
+      const Coord po = Pa.ccentre[(int64_t)ta[2] * Pa.NN + Pa.id(d, ip + ta[0], jp + ta[1])];
+      const int* u = ije[k == 1 ? S_UZP : S_UZM];
+      const int slot = k == 1 ? 0 : 2;
+      if (dist(po, cc(u[0], u[1], adj_tri[u[2]][1 - k])) < eps()) {  // coinciding circumcentres
+        const double z[3] = {0.0, 0.0, 0.0};
+        store(enc[slot][0], enc[slot][1], z);
+        store(enc[slot + 1][0], enc[slot + 1][1], z);
+        continue;
+      }
+      const int* lcsd;
+      if (typ[k] == OUTER1) lcsd = ije[k == 1 ? S_VPP : S_VMM];
+      else if (typ[k] == OUTER2) lcsd = ije[k == 1 ? S_WMP : S_WPM];
+      else lcsd = ije[k == 1 ? S_UZP : S_UZM];
+      double w[6];
+      interp(k, lcsd, po, ije, k == 1 ? ST1 : ST0, w);
+      double o[6];
+      if (e == RT) {
+        const double t[6] = {w[1], w[2], w[0], w[4], w[5], w[3]};
+        std::memcpy(o, t, sizeof t);
+      } else {
+        const double t[6] = {w[2], w[0], w[1], w[5], w[3], w[4]};
+        std::memcpy(o, t, sizeof t);
+      }
+      store(enc[slot][0], enc[slot][1], o);
+      store(enc[slot + 1][0], enc[slot + 1][1], o + 3);
+    }
+  }
+};
+
+// set_RF_wgts over the parents [0, n_par)^2 of every lozenge: the overlap
+// type of the RT child (2i+1, 2j) feeds the RT weights, that of the UP child
+// (2i, 2j+1) the UP weights.
+void rf_weights(Level& Pa, Level& L) {
+  L.rf_wgt.assign((size_t)3 * L.NN, 0.0);
+  L.rf_set.assign((size_t)L.NN, 0);
+  int bad = 0;
+  double conflict = 0.0;
+  for (int d = 0; d < N_LOZ; ++d) {
+    RFWeights W{Pa, L, d, C(0, 0, 0), C(0, 0, 0)};
+    for (int jp = 0; jp < Pa.n; ++jp)
+      for (int ip = 0; ip < Pa.n; ++ip) {
+        double area[8];
+        int typ[2];
+        get_overl_areas(Pa, L, d, ip, jp, 2 * ip + 1, 2 * jp, RT, area, typ);
+        W.compute(ip, jp, RT, typ);
+        get_overl_areas(Pa, L, d, ip, jp, 2 * ip, 2 * jp + 1, UP, area, typ);
+        W.compute(ip, jp, UP, typ);
+      }
+    bad += W.bad;
+    conflict = std::max(conflict, W.conflict);
+  }
+  L.rf_conflict = conflict;
+  L.rf_set.clear();
+  if (bad) std::fprintf(stderr, "wtg: %d reads outside the padded level in flux-restriction weights (level %d)\n",
+                        bad, L.l);
+}
+
 // comm_nodes9(get_areas, set_areas) + area_post_comm (src/refine_patch.f90:436-486)
 void comm_areas(const Grid& g, Level& L) {
   for (auto& h : L.halo_node) {
@@ -814,6 +999,7 @@ void build_grid(Grid& g, int min_level, int max_level, int domain_level, double 
     if (l > min_level - 1) {
       overlap_areas(g.at(l - 1), L);
       velo_weights(g, g.at(l - 1), L);
+      rf_weights(g.at(l - 1), L);
     }
     comm_areas(g, L);
   }

@@ -42,6 +42,9 @@ struct Level {
   std::vector<double> overl_a;            // [4*NN]  Overl_Area%a
   std::vector<double> overl_split;        // [2*NN]  Overl_Area%split
   std::vector<double> iu_wgt;             // [9*NN]  I_u_wgt%enc (k at k*NN + node); levels > min_level-1
+  std::vector<double> rf_wgt;             // [3*NN]  R_F_wgt%enc (c at c*NN + node); levels > min_level-1
+  std::vector<uint8_t> rf_set;            // build scratch: slot already written
+  double rf_conflict = 0.0;               // largest difference between two writers of one R_F_wgt slot
   std::vector<uint8_t> valid;             // [NN] 1 where node coordinates are defined
   std::vector<HaloNode> halo_node;
   std::vector<HaloEdge> halo_edge;

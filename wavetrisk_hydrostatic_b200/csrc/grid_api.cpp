@@ -46,7 +46,9 @@ int wt_grid_level_dims(const wt_grid* gh, int level, wt_level_dims* dims) {
 // (doubles unless stated): "node" 3*NN (x plane, y plane, z plane),
 // "len"/"pedlen" 3*NN, "part" 6*NN, "hex_inv" NN, "triarea"/"coriolis" 2*NN,
 // "overl_a" 4*NN, "overl_split" 2*NN, "ccentre" 6*NN (xyz planes of LORT then
-// UPLT), "halo_node" 2*n_halo_node int64, "halo_edge" 3*n_halo_edge int64.
+// UPLT), "halo_node" 2*n_halo_node int64, "halo_edge" 3*n_halo_edge int64;
+// above the coarsest level also "iu_wgt" 9*NN, "rf_wgt" 3*NN and "rf_conflict"
+// (1 double: the largest difference between two writers of one R_F_wgt slot).
 int wt_grid_copy(const wt_grid* gh, int level, const char* name, void* dst) {
   const Grid* g = reinterpret_cast<const Grid*>(gh);
   if (!g || !name || !dst || level < g->min_level - 1 || level > g->max_level) return WT_ERR_ARG;
@@ -72,6 +74,12 @@ int wt_grid_copy(const wt_grid* gh, int level, const char* name, void* dst) {
   else if (!std::strcmp(name, "iu_wgt")) {
     if (L.iu_wgt.empty()) return WT_ERR_ARG;
     cp(L.iu_wgt);
+  } else if (!std::strcmp(name, "rf_wgt")) {
+    if (L.rf_wgt.empty()) return WT_ERR_ARG;
+    cp(L.rf_wgt);
+  } else if (!std::strcmp(name, "rf_conflict")) {
+    if (L.rf_wgt.empty()) return WT_ERR_ARG;
+    d[0] = L.rf_conflict;
   }
   else if (!std::strcmp(name, "halo_node")) {
     int64_t* o = static_cast<int64_t*>(dst);

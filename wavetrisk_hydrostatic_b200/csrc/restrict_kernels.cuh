@@ -1,0 +1,224 @@
+// Coarse-level compute-or-restrict kernels of the multi-level trend
+// (src/multi_level.f90:311-659): one thread per (layer, lozenge, parent node),
+// node index fastest so that a warp reads consecutive parents and the
+// stride-2 child rows.  Ghost values of the child flux and dscalar are read
+// through the level's remaps (the reference ghost-copies them first);
+// R_F_wgt, the overlap areas and the masks are read where they are stored.
+// FP64 with the reference's operand order (the build turns FMA contraction off).
+#pragma once
+#include "wavelet_kernels.cuh"
+
+namespace wtw {
+
+enum { S_UZM = 0, S_UPZ, S_UMZ, S_UZP, S_VMM, S_VPM, S_VMP, S_VPP, S_WMM, S_WPM, S_WMP, S_WPP, S_WMMM, S_WPPP,
+       S_VMPP, S_VPMM };
+constexpr int M_RESTRCT = 12, M_ADJZONE = 8;
+
+// nghb_pt and bfly_no2 (src/shared.f90:285,330)
+__constant__ int c_nghb_pt[10][2] = {{1, 0}, {1, 1}, {0, 1}, {-1, 0}, {-1, -1}, {0, -1}, {1, 0}, {1, 1}, {0, 1}, {-1, 0}};
+__constant__ int c_bfly_no2[3][4][2] = {{{-3, -2}, {1, -2}, {3, 2}, {-1, 2}},
+                                        {{1, 3}, {-3, -1}, {-1, -3}, {3, 1}},
+                                        {{2, -1}, {2, 3}, {-2, 1}, {-2, -3}}};
+
+// get_indices (src/multi_level.f90:617-659): the 16 stencil edges as (i, j, e)
+// and the diagonal neighbours MP, PP, PM, MM.
+struct RInd {
+  int ei[16], ej[16], ee[16];
+  int ni[4], nj[4];
+};
+
+__device__ __forceinline__ void rset(RInd& r, int s, int i, int j, int k) {
+  r.ei[s] = i + c_hex_sides[k][0];
+  r.ej[s] = j + c_hex_sides[k][1];
+  r.ee[s] = c_hex_sides[k][2];
+}
+
+__device__ __forceinline__ RInd get_indices(int i, int j, int e) {
+  RInd r;
+  const int hs = c_hex_s_offs[e];
+  rset(r, S_UMZ, i, j, hs + 1);
+  rset(r, S_UPZ, i, j, hs + 4);
+  rset(r, S_WMP, i, j, hs + 0);
+  rset(r, S_VPP, i, j, hs + 5);
+  rset(r, S_WPM, i, j, hs + 3);
+  rset(r, S_VMM, i, j, hs + 2);
+  const int off[4] = {0, 5, 3, 2};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    r.ni[q] = i + c_nghb_pt[hs + off[q]][0];
+    r.nj[q] = j + c_nghb_pt[hs + off[q]][1];
+  }
+  rset(r, S_VMP, r.ni[0], r.nj[0], hs + 2);
+  rset(r, S_VMPP, r.ni[0], r.nj[0], hs + 5);
+  rset(r, S_UZP, r.ni[0], r.nj[0], hs + 4);
+  rset(r, S_WPPP, r.ni[1], r.nj[1], hs + 0);
+  rset(r, S_WPP, r.ni[1], r.nj[1], hs + 3);
+  rset(r, S_VPM, r.ni[2], r.nj[2], hs + 5);
+  rset(r, S_VPMM, r.ni[2], r.nj[2], hs + 2);
+  rset(r, S_UZM, r.ni[2], r.nj[2], hs + 1);
+  rset(r, S_WMMM, r.ni[3], r.nj[3], hs + 3);
+  rset(r, S_WMM, r.ni[3], r.nj[3], hs + 0);
+  return r;
+}
+
+struct RChild {
+  const WLev& C;
+  const double* __restrict__ h;   // child flux, one layer
+  const double* __restrict__ ds;  // child dscalar, one layer
+  int d;
+
+  __device__ __forceinline__ double f(const RInd& r, int s) const { return re(C, h, r.ee[s], d, r.ei[s], r.ej[s]); }
+  __device__ __forceinline__ double dsn(int i, int j) const { return rn(C, ds, d, i, j); }
+  __device__ __forceinline__ double a(int i, int j, int k) const { return C.oa[k * C.NN + nid(C, d, i, j)]; }
+  __device__ __forceinline__ double sp(int i, int j, int k) const { return C.split[k * C.NN + nid(C, d, i, j)]; }
+  __device__ __forceinline__ double hi(int i, int j) const { return C.hinv[nid(C, d, i, j)]; }
+  __device__ __forceinline__ double rf(int i, int j, int c) const { return C.rf[c * C.NN + nid(C, d, i, j)]; }
+
+  // - sum(f(a) * rf(i0,j0)) - sum((f(p) - f(m)) * rf(i1,j1)), or + ... + when pos
+  __device__ __forceinline__ double small(const RInd& r, const int a3[3], const int p3[3], const int m3[3], int i0,
+                                          int j0, int i1, int j1, bool pos) const {
+    double s1 = f(r, a3[0]) * rf(i0, j0, 0);
+    s1 = s1 + f(r, a3[1]) * rf(i0, j0, 1);
+    s1 = s1 + f(r, a3[2]) * rf(i0, j0, 2);
+    double s2 = (f(r, p3[0]) - f(r, m3[0])) * rf(i1, j1, 0);
+    s2 = s2 + (f(r, p3[1]) - f(r, m3[1])) * rf(i1, j1, 1);
+    s2 = s2 + (f(r, p3[2]) - f(r, m3[2])) * rf(i1, j1, 2);
+    return pos ? s1 + s2 : -s1 - s2;
+  }
+
+  // interp_flux (src/multi_level.f90:453-482) at child (i, j)
+  __device__ void interp_flux(int i, int j, double sm[4]) const {
+    RInd r = get_indices(i + 1, j, RT);
+    {
+      const int a3[3] = {S_WPM, S_UZM, S_VMM}, p3[3] = {S_VPM, S_WMMM, S_UMZ}, m3[3] = {S_UPZ, S_VPMM, S_WMM};
+      sm[0] = small(r, a3, p3, m3, i + 1, j - 2, i + 1, j - 1, false);
+    }
+    {
+      const int a3[3] = {S_WMP, S_UZP, S_VPP}, p3[3] = {S_VMP, S_WPPP, S_UPZ}, m3[3] = {S_UMZ, S_VMPP, S_WPP};
+      sm[1] = small(r, a3, p3, m3, i, j, i, j + 1, true);
+    }
+    r = get_indices(i, j + 1, UP);
+    {
+      const int a3[3] = {S_UZM, S_VMM, S_WPM}, p3[3] = {S_WMMM, S_UMZ, S_VPM}, m3[3] = {S_VPMM, S_WMM, S_UPZ};
+      sm[2] = small(r, a3, p3, m3, i + 1, j, i + 1, j + 1, false);
+    }
+    {
+      const int a3[3] = {S_UZP, S_VPP, S_WMP}, p3[3] = {S_WPPP, S_UPZ, S_VMP}, m3[3] = {S_VMPP, S_WPP, S_UMZ};
+      sm[3] = small(r, a3, p3, m3, i - 2, j, i - 2, j + 1, true);
+    }
+  }
+
+  // part_coarse_flux (src/multi_level.f90:510-538)
+  __device__ double part_coarse_flux(int i, int j, int e) const {
+    const RInd r = get_indices(i, j, e);
+    double ar0 = a(i, j, 0), ar1 = a(i, j, 1);
+    double o0 = sp(i, j, 0), o1 = sp(i, j, 1);
+    double o2 = a(i, j, 2) - o0, o3 = a(i, j, 3) - o1;
+    ar0 = ar0 + o0 + o3;
+    ar1 = ar1 + o1 + o2;
+    const double s = ar0 + ar1;
+    ar0 = ar0 / s;
+    ar1 = ar1 / s;
+    const int mpi = r.ni[0], mpj = r.nj[0], ppi = r.ni[1], ppj = r.nj[1];
+    const int pmi = r.ni[2], pmj = r.nj[2], mmi = r.ni[3], mmj = r.nj[3];
+    o0 = sp(ppi, ppj, 0);
+    o1 = sp(mmi, mmj, 1);
+    o2 = a(mpi, mpj, 2) - sp(mpi, mpj, 0);
+    o3 = a(pmi, pmj, 3) - sp(pmi, pmj, 1);
+    double t = f(r, S_UPZ) * ar0;
+    t = t + f(r, S_UMZ) * ar1;
+    t = t - (f(r, S_VMM) + f(r, S_WMP)) * ar1;
+    t = t - (f(r, S_WPM) + f(r, S_VPP)) * ar0;
+    t = t + o2 * dsn(mpi, mpj);
+    t = t - o3 * dsn(pmi, pmj);
+    t = t - o0 * dsn(ppi, ppj);
+    return t + o1 * dsn(mmi, mmj);
+  }
+
+  // coarse_flux (src/multi_level.f90:540-573); dscalar reads outside the
+  // padded level take 0 (their area weights are zero there).
+  __device__ double coarse_flux(int i, int j, int e) const {
+    const int hs = c_hex_s_offs[e];
+#define NB(k, X) const int X##i = i + c_nghb_pt[hs + k][0], X##j = j + c_nghb_pt[hs + k][1];
+    NB(1, mz) NB(4, pz) NB(0, mp) NB(5, pp) NB(3, pm) NB(2, mm)
+#undef NB
+    const double wpp = a(ppi, ppj, 2) * a(ppi, ppj, 3) * hi(ppi, ppj);
+    const double wpm = a(pmi, pmj, 2) * a(pmi, pmj, 3) * hi(pmi, pmj);
+    const double wmp = a(mpi, mpj, 2) * a(mpi, mpj, 3) * hi(mpi, mpj);
+    const double wmm = a(mmi, mmj, 2) * a(mmi, mmj, 3) * hi(mmi, mmj);
+    const double d_mm2 = dsn(i + c_bfly_no2[e][0][0], j + c_bfly_no2[e][0][1]);
+    const double d_pm2 = dsn(i + c_bfly_no2[e][1][0], j + c_bfly_no2[e][1][1]);
+    const double d_pp2 = dsn(i + c_bfly_no2[e][2][0], j + c_bfly_no2[e][2][1]);
+    const double d_mp2 = dsn(i + c_bfly_no2[e][3][0], j + c_bfly_no2[e][3][1]);
+    const double dmz = dsn(mzi, mzj), dpz = dsn(pzi, pzj);
+    double c = a(i, j, 0) * a(i, j, 1) * hi(i, j);
+    c = c + a(mpi, mpj, 1) * a(mpi, mpj, 2) * hi(mpi, mpj);
+    c = c + a(ppi, ppj, 0) * a(ppi, ppj, 2) * hi(ppi, ppj);
+    c = c + a(pmi, pmj, 0) * a(pmi, pmj, 3) * hi(pmi, pmj);
+    c = c + a(mmi, mmj, 1) * a(mmi, mmj, 3) * hi(mmi, mmj);
+    double t = c * (dpz - dmz);
+    t = t + wpp * 0.5 * (d_pp2 - dmz);
+    t = t + wpm * 0.5 * (d_pm2 - dmz);
+    t = t + wmp * 0.5 * (dpz - d_mp2);
+    return t + wmm * 0.5 * (dpz - d_mm2);
+  }
+};
+
+// scalar_cpt_restr over parents [0, n]^2, every layer.
+__global__ void k_restr_scalar(WLev P, WLev C, int nz) {
+  const int m = P.n + 1;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nz * 10 * m * m) return;
+  const int ip = (int)(t % m), jp = (int)((t / m) % m), d = (int)((t / ((int64_t)m * m)) % 10);
+  const int k = (int)(t / ((int64_t)10 * m * m));
+  const int idp = nid(P, d, ip, jp);
+  if (P.mask_n[idp] >= M_RESTRCT)
+    P.scal[(int64_t)k * P.NN + idp] = C.scal[(int64_t)k * C.NN + nid(C, d, 2 * ip, 2 * jp)];
+}
+
+// flux_cpt_restr over parents [0, n)^2, every layer.
+__global__ void k_restr_flux(WLev P, WLev C, int nz) {
+  const int m = P.n;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nz * 10 * m * m) return;
+  const int ip = (int)(t % m), jp = (int)((t / m) % m), d = (int)((t / ((int64_t)m * m)) % 10);
+  const int k = (int)(t / ((int64_t)10 * m * m));
+  const int idp = nid(P, d, ip, jp);
+  const int m0 = P.mask_e[idp], m1 = P.mask_e[P.NN + idp], m2 = P.mask_e[2 * P.NN + idp];
+  const int mx = max(max(m0, m1), m2);
+  if (mx < M_RESTRCT) return;
+  const RChild R{C, C.flux + (int64_t)3 * k * C.NN, C.dscal + (int64_t)k * C.NN, d};
+  const int ic = 2 * ip, jc = 2 * jp;
+  double sm[4];
+  R.interp_flux(ic, jc, sm);
+  double* fp = P.flux + (int64_t)3 * k * P.NN;
+  if (m0 >= M_RESTRCT) {
+    const double p = R.part_coarse_flux(ic + 1, jc, RT), c = R.coarse_flux(ic + 1, jc, RT);
+    fp[idp] = p + c + sm[0] + sm[1];
+  }
+  if (m1 >= M_RESTRCT) {
+    const double p = R.part_coarse_flux(ic + 1, jc + 1, DG), c = R.coarse_flux(ic + 1, jc + 1, DG);
+    fp[P.NN + idp] = p + c + sm[1] + sm[2];
+  }
+  if (m2 >= M_RESTRCT) {
+    const double p = R.part_coarse_flux(ic, jc + 1, UP), c = R.coarse_flux(ic, jc + 1, UP);
+    fp[2 * P.NN + idp] = p + c + sm[2] + sm[3];
+  }
+}
+
+// The restriction of u_source_cpt_restr over parents [0, n)^2, every layer.
+__global__ void k_restr_u_source(WLev P, WLev C, int nz) {
+  const int m = P.n;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nz * 10 * m * m) return;
+  const int ip = (int)(t % m), jp = (int)((t / m) % m), d = (int)((t / ((int64_t)m * m)) % 10);
+  const int k = (int)(t / ((int64_t)10 * m * m));
+  const int idp = nid(P, d, ip, jp), idc = nid(C, d, 2 * ip, 2 * jp);
+  const double* vc = C.dvelo + (int64_t)3 * k * C.NN;
+  double* vp = P.dvelo + (int64_t)3 * k * P.NN;
+  if (C.mask_e[idc] >= M_ADJZONE) vp[idp] = vc[idc] + vc[idc + 1];
+  if (C.mask_e[C.NN + idc] >= M_ADJZONE) vp[P.NN + idp] = vc[C.NN + idc] + vc[C.NN + idc + C.P + 1];
+  if (C.mask_e[2 * C.NN + idc] >= M_ADJZONE) vp[2 * P.NN + idp] = vc[2 * C.NN + idc] + vc[2 * C.NN + idc + C.P];
+}
+
+}  // namespace wtw

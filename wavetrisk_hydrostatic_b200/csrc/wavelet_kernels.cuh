@@ -32,6 +32,10 @@ struct WLev {
   int* mask_e;                      // 3*NN
   double *sm, *st, *sv;             // scaling: [nz][NN], [nz][NN], [nz][3*NN]
   double *wm, *wt, *wv;             // wavelets, same shapes
+  const double* __restrict__ split; // 2*NN Overl_Area%split (may be null)
+  const double* __restrict__ rf;    // 3*NN flux-restriction weights (null on the coarsest level)
+  double *scal, *dscal;             // multi-level trend work fields: [nz][NN]
+  double *flux, *dvelo;             // [nz][3*NN]
 };
 
 __constant__ int c_end_pt[3][2][2] = {{{0, 0}, {1, 0}}, {{1, 1}, {0, 0}}, {{0, 0}, {0, 1}}};

@@ -129,6 +129,8 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
     if ((rc = dev_copy(&D.overl_a, ld.overl_a, 4 * NN))) break;
     if ((rc = dev_copy(&D.topo, ld.topo, NN))) break;
     if (ld.iu_wgt && (rc = dev_copy(&D.iu_wgt, ld.iu_wgt, 9 * NN))) break;
+    if (ld.overl_split && (rc = dev_copy(&D.overl_split, ld.overl_split, 2 * NN))) break;
+    if (ld.rf_wgt && (rc = dev_copy(&D.rf_wgt, ld.rf_wgt, 3 * NN))) break;
     std::vector<int2> hn(ld.n_halo_node);
     for (int64_t k = 0; k < ld.n_halo_node; ++k) {
       int64_t a = ld.halo_node[2 * k], b = ld.halo_node[2 * k + 1];

@@ -122,6 +122,21 @@ int wt_step1_flux(wt_handle* h, int itype, int layer, const double* scalar, doub
   return WT_OK;
 }
 
+int wt_step1_vort(wt_handle* h, int layer, double* vort) {
+  if (!h || !vort || layer < 0 || layer >= h->nz) return WT_ERR_ARG;
+  if (int rc = ensure(h)) return rc;
+  BaroCtx* B = static_cast<BaroCtx*>(h->baro);
+  const DevLevel& D = h->top();
+  const size_t NN = (size_t)D.NN;
+  CKB(cudaMemsetAsync(B->grad, 0, 2 * NN * 8, h->stream));
+  const int m = D.n + 1;
+  wtb::k_step1_vort<<<nb(10 * m * m), TPB, 0, h->stream>>>(D.view(), h->velo + 3 * (int64_t)layer * D.NN, B->grad);
+  CKB(cudaGetLastError());
+  CKB(cudaMemcpyAsync(vort, B->grad, 2 * NN * 8, cudaMemcpyDeviceToHost, h->stream));
+  CKB(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
 int wt_barotropic_download(wt_handle* h, double* div_flux, double* rhs, double* grad) {
   if (!h) return WT_ERR_ARG;
   if (!h->baro) return WT_ERR_STATE;

@@ -13,6 +13,8 @@ struct DevLevel {
   double *len = nullptr, *pedlen = nullptr, *part = nullptr, *hex_inv = nullptr, *triarea = nullptr,
          *coriolis = nullptr, *overl_a = nullptr, *topo = nullptr;
   double* iu_wgt = nullptr;  // 9*NN outer velocity weights (levels above level_start)
+  double* overl_split = nullptr;  // 2*NN Overl_Area%split
+  double* rf_wgt = nullptr;       // 3*NN flux-restriction weights (levels above level_start)
   int2* hn = nullptr;
   int3* he = nullptr;
   int n_hn = 0, n_he = 0;
@@ -22,7 +24,7 @@ struct DevLevel {
     return wtk::LevelDev{n, P, (int)NN, len, pedlen, part, hex_inv, triarea, coriolis, topo, nsrc, esrc};
   }
   void release() {
-    double* a[] = {len, pedlen, part, hex_inv, triarea, coriolis, overl_a, topo, iu_wgt};
+    double* a[] = {len, pedlen, part, hex_inv, triarea, coriolis, overl_a, topo, iu_wgt, overl_split, rf_wgt};
     for (double* p : a)
       if (p) cudaFree(p);
     if (hn) cudaFree(hn);
@@ -30,7 +32,7 @@ struct DevLevel {
     if (nsrc) cudaFree(nsrc);
     if (esrc) cudaFree(esrc);
     nsrc = esrc = nullptr;
-    len = pedlen = part = hex_inv = triarea = coriolis = overl_a = topo = iu_wgt = nullptr;
+    len = pedlen = part = hex_inv = triarea = coriolis = overl_a = topo = iu_wgt = overl_split = rf_wgt = nullptr;
     hn = nullptr;
     he = nullptr;
   }

@@ -5,10 +5,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <initializer_list>
 #include <cstdio>
 #include <vector>
 
 #include "../../include/wavetrisk_gpu.h"
+#include "restrict_kernels.cuh"
 #include "wavelet_kernels.cuh"
 #include "wt_handle.cuh"
 
@@ -23,6 +25,7 @@ struct WavLevel {
   double *sm = nullptr, *st = nullptr, *sv = nullptr;  // scaling (owned below level_end)
   double *wm = nullptr, *wt = nullptr, *wv = nullptr;
   int *mask_n = nullptr, *mask_e = nullptr;
+  double *scal = nullptr, *dscal = nullptr, *flux = nullptr, *dvelo = nullptr;  // work fields, on first use
   bool own_scaling = false;
 };
 
@@ -62,6 +65,12 @@ WLev view(wt_handle* h, int l) {
   v.wm = W.wm;
   v.wt = W.wt;
   v.wv = W.wv;
+  v.split = D.overl_split;
+  v.rf = D.rf_wgt;
+  v.scal = W.scal;
+  v.dscal = W.dscal;
+  v.flux = W.flux;
+  v.dvelo = W.dvelo;
   return v;
 }
 
@@ -76,6 +85,22 @@ int fail(const char* where, cudaError_t e) { return wt_handle_fail(where, e); }
 int ready(wt_handle* h) {
   if (!h) return WT_ERR_ARG;
   if (!h->wav) return WT_ERR_STATE;
+  return WT_OK;
+}
+
+// The work field `field` (WT_WORK_*) of level l, allocated and zeroed on first use.
+int work_field(wt_handle* h, int l, int field, double** out, size_t* bytes) {
+  WavLevel& V = ctx(h)->L[l - h->level_start];
+  const size_t nn = (size_t)h->nz * h->at(l).NN;
+  double** slot = field == WT_WORK_SCALAR ? &V.scal : field == WT_WORK_DSCALAR ? &V.dscal
+                : field == WT_WORK_FLUX ? &V.flux : &V.dvelo;
+  const size_t n = (field == WT_WORK_FLUX || field == WT_WORK_DVELO) ? 3 * nn : nn;
+  if (!*slot) {
+    CKW(ctx(h)->alloc(slot, n));
+    CKW(cudaMemsetAsync(*slot, 0, n * 8, h->stream));
+  }
+  *out = *slot;
+  if (bytes) *bytes = n * 8;
   return WT_OK;
 }
 
@@ -178,7 +203,15 @@ int wt_wavelet_setup(wt_handle* h) {
 
 int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
   if (int rc = ready(h)) return rc;
-  if (!src || level < h->level_start || level > h->level_end || field < 0 || field > WT_MASK_EDGE) return WT_ERR_ARG;
+  if (!src || level < h->level_start || level > h->level_end || field < 0 || field > WT_WORK_DVELO) return WT_ERR_ARG;
+  if (field >= WT_WORK_SCALAR) {
+    double* p;
+    size_t bytes;
+    if (int rc = work_field(h, level, field, &p, &bytes)) return rc;
+    CKW(cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, h->stream));
+    CKW(cudaStreamSynchronize(h->stream));
+    return WT_OK;
+  }
   const DevLevel& D = h->at(level);
   WavLevel& V = ctx(h)->L[level - h->level_start];
   const size_t nn = (size_t)h->nz * D.NN;
@@ -192,7 +225,15 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
 
 int wt_download_field(wt_handle* h, int level, int field, void* dst) {
   if (int rc = ready(h)) return rc;
-  if (!dst || level < h->level_start || level > h->level_end || field < 0 || field > WT_MASK_EDGE) return WT_ERR_ARG;
+  if (!dst || level < h->level_start || level > h->level_end || field < 0 || field > WT_WORK_DVELO) return WT_ERR_ARG;
+  if (field >= WT_WORK_SCALAR) {
+    double* p;
+    size_t bytes;
+    if (int rc = work_field(h, level, field, &p, &bytes)) return rc;
+    CKW(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CKW(cudaStreamSynchronize(h->stream));
+    return WT_OK;
+  }
   const DevLevel& D = h->at(level);
   WavLevel& V = ctx(h)->L[level - h->level_start];
   const size_t nn = (size_t)h->nz * D.NN;
@@ -356,6 +397,52 @@ int wt_wt_after_step(wt_handle* h) {
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   h->state_halo_done = false;
+  return WT_OK;
+}
+
+// ---- compute-or-restrict of the multi-level trend (src/multi_level.f90:311-659)
+
+namespace {
+// Parent `level` and child level+1 with the given work fields allocated on both.
+int restrict_pair(wt_handle* h, int level, std::initializer_list<int> fields) {
+  if (int rc = ready(h)) return rc;
+  if (level < h->level_start || level >= h->level_end) return WT_ERR_ARG;
+  for (int f : fields)
+    for (int l = level; l <= level + 1; ++l) {
+      double* p;
+      if (int rc = work_field(h, l, f, &p, nullptr)) return rc;
+    }
+  return WT_OK;
+}
+}  // namespace
+
+int wt_restrict_scalar(wt_handle* h, int level) {
+  if (int rc = restrict_pair(h, level, {WT_WORK_SCALAR})) return rc;
+  const int m = h->at(level).n + 1;
+  k_restr_scalar<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_restrict_flux(wt_handle* h, int level) {
+  if (int rc = restrict_pair(h, level, {WT_WORK_FLUX, WT_WORK_DSCALAR})) return rc;
+  const DevLevel& C = h->at(level + 1);
+  if (!C.rf_wgt || !C.overl_split) return WT_ERR_ARG;
+  const int m = h->at(level).n;
+  k_restr_flux<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_restrict_u_source(wt_handle* h, int level) {
+  if (int rc = restrict_pair(h, level, {WT_WORK_DVELO})) return rc;
+  const int m = h->at(level).n;
+  k_restr_u_source<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1),
+                                                                            h->nz);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
 }
 

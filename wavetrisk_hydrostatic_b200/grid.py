@@ -37,6 +37,8 @@ class LevelGeom:
     halo_node: np.ndarray     # (n_halo_node, 2) int64
     halo_edge: np.ndarray     # (n_halo_edge, 3) int64
     iu_wgt: np.ndarray | None = None   # (9, NN) outer velocity weights I_u_wgt (levels above min_level-1)
+    rf_wgt: np.ndarray | None = None   # (3, NN) flux-restriction weights R_F_wgt (levels above min_level-1)
+    rf_conflict: float = 0.0           # largest difference between two writers of one R_F_wgt slot
     _owned: np.ndarray | None = field(default=None, repr=False)
 
     def idx(self, d, i, j):
@@ -109,6 +111,8 @@ class Grid:
             halo_node=get("halo_node", (dims.n_halo_node, 2), np.int64),
             halo_edge=get("halo_edge", (dims.n_halo_edge, 3), np.int64),
             iu_wgt=get("iu_wgt", (9, NN)) if l > self.min_level - 1 else None,
+            rf_wgt=get("rf_wgt", (3, NN)) if l > self.min_level - 1 else None,
+            rf_conflict=float(get("rf_conflict", (1,))[0]) if l > self.min_level - 1 else 0.0,
         )
         self._levels[l] = g
         return g

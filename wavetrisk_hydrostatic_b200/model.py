@@ -41,10 +41,11 @@ class _LevelDescs:
             he = np.ascontiguousarray(g.halo_edge, dtype=np.int64)
             self.keep += bufs + [hn, he]
             iu = _c(g.iu_wgt) if (g.iu_wgt is not None and q > 0) else None
-            if iu is not None:
-                self.keep.append(iu)
+            rf = _c(g.rf_wgt) if (getattr(g, "rf_wgt", None) is not None and q > 0) else None
+            sp = _c(g.overl_split)
+            self.keep += [x for x in (iu, rf, sp) if x is not None]
             arr[q] = N.wt_level_desc(g.level, g.n, g.P, g.NN, *[N.dptr(b) for b in bufs],
-                                     N.iptr(hn), len(hn), N.iptr(he), len(he), N.dptr(iu))
+                                     N.iptr(hn), len(hn), N.iptr(he), len(he), N.dptr(iu), N.dptr(sp), N.dptr(rf))
         self.arr = arr
 
 
@@ -146,8 +147,16 @@ def _step1_flux(model, itype: int, layer: int = 0, scalar: np.ndarray | None = N
     return flux
 
 
+def _step1_vort(model, layer: int = 0) -> np.ndarray:
+    vort = np.empty(2 * model.g.NN)
+    N.check("wt_step1_vort", N.lib().wt_step1_vort(model.h, int(layer), N.dptr(vort)))
+    return vort
+
+
 TriskModel.step1_flux = _step1_flux
 TriskModel.step1_flux.__doc__ = """step1 itype 1, 5, 6 or 7 on one layer of the resident state: edge flux (3*NN)."""
+TriskModel.step1_vort = _step1_vort
+TriskModel.step1_vort.__doc__ = """step1 itype 8 + post_vort on one layer of the resident velocity: vorticity (2*NN)."""
 
 
 class WaveletHierarchy(DeviceGrid):
@@ -155,10 +164,13 @@ class WaveletHierarchy(DeviceGrid):
     uniform hierarchy, their wavelet coefficients and the node/edge masks, with
     the reference's forward_wavelet_transform, inverse_wavelet_transform,
     mask_tol_vars, compress_wavelets and WT_after_step (src/wavelet.f90,
-    src/mask.f90, src/adapt.f90).  Level level_end's scaling fields are the
+    src/mask.f90, src/adapt.f90), and the multi-level trend's work fields
+    (scalar, dscalar, flux, dvelo) with its compute-or-restrict operators
+    (src/multi_level.f90:311-659).  Level level_end's scaling fields are the
     stepper's state."""
 
-    FIELDS = {"mass": 0, "temp": 1, "velo": 2, "wc_mass": 3, "wc_temp": 4, "wc_velo": 5, "mask_n": 6, "mask_e": 7}
+    FIELDS = {"mass": 0, "temp": 1, "velo": 2, "wc_mass": 3, "wc_temp": 4, "wc_velo": 5, "mask_n": 6, "mask_e": 7,
+              "scalar": 8, "dscalar": 9, "flux": 10, "dvelo": 11}
 
     def __init__(self, levels: list[LevelGeom], topos: list[np.ndarray], nz: int, ph: OceanParams | None = None):
         super().__init__(levels, topos, nz, ph)
@@ -171,7 +183,8 @@ class WaveletHierarchy(DeviceGrid):
             return (NN,), np.int32
         if name == "mask_e":
             return (3 * NN,), np.int32
-        return (self.nz, (3 if name.endswith("velo") else 1) * NN), np.float64
+        edge = name.endswith("velo") or name == "flux"
+        return (self.nz, (3 if edge else 1) * NN), np.float64
 
     def upload(self, level: int, name: str, a: np.ndarray) -> None:
         shape, dt = self._shape(level, name)
@@ -211,6 +224,18 @@ class WaveletHierarchy(DeviceGrid):
 
     def wt_after_step(self) -> None:
         N.check("wt_wt_after_step", N.lib().wt_wt_after_step(self.h))
+
+    def restrict_scalar(self, level: int) -> None:
+        """scalar_cpt_restr of the work scalar from level+1 to level."""
+        N.check("wt_restrict_scalar", N.lib().wt_restrict_scalar(self.h, int(level)))
+
+    def restrict_flux(self, level: int) -> None:
+        """flux_cpt_restr of the work flux from level+1's flux and dscalar."""
+        N.check("wt_restrict_flux", N.lib().wt_restrict_flux(self.h, int(level)))
+
+    def restrict_u_source(self, level: int) -> None:
+        """The restriction of u_source_cpt_restr on the work dvelo."""
+        N.check("wt_restrict_u_source", N.lib().wt_restrict_u_source(self.h, int(level)))
 
 
 def solver_opts(method: str = "fmg", tol: float = 1e-10, **kw):

@@ -205,7 +205,10 @@ enum {
    * a node scalar (Bernoulli or Exner), the scalar trend dscalar, the
    * horizontal flux h_flux and the velocity trend dvelo of every layer. */
   WT_WORK_SCALAR = 8, WT_WORK_DSCALAR = 9,                   /* [nz][NN] doubles                             */
-  WT_WORK_FLUX = 10, WT_WORK_DVELO = 11                      /* [nz][3*NN] doubles                           */
+  WT_WORK_FLUX = 10, WT_WORK_DVELO = 11,                     /* [nz][3*NN] doubles                           */
+  /* Layer means sol_mean(S_MASS/S_TEMP, k) of the level, [nz][NN] doubles; on
+   * level_end they are the stepper's (wt_upload_state). */
+  WT_FIELD_MEAN_MASS = 12, WT_FIELD_MEAN_TEMP = 13
 };
 /* Mask values (src/shared.f90:58-73). */
 enum { WT_MASK_ZERO = 0, WT_MASK_TRSK = 2, WT_MASK_ADJZONE = 8, WT_MASK_RESTRCT = 12, WT_MASK_TOLRNZ = 16,
@@ -265,6 +268,19 @@ int wt_restrict_flux(wt_handle* h, int level);
  * velocity trend of parent edges whose first child edge has mask_e >= ADJZONE
  * is the sum of the two child edges; the others keep the parent's value. */
 int wt_restrict_u_source(wt_handle* h, int level);
+
+/* trend_ml over the whole hierarchy (src/multi_level.f90:5-188), every level
+ * present: per level from level_end down to level_start, integrate_pressure_up,
+ * step1 and post_step1 on the level's scaling fields and layer means, the
+ * compute-or-restrict of Bernoulli, Exner and the mass and Theta fluxes from
+ * the level above (below level_end), scalar_trend with mask_n >= TRSK, the
+ * velocity source computed or restricted (cpt_or_restr_u_source), and du_grad
+ * with mask_n >= TRSK.  Needs wt_wavelet_setup, the masks of every level and
+ * the layer means (WT_FIELD_MEAN_*) below level_end. */
+int wt_trend_multi(wt_handle* h);
+/* The trends of one level from the last wt_trend_multi: dmass, dtemp [nz][NN],
+ * dvelo [nz][3*NN] host doubles (any may be NULL). */
+int wt_download_trend_level(wt_handle* h, int level, double* dmass, double* dtemp, double* dvelo);
 
 /* ---------------------------------------------------------- barotropic ---- */
 /* The free-surface pieces of the mode-split step on level_end, around the

@@ -103,3 +103,40 @@ def get_threads() -> int:
     L = lib()
     L.orc_get_threads.restype = C.c_int
     return int(L.orc_get_threads())
+
+
+class orc_mlevel(C.Structure):
+    _fields_ = [("geo", orc_level), ("overl_a", _dp), ("overl_split", _dp), ("rf_wgt", _dp),
+                ("mask_n", C.POINTER(C.c_int32)), ("mask_e", C.POINTER(C.c_int32)),
+                ("mass", _dp), ("temp", _dp), ("velo", _dp), ("mean_m", _dp), ("mean_t", _dp), ("topo", _dp),
+                ("dmass", _dp), ("dtemp", _dp), ("dvelo", _dp)]
+
+
+def trend_multi(levels, nz, ph, states, masks):
+    """trend_ml over the hierarchy levels[0] .. levels[-1] (level_start ..
+    level_end), every level present.  states[q]: dict of mass, temp, velo,
+    mean_m, mean_t, topo of levels[q]; masks[q]: (mask_n, mask_e) int32.
+    Returns per level (dmass, dtemp, dvelo, state_after_halo)."""
+    L = lib()
+    L.orc_trend_multi.argtypes = [C.POINTER(orc_mlevel), C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+    L.orc_trend_multi.restype = C.c_int
+    arr = (orc_mlevel * len(levels))()
+    keep, out = [], []
+    i32 = C.POINTER(C.c_int32)
+    for q, g in enumerate(levels):
+        lv = _Level(g)
+        st = states[q]
+        m, t, v = (np.ascontiguousarray(st[k], dtype=np.float64).copy() for k in ("mass", "temp", "velo"))
+        mm, mt, tp = (np.ascontiguousarray(st[k], dtype=np.float64) for k in ("mean_m", "mean_t", "topo"))
+        geo = [np.ascontiguousarray(x, dtype=np.float64) for x in (g.overl_a, g.overl_split)]
+        rf = None if (q == 0 or g.rf_wgt is None) else np.ascontiguousarray(g.rf_wgt, dtype=np.float64)
+        mn, me = (np.ascontiguousarray(x, dtype=np.int32) for x in masks[q])
+        dm, dt, dv = np.zeros_like(m), np.zeros_like(t), np.zeros_like(v)
+        keep += [lv, m, t, v, mm, mt, tp, mn, me, dm, dt, dv, rf] + geo
+        arr[q] = orc_mlevel(lv.s, _d(geo[0]), _d(geo[1]), None if rf is None else _d(rf),
+                            mn.ctypes.data_as(i32), me.ctypes.data_as(i32), _d(m), _d(t), _d(v), _d(mm), _d(mt),
+                            _d(tp), _d(dm), _d(dt), _d(dv))
+        out.append((dm, dt, dv, dict(mass=m, temp=t, velo=v)))
+    rc = L.orc_trend_multi(arr, len(levels), nz, ph.grav, ph.ref_density, ph.p_top)
+    assert rc == 0
+    return out

@@ -24,19 +24,7 @@
 #include <cstring>
 #include <vector>
 
-extern "C" {
-struct orc_rlevel {
-  int n, P;
-  int64_t NN;
-  const double *hex_inv, *overl_a, *overl_split, *rf_wgt;  // [NN], [4*NN], [2*NN], [3*NN]
-  const int64_t* hn;
-  int64_t nhn;
-  const int64_t* he;
-  int64_t nhe;
-  const int32_t *mask_n, *mask_e;                            // [NN], [3*NN]
-  double *scal, *dscal, *flux, *dvelo;                       // [nz][NN], [nz][NN], [nz][3*NN], [nz][3*NN]
-};
-}
+#include "oracle_restrict.h"
 
 namespace {
 

@@ -23,6 +23,12 @@
 //   du_grad, gradi_e               src/ops.f90:787-832,1280-1301
 //   RK4, RK_sub_step               src/time_integr.f90:78-103,206-225
 //   cp_bdry_inside                 src/comm.f90:785-808
+//   trend_ml over a hierarchy (orc_trend_multi): basic_operators with the
+//   compute-or-restrict of Bernoulli, Exner and fluxes, cal_scalar_trend,
+//   velocity_trend_source with cpt_or_restr_u_source, velocity_trend_grad
+//   (src/multi_level.f90:5-188, 311-392) and the masks of scalar_trend,
+//   du_source and du_grad (src/ops.f90:750,773,803); the restrictions are
+//   those of oracle_restrict.cpp.
 // Compiled with -O2 -ffp-contract=off (no FMA), like gfortran -O2 on x86-64.
 #include <cstdint>
 #include <cstring>
@@ -31,6 +37,8 @@
 #include <functional>
 #include <mutex>
 #include <thread>
+
+#include "oracle_restrict.h"
 
 namespace {
 
@@ -594,6 +602,217 @@ int orc_rk4(const orc_level* lev, int nz, double grav, double ref_density, doubl
         halo_nodes(L, om + k * NN);
         halo_nodes(L, ot + k * NN);
         halo_edges(L, ov + k * 3 * NN);
+      }
+    }
+  }
+  return 0;
+}
+
+// One level of a uniform hierarchy for trend_ml over levels level_start ..
+// level_end: geometry, weights, masks, state (updated in place by the halo
+// copy) and trends (out).
+struct orc_mlevel {
+  orc_level geo;
+  const double *overl_a, *overl_split, *rf_wgt;  // rf_wgt may be NULL on level_start
+  const int32_t *mask_n, *mask_e;
+  double *mass, *temp, *velo;                    // [nz][NN], [nz][NN], [nz][3*NN]
+  const double *mean_m, *mean_t, *topo;
+  double *dmass, *dtemp, *dvelo;                 // out, same shapes
+};
+
+int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double ref_density, double p_top) {
+  constexpr int TRSK = 2, ADJZONE = 8;
+  Phys ph{grav, ref_density, p_top};
+  std::vector<Lev> L;
+  std::vector<Work> W;
+  for (int q = 0; q < nlev; ++q) {
+    L.push_back(to_lev(&lv[q].geo));
+    W.emplace_back(L[q].NN);
+  }
+  auto ctx = [&](int q, int d, int k) {
+    Ctx c(L[q], ph);
+    Work& w = W[q];
+    const orc_mlevel& m = lv[q];
+    const int64_t NN = L[q].NN;
+    c.d = d;
+    c.qe = w.qe.data(); c.vort = w.vort.data(); c.ke = w.ke.data(); c.bernoulli = w.bernoulli.data();
+    c.exner = w.exner.data(); c.hflux_m = w.hflux_m.data(); c.hflux_t = w.hflux_t.data(); c.geopot = w.geopot.data();
+    c.geopot_lower = w.geopot_lower.data(); c.press = w.press.data(); c.press_lower = w.press_lower.data();
+    c.surf_press = w.surf_press.data(); c.topo = m.topo;
+    c.mass = m.mass + k * NN; c.temp = m.temp + k * NN; c.velo = m.velo + k * 3 * NN;
+    c.mean_m = m.mean_m + k * NN; c.mean_t = m.mean_t + k * NN;
+    return c;
+  };
+  // restriction records of level q with the given layer fields
+  auto rlev = [&](int q, double* scal, double* dscal, double* flux, double* dvelo) {
+    const orc_mlevel& m = lv[q];
+    return orc_rlevel{L[q].n, L[q].P, L[q].NN, L[q].hex_inv, m.overl_a, m.overl_split, m.rf_wgt,
+                      L[q].hnode, L[q].n_hnode, L[q].hedge, L[q].n_hedge, m.mask_n, m.mask_e,
+                      scal, dscal, flux, dvelo};
+  };
+  // update_bdry(q, NONE) and zero_float_field of the trends
+  for (int q = 0; q < nlev; ++q) {
+    const int64_t NN = L[q].NN;
+    for (int k = 0; k < nz; ++k) {
+      halo_nodes(L[q], lv[q].mass + k * NN);
+      halo_nodes(L[q], lv[q].temp + k * NN);
+      halo_edges(L[q], lv[q].velo + k * 3 * NN);
+    }
+    std::memset(lv[q].dmass, 0, nz * NN * sizeof(double));
+    std::memset(lv[q].dtemp, 0, nz * NN * sizeof(double));
+    std::memset(lv[q].dvelo, 0, 3 * nz * NN * sizeof(double));
+  }
+  // cal_surf_press on every level
+  for (int q = 0; q < nlev; ++q) {
+    const int64_t NN = L[q].NN;
+    const int n = L[q].n;
+    Work& w = W[q];
+    const orc_mlevel& m = lv[q];
+    for (int64_t id = 0; id < NN; ++id) w.surf_press[id] = 0.0;
+    for (int d = 0; d < 10; ++d) {
+      Ctx c = ctx(q, d, 0);
+      for (int j = -1; j <= n + 1; ++j)
+        for (int i = -1; i <= n + 1; ++i) w.geopot[c.id(i, j)] = ph.grav * m.topo[c.id(i, j)];
+      for (int k = 0; k < nz; ++k)
+        for (int j = 0; j <= n; ++j)
+          for (int i = 0; i <= n; ++i) {
+            const int64_t id = c.id(i, j);
+            const double rho_dz = m.mean_m[k * NN + id] + m.mass[k * NN + id];
+            const double rho_dz_theta = m.mean_t[k * NN + id] + m.temp[k * NN + id];
+            w.surf_press[id] = w.surf_press[id] + (rho_dz - rho_dz_theta);
+          }
+    }
+    for (int64_t id = 0; id < NN; ++id) {
+      w.surf_press[id] = ph.grav * w.surf_press[id] + ph.p_top;
+      w.press_lower[id] = w.surf_press[id];
+    }
+  }
+  for (int k = 0; k < nz; ++k) {
+    for (int q = nlev - 1; q >= 0; --q) {
+      const Lev& Lq = L[q];
+      const int64_t NN = Lq.NN;
+      const int n = Lq.n;
+      Work& w = W[q];
+      const orc_mlevel& m = lv[q];
+      // basic_operators
+      for (int d = 0; d < 10; ++d) {
+        Ctx c = ctx(q, d, k);
+        for (int j = 0; j <= n; ++j)
+          for (int i = 0; i <= n; ++i) {
+            const int64_t id = c.id(i, j);
+            const double rho_dz = c.mean_m[id] + c.mass[id];
+            const double rho_dz_theta = c.mean_t[id] + c.temp[id];
+            w.geopot_lower[id] = w.geopot[id];
+            const double p_upper = w.press_lower[id] - ph.grav * (rho_dz - rho_dz_theta);
+            w.press[id] = interp(w.press_lower[id], p_upper);
+            w.geopot[id] = w.geopot_lower[id] + ph.grav * rho_dz / (ph.ref_density * 1.0);
+            w.press_lower[id] = p_upper;
+          }
+        step1(c);
+        for (int corner = 5; corner <= 8; ++corner) post_step1(c, corner);
+      }
+      if (q < nlev - 1) {
+        Work& wc = W[q + 1];
+        const int64_t NC = L[q + 1].NN;
+        orc_rlevel P = rlev(q, w.bernoulli.data(), nullptr, nullptr, nullptr);
+        orc_rlevel C = rlev(q + 1, wc.bernoulli.data(), nullptr, nullptr, nullptr);
+        orc_restrict_scalar(&P, &C, 1);
+        P.scal = w.exner.data();
+        C.scal = wc.exner.data();
+        orc_restrict_scalar(&P, &C, 1);
+        P.flux = w.hflux_m.data();
+        C.flux = wc.hflux_m.data();
+        C.dscal = lv[q + 1].dmass + k * NC;
+        orc_restrict_flux(&P, &C, 1);
+        P.flux = w.hflux_t.data();
+        C.flux = wc.hflux_t.data();
+        C.dscal = lv[q + 1].dtemp + k * NC;
+        orc_restrict_flux(&P, &C, 1);
+      }
+      // cal_scalar_trend: update_bdry(horiz_flux, l), scalar_trend over [0, n]
+      halo_edges(Lq, w.hflux_m.data());
+      halo_edges(Lq, w.hflux_t.data());
+      for (int d = 0; d < 10; ++d) {
+        Ctx c = ctx(q, d, k);
+        for (int j = 0; j <= n; ++j)
+          for (int i = 0; i <= n; ++i) {
+            const int64_t id = c.id(i, j);
+            const bool on = m.mask_n[id] >= TRSK;
+            m.dmass[k * NN + id] = on ? -divg(c, w.hflux_m.data(), i, j) : 0.0;
+            m.dtemp[k * NN + id] = on ? -divg(c, w.hflux_t.data(), i, j) : 0.0;
+          }
+      }
+      // velocity_trend_source
+      double* dv = m.dvelo + k * 3 * NN;
+      auto u_source = [&](Ctx& c, int i, int j) {
+        const int64_t id = c.id(i, j);
+        if (m.mask_n[id] >= TRSK) {
+          double Q[3];
+          Qperp(c, i, j, Q);
+          for (int e = 0; e < 3; ++e) dv[e * NN + id] = -Q[e] + 0.0 * Lq.len[e * NN + id];
+        } else {
+          for (int e = 0; e < 3; ++e) dv[e * NN + id] = 0.0;
+        }
+      };
+      if (q == nlev - 1) {
+        for (int d = 0; d < 10; ++d) {
+          Ctx c = ctx(q, d, k);
+          for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) u_source(c, i, j);
+        }
+      } else {
+        const Lev& Lc = L[q + 1];
+        const int32_t* mc = lv[q + 1].mask_e;
+        for (int d = 0; d < 10; ++d) {
+          Ctx c = ctx(q, d, k);
+          for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+              const int64_t idc = ((int64_t)d * Lc.P + 2 * j + 2) * Lc.P + 2 * i + 2;
+              int mn = mc[idc];
+              for (int e = 1; e < 3; ++e) mn = mc[e * Lc.NN + idc] < mn ? mc[e * Lc.NN + idc] : mn;
+              if (mn < ADJZONE) u_source(c, i, j);
+            }
+        }
+        orc_rlevel P = rlev(q, nullptr, nullptr, nullptr, dv);
+        orc_rlevel C = rlev(q + 1, nullptr, nullptr, nullptr, lv[q + 1].dvelo + k * 3 * Lc.NN);
+        orc_restrict_u_source(&P, &C, 1);
+      }
+    }
+    // velocity_trend_grad on every level
+    for (int q = 0; q < nlev; ++q) {
+      const Lev& Lq = L[q];
+      const int64_t NN = Lq.NN;
+      const int n = Lq.n;
+      Work& w = W[q];
+      const orc_mlevel& m = lv[q];
+      double* dv = m.dvelo + k * 3 * NN;
+      for (int d = 0; d < 10; ++d) {
+        Ctx c = ctx(q, d, k);
+        for (int j = 0; j < n; ++j)
+          for (int i = 0; i < n; ++i) {
+            const int64_t id = c.id(i, j), idE = c.id(i + 1, j), idN = c.id(i, j + 1), idNE = c.id(i + 1, j + 1);
+            if (m.mask_n[id] < TRSK) {
+              for (int e = 0; e < 3; ++e) dv[e * NN + id] = 0.0;
+              continue;
+            }
+            const int64_t ids[4] = {id, idE, idNE, idN};
+            double theta[4];
+            for (int t = 0; t < 4; ++t) {
+              const double rdz = c.mean_m[ids[t]] + c.mass[ids[t]];
+              const double rdzt = c.mean_t[ids[t]] + c.temp[ids[t]];
+              theta[t] = rdzt / rdz;
+            }
+            const double theta_e[3] = {interp(theta[0], theta[1]), interp(theta[0], theta[2]),
+                                       interp(theta[0], theta[3])};
+            const double* B = w.bernoulli.data();
+            const double* X = w.exner.data();
+            const double gradB[3] = {(B[idE] - B[id]) / Lq.len[RT * NN + id], (B[id] - B[idNE]) / Lq.len[DG * NN + id],
+                                     (B[idN] - B[id]) / Lq.len[UP * NN + id]};
+            const double gradE[3] = {(X[idE] - X[id]) / Lq.len[RT * NN + id], (X[id] - X[idNE]) / Lq.len[DG * NN + id],
+                                     (X[idN] - X[id]) / Lq.len[UP * NN + id]};
+            for (int e = 0; e < 3; ++e)
+              dv[e * NN + id] = dv[e * NN + id] / Lq.len[e * NN + id] - gradB[e] - theta_e[e] * gradE[e];
+          }
       }
     }
   }

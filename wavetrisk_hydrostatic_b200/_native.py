@@ -130,6 +130,8 @@ _DEVICE_SIGS = {
     "wt_mask_build": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "wt_wt_after_step": [_vp],
     "wt_step1_vort": [_vp, C.c_int, _dp],
+    "wt_trend_multi": [_vp],
+    "wt_download_trend_level": [_vp, C.c_int, _dp, _dp, _dp],
     "wt_restrict_scalar": [_vp, C.c_int],
     "wt_restrict_flux": [_vp, C.c_int],
     "wt_restrict_u_source": [_vp, C.c_int],

@@ -329,22 +329,6 @@ struct TrendIO {
   double* dm; double* dtt; double* dv;
 };
 
-__device__ __forceinline__ void weights5(const LevelDev& L, int id, int offs, double w[5]) {  // get_weights
-  const int NN = L.NN;
-  double acc = L.part[offs * NN + id];
-  double hinv = L.hex_inv[id];
-  double wgt[5];
-  wgt[0] = acc;
-#pragma unroll
-  for (int q = 2; q <= 5; ++q) {
-    acc = acc + L.part[((q + offs - 1) % 6) * NN + id];
-    wgt[q - 1] = acc;
-  }
-#pragma unroll
-  for (int q = 0; q < 5; ++q) wgt[q] = 0.5 - wgt[q] * hinv;
-  w[0] = wgt[0]; w[1] = -wgt[1]; w[2] = wgt[2]; w[3] = -wgt[3]; w[4] = wgt[4];
-}
-
 template <int MODE>
 __global__ void __launch_bounds__(NODE_TILE, 3) k_trend(LevelDev L, int nz, TrendIO io) {
   int k, id, i, j;
@@ -372,32 +356,10 @@ __global__ void __launch_bounds__(NODE_TILE, 3) k_trend(LevelDev L, int nz, Tren
   if (own) {
     const double* __restrict__ hm = io.hfm + 3 * ko;
     const double* __restrict__ qe = io.qe + 3 * ko;
-    const int idNW = id + P - 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idE = id + 1, idSW = id - P - 1,
-              idS = id - P, idSE = id - P + 1;
-#define TQ(e1, n1, q0, w) (R.e(hm, (e1) * NN + (n1)) * interp(qe[(e1) * NN + (n1)], (q0)) * (w))
-    double w1[5], w2[5];
-    double q0 = qe[RT * NN + id];
-    weights5(L, id, 0, w1);
-    weights5(L, idE, 3, w2);
-    const double Q0 = TQ(DG, id, q0, w1[0]) + TQ(UP, id, q0, w1[1]) + TQ(RT, idW, q0, w1[2]) +
-                      TQ(DG, idSW, q0, w1[3]) + TQ(UP, idS, q0, w1[4]) + TQ(DG, idS, q0, w2[0]) +
-                      TQ(UP, idSE, q0, w2[1]) + TQ(RT, idE, q0, w2[2]) + TQ(DG, idE, q0, w2[3]) +
-                      TQ(UP, idE, q0, w2[4]);
-    q0 = qe[DG * NN + id];
-    weights5(L, id, 1, w1);
-    weights5(L, idNE, 4, w2);
-    const double Q1 = TQ(UP, id, q0, w1[0]) + TQ(RT, idW, q0, w1[1]) + TQ(DG, idSW, q0, w1[2]) +
-                      TQ(UP, idS, q0, w1[3]) + TQ(RT, id, q0, w1[4]) + TQ(UP, idE, q0, w2[0]) +
-                      TQ(RT, idNE, q0, w2[1]) + TQ(DG, idNE, q0, w2[2]) + TQ(UP, idNE, q0, w2[3]) +
-                      TQ(RT, idN, q0, w2[4]);
-    q0 = qe[UP * NN + id];
-    weights5(L, id, 2, w1);
-    weights5(L, idN, 5, w2);
-    const double Q2 = TQ(RT, idW, q0, w1[0]) + TQ(DG, idSW, q0, w1[1]) + TQ(UP, idS, q0, w1[2]) +
-                      TQ(RT, id, q0, w1[3]) + TQ(DG, id, q0, w1[4]) + TQ(RT, idN, q0, w2[0]) +
-                      TQ(DG, idN, q0, w2[1]) + TQ(UP, idN, q0, w2[2]) + TQ(RT, idNW, q0, w2[3]) +
-                      TQ(DG, idW, q0, w2[4]);
-#undef TQ
+    const int idN = id + P, idNE = id + P + 1, idE = id + 1;
+    double Q[3];
+    qperp(L, R, hm, qe, id, Q);
+    const double Q0 = Q[0], Q1 = Q[1], Q2 = Q[2];
     // du_grad
     const double* __restrict__ th = io.theta + ko;
     const double th0 = th[id], thE = th[idE], thNE = th[idNE], thN = th[idN];

@@ -1,0 +1,102 @@
+// Trend of one level of the multi-level trend_ml (src/multi_level.f90:5-188):
+// scalar_trend with its mask, the velocity source computed (du_source) or
+// restricted from the child level (u_source_cpt_restr, src/multi_level.f90:
+// 365-392), and du_grad with its mask (src/ops.f90:739-832), in one pass per
+// (layer, node).  The Bernoulli function, Phi_k and the mass and Theta fluxes
+// it reads are those of the level after their compute-or-restrict step.
+#pragma once
+#include "trisk_read.cuh"
+
+namespace wtk {
+
+struct TrendML {
+  const double* __restrict__ theta;  // Theta/rho of the level's state (k_step1)
+  const double* __restrict__ qe;
+  const double* __restrict__ hfm;
+  const double* __restrict__ hft;
+  const double* __restrict__ bern;
+  const double* __restrict__ phik;    // exner = -Phi_k
+  const int* __restrict__ mask_n;     // [NN] of the level
+  const int* __restrict__ mask_e_chd; // [3*NN_chd] of level+1; null on level_end
+  const double* __restrict__ src_chd; // [nz][3][NN_chd] velocity sources of level+1; null on level_end
+  int P_chd, NN_chd;
+  double* dm;
+  double* dtt;
+  double* dv;
+  double* src;                        // [nz][3][NN] velocity sources of this level (for level-1)
+};
+
+constexpr int ML_TRSK = 2, ML_ADJZONE = 8;
+
+__global__ void __launch_bounds__(NODE_TILE, 3) k_trend_ml(LevelDev L, int nz, TrendML io) {
+  int k, id, i, j;
+  if (!layer_node(L, nz, k, id, i, j)) return;
+  const int P = L.P;
+  const int NN = L.NN;
+  const int n = L.n;
+  const int64_t ko = (int64_t)k * NN;
+  const Rd R(L, i >= 1 && j >= 1 && i <= n - 2 && j <= n - 2);
+  const bool on = io.mask_n[id] >= ML_TRSK;
+  if (i >= 0 && j >= 0 && i <= n && j <= n) {
+    double dms = 0.0, dts = 0.0;
+    if (on) {
+      const int idW = id - 1, idS = id - P, idSW = id - P - 1;
+      const double* __restrict__ fm = io.hfm + 3 * ko;
+      const double* __restrict__ ft = io.hft + 3 * ko;
+      const double hinv = L.hex_inv[id];
+      const double divm = (R.e(fm, RT * NN + id) - R.e(fm, RT * NN + idW) + R.e(fm, DG * NN + idSW) -
+                           R.e(fm, DG * NN + id) + R.e(fm, UP * NN + id) - R.e(fm, UP * NN + idS)) * hinv;
+      const double divt = (R.e(ft, RT * NN + id) - R.e(ft, RT * NN + idW) + R.e(ft, DG * NN + idSW) -
+                           R.e(ft, DG * NN + id) + R.e(ft, UP * NN + id) - R.e(ft, UP * NN + idS)) * hinv;
+      dms = -divm;
+      dts = -divt;
+    }
+    io.dm[ko + id] = dms;
+    io.dtt[ko + id] = dts;
+  }
+  if (!(i >= 0 && j >= 0 && i < n && j < n)) return;
+  const double len3[3] = {L.len[RT * NN + id], L.len[DG * NN + id], L.len[UP * NN + id]};
+  double s[3];
+  bool restr[3] = {false, false, false};
+  if (io.src_chd) {
+    const int d = id / (P * P);
+    const int Pc = io.P_chd, NC = io.NN_chd;
+    const int idc = (d * Pc + 2 * j + 2) * Pc + 2 * i + 2;
+    const int nbc[3] = {1, Pc + 1, Pc};  // E, NE, N child of the edge
+    const double* __restrict__ sc = io.src_chd + (int64_t)3 * k * NC;
+#pragma unroll
+    for (int e = 0; e < 3; ++e)
+      if (io.mask_e_chd[e * NC + idc] >= ML_ADJZONE) {
+        restr[e] = true;
+        s[e] = sc[e * NC + idc] + sc[e * NC + idc + nbc[e]];
+      }
+  }
+  if (!(restr[0] && restr[1] && restr[2])) {
+    double Q[3] = {0.0, 0.0, 0.0};
+    if (on) qperp(L, R, io.hfm + 3 * ko, io.qe + 3 * ko, id, Q);
+#pragma unroll
+    for (int e = 0; e < 3; ++e)
+      if (!restr[e]) s[e] = on ? -Q[e] + 0.0 * len3[e] : 0.0;
+  }
+  const int64_t vo = 3 * ko + id;
+#pragma unroll
+  for (int e = 0; e < 3; ++e) io.src[vo + e * NN] = s[e];
+  if (!on) {
+#pragma unroll
+    for (int e = 0; e < 3; ++e) io.dv[vo + e * NN] = 0.0;
+    return;
+  }
+  const int idN = id + P, idNE = id + P + 1, idE = id + 1;
+  const double* __restrict__ th = io.theta + ko;
+  const double th0 = th[id], thE = th[idE], thNE = th[idNE], thN = th[idN];
+  const double* __restrict__ B = io.bern + ko;
+  const double* __restrict__ F = io.phik + ko;
+  const double gB0 = (B[idE] - B[id]) / len3[0], gB1 = (B[id] - B[idNE]) / len3[1], gB2 = (B[idN] - B[id]) / len3[2];
+  const double xE = -F[idE], x0 = -F[id], xNE = -F[idNE], xN = -F[idN];
+  const double gE0 = (xE - x0) / len3[0], gE1 = (x0 - xNE) / len3[1], gE2 = (xN - x0) / len3[2];
+  io.dv[vo] = s[0] / len3[0] - gB0 - interp(th0, thE) * gE0;
+  io.dv[vo + NN] = s[1] / len3[1] - gB1 - interp(th0, thNE) * gE1;
+  io.dv[vo + 2 * NN] = s[2] / len3[2] - gB2 - interp(th0, thN) * gE2;
+}
+
+}  // namespace wtk

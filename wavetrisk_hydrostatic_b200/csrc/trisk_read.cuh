@@ -7,6 +7,7 @@
 
 #include "trisk_types.cuh"
 
+
 namespace wtk {
 
 __device__ __forceinline__ double interp(double a, double b) { return 0.5 * (a + b); }  // src/utils.f90:528
@@ -52,5 +53,52 @@ struct Rd {
     return (c & 1) ? -v : v;
   }
 };
+
+__device__ __forceinline__ void weights5(const LevelDev& L, int id, int offs, double w[5]) {  // get_weights
+  const int NN = L.NN;
+  double acc = L.part[offs * NN + id];
+  double hinv = L.hex_inv[id];
+  double wgt[5];
+  wgt[0] = acc;
+#pragma unroll
+  for (int q = 2; q <= 5; ++q) {
+    acc = acc + L.part[((q + offs - 1) % 6) * NN + id];
+    wgt[q - 1] = acc;
+  }
+#pragma unroll
+  for (int q = 0; q < 5; ++q) wgt[q] = 0.5 - wgt[q] * hinv;
+  w[0] = wgt[0]; w[1] = -wgt[1]; w[2] = wgt[2]; w[3] = -wgt[3]; w[4] = wgt[4];
+}
+
+// Qperp (src/ops.f90:834-901): the TRiSK Coriolis term of the three edges of
+// node id from the mass flux hm and qe of one layer (ghost edges of hm read
+// through the remap).
+__device__ __forceinline__ void qperp(const LevelDev& L, const Rd& R, const double* __restrict__ hm,
+                                      const double* __restrict__ qe, int id, double Q[3]) {
+  const int P = L.P, NN = L.NN;
+  const int idNW = id + P - 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idE = id + 1, idSW = id - P - 1,
+            idS = id - P, idSE = id - P + 1;
+#define TQ(e1, n1, q0, w) (R.e(hm, (e1) * NN + (n1)) * interp(qe[(e1) * NN + (n1)], (q0)) * (w))
+  double w1[5], w2[5];
+  double q0 = qe[RT * NN + id];
+  weights5(L, id, 0, w1);
+  weights5(L, idE, 3, w2);
+  Q[0] = TQ(DG, id, q0, w1[0]) + TQ(UP, id, q0, w1[1]) + TQ(RT, idW, q0, w1[2]) + TQ(DG, idSW, q0, w1[3]) +
+         TQ(UP, idS, q0, w1[4]) + TQ(DG, idS, q0, w2[0]) + TQ(UP, idSE, q0, w2[1]) + TQ(RT, idE, q0, w2[2]) +
+         TQ(DG, idE, q0, w2[3]) + TQ(UP, idE, q0, w2[4]);
+  q0 = qe[DG * NN + id];
+  weights5(L, id, 1, w1);
+  weights5(L, idNE, 4, w2);
+  Q[1] = TQ(UP, id, q0, w1[0]) + TQ(RT, idW, q0, w1[1]) + TQ(DG, idSW, q0, w1[2]) + TQ(UP, idS, q0, w1[3]) +
+         TQ(RT, id, q0, w1[4]) + TQ(UP, idE, q0, w2[0]) + TQ(RT, idNE, q0, w2[1]) + TQ(DG, idNE, q0, w2[2]) +
+         TQ(UP, idNE, q0, w2[3]) + TQ(RT, idN, q0, w2[4]);
+  q0 = qe[UP * NN + id];
+  weights5(L, id, 2, w1);
+  weights5(L, idN, 5, w2);
+  Q[2] = TQ(RT, idW, q0, w1[0]) + TQ(DG, idSW, q0, w1[1]) + TQ(UP, idS, q0, w1[2]) + TQ(RT, id, q0, w1[3]) +
+         TQ(DG, id, q0, w1[4]) + TQ(RT, idN, q0, w2[0]) + TQ(DG, idN, q0, w2[1]) + TQ(UP, idN, q0, w2[2]) +
+         TQ(RT, idNW, q0, w2[3]) + TQ(DG, idW, q0, w2[4]);
+#undef TQ
+}
 
 }  // namespace wtk

@@ -349,6 +349,20 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   return WT_OK;
 }
 
+int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
+                   const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
+                   double* bern, double* theta) {
+  const DevLevel& D = h->at(level);
+  const LevelDev L = D.view();
+  const int nz = h->nz;
+  const unsigned chunks = blocks_for(D.NN, NODE_TILE);
+  k_column<<<chunks, NODE_TILE, 0, h->stream>>>(L, h->ph, nz, m, t, mean_m, mean_t, phik, pterm);
+  Step1Out so{qe, hfm, hft, bern, theta};
+  k_step1<<<chunks * nz, NODE_TILE, 0, h->stream>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so);
+  CK(cudaGetLastError());
+  return WT_OK;
+}
+
 extern "C" {
 
 int wt_trend(wt_handle* h) {

@@ -105,6 +105,7 @@ static void ell_free(Ell* E) {
 void wt_handle::release_extra() {
   if (ell) ell_free(static_cast<Ell*>(ell));
   ell = nullptr;
+  wt_trend_ml_release(this);
   wt_wavelet_release(this);
   wt_barotropic_release(this);
 }

@@ -66,6 +66,8 @@ struct wt_handle {
   void* wav = nullptr;
   // free-surface fields of the barotropic step (allocated on first use)
   void* baro = nullptr;
+  // per-level operator arrays of the multi-level trend (allocated on first use)
+  void* ml = nullptr;
   void release_extra();
 
   DevLevel& top() { return lev.back(); }
@@ -75,3 +77,22 @@ struct wt_handle {
 int wt_handle_fail(const char* where, cudaError_t e);
 void wt_wavelet_release(wt_handle* h);
 void wt_barotropic_release(wt_handle* h);
+void wt_trend_ml_release(wt_handle* h);
+
+// Launchers shared between translation units (stream-ordered, no sync).
+// integrate_pressure_up + step1 (itype 0) + post_step1 of every layer of `level`
+// on the given state, into the given operator arrays (wt_api.cu).
+int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
+                   const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
+                   double* bern, double* theta);
+// scalar_cpt_restr / flux_cpt_restr of every layer from level+1 to `level`
+// with the masks of the hierarchy (wt_wavelet.cu).
+int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd);
+int wt_level_restrict_flux(wt_handle* h, int level, double* par_flux, const double* chd_flux,
+                           const double* chd_dscal);
+// The layer mean WT_FIELD_MEAN_MASS/TEMP of a level (wt_wavelet.cu).
+int wt_level_mean(wt_handle* h, int level, int field, double** out);
+// The masks of a level, or null before wt_wavelet_setup (wt_wavelet.cu).
+void wt_level_masks(wt_handle* h, int level, const int** mask_n, const int** mask_e);
+// The scaling fields (mass, Theta, velocity) of a level (wt_wavelet.cu).
+void wt_level_state(wt_handle* h, int level, double** m, double** t, double** v);

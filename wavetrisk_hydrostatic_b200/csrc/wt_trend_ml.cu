@@ -1,0 +1,130 @@
+// C-ABI of trend_ml over the handle's whole hierarchy (src/multi_level.f90:5-188):
+// per level, fine to coarse, the level's operator arrays are computed by the
+// single-level column and step1 kernels, the coarse ones are then restricted
+// from the level above, and k_trend_ml finishes the level (scalar trends,
+// velocity source computed or restricted, gradient terms).  All layers of a
+// level are processed per launch: the layers interact only through the
+// pressure column, which k_column integrates bottom-up.
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/wavetrisk_gpu.h"
+#include "trisk_ml.cuh"
+#include "wt_handle.cuh"
+
+namespace {
+
+struct MLLevel {
+  double *phik = nullptr, *pterm = nullptr, *qe = nullptr, *hfm = nullptr, *hft = nullptr, *bern = nullptr,
+         *theta = nullptr, *dm = nullptr, *dt = nullptr, *dv = nullptr, *src = nullptr;
+};
+
+struct MLCtx {
+  std::vector<MLLevel> L;
+  std::vector<void*> allocs;
+};
+
+#define CKM(x)                                            \
+  do {                                                    \
+    cudaError_t e_ = (x);                                 \
+    if (e_ != cudaSuccess) return wt_handle_fail(#x, e_); \
+  } while (0)
+
+int ensure(wt_handle* h) {
+  if (h->ml) return WT_OK;
+  MLCtx* M = new MLCtx();
+  h->ml = M;
+  M->L.resize(h->level_end - h->level_start + 1);
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    MLLevel& V = M->L[l - h->level_start];
+    const size_t nn = (size_t)h->nz * h->at(l).NN;
+    double** node[] = {&V.phik, &V.pterm, &V.bern, &V.theta, &V.dm, &V.dt};
+    double** edge[] = {&V.qe, &V.hfm, &V.hft, &V.dv, &V.src};
+    for (double** p : node) {
+      CKM(cudaMalloc(p, nn * 8));
+      M->allocs.push_back(*p);
+      CKM(cudaMemsetAsync(*p, 0, nn * 8, h->stream));
+    }
+    for (double** p : edge) {
+      CKM(cudaMalloc(p, 3 * nn * 8));
+      M->allocs.push_back(*p);
+      CKM(cudaMemsetAsync(*p, 0, 3 * nn * 8, h->stream));
+    }
+  }
+  return WT_OK;
+}
+
+}  // namespace
+
+void wt_trend_ml_release(wt_handle* h) {
+  if (!h || !h->ml) return;
+  MLCtx* M = static_cast<MLCtx*>(h->ml);
+  for (void* p : M->allocs) cudaFree(p);
+  delete M;
+  h->ml = nullptr;
+}
+
+extern "C" {
+
+int wt_trend_multi(wt_handle* h) {
+  if (!h) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure(h)) return rc;
+  MLCtx* M = static_cast<MLCtx*>(h->ml);
+  const int nz = h->nz;
+  for (int l = h->level_end; l >= h->level_start; --l) {
+    MLLevel& V = M->L[l - h->level_start];
+    const DevLevel& D = h->at(l);
+    double *m, *t, *v, *mm, *mt;
+    if (l == h->level_end) {
+      m = h->mass;
+      t = h->temp;
+      v = h->velo;
+    } else {
+      wt_level_state(h, l, &m, &t, &v);
+    }
+    if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
+    if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
+    if (int rc = wt_level_step1(h, l, m, t, v, mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern, V.theta))
+      return rc;
+    wtk::TrendML io{};
+    const int *mask_n, *mask_e;
+    wt_level_masks(h, l, &mask_n, &mask_e);
+    io.mask_n = mask_n;
+    if (l < h->level_end) {
+      MLLevel& C = M->L[l + 1 - h->level_start];
+      if (int rc = wt_level_restrict_scalar(h, l, V.bern, C.bern)) return rc;
+      if (int rc = wt_level_restrict_scalar(h, l, V.phik, C.phik)) return rc;  // exner = -Phi_k
+      if (int rc = wt_level_restrict_flux(h, l, V.hfm, C.hfm, C.dm)) return rc;
+      if (int rc = wt_level_restrict_flux(h, l, V.hft, C.hft, C.dt)) return rc;
+      const int *mask_n_c, *mask_e_c;
+      wt_level_masks(h, l + 1, &mask_n_c, &mask_e_c);
+      io.mask_e_chd = mask_e_c;
+      io.src_chd = C.src;
+      io.P_chd = h->at(l + 1).P;
+      io.NN_chd = (int)h->at(l + 1).NN;
+    }
+    io.theta = V.theta; io.qe = V.qe; io.hfm = V.hfm; io.hft = V.hft; io.bern = V.bern; io.phik = V.phik;
+    io.dm = V.dm; io.dtt = V.dt; io.dv = V.dv; io.src = V.src;
+    const unsigned chunks = (unsigned)((D.NN + wtk::NODE_TILE - 1) / wtk::NODE_TILE);
+    wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
+    CKM(cudaGetLastError());
+  }
+  CKM(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_download_trend_level(wt_handle* h, int level, double* dmass, double* dtemp, double* dvelo) {
+  if (!h || level < h->level_start || level > h->level_end) return WT_ERR_ARG;
+  if (!h->ml) return WT_ERR_STATE;
+  MLLevel& V = static_cast<MLCtx*>(h->ml)->L[level - h->level_start];
+  const size_t nn = (size_t)h->nz * h->at(level).NN;
+  if (dmass) CKM(cudaMemcpyAsync(dmass, V.dm, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (dtemp) CKM(cudaMemcpyAsync(dtemp, V.dt, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (dvelo) CKM(cudaMemcpyAsync(dvelo, V.dv, 3 * nn * 8, cudaMemcpyDeviceToHost, h->stream));
+  CKM(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// Device storage of the multi-level fields of a handle (h->wav): per level the
+// scaling fields below level_end, the wavelet coefficients, the masks, the
+// work fields of the compute-or-restrict operators and the layer means; and
+// the WLev view that the wavelet, mask and restriction kernels take.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "wavelet_kernels.cuh"
+#include "wt_handle.cuh"
+
+namespace wtw {
+
+struct WavLevel {
+  double *sm = nullptr, *st = nullptr, *sv = nullptr;  // scaling (owned below level_end)
+  double *wm = nullptr, *wt = nullptr, *wv = nullptr;
+  int *mask_n = nullptr, *mask_e = nullptr;
+  double *scal = nullptr, *dscal = nullptr, *flux = nullptr, *dvelo = nullptr;  // work fields, on first use
+  double *mean_m = nullptr, *mean_t = nullptr;  // layer means below level_end, on first use
+  bool own_scaling = false;
+};
+
+struct WavCtx {
+  std::vector<WavLevel> L;
+  double* thr = nullptr;  // [3][nz] thresholds
+  std::vector<void*> allocs;
+  template <class T>
+  cudaError_t alloc(T** p, size_t count) {
+    cudaError_t e = cudaMalloc(p, count * sizeof(T));
+    if (e == cudaSuccess) allocs.push_back(*p);
+    return e;
+  }
+};
+
+inline WavCtx* ctx(wt_handle* h) { return static_cast<WavCtx*>(h->wav); }
+
+inline WLev view(wt_handle* h, int l) {
+  const DevLevel& D = h->at(l);
+  WavLevel& W = ctx(h)->L[l - h->level_start];
+  WLev v;
+  v.n = D.n;
+  v.P = D.P;
+  v.NN = (int)D.NN;
+  v.len = D.len;
+  v.tri = D.triarea;
+  v.hinv = D.hex_inv;
+  v.oa = D.overl_a;
+  v.iu = D.iu_wgt;
+  v.nsrc = D.nsrc;
+  v.esrc = D.esrc;
+  v.mask_n = W.mask_n;
+  v.mask_e = W.mask_e;
+  v.sm = W.sm;
+  v.st = W.st;
+  v.sv = W.sv;
+  v.wm = W.wm;
+  v.wt = W.wt;
+  v.wv = W.wv;
+  v.split = D.overl_split;
+  v.rf = D.rf_wgt;
+  v.scal = W.scal;
+  v.dscal = W.dscal;
+  v.flux = W.flux;
+  v.dvelo = W.dvelo;
+  return v;
+}
+
+}  // namespace wtw

@@ -13,6 +13,7 @@
 #include "restrict_kernels.cuh"
 #include "wavelet_kernels.cuh"
 #include "wt_handle.cuh"
+#include "wt_wavctx.cuh"
 
 using namespace wtw;
 
@@ -20,59 +21,6 @@ namespace {
 
 constexpr int TPB = 256;
 inline unsigned nb(int64_t n) { return (unsigned)((n + TPB - 1) / TPB); }
-
-struct WavLevel {
-  double *sm = nullptr, *st = nullptr, *sv = nullptr;  // scaling (owned below level_end)
-  double *wm = nullptr, *wt = nullptr, *wv = nullptr;
-  int *mask_n = nullptr, *mask_e = nullptr;
-  double *scal = nullptr, *dscal = nullptr, *flux = nullptr, *dvelo = nullptr;  // work fields, on first use
-  bool own_scaling = false;
-};
-
-struct WavCtx {
-  std::vector<WavLevel> L;
-  double* thr = nullptr;  // [3][nz] thresholds
-  std::vector<void*> allocs;
-  template <class T>
-  cudaError_t alloc(T** p, size_t count) {
-    cudaError_t e = cudaMalloc(p, count * sizeof(T));
-    if (e == cudaSuccess) allocs.push_back(*p);
-    return e;
-  }
-};
-
-WavCtx* ctx(wt_handle* h) { return static_cast<WavCtx*>(h->wav); }
-
-WLev view(wt_handle* h, int l) {
-  const DevLevel& D = h->at(l);
-  WavLevel& W = ctx(h)->L[l - h->level_start];
-  WLev v;
-  v.n = D.n;
-  v.P = D.P;
-  v.NN = (int)D.NN;
-  v.len = D.len;
-  v.tri = D.triarea;
-  v.hinv = D.hex_inv;
-  v.oa = D.overl_a;
-  v.iu = D.iu_wgt;
-  v.nsrc = D.nsrc;
-  v.esrc = D.esrc;
-  v.mask_n = W.mask_n;
-  v.mask_e = W.mask_e;
-  v.sm = W.sm;
-  v.st = W.st;
-  v.sv = W.sv;
-  v.wm = W.wm;
-  v.wt = W.wt;
-  v.wv = W.wv;
-  v.split = D.overl_split;
-  v.rf = D.rf_wgt;
-  v.scal = W.scal;
-  v.dscal = W.dscal;
-  v.flux = W.flux;
-  v.dvelo = W.dvelo;
-  return v;
-}
 
 int fail(const char* where, cudaError_t e) { return wt_handle_fail(where, e); }
 
@@ -103,6 +51,42 @@ int work_field(wt_handle* h, int l, int field, double** out, size_t* bytes) {
   if (bytes) *bytes = n * 8;
   return WT_OK;
 }
+
+}  // namespace
+
+// The layer mean of mass or Theta (WT_FIELD_MEAN_*) of level l: the stepper's
+// on level_end, allocated (zero) on first use below it.
+int wt_level_mean(wt_handle* h, int l, int field, double** out) {
+  if (l == h->level_end) {
+    *out = field == WT_FIELD_MEAN_MASS ? h->mean_m : h->mean_t;
+    return WT_OK;
+  }
+  WavLevel& V = ctx(h)->L[l - h->level_start];
+  double** slot = field == WT_FIELD_MEAN_MASS ? &V.mean_m : &V.mean_t;
+  const size_t n = (size_t)h->nz * h->at(l).NN;
+  if (!*slot) {
+    CKW(ctx(h)->alloc(slot, n));
+    CKW(cudaMemsetAsync(*slot, 0, n * 8, h->stream));
+  }
+  *out = *slot;
+  return WT_OK;
+}
+
+void wt_level_masks(wt_handle* h, int l, const int** mask_n, const int** mask_e) {
+  if (!h->wav) { *mask_n = *mask_e = nullptr; return; }
+  WavLevel& V = ctx(h)->L[l - h->level_start];
+  *mask_n = V.mask_n;
+  *mask_e = V.mask_e;
+}
+
+void wt_level_state(wt_handle* h, int l, double** m, double** t, double** v) {
+  WavLevel& V = ctx(h)->L[l - h->level_start];
+  *m = V.sm;
+  *t = V.st;
+  *v = V.sv;
+}
+
+namespace {
 
 void zero_wavelets(wt_handle* h) {
   for (int l = h->level_start; l <= h->level_end; ++l) {
@@ -203,7 +187,15 @@ int wt_wavelet_setup(wt_handle* h) {
 
 int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
   if (int rc = ready(h)) return rc;
-  if (!src || level < h->level_start || level > h->level_end || field < 0 || field > WT_WORK_DVELO) return WT_ERR_ARG;
+  if (!src || level < h->level_start || level > h->level_end || field < 0 || field > WT_FIELD_MEAN_TEMP)
+    return WT_ERR_ARG;
+  if (field >= WT_FIELD_MEAN_MASS) {
+    double* p;
+    if (int rc = wt_level_mean(h, level, field, &p)) return rc;
+    CKW(cudaMemcpyAsync(p, src, (size_t)h->nz * h->at(level).NN * 8, cudaMemcpyHostToDevice, h->stream));
+    CKW(cudaStreamSynchronize(h->stream));
+    return WT_OK;
+  }
   if (field >= WT_WORK_SCALAR) {
     double* p;
     size_t bytes;
@@ -225,7 +217,15 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
 
 int wt_download_field(wt_handle* h, int level, int field, void* dst) {
   if (int rc = ready(h)) return rc;
-  if (!dst || level < h->level_start || level > h->level_end || field < 0 || field > WT_WORK_DVELO) return WT_ERR_ARG;
+  if (!dst || level < h->level_start || level > h->level_end || field < 0 || field > WT_FIELD_MEAN_TEMP)
+    return WT_ERR_ARG;
+  if (field >= WT_FIELD_MEAN_MASS) {
+    double* p;
+    if (int rc = wt_level_mean(h, level, field, &p)) return rc;
+    CKW(cudaMemcpyAsync(dst, p, (size_t)h->nz * h->at(level).NN * 8, cudaMemcpyDeviceToHost, h->stream));
+    CKW(cudaStreamSynchronize(h->stream));
+    return WT_OK;
+  }
   if (field >= WT_WORK_SCALAR) {
     double* p;
     size_t bytes;
@@ -401,6 +401,33 @@ int wt_wt_after_step(wt_handle* h) {
 }
 
 // ---- compute-or-restrict of the multi-level trend (src/multi_level.f90:311-659)
+
+}  // extern "C"
+
+int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd) {
+  WLev P = view(h, level), C = view(h, level + 1);
+  P.scal = par;
+  C.scal = const_cast<double*>(chd);
+  const int m = h->at(level).n + 1;
+  k_restr_scalar<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(P, C, h->nz);
+  CKW(cudaGetLastError());
+  return WT_OK;
+}
+
+int wt_level_restrict_flux(wt_handle* h, int level, double* par_flux, const double* chd_flux,
+                           const double* chd_dscal) {
+  if (!h->at(level + 1).rf_wgt || !h->at(level + 1).overl_split) return WT_ERR_ARG;
+  WLev P = view(h, level), C = view(h, level + 1);
+  P.flux = par_flux;
+  C.flux = const_cast<double*>(chd_flux);
+  C.dscal = const_cast<double*>(chd_dscal);
+  const int m = h->at(level).n;
+  k_restr_flux<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(P, C, h->nz);
+  CKW(cudaGetLastError());
+  return WT_OK;
+}
+
+extern "C" {
 
 namespace {
 // Parent `level` and child level+1 with the given work fields allocated on both.

@@ -170,7 +170,7 @@ class WaveletHierarchy(DeviceGrid):
     stepper's state."""
 
     FIELDS = {"mass": 0, "temp": 1, "velo": 2, "wc_mass": 3, "wc_temp": 4, "wc_velo": 5, "mask_n": 6, "mask_e": 7,
-              "scalar": 8, "dscalar": 9, "flux": 10, "dvelo": 11}
+              "scalar": 8, "dscalar": 9, "flux": 10, "dvelo": 11, "mean_m": 12, "mean_t": 13}
 
     def __init__(self, levels: list[LevelGeom], topos: list[np.ndarray], nz: int, ph: OceanParams | None = None):
         super().__init__(levels, topos, nz, ph)
@@ -224,6 +224,18 @@ class WaveletHierarchy(DeviceGrid):
 
     def wt_after_step(self) -> None:
         N.check("wt_wt_after_step", N.lib().wt_wt_after_step(self.h))
+
+    def trend_multi(self) -> None:
+        """trend_ml over every level of the hierarchy (scaling fields, layer means and masks as uploaded)."""
+        N.check("wt_trend_multi", N.lib().wt_trend_multi(self.h))
+
+    def download_trend(self, level: int):
+        """(dmass, dtemp, dvelo) of `level` from the last trend_multi."""
+        NN = self.levels[level - self.ls].NN
+        dm, dt, dv = np.empty((self.nz, NN)), np.empty((self.nz, NN)), np.empty((self.nz, 3 * NN))
+        N.check("wt_download_trend_level", N.lib().wt_download_trend_level(self.h, int(level), N.dptr(dm),
+                                                                           N.dptr(dt), N.dptr(dv)))
+        return dm, dt, dv
 
     def restrict_scalar(self, level: int) -> None:
         """scalar_cpt_restr of the work scalar from level+1 to level."""

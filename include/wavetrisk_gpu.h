@@ -278,6 +278,12 @@ int wt_restrict_u_source(wt_handle* h, int level);
  * with mask_n >= TRSK.  Needs wt_wavelet_setup, the masks of every level and
  * the layer means (WT_FIELD_MEAN_*) below level_end. */
 int wt_trend_multi(wt_handle* h);
+/* RK4 (src/time_integr.f90:78-103) over the hierarchy, nsteps steps of dt:
+ * each stage evaluates wt_trend_multi's trend, takes RK_sub_step on every
+ * level (src/time_integr.f90:206-225) and runs WT_after_step on the stage
+ * state; the masks are held fixed.  The solution is the hierarchy's scaling
+ * fields (level_end's is the stepper's state). */
+int wt_rk4_multi(wt_handle* h, double dt, int nsteps);
 /* The trends of one level from the last wt_trend_multi: dmass, dtemp [nz][NN],
  * dvelo [nz][3*NN] host doubles (any may be NULL). */
 int wt_download_trend_level(wt_handle* h, int level, double* dmass, double* dtemp, double* dvelo);

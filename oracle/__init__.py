@@ -140,3 +140,36 @@ def trend_multi(levels, nz, ph, states, masks):
     rc = L.orc_trend_multi(arr, len(levels), nz, ph.grav, ph.ref_density, ph.p_top)
     assert rc == 0
     return out
+
+
+def rk4_multi(levels, nz, ph, states, masks, dt, nsteps=1):
+    """RK4 (src/time_integr.f90:78-103) over the hierarchy: per stage
+    trend_multi on every level, RK_sub_step on every level, then
+    WT_after_step (src/adapt.f90:186-237) of the stage state with the masks
+    held fixed.  Returns per level the new (mass, temp, velo)."""
+    from .wavelet import Hierarchy
+    H = Hierarchy(levels, nz)
+    for g, (mn, me) in zip(levels, masks):
+        H.set(g.level, "mask_n", mn)
+        H.set(g.level, "mask_e", me)
+    keys = ("mass", "temp", "velo")
+    q = [{k: np.array(st[k], dtype=np.float64) for k in keys} for st in states]
+    hs = (dt / 4.0, dt / 3.0, dt / 2.0, dt)
+    for _ in range(nsteps):
+        q1 = None
+        for stage in range(4):
+            src = q if stage == 0 else q1
+            st = [dict(states[i], **src[i]) for i in range(len(levels))]
+            tr = trend_multi(levels, nz, ph, st, masks)
+            dest = [{k: q[i][k] + hs[stage] * tr[i][j] for j, k in enumerate(keys)} for i in range(len(levels))]
+            for i, g in enumerate(levels):
+                for k, f in zip(keys, ("s_m", "s_t", "s_v")):
+                    H.set(g.level, f, dest[i][k])
+            H.wt_after_step()
+            dest = [{k: H.field(g.level, f).copy() for k, f in zip(keys, ("s_m", "s_t", "s_v"))}
+                    for g in levels]
+            if stage < 3:
+                q1 = dest
+            else:
+                q = dest
+    return [(x["mass"], x["temp"], x["velo"]) for x in q]

@@ -85,3 +85,45 @@ def test_trend_multi_matches_oracle(lmin, lmax, nz, masks):
         assert np.abs(odv[:, e]).max() > 0
     assert dev.status() == 0
     dev.close()
+
+
+def test_rk4_multi_matches_oracle():
+    """Two RK4 steps of the whole hierarchy (trend_ml on every level, RK
+    sub-step on every level, WT_after_step per stage) with adapt-built masks."""
+    ph = OceanParams()
+    lmin, lmax, nz, dt = 3, 5, 2, 300.0
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    top = jet_state(levels[-1], nz, seed=3, ph=ph)
+    top["velo"] = top["velo"] + 0.05 * np.random.default_rng(4).standard_normal(top["velo"].shape)
+    halo_edges(levels[-1], top["velo"])
+    orc_h = Hierarchy(levels, nz)
+    for name, key in (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v")):
+        orc_h.set(lmax, key, top[name])
+    orc_h.forward()
+    thr = np.full((3, nz), 0.12)
+    thr[0] = 5.0
+    orc_h.mask_build(thr, 0, lmax + 1)
+    masks = [(orc_h.field(g.level, "mask_n").copy(), orc_h.field(g.level, "mask_e").copy()) for g in levels]
+    states = []
+    for g in levels:
+        st = jet_state(g, nz, seed=3, ph=ph)  # means and topography of the level
+        for name, key in (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v")):
+            st[name] = orc_h.field(g.level, key).copy()
+        states.append(st)
+    dev = WaveletHierarchy(levels, [st["topo"] for st in states], nz, ph)
+    for g, st, (mn, me) in zip(levels, states, masks):
+        for name in ("mass", "temp", "velo", "mean_m", "mean_t"):
+            dev.upload(g.level, name, st[name])
+        dev.upload(g.level, "mask_n", mn)
+        dev.upload(g.level, "mask_e", me)
+    ref = oracle.rk4_multi(levels, nz, ph, states, masks, dt, nsteps=2)
+    dev.rk4_multi(dt, 2)
+    for q, g in enumerate(levels):
+        own = np.nonzero(g.owned)[0]
+        e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+        for name, o, k in (("mass", ref[q][0], own), ("temp", ref[q][1], own), ("velo", ref[q][2], e)):
+            d = dev.download(g.level, name)
+            assert _rel(d[:, k], o[:, k]) <= TOL, (g.level, name, _rel(d[:, k], o[:, k]))
+    assert dev.status() == 0
+    dev.close()

@@ -94,5 +94,8 @@ int wt_level_restrict_flux(wt_handle* h, int level, double* par_flux, const doub
 int wt_level_mean(wt_handle* h, int level, int field, double** out);
 // The masks of a level, or null before wt_wavelet_setup (wt_wavelet.cu).
 void wt_level_masks(wt_handle* h, int level, const int** mask_n, const int** mask_e);
+// WT_after_step on the given per-level scaling fields (level_start first), or on
+// the hierarchy's own when the arrays are null; stream-ordered (wt_wavelet.cu).
+int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v);
 // The scaling fields (mass, Theta, velocity) of a level (wt_wavelet.cu).
 void wt_level_state(wt_handle* h, int level, double** m, double** t, double** v);

@@ -18,6 +18,7 @@ namespace {
 struct MLLevel {
   double *phik = nullptr, *pterm = nullptr, *qe = nullptr, *hfm = nullptr, *hft = nullptr, *bern = nullptr,
          *theta = nullptr, *dm = nullptr, *dt = nullptr, *dv = nullptr, *src = nullptr;
+  double *m1 = nullptr, *t1 = nullptr, *v1 = nullptr;  // RK stage state q1
 };
 
 struct MLCtx {
@@ -39,8 +40,8 @@ int ensure(wt_handle* h) {
   for (int l = h->level_start; l <= h->level_end; ++l) {
     MLLevel& V = M->L[l - h->level_start];
     const size_t nn = (size_t)h->nz * h->at(l).NN;
-    double** node[] = {&V.phik, &V.pterm, &V.bern, &V.theta, &V.dm, &V.dt};
-    double** edge[] = {&V.qe, &V.hfm, &V.hft, &V.dv, &V.src};
+    double** node[] = {&V.phik, &V.pterm, &V.bern, &V.theta, &V.dm, &V.dt, &V.m1, &V.t1};
+    double** edge[] = {&V.qe, &V.hfm, &V.hft, &V.dv, &V.src, &V.v1};
     for (double** p : node) {
       CKM(cudaMalloc(p, nn * 8));
       M->allocs.push_back(*p);
@@ -65,18 +66,17 @@ void wt_trend_ml_release(wt_handle* h) {
   h->ml = nullptr;
 }
 
-extern "C" {
+namespace {
 
-int wt_trend_multi(wt_handle* h) {
-  if (!h) return WT_ERR_ARG;
-  if (!h->wav) return WT_ERR_STATE;
-  if (int rc = ensure(h)) return rc;
-  MLCtx* M = static_cast<MLCtx*>(h->ml);
-  const int nz = h->nz;
-  for (int l = h->level_end; l >= h->level_start; --l) {
-    MLLevel& V = M->L[l - h->level_start];
-    const DevLevel& D = h->at(l);
-    double *m, *t, *v, *mm, *mt;
+// The scaling fields of every level (level_start first).
+struct States {
+  std::vector<double*> m, t, v;
+};
+
+States hierarchy_state(wt_handle* h) {
+  States S;
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    double *m, *t, *v;
     if (l == h->level_end) {
       m = h->mass;
       t = h->temp;
@@ -84,16 +84,33 @@ int wt_trend_multi(wt_handle* h) {
     } else {
       wt_level_state(h, l, &m, &t, &v);
     }
+    S.m.push_back(m);
+    S.t.push_back(t);
+    S.v.push_back(v);
+  }
+  return S;
+}
+
+// trend_ml of the state S into each level's dm, dt, dv (stream-ordered).
+int trend_multi(wt_handle* h, const States& S) {
+  MLCtx* M = static_cast<MLCtx*>(h->ml);
+  const int nz = h->nz;
+  for (int l = h->level_end; l >= h->level_start; --l) {
+    const int q = l - h->level_start;
+    MLLevel& V = M->L[q];
+    const DevLevel& D = h->at(l);
+    double *mm, *mt;
     if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
     if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
-    if (int rc = wt_level_step1(h, l, m, t, v, mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern, V.theta))
+    if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern,
+                                V.theta))
       return rc;
     wtk::TrendML io{};
     const int *mask_n, *mask_e;
     wt_level_masks(h, l, &mask_n, &mask_e);
     io.mask_n = mask_n;
     if (l < h->level_end) {
-      MLLevel& C = M->L[l + 1 - h->level_start];
+      MLLevel& C = M->L[q + 1];
       if (int rc = wt_level_restrict_scalar(h, l, V.bern, C.bern)) return rc;
       if (int rc = wt_level_restrict_scalar(h, l, V.phik, C.phik)) return rc;  // exner = -Phi_k
       if (int rc = wt_level_restrict_flux(h, l, V.hfm, C.hfm, C.dm)) return rc;
@@ -111,7 +128,69 @@ int wt_trend_multi(wt_handle* h) {
     wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
     CKM(cudaGetLastError());
   }
+  return WT_OK;
+}
+
+// RK_sub_step (src/time_integr.f90:206-225): dest = sol + hs * trend.
+__global__ void k_rk_sub(int64_t n, const double* __restrict__ sol, const double* __restrict__ trend, double hs,
+                         double* dest) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dest[i] = sol[i] + hs * trend[i];
+}
+
+int rk_sub_step(wt_handle* h, const States& sol, const States& dest, double hs) {
+  MLCtx* M = static_cast<MLCtx*>(h->ml);
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    const int q = l - h->level_start;
+    const int64_t nn = (int64_t)h->nz * h->at(l).NN;
+    const unsigned nb1 = (unsigned)((nn + 255) / 256), nb3 = (unsigned)((3 * nn + 255) / 256);
+    k_rk_sub<<<nb1, 256, 0, h->stream>>>(nn, sol.m[q], M->L[q].dm, hs, dest.m[q]);
+    k_rk_sub<<<nb1, 256, 0, h->stream>>>(nn, sol.t[q], M->L[q].dt, hs, dest.t[q]);
+    k_rk_sub<<<nb3, 256, 0, h->stream>>>(3 * nn, sol.v[q], M->L[q].dv, hs, dest.v[q]);
+  }
+  CKM(cudaGetLastError());
+  return WT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wt_trend_multi(wt_handle* h) {
+  if (!h) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure(h)) return rc;
+  if (int rc = trend_multi(h, hierarchy_state(h))) return rc;
   CKM(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+// RK4 (src/time_integr.f90:78-103) over the hierarchy: each stage evaluates
+// trend_ml on every level, takes the RK sub-step on every level and runs
+// WT_after_step on the new stage state, with the masks held fixed.
+int wt_rk4_multi(wt_handle* h, double dt, int nsteps) {
+  if (!h || nsteps < 0) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure(h)) return rc;
+  MLCtx* M = static_cast<MLCtx*>(h->ml);
+  const States q = hierarchy_state(h);
+  States q1;
+  for (auto& V : M->L) {
+    q1.m.push_back(V.m1);
+    q1.t.push_back(V.t1);
+    q1.v.push_back(V.v1);
+  }
+  const double hs[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
+  for (int s = 0; s < nsteps; ++s)
+    for (int stage = 0; stage < 4; ++stage) {
+      const States& src = stage == 0 ? q : q1;
+      const States& dest = stage == 3 ? q : q1;
+      if (int rc = trend_multi(h, src)) return rc;
+      if (int rc = rk_sub_step(h, q, dest, hs[stage])) return rc;
+      if (int rc = wt_level_after_step(h, dest.m.data(), dest.t.data(), dest.v.data())) return rc;
+    }
+  CKM(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
   return WT_OK;
 }
 

@@ -135,6 +135,35 @@ void compress(wt_handle* h) {
 
 }  // namespace
 
+// WT_after_step on the scaling fields m[q], t[q], v[q] of level level_start+q
+// (the hierarchy's own scaling fields when the arrays are null): the launches
+// read the pointers when they are made, so the hierarchy's are put back at once.
+int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v) {
+  WavCtx* W = ctx(h);
+  const int nl = h->level_end - h->level_start + 1;
+  std::vector<WavLevel> saved(W->L);
+  if (m)
+    for (int q = 0; q < nl; ++q) {
+      W->L[q].sm = m[q];
+      W->L[q].st = t[q];
+      W->L[q].sv = v[q];
+    }
+  zero_wavelets(h);
+  for (int l = h->level_start; l <= h->level_end - 1; ++l) {
+    launch_scalar_wc(h, l);
+    launch_velo_wc(h, l);
+  }
+  compress(h);
+  inverse(h);
+  for (int q = 0; q < nl; ++q) {
+    W->L[q].sm = saved[q].sm;
+    W->L[q].st = saved[q].st;
+    W->L[q].sv = saved[q].sv;
+  }
+  CKW(cudaGetLastError());
+  return WT_OK;
+}
+
 void wt_wavelet_release(wt_handle* h) {
   if (!h || !h->wav) return;
   for (void* p : ctx(h)->allocs) cudaFree(p);
@@ -387,14 +416,7 @@ int wt_compress(wt_handle* h) {
 
 int wt_wt_after_step(wt_handle* h) {
   if (int rc = ready(h)) return rc;
-  zero_wavelets(h);
-  for (int l = h->level_start; l <= h->level_end - 1; ++l) {
-    launch_scalar_wc(h, l);
-    launch_velo_wc(h, l);
-  }
-  compress(h);
-  inverse(h);
-  CKW(cudaGetLastError());
+  if (int rc = wt_level_after_step(h, nullptr, nullptr, nullptr)) return rc;
   CKW(cudaStreamSynchronize(h->stream));
   h->state_halo_done = false;
   return WT_OK;

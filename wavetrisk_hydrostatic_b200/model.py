@@ -229,6 +229,10 @@ class WaveletHierarchy(DeviceGrid):
         """trend_ml over every level of the hierarchy (scaling fields, layer means and masks as uploaded)."""
         N.check("wt_trend_multi", N.lib().wt_trend_multi(self.h))
 
+    def rk4_multi(self, dt: float, nsteps: int = 1) -> None:
+        """nsteps RK4 steps of the whole hierarchy with WT_after_step per stage (masks fixed)."""
+        N.check("wt_rk4_multi", N.lib().wt_rk4_multi(self.h, float(dt), int(nsteps)))
+
     def download_trend(self, level: int):
         """(dmass, dtemp, dvelo) of `level` from the last trend_multi."""
         NN = self.levels[level - self.ls].NN

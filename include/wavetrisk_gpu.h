@@ -245,6 +245,13 @@ int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill);
  * hierarchy exists (a fully refined tree). */
 int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max_level, int patch_size,
                   unsigned char* child_required);
+/* cal_lnorm (src/lnorms.f90:7-58) of the hierarchy's scaling fields over
+ * levels level_start..level_end: out[v*nz + k] for v = mass, Theta, velocity;
+ * scalars are mean + perturbation over nodes [0, n]^2, velocities over the
+ * edges of nodes [0, n)^2, both where mask_n >= ADJZONE.  order: 0 "inf"
+ * (max |.|), 1 "1" (mean |.|), 2 "2" (rms), 3 "min"; the mean and rms divide
+ * by the count of nodes [-1, n+1]^2 with mask_n >= ADJZONE. */
+int wt_lnorm(wt_handle* h, int order, double* out);
 /* compress_wavelets (src/adapt.f90:79-103): zero the wavelets of inactive points. */
 int wt_compress(wt_handle* h);
 /* WT_after_step (src/adapt.f90:234-283): wavelets of the current scaling fields,

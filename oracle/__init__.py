@@ -142,13 +142,16 @@ def trend_multi(levels, nz, ph, states, masks):
     return out
 
 
-def rk4_multi(levels, nz, ph, states, masks, dt, nsteps=1):
+def rk4_multi(levels, nz, ph, states, masks, dt, nsteps=1, H=None):
     """RK4 (src/time_integr.f90:78-103) over the hierarchy: per stage
     trend_multi on every level, RK_sub_step on every level, then
     WT_after_step (src/adapt.f90:186-237) of the stage state with the masks
-    held fixed.  Returns per level the new (mass, temp, velo)."""
+    held fixed.  Returns per level the new (mass, temp, velo).  H (an
+    oracle.wavelet.Hierarchy, optional) receives the masks and is left holding
+    the final state and its compressed wavelets, as adapt needs them."""
     from .wavelet import Hierarchy
-    H = Hierarchy(levels, nz)
+    if H is None:
+        H = Hierarchy(levels, nz)
     for g, (mn, me) in zip(levels, masks):
         H.set(g.level, "mask_n", mn)
         H.set(g.level, "mask_e", me)

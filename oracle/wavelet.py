@@ -102,3 +102,50 @@ class Hierarchy:
 
     def wt_after_step(self):
         self.L.orc_wt_after_step(self.arr, self.ls, self.le, self.nz)
+
+
+def lnorm(levels, masks, fields, order="inf"):
+    """cal_lnorm (src/lnorms.f90:7-58) over the hierarchy in numpy: (3, nz)
+    for mass, Theta, velocity.  fields[q]: dict of mass, temp, velo, mean_m,
+    mean_t of levels[q]; masks[q]: (mask_n, mask_e).  Scalars are mean +
+    perturbation at nodes [0, n]^2, velocities the edges of nodes [0, n)^2,
+    where mask_n >= ADJZONE; "1" and "2" divide by the count of nodes
+    [-1, n+1]^2 with mask_n >= ADJZONE."""
+    nz = fields[0]["mass"].shape[0]
+    init = 1e16 if order == "min" else 0.0
+    out = np.full((3, nz), init)
+    count = 0
+
+    def sel(g, lo, hi):
+        i = np.arange(lo, hi)
+        ii, jj = np.meshgrid(i, i, indexing="xy")
+        return np.concatenate([((d * g.P + jj + 2) * g.P + ii + 2).ravel() for d in range(10)])
+
+    for g, (mn, _), f in zip(levels, masks, fields):
+        count += int(np.count_nonzero(mn[sel(g, -1, g.n + 2)] >= ADJZONE))
+        ids = sel(g, 0, g.n + 1)
+        ids = ids[mn[ids] >= ADJZONE]
+        own = sel(g, 0, g.n)
+        own = own[mn[own] >= ADJZONE]
+        e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+        for v, x in enumerate((f["mean_m"] + f["mass"], f["mean_t"] + f["temp"])):
+            a = x[:, ids]
+            out[v] = _red(order, out[v], a)
+        out[2] = _red(order, out[2], f["velo"][:, e])
+    if order == "1":
+        out = out / count
+    elif order == "2":
+        out = np.sqrt(out / count)
+    return out
+
+
+def _red(order, acc, a):
+    if a.shape[1] == 0:
+        return acc
+    if order == "inf":
+        return np.maximum(acc, np.abs(a).max(axis=1))
+    if order == "min":
+        return np.minimum(acc, a.min(axis=1))
+    if order == "1":
+        return acc + np.abs(a).sum(axis=1)
+    return acc + (a * a).sum(axis=1)

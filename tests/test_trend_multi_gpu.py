@@ -127,3 +127,34 @@ def test_rk4_multi_matches_oracle():
             assert _rel(d[:, k], o[:, k]) <= TOL, (g.level, name, _rel(d[:, k], o[:, k]))
     assert dev.status() == 0
     dev.close()
+
+
+@pytest.mark.parametrize("order", ["inf", "min", "1", "2"])
+def test_lnorm_matches_numpy(order):
+    from oracle.wavelet import lnorm
+    ph = OceanParams()
+    nz = 2
+    G = Grid(3, 5, radius=6371e3)
+    levels = [G.level(l) for l in range(3, 6)]
+    dev = WaveletHierarchy(levels, [np.full(g.NN, -4000.0) for g in levels], nz, ph)
+    rng = np.random.default_rng(5)
+    fields, masks = [], []
+    for g in levels:
+        st = jet_state(g, nz, seed=g.level, ph=ph)
+        st["velo"] = st["velo"] + rng.standard_normal(st["velo"].shape)
+        f = {k: st[k] for k in ("mass", "temp", "velo", "mean_m", "mean_t")}
+        for k, a in f.items():
+            dev.upload(g.level, k, a)
+        mn = rng.choice([0, 2, 8, 12, 16], size=g.NN).astype(np.int32)
+        me = np.full(3 * g.NN, 16, np.int32)
+        dev.upload(g.level, "mask_n", mn)
+        dev.upload(g.level, "mask_e", me)
+        fields.append(f)
+        masks.append((mn, me))
+    got = dev.lnorm(order)
+    ref = lnorm(levels, masks, fields, order)
+    if order in ("inf", "min"):
+        assert np.array_equal(got, ref)
+    else:
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+    dev.close()

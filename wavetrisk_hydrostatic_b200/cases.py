@@ -94,6 +94,33 @@ def jet_state(g: LevelGeom, nz: int, seed: int = 0, ph: OceanParams | None = Non
     return dict(mass=mass, temp=temp, velo=velo, mean_m=mean_m, mean_t=mean_t, topo=topo)
 
 
+def bump_state(g: LevelGeom, nz: int, seed: int = 0, ph: OceanParams | None = None, nbumps: int = 8,
+               radius: float = 300e3, amp: float = 0.05, **jet_kw):
+    """jet_state plus a seeded baroclinic perturbation: nbumps Gaussian bumps of
+    the given radius (m) and amplitude (m) in the thickness of every layer, at
+    seeded centres on the sphere (the same centres on every level).  The layer
+    densities are unchanged, so Theta mass moves with the layer mass."""
+    ph = ph or OceanParams()
+    st = jet_state(g, nz, seed=seed, ph=ph, **jet_kw)
+    rng = np.random.default_rng(10_000 + seed)
+    c = rng.standard_normal((nbumps, 3))
+    c /= np.linalg.norm(c, axis=1, keepdims=True)
+    nrm = np.linalg.norm(g.node, axis=0)
+    ok = nrm > 0  # padding corners without coordinates keep dz = 0
+    x = g.node[:, ok] / nrm[ok]
+    R = float(nrm[g.owned][0])
+    dz = np.zeros(g.NN)
+    for q in range(nbumps):
+        ang = np.arccos(np.clip(c[q] @ x, -1.0, 1.0))
+        dz[ok] += amp * np.exp(-((R * ang) / radius) ** 2)
+    halo_nodes(g, dz)
+    for k in range(nz):
+        dm = ph.ref_density * dz
+        st["mass"][k] = st["mass"][k] + dm
+        st["temp"][k] = st["temp"][k] + dm * (st["mean_t"][k] / st["mean_m"][k])
+    return st
+
+
 def bathymetry(g: LevelGeom, seed: int = 0, lmax: int = 32, nterms: int = 160,
                hmin: float = 500.0, hmax: float = 5000.0, _cache: dict = {}) -> np.ndarray:
     """Smooth seeded random depth H in [hmin, hmax] m: a sum of zonal harmonics

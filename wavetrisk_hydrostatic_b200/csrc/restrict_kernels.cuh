@@ -222,3 +222,85 @@ __global__ void k_restr_u_source(WLev P, WLev C, int nz) {
 }
 
 }  // namespace wtw
+
+namespace wtw {
+
+// cal_lnorm (src/lnorms.f90:7-58) partials: block (x, k) reduces layer k of
+// nodes x*256 .. of the level into part[k][x] = {mass, Theta, velocity}; node
+// scalars over [0, n]^2 and velocities over [0, n)^2 of nodes with mask_n >=
+// ADJZONE.  order 0 "inf" (max |.|), 1 "1" (sum |.|), 2 "2" (sum of squares),
+// 3 "min" (min).  cnt (k = 0 blocks only) counts nodes [-1, n+1]^2 with mask_n
+// >= ADJZONE (count_norm).
+__device__ __forceinline__ double lnorm_op(int order, double a, double b) {
+  return order == 0 ? fmax(a, b) : order == 3 ? fmin(a, b) : a + b;
+}
+
+__global__ void k_lnorm_part(WLev V, const double* __restrict__ mean_m, const double* __restrict__ mean_t,
+                             int order, double* part, int* cnt) {
+  const int k = blockIdx.y;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const double id0 = order == 3 ? 1e16 : 0.0;
+  double r[3] = {id0, id0, id0};
+  int c = 0;
+  if (x < V.NN) {
+    const int pp = V.P * V.P, rr = x % pp, i = rr % V.P - 2, j = rr / V.P - 2;
+    const bool act = V.mask_n[x] >= M_ADJZONE;
+    if (act && i >= -1 && j >= -1 && i <= V.n + 1 && j <= V.n + 1) c = 1;
+    if (act && i >= 0 && j >= 0 && i <= V.n && j <= V.n) {
+      const int64_t o = (int64_t)k * V.NN + x;
+      const double sm = mean_m[o] + V.sm[o], st = mean_t[o] + V.st[o];
+      const double vm = order == 3 ? sm : order == 2 ? sm * sm : fabs(sm);
+      const double vt = order == 3 ? st : order == 2 ? st * st : fabs(st);
+      r[0] = lnorm_op(order, r[0], vm);
+      r[1] = lnorm_op(order, r[1], vt);
+      if (i < V.n && j < V.n)
+        for (int e = 0; e < 3; ++e) {
+          const double u = V.sv[(int64_t)3 * k * V.NN + (int64_t)e * V.NN + x];
+          r[2] = lnorm_op(order, r[2], order == 3 ? u : order == 2 ? u * u : fabs(u));
+        }
+    }
+  }
+  __shared__ double sh[3][256];
+  __shared__ int shc[256];
+  for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] = r[q];
+  shc[threadIdx.x] = c;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] = lnorm_op(order, sh[q][threadIdx.x], sh[q][threadIdx.x + s]);
+      shc[threadIdx.x] += shc[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 3; ++q) part[((int64_t)k * gridDim.x + blockIdx.x) * 3 + q] = sh[q][0];
+    if (k == 0) cnt[blockIdx.x] = shc[0];
+  }
+}
+
+// Final reduction of the partials of every level (one block per layer).
+__global__ void k_lnorm_final(const double* __restrict__ part, const int* __restrict__ nparts, int nlev,
+                              const int* __restrict__ cnt, int order, int nz, double* out) {
+  const int k = blockIdx.x;
+  if (threadIdx.x != 0) return;
+  const double id0 = order == 3 ? 1e16 : 0.0;
+  double r[3] = {id0, id0, id0};
+  long long n = 0;
+  int64_t base = 0, cbase = 0;
+  for (int l = 0; l < nlev; ++l) {
+    const int np = nparts[l];
+    for (int b = 0; b < np; ++b)
+      for (int q = 0; q < 3; ++q) r[q] = lnorm_op(order, r[q], part[base + ((int64_t)k * np + b) * 3 + q]);
+    for (int b = 0; b < np; ++b) n += cnt[cbase + b];
+    base += (int64_t)nz * np * 3;
+    cbase += np;
+  }
+  for (int q = 0; q < 3; ++q) {
+    double v = r[q];
+    if (order == 1) v = v / (double)n;
+    if (order == 2) v = sqrt(v / (double)n);
+    out[q * nz + k] = v;
+  }
+}
+
+}  // namespace wtw

@@ -495,4 +495,49 @@ int wt_restrict_u_source(wt_handle* h, int level) {
   return WT_OK;
 }
 
+// cal_lnorm (src/lnorms.f90:7-58) of the hierarchy's scaling fields: out[v][k]
+// for v = mass, Theta, velocity.
+int wt_lnorm(wt_handle* h, int order, double* out) {
+  if (int rc = ready(h)) return rc;
+  if (!out || order < 0 || order > 3) return WT_ERR_ARG;
+  const int nz = h->nz, nl = h->level_end - h->level_start + 1;
+  std::vector<int> nparts(nl);
+  int64_t np_tot = 0;
+  for (int q = 0; q < nl; ++q) {
+    nparts[q] = (int)nb(h->at(h->level_start + q).NN);
+    np_tot += nparts[q];
+  }
+  double *part = nullptr, *dout = nullptr;
+  int *cnt = nullptr, *dn = nullptr;
+  cudaError_t e = cudaMalloc(&part, np_tot * nz * 3 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&cnt, np_tot * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&dn, nl * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&dout, 3 * nz * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dn, nparts.data(), nl * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+  int64_t base = 0, cbase = 0;
+  for (int q = 0; q < nl && e == cudaSuccess; ++q) {
+    const int l = h->level_start + q;
+    double *mm, *mt;
+    int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm);
+    if (!rc) rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt);
+    if (rc) { e = cudaErrorMemoryAllocation; break; }
+    k_lnorm_part<<<dim3(nparts[q], nz), TPB, 0, h->stream>>>(view(h, l), mm, mt, order, part + base, cnt + cbase);
+    base += (int64_t)nz * nparts[q] * 3;
+    cbase += nparts[q];
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    k_lnorm_final<<<nz, 32, 0, h->stream>>>(part, dn, nl, cnt, order, nz, dout);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, 3 * nz * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(part);
+  cudaFree(cnt);
+  cudaFree(dn);
+  cudaFree(dout);
+  if (e != cudaSuccess) return fail("lnorm", e);
+  return WT_OK;
+}
+
 }  // extern "C"

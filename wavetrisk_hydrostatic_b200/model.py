@@ -229,6 +229,13 @@ class WaveletHierarchy(DeviceGrid):
         """trend_ml over every level of the hierarchy (scaling fields, layer means and masks as uploaded)."""
         N.check("wt_trend_multi", N.lib().wt_trend_multi(self.h))
 
+    def lnorm(self, order: str = "inf") -> np.ndarray:
+        """cal_lnorm of the scaling fields: (3, nz) for mass, Theta, velocity; order "inf", "1", "2" or "min"."""
+        out = np.empty((3, self.nz))
+        code = {"inf": 0, "1": 1, "2": 2, "min": 3}[order]
+        N.check("wt_lnorm", N.lib().wt_lnorm(self.h, code, N.dptr(out)))
+        return out
+
     def rk4_multi(self, dt: float, nsteps: int = 1) -> None:
         """nsteps RK4 steps of the whole hierarchy with WT_after_step per stage (masks fixed)."""
         N.check("wt_rk4_multi", N.lib().wt_rk4_multi(self.h, float(dt), int(nsteps)))

@@ -33,12 +33,14 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-DT = 300.0
+DT = 300.0      # uniform stepper (explicit RK4, J5 config)
+DT_AD = 150.0   # adaptive run
+TOL_AD = 5e-3   # wavelet threshold tolerance of the adaptive run
 DAY = 86400.0
 
 
-def sim_days_per_hour(steps, seconds):
-    return (steps * DT / DAY) / (seconds / 3600.0)
+def sim_days_per_hour(steps, seconds, dt=DT):
+    return (steps * dt / DAY) / (seconds / 3600.0)
 
 
 def parse():
@@ -47,6 +49,8 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--mode", default="adaptive", choices=["adaptive", "uniform"])
+    p.add_argument("--lmin", type=int, default=4)
     p.add_argument("--level", type=int, default=7)
     p.add_argument("--nz", type=int, default=16)
     p.add_argument("--no-extra", action="store_true")
@@ -231,6 +235,16 @@ def elliptic_case(lmax, repeats=3):
 
 def workload_config(args, world=1):
     cells = 10 * 4 ** args.level + 2
+    if args.mode == "adaptive":
+        return {
+            "workload": f"adaptive run J{args.lmin}..J{args.level} ({cells} cells at J{args.level}), {args.nz} "
+                        f"Boussinesq layers, every patch of the hierarchy present (fully refined tree; masks and "
+                        f"adapt every step), jet + 8 seeded Gaussian bumps (300 km, 0.05 m), tol {TOL_AD} "
+                        f"thresholds, explicit RK4 dt={DT_AD:g} s, WT_after_step per stage",
+            "min_level": args.lmin, "max_level": args.level, "layers": args.nz, "dt_s": DT_AD, "tol": TOL_AD,
+            "parallelism": f"replicas x{world} (independent ensemble members)" if world > 1 else "single GPU",
+            "l2": "flushed (256 MB write) between timed steps, outside the timed region",
+        }
     return {
         "workload": f"uniform J{args.level} icosahedral grid ({cells} cells), {args.nz} Boussinesq layers, "
                     f"flat 4000 m bottom, explicit RK4 dt=300 s"
@@ -283,6 +297,119 @@ def wavelet_case(lmin, lmax, nz, repeats=5, device=None):
     return out
 
 
+def adaptive_launches(L):
+    """Kernels launched by one adaptive step of L levels (AdaptiveOcean.step
+    with fixed thresholds, max_level = level_end): RK4 of the hierarchy (per
+    stage: column + step1 and k_trend_ml per level, four restrictions per
+    coarse level, three RK sub-step kernels per level, WT_after_step with two
+    wavelet kernels per coarse level, one compression kernel per fine level
+    and four inverse-transform kernels per coarse level), wt_mask_build's
+    sweeps (comm_masks launches one kernel per level), compression and the
+    inverse transform."""
+    stage = 3 * L + 4 * (L - 1) + 3 * L + 2 * (L - 1) + (L - 1) + 4 * (L - 1)
+    masks = ((L - 1) + 1 + L + (L - 1) * (L + 2) + L + L + L + (L - 1) + L + L + 2 * (L - 1) + L
+             + (L - 2) * (2 + 2 * L) + (1 + L) + 2 * (L - 2) + 1 + L + L)
+    return 4 * stage + masks + (L - 1) + 4 * (L - 1)
+
+
+def algorithmic_bytes_trend_ml(level, nz):
+    """Compulsory bytes of one k_trend_ml launch on a level: node-layers of
+    [0, n]^2 read theta, qe(3), hflux_mass(3), hflux_Theta(3), Bernoulli and Phi
+    (12 words) and write dmass, dTheta, dvelo(3) and the velocity source(3)
+    (8 words); geometry len(3), part(6), hex_inv and the node mask are read
+    once per node of [0, n]^2."""
+    n = 2 ** level
+    inner = 10 * (n + 1) ** 2
+    return nz * inner * 20 * 8 + inner * (10 * 8 + 4)
+
+
+def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile=True):
+    """The adaptive run on the fully refined hierarchy lmin..lmax: jet +
+    8 Gaussian bumps, tol 5e-3 thresholds (initialize_thresholds_case), one
+    step = RK4 of the hierarchy (dt 150 s) + adapt + inverse transform.
+    CUDA-event time per step on the handle's stream."""
+    import numpy as np
+    import torch
+
+    from wavetrisk_hydrostatic_b200 import Grid, OceanParams
+    from wavetrisk_hydrostatic_b200 import _native as Nt
+    from wavetrisk_hydrostatic_b200.adaptive import AdaptiveOcean
+    from wavetrisk_hydrostatic_b200.cases import bump_state
+
+    ph = OceanParams()
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    states = [bump_state(g, nz, seed=seed, ph=ph) for g in levels]
+    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=TOL_AD)
+    dev = model.dev
+    stream = torch.cuda.ExternalStream(dev.stream, device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    for _ in range(warmup):
+        model.step(DT_AD)
+    torch.cuda.synchronize(device)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for s in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(s))
+        ev[s][0].record(stream)
+        model.step(DT_AD)
+        ev[s][1].record(stream)
+    torch.cuda.synchronize(device)
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    out = {"ms_total": ms, "ms_per_step": ms / steps}
+    act = []
+    for g, (mn, me) in zip(levels, model.masks()):
+        own = np.nonzero(g.owned)[0]
+        e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+        act.append({"level": g.level, "active_nodes": int(np.count_nonzero(mn[own] >= 8)),
+                    "active_edges": int(np.count_nonzero(me[e] >= 8)), "edges": int(e.size)})
+    out["masks"] = act
+    if profile:
+        pm = (Nt.C.c_double * 7)()
+        pc = (Nt.C.c_int * 7)()
+        Nt.check("wt_profile_rk4_multi", Nt.lib().wt_profile_rk4_multi(dev.h, DT_AD, 2, pm, pc))
+        names = ["step1_top", "step1_coarse", "restrict", "trend_ml_top", "trend_ml_coarse", "rk_sub", "wt_after_step"]
+        out["phase_ms"] = {names[p]: pm[p] for p in range(7)}
+        out["phase_count_per_step"] = {names[p]: pc[p] for p in range(7)}
+    if e2e:
+        pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+        bufs = []
+        for g in levels:
+            bufs.append({"mass": pin((nz, g.NN)), "temp": pin((nz, g.NN)), "velo": pin((nz, 3 * g.NN)),
+                         "mask_n": torch.empty(g.NN, dtype=torch.int32, pin_memory=True).numpy(),
+                         "mask_e": torch.empty(3 * g.NN, dtype=torch.int32, pin_memory=True).numpy()})
+        ids = dev.FIELDS
+        L = Nt.lib()
+
+        def put(g, b):
+            for k in ("mass", "temp", "velo"):
+                Nt.check("wt_upload_field", L.wt_upload_field(dev.h, g.level, ids[k], b[k].ctypes.data))
+
+        def get(g, b):
+            for k in ("mass", "temp", "velo", "mask_n", "mask_e"):
+                Nt.check("wt_download_field", L.wt_download_field(dev.h, g.level, ids[k], b[k].ctypes.data))
+
+        for g, b in zip(levels, bufs):
+            get(g, b)
+        nsteps_e2e = max(1, steps // 2)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for _ in range(nsteps_e2e):
+            for g, b in zip(levels, bufs):
+                put(g, b)
+            model.step(DT_AD)
+            for g, b in zip(levels, bufs):
+                get(g, b)
+        t1 = time.perf_counter()
+        out["e2e_s"] = t1 - t0
+        out["e2e_steps"] = nsteps_e2e
+        out["h2d_bytes_per_step"] = int(sum(b[k].nbytes for b in bufs for k in ("mass", "temp", "velo")))
+        out["d2h_bytes_per_step"] = int(sum(b[k].nbytes for b in bufs for k in b))
+    out["cells_finest"] = 10 * 4 ** lmax + 2
+    model.close()
+    return out
+
+
 def algorithmic_bytes_trend_rk(level, nz):
     """Compulsory bytes of one k_trend launch (MODE_RK).  Node-layers of the
     computed range [0, n]^2 read theta, qe(3), hflux_mass(3), hflux_Theta(3),
@@ -298,6 +425,109 @@ def algorithmic_bytes_trend_rk(level, nz):
 
 
 def bench_ours(args):
+    if args.mode == "uniform":
+        return bench_ours_uniform(args)
+    import torch
+
+    world, rank, local, pg = dist_init(args)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    barrier(pg)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    torch.cuda.synchronize(device)
+    barrier(pg)
+    r = adaptive_case(args.lmin, args.level, args.nz, args.steps, args.warmup, seed=1 + rank, device=device)
+    torch.cuda.synchronize(device)
+    barrier(pg)
+    clocks = sampler.stop() if sampler else None
+    ms_max = allreduce_max(pg, r["ms_total"], device)
+    e2e_max = allreduce_max(pg, r["e2e_s"], device)
+    value = world * sim_days_per_hour(args.steps, ms_max / 1e3, DT_AD)
+    e2e_value = world * sim_days_per_hour(r["e2e_steps"], e2e_max, DT_AD)
+
+    extra = []
+    if not args.no_extra and rank == 0 and world == 1:
+        for (lv, nz, steps) in [(7, 16, 50), (5, 8, 100), (8, 32, 10)]:
+            rr = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False)
+            kt = rr["kernel_ms_per_launch"]
+            ab = algorithmic_bytes_trend_rk(lv, nz)
+            extra.append({
+                "workload": f"uniform J{lv} ({rr['cells']} cells), {nz} layers, single-level RK4 dt=300 s "
+                            f"(the fused uniform stepper)",
+                "ms_per_step": rr["ms_per_step"], "value": sim_days_per_hour(steps, rr["ms_total"] / 1e3),
+                "unit": "simulated days per wall-clock hour",
+                "kernel_ms_per_launch": kt,
+                "trend_rk_GBps": ab / (kt["trend_rk"] / 1e3) / 1e9,
+                "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,
+            })
+        for lmax in (6, 7, 8):
+            extra.append(elliptic_case(lmax))
+        for (lmin, lmax, nzw) in ((5, 7, 16), (5, 8, 32)):
+            extra.append(wavelet_case(lmin, lmax, nzw, device=device))
+
+    if rank == 0:
+        pm, pc = r["phase_ms"], r["phase_count_per_step"]
+        share = {k: pm[k] * pc[k] for k in pm}
+        tot = sum(share.values())
+        dom = max(share, key=lambda k: share[k])
+        ab = algorithmic_bytes_trend_ml(args.level, args.nz)
+        ach = ab / (pm["trend_ml_top"] / 1e3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "trend_ml_traffic.json")
+        if os.path.exists(tf):
+            try:
+                traffic = json.load(open(tf)).get(f"J{args.level}_nz{args.nz}")
+            except Exception:
+                traffic = None
+        cpu = cpu_baseline(args, quick=True)
+        L = args.level - args.lmin + 1
+        line = {
+            "metric": "sim-days/hour",
+            "value": value,
+            "unit": "simulated days per wall-clock hour",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded jet + Gaussian bumps)",
+            "config": workload_config(args, world),
+            "e2e": {"value": e2e_value, "unit": "simulated days per wall-clock hour",
+                    "h2d_bytes_per_step": r["h2d_bytes_per_step"], "d2h_bytes_per_step": r["d2h_bytes_per_step"],
+                    "path": "C-ABI wt_upload_field / wt_rk4_multi + wt_mask_build + wt_compress + wt_inverse_wt / "
+                            "wt_download_field, pinned host buffers: every level's state in, every level's state "
+                            "and masks out, every step"},
+            "gpu_launches": adaptive_launches(L) * args.steps,
+            "roofline": {"bound": "hbm", "kernel": "k_trend_ml (level_end)", "achieved": ach, "peak": hbm,
+                         "unit": "GB/s", "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
+                         "dominant_phase_by_time": dom,
+                         "phase_share": {k: v / tot for k, v in share.items()},
+                         "phase_ms_per_occurrence": pm, "phase_count_per_step": pc},
+            "masks_after_run": r["masks"],
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        if extra:
+            line["extra"] = extra
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def bench_ours_uniform(args):
     import torch
 
     world, rank, local, pg = dist_init(args)
@@ -391,6 +621,8 @@ def bench_ours(args):
 # ----------------------------------------------------------- reference ----
 def cpu_baseline(args, quick=False):
     """Times the CPU restatement (oracle) on a bounded sample of the workload."""
+    if args.mode == "adaptive":
+        return cpu_baseline_adaptive(args, quick)
     import numpy as np
 
     import oracle
@@ -416,6 +648,52 @@ def cpu_baseline(args, quick=False):
             "sample": f"{steps} RK4 steps of the same workload ({t_used:.1f} s of CPU time)"}
 
 
+def cpu_baseline_adaptive(args, quick=False):
+    """The oracle's adaptive step on the same hierarchy (multi-level trend,
+    RK4, WT_after_step, adapt's mask sequence, compression, inverse
+    transform), timed over whole steps until the budget is used."""
+    import numpy as np
+
+    import oracle
+    from oracle.wavelet import Hierarchy
+    from wavetrisk_hydrostatic_b200 import Grid, OceanParams
+    from wavetrisk_hydrostatic_b200.cases import bump_state
+
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    ph = OceanParams()
+    lmin, lmax, nz = args.lmin, args.level, args.nz
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    states = [bump_state(g, nz, seed=1, ph=ph) for g in levels]
+    keys = (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v"))
+    dz = states[-1]["mean_m"][:, 0] / ph.ref_density
+    thr = TOL_AD * np.stack([ph.ref_density * dz, np.full(nz, 1e16), np.full(nz, 1.0)])
+    H = Hierarchy(levels, nz)
+    for name, key in keys:
+        H.set(lmax, key, states[-1][name])
+    H.forward()
+    H.mask_build(thr, 0, lmax)
+    H.compress()
+    H.inverse()
+    budget = args.cpu_seconds if not quick else min(args.cpu_seconds, 10.0)
+    steps, t_used = 0, 0.0
+    while t_used < budget:
+        t0 = time.perf_counter()
+        cur = [dict(states[q], **{n: H.field(g.level, k).copy() for n, k in keys}) for q, g in enumerate(levels)]
+        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in levels]
+        oracle.rk4_multi(levels, nz, ph, cur, masks, DT_AD, 1, H=H)
+        H.mask_build(thr, 0, lmax)
+        H.compress()
+        H.inverse()
+        t_used += time.perf_counter() - t0
+        steps += 1
+    return {"value": sim_days_per_hour(steps, t_used, DT_AD), "unit": "simulated days per wall-clock hour",
+            "cores": oracle.get_threads(), "kind": "port",
+            "sample": f"{steps} adaptive steps of the same workload ({t_used:.1f} s): the multi-level trend on "
+                      f"{oracle.get_threads()} threads (one per lozenge), wavelets and masks on one thread"}
+
+
 def bench_reference(args):
     world, rank, local, pg = dist_init(args)
     if rank != 0:
@@ -436,7 +714,8 @@ def bench_reference(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded jet + white-noise free surface)",
+        "data": "synthetic (seeded jet + Gaussian bumps)" if args.mode == "adaptive"
+                else "synthetic (seeded jet + white-noise free surface)",
         "config": dict(workload_config(args, world),
                        note="CPU restatement of the reference path (no Fortran compiler on the host)"),
         "cpu_baseline": cb,

@@ -291,6 +291,12 @@ int wt_trend_multi(wt_handle* h);
  * state; the masks are held fixed.  The solution is the hierarchy's scaling
  * fields (level_end's is the stepper's state). */
 int wt_rk4_multi(wt_handle* h, double dt, int nsteps);
+/* wt_rk4_multi with CUDA events around its phases (7 entries): ms[p] is the
+ * mean duration of one occurrence of phase p and count[p] its occurrences per
+ * step: 0 column+step1 of level_end, 1 column+step1 of a coarser level,
+ * 2 restrictions into a level, 3 k_trend_ml of level_end, 4 k_trend_ml of a
+ * coarser level, 5 RK sub-step of the hierarchy, 6 WT_after_step. */
+int wt_profile_rk4_multi(wt_handle* h, double dt, int nsteps, double* ms, int* count);
 /* The trends of one level from the last wt_trend_multi: dmass, dtemp [nz][NN],
  * dvelo [nz][3*NN] host doubles (any may be NULL). */
 int wt_download_trend_level(wt_handle* h, int level, double* dmass, double* dtemp, double* dvelo);

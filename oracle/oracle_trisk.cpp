@@ -695,7 +695,7 @@ int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double 
       Work& w = W[q];
       const orc_mlevel& m = lv[q];
       // basic_operators
-      for (int d = 0; d < 10; ++d) {
+      pool().run([&](int d) {
         Ctx c = ctx(q, d, k);
         for (int j = 0; j <= n; ++j)
           for (int i = 0; i <= n; ++i) {
@@ -710,7 +710,7 @@ int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double 
           }
         step1(c);
         for (int corner = 5; corner <= 8; ++corner) post_step1(c, corner);
-      }
+      });
       if (q < nlev - 1) {
         Work& wc = W[q + 1];
         const int64_t NC = L[q + 1].NN;
@@ -732,7 +732,7 @@ int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double 
       // cal_scalar_trend: update_bdry(horiz_flux, l), scalar_trend over [0, n]
       halo_edges(Lq, w.hflux_m.data());
       halo_edges(Lq, w.hflux_t.data());
-      for (int d = 0; d < 10; ++d) {
+      pool().run([&](int d) {
         Ctx c = ctx(q, d, k);
         for (int j = 0; j <= n; ++j)
           for (int i = 0; i <= n; ++i) {
@@ -741,7 +741,7 @@ int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double 
             m.dmass[k * NN + id] = on ? -divg(c, w.hflux_m.data(), i, j) : 0.0;
             m.dtemp[k * NN + id] = on ? -divg(c, w.hflux_t.data(), i, j) : 0.0;
           }
-      }
+      });
       // velocity_trend_source
       double* dv = m.dvelo + k * 3 * NN;
       auto u_source = [&](Ctx& c, int i, int j) {
@@ -755,15 +755,15 @@ int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double 
         }
       };
       if (q == nlev - 1) {
-        for (int d = 0; d < 10; ++d) {
+        pool().run([&](int d) {
           Ctx c = ctx(q, d, k);
           for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i) u_source(c, i, j);
-        }
+        });
       } else {
         const Lev& Lc = L[q + 1];
         const int32_t* mc = lv[q + 1].mask_e;
-        for (int d = 0; d < 10; ++d) {
+        pool().run([&](int d) {
           Ctx c = ctx(q, d, k);
           for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i) {
@@ -772,7 +772,7 @@ int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double 
               for (int e = 1; e < 3; ++e) mn = mc[e * Lc.NN + idc] < mn ? mc[e * Lc.NN + idc] : mn;
               if (mn < ADJZONE) u_source(c, i, j);
             }
-        }
+        });
         orc_rlevel P = rlev(q, nullptr, nullptr, nullptr, dv);
         orc_rlevel C = rlev(q + 1, nullptr, nullptr, nullptr, lv[q + 1].dvelo + k * 3 * Lc.NN);
         orc_restrict_u_source(&P, &C, 1);
@@ -786,7 +786,7 @@ int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double 
       Work& w = W[q];
       const orc_mlevel& m = lv[q];
       double* dv = m.dvelo + k * 3 * NN;
-      for (int d = 0; d < 10; ++d) {
+      pool().run([&](int d) {
         Ctx c = ctx(q, d, k);
         for (int j = 0; j < n; ++j)
           for (int i = 0; i < n; ++i) {
@@ -813,7 +813,7 @@ int orc_trend_multi(const orc_mlevel* lv, int nlev, int nz, double grav, double 
             for (int e = 0; e < 3; ++e)
               dv[e * NN + id] = dv[e * NN + id] / Lq.len[e * NN + id] - gradB[e] - theta_e[e] * gradE[e];
           }
-      }
+      });
     }
   }
   return 0;

@@ -55,7 +55,7 @@ def test_reference_arm_under_torchrun_prints_once():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl", "reference",
-           "--gpus", "2", "--steps", "1", "--warmup", "0", "--level", "3", "--nz", "2", "--cpu-seconds", "0.5"]
+           "--gpus", "2", "--steps", "1", "--warmup", "0", "--lmin", "3", "--level", "4", "--nz", "2", "--cpu-seconds", "0.5"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]

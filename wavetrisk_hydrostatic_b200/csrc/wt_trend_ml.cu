@@ -68,6 +68,29 @@ void wt_trend_ml_release(wt_handle* h) {
 
 namespace {
 
+// Phase timer of the profiling entry point: CUDA events on the handle's stream
+// around each phase, accumulated per phase id.
+struct PhaseTimer {
+  cudaStream_t s;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> ids;
+  void mark(int id) {  // begin (id < 0) or end of phase id
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, s);
+    ev.push_back(e);
+    if (id >= 0) ids.push_back(id);
+  }
+  ~PhaseTimer() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+enum { PH_STEP1_TOP = 0, PH_STEP1_COARSE, PH_RESTRICT, PH_TREND_TOP, PH_TREND_COARSE, PH_RK_SUB, PH_AFTER_STEP, NPH };
+#define PB(t) \
+  if (t) (t)->mark(-1)
+#define PE(t, id) \
+  if (t) (t)->mark(id)
+
 // The scaling fields of every level (level_start first).
 struct States {
   std::vector<double*> m, t, v;
@@ -92,7 +115,7 @@ States hierarchy_state(wt_handle* h) {
 }
 
 // trend_ml of the state S into each level's dm, dt, dv (stream-ordered).
-int trend_multi(wt_handle* h, const States& S) {
+int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const int nz = h->nz;
   for (int l = h->level_end; l >= h->level_start; --l) {
@@ -102,19 +125,23 @@ int trend_multi(wt_handle* h, const States& S) {
     double *mm, *mt;
     if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
     if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
+    PB(tm);
     if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern,
                                 V.theta))
       return rc;
+    PE(tm, l == h->level_end ? PH_STEP1_TOP : PH_STEP1_COARSE);
     wtk::TrendML io{};
     const int *mask_n, *mask_e;
     wt_level_masks(h, l, &mask_n, &mask_e);
     io.mask_n = mask_n;
     if (l < h->level_end) {
       MLLevel& C = M->L[q + 1];
+      PB(tm);
       if (int rc = wt_level_restrict_scalar(h, l, V.bern, C.bern)) return rc;
       if (int rc = wt_level_restrict_scalar(h, l, V.phik, C.phik)) return rc;  // exner = -Phi_k
       if (int rc = wt_level_restrict_flux(h, l, V.hfm, C.hfm, C.dm)) return rc;
       if (int rc = wt_level_restrict_flux(h, l, V.hft, C.hft, C.dt)) return rc;
+      PE(tm, PH_RESTRICT);
       const int *mask_n_c, *mask_e_c;
       wt_level_masks(h, l + 1, &mask_n_c, &mask_e_c);
       io.mask_e_chd = mask_e_c;
@@ -125,7 +152,9 @@ int trend_multi(wt_handle* h, const States& S) {
     io.theta = V.theta; io.qe = V.qe; io.hfm = V.hfm; io.hft = V.hft; io.bern = V.bern; io.phik = V.phik;
     io.dm = V.dm; io.dtt = V.dt; io.dv = V.dv; io.src = V.src;
     const unsigned chunks = (unsigned)((D.NN + wtk::NODE_TILE - 1) / wtk::NODE_TILE);
+    PB(tm);
     wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
+    PE(tm, l == h->level_end ? PH_TREND_TOP : PH_TREND_COARSE);
     CKM(cudaGetLastError());
   }
   return WT_OK;
@@ -165,13 +194,10 @@ int wt_trend_multi(wt_handle* h) {
   return WT_OK;
 }
 
-// RK4 (src/time_integr.f90:78-103) over the hierarchy: each stage evaluates
-// trend_ml on every level, takes the RK sub-step on every level and runs
-// WT_after_step on the new stage state, with the masks held fixed.
-int wt_rk4_multi(wt_handle* h, double dt, int nsteps) {
-  if (!h || nsteps < 0) return WT_ERR_ARG;
-  if (!h->wav) return WT_ERR_STATE;
-  if (int rc = ensure(h)) return rc;
+}  // extern "C"
+
+namespace {
+int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const States q = hierarchy_state(h);
   States q1;
@@ -185,11 +211,57 @@ int wt_rk4_multi(wt_handle* h, double dt, int nsteps) {
     for (int stage = 0; stage < 4; ++stage) {
       const States& src = stage == 0 ? q : q1;
       const States& dest = stage == 3 ? q : q1;
-      if (int rc = trend_multi(h, src)) return rc;
+      if (int rc = trend_multi(h, src, tm)) return rc;
+      PB(tm);
       if (int rc = rk_sub_step(h, q, dest, hs[stage])) return rc;
+      PE(tm, PH_RK_SUB);
+      PB(tm);
       if (int rc = wt_level_after_step(h, dest.m.data(), dest.t.data(), dest.v.data())) return rc;
+      PE(tm, PH_AFTER_STEP);
     }
+  return WT_OK;
+}
+}  // namespace
+
+extern "C" {
+
+// RK4 (src/time_integr.f90:78-103) over the hierarchy: each stage evaluates
+// trend_ml on every level, takes the RK sub-step on every level and runs
+// WT_after_step on the new stage state, with the masks held fixed.
+int wt_rk4_multi(wt_handle* h, double dt, int nsteps) {
+  if (!h || nsteps < 0) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure(h)) return rc;
+  if (int rc = rk4_multi(h, dt, nsteps, nullptr)) return rc;
   CKM(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
+  return WT_OK;
+}
+
+// wt_rk4_multi with CUDA events around its phases: ms[p] = mean time of one
+// occurrence of phase p (0 column+step1 of level_end, 1 column+step1 of one
+// coarser level, 2 restrictions into one level, 3 k_trend_ml of level_end,
+// 4 k_trend_ml of one coarser level, 5 RK sub-step of the hierarchy,
+// 6 WT_after_step); count[p] = occurrences per step.
+int wt_profile_rk4_multi(wt_handle* h, double dt, int nsteps, double* ms, int* count) {
+  if (!h || nsteps < 1 || !ms || !count) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure(h)) return rc;
+  PhaseTimer tm{h->stream, {}, {}};
+  if (int rc = rk4_multi(h, dt, nsteps, &tm)) return rc;
+  CKM(cudaStreamSynchronize(h->stream));
+  double tot[NPH] = {0};
+  int cnt[NPH] = {0};
+  for (size_t q = 0; q < tm.ids.size(); ++q) {
+    float t = 0.f;
+    CKM(cudaEventElapsedTime(&t, tm.ev[2 * q], tm.ev[2 * q + 1]));
+    tot[tm.ids[q]] += t;
+    cnt[tm.ids[q]] += 1;
+  }
+  for (int p = 0; p < NPH; ++p) {
+    ms[p] = cnt[p] ? tot[p] / cnt[p] : 0.0;
+    count[p] = cnt[p] / nsteps;
+  }
   h->state_halo_done = false;
   return WT_OK;
 }

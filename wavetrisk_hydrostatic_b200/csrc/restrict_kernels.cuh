@@ -164,6 +164,170 @@ struct RChild {
   }
 };
 
+// flux_cpt_restr, one thread per restricted parent edge (e slowest, node
+// fastest), every layer and up to two fluxes (mass, Theta) per thread.  The
+// ghost remaps, R_F_wgt, the overlap-area factors of part_coarse_flux and
+// coarse_flux and the small-flux weights depend only on the grid, so they are
+// resolved once per thread; the layer loop then evaluates the same expression
+// trees as RChild (the small fluxes sm[e], sm[e+1] of the edge are evaluated by
+// each of the two edges that use them, in the same order, so both get the same
+// bits).  Edge reads outside the padded child level and node reads outside it
+// take 0, as the remapped readers do.
+struct SmTerm {  // one interp_flux small flux: +-(sum f(a) w0 + sum (f(p) - f(m)) w1)
+  int a[3], p[3], m[3];  // signed edge codes (slot * 2 + negate), -1 outside
+  double w0[3], w1[3];
+  bool pos;
+};
+
+__device__ __forceinline__ int ecode(const WLev& C, int d, int i, int j, int e) {
+  if (!inr(C, i, j)) return -1;
+  return __ldg(C.esrc + e * C.NN + nid(C, d, i, j));
+}
+__device__ __forceinline__ int ncode(const WLev& C, int d, int i, int j) {
+  if (!inr(C, i, j)) return -1;
+  return __ldg(C.nsrc + nid(C, d, i, j));
+}
+__device__ __forceinline__ double fe(const double* __restrict__ f, int c) {
+  if (c < 0) return 0.0;
+  const double v = f[c >> 1];
+  return (c & 1) ? -v : v;
+}
+__device__ __forceinline__ double fn(const double* __restrict__ f, int c) { return c < 0 ? 0.0 : f[c]; }
+
+__device__ __forceinline__ void sm_build(SmTerm& t, const WLev& C, int d, const RInd& r, const int a3[3],
+                                         const int p3[3], const int m3[3], int i0, int j0, int i1, int j1, bool pos) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    t.a[q] = ecode(C, d, r.ei[a3[q]], r.ej[a3[q]], r.ee[a3[q]]);
+    t.p[q] = ecode(C, d, r.ei[p3[q]], r.ej[p3[q]], r.ee[p3[q]]);
+    t.m[q] = ecode(C, d, r.ei[m3[q]], r.ej[m3[q]], r.ee[m3[q]]);
+    t.w0[q] = C.rf[q * C.NN + nid(C, d, i0, j0)];
+    t.w1[q] = C.rf[q * C.NN + nid(C, d, i1, j1)];
+  }
+  t.pos = pos;
+}
+__device__ __forceinline__ double sm_eval(const SmTerm& t, const double* __restrict__ h) {
+  double s1 = fe(h, t.a[0]) * t.w0[0];
+  s1 = s1 + fe(h, t.a[1]) * t.w0[1];
+  s1 = s1 + fe(h, t.a[2]) * t.w0[2];
+  double s2 = (fe(h, t.p[0]) - fe(h, t.m[0])) * t.w1[0];
+  s2 = s2 + (fe(h, t.p[1]) - fe(h, t.m[1])) * t.w1[1];
+  s2 = s2 + (fe(h, t.p[2]) - fe(h, t.m[2])) * t.w1[2];
+  return t.pos ? s1 + s2 : -s1 - s2;
+}
+// small flux q of interp_flux at child (i, j) (q = 0..3: UPLT S, LORT, UPLT, LORT W)
+__device__ __forceinline__ void sm_make(SmTerm& t, const WLev& C, int d, int i, int j, int q) {
+  if (q <= 1) {
+    const RInd r = get_indices(i + 1, j, RT);
+    if (q == 0) {
+      const int a3[3] = {S_WPM, S_UZM, S_VMM}, p3[3] = {S_VPM, S_WMMM, S_UMZ}, m3[3] = {S_UPZ, S_VPMM, S_WMM};
+      sm_build(t, C, d, r, a3, p3, m3, i + 1, j - 2, i + 1, j - 1, false);
+    } else {
+      const int a3[3] = {S_WMP, S_UZP, S_VPP}, p3[3] = {S_VMP, S_WPPP, S_UPZ}, m3[3] = {S_UMZ, S_VMPP, S_WPP};
+      sm_build(t, C, d, r, a3, p3, m3, i, j, i, j + 1, true);
+    }
+  } else {
+    const RInd r = get_indices(i, j + 1, UP);
+    if (q == 2) {
+      const int a3[3] = {S_UZM, S_VMM, S_WPM}, p3[3] = {S_WMMM, S_UMZ, S_VPM}, m3[3] = {S_VPMM, S_WMM, S_UPZ};
+      sm_build(t, C, d, r, a3, p3, m3, i + 1, j, i + 1, j + 1, false);
+    } else {
+      const int a3[3] = {S_UZP, S_VPP, S_WMP}, p3[3] = {S_WPPP, S_UPZ, S_VMP}, m3[3] = {S_VMPP, S_WPP, S_UMZ};
+      sm_build(t, C, d, r, a3, p3, m3, i - 2, j, i - 2, j + 1, true);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_restr_flux2(WLev P, WLev C, int nz, double* __restrict__ fp0,
+                                                     double* __restrict__ fp1, const double* __restrict__ fc0,
+                                                     const double* __restrict__ fc1, const double* __restrict__ dc0,
+                                                     const double* __restrict__ dc1) {
+  const int m = P.n;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)3 * 10 * m * m) return;
+  const int ip = (int)(t % m), jp = (int)((t / m) % m), d = (int)((t / ((int64_t)m * m)) % 10);
+  const int e = (int)(t / ((int64_t)10 * m * m));
+  const int idp = nid(P, d, ip, jp);
+  if (P.mask_e[e * P.NN + idp] < M_RESTRCT) return;
+  const int ic = 2 * ip, jc = 2 * jp;
+  // the two small fluxes of the edge: RT sm0, sm1; DG sm1, sm2; UP sm2, sm3
+  SmTerm sa, sb;
+  sm_make(sa, C, d, ic, jc, e);
+  sm_make(sb, C, d, ic, jc, e + 1);
+  // child node of the edge
+  const int ci = (e == UP) ? ic : ic + 1, cj = (e == RT) ? jc : jc + 1;
+  const RInd r = get_indices(ci, cj, e);
+  // part_coarse_flux constants
+  const RChild G{C, nullptr, nullptr, d};
+  double ar0 = G.a(ci, cj, 0), ar1 = G.a(ci, cj, 1);
+  double o0 = G.sp(ci, cj, 0), o1 = G.sp(ci, cj, 1);
+  double o2 = G.a(ci, cj, 2) - o0, o3 = G.a(ci, cj, 3) - o1;
+  ar0 = ar0 + o0 + o3;
+  ar1 = ar1 + o1 + o2;
+  const double s = ar0 + ar1;
+  ar0 = ar0 / s;
+  ar1 = ar1 / s;
+  const int mpi = r.ni[0], mpj = r.nj[0], ppi = r.ni[1], ppj = r.nj[1];
+  const int pmi = r.ni[2], pmj = r.nj[2], mmi = r.ni[3], mmj = r.nj[3];
+  o0 = G.sp(ppi, ppj, 0);
+  o1 = G.sp(mmi, mmj, 1);
+  o2 = G.a(mpi, mpj, 2) - G.sp(mpi, mpj, 0);
+  o3 = G.a(pmi, pmj, 3) - G.sp(pmi, pmj, 1);
+  const int cUPZ = ecode(C, d, r.ei[S_UPZ], r.ej[S_UPZ], r.ee[S_UPZ]);
+  const int cUMZ = ecode(C, d, r.ei[S_UMZ], r.ej[S_UMZ], r.ee[S_UMZ]);
+  const int cVMM = ecode(C, d, r.ei[S_VMM], r.ej[S_VMM], r.ee[S_VMM]);
+  const int cWMP = ecode(C, d, r.ei[S_WMP], r.ej[S_WMP], r.ee[S_WMP]);
+  const int cWPM = ecode(C, d, r.ei[S_WPM], r.ej[S_WPM], r.ee[S_WPM]);
+  const int cVPP = ecode(C, d, r.ei[S_VPP], r.ej[S_VPP], r.ee[S_VPP]);
+  const int nMP = ncode(C, d, mpi, mpj), nPP = ncode(C, d, ppi, ppj);
+  const int nPM = ncode(C, d, pmi, pmj), nMM = ncode(C, d, mmi, mmj);
+  // coarse_flux constants (the neighbours mp, pp, pm, mm are part_coarse_flux's MP, PP, PM, MM)
+  const int hs = c_hex_s_offs[e];
+  const int mzi = ci + c_nghb_pt[hs + 1][0], mzj = cj + c_nghb_pt[hs + 1][1];
+  const int pzi = ci + c_nghb_pt[hs + 4][0], pzj = cj + c_nghb_pt[hs + 4][1];
+  const double wpp = G.a(ppi, ppj, 2) * G.a(ppi, ppj, 3) * G.hi(ppi, ppj);
+  const double wpm = G.a(pmi, pmj, 2) * G.a(pmi, pmj, 3) * G.hi(pmi, pmj);
+  const double wmp = G.a(mpi, mpj, 2) * G.a(mpi, mpj, 3) * G.hi(mpi, mpj);
+  const double wmm = G.a(mmi, mmj, 2) * G.a(mmi, mmj, 3) * G.hi(mmi, mmj);
+  double cc = G.a(ci, cj, 0) * G.a(ci, cj, 1) * G.hi(ci, cj);
+  cc = cc + G.a(mpi, mpj, 1) * G.a(mpi, mpj, 2) * G.hi(mpi, mpj);
+  cc = cc + G.a(ppi, ppj, 0) * G.a(ppi, ppj, 2) * G.hi(ppi, ppj);
+  cc = cc + G.a(pmi, pmj, 0) * G.a(pmi, pmj, 3) * G.hi(pmi, pmj);
+  cc = cc + G.a(mmi, mmj, 1) * G.a(mmi, mmj, 3) * G.hi(mmi, mmj);
+  const double hpp = wpp * 0.5, hpm = wpm * 0.5, hmp = wmp * 0.5, hmm = wmm * 0.5;
+  const int nMZ = ncode(C, d, mzi, mzj), nPZ = ncode(C, d, pzi, pzj);
+  const int nMM2 = ncode(C, d, ci + c_bfly_no2[e][0][0], cj + c_bfly_no2[e][0][1]);
+  const int nPM2 = ncode(C, d, ci + c_bfly_no2[e][1][0], cj + c_bfly_no2[e][1][1]);
+  const int nPP2 = ncode(C, d, ci + c_bfly_no2[e][2][0], cj + c_bfly_no2[e][2][1]);
+  const int nMP2 = ncode(C, d, ci + c_bfly_no2[e][3][0], cj + c_bfly_no2[e][3][1]);
+  const int64_t so = (int64_t)e * P.NN + idp;
+  for (int k = 0; k < nz; ++k) {
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+      double* __restrict__ fp = f == 0 ? fp0 : fp1;
+      if (!fp) continue;
+      const double* __restrict__ h = (f == 0 ? fc0 : fc1) + (int64_t)3 * k * C.NN;
+      const double* __restrict__ ds = (f == 0 ? dc0 : dc1) + (int64_t)k * C.NN;
+      const double sma = sm_eval(sa, h), smb = sm_eval(sb, h);
+      double tp = fe(h, cUPZ) * ar0;
+      tp = tp + fe(h, cUMZ) * ar1;
+      tp = tp - (fe(h, cVMM) + fe(h, cWMP)) * ar1;
+      tp = tp - (fe(h, cWPM) + fe(h, cVPP)) * ar0;
+      tp = tp + o2 * fn(ds, nMP);
+      tp = tp - o3 * fn(ds, nPM);
+      tp = tp - o0 * fn(ds, nPP);
+      tp = tp + o1 * fn(ds, nMM);
+      const double dmz = fn(ds, nMZ), dpz = fn(ds, nPZ);
+      double tc = cc * (dpz - dmz);
+      tc = tc + hpp * (fn(ds, nPP2) - dmz);
+      tc = tc + hpm * (fn(ds, nPM2) - dmz);
+      tc = tc + hmp * (dpz - fn(ds, nMP2));
+      tc = tc + hmm * (dpz - fn(ds, nMM2));
+      fp[(int64_t)3 * k * P.NN + so] = tp + tc + sma + smb;
+    }
+  }
+}
+
 // scalar_cpt_restr over parents [0, n]^2, every layer.
 __global__ void k_restr_scalar(WLev P, WLev C, int nz) {
   const int m = P.n + 1;

@@ -139,8 +139,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr) {
       PB(tm);
       if (int rc = wt_level_restrict_scalar(h, l, V.bern, C.bern)) return rc;
       if (int rc = wt_level_restrict_scalar(h, l, V.phik, C.phik)) return rc;  // exner = -Phi_k
-      if (int rc = wt_level_restrict_flux(h, l, V.hfm, C.hfm, C.dm)) return rc;
-      if (int rc = wt_level_restrict_flux(h, l, V.hft, C.hft, C.dt)) return rc;
+      if (int rc = wt_level_restrict_flux(h, l, V.hfm, V.hft, C.hfm, C.hft, C.dm, C.dt)) return rc;
       PE(tm, PH_RESTRICT);
       const int *mask_n_c, *mask_e_c;
       wt_level_masks(h, l + 1, &mask_n_c, &mask_e_c);

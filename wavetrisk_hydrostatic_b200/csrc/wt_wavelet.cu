@@ -436,15 +436,12 @@ int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double*
   return WT_OK;
 }
 
-int wt_level_restrict_flux(wt_handle* h, int level, double* par_flux, const double* chd_flux,
-                           const double* chd_dscal) {
+int wt_level_restrict_flux(wt_handle* h, int level, double* par0, double* par1, const double* chd0,
+                           const double* chd1, const double* dsc0, const double* dsc1) {
   if (!h->at(level + 1).rf_wgt || !h->at(level + 1).overl_split) return WT_ERR_ARG;
-  WLev P = view(h, level), C = view(h, level + 1);
-  P.flux = par_flux;
-  C.flux = const_cast<double*>(chd_flux);
-  C.dscal = const_cast<double*>(chd_dscal);
   const int m = h->at(level).n;
-  k_restr_flux<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(P, C, h->nz);
+  k_restr_flux2<<<nb((int64_t)3 * 10 * m * m), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz, par0,
+                                                                     par1, chd0, chd1, dsc0, dsc1);
   CKW(cudaGetLastError());
   return WT_OK;
 }
@@ -476,10 +473,11 @@ int wt_restrict_scalar(wt_handle* h, int level) {
 
 int wt_restrict_flux(wt_handle* h, int level) {
   if (int rc = restrict_pair(h, level, {WT_WORK_FLUX, WT_WORK_DSCALAR})) return rc;
-  const DevLevel& C = h->at(level + 1);
-  if (!C.rf_wgt || !C.overl_split) return WT_ERR_ARG;
+  if (!h->at(level + 1).rf_wgt || !h->at(level + 1).overl_split) return WT_ERR_ARG;
+  const WLev P = view(h, level), C = view(h, level + 1);
   const int m = h->at(level).n;
-  k_restr_flux<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz);
+  k_restr_flux2<<<nb((int64_t)3 * 10 * m * m), TPB, 0, h->stream>>>(P, C, h->nz, P.flux, nullptr, C.flux, nullptr,
+                                                                     C.dscal, nullptr);
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;

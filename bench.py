@@ -300,13 +300,14 @@ def wavelet_case(lmin, lmax, nz, repeats=5, device=None):
 def adaptive_launches(L):
     """Kernels launched by one adaptive step of L levels (AdaptiveOcean.step
     with fixed thresholds, max_level = level_end): RK4 of the hierarchy (per
-    stage: column + step1 and k_trend_ml per level, four restrictions per
-    coarse level, three RK sub-step kernels per level, WT_after_step with two
-    wavelet kernels per coarse level, one compression kernel per fine level
+    stage: column + step1 and k_trend_ml per level, three restrictions per
+    coarse level (Bernoulli, Exner, both fluxes), three RK sub-step kernels per
+    level, WT_after_step with three wavelet kernels per coarse level (scalar,
+    outer and inner velocity), one compression kernel per fine level
     and four inverse-transform kernels per coarse level), wt_mask_build's
     sweeps (comm_masks launches one kernel per level), compression and the
     inverse transform."""
-    stage = 3 * L + 4 * (L - 1) + 3 * L + 2 * (L - 1) + (L - 1) + 4 * (L - 1)
+    stage = 3 * L + 3 * (L - 1) + 3 * L + 3 * (L - 1) + (L - 1) + 4 * (L - 1)
     masks = ((L - 1) + 1 + L + (L - 1) * (L + 2) + L + L + L + (L - 1) + L + L + 2 * (L - 1) + L
              + (L - 2) * (2 + 2 * L) + (1 + L) + 2 * (L - 2) + 1 + L + L)
     return 4 * stage + masks + (L - 1) + 4 * (L - 1)

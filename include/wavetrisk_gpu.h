@@ -252,6 +252,11 @@ int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max
  * (max |.|), 1 "1" (mean |.|), 2 "2" (rms), 3 "min"; the mean and rms divide
  * by the count of nodes [-1, n+1]^2 with mask_n >= ADJZONE. */
 int wt_lnorm(wt_handle* h, int order, double* out);
+/* Launch-shape tuning (process-wide).  WT_TUNE_WAVELET_LAYERS: layers per
+ * thread of the interscale wavelet kernels (1..64; 0 = default: 2 up to 16
+ * layers, 4 above). */
+enum { WT_TUNE_WAVELET_LAYERS = 1 };
+int wt_tune(wt_handle* h, int param, int value);
 /* compress_wavelets (src/adapt.f90:79-103): zero the wavelets of inactive points. */
 int wt_compress(wt_handle* h);
 /* WT_after_step (src/adapt.f90:234-283): wavelets of the current scaling fields,

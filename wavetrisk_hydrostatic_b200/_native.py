@@ -134,6 +134,7 @@ _DEVICE_SIGS = {
     "wt_rk4_multi": [_vp, C.c_double, C.c_int],
     "wt_profile_rk4_multi": [_vp, C.c_double, C.c_int, _dp, C.POINTER(C.c_int)],
     "wt_lnorm": [_vp, C.c_int, _dp],
+    "wt_tune": [_vp, C.c_int, C.c_int],
     "wt_download_trend_level": [_vp, C.c_int, _dp, _dp, _dp],
     "wt_restrict_scalar": [_vp, C.c_int],
     "wt_restrict_flux": [_vp, C.c_int],

@@ -4,7 +4,9 @@
 //
 // Each kernel is one interscale (parent level l, child level l+1) or onescale
 // pass of the reference's drivers (src/wavelet.f90, src/adapt.f90,
-// src/mask.f90), one thread per (layer, lozenge, node) of the pass's range.
+// src/mask.f90), one thread per (layer, lozenge, node) of the pass's range;
+// the interscale transform kernels that run every layer of a parent per thread
+// are in wavelet_layers.cuh, with the pentagon helpers here.
 // Ghost values are read through the level's remap tables (the node or signed
 // edge that update_bdry copies there); masks and weights are read as stored.
 // Floating point keeps the reference's operand order (compiled with
@@ -99,32 +101,6 @@ __device__ __forceinline__ bool decode(int nz, int m, int& k, int& d, int& i, in
   return true;
 }
 
-// Interp_node (src/wavelet.f90:1487-1498)
-__device__ __forceinline__ double interp_node(const WLev& C, const double* s, int d, int i, int j, int i1, int j1,
-                                              int i2, int j2, int i3, int j3, int i4, int j4) {
-  return (oa(C, d, i, j, 1) * rn(C, s, d, i1, j1) + oa(C, d, i, j, 2) * rn(C, s, d, i2, j2) +
-          oa(C, d, i, j, 3) * rn(C, s, d, i3, j3) + oa(C, d, i, j, 4) * rn(C, s, d, i4, j4)) *
-         hv(C, d, i, j);
-}
-
-// Compute_scalar_wavelets (src/wavelet.f90:642-670), parents [0, np)^2, both scalars.
-__global__ void k_scalar_wc(WLev C, int np, int nz) {
-  int k, d, ip, jp;
-  if (!decode(nz, np, k, d, ip, jp)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  for (int v = 0; v < 2; ++v) {
-    const double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
-    double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
-    if (mn(C, d, i + 1, j) >= ADJZONE)
-      wc[nid(C, d, i + 1, j)] = rn(C, s, d, i + 1, j) - interp_node(C, s, d, i + 1, j, i, j, i + 2, j, i + 2, j + 2, i, j - 2);
-    if (mn(C, d, i + 1, j + 1) >= ADJZONE)
-      wc[nid(C, d, i + 1, j + 1)] =
-          rn(C, s, d, i + 1, j + 1) - interp_node(C, s, d, i + 1, j + 1, i + 2, j + 2, i, j, i + 2, j, i, j + 2);
-    if (mn(C, d, i, j + 1) >= ADJZONE)
-      wc[nid(C, d, i, j + 1)] = rn(C, s, d, i, j + 1) - interp_node(C, s, d, i, j + 1, i, j, i, j + 2, i - 2, j, i + 2, j + 2);
-  }
-}
-
 // Restrict_scalar (parents [0, np]^2, src/wavelet.f90:520-569) and
 // Restrict_velo (parents [0, np)^2, :1154-1174).
 __global__ void k_restrict(WLev Pa, WLev C, int nz) {
@@ -157,91 +133,12 @@ __global__ void k_restrict(WLev Pa, WLev C, int nz) {
   }
 }
 
-// Interp_outer_velo (src/wavelet.f90:1064-1094): child weights at (ic, jc).
-__device__ double interp_outer(const WLev& Pa, const WLev& C, const double* vp, int d, int ip, int jp, int ic, int jc,
-                               int e) {
-  const int hs = c_hex_s_offs[e];
-  auto ved = [&](const int* off, int col) {
-    return re(Pa, vp, c_hex_sides[col][2], d, ip + off[0] + c_hex_sides[col][0], jp + off[1] + c_hex_sides[col][1]);
-  };
-  const int* e1 = c_end_pt[e][0];
-  const int* e2 = c_end_pt[e][1];
-  const int* o1 = c_opp_no[e][0];
-  const int* o2 = c_opp_no[e][1];
-  double t[9];
-  t[0] = re(Pa, vp, e, d, ip, jp);
-  t[1] = ved(e2, hs + 2);
-  t[2] = ved(e1, hs + 3);
-  t[3] = ved(e1, hs + 5);
-  t[4] = ved(e2, hs + 0);
-  t[5] = ved(o1, hs + 1) - ved(e1, hs + 2);
-  t[6] = ved(e2, hs + 3) - ved(o1, hs + 4);
-  t[7] = ved(o2, hs + 4) - ved(e2, hs + 5);
-  t[8] = ved(e1, hs + 0) - ved(o2, hs + 1);
-  double sum = 0.0;
-#pragma unroll
-  for (int q = 0; q < 9; ++q) sum = sum + (c_iu_base[q] + iw(C, q, d, ic, jc)) * t[q];
-  return sum;
-}
-
-// Interp_inner_velo (src/wavelet.f90:1005-1062)
-__device__ void interp_inner(const WLev& Pa, const WLev& C, const double* vp, const double* v, int d, int ip, int jp,
-                             double u[6]) {
-  double curl[2];
-#pragma unroll
-  for (int t = LORT; t <= UPLT; ++t) {
-    const int i1 = ip - t + 1, j1 = jp, i2 = ip, j2 = jp + t;
-    curl[t] = (re(Pa, vp, DG, d, ip, jp) * ln(Pa, DG, d, ip, jp) + re(Pa, vp, UP, d, i1, j1) * ln(Pa, UP, d, i1, j1) +
-               re(Pa, vp, RT, d, i2, j2) * ln(Pa, RT, d, i2, j2)) /
-              ta(Pa, t, d, ip, jp);
-  }
-  const int i = 2 * ip, j = 2 * jp;
-  auto pr = [&](int e, int a, int b) { return re(C, v, e, d, a, b) * ln(C, e, d, a, b); };
-  u[0] = (ta(C, LORT, d, i, j) * curl[LORT] - pr(RT, i, j) - pr(DG, i, j)) / ln(C, UP, d, i + 1, j);
-  u[1] = (ta(C, LORT, d, i + 1, j) * curl[LORT] - pr(RT, i + 1, j) - pr(UP, i + 2, j)) / ln(C, DG, d, i + 1, j);
-  u[2] = (ta(C, LORT, d, i + 1, j + 1) * curl[LORT] - pr(DG, i + 1, j + 1) - pr(UP, i + 2, j + 1)) /
-         ln(C, RT, d, i + 1, j + 1);
-  u[3] = (ta(C, UPLT, d, i, j) * curl[UPLT] - pr(UP, i, j) - pr(DG, i, j)) / ln(C, RT, d, i, j + 1);
-  u[4] = (ta(C, UPLT, d, i, j + 1) * curl[UPLT] - pr(UP, i, j + 1) - pr(RT, i, j + 2)) / ln(C, DG, d, i, j + 1);
-  u[5] = (ta(C, UPLT, d, i + 1, j + 1) * curl[UPLT] - pr(DG, i + 1, j + 1) - pr(RT, i + 1, j + 2)) /
-         ln(C, UP, d, i + 1, j + 1);
-}
-
 __device__ __forceinline__ double& ee(const WLev& L, double* f, int e, int d, int i, int j) {
   return f[e * L.NN + nid(L, d, i, j)];
 }
 
 __device__ void penta_compute(const WLev& Pa, const WLev& C, const double* vp, double* wc, int d, int ip, int jp);
 __device__ void penta_reconstruct(const WLev& Pa, const WLev& C, const double* vp, double* v, int d, int ip, int jp);
-
-// Compute_velo_wavelets (src/wavelet.f90:672-710), parents [0, np)^2, then the
-// pentagon corrections of the corner parents.
-__global__ void k_velo_wc(WLev Pa, WLev C, int nz) {
-  int k, d, ip, jp;
-  if (!decode(nz, Pa.n, k, d, ip, jp)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
-  const double* v = C.sv + (int64_t)k * 3 * C.NN;
-  double* wc = C.wv + (int64_t)k * 3 * C.NN;
-  for (int e = 0; e < 3; ++e) {
-    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
-    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
-    if (me(C, e, d, a2, b2) < ADJZONE) continue;
-    const double u = interp_outer(Pa, C, vp, d, ip, jp, a2, b2, e);
-    const double w = re(C, v, e, d, a2, b2) - u;
-    ee(C, wc, e, d, a2, b2) = w;
-    ee(C, wc, e, d, a1, b1) = -w;
-  }
-  double u[6];
-  interp_inner(Pa, C, vp, v, d, ip, jp, u);
-  if (me(C, UP, d, i + 1, j) >= ADJZONE) ee(C, wc, UP, d, i + 1, j) = re(C, v, UP, d, i + 1, j) - u[0];
-  if (me(C, DG, d, i + 1, j) >= ADJZONE) ee(C, wc, DG, d, i + 1, j) = re(C, v, DG, d, i + 1, j) - u[1];
-  if (me(C, RT, d, i + 1, j + 1) >= ADJZONE) ee(C, wc, RT, d, i + 1, j + 1) = re(C, v, RT, d, i + 1, j + 1) - u[2];
-  if (me(C, RT, d, i, j + 1) >= ADJZONE) ee(C, wc, RT, d, i, j + 1) = re(C, v, RT, d, i, j + 1) - u[3];
-  if (me(C, DG, d, i, j + 1) >= ADJZONE) ee(C, wc, DG, d, i, j + 1) = re(C, v, DG, d, i, j + 1) - u[4];
-  if (me(C, UP, d, i + 1, j + 1) >= ADJZONE) ee(C, wc, UP, d, i + 1, j + 1) = re(C, v, UP, d, i + 1, j + 1) - u[5];
-  if ((ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1)) penta_compute(Pa, C, vp, wc, d, ip, jp);
-}
 
 // velo_interp_penta_corr (src/wavelet.f90:927-952) at the south-west corner.
 __device__ void penta_corr(const WLev& Pa, const WLev& C, const double* vp, int d, double u[2]) {
@@ -307,84 +204,6 @@ __device__ void penta_reconstruct(const WLev& Pa, const WLev& C, const double* v
     ee(C, v, UP, d, 0, nc - 2) = ee(C, v, UP, d, 0, nc - 2) - vv;
     ee(C, v, UP, d, 0, nc - 1) = ee(C, v, UP, d, 0, nc - 1) + vv;
   }
-}
-
-// Prolong_scalar (src/wavelet.f90:571-612), parents [0, np]^2: eleven of the
-// twelve lifting terms, as the reference sums them.
-__global__ void k_prolong(WLev Pa, WLev C, int nz) {
-  const int np = Pa.n;
-  int k, d, ip, jp;
-  if (!decode(nz, np + 1, k, d, ip, jp)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  if (mn(C, d, i, j) == FROZEN) return;
-  for (int v = 0; v < 2; ++v) {
-    const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
-    const double* sp = (v == 0 ? Pa.sm : Pa.st) + (int64_t)k * Pa.NN;
-    double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
-    const double sum =
-        rn(C, wc, d, i + 1, j) * oa(C, d, i + 1, j, 1) + rn(C, wc, d, i + 1, j + 1) * oa(C, d, i + 1, j + 1, 2) +
-        rn(C, wc, d, i + 2, j + 1) * oa(C, d, i + 2, j + 1, 3) + rn(C, wc, d, i, j + 1) * oa(C, d, i, j + 1, 1) +
-        rn(C, wc, d, i - 1, j) * oa(C, d, i - 1, j, 2) + rn(C, wc, d, i - 1, j + 1) * oa(C, d, i - 1, j + 1, 3) +
-        rn(C, wc, d, i - 2, j - 1) * oa(C, d, i - 2, j - 1, 4) + rn(C, wc, d, i - 1, j - 1) * oa(C, d, i - 1, j - 1, 1) +
-        rn(C, wc, d, i, j - 1) * oa(C, d, i, j - 1, 2) + rn(C, wc, d, i - 1, j - 2) * oa(C, d, i - 1, j - 2, 3) +
-        rn(C, wc, d, i + 1, j - 1) * oa(C, d, i + 1, j - 1, 4);
-    s[nid(C, d, i, j)] = rn(Pa, sp, d, ip, jp) - sum * hv(Pa, d, ip, jp);
-  }
-}
-
-// Reconstruct_outer_velo (src/wavelet.f90:954-976), parents [0, np]^2, then
-// Reconstruct_velo_penta by the corner parents.
-__global__ void k_recon_outer(WLev Pa, WLev C, int nz) {
-  int k, d, ip, jp;
-  if (!decode(nz, Pa.n + 1, k, d, ip, jp)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
-  const double* wc = C.wv + (int64_t)k * 3 * C.NN;
-  double* v = C.sv + (int64_t)k * 3 * C.NN;
-  for (int e = 0; e < 3; ++e) {
-    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
-    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
-    const double u = interp_outer(Pa, C, vp, d, ip, jp, a2, b2, e);
-    const double v2 = u + re(C, wc, e, d, a2, b2);
-    ee(C, v, e, d, a2, b2) = v2;
-    ee(C, v, e, d, a1, b1) = 2.0 * re(Pa, vp, e, d, ip, jp) - v2;
-  }
-  if ((ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1)) penta_reconstruct(Pa, C, vp, v, d, ip, jp);
-}
-
-// Reconstruct_scalar (src/wavelet.f90:614-640), parents [0, np)^2.
-__global__ void k_recon_scalar(WLev C, int np, int nz) {
-  int k, d, ip, jp;
-  if (!decode(nz, np, k, d, ip, jp)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  for (int v = 0; v < 2; ++v) {
-    const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
-    double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
-    const double a = interp_node(C, s, d, i + 1, j, i, j, i + 2, j, i + 2, j + 2, i, j - 2) + rn(C, wc, d, i + 1, j);
-    const double b = interp_node(C, s, d, i + 1, j + 1, i + 2, j + 2, i, j, i + 2, j, i, j + 2) + rn(C, wc, d, i + 1, j + 1);
-    const double c = interp_node(C, s, d, i, j + 1, i, j, i, j + 2, i - 2, j, i + 2, j + 2) + rn(C, wc, d, i, j + 1);
-    s[nid(C, d, i + 1, j)] = a;
-    s[nid(C, d, i + 1, j + 1)] = b;
-    s[nid(C, d, i, j + 1)] = c;
-  }
-}
-
-// Reconstruct_inner_velo (src/wavelet.f90:978-1003), parents [0, np)^2.
-__global__ void k_recon_inner(WLev Pa, WLev C, int nz) {
-  int k, d, ip, jp;
-  if (!decode(nz, Pa.n, k, d, ip, jp)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
-  const double* wc = C.wv + (int64_t)k * 3 * C.NN;
-  double* v = C.sv + (int64_t)k * 3 * C.NN;
-  double u[6];
-  interp_inner(Pa, C, vp, v, d, ip, jp, u);
-  ee(C, v, UP, d, i + 1, j) = u[0] + re(C, wc, UP, d, i + 1, j);
-  ee(C, v, DG, d, i + 1, j) = u[1] + re(C, wc, DG, d, i + 1, j);
-  ee(C, v, RT, d, i + 1, j + 1) = u[2] + re(C, wc, RT, d, i + 1, j + 1);
-  ee(C, v, RT, d, i, j + 1) = u[3] + re(C, wc, RT, d, i, j + 1);
-  ee(C, v, DG, d, i, j + 1) = u[4] + re(C, wc, DG, d, i, j + 1);
-  ee(C, v, UP, d, i + 1, j + 1) = u[5] + re(C, wc, UP, d, i + 1, j + 1);
 }
 
 // mask_tol_vars (src/mask.f90:102-156) on nodes [st, n-1+en]^2 of one level,

@@ -1,0 +1,387 @@
+// Interscale wavelet kernels with the layer loop inside the thread: one thread
+// per (lozenge, parent node) resolves its ghost remaps, masks, overlap areas
+// and interpolation weights once, then runs every layer (and both scalars)
+// with the same expressions, in the same operand order, as the reference's
+// per-node routines (src/wavelet.f90).  A warp still covers consecutive
+// parents, so each layer's loads and stores stay coalesced along rows.
+#pragma once
+#include "wavelet_kernels.cuh"
+
+namespace wtw {
+
+// Codes of the remapped readers: node code = source node, edge code = source
+// slot * 2 + negate; -1 outside the padded level (the reader returns 0).
+__device__ __forceinline__ int wn_code(const WLev& L, int d, int i, int j) {
+  return inr(L, i, j) ? __ldg(L.nsrc + nid(L, d, i, j)) : -1;
+}
+__device__ __forceinline__ int we_code(const WLev& L, int e, int d, int i, int j) {
+  return inr(L, i, j) ? __ldg(L.esrc + e * L.NN + nid(L, d, i, j)) : -1;
+}
+__device__ __forceinline__ double wn(const double* __restrict__ f, int c) { return c < 0 ? 0.0 : f[c]; }
+__device__ __forceinline__ double we(const double* __restrict__ f, int c) {
+  if (c < 0) return 0.0;
+  const double v = f[c >> 1];
+  return (c & 1) ? -v : v;
+}
+
+// Parent (d, ip, jp) of [0, m)^2 and layer range [k0, k1) of this thread: the
+// layers are split into groups of lpt (grid: 10 m^2 threads per group, group
+// slowest), trading the once-per-thread setup against the number of threads.
+__device__ __forceinline__ bool parent_of(int m, int nz, int lpt, int& d, int& ip, int& jp, int& k0, int& k1) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t per = (int64_t)10 * m * m;
+  const int ng = (nz + lpt - 1) / lpt;
+  if (t >= per * ng) return false;
+  const int g = (int)(t / per);
+  const int r0 = (int)(t - (int64_t)g * per);
+  d = r0 / (m * m);
+  const int r = r0 - d * m * m;
+  jp = r / m;
+  ip = r - jp * m;
+  k0 = g * lpt;
+  k1 = min(nz, k0 + lpt);
+  return true;
+}
+
+// Interp_node's four weights and hex_inv at child node (i, j) with its four
+// neighbours' codes.
+struct NodeInterp {
+  double o[4], h;
+  int c[4];
+};
+__device__ __forceinline__ void node_interp(NodeInterp& N, const WLev& C, int d, int i, int j, int i1, int j1,
+                                            int i2, int j2, int i3, int j3, int i4, int j4) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) N.o[q] = oa(C, d, i, j, q + 1);
+  N.h = hv(C, d, i, j);
+  N.c[0] = wn_code(C, d, i1, j1);
+  N.c[1] = wn_code(C, d, i2, j2);
+  N.c[2] = wn_code(C, d, i3, j3);
+  N.c[3] = wn_code(C, d, i4, j4);
+}
+__device__ __forceinline__ double node_eval(const NodeInterp& N, const double* __restrict__ s) {
+  return (N.o[0] * wn(s, N.c[0]) + N.o[1] * wn(s, N.c[1]) + N.o[2] * wn(s, N.c[2]) + N.o[3] * wn(s, N.c[3])) * N.h;
+}
+// The three new child nodes of parent (ip, jp): E (i+1, j), NE (i+1, j+1), N (i, j+1).
+__device__ __forceinline__ void child_interps(NodeInterp N[3], const WLev& C, int d, int i, int j) {
+  node_interp(N[0], C, d, i + 1, j, i, j, i + 2, j, i + 2, j + 2, i, j - 2);
+  node_interp(N[1], C, d, i + 1, j + 1, i + 2, j + 2, i, j, i + 2, j, i, j + 2);
+  node_interp(N[2], C, d, i, j + 1, i, j, i, j + 2, i - 2, j, i + 2, j + 2);
+}
+
+// Compute_scalar_wavelets (src/wavelet.f90:642-670), parents [0, np)^2.
+__global__ void __launch_bounds__(128) k_scalar_wc_l(WLev C, int np, int nz, int lpt) {
+  int d, ip, jp;
+  int k0, k1;
+  if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  const int ci[3] = {i + 1, i + 1, i}, cj[3] = {j, j + 1, j + 1};
+  bool on[3];
+  int self[3], at[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    on[q] = mn(C, d, ci[q], cj[q]) >= ADJZONE;
+    self[q] = wn_code(C, d, ci[q], cj[q]);
+    at[q] = nid(C, d, ci[q], cj[q]);
+  }
+  if (!(on[0] || on[1] || on[2])) return;
+  NodeInterp N[3];
+  child_interps(N, C, d, i, j);
+  for (int k = k0; k < k1; ++k)
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+      double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        if (on[q]) wc[at[q]] = wn(s, self[q]) - node_eval(N[q], s);
+    }
+}
+
+// Reconstruct_scalar (src/wavelet.f90:614-640), parents [0, np)^2.
+__global__ void __launch_bounds__(128) k_recon_scalar_l(WLev C, int np, int nz, int lpt) {
+  int d, ip, jp;
+  int k0, k1;
+  if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  const int ci[3] = {i + 1, i + 1, i}, cj[3] = {j, j + 1, j + 1};
+  int self[3], at[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    self[q] = wn_code(C, d, ci[q], cj[q]);
+    at[q] = nid(C, d, ci[q], cj[q]);
+  }
+  NodeInterp N[3];
+  child_interps(N, C, d, i, j);
+  for (int k = k0; k < k1; ++k)
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+      double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+      double r[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) r[q] = node_eval(N[q], s) + wn(wc, self[q]);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) s[at[q]] = r[q];
+    }
+}
+
+// Prolong_scalar (src/wavelet.f90:571-612), parents [0, np]^2: the eleven
+// lifting terms the reference sums.
+__global__ void __launch_bounds__(128) k_prolong_l(WLev Pa, WLev C, int nz, int lpt) {
+  const int np = Pa.n;
+  int d, ip, jp;
+  int k0, k1;
+  if (!parent_of(np + 1, nz, lpt, d, ip, jp, k0, k1)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  if (mn(C, d, i, j) == FROZEN) return;
+  const int ti[11] = {i + 1, i + 1, i + 2, i, i - 1, i - 1, i - 2, i - 1, i, i - 1, i + 1};
+  const int tj[11] = {j, j + 1, j + 1, j + 1, j, j + 1, j - 1, j - 1, j - 1, j - 2, j - 1};
+  const int tk[11] = {1, 2, 3, 1, 2, 3, 4, 1, 2, 3, 4};
+  double w[11];
+  int c[11];
+#pragma unroll
+  for (int q = 0; q < 11; ++q) {
+    w[q] = oa(C, d, ti[q], tj[q], tk[q]);
+    c[q] = wn_code(C, d, ti[q], tj[q]);
+  }
+  const double hp = hv(Pa, d, ip, jp);
+  const int cp = wn_code(Pa, d, ip, jp);
+  const int at = nid(C, d, i, j);
+  for (int k = k0; k < k1; ++k)
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+      const double* sp = (v == 0 ? Pa.sm : Pa.st) + (int64_t)k * Pa.NN;
+      double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+      double sum = wn(wc, c[0]) * w[0];
+#pragma unroll
+      for (int q = 1; q < 11; ++q) sum = sum + wn(wc, c[q]) * w[q];
+      s[at] = wn(sp, cp) - sum * hp;
+    }
+}
+
+// Interp_outer_velo (src/wavelet.f90:1064-1094) of the outer child edge e of
+// parent (ip, jp): the nine weights and the parent edge codes of its terms.
+struct OuterInterp {
+  double w[9];
+  int c[13];  // t0, t1..t4, then the pairs of t5..t8
+};
+__device__ __forceinline__ void outer_interp(OuterInterp& O, const WLev& Pa, const WLev& C, int d, int ip, int jp,
+                                             int ic, int jc, int e) {
+  const int hs = c_hex_s_offs[e];
+  auto code = [&](const int* off, int col) {
+    return we_code(Pa, c_hex_sides[col][2], d, ip + off[0] + c_hex_sides[col][0], jp + off[1] + c_hex_sides[col][1]);
+  };
+  const int* e1 = c_end_pt[e][0];
+  const int* e2 = c_end_pt[e][1];
+  const int* o1 = c_opp_no[e][0];
+  const int* o2 = c_opp_no[e][1];
+  O.c[0] = we_code(Pa, e, d, ip, jp);
+  O.c[1] = code(e2, hs + 2);
+  O.c[2] = code(e1, hs + 3);
+  O.c[3] = code(e1, hs + 5);
+  O.c[4] = code(e2, hs + 0);
+  O.c[5] = code(o1, hs + 1);
+  O.c[6] = code(e1, hs + 2);
+  O.c[7] = code(e2, hs + 3);
+  O.c[8] = code(o1, hs + 4);
+  O.c[9] = code(o2, hs + 4);
+  O.c[10] = code(e2, hs + 5);
+  O.c[11] = code(e1, hs + 0);
+  O.c[12] = code(o2, hs + 1);
+#pragma unroll
+  for (int q = 0; q < 9; ++q) O.w[q] = c_iu_base[q] + iw(C, q, d, ic, jc);
+}
+__device__ __forceinline__ double outer_eval(const OuterInterp& O, const double* __restrict__ vp, double& t0) {
+  double t[9];
+  t[0] = we(vp, O.c[0]);
+  t[1] = we(vp, O.c[1]);
+  t[2] = we(vp, O.c[2]);
+  t[3] = we(vp, O.c[3]);
+  t[4] = we(vp, O.c[4]);
+  t[5] = we(vp, O.c[5]) - we(vp, O.c[6]);
+  t[6] = we(vp, O.c[7]) - we(vp, O.c[8]);
+  t[7] = we(vp, O.c[9]) - we(vp, O.c[10]);
+  t[8] = we(vp, O.c[11]) - we(vp, O.c[12]);
+  t0 = t[0];
+  double sum = 0.0;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) sum = sum + O.w[q] * t[q];
+  return sum;
+}
+
+// Compute_velo_wavelets' outer edges (src/wavelet.f90:672-710), parents
+// [0, np)^2, with the pentagon corrections of the corner parents.
+__global__ void __launch_bounds__(128) k_velo_wc_outer_l(WLev Pa, WLev C, int nz, int lpt) {
+  int d, ip, jp;
+  int k0, k1;
+  if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  const bool corner = (ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1);
+  for (int e = 0; e < 3; ++e) {
+    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
+    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
+    if (me(C, e, d, a2, b2) < ADJZONE) continue;
+    OuterInterp O;
+    outer_interp(O, Pa, C, d, ip, jp, a2, b2, e);
+    const int cv = we_code(C, e, d, a2, b2);
+    const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
+    for (int k = k0; k < k1; ++k) {
+      const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+      const double* v = C.sv + (int64_t)k * 3 * C.NN;
+      double* wc = C.wv + (int64_t)k * 3 * C.NN;
+      double t0;
+      const double u = outer_eval(O, vp, t0);
+      const double w = we(v, cv) - u;
+      wc[x2] = w;
+      wc[x1] = -w;
+    }
+  }
+  if (corner)
+    for (int k = k0; k < k1; ++k)
+      penta_compute(Pa, C, Pa.sv + (int64_t)k * 3 * Pa.NN, C.wv + (int64_t)k * 3 * C.NN, d, ip, jp);
+}
+
+// Reconstruct_outer_velo (src/wavelet.f90:954-976), parents [0, np]^2, then
+// Reconstruct_velo_penta by the corner parents.
+__global__ void __launch_bounds__(128) k_recon_outer_l(WLev Pa, WLev C, int nz, int lpt) {
+  int d, ip, jp;
+  int k0, k1;
+  if (!parent_of(Pa.n + 1, nz, lpt, d, ip, jp, k0, k1)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  for (int e = 0; e < 3; ++e) {
+    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
+    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
+    OuterInterp O;
+    outer_interp(O, Pa, C, d, ip, jp, a2, b2, e);
+    const int cw = we_code(C, e, d, a2, b2);
+    const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
+    for (int k = k0; k < k1; ++k) {
+      const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+      const double* wc = C.wv + (int64_t)k * 3 * C.NN;
+      double* v = C.sv + (int64_t)k * 3 * C.NN;
+      double t0;
+      const double u = outer_eval(O, vp, t0);
+      const double v2 = u + we(wc, cw);
+      v[x2] = v2;
+      v[x1] = 2.0 * t0 - v2;
+    }
+  }
+  if ((ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1))
+    for (int k = k0; k < k1; ++k)
+      penta_reconstruct(Pa, C, Pa.sv + (int64_t)k * 3 * Pa.NN, C.sv + (int64_t)k * 3 * C.NN, d, ip, jp);
+}
+
+// Interp_inner_velo (src/wavelet.f90:1005-1062) of parent (ip, jp): parent
+// circulation terms and the six inner child edges' coefficients.
+struct InnerInterp {
+  double lp[5], tp[2];     // parent lengths DG(ip,jp), UP(ip+1,jp), RT(ip,jp), UP(ip,jp), RT(ip,jp+1); areas
+  int cp[5];               // their codes
+  double lc[10];           // child lengths of the ten edges in the circulation terms
+  int cc[10];              // their codes
+  double tc[6], den[6];    // child triangle areas and the target edges' lengths
+  int ct[6], xt[6];        // target edges: codes and slots
+};
+__device__ __forceinline__ void inner_interp(InnerInterp& I, const WLev& Pa, const WLev& C, int d, int ip, int jp) {
+  const int pe[5] = {DG, UP, RT, UP, RT};
+  const int pi[5] = {ip, ip + 1, ip, ip, ip};
+  const int pj[5] = {jp, jp, jp, jp, jp + 1};
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    I.lp[q] = ln(Pa, pe[q], d, pi[q], pj[q]);
+    I.cp[q] = we_code(Pa, pe[q], d, pi[q], pj[q]);
+  }
+  I.tp[0] = ta(Pa, LORT, d, ip, jp);
+  I.tp[1] = ta(Pa, UPLT, d, ip, jp);
+  const int i = 2 * ip, j = 2 * jp;
+  // RT(i,j) DG(i,j) RT(i+1,j) UP(i+2,j) DG(i+1,j+1) UP(i+2,j+1) UP(i,j) UP(i,j+1) RT(i,j+2) RT(i+1,j+2)
+  const int ce[10] = {RT, DG, RT, UP, DG, UP, UP, UP, RT, RT};
+  const int ci[10] = {i, i, i + 1, i + 2, i + 1, i + 2, i, i, i, i + 1};
+  const int cj[10] = {j, j, j, j, j + 1, j + 1, j, j + 1, j + 2, j + 2};
+#pragma unroll
+  for (int q = 0; q < 10; ++q) {
+    I.lc[q] = ln(C, ce[q], d, ci[q], cj[q]);
+    I.cc[q] = we_code(C, ce[q], d, ci[q], cj[q]);
+  }
+  const int tt[6] = {LORT, LORT, LORT, UPLT, UPLT, UPLT};
+  const int ti[6] = {i, i + 1, i + 1, i, i, i + 1};
+  const int tj[6] = {j, j, j + 1, j, j + 1, j + 1};
+  // target edges UP(i+1,j) DG(i+1,j) RT(i+1,j+1) RT(i,j+1) DG(i,j+1) UP(i+1,j+1)
+  const int ge[6] = {UP, DG, RT, RT, DG, UP};
+  const int gi[6] = {i + 1, i + 1, i + 1, i, i, i + 1};
+  const int gj[6] = {j, j, j + 1, j + 1, j + 1, j + 1};
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    I.tc[q] = ta(C, tt[q], d, ti[q], tj[q]);
+    I.den[q] = ln(C, ge[q], d, gi[q], gj[q]);
+    I.ct[q] = we_code(C, ge[q], d, gi[q], gj[q]);
+    I.xt[q] = ge[q] * C.NN + nid(C, d, gi[q], gj[q]);
+  }
+}
+__device__ __forceinline__ void inner_eval(const InnerInterp& I, const double* __restrict__ vp,
+                                           const double* __restrict__ v, double u[6]) {
+  const double pDG = we(vp, I.cp[0]) * I.lp[0];
+  const double curl0 = (pDG + we(vp, I.cp[1]) * I.lp[1] + we(vp, I.cp[2]) * I.lp[2]) / I.tp[0];
+  const double curl1 = (pDG + we(vp, I.cp[3]) * I.lp[3] + we(vp, I.cp[4]) * I.lp[4]) / I.tp[1];
+  double pr[10];
+#pragma unroll
+  for (int q = 0; q < 10; ++q) pr[q] = we(v, I.cc[q]) * I.lc[q];
+  u[0] = (I.tc[0] * curl0 - pr[0] - pr[1]) / I.den[0];
+  u[1] = (I.tc[1] * curl0 - pr[2] - pr[3]) / I.den[1];
+  u[2] = (I.tc[2] * curl0 - pr[4] - pr[5]) / I.den[2];
+  u[3] = (I.tc[3] * curl1 - pr[6] - pr[1]) / I.den[3];
+  u[4] = (I.tc[4] * curl1 - pr[7] - pr[8]) / I.den[4];
+  u[5] = (I.tc[5] * curl1 - pr[4] - pr[9]) / I.den[5];
+}
+
+// Compute_velo_wavelets' inner edges (src/wavelet.f90:672-710), parents [0, np)^2.
+__global__ void __launch_bounds__(128) k_velo_wc_inner_l(WLev Pa, WLev C, int nz, int lpt) {
+  int d, ip, jp;
+  int k0, k1;
+  if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
+  const int i = 2 * ip, j = 2 * jp;
+  const int ge[6] = {UP, DG, RT, RT, DG, UP};
+  const int gi[6] = {i + 1, i + 1, i + 1, i, i, i + 1};
+  const int gj[6] = {j, j, j + 1, j + 1, j + 1, j + 1};
+  bool on[6];
+  bool any = false;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    on[q] = me(C, ge[q], d, gi[q], gj[q]) >= ADJZONE;
+    any = any || on[q];
+  }
+  if (!any) return;
+  InnerInterp I;
+  inner_interp(I, Pa, C, d, ip, jp);
+  for (int k = k0; k < k1; ++k) {
+    const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+    const double* v = C.sv + (int64_t)k * 3 * C.NN;
+    double* wc = C.wv + (int64_t)k * 3 * C.NN;
+    double u[6];
+    inner_eval(I, vp, v, u);
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      if (on[q]) wc[I.xt[q]] = we(v, I.ct[q]) - u[q];
+  }
+}
+
+// Reconstruct_inner_velo (src/wavelet.f90:978-1003), parents [0, np)^2.
+__global__ void __launch_bounds__(128) k_recon_inner_l(WLev Pa, WLev C, int nz, int lpt) {
+  int d, ip, jp;
+  int k0, k1;
+  if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
+  InnerInterp I;
+  inner_interp(I, Pa, C, d, ip, jp);
+  for (int k = k0; k < k1; ++k) {
+    const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+    const double* wc = C.wv + (int64_t)k * 3 * C.NN;
+    double* v = C.sv + (int64_t)k * 3 * C.NN;
+    double u[6];
+    inner_eval(I, vp, v, u);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) v[I.xt[q]] = u[q] + we(wc, I.ct[q]);
+  }
+}
+
+}  // namespace wtw

@@ -12,6 +12,7 @@
 #include "../../include/wavetrisk_gpu.h"
 #include "restrict_kernels.cuh"
 #include "wavelet_kernels.cuh"
+#include "wavelet_layers.cuh"
 #include "wt_handle.cuh"
 #include "wt_wavctx.cuh"
 
@@ -21,6 +22,16 @@ namespace {
 
 constexpr int TPB = 256;
 inline unsigned nb(int64_t n) { return (unsigned)((n + TPB - 1) / TPB); }
+constexpr int TPBL = 128;  // the layer-group kernels (wavelet_layers.cuh)
+int g_lpt_set = 0;         // layers per thread of those kernels (wt_tune); 0: by layer count
+// Measured on B200 (J5..J7 x 16 and J6..J8 x 32): 2 layers per thread up to
+// 16 layers, 4 beyond.
+inline int lpt_for(int nz) { return g_lpt_set > 0 ? g_lpt_set : (nz > 16 ? 4 : 2); }
+// blocks for n parents per layer group
+inline unsigned nbl(int64_t n, int nz) {
+  const int lpt = lpt_for(nz);
+  return (unsigned)((n * ((nz + lpt - 1) / lpt) + TPBL - 1) / TPBL);
+}
 
 int fail(const char* where, cudaError_t e) { return wt_handle_fail(where, e); }
 
@@ -102,13 +113,14 @@ void zero_wavelets(wt_handle* h) {
 // Scalar wavelets of level l+1 (Compute_scalar_wavelets over parents [0, n_l)).
 void launch_scalar_wc(wt_handle* h, int l) {
   const int np = h->at(l).n, nz = h->nz;
-  k_scalar_wc<<<nb((int64_t)nz * 10 * np * np), TPB, 0, h->stream>>>(view(h, l + 1), np, nz);
+  k_scalar_wc_l<<<nbl((int64_t)10 * np * np, nz), TPBL, 0, h->stream>>>(view(h, l + 1), np, nz, lpt_for(nz));
 }
 
 // Velocity wavelets of level l+1 (pentagon corrections included).
 void launch_velo_wc(wt_handle* h, int l) {
   const int np = h->at(l).n, nz = h->nz;
-  k_velo_wc<<<nb((int64_t)nz * 10 * np * np), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), nz);
+  k_velo_wc_outer_l<<<nbl((int64_t)10 * np * np, nz), TPBL, 0, h->stream>>>(view(h, l), view(h, l + 1), nz, lpt_for(nz));
+  k_velo_wc_inner_l<<<nbl((int64_t)10 * np * np, nz), TPBL, 0, h->stream>>>(view(h, l), view(h, l + 1), nz, lpt_for(nz));
 }
 
 // inverse_wavelet_transform (src/wavelet.f90:208-296) from level_start.
@@ -117,11 +129,11 @@ void inverse(wt_handle* h) {
   for (int l = h->level_start; l <= h->level_end - 1; ++l) {
     const int np = h->at(l).n;
     const WLev P = view(h, l), C = view(h, l + 1);
-    const int64_t par1 = (int64_t)nz * 10 * (np + 1) * (np + 1), par0 = (int64_t)nz * 10 * np * np;
-    k_prolong<<<nb(par1), TPB, 0, h->stream>>>(P, C, nz);
-    k_recon_outer<<<nb(par1), TPB, 0, h->stream>>>(P, C, nz);
-    k_recon_scalar<<<nb(par0), TPB, 0, h->stream>>>(C, np, nz);
-    k_recon_inner<<<nb(par0), TPB, 0, h->stream>>>(P, C, nz);
+    const int64_t par1 = (int64_t)10 * (np + 1) * (np + 1), par0 = (int64_t)10 * np * np;
+    k_prolong_l<<<nbl(par1, nz), TPBL, 0, h->stream>>>(P, C, nz, lpt_for(nz));
+    k_recon_outer_l<<<nbl(par1, nz), TPBL, 0, h->stream>>>(P, C, nz, lpt_for(nz));
+    k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, h->stream>>>(C, np, nz, lpt_for(nz));
+    k_recon_inner_l<<<nbl(par0, nz), TPBL, 0, h->stream>>>(P, C, nz, lpt_for(nz));
   }
 }
 
@@ -536,6 +548,19 @@ int wt_lnorm(wt_handle* h, int order, double* out) {
   cudaFree(dout);
   if (e != cudaSuccess) return fail("lnorm", e);
   return WT_OK;
+}
+
+// Launch-shape tuning of the wavelet kernels: WT_TUNE_WAVELET_LAYERS = layers
+// per thread of the layer-group kernels (1 .. 64; 0 restores the default
+// chosen from the layer count).  Process-wide.
+int wt_tune(wt_handle* h, int param, int value) {
+  (void)h;
+  if (param == WT_TUNE_WAVELET_LAYERS) {
+    if (value < 0 || value > 64) return WT_ERR_ARG;
+    g_lpt_set = value;
+    return WT_OK;
+  }
+  return WT_ERR_ARG;
 }
 
 }  // extern "C"

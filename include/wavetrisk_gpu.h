@@ -296,6 +296,11 @@ int wt_trend_multi(wt_handle* h);
  * state; the masks are held fixed.  The solution is the hierarchy's scaling
  * fields (level_end's is the stepper's state). */
 int wt_rk4_multi(wt_handle* h, double dt, int nsteps);
+/* nsteps adaptive time steps of the hierarchy (the reference's time_step,
+ * src/main.f90:405-444, explicit RK4, fixed thresholds): wt_rk4_multi(dt, 1),
+ * adapt's mask sequence with threshold[3][nz] (wt_mask_build without the
+ * child flags), wt_compress and wt_inverse_wt, replayed as one CUDA graph. */
+int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level_fill, int max_level, int nsteps);
 /* wt_rk4_multi with CUDA events around its phases (7 entries): ms[p] is the
  * mean duration of one occurrence of phase p and count[p] its occurrences per
  * step: 0 column+step1 of level_end, 1 column+step1 of a coarser level,

@@ -132,6 +132,7 @@ _DEVICE_SIGS = {
     "wt_step1_vort": [_vp, C.c_int, _dp],
     "wt_trend_multi": [_vp],
     "wt_rk4_multi": [_vp, C.c_double, C.c_int],
+    "wt_adaptive_step": [_vp, C.c_double, _dp, C.c_int, C.c_int, C.c_int],
     "wt_profile_rk4_multi": [_vp, C.c_double, C.c_int, _dp, C.POINTER(C.c_int)],
     "wt_lnorm": [_vp, C.c_int, _dp],
     "wt_tune": [_vp, C.c_int, C.c_int],

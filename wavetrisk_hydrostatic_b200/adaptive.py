@@ -73,10 +73,17 @@ class AdaptiveOcean:
         return req
 
     def step(self, dt: float) -> None:
-        """One time step: RK4 of the hierarchy, adapt, inverse transform."""
-        self.dev.rk4_multi(dt, 1)
-        self.adapt()
-        self.dev.inverse()
+        """One time step: RK4 of the hierarchy, adapt, inverse transform.  With
+        fixed thresholds the whole step is one graph replay on the device
+        (wt_adaptive_step); dynamic thresholds need cal_lnorm of the new state
+        on the host between the RK4 and the mask sequence."""
+        if not self.dynamic:
+            self.set_thresholds()
+            self.dev.adaptive_step(dt, self.threshold, self.level_fill, self.max_level)
+        else:
+            self.dev.rk4_multi(dt, 1)
+            self.adapt()
+            self.dev.inverse()
         self.istep += 1
 
     def masks(self):

@@ -98,5 +98,11 @@ void wt_level_masks(wt_handle* h, int level, const int** mask_n, const int** mas
 // WT_after_step on the given per-level scaling fields (level_start first), or on
 // the hierarchy's own when the arrays are null; stream-ordered (wt_wavelet.cu).
 int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v);
+// adapt's mask sequence without host synchronisation (capturable), compression
+// and inverse transform of the hierarchy, and the threshold upload (wt_wavelet.cu).
+int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq);
+void wt_level_compress(wt_handle* h);
+void wt_level_inverse(wt_handle* h);
+int wt_level_set_thresholds(wt_handle* h, const double* threshold);
 // The scaling fields (mass, Theta, velocity) of a level (wt_wavelet.cu).
 void wt_level_state(wt_handle* h, int level, double** m, double** t, double** v);

@@ -24,6 +24,10 @@ struct MLLevel {
 struct MLCtx {
   std::vector<MLLevel> L;
   std::vector<void*> allocs;
+  // graph of one adaptive step and the parameters it was captured with
+  cudaGraphExec_t step_graph = nullptr;
+  double g_dt = 0.0;
+  int g_fill = -1, g_max = -1;
 };
 
 #define CKM(x)                                            \
@@ -61,6 +65,7 @@ int ensure(wt_handle* h) {
 void wt_trend_ml_release(wt_handle* h) {
   if (!h || !h->ml) return;
   MLCtx* M = static_cast<MLCtx*>(h->ml);
+  if (M->step_graph) cudaGraphExecDestroy(M->step_graph);
   for (void* p : M->allocs) cudaFree(p);
   delete M;
   h->ml = nullptr;
@@ -232,6 +237,52 @@ int wt_rk4_multi(wt_handle* h, double dt, int nsteps) {
   if (!h->wav) return WT_ERR_STATE;
   if (int rc = ensure(h)) return rc;
   if (int rc = rk4_multi(h, dt, nsteps, nullptr)) return rc;
+  CKM(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
+  return WT_OK;
+}
+
+// One adaptive time step of the fully refined hierarchy, as the reference's
+// time_step (src/main.f90:405-444) with fixed thresholds: RK4 of the hierarchy
+// (trend_ml, RK_sub_step, WT_after_step per stage), adapt's mask sequence and
+// compression, and the inverse wavelet transform.  The ~330 launches of a step
+// are captured once into a CUDA graph (re-captured when dt, level_fill or
+// max_level change) and replayed; the thresholds are uploaded before each call.
+int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level_fill, int max_level, int nsteps) {
+  if (!h || !threshold || nsteps < 0) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure(h)) return rc;
+  MLCtx* M = static_cast<MLCtx*>(h->ml);
+  for (int l = h->level_start; l <= h->level_end; ++l) {  // allocate before any capture
+    double* p;
+    if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &p)) return rc;
+    if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &p)) return rc;
+  }
+  if (int rc = wt_level_set_thresholds(h, threshold)) return rc;
+  if (!M->step_graph || M->g_dt != dt || M->g_fill != level_fill || M->g_max != max_level) {
+    if (M->step_graph) {
+      cudaGraphExecDestroy(M->step_graph);
+      M->step_graph = nullptr;
+    }
+    cudaGraph_t g;
+    CKM(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = rk4_multi(h, dt, 1, nullptr);
+    if (!rc) rc = wt_level_mask_sequence(h, level_fill, max_level, 0, nullptr);
+    if (!rc) {
+      wt_level_compress(h);
+      wt_level_inverse(h);
+    }
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return wt_handle_fail("capture", e);
+    e = cudaGraphInstantiate(&M->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return wt_handle_fail("instantiate", e);
+    M->g_dt = dt;
+    M->g_fill = level_fill;
+    M->g_max = max_level;
+  }
+  for (int s = 0; s < nsteps; ++s) CKM(cudaGraphLaunch(M->step_graph, h->stream));
   CKM(cudaStreamSynchronize(h->stream));
   h->state_halo_done = false;
   return WT_OK;

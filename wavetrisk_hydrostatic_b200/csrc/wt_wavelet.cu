@@ -343,15 +343,17 @@ inline unsigned nodes_blocks(int m) { return nb((int64_t)10 * m * m); }
 }  // namespace
 
 // adapt (src/adapt.f90:14-65) without tree surgery, on the dense hierarchy.
-int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max_level, int patch_size,
-                  unsigned char* child_required) {
-  if (int rc = ready(h)) return rc;
+}  // extern "C"
+
+// adapt's mask sequence (src/adapt.f90:14-65) on the dense hierarchy, stream-
+// ordered and without host synchronisation (so that it can be captured in a
+// graph); the thresholds are already in the context's device buffer.  With
+// dreq non-null, check_child_required flags go there (patch_size > 0).
+int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq) {
   const int ls = h->level_start, le = h->level_end, nz = h->nz;
-  if (!threshold) return WT_ERR_ARG;
-  if (child_required && (patch_size < 2 || (patch_size & 1) || h->at(ls).n % patch_size)) return WT_ERR_ARG;
   WavCtx* W = ctx(h);
   cudaStream_t s = h->stream;
-  CKW(cudaMemcpyAsync(W->thr, threshold, 3 * nz * sizeof(double), cudaMemcpyHostToDevice, s));
+  const bool child_required = dreq != nullptr;
   for (int l = ls + 1; l <= le; ++l) k_mask_zero<<<nb(3 * h->at(l).NN), TPB, 0, s>>>(view(h, l));
   // mask_active
   auto tol = [&](int l, int st, int en) {
@@ -371,18 +373,12 @@ int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max
   for (int l = ls; l <= std::min(le, max_level - 1); ++l)
     k_mask_restrict_flux<<<nodes_blocks(h->at(l).n), TPB, 0, s>>>(view(h, l));
   comm_masks(h);
-  unsigned char* dreq = nullptr;
-  int64_t nreq = 0;
   if (child_required) {
-    for (int l = ls; l <= le - 1; ++l) nreq += (int64_t)10 * (h->at(l).n / patch_size) * (h->at(l).n / patch_size) * 4;
-    if (nreq > 0) {
-      CKW(cudaMalloc(&dreq, nreq));
-      int64_t o = 0;
-      for (int l = ls; l <= le - 1; ++l) {
-        const int64_t cnt = (int64_t)10 * (h->at(l).n / patch_size) * (h->at(l).n / patch_size) * 4;
-        k_child_required<<<nb(cnt), TPB, 0, s>>>(view(h, l), patch_size, dreq + o);
-        o += cnt;
-      }
+    int64_t o = 0;
+    for (int l = ls; l <= le - 1; ++l) {
+      const int64_t cnt = (int64_t)10 * (h->at(l).n / patch_size) * (h->at(l).n / patch_size) * 4;
+      k_child_required<<<nb(cnt), TPB, 0, s>>>(view(h, l), patch_size, dreq + o);
+      o += cnt;
     }
   }
   comm_masks(h);  // post_refine
@@ -410,10 +406,40 @@ int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max
   comm_masks(h);
   // mask_trsk
   for (int l = ls; l <= le; ++l) k_mask_trsk<<<nodes_blocks(h->at(l).n + 4), TPB, 0, s>>>(view(h, l));
+  CKW(cudaGetLastError());
+  return WT_OK;
+}
+
+void wt_level_compress(wt_handle* h) { compress(h); }
+void wt_level_inverse(wt_handle* h) { inverse(h); }
+int wt_level_set_thresholds(wt_handle* h, const double* threshold) {
+  CKW(cudaMemcpyAsync(ctx(h)->thr, threshold, 3 * h->nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  return WT_OK;
+}
+
+extern "C" {
+
+int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max_level, int patch_size,
+                  unsigned char* child_required) {
+  if (int rc = ready(h)) return rc;
+  const int ls = h->level_start, le = h->level_end, nz = h->nz;
+  if (!threshold) return WT_ERR_ARG;
+  if (child_required && (patch_size < 2 || (patch_size & 1) || h->at(ls).n % patch_size)) return WT_ERR_ARG;
+  WavCtx* W = ctx(h);
+  cudaStream_t s = h->stream;
+  CKW(cudaMemcpyAsync(W->thr, threshold, 3 * nz * sizeof(double), cudaMemcpyHostToDevice, s));
+  unsigned char* dreq = nullptr;
+  int64_t nreq = 0;
+  if (child_required) {
+    for (int l = ls; l <= le - 1; ++l) nreq += (int64_t)10 * (h->at(l).n / patch_size) * (h->at(l).n / patch_size) * 4;
+    if (nreq > 0) CKW(cudaMalloc(&dreq, nreq));
+  }
+  int rc = wt_level_mask_sequence(h, level_fill, max_level, patch_size, dreq);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e == cudaSuccess && dreq) e = cudaMemcpy(child_required, dreq, nreq, cudaMemcpyDeviceToHost);
   if (dreq) cudaFree(dreq);
+  if (rc) return rc;
   if (e != cudaSuccess) return fail("mask_build", e);
   return WT_OK;
 }

@@ -229,6 +229,14 @@ class WaveletHierarchy(DeviceGrid):
         """trend_ml over every level of the hierarchy (scaling fields, layer means and masks as uploaded)."""
         N.check("wt_trend_multi", N.lib().wt_trend_multi(self.h))
 
+    def adaptive_step(self, dt: float, threshold: np.ndarray, level_fill: int, max_level: int,
+                      nsteps: int = 1) -> None:
+        """nsteps adaptive time steps (RK4 of the hierarchy, adapt's masks and compression,
+        inverse transform) replayed as one CUDA graph per step."""
+        thr = _c(np.asarray(threshold).reshape(3, self.nz))
+        N.check("wt_adaptive_step", N.lib().wt_adaptive_step(self.h, float(dt), N.dptr(thr), int(level_fill),
+                                                             int(max_level), int(nsteps)))
+
     def lnorm(self, order: str = "inf") -> np.ndarray:
         """cal_lnorm of the scaling fields: (3, nz) for mass, Theta, velocity; order "inf", "1", "2" or "min"."""
         out = np.empty((3, self.nz))

@@ -158,3 +158,28 @@ def test_lnorm_matches_numpy(order):
     else:
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
     dev.close()
+
+
+def test_rk4_multi_tma_step1_matches_plain(monkeypatch):
+    """The finest level's step1 runs TMA-staged in the multi-level RK4 when the
+    handle selects it (J6 and up, or WAVETRISK_TREND_KERNEL=tma); the hierarchy
+    then steps to the same bits as with the L1 step1."""
+    ph = OceanParams()
+    lmin, lmax, nz = 3, 5, 2
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    states = [jet_state(g, nz, seed=2 + q, ph=ph) for q, g in enumerate(levels)]
+    outs = []
+    for variant in ("tma", "plain"):
+        monkeypatch.setenv("WAVETRISK_TREND_KERNEL", variant)
+        dev = WaveletHierarchy(levels, [st["topo"] for st in states], nz, ph)
+        for g, st in zip(levels, states):
+            for name in ("mass", "temp", "velo", "mean_m", "mean_t"):
+                dev.upload(g.level, name, st[name])
+        dev.rk4_multi(150.0, 2)
+        outs.append([[dev.download(g.level, name) for name in ("mass", "temp", "velo")] for g in levels])
+        assert dev.status() == 0
+        dev.close()
+    for a, b in zip(outs[0], outs[1]):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)

@@ -164,8 +164,9 @@ struct RChild {
   }
 };
 
-// flux_cpt_restr, one thread per restricted parent edge (e slowest, node
-// fastest), every layer and up to two fluxes (mass, Theta) per thread.  The
+// flux_cpt_restr, one thread per (group of lpt layers, restricted parent edge)
+// (group slowest, then e, node fastest), up to two fluxes (mass, Theta) per
+// thread.  The
 // ghost remaps, R_F_wgt, the overlap-area factors of part_coarse_flux and
 // coarse_flux and the small-flux weights depend only on the grid, so they are
 // resolved once per thread; the layer loop then evaluates the same expression
@@ -238,15 +239,20 @@ __device__ __forceinline__ void sm_make(SmTerm& t, const WLev& C, int d, int i, 
   }
 }
 
-__global__ void __launch_bounds__(256) k_restr_flux2(WLev P, WLev C, int nz, double* __restrict__ fp0,
+__global__ void __launch_bounds__(256) k_restr_flux2(WLev P, WLev C, int nz, int lpt, double* __restrict__ fp0,
                                                      double* __restrict__ fp1, const double* __restrict__ fc0,
                                                      const double* __restrict__ fc1, const double* __restrict__ dc0,
                                                      const double* __restrict__ dc1) {
   const int m = P.n;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)3 * 10 * m * m) return;
-  const int ip = (int)(t % m), jp = (int)((t / m) % m), d = (int)((t / ((int64_t)m * m)) % 10);
-  const int e = (int)(t / ((int64_t)10 * m * m));
+  const int64_t per = (int64_t)3 * 10 * m * m;  // parent edges per layer group
+  const int ng = (nz + lpt - 1) / lpt;
+  if (t >= per * ng) return;
+  const int g = (int)(t / per);
+  const int64_t u = t - (int64_t)g * per;
+  const int ip = (int)(u % m), jp = (int)((u / m) % m), d = (int)((u / ((int64_t)m * m)) % 10);
+  const int e = (int)(u / ((int64_t)10 * m * m));
+  const int k0 = g * lpt, k1 = min(nz, k0 + lpt);
   const int idp = nid(P, d, ip, jp);
   if (P.mask_e[e * P.NN + idp] < M_RESTRCT) return;
   const int ic = 2 * ip, jc = 2 * jp;
@@ -301,7 +307,7 @@ __global__ void __launch_bounds__(256) k_restr_flux2(WLev P, WLev C, int nz, dou
   const int nPP2 = ncode(C, d, ci + c_bfly_no2[e][2][0], cj + c_bfly_no2[e][2][1]);
   const int nMP2 = ncode(C, d, ci + c_bfly_no2[e][3][0], cj + c_bfly_no2[e][3][1]);
   const int64_t so = (int64_t)e * P.NN + idp;
-  for (int k = 0; k < nz; ++k) {
+  for (int k = k0; k < k1; ++k) {
 #pragma unroll
     for (int f = 0; f < 2; ++f) {
       double* __restrict__ fp = f == 0 ? fp0 : fp1;

@@ -49,7 +49,7 @@ static int dev_zero(double** dst, int64_t count) { return dev_copy(dst, nullptr,
 // Tensor maps of the trend inputs on the top level: dims (P, P, 10 lozenges,
 // planes), boxes of TB_X x TB_Y nodes.  The encoder is taken from the driver
 // through the runtime, so the library does not link libcuda directly.
-static int make_trend_maps(wt_handle* h) {
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -57,20 +57,45 @@ static int make_trend_maps(wt_handle* h) {
     cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
     if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) {
       std::fprintf(stderr, "wavetrisk_gpu: cuTensorMapEncodeTiled unavailable\n");
-      return WT_ERR_CUDA;
+      return nullptr;
     }
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
+  return encode;
+}
+
+// Tensor map of a top-level field of `planes` planes of NN doubles.
+static bool top_map(wt_handle* h, CUtensorMap* m, const double* base, int planes) {
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (!encode) return false;
   const DevLevel& D = h->top();
-  auto mk = [&](CUtensorMap* m, const double* base, int planes) {
-    const cuuint64_t dims[4] = {(cuuint64_t)D.P, (cuuint64_t)D.P, 10, (cuuint64_t)planes};
-    const cuuint64_t strides[3] = {(cuuint64_t)D.P * 8, (cuuint64_t)D.P * D.P * 8, (cuuint64_t)D.NN * 8};
-    const cuuint32_t box[4] = {(cuuint32_t)TB_X, (cuuint32_t)TB_Y, 1, 1};
-    const cuuint32_t elem[4] = {1, 1, 1, 1};
-    return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(base), dims, strides, box, elem,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-  };
+  const cuuint64_t dims[4] = {(cuuint64_t)D.P, (cuuint64_t)D.P, 10, (cuuint64_t)planes};
+  const cuuint64_t strides[3] = {(cuuint64_t)D.P * 8, (cuuint64_t)D.P * D.P * 8, (cuuint64_t)D.NN * 8};
+  const cuuint32_t box[4] = {(cuuint32_t)TB_X, (cuuint32_t)TB_Y, 1, 1};
+  const cuuint32_t elem[4] = {1, 1, 1, 1};
+  return encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(base), dims, strides, box, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The step1 input maps of a top-level state (m, t, v) with the top level's means and geometry.
+static bool step1_maps(wt_handle* h, const double* m, const double* t, const double* v, Step1Maps* S) {
+  const DevLevel& D = h->top();
+  const int nz = h->nz;
+  return top_map(h, &S->mass, m, nz) && top_map(h, &S->temp, t, nz) && top_map(h, &S->velo, v, 3 * nz) &&
+         top_map(h, &S->mean_m, h->mean_m, nz) && top_map(h, &S->mean_t, h->mean_t, nz) &&
+         top_map(h, &S->len, D.len, 3) && top_map(h, &S->ped, D.pedlen, 3) && top_map(h, &S->part, D.part, 6) &&
+         top_map(h, &S->cor, D.coriolis, 2);
+}
+
+int wt_make_step1_maps(wt_handle* h, const double* m, const double* t, const double* v, wtk::Step1Maps* out) {
+  if (h->trend_variant != 0) return WT_ERR_STATE;
+  return step1_maps(h, m, t, v, out) ? WT_OK : WT_ERR_CUDA;
+}
+
+static int make_trend_maps(wt_handle* h) {
+  const DevLevel& D = h->top();
+  auto mk = [&](CUtensorMap* m, const double* base, int planes) { return top_map(h, m, base, planes); };
   TrendMaps& M = h->maps;
   const int nz = h->nz;
   bool ok = mk(&M.hfm, h->hfm, 3 * nz) && mk(&M.hft, h->hft, 3 * nz) && mk(&M.qe, h->qe, 3 * nz) &&
@@ -79,12 +104,7 @@ static int make_trend_maps(wt_handle* h) {
   double* SM[3] = {h->mass, h->m1, h->m2};
   double* ST[3] = {h->temp, h->t1, h->t2};
   double* SV[3] = {h->velo, h->v1, h->v2};
-  for (int b = 0; b < 3 && ok; ++b) {
-    Step1Maps& S = h->s1maps[b];
-    ok = mk(&S.mass, SM[b], nz) && mk(&S.temp, ST[b], nz) && mk(&S.velo, SV[b], 3 * nz) && mk(&S.mean_m, h->mean_m, nz) &&
-         mk(&S.mean_t, h->mean_t, nz) && mk(&S.len, D.len, 3) && mk(&S.ped, D.pedlen, 3) && mk(&S.part, D.part, 6) &&
-         mk(&S.cor, D.coriolis, 2);
-  }
+  for (int b = 0; b < 3 && ok; ++b) ok = step1_maps(h, SM[b], ST[b], SV[b], &h->s1maps[b]);
   if (!ok) {
     std::fprintf(stderr, "wavetrisk_gpu: tensor map encoding failed\n");
     return WT_ERR_CUDA;
@@ -351,14 +371,21 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
 
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
-                   double* bern, double* theta) {
+                   double* bern, double* theta, const wtk::Step1Maps* maps) {
   const DevLevel& D = h->at(level);
   const LevelDev L = D.view();
   const int nz = h->nz;
   const unsigned chunks = blocks_for(D.NN, NODE_TILE);
   k_column<<<chunks, NODE_TILE, 0, h->stream>>>(L, h->ph, nz, m, t, mean_m, mean_t, phik, pterm);
   Step1Out so{qe, hfm, hft, bern, theta};
-  k_step1<<<chunks * nz, NODE_TILE, 0, h->stream>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so);
+  if (maps && level == h->level_end && h->trend_variant == 0) {
+    const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;
+    const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
+    k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, h->stream>>>(L, nz, nbx, nby, m, t, v, mean_m, phik, pterm, so,
+                                                                   h->dflag, *maps);
+  } else {
+    k_step1<<<chunks * nz, NODE_TILE, 0, h->stream>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so);
+  }
   CK(cudaGetLastError());
   return WT_OK;
 }

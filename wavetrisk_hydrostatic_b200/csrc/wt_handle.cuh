@@ -82,9 +82,13 @@ void wt_trend_ml_release(wt_handle* h);
 // Launchers shared between translation units (stream-ordered, no sync).
 // integrate_pressure_up + step1 (itype 0) + post_step1 of every layer of `level`
 // on the given state, into the given operator arrays (wt_api.cu).
+// With maps (the top level's step1 input maps of this state) the top level runs
+// the TMA-staged step1 when the handle selected it.
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
-                   double* bern, double* theta);
+                   double* bern, double* theta, const wtk::Step1Maps* maps);
+// The step1 input maps of a top-level state (WT_ERR_STATE when the handle runs the L1 kernels) (wt_api.cu).
+int wt_make_step1_maps(wt_handle* h, const double* m, const double* t, const double* v, wtk::Step1Maps* out);
 // scalar_cpt_restr / flux_cpt_restr of every layer from level+1 to `level`
 // with the masks of the hierarchy (wt_wavelet.cu).
 int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd);

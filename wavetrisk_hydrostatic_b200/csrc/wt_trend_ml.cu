@@ -24,6 +24,9 @@ struct MLLevel {
 struct MLCtx {
   std::vector<MLLevel> L;
   std::vector<void*> allocs;
+  // step1 input maps of the top level's RK stage state (TMA-staged step1)
+  wtk::Step1Maps q1maps{};
+  bool q1maps_ok = false;
   // graph of one adaptive step and the parameters it was captured with
   cudaGraphExec_t step_graph = nullptr;
   double g_dt = 0.0;
@@ -131,8 +134,20 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr) {
     if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
     if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
     PB(tm);
+    const wtk::Step1Maps* maps = nullptr;
+    if (l == h->level_end && h->trend_variant == 0) {
+      if (S.m[q] == h->mass && S.t[q] == h->temp && S.v[q] == h->velo) {
+        maps = &h->s1maps[0];
+      } else if (S.m[q] == V.m1 && S.t[q] == V.t1 && S.v[q] == V.v1) {
+        if (!M->q1maps_ok) {
+          if (int rc = wt_make_step1_maps(h, V.m1, V.t1, V.v1, &M->q1maps)) return rc;
+          M->q1maps_ok = true;
+        }
+        maps = &M->q1maps;
+      }
+    }
     if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern,
-                                V.theta))
+                                V.theta, maps))
       return rc;
     PE(tm, l == h->level_end ? PH_STEP1_TOP : PH_STEP1_COARSE);
     wtk::TrendML io{};

@@ -477,9 +477,10 @@ int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double*
 int wt_level_restrict_flux(wt_handle* h, int level, double* par0, double* par1, const double* chd0,
                            const double* chd1, const double* dsc0, const double* dsc1) {
   if (!h->at(level + 1).rf_wgt || !h->at(level + 1).overl_split) return WT_ERR_ARG;
-  const int m = h->at(level).n;
-  k_restr_flux2<<<nb((int64_t)3 * 10 * m * m), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz, par0,
-                                                                     par1, chd0, chd1, dsc0, dsc1);
+  const int m = h->at(level).n, lpt = lpt_for(h->nz);
+  const int64_t n = (int64_t)3 * 10 * m * m * ((h->nz + lpt - 1) / lpt);
+  k_restr_flux2<<<nb(n), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz, lpt, par0, par1, chd0, chd1,
+                                              dsc0, dsc1);
   CKW(cudaGetLastError());
   return WT_OK;
 }
@@ -513,9 +514,9 @@ int wt_restrict_flux(wt_handle* h, int level) {
   if (int rc = restrict_pair(h, level, {WT_WORK_FLUX, WT_WORK_DSCALAR})) return rc;
   if (!h->at(level + 1).rf_wgt || !h->at(level + 1).overl_split) return WT_ERR_ARG;
   const WLev P = view(h, level), C = view(h, level + 1);
-  const int m = h->at(level).n;
-  k_restr_flux2<<<nb((int64_t)3 * 10 * m * m), TPB, 0, h->stream>>>(P, C, h->nz, P.flux, nullptr, C.flux, nullptr,
-                                                                     C.dscal, nullptr);
+  const int m = h->at(level).n, lpt = lpt_for(h->nz);
+  const int64_t n = (int64_t)3 * 10 * m * m * ((h->nz + lpt - 1) / lpt);
+  k_restr_flux2<<<nb(n), TPB, 0, h->stream>>>(P, C, h->nz, lpt, P.flux, nullptr, C.flux, nullptr, C.dscal, nullptr);
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;

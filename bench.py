@@ -313,15 +313,18 @@ def adaptive_launches(L):
     return 4 * stage + masks + (L - 1) + 4 * (L - 1)
 
 
-def algorithmic_bytes_trend_ml(level, nz):
-    """Compulsory bytes of one k_trend_ml launch on a level: node-layers of
-    [0, n]^2 read theta, qe(3), hflux_mass(3), hflux_Theta(3), Bernoulli and Phi
-    (12 words) and write dmass, dTheta, dvelo(3) and the velocity source(3)
-    (8 words); geometry len(3), part(6), hex_inv and the node mask are read
-    once per node of [0, n]^2."""
+def algorithmic_bytes_trend_ml(level, nz, n_on=None, n_own=None):
+    """Compulsory bytes of one k_trend_ml launch on a level.  Every node of
+    [0, n]^2 reads its mask and writes dmass and dTheta (2 words a layer);
+    every owned node writes dvelo(3) and the velocity source(3); the n_on nodes
+    with mask_n >= TRSK also read theta, qe(3), hflux_mass(3), hflux_Theta(3),
+    Bernoulli and Phi (12 words a layer) and len(3), part(6), hex_inv once.
+    Without n_on every node counts as active."""
     n = 2 ** level
     inner = 10 * (n + 1) ** 2
-    return nz * inner * 20 * 8 + inner * (10 * 8 + 4)
+    own = 10 * n * n if n_own is None else n_own
+    on = inner if n_on is None else n_on
+    return nz * (inner * 2 * 8 + own * 6 * 8 + on * 12 * 8) + inner * 4 + on * 10 * 8
 
 
 def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile=True):
@@ -362,8 +365,12 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
     for g, (mn, me) in zip(levels, model.masks()):
         own = np.nonzero(g.owned)[0]
         e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+        ii = np.arange(g.n + 1)
+        I, J = np.meshgrid(ii, ii, indexing="xy")
+        inner = np.concatenate([((d * g.P + J + 2) * g.P + I + 2).ravel() for d in range(10)])
         act.append({"level": g.level, "active_nodes": int(np.count_nonzero(mn[own] >= 8)),
-                    "active_edges": int(np.count_nonzero(me[e] >= 8)), "edges": int(e.size)})
+                    "active_edges": int(np.count_nonzero(me[e] >= 8)), "edges": int(e.size),
+                    "trsk_nodes_0n": int(np.count_nonzero(mn[inner] >= 2))})
     out["masks"] = act
     if profile:
         pm = (Nt.C.c_double * 7)()
@@ -481,7 +488,7 @@ def bench_ours(args):
         share = {k: pm[k] * pc[k] for k in pm}
         tot = sum(share.values())
         dom = max(share, key=lambda k: share[k])
-        ab = algorithmic_bytes_trend_ml(args.level, args.nz)
+        ab = algorithmic_bytes_trend_ml(args.level, args.nz, n_on=r["masks"][-1]["trsk_nodes_0n"])
         ach = ab / (pm["trend_ml_top"] / 1e3) / 1e9
         traffic = None
         tf = os.path.join(ROOT, "profiles", "trend_ml_traffic.json")
@@ -514,6 +521,7 @@ def bench_ours(args):
             "gpu_launches": adaptive_launches(L) * args.steps,
             "roofline": {"bound": "hbm", "kernel": "k_trend_ml (level_end)", "achieved": ach, "peak": hbm,
                          "unit": "GB/s", "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": ab,
                          "dominant_phase_by_time": dom,
                          "phase_share": {k: v / tot for k, v in share.items()},
                          "phase_ms_per_occurrence": pm, "phase_count_per_step": pc},

@@ -300,31 +300,34 @@ def wavelet_case(lmin, lmax, nz, repeats=5, device=None):
 def adaptive_launches(L):
     """Kernels launched by one adaptive step of L levels (AdaptiveOcean.step
     with fixed thresholds, max_level = level_end): RK4 of the hierarchy (per
-    stage: column + step1 and k_trend_ml per level, three restrictions per
-    coarse level (Bernoulli, Exner, both fluxes), three RK sub-step kernels per
-    level, WT_after_step with three wavelet kernels per coarse level (scalar,
+    stage: column + step1 and k_trend_ml (with the RK sub-step) per level,
+    three restrictions per coarse level (Bernoulli, Exner, both fluxes),
+    WT_after_step with three wavelet kernels per coarse level (scalar,
     outer and inner velocity), one compression kernel per fine level
     and four inverse-transform kernels per coarse level), wt_mask_build's
     sweeps (comm_masks launches one kernel per level), compression and the
     inverse transform."""
-    stage = 3 * L + 3 * (L - 1) + 3 * L + 3 * (L - 1) + (L - 1) + 4 * (L - 1)
+    stage = 3 * L + 3 * (L - 1) + 3 * (L - 1) + (L - 1) + 4 * (L - 1)
     masks = ((L - 1) + 1 + L + (L - 1) * (L + 2) + L + L + L + (L - 1) + L + L + 2 * (L - 1) + L
              + (L - 2) * (2 + 2 * L) + (1 + L) + 2 * (L - 2) + 1 + L + L)
     return 4 * stage + masks + (L - 1) + 4 * (L - 1)
 
 
 def algorithmic_bytes_trend_ml(level, nz, n_on=None, n_own=None):
-    """Compulsory bytes of one k_trend_ml launch on a level.  Every node of
-    [0, n]^2 reads its mask and writes dmass and dTheta (2 words a layer);
-    every owned node writes dvelo(3) and the velocity source(3); the n_on nodes
-    with mask_n >= TRSK also read theta, qe(3), hflux_mass(3), hflux_Theta(3),
-    Bernoulli and Phi (12 words a layer) and len(3), part(6), hex_inv once.
-    Without n_on every node counts as active."""
+    """Compulsory bytes of one k_trend_ml launch on a level with the fused RK
+    sub-step.  Every node of [0, n]^2 reads its mask and writes dmass and dTheta
+    (2 words a layer); every owned node writes the velocity source (3); the
+    n_on nodes with mask_n >= TRSK also read theta, qe(3), hflux_mass(3),
+    hflux_Theta(3), Bernoulli and Phi (12 words a layer) and len(3), part(6),
+    hex_inv once; every padded node reads the RK base state and writes the stage
+    state (5 + 5 words a layer).  Without n_on every node counts as active."""
     n = 2 ** level
+    P = n + 4
+    NN = 10 * P * P
     inner = 10 * (n + 1) ** 2
     own = 10 * n * n if n_own is None else n_own
     on = inner if n_on is None else n_on
-    return nz * (inner * 2 * 8 + own * 6 * 8 + on * 12 * 8) + inner * 4 + on * 10 * 8
+    return nz * (inner * 2 * 8 + own * 3 * 8 + on * 12 * 8 + NN * 10 * 8) + inner * 4 + on * 10 * 8
 
 
 def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile=True):

@@ -304,8 +304,8 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
 /* wt_rk4_multi with CUDA events around its phases (7 entries): ms[p] is the
  * mean duration of one occurrence of phase p and count[p] its occurrences per
  * step: 0 column+step1 of level_end, 1 column+step1 of a coarser level,
- * 2 restrictions into a level, 3 k_trend_ml of level_end, 4 k_trend_ml of a
- * coarser level, 5 RK sub-step of the hierarchy, 6 WT_after_step. */
+ * 2 restrictions into a level, 3 k_trend_ml of level_end (with the fused RK
+ * sub-step), 4 the same on a coarser level, 5 unused, 6 WT_after_step. */
 int wt_profile_rk4_multi(wt_handle* h, double dt, int nsteps, double* ms, int* count);
 /* The trends of one level from the last wt_trend_multi: dmass, dtemp [nz][NN],
  * dvelo [nz][3*NN] host doubles (any may be NULL). */

@@ -122,8 +122,12 @@ States hierarchy_state(wt_handle* h) {
   return S;
 }
 
-// trend_ml of the state S into each level's dm, dt, dv (stream-ordered).
-int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr) {
+// trend_ml of the state S into each level's dm, dt, dv (stream-ordered).  With
+// base and dest, each level's k_trend_ml also takes the RK sub-step
+// dest = base + hs * trend (RK_sub_step, src/time_integr.f90:206-225) instead of
+// writing dv: a level's state is not read after its step1, so dest may be S.
+int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const States* base = nullptr,
+                const States* dest = nullptr, double hs = 0.0) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const int nz = h->nz;
   for (int l = h->level_end; l >= h->level_start; --l) {
@@ -170,33 +174,18 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr) {
     }
     io.theta = V.theta; io.qe = V.qe; io.hfm = V.hfm; io.hft = V.hft; io.bern = V.bern; io.phik = V.phik;
     io.dm = V.dm; io.dtt = V.dt; io.dv = V.dv; io.src = V.src;
+    if (base && dest) {
+      io.dv = nullptr;
+      io.base_m = base->m[q]; io.base_t = base->t[q]; io.base_v = base->v[q];
+      io.dst_m = dest->m[q]; io.dst_t = dest->t[q]; io.dst_v = dest->v[q];
+      io.h = hs;
+    }
     const unsigned chunks = (unsigned)((D.NN + wtk::NODE_TILE - 1) / wtk::NODE_TILE);
     PB(tm);
     wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
     PE(tm, l == h->level_end ? PH_TREND_TOP : PH_TREND_COARSE);
     CKM(cudaGetLastError());
   }
-  return WT_OK;
-}
-
-// RK_sub_step (src/time_integr.f90:206-225): dest = sol + hs * trend.
-__global__ void k_rk_sub(int64_t n, const double* __restrict__ sol, const double* __restrict__ trend, double hs,
-                         double* dest) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) dest[i] = sol[i] + hs * trend[i];
-}
-
-int rk_sub_step(wt_handle* h, const States& sol, const States& dest, double hs) {
-  MLCtx* M = static_cast<MLCtx*>(h->ml);
-  for (int l = h->level_start; l <= h->level_end; ++l) {
-    const int q = l - h->level_start;
-    const int64_t nn = (int64_t)h->nz * h->at(l).NN;
-    const unsigned nb1 = (unsigned)((nn + 255) / 256), nb3 = (unsigned)((3 * nn + 255) / 256);
-    k_rk_sub<<<nb1, 256, 0, h->stream>>>(nn, sol.m[q], M->L[q].dm, hs, dest.m[q]);
-    k_rk_sub<<<nb1, 256, 0, h->stream>>>(nn, sol.t[q], M->L[q].dt, hs, dest.t[q]);
-    k_rk_sub<<<nb3, 256, 0, h->stream>>>(3 * nn, sol.v[q], M->L[q].dv, hs, dest.v[q]);
-  }
-  CKM(cudaGetLastError());
   return WT_OK;
 }
 
@@ -230,10 +219,7 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm) {
     for (int stage = 0; stage < 4; ++stage) {
       const States& src = stage == 0 ? q : q1;
       const States& dest = stage == 3 ? q : q1;
-      if (int rc = trend_multi(h, src, tm)) return rc;
-      PB(tm);
-      if (int rc = rk_sub_step(h, q, dest, hs[stage])) return rc;
-      PE(tm, PH_RK_SUB);
+      if (int rc = trend_multi(h, src, tm, &q, &dest, hs[stage])) return rc;
       PB(tm);
       if (int rc = wt_level_after_step(h, dest.m.data(), dest.t.data(), dest.v.data())) return rc;
       PE(tm, PH_AFTER_STEP);
@@ -305,9 +291,9 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
 
 // wt_rk4_multi with CUDA events around its phases: ms[p] = mean time of one
 // occurrence of phase p (0 column+step1 of level_end, 1 column+step1 of one
-// coarser level, 2 restrictions into one level, 3 k_trend_ml of level_end,
-// 4 k_trend_ml of one coarser level, 5 RK sub-step of the hierarchy,
-// 6 WT_after_step); count[p] = occurrences per step.
+// coarser level, 2 restrictions into one level, 3 k_trend_ml of level_end with
+// the fused RK sub-step, 4 the same on one coarser level, 5 unused (the RK
+// sub-step is fused), 6 WT_after_step); count[p] = occurrences per step.
 int wt_profile_rk4_multi(wt_handle* h, double dt, int nsteps, double* ms, int* count) {
   if (!h || nsteps < 1 || !ms || !count) return WT_ERR_ARG;
   if (!h->wav) return WT_ERR_STATE;

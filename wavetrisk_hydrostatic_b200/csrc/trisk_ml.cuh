@@ -33,7 +33,7 @@ struct TrendML {
 
 constexpr int ML_TRSK = 2, ML_ADJZONE = 8;
 
-__global__ void __launch_bounds__(NODE_TILE, 3) k_trend_ml(LevelDev L, int nz, TrendML io) {
+__global__ void __launch_bounds__(NODE_TILE, 4) k_trend_ml(LevelDev L, int nz, TrendML io) {
   int k, id, i, j;
   if (!layer_node(L, nz, k, id, i, j)) return;
   const int P = L.P;

@@ -321,6 +321,19 @@ int wt_barotropic_upload(wt_handle* h, const double* eta, const double* div_old)
  * vertically summed mass flux of the resident state, and cal_div) and
  * rhs_elliptic (:151-185): rhs = -eta + dt (theta2 div + (1-theta2) div_old) / rho0. */
 int wt_rhs_elliptic(wt_handle* h, double dt, double theta2);
+/* The same pieces on every level of the hierarchy (after wt_wavelet_setup;
+ * coarser levels use the hierarchy's scaling fields, layer means and masks).
+ * wt_barotropic_upload_level sets a level's free surface and previous flux
+ * divergence (either may be NULL).  wt_rhs_elliptic_multi: flux_divergence
+ * over the hierarchy (src/barotropic_2d.f90:326-366) -- on coarser levels the
+ * flux is computed or restricted (cpt_or_restr_flux with the child's
+ * divergence) -- and rhs_elliptic on every level.  wt_u_update_multi: grad_eta
+ * over the hierarchy with cpt_or_restr_eta (:414-474) and u_update (:131-149)
+ * on every level. */
+int wt_barotropic_upload_level(wt_handle* h, int level, const double* eta, const double* div_old);
+int wt_rhs_elliptic_multi(wt_handle* h, double dt, double theta2);
+int wt_u_update_multi(wt_handle* h, double dt, double theta1);
+int wt_barotropic_download_level(wt_handle* h, int level, double* div_flux, double* rhs, double* grad);
 /* grad_eta (src/barotropic_2d.f90:455-474: step1 itype 3, g grad eta) and
  * u_update (:131-149): velo_k -= theta1 dt grad eta on every layer. */
 int wt_u_update(wt_handle* h, double dt, double theta1);

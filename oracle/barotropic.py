@@ -76,3 +76,53 @@ def step1_vort(g, velo):
     rc = L.orc_step1_vort(C.byref(lv.s), _p(tri), _p(_c(velo)), _p(vort))
     assert rc == 0
     return vort
+
+
+def _multi(levels, nz, states, masks, etas, div_olds):
+    from .restrict import orc_rlevel
+    i32 = C.POINTER(C.c_int32)
+
+    class orc_bml(C.Structure):
+        _fields_ = [("b", orc_blevel), ("r", orc_rlevel), ("mass", _dp), ("mean_m", _dp), ("velo", _dp),
+                    ("eta", _dp), ("div_old", _dp), ("div", _dp), ("rhs", _dp), ("grad", _dp)]
+
+    arr = (orc_bml * len(levels))()
+    keep, outs = [], []
+    for q, g in enumerate(levels):
+        lv = _Level(g)
+        rf = g.rf_wgt if (q > 0 and g.rf_wgt is not None) else np.zeros((3, g.NN))
+        geo = [_c(x) for x in (g.hex_inv, g.overl_a, g.overl_split, rf)]
+        hn = np.ascontiguousarray(g.halo_node, dtype=np.int64)
+        he = np.ascontiguousarray(g.halo_edge, dtype=np.int64)
+        mn, me = (np.ascontiguousarray(x, dtype=np.int32) for x in masks[q])
+        r = orc_rlevel(g.n, g.P, g.NN, *[_p(x) for x in geo], _p(hn, _ip), len(hn), _p(he, _ip), len(he),
+                       mn.ctypes.data_as(i32), me.ctypes.data_as(i32), None, None, None, None)
+        m, mm = _c(states[q]["mass"]), _c(states[q]["mean_m"])
+        v = _c(states[q]["velo"]).copy()
+        e, do = _c(etas[q]), _c(div_olds[q])
+        div, rhs, grad = np.zeros(g.NN), np.zeros(g.NN), np.zeros(3 * g.NN)
+        keep += [lv, geo, hn, he, mn, me, m, mm, v, e, do]
+        outs.append(dict(div=div, rhs=rhs, grad=grad, velo=v))
+        arr[q] = orc_bml(lv.s, r, _p(m), _p(mm), _p(v), _p(e), _p(do), _p(div), _p(rhs), _p(grad))
+    return arr, keep, outs
+
+
+def rhs_elliptic_multi(levels, nz, states, masks, etas, div_olds, dt, theta2, rho0):
+    """flux_divergence (with cpt_or_restr_flux) + rhs_elliptic over the hierarchy:
+    per level dict(div, rhs)."""
+    L = lib()
+    arr, keep, outs = _multi(levels, nz, states, masks, etas, div_olds)
+    L.orc_rhs_elliptic_multi.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+    L.orc_rhs_elliptic_multi.restype = C.c_int
+    assert L.orc_rhs_elliptic_multi(C.addressof(arr), len(levels), nz, dt, theta2, rho0) == 0
+    return outs
+
+
+def u_update_multi(levels, nz, states, masks, etas, grav, dt, theta1):
+    """grad_eta (with cpt_or_restr_eta) + u_update over the hierarchy: per level dict(grad, velo)."""
+    L = lib()
+    arr, keep, outs = _multi(levels, nz, states, masks, etas, [np.zeros(g.NN) for g in levels])
+    L.orc_u_update_multi.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+    L.orc_u_update_multi.restype = C.c_int
+    assert L.orc_u_update_multi(C.addressof(arr), len(levels), nz, grav, dt, theta1) == 0
+    return outs

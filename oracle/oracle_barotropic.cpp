@@ -14,6 +14,13 @@
 //   step1 itype 8 (comput :256-271, comp_SW :460-471) + post_vort :1159-1228
 //     in the reference's visiting order for a patch covering the lozenge:
 //     nodes [0, n)^2 row by row, the north row and (n, n), the east column.
+//   flux_divergence over a hierarchy, with cpt_or_restr_flux    src/barotropic_2d.f90:326-366
+//   rhs_elliptic over a hierarchy                               src/barotropic_2d.f90:151-185
+//   grad_eta over a hierarchy, with cpt_or_restr_eta            src/barotropic_2d.f90:414-474
+//   u_update over a hierarchy                                   src/barotropic_2d.f90:131-149
+// In grad_eta the restricted copy of eta is not ghost-copied again: the west
+// and south ghosts keep the values of the first update_bdry, the east and
+// north ghost rows (parents [0, n]) are restricted directly.
 // step1 visits nodes [0, n]^2 of each lozenge and runs comp_SW on the south
 // and west borders; update_bdry is the level's ghost copy.  u_update is
 // applied to the edges grad_eta writes (the reference's element range also
@@ -21,6 +28,8 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+
+#include "oracle_restrict.h"
 
 extern "C" {
 struct orc_blevel {
@@ -293,6 +302,161 @@ int orc_step1_vort(const orc_blevel* Lp, const double* triarea, const double* v_
       put(LORT, id, up(RT, id) - up(RT, idN) - up(UP, id));
       vort[UPLT * NN + id] = vort[LORT * NN + id];
     }
+  }
+  return 0;
+}
+
+// One level of a hierarchy for the barotropic pieces: the level record, the
+// compute-or-restrict record (masks, overlap areas, R_F_wgt) and the level's
+// fields.
+struct orc_bml {
+  orc_blevel b;
+  orc_rlevel r;                     // flux / dscal / scal / dvelo pointers unused
+  const double *mass, *mean_m;      // [nz][NN]
+  double* velo;                     // [nz][3*NN], updated by orc_u_update_multi
+  const double *eta, *div_old;      // [NN]
+  double *div, *rhs, *grad;         // out: [NN], [NN], [3*NN]
+};
+
+// flux_divergence + rhs_elliptic over levels lv[0..nlev-1] (level_start first).
+int orc_rhs_elliptic_multi(orc_bml* lv, int nlev, int nz, double dt, double theta2, double rho0) {
+  std::vector<std::vector<double>> flux(nlev);
+  for (int q = nlev - 1; q >= 0; --q) {
+    orc_bml& M = lv[q];
+    const orc_blevel& L = M.b;
+    B b{L};
+    const int64_t NN = L.NN;
+    const int P = L.P;
+    std::vector<double> m(M.mass, M.mass + nz * NN), v(M.velo, M.velo + 3 * nz * NN);
+    for (int k = 0; k < nz; ++k) {
+      b.halo_n(m.data() + k * NN);
+      b.halo_e(v.data() + 3 * k * NN);
+    }
+    flux[q].assign(3 * NN, 0.0);
+    double* hf = flux[q].data();
+    // step1 itype 4
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j <= L.n; ++j)
+        for (int i = 0; i <= L.n; ++i) {
+          const int64_t id = b.id(d, i, j);
+          const int64_t idE = id + 1, idN = id + P, idNE = id + P + 1, idW = id - 1, idS = id - P, idSW = id - P - 1;
+          double f[3] = {0.0, 0.0, 0.0};
+          for (int k = 0; k < nz; ++k) {
+            const double* Mm = m.data() + k * NN;
+            const double* A = M.mean_m + k * NN;
+            const double* V = v.data() + 3 * k * NN;
+            const double dz0 = Mm[id] + A[id];
+            double dz = interp(dz0, Mm[idE] + A[idE]);
+            f[RT] = f[RT] + V[RT * NN + id] * dz;
+            dz = interp(dz0, Mm[idNE] + A[idNE]);
+            f[DG] = f[DG] + V[DG * NN + id] * dz;
+            dz = interp(dz0, Mm[idN] + A[idN]);
+            f[UP] = f[UP] + V[UP * NN + id] * dz;
+          }
+          for (int e = 0; e < 3; ++e) hf[e * NN + id] = f[e] * L.pedlen[e * NN + id];
+          if (i == 0 || j == 0) {
+            double g[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k < nz; ++k) {
+              const double* Mm = m.data() + k * NN;
+              const double* A = M.mean_m + k * NN;
+              const double* V = v.data() + 3 * k * NN;
+              const double dz0 = Mm[id] + A[id];
+              double dz = interp(dz0, Mm[idW] + A[idW]);
+              g[0] = g[0] + V[RT * NN + idW] * dz;
+              dz = interp(dz0, Mm[idSW] + A[idSW]);
+              g[1] = g[1] + V[DG * NN + idSW] * dz;
+              dz = interp(dz0, Mm[idS] + A[idS]);
+              g[2] = g[2] + V[UP * NN + idS] * dz;
+            }
+            hf[RT * NN + idW] = g[0] * L.pedlen[RT * NN + idW];
+            hf[DG * NN + idSW] = g[1] * L.pedlen[DG * NN + idSW];
+            hf[UP * NN + idS] = g[2] * L.pedlen[UP * NN + idS];
+          }
+        }
+    if (q < nlev - 1) {  // cpt_or_restr_flux with dscalar => div_flux of the child
+      orc_rlevel Pr = M.r, Cr = lv[q + 1].r;
+      Pr.flux = hf;
+      Cr.flux = flux[q + 1].data();
+      Cr.dscal = lv[q + 1].div;
+      orc_restrict_flux(&Pr, &Cr, 1);
+    }
+    b.halo_e(hf);
+    std::memset(M.div, 0, NN * sizeof(double));
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j <= L.n; ++j)
+        for (int i = 0; i <= L.n; ++i) {
+          const int64_t id = b.id(d, i, j);
+          M.div[id] = (hf[RT * NN + id] - hf[RT * NN + id - 1] + hf[DG * NN + id - P - 1] - hf[DG * NN + id] +
+                       hf[UP * NN + id] - hf[UP * NN + id - P]) *
+                      L.hex_inv[id];
+        }
+    b.halo_n(M.div);
+  }
+  for (int q = nlev - 1; q >= 0; --q) {  // cal_rhs_elliptic on every level
+    orc_bml& M = lv[q];
+    const orc_blevel& L = M.b;
+    B b{L};
+    const int64_t NN = L.NN;
+    std::vector<double> e(M.eta, M.eta + NN), dold(M.div_old, M.div_old + NN);
+    b.halo_n(e.data());
+    b.halo_n(dold.data());
+    std::memset(M.rhs, 0, NN * sizeof(double));
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j <= L.n; ++j)
+        for (int i = 0; i <= L.n; ++i) {
+          const int64_t id = b.id(d, i, j);
+          M.rhs[id] = -e[id] + dt * (theta2 * M.div[id] + (1.0 - theta2) * dold[id]) / rho0;
+        }
+  }
+  return 0;
+}
+
+// grad_eta + u_update over the hierarchy.
+int orc_u_update_multi(orc_bml* lv, int nlev, int nz, double grav, double dt, double theta1) {
+  constexpr int RESTRCT = 12;
+  std::vector<std::vector<double>> ew(nlev);
+  for (int q = 0; q < nlev; ++q) {  // update_bdry(sol(S_MASS, zlevels+1)); copy to the work field
+    B b{lv[q].b};
+    ew[q].assign(lv[q].eta, lv[q].eta + lv[q].b.NN);
+    b.halo_n(ew[q].data());
+  }
+  for (int q = nlev - 1; q >= 0; --q) {
+    orc_bml& M = lv[q];
+    const orc_blevel& L = M.b;
+    B b{L};
+    const int64_t NN = L.NN;
+    const int P = L.P;
+    double* e = ew[q].data();
+    if (q < nlev - 1) {  // cpt_or_restr_eta: parents [0, n]^2 with mask_n >= RESTRCT
+      const orc_blevel& Lc = lv[q + 1].b;
+      B bc{Lc};
+      for (int d = 0; d < 10; ++d)
+        for (int jp = 0; jp <= L.n; ++jp)
+          for (int ip = 0; ip <= L.n; ++ip)
+            if (M.r.mask_n[b.id(d, ip, jp)] >= RESTRCT) e[b.id(d, ip, jp)] = ew[q + 1][bc.id(d, 2 * ip, 2 * jp)];
+    }
+    std::memset(M.grad, 0, 3 * NN * sizeof(double));
+    std::vector<char> written(3 * NN, 0);
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j <= L.n; ++j)
+        for (int i = 0; i <= L.n; ++i) {
+          const int64_t id = b.id(d, i, j);
+          double* g = M.grad;
+          g[RT * NN + id] = grav * (e[id + 1] / 1.0 - e[id] / 1.0) / L.len[RT * NN + id];
+          g[DG * NN + id] = grav * (e[id] / 1.0 - e[id + P + 1] / 1.0) / L.len[DG * NN + id];
+          g[UP * NN + id] = grav * (e[id + P] / 1.0 - e[id] / 1.0) / L.len[UP * NN + id];
+          written[RT * NN + id] = written[DG * NN + id] = written[UP * NN + id] = 1;
+          if (i == 0 || j == 0) {
+            g[RT * NN + id - 1] = -(grav * (e[id - 1] / 1.0 - e[id] / 1.0) / L.len[RT * NN + id - 1]);
+            g[DG * NN + id - P - 1] = -(grav * (e[id] / 1.0 - e[id - P - 1] / 1.0) / L.len[DG * NN + id - P - 1]);
+            g[UP * NN + id - P] = -(grav * (e[id - P] / 1.0 - e[id] / 1.0) / L.len[UP * NN + id - P]);
+            written[RT * NN + id - 1] = written[DG * NN + id - P - 1] = written[UP * NN + id - P] = 1;
+          }
+        }
+    const double s = theta1 * dt;
+    for (int k = 0; k < nz; ++k)
+      for (int64_t x = 0; x < 3 * NN; ++x)
+        if (written[x]) M.velo[3 * k * NN + x] = M.velo[3 * k * NN + x] - s * M.grad[x];
   }
   return 0;
 }

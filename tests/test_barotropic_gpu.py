@@ -89,3 +89,59 @@ def test_step1_vorticity_matches_oracle_exactly(level):
         assert np.count_nonzero(ov) > 0
         assert np.array_equal(v, ov), (k, np.abs(v - ov).max())
     model.close()
+
+
+@pytest.mark.parametrize("masks_kind", ["tolrnz", "built"])
+def test_barotropic_pieces_on_the_hierarchy_match_oracle(masks_kind):
+    """flux_divergence with cpt_or_restr_flux, rhs_elliptic, grad_eta with
+    cpt_or_restr_eta and u_update on every level of a J3..J5 hierarchy."""
+    from oracle.wavelet import Hierarchy
+    from wavetrisk_hydrostatic_b200.model import WaveletHierarchy
+
+    lmin, lmax, nz, dt = 3, 5, 2, 300.0
+    ph = OceanParams()
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    states = [jet_state(g, nz, seed=7 + q, ph=ph) for q, g in enumerate(levels)]
+    rng = np.random.default_rng(5)
+    etas, dolds = [], []
+    for g in levels:
+        e, d = rng.standard_normal(g.NN) * 0.1, rng.standard_normal(g.NN) * 1e-6
+        halo_nodes(g, e)
+        halo_nodes(g, d)
+        etas.append(e)
+        dolds.append(d)
+    if masks_kind == "built":
+        H = Hierarchy(levels, nz)
+        for name, key in (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v")):
+            H.set(lmax, key, states[-1][name])
+        H.forward()
+        H.mask_build(np.array([[5.0] * nz, [1e16] * nz, [0.05] * nz]), 0, lmax)
+        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in levels]
+        assert np.count_nonzero(masks[1][0] >= 12) < np.count_nonzero(levels[1].owned)
+    else:
+        masks = [(np.full(g.NN, 16, np.int32), np.full(3 * g.NN, 16, np.int32)) for g in levels]
+    dev = WaveletHierarchy(levels, [st["topo"] for st in states], nz, ph)
+    for g, st, (mn, me), e, d in zip(levels, states, masks, etas, dolds):
+        for name in ("mass", "temp", "velo", "mean_m", "mean_t"):
+            dev.upload(g.level, name, st[name])
+        dev.upload(g.level, "mask_n", mn)
+        dev.upload(g.level, "mask_e", me)
+        dev.barotropic_upload(g.level, e, d)
+    ro = ob.rhs_elliptic_multi(levels, nz, states, masks, etas, dolds, dt, 0.75, ph.ref_density)
+    dev.rhs_elliptic_multi(dt, 0.75)
+    uo = ob.u_update_multi(levels, nz, states, masks, etas, ph.grav, dt, 0.6)
+    dev.u_update_multi(dt, 0.6)
+    for q, g in enumerate(levels):
+        div, rhs, grad = dev.barotropic_download(g.level)
+        own = np.nonzero(g.owned)[0]
+        e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+        assert rel(div[own], ro[q]["div"][own]) <= TOL, (g.level, "div")
+        assert rel(rhs[own], ro[q]["rhs"][own]) <= TOL, (g.level, "rhs")
+        assert rel(grad[e], uo[q]["grad"][e]) <= TOL, (g.level, "grad")
+        v = dev.download(g.level, "velo")
+        ov = uo[q]["velo"].copy()
+        halo_edges(g, ov)
+        assert rel(v[:, e], ov[:, e]) <= TOL, (g.level, "velo")
+    assert dev.status() == 0
+    dev.close()

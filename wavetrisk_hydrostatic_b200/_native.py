@@ -130,6 +130,10 @@ _DEVICE_SIGS = {
     "wt_mask_build": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p],
     "wt_wt_after_step": [_vp],
     "wt_step1_vort": [_vp, C.c_int, _dp],
+    "wt_barotropic_upload_level": [_vp, C.c_int, _dp, _dp],
+    "wt_rhs_elliptic_multi": [_vp, C.c_double, C.c_double],
+    "wt_u_update_multi": [_vp, C.c_double, C.c_double],
+    "wt_barotropic_download_level": [_vp, C.c_int, _dp, _dp, _dp],
     "wt_trend_multi": [_vp],
     "wt_rk4_multi": [_vp, C.c_double, C.c_int],
     "wt_adaptive_step": [_vp, C.c_double, _dp, C.c_int, C.c_int, C.c_int],

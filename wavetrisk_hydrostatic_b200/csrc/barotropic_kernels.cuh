@@ -79,6 +79,12 @@ __global__ void k_flux_sum(LevelDev L, int nz, const double* __restrict__ mass, 
   }
 }
 
+// Ghost copy of one node field of a level (update_bdry): dst = src per entry.
+__global__ void k_halo_nodes(const int2* __restrict__ hn, int n_hn, double* f) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n_hn) f[hn[q].x] = f[hn[q].y];
+}
+
 // cal_div (src/ops.f90:1325-1355) at nodes [0, n]^2:
 //   div = hex_inv * (F_RT - F_RT,W + F_DG,SW - F_DG + F_UP - F_UP,S)
 __global__ void k_div(LevelDev L, const double* __restrict__ hflux, double* __restrict__ div) {
@@ -112,6 +118,9 @@ __global__ void k_rhs(LevelDev L, const double* __restrict__ div, const double* 
 // step1 itype 3 (src/ops.f90:225-228, comp_SW :416-419) with porosity 1,
 // h_flux = g (eta_far - eta_near) / len, and u_update
 // (src/barotropic_2d.f90:131-149): velo_k -= theta1 dt h_flux on every layer.
+// With DIRECT, eta is read where it is stored (ghosts included): the copy that
+// grad_eta restricts on coarser levels is not ghost-copied again.
+template <bool DIRECT = false>
 __global__ void k_grad_eta_update(LevelDev L, int nz, double grav, const double* __restrict__ eta, double scale,
                                   double* __restrict__ grad, double* __restrict__ velo) {
   const int m = L.n + 1;
@@ -120,7 +129,7 @@ __global__ void k_grad_eta_update(LevelDev L, int nz, double grav, const double*
   const int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
   const int P = L.P, NN = L.NN;
   const int id = (d * P + j + 2) * P + i + 2;
-  const Rd R(L, i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2);
+  const Rd R(L, DIRECT || (i >= 1 && j >= 1 && i <= L.n - 2 && j <= L.n - 2));
   const double e0 = R.n(eta, id) / 1.0;
   int slot[6];
   double g[6];

@@ -3,6 +3,8 @@
 // (src/barotropic_2d.f90:118-185, 326-366, 131-149, 455-474).
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "../../include/wavetrisk_gpu.h"
 #include "barotropic_kernels.cuh"
 #include "wt_handle.cuh"
@@ -12,8 +14,16 @@ namespace {
 constexpr int TPB = 256;
 inline unsigned nb(int64_t n) { return (unsigned)((n + TPB - 1) / TPB); }
 
+// Free-surface fields of one level of the hierarchy.
+struct BaroLevel {
+  double *eta = nullptr, *eta_w = nullptr, *div_old = nullptr, *div = nullptr, *rhs = nullptr, *flux = nullptr,
+         *grad = nullptr;
+};
+
 struct BaroCtx {
   double *eta = nullptr, *div_old = nullptr, *div = nullptr, *rhs = nullptr, *flux = nullptr, *grad = nullptr;
+  std::vector<BaroLevel> L;  // every level, on first use of the hierarchy entry points
+  std::vector<void*> allocs;
 };
 
 #define CKB(x)                                             \
@@ -39,6 +49,43 @@ int ensure(wt_handle* h) {
   return WT_OK;
 }
 
+// Per-level free-surface fields of the hierarchy (zeroed on first use).
+int ensure_levels(wt_handle* h) {
+  if (int rc = ensure(h)) return rc;
+  BaroCtx* B = static_cast<BaroCtx*>(h->baro);
+  if (!B->L.empty()) return WT_OK;
+  B->L.resize(h->level_end - h->level_start + 1);
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    BaroLevel& V = B->L[l - h->level_start];
+    const size_t NN = (size_t)h->at(l).NN;
+    double** node[] = {&V.eta, &V.eta_w, &V.div_old, &V.div, &V.rhs};
+    for (double** p : node) {
+      CKB(cudaMalloc(p, NN * 8));
+      B->allocs.push_back(*p);
+      CKB(cudaMemsetAsync(*p, 0, NN * 8, h->stream));
+    }
+    double** edge[] = {&V.flux, &V.grad};
+    for (double** p : edge) {
+      CKB(cudaMalloc(p, 3 * NN * 8));
+      B->allocs.push_back(*p);
+      CKB(cudaMemsetAsync(*p, 0, 3 * NN * 8, h->stream));
+    }
+  }
+  return WT_OK;
+}
+
+// State (mass, velocity) and mean mass of a level.
+void level_state(wt_handle* h, int l, double** m, double** v, double** mm) {
+  double* t;
+  if (l == h->level_end) {
+    *m = h->mass;
+    *v = h->velo;
+  } else {
+    wt_level_state(h, l, m, &t, v);
+  }
+  wt_level_mean(h, l, WT_FIELD_MEAN_MASS, mm);
+}
+
 }  // namespace
 
 void wt_barotropic_release(wt_handle* h) {
@@ -47,6 +94,7 @@ void wt_barotropic_release(wt_handle* h) {
   double* a[] = {B->eta, B->div_old, B->div, B->rhs, B->flux, B->grad};
   for (double* p : a)
     if (p) cudaFree(p);
+  for (void* p : B->allocs) cudaFree(p);
   delete B;
   h->baro = nullptr;
 }
@@ -86,7 +134,7 @@ int wt_u_update(wt_handle* h, double dt, double theta1) {
   BaroCtx* B = static_cast<BaroCtx*>(h->baro);
   const DevLevel& D = h->top();
   const int m = D.n + 1;
-  wtb::k_grad_eta_update<<<nb(10 * m * m), TPB, 0, h->stream>>>(D.view(), h->nz, h->ph.grav, B->eta, theta1 * dt,
+  wtb::k_grad_eta_update<false><<<nb(10 * m * m), TPB, 0, h->stream>>>(D.view(), h->nz, h->ph.grav, B->eta, theta1 * dt,
                                                                  B->grad, h->velo);
   CKB(cudaGetLastError());
   CKB(cudaStreamSynchronize(h->stream));
@@ -133,6 +181,92 @@ int wt_step1_vort(wt_handle* h, int layer, double* vort) {
   wtb::k_step1_vort<<<nb(10 * m * m), TPB, 0, h->stream>>>(D.view(), h->velo + 3 * (int64_t)layer * D.NN, B->grad);
   CKB(cudaGetLastError());
   CKB(cudaMemcpyAsync(vort, B->grad, 2 * NN * 8, cudaMemcpyDeviceToHost, h->stream));
+  CKB(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_barotropic_upload_level(wt_handle* h, int level, const double* eta, const double* div_old) {
+  if (!h || level < h->level_start || level > h->level_end) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure_levels(h)) return rc;
+  BaroLevel& V = static_cast<BaroCtx*>(h->baro)->L[level - h->level_start];
+  const size_t NN = (size_t)h->at(level).NN;
+  if (eta) CKB(cudaMemcpyAsync(V.eta, eta, NN * 8, cudaMemcpyHostToDevice, h->stream));
+  if (div_old) CKB(cudaMemcpyAsync(V.div_old, div_old, NN * 8, cudaMemcpyHostToDevice, h->stream));
+  CKB(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+// flux_divergence over the hierarchy (src/barotropic_2d.f90:326-366): per level
+// from level_end down, the vertically summed mass flux, on coarser levels the
+// compute-or-restrict of that flux with the child's divergence as dscalar
+// (cpt_or_restr_flux), and the divergence; then rhs_elliptic on every level.
+int wt_rhs_elliptic_multi(wt_handle* h, double dt, double theta2) {
+  if (!h) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure_levels(h)) return rc;
+  BaroCtx* B = static_cast<BaroCtx*>(h->baro);
+  for (int l = h->level_end; l >= h->level_start; --l) {
+    BaroLevel& V = B->L[l - h->level_start];
+    const DevLevel& D = h->at(l);
+    const wtk::LevelDev L = D.view();
+    const int m = D.n + 1;
+    double *ms, *v, *mm;
+    level_state(h, l, &ms, &v, &mm);
+    wtb::k_flux_sum<<<nb(10 * m * m), TPB, 0, h->stream>>>(L, h->nz, ms, mm, v, V.flux);
+    if (l < h->level_end) {
+      BaroLevel& C = B->L[l + 1 - h->level_start];
+      if (int rc = wt_level_restrict_flux(h, l, V.flux, nullptr, C.flux, nullptr, C.div, nullptr, 1)) return rc;
+    }
+    wtb::k_div<<<nb(10 * m * m), TPB, 0, h->stream>>>(L, V.flux, V.div);
+    wtb::k_rhs<<<nb(10 * m * m), TPB, 0, h->stream>>>(L, V.div, V.eta, V.div_old, dt, theta2, h->ph.ref_density,
+                                                       V.rhs);
+  }
+  CKB(cudaGetLastError());
+  CKB(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+// grad_eta over the hierarchy (src/barotropic_2d.f90:455-474) with
+// cpt_or_restr_eta (:414-453), and u_update (:131-149) on every level.  The
+// free surface is ghost-copied once into a work copy; coarser levels restrict
+// that copy (parents [0, n]^2 with mask_n >= RESTRCT) and read it as stored.
+int wt_u_update_multi(wt_handle* h, double dt, double theta1) {
+  if (!h) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure_levels(h)) return rc;
+  BaroCtx* B = static_cast<BaroCtx*>(h->baro);
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    BaroLevel& V = B->L[l - h->level_start];
+    const DevLevel& D = h->at(l);
+    CKB(cudaMemcpyAsync(V.eta_w, V.eta, (size_t)D.NN * 8, cudaMemcpyDeviceToDevice, h->stream));
+    if (D.n_hn > 0) wtb::k_halo_nodes<<<nb(D.n_hn), TPB, 0, h->stream>>>(D.hn, D.n_hn, V.eta_w);
+  }
+  for (int l = h->level_end; l >= h->level_start; --l) {
+    BaroLevel& V = B->L[l - h->level_start];
+    const DevLevel& D = h->at(l);
+    const int m = D.n + 1;
+    if (l < h->level_end)
+      if (int rc = wt_level_restrict_scalar(h, l, V.eta_w, B->L[l + 1 - h->level_start].eta_w, 1)) return rc;
+    double *ms, *v, *mm;
+    level_state(h, l, &ms, &v, &mm);
+    wtb::k_grad_eta_update<true><<<nb(10 * m * m), TPB, 0, h->stream>>>(D.view(), h->nz, h->ph.grav, V.eta_w,
+                                                                       theta1 * dt, V.grad, v);
+  }
+  CKB(cudaGetLastError());
+  CKB(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
+  return WT_OK;
+}
+
+int wt_barotropic_download_level(wt_handle* h, int level, double* div_flux, double* rhs, double* grad) {
+  if (!h || level < h->level_start || level > h->level_end) return WT_ERR_ARG;
+  if (!h->baro || static_cast<BaroCtx*>(h->baro)->L.empty()) return WT_ERR_STATE;
+  BaroLevel& V = static_cast<BaroCtx*>(h->baro)->L[level - h->level_start];
+  const size_t NN = (size_t)h->at(level).NN;
+  if (div_flux) CKB(cudaMemcpyAsync(div_flux, V.div, NN * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (rhs) CKB(cudaMemcpyAsync(rhs, V.rhs, NN * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (grad) CKB(cudaMemcpyAsync(grad, V.grad, 3 * NN * 8, cudaMemcpyDeviceToHost, h->stream));
   CKB(cudaStreamSynchronize(h->stream));
   return WT_OK;
 }

@@ -89,12 +89,12 @@ int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, co
                    double* bern, double* theta, const wtk::Step1Maps* maps);
 // The step1 input maps of a top-level state (WT_ERR_STATE when the handle runs the L1 kernels) (wt_api.cu).
 int wt_make_step1_maps(wt_handle* h, const double* m, const double* t, const double* v, wtk::Step1Maps* out);
-// scalar_cpt_restr / flux_cpt_restr of every layer from level+1 to `level`
-// with the masks of the hierarchy (wt_wavelet.cu).
-int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd);
+// scalar_cpt_restr / flux_cpt_restr of the nz layers of the given fields from
+// level+1 to `level` with the masks of the hierarchy (wt_wavelet.cu).
+int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd, int nz);
 // flux_cpt_restr of two fluxes (par1/chd1/dsc1 may be null) in one launch.
 int wt_level_restrict_flux(wt_handle* h, int level, double* par0, double* par1, const double* chd0,
-                           const double* chd1, const double* dsc0, const double* dsc1);
+                           const double* chd1, const double* dsc0, const double* dsc1, int nz);
 // The layer mean WT_FIELD_MEAN_MASS/TEMP of a level (wt_wavelet.cu).
 int wt_level_mean(wt_handle* h, int level, int field, double** out);
 // The masks of a level, or null before wt_wavelet_setup (wt_wavelet.cu).

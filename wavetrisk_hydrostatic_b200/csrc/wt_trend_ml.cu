@@ -161,9 +161,9 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
     if (l < h->level_end) {
       MLLevel& C = M->L[q + 1];
       PB(tm);
-      if (int rc = wt_level_restrict_scalar(h, l, V.bern, C.bern)) return rc;
-      if (int rc = wt_level_restrict_scalar(h, l, V.phik, C.phik)) return rc;  // exner = -Phi_k
-      if (int rc = wt_level_restrict_flux(h, l, V.hfm, V.hft, C.hfm, C.hft, C.dm, C.dt)) return rc;
+      if (int rc = wt_level_restrict_scalar(h, l, V.bern, C.bern, nz)) return rc;
+      if (int rc = wt_level_restrict_scalar(h, l, V.phik, C.phik, nz)) return rc;  // exner = -Phi_k
+      if (int rc = wt_level_restrict_flux(h, l, V.hfm, V.hft, C.hfm, C.hft, C.dm, C.dt, nz)) return rc;
       PE(tm, PH_RESTRICT);
       const int *mask_n_c, *mask_e_c;
       wt_level_masks(h, l + 1, &mask_n_c, &mask_e_c);

@@ -464,22 +464,22 @@ int wt_wt_after_step(wt_handle* h) {
 
 }  // extern "C"
 
-int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd) {
+int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd, int nz) {
   WLev P = view(h, level), C = view(h, level + 1);
   P.scal = par;
   C.scal = const_cast<double*>(chd);
   const int m = h->at(level).n + 1;
-  k_restr_scalar<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(P, C, h->nz);
+  k_restr_scalar<<<nb((int64_t)nz * 10 * m * m), TPB, 0, h->stream>>>(P, C, nz);
   CKW(cudaGetLastError());
   return WT_OK;
 }
 
 int wt_level_restrict_flux(wt_handle* h, int level, double* par0, double* par1, const double* chd0,
-                           const double* chd1, const double* dsc0, const double* dsc1) {
+                           const double* chd1, const double* dsc0, const double* dsc1, int nz) {
   if (!h->at(level + 1).rf_wgt || !h->at(level + 1).overl_split) return WT_ERR_ARG;
-  const int m = h->at(level).n, lpt = lpt_for(h->nz);
-  const int64_t n = (int64_t)3 * 10 * m * m * ((h->nz + lpt - 1) / lpt);
-  k_restr_flux2<<<nb(n), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz, lpt, par0, par1, chd0, chd1,
+  const int m = h->at(level).n, lpt = lpt_for(nz);
+  const int64_t n = (int64_t)3 * 10 * m * m * ((nz + lpt - 1) / lpt);
+  k_restr_flux2<<<nb(n), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), nz, lpt, par0, par1, chd0, chd1,
                                               dsc0, dsc1);
   CKW(cudaGetLastError());
   return WT_OK;

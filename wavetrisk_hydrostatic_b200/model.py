@@ -237,6 +237,28 @@ class WaveletHierarchy(DeviceGrid):
         N.check("wt_adaptive_step", N.lib().wt_adaptive_step(self.h, float(dt), N.dptr(thr), int(level_fill),
                                                              int(max_level), int(nsteps)))
 
+    def barotropic_upload(self, level: int, eta=None, div_old=None) -> None:
+        """Free surface and previous flux divergence of one level (NN each; either may be None)."""
+        N.check("wt_barotropic_upload_level", N.lib().wt_barotropic_upload_level(
+            self.h, int(level), N.dptr(None if eta is None else _c(eta)),
+            N.dptr(None if div_old is None else _c(div_old))))
+
+    def rhs_elliptic_multi(self, dt: float, theta2: float = 1.0) -> None:
+        """flux_divergence with its compute-or-restrict and rhs_elliptic on every level."""
+        N.check("wt_rhs_elliptic_multi", N.lib().wt_rhs_elliptic_multi(self.h, float(dt), float(theta2)))
+
+    def u_update_multi(self, dt: float, theta1: float = 1.0) -> None:
+        """grad_eta with cpt_or_restr_eta and u_update on every level."""
+        N.check("wt_u_update_multi", N.lib().wt_u_update_multi(self.h, float(dt), float(theta1)))
+
+    def barotropic_download(self, level: int):
+        """(div_flux, rhs, grad_eta) of one level."""
+        NN = self.levels[level - self.ls].NN
+        div, rhs, grad = np.empty(NN), np.empty(NN), np.empty(3 * NN)
+        N.check("wt_barotropic_download_level", N.lib().wt_barotropic_download_level(
+            self.h, int(level), N.dptr(div), N.dptr(rhs), N.dptr(grad)))
+        return div, rhs, grad
+
     def lnorm(self, order: str = "inf") -> np.ndarray:
         """cal_lnorm of the scaling fields: (3, nz) for mass, Theta, velocity; order "inf", "1", "2" or "min"."""
         out = np.empty((3, self.nz))

@@ -31,10 +31,15 @@
 // lozenge corner is a pentagon (set_penta).  update_bdry is the level's ghost
 // copy (cp_bdry_inside) of every level, applied where the reference's drivers
 // call it.
-// Reads outside the padded array take 0.
+// Reads outside the padded array take 0.  The layers of a transform run on the
+// oracle's worker threads (orc_set_threads); layers share no data.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <thread>
 #include <vector>
+
+extern "C" int orc_get_threads(void);  // oracle_trisk.cpp
 
 namespace {
 
@@ -71,6 +76,23 @@ struct orc_wlevel {
 }
 
 namespace {
+
+// Runs f(k) for the layers k = 0..nz-1 on the oracle's worker count: the
+// transforms of different layers share no data, so the order does not matter.
+template <class F>
+void par_k(int nz, F f) {
+  const int nt = std::min(std::max(1, orc_get_threads()), nz);
+  if (nt <= 1) {
+    for (int k = 0; k < nz; ++k) f(k);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&, t] {
+      for (int k = t; k < nz; k += nt) f(k);
+    });
+  for (auto& x : th) x.join();
+}
 
 struct W {
   orc_wlevel* lv;
@@ -420,20 +442,20 @@ struct W {
     zero_wavelets();
     for (int l = le - 1; l >= ls; --l) {
       halo_scalars(l + 1, false);
-      for (int k = 0; k < nz; ++k) {
+      par_k(nz, [&](int k) {
         compute_scalar_wavelets(l, SM(l + 1, k), WM(l + 1, k));
         compute_scalar_wavelets(l, ST(l + 1, k), WT(l + 1, k));
-      }
+      });
       halo_scalars(l + 1, true);
-      for (int k = 0; k < nz; ++k) {
+      par_k(nz, [&](int k) {
         restrict_scalar(l, SM(l + 1, k), WM(l + 1, k), SM(l, k));
         restrict_scalar(l, ST(l + 1, k), WT(l + 1, k), ST(l, k));
         restrict_velo(l, SV(l + 1, k), SV(l, k));
-      }
+      });
     }
     for (int l = ls; l <= le; ++l) halo_velo(l, false);
     for (int l = le - 1; l >= ls; --l)
-      for (int k = 0; k < nz; ++k) compute_velo_wavelets(l, SV(l, k), SV(l + 1, k), WV(l + 1, k));
+      par_k(nz, [&](int k) { compute_velo_wavelets(l, SV(l, k), SV(l + 1, k), WV(l + 1, k)); });
   }
 
   void inverse() {
@@ -446,19 +468,19 @@ struct W {
       halo_velo(l, false);
     }
     for (int l = ls; l <= le - 1; ++l) {
-      for (int k = 0; k < nz; ++k) {
+      par_k(nz, [&](int k) {
         prolong_scalar(l, SM(l, k), WM(l + 1, k), SM(l + 1, k));
         prolong_scalar(l, ST(l, k), WT(l + 1, k), ST(l + 1, k));
-      }
+      });
       if (l > ls) halo_velo(l, false);
       halo_scalars(l + 1, false);
-      for (int k = 0; k < nz; ++k) reconstruct_outer_velo(l, SV(l, k), WV(l + 1, k), SV(l + 1, k));
+      par_k(nz, [&](int k) { reconstruct_outer_velo(l, SV(l, k), WV(l + 1, k), SV(l + 1, k)); });
       halo_velo(l + 1, false);
-      for (int k = 0; k < nz; ++k) {
+      par_k(nz, [&](int k) {
         reconstruct_scalar(l, WM(l + 1, k), SM(l + 1, k));
         reconstruct_scalar(l, WT(l + 1, k), ST(l + 1, k));
-      }
-      for (int k = 0; k < nz; ++k) reconstruct_inner_velo(l, SV(l, k), WV(l + 1, k), SV(l + 1, k));
+      });
+      par_k(nz, [&](int k) { reconstruct_inner_velo(l, SV(l, k), WV(l + 1, k), SV(l + 1, k)); });
     }
   }
 
@@ -499,7 +521,7 @@ struct W {
       halo_scalars(l, true);
       halo_velo(l, true);
     }
-    for (int k = 0; k < nz; ++k)
+    par_k(nz, [&](int k) {
       for (int l = ls + 1; l <= le; ++l) {
         orc_wlevel& g = L(l);
         for (int d = 0; d < 10; ++d) {
@@ -519,6 +541,7 @@ struct W {
             }
         }
       }
+    });
   }
 
   // ---- masks (one level; out-of-array reads are ZERO, writes are skipped)
@@ -850,12 +873,13 @@ struct W {
       halo_scalars(l, false);
       halo_velo(l, false);
     }
-    for (int k = 0; k < nz; ++k)
+    par_k(nz, [&](int k) {
       for (int l = ls; l <= le - 1; ++l) {
         compute_scalar_wavelets(l, SM(l + 1, k), WM(l + 1, k));
         compute_scalar_wavelets(l, ST(l + 1, k), WT(l + 1, k));
         compute_velo_wavelets(l, SV(l, k), SV(l + 1, k), WV(l + 1, k));
       }
+    });
     compress();
     inverse();
   }

@@ -663,7 +663,8 @@ def cpu_baseline(args, quick=False):
 def cpu_baseline_adaptive(args, quick=False):
     """The oracle's adaptive step on the same hierarchy (multi-level trend,
     RK4, WT_after_step, adapt's mask sequence, compression, inverse
-    transform), timed over whole steps until the budget is used."""
+    transform) on all host threads, timed over whole steps until the budget is
+    used."""
     import numpy as np
 
     import oracle
@@ -702,8 +703,9 @@ def cpu_baseline_adaptive(args, quick=False):
         steps += 1
     return {"value": sim_days_per_hour(steps, t_used, DT_AD), "unit": "simulated days per wall-clock hour",
             "cores": oracle.get_threads(), "kind": "port",
-            "sample": f"{steps} adaptive steps of the same workload ({t_used:.1f} s): the multi-level trend on "
-                      f"{oracle.get_threads()} threads (one per lozenge), wavelets and masks on one thread"}
+            "sample": f"{steps} adaptive steps of the same workload ({t_used:.1f} s): the multi-level trend "
+                      f"over lozenges and the wavelet transforms over layers on {oracle.get_threads()} threads, "
+                      f"the mask sequence on one"}
 
 
 def bench_reference(args):

@@ -7,6 +7,20 @@
 #pragma once
 #include "wavelet_kernels.cuh"
 
+// Minimum resident blocks per SM of the layer-group kernels, i.e. register
+// caps.  Measured on B200 (WT_after_step, J5..J7 x 16 / J6..J8 x 32): no caps
+// 0.80 / 4.92 ms; scalar and outer 6, inner 4 (the inner kernels spill about
+// 60 bytes) 0.66 / 3.83 ms; 8, 8, 4 0.67 / 3.76 ms.
+#ifndef WL_MINB_SCALAR
+#define WL_MINB_SCALAR 6
+#endif
+#ifndef WL_MINB_OUTER
+#define WL_MINB_OUTER 6
+#endif
+#ifndef WL_MINB_INNER
+#define WL_MINB_INNER 4
+#endif
+
 namespace wtw {
 
 // Codes of the remapped readers: node code = source node, edge code = source
@@ -70,7 +84,7 @@ __device__ __forceinline__ void child_interps(NodeInterp N[3], const WLev& C, in
 }
 
 // Compute_scalar_wavelets (src/wavelet.f90:642-670), parents [0, np)^2.
-__global__ void __launch_bounds__(128) k_scalar_wc_l(WLev C, int np, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int np, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
   if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
@@ -99,7 +113,7 @@ __global__ void __launch_bounds__(128) k_scalar_wc_l(WLev C, int np, int nz, int
 }
 
 // Reconstruct_scalar (src/wavelet.f90:614-640), parents [0, np)^2.
-__global__ void __launch_bounds__(128) k_recon_scalar_l(WLev C, int np, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_recon_scalar_l(WLev C, int np, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
   if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
@@ -128,7 +142,7 @@ __global__ void __launch_bounds__(128) k_recon_scalar_l(WLev C, int np, int nz, 
 
 // Prolong_scalar (src/wavelet.f90:571-612), parents [0, np]^2: the eleven
 // lifting terms the reference sums.
-__global__ void __launch_bounds__(128) k_prolong_l(WLev Pa, WLev C, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_prolong_l(WLev Pa, WLev C, int nz, int lpt) {
   const int np = Pa.n;
   int d, ip, jp;
   int k0, k1;
@@ -213,7 +227,7 @@ __device__ __forceinline__ double outer_eval(const OuterInterp& O, const double*
 
 // Compute_velo_wavelets' outer edges (src/wavelet.f90:672-710), parents
 // [0, np)^2, with the pentagon corrections of the corner parents.
-__global__ void __launch_bounds__(128) k_velo_wc_outer_l(WLev Pa, WLev C, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa, WLev C, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
   if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
@@ -245,7 +259,7 @@ __global__ void __launch_bounds__(128) k_velo_wc_outer_l(WLev Pa, WLev C, int nz
 
 // Reconstruct_outer_velo (src/wavelet.f90:954-976), parents [0, np]^2, then
 // Reconstruct_velo_penta by the corner parents.
-__global__ void __launch_bounds__(128) k_recon_outer_l(WLev Pa, WLev C, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_OUTER) k_recon_outer_l(WLev Pa, WLev C, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
   if (!parent_of(Pa.n + 1, nz, lpt, d, ip, jp, k0, k1)) return;
@@ -336,7 +350,7 @@ __device__ __forceinline__ void inner_eval(const InnerInterp& I, const double* _
 }
 
 // Compute_velo_wavelets' inner edges (src/wavelet.f90:672-710), parents [0, np)^2.
-__global__ void __launch_bounds__(128) k_velo_wc_inner_l(WLev Pa, WLev C, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa, WLev C, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
   if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
@@ -367,7 +381,7 @@ __global__ void __launch_bounds__(128) k_velo_wc_inner_l(WLev Pa, WLev C, int nz
 }
 
 // Reconstruct_inner_velo (src/wavelet.f90:978-1003), parents [0, np)^2.
-__global__ void __launch_bounds__(128) k_recon_inner_l(WLev Pa, WLev C, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_INNER) k_recon_inner_l(WLev Pa, WLev C, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
   if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;

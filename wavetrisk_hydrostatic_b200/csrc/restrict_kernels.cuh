@@ -239,7 +239,13 @@ __device__ __forceinline__ void sm_make(SmTerm& t, const WLev& C, int d, int i, 
   }
 }
 
-__global__ void __launch_bounds__(256) k_restr_flux2(WLev P, WLev C, int nz, int lpt, double* __restrict__ fp0,
+// Minimum resident blocks per SM of k_restr_flux2 (register cap).  Measured on
+// B200 (restriction into one level of J4..J7 x 16): no cap (127 registers)
+// 0.115 ms, 3 blocks 0.087 ms, 4 blocks (64 registers, spilling to L1) 0.079 ms.
+#ifndef RF_MINB
+#define RF_MINB 4
+#endif
+__global__ void __launch_bounds__(256, RF_MINB) k_restr_flux2(WLev P, WLev C, int nz, int lpt, double* __restrict__ fp0,
                                                      double* __restrict__ fp1, const double* __restrict__ fc0,
                                                      const double* __restrict__ fc1, const double* __restrict__ dc0,
                                                      const double* __restrict__ dc1) {

@@ -371,20 +371,21 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
 
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
-                   double* bern, double* theta, const wtk::Step1Maps* maps) {
+                   double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream) {
   const DevLevel& D = h->at(level);
   const LevelDev L = D.view();
   const int nz = h->nz;
+  cudaStream_t s = stream ? stream : h->stream;
   const unsigned chunks = blocks_for(D.NN, NODE_TILE);
-  k_column<<<chunks, NODE_TILE, 0, h->stream>>>(L, h->ph, nz, m, t, mean_m, mean_t, phik, pterm);
+  k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, mean_m, mean_t, phik, pterm);
   Step1Out so{qe, hfm, hft, bern, theta};
   if (maps && level == h->level_end && h->trend_variant == 0) {
     const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;
     const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
-    k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, h->stream>>>(L, nz, nbx, nby, m, t, v, mean_m, phik, pterm, so,
-                                                                   h->dflag, *maps);
+    k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, s>>>(L, nz, nbx, nby, m, t, v, mean_m, phik, pterm, so,
+                                                           h->dflag, *maps);
   } else {
-    k_step1<<<chunks * nz, NODE_TILE, 0, h->stream>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so);
+    k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so);
   }
   CK(cudaGetLastError());
   return WT_OK;

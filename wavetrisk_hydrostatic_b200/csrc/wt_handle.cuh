@@ -84,9 +84,10 @@ void wt_trend_ml_release(wt_handle* h);
 // on the given state, into the given operator arrays (wt_api.cu).
 // With maps (the top level's step1 input maps of this state) the top level runs
 // the TMA-staged step1 when the handle selected it.
+// stream: the handle's when null.
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
-                   double* bern, double* theta, const wtk::Step1Maps* maps);
+                   double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream);
 // The step1 input maps of a top-level state (WT_ERR_STATE when the handle runs the L1 kernels) (wt_api.cu).
 int wt_make_step1_maps(wt_handle* h, const double* m, const double* t, const double* v, wtk::Step1Maps* out);
 // scalar_cpt_restr / flux_cpt_restr of the nz layers of the given fields from

@@ -31,6 +31,11 @@ struct MLCtx {
   cudaGraphExec_t step_graph = nullptr;
   double g_dt = 0.0;
   int g_fill = -1, g_max = -1;
+  // column + step1 of the coarser levels run on side streams, forked from the
+  // handle's stream and joined before each level's restriction
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> done;
+  cudaEvent_t fork = nullptr;
 };
 
 #define CKM(x)                                            \
@@ -60,6 +65,15 @@ int ensure(wt_handle* h) {
       CKM(cudaMemsetAsync(*p, 0, 3 * nn * 8, h->stream));
     }
   }
+  CKM(cudaEventCreateWithFlags(&M->fork, cudaEventDisableTiming));
+  for (int l = h->level_start; l < h->level_end; ++l) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    CKM(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    M->side.push_back(s);
+    CKM(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    M->done.push_back(e);
+  }
   return WT_OK;
 }
 
@@ -69,6 +83,9 @@ void wt_trend_ml_release(wt_handle* h) {
   if (!h || !h->ml) return;
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   if (M->step_graph) cudaGraphExecDestroy(M->step_graph);
+  for (cudaEvent_t e : M->done) cudaEventDestroy(e);
+  for (cudaStream_t s : M->side) cudaStreamDestroy(s);
+  if (M->fork) cudaEventDestroy(M->fork);
   for (void* p : M->allocs) cudaFree(p);
   delete M;
   h->ml = nullptr;
@@ -130,30 +147,54 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
                 const States* dest = nullptr, double hs = 0.0) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const int nz = h->nz;
+  // Column + step1 of a level read only that level's state and write only its
+  // own work fields, so the coarser levels' run beside the finest level's on
+  // side streams (parallel branches of a captured graph).  The phase timer
+  // keeps them on the handle's stream so that its events bracket them.
+  const bool concurrent = tm == nullptr && h->level_end > h->level_start;
+  if (concurrent) {
+    CKM(cudaEventRecord(M->fork, h->stream));
+    for (int l = h->level_start; l < h->level_end; ++l) {
+      const int q = l - h->level_start;
+      MLLevel& V = M->L[q];
+      double *mm, *mt;
+      if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
+      if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
+      CKM(cudaStreamWaitEvent(M->side[q], M->fork, 0));
+      if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern,
+                                  V.theta, nullptr, M->side[q]))
+        return rc;
+      CKM(cudaEventRecord(M->done[q], M->side[q]));
+    }
+  }
   for (int l = h->level_end; l >= h->level_start; --l) {
     const int q = l - h->level_start;
     MLLevel& V = M->L[q];
     const DevLevel& D = h->at(l);
-    double *mm, *mt;
-    if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
-    if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
-    PB(tm);
-    const wtk::Step1Maps* maps = nullptr;
-    if (l == h->level_end && h->trend_variant == 0) {
-      if (S.m[q] == h->mass && S.t[q] == h->temp && S.v[q] == h->velo) {
-        maps = &h->s1maps[0];
-      } else if (S.m[q] == V.m1 && S.t[q] == V.t1 && S.v[q] == V.v1) {
-        if (!M->q1maps_ok) {
-          if (int rc = wt_make_step1_maps(h, V.m1, V.t1, V.v1, &M->q1maps)) return rc;
-          M->q1maps_ok = true;
+    if (concurrent && l < h->level_end) {
+      CKM(cudaStreamWaitEvent(h->stream, M->done[q], 0));
+    } else {
+      double *mm, *mt;
+      if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
+      if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
+      PB(tm);
+      const wtk::Step1Maps* maps = nullptr;
+      if (l == h->level_end && h->trend_variant == 0) {
+        if (S.m[q] == h->mass && S.t[q] == h->temp && S.v[q] == h->velo) {
+          maps = &h->s1maps[0];
+        } else if (S.m[q] == V.m1 && S.t[q] == V.t1 && S.v[q] == V.v1) {
+          if (!M->q1maps_ok) {
+            if (int rc = wt_make_step1_maps(h, V.m1, V.t1, V.v1, &M->q1maps)) return rc;
+            M->q1maps_ok = true;
+          }
+          maps = &M->q1maps;
         }
-        maps = &M->q1maps;
       }
+      if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft,
+                                  V.bern, V.theta, maps, nullptr))
+        return rc;
+      PE(tm, l == h->level_end ? PH_STEP1_TOP : PH_STEP1_COARSE);
     }
-    if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern,
-                                V.theta, maps))
-      return rc;
-    PE(tm, l == h->level_end ? PH_STEP1_TOP : PH_STEP1_COARSE);
     wtk::TrendML io{};
     const int *mask_n, *mask_e;
     wt_level_masks(h, l, &mask_n, &mask_e);

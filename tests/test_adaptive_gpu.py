@@ -23,8 +23,12 @@ def _rel(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-@pytest.mark.parametrize("lmin,lmax,nz,tol", [(3, 5, 2, 5e-3), (3, 6, 2, 1e-2)])
-def test_adaptive_steps_match_oracle(lmin, lmax, nz, tol):
+@pytest.mark.parametrize("lmin,lmax,nz,tol,upload", [(3, 5, 2, 5e-3, False), (3, 6, 2, 1e-2, False),
+                                                      (3, 5, 2, 5e-3, True)])
+def test_adaptive_steps_match_oracle(lmin, lmax, nz, tol, upload):
+    """upload: random wavelets are uploaded into every slot of every level
+    between the steps; the step's first WT_after_step zeroes them (zero_float),
+    so the replayed graph must give the oracle's step all the same."""
     ph = OceanParams()
     dt, nsteps = 300.0, 2
     G = Grid(lmin, lmax, radius=6371e3)
@@ -58,6 +62,12 @@ def test_adaptive_steps_match_oracle(lmin, lmax, nz, tol):
         H.inverse()
         model.step(dt)
         check_masks(f"step {s}")
+        if upload:
+            rng = np.random.default_rng(s)
+            for g in levels:
+                for name in ("wc_mass", "wc_temp", "wc_velo"):
+                    n = 3 * g.NN if name == "wc_velo" else g.NN
+                    model.dev.upload(g.level, name, rng.standard_normal((nz, n)))
     for g in levels:
         own = np.nonzero(g.owned)[0]
         e = np.concatenate([own, own + g.NN, own + 2 * g.NN])

@@ -141,6 +141,43 @@ def test_compress_and_wt_after_step_match_oracle():
     dev.close()
 
 
+def test_wt_after_step_after_wavelet_upload_matches_oracle():
+    """WT_after_step starts from zeroed wavelets (zero_float): wavelets uploaded
+    from the host into every slot (parent-coincident nodes and the coarsest
+    level included) must not survive it, on the direct path nor in the graph
+    of the adaptive step."""
+    levels, orc, dev = _setup(3, 5, 2)
+    _random_fine(levels, orc, dev, 2, seed=53)
+    orc.forward()
+    dev.forward()
+    thr = np.full((3, 2), 0.5)
+    orc.mask_tol(thr, 0)
+    dev.mask_tol_vars(thr, 0)
+    rng = np.random.default_rng(7)
+    for g in levels:
+        for name in ("wc_mass", "wc_temp", "wc_velo"):
+            a = rng.standard_normal(orc.field(g.level, NAMES[name]).shape)
+            orc.set(g.level, NAMES[name], a)
+            dev.upload(g.level, name, a)
+    orc.wt_after_step()
+    dev.wt_after_step()
+    _compare(levels, orc, dev, NAMES)
+    for g in levels:  # parent-coincident slots and the coarsest level hold 0
+        w = dev.download(g.level, "wc_mass")
+        own = np.nonzero(g.owned)[0]
+        d, r = np.divmod(own, g.P * g.P)
+        j, i = np.divmod(r, g.P)
+        even = own[((i - 2) % 2 == 0) & ((j - 2) % 2 == 0)]
+        assert not np.any(w[:, even]), g.level
+    orc.mask_tol(thr, 0)
+    dev.mask_tol_vars(thr, 0)
+    for g in levels:
+        for name in ("mask_n", "mask_e"):
+            assert np.array_equal(dev.download(g.level, name), orc.field(g.level, name)), (g.level, name)
+    assert dev.status() == 0
+    dev.close()
+
+
 @pytest.mark.parametrize("level_fill,scale", [(3, 0.3), (0, 0.05), (4, 1.0)])
 def test_mask_build_matches_oracle_exactly(level_fill, scale):
     """adapt's mask sequence: every node and edge mask of every level (ghost

@@ -84,6 +84,11 @@ __device__ __forceinline__ void child_interps(NodeInterp N[3], const WLev& C, in
 }
 
 // Compute_scalar_wavelets (src/wavelet.f90:642-670), parents [0, np)^2.
+// CMP: the wavelets are not zeroed beforehand and compress_wavelets follows
+// (WT_after_step), so each of the three child slots is written, with 0 where
+// the child's mask is below ADJZONE; the other slots of the level (parent-
+// coincident nodes, ghost rows) hold 0 from the last zeroing.
+template <bool CMP>
 __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int np, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
@@ -98,7 +103,16 @@ __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int
     self[q] = wn_code(C, d, ci[q], cj[q]);
     at[q] = nid(C, d, ci[q], cj[q]);
   }
-  if (!(on[0] || on[1] || on[2])) return;
+  if (!(on[0] || on[1] || on[2])) {
+    if (CMP)
+      for (int k = k0; k < k1; ++k)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          C.wm[(int64_t)k * C.NN + at[q]] = 0.0;
+          C.wt[(int64_t)k * C.NN + at[q]] = 0.0;
+        }
+    return;
+  }
   NodeInterp N[3];
   child_interps(N, C, d, i, j);
   for (int k = k0; k < k1; ++k)
@@ -108,7 +122,10 @@ __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int
       double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
 #pragma unroll
       for (int q = 0; q < 3; ++q)
-        if (on[q]) wc[at[q]] = wn(s, self[q]) - node_eval(N[q], s);
+        if (on[q])
+          wc[at[q]] = wn(s, self[q]) - node_eval(N[q], s);
+        else if (CMP)
+          wc[at[q]] = 0.0;
     }
 }
 
@@ -226,7 +243,11 @@ __device__ __forceinline__ double outer_eval(const OuterInterp& O, const double*
 }
 
 // Compute_velo_wavelets' outer edges (src/wavelet.f90:672-710), parents
-// [0, np)^2, with the pentagon corrections of the corner parents.
+// [0, np)^2, with the pentagon corrections of the corner parents.  CMP as for
+// k_scalar_wc_l: both child slots of each parent edge are written and
+// compress_vector's rule (0 where the slot's own mask is below ADJZONE) is
+// applied to them, after the pentagon corrections in the corner parents.
+template <bool CMP>
 __global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa, WLev C, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
@@ -236,11 +257,19 @@ __global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa,
   for (int e = 0; e < 3; ++e) {
     const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
     const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
-    if (me(C, e, d, a2, b2) < ADJZONE) continue;
+    const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
+    if (me(C, e, d, a2, b2) < ADJZONE) {
+      if (CMP)
+        for (int k = k0; k < k1; ++k) {
+          C.wv[(int64_t)k * 3 * C.NN + x2] = 0.0;
+          C.wv[(int64_t)k * 3 * C.NN + x1] = 0.0;
+        }
+      continue;
+    }
+    const bool keep1 = !CMP || corner || me(C, e, d, a1, b1) >= ADJZONE;
     OuterInterp O;
     outer_interp(O, Pa, C, d, ip, jp, a2, b2, e);
     const int cv = we_code(C, e, d, a2, b2);
-    const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
     for (int k = k0; k < k1; ++k) {
       const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
       const double* v = C.sv + (int64_t)k * 3 * C.NN;
@@ -249,12 +278,22 @@ __global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa,
       const double u = outer_eval(O, vp, t0);
       const double w = we(v, cv) - u;
       wc[x2] = w;
-      wc[x1] = -w;
+      wc[x1] = keep1 ? -w : 0.0;
     }
   }
-  if (corner)
+  if (corner) {
     for (int k = k0; k < k1; ++k)
       penta_compute(Pa, C, Pa.sv + (int64_t)k * 3 * Pa.NN, C.wv + (int64_t)k * 3 * C.NN, d, ip, jp);
+    if (CMP)
+      for (int e = 0; e < 3; ++e)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int a = i + c_end_pt[e][h][0], b = j + c_end_pt[e][h][1];
+          if (me(C, e, d, a, b) >= ADJZONE) continue;
+          const int x = e * C.NN + nid(C, d, a, b);
+          for (int k = k0; k < k1; ++k) C.wv[(int64_t)k * 3 * C.NN + x] = 0.0;
+        }
+  }
 }
 
 // Reconstruct_outer_velo (src/wavelet.f90:954-976), parents [0, np]^2, then
@@ -349,7 +388,9 @@ __device__ __forceinline__ void inner_eval(const InnerInterp& I, const double* _
   u[5] = (I.tc[5] * curl1 - pr[4] - pr[9]) / I.den[5];
 }
 
-// Compute_velo_wavelets' inner edges (src/wavelet.f90:672-710), parents [0, np)^2.
+// Compute_velo_wavelets' inner edges (src/wavelet.f90:672-710), parents
+// [0, np)^2; CMP as for k_scalar_wc_l.
+template <bool CMP>
 __global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa, WLev C, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
@@ -365,7 +406,13 @@ __global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa,
     on[q] = me(C, ge[q], d, gi[q], gj[q]) >= ADJZONE;
     any = any || on[q];
   }
-  if (!any) return;
+  if (!any) {
+    if (CMP)
+      for (int k = k0; k < k1; ++k)
+#pragma unroll
+        for (int q = 0; q < 6; ++q) C.wv[(int64_t)k * 3 * C.NN + ge[q] * C.NN + nid(C, d, gi[q], gj[q])] = 0.0;
+    return;
+  }
   InnerInterp I;
   inner_interp(I, Pa, C, d, ip, jp);
   for (int k = k0; k < k1; ++k) {
@@ -376,7 +423,10 @@ __global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa,
     inner_eval(I, vp, v, u);
 #pragma unroll
     for (int q = 0; q < 6; ++q)
-      if (on[q]) wc[I.xt[q]] = we(v, I.ct[q]) - u[q];
+      if (on[q])
+        wc[I.xt[q]] = we(v, I.ct[q]) - u[q];
+      else if (CMP)
+        wc[I.xt[q]] = 0.0;
   }
 }
 

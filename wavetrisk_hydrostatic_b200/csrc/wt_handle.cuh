@@ -107,6 +107,9 @@ int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double
 // and inverse transform of the hierarchy, and the threshold upload (wt_wavelet.cu).
 int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq);
 void wt_level_compress(wt_handle* h);
+// zero every wavelet array if a host upload wrote wavelets since the last
+// zeroing (stream-ordered; WT_after_step then writes only the slots it computes)
+void wt_level_clean_wavelets(wt_handle* h);
 void wt_level_inverse(wt_handle* h);
 int wt_level_set_thresholds(wt_handle* h, const double* threshold);
 // The scaling fields (mass, Theta, velocity) of a level (wt_wavelet.cu).

@@ -287,7 +287,7 @@ int wt_rk4_multi(wt_handle* h, double dt, int nsteps) {
 // One adaptive time step of the fully refined hierarchy, as the reference's
 // time_step (src/main.f90:405-444) with fixed thresholds: RK4 of the hierarchy
 // (trend_ml, RK_sub_step, WT_after_step per stage), adapt's mask sequence and
-// compression, and the inverse wavelet transform.  The ~330 launches of a step
+// compression, and the inverse wavelet transform.  The ~280 launches of a step
 // are captured once into a CUDA graph (re-captured when dt, level_fill or
 // max_level change) and replayed; the thresholds are uploaded before each call.
 int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level_fill, int max_level, int nsteps) {
@@ -301,6 +301,7 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
     if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &p)) return rc;
   }
   if (int rc = wt_level_set_thresholds(h, threshold)) return rc;
+  wt_level_clean_wavelets(h);  // outside the graph, which assumes clean wavelet arrays
   if (!M->step_graph || M->g_dt != dt || M->g_fill != level_fill || M->g_max != max_level) {
     if (M->step_graph) {
       cudaGraphExecDestroy(M->step_graph);

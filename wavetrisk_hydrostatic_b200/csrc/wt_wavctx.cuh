@@ -25,6 +25,14 @@ struct WavCtx {
   std::vector<WavLevel> L;
   double* thr = nullptr;  // [3][nz] thresholds
   std::vector<void*> allocs;
+  // Wavelet slots that no transform kernel writes (parent-coincident nodes,
+  // ghost rows, the coarsest level) hold 0 unless a host upload wrote them;
+  // WT_after_step re-zeroes the arrays only then.
+  bool wav_dirty = false;
+  // side streams of the transforms: scalar chain (0) and inner velocity
+  // wavelets (1), forked from and joined back into the handle's stream
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   template <class T>
   cudaError_t alloc(T** p, size_t count) {
     cudaError_t e = cudaMalloc(p, count * sizeof(T));

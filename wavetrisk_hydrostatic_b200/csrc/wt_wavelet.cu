@@ -111,30 +111,43 @@ void zero_wavelets(wt_handle* h) {
 }
 
 // Scalar wavelets of level l+1 (Compute_scalar_wavelets over parents [0, n_l)).
-void launch_scalar_wc(wt_handle* h, int l) {
+template <bool CMP>
+void launch_scalar_wc(wt_handle* h, int l, cudaStream_t s) {
   const int np = h->at(l).n, nz = h->nz;
-  k_scalar_wc_l<<<nbl((int64_t)10 * np * np, nz), TPBL, 0, h->stream>>>(view(h, l + 1), np, nz, lpt_for(nz));
+  k_scalar_wc_l<CMP><<<nbl((int64_t)10 * np * np, nz), TPBL, 0, s>>>(view(h, l + 1), np, nz, lpt_for(nz));
 }
 
-// Velocity wavelets of level l+1 (pentagon corrections included).
-void launch_velo_wc(wt_handle* h, int l) {
+// Velocity wavelets of level l+1 (pentagon corrections included): outer edges
+// on s, inner edges on si (they read only the scaling fields).
+template <bool CMP>
+void launch_velo_wc(wt_handle* h, int l, cudaStream_t s, cudaStream_t si) {
   const int np = h->at(l).n, nz = h->nz;
-  k_velo_wc_outer_l<<<nbl((int64_t)10 * np * np, nz), TPBL, 0, h->stream>>>(view(h, l), view(h, l + 1), nz, lpt_for(nz));
-  k_velo_wc_inner_l<<<nbl((int64_t)10 * np * np, nz), TPBL, 0, h->stream>>>(view(h, l), view(h, l + 1), nz, lpt_for(nz));
+  const unsigned g = nbl((int64_t)10 * np * np, nz);
+  k_velo_wc_outer_l<CMP><<<g, TPBL, 0, s>>>(view(h, l), view(h, l + 1), nz, lpt_for(nz));
+  k_velo_wc_inner_l<CMP><<<g, TPBL, 0, si>>>(view(h, l), view(h, l + 1), nz, lpt_for(nz));
 }
 
-// inverse_wavelet_transform (src/wavelet.f90:208-296) from level_start.
+// inverse_wavelet_transform (src/wavelet.f90:208-296) from level_start.  The
+// scalars and the velocity reconstruct independently of each other, so the
+// scalar chain (Prolong_scalar, Reconstruct_scalar per level) runs on a side
+// stream beside the velocity chain (outer, then inner edges per level).
 void inverse(wt_handle* h) {
   const int nz = h->nz;
+  WavCtx* W = ctx(h);
+  cudaStream_t s = h->stream, sa = W->side[0];
+  cudaEventRecord(W->ev[0], s);
+  cudaStreamWaitEvent(sa, W->ev[0], 0);
   for (int l = h->level_start; l <= h->level_end - 1; ++l) {
     const int np = h->at(l).n;
     const WLev P = view(h, l), C = view(h, l + 1);
     const int64_t par1 = (int64_t)10 * (np + 1) * (np + 1), par0 = (int64_t)10 * np * np;
-    k_prolong_l<<<nbl(par1, nz), TPBL, 0, h->stream>>>(P, C, nz, lpt_for(nz));
-    k_recon_outer_l<<<nbl(par1, nz), TPBL, 0, h->stream>>>(P, C, nz, lpt_for(nz));
-    k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, h->stream>>>(C, np, nz, lpt_for(nz));
-    k_recon_inner_l<<<nbl(par0, nz), TPBL, 0, h->stream>>>(P, C, nz, lpt_for(nz));
+    k_prolong_l<<<nbl(par1, nz), TPBL, 0, sa>>>(P, C, nz, lpt_for(nz));
+    k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, sa>>>(C, np, nz, lpt_for(nz));
+    k_recon_outer_l<<<nbl(par1, nz), TPBL, 0, s>>>(P, C, nz, lpt_for(nz));
+    k_recon_inner_l<<<nbl(par0, nz), TPBL, 0, s>>>(P, C, nz, lpt_for(nz));
   }
+  cudaEventRecord(W->ev[1], sa);
+  cudaStreamWaitEvent(s, W->ev[1], 0);
 }
 
 void compress(wt_handle* h) {
@@ -160,12 +173,22 @@ int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double
       W->L[q].st = t[q];
       W->L[q].sv = v[q];
     }
-  zero_wavelets(h);
+  wt_level_clean_wavelets(h);
+  // zero_float, the wavelets of every level and compress_wavelets in one pass
+  // of the forward kernels per level (CMP); the three kinds of wavelets read
+  // only the scaling fields, so they run on three streams.
+  cudaStream_t s = h->stream;
+  CKW(cudaEventRecord(W->ev[0], s));
+  CKW(cudaStreamWaitEvent(W->side[0], W->ev[0], 0));
+  CKW(cudaStreamWaitEvent(W->side[1], W->ev[0], 0));
   for (int l = h->level_start; l <= h->level_end - 1; ++l) {
-    launch_scalar_wc(h, l);
-    launch_velo_wc(h, l);
+    launch_scalar_wc<true>(h, l, W->side[0]);
+    launch_velo_wc<true>(h, l, s, W->side[1]);
   }
-  compress(h);
+  CKW(cudaEventRecord(W->ev[1], W->side[0]));
+  CKW(cudaEventRecord(W->ev[2], W->side[1]));
+  CKW(cudaStreamWaitEvent(s, W->ev[1], 0));
+  CKW(cudaStreamWaitEvent(s, W->ev[2], 0));
   inverse(h);
   for (int q = 0; q < nl; ++q) {
     W->L[q].sm = saved[q].sm;
@@ -178,6 +201,10 @@ int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double
 
 void wt_wavelet_release(wt_handle* h) {
   if (!h || !h->wav) return;
+  for (cudaEvent_t e : ctx(h)->ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t s : ctx(h)->side)
+    if (s) cudaStreamDestroy(s);
   for (void* p : ctx(h)->allocs) cudaFree(p);
   delete ctx(h);
   h->wav = nullptr;
@@ -221,6 +248,8 @@ int wt_wavelet_setup(wt_handle* h) {
     CKW(cudaMemcpy(V.mask_e, tol.data(), 3 * D.NN * sizeof(int), cudaMemcpyHostToDevice));
   }
   CKW(W->alloc(&W->thr, (size_t)3 * nz));
+  for (cudaStream_t& s : W->side) CKW(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : W->ev) CKW(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   zero_wavelets(h);
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
@@ -253,6 +282,7 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
   CKW(cudaMemcpyAsync(dst[field], src, bytes[field], cudaMemcpyHostToDevice, h->stream));
   CKW(cudaStreamSynchronize(h->stream));
   if (level == h->level_end && field <= WT_FIELD_VELO) h->state_halo_done = false;
+  if (field >= WT_WAVE_MASS && field <= WT_WAVE_VELO) ctx(h)->wav_dirty = true;
   return WT_OK;
 }
 
@@ -297,12 +327,13 @@ int wt_forward_wt(wt_handle* h) {
   if (int rc = ready(h)) return rc;
   const int nz = h->nz;
   zero_wavelets(h);
+  ctx(h)->wav_dirty = false;
   for (int l = h->level_end - 1; l >= h->level_start; --l) {
     const int np = h->at(l).n;
-    launch_scalar_wc(h, l);
+    launch_scalar_wc<false>(h, l, h->stream);
     k_restrict<<<nb((int64_t)nz * 10 * (np + 1) * (np + 1)), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), nz);
   }
-  for (int l = h->level_end - 1; l >= h->level_start; --l) launch_velo_wc(h, l);
+  for (int l = h->level_end - 1; l >= h->level_start; --l) launch_velo_wc<false>(h, l, h->stream, h->stream);
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
@@ -411,6 +442,11 @@ int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patc
 }
 
 void wt_level_compress(wt_handle* h) { compress(h); }
+void wt_level_clean_wavelets(wt_handle* h) {
+  if (!ctx(h)->wav_dirty) return;
+  zero_wavelets(h);
+  ctx(h)->wav_dirty = false;
+}
 void wt_level_inverse(wt_handle* h) { inverse(h); }
 int wt_level_set_thresholds(wt_handle* h, const double* threshold) {
   CKW(cudaMemcpyAsync(ctx(h)->thr, threshold, 3 * h->nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));

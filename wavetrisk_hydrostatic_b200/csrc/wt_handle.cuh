@@ -92,7 +92,8 @@ int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, co
 int wt_make_step1_maps(wt_handle* h, const double* m, const double* t, const double* v, wtk::Step1Maps* out);
 // scalar_cpt_restr / flux_cpt_restr of the nz layers of the given fields from
 // level+1 to `level` with the masks of the hierarchy (wt_wavelet.cu).
-int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd, int nz);
+int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd, int nz,
+                             cudaStream_t stream = nullptr);
 // flux_cpt_restr of two fluxes (par1/chd1/dsc1 may be null) in one launch.
 int wt_level_restrict_flux(wt_handle* h, int level, double* par0, double* par1, const double* chd0,
                            const double* chd1, const double* dsc0, const double* dsc1, int nz);
@@ -103,6 +104,14 @@ void wt_level_masks(wt_handle* h, int level, const int** mask_n, const int** mas
 // WT_after_step on the given per-level scaling fields (level_start first), or on
 // the hierarchy's own when the arrays are null; stream-ordered (wt_wavelet.cu).
 int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v);
+// WT_after_step in pieces, for callers that launch each level pair's forward
+// wavelets as soon as both levels' fields are written: bind the stage's scaling
+// fields, wt_level_clean_wavelets, wt_level_wav_forward_pair for every l in
+// [level_start, level_end), wt_level_wav_finish, unbind.
+void wt_level_wav_bind(wt_handle* h, double* const* m, double* const* t, double* const* v);
+void wt_level_wav_unbind(wt_handle* h);
+int wt_level_wav_forward_pair(wt_handle* h, int level);
+int wt_level_wav_finish(wt_handle* h);
 // adapt's mask sequence without host synchronisation (capturable), compression
 // and inverse transform of the hierarchy, and the threshold upload (wt_wavelet.cu).
 int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq);

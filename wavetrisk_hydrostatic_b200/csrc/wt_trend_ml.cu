@@ -36,6 +36,11 @@ struct MLCtx {
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> done;
   cudaEvent_t fork = nullptr;
+  // the Bernoulli and Exner restrictions, level by level on their own stream
+  // (they need both levels' step1 and the finer restriction, not the trends)
+  cudaStream_t rs = nullptr;
+  std::vector<cudaEvent_t> rsd;
+  cudaEvent_t s1top = nullptr;
 };
 
 #define CKM(x)                                            \
@@ -66,13 +71,17 @@ int ensure(wt_handle* h) {
     }
   }
   CKM(cudaEventCreateWithFlags(&M->fork, cudaEventDisableTiming));
+  CKM(cudaEventCreateWithFlags(&M->s1top, cudaEventDisableTiming));
+  CKM(cudaStreamCreateWithFlags(&M->rs, cudaStreamNonBlocking));
   for (int l = h->level_start; l < h->level_end; ++l) {
     cudaStream_t s;
-    cudaEvent_t e;
+    cudaEvent_t e, r;
     CKM(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     M->side.push_back(s);
     CKM(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     M->done.push_back(e);
+    CKM(cudaEventCreateWithFlags(&r, cudaEventDisableTiming));
+    M->rsd.push_back(r);
   }
   return WT_OK;
 }
@@ -84,8 +93,11 @@ void wt_trend_ml_release(wt_handle* h) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   if (M->step_graph) cudaGraphExecDestroy(M->step_graph);
   for (cudaEvent_t e : M->done) cudaEventDestroy(e);
+  for (cudaEvent_t e : M->rsd) cudaEventDestroy(e);
   for (cudaStream_t s : M->side) cudaStreamDestroy(s);
+  if (M->rs) cudaStreamDestroy(M->rs);
   if (M->fork) cudaEventDestroy(M->fork);
+  if (M->s1top) cudaEventDestroy(M->s1top);
   for (void* p : M->allocs) cudaFree(p);
   delete M;
   h->ml = nullptr;
@@ -143,8 +155,12 @@ States hierarchy_state(wt_handle* h) {
 // base and dest, each level's k_trend_ml also takes the RK sub-step
 // dest = base + hs * trend (RK_sub_step, src/time_integr.f90:206-225) instead of
 // writing dv: a level's state is not read after its step1, so dest may be S.
+// With wav (and dest), the forward wavelets of WT_after_step for the level
+// pair (l, l+1) are launched as soon as level l's sub-step is written, beside
+// the coarser levels' trend; the caller binds dest to the wavelet context
+// before and finishes WT_after_step after.
 int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const States* base = nullptr,
-                const States* dest = nullptr, double hs = 0.0) {
+                const States* dest = nullptr, double hs = 0.0, bool wav = false) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const int nz = h->nz;
   // Column + step1 of a level read only that level's state and write only its
@@ -194,6 +210,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
                                   V.bern, V.theta, maps, nullptr))
         return rc;
       PE(tm, l == h->level_end ? PH_STEP1_TOP : PH_STEP1_COARSE);
+      if (concurrent) CKM(cudaEventRecord(M->s1top, h->stream));
     }
     wtk::TrendML io{};
     const int *mask_n, *mask_e;
@@ -202,9 +219,19 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
     if (l < h->level_end) {
       MLLevel& C = M->L[q + 1];
       PB(tm);
-      if (int rc = wt_level_restrict_scalar(h, l, V.bern, C.bern, nz)) return rc;
-      if (int rc = wt_level_restrict_scalar(h, l, V.phik, C.phik, nz)) return rc;  // exner = -Phi_k
+      cudaStream_t rs = h->stream;
+      if (concurrent) {  // after this level's and the child's step1; the finer restriction precedes on rs
+        rs = M->rs;
+        CKM(cudaStreamWaitEvent(rs, M->done[q], 0));
+        CKM(cudaStreamWaitEvent(rs, l + 1 == h->level_end ? M->s1top : M->done[q + 1], 0));
+      }
+      if (int rc = wt_level_restrict_scalar(h, l, V.bern, C.bern, nz, rs)) return rc;
+      if (int rc = wt_level_restrict_scalar(h, l, V.phik, C.phik, nz, rs)) return rc;  // exner = -Phi_k
       if (int rc = wt_level_restrict_flux(h, l, V.hfm, V.hft, C.hfm, C.hft, C.dm, C.dt, nz)) return rc;
+      if (concurrent) {
+        CKM(cudaEventRecord(M->rsd[q], rs));
+        CKM(cudaStreamWaitEvent(h->stream, M->rsd[q], 0));
+      }
       PE(tm, PH_RESTRICT);
       const int *mask_n_c, *mask_e_c;
       wt_level_masks(h, l + 1, &mask_n_c, &mask_e_c);
@@ -226,6 +253,8 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
     wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
     PE(tm, l == h->level_end ? PH_TREND_TOP : PH_TREND_COARSE);
     CKM(cudaGetLastError());
+    if (wav && dest && l < h->level_end)
+      if (int rc = wt_level_wav_forward_pair(h, l)) return rc;
   }
   return WT_OK;
 }
@@ -260,10 +289,20 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm) {
     for (int stage = 0; stage < 4; ++stage) {
       const States& src = stage == 0 ? q : q1;
       const States& dest = stage == 3 ? q : q1;
-      if (int rc = trend_multi(h, src, tm, &q, &dest, hs[stage])) return rc;
-      PB(tm);
-      if (int rc = wt_level_after_step(h, dest.m.data(), dest.t.data(), dest.v.data())) return rc;
-      PE(tm, PH_AFTER_STEP);
+      if (tm) {  // phase by phase
+        if (int rc = trend_multi(h, src, tm, &q, &dest, hs[stage])) return rc;
+        PB(tm);
+        if (int rc = wt_level_after_step(h, dest.m.data(), dest.t.data(), dest.v.data())) return rc;
+        PE(tm, PH_AFTER_STEP);
+        continue;
+      }
+      // WT_after_step's forward wavelets start inside the trend, level pair by level pair
+      wt_level_wav_bind(h, dest.m.data(), dest.t.data(), dest.v.data());
+      wt_level_clean_wavelets(h);
+      int rc = trend_multi(h, src, nullptr, &q, &dest, hs[stage], true);
+      if (!rc) rc = wt_level_wav_finish(h);
+      wt_level_wav_unbind(h);
+      if (rc) return rc;
     }
   return WT_OK;
 }

@@ -29,10 +29,14 @@ struct WavCtx {
   // ghost rows, the coarsest level) hold 0 unless a host upload wrote them;
   // WT_after_step re-zeroes the arrays only then.
   bool wav_dirty = false;
-  // side streams of the transforms: scalar chain (0) and inner velocity
-  // wavelets (1), forked from and joined back into the handle's stream
-  cudaStream_t side[2] = {nullptr, nullptr};
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  // side streams of the transforms: scalar wavelets and the scalar chain of
+  // the inverse (0), inner (1) and outer (2) velocity wavelets, forked from and
+  // joined back into the handle's stream
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> fork;  // per level pair: its forward wavelets may start
+  // scaling-field pointers put aside while WT_after_step runs on other arrays
+  std::vector<WavLevel> bound_saved;
   template <class T>
   cudaError_t alloc(T** p, size_t count) {
     cudaError_t e = cudaMalloc(p, count * sizeof(T));

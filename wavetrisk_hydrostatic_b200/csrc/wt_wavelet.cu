@@ -160,48 +160,74 @@ void compress(wt_handle* h) {
 
 }  // namespace
 
-// WT_after_step on the scaling fields m[q], t[q], v[q] of level level_start+q
-// (the hierarchy's own scaling fields when the arrays are null): the launches
-// read the pointers when they are made, so the hierarchy's are put back at once.
-int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v) {
+// WT_after_step's scaling fields: m[q], t[q], v[q] of level level_start+q
+// replace the hierarchy's own until wt_level_wav_unbind.  Launches read the
+// pointers when they are made.
+void wt_level_wav_bind(wt_handle* h, double* const* m, double* const* t, double* const* v) {
   WavCtx* W = ctx(h);
-  const int nl = h->level_end - h->level_start + 1;
-  std::vector<WavLevel> saved(W->L);
-  if (m)
-    for (int q = 0; q < nl; ++q) {
-      W->L[q].sm = m[q];
-      W->L[q].st = t[q];
-      W->L[q].sv = v[q];
-    }
-  wt_level_clean_wavelets(h);
-  // zero_float, the wavelets of every level and compress_wavelets in one pass
-  // of the forward kernels per level (CMP); the three kinds of wavelets read
-  // only the scaling fields, so they run on three streams.
-  cudaStream_t s = h->stream;
-  CKW(cudaEventRecord(W->ev[0], s));
-  CKW(cudaStreamWaitEvent(W->side[0], W->ev[0], 0));
-  CKW(cudaStreamWaitEvent(W->side[1], W->ev[0], 0));
-  for (int l = h->level_start; l <= h->level_end - 1; ++l) {
-    launch_scalar_wc<true>(h, l, W->side[0]);
-    launch_velo_wc<true>(h, l, s, W->side[1]);
+  W->bound_saved = W->L;
+  for (size_t q = 0; q < W->L.size(); ++q) {
+    W->L[q].sm = m[q];
+    W->L[q].st = t[q];
+    W->L[q].sv = v[q];
   }
-  CKW(cudaEventRecord(W->ev[1], W->side[0]));
-  CKW(cudaEventRecord(W->ev[2], W->side[1]));
-  CKW(cudaStreamWaitEvent(s, W->ev[1], 0));
-  CKW(cudaStreamWaitEvent(s, W->ev[2], 0));
-  inverse(h);
-  for (int q = 0; q < nl; ++q) {
-    W->L[q].sm = saved[q].sm;
-    W->L[q].st = saved[q].st;
-    W->L[q].sv = saved[q].sv;
+}
+void wt_level_wav_unbind(wt_handle* h) {
+  WavCtx* W = ctx(h);
+  for (size_t q = 0; q < W->L.size(); ++q) {
+    W->L[q].sm = W->bound_saved[q].sm;
+    W->L[q].st = W->bound_saved[q].st;
+    W->L[q].sv = W->bound_saved[q].sv;
   }
+}
+
+// The wavelets of level l+1 from the scaling fields of levels l and l+1, with
+// zero_float and compress_wavelets folded in (CMP), once both levels' fields
+// are written on the handle's stream: the scalar, inner and outer velocity
+// wavelets run on three side streams forked here.  The arrays must be clean
+// (wt_level_clean_wavelets) before the first pair of a WT_after_step.
+int wt_level_wav_forward_pair(wt_handle* h, int l) {
+  WavCtx* W = ctx(h);
+  cudaEvent_t f = W->fork[l - h->level_start];
+  CKW(cudaEventRecord(f, h->stream));
+  for (cudaStream_t s : W->side) CKW(cudaStreamWaitEvent(s, f, 0));
+  launch_scalar_wc<true>(h, l, W->side[0]);
+  launch_velo_wc<true>(h, l, W->side[2], W->side[1]);
   CKW(cudaGetLastError());
   return WT_OK;
+}
+
+// The end of WT_after_step once every level pair's forward wavelets are
+// launched: join the side streams, then the inverse transform.
+int wt_level_wav_finish(wt_handle* h) {
+  WavCtx* W = ctx(h);
+  for (int k = 0; k < 3; ++k) {
+    CKW(cudaEventRecord(W->ev[1 + k], W->side[k]));
+    CKW(cudaStreamWaitEvent(h->stream, W->ev[1 + k], 0));
+  }
+  inverse(h);
+  CKW(cudaGetLastError());
+  return WT_OK;
+}
+
+// WT_after_step (src/adapt.f90:192-237) on the scaling fields m[q], t[q], v[q]
+// of level level_start+q (the hierarchy's own scaling fields when the arrays
+// are null).
+int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v) {
+  if (m) wt_level_wav_bind(h, m, t, v);
+  wt_level_clean_wavelets(h);
+  int rc = WT_OK;
+  for (int l = h->level_start; l <= h->level_end - 1 && !rc; ++l) rc = wt_level_wav_forward_pair(h, l);
+  if (!rc) rc = wt_level_wav_finish(h);
+  if (m) wt_level_wav_unbind(h);
+  return rc;
 }
 
 void wt_wavelet_release(wt_handle* h) {
   if (!h || !h->wav) return;
   for (cudaEvent_t e : ctx(h)->ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx(h)->fork)
     if (e) cudaEventDestroy(e);
   for (cudaStream_t s : ctx(h)->side)
     if (s) cudaStreamDestroy(s);
@@ -250,6 +276,8 @@ int wt_wavelet_setup(wt_handle* h) {
   CKW(W->alloc(&W->thr, (size_t)3 * nz));
   for (cudaStream_t& s : W->side) CKW(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   for (cudaEvent_t& e : W->ev) CKW(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  W->fork.assign(W->L.size(), nullptr);
+  for (cudaEvent_t& e : W->fork) CKW(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   zero_wavelets(h);
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
@@ -500,12 +528,12 @@ int wt_wt_after_step(wt_handle* h) {
 
 }  // extern "C"
 
-int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd, int nz) {
+int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double* chd, int nz, cudaStream_t stream) {
   WLev P = view(h, level), C = view(h, level + 1);
   P.scal = par;
   C.scal = const_cast<double*>(chd);
   const int m = h->at(level).n + 1;
-  k_restr_scalar<<<nb((int64_t)nz * 10 * m * m), TPB, 0, h->stream>>>(P, C, nz);
+  k_restr_scalar<<<nb((int64_t)nz * 10 * m * m), TPB, 0, stream ? stream : h->stream>>>(P, C, nz);
   CKW(cudaGetLastError());
   return WT_OK;
 }

@@ -239,64 +239,71 @@ __device__ __forceinline__ void sm_make(SmTerm& t, const WLev& C, int d, int i, 
   }
 }
 
-// Minimum resident blocks per SM of k_restr_flux2 (register cap).  Measured on
-// B200 (restriction into one level of J4..J7 x 16): no cap (127 registers)
-// 0.115 ms, 3 blocks 0.087 ms, 4 blocks (64 registers, spilling to L1) 0.079 ms.
-#ifndef RF_MINB
-#define RF_MINB 4
-#endif
-__global__ void __launch_bounds__(256, RF_MINB) k_restr_flux2(WLev P, WLev C, int nz, int lpt, double* __restrict__ fp0,
-                                                     double* __restrict__ fp1, const double* __restrict__ fc0,
-                                                     const double* __restrict__ fc1, const double* __restrict__ dc0,
-                                                     const double* __restrict__ dc1) {
+// flux_cpt_restr in two parts.  Everything of a parent edge's restriction that
+// does not depend on the layer (remap codes of the child stencil, R_F_wgt, the
+// overlap-area factors of part_coarse_flux and coarse_flux) is geometry, so
+// k_rf_plan computes it once per hierarchy into a plan (structure of arrays
+// over the parent edges u = ((e*10 + d)*m + jp)*m + ip, m = n_par); the
+// per-step kernel k_restr_flux3 stages 32 edges' plans in shared memory and
+// evaluates the layers with few live registers.
+// int slots: the small fluxes sm[e] (0-8: a, p, m) and sm[e+1] (9-17), the six
+// edge codes of part_coarse_flux (18-23: UPZ, UMZ, VMM, WMP, WPM, VPP), the node
+// codes MP, PP, PM, MM (24-27), MZ, PZ (28-29), MM2, PM2, PP2, MP2 (30-33).
+// double slots: w0, w1 of sm[e] (0-5) and sm[e+1] (6-11); ar0, ar1, o0-o3
+// (12-17); the coarse_flux weights c, wpp/2, wpm/2, wmp/2, wmm/2 (18-22).
+constexpr int RF_NI = 34, RF_ND = 23;
+
+__global__ void k_rf_plan(WLev P, WLev C, int* __restrict__ pi, double* __restrict__ pd) {
   const int m = P.n;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t per = (int64_t)3 * 10 * m * m;  // parent edges per layer group
-  const int ng = (nz + lpt - 1) / lpt;
-  if (t >= per * ng) return;
-  const int g = (int)(t / per);
-  const int64_t u = t - (int64_t)g * per;
+  const int64_t ne = (int64_t)3 * 10 * m * m;
+  const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= ne) return;
   const int ip = (int)(u % m), jp = (int)((u / m) % m), d = (int)((u / ((int64_t)m * m)) % 10);
   const int e = (int)(u / ((int64_t)10 * m * m));
-  const int k0 = g * lpt, k1 = min(nz, k0 + lpt);
-  const int idp = nid(P, d, ip, jp);
-  if (P.mask_e[e * P.NN + idp] < M_RESTRCT) return;
   const int ic = 2 * ip, jc = 2 * jp;
-  // the two small fluxes of the edge: RT sm0, sm1; DG sm1, sm2; UP sm2, sm3
+  int ci_[RF_NI];
+  double cd[RF_ND];
   SmTerm sa, sb;
   sm_make(sa, C, d, ic, jc, e);
   sm_make(sb, C, d, ic, jc, e + 1);
-  // child node of the edge
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    ci_[q] = sa.a[q]; ci_[3 + q] = sa.p[q]; ci_[6 + q] = sa.m[q];
+    ci_[9 + q] = sb.a[q]; ci_[12 + q] = sb.p[q]; ci_[15 + q] = sb.m[q];
+    cd[q] = sa.w0[q]; cd[3 + q] = sa.w1[q]; cd[6 + q] = sb.w0[q]; cd[9 + q] = sb.w1[q];
+  }
   const int ci = (e == UP) ? ic : ic + 1, cj = (e == RT) ? jc : jc + 1;
   const RInd r = get_indices(ci, cj, e);
-  // part_coarse_flux constants
+  // part_coarse_flux
   const RChild G{C, nullptr, nullptr, d};
   double ar0 = G.a(ci, cj, 0), ar1 = G.a(ci, cj, 1);
   double o0 = G.sp(ci, cj, 0), o1 = G.sp(ci, cj, 1);
   double o2 = G.a(ci, cj, 2) - o0, o3 = G.a(ci, cj, 3) - o1;
   ar0 = ar0 + o0 + o3;
   ar1 = ar1 + o1 + o2;
-  const double s = ar0 + ar1;
-  ar0 = ar0 / s;
-  ar1 = ar1 / s;
+  const double sum = ar0 + ar1;
+  ar0 = ar0 / sum;
+  ar1 = ar1 / sum;
   const int mpi = r.ni[0], mpj = r.nj[0], ppi = r.ni[1], ppj = r.nj[1];
   const int pmi = r.ni[2], pmj = r.nj[2], mmi = r.ni[3], mmj = r.nj[3];
   o0 = G.sp(ppi, ppj, 0);
   o1 = G.sp(mmi, mmj, 1);
   o2 = G.a(mpi, mpj, 2) - G.sp(mpi, mpj, 0);
   o3 = G.a(pmi, pmj, 3) - G.sp(pmi, pmj, 1);
-  const int cUPZ = ecode(C, d, r.ei[S_UPZ], r.ej[S_UPZ], r.ee[S_UPZ]);
-  const int cUMZ = ecode(C, d, r.ei[S_UMZ], r.ej[S_UMZ], r.ee[S_UMZ]);
-  const int cVMM = ecode(C, d, r.ei[S_VMM], r.ej[S_VMM], r.ee[S_VMM]);
-  const int cWMP = ecode(C, d, r.ei[S_WMP], r.ej[S_WMP], r.ee[S_WMP]);
-  const int cWPM = ecode(C, d, r.ei[S_WPM], r.ej[S_WPM], r.ee[S_WPM]);
-  const int cVPP = ecode(C, d, r.ei[S_VPP], r.ej[S_VPP], r.ee[S_VPP]);
-  const int nMP = ncode(C, d, mpi, mpj), nPP = ncode(C, d, ppi, ppj);
-  const int nPM = ncode(C, d, pmi, pmj), nMM = ncode(C, d, mmi, mmj);
-  // coarse_flux constants (the neighbours mp, pp, pm, mm are part_coarse_flux's MP, PP, PM, MM)
+  const int es[6] = {S_UPZ, S_UMZ, S_VMM, S_WMP, S_WPM, S_VPP};
+#pragma unroll
+  for (int q = 0; q < 6; ++q) ci_[18 + q] = ecode(C, d, r.ei[es[q]], r.ej[es[q]], r.ee[es[q]]);
+  ci_[24] = ncode(C, d, mpi, mpj);
+  ci_[25] = ncode(C, d, ppi, ppj);
+  ci_[26] = ncode(C, d, pmi, pmj);
+  ci_[27] = ncode(C, d, mmi, mmj);
+  cd[12] = ar0; cd[13] = ar1; cd[14] = o0; cd[15] = o1; cd[16] = o2; cd[17] = o3;
+  // coarse_flux (the neighbours mp, pp, pm, mm are part_coarse_flux's MP, PP, PM, MM)
   const int hs = c_hex_s_offs[e];
-  const int mzi = ci + c_nghb_pt[hs + 1][0], mzj = cj + c_nghb_pt[hs + 1][1];
-  const int pzi = ci + c_nghb_pt[hs + 4][0], pzj = cj + c_nghb_pt[hs + 4][1];
+  ci_[28] = ncode(C, d, ci + c_nghb_pt[hs + 1][0], cj + c_nghb_pt[hs + 1][1]);
+  ci_[29] = ncode(C, d, ci + c_nghb_pt[hs + 4][0], cj + c_nghb_pt[hs + 4][1]);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) ci_[30 + q] = ncode(C, d, ci + c_bfly_no2[e][q][0], cj + c_bfly_no2[e][q][1]);
   const double wpp = G.a(ppi, ppj, 2) * G.a(ppi, ppj, 3) * G.hi(ppi, ppj);
   const double wpm = G.a(pmi, pmj, 2) * G.a(pmi, pmj, 3) * G.hi(pmi, pmj);
   const double wmp = G.a(mpi, mpj, 2) * G.a(mpi, mpj, 3) * G.hi(mpi, mpj);
@@ -306,35 +313,88 @@ __global__ void __launch_bounds__(256, RF_MINB) k_restr_flux2(WLev P, WLev C, in
   cc = cc + G.a(ppi, ppj, 0) * G.a(ppi, ppj, 2) * G.hi(ppi, ppj);
   cc = cc + G.a(pmi, pmj, 0) * G.a(pmi, pmj, 3) * G.hi(pmi, pmj);
   cc = cc + G.a(mmi, mmj, 1) * G.a(mmi, mmj, 3) * G.hi(mmi, mmj);
-  const double hpp = wpp * 0.5, hpm = wpm * 0.5, hmp = wmp * 0.5, hmm = wmm * 0.5;
-  const int nMZ = ncode(C, d, mzi, mzj), nPZ = ncode(C, d, pzi, pzj);
-  const int nMM2 = ncode(C, d, ci + c_bfly_no2[e][0][0], cj + c_bfly_no2[e][0][1]);
-  const int nPM2 = ncode(C, d, ci + c_bfly_no2[e][1][0], cj + c_bfly_no2[e][1][1]);
-  const int nPP2 = ncode(C, d, ci + c_bfly_no2[e][2][0], cj + c_bfly_no2[e][2][1]);
-  const int nMP2 = ncode(C, d, ci + c_bfly_no2[e][3][0], cj + c_bfly_no2[e][3][1]);
-  const int64_t so = (int64_t)e * P.NN + idp;
-  for (int k = k0; k < k1; ++k) {
+  cd[18] = cc; cd[19] = wpp * 0.5; cd[20] = wpm * 0.5; cd[21] = wmp * 0.5; cd[22] = wmm * 0.5;
+#pragma unroll
+  for (int q = 0; q < RF_NI; ++q) pi[q * ne + u] = ci_[q];
+#pragma unroll
+  for (int q = 0; q < RF_ND; ++q) pd[q * ne + u] = cd[q];
+}
+
+// One small flux of interp_flux from the staged plan: slots a at ia (9 codes)
+// and wd (6 weights) of edge x, sign pos.
+__device__ __forceinline__ double sm_eval_s(const int (*si)[32], const double (*sd)[32], int ia, int wd, int x,
+                                            bool pos, const double* __restrict__ h) {
+  double s1 = fe(h, si[ia + 0][x]) * sd[wd + 0][x];
+  s1 = s1 + fe(h, si[ia + 1][x]) * sd[wd + 1][x];
+  s1 = s1 + fe(h, si[ia + 2][x]) * sd[wd + 2][x];
+  double s2 = (fe(h, si[ia + 3][x]) - fe(h, si[ia + 6][x])) * sd[wd + 3][x];
+  s2 = s2 + (fe(h, si[ia + 4][x]) - fe(h, si[ia + 7][x])) * sd[wd + 4][x];
+  s2 = s2 + (fe(h, si[ia + 5][x]) - fe(h, si[ia + 8][x])) * sd[wd + 5][x];
+  return pos ? s1 + s2 : -s1 - s2;
+}
+
+// flux_cpt_restr of up to two fluxes (mass, Theta: fp0/fp1 from the child's
+// fc0/fc1 and dscalar dc0/dc1) on the restricted parent edges (mask_e >=
+// RESTRCT).  Block (32, ny): 32 consecutive parent edges of the plan, ny
+// threads per edge taking layers y, y + ny, ...; blocks without a restricted
+// edge return before staging.  Same expression trees and operand order as
+// part_coarse_flux + coarse_flux + interp_flux of the reference.
+__global__ void __launch_bounds__(256) k_restr_flux3(WLev P, int m, int nz, const int* __restrict__ pi,
+                                                     const double* __restrict__ pd, double* __restrict__ fp0,
+                                                     double* __restrict__ fp1, const double* __restrict__ fc0,
+                                                     const double* __restrict__ fc1, const double* __restrict__ dc0,
+                                                     const double* __restrict__ dc1, int NNc) {
+  __shared__ int si[RF_NI][32];
+  __shared__ double sd[RF_ND][32];
+  const int64_t ne = (int64_t)3 * 10 * m * m;
+  const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
+  const int64_t u0 = (int64_t)blockIdx.x * 32;
+  const int64_t u = u0 + x;
+  int ip = 0, jp = 0, d = 0, e = 0;
+  bool on = false;
+  if (u < ne) {
+    ip = (int)(u % m);
+    jp = (int)((u / m) % m);
+    d = (int)((u / ((int64_t)m * m)) % 10);
+    e = (int)(u / ((int64_t)10 * m * m));
+    on = P.mask_e[e * P.NN + nid(P, d, ip, jp)] >= M_RESTRCT;
+  }
+  if (!__syncthreads_or(on)) return;
+  const int nv = (int)min((int64_t)32, ne - u0);
+  for (int q = y; q < RF_NI + RF_ND; q += ny)
+    if (x < nv) {
+      if (q < RF_NI)
+        si[q][x] = pi[q * ne + u];
+      else
+        sd[q - RF_NI][x] = pd[(q - RF_NI) * ne + u];
+    }
+  __syncthreads();
+  if (!on) return;
+  const bool pa = (e & 1) != 0, pb = ((e + 1) & 1) != 0;
+  const int64_t so = (int64_t)e * P.NN + nid(P, d, ip, jp);
+  const double ar0 = sd[12][x], ar1 = sd[13][x], o0 = sd[14][x], o1 = sd[15][x], o2 = sd[16][x], o3 = sd[17][x];
+  for (int k = y; k < nz; k += ny) {
 #pragma unroll
     for (int f = 0; f < 2; ++f) {
       double* __restrict__ fp = f == 0 ? fp0 : fp1;
       if (!fp) continue;
-      const double* __restrict__ h = (f == 0 ? fc0 : fc1) + (int64_t)3 * k * C.NN;
-      const double* __restrict__ ds = (f == 0 ? dc0 : dc1) + (int64_t)k * C.NN;
-      const double sma = sm_eval(sa, h), smb = sm_eval(sb, h);
-      double tp = fe(h, cUPZ) * ar0;
-      tp = tp + fe(h, cUMZ) * ar1;
-      tp = tp - (fe(h, cVMM) + fe(h, cWMP)) * ar1;
-      tp = tp - (fe(h, cWPM) + fe(h, cVPP)) * ar0;
-      tp = tp + o2 * fn(ds, nMP);
-      tp = tp - o3 * fn(ds, nPM);
-      tp = tp - o0 * fn(ds, nPP);
-      tp = tp + o1 * fn(ds, nMM);
-      const double dmz = fn(ds, nMZ), dpz = fn(ds, nPZ);
-      double tc = cc * (dpz - dmz);
-      tc = tc + hpp * (fn(ds, nPP2) - dmz);
-      tc = tc + hpm * (fn(ds, nPM2) - dmz);
-      tc = tc + hmp * (dpz - fn(ds, nMP2));
-      tc = tc + hmm * (dpz - fn(ds, nMM2));
+      const double* __restrict__ h = (f == 0 ? fc0 : fc1) + (int64_t)3 * k * NNc;
+      const double* __restrict__ ds = (f == 0 ? dc0 : dc1) + (int64_t)k * NNc;
+      const double sma = sm_eval_s(si, sd, 0, 0, x, pa, h), smb = sm_eval_s(si, sd, 9, 6, x, pb, h);
+      double tp = fe(h, si[18][x]) * ar0;
+      tp = tp + fe(h, si[19][x]) * ar1;
+      tp = tp - (fe(h, si[20][x]) + fe(h, si[21][x])) * ar1;
+      tp = tp - (fe(h, si[22][x]) + fe(h, si[23][x])) * ar0;
+      tp = tp + o2 * fn(ds, si[24][x]);
+      tp = tp - o3 * fn(ds, si[26][x]);
+      tp = tp - o0 * fn(ds, si[25][x]);
+      tp = tp + o1 * fn(ds, si[27][x]);
+      const double dmz = fn(ds, si[28][x]), dpz = fn(ds, si[29][x]);
+      double tc = sd[18][x] * (dpz - dmz);
+      tc = tc + sd[19][x] * (fn(ds, si[32][x]) - dmz);
+      tc = tc + sd[20][x] * (fn(ds, si[31][x]) - dmz);
+      tc = tc + sd[21][x] * (dpz - fn(ds, si[33][x]));
+      tc = tc + sd[22][x] * (dpz - fn(ds, si[30][x]));
       fp[(int64_t)3 * k * P.NN + so] = tp + tc + sma + smb;
     }
   }

@@ -18,6 +18,8 @@ struct WavLevel {
   int *mask_n = nullptr, *mask_e = nullptr;
   double *scal = nullptr, *dscal = nullptr, *flux = nullptr, *dvelo = nullptr;  // work fields, on first use
   double *mean_m = nullptr, *mean_t = nullptr;  // layer means below level_end, on first use
+  int* rf_pi = nullptr;     // flux-restriction plan into this level (k_rf_plan), below level_end
+  double* rf_pd = nullptr;
   bool own_scaling = false;
 };
 

@@ -274,6 +274,18 @@ int wt_wavelet_setup(wt_handle* h) {
     CKW(cudaMemcpy(V.mask_e, tol.data(), 3 * D.NN * sizeof(int), cudaMemcpyHostToDevice));
   }
   CKW(W->alloc(&W->thr, (size_t)3 * nz));
+  // flux-restriction plans of every parent level whose child has R_F_wgt
+  for (int l = h->level_start; l < h->level_end; ++l) {
+    const DevLevel& Dc = h->at(l + 1);
+    if (!Dc.rf_wgt || !Dc.overl_split) continue;
+    WavLevel& V = W->L[l - h->level_start];
+    const int m = h->at(l).n;
+    const int64_t ne = (int64_t)3 * 10 * m * m;
+    CKW(W->alloc(&V.rf_pi, (size_t)RF_NI * ne));
+    CKW(W->alloc(&V.rf_pd, (size_t)RF_ND * ne));
+    k_rf_plan<<<nb(ne), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), V.rf_pi, V.rf_pd);
+    CKW(cudaGetLastError());
+  }
   for (cudaStream_t& s : W->side) CKW(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   for (cudaEvent_t& e : W->ev) CKW(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   W->fork.assign(W->L.size(), nullptr);
@@ -538,15 +550,26 @@ int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double*
   return WT_OK;
 }
 
-int wt_level_restrict_flux(wt_handle* h, int level, double* par0, double* par1, const double* chd0,
-                           const double* chd1, const double* dsc0, const double* dsc1, int nz) {
-  if (!h->at(level + 1).rf_wgt || !h->at(level + 1).overl_split) return WT_ERR_ARG;
-  const int m = h->at(level).n, lpt = lpt_for(nz);
-  const int64_t n = (int64_t)3 * 10 * m * m * ((nz + lpt - 1) / lpt);
-  k_restr_flux2<<<nb(n), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), nz, lpt, par0, par1, chd0, chd1,
-                                              dsc0, dsc1);
+namespace {
+// flux_cpt_restr of parent `level` from the plan built at setup (k_rf_plan).
+int restrict_flux(wt_handle* h, int level, double* par0, double* par1, const double* chd0, const double* chd1,
+                  const double* dsc0, const double* dsc1, int nz) {
+  const WavLevel& V = ctx(h)->L[level - h->level_start];
+  if (!V.rf_pi) return WT_ERR_ARG;
+  const int m = h->at(level).n;
+  const int64_t ne = (int64_t)3 * 10 * m * m;
+  const dim3 blk(32, std::min(nz, 8));
+  k_restr_flux3<<<(unsigned)((ne + 31) / 32), blk, 0, h->stream>>>(view(h, level), m, nz, V.rf_pi, V.rf_pd, par0,
+                                                                    par1, chd0, chd1, dsc0, dsc1,
+                                                                    (int)h->at(level + 1).NN);
   CKW(cudaGetLastError());
   return WT_OK;
+}
+}  // namespace
+
+int wt_level_restrict_flux(wt_handle* h, int level, double* par0, double* par1, const double* chd0,
+                           const double* chd1, const double* dsc0, const double* dsc1, int nz) {
+  return restrict_flux(h, level, par0, par1, chd0, chd1, dsc0, dsc1, nz);
 }
 
 extern "C" {
@@ -576,12 +599,8 @@ int wt_restrict_scalar(wt_handle* h, int level) {
 
 int wt_restrict_flux(wt_handle* h, int level) {
   if (int rc = restrict_pair(h, level, {WT_WORK_FLUX, WT_WORK_DSCALAR})) return rc;
-  if (!h->at(level + 1).rf_wgt || !h->at(level + 1).overl_split) return WT_ERR_ARG;
   const WLev P = view(h, level), C = view(h, level + 1);
-  const int m = h->at(level).n, lpt = lpt_for(h->nz);
-  const int64_t n = (int64_t)3 * 10 * m * m * ((h->nz + lpt - 1) / lpt);
-  k_restr_flux2<<<nb(n), TPB, 0, h->stream>>>(P, C, h->nz, lpt, P.flux, nullptr, C.flux, nullptr, C.dscal, nullptr);
-  CKW(cudaGetLastError());
+  if (int rc = restrict_flux(h, level, P.flux, nullptr, C.flux, nullptr, C.dscal, nullptr, h->nz)) return rc;
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
 }

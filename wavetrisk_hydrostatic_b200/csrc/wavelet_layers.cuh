@@ -296,36 +296,6 @@ __global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa,
   }
 }
 
-// Reconstruct_outer_velo (src/wavelet.f90:954-976), parents [0, np]^2, then
-// Reconstruct_velo_penta by the corner parents.
-__global__ void __launch_bounds__(128, WL_MINB_OUTER) k_recon_outer_l(WLev Pa, WLev C, int nz, int lpt) {
-  int d, ip, jp;
-  int k0, k1;
-  if (!parent_of(Pa.n + 1, nz, lpt, d, ip, jp, k0, k1)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  for (int e = 0; e < 3; ++e) {
-    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
-    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
-    OuterInterp O;
-    outer_interp(O, Pa, C, d, ip, jp, a2, b2, e);
-    const int cw = we_code(C, e, d, a2, b2);
-    const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
-    for (int k = k0; k < k1; ++k) {
-      const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
-      const double* wc = C.wv + (int64_t)k * 3 * C.NN;
-      double* v = C.sv + (int64_t)k * 3 * C.NN;
-      double t0;
-      const double u = outer_eval(O, vp, t0);
-      const double v2 = u + we(wc, cw);
-      v[x2] = v2;
-      v[x1] = 2.0 * t0 - v2;
-    }
-  }
-  if ((ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1))
-    for (int k = k0; k < k1; ++k)
-      penta_reconstruct(Pa, C, Pa.sv + (int64_t)k * 3 * Pa.NN, C.sv + (int64_t)k * 3 * C.NN, d, ip, jp);
-}
-
 // Interp_inner_velo (src/wavelet.f90:1005-1062) of parent (ip, jp): parent
 // circulation terms and the six inner child edges' coefficients.
 struct InnerInterp {
@@ -430,21 +400,212 @@ __global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa,
   }
 }
 
-// Reconstruct_inner_velo (src/wavelet.f90:978-1003), parents [0, np)^2.
-__global__ void __launch_bounds__(128, WL_MINB_INNER) k_recon_inner_l(WLev Pa, WLev C, int nz, int lpt) {
-  int d, ip, jp;
-  int k0, k1;
-  if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
+// ---------------------------------------------------------------------------
+// Velocity reconstruction from per-parent plans.  Everything of
+// Interp_outer_velo and Interp_inner_velo that does not depend on the layer
+// (remap codes of the parent and child edges, the outer weights Iu_Base_Wgt +
+// I_u_wgt, lengths and triangle areas) is geometry: k_outer_plan and
+// k_inner_plan store it once per hierarchy (structure of arrays over the
+// parents), and the reconstruction kernels stage 32 parents' plans in shared
+// memory.  Block (32, ny): 32 consecutive parents, ny threads per parent taking
+// layers y, y + ny, ...  Same expression trees and operand order as the
+// reference's routines.  Measured on B200 against the per-thread kernels
+// (k_*_l): inverse transform J5..J7 x 16 0.247 vs 0.266 ms, J6..J8 x 32 1.62 vs
+// 1.81 ms; the same plans in the forward wavelet kernels were slower (J5..J7 x
+// 16 forward 0.459 vs 0.429 ms), so those resolve the geometry per thread.
+//
+// Outer plan, parents [0, np]^2 (u = (d*(np+1) + jp)*(np+1) + ip): per edge e
+// int slots e*14 + (0-12: Interp_outer_velo's parent codes, 13: the child edge
+// (a2, b2)'s code), double slots e*9 + (0-8: weights).
+constexpr int OP_NI = 42, OP_ND = 27;
+// Minimum resident blocks per SM of the inner-edge plan kernels (register cap):
+// uncapped they take about 148 registers, one block per SM.
+#ifndef WL_PLAN_MINB
+#define WL_PLAN_MINB 2
+#endif
+// Inner plan, parents [0, np)^2 (u = (d*np + jp)*np + ip): int slots parent
+// codes (0-4), child circulation codes (5-14), target codes (15-20); double
+// slots parent lengths (0-4), parent areas (5-6), child lengths (7-16), child
+// areas (17-22), target lengths (23-28).
+constexpr int IP_NI = 21, IP_ND = 29;
+
+__global__ void k_outer_plan(WLev Pa, WLev C, int* __restrict__ pi, double* __restrict__ pd) {
+  const int m = Pa.n + 1;
+  const int64_t ne = (int64_t)10 * m * m;
+  const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= ne) return;
+  const int d = (int)(u / ((int64_t)m * m)), r = (int)(u - (int64_t)d * m * m);
+  const int jp = r / m, ip = r - jp * m;
+  const int i = 2 * ip, j = 2 * jp;
+  for (int e = 0; e < 3; ++e) {
+    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
+    OuterInterp O;
+    outer_interp(O, Pa, C, d, ip, jp, a2, b2, e);
+#pragma unroll
+    for (int q = 0; q < 13; ++q) pi[(e * 14 + q) * ne + u] = O.c[q];
+    pi[(e * 14 + 13) * ne + u] = we_code(C, e, d, a2, b2);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) pd[(e * 9 + q) * ne + u] = O.w[q];
+  }
+}
+
+__global__ void k_inner_plan(WLev Pa, WLev C, int* __restrict__ pi, double* __restrict__ pd) {
+  const int m = Pa.n;
+  const int64_t ne = (int64_t)10 * m * m;
+  const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= ne) return;
+  const int d = (int)(u / ((int64_t)m * m)), r = (int)(u - (int64_t)d * m * m);
+  const int jp = r / m, ip = r - jp * m;
   InnerInterp I;
   inner_interp(I, Pa, C, d, ip, jp);
-  for (int k = k0; k < k1; ++k) {
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    pi[q * ne + u] = I.cp[q];
+    pd[q * ne + u] = I.lp[q];
+  }
+  pd[5 * ne + u] = I.tp[0];
+  pd[6 * ne + u] = I.tp[1];
+#pragma unroll
+  for (int q = 0; q < 10; ++q) {
+    pi[(5 + q) * ne + u] = I.cc[q];
+    pd[(7 + q) * ne + u] = I.lc[q];
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    pi[(15 + q) * ne + u] = I.ct[q];
+    pd[(17 + q) * ne + u] = I.tc[q];
+    pd[(23 + q) * ne + u] = I.den[q];
+  }
+}
+
+// Stage slots [0, ni) and [0, nd) of the plan rows u0 .. u0+31 (nv valid).
+template <int NI, int ND>
+__device__ __forceinline__ void stage_plan(int (*si)[32], double (*sd)[32], const int* __restrict__ pi,
+                                           const double* __restrict__ pd, int64_t ne, int64_t u0, int nv) {
+  const int x = threadIdx.x;
+  if (x < nv)
+    for (int q = threadIdx.y; q < NI + ND; q += blockDim.y) {
+      if (q < NI)
+        si[q][x] = pi[q * ne + u0 + x];
+      else
+        sd[q - NI][x] = pd[(q - NI) * ne + u0 + x];
+    }
+}
+
+// Interp_outer_velo of edge e of staged parent x (outer_eval's expression).
+__device__ __forceinline__ double outer_eval_s(const int (*si)[32], const double (*sd)[32], int e, int x,
+                                               const double* __restrict__ vp, double& t0) {
+  const int b = e * 14, w = e * 9;
+  double t[9];
+  t[0] = we(vp, si[b + 0][x]);
+  t[1] = we(vp, si[b + 1][x]);
+  t[2] = we(vp, si[b + 2][x]);
+  t[3] = we(vp, si[b + 3][x]);
+  t[4] = we(vp, si[b + 4][x]);
+  t[5] = we(vp, si[b + 5][x]) - we(vp, si[b + 6][x]);
+  t[6] = we(vp, si[b + 7][x]) - we(vp, si[b + 8][x]);
+  t[7] = we(vp, si[b + 9][x]) - we(vp, si[b + 10][x]);
+  t[8] = we(vp, si[b + 11][x]) - we(vp, si[b + 12][x]);
+  t0 = t[0];
+  double sum = 0.0;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) sum = sum + sd[w + q][x] * t[q];
+  return sum;
+}
+
+// Interp_inner_velo of staged parent x (inner_eval's expression).
+__device__ __forceinline__ void inner_eval_s(const int (*si)[32], const double (*sd)[32], int x,
+                                             const double* __restrict__ vp, const double* __restrict__ v,
+                                             double u[6]) {
+  const double pDG = we(vp, si[0][x]) * sd[0][x];
+  const double curl0 = (pDG + we(vp, si[1][x]) * sd[1][x] + we(vp, si[2][x]) * sd[2][x]) / sd[5][x];
+  const double curl1 = (pDG + we(vp, si[3][x]) * sd[3][x] + we(vp, si[4][x]) * sd[4][x]) / sd[6][x];
+  double pr[10];
+#pragma unroll
+  for (int q = 0; q < 10; ++q) pr[q] = we(v, si[5 + q][x]) * sd[7 + q][x];
+  u[0] = (sd[17][x] * curl0 - pr[0] - pr[1]) / sd[23][x];
+  u[1] = (sd[18][x] * curl0 - pr[2] - pr[3]) / sd[24][x];
+  u[2] = (sd[19][x] * curl0 - pr[4] - pr[5]) / sd[25][x];
+  u[3] = (sd[20][x] * curl1 - pr[6] - pr[1]) / sd[26][x];
+  u[4] = (sd[21][x] * curl1 - pr[7] - pr[8]) / sd[27][x];
+  u[5] = (sd[22][x] * curl1 - pr[4] - pr[9]) / sd[28][x];
+}
+
+// Parent (d, ip, jp) of plan row u over [0, m)^2.
+__device__ __forceinline__ void plan_parent(int64_t u, int m, int& d, int& ip, int& jp) {
+  d = (int)(u / ((int64_t)m * m));
+  const int r = (int)(u - (int64_t)d * m * m);
+  jp = r / m;
+  ip = r - jp * m;
+}
+
+// Reconstruct_outer_velo (src/wavelet.f90:954-976) from the outer plan,
+// parents [0, np]^2, then Reconstruct_velo_penta by the corner parents.
+__global__ void __launch_bounds__(256) k_recon_outer_p(WLev Pa, WLev C, int nz, const int* __restrict__ pi,
+                                                       const double* __restrict__ pd) {
+  __shared__ int si[OP_NI][32];
+  __shared__ double sd[OP_ND][32];
+  const int np = Pa.n, m = np + 1;
+  const int64_t ne = (int64_t)10 * m * m, u0 = (int64_t)blockIdx.x * 32;
+  const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
+  stage_plan<OP_NI, OP_ND>(si, sd, pi, pd, ne, u0, (int)min((int64_t)32, ne - u0));
+  __syncthreads();
+  if (u0 + x >= ne) return;
+  int d, ip, jp;
+  plan_parent(u0 + x, m, d, ip, jp);
+  const int i = 2 * ip, j = 2 * jp;
+  for (int e = 0; e < 3; ++e) {
+    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
+    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
+    const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
+    const int cw = si[e * 14 + 13][x];
+    for (int k = y; k < nz; k += ny) {
+      const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+      const double* wc = C.wv + (int64_t)k * 3 * C.NN;
+      double* v = C.sv + (int64_t)k * 3 * C.NN;
+      double t0;
+      const double uu = outer_eval_s(si, sd, e, x, vp, t0);
+      const double v2 = uu + we(wc, cw);
+      v[x2] = v2;
+      v[x1] = 2.0 * t0 - v2;
+    }
+  }
+  if ((ip == 0 || ip == np - 1) && (jp == 0 || jp == np - 1))
+    for (int k = y; k < nz; k += ny)
+      penta_reconstruct(Pa, C, Pa.sv + (int64_t)k * 3 * Pa.NN, C.sv + (int64_t)k * 3 * C.NN, d, ip, jp);
+}
+
+// target edges of the inner plan: UP(i+1,j) DG(i+1,j) RT(i+1,j+1) RT(i,j+1) DG(i,j+1) UP(i+1,j+1)
+__device__ __forceinline__ int inner_target(const WLev& C, int q, int d, int i, int j) {
+  const int ge[6] = {UP, DG, RT, RT, DG, UP};
+  const int gi[6] = {i + 1, i + 1, i + 1, i, i, i + 1};
+  const int gj[6] = {j, j, j + 1, j + 1, j + 1, j + 1};
+  return ge[q] * C.NN + nid(C, d, gi[q], gj[q]);
+}
+
+// Reconstruct_inner_velo (src/wavelet.f90:978-1003) from the inner plan,
+// parents [0, np)^2.
+__global__ void __launch_bounds__(256, WL_PLAN_MINB) k_recon_inner_p(WLev Pa, WLev C, int nz, const int* __restrict__ pi,
+                                                       const double* __restrict__ pd) {
+  __shared__ int si[IP_NI][32];
+  __shared__ double sd[IP_ND][32];
+  const int m = Pa.n;
+  const int64_t ne = (int64_t)10 * m * m, u0 = (int64_t)blockIdx.x * 32;
+  const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
+  stage_plan<IP_NI, IP_ND>(si, sd, pi, pd, ne, u0, (int)min((int64_t)32, ne - u0));
+  __syncthreads();
+  if (u0 + x >= ne) return;
+  int d, ip, jp;
+  plan_parent(u0 + x, m, d, ip, jp);
+  const int i = 2 * ip, j = 2 * jp;
+  for (int k = y; k < nz; k += ny) {
     const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
     const double* wc = C.wv + (int64_t)k * 3 * C.NN;
     double* v = C.sv + (int64_t)k * 3 * C.NN;
-    double u[6];
-    inner_eval(I, vp, v, u);
+    double uu[6];
+    inner_eval_s(si, sd, x, vp, v, uu);
 #pragma unroll
-    for (int q = 0; q < 6; ++q) v[I.xt[q]] = u[q] + we(wc, I.ct[q]);
+    for (int q = 0; q < 6; ++q) v[inner_target(C, q, d, i, j)] = uu[q] + we(wc, si[15 + q][x]);
   }
 }
 

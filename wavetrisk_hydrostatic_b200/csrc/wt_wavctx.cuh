@@ -20,6 +20,10 @@ struct WavLevel {
   double *mean_m = nullptr, *mean_t = nullptr;  // layer means below level_end, on first use
   int* rf_pi = nullptr;     // flux-restriction plan into this level (k_rf_plan), below level_end
   double* rf_pd = nullptr;
+  int* op_i = nullptr;      // outer and inner velocity-wavelet plans of this level's parents
+  double* op_d = nullptr;   // (k_outer_plan, k_inner_plan), below level_end
+  int* ip_i = nullptr;
+  double* ip_d = nullptr;
   bool own_scaling = false;
 };
 

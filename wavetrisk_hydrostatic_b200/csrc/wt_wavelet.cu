@@ -117,6 +117,9 @@ void launch_scalar_wc(wt_handle* h, int l, cudaStream_t s) {
   k_scalar_wc_l<CMP><<<nbl((int64_t)10 * np * np, nz), TPBL, 0, s>>>(view(h, l + 1), np, nz, lpt_for(nz));
 }
 
+// Blocks of 32 plan rows by min(nz, 8) layer threads (the plan kernels).
+inline dim3 plan_block(int nz) { return dim3(32, std::min(nz, 8)); }
+inline unsigned plan_grid(int64_t rows) { return (unsigned)((rows + 31) / 32); }
 // Velocity wavelets of level l+1 (pentagon corrections included): outer edges
 // on s, inner edges on si (they read only the scaling fields).
 template <bool CMP>
@@ -143,8 +146,9 @@ void inverse(wt_handle* h) {
     const int64_t par1 = (int64_t)10 * (np + 1) * (np + 1), par0 = (int64_t)10 * np * np;
     k_prolong_l<<<nbl(par1, nz), TPBL, 0, sa>>>(P, C, nz, lpt_for(nz));
     k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, sa>>>(C, np, nz, lpt_for(nz));
-    k_recon_outer_l<<<nbl(par1, nz), TPBL, 0, s>>>(P, C, nz, lpt_for(nz));
-    k_recon_inner_l<<<nbl(par0, nz), TPBL, 0, s>>>(P, C, nz, lpt_for(nz));
+    const WavLevel& V = W->L[l - h->level_start];
+    k_recon_outer_p<<<plan_grid(par1), plan_block(nz), 0, s>>>(P, C, nz, V.op_i, V.op_d);
+    k_recon_inner_p<<<plan_grid(par0), plan_block(nz), 0, s>>>(P, C, nz, V.ip_i, V.ip_d);
   }
   cudaEventRecord(W->ev[1], sa);
   cudaStreamWaitEvent(s, W->ev[1], 0);
@@ -274,6 +278,19 @@ int wt_wavelet_setup(wt_handle* h) {
     CKW(cudaMemcpy(V.mask_e, tol.data(), 3 * D.NN * sizeof(int), cudaMemcpyHostToDevice));
   }
   CKW(W->alloc(&W->thr, (size_t)3 * nz));
+  // velocity-wavelet plans of every parent level
+  for (int l = h->level_start; l < h->level_end; ++l) {
+    WavLevel& V = W->L[l - h->level_start];
+    const int m = h->at(l).n;
+    const int64_t n1 = (int64_t)10 * (m + 1) * (m + 1), n0 = (int64_t)10 * m * m;
+    CKW(W->alloc(&V.op_i, (size_t)OP_NI * n1));
+    CKW(W->alloc(&V.op_d, (size_t)OP_ND * n1));
+    CKW(W->alloc(&V.ip_i, (size_t)IP_NI * n0));
+    CKW(W->alloc(&V.ip_d, (size_t)IP_ND * n0));
+    k_outer_plan<<<nb(n1), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), V.op_i, V.op_d);
+    k_inner_plan<<<nb(n0), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), V.ip_i, V.ip_d);
+    CKW(cudaGetLastError());
+  }
   // flux-restriction plans of every parent level whose child has R_F_wgt
   for (int l = h->level_start; l < h->level_end; ++l) {
     const DevLevel& Dc = h->at(l + 1);

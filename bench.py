@@ -304,11 +304,13 @@ def adaptive_launches(L):
     three restrictions per coarse level (Bernoulli, Exner, both fluxes),
     WT_after_step with three wavelet kernels per coarse level (scalar,
     outer and inner velocity, compression fused) and four inverse-transform
-    kernels per coarse level), wt_mask_build's sweeps (comm_masks launches
-    one kernel per level), compression and the inverse transform."""
+    kernels per coarse level), wt_mask_build's sweeps (each comm_masks is
+    one launch over all levels, 3L + 3 of them), compression and the inverse
+    transform."""
     stage = 3 * L + 3 * (L - 1) + 3 * (L - 1) + 4 * (L - 1)
-    masks = ((L - 1) + 1 + L + (L - 1) * (L + 2) + L + L + L + (L - 1) + L + L + 2 * (L - 1) + L
-             + (L - 2) * (2 + 2 * L) + (1 + L) + 2 * (L - 2) + 1 + L + L)
+    comm = 3 * L + 3
+    masks = ((L - 1) + 1 + 2 * (L - 1) + L + (L - 1) + 2 * (L - 1) + 2 * (L - 2) + 1 + 2 * (L - 2) + 1 + L
+             + comm)
     return 4 * stage + masks + (L - 1) + 4 * (L - 1)
 
 

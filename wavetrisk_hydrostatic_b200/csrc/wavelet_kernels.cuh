@@ -206,40 +206,6 @@ __device__ void penta_reconstruct(const WLev& Pa, const WLev& C, const double* v
   }
 }
 
-// mask_tol_vars (src/mask.f90:102-156) on nodes [st, n-1+en]^2 of one level,
-// all layers per thread.  thr[v*nz + k]: v = 0 mass, 1 Theta, 2 velocity.
-__global__ void k_mask_tol(WLev L, int nz, int st, int en, const double* __restrict__ thr, int below_fill) {
-  const int m = L.n + en - st;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)10 * m * m) return;
-  const int d = (int)(t / ((int64_t)m * m));
-  int r = (int)(t - (int64_t)d * m * m);
-  const int j = r / m + st, i = r % m + st;
-  if (!inr(L, i, j)) return;
-  const int x = nid(L, d, i, j);
-  if (L.mask_n[x] == FROZEN) return;
-  bool active = false;
-  for (int k = 0; k < nz; ++k) {
-    const double wm = rn(L, L.wm + (int64_t)k * L.NN, d, i, j), wt = rn(L, L.wt + (int64_t)k * L.NN, d, i, j);
-    if (fabs(wm) >= thr[0 * nz + k] || below_fill) active = true;
-    if (fabs(wt) >= thr[1 * nz + k] || below_fill) active = true;
-  }
-  if (active)
-    L.mask_n[x] = TOLRNZ;
-  else if (L.mask_n[x] > ADJZONE)
-    L.mask_n[x] = ADJZONE;
-  for (int e = 0; e < 3; ++e) {
-    active = false;
-    for (int k = 0; k < nz; ++k)
-      if (fabs(re(L, L.wv + (int64_t)k * 3 * L.NN, e, d, i, j)) >= thr[2 * nz + k] || below_fill) active = true;
-    int& me_ = L.mask_e[e * L.NN + x];
-    if (active)
-      me_ = TOLRNZ;
-    else if (me_ > ADJZONE)
-      me_ = ADJZONE;
-  }
-}
-
 // compress_scalar on nodes [0, n]^2 and compress_vector on [0, n)^2
 // (src/adapt.f90:79-232) of one level, one thread per (layer, node).
 __global__ void k_compress(WLev L, int nz) {
@@ -310,13 +276,89 @@ __device__ __forceinline__ bool node_of(int m, int st, int& d, int& i, int& j) {
 
 // serial comm_masks_mpi (src/comm.f90:531-553): node and edge masks to their
 // ghost copies (the tables have no chains, so the copy order is immaterial).
-__global__ void k_mask_halo(WLev g, const int2* __restrict__ hn, int n_hn, const int3* __restrict__ he, int n_he) {
+// The mask ghost copy of every level in one launch (comm_masks): thread t
+// belongs to the level q with start[q] <= t < start[q+1].
+constexpr int MH_MAXL = 16;
+struct MaskHaloSet {
+  int nl;
+  int start[MH_MAXL + 1];
+  int n_hn[MH_MAXL];
+  int* mask_n[MH_MAXL];
+  int* mask_e[MH_MAXL];
+  const int2* hn[MH_MAXL];
+  const int3* he[MH_MAXL];
+};
+__global__ void k_mask_halo_all(MaskHaloSet S) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n_hn) {
-    g.mask_n[hn[t].x] = g.mask_n[hn[t].y];
-  } else if (t < n_hn + n_he) {
-    const int3 e = he[t - n_hn];
-    g.mask_e[e.x] = g.mask_e[e.y];
+  if (t >= S.start[S.nl]) return;
+  int q = 0;
+  while (t >= S.start[q + 1]) ++q;
+  const int r = t - S.start[q];
+  if (r < S.n_hn[q]) {
+    const int2 c = S.hn[q][r];
+    S.mask_n[q][c.x] = S.mask_n[q][c.y];
+  } else {
+    const int3 c = S.he[q][r - S.n_hn[q]];
+    S.mask_e[q][c.x] = S.mask_e[q][c.y];
+  }
+}
+
+// mask_tol_vars (src/mask.f90:102-156) on nodes [st, n-1+en]^2 of one level:
+// block (32 nodes, ny), thread y tests layers y, y + ny, ... of the node's two
+// scalars and three edges (read through the ghost remaps), and the flags are
+// OR-ed in shared memory before the y = 0 thread updates the masks.
+// thr[v*nz + k]: v = 0 mass, 1 Theta, 2 velocity.
+__global__ void k_mask_tol_y(WLev L, int nz, int st, int en, const double* __restrict__ thr, int below_fill) {
+  __shared__ int fl[8][32];  // ny <= 8
+  const int m = L.n + en - st;
+  const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
+  const int64_t t = (int64_t)blockIdx.x * 32 + x;
+  bool in = t < (int64_t)10 * m * m;
+  int d = 0, i = 0, j = 0;
+  if (in) {
+    d = (int)(t / ((int64_t)m * m));
+    const int r = (int)(t - (int64_t)d * m * m);
+    j = r / m + st;
+    i = r % m + st;
+    in = inr(L, i, j);
+  }
+  int x_ = 0;
+  if (in) {
+    x_ = nid(L, d, i, j);
+    in = L.mask_n[x_] != FROZEN;
+  }
+  int f = 0;
+  if (in) {
+    const int cn = __ldg(L.nsrc + x_);
+    int ce[3];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) ce[e] = __ldg(L.esrc + e * L.NN + x_);
+    for (int k = y; k < nz; k += ny) {
+      const double wm = L.wm[(int64_t)k * L.NN + cn], wt = L.wt[(int64_t)k * L.NN + cn];
+      if (fabs(wm) >= thr[0 * nz + k] || below_fill) f |= 1;
+      if (fabs(wt) >= thr[1 * nz + k] || below_fill) f |= 1;
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        const int c = ce[e];
+        const double v = L.wv[(int64_t)k * 3 * L.NN + (c >> 1)];
+        if (fabs((c & 1) ? -v : v) >= thr[2 * nz + k] || below_fill) f |= 2 << e;
+      }
+    }
+  }
+  fl[y][x] = f;
+  __syncthreads();
+  if (y != 0 || !in) return;
+  for (int q = 1; q < ny; ++q) f |= fl[q][x];
+  if (f & 1)
+    L.mask_n[x_] = TOLRNZ;
+  else if (L.mask_n[x_] > ADJZONE)
+    L.mask_n[x_] = ADJZONE;
+  for (int e = 0; e < 3; ++e) {
+    int& me_ = L.mask_e[e * L.NN + x_];
+    if (f & (2 << e))
+      me_ = TOLRNZ;
+    else if (me_ > ADJZONE)
+      me_ = ADJZONE;
   }
 }
 

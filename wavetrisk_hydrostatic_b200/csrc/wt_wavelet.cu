@@ -404,6 +404,37 @@ int wt_inverse_wt(wt_handle* h) {
   return WT_OK;
 }
 
+}  // extern "C"
+
+namespace {
+void comm_masks(wt_handle* h) {
+  MaskHaloSet S{};
+  S.nl = h->level_end - h->level_start + 1;
+  for (int q = 0; q < S.nl; ++q) {
+    const DevLevel& D = h->at(h->level_start + q);
+    const WavLevel& V = ctx(h)->L[q];
+    S.n_hn[q] = D.n_hn;
+    S.mask_n[q] = V.mask_n;
+    S.mask_e[q] = V.mask_e;
+    S.hn[q] = D.hn;
+    S.he[q] = D.he;
+    S.start[q + 1] = S.start[q] + D.n_hn + D.n_he;
+  }
+  k_mask_halo_all<<<nb(S.start[S.nl]), TPB, 0, h->stream>>>(S);
+}
+// mask_tol_vars of level l on nodes [st, n-1+en]^2
+void mask_tol(wt_handle* h, int l, int st, int en, int level_fill) {
+  const int m = h->at(l).n + en - st;
+  const dim3 blk(32, std::min(h->nz, 8));
+  k_mask_tol_y<<<(unsigned)(((int64_t)10 * m * m + 31) / 32), blk, 0, h->stream>>>(view(h, l), h->nz, st, en,
+                                                                                     ctx(h)->thr,
+                                                                                     l < level_fill ? 1 : 0);
+}
+inline unsigned nodes_blocks(int m) { return nb((int64_t)10 * m * m); }
+}  // namespace
+
+extern "C" {
+
 int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill) {
   if (int rc = ready(h)) return rc;
   if (!threshold) return WT_ERR_ARG;
@@ -412,23 +443,13 @@ int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill) {
   CKW(cudaMemcpyAsync(W->thr, threshold, 3 * nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   for (int l = h->level_end; l >= h->level_start; --l) {
     const int st = (l == h->level_end) ? 0 : -1, en = (l == h->level_end) ? 1 : 2;
-    const int m = h->at(l).n + en - st;
-    k_mask_tol<<<nb((int64_t)10 * m * m), TPB, 0, h->stream>>>(view(h, l), nz, st, en, W->thr, l < level_fill ? 1 : 0);
+    mask_tol(h, l, st, en, level_fill);
   }
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
 }
 
-namespace {
-void comm_masks(wt_handle* h) {
-  for (int l = h->level_start; l <= h->level_end; ++l) {
-    const DevLevel& D = h->at(l);
-    k_mask_halo<<<nb(D.n_hn + D.n_he), TPB, 0, h->stream>>>(view(h, l), D.hn, D.n_hn, D.he, D.n_he);
-  }
-}
-inline unsigned nodes_blocks(int m) { return nb((int64_t)10 * m * m); }
-}  // namespace
 
 // adapt (src/adapt.f90:14-65) without tree surgery, on the dense hierarchy.
 }  // extern "C"
@@ -444,10 +465,7 @@ int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patc
   const bool child_required = dreq != nullptr;
   for (int l = ls + 1; l <= le; ++l) k_mask_zero<<<nb(3 * h->at(l).NN), TPB, 0, s>>>(view(h, l));
   // mask_active
-  auto tol = [&](int l, int st, int en) {
-    const int m = h->at(l).n + en - st;
-    k_mask_tol<<<nb((int64_t)10 * m * m), TPB, 0, s>>>(view(h, l), nz, st, en, W->thr, l < level_fill ? 1 : 0);
-  };
+  auto tol = [&](int l, int st, int en) { mask_tol(h, l, st, en, level_fill); };
   tol(le, 0, 1);
   comm_masks(h);
   for (int l = le - 1; l >= ls; --l) {

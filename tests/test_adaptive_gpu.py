@@ -77,3 +77,48 @@ def test_adaptive_steps_match_oracle(lmin, lmax, nz, tol, upload):
             assert _rel(d[:, k], o[:, k]) <= 1e-12, (g.level, name, _rel(d[:, k], o[:, k]))
     assert model.dev.status() == 0
     model.close()
+
+
+@pytest.mark.parametrize("lmin,lmax,nz,dt,nsteps", [(3, 5, 2, 300.0, 50), (4, 6, 4, 150.0, 10)])
+def test_adaptive_long_run_masks_every_step(lmin, lmax, nz, dt, nsteps):
+    """The adaptive run of the headline workload's kind (jet + Gaussian bumps,
+    tol 5e-3 thresholds) over many steps: every mask of every level equal to
+    the oracle's after every step, the masks changing during the run, and the
+    scaling fields of every level within 1e-12 at the end."""
+    ph = OceanParams()
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    states = [bump_state(g, nz, seed=2, ph=ph) for g in levels]
+    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3)
+    H = Hierarchy(levels, nz)
+    for name, key in KEYS:
+        H.set(lmax, key, states[-1][name])
+    thr = model.threshold_def
+    H.forward()
+    H.mask_build(thr, 0, lmax)
+    H.compress()
+    H.inverse()
+    first = [H.field(g.level, "mask_e").copy() for g in levels]
+    changed = False
+    for s in range(nsteps):
+        cur = [dict(states[q], **{n: H.field(g.level, k).copy() for n, k in KEYS}) for q, g in enumerate(levels)]
+        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in levels]
+        oracle.rk4_multi(levels, nz, ph, cur, masks, dt, 1, H=H)
+        H.mask_build(thr, 0, lmax)
+        H.compress()
+        H.inverse()
+        model.step(dt)
+        for g, (mn, me) in zip(levels, model.masks()):
+            assert np.array_equal(mn, H.field(g.level, "mask_n")), (s, g.level, "mask_n")
+            assert np.array_equal(me, H.field(g.level, "mask_e")), (s, g.level, "mask_e")
+        changed = changed or any(not np.array_equal(f, H.field(g.level, "mask_e")) for f, g in zip(first, levels))
+    assert changed
+    for g in levels:
+        own = np.nonzero(g.owned)[0]
+        e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+        for name, key in KEYS:
+            k = e if name == "velo" else own
+            d, o = model.dev.download(g.level, name), H.field(g.level, key)
+            assert _rel(d[:, k], o[:, k]) <= 1e-12, (g.level, name, _rel(d[:, k], o[:, k]))
+    assert model.dev.status() == 0
+    model.close()

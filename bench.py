@@ -306,11 +306,12 @@ def adaptive_launches(L):
     outer and inner velocity, compression fused) and four inverse-transform
     kernels per coarse level), wt_mask_build's sweeps (each comm_masks is
     one launch over all levels, 3L + 3 of them), compression and the inverse
-    transform."""
+    transform.  The mask sequence ends with the finest level's needed-node
+    map (a seed and six dilation launches)."""
     stage = 3 * L + 3 * (L - 1) + 3 * (L - 1) + 4 * (L - 1)
     comm = 3 * L + 3
     masks = ((L - 1) + 1 + 2 * (L - 1) + L + (L - 1) + 2 * (L - 1) + 2 * (L - 2) + 1 + 2 * (L - 2) + 1 + L
-             + comm)
+             + comm + (7 if L > 1 else 0))
     return 4 * stage + masks + (L - 1) + 4 * (L - 1)
 
 

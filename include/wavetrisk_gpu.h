@@ -252,14 +252,19 @@ int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max
  * (max |.|), 1 "1" (mean |.|), 2 "2" (rms), 3 "min"; the mean and rms divide
  * by the count of nodes [-1, n+1]^2 with mask_n >= ADJZONE. */
 int wt_lnorm(wt_handle* h, int order, double* out);
-/* Launch-shape tuning (process-wide).  WT_TUNE_WAVELET_LAYERS: layers per
- * thread of the interscale wavelet kernels (1..64; 0 = default: 2 up to 16
- * layers, 4 above). */
-enum { WT_TUNE_WAVELET_LAYERS = 1 };
+/* Tuning.  WT_TUNE_WAVELET_LAYERS (process-wide): layers per thread of the
+ * interscale wavelet kernels (1..64; 0 = default: 2 up to 16 layers, 4 above).
+ * WT_TUNE_SKIP_INACTIVE (per handle, 1 = default): in the RK stages of the
+ * hierarchy (wt_rk4_multi, wt_adaptive_step) the finest level's step1 and
+ * trend leave out the nodes whose results cannot reach the state after
+ * WT_after_step (no counterpart in the reference, which computes every node of
+ * every existing patch; the states and masks are the same either way); 0
+ * computes every node. */
+enum { WT_TUNE_WAVELET_LAYERS = 1, WT_TUNE_SKIP_INACTIVE = 2 };
 int wt_tune(wt_handle* h, int param, int value);
 /* compress_wavelets (src/adapt.f90:79-103): zero the wavelets of inactive points. */
 int wt_compress(wt_handle* h);
-/* WT_after_step (src/adapt.f90:234-283): wavelets of the current scaling fields,
+/* WT_after_step (src/adapt.f90:192-237): wavelets of the current scaling fields,
  * compression, inverse transform. */
 int wt_wt_after_step(wt_handle* h);
 

@@ -15,7 +15,7 @@
 //   Reconstruct_velo_penta, Restrict_velo                 src/wavelet.f90:1096-1174
 //   mask_tol_vars                                         src/mask.f90:102-156
 //   compress_wavelets, compress_scalar, compress_vector   src/adapt.f90:79-232
-//   WT_after_step                                         src/adapt.f90:234-283
+//   WT_after_step                                         src/adapt.f90:192-237
 //   adapt's mask sequence without tree surgery            src/adapt.f90:14-65
 //     init_masks_zero, mask_active, mask_adj_same_scale, mask_restrict_same_scale,
 //     mask_adj_finer_scale, complete_masks, mask_trsk      src/mask.f90:7-100,734-768

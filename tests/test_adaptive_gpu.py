@@ -122,3 +122,34 @@ def test_adaptive_long_run_masks_every_step(lmin, lmax, nz, dt, nsteps):
             assert _rel(d[:, k], o[:, k]) <= 1e-12, (g.level, name, _rel(d[:, k], o[:, k]))
     assert model.dev.status() == 0
     model.close()
+
+
+@pytest.mark.parametrize("lmin,lmax,nz,dt,nsteps", [(4, 7, 4, 150.0, 6), (3, 6, 2, 300.0, 20)])
+def test_skipping_inactive_nodes_changes_nothing(lmin, lmax, nz, dt, nsteps):
+    """The finest level's step1 and trend leave out the nodes outside the
+    needed-node map (WT_TUNE_SKIP_INACTIVE, the default): every mask and every
+    owned value of every level must equal, bit for bit, those of the same run
+    computing every node, after every step (graph-replayed adaptive steps, the
+    finest level J7 in the first case)."""
+    ph = OceanParams()
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    states = [bump_state(g, nz, seed=3, ph=ph) for g in levels]
+    a = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3)
+    b = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3)
+    b.dev.skip_inactive(False)
+    for s in range(nsteps):
+        a.step(dt)
+        b.step(dt)
+        for g, (ma, mb) in zip(levels, zip(a.masks(), b.masks())):
+            assert np.array_equal(ma[0], mb[0]) and np.array_equal(ma[1], mb[1]), (s, g.level)
+        for g in levels:
+            own = np.nonzero(g.owned)[0]
+            e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+            for name in ("mass", "temp", "velo"):
+                k = e if name == "velo" else own
+                da, db = a.dev.download(g.level, name)[:, k], b.dev.download(g.level, name)[:, k]
+                assert np.array_equal(da, db), (s, g.level, name, np.abs(da - db).max())
+    assert a.dev.status() == 0 and b.dev.status() == 0
+    a.close()
+    b.close()

@@ -29,6 +29,9 @@ struct TrendML {
   const double* base_m; const double* base_t; const double* base_v;
   double* dst_m; double* dst_t; double* dst_v;
   double h;
+  // needed-node map (need_map.cuh) of the finest level, or null: nodes with
+  // need[nsrc[id]] == 0 write nothing
+  const unsigned char* need;
 };
 
 constexpr int ML_TRSK = 2, ML_ADJZONE = 8;
@@ -36,6 +39,7 @@ constexpr int ML_TRSK = 2, ML_ADJZONE = 8;
 __global__ void __launch_bounds__(NODE_TILE, 4) k_trend_ml(LevelDev L, int nz, TrendML io) {
   int k, id, i, j;
   if (!layer_node(L, nz, k, id, i, j)) return;
+  if (io.need && !io.need[__ldg(L.nsrc + id)]) return;
   const int P = L.P;
   const int NN = L.NN;
   const int n = L.n;

@@ -279,7 +279,8 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
     k_step1_tma(LevelDev L, int nz, int nbx, int nby, const double* __restrict__ mass, const double* __restrict__ temp,
                 const double* __restrict__ velo, const double* __restrict__ mean_m,
                 const double* __restrict__ phik, const double* __restrict__ pterm, Step1Out out,
-                int* __restrict__ err, const __grid_constant__ Step1Maps M) {
+                int* __restrict__ err, const __grid_constant__ Step1Maps M,
+                const unsigned char* __restrict__ need) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* __restrict__ S = reinterpret_cast<double*>(smem_raw);
   const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(smem_raw);
@@ -294,6 +295,12 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
   const int d = b / nby;
   const int cx = TT_X * bx, cy = 1 + TT_Y * by;  // box origin (padded coordinates)
   const int tid = threadIdx.x;
+  if (need) {  // a tile none of whose nodes is needed is left out, before any copy is issued
+    const int ni = cx + tid % TT_X, nj = cy - 1 + tid / TT_X;
+    int v = 0;
+    if (ni <= L.n && nj <= L.n) v = need[__ldg(L.nsrc + (d * L.P + nj + 2) * L.P + ni + 2)];
+    if (!__syncthreads_or(v)) return;
+  }
 
   if (tid == 0) {
     mbar_init(bar, 1);

@@ -341,7 +341,7 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
     const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;
     const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
     k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, s>>>(L, nz, nbx, nby, m, t, v, h->mean_m, h->phik, h->pterm, so,
-                                                           h->dflag, h->s1maps[sb]);
+                                                           h->dflag, h->s1maps[sb], nullptr);
   } else {
     k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
   }
@@ -371,7 +371,8 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
 
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
-                   double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream) {
+                   double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream,
+                   const unsigned char* need) {
   const DevLevel& D = h->at(level);
   const LevelDev L = D.view();
   const int nz = h->nz;
@@ -383,7 +384,7 @@ int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, co
     const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;
     const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
     k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, s>>>(L, nz, nbx, nby, m, t, v, mean_m, phik, pterm, so,
-                                                           h->dflag, *maps);
+                                                           h->dflag, *maps, need);
   } else {
     k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so);
   }

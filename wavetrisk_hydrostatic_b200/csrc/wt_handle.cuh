@@ -84,10 +84,12 @@ void wt_trend_ml_release(wt_handle* h);
 // on the given state, into the given operator arrays (wt_api.cu).
 // With maps (the top level's step1 input maps of this state) the top level runs
 // the TMA-staged step1 when the handle selected it.
-// stream: the handle's when null.
+// stream: the handle's when null.  need: the TMA variant leaves out the tiles
+// with no node in this needed-node map (need_map.cuh).
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
-                   double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream);
+                   double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream,
+                   const unsigned char* need = nullptr);
 // The step1 input maps of a top-level state (WT_ERR_STATE when the handle runs the L1 kernels) (wt_api.cu).
 int wt_make_step1_maps(wt_handle* h, const double* m, const double* t, const double* v, wtk::Step1Maps* out);
 // scalar_cpt_restr / flux_cpt_restr of the nz layers of the given fields from
@@ -119,6 +121,14 @@ void wt_level_compress(wt_handle* h);
 // zero every wavelet array if a host upload wrote wavelets since the last
 // zeroing (stream-ordered; WT_after_step then writes only the slots it computes)
 void wt_level_clean_wavelets(wt_handle* h);
+// The finest level's needed-node map (need_map.cuh): build it from the current
+// masks (stream-ordered; the mask sequence does so at its end); the map the
+// RK stages may skip by, or null; the count of changes to WT_TUNE_SKIP_INACTIVE.
+int wt_level_need_build(wt_handle* h);
+const unsigned char* wt_level_need(wt_handle* h);
+int wt_level_skip_epoch(wt_handle* h);
+// build the map if skipping is on and the masks changed since the last build
+int wt_level_need_refresh(wt_handle* h);
 void wt_level_inverse(wt_handle* h);
 int wt_level_set_thresholds(wt_handle* h, const double* threshold);
 // The scaling fields (mass, Theta, velocity) of a level (wt_wavelet.cu).

@@ -30,7 +30,7 @@ struct MLCtx {
   // graph of one adaptive step and the parameters it was captured with
   cudaGraphExec_t step_graph = nullptr;
   double g_dt = 0.0;
-  int g_fill = -1, g_max = -1;
+  int g_fill = -1, g_max = -1, g_epoch = -1;
   // column + step1 of the coarser levels run on side streams, forked from the
   // handle's stream and joined before each level's restriction
   std::vector<cudaStream_t> side;
@@ -163,6 +163,9 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
                 const States* dest = nullptr, double hs = 0.0, bool wav = false) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const int nz = h->nz;
+  // With WT_after_step following (wav), the finest level's results are read
+  // only where the needed-node map says so (need_map.cuh).
+  const unsigned char* need = (wav && dest) ? wt_level_need(h) : nullptr;
   // Column + step1 of a level read only that level's state and write only its
   // own work fields, so the coarser levels' run beside the finest level's on
   // side streams (parallel branches of a captured graph).  The phase timer
@@ -207,7 +210,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
         }
       }
       if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft,
-                                  V.bern, V.theta, maps, nullptr))
+                                  V.bern, V.theta, maps, nullptr, l == h->level_end ? need : nullptr))
         return rc;
       PE(tm, l == h->level_end ? PH_STEP1_TOP : PH_STEP1_COARSE);
       if (concurrent) CKM(cudaEventRecord(M->s1top, h->stream));
@@ -248,6 +251,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
       io.dst_m = dest->m[q]; io.dst_t = dest->t[q]; io.dst_v = dest->v[q];
       io.h = hs;
     }
+    if (l == h->level_end) io.need = need;
     const unsigned chunks = (unsigned)((D.NN + wtk::NODE_TILE - 1) / wtk::NODE_TILE);
     PB(tm);
     wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
@@ -285,6 +289,8 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm) {
     q1.v.push_back(V.v1);
   }
   const double hs[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
+  if (!tm)
+    if (int rc = wt_level_need_refresh(h)) return rc;
   for (int s = 0; s < nsteps; ++s)
     for (int stage = 0; stage < 4; ++stage) {
       const States& src = stage == 0 ? q : q1;
@@ -341,7 +347,9 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
   }
   if (int rc = wt_level_set_thresholds(h, threshold)) return rc;
   wt_level_clean_wavelets(h);  // outside the graph, which assumes clean wavelet arrays
-  if (!M->step_graph || M->g_dt != dt || M->g_fill != level_fill || M->g_max != max_level) {
+  if (int rc = wt_level_need_refresh(h)) return rc;  // likewise a current needed-node map
+  if (!M->step_graph || M->g_dt != dt || M->g_fill != level_fill || M->g_max != max_level ||
+      M->g_epoch != wt_level_skip_epoch(h)) {
     if (M->step_graph) {
       cudaGraphExecDestroy(M->step_graph);
       M->step_graph = nullptr;
@@ -363,6 +371,7 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
     M->g_dt = dt;
     M->g_fill = level_fill;
     M->g_max = max_level;
+    M->g_epoch = wt_level_skip_epoch(h);
   }
   for (int s = 0; s < nsteps; ++s) CKM(cudaGraphLaunch(M->step_graph, h->stream));
   CKM(cudaStreamSynchronize(h->stream));

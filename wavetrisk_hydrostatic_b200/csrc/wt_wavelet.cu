@@ -13,6 +13,7 @@
 #include "restrict_kernels.cuh"
 #include "wavelet_kernels.cuh"
 #include "wavelet_layers.cuh"
+#include "need_map.cuh"
 #include "wt_handle.cuh"
 #include "wt_wavctx.cuh"
 
@@ -278,6 +279,12 @@ int wt_wavelet_setup(wt_handle* h) {
     CKW(cudaMemcpy(V.mask_e, tol.data(), 3 * D.NN * sizeof(int), cudaMemcpyHostToDevice));
   }
   CKW(W->alloc(&W->thr, (size_t)3 * nz));
+  // needed-node map of the finest level (NEED_R is even: the map ends in need[0])
+  if (h->level_end > h->level_start) {
+    const size_t NN = (size_t)h->at(h->level_end).NN;
+    CKW(W->alloc(&W->need[0], NN));
+    CKW(W->alloc(&W->need[1], NN));
+  }
   // velocity-wavelet plans of every parent level
   for (int l = h->level_start; l < h->level_end; ++l) {
     WavLevel& V = W->L[l - h->level_start];
@@ -340,6 +347,7 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
   CKW(cudaStreamSynchronize(h->stream));
   if (level == h->level_end && field <= WT_FIELD_VELO) h->state_halo_done = false;
   if (field >= WT_WAVE_MASS && field <= WT_WAVE_VELO) ctx(h)->wav_dirty = true;
+  if (field == WT_MASK_NODE || field == WT_MASK_EDGE) ctx(h)->need_ok = false;
   return WT_OK;
 }
 
@@ -513,6 +521,35 @@ int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patc
   // mask_trsk
   for (int l = ls; l <= le; ++l) k_mask_trsk<<<nodes_blocks(h->at(l).n + 4), TPB, 0, s>>>(view(h, l));
   CKW(cudaGetLastError());
+  return wt_level_need_build(h);
+}
+
+// The finest level's needed-node map from the current masks (stream-ordered).
+int wt_level_need_build(wt_handle* h) {
+  WavCtx* W = ctx(h);
+  if (!W->need[0]) return WT_OK;
+  const int le = h->level_end;
+  const int64_t NN = h->at(le).NN;
+  k_need_seed<<<nb(NN), TPB, 0, h->stream>>>(view(h, le), view(h, le - 1), W->need[0]);
+  for (int r = 0; r < NEED_R; ++r)
+    k_need_dilate<<<nb(NN), TPB, 0, h->stream>>>(view(h, le), W->need[r & 1], W->need[(r + 1) & 1]);
+  CKW(cudaGetLastError());
+  W->need_ok = true;
+  return WT_OK;
+}
+
+// The map the finest level's step1 and trend may skip by, or null (no map,
+// skipping turned off, or masks uploaded since the last build and no build
+// wanted now).
+const unsigned char* wt_level_need(wt_handle* h) {
+  WavCtx* W = ctx(h);
+  if (!W->need[0] || !W->skip_inactive || !W->need_ok) return nullptr;
+  return W->need[0];
+}
+int wt_level_skip_epoch(wt_handle* h) { return ctx(h)->skip_epoch; }
+int wt_level_need_refresh(wt_handle* h) {
+  WavCtx* W = ctx(h);
+  if (W->need[0] && W->skip_inactive && !W->need_ok) return wt_level_need_build(h);
   return WT_OK;
 }
 
@@ -699,10 +736,19 @@ int wt_lnorm(wt_handle* h, int order, double* out) {
 // per thread of the layer-group kernels (1 .. 64; 0 restores the default
 // chosen from the layer count).  Process-wide.
 int wt_tune(wt_handle* h, int param, int value) {
-  (void)h;
   if (param == WT_TUNE_WAVELET_LAYERS) {
     if (value < 0 || value > 64) return WT_ERR_ARG;
     g_lpt_set = value;
+    return WT_OK;
+  }
+  if (param == WT_TUNE_SKIP_INACTIVE) {
+    if (!h) return WT_ERR_ARG;
+    if (!h->wav) return WT_ERR_STATE;
+    if (value != 0 && value != 1) return WT_ERR_ARG;
+    if (ctx(h)->skip_inactive != (value == 1)) {
+      ctx(h)->skip_inactive = value == 1;
+      ++ctx(h)->skip_epoch;
+    }
     return WT_OK;
   }
   return WT_ERR_ARG;

@@ -266,6 +266,12 @@ class WaveletHierarchy(DeviceGrid):
         N.check("wt_lnorm", N.lib().wt_lnorm(self.h, code, N.dptr(out)))
         return out
 
+    def skip_inactive(self, on: bool) -> None:
+        """WT_TUNE_SKIP_INACTIVE: let the RK stages leave out the finest level's
+        nodes whose step1 and trend results cannot reach the state after
+        WT_after_step (on by default; the states and masks are the same)."""
+        N.check("wt_tune", N.lib().wt_tune(self.h, 2, 1 if on else 0))
+
     def rk4_multi(self, dt: float, nsteps: int = 1) -> None:
         """nsteps RK4 steps of the whole hierarchy with WT_after_step per stage (masks fixed)."""
         N.check("wt_rk4_multi", N.lib().wt_rk4_multi(self.h, float(dt), int(nsteps)))

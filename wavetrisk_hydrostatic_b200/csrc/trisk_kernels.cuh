@@ -53,11 +53,14 @@ __global__ void k_halo_state(int nz, int64_t NN, const int2* __restrict__ hn, in
 __global__ void __launch_bounds__(NODE_TILE) k_column(LevelDev L, Phys ph, int nz, const double* __restrict__ mass,
                                                       const double* __restrict__ temp, const double* __restrict__ mean_m,
                                                       const double* __restrict__ mean_t, double* __restrict__ phik,
-                                                      double* __restrict__ pterm) {
-  // one thread per padded node, all layers
+                                                      double* __restrict__ pterm,
+                                                      const unsigned char* __restrict__ need) {
+  // one thread per padded node, all layers; with a needed-node map (need[nsrc])
+  // only the nodes it marks
   int k0, id, i, j;
   if (!layer_node(L, 1, k0, id, i, j)) return;
   if (i < 0 || j < 0 || i > L.n || j > L.n) return;
+  if (need && !need[__ldg(L.nsrc + id)]) return;
   const int src = (i < L.n && j < L.n) ? id : L.nsrc[id];
   double sp = 0.0;
   for (int k = 0; k < nz; ++k) {

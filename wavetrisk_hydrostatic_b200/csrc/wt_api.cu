@@ -332,7 +332,7 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   // block b: layer b % nz of node chunk b / nz (layer_node in trisk_kernels.cuh)
   const unsigned chunks = blocks_for(D.NN, NODE_TILE);
   TB(1);
-  k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm);
+  k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm, nullptr);
   TE(1);
   Step1Out so{h->qe, h->hfm, h->hft, h->bern, h->theta};
   TB(2);
@@ -378,7 +378,7 @@ int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, co
   const int nz = h->nz;
   cudaStream_t s = stream ? stream : h->stream;
   const unsigned chunks = blocks_for(D.NN, NODE_TILE);
-  k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, mean_m, mean_t, phik, pterm);
+  k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, mean_m, mean_t, phik, pterm, need);
   Step1Out so{qe, hfm, hft, bern, theta};
   if (maps && level == h->level_end && h->trend_variant == 0) {
     const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;

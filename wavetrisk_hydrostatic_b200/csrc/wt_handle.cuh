@@ -84,8 +84,9 @@ void wt_trend_ml_release(wt_handle* h);
 // on the given state, into the given operator arrays (wt_api.cu).
 // With maps (the top level's step1 input maps of this state) the top level runs
 // the TMA-staged step1 when the handle selected it.
-// stream: the handle's when null.  need: the TMA variant leaves out the tiles
-// with no node in this needed-node map (need_map.cuh).
+// stream: the handle's when null.  need: the column leaves out the nodes outside
+// this needed-node map (need_map.cuh) and the TMA variant of step1 the tiles
+// with none of them; step1 reads the column's results only at its own node.
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
                    double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream,

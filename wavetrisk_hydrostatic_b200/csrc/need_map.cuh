@@ -16,7 +16,10 @@
 
 namespace wtw {
 
-constexpr int NEED_R = 6;
+#ifndef WT_NEED_R
+#define WT_NEED_R 6
+#endif
+constexpr int NEED_R = WT_NEED_R;
 
 // seed of every padded slot of level C (parent level P)
 __global__ void k_need_seed(WLev C, WLev P, unsigned char* __restrict__ out) {

@@ -43,8 +43,8 @@ struct WavCtx {
   std::vector<cudaEvent_t> fork;  // per level pair: its forward wavelets may start
   // scaling-field pointers put aside while WT_after_step runs on other arrays
   std::vector<WavLevel> bound_saved;
-  // needed-node map of the finest level (need_map.cuh): need[0] is the map,
-  // need[1] scratch; need_ok once built from the current masks.  skip_inactive
+  // needed-node map of the finest level (need_map.cuh) in need[NEED_R & 1], the
+  // other buffer its dilation scratch; need_ok once built from the current masks.  skip_inactive
   // lets the RK stages of the hierarchy leave the finest level's step1 and
   // trend out where the map is 0; skip_epoch counts its changes.
   unsigned char* need[2] = {nullptr, nullptr};

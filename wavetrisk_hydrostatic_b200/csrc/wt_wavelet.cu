@@ -279,7 +279,7 @@ int wt_wavelet_setup(wt_handle* h) {
     CKW(cudaMemcpy(V.mask_e, tol.data(), 3 * D.NN * sizeof(int), cudaMemcpyHostToDevice));
   }
   CKW(W->alloc(&W->thr, (size_t)3 * nz));
-  // needed-node map of the finest level (NEED_R is even: the map ends in need[0])
+  // needed-node map of the finest level and its dilation scratch
   if (h->level_end > h->level_start) {
     const size_t NN = (size_t)h->at(h->level_end).NN;
     CKW(W->alloc(&W->need[0], NN));
@@ -467,8 +467,7 @@ int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill) {
 // graph); the thresholds are already in the context's device buffer.  With
 // dreq non-null, check_child_required flags go there (patch_size > 0).
 int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq) {
-  const int ls = h->level_start, le = h->level_end, nz = h->nz;
-  WavCtx* W = ctx(h);
+  const int ls = h->level_start, le = h->level_end;
   cudaStream_t s = h->stream;
   const bool child_required = dreq != nullptr;
   for (int l = ls + 1; l <= le; ++l) k_mask_zero<<<nb(3 * h->at(l).NN), TPB, 0, s>>>(view(h, l));
@@ -544,7 +543,7 @@ int wt_level_need_build(wt_handle* h) {
 const unsigned char* wt_level_need(wt_handle* h) {
   WavCtx* W = ctx(h);
   if (!W->need[0] || !W->skip_inactive || !W->need_ok) return nullptr;
-  return W->need[0];
+  return W->need[NEED_R & 1];  // the last dilation's output
 }
 int wt_level_skip_epoch(wt_handle* h) { return ctx(h)->skip_epoch; }
 int wt_level_need_refresh(wt_handle* h) {

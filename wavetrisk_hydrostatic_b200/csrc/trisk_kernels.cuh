@@ -315,22 +315,10 @@ __global__ void __launch_bounds__(NODE_TILE, 3)
 // reference's update_bdry(horiz_flux)).  For MODE_RK every node of the padded
 // level (all layers) is written as dest = base + h * trend (trend = 0 where
 // the reference leaves it zero); MODE_TREND writes the trends themselves.
-enum { MODE_TREND = 0, MODE_RK = 1 };
+// MODE_ML: one level of the multi-level trend_ml at the finest level (no
+// restricted source), with the RK sub-step (trisk_tma.cuh only).
+enum { MODE_TREND = 0, MODE_RK = 1, MODE_ML = 2 };
 
-struct TrendIO {
-  const double* __restrict__ theta;  // Theta/rho of the stage state at [0, n]^2 (k_step1)
-  const double* __restrict__ qe;
-  const double* __restrict__ hfm;
-  const double* __restrict__ hft;
-  const double* __restrict__ bern;
-  const double* __restrict__ phik;
-  // MODE_RK
-  const double* base_m; const double* base_t; const double* base_v;
-  double* dst_m; double* dst_t; double* dst_v;
-  double h;
-  // MODE_TREND
-  double* dm; double* dtt; double* dv;
-};
 
 template <int MODE>
 __global__ void __launch_bounds__(NODE_TILE, 3) k_trend(LevelDev L, int nz, TrendIO io) {

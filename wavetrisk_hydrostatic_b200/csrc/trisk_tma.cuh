@@ -96,6 +96,11 @@ __device__ __forceinline__ void weights5_s(const double* __restrict__ S, int q, 
 
 // Same trends and sub-step as k_trend (scalar_trend, du_source/Qperp, du_grad,
 // RK_sub_step; src/ops.f90:739-901, src/time_integr.f90:206-225).
+// MODE_ML is k_trend_ml of the finest level of a hierarchy (src/multi_level.f90:
+// 5-188): trends only where mask_n >= TRSK, dmass and dTheta written on
+// [0, n]^2, the velocity source on [0, n)^2, the sub-step on every padded node;
+// with a needed-node map, tiles with no needed node are left out before any
+// copy is issued and nodes that are not needed write nothing.
 // Block b: layer b % nz, then tile x, tile y, lozenge.  io.err receives 1 when a
 // block's copies did not complete within the wait limit.
 template <int MODE>
@@ -116,6 +121,12 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
   const int d = b / nby;
   const int x0 = bx * TT_X, y0 = by * TT_Y;
   const int tid = threadIdx.x;
+  if (MODE == MODE_ML && io.need) {
+    const int pi = x0 + tid % TT_X, pj = y0 + tid / TT_X;
+    int v = 0;
+    if (pi < L.P && pj < L.P) v = io.need[__ldg(L.nsrc + (d * L.P + pj) * L.P + pi)];
+    if (!__syncthreads_or(v)) return;
+  }
 
   if (tid == 0) {
     mbar_init(bar, 1);
@@ -151,7 +162,7 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
   const bool own = inside && i >= 0 && j >= 0 && i < n && j < n;
   const int64_t vo = 3 * ko + id;
   double bm = 0.0, bt = 0.0, bv0 = 0.0, bv1 = 0.0, bv2 = 0.0;
-  if (MODE == MODE_RK && inside) {
+  if ((MODE == MODE_RK || MODE == MODE_ML) && inside) {
     bm = io.base_m[ko + id];
     bt = io.base_t[ko + id];
     bv0 = io.base_v[vo];
@@ -197,12 +208,18 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
   __syncthreads();
 
   if (!inside) return;
+  bool on = true;
+  if (MODE == MODE_ML) {
+    if (io.need && !io.need[__ldg(L.nsrc + id)]) return;
+    on = io.mask_n[id] >= 2;  // TRSK
+  }
   const int q0 = (ty + 1) * TB_X + (tx + 2);
   constexpr int oE = 1, oW = -1, oN = TB_X, oS = -TB_X, oNE = TB_X + 1, oSW = -TB_X - 1, oSE = 1 - TB_X,
                 oNW = TB_X - 1;
 #define SM(pl, o) S[(pl) * PLANE_STRIDE + q0 + (o)]
   double dms = 0.0, dts = 0.0, dv0 = 0.0, dv1 = 0.0, dv2 = 0.0;
-  if (scal) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;  // velocity source -Qperp
+  if (scal && on) {
     const double hinv = SM(S_HINV, 0);
     const double divm = (SM(S_HFM + RT, 0) - SM(S_HFM + RT, oW) + SM(S_HFM + DG, oSW) - SM(S_HFM + DG, 0) +
                          SM(S_HFM + UP, 0) - SM(S_HFM + UP, oS)) * hinv;
@@ -211,7 +228,7 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
     dms = -divm;
     dts = -divt;
   }
-  if (own) {
+  if (own && on) {
 #define TQ(e1, o1, q0v, w) (SM(S_HFM + (e1), o1) * interp(SM(S_QE + (e1), o1), (q0v)) * (w))
     double w1[5], w2[5];
     double qv = SM(S_QE + RT, 0);
@@ -238,12 +255,26 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
                  gB2 = (SM(S_B, oN) - SM(S_B, 0)) / lUP;
     const double xE = -SM(S_F, oE), x0v = -SM(S_F, 0), xNE = -SM(S_F, oNE), xN = -SM(S_F, oN);
     const double gE0 = (xE - x0v) / lRT, gE1 = (x0v - xNE) / lDG, gE2 = (xN - x0v) / lUP;
-    dv0 = (-Q0 + 0.0 * lRT) / lRT - gB0 - interp(th0, thE) * gE0;
-    dv1 = (-Q1 + 0.0 * lDG) / lDG - gB1 - interp(th0, thNE) * gE1;
-    dv2 = (-Q2 + 0.0 * lUP) / lUP - gB2 - interp(th0, thN) * gE2;
+    s0 = -Q0 + 0.0 * lRT;
+    s1 = -Q1 + 0.0 * lDG;
+    s2 = -Q2 + 0.0 * lUP;
+    dv0 = s0 / lRT - gB0 - interp(th0, thE) * gE0;
+    dv1 = s1 / lDG - gB1 - interp(th0, thNE) * gE1;
+    dv2 = s2 / lUP - gB2 - interp(th0, thN) * gE2;
   }
 #undef SM
-  if (MODE == MODE_RK) {
+  if (MODE == MODE_ML) {
+    if (scal) {
+      io.dm[ko + id] = dms;
+      io.dtt[ko + id] = dts;
+    }
+    if (own) {
+      io.src[vo] = s0;
+      io.src[vo + NN] = s1;
+      io.src[vo + 2 * NN] = s2;
+    }
+  }
+  if (MODE == MODE_RK || MODE == MODE_ML) {
     const double h = io.h;
     io.dst_m[ko + id] = bm + h * dms;
     io.dst_t[ko + id] = bt + h * dts;

@@ -41,6 +41,25 @@ struct Step1Maps {
   CUtensorMap len, ped, part, cor;  // plane = edge orientation / area part / triangle
 };
 
+// Inputs and outputs of the trend kernels (trisk_kernels.cuh, trisk_tma.cuh).
+struct TrendIO {
+  const double* __restrict__ theta;  // Theta/rho of the stage state at [0, n]^2 (k_step1)
+  const double* __restrict__ qe;
+  const double* __restrict__ hfm;
+  const double* __restrict__ hft;
+  const double* __restrict__ bern;
+  const double* __restrict__ phik;
+  // MODE_RK
+  const double* base_m; const double* base_t; const double* base_v;
+  double* dst_m; double* dst_t; double* dst_v;
+  double h;
+  // MODE_TREND (and dm, dtt in MODE_ML)
+  double* dm; double* dtt; double* dv;
+  // MODE_ML: the level's node masks, the velocity source it writes on
+  // [0, n)^2, and the needed-node map (need_map.cuh) or null
+  const int* mask_n; double* src; const unsigned char* need;
+};
+
 struct Phys {
   double grav, ref_density, p_top;
 };

@@ -93,6 +93,18 @@ int wt_make_step1_maps(wt_handle* h, const double* m, const double* t, const dou
   return step1_maps(h, m, t, v, out) ? WT_OK : WT_ERR_CUDA;
 }
 
+int wt_make_trend_maps(wt_handle* h, const double* hfm, const double* hft, const double* qe, const double* theta,
+                       const double* bern, const double* phik, wtk::TrendMaps* M) {
+  if (h->trend_variant != 0) return WT_ERR_STATE;
+  const DevLevel& D = h->top();
+  const int nz = h->nz;
+  const bool ok = top_map(h, &M->hfm, hfm, 3 * nz) && top_map(h, &M->hft, hft, 3 * nz) &&
+                  top_map(h, &M->qe, qe, 3 * nz) && top_map(h, &M->theta, theta, nz) &&
+                  top_map(h, &M->bern, bern, nz) && top_map(h, &M->phik, phik, nz) &&
+                  top_map(h, &M->part, D.part, 6) && top_map(h, &M->hinv, D.hex_inv, 1);
+  return ok ? WT_OK : WT_ERR_CUDA;
+}
+
 static int make_trend_maps(wt_handle* h) {
   const DevLevel& D = h->top();
   auto mk = [&](CUtensorMap* m, const double* base, int planes) { return top_map(h, m, base, planes); };
@@ -112,6 +124,7 @@ static int make_trend_maps(wt_handle* h) {
   CK(cudaFuncSetAttribute(k_step1_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, STEP1_TMA_SMEM));
   CK(cudaFuncSetAttribute(k_trend_tma<MODE_RK>, cudaFuncAttributeMaxDynamicSharedMemorySize, TREND_TMA_SMEM));
   CK(cudaFuncSetAttribute(k_trend_tma<MODE_TREND>, cudaFuncAttributeMaxDynamicSharedMemorySize, TREND_TMA_SMEM));
+  CK(cudaFuncSetAttribute(k_trend_tma<MODE_ML>, cudaFuncAttributeMaxDynamicSharedMemorySize, TREND_TMA_SMEM));
   return WT_OK;
 }
 
@@ -365,6 +378,19 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
       k_trend<MODE_TREND><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
   }
   TE(5);
+  CK(cudaGetLastError());
+  return WT_OK;
+}
+
+// k_trend_tma<MODE_ML> on the top level: the multi-level trend of the finest
+// level with the RK sub-step, its inputs read through the maps M.
+int wt_level_trend_ml_tma(wt_handle* h, const wtk::TrendIO& io, const wtk::TrendMaps& M, cudaStream_t stream) {
+  const DevLevel& D = h->top();
+  const int nz = h->nz;
+  const int nbx = (D.P + TT_X - 1) / TT_X, nby = (D.P + TT_Y - 1) / TT_Y;
+  const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
+  k_trend_tma<MODE_ML><<<nblk, TT_X * TT_Y, TREND_TMA_SMEM, stream ? stream : h->stream>>>(D.view(), nz, nbx, nby, io,
+                                                                                           h->dflag, M);
   CK(cudaGetLastError());
   return WT_OK;
 }

@@ -87,6 +87,12 @@ void wt_trend_ml_release(wt_handle* h);
 // stream: the handle's when null.  need: the column leaves out the nodes outside
 // this needed-node map (need_map.cuh) and the TMA variant of step1 the tiles
 // with none of them; step1 reads the column's results only at its own node.
+// Tensor maps of the top level's trend inputs held in the given arrays (with the
+// level's geometry), for k_trend_tma; WT_ERR_STATE unless the TMA variant is on.
+int wt_make_trend_maps(wt_handle* h, const double* hfm, const double* hft, const double* qe, const double* theta,
+                       const double* bern, const double* phik, wtk::TrendMaps* M);
+// k_trend_tma<MODE_ML> on the top level (stream: the handle's when null).
+int wt_level_trend_ml_tma(wt_handle* h, const wtk::TrendIO& io, const wtk::TrendMaps& M, cudaStream_t stream);
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
                    double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream,

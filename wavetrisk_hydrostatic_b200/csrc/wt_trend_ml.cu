@@ -27,6 +27,9 @@ struct MLCtx {
   // step1 input maps of the top level's RK stage state (TMA-staged step1)
   wtk::Step1Maps q1maps{};
   bool q1maps_ok = false;
+  // trend input maps of the top level's work arrays (TMA-staged trend)
+  wtk::TrendMaps tmaps{};
+  bool tmaps_ok = false;
   // graph of one adaptive step and the parameters it was captured with
   cudaGraphExec_t step_graph = nullptr;
   double g_dt = 0.0;
@@ -69,6 +72,10 @@ int ensure(wt_handle* h) {
       M->allocs.push_back(*p);
       CKM(cudaMemsetAsync(*p, 0, 3 * nn * 8, h->stream));
     }
+  }
+  if (h->trend_variant == 0) {
+    const MLLevel& T = M->L.back();
+    M->tmaps_ok = wt_make_trend_maps(h, T.hfm, T.hft, T.qe, T.theta, T.bern, T.phik, &M->tmaps) == WT_OK;
   }
   CKM(cudaEventCreateWithFlags(&M->fork, cudaEventDisableTiming));
   CKM(cudaEventCreateWithFlags(&M->s1top, cudaEventDisableTiming));
@@ -254,7 +261,16 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
     if (l == h->level_end) io.need = need;
     const unsigned chunks = (unsigned)((D.NN + wtk::NODE_TILE - 1) / wtk::NODE_TILE);
     PB(tm);
-    wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
+    if (l == h->level_end && M->tmaps_ok && base && dest) {  // TMA-staged, the same arithmetic
+      wtk::TrendIO t{};
+      t.theta = V.theta; t.qe = V.qe; t.hfm = V.hfm; t.hft = V.hft; t.bern = V.bern; t.phik = V.phik;
+      t.base_m = io.base_m; t.base_t = io.base_t; t.base_v = io.base_v;
+      t.dst_m = io.dst_m; t.dst_t = io.dst_t; t.dst_v = io.dst_v; t.h = io.h;
+      t.dm = V.dm; t.dtt = V.dt; t.mask_n = mask_n; t.src = V.src; t.need = io.need;
+      if (int rc = wt_level_trend_ml_tma(h, t, M->tmaps, nullptr)) return rc;
+    } else {
+      wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
+    }
     PE(tm, l == h->level_end ? PH_TREND_TOP : PH_TREND_COARSE);
     CKM(cudaGetLastError());
     if (wav && dest && l < h->level_end)

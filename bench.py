@@ -316,8 +316,9 @@ def adaptive_launches(L):
 
 
 def algorithmic_bytes_trend_ml(level, nz, n_on=None, n_own=None):
-    """Compulsory bytes of one k_trend_ml launch on a level with the fused RK
-    sub-step.  Every node of [0, n]^2 reads its mask and writes dmass and dTheta
+    """Compulsory bytes of one multi-level trend launch on a level with the
+    fused RK sub-step (k_trend_ml, or k_trend_tma<MODE_ML> on the finest level,
+    which stages every input plane of a tile, so its traffic is higher).  Every node of [0, n]^2 reads its mask and writes dmass and dTheta
     (2 words a layer); every owned node writes the velocity source (3); the
     n_on nodes with mask_n >= TRSK also read theta, qe(3), hflux_mass(3),
     hflux_Theta(3), Bernoulli and Phi (12 words a layer) and len(3), part(6),
@@ -520,11 +521,10 @@ def bench_ours(args):
             "config": workload_config(args, world),
             "e2e": {"value": e2e_value, "unit": "simulated days per wall-clock hour",
                     "h2d_bytes_per_step": r["h2d_bytes_per_step"], "d2h_bytes_per_step": r["d2h_bytes_per_step"],
-                    "path": "C-ABI wt_upload_field / wt_rk4_multi + wt_mask_build + wt_compress + wt_inverse_wt / "
-                            "wt_download_field, pinned host buffers: every level's state in, every level's state "
-                            "and masks out, every step"},
+                    "path": "C-ABI wt_upload_field / wt_adaptive_step / wt_download_field, pinned host "
+                            "buffers: every level's state in, every level's state and masks out, every step"},
             "gpu_launches": adaptive_launches(L) * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_trend_ml (level_end)", "achieved": ach, "peak": hbm,
+            "roofline": {"bound": "hbm", "kernel": "k_trend_tma<MODE_ML> (level_end)", "achieved": ach, "peak": hbm,
                          "unit": "GB/s", "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
                          "algorithmic_bytes_per_launch": ab,
                          "dominant_phase_by_time": dom,

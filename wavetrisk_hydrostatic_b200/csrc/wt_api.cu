@@ -219,7 +219,14 @@ int wt_create(const wt_grid_desc* desc, wt_handle** out) {
       for (double** p : edge_arrays)
         if ((rc = dev_zero(p, ne))) break;
     if (rc == WT_OK) {
-      cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+      // The handle's stream carries the critical path of a step (the finest
+      // level's step1 and trend, the restrictions, the coarser trends, the
+      // velocity reconstruction); the side streams that run beside it (coarser
+      // levels' step1, forward wavelets, scalar reconstruction) keep the default
+      // priority, so the block scheduler serves this stream's blocks first.
+      int least = 0, greatest = 0;
+      cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+      if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatest);
       if (e != cudaSuccess) rc = wt_handle_fail("stream", e);
     }
     if (rc == WT_OK) {

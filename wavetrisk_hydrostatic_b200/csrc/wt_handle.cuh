@@ -134,6 +134,10 @@ void wt_level_clean_wavelets(wt_handle* h);
 int wt_level_need_build(wt_handle* h);
 const unsigned char* wt_level_need(wt_handle* h);
 int wt_level_skip_epoch(wt_handle* h);
+// make stream st wait until the last inverse transform (wt_level_inverse or
+// WT_after_step) has completed level's state; only valid when that transform was
+// issued after every other write of the state (stream-ordered)
+int wt_level_ready_wait(wt_handle* h, int level, cudaStream_t st);
 // build the map if skipping is on and the masks changed since the last build
 int wt_level_need_refresh(wt_handle* h);
 void wt_level_inverse(wt_handle* h);

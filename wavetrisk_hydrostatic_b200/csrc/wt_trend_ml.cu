@@ -79,11 +79,17 @@ int ensure(wt_handle* h) {
   }
   CKM(cudaEventCreateWithFlags(&M->fork, cudaEventDisableTiming));
   CKM(cudaEventCreateWithFlags(&M->s1top, cudaEventDisableTiming));
-  CKM(cudaStreamCreateWithFlags(&M->rs, cudaStreamNonBlocking));
+  // The restriction chain feeds the critical path (top priority); the coarser
+  // levels' column and step1 run in the slack of the inverse transform and of
+  // the finest level's kernels, above the forward wavelets (lowest).
+  int least = 0, greatest = 0;
+  CKM(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  const int medium = greatest < least ? greatest + 1 : greatest;
+  CKM(cudaStreamCreateWithPriority(&M->rs, cudaStreamNonBlocking, greatest));
   for (int l = h->level_start; l < h->level_end; ++l) {
     cudaStream_t s;
     cudaEvent_t e, r;
-    CKM(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CKM(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, medium));
     M->side.push_back(s);
     CKM(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     M->done.push_back(e);
@@ -166,8 +172,12 @@ States hierarchy_state(wt_handle* h) {
 // pair (l, l+1) are launched as soon as level l's sub-step is written, beside
 // the coarser levels' trend; the caller binds dest to the wavelet context
 // before and finishes WT_after_step after.
+// With after_inverse, the state S was completed by the inverse transform issued
+// last (the previous RK stage's WT_after_step): a coarser level's column and
+// step1 start as soon as that transform has rebuilt the level, beside the finer
+// levels' reconstruction.
 int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const States* base = nullptr,
-                const States* dest = nullptr, double hs = 0.0, bool wav = false) {
+                const States* dest = nullptr, double hs = 0.0, bool wav = false, bool after_inverse = false) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const int nz = h->nz;
   // With WT_after_step following (wav), the finest level's results are read
@@ -186,7 +196,11 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
       double *mm, *mt;
       if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
       if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
-      CKM(cudaStreamWaitEvent(M->side[q], M->fork, 0));
+      if (after_inverse) {
+        if (int rc = wt_level_ready_wait(h, l, M->side[q])) return rc;
+      } else {
+        CKM(cudaStreamWaitEvent(M->side[q], M->fork, 0));
+      }
       if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern,
                                   V.theta, nullptr, M->side[q]))
         return rc;
@@ -321,7 +335,7 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm) {
       // WT_after_step's forward wavelets start inside the trend, level pair by level pair
       wt_level_wav_bind(h, dest.m.data(), dest.t.data(), dest.v.data());
       wt_level_clean_wavelets(h);
-      int rc = trend_multi(h, src, nullptr, &q, &dest, hs[stage], true);
+      int rc = trend_multi(h, src, nullptr, &q, &dest, hs[stage], true, stage > 0);
       if (!rc) rc = wt_level_wav_finish(h);
       wt_level_wav_unbind(h);
       if (rc) return rc;
@@ -381,7 +395,8 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return wt_handle_fail("capture", e);
-    e = cudaGraphInstantiate(&M->step_graph, g, 0);
+    // the nodes keep the priorities of the streams they were captured from
+    e = cudaGraphInstantiate(&M->step_graph, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return wt_handle_fail("instantiate", e);
     M->g_dt = dt;

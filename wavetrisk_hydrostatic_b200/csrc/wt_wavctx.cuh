@@ -35,12 +35,17 @@ struct WavCtx {
   // ghost rows, the coarsest level) hold 0 unless a host upload wrote them;
   // WT_after_step re-zeroes the arrays only then.
   bool wav_dirty = false;
-  // side streams of the transforms: scalar wavelets and the scalar chain of
-  // the inverse (0), inner (1) and outer (2) velocity wavelets, forked from and
-  // joined back into the handle's stream
-  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // side streams of the transforms, forked from and joined back into the
+  // handle's stream: the scalar chain of the inverse (0, top priority: it is as
+  // long as the velocity chain on the handle's stream), and the forward scalar
+  // (3), inner (1) and outer (2) velocity wavelets (lowest priority: they run
+  // beside the coarser levels' trend)
+  cudaStream_t side[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> fork;  // per level pair: its forward wavelets may start
+  // per level: its state is complete in the last inverse transform (velocity
+  // chain on the handle's stream, scalar chain on side[0])
+  std::vector<cudaEvent_t> ready_v, ready_s;
   // scaling-field pointers put aside while WT_after_step runs on other arrays
   std::vector<WavLevel> bound_saved;
   // needed-node map of the finest level (need_map.cuh) in need[NEED_R & 1], the

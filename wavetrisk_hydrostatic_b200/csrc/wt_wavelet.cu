@@ -141,15 +141,18 @@ void inverse(wt_handle* h) {
   cudaStream_t s = h->stream, sa = W->side[0];
   cudaEventRecord(W->ev[0], s);
   cudaStreamWaitEvent(sa, W->ev[0], 0);
+  cudaEventRecord(W->ready_v[0], s);  // level_start is not rebuilt
   for (int l = h->level_start; l <= h->level_end - 1; ++l) {
-    const int np = h->at(l).n;
+    const int np = h->at(l).n, q = l + 1 - h->level_start;
     const WLev P = view(h, l), C = view(h, l + 1);
     const int64_t par1 = (int64_t)10 * (np + 1) * (np + 1), par0 = (int64_t)10 * np * np;
     k_prolong_l<<<nbl(par1, nz), TPBL, 0, sa>>>(P, C, nz, lpt_for(nz));
     k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, sa>>>(C, np, nz, lpt_for(nz));
+    cudaEventRecord(W->ready_s[q], sa);
     const WavLevel& V = W->L[l - h->level_start];
     k_recon_outer_p<<<plan_grid(par1), plan_block(nz), 0, s>>>(P, C, nz, V.op_i, V.op_d);
     k_recon_inner_p<<<plan_grid(par0), plan_block(nz), 0, s>>>(P, C, nz, V.ip_i, V.ip_d);
+    cudaEventRecord(W->ready_v[q], s);
   }
   cudaEventRecord(W->ev[1], sa);
   cudaStreamWaitEvent(s, W->ev[1], 0);
@@ -195,8 +198,8 @@ int wt_level_wav_forward_pair(wt_handle* h, int l) {
   WavCtx* W = ctx(h);
   cudaEvent_t f = W->fork[l - h->level_start];
   CKW(cudaEventRecord(f, h->stream));
-  for (cudaStream_t s : W->side) CKW(cudaStreamWaitEvent(s, f, 0));
-  launch_scalar_wc<true>(h, l, W->side[0]);
+  for (int k = 1; k < 4; ++k) CKW(cudaStreamWaitEvent(W->side[k], f, 0));
+  launch_scalar_wc<true>(h, l, W->side[3]);
   launch_velo_wc<true>(h, l, W->side[2], W->side[1]);
   CKW(cudaGetLastError());
   return WT_OK;
@@ -206,7 +209,7 @@ int wt_level_wav_forward_pair(wt_handle* h, int l) {
 // launched: join the side streams, then the inverse transform.
 int wt_level_wav_finish(wt_handle* h) {
   WavCtx* W = ctx(h);
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 1; k < 4; ++k) {
     CKW(cudaEventRecord(W->ev[1 + k], W->side[k]));
     CKW(cudaStreamWaitEvent(h->stream, W->ev[1 + k], 0));
   }
@@ -232,8 +235,9 @@ void wt_wavelet_release(wt_handle* h) {
   if (!h || !h->wav) return;
   for (cudaEvent_t e : ctx(h)->ev)
     if (e) cudaEventDestroy(e);
-  for (cudaEvent_t e : ctx(h)->fork)
-    if (e) cudaEventDestroy(e);
+  for (auto* v : {&ctx(h)->fork, &ctx(h)->ready_v, &ctx(h)->ready_s})
+    for (cudaEvent_t e : *v)
+      if (e) cudaEventDestroy(e);
   for (cudaStream_t s : ctx(h)->side)
     if (s) cudaStreamDestroy(s);
   for (void* p : ctx(h)->allocs) cudaFree(p);
@@ -310,10 +314,16 @@ int wt_wavelet_setup(wt_handle* h) {
     k_rf_plan<<<nb(ne), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), V.rf_pi, V.rf_pd);
     CKW(cudaGetLastError());
   }
-  for (cudaStream_t& s : W->side) CKW(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  int least = 0, greatest = 0;
+  CKW(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  CKW(cudaStreamCreateWithPriority(&W->side[0], cudaStreamNonBlocking, greatest));
+  for (int k = 1; k < 4; ++k) CKW(cudaStreamCreateWithPriority(&W->side[k], cudaStreamNonBlocking, least));
   for (cudaEvent_t& e : W->ev) CKW(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   W->fork.assign(W->L.size(), nullptr);
-  for (cudaEvent_t& e : W->fork) CKW(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  W->ready_v.assign(W->L.size(), nullptr);
+  W->ready_s.assign(W->L.size(), nullptr);
+  for (auto* v : {&W->fork, &W->ready_v, &W->ready_s})
+    for (cudaEvent_t& e : *v) CKW(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   zero_wavelets(h);
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
@@ -546,6 +556,15 @@ const unsigned char* wt_level_need(wt_handle* h) {
   return W->need[NEED_R & 1];  // the last dilation's output
 }
 int wt_level_skip_epoch(wt_handle* h) { return ctx(h)->skip_epoch; }
+
+// Make stream st wait until the last inverse transform has completed level's state.
+int wt_level_ready_wait(wt_handle* h, int level, cudaStream_t st) {
+  WavCtx* W = ctx(h);
+  const int q = level - h->level_start;
+  CKW(cudaStreamWaitEvent(st, W->ready_v[q], 0));
+  if (q > 0) CKW(cudaStreamWaitEvent(st, W->ready_s[q], 0));
+  return WT_OK;
+}
 int wt_level_need_refresh(wt_handle* h) {
   WavCtx* W = ctx(h);
   if (W->need[0] && W->skip_inactive && !W->need_ok) return wt_level_need_build(h);

@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--kernels-only", action="store_true")
     p.add_argument("--wavelets-only", action="store_true")
+    p.add_argument("--trace", default=None, metavar="PATH",
+                   help="record a CUDA kernel timeline of --steps adaptive steps (after --warmup) into PATH "
+                        "(Chrome trace) and print its summary instead of the bench line")
     return p.parse_args()
 
 
@@ -306,8 +309,8 @@ def adaptive_launches(L):
     outer and inner velocity, compression fused) and four inverse-transform
     kernels per coarse level), wt_mask_build's sweeps (each comm_masks is
     one launch over all levels, 3L + 3 of them), compression and the inverse
-    transform.  The mask sequence ends with the finest level's needed-node
-    map (a seed and six dilation launches)."""
+    transform.  The mask sequence ends with the needed-node maps of the
+    levels above level_start (a seed and six dilation launches)."""
     stage = 3 * L + 3 * (L - 1) + 3 * (L - 1) + 4 * (L - 1)
     comm = 3 * L + 3
     masks = ((L - 1) + 1 + 2 * (L - 1) + L + (L - 1) + 2 * (L - 1) + 2 * (L - 2) + 1 + 2 * (L - 2) + 1 + L
@@ -754,6 +757,55 @@ def bench_kernels(args):
                       "unit": "simulated days per wall-clock hour"}), flush=True)
 
 
+def bench_trace(args):
+    """Kernel timeline of graph-replayed adaptive steps (torch.profiler's CUDA
+    activity trace, which sees every kernel of the process with its stream):
+    per step the span, the time some kernel is running, and each kernel's
+    summed duration.  A profiling aid; its times are not bench values."""
+    import collections
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    from wavetrisk_hydrostatic_b200 import Grid, OceanParams
+    from wavetrisk_hydrostatic_b200.adaptive import AdaptiveOcean
+    from wavetrisk_hydrostatic_b200.cases import bump_state
+
+    torch.cuda.set_device(0)
+    ph = OceanParams()
+    G = Grid(args.lmin, args.level, radius=6371e3)
+    levels = [G.level(l) for l in range(args.lmin, args.level + 1)]
+    model = AdaptiveOcean(G, args.lmin, args.level, args.nz, [bump_state(g, args.nz, seed=1, ph=ph) for g in levels],
+                          ph, tol=TOL_AD)
+    for _ in range(args.warmup):
+        model.step(DT_AD)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(args.steps):
+            model.step(DT_AD)
+        torch.cuda.synchronize()
+    prof.export_chrome_trace(args.trace)
+    ev = [e for e in json.load(open(args.trace))["traceEvents"] if e.get("cat") == "kernel"]
+    iv = sorted((e["ts"], e["ts"] + e["dur"]) for e in ev)
+    busy, (cs, ce) = 0.0, iv[0]
+    for a, b in iv[1:]:
+        if a > ce:
+            busy += ce - cs
+            cs, ce = a, b
+        else:
+            ce = max(ce, b)
+    busy += ce - cs
+    span = max(b for _, b in iv) - iv[0][0]
+    tot = collections.Counter()
+    for e in ev:
+        tot[e["name"].split("(")[0].replace("void ", "")] += e["dur"]
+    print(json.dumps({"workload": f"adaptive run J{args.lmin}..J{args.level}, {args.nz} layers", "steps": args.steps,
+                      "kernels": len(ev), "span_us_per_step": span / args.steps,
+                      "busy_us_per_step": busy / args.steps,
+                      "kernel_us_per_step": {k: v / args.steps for k, v in tot.most_common()}}), flush=True)
+    model.close()
+
+
 def bench_wavelets(args):
     import torch
 
@@ -769,6 +821,8 @@ def main():
         bench_reference(args)
     elif args.kernels_only:
         bench_kernels(args)
+    elif args.trace:
+        bench_trace(args)
     elif args.wavelets_only:
         bench_wavelets(args)
     else:

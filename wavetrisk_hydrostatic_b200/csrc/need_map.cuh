@@ -1,16 +1,19 @@
-// Nodes of the finest level whose step1 and trend results can reach the state
-// after WT_after_step.  After every RK stage the finest level is rebuilt by
-// the inverse transform from the next coarser level and the wavelets kept by
-// compress_wavelets, so its stage results are read only
-//   * by the trend where mask_n >= TRSK (stencils of radius 2),
-//   * by the forward wavelets of slots with mask >= ADJZONE (radius 2),
-//   * by the restriction into parents with mask >= RESTRCT (radius 3 around the
-//     parent's child node), and by the coarser trend's restricted velocity
-//     source (child edges with mask >= ADJZONE).
+// Nodes whose step1 and trend results can reach the state after WT_after_step,
+// for every level above level_start.  After every RK stage the inverse
+// transform rebuilds such a level from the next coarser one and the wavelets
+// kept by compress_wavelets, so its stage results are read only
+//   * by its trend where mask_n >= TRSK (stencils of hex radius 2),
+//   * by the forward wavelets of its slots with mask >= ADJZONE (radius 2),
+//   * by the restriction into the parents with mask >= RESTRCT (radius 4 around
+//     the parent's node) and by the coarser trend's restricted velocity source
+//     (child edges with mask >= ADJZONE),
+//   * as the parent velocities of the next finer level's forward wavelets
+//     (radius 2 around the parents of that level's slots with mask >= TRSK).
 // The map seeds those nodes and dilates them NEED_R hex steps through the ghost
 // remaps; the lozenge corners (pentagons, poles), whose neighbourhoods the
-// remaps describe only for the stencils that use them, are always in the map.
-// Values of the map are read through nsrc: need[nsrc[x]].
+// remaps describe only for the stencils that use them, are always in it.
+// Values are read through nsrc: need[nsrc[x]].  level_start has no map: the
+// inverse transform does not rebuild it.
 #pragma once
 #include "wavelet_kernels.cuh"
 
@@ -20,45 +23,81 @@ namespace wtw {
 #define WT_NEED_R 6
 #endif
 constexpr int NEED_R = WT_NEED_R;
+constexpr int NEED_MAXL = 16;
 
-// seed of every padded slot of level C (parent level P)
-__global__ void k_need_seed(WLev C, WLev P, unsigned char* __restrict__ out) {
-  const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= C.NN) return;
-  const int PP = C.P * C.P;
-  const int d = (int)(x / PP), r = (int)(x - (int64_t)d * PP);
-  const int i = r % C.P - 2, j = r / C.P - 2, n = C.n;
-  int v;
-  if (i >= 0 && j >= 0 && i < n && j < n) {
-    v = C.mask_n[x] >= TRSK || C.mask_e[x] >= TRSK || C.mask_e[C.NN + x] >= TRSK || C.mask_e[2 * C.NN + x] >= TRSK;
-    if (!v && !(i & 1) && !(j & 1)) {
-      const int p = nid(P, d, i / 2, j / 2);
-      v = P.mask_n[p] >= RESTRCT || P.mask_e[p] >= RESTRCT || P.mask_e[P.NN + p] >= RESTRCT ||
-          P.mask_e[2 * P.NN + p] >= RESTRCT;
-    }
-    const int c = NEED_R + 1;
-    if ((i <= c || i >= n - 1 - c) && (j <= c || j >= n - 1 - c)) v = 1;
-  } else {
-    v = __ldg(C.nsrc + x) == (int)x;  // a slot outside [0, n)^2 that is its own source
-  }
-  out[x] = (unsigned char)v;
+// Entry q is level level_start + q; entry 0 (level_start) only lends its masks.
+struct NeedLev {
+  int n, P, NN;
+  const int* nsrc;
+  const int* mask_n;
+  const int* mask_e;
+  unsigned char* buf[2];  // map and dilation scratch (null on entry 0)
+};
+struct NeedSet {
+  int nl;                      // entries, level_start included
+  int start[NEED_MAXL + 1];    // thread offsets of entries 1..nl-1 (start[1] = 0)
+  NeedLev L[NEED_MAXL];
+};
+
+__device__ __forceinline__ bool need_entry(const NeedSet& S, int64_t t, int& q, int& x) {
+  if (t >= S.start[S.nl]) return false;
+  q = 1;
+  while (t >= S.start[q + 1]) ++q;
+  x = (int)(t - S.start[q]);
+  return true;
 }
 
-// one hex step: a slot is needed if it or one of its six neighbours is
-__global__ void k_need_dilate(WLev C, const unsigned char* __restrict__ in, unsigned char* __restrict__ out) {
-  const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= C.NN) return;
-  const int PP = C.P * C.P;
-  const int d = (int)(x / PP), r = (int)(x - (int64_t)d * PP);
-  const int i = r % C.P - 2, j = r / C.P - 2;
-  int v = in[__ldg(C.nsrc + x)];
+__device__ __forceinline__ bool any_mask(const NeedLev& E, int x, int thr) {
+  return E.mask_n[x] >= thr || E.mask_e[x] >= thr || E.mask_e[E.NN + x] >= thr || E.mask_e[2 * E.NN + x] >= thr;
+}
+
+// seeds of every padded slot of every entry into buf[0]
+__global__ void k_need_seed(NeedSet S) {
+  int q, x;
+  if (!need_entry(S, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, q, x)) return;
+  const NeedLev& E = S.L[q];
+  const int PP = E.P * E.P;
+  const int d = x / PP, r = x - d * PP;
+  const int i = r % E.P - 2, j = r / E.P - 2, n = E.n;
+  int v;
+  if (i >= 0 && j >= 0 && i < n && j < n) {
+    v = any_mask(E, x, TRSK);
+    if (!v && !(i & 1) && !(j & 1)) {  // parent node with a restricted value or flux
+      const NeedLev& Pa = S.L[q - 1];
+      v = any_mask(Pa, (d * Pa.P + j / 2 + 2) * Pa.P + i / 2 + 2, RESTRCT);
+    }
+    if (!v && q + 1 < S.nl) {  // parent of finer slots whose wavelets are computed
+      const NeedLev& C = S.L[q + 1];
+      for (int c = 0; c < 4 && !v; ++c)
+        v = any_mask(C, (d * C.P + 2 * j + (c >> 1) + 2) * C.P + 2 * i + (c & 1) + 2, TRSK);
+    }
+    const int cr = NEED_R + 1;
+    if ((i <= cr || i >= n - 1 - cr) && (j <= cr || j >= n - 1 - cr)) v = 1;
+  } else {
+    v = __ldg(E.nsrc + x) == x;  // a slot outside [0, n)^2 that is its own source
+  }
+  E.buf[0][x] = (unsigned char)v;
+}
+
+// one hex step from buf[r & 1] into buf[(r + 1) & 1]: a slot is needed if it
+// or one of its six neighbours is
+__global__ void k_need_dilate(NeedSet S, int r) {
+  int q, x;
+  if (!need_entry(S, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, q, x)) return;
+  const NeedLev& E = S.L[q];
+  const unsigned char* __restrict__ in = E.buf[r & 1];
+  const int PP = E.P * E.P;
+  const int d = x / PP, rr = x - d * PP;
+  const int i = rr % E.P - 2, j = rr / E.P - 2;
+  int v = in[__ldg(E.nsrc + x)];
   const int di[6] = {1, -1, 0, 0, 1, -1}, dj[6] = {0, 0, 1, -1, 1, -1};
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    const int a = i + di[q], b = j + dj[q];
-    if (inr(C, a, b)) v |= in[__ldg(C.nsrc + nid(C, d, a, b))];
+  for (int k = 0; k < 6; ++k) {
+    const int a = i + di[k], b = j + dj[k];
+    if (a >= -2 && b >= -2 && a < E.n + 2 && b < E.n + 2)
+      v |= in[__ldg(E.nsrc + (d * E.P + b + 2) * E.P + a + 2)];
   }
-  out[x] = (unsigned char)v;
+  E.buf[(r + 1) & 1][x] = (unsigned char)v;
 }
 
 }  // namespace wtw

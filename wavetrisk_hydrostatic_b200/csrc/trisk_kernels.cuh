@@ -194,10 +194,12 @@ __device__ __noinline__ void post_corner(const LevelDev L, int c, int d, int64_t
 __global__ void __launch_bounds__(NODE_TILE, 3)
     k_step1(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
             const double* __restrict__ velo, const double* __restrict__ mean_m, const double* __restrict__ mean_t,
-            const double* __restrict__ phik, const double* __restrict__ pterm, Step1Out out) {
+            const double* __restrict__ phik, const double* __restrict__ pterm, Step1Out out,
+            const unsigned char* __restrict__ need) {
   int k, id, i, j;
   if (!layer_node(L, nz, k, id, i, j)) return;
   if (i < 0 || j < 0 || i > L.n || j > L.n) return;
+  if (need && !need[__ldg(L.nsrc + id)]) return;  // needed-node map (need_map.cuh)
   const int NN = L.NN;
   const int P = L.P;
   const int idN = id + P, idE = id + 1, idS = id - P, idW = id - 1, idNE = id + P + 1, idSW = id - P - 1;

@@ -363,7 +363,7 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
     k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, s>>>(L, nz, nbx, nby, m, t, v, h->mean_m, h->phik, h->pterm, so,
                                                            h->dflag, h->s1maps[sb], nullptr);
   } else {
-    k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so);
+    k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so, nullptr);
   }
   TE(2);
   TrendIO io{};
@@ -419,7 +419,7 @@ int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, co
     k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, s>>>(L, nz, nbx, nby, m, t, v, mean_m, phik, pterm, so,
                                                            h->dflag, *maps, need);
   } else {
-    k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so);
+    k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so, need);
   }
   CK(cudaGetLastError());
   return WT_OK;

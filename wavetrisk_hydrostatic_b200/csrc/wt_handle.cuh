@@ -84,8 +84,8 @@ void wt_trend_ml_release(wt_handle* h);
 // on the given state, into the given operator arrays (wt_api.cu).
 // With maps (the top level's step1 input maps of this state) the top level runs
 // the TMA-staged step1 when the handle selected it.
-// stream: the handle's when null.  need: the column leaves out the nodes outside
-// this needed-node map (need_map.cuh) and the TMA variant of step1 the tiles
+// stream: the handle's when null.  need: the column and the L1 step1 leave out
+// the nodes outside this needed-node map (need_map.cuh), the TMA step1 the tiles
 // with none of them; step1 reads the column's results only at its own node.
 // Tensor maps of the top level's trend inputs held in the given arrays (with the
 // level's geometry), for k_trend_tma; WT_ERR_STATE unless the TMA variant is on.
@@ -128,11 +128,12 @@ void wt_level_compress(wt_handle* h);
 // zero every wavelet array if a host upload wrote wavelets since the last
 // zeroing (stream-ordered; WT_after_step then writes only the slots it computes)
 void wt_level_clean_wavelets(wt_handle* h);
-// The finest level's needed-node map (need_map.cuh): build it from the current
-// masks (stream-ordered; the mask sequence does so at its end); the map the
-// RK stages may skip by, or null; the count of changes to WT_TUNE_SKIP_INACTIVE.
+// The needed-node maps of the levels above level_start (need_map.cuh): build
+// them from the current masks (stream-ordered; the mask sequence does so at its
+// end); the map a level's RK-stage kernels may skip by, or null; the count of
+// changes to WT_TUNE_SKIP_INACTIVE.
 int wt_level_need_build(wt_handle* h);
-const unsigned char* wt_level_need(wt_handle* h);
+const unsigned char* wt_level_need(wt_handle* h, int level);
 int wt_level_skip_epoch(wt_handle* h);
 // make stream st wait until the last inverse transform (wt_level_inverse or
 // WT_after_step) has completed level's state; only valid when that transform was

@@ -180,9 +180,9 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
                 const States* dest = nullptr, double hs = 0.0, bool wav = false, bool after_inverse = false) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const int nz = h->nz;
-  // With WT_after_step following (wav), the finest level's results are read
-  // only where the needed-node map says so (need_map.cuh).
-  const unsigned char* need = (wav && dest) ? wt_level_need(h) : nullptr;
+  // With WT_after_step following (wav), a level's results above level_start are
+  // read only where its needed-node map says so (need_map.cuh).
+  auto need = [&](int l) -> const unsigned char* { return (wav && dest) ? wt_level_need(h, l) : nullptr; };
   // Column + step1 of a level read only that level's state and write only its
   // own work fields, so the coarser levels' run beside the finest level's on
   // side streams (parallel branches of a captured graph).  The phase timer
@@ -202,7 +202,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
         CKM(cudaStreamWaitEvent(M->side[q], M->fork, 0));
       }
       if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern,
-                                  V.theta, nullptr, M->side[q]))
+                                  V.theta, nullptr, M->side[q], need(l)))
         return rc;
       CKM(cudaEventRecord(M->done[q], M->side[q]));
     }
@@ -231,7 +231,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
         }
       }
       if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft,
-                                  V.bern, V.theta, maps, nullptr, l == h->level_end ? need : nullptr))
+                                  V.bern, V.theta, maps, nullptr, need(l)))
         return rc;
       PE(tm, l == h->level_end ? PH_STEP1_TOP : PH_STEP1_COARSE);
       if (concurrent) CKM(cudaEventRecord(M->s1top, h->stream));
@@ -272,7 +272,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
       io.dst_m = dest->m[q]; io.dst_t = dest->t[q]; io.dst_v = dest->v[q];
       io.h = hs;
     }
-    if (l == h->level_end) io.need = need;
+    io.need = need(l);
     const unsigned chunks = (unsigned)((D.NN + wtk::NODE_TILE - 1) / wtk::NODE_TILE);
     PB(tm);
     if (l == h->level_end && M->tmaps_ok && base && dest) {  // TMA-staged, the same arithmetic

@@ -48,11 +48,13 @@ struct WavCtx {
   std::vector<cudaEvent_t> ready_v, ready_s;
   // scaling-field pointers put aside while WT_after_step runs on other arrays
   std::vector<WavLevel> bound_saved;
-  // needed-node map of the finest level (need_map.cuh) in need[NEED_R & 1], the
-  // other buffer its dilation scratch; need_ok once built from the current masks.  skip_inactive
+  // needed-node maps of the levels above level_start (need_map.cuh): level
+  // level_start + q uses need[NEED_R & 1] + need_off[q], the other buffer is the
+  // dilation scratch; need_ok once built from the current masks.  skip_inactive
   // lets the RK stages of the hierarchy leave the finest level's step1 and
   // trend out where the map is 0; skip_epoch counts its changes.
   unsigned char* need[2] = {nullptr, nullptr};
+  std::vector<size_t> need_off;
   bool need_ok = false;
   bool skip_inactive = true;
   int skip_epoch = 0;

@@ -283,11 +283,16 @@ int wt_wavelet_setup(wt_handle* h) {
     CKW(cudaMemcpy(V.mask_e, tol.data(), 3 * D.NN * sizeof(int), cudaMemcpyHostToDevice));
   }
   CKW(W->alloc(&W->thr, (size_t)3 * nz));
-  // needed-node map of the finest level and its dilation scratch
-  if (h->level_end > h->level_start) {
-    const size_t NN = (size_t)h->at(h->level_end).NN;
-    CKW(W->alloc(&W->need[0], NN));
-    CKW(W->alloc(&W->need[1], NN));
+  // needed-node maps of the levels above level_start and their dilation scratch
+  if (h->level_end > h->level_start && h->level_end - h->level_start < NEED_MAXL) {
+    size_t tot = 0;
+    W->need_off.assign(W->L.size(), 0);
+    for (int l = h->level_start + 1; l <= h->level_end; ++l) {
+      W->need_off[l - h->level_start] = tot;
+      tot += (size_t)h->at(l).NN;
+    }
+    CKW(W->alloc(&W->need[0], tot));
+    CKW(W->alloc(&W->need[1], tot));
   }
   // velocity-wavelet plans of every parent level
   for (int l = h->level_start; l < h->level_end; ++l) {
@@ -533,27 +538,42 @@ int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patc
   return wt_level_need_build(h);
 }
 
-// The finest level's needed-node map from the current masks (stream-ordered).
+// The needed-node maps of the levels above level_start from the current masks
+// (stream-ordered).
 int wt_level_need_build(wt_handle* h) {
   WavCtx* W = ctx(h);
   if (!W->need[0]) return WT_OK;
-  const int le = h->level_end;
-  const int64_t NN = h->at(le).NN;
-  k_need_seed<<<nb(NN), TPB, 0, h->stream>>>(view(h, le), view(h, le - 1), W->need[0]);
-  for (int r = 0; r < NEED_R; ++r)
-    k_need_dilate<<<nb(NN), TPB, 0, h->stream>>>(view(h, le), W->need[r & 1], W->need[(r + 1) & 1]);
+  NeedSet S{};
+  S.nl = h->level_end - h->level_start + 1;
+  for (int q = 0; q < S.nl; ++q) {
+    const DevLevel& D = h->at(h->level_start + q);
+    NeedLev& E = S.L[q];
+    E.n = D.n;
+    E.P = D.P;
+    E.NN = (int)D.NN;
+    E.nsrc = D.nsrc;
+    E.mask_n = W->L[q].mask_n;
+    E.mask_e = W->L[q].mask_e;
+    if (q > 0) {
+      E.buf[0] = W->need[0] + W->need_off[q];
+      E.buf[1] = W->need[1] + W->need_off[q];
+      S.start[q + 1] = S.start[q] + E.NN;
+    }
+  }
+  const unsigned g = nb(S.start[S.nl]);
+  k_need_seed<<<g, TPB, 0, h->stream>>>(S);
+  for (int r = 0; r < NEED_R; ++r) k_need_dilate<<<g, TPB, 0, h->stream>>>(S, r);
   CKW(cudaGetLastError());
   W->need_ok = true;
   return WT_OK;
 }
 
-// The map the finest level's step1 and trend may skip by, or null (no map,
-// skipping turned off, or masks uploaded since the last build and no build
-// wanted now).
-const unsigned char* wt_level_need(wt_handle* h) {
+// The map level's step1 and trend may skip by, or null (level_start, no map,
+// skipping turned off, or masks uploaded since the last build).
+const unsigned char* wt_level_need(wt_handle* h, int level) {
   WavCtx* W = ctx(h);
-  if (!W->need[0] || !W->skip_inactive || !W->need_ok) return nullptr;
-  return W->need[NEED_R & 1];  // the last dilation's output
+  if (level <= h->level_start || !W->need[0] || !W->skip_inactive || !W->need_ok) return nullptr;
+  return W->need[NEED_R & 1] + W->need_off[level - h->level_start];  // the last dilation's output
 }
 int wt_level_skip_epoch(wt_handle* h) { return ctx(h)->skip_epoch; }
 

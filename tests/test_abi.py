@@ -42,3 +42,12 @@ def test_create_without_device_fails_cleanly():
     desc.levels = None
     rc = lib.wt_create(ctypes.byref(desc), ctypes.byref(h))
     assert rc == _native.WT_ERR_ARG
+
+
+def test_tune_rejects_bad_arguments_without_a_device():
+    """wt_tune checks its arguments before touching a handle or the device."""
+    lib = _native.lib()
+    assert lib.wt_tune(None, 1, -1) == _native.WT_ERR_ARG      # WT_TUNE_WAVELET_LAYERS out of range
+    assert lib.wt_tune(None, 1, 65) == _native.WT_ERR_ARG
+    assert lib.wt_tune(None, 2, 1) == _native.WT_ERR_ARG       # WT_TUNE_SKIP_INACTIVE needs a handle
+    assert lib.wt_tune(None, 99, 0) == _native.WT_ERR_ARG      # unknown parameter

@@ -101,3 +101,60 @@ __global__ void k_need_dilate(NeedSet S, int r) {
 }
 
 }  // namespace wtw
+
+namespace wtw {
+
+// Parents each inverse transform of an intermediate RK stage rebuilds.  Between
+// the stages a level's state is read only by the next stage's step1 (radius 2
+// around its needed nodes) and, as the parent of the next finer level, by that
+// level's reconstruction (radius 2 around the parents it rebuilds).  From the
+// finest level down: rec(c) = dilate(need(c) | recpar(c), 2) on child level c,
+// recpar(c-1) = dilate(parents of rec(c), 2) on its parent level; a parent is
+// rebuilt where recpar says so (read through nsrc).  The step's last stage and
+// the inverse after adapt rebuild every parent.
+struct MapLev {
+  int n, P, NN;
+  const int* nsrc;
+};
+
+__global__ void k_map_or(int NN, const unsigned char* __restrict__ a, const unsigned char* __restrict__ b,
+                         unsigned char* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x < NN) out[x] = (unsigned char)(a[x] | (b ? b[x] : 0));
+}
+
+__global__ void k_map_dilate(MapLev L, const unsigned char* __restrict__ in, unsigned char* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= L.NN) return;
+  const int PP = L.P * L.P;
+  const int d = x / PP, r = x - d * PP;
+  const int i = r % L.P - 2, j = r / L.P - 2;
+  int v = in[__ldg(L.nsrc + x)];
+  const int di[6] = {1, -1, 0, 0, 1, -1}, dj[6] = {0, 0, 1, -1, 1, -1};
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const int a = i + di[k], b = j + dj[k];
+    if (a >= -2 && b >= -2 && a < L.n + 2 && b < L.n + 2)
+      v |= in[__ldg(L.nsrc + (d * L.P + b + 2) * L.P + a + 2)];
+  }
+  out[x] = (unsigned char)v;
+}
+
+// parent slot x of level Pa is marked if one of its four children is marked
+__global__ void k_map_up(MapLev C, MapLev Pa, const unsigned char* __restrict__ cin, unsigned char* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= Pa.NN) return;
+  const int PP = Pa.P * Pa.P;
+  const int d = x / PP, r = x - d * PP;
+  const int ip = r % Pa.P - 2, jp = r / Pa.P - 2;
+  int v = 0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int a = 2 * ip + (c & 1), b = 2 * jp + (c >> 1);
+    if (a >= -2 && b >= -2 && a < C.n + 2 && b < C.n + 2)
+      v |= cin[__ldg(C.nsrc + (d * C.P + b + 2) * C.P + a + 2)];
+  }
+  out[x] = (unsigned char)v;
+}
+
+}  // namespace wtw

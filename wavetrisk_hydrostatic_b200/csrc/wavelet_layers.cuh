@@ -57,6 +57,12 @@ __device__ __forceinline__ bool parent_of(int m, int nz, int lpt, int& d, int& i
   return true;
 }
 
+// Whether the inverse transform rebuilds parent (d, ip, jp) of level Pa: every
+// parent when rec is null, else where the parent map rec (need_map.cuh) says so.
+__device__ __forceinline__ bool rebuilt(const unsigned char* __restrict__ rec, const WLev& Pa, int d, int ip, int jp) {
+  return !rec || rec[__ldg(Pa.nsrc + nid(Pa, d, ip, jp))];
+}
+
 // Interp_node's four weights and hex_inv at child node (i, j) with its four
 // neighbours' codes.
 struct NodeInterp {
@@ -130,10 +136,12 @@ __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int
 }
 
 // Reconstruct_scalar (src/wavelet.f90:614-640), parents [0, np)^2.
-__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_recon_scalar_l(WLev C, int np, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_recon_scalar_l(WLev Pa, WLev C, int np, int nz, int lpt,
+                                                                         const unsigned char* __restrict__ rec) {
   int d, ip, jp;
   int k0, k1;
   if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
+  if (!rebuilt(rec, Pa, d, ip, jp)) return;
   const int i = 2 * ip, j = 2 * jp;
   const int ci[3] = {i + 1, i + 1, i}, cj[3] = {j, j + 1, j + 1};
   int self[3], at[3];
@@ -159,11 +167,13 @@ __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_recon_scalar_l(WLev C, 
 
 // Prolong_scalar (src/wavelet.f90:571-612), parents [0, np]^2: the eleven
 // lifting terms the reference sums.
-__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_prolong_l(WLev Pa, WLev C, int nz, int lpt) {
+__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_prolong_l(WLev Pa, WLev C, int nz, int lpt,
+                                                                    const unsigned char* __restrict__ rec) {
   const int np = Pa.n;
   int d, ip, jp;
   int k0, k1;
   if (!parent_of(np + 1, nz, lpt, d, ip, jp, k0, k1)) return;
+  if (!rebuilt(rec, Pa, d, ip, jp)) return;
   const int i = 2 * ip, j = 2 * jp;
   if (mn(C, d, i, j) == FROZEN) return;
   const int ti[11] = {i + 1, i + 1, i + 2, i, i - 1, i - 1, i - 2, i - 1, i, i - 1, i + 1};
@@ -542,17 +552,23 @@ __device__ __forceinline__ void plan_parent(int64_t u, int m, int& d, int& ip, i
 // Reconstruct_outer_velo (src/wavelet.f90:954-976) from the outer plan,
 // parents [0, np]^2, then Reconstruct_velo_penta by the corner parents.
 __global__ void __launch_bounds__(256) k_recon_outer_p(WLev Pa, WLev C, int nz, const int* __restrict__ pi,
-                                                       const double* __restrict__ pd) {
+                                                       const double* __restrict__ pd,
+                                                       const unsigned char* __restrict__ rec) {
   __shared__ int si[OP_NI][32];
   __shared__ double sd[OP_ND][32];
   const int np = Pa.n, m = np + 1;
   const int64_t ne = (int64_t)10 * m * m, u0 = (int64_t)blockIdx.x * 32;
   const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
+  int d = 0, ip = 0, jp = 0;
+  bool live = u0 + x < ne;
+  if (live) {
+    plan_parent(u0 + x, m, d, ip, jp);
+    live = rebuilt(rec, Pa, d, ip, jp);
+  }
+  if (!__syncthreads_or(live)) return;
   stage_plan<OP_NI, OP_ND>(si, sd, pi, pd, ne, u0, (int)min((int64_t)32, ne - u0));
   __syncthreads();
-  if (u0 + x >= ne) return;
-  int d, ip, jp;
-  plan_parent(u0 + x, m, d, ip, jp);
+  if (!live) return;
   const int i = 2 * ip, j = 2 * jp;
   for (int e = 0; e < 3; ++e) {
     const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
@@ -586,17 +602,23 @@ __device__ __forceinline__ int inner_target(const WLev& C, int q, int d, int i, 
 // Reconstruct_inner_velo (src/wavelet.f90:978-1003) from the inner plan,
 // parents [0, np)^2.
 __global__ void __launch_bounds__(256, WL_PLAN_MINB) k_recon_inner_p(WLev Pa, WLev C, int nz, const int* __restrict__ pi,
-                                                       const double* __restrict__ pd) {
+                                                       const double* __restrict__ pd,
+                                                       const unsigned char* __restrict__ rec) {
   __shared__ int si[IP_NI][32];
   __shared__ double sd[IP_ND][32];
   const int m = Pa.n;
   const int64_t ne = (int64_t)10 * m * m, u0 = (int64_t)blockIdx.x * 32;
   const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
+  int d = 0, ip = 0, jp = 0;
+  bool live = u0 + x < ne;
+  if (live) {
+    plan_parent(u0 + x, m, d, ip, jp);
+    live = rebuilt(rec, Pa, d, ip, jp);
+  }
+  if (!__syncthreads_or(live)) return;
   stage_plan<IP_NI, IP_ND>(si, sd, pi, pd, ne, u0, (int)min((int64_t)32, ne - u0));
   __syncthreads();
-  if (u0 + x >= ne) return;
-  int d, ip, jp;
-  plan_parent(u0 + x, m, d, ip, jp);
+  if (!live) return;
   const int i = 2 * ip, j = 2 * jp;
   for (int k = y; k < nz; k += ny) {
     const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;

@@ -120,7 +120,10 @@ int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double
 void wt_level_wav_bind(wt_handle* h, double* const* m, double* const* t, double* const* v);
 void wt_level_wav_unbind(wt_handle* h);
 int wt_level_wav_forward_pair(wt_handle* h, int level);
-int wt_level_wav_finish(wt_handle* h);
+// partial: the inverse rebuilds only the parents of wt_level_rec (an
+// intermediate RK stage, whose state the next stage reads only where needed)
+int wt_level_wav_finish(wt_handle* h, bool partial = false);
+const unsigned char* wt_level_rec(wt_handle* h, int level);
 // adapt's mask sequence without host synchronisation (capturable), compression
 // and inverse transform of the hierarchy, and the threshold upload (wt_wavelet.cu).
 int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq);

@@ -336,7 +336,7 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm) {
       wt_level_wav_bind(h, dest.m.data(), dest.t.data(), dest.v.data());
       wt_level_clean_wavelets(h);
       int rc = trend_multi(h, src, nullptr, &q, &dest, hs[stage], true, stage > 0);
-      if (!rc) rc = wt_level_wav_finish(h);
+      if (!rc) rc = wt_level_wav_finish(h, stage < 3);  // the last stage's state is the step's result
       wt_level_wav_unbind(h);
       if (rc) return rc;
     }

@@ -55,6 +55,11 @@ struct WavCtx {
   // trend out where the map is 0; skip_epoch counts its changes.
   unsigned char* need[2] = {nullptr, nullptr};
   std::vector<size_t> need_off;
+  // parents the inverse transforms of the intermediate RK stages rebuild, per
+  // parent level (need_map.cuh), at recpar + rec_off[q]; rscr: scratch maps
+  unsigned char* recpar = nullptr;
+  std::vector<size_t> rec_off;
+  unsigned char* rscr[2] = {nullptr, nullptr};
   bool need_ok = false;
   bool skip_inactive = true;
   int skip_epoch = 0;

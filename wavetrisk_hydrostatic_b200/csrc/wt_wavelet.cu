@@ -135,7 +135,7 @@ void launch_velo_wc(wt_handle* h, int l, cudaStream_t s, cudaStream_t si) {
 // scalars and the velocity reconstruct independently of each other, so the
 // scalar chain (Prolong_scalar, Reconstruct_scalar per level) runs on a side
 // stream beside the velocity chain (outer, then inner edges per level).
-void inverse(wt_handle* h) {
+void inverse(wt_handle* h, bool partial = false) {
   const int nz = h->nz;
   WavCtx* W = ctx(h);
   cudaStream_t s = h->stream, sa = W->side[0];
@@ -146,12 +146,13 @@ void inverse(wt_handle* h) {
     const int np = h->at(l).n, q = l + 1 - h->level_start;
     const WLev P = view(h, l), C = view(h, l + 1);
     const int64_t par1 = (int64_t)10 * (np + 1) * (np + 1), par0 = (int64_t)10 * np * np;
-    k_prolong_l<<<nbl(par1, nz), TPBL, 0, sa>>>(P, C, nz, lpt_for(nz));
-    k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, sa>>>(C, np, nz, lpt_for(nz));
+    const unsigned char* rec = partial ? wt_level_rec(h, l) : nullptr;
+    k_prolong_l<<<nbl(par1, nz), TPBL, 0, sa>>>(P, C, nz, lpt_for(nz), rec);
+    k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, sa>>>(P, C, np, nz, lpt_for(nz), rec);
     cudaEventRecord(W->ready_s[q], sa);
     const WavLevel& V = W->L[l - h->level_start];
-    k_recon_outer_p<<<plan_grid(par1), plan_block(nz), 0, s>>>(P, C, nz, V.op_i, V.op_d);
-    k_recon_inner_p<<<plan_grid(par0), plan_block(nz), 0, s>>>(P, C, nz, V.ip_i, V.ip_d);
+    k_recon_outer_p<<<plan_grid(par1), plan_block(nz), 0, s>>>(P, C, nz, V.op_i, V.op_d, rec);
+    k_recon_inner_p<<<plan_grid(par0), plan_block(nz), 0, s>>>(P, C, nz, V.ip_i, V.ip_d, rec);
     cudaEventRecord(W->ready_v[q], s);
   }
   cudaEventRecord(W->ev[1], sa);
@@ -207,13 +208,13 @@ int wt_level_wav_forward_pair(wt_handle* h, int l) {
 
 // The end of WT_after_step once every level pair's forward wavelets are
 // launched: join the side streams, then the inverse transform.
-int wt_level_wav_finish(wt_handle* h) {
+int wt_level_wav_finish(wt_handle* h, bool partial) {
   WavCtx* W = ctx(h);
   for (int k = 1; k < 4; ++k) {
     CKW(cudaEventRecord(W->ev[1 + k], W->side[k]));
     CKW(cudaStreamWaitEvent(h->stream, W->ev[1 + k], 0));
   }
-  inverse(h);
+  inverse(h, partial);
   CKW(cudaGetLastError());
   return WT_OK;
 }
@@ -293,6 +294,18 @@ int wt_wavelet_setup(wt_handle* h) {
     }
     CKW(W->alloc(&W->need[0], tot));
     CKW(W->alloc(&W->need[1], tot));
+    size_t ptot = 0, mx = 0;
+    W->rec_off.assign(W->L.size(), 0);
+    for (int l = h->level_start; l <= h->level_end; ++l) {
+      if (l < h->level_end) {
+        W->rec_off[l - h->level_start] = ptot;
+        ptot += (size_t)h->at(l).NN;
+      }
+      mx = std::max(mx, (size_t)h->at(l).NN);
+    }
+    CKW(W->alloc(&W->recpar, ptot));
+    CKW(W->alloc(&W->rscr[0], mx));
+    CKW(W->alloc(&W->rscr[1], mx));
   }
   // velocity-wavelet plans of every parent level
   for (int l = h->level_start; l < h->level_end; ++l) {
@@ -561,11 +574,39 @@ int wt_level_need_build(wt_handle* h) {
     }
   }
   const unsigned g = nb(S.start[S.nl]);
-  k_need_seed<<<g, TPB, 0, h->stream>>>(S);
-  for (int r = 0; r < NEED_R; ++r) k_need_dilate<<<g, TPB, 0, h->stream>>>(S, r);
+  cudaStream_t s = h->stream;
+  k_need_seed<<<g, TPB, 0, s>>>(S);
+  for (int r = 0; r < NEED_R; ++r) k_need_dilate<<<g, TPB, 0, s>>>(S, r);
+  // parents rebuilt by the intermediate stages' inverse transforms, finest first
+  auto ml = [&](int l) {
+    const DevLevel& D = h->at(l);
+    return MapLev{D.n, D.P, (int)D.NN, D.nsrc};
+  };
+  unsigned char *A = W->rscr[0], *B = W->rscr[1];
+  for (int l = h->level_end - 1; l >= h->level_start; --l) {
+    const int c = l + 1;
+    const MapLev Lc = ml(c), Lp = ml(l);
+    const unsigned char* nc = W->need[NEED_R & 1] + W->need_off[c - h->level_start];
+    const unsigned char* rc = c < h->level_end ? W->recpar + W->rec_off[c - h->level_start] : nullptr;
+    unsigned char* rp = W->recpar + W->rec_off[l - h->level_start];
+    k_map_or<<<nb(Lc.NN), TPB, 0, s>>>(Lc.NN, nc, rc, A);
+    k_map_dilate<<<nb(Lc.NN), TPB, 0, s>>>(Lc, A, B);
+    k_map_dilate<<<nb(Lc.NN), TPB, 0, s>>>(Lc, B, A);  // rec(c)
+    k_map_up<<<nb(Lp.NN), TPB, 0, s>>>(Lc, Lp, A, B);
+    k_map_dilate<<<nb(Lp.NN), TPB, 0, s>>>(Lp, B, A);
+    k_map_dilate<<<nb(Lp.NN), TPB, 0, s>>>(Lp, A, rp);  // recpar(l)
+  }
   CKW(cudaGetLastError());
   W->need_ok = true;
   return WT_OK;
+}
+
+// The parents of level that the inverse transform of an intermediate RK stage
+// rebuilds, or null (rebuild every parent).
+const unsigned char* wt_level_rec(wt_handle* h, int level) {
+  WavCtx* W = ctx(h);
+  if (level >= h->level_end || !W->recpar || !W->skip_inactive || !W->need_ok) return nullptr;
+  return W->recpar + W->rec_off[level - h->level_start];
 }
 
 // The map level's step1 and trend may skip by, or null (level_start, no map,

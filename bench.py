@@ -310,11 +310,13 @@ def adaptive_launches(L):
     kernels per coarse level), wt_mask_build's sweeps (each comm_masks is
     one launch over all levels, 3L + 3 of them), compression and the inverse
     transform.  The mask sequence ends with the needed-node maps of the
-    levels above level_start (a seed and six dilation launches)."""
+    levels above level_start (a seed and six dilation launches) and the
+    reconstruct maps of the intermediate stages' inverse transforms (six
+    launches per coarser level)."""
     stage = 3 * L + 3 * (L - 1) + 3 * (L - 1) + 4 * (L - 1)
     comm = 3 * L + 3
     masks = ((L - 1) + 1 + 2 * (L - 1) + L + (L - 1) + 2 * (L - 1) + 2 * (L - 2) + 1 + 2 * (L - 2) + 1 + L
-             + comm + (7 if L > 1 else 0))
+             + comm + (7 + 6 * (L - 1) if L > 1 else 0))
     return 4 * stage + masks + (L - 1) + 4 * (L - 1)
 
 

@@ -317,7 +317,8 @@ def adaptive_launches(L):
     comm = 3 * L + 3
     masks = ((L - 1) + 1 + 2 * (L - 1) + L + (L - 1) + 2 * (L - 1) + 2 * (L - 2) + 1 + 2 * (L - 2) + 1 + L
              + comm + (7 + 6 * (L - 1) if L > 1 else 0))
-    return 4 * stage + masks + (L - 1) + 4 * (L - 1)
+    # the last stage's inverse transform is left out (the one after adapt rebuilds the levels)
+    return 4 * stage - 4 * (L - 1) + masks + (L - 1) + 4 * (L - 1)
 
 
 def algorithmic_bytes_trend_ml(level, nz, n_on=None, n_own=None):

@@ -121,8 +121,10 @@ void wt_level_wav_bind(wt_handle* h, double* const* m, double* const* t, double*
 void wt_level_wav_unbind(wt_handle* h);
 int wt_level_wav_forward_pair(wt_handle* h, int level);
 // partial: the inverse rebuilds only the parents of wt_level_rec (an
-// intermediate RK stage, whose state the next stage reads only where needed)
-int wt_level_wav_finish(wt_handle* h, bool partial = false);
+// intermediate RK stage, whose state the next stage reads only where needed);
+// rebuild false: join the forward wavelets and leave the inverse out (its result
+// would be overwritten before anything reads it)
+int wt_level_wav_finish(wt_handle* h, bool partial = false, bool rebuild = true);
 const unsigned char* wt_level_rec(wt_handle* h, int level);
 // adapt's mask sequence without host synchronisation (capturable), compression
 // and inverse transform of the hierarchy, and the threshold upload (wt_wavelet.cu).

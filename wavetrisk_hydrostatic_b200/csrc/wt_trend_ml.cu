@@ -309,7 +309,10 @@ int wt_trend_multi(wt_handle* h) {
 }  // extern "C"
 
 namespace {
-int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm) {
+// last_inverse false: the last stage's WT_after_step computes its wavelets but
+// not the inverse transform, for a caller that rebuilds the hierarchy from
+// them next (adapt, then inverse_wavelet_transform) without reading the state.
+int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm, bool last_inverse = true) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const States q = hierarchy_state(h);
   States q1;
@@ -336,7 +339,8 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm) {
       wt_level_wav_bind(h, dest.m.data(), dest.t.data(), dest.v.data());
       wt_level_clean_wavelets(h);
       int rc = trend_multi(h, src, nullptr, &q, &dest, hs[stage], true, stage > 0);
-      if (!rc) rc = wt_level_wav_finish(h, stage < 3);  // the last stage's state is the step's result
+      // the last stage's state is the step's result: rebuilt completely, unless the caller rebuilds it
+      if (!rc) rc = wt_level_wav_finish(h, stage < 3, stage < 3 || s < nsteps - 1 || last_inverse);
       wt_level_wav_unbind(h);
       if (rc) return rc;
     }
@@ -386,7 +390,10 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
     }
     cudaGraph_t g;
     CKM(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = rk4_multi(h, dt, 1, nullptr);
+    // adapt reads wavelets and masks only, and the inverse transform after it
+    // rebuilds every level above level_start: the last stage's own inverse is
+    // left out
+    int rc = rk4_multi(h, dt, 1, nullptr, false);
     if (!rc) rc = wt_level_mask_sequence(h, level_fill, max_level, 0, nullptr);
     if (!rc) {
       wt_level_compress(h);

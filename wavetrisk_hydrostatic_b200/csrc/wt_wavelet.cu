@@ -208,13 +208,13 @@ int wt_level_wav_forward_pair(wt_handle* h, int l) {
 
 // The end of WT_after_step once every level pair's forward wavelets are
 // launched: join the side streams, then the inverse transform.
-int wt_level_wav_finish(wt_handle* h, bool partial) {
+int wt_level_wav_finish(wt_handle* h, bool partial, bool rebuild) {
   WavCtx* W = ctx(h);
   for (int k = 1; k < 4; ++k) {
     CKW(cudaEventRecord(W->ev[1 + k], W->side[k]));
     CKW(cudaStreamWaitEvent(h->stream, W->ev[1 + k], 0));
   }
-  inverse(h, partial);
+  if (rebuild) inverse(h, partial);
   CKW(cudaGetLastError());
   return WT_OK;
 }

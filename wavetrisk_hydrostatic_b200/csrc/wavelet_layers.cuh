@@ -90,11 +90,14 @@ __device__ __forceinline__ void child_interps(NodeInterp N[3], const WLev& C, in
 }
 
 // Compute_scalar_wavelets (src/wavelet.f90:642-670), parents [0, np)^2.
-// CMP: the wavelets are not zeroed beforehand and compress_wavelets follows
+// CMP 1: the wavelets are not zeroed beforehand and compress_wavelets follows
 // (WT_after_step), so each of the three child slots is written, with 0 where
 // the child's mask is below ADJZONE; the other slots of the level (parent-
-// coincident nodes, ghost rows) hold 0 from the last zeroing.
-template <bool CMP>
+// coincident nodes, ghost rows) hold 0 from the last zeroing.  CMP 2: the same
+// when the slots below ADJZONE already hold 0 (compress_wavelets ran under the
+// current masks), so only the kept slots are written.  CMP 0: the forward
+// transform (wavelets zeroed beforehand, no compression).
+template <int CMP>
 __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int np, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
@@ -110,7 +113,7 @@ __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int
     at[q] = nid(C, d, ci[q], cj[q]);
   }
   if (!(on[0] || on[1] || on[2])) {
-    if (CMP)
+    if (CMP == 1)
       for (int k = k0; k < k1; ++k)
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -130,7 +133,7 @@ __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int
       for (int q = 0; q < 3; ++q)
         if (on[q])
           wc[at[q]] = wn(s, self[q]) - node_eval(N[q], s);
-        else if (CMP)
+        else if (CMP == 1)
           wc[at[q]] = 0.0;
     }
 }
@@ -254,10 +257,11 @@ __device__ __forceinline__ double outer_eval(const OuterInterp& O, const double*
 
 // Compute_velo_wavelets' outer edges (src/wavelet.f90:672-710), parents
 // [0, np)^2, with the pentagon corrections of the corner parents.  CMP as for
-// k_scalar_wc_l: both child slots of each parent edge are written and
-// compress_vector's rule (0 where the slot's own mask is below ADJZONE) is
-// applied to them, after the pentagon corrections in the corner parents.
-template <bool CMP>
+// k_scalar_wc_l: both child slots of each parent edge are written (CMP 1; CMP 2
+// leaves out the pairs whose slots hold 0 already) and compress_vector's rule
+// (0 where the slot's own mask is below ADJZONE) is applied to them, after the
+// pentagon corrections in the corner parents.
+template <int CMP>
 __global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa, WLev C, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
@@ -269,14 +273,16 @@ __global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa,
     const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
     const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
     if (me(C, e, d, a2, b2) < ADJZONE) {
-      if (CMP)
+      if (CMP == 1)
         for (int k = k0; k < k1; ++k) {
           C.wv[(int64_t)k * 3 * C.NN + x2] = 0.0;
           C.wv[(int64_t)k * 3 * C.NN + x1] = 0.0;
         }
+      else if (CMP == 2 && me(C, e, d, a1, b1) >= ADJZONE)  // a kept slot that the pair leaves at 0
+        for (int k = k0; k < k1; ++k) C.wv[(int64_t)k * 3 * C.NN + x1] = 0.0;
       continue;
     }
-    const bool keep1 = !CMP || corner || me(C, e, d, a1, b1) >= ADJZONE;
+    const bool keep1 = CMP == 0 || corner || me(C, e, d, a1, b1) >= ADJZONE;
     OuterInterp O;
     outer_interp(O, Pa, C, d, ip, jp, a2, b2, e);
     const int cv = we_code(C, e, d, a2, b2);
@@ -370,7 +376,7 @@ __device__ __forceinline__ void inner_eval(const InnerInterp& I, const double* _
 
 // Compute_velo_wavelets' inner edges (src/wavelet.f90:672-710), parents
 // [0, np)^2; CMP as for k_scalar_wc_l.
-template <bool CMP>
+template <int CMP>
 __global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa, WLev C, int nz, int lpt) {
   int d, ip, jp;
   int k0, k1;
@@ -387,7 +393,7 @@ __global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa,
     any = any || on[q];
   }
   if (!any) {
-    if (CMP)
+    if (CMP == 1)
       for (int k = k0; k < k1; ++k)
 #pragma unroll
         for (int q = 0; q < 6; ++q) C.wv[(int64_t)k * 3 * C.NN + ge[q] * C.NN + nid(C, d, gi[q], gj[q])] = 0.0;
@@ -405,7 +411,7 @@ __global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa,
     for (int q = 0; q < 6; ++q)
       if (on[q])
         wc[I.xt[q]] = we(v, I.ct[q]) - u[q];
-      else if (CMP)
+      else if (CMP == 1)
         wc[I.xt[q]] = 0.0;
   }
 }

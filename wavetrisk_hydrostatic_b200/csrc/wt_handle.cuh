@@ -133,6 +133,9 @@ void wt_level_compress(wt_handle* h);
 // zero every wavelet array if a host upload wrote wavelets since the last
 // zeroing (stream-ordered; WT_after_step then writes only the slots it computes)
 void wt_level_clean_wavelets(wt_handle* h);
+// whether every wavelet slot that WT_after_step sets to 0 under the current
+// masks holds 0 already (then the forward wavelets write only the kept slots)
+bool wt_level_zero_ok(wt_handle* h);
 // The needed-node maps of the levels above level_start (need_map.cuh): build
 // them from the current masks (stream-ordered; the mask sequence does so at its
 // end); the map a level's RK-stage kernels may skip by, or null; the count of

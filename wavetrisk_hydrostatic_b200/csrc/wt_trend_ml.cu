@@ -381,6 +381,9 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
   }
   if (int rc = wt_level_set_thresholds(h, threshold)) return rc;
   wt_level_clean_wavelets(h);  // outside the graph, which assumes clean wavelet arrays
+  // and wavelets compressed under the current masks: the graph's first stage
+  // writes only the kept slots (the wavelets on entry are not read otherwise)
+  if (!wt_level_zero_ok(h)) wt_level_compress(h);
   if (int rc = wt_level_need_refresh(h)) return rc;  // likewise a current needed-node map
   if (!M->step_graph || M->g_dt != dt || M->g_fill != level_fill || M->g_max != max_level ||
       M->g_epoch != wt_level_skip_epoch(h)) {

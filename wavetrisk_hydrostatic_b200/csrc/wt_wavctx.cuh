@@ -35,6 +35,10 @@ struct WavCtx {
   // ghost rows, the coarsest level) hold 0 unless a host upload wrote them;
   // WT_after_step re-zeroes the arrays only then.
   bool wav_dirty = false;
+  // Every wavelet slot that WT_after_step sets to 0 under the current masks
+  // holds 0 already (compress_wavelets ran under them, or a WT_after_step did):
+  // the forward kernels then write the kept slots only (CMP 2).
+  bool zero_ok = false;
   // side streams of the transforms, forked from and joined back into the
   // handle's stream: the scalar chain of the inverse (0, top priority: it is as
   // long as the velocity chain on the handle's stream), and the forward scalar

@@ -112,7 +112,7 @@ void zero_wavelets(wt_handle* h) {
 }
 
 // Scalar wavelets of level l+1 (Compute_scalar_wavelets over parents [0, n_l)).
-template <bool CMP>
+template <int CMP>
 void launch_scalar_wc(wt_handle* h, int l, cudaStream_t s) {
   const int np = h->at(l).n, nz = h->nz;
   k_scalar_wc_l<CMP><<<nbl((int64_t)10 * np * np, nz), TPBL, 0, s>>>(view(h, l + 1), np, nz, lpt_for(nz));
@@ -123,7 +123,7 @@ inline dim3 plan_block(int nz) { return dim3(32, std::min(nz, 8)); }
 inline unsigned plan_grid(int64_t rows) { return (unsigned)((rows + 31) / 32); }
 // Velocity wavelets of level l+1 (pentagon corrections included): outer edges
 // on s, inner edges on si (they read only the scaling fields).
-template <bool CMP>
+template <int CMP>
 void launch_velo_wc(wt_handle* h, int l, cudaStream_t s, cudaStream_t si) {
   const int np = h->at(l).n, nz = h->nz;
   const unsigned g = nbl((int64_t)10 * np * np, nz);
@@ -165,6 +165,7 @@ void compress(wt_handle* h) {
     const int n = h->at(l).n;
     k_compress<<<nb((int64_t)nz * 10 * (n + 1) * (n + 1)), TPB, 0, h->stream>>>(view(h, l), nz);
   }
+  ctx(h)->zero_ok = true;
 }
 
 }  // namespace
@@ -200,8 +201,13 @@ int wt_level_wav_forward_pair(wt_handle* h, int l) {
   cudaEvent_t f = W->fork[l - h->level_start];
   CKW(cudaEventRecord(f, h->stream));
   for (int k = 1; k < 4; ++k) CKW(cudaStreamWaitEvent(W->side[k], f, 0));
-  launch_scalar_wc<true>(h, l, W->side[3]);
-  launch_velo_wc<true>(h, l, W->side[2], W->side[1]);
+  if (W->zero_ok) {
+    launch_scalar_wc<2>(h, l, W->side[3]);
+    launch_velo_wc<2>(h, l, W->side[2], W->side[1]);
+  } else {
+    launch_scalar_wc<1>(h, l, W->side[3]);
+    launch_velo_wc<1>(h, l, W->side[2], W->side[1]);
+  }
   CKW(cudaGetLastError());
   return WT_OK;
 }
@@ -214,6 +220,7 @@ int wt_level_wav_finish(wt_handle* h, bool partial, bool rebuild) {
     CKW(cudaEventRecord(W->ev[1 + k], W->side[k]));
     CKW(cudaStreamWaitEvent(h->stream, W->ev[1 + k], 0));
   }
+  W->zero_ok = true;  // every level pair's forward wavelets are launched
   if (rebuild) inverse(h, partial);
   CKW(cudaGetLastError());
   return WT_OK;
@@ -376,6 +383,7 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
   if (level == h->level_end && field <= WT_FIELD_VELO) h->state_halo_done = false;
   if (field >= WT_WAVE_MASS && field <= WT_WAVE_VELO) ctx(h)->wav_dirty = true;
   if (field == WT_MASK_NODE || field == WT_MASK_EDGE) ctx(h)->need_ok = false;
+  if (field >= WT_WAVE_MASS && field <= WT_MASK_EDGE) ctx(h)->zero_ok = false;
   return WT_OK;
 }
 
@@ -421,12 +429,13 @@ int wt_forward_wt(wt_handle* h) {
   const int nz = h->nz;
   zero_wavelets(h);
   ctx(h)->wav_dirty = false;
+  ctx(h)->zero_ok = false;  // the forward transform keeps what compress_wavelets would zero
   for (int l = h->level_end - 1; l >= h->level_start; --l) {
     const int np = h->at(l).n;
-    launch_scalar_wc<false>(h, l, h->stream);
+    launch_scalar_wc<0>(h, l, h->stream);
     k_restrict<<<nb((int64_t)nz * 10 * (np + 1) * (np + 1)), TPB, 0, h->stream>>>(view(h, l), view(h, l + 1), nz);
   }
-  for (int l = h->level_end - 1; l >= h->level_start; --l) launch_velo_wc<false>(h, l, h->stream, h->stream);
+  for (int l = h->level_end - 1; l >= h->level_start; --l) launch_velo_wc<0>(h, l, h->stream, h->stream);
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
@@ -481,6 +490,8 @@ int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill) {
     const int st = (l == h->level_end) ? 0 : -1, en = (l == h->level_end) ? 1 : 2;
     mask_tol(h, l, st, en, level_fill);
   }
+  W->zero_ok = false;
+  W->need_ok = false;
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
@@ -548,6 +559,7 @@ int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patc
   // mask_trsk
   for (int l = ls; l <= le; ++l) k_mask_trsk<<<nodes_blocks(h->at(l).n + 4), TPB, 0, s>>>(view(h, l));
   CKW(cudaGetLastError());
+  ctx(h)->zero_ok = false;  // new masks: compress_wavelets has not run under them
   return wt_level_need_build(h);
 }
 
@@ -637,7 +649,9 @@ void wt_level_clean_wavelets(wt_handle* h) {
   if (!ctx(h)->wav_dirty) return;
   zero_wavelets(h);
   ctx(h)->wav_dirty = false;
+  ctx(h)->zero_ok = true;  // every slot is 0
 }
+bool wt_level_zero_ok(wt_handle* h) { return ctx(h)->zero_ok; }
 void wt_level_inverse(wt_handle* h) { inverse(h); }
 int wt_level_set_thresholds(wt_handle* h, const double* threshold) {
   CKW(cudaMemcpyAsync(ctx(h)->thr, threshold, 3 * h->nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));

@@ -401,25 +401,32 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
         ids = dev.FIELDS
         L = Nt.lib()
 
-        def put(g, b):
-            for k in ("mass", "temp", "velo"):
-                Nt.check("wt_upload_field", L.wt_upload_field(dev.h, g.level, ids[k], b[k].ctypes.data))
+        # one batch each way per step (wt_upload_fields / wt_download_fields), finest level first
+        up = [(g.level, k, b[k]) for g, b in reversed(list(zip(levels, bufs))) for k in ("mass", "temp", "velo")]
+        dn = [(g.level, k, b[k]) for g, b in reversed(list(zip(levels, bufs)))
+              for k in ("mass", "temp", "velo", "mask_n", "mask_e")]
 
-        def get(g, b):
-            for k in ("mass", "temp", "velo", "mask_n", "mask_e"):
-                Nt.check("wt_download_field", L.wt_download_field(dev.h, g.level, ids[k], b[k].ctypes.data))
+        def batch(items):
+            n = len(items)
+            return (n, (Nt.C.c_int * n)(*[l for l, _, _ in items]), (Nt.C.c_int * n)(*[ids[k] for _, k, _ in items]),
+                    (Nt.C.c_void_p * n)(*[a.ctypes.data for _, _, a in items]))
 
-        for g, b in zip(levels, bufs):
-            get(g, b)
+        bu, bd = batch(up), batch(dn)
+
+        def put():
+            Nt.check("wt_upload_fields", L.wt_upload_fields(dev.h, *bu))
+
+        def get():
+            Nt.check("wt_download_fields", L.wt_download_fields(dev.h, *bd))
+
+        get()
         nsteps_e2e = max(1, steps // 2)
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
         for _ in range(nsteps_e2e):
-            for g, b in zip(levels, bufs):
-                put(g, b)
+            put()
             model.step(DT_AD)
-            for g, b in zip(levels, bufs):
-                get(g, b)
+            get()
         t1 = time.perf_counter()
         out["e2e_s"] = t1 - t0
         out["e2e_steps"] = nsteps_e2e
@@ -527,7 +534,7 @@ def bench_ours(args):
             "config": workload_config(args, world),
             "e2e": {"value": e2e_value, "unit": "simulated days per wall-clock hour",
                     "h2d_bytes_per_step": r["h2d_bytes_per_step"], "d2h_bytes_per_step": r["d2h_bytes_per_step"],
-                    "path": "C-ABI wt_upload_field / wt_adaptive_step / wt_download_field, pinned host "
+                    "path": "C-ABI wt_upload_fields / wt_adaptive_step / wt_download_fields, pinned host "
                             "buffers: every level's state in, every level's state and masks out, every step"},
             "gpu_launches": adaptive_launches(L) * args.steps,
             "roofline": {"bound": "hbm", "kernel": "k_trend_tma<MODE_ML> (level_end)", "achieved": ach, "peak": hbm,

@@ -222,6 +222,13 @@ int wt_wavelet_setup(wt_handle* h);
  * Downloads of scaling and wavelet fields first give ghosts their copies. */
 int wt_upload_field(wt_handle* h, int level, int field, const void* src);
 int wt_download_field(wt_handle* h, int level, int field, void* dst);
+/* The same for n (level, field) pairs at once (the drop-in boundary's
+ * wt_upload_fields / wt_download_fields(h, which, host_ptrs)): the copies are
+ * queued back to back on the handle's stream with one synchronisation at the
+ * end, and each level's ghost copy runs once per download batch.  Arguments are
+ * checked before anything is queued. */
+int wt_upload_fields(wt_handle* h, int n, const int* levels, const int* fields, const void* const* src);
+int wt_download_fields(wt_handle* h, int n, const int* levels, const int* fields, void* const* dst);
 /* forward_wavelet_transform(scaling, wavelet, level_start+1) (src/wavelet.f90:20-98):
  * scalar and velocity wavelets of levels > level_start, coarse scaling by
  * lifting (scalars) and averaging (velocity). */

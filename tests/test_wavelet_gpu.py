@@ -195,3 +195,27 @@ def test_mask_build_matches_oracle_exactly(level_fill, scale):
     assert np.array_equal(rq_d, rq_o)
     assert rq_o.sum() > 0
     dev.close()
+
+
+def test_batched_transfers_match_single_field_transfers():
+    """wt_upload_fields / wt_download_fields move the same bytes as the
+    per-field calls, ghost copies included."""
+    levels, orc, dev = _setup(3, 5, 2)
+    _random_fine(levels, orc, dev, 2, seed=71)
+    dev.forward()
+    names = ("mass", "temp", "velo", "wc_mass", "wc_temp", "wc_velo", "mask_n", "mask_e")
+    single = {(g.level, f): dev.download(g.level, f) for g in levels for f in names}
+    outs = {k: np.empty_like(v) for k, v in single.items()}
+    dev.download_many([(l, f, outs[(l, f)]) for (l, f) in outs])
+    for k in single:
+        assert np.array_equal(single[k], outs[k]), k
+    rng = np.random.default_rng(5)
+    new = {(g.level, f): rng.standard_normal(single[(g.level, f)].shape) for g in levels for f in ("mass", "velo")}
+    dev.upload_many([(l, f, a) for (l, f), a in new.items()])
+    for (l, f), a in new.items():
+        own = np.nonzero(levels[l - levels[0].level].owned)[0]
+        g = levels[l - levels[0].level]
+        k = np.concatenate([own, own + g.NN, own + 2 * g.NN]) if f == "velo" else own
+        assert np.array_equal(dev.download(l, f)[:, k], a[:, k]), (l, f)
+    assert dev.status() == 0
+    dev.close()

@@ -123,6 +123,8 @@ _DEVICE_SIGS = {
     "wt_wavelet_setup": [_vp],
     "wt_upload_field": [_vp, C.c_int, C.c_int, _vp],
     "wt_download_field": [_vp, C.c_int, C.c_int, _vp],
+    "wt_upload_fields": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(_vp)],
+    "wt_download_fields": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(_vp)],
     "wt_forward_wt": [_vp],
     "wt_inverse_wt": [_vp],
     "wt_mask_tol_vars": [_vp, _dp, C.c_int],

@@ -354,15 +354,20 @@ int wt_wavelet_setup(wt_handle* h) {
   return WT_OK;
 }
 
-int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
-  if (int rc = ready(h)) return rc;
-  if (!src || level < h->level_start || level > h->level_end || field < 0 || field > WT_FIELD_MEAN_TEMP)
-    return WT_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+bool field_ok(wt_handle* h, int level, int field) {
+  return level >= h->level_start && level <= h->level_end && field >= 0 && field <= WT_FIELD_MEAN_TEMP;
+}
+
+// Queue the host-to-device copy of one field of one level (no synchronisation).
+int enqueue_upload(wt_handle* h, int level, int field, const void* src) {
   if (field >= WT_FIELD_MEAN_MASS) {
     double* p;
     if (int rc = wt_level_mean(h, level, field, &p)) return rc;
     CKW(cudaMemcpyAsync(p, src, (size_t)h->nz * h->at(level).NN * 8, cudaMemcpyHostToDevice, h->stream));
-    CKW(cudaStreamSynchronize(h->stream));
     return WT_OK;
   }
   if (field >= WT_WORK_SCALAR) {
@@ -370,7 +375,6 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
     size_t bytes;
     if (int rc = work_field(h, level, field, &p, &bytes)) return rc;
     CKW(cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, h->stream));
-    CKW(cudaStreamSynchronize(h->stream));
     return WT_OK;
   }
   const DevLevel& D = h->at(level);
@@ -379,7 +383,6 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
   void* dst[8] = {V.sm, V.st, V.sv, V.wm, V.wt, V.wv, V.mask_n, V.mask_e};
   const size_t bytes[8] = {nn * 8, nn * 8, 3 * nn * 8, nn * 8, nn * 8, 3 * nn * 8, (size_t)D.NN * 4, (size_t)3 * D.NN * 4};
   CKW(cudaMemcpyAsync(dst[field], src, bytes[field], cudaMemcpyHostToDevice, h->stream));
-  CKW(cudaStreamSynchronize(h->stream));
   if (level == h->level_end && field <= WT_FIELD_VELO) h->state_halo_done = false;
   if (field >= WT_WAVE_MASS && field <= WT_WAVE_VELO) ctx(h)->wav_dirty = true;
   if (field == WT_MASK_NODE || field == WT_MASK_EDGE) ctx(h)->need_ok = false;
@@ -387,15 +390,23 @@ int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
   return WT_OK;
 }
 
-int wt_download_field(wt_handle* h, int level, int field, void* dst) {
-  if (int rc = ready(h)) return rc;
-  if (!dst || level < h->level_start || level > h->level_end || field < 0 || field > WT_FIELD_MEAN_TEMP)
-    return WT_ERR_ARG;
+// Queue the ghost copy of level's scaling (wav false) or wavelet fields.
+int enqueue_halo(wt_handle* h, int level, bool wav) {
+  const DevLevel& D = h->at(level);
+  WavLevel& V = ctx(h)->L[level - h->level_start];
+  const int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * h->nz;
+  k_halo_level<<<nb(nt), TPB, 0, h->stream>>>(h->nz, (int)D.NN, D.hn, D.n_hn, D.he, D.n_he, wav ? V.wm : V.sm,
+                                               wav ? V.wt : V.st, wav ? V.wv : V.sv);
+  CKW(cudaGetLastError());
+  return WT_OK;
+}
+
+// Queue the device-to-host copy of one field of one level (ghosts as they are).
+int enqueue_download(wt_handle* h, int level, int field, void* dst) {
   if (field >= WT_FIELD_MEAN_MASS) {
     double* p;
     if (int rc = wt_level_mean(h, level, field, &p)) return rc;
     CKW(cudaMemcpyAsync(dst, p, (size_t)h->nz * h->at(level).NN * 8, cudaMemcpyDeviceToHost, h->stream));
-    CKW(cudaStreamSynchronize(h->stream));
     return WT_OK;
   }
   if (field >= WT_WORK_SCALAR) {
@@ -403,22 +414,66 @@ int wt_download_field(wt_handle* h, int level, int field, void* dst) {
     size_t bytes;
     if (int rc = work_field(h, level, field, &p, &bytes)) return rc;
     CKW(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyDeviceToHost, h->stream));
-    CKW(cudaStreamSynchronize(h->stream));
     return WT_OK;
   }
   const DevLevel& D = h->at(level);
   WavLevel& V = ctx(h)->L[level - h->level_start];
   const size_t nn = (size_t)h->nz * D.NN;
-  if (field <= WT_WAVE_VELO) {
-    const bool wav = field >= WT_WAVE_MASS;
-    const int64_t nt = (int64_t)(2 * D.n_hn + D.n_he) * h->nz;
-    k_halo_level<<<nb(nt), TPB, 0, h->stream>>>(h->nz, (int)D.NN, D.hn, D.n_hn, D.he, D.n_he, wav ? V.wm : V.sm,
-                                                 wav ? V.wt : V.st, wav ? V.wv : V.sv);
-    CKW(cudaGetLastError());
-  }
   const void* src[8] = {V.sm, V.st, V.sv, V.wm, V.wt, V.wv, V.mask_n, V.mask_e};
   const size_t bytes[8] = {nn * 8, nn * 8, 3 * nn * 8, nn * 8, nn * 8, 3 * nn * 8, (size_t)D.NN * 4, (size_t)3 * D.NN * 4};
   CKW(cudaMemcpyAsync(dst, src[field], bytes[field], cudaMemcpyDeviceToHost, h->stream));
+  return WT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wt_upload_field(wt_handle* h, int level, int field, const void* src) {
+  if (int rc = ready(h)) return rc;
+  if (!src || !field_ok(h, level, field)) return WT_ERR_ARG;
+  if (int rc = enqueue_upload(h, level, field, src)) return rc;
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_download_field(wt_handle* h, int level, int field, void* dst) {
+  if (int rc = ready(h)) return rc;
+  if (!dst || !field_ok(h, level, field)) return WT_ERR_ARG;
+  if (field <= WT_WAVE_VELO)
+    if (int rc = enqueue_halo(h, level, field >= WT_WAVE_MASS)) return rc;
+  if (int rc = enqueue_download(h, level, field, dst)) return rc;
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_upload_fields(wt_handle* h, int n, const int* levels, const int* fields, const void* const* src) {
+  if (int rc = ready(h)) return rc;
+  if (n < 0 || (n > 0 && (!levels || !fields || !src))) return WT_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (!src[i] || !field_ok(h, levels[i], fields[i])) return WT_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (int rc = enqueue_upload(h, levels[i], fields[i], src[i])) return rc;
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_download_fields(wt_handle* h, int n, const int* levels, const int* fields, void* const* dst) {
+  if (int rc = ready(h)) return rc;
+  if (n < 0 || (n > 0 && (!levels || !fields || !dst))) return WT_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (!dst[i] || !field_ok(h, levels[i], fields[i])) return WT_ERR_ARG;
+  std::vector<char> done(2 * (h->level_end - h->level_start + 1), 0);  // ghost copy per (level, kind)
+  for (int i = 0; i < n; ++i)
+    if (fields[i] <= WT_WAVE_VELO) {
+      const int k = 2 * (levels[i] - h->level_start) + (fields[i] >= WT_WAVE_MASS ? 1 : 0);
+      if (!done[k]) {
+        done[k] = 1;
+        if (int rc = enqueue_halo(h, levels[i], fields[i] >= WT_WAVE_MASS)) return rc;
+      }
+    }
+  for (int i = 0; i < n; ++i)
+    if (int rc = enqueue_download(h, levels[i], fields[i], dst[i])) return rc;
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
 }

@@ -197,6 +197,33 @@ class WaveletHierarchy(DeviceGrid):
         N.check("wt_download_field", N.lib().wt_download_field(self.h, level, self.FIELDS[name], buf.ctypes.data))
         return buf
 
+    def _batch(self, items):
+        n = len(items)
+        lv = (N.C.c_int * n)(*[int(l) for l, _, _ in items])
+        fd = (N.C.c_int * n)(*[self.FIELDS[f] for _, f, _ in items])
+        return n, lv, fd
+
+    def upload_many(self, items) -> None:
+        """items: (level, name, array) triples, copied in one batch (wt_upload_fields)."""
+        bufs = []
+        for l, f, a in items:
+            shape, dt = self._shape(l, f)
+            bufs.append(np.ascontiguousarray(np.broadcast_to(a, shape), dtype=dt))
+        n, lv, fd = self._batch(items)
+        ptr = (N.C.c_void_p * n)(*[b.ctypes.data for b in bufs])
+        N.check("wt_upload_fields", N.lib().wt_upload_fields(self.h, n, lv, fd, ptr))
+
+    def download_many(self, items) -> None:
+        """items: (level, name, out) triples; out arrays of the field's shape and
+        dtype, C-contiguous, filled in one batch (wt_download_fields)."""
+        for l, f, out in items:
+            shape, dt = self._shape(l, f)
+            if out.shape != shape or out.dtype != dt or not out.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"download_many: {f} of level {l} needs a C-contiguous {dt} array {shape}")
+        n, lv, fd = self._batch(items)
+        ptr = (N.C.c_void_p * n)(*[o.ctypes.data for _, _, o in items])
+        N.check("wt_download_fields", N.lib().wt_download_fields(self.h, n, lv, fd, ptr))
+
     def forward(self) -> None:
         N.check("wt_forward_wt", N.lib().wt_forward_wt(self.h))
 

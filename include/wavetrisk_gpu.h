@@ -308,6 +308,17 @@ int wt_trend_multi(wt_handle* h);
  * state; the masks are held fixed.  The solution is the hierarchy's scaling
  * fields (level_end's is the stepper's state). */
 int wt_rk4_multi(wt_handle* h, double dt, int nsteps);
+/* The explicit part of one mode-split step, RK4_split (src/time_integr.f90:
+ * 360-382) without free_surface_update: RK_split (:444-463) four times, each
+ * barotropic_correction of the stage's source state (src/barotropic_2d.f90:
+ * 52-116, with total_height :368-412), trend_ml, scalar_star and u_star
+ * (:9-50, external pressure gradient grad_eta of each level's free surface
+ * weighted by theta1) and WT_after_step.  Uses the free surface of every level
+ * (wt_barotropic_upload_level) and the masks as they are. */
+int wt_rk4_split_explicit(wt_handle* h, double dt, double theta1);
+/* barotropic_correction (src/barotropic_2d.f90:52-116) of the hierarchy's
+ * scaling fields from each level's free surface. */
+int wt_barotropic_correction_multi(wt_handle* h);
 /* nsteps adaptive time steps of the hierarchy (the reference's time_step,
  * src/main.f90:405-444, explicit RK4, fixed thresholds): wt_rk4_multi(dt, 1),
  * adapt's mask sequence with threshold[3][nz] (wt_mask_build without the

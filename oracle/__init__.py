@@ -176,3 +176,48 @@ def rk4_multi(levels, nz, ph, states, masks, dt, nsteps=1, H=None):
             else:
                 q = dest
     return [(x["mass"], x["temp"], x["velo"]) for x in q]
+
+
+def rk4_split_explicit(levels, nz, ph, states, masks, etas, dt, theta1, H=None):
+    """The four RK_split calls of RK4_split (src/time_integr.f90:360-382,
+    444-463) over the hierarchy, without free_surface_update: per stage
+    barotropic_correction of the stage's source state (in place, so the first
+    stage corrects the solution itself), trend_ml, scalar_star and u_star
+    (src/barotropic_2d.f90:9-50: the base is the solution, the velocity adds
+    theta1 times grad_eta of each level's free surface) and WT_after_step.
+    Returns per level the new (mass, temp, velo)."""
+    from .barotropic import barotropic_correction_multi, u_update_multi
+    from .wavelet import Hierarchy
+    if H is None:
+        H = Hierarchy(levels, nz)
+    for g, (mn, me) in zip(levels, masks):
+        H.set(g.level, "mask_n", mn)
+        H.set(g.level, "mask_e", me)
+    keys = ("mass", "temp", "velo")
+    q = [{k: np.array(st[k], dtype=np.float64) for k in keys} for st in states]
+    hs = (dt / 4.0, dt / 3.0, dt / 2.0, dt)
+    q1 = None
+    for stage in range(4):
+        src = q if stage == 0 else q1
+        st = [dict(states[i], **src[i]) for i in range(len(levels))]
+        for i, (m, t) in enumerate(barotropic_correction_multi(levels, nz, ph, st, etas)):
+            src[i]["mass"], src[i]["temp"] = m, t
+        st = [dict(states[i], **src[i]) for i in range(len(levels))]
+        tr = trend_multi(levels, nz, ph, st, masks)
+        grad = [o["grad"] for o in u_update_multi(levels, nz, st, masks, etas, ph.grav, 0.0, 0.0)]
+        dest = []
+        for i in range(len(levels)):
+            d = {"mass": q[i]["mass"] + hs[stage] * tr[i][0], "temp": q[i]["temp"] + hs[stage] * tr[i][1],
+                 "velo": q[i]["velo"] + hs[stage] * (tr[i][2] + theta1 * grad[i][None, :])}
+            dest.append(d)
+        for i, g in enumerate(levels):
+            for k, f in zip(keys, ("s_m", "s_t", "s_v")):
+                H.set(g.level, f, dest[i][k])
+        H.wt_after_step()
+        dest = [{k: H.field(g.level, f).copy() for k, f in zip(keys, ("s_m", "s_t", "s_v"))} for g in levels]
+        if stage < 3:
+            q1 = dest
+        else:
+            q = dest
+    return [(x["mass"], x["temp"], x["velo"]) for x in q]
+

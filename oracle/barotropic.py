@@ -126,3 +126,33 @@ def u_update_multi(levels, nz, states, masks, etas, grav, dt, theta1):
     L.orc_u_update_multi.restype = C.c_int
     assert L.orc_u_update_multi(C.addressof(arr), len(levels), nz, grav, dt, theta1) == 0
     return outs
+
+
+def barotropic_correction_multi(levels, nz, ph, states, etas):
+    """barotropic_correction (src/barotropic_2d.f90:52-116) on every level:
+    total_height/cal_height (:368-412) summed over the layers from 0, then the
+    layer-dilation correction cal_barotropic_correction (:85-116) of each
+    layer's mass and mass-weighted buoyancy from the free surface eta, porosity
+    1.  Element by element with the reference's operand order; returns per
+    level (mass, temp).  Slots whose column is empty come out non-finite and are
+    not compared."""
+    out = []
+    rho0 = ph.ref_density
+    for q, g in enumerate(levels):
+        st = states[q]
+        mass = np.array(st["mass"], dtype=np.float64).copy()
+        temp = np.array(st["temp"], dtype=np.float64).copy()
+        mm, mt, topo = st["mean_m"], st["mean_t"], st["topo"]
+        with np.errstate(all="ignore"):
+            height = np.zeros(g.NN)
+            for k in range(nz):
+                height = height + (mm[k] + mass[k]) / (rho0 * 1.0)
+            e = np.asarray(etas[q], dtype=np.float64) / 1.0
+            for k in range(nz):
+                rho_dz = mm[k] + mass[k]
+                theta = (mt[k] + temp[k]) / rho_dz
+                mass[k] = (e - topo) / height * rho_dz - mm[k]
+                rho_dz = mm[k] + mass[k]
+                temp[k] = rho_dz * theta - mt[k]
+        out.append((mass, temp))
+    return out

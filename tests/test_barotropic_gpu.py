@@ -145,3 +145,70 @@ def test_barotropic_pieces_on_the_hierarchy_match_oracle(masks_kind):
         assert rel(v[:, e], ov[:, e]) <= TOL, (g.level, "velo")
     assert dev.status() == 0
     dev.close()
+
+
+def _split_case(masks_kind, lmin=3, lmax=5, nz=2):
+    from oracle.wavelet import Hierarchy
+    from wavetrisk_hydrostatic_b200.model import WaveletHierarchy
+
+    ph = OceanParams()
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    states = [jet_state(g, nz, seed=11 + q, ph=ph) for q, g in enumerate(levels)]
+    rng = np.random.default_rng(9)
+    etas = []
+    for g in levels:
+        e = rng.standard_normal(g.NN) * 0.1
+        halo_nodes(g, e)
+        etas.append(e)
+    if masks_kind == "built":
+        H = Hierarchy(levels, nz)
+        for name, key in (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v")):
+            H.set(lmax, key, states[-1][name])
+        H.forward()
+        H.mask_build(np.array([[5.0] * nz, [1e16] * nz, [0.05] * nz]), 0, lmax)
+        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in levels]
+    else:
+        masks = [(np.full(g.NN, 16, np.int32), np.full(3 * g.NN, 16, np.int32)) for g in levels]
+    dev = WaveletHierarchy(levels, [st["topo"] for st in states], nz, ph)
+    for g, st, (mn, me), e in zip(levels, states, masks, etas):
+        for name in ("mass", "temp", "velo", "mean_m", "mean_t"):
+            dev.upload(g.level, name, st[name])
+        dev.upload(g.level, "mask_n", mn)
+        dev.upload(g.level, "mask_e", me)
+        dev.barotropic_upload(g.level, e, None)
+    return ph, levels, states, masks, etas, dev
+
+
+def test_barotropic_correction_on_the_hierarchy_matches_oracle():
+    """barotropic_correction with total_height on every level of J3..J5."""
+    ph, levels, states, masks, etas, dev = _split_case("tolrnz")
+    ref = ob.barotropic_correction_multi(levels, 2, ph, states, etas)
+    dev.barotropic_correction()
+    for (m, t), g in zip(ref, levels):
+        own = np.nonzero(g.owned)[0]
+        assert rel(dev.download(g.level, "mass")[:, own], m[:, own]) <= TOL, (g.level, "mass")
+        assert rel(dev.download(g.level, "temp")[:, own], t[:, own]) <= TOL, (g.level, "temp")
+    assert dev.status() == 0
+    dev.close()
+
+
+@pytest.mark.parametrize("masks_kind", ["tolrnz", "built"])
+def test_rk4_split_explicit_matches_oracle(masks_kind):
+    """RK4_split's four RK_split stages (barotropic_correction, trend_ml,
+    scalar_star, u_star with grad_eta, WT_after_step) on J3..J5: every level's
+    state on owned nodes and edges."""
+    import oracle
+
+    ph, levels, states, masks, etas, dev = _split_case(masks_kind)
+    dt, theta1 = 150.0, 0.5
+    ref = oracle.rk4_split_explicit(levels, 2, ph, states, masks, etas, dt, theta1)
+    dev.rk4_split_explicit(dt, theta1)
+    for (m, t, v), g in zip(ref, levels):
+        own = np.nonzero(g.owned)[0]
+        e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+        assert rel(dev.download(g.level, "mass")[:, own], m[:, own]) <= TOL, (g.level, "mass")
+        assert rel(dev.download(g.level, "temp")[:, own], t[:, own]) <= TOL, (g.level, "temp")
+        assert rel(dev.download(g.level, "velo")[:, e], v[:, e]) <= TOL, (g.level, "velo")
+    assert dev.status() == 0
+    dev.close()

@@ -123,6 +123,8 @@ _DEVICE_SIGS = {
     "wt_wavelet_setup": [_vp],
     "wt_upload_field": [_vp, C.c_int, C.c_int, _vp],
     "wt_download_field": [_vp, C.c_int, C.c_int, _vp],
+    "wt_rk4_split_explicit": [_vp, C.c_double, C.c_double],
+    "wt_barotropic_correction_multi": [_vp],
     "wt_upload_fields": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(_vp)],
     "wt_download_fields": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(_vp)],
     "wt_forward_wt": [_vp],

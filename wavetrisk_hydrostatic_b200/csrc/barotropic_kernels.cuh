@@ -165,6 +165,44 @@ __global__ void k_grad_eta_update(LevelDev L, int nz, double grav, const double*
   }
 }
 
+// barotropic_correction (src/barotropic_2d.f90:52-116) on one level: the total
+// height of the column (total_height/cal_height, :368-412: the layers' rho dz /
+// (rho0 phi) summed bottom-up from 0) and the layer-dilation correction of
+// every layer's mass and mass-weighted buoyancy from the free surface eta:
+//   theta = (mean_t + temp) / (mean_m + mass)
+//   mass  = (eta/phi - topo) / height * (mean_m + mass) - mean_m
+//   temp  = (mean_m + mass) * theta - mean_t
+// with porosity phi = 1.  One thread per node of [0, n]^2 that is its own
+// source: owned nodes, and the slots of row n near the pentagon corners that no
+// ghost copy fills (stencils read them as stored).  Ghost copies of row n are
+// left alone: every kernel reads them through the remaps.
+__global__ void k_barotropic_correction(LevelDev L, int nz, double rho0, const double* __restrict__ eta,
+                                        const double* __restrict__ mean_m, const double* __restrict__ mean_t,
+                                        double* __restrict__ mass, double* __restrict__ temp) {
+  const int m = L.n + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 10 * m * m) return;
+  const int d = t / (m * m), r = t - d * m * m, j = r / m, i = r - j * m;
+  const int64_t NN = L.NN;
+  const int id = (d * L.P + j + 2) * L.P + i + 2;
+  if (__ldg(L.nsrc + id) != id) return;
+  double height = 0.0;
+  for (int k = 0; k < nz; ++k) {
+    const double rho_dz = mean_m[k * NN + id] + mass[k * NN + id];
+    height = height + rho_dz / (rho0 * 1.0);
+  }
+  const double e = eta[id] / 1.0;
+  for (int k = 0; k < nz; ++k) {
+    const int64_t x = k * NN + id;
+    double rho_dz = mean_m[x] + mass[x];
+    const double rho_dz_theta = mean_t[x] + temp[x];
+    const double theta = rho_dz_theta / rho_dz;
+    mass[x] = (e - L.topo[id]) / height * rho_dz - mean_m[x];
+    rho_dz = mean_m[x] + mass[x];
+    temp[x] = rho_dz * theta - mean_t[x];
+  }
+}
+
 }  // namespace wtb
 
 namespace wtb {

@@ -32,6 +32,11 @@ struct TrendML {
   // needed-node map (need_map.cuh) of the finest level, or null: nodes with
   // need[nsrc[id]] == 0 write nothing
   const unsigned char* need;
+  // u_star (src/barotropic_2d.f90:29-50) when grad is set: the velocity sub-step
+  // is base + h * (trend + th1 * grad), grad the level's external pressure
+  // gradient [3][NN] (grad_eta)
+  const double* grad;
+  double th1;
 };
 
 constexpr int ML_TRSK = 2, ML_ADJZONE = 8;
@@ -116,7 +121,9 @@ __global__ void __launch_bounds__(NODE_TILE, 4) k_trend_ml(LevelDev L, int nz, T
     io.dst_m[ko + id] = io.base_m[ko + id] + h * dms;
     io.dst_t[ko + id] = io.base_t[ko + id] + h * dts;
 #pragma unroll
-    for (int e = 0; e < 3; ++e) io.dst_v[vo + e * NN] = io.base_v[vo + e * NN] + h * dv3[e];
+    for (int e = 0; e < 3; ++e)
+      io.dst_v[vo + e * NN] = io.grad ? io.base_v[vo + e * NN] + h * (dv3[e] + io.th1 * io.grad[e * NN + id])
+                                      : io.base_v[vo + e * NN] + h * dv3[e];
   }
 }
 

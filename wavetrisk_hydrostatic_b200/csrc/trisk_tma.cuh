@@ -274,7 +274,14 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
       io.src[vo + 2 * NN] = s2;
     }
   }
-  if (MODE == MODE_RK || MODE == MODE_ML) {
+  if (MODE == MODE_ML && io.grad) {  // u_star
+    const double h = io.h, t1 = io.th1;
+    io.dst_m[ko + id] = bm + h * dms;
+    io.dst_t[ko + id] = bt + h * dts;
+    io.dst_v[vo] = bv0 + h * (dv0 + t1 * io.grad[id]);
+    io.dst_v[vo + NN] = bv1 + h * (dv1 + t1 * io.grad[NN + id]);
+    io.dst_v[vo + 2 * NN] = bv2 + h * (dv2 + t1 * io.grad[2 * NN + id]);
+  } else if (MODE == MODE_RK || MODE == MODE_ML) {
     const double h = io.h;
     io.dst_m[ko + id] = bm + h * dms;
     io.dst_t[ko + id] = bt + h * dts;

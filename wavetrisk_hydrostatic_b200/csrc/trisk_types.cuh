@@ -58,6 +58,8 @@ struct TrendIO {
   // MODE_ML: the level's node masks, the velocity source it writes on
   // [0, n)^2, and the needed-node map (need_map.cuh) or null
   const int* mask_n; double* src; const unsigned char* need;
+  // MODE_ML with u_star: velocity sub-step base + h * (trend + th1 * grad)
+  const double* grad; double th1;
 };
 
 struct Phys {

@@ -259,6 +259,76 @@ int wt_u_update_multi(wt_handle* h, double dt, double theta1) {
   return WT_OK;
 }
 
+}  // extern "C"
+
+// barotropic_correction (src/barotropic_2d.f90:52-116) of the scaling fields
+// m[q], t[q] of level level_start+q (the hierarchy's own when m is null), from
+// each level's free surface; stream-ordered.
+int wt_level_barotropic_correction(wt_handle* h, double* const* m, double* const* t) {
+  if (int rc = ensure_levels(h)) return rc;
+  BaroCtx* B = static_cast<BaroCtx*>(h->baro);
+  for (int l = h->level_end; l >= h->level_start; --l) {
+    const int q = l - h->level_start;
+    const DevLevel& D = h->at(l);
+    double *ms, *ts, *vs, *mm, *mt;
+    if (l == h->level_end) {
+      ms = h->mass;
+      ts = h->temp;
+    } else {
+      wt_level_state(h, l, &ms, &ts, &vs);
+    }
+    if (m) {
+      ms = m[q];
+      ts = t[q];
+    }
+    if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm)) return rc;
+    if (int rc = wt_level_mean(h, l, WT_FIELD_MEAN_TEMP, &mt)) return rc;
+    wtb::k_barotropic_correction<<<nb(10 * (D.n + 1) * (D.n + 1)), TPB, 0, h->stream>>>(D.view(), h->nz, h->ph.ref_density,
+                                                                            B->L[q].eta, mm, mt, ms, ts);
+  }
+  CKB(cudaGetLastError());
+  return WT_OK;
+}
+
+// grad_eta over the hierarchy (src/barotropic_2d.f90:455-474, with
+// cpt_or_restr_eta) into each level's gradient field, without the velocity
+// update; grad[q] receives level level_start+q's [3][NN] field.  Stream-ordered.
+int wt_level_grad_eta(wt_handle* h, const double** grad) {
+  if (int rc = ensure_levels(h)) return rc;
+  BaroCtx* B = static_cast<BaroCtx*>(h->baro);
+  for (int l = h->level_start; l <= h->level_end; ++l) {
+    BaroLevel& V = B->L[l - h->level_start];
+    const DevLevel& D = h->at(l);
+    CKB(cudaMemcpyAsync(V.eta_w, V.eta, (size_t)D.NN * 8, cudaMemcpyDeviceToDevice, h->stream));
+    if (D.n_hn > 0) wtb::k_halo_nodes<<<nb(D.n_hn), TPB, 0, h->stream>>>(D.hn, D.n_hn, V.eta_w);
+  }
+  for (int l = h->level_end; l >= h->level_start; --l) {
+    BaroLevel& V = B->L[l - h->level_start];
+    const DevLevel& D = h->at(l);
+    const int m = D.n + 1;
+    if (l < h->level_end)
+      if (int rc = wt_level_restrict_scalar(h, l, V.eta_w, B->L[l + 1 - h->level_start].eta_w, 1)) return rc;
+    wtb::k_grad_eta_update<true><<<nb(10 * m * m), TPB, 0, h->stream>>>(D.view(), 0, h->ph.grav, V.eta_w, 0.0,
+                                                                       V.grad, nullptr);
+    grad[l - h->level_start] = V.grad;
+  }
+  CKB(cudaGetLastError());
+  return WT_OK;
+}
+
+extern "C" {
+
+// barotropic_correction of the hierarchy's scaling fields from the free surface
+// of each level (wt_barotropic_upload_level).
+int wt_barotropic_correction_multi(wt_handle* h) {
+  if (!h) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = wt_level_barotropic_correction(h, nullptr, nullptr)) return rc;
+  CKB(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
+  return WT_OK;
+}
+
 int wt_barotropic_download_level(wt_handle* h, int level, double* div_flux, double* rhs, double* grad) {
   if (!h || level < h->level_start || level > h->level_end) return WT_ERR_ARG;
   if (!h->baro || static_cast<BaroCtx*>(h->baro)->L.empty()) return WT_ERR_STATE;

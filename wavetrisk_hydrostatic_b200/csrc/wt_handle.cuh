@@ -143,6 +143,11 @@ bool wt_level_zero_ok(wt_handle* h);
 int wt_level_need_build(wt_handle* h);
 const unsigned char* wt_level_need(wt_handle* h, int level);
 int wt_level_skip_epoch(wt_handle* h);
+// barotropic_correction of the given per-level scaling fields (hierarchy's own
+// when m is null) and grad_eta per level, without the velocity update
+// (wt_barotropic.cu); stream-ordered.
+int wt_level_barotropic_correction(wt_handle* h, double* const* m, double* const* t);
+int wt_level_grad_eta(wt_handle* h, const double** grad);
 // make stream st wait until the last inverse transform (wt_level_inverse or
 // WT_after_step) has completed level's state; only valid when that transform was
 // issued after every other write of the state (stream-ordered)

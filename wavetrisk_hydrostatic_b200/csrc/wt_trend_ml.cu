@@ -176,13 +176,16 @@ States hierarchy_state(wt_handle* h) {
 // last (the previous RK stage's WT_after_step): a coarser level's column and
 // step1 start as soon as that transform has rebuilt the level, beside the finer
 // levels' reconstruction.
+// With grad (per level), the velocity sub-step is u_star's base + hs * (trend +
+// th1 * grad) (src/barotropic_2d.f90:29-50), every node computed.
 int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const States* base = nullptr,
-                const States* dest = nullptr, double hs = 0.0, bool wav = false, bool after_inverse = false) {
+                const States* dest = nullptr, double hs = 0.0, bool wav = false, bool after_inverse = false,
+                const double* const* grad = nullptr, double th1 = 0.0) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const int nz = h->nz;
   // With WT_after_step following (wav), a level's results above level_start are
   // read only where its needed-node map says so (need_map.cuh).
-  auto need = [&](int l) -> const unsigned char* { return (wav && dest) ? wt_level_need(h, l) : nullptr; };
+  auto need = [&](int l) -> const unsigned char* { return (wav && dest && !grad) ? wt_level_need(h, l) : nullptr; };
   // Column + step1 of a level read only that level's state and write only its
   // own work fields, so the coarser levels' run beside the finest level's on
   // side streams (parallel branches of a captured graph).  The phase timer
@@ -271,6 +274,8 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
       io.base_m = base->m[q]; io.base_t = base->t[q]; io.base_v = base->v[q];
       io.dst_m = dest->m[q]; io.dst_t = dest->t[q]; io.dst_v = dest->v[q];
       io.h = hs;
+      io.grad = grad ? grad[q] : nullptr;
+      io.th1 = th1;
     }
     io.need = need(l);
     const unsigned chunks = (unsigned)((D.NN + wtk::NODE_TILE - 1) / wtk::NODE_TILE);
@@ -281,6 +286,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
       t.base_m = io.base_m; t.base_t = io.base_t; t.base_v = io.base_v;
       t.dst_m = io.dst_m; t.dst_t = io.dst_t; t.dst_v = io.dst_v; t.h = io.h;
       t.dm = V.dm; t.dtt = V.dt; t.mask_n = mask_n; t.src = V.src; t.need = io.need;
+      t.grad = io.grad; t.th1 = io.th1;
       if (int rc = wt_level_trend_ml_tma(h, t, M->tmaps, nullptr)) return rc;
     } else {
       wtk::k_trend_ml<<<chunks * nz, wtk::NODE_TILE, 0, h->stream>>>(D.view(), nz, io);
@@ -348,7 +354,54 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm, bool last_inv
 }
 }  // namespace
 
+namespace {
+// The four RK_split calls of RK4_split (src/time_integr.f90:360-382, 444-463)
+// over the hierarchy, without free_surface_update: per stage
+// barotropic_correction of the stage's source state, trend_ml, scalar_star and
+// u_star (src/barotropic_2d.f90:9-50; the base is always the solution, as the
+// reference's sol), and WT_after_step of the stage state.  Every node computed.
+int rk4_split_explicit(wt_handle* h, double dt, double theta1) {
+  MLCtx* M = static_cast<MLCtx*>(h->ml);
+  const States q = hierarchy_state(h);
+  States q1;
+  for (auto& V : M->L) {
+    q1.m.push_back(V.m1);
+    q1.t.push_back(V.t1);
+    q1.v.push_back(V.v1);
+  }
+  const double hs[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
+  std::vector<const double*> grad(M->L.size(), nullptr);
+  for (int stage = 0; stage < 4; ++stage) {
+    const States& src = stage == 0 ? q : q1;
+    const States& dest = stage == 3 ? q : q1;
+    if (int rc = wt_level_barotropic_correction(h, src.m.data(), src.t.data())) return rc;
+    if (int rc = wt_level_grad_eta(h, grad.data())) return rc;
+    wt_level_wav_bind(h, dest.m.data(), dest.t.data(), dest.v.data());
+    wt_level_clean_wavelets(h);
+    int rc = trend_multi(h, src, nullptr, &q, &dest, hs[stage], true, false, grad.data(), theta1);
+    if (!rc) rc = wt_level_wav_finish(h, false);
+    wt_level_wav_unbind(h);
+    if (rc) return rc;
+  }
+  return WT_OK;
+}
+}  // namespace
+
 extern "C" {
+
+// The explicit part of RK4_split over the hierarchy (RK_split four times: see
+// rk4_split_explicit); the host then takes free_surface_update (eta_update,
+// barotropic_correction, u_update, WT_after_step).  Uses each level's free
+// surface (wt_barotropic_upload_level) and the masks as they are.
+int wt_rk4_split_explicit(wt_handle* h, double dt, double theta1) {
+  if (!h) return WT_ERR_ARG;
+  if (!h->wav) return WT_ERR_STATE;
+  if (int rc = ensure(h)) return rc;
+  if (int rc = rk4_split_explicit(h, dt, theta1)) return rc;
+  CKM(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
+  return WT_OK;
+}
 
 // RK4 (src/time_integr.f90:78-103) over the hierarchy: each stage evaluates
 // trend_ml on every level, takes the RK sub-step on every level and runs

@@ -293,6 +293,15 @@ class WaveletHierarchy(DeviceGrid):
         N.check("wt_lnorm", N.lib().wt_lnorm(self.h, code, N.dptr(out)))
         return out
 
+    def rk4_split_explicit(self, dt: float, theta1: float) -> None:
+        """RK4_split's four RK_split stages (barotropic_correction, trend_ml,
+        scalar_star, u_star, WT_after_step) with each level's free surface."""
+        N.check("wt_rk4_split_explicit", N.lib().wt_rk4_split_explicit(self.h, float(dt), float(theta1)))
+
+    def barotropic_correction(self) -> None:
+        """barotropic_correction of every level's scaling fields from its free surface."""
+        N.check("wt_barotropic_correction_multi", N.lib().wt_barotropic_correction_multi(self.h))
+
     def skip_inactive(self, on: bool) -> None:
         """WT_TUNE_SKIP_INACTIVE: let the RK stages leave out the finest level's
         nodes whose step1 and trend results cannot reach the state after

@@ -218,10 +218,22 @@ def elliptic_case(lmax, repeats=3):
     _, fr = S.download()
     out = {"workload": f"Helmholtz free-surface solve, uniform J{lmax} ({10 * 4 ** lmax + 2} cells), "
                        f"hierarchy J5..J{lmax}, seeded bathymetry 500-5000 m, dt 600 s, rel. residual 1e-10"}
+    # the learned preconditioner: trained once on this level on residual/error
+    # pairs of the FP64 multigrid (training time reported apart from the solves)
+    S.learned_setup(1)
+    tr = S.learned_train(n_rhs=8, cycles=4, epochs=15, lr=2e-3, seed=1)
+    out["learned_training"] = {"pairs": tr.pairs, "adam_steps": tr.steps, "loss_first_epoch": tr.loss_first_epoch,
+                               "loss_last_epoch": tr.loss_last_epoch, "ms_generate": tr.ms_generate,
+                               "ms_train": tr.ms_train}
+    it = dict(ir_max=2000)
     methods = [("fmg", solver_opts("fmg", 1e-10, max_vcycle=50, coarse_iter=300)),
                ("srj", solver_opts("srj", 1e-10, max_srj_iter=4000, coarse_iter=300)),
                ("mg64", solver_opts("mg64", 1e-10, down_iter=2, up_iter=2, coarse_iter=20)),
-               ("mixed", solver_opts("mixed", 1e-10, down_iter=2, up_iter=2, coarse_iter=20))]
+               ("mixed", solver_opts("mixed", 1e-10, down_iter=2, up_iter=2, coarse_iter=20)),
+               ("fcg_learned", solver_opts("fcg_learned", 1e-10, down_iter=2, up_iter=2, coarse_iter=20, **it)),
+               ("fcg", solver_opts("fcg", 1e-10, **it)),
+               ("fcg_mg", solver_opts("fcg_mg", 1e-10, down_iter=2, up_iter=2, coarse_iter=20, **it))]
+    q = len(levels) - 1
     for name, o in methods:
         best, rep = None, None
         for _ in range(repeats):
@@ -230,8 +242,12 @@ def elliptic_case(lmax, repeats=3):
             best = rep.ms if best is None else min(best, rep.ms)
         out[name] = {"ms": best, "rel_residual": rep.true_rel_residual, "status": rep.status,
                      "outer_iterations": rep.outer_iterations}
+        if name.startswith("fcg"):
+            out[name].update(iterations=rep.iterations[q], restarts=rep.restarts, fallback_at=rep.precond_fallback)
     out["mixed_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["mixed"]["ms"]
     out["mixed_speedup_vs_fmg"] = out["fmg"]["ms"] / out["mixed"]["ms"]
+    out["learned_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["fcg_learned"]["ms"]
+    out["learned_iterations_vs_fcg"] = out["fcg_learned"]["iterations"] / max(1, out["fcg"]["iterations"])
     S.close()
     return out
 

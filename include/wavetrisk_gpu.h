@@ -127,7 +127,14 @@ int wt_profile_rk4(wt_handle* h, double dt, int nsteps, double* ms_per_launch, i
  * uniform hierarchy level_start..level_end of the handle.  Fields u (solution,
  * initial guess) and f (right-hand side) are multi-level: the levels' NN-node
  * arrays concatenated from level_start to level_end. */
-enum { WT_SOLVER_FMG = 0, WT_SOLVER_SRJ = 1, WT_SOLVER_MIXED_IR = 2, WT_SOLVER_MG64 = 3 };
+enum { WT_SOLVER_FMG = 0, WT_SOLVER_SRJ = 1, WT_SOLVER_MIXED_IR = 2, WT_SOLVER_MG64 = 3,
+       /* Flexible CG (truncated to one previous direction, area-weighted inner
+        * product) on level_end, ir_tol / ir_max as for WT_SOLVER_MIXED_IR:
+        * preconditioned by the learned network with the FP64 V-cycle as the
+        * fallback when it fails to contract (FCG_LEARNED), unpreconditioned
+        * (FCG, the method without the network) or by the FP64 V-cycle alone
+        * (FCG_MG).  No reference counterpart. */
+       WT_SOLVER_FCG_LEARNED = 4, WT_SOLVER_FCG = 5, WT_SOLVER_FCG_MG = 6 };
 
 typedef struct {
   int method;                 /* WT_SOLVER_*                                         */
@@ -151,6 +158,9 @@ typedef struct {
   int outer_iterations;       /* refinement steps (WT_SOLVER_MIXED_IR)              */
   double true_rel_residual;   /* FP64 ||f - L u|| / ||f|| on level_end after solve  */
   double ms;                  /* host wall time of the solve                         */
+  int precond_fallback;       /* FCG_LEARNED: iteration at which the V-cycle took
+                               * over from the network (0: it never did)             */
+  int restarts;               /* FCG: restarts from the true residual               */
 } wt_solver_report;
 
 /* Builds the operator tables (replaces the per-call coefficient work of
@@ -171,6 +181,52 @@ int wt_elliptic_l2(wt_handle* h, int level, int which, double* out);
  * on the resident u, f.  Returns WT_ERR_NOT_CONVERGED when the mixed solver
  * stops at ir_max above ir_tol. */
 int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report* rep);
+
+/* ------------------------------------------------ learned preconditioner ---- */
+/* A hexagonal-stencil convolution network (7 taps: a node and its six
+ * neighbours; 2 -> 32 -> 32 -> 1 channels, ReLU) mapping a residual r of
+ * level_end, scaled by its rms, and the depth |H| to an approximation of the
+ * error e with L e = r.  FP32 master weights, BF16 weights in every forward
+ * and backward kernel, FP32 activations and accumulation.  The nodes are the
+ * slots of [0, n]^2 of each lozenge that are their own ghost source, numbered
+ * lozenge, row j, column i.  Requires wt_elliptic_setup; no reference
+ * counterpart (the reference preconditions nothing). */
+typedef struct {
+  int n_rhs;       /* seeded N(0,1) right-hand sides, zero mean                   */
+  int cycles;      /* residual/error pairs per right-hand side: before each of the
+                    * first `cycles` FP64 V-cycles of a solve from 0              */
+  int epochs;      /* Adam passes over all pairs, one pair per step              */
+  float lr;        /* Adam step, cosine-decayed to lr / 20                       */
+  unsigned long long seed;
+  int down_iter, up_iter, coarse_iter;   /* the generating V-cycle              */
+} wt_learn_opts;
+
+typedef struct {
+  int pairs, steps;
+  double loss_first_epoch, loss_last_epoch;  /* mean energy-norm loss (below)      */
+  double ms_generate, ms_train;              /* host wall time                   */
+} wt_learn_report;
+
+int wt_learned_setup(wt_handle* h, unsigned long long seed);   /* He-initialised weights */
+int wt_learned_num_params(void);
+/* FP32 master parameters (wt_learned_num_params floats); get or set may be NULL. */
+int wt_learned_params(wt_handle* h, float* get, const float* set);
+/* Node count; with slot/tap non-NULL also the node slots (ns) and the taps
+ * (7*ns, tap-major, -1 where a tap leaves the node set). */
+int wt_learned_layout(wt_handle* h, int* ns, int* slot, int* tap);
+/* The preconditioner, odd in r: z = rms(r) (net(r/rms(r)) - net(-r/rms(r))) / 2
+ * on the ns nodes (host arrays). */
+int wt_learned_infer(wt_handle* h, const double* r, double* z);
+/* Training loss, the error in the energy norm of the solve,
+ *   <d, -L d>_A / |A|,  d = net(r/rms(r)) - e/rms(r),
+ * (<,>_A weighted by the cell areas 1/hex_inv, |A| their sum) and the gradient
+ * 2 A (-L d) / |A| pushed back through the network to the parameters (host
+ * arrays; grad: wt_learned_num_params floats).  The solve's u, f are kept. */
+int wt_learned_grad(wt_handle* h, const double* r, const double* e, double* loss, float* grad);
+/* Generates residual/error pairs with the FP64 multigrid (u and f of
+ * level_end are kept) and trains the network on them with Adam on the GPU,
+ * each pair seen with either sign. */
+int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep);
 
 /* ------------------------------------------------------ no allocation ---- */
 /* Weighted l2 norm of one level (the solver's l2, src/lin_solve.f90:433-464)

@@ -67,7 +67,18 @@ class wt_solver_opts(C.Structure):
 
 class wt_solver_report(C.Structure):
     _fields_ = [("nrm_res_init", C.c_double * 16), ("nrm_res_final", C.c_double * 16), ("iterations", C.c_int * 16),
-                ("outer_iterations", C.c_int), ("true_rel_residual", C.c_double), ("ms", C.c_double)]
+                ("outer_iterations", C.c_int), ("true_rel_residual", C.c_double), ("ms", C.c_double),
+                ("precond_fallback", C.c_int), ("restarts", C.c_int)]
+
+
+class wt_learn_opts(C.Structure):
+    _fields_ = [("n_rhs", C.c_int), ("cycles", C.c_int), ("epochs", C.c_int), ("lr", C.c_float),
+                ("seed", C.c_ulonglong), ("down_iter", C.c_int), ("up_iter", C.c_int), ("coarse_iter", C.c_int)]
+
+
+class wt_learn_report(C.Structure):
+    _fields_ = [("pairs", C.c_int), ("steps", C.c_int), ("loss_first_epoch", C.c_double),
+                ("loss_last_epoch", C.c_double), ("ms_generate", C.c_double), ("ms_train", C.c_double)]
 
 
 _lib = None
@@ -120,6 +131,13 @@ _DEVICE_SIGS = {
     "wt_elliptic_prolong": [_vp, C.c_int],
     "wt_elliptic_l2": [_vp, C.c_int, C.c_int, _dp],
     "wt_elliptic_solve": [_vp, C.POINTER(wt_solver_opts), C.POINTER(wt_solver_report)],
+    "wt_learned_setup": [_vp, C.c_ulonglong],
+    "wt_learned_num_params": [],
+    "wt_learned_params": [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float)],
+    "wt_learned_layout": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "wt_learned_infer": [_vp, _dp, _dp],
+    "wt_learned_grad": [_vp, _dp, _dp, _dp, C.POINTER(C.c_float)],
+    "wt_learned_train": [_vp, C.POINTER(wt_learn_opts), C.POINTER(wt_learn_report)],
     "wt_wavelet_setup": [_vp],
     "wt_upload_field": [_vp, C.c_int, C.c_int, _vp],
     "wt_download_field": [_vp, C.c_int, C.c_int, _vp],

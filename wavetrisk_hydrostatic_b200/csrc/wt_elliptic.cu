@@ -55,6 +55,7 @@ struct Ell {
   int cycle_key[2] = {-1, -1};
   int nbmax = 0;
   std::vector<void*> allocs;
+  void* lp = nullptr;  // learned preconditioner (wt_learned.cuh)
 
   EllLev view(int l) const {
     const DevLevel& D = const_cast<wt_handle*>(h)->at(l);
@@ -94,8 +95,11 @@ int alloc_field(Ell& E, MField& F, bool fp32 = false) {
 }  // namespace
 
 // ---------------------------------------------------------------- setup ----
+void lp_release(void* p);
+
 static void ell_free(Ell* E) {
   if (!E) return;
+  lp_release(E->lp);
   for (auto& ex : E->cycle_exec)
     if (ex) cudaGraphExecDestroy(ex);
   for (void* p : E->allocs) cudaFree(p);
@@ -410,6 +414,7 @@ void srj(Ell& E, const wt_solver_opts& o, wt_solver_report& rep) {
 }  // namespace
 
 #include "wt_elliptic_mixed.cuh"
+#include "wt_learned.cuh"
 
 // ---------------------------------------------------------------- C-ABI ----
 extern "C" {
@@ -492,6 +497,9 @@ int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report
   else if (opts->method == WT_SOLVER_SRJ) srj(E, *opts, *rep);
   else if (opts->method == WT_SOLVER_MIXED_IR) rc = mixed_ir(E, *opts, *rep);
   else if (opts->method == WT_SOLVER_MG64) rc = mixed_ir(E, *opts, *rep, true);
+  else if (opts->method == WT_SOLVER_FCG_LEARNED) rc = fcg_solve(E, *opts, *rep, PRE_NET);
+  else if (opts->method == WT_SOLVER_FCG) rc = fcg_solve(E, *opts, *rep, PRE_NONE);
+  else if (opts->method == WT_SOLVER_FCG_MG) rc = fcg_solve(E, *opts, *rep, PRE_MG);
   else return WT_ERR_ARG;
   CKE(cudaStreamSynchronize(E.s()));
   auto t1 = std::chrono::steady_clock::now();

@@ -1,0 +1,558 @@
+// Learned preconditioner of the free-surface solve (network in
+// learned_kernels.cuh): node layout, training-pair generation with the FP64
+// multigrid, Adam training, and flexible CG preconditioned by the network
+// with the FP64 V-cycle as fallback.  Included by wt_elliptic.cu only, after
+// wt_elliptic_mixed.cuh.
+#pragma once
+
+#include <random>
+
+#include "learned_kernels.cuh"
+
+void lp_release(void* p);
+
+namespace {
+
+using namespace wtl;
+
+constexpr int LP_TPB = 128, LP_DOT = 256;
+
+struct LPNet {
+  int l = 0, ns = 0;
+  int64_t NN = 0;
+  int* slot = nullptr;  // ns node slots of the level
+  int* tap = nullptr;   // 7*ns compact tap indices
+  float *w = nullptr, *wr = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+  float *x = nullptr, *h1 = nullptr, *h2 = nullptr, *y = nullptr, *dy = nullptr, *dh1 = nullptr, *dh2 = nullptr;
+  double *rs = nullptr, *fcg = nullptr, *partial = nullptr, *losses = nullptr;
+  double *rc = nullptr, *ec = nullptr;  // one compact pair (grad / infer)
+  double *pr = nullptr, *pe = nullptr, *pscale = nullptr;  // training pairs
+  int npairs = 0;
+  double *r = nullptr, *z = nullptr, *lz = nullptr, *p = nullptr, *lp = nullptr, *ustar = nullptr,
+         *usave = nullptr, *fsave = nullptr;  // level arrays
+  int adam_t = 0;
+  double inv_area = 1.0;  // 1 / sum of the node areas 1 / hex_inv
+  cudaGraphExec_t it_exec[3] = {nullptr, nullptr, nullptr};
+  int it_key[3] = {-1, -1, -1};
+  std::vector<void*> allocs, pair_allocs;
+  int nbd() const { return (ns + LP_DOT - 1) / LP_DOT; }
+};
+
+template <class T>
+int lpalloc(std::vector<void*>& A, T** p, int64_t n) {
+  cudaError_t e = cudaMalloc(p, sizeof(T) * std::max<int64_t>(1, n));
+  if (e != cudaSuccess) return wt_handle_fail("learned alloc", e);
+  cudaMemset(*p, 0, sizeof(T) * std::max<int64_t>(1, n));
+  A.push_back(*p);
+  return WT_OK;
+}
+
+void lp_free_pairs(LPNet* N) {
+  for (void* q : N->pair_allocs) cudaFree(q);
+  N->pair_allocs.clear();
+  N->pr = N->pe = N->pscale = nullptr;
+  N->npairs = 0;
+}
+
+inline unsigned lpg(int64_t n, int tpb = LP_TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+// Box-Muller normal deviates from a 64-bit Mersenne twister (same sequence on
+// every platform, unlike std::normal_distribution).
+struct Normal {
+  std::mt19937_64 g;
+  explicit Normal(uint64_t s) : g(s) {}
+  double u() { return ((g() >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
+  double operator()() {
+    const double a = u(), b = u();
+    return std::sqrt(-2.0 * std::log(a)) * std::cos(6.283185307179586 * b);
+  }
+};
+
+int lp_init_params(LPNet& N, uint64_t seed) {
+  std::vector<float> w(kLpParams, 0.f);
+  Normal rn(seed);
+  auto fill = [&](int off, int cnt, double sd) {
+    for (int k = 0; k < cnt; ++k) w[off + k] = (float)(sd * rn());
+  };
+  fill(kW1, kTaps * kIn * kC, std::sqrt(2.0 / (kTaps * kIn)));
+  fill(kW2, kTaps * kC * kC, std::sqrt(2.0 / (kTaps * kC)));
+  fill(kW3, kTaps * kC, 0.1 * std::sqrt(1.0 / (kTaps * kC)));
+  cudaMemcpy(N.w, w.data(), 4 * kLpParams, cudaMemcpyHostToDevice);
+  cudaMemset(N.m, 0, 4 * kLpParams);
+  cudaMemset(N.v, 0, 4 * kLpParams);
+  N.adam_t = 0;
+  k_lp_round<<<lpg(kLpParams), LP_TPB>>>(N.w, N.wr, kLpParams);
+  cudaError_t e = cudaDeviceSynchronize();
+  return e == cudaSuccess ? WT_OK : wt_handle_fail("learned init", e);
+}
+
+int lp_build(Ell& E, uint64_t seed) {
+  auto* N = new LPNet();
+  DevLevel& D = E.h->at(E.le);
+  N->l = E.le;
+  N->NN = D.NN;
+  const int n = D.n, P = D.P;
+  std::vector<int> nsrc(D.NN);
+  cudaMemcpy(nsrc.data(), D.nsrc, 4 * D.NN, cudaMemcpyDeviceToHost);
+  std::vector<int> slot, cid(D.NN, -1);
+  for (int d = 0; d < 10; ++d)
+    for (int j = 0; j <= n; ++j)
+      for (int i = 0; i <= n; ++i) {
+        const int k = (d * P + j + 2) * P + i + 2;
+        if (nsrc[k] == k) {
+          cid[k] = (int)slot.size();
+          slot.push_back(k);
+        }
+      }
+  const int ns = (int)slot.size();
+  N->ns = ns;
+  {
+    std::vector<double> hinv(D.NN);
+    cudaMemcpy(hinv.data(), D.hex_inv, 8 * D.NN, cudaMemcpyDeviceToHost);
+    double area = 0.0;
+    for (int k : slot) area += 1.0 / hinv[k];
+    N->inv_area = 1.0 / area;
+  }
+  static const int di[kTaps] = {0, 1, 1, 0, -1, -1, 0}, dj[kTaps] = {0, 0, 1, 1, 0, -1, -1};
+  std::vector<int> tap((size_t)kTaps * ns);
+  for (int s = 0; s < ns; ++s) {
+    const int k = slot[s], d = k / (P * P), r = k % (P * P), i = r % P - 2, j = r / P - 2;
+    for (int t = 0; t < kTaps; ++t) {
+      const int kn = (d * P + j + dj[t] + 2) * P + i + di[t] + 2;
+      tap[(size_t)t * ns + s] = cid[nsrc[kn]];
+    }
+  }
+  auto& A = N->allocs;
+  int rc = WT_OK;
+  auto al = [&](auto** p, int64_t cnt) {
+    if (rc == WT_OK) rc = lpalloc(A, p, cnt);
+  };
+  al(&N->slot, ns);
+  al(&N->tap, (int64_t)kTaps * ns);
+  for (float** p : {&N->w, &N->wr, &N->g, &N->m, &N->v}) al(p, kLpParams);
+  al(&N->x, (int64_t)kIn * ns);
+  al(&N->h1, (int64_t)kC * ns);
+  al(&N->h2, (int64_t)kC * ns);
+  al(&N->dh1, (int64_t)kC * ns);
+  al(&N->dh2, (int64_t)kC * ns);
+  al(&N->y, ns);
+  al(&N->dy, ns);
+  al(&N->rs, 2);
+  al(&N->fcg, FCG_N);
+  al(&N->partial, N->nbd());
+  al(&N->losses, 1);
+  al(&N->rc, ns);
+  al(&N->ec, ns);
+  for (double** p : {&N->r, &N->z, &N->lz, &N->p, &N->lp, &N->ustar, &N->usave, &N->fsave}) al(p, D.NN);
+  if (rc == WT_OK) {
+    cudaMemcpy(N->slot, slot.data(), 4 * (size_t)ns, cudaMemcpyHostToDevice);
+    cudaMemcpy(N->tap, tap.data(), 4 * tap.size(), cudaMemcpyHostToDevice);
+    rc = lp_init_params(*N, seed);
+  }
+  if (rc != WT_OK) {
+    lp_release(N);
+    return rc;
+  }
+  if (E.lp) lp_release(E.lp);
+  E.lp = N;
+  return WT_OK;
+}
+
+// rs = rms of r over the nodes, -rs in rs[1] (r read at slot[s]; nullptr: compact).
+void lp_rms(LPNet& N, cudaStream_t st, const int* slot, const double* r, double* rs) {
+  k_lp_dot<LP_DOT><<<N.nbd(), LP_DOT, 0, st>>>(N.ns, slot, r, r, nullptr, N.partial);
+  k_lp_sum<<<1, 256, 0, st>>>(N.partial, N.nbd(), rs, 1, 1.0 / N.ns);
+}
+
+// Network output y for input r / *rs (r read at slot[s]; nullptr: compact).
+void lp_forward(Ell& E, LPNet& N, const int* slot, const double* r, const double* rs) {
+  cudaStream_t st = E.s();
+  const int ns = N.ns;
+  k_lp_input<<<lpg(ns), LP_TPB, 0, st>>>(ns, slot, N.slot, r, rs, E.h->at(N.l).topo, N.x);
+  k_lp_conv<kIn, kC, true><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.x, N.wr + kW1, N.wr + kB1, N.h1);
+  k_lp_conv<kC, kC, true><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h1, N.wr + kW2, N.wr + kB2, N.h2);
+  k_lp_conv<kC, 1, false><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h2, N.wr + kW3, N.wr + kB3, N.y);
+}
+
+// The preconditioner z = rs (net(r/rs) - net(-r/rs)) / 2, rs = rms(r): odd in
+// r and proportional to |r|.  r read and z written at slot[s] (nullptr: compact).
+void lp_precondition(Ell& E, LPNet& N, const int* slot, const double* r, double* z) {
+  cudaStream_t st = E.s();
+  lp_rms(N, st, slot, r, N.rs);
+  for (int pass = 0; pass < 2; ++pass) {
+    lp_forward(E, N, slot, r, N.rs + pass);
+    k_lp_output<<<lpg(N.ns), LP_TPB, 0, st>>>(N.ns, slot, N.y, N.rs + pass, z, pass);
+  }
+}
+
+// Energy-norm loss of the network output against the compact target e (scaled
+// by *rs) into *loss, then the parameter gradient into N.g.
+void lp_backward(Ell& E, LPNet& N, const double* e, const double* rs, double* loss) {
+  cudaStream_t st = E.s();
+  const int ns = N.ns;
+  k_lp_err<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.y, e, rs, N.z);
+  op(E, OP_APPLY, N.l, N.z, nullptr, N.lz);
+  k_lp_aloss<LP_DOT><<<N.nbd(), LP_DOT, 0, st>>>(ns, N.slot, N.z, N.lz, E.h->at(N.l).hex_inv, N.inv_area, N.dy,
+                                                 N.partial);
+  k_lp_sum<<<1, 256, 0, st>>>(N.partial, N.nbd(), loss, 0, N.inv_area);
+  cudaMemsetAsync(N.g, 0, 4 * kLpParams, st);
+  cudaMemsetAsync(N.dh1, 0, 4 * (size_t)kC * ns, st);
+  cudaMemsetAsync(N.dh2, 0, 4 * (size_t)kC * ns, st);
+  const unsigned gw = std::min<unsigned>((ns + kChunk - 1) / kChunk, 148 * 4);
+  k_lp_wgrad<kC, 1><<<gw, 256, 0, st>>>(ns, N.tap, N.h2, N.dy, N.g + kW3, N.g + kB3);
+  k_lp_igrad<kC, 1><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.wr + kW3, N.dy, N.dh2);
+  k_lp_relu_back<<<lpg((int64_t)kC * ns, 256), 256, 0, st>>>(kC * ns, N.h2, N.dh2);
+  k_lp_wgrad<kC, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.h1, N.dh2, N.g + kW2, N.g + kB2);
+  k_lp_igrad<kC, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.wr + kW2, N.dh2, N.dh1);
+  k_lp_relu_back<<<lpg((int64_t)kC * ns, 256), 256, 0, st>>>(kC * ns, N.h1, N.dh1);
+  k_lp_wgrad<kIn, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.x, N.dh1, N.g + kW1, N.g + kB1);
+}
+
+void lp_adam(Ell& E, LPNet& N, float lr) {
+  cudaStream_t st = E.s();
+  ++N.adam_t;
+  k_lp_adam<<<lpg(kLpParams, 256), 256, 0, st>>>(kLpParams, N.w, N.g, N.m, N.v, lr, 0.9f, 0.999f, 1e-8f, N.adam_t);
+  k_lp_round<<<lpg(kLpParams, 256), 256, 0, st>>>(N.w, N.wr, kLpParams);
+}
+
+// Residual/error pairs from FP64 multigrid: for each seeded right-hand side,
+// the solution u* to 1e-11, then from u = 0 the residual f - L u and error
+// u* - u before each of `cycles` V-cycles.  u and f of the level are kept.
+int lp_generate(Ell& E, LPNet& N, const wt_learn_opts& lo, const wt_solver_opts& mg) {
+  const int q = E.le - E.ls, ns = N.ns, l = E.le;
+  const int64_t NN = N.NN;
+  cudaStream_t st = E.s();
+  lp_free_pairs(&N);
+  const int np = lo.n_rhs * lo.cycles;
+  int rc = WT_OK;
+  if ((rc = lpalloc(N.pair_allocs, &N.pr, (int64_t)np * ns))) return rc;
+  if ((rc = lpalloc(N.pair_allocs, &N.pe, (int64_t)np * ns))) return rc;
+  if ((rc = lpalloc(N.pair_allocs, &N.pscale, 2 * (int64_t)np))) return rc;
+  N.npairs = np;
+  cudaMemcpyAsync(N.usave, E.u.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(N.fsave, E.f.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, st);
+  std::vector<double> fc(ns);
+  wt_solver_opts o = mg;
+  o.ir_tol = 1e-11;
+  o.ir_max = std::max(o.ir_max, 60);
+  for (int k = 0; k < lo.n_rhs; ++k) {
+    Normal rn(lo.seed * 1000003ull + 7919ull * (uint64_t)k + 1);
+    double mean = 0.0;
+    for (double& v : fc) mean += (v = rn());
+    mean /= ns;
+    for (double& v : fc) v -= mean;
+    cudaMemcpyAsync(N.rc, fc.data(), 8 * (size_t)ns, cudaMemcpyHostToDevice, st);
+    k_lp_scatter<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.rc, E.f.lv[q]);
+    zero_level(E, l, E.u.lv[q]);
+    wt_solver_report rep{};
+    rc = mixed_ir(E, o, rep, true);
+    if (rc != WT_OK && rc != WT_ERR_NOT_CONVERGED) break;
+    rc = WT_OK;
+    cudaMemcpyAsync(N.ustar, E.u.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, st);
+    zero_level(E, l, E.u.lv[q]);
+    for (int c = 0; c < lo.cycles; ++c) {
+      const int64_t idx = (int64_t)k * lo.cycles + c;
+      op(E, OP_RESID, l, E.u.lv[q], E.f.lv[q], E.res.lv[q]);
+      k_lp_gather<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, E.res.lv[q], N.pr + idx * ns);
+      k_lp_diff<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.ustar, E.u.lv[q], N.pe + idx * ns);
+      lp_rms(N, st, nullptr, N.pr + idx * ns, N.rs);
+      cudaMemcpyAsync(N.pscale + idx, N.rs, 8, cudaMemcpyDeviceToDevice, st);
+      vcycle64(E, o);
+      k_axpy_d<<<nb(NN), TPB, 0, st>>>(NN, E.u.lv[q], E.corr.lv[q]);
+    }
+  }
+  k_lp_negate<<<lpg(np), LP_TPB, 0, st>>>(np, N.pscale, N.pscale + np);  // sign-flipped pairs
+  cudaMemcpyAsync(E.u.lv[q], N.usave, 8 * NN, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(E.f.lv[q], N.fsave, 8 * NN, cudaMemcpyDeviceToDevice, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return wt_handle_fail("learned generate", e);
+  return rc;
+}
+
+int lp_train(Ell& E, LPNet& N, const wt_learn_opts& lo, wt_learn_report& rep) {
+  cudaStream_t st = E.s();
+  const int np = N.npairs, ns = N.ns;
+  const int steps = std::max(1, lo.epochs) * np;
+  double* losses = nullptr;
+  std::vector<void*> tmp;
+  if (int rc = lpalloc(tmp, &losses, steps)) return rc;
+  std::mt19937_64 g(lo.seed ^ 0x5bd1e995ull);
+  std::vector<int> perm(np);
+  for (int k = 0; k < np; ++k) perm[k] = k;
+  std::uniform_int_distribution<int> coin(0, 1);
+  int step = 0;
+  const double PI = std::acos(-1.0);
+  for (int ep = 0; ep < std::max(1, lo.epochs); ++ep) {
+    std::shuffle(perm.begin(), perm.end(), g);
+    for (int k : perm) {
+      const float lr =
+          (float)(lo.lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(PI * step / std::max(1, steps - 1)))));
+      // each pair is seen with either sign (the network is made odd at use)
+      const double* sc = N.pscale + k + (coin(g) ? np : 0);
+      lp_forward(E, N, nullptr, N.pr + (int64_t)k * ns, sc);
+      lp_backward(E, N, N.pe + (int64_t)k * ns, sc, losses + step);
+      lp_adam(E, N, lr);
+      ++step;
+    }
+  }
+  std::vector<double> h(steps);
+  cudaMemcpyAsync(h.data(), losses, 8 * (size_t)steps, cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  for (void* p : tmp) cudaFree(p);
+  if (e != cudaSuccess) return wt_handle_fail("learned train", e);
+  double a = 0, b = 0;
+  for (int k = 0; k < np; ++k) {
+    a += h[k];
+    b += h[steps - np + k];
+  }
+  rep.pairs = np;
+  rep.steps = steps;
+  rep.loss_first_epoch = a / np;
+  rep.loss_last_epoch = b / np;
+  for (int k = 0; k < steps; ++k)
+    if (!std::isfinite(h[k])) return WT_ERR_NONFINITE;
+  return WT_OK;
+}
+
+// ------------------------------------------------------- flexible CG ----
+enum { PRE_NONE = 0, PRE_NET = 1, PRE_MG = 2 };
+
+// One FCG iteration as a stream sequence (captured once per preconditioner):
+// z = M(r); Lz; beta and the new direction; alpha and the update; ||r||.
+void fcg_iteration(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
+  cudaStream_t st = E.s();
+  const int q = E.le - E.ls, l = E.le, ns = N.ns;
+  const double* hinv = E.h->at(l).hex_inv;
+  if (pre == PRE_NONE) {
+    k_fcg_neg<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.r, N.z);
+  } else if (pre == PRE_NET) {
+    lp_precondition(E, N, N.slot, N.r, N.z);
+  } else {
+    cudaMemcpyAsync(E.res.lv[q], N.r, 8 * N.NN, cudaMemcpyDeviceToDevice, st);
+    vcycle64(E, o);
+    cudaMemcpyAsync(N.z, E.corr.lv[q], 8 * N.NN, cudaMemcpyDeviceToDevice, st);
+  }
+  op(E, OP_APPLY, l, N.z, nullptr, N.lz);
+  auto wdot = [&](const double* a, const double* b, int slotv) {
+    k_lp_dot<LP_DOT><<<N.nbd(), LP_DOT, 0, st>>>(ns, N.slot, a, b, hinv, N.partial);
+    k_lp_sum<<<1, 256, 0, st>>>(N.partial, N.nbd(), N.fcg + slotv, 0, 1.0);
+  };
+  wdot(N.z, N.lp, FCG_ZLP);
+  k_fcg_dir<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.fcg, N.z, N.lz, N.p, N.lp);
+  wdot(N.p, N.r, FCG_PR);
+  wdot(N.p, N.lp, FCG_DELTA);
+  k_fcg_step<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.fcg, N.p, N.lp, E.u.lv[q], N.r);
+  EllLev V = E.view(l);
+  const unsigned g = nb(10 * E.m(l) * E.m(l));
+  k_ell_dot<TPB><<<g, TPB, 0, st>>>(V, N.r, N.r, E.partial);
+  k_final_sum<<<1, 256, 0, st>>>(E.partial, (int)g, N.fcg + FCG_RNORM, 1, nullptr);
+}
+
+int fcg_launch(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
+  cudaGraphExec_t& ex = N.it_exec[pre];
+  const int key = pre == PRE_MG ? o.down_iter * 1000000 + o.up_iter * 10000 + o.coarse_iter : 0;
+  if (!ex || N.it_key[pre] != key) {
+    if (ex) {
+      cudaGraphExecDestroy(ex);
+      ex = nullptr;
+    }
+    cudaGraph_t g;
+    cudaStreamBeginCapture(E.s(), cudaStreamCaptureModeThreadLocal);
+    fcg_iteration(E, N, o, pre);
+    cudaError_t ce = cudaStreamEndCapture(E.s(), &g);
+    if (ce != cudaSuccess) return wt_handle_fail("fcg capture", ce);
+    ce = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return wt_handle_fail("fcg instantiate", ce);
+    N.it_key[pre] = key;
+  }
+  cudaError_t le = cudaGraphLaunch(ex, E.s());
+  return le == cudaSuccess ? WT_OK : wt_handle_fail("fcg launch", le);
+}
+
+// r = f - L u (true residual) and a restart of the recurrences.
+void fcg_restart(Ell& E, LPNet& N) {
+  const int q = E.le - E.ls;
+  op(E, OP_RESID, E.le, E.u.lv[q], E.f.lv[q], N.r);
+  cudaMemsetAsync(N.fcg, 0, 8 * FCG_N, E.s());
+}
+
+// Flexible CG on level_end to ir_tol (relative to ||f||, the solver's l2).
+// With the network (PRE_NET) the V-cycle takes over when the residual has not
+// halved over the last kWin iterations, or when a step breaks down (<p, Lp> not
+// negative or not finite).
+int fcg_solve(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, int pre) {
+  if (!E.lp) {
+    if (int rc = lp_build(E, 1)) return rc;
+  }
+  LPNet& N = *static_cast<LPNet*>(E.lp);
+  const int q = E.le - E.ls, l = E.le;
+  constexpr int kWin = 10;
+  double nf = l2(E, l, E.f.lv[q]);
+  if (nf == 0.0) nf = 1.0;
+  fcg_restart(E, N);
+  double err = l2(E, l, N.r) / nf;
+  rep.nrm_res_init[q] = err;
+  std::vector<double> hist{err};
+  int it = 0, since = 0, net_its = 0, breaks = 0;
+  int mode = pre;
+  int rc = WT_OK;
+  while (err > o.ir_tol && it < o.ir_max) {
+    if ((rc = fcg_launch(E, N, o, mode))) return rc;
+    ++it;
+    ++since;
+    if (mode == PRE_NET) ++net_its;
+    double sc[FCG_N];
+    cudaMemcpyAsync(sc, N.fcg, 8 * FCG_N, cudaMemcpyDeviceToHost, E.s());
+    cudaError_t ce = cudaStreamSynchronize(E.s());
+    if (ce != cudaSuccess) return wt_handle_fail("fcg sync", ce);
+    err = sc[FCG_RNORM] / nf;
+    hist.push_back(err);
+    const bool broke = sc[FCG_BREAK] != 0.0 || !std::isfinite(err);
+    const bool stalled = since >= kWin && err > 0.5 * hist[hist.size() - 1 - kWin];
+    if (mode == PRE_NET && (broke || stalled)) {
+      mode = PRE_MG;
+      rep.precond_fallback = it;
+      since = 0;
+      fcg_restart(E, N);
+      ++rep.restarts;
+      err = l2(E, l, N.r) / nf;
+      continue;
+    }
+    if (broke) {
+      if (++breaks > 3) break;
+      since = 0;
+      fcg_restart(E, N);
+      ++rep.restarts;
+      err = l2(E, l, N.r) / nf;
+      continue;
+    }
+    if (err <= o.ir_tol) {
+      // the recurrence's residual drifts from the true one: check and restart
+      fcg_restart(E, N);
+      err = l2(E, l, N.r) / nf;
+      if (err > o.ir_tol) {
+        ++rep.restarts;
+        since = 0;
+      }
+    }
+  }
+  DevLevel& D = E.h->at(l);
+  k_lp_fill_ghost<<<nb(D.NN), TPB, 0, E.s()>>>(D.NN, D.nsrc, E.u.lv[q]);
+  rep.iterations[q] = it;
+  rep.outer_iterations = pre == PRE_NET ? net_its : it;
+  rep.nrm_res_final[q] = err;
+  return err <= o.ir_tol ? WT_OK : WT_ERR_NOT_CONVERGED;
+}
+
+}  // namespace
+
+void lp_release(void* p) {
+  if (!p) return;
+  auto* N = static_cast<LPNet*>(p);
+  for (auto& ex : N->it_exec)
+    if (ex) cudaGraphExecDestroy(ex);
+  lp_free_pairs(N);
+  for (void* q : N->allocs) cudaFree(q);
+  delete N;
+}
+
+// ---------------------------------------------------------------- C-ABI ----
+extern "C" {
+
+static int lp_get(wt_handle* h, Ell** E, LPNet** N) {
+  if (!h || !h->ell) return WT_ERR_STATE;
+  *E = static_cast<Ell*>(h->ell);
+  if (!(*E)->lp) return WT_ERR_STATE;
+  *N = static_cast<LPNet*>((*E)->lp);
+  return WT_OK;
+}
+
+int wt_learned_setup(wt_handle* h, unsigned long long seed) {
+  if (!h || !h->ell) return WT_ERR_STATE;
+  return lp_build(*static_cast<Ell*>(h->ell), seed);
+}
+
+int wt_learned_num_params(void) { return kLpParams; }
+
+int wt_learned_params(wt_handle* h, float* get, const float* set) {
+  Ell* E;
+  LPNet* N;
+  if (int rc = lp_get(h, &E, &N)) return rc;
+  CKE(cudaStreamSynchronize(E->s()));
+  if (set) {
+    CKE(cudaMemcpy(N->w, set, 4 * kLpParams, cudaMemcpyHostToDevice));
+    k_lp_round<<<lpg(kLpParams), LP_TPB, 0, E->s()>>>(N->w, N->wr, kLpParams);
+    CKE(cudaStreamSynchronize(E->s()));
+  }
+  if (get) CKE(cudaMemcpy(get, N->w, 4 * kLpParams, cudaMemcpyDeviceToHost));
+  return WT_OK;
+}
+
+int wt_learned_layout(wt_handle* h, int* ns, int* slot, int* tap) {
+  Ell* E;
+  LPNet* N;
+  if (int rc = lp_get(h, &E, &N)) return rc;
+  if (ns) *ns = N->ns;
+  if (slot) CKE(cudaMemcpy(slot, N->slot, 4 * (size_t)N->ns, cudaMemcpyDeviceToHost));
+  if (tap) CKE(cudaMemcpy(tap, N->tap, 4 * (size_t)kTaps * N->ns, cudaMemcpyDeviceToHost));
+  return WT_OK;
+}
+
+int wt_learned_infer(wt_handle* h, const double* r, double* z) {
+  Ell* E;
+  LPNet* N;
+  if (int rc = lp_get(h, &E, &N)) return rc;
+  if (!r || !z) return WT_ERR_ARG;
+  cudaStream_t st = E->s();
+  CKE(cudaMemcpyAsync(N->rc, r, 8 * (size_t)N->ns, cudaMemcpyHostToDevice, st));
+  lp_precondition(*E, *N, nullptr, N->rc, N->ec);
+  CKE(cudaMemcpyAsync(z, N->ec, 8 * (size_t)N->ns, cudaMemcpyDeviceToHost, st));
+  CKE(cudaStreamSynchronize(st));
+  return WT_OK;
+}
+
+int wt_learned_grad(wt_handle* h, const double* r, const double* e, double* loss, float* grad) {
+  Ell* E;
+  LPNet* N;
+  if (int rc = lp_get(h, &E, &N)) return rc;
+  if (!r || !e) return WT_ERR_ARG;
+  cudaStream_t st = E->s();
+  CKE(cudaMemcpyAsync(N->rc, r, 8 * (size_t)N->ns, cudaMemcpyHostToDevice, st));
+  CKE(cudaMemcpyAsync(N->ec, e, 8 * (size_t)N->ns, cudaMemcpyHostToDevice, st));
+  lp_rms(*N, st, nullptr, N->rc, N->rs);
+  lp_forward(*E, *N, nullptr, N->rc, N->rs);
+  lp_backward(*E, *N, N->ec, N->rs, N->losses);
+  if (loss) CKE(cudaMemcpyAsync(loss, N->losses, 8, cudaMemcpyDeviceToHost, st));
+  if (grad) CKE(cudaMemcpyAsync(grad, N->g, 4 * kLpParams, cudaMemcpyDeviceToHost, st));
+  CKE(cudaStreamSynchronize(st));
+  CKE(cudaGetLastError());
+  return WT_OK;
+}
+
+int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep) {
+  Ell* E;
+  LPNet* N;
+  if (int rc = lp_get(h, &E, &N)) return rc;
+  if (!o || !rep || o->n_rhs < 1 || o->cycles < 1 || o->epochs < 1 || !(o->lr > 0)) return WT_ERR_ARG;
+  std::memset(rep, 0, sizeof(*rep));
+  wt_solver_opts mg{};
+  mg.method = WT_SOLVER_MG64;
+  mg.down_iter = o->down_iter > 0 ? o->down_iter : 2;
+  mg.up_iter = o->up_iter > 0 ? o->up_iter : 2;
+  mg.coarse_iter = o->coarse_iter > 0 ? o->coarse_iter : 20;
+  mg.ir_max = 60;
+  CKE(cudaStreamSynchronize(E->s()));
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = lp_generate(*E, *N, *o, mg);
+  auto t1 = std::chrono::steady_clock::now();
+  if (rc == WT_OK) rc = lp_train(*E, *N, *o, *rep);
+  auto t2 = std::chrono::steady_clock::now();
+  rep->ms_generate = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  rep->ms_train = std::chrono::duration<double, std::milli>(t2 - t1).count();
+  lp_free_pairs(N);
+  CKE(cudaGetLastError());
+  return rc;
+}
+
+}  // extern "C"

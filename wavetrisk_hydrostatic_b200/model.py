@@ -336,9 +336,13 @@ class WaveletHierarchy(DeviceGrid):
 def solver_opts(method: str = "fmg", tol: float = 1e-10, **kw):
     """wt_solver_opts with the reference's defaults (src/lin_solve.f90:11-26),
     tolerances set to tol.  method: 'fmg', 'srj' (the reference's solvers),
-    'mixed' (FP32 V-cycles in FP64 refinement) or 'mg64' (same cycle in FP64)."""
+    'mixed' (FP32 V-cycles in FP64 refinement), 'mg64' (same cycle in FP64),
+    'fcg_learned' (flexible CG preconditioned by the learned network, the FP64
+    V-cycle as fallback), 'fcg' (flexible CG without a preconditioner) or
+    'fcg_mg' (flexible CG preconditioned by the FP64 V-cycle); ir_tol/ir_max
+    bound every iterative method after the reference's two."""
     o = N.wt_solver_opts()
-    o.method = {"fmg": 0, "srj": 1, "mixed": 2, "mg64": 3}[method]
+    o.method = {"fmg": 0, "srj": 1, "mixed": 2, "mg64": 3, "fcg_learned": 4, "fcg": 5, "fcg_mg": 6}[method]
     o.coarse_iter, o.max_vcycle = 50, 3
     o.pre_iter, o.down_iter, o.up_iter, o.post_iter = 2, 2, 2, 4
     o.max_srj_iter = 200
@@ -385,6 +389,59 @@ class EllipticSolver(DeviceGrid):
         v = C.c_double()
         N.check("wt_elliptic_l2", N.lib().wt_elliptic_l2(self.h, level, which, C.byref(v)))
         return v.value
+
+    # ---- learned preconditioner (network on level_end) ----
+    def learned_setup(self, seed: int = 1) -> int:
+        """He-initialised network; returns its node count ns."""
+        N.check("wt_learned_setup", N.lib().wt_learned_setup(self.h, int(seed)))
+        return self.learned_layout()[0]
+
+    def learned_layout(self, full: bool = False):
+        ns = C.c_int()
+        N.check("wt_learned_layout", N.lib().wt_learned_layout(self.h, C.byref(ns), None, None))
+        if not full:
+            return ns.value, None, None
+        slot = np.zeros(ns.value, np.int32)
+        tap = np.zeros((7, ns.value), np.int32)
+        N.check("wt_learned_layout", N.lib().wt_learned_layout(
+            self.h, C.byref(ns), slot.ctypes.data_as(C.POINTER(C.c_int)), tap.ctypes.data_as(C.POINTER(C.c_int))))
+        return ns.value, slot, tap
+
+    def learned_params(self, set_to: np.ndarray | None = None) -> np.ndarray:
+        """FP32 master parameters (after setting them to set_to, if given)."""
+        out = np.zeros(N.lib().wt_learned_num_params(), np.float32)
+        src = None
+        if set_to is not None:
+            src = np.ascontiguousarray(set_to, dtype=np.float32)
+            assert src.size == out.size
+            src = src.ctypes.data_as(C.POINTER(C.c_float))
+        N.check("wt_learned_params", N.lib().wt_learned_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), src))
+        return out
+
+    def learned_infer(self, r: np.ndarray) -> np.ndarray:
+        """The preconditioner applied to a compact residual r (ns,)."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        N.check("wt_learned_infer", N.lib().wt_learned_infer(self.h, N.dptr(r), N.dptr(z)))
+        return z
+
+    def learned_grad(self, r: np.ndarray, e: np.ndarray):
+        """(loss, parameter gradient) of the training loss for one pair."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        loss = np.zeros(1)
+        g = np.zeros(N.lib().wt_learned_num_params(), np.float32)
+        N.check("wt_learned_grad", N.lib().wt_learned_grad(self.h, N.dptr(r), N.dptr(e), N.dptr(loss),
+                                                           g.ctypes.data_as(C.POINTER(C.c_float))))
+        return float(loss[0]), g
+
+    def learned_train(self, n_rhs: int = 8, cycles: int = 4, epochs: int = 15, lr: float = 2e-3, seed: int = 1,
+                      down_iter: int = 2, up_iter: int = 2, coarse_iter: int = 20) -> "N.wt_learn_report":
+        """Pairs from the FP64 multigrid, then Adam on the GPU (wt_learned_train)."""
+        o = N.wt_learn_opts(n_rhs, cycles, epochs, lr, seed, down_iter, up_iter, coarse_iter)
+        rep = N.wt_learn_report()
+        N.check("wt_learned_train", N.lib().wt_learned_train(self.h, C.byref(o), C.byref(rep)))
+        return rep
 
     def solve(self, opts) -> "N.wt_solver_report":
         rep = N.wt_solver_report()

@@ -247,7 +247,8 @@ def elliptic_case(lmax, repeats=3):
     out["mixed_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["mixed"]["ms"]
     out["mixed_speedup_vs_fmg"] = out["fmg"]["ms"] / out["mixed"]["ms"]
     out["learned_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["fcg_learned"]["ms"]
-    out["learned_iterations_vs_fcg"] = out["fcg_learned"]["iterations"] / max(1, out["fcg"]["iterations"])
+    out["learned_speedup_vs_vcycle_fcg"] = out["fcg_mg"]["ms"] / out["fcg_learned"]["ms"]
+    out["learned_iterations_vs_vcycle_fcg"] = out["fcg_learned"]["iterations"] / max(1, out["fcg_mg"]["iterations"])
     S.close()
     return out
 

@@ -130,10 +130,11 @@ int wt_profile_rk4(wt_handle* h, double dt, int nsteps, double* ms_per_launch, i
 enum { WT_SOLVER_FMG = 0, WT_SOLVER_SRJ = 1, WT_SOLVER_MIXED_IR = 2, WT_SOLVER_MG64 = 3,
        /* Flexible CG (truncated to one previous direction, area-weighted inner
         * product) on level_end, ir_tol / ir_max as for WT_SOLVER_MIXED_IR:
-        * preconditioned by the learned network with the FP64 V-cycle as the
-        * fallback when it fails to contract (FCG_LEARNED), unpreconditioned
-        * (FCG, the method without the network) or by the FP64 V-cycle alone
-        * (FCG_MG).  No reference counterpart. */
+        * preconditioned by the FP64 V-cycle followed by the learned network's
+        * correction of the residual the V-cycle leaves, with the V-cycle alone
+        * as the fallback when that fails to contract (FCG_LEARNED); by the
+        * FP64 V-cycle alone (FCG_MG, the method without the network); or
+        * unpreconditioned (FCG).  No reference counterpart. */
        WT_SOLVER_FCG_LEARNED = 4, WT_SOLVER_FCG = 5, WT_SOLVER_FCG_MG = 6 };
 
 typedef struct {
@@ -184,16 +185,20 @@ int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report
 
 /* ------------------------------------------------ learned preconditioner ---- */
 /* A hexagonal-stencil convolution network (7 taps: a node and its six
- * neighbours; 2 -> 32 -> 32 -> 1 channels, ReLU) mapping a residual r of
- * level_end, scaled by its rms, and the depth |H| to an approximation of the
- * error e with L e = r.  FP32 master weights, BF16 weights in every forward
- * and backward kernel, FP32 activations and accumulation.  The nodes are the
+ * neighbours; 2 -> 32 -> 32 -> 1 channels) mapping a residual r of level_end,
+ * scaled by its rms, to an approximation of the error e with L e = r, trained
+ * on the residuals a V-cycle leaves and used to correct them
+ * (WT_SOLVER_FCG_LEARNED).  Its inputs are r and r times a depth feature
+ * (|H| / 2750 m - 1); it has no biases and identity activations (a depth-aware
+ * linear operator reaching three neighbours out), and its output is 0 at the
+ * pole slots (slots of [0, n]^2 outside [0, n)^2).  FP32 master weights, BF16 weights
+ * in every forward and backward kernel, FP32 activations and accumulation.  The nodes are the
  * slots of [0, n]^2 of each lozenge that are their own ghost source, numbered
  * lozenge, row j, column i.  Requires wt_elliptic_setup; no reference
  * counterpart (the reference preconditions nothing). */
 typedef struct {
   int n_rhs;       /* seeded N(0,1) right-hand sides, zero mean                   */
-  int cycles;      /* residual/error pairs per right-hand side: before each of the
+  int cycles;      /* residual/error pairs per right-hand side: after each of the
                     * first `cycles` FP64 V-cycles of a solve from 0              */
   int epochs;      /* Adam passes over all pairs, one pair per step              */
   float lr;        /* Adam step, cosine-decayed to lr / 20                       */
@@ -214,18 +219,17 @@ int wt_learned_params(wt_handle* h, float* get, const float* set);
 /* Node count; with slot/tap non-NULL also the node slots (ns) and the taps
  * (7*ns, tap-major, -1 where a tap leaves the node set). */
 int wt_learned_layout(wt_handle* h, int* ns, int* slot, int* tap);
-/* The preconditioner, odd in r: z = rms(r) (net(r/rms(r)) - net(-r/rms(r))) / 2
- * on the ns nodes (host arrays). */
+/* The network's correction z = rms(r) net(r / rms(r)) on the ns nodes (host arrays). */
 int wt_learned_infer(wt_handle* h, const double* r, double* z);
 /* Training loss, the error in the energy norm of the solve,
- *   <d, -L d>_A / |A|,  d = net(r/rms(r)) - e/rms(r),
+ *   <d, -L d>_A / |A|,  d = net(r/rms(r)) - e/rms(r) (net 0 at the poles),
  * (<,>_A weighted by the cell areas 1/hex_inv, |A| their sum) and the gradient
  * 2 A (-L d) / |A| pushed back through the network to the parameters (host
  * arrays; grad: wt_learned_num_params floats).  The solve's u, f are kept. */
 int wt_learned_grad(wt_handle* h, const double* r, const double* e, double* loss, float* grad);
-/* Generates residual/error pairs with the FP64 multigrid (u and f of
- * level_end are kept) and trains the network on them with Adam on the GPU,
- * each pair seen with either sign. */
+/* Generates residual/error pairs with the FP64 multigrid, those after each
+ * V-cycle (u and f of level_end are kept), and trains the network on them
+ * with Adam on the GPU. */
 int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep);
 
 /* ------------------------------------------------------ no allocation ---- */

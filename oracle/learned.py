@@ -8,10 +8,13 @@ so this restates the network the CUDA kernels define:
           source (lozenge, row j, column i order);
   taps  : the node and its neighbours (+1,0), (+1,+1), (0,+1), (-1,0),
           (-1,-1), (0,-1), resolved through the ghost remap; -1 outside;
-  net   : x = [r / rms(r), |H| / 2750 - 1] -> 32 -> 32 -> 1 channels, each a
-          7-tap convolution with BF16-rounded weights, ReLU between layers;
-  use   : z = rms(r) (y(r/rms) - y(-r/rms)) / 2 (odd in r);
-  loss  : <d, -L d>_W / |W| with d = y - e / rms(r), W the cell areas
+  net   : x = [r / rms(r), (r / rms(r)) (|H| / 2750 - 1)] -> 32 -> 32 -> 1
+          channels, each a 7-tap convolution with BF16-rounded weights, no
+          biases, identity activations (linear in r);
+  use   : z = rms(r) y own, own = 0 at the pole slots (slots outside
+          [0, n)^2) and 1 elsewhere; the solver adds it to a V-cycle's
+          correction, z = c + net(r - L c);
+  loss  : <d, -L d>_W / |W| with d = own y - e / rms(r), W the cell areas
           1 / hex_inv (the error in the energy norm of the solve).
 
 Everything is evaluated in float64 from float32-rounded inputs, so the CUDA
@@ -21,8 +24,7 @@ import numpy as np
 TAPS, C, CIN = 7, 32, 2
 DI = (0, 1, 1, 0, -1, -1, 0)
 DJ = (0, 0, 1, 1, 0, -1, -1)
-SHAPES = [("W1", (TAPS, CIN, C)), ("b1", (C,)), ("W2", (TAPS, C, C)), ("b2", (C,)),
-          ("W3", (TAPS, C, 1)), ("b3", (1,))]
+SHAPES = [("W1", (TAPS, CIN, C)), ("W2", (TAPS, C, C)), ("W3", (TAPS, C, 1))]
 NPARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
 
 
@@ -75,8 +77,8 @@ def _gather(a, tap_t):
     return g
 
 
-def _conv(a, W, b, tap):
-    out = np.repeat(b[:, None], a.shape[1], axis=1)
+def _conv(a, W, tap):
+    out = np.zeros((W.shape[2], a.shape[1]))
     for t in range(TAPS):
         out += W[t].T @ _gather(a, tap[t])
     return out
@@ -84,24 +86,23 @@ def _conv(a, W, b, tap):
 
 def forward(theta, r, depth, tap, round_weights=True):
     """Activations of the network for compact residual r and depth |H| (ns,).
-    Returns a dict with x, z1, h1, z2, h2, y (channel-major), rs and the
-    parameters P used."""
+    Returns a dict with x, h1, h2, y (channel-major), rs and the parameters P
+    used."""
     P = unpack(bf16_round(np.asarray(theta, np.float32)) if round_weights else theta)
     r = np.asarray(r, np.float64)
     rs = np.sqrt(np.mean(r * r))
     if not rs > 0:
         rs = 1.0
-    x = np.stack([(r / rs).astype(np.float32), (np.abs(depth) / 2750.0 - 1.0).astype(np.float32)]).astype(np.float64)
-    z1 = _conv(x, P["W1"], P["b1"], tap)
-    h1 = np.maximum(z1, 0.0)
-    z2 = _conv(h1, P["W2"], P["b2"], tap)
-    h2 = np.maximum(z2, 0.0)
-    y = _conv(h2, P["W3"], P["b3"], tap)[0]
-    return {"x": x, "z1": z1, "h1": h1, "z2": z2, "h2": h2, "y": y, "rs": rs, "P": P}
+    v = (r / rs).astype(np.float32)
+    x = np.stack([v, v * (np.abs(depth) / 2750.0 - 1.0).astype(np.float32)]).astype(np.float64)
+    h1 = _conv(x, P["W1"], tap)
+    h2 = _conv(h1, P["W2"], tap)
+    y = _conv(h2, P["W3"], tap)[0]
+    return {"x": x, "h1": h1, "h2": h2, "y": y, "rs": rs, "P": P}
 
 
 def _conv_back(a, W, dout, tap):
-    """Gradients of one layer: (dW, db, din) for input a and output gradient dout."""
+    """Gradients of one layer: (dW, din) for input a and output gradient dout."""
     dW = np.zeros_like(W)
     din = np.zeros_like(a)
     for t in range(TAPS):
@@ -110,7 +111,7 @@ def _conv_back(a, W, dout, tap):
         contrib = W[t] @ dout
         ok = tap[t] >= 0
         np.add.at(din.T, tap[t][ok], contrib[:, ok].T)
-    return dW, dout.sum(axis=1), din
+    return dW, din
 
 
 def backward(A, dy, tap):
@@ -118,12 +119,10 @@ def backward(A, dy, tap):
     straight through the BF16 rounding (the gradient of the rounded weights)."""
     dy = np.asarray(dy, np.float64)[None, :]
     P = A["P"]
-    dW3, db3, dh2 = _conv_back(A["h2"], P["W3"], dy, tap)
-    dz2 = dh2 * (A["z2"] > 0)
-    dW2, db2, dh1 = _conv_back(A["h1"], P["W2"], dz2, tap)
-    dz1 = dh1 * (A["z1"] > 0)
-    dW1, db1, _ = _conv_back(A["x"], P["W1"], dz1, tap)
-    return pack({"W1": dW1, "b1": db1, "W2": dW2, "b2": db2, "W3": dW3, "b3": db3})
+    dW3, dh2 = _conv_back(A["h2"], P["W3"], dy, tap)
+    dW2, dh1 = _conv_back(A["h1"], P["W2"], dh2, tap)
+    dW1, _ = _conv_back(A["x"], P["W1"], dh1, tap)
+    return pack({"W1": dW1, "W2": dW2, "W3": dW3})
 
 
 def loss_and_grad(theta, r, e, depth, tap, round_weights=True):
@@ -134,35 +133,34 @@ def loss_and_grad(theta, r, e, depth, tap, round_weights=True):
     return float(np.mean(d * d)), backward(A, 2.0 * d / d.size, tap)
 
 
-def energy_loss_and_grad(theta, r, e, depth, tap, slot, hinv, NN, apply_L):
+def energy_loss_and_grad(theta, r, e, depth, tap, slot, hinv, NN, apply_L, own):
     """The training loss of the CUDA network: the error in the energy norm,
-      loss = <d, -L d>_W / |W|,  d = y - e/rs,  W = 1/hex_inv on the nodes,
+      loss = <d, -L d>_W / |W|,  d = own y - e/rs,  W = 1/hex_inv on the nodes,
     with apply_L(q) = L q for a level array q (ghosts not filled), and the
     gradient the CUDA kernels use, dy = 2 W (-L d) / |W| (exact when L is
     self-adjoint in <,>_W; the discrete operator is, to a few tenths of a
     percent)."""
     A = forward(theta, r, depth, tap)
     d = np.zeros(NN)
-    d[slot] = A["y"] - np.asarray(e, np.float64) / A["rs"]
+    d[slot] = own * A["y"] - np.asarray(e, np.float64) / A["rs"]
     w = 1.0 / np.asarray(hinv, np.float64)[slot]
     inv_area = 1.0 / w.sum()
     a = -apply_L(d)[slot] * w
     loss = float((d[slot] * a).sum() * inv_area)
-    return loss, backward(A, 2.0 * a * inv_area, tap)
+    return loss, backward(A, own * 2.0 * a * inv_area, tap)
 
 
-def infer(theta, r, depth, tap):
-    """Preconditioned vector, odd in r: z = rs (y(r/rs) - y(-r/rs)) / 2."""
+def infer(theta, r, depth, tap, own):
+    """The network's correction z = rs * y * own."""
     A = forward(theta, r, depth, tap)
-    B = forward(theta, -np.asarray(r, np.float64), depth, tap)
-    return 0.5 * A["rs"] * (A["y"] - B["y"])
+    return A["rs"] * A["y"] * own
 
 
 def init_params(seed):
-    """He-initialised parameters (same scales as the CUDA set-up; not the same
-    random stream)."""
+    """Random parameters with the CUDA set-up's scales (variance-preserving
+    linear layers, a small last layer; not the same random stream)."""
     rng = np.random.default_rng(seed)
-    d = {"W1": rng.standard_normal((TAPS, CIN, C)) * np.sqrt(2.0 / (TAPS * CIN)), "b1": np.zeros(C),
-         "W2": rng.standard_normal((TAPS, C, C)) * np.sqrt(2.0 / (TAPS * C)), "b2": np.zeros(C),
-         "W3": rng.standard_normal((TAPS, C, 1)) * 0.1 * np.sqrt(1.0 / (TAPS * C)), "b3": np.zeros(1)}
+    d = {"W1": rng.standard_normal((TAPS, CIN, C)) * np.sqrt(1.0 / (TAPS * CIN)),
+         "W2": rng.standard_normal((TAPS, C, C)) * np.sqrt(1.0 / (TAPS * C)),
+         "W3": rng.standard_normal((TAPS, C, 1)) * 0.1 * np.sqrt(1.0 / (TAPS * C))}
     return pack(d).astype(np.float32)

@@ -3,9 +3,10 @@ its node layout, the preconditioner and the gradient of the training loss
 against the CPU oracle (float64 from the same BF16-rounded weights; FP32
 accumulation on the GPU, so 2e-5 relative on the output and 1e-4 relative to
 the largest entry of each parameter block on the gradient), training on
-residual/error pairs from the FP64 multigrid, and flexible CG with the trained
-network: it reaches the true FP64 residual 1e-10 in fewer iterations than
-flexible CG without it, and the V-cycle takes over when the network fails."""
+residual/error pairs from the FP64 multigrid, and flexible CG preconditioned by a V-cycle
+plus the trained network's correction: it reaches the true FP64 residual
+1e-10 in fewer iterations than flexible CG with the V-cycle alone, and the
+V-cycle alone takes over when the network fails to contract."""
 import numpy as np
 import pytest
 
@@ -26,13 +27,6 @@ def make(lmin, lmax, seed=1):
     return levels, topos, EllipticSolver(levels, topos)
 
 
-def with_biases(theta, b):
-    d = LO.unpack(theta)
-    for k in ("b1", "b2", "b3"):
-        d[k] = np.full(d[k].shape, b)
-    return LO.pack(d).astype(np.float32)
-
-
 @pytest.fixture(scope="module")
 def small():
     levels, topos, S = make(4, 5)
@@ -40,6 +34,11 @@ def small():
     slot, tap = LO.layout(levels[-1])
     yield S, levels, topos, slot, tap
     S.close()
+
+
+def small_own(small):
+    _, levels, _, slot, _ = small
+    return levels[-1].owned[slot].astype(np.float64)
 
 
 def test_layout_matches_oracle(small):
@@ -51,19 +50,19 @@ def test_layout_matches_oracle(small):
 
 def test_infer_matches_oracle(small):
     S, _, topos, slot, tap = small
-    theta = with_biases(LO.init_params(11), 0.05)
+    theta = LO.init_params(11)
     S.learned_params(theta)
     assert np.array_equal(S.learned_params(), theta)
     rng = np.random.default_rng(2)
     r = rng.standard_normal(slot.size) * 3e-4
     z = S.learned_infer(r)
-    ref = LO.infer(theta, r, topos[-1][slot], tap)
+    ref = LO.infer(theta, r, topos[-1][slot], tap, small_own(small))
     assert np.abs(z - ref).max() <= 2e-5 * np.abs(ref).max()
 
 
 def test_gradient_matches_oracle(small):
     S, levels, topos, slot, tap = small
-    theta = with_biases(LO.init_params(12), 0.02)
+    theta = LO.init_params(12)
     S.learned_params(theta)
     rng = np.random.default_rng(4)
     r, e = rng.standard_normal(slot.size), rng.standard_normal(slot.size) * 0.3
@@ -78,7 +77,8 @@ def test_gradient_matches_oracle(small):
         full[off[-2]:] = x
         return H.apply(lv.level, full)[off[-2]:]
 
-    loss_o, g_o = LO.energy_loss_and_grad(theta, r, e, topos[-1][slot], tap, slot, lv.hex_inv, lv.NN, apply_L)
+    loss_o, g_o = LO.energy_loss_and_grad(theta, r, e, topos[-1][slot], tap, slot, lv.hex_inv, lv.NN, apply_L,
+                                          small_own(small))
     assert abs(loss - loss_o) <= 1e-5 * loss_o
     o = 0
     for name, shp in LO.SHAPES:                      # every parameter block on its own scale
@@ -96,7 +96,8 @@ def trained():
     off = S.offsets
     f = np.zeros(off[-1])
     f[off[-2]:off[-1]] = elliptic_rhs(levels[-1], seed=2)
-    yield S, rep, f
+    slot, _ = LO.layout(levels[-1])
+    yield S, rep, f, off[-2] + slot                  # the finest level's nodes in the multi-level arrays
     S.close()
 
 
@@ -108,41 +109,42 @@ def run(S, f, method, **kw):
 
 
 def test_training_reduces_loss(trained):
-    _, rep, _ = trained
+    _, rep, _, _ = trained
     assert rep.pairs == 32 and rep.steps == 32 * 15
     assert rep.loss_last_epoch < 0.5 * rep.loss_first_epoch
 
 
 def test_learned_fcg_beats_fcg_without_network(trained):
-    S, _, f = trained
+    """The method without the network is FCG preconditioned by the V-cycle
+    alone; the trained network's correction must save iterations over it."""
+    S, _, f, nodes = trained
     r_net, u_net = run(S, f, "fcg_learned")
-    r_cg, _ = run(S, f, "fcg")
+    r_v, _ = run(S, f, "fcg_mg")
     r_mg, u_mg = run(S, f, "mg64")
-    assert r_net.status == 0 and r_cg.status == 0 and r_mg.status == 0
-    assert r_net.true_rel_residual <= 1e-10 and r_cg.true_rel_residual <= 1e-10
+    assert r_net.status == 0 and r_v.status == 0 and r_mg.status == 0
+    assert r_net.true_rel_residual <= 1e-10 and r_v.true_rel_residual <= 1e-10
     assert r_net.precond_fallback == 0
     q = len(S.offsets) - 2
-    assert r_net.iterations[q] <= 0.7 * r_cg.iterations[q], (r_net.iterations[q], r_cg.iterations[q])
-    sl = slice(S.offsets[-2], S.offsets[-1])
-    assert np.abs(u_net[sl] - u_mg[sl]).max() <= 1e-8 * np.abs(u_mg[sl]).max()
+    assert r_net.iterations[q] < r_v.iterations[q], (r_net.iterations[q], r_v.iterations[q])
+    assert np.abs(u_net[nodes] - u_mg[nodes]).max() <= 1e-8 * np.abs(u_mg[nodes]).max()
 
 
 def test_fallback_when_network_fails(trained):
-    S, _, f = trained
+    S, _, f, _ = trained
     keep = S.learned_params()
-    S.learned_params(np.zeros_like(keep))            # z = 0: the first step breaks down
+    bad = np.random.default_rng(0).standard_normal(keep.size).astype(np.float32)
+    S.learned_params(bad)                            # an untrained network adding noise to the V-cycle
     try:
         rep, _ = run(S, f, "fcg_learned")
     finally:
         S.learned_params(keep)
     assert rep.status == 0 and rep.true_rel_residual <= 1e-10
-    assert rep.precond_fallback == 1
+    assert rep.precond_fallback > 0
 
 
 def test_fcg_with_vcycle_matches_mg(trained):
-    S, _, f = trained
+    S, _, f, nodes = trained
     rep, u = run(S, f, "fcg_mg")
     _, u_mg = run(S, f, "mg64")
     assert rep.status == 0 and rep.true_rel_residual <= 1e-10
-    sl = slice(S.offsets[-2], S.offsets[-1])
-    assert np.abs(u[sl] - u_mg[sl]).max() <= 1e-8 * np.abs(u_mg[sl]).max()
+    assert np.abs(u[nodes] - u_mg[nodes]).max() <= 1e-8 * np.abs(u_mg[nodes]).max()

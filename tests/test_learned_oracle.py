@@ -38,10 +38,7 @@ def test_oracle_gradient_finite_differences():
     depth = bathymetry(lv, seed=3)[slot]
     rng = np.random.default_rng(5)
     r, e = rng.standard_normal(slot.size), rng.standard_normal(slot.size)
-    d = LO.unpack(LO.init_params(7).astype(np.float64))
-    for k in ("b1", "b2", "b3"):                     # nonzero biases
-        d[k] = 0.05 * rng.standard_normal(d[k].shape)
-    theta = LO.pack(d)
+    theta = LO.init_params(7).astype(np.float64)
     loss, grad = LO.loss_and_grad(theta, r, e, depth, tap, round_weights=False)
     idx = rng.choice(LO.NPARAMS, 24, replace=False)
     h = 1e-6
@@ -54,13 +51,18 @@ def test_oracle_gradient_finite_differences():
     assert loss > 0
 
 
-def test_infer_is_odd_and_scale_equivariant():
+def test_infer_is_linear_in_the_residual():
     g = Grid(3, 3, radius=6371e3)
     lv = g.level(3)
     slot, tap = LO.layout(lv)
     depth = bathymetry(lv, seed=3)[slot]
     theta = LO.init_params(9)
+    own = lv.owned[slot].astype(np.float64)
     r = np.random.default_rng(1).standard_normal(slot.size)
-    z = LO.infer(theta, r, depth, tap)
-    assert np.allclose(LO.infer(theta, -r, depth, tap), -z, rtol=0, atol=1e-12 * np.abs(z).max())
-    assert np.allclose(LO.infer(theta, 4.0 * r, depth, tap), 4.0 * z, rtol=1e-12, atol=0)
+    z = LO.infer(theta, r, depth, tap, own)
+    assert np.allclose(LO.infer(theta, -r, depth, tap, own), -z, rtol=0, atol=1e-12 * np.abs(z).max())
+    assert np.allclose(LO.infer(theta, 4.0 * r, depth, tap, own), 4.0 * z, rtol=1e-12, atol=0)
+    r2 = np.random.default_rng(2).standard_normal(slot.size)
+    z12 = LO.infer(theta, r + r2, depth, tap, own)     # additive up to the FP32 rounding of the inputs
+    assert np.abs(z12 - z - LO.infer(theta, r2, depth, tap, own)).max() <= 1e-5 * np.abs(z12).max()
+    assert (z[own == 0] == 0).all() and own.sum() == 10 * lv.n ** 2

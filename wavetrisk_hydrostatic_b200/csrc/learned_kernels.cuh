@@ -1,16 +1,22 @@
 // Learned preconditioner of the free-surface solve: a hexagonal-stencil
-// convolution network over the nodes of one level, 2 -> 32 -> 32 -> 1 channels,
-// ReLU between layers.  Each layer sums over seven taps (the node and its six
-// neighbours in lozenge directions (+1,0), (+1,+1), (0,+1), (-1,0), (-1,-1),
-// (0,-1), read through the ghost remap) and its input channels:
-//   out[co](s) = b[co] + sum_t sum_ci W[t][ci][co] * in[ci](tap_t(s)).
-// The weights are FP32 master copies rounded to BF16 for every use (BF16
-// weights, FP32 activations and accumulation).  Nodes are numbered compactly:
-// the slots of [0, n]^2 of every lozenge that are their own ghost source; a
-// tap that leaves that set reads 0.  Activations are channel-major, in[c * ns + s].
+// convolution network over the nodes of one level, 2 -> 32 -> 32 -> 1 channels.
+// Each layer sums over seven taps (the node and its six neighbours in lozenge
+// directions (+1,0), (+1,+1), (0,+1), (-1,0), (-1,-1), (0,-1), read through the
+// ghost remap) and its input channels:
+//   out[co](s) = sum_t sum_ci W[t][ci][co] * in[ci](tap_t(s)).
+// The network is linear in the residual (inputs r/rs and (r/rs) * depth
+// feature, no biases, identity activations): a fixed, depth-aware linear
+// operator of three hops' reach, which generalises from the training
+// residuals to any residual.  It corrects what a multigrid V-cycle leaves: the
+// preconditioner is z = c + net(r - L c) with c the V-cycle's correction, and
+// the network's output is masked to 0 at the pole slots (slots of [0, n]^2
+// outside [0, n)^2, whose lozenge-frame taps are degenerate).  The weights are FP32 master copies rounded to BF16 for every use
+// (BF16 weights, FP32 activations and accumulation).  Nodes are numbered
+// compactly: the slots of [0, n]^2 of every lozenge that are their own ghost
+// source; a tap that leaves that set reads 0.  Activations are channel-major,
+// in[c * ns + s].
 //
-// Parameter layout (kLpParams floats): W1[7][2][32], b1[32], W2[7][32][32],
-// b2[32], W3[7][32][1], b3[1].
+// Parameter layout (kLpParams floats): W1[7][2][32], W2[7][32][32], W3[7][32][1].
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -20,8 +26,7 @@
 namespace wtl {
 
 constexpr int kTaps = 7, kC = 32, kIn = 2;
-constexpr int kW1 = 0, kB1 = kW1 + kTaps * kIn * kC, kW2 = kB1 + kC, kB2 = kW2 + kTaps * kC * kC, kW3 = kB2 + kC,
-              kB3 = kW3 + kTaps * kC, kLpParams = kB3 + 1;
+constexpr int kW1 = 0, kW2 = kW1 + kTaps * kIn * kC, kW3 = kW2 + kTaps * kC * kC, kLpParams = kW3 + kTaps * kC;
 constexpr int kDepthRef = 2750;  // depth feature |H| / 2750 m - 1
 
 __device__ __forceinline__ float bf16r(float w) { return __bfloat162float(__float2bfloat16_rn(w)); }
@@ -64,8 +69,7 @@ __global__ void __launch_bounds__(NT) k_lp_dot(int ns, const int* __restrict__ s
 }
 
 // out = scale * (sum of nb partials, fixed order); mode 1: the square root of
-// that, replaced by 1 where it is 0 or not finite (the residual scale), and
-// its negative in out[1].
+// that, replaced by 1 where it is 0 or not finite (the residual scale).
 __global__ void k_lp_sum(const double* __restrict__ partial, int nb, double* __restrict__ out, int mode,
                          double scale) {
   __shared__ double sh[256];
@@ -82,40 +86,38 @@ __global__ void k_lp_sum(const double* __restrict__ partial, int nb, double* __r
     if (mode == 1) {
       r = sqrt(r);
       if (!(r > 0.0) || !isfinite(r)) r = 1.0;
-      out[1] = -r;
     }
     out[0] = r;
   }
 }
 
-// Network input of every node: the residual scaled by 1 / rscale and the depth
-// feature.  r read at slot[s] (nullptr: compact), topo at tslot[s].
+// Network input of every node: the residual scaled by 1 / rscale, and the same
+// times the depth feature |H| / 2750 m - 1.  r read at slot[s] (nullptr:
+// compact), topo at tslot[s].
 __global__ void k_lp_input(int ns, const int* __restrict__ slot, const int* __restrict__ tslot,
                            const double* __restrict__ r, const double* __restrict__ rscale,
                            const double* __restrict__ topo, float* __restrict__ x) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   const double inv = 1.0 / *rscale;
-  x[s] = (float)(r[slot ? slot[s] : s] * inv);
-  x[ns + s] = (float)(fabs(topo[tslot[s]]) / (double)kDepthRef - 1.0);
+  const float v = (float)(r[slot ? slot[s] : s] * inv);
+  x[s] = v;
+  x[ns + s] = v * (float)(fabs(topo[tslot[s]]) / (double)kDepthRef - 1.0);
 }
 
 // One convolution layer, one thread per node computing all COUT outputs from
 // the 7 x CIN tap inputs; BF16-valued weights staged in shared memory.
-template <int CIN, int COUT, bool RELU>
+template <int CIN, int COUT>
 __global__ void __launch_bounds__(128) k_lp_conv(int ns, const int* __restrict__ tap, const float* __restrict__ in,
-                                                 const float* __restrict__ W, const float* __restrict__ b,
-                                                 float* __restrict__ out) {
+                                                 const float* __restrict__ W, float* __restrict__ out) {
   __shared__ float sw[kTaps * CIN * COUT];
-  __shared__ float sb[COUT];
   for (int q = threadIdx.x; q < kTaps * CIN * COUT; q += blockDim.x) sw[q] = W[q];
-  for (int q = threadIdx.x; q < COUT; q += blockDim.x) sb[q] = b[q];
   __syncthreads();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   float acc[COUT];
 #pragma unroll
-  for (int co = 0; co < COUT; ++co) acc[co] = sb[co];
+  for (int co = 0; co < COUT; ++co) acc[co] = 0.0f;
   for (int t = 0; t < kTaps; ++t) {
     const int u = tap[t * ns + s];
     if (u < 0) continue;
@@ -127,64 +129,64 @@ __global__ void __launch_bounds__(128) k_lp_conv(int ns, const int* __restrict__
     }
   }
 #pragma unroll
-  for (int co = 0; co < COUT; ++co) out[co * ns + s] = RELU ? fmaxf(acc[co], 0.0f) : acc[co];
+  for (int co = 0; co < COUT; ++co) out[co * ns + s] = acc[co];
 }
 
-// Preconditioned vector, odd in r: z = rscale * (y(r/rs) - y(-r/rs)) / 2,
-// accumulated over the two passes (rscale = rs, then -rs; acc = 0, then 1)
-// into slot[s] of a level array (nullptr: compact).
+// z = base + own * rscale * y into slot[s] of a level array (nullptr:
+// compact; base == nullptr: 0), own = 1 on the owned nodes, 0 at the poles.
 __global__ void k_lp_output(int ns, const int* __restrict__ slot, const float* __restrict__ y,
-                            const double* __restrict__ rscale, double* __restrict__ z, int acc) {
+                            const double* __restrict__ rscale, const float* __restrict__ own,
+                            const double* __restrict__ base, double* __restrict__ z) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   const int id = slot ? slot[s] : s;
-  const double v = 0.5 * (double)y[s] * *rscale;
-  z[id] = acc ? z[id] + v : v;
+  z[id] = (base ? base[id] : 0.0) + (double)(own[s] * y[s]) * *rscale;
 }
 
-// b = -a (the residual scales of the sign-flipped training pairs).
-__global__ void k_lp_negate(int n, const double* __restrict__ a, double* __restrict__ b) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) b[i] = -a[i];
+// out = x - y on the node slots (the residual a V-cycle correction leaves).
+__global__ void k_lp_sub(int ns, const int* __restrict__ slot, const double* __restrict__ x,
+                         const double* __restrict__ y, double* __restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < ns) out[slot[s]] = x[slot[s]] - y[slot[s]];
 }
 
 // Training loss: the error of the network in the energy norm of the solve,
-//   loss = <d, -L d>_W / |W|,  d = y - e / rscale,  W = 1 / hex_inv (cell area),
+//   loss = <d, -L d>_W / |W|,  d = own y - e / rscale,  W = 1 / hex_inv (cell area),
 // the norm flexible CG minimises (-L is positive definite in <,>_W).
 // k_lp_err writes d on the node slots of a level array; after Ld = L d,
 // k_lp_aloss forms the loss partials and dy = 2 W (-Ld) / |W|.
 __global__ void k_lp_err(int ns, const int* __restrict__ slot, const float* __restrict__ y,
-                         const double* __restrict__ e, const double* __restrict__ rscale, double* __restrict__ d) {
+                         const float* __restrict__ own, const double* __restrict__ e,
+                         const double* __restrict__ rscale, double* __restrict__ d) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < ns) d[slot[s]] = (double)y[s] - e[s] / *rscale;
+  if (s < ns) d[slot[s]] = (double)(own[s] * y[s]) - e[s] / *rscale;
 }
 template <int NT>
 __global__ void __launch_bounds__(NT) k_lp_aloss(int ns, const int* __restrict__ slot, const double* __restrict__ d,
                                                  const double* __restrict__ Ld, const double* __restrict__ hinv,
-                                                 double inv_area, float* __restrict__ dy,
-                                                 double* __restrict__ partial) {
+                                                 const float* __restrict__ own, double inv_area,
+                                                 float* __restrict__ dy, double* __restrict__ partial) {
   const int s = blockIdx.x * NT + threadIdx.x;
   double v = 0.0;
   if (s < ns) {
     const int id = slot[s];
     const double a = -Ld[id] / hinv[id];
-    dy[s] = (float)(2.0 * a * inv_area);
+    dy[s] = own[s] * (float)(2.0 * a * inv_area);
     v = d[id] * a;
   }
   block_partial<NT>(v, partial);
 }
 
-// Weight and bias gradient of one layer: dW[t][ci][co] = sum_s dz[co](s) *
-// in[ci](tap_t(s)), db[co] = sum_s dz[co](s).  A block stages a chunk of
-// kChunk nodes (their tap inputs A[s][t*CIN+ci], a 1 for the bias, and dz) in
-// shared memory; each thread owns fixed entries of the gradient and sums them
-// over the block's chunks, then adds them once to the global gradient.
+// Weight gradient of one layer: dW[t][ci][co] = sum_s dz[co](s) *
+// in[ci](tap_t(s)).  A block stages a chunk of kChunk nodes (their tap inputs
+// A[s][t*CIN+ci] and dz) in shared memory; each thread owns fixed entries of
+// the gradient and sums them over the block's chunks, then adds them once to
+// the global gradient.
 constexpr int kChunk = 32;
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(256) k_lp_wgrad(int ns, const int* __restrict__ tap, const float* __restrict__ in,
-                                                  const float* __restrict__ dz, float* __restrict__ dW,
-                                                  float* __restrict__ db) {
-  constexpr int K = kTaps * CIN + 1;         // rows of A (last: bias)
+                                                  const float* __restrict__ dz, float* __restrict__ dW) {
+  constexpr int K = kTaps * CIN;             // rows of A
   constexpr int NE = K * COUT;               // gradient entries
   constexpr int PER = (NE + 255) / 256;      // entries per thread
   __shared__ float A[kChunk][K];
@@ -200,12 +202,8 @@ __global__ void __launch_bounds__(256) k_lp_wgrad(int ns, const int* __restrict_
       const int nl = q / K, k = q % K, s = s0 + nl;
       float v = 0.0f;
       if (s < ns) {
-        if (k == K - 1) {
-          v = 1.0f;
-        } else {
-          const int t = k / CIN, ci = k % CIN, u = tap[t * ns + s];
-          v = u >= 0 ? in[ci * ns + u] : 0.0f;
-        }
+        const int t = k / CIN, ci = k % CIN, u = tap[t * ns + s];
+        v = u >= 0 ? in[ci * ns + u] : 0.0f;
       }
       A[nl][k] = v;
     }
@@ -230,15 +228,13 @@ __global__ void __launch_bounds__(256) k_lp_wgrad(int ns, const int* __restrict_
   for (int r = 0; r < PER; ++r) {
     const int e = threadIdx.x + 256 * r;
     if (e < NE) {
-      const int k = e / COUT, co = e % COUT;
-      atomicAdd(k == K - 1 ? &db[co] : &dW[k * COUT + co], acc[r]);
+      atomicAdd(&dW[e], acc[r]);
     }
   }
 }
 
 // Input gradient of one layer: din[ci](tap_t(s)) += sum_co W[t][ci][co] *
-// dz[co](s), scattered to the tap's node; then masked by the producing ReLU
-// in k_lp_relu_back.
+// dz[co](s), scattered to the tap's node.
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(128) k_lp_igrad(int ns, const int* __restrict__ tap, const float* __restrict__ W,
                                                   const float* __restrict__ dz, float* __restrict__ din) {
@@ -261,12 +257,6 @@ __global__ void __launch_bounds__(128) k_lp_igrad(int ns, const int* __restrict_
       atomicAdd(&din[ci * ns + u], a);
     }
   }
-}
-
-// ReLU backward in place: d = 0 where the activation h was clipped.
-__global__ void k_lp_relu_back(int n, const float* __restrict__ h, float* __restrict__ d) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && !(h[i] > 0.0f)) d[i] = 0.0f;
 }
 
 // Adam step on the FP32 master parameters (bias-corrected; step t >= 1).

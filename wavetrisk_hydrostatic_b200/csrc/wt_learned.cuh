@@ -1,7 +1,7 @@
 // Learned preconditioner of the free-surface solve (network in
 // learned_kernels.cuh): node layout, training-pair generation with the FP64
-// multigrid, Adam training, and flexible CG preconditioned by the network
-// with the FP64 V-cycle as fallback.  Included by wt_elliptic.cu only, after
+// multigrid, Adam training, and flexible CG preconditioned by an FP64 V-cycle
+// plus the network's correction, with the V-cycle alone as the fallback.  Included by wt_elliptic.cu only, after
 // wt_elliptic_mixed.cuh.
 #pragma once
 
@@ -22,6 +22,7 @@ struct LPNet {
   int64_t NN = 0;
   int* slot = nullptr;  // ns node slots of the level
   int* tap = nullptr;   // 7*ns compact tap indices
+  float* own = nullptr; // ns: 1 on owned nodes, 0 at the pole slots
   float *w = nullptr, *wr = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
   float *x = nullptr, *h1 = nullptr, *h2 = nullptr, *y = nullptr, *dy = nullptr, *dh1 = nullptr, *dh2 = nullptr;
   double *rs = nullptr, *fcg = nullptr, *partial = nullptr, *losses = nullptr;
@@ -29,7 +30,9 @@ struct LPNet {
   double *pr = nullptr, *pe = nullptr, *pscale = nullptr;  // training pairs
   int npairs = 0;
   double *r = nullptr, *z = nullptr, *lz = nullptr, *p = nullptr, *lp = nullptr, *ustar = nullptr,
-         *usave = nullptr, *fsave = nullptr;  // level arrays
+         *usave = nullptr, *fsave = nullptr, *c = nullptr, *r2 = nullptr;
+  // level arrays (usave: also u at the start of a learned solve; c, r2: the
+  // V-cycle's correction and the residual it leaves)
   int adam_t = 0;
   double inv_area = 1.0;  // 1 / sum of the node areas 1 / hex_inv
   cudaGraphExec_t it_exec[3] = {nullptr, nullptr, nullptr};
@@ -74,8 +77,9 @@ int lp_init_params(LPNet& N, uint64_t seed) {
   auto fill = [&](int off, int cnt, double sd) {
     for (int k = 0; k < cnt; ++k) w[off + k] = (float)(sd * rn());
   };
-  fill(kW1, kTaps * kIn * kC, std::sqrt(2.0 / (kTaps * kIn)));
-  fill(kW2, kTaps * kC * kC, std::sqrt(2.0 / (kTaps * kC)));
+  // variance-preserving scales for linear layers; a small last layer
+  fill(kW1, kTaps * kIn * kC, std::sqrt(1.0 / (kTaps * kIn)));
+  fill(kW2, kTaps * kC * kC, std::sqrt(1.0 / (kTaps * kC)));
   fill(kW3, kTaps * kC, 0.1 * std::sqrt(1.0 / (kTaps * kC)));
   cudaMemcpy(N.w, w.data(), 4 * kLpParams, cudaMemcpyHostToDevice);
   cudaMemset(N.m, 0, 4 * kLpParams);
@@ -115,8 +119,10 @@ int lp_build(Ell& E, uint64_t seed) {
   }
   static const int di[kTaps] = {0, 1, 1, 0, -1, -1, 0}, dj[kTaps] = {0, 0, 1, 1, 0, -1, -1};
   std::vector<int> tap((size_t)kTaps * ns);
+  std::vector<float> own(ns);
   for (int s = 0; s < ns; ++s) {
     const int k = slot[s], d = k / (P * P), r = k % (P * P), i = r % P - 2, j = r / P - 2;
+    own[s] = (i < n && j < n) ? 1.f : 0.f;
     for (int t = 0; t < kTaps; ++t) {
       const int kn = (d * P + j + dj[t] + 2) * P + i + di[t] + 2;
       tap[(size_t)t * ns + s] = cid[nsrc[kn]];
@@ -129,6 +135,7 @@ int lp_build(Ell& E, uint64_t seed) {
   };
   al(&N->slot, ns);
   al(&N->tap, (int64_t)kTaps * ns);
+  al(&N->own, ns);
   for (float** p : {&N->w, &N->wr, &N->g, &N->m, &N->v}) al(p, kLpParams);
   al(&N->x, (int64_t)kIn * ns);
   al(&N->h1, (int64_t)kC * ns);
@@ -137,16 +144,18 @@ int lp_build(Ell& E, uint64_t seed) {
   al(&N->dh2, (int64_t)kC * ns);
   al(&N->y, ns);
   al(&N->dy, ns);
-  al(&N->rs, 2);
+  al(&N->rs, 1);
   al(&N->fcg, FCG_N);
   al(&N->partial, N->nbd());
   al(&N->losses, 1);
   al(&N->rc, ns);
   al(&N->ec, ns);
-  for (double** p : {&N->r, &N->z, &N->lz, &N->p, &N->lp, &N->ustar, &N->usave, &N->fsave}) al(p, D.NN);
+  for (double** p : {&N->r, &N->z, &N->lz, &N->p, &N->lp, &N->ustar, &N->usave, &N->fsave, &N->c, &N->r2})
+    al(p, D.NN);
   if (rc == WT_OK) {
     cudaMemcpy(N->slot, slot.data(), 4 * (size_t)ns, cudaMemcpyHostToDevice);
     cudaMemcpy(N->tap, tap.data(), 4 * tap.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(N->own, own.data(), 4 * (size_t)ns, cudaMemcpyHostToDevice);
     rc = lp_init_params(*N, seed);
   }
   if (rc != WT_OK) {
@@ -158,7 +167,7 @@ int lp_build(Ell& E, uint64_t seed) {
   return WT_OK;
 }
 
-// rs = rms of r over the nodes, -rs in rs[1] (r read at slot[s]; nullptr: compact).
+// rs = rms of r over the nodes (r read at slot[s]; nullptr: compact).
 void lp_rms(LPNet& N, cudaStream_t st, const int* slot, const double* r, double* rs) {
   k_lp_dot<LP_DOT><<<N.nbd(), LP_DOT, 0, st>>>(N.ns, slot, r, r, nullptr, N.partial);
   k_lp_sum<<<1, 256, 0, st>>>(N.partial, N.nbd(), rs, 1, 1.0 / N.ns);
@@ -169,20 +178,19 @@ void lp_forward(Ell& E, LPNet& N, const int* slot, const double* r, const double
   cudaStream_t st = E.s();
   const int ns = N.ns;
   k_lp_input<<<lpg(ns), LP_TPB, 0, st>>>(ns, slot, N.slot, r, rs, E.h->at(N.l).topo, N.x);
-  k_lp_conv<kIn, kC, true><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.x, N.wr + kW1, N.wr + kB1, N.h1);
-  k_lp_conv<kC, kC, true><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h1, N.wr + kW2, N.wr + kB2, N.h2);
-  k_lp_conv<kC, 1, false><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h2, N.wr + kW3, N.wr + kB3, N.y);
+  k_lp_conv<kIn, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.x, N.wr + kW1, N.h1);
+  k_lp_conv<kC, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h1, N.wr + kW2, N.h2);
+  k_lp_conv<kC, 1><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h2, N.wr + kW3, N.y);
 }
 
-// The preconditioner z = rs (net(r/rs) - net(-r/rs)) / 2, rs = rms(r): odd in
-// r and proportional to |r|.  r read and z written at slot[s] (nullptr: compact).
-void lp_precondition(Ell& E, LPNet& N, const int* slot, const double* r, double* z) {
+// The network's correction z = base + own * rs * net(r/rs), rs = rms(r) (the
+// scaling keeps FP32 in range; the network is linear).  r read and z written
+// at slot[s] (nullptr: compact); base may be nullptr.
+void lp_precondition(Ell& E, LPNet& N, const int* slot, const double* r, const double* base, double* z) {
   cudaStream_t st = E.s();
   lp_rms(N, st, slot, r, N.rs);
-  for (int pass = 0; pass < 2; ++pass) {
-    lp_forward(E, N, slot, r, N.rs + pass);
-    k_lp_output<<<lpg(N.ns), LP_TPB, 0, st>>>(N.ns, slot, N.y, N.rs + pass, z, pass);
-  }
+  lp_forward(E, N, slot, r, N.rs);
+  k_lp_output<<<lpg(N.ns), LP_TPB, 0, st>>>(N.ns, slot, N.y, N.rs, N.own, base, z);
 }
 
 // Energy-norm loss of the network output against the compact target e (scaled
@@ -190,22 +198,20 @@ void lp_precondition(Ell& E, LPNet& N, const int* slot, const double* r, double*
 void lp_backward(Ell& E, LPNet& N, const double* e, const double* rs, double* loss) {
   cudaStream_t st = E.s();
   const int ns = N.ns;
-  k_lp_err<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.y, e, rs, N.z);
+  k_lp_err<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.y, N.own, e, rs, N.z);
   op(E, OP_APPLY, N.l, N.z, nullptr, N.lz);
-  k_lp_aloss<LP_DOT><<<N.nbd(), LP_DOT, 0, st>>>(ns, N.slot, N.z, N.lz, E.h->at(N.l).hex_inv, N.inv_area, N.dy,
-                                                 N.partial);
+  k_lp_aloss<LP_DOT><<<N.nbd(), LP_DOT, 0, st>>>(ns, N.slot, N.z, N.lz, E.h->at(N.l).hex_inv, N.own, N.inv_area,
+                                                 N.dy, N.partial);
   k_lp_sum<<<1, 256, 0, st>>>(N.partial, N.nbd(), loss, 0, N.inv_area);
   cudaMemsetAsync(N.g, 0, 4 * kLpParams, st);
   cudaMemsetAsync(N.dh1, 0, 4 * (size_t)kC * ns, st);
   cudaMemsetAsync(N.dh2, 0, 4 * (size_t)kC * ns, st);
   const unsigned gw = std::min<unsigned>((ns + kChunk - 1) / kChunk, 148 * 4);
-  k_lp_wgrad<kC, 1><<<gw, 256, 0, st>>>(ns, N.tap, N.h2, N.dy, N.g + kW3, N.g + kB3);
+  k_lp_wgrad<kC, 1><<<gw, 256, 0, st>>>(ns, N.tap, N.h2, N.dy, N.g + kW3);
   k_lp_igrad<kC, 1><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.wr + kW3, N.dy, N.dh2);
-  k_lp_relu_back<<<lpg((int64_t)kC * ns, 256), 256, 0, st>>>(kC * ns, N.h2, N.dh2);
-  k_lp_wgrad<kC, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.h1, N.dh2, N.g + kW2, N.g + kB2);
+  k_lp_wgrad<kC, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.h1, N.dh2, N.g + kW2);
   k_lp_igrad<kC, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.wr + kW2, N.dh2, N.dh1);
-  k_lp_relu_back<<<lpg((int64_t)kC * ns, 256), 256, 0, st>>>(kC * ns, N.h1, N.dh1);
-  k_lp_wgrad<kIn, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.x, N.dh1, N.g + kW1, N.g + kB1);
+  k_lp_wgrad<kIn, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.x, N.dh1, N.g + kW1);
 }
 
 void lp_adam(Ell& E, LPNet& N, float lr) {
@@ -217,7 +223,8 @@ void lp_adam(Ell& E, LPNet& N, float lr) {
 
 // Residual/error pairs from FP64 multigrid: for each seeded right-hand side,
 // the solution u* to 1e-11, then from u = 0 the residual f - L u and error
-// u* - u before each of `cycles` V-cycles.  u and f of the level are kept.
+// u* - u after each of `cycles` V-cycles (what a V-cycle leaves, which the
+// network learns to correct).  u and f of the level are kept.
 int lp_generate(Ell& E, LPNet& N, const wt_learn_opts& lo, const wt_solver_opts& mg) {
   const int q = E.le - E.ls, ns = N.ns, l = E.le;
   const int64_t NN = N.NN;
@@ -227,7 +234,7 @@ int lp_generate(Ell& E, LPNet& N, const wt_learn_opts& lo, const wt_solver_opts&
   int rc = WT_OK;
   if ((rc = lpalloc(N.pair_allocs, &N.pr, (int64_t)np * ns))) return rc;
   if ((rc = lpalloc(N.pair_allocs, &N.pe, (int64_t)np * ns))) return rc;
-  if ((rc = lpalloc(N.pair_allocs, &N.pscale, 2 * (int64_t)np))) return rc;
+  if ((rc = lpalloc(N.pair_allocs, &N.pscale, np))) return rc;
   N.npairs = np;
   cudaMemcpyAsync(N.usave, E.u.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(N.fsave, E.f.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, st);
@@ -250,18 +257,17 @@ int lp_generate(Ell& E, LPNet& N, const wt_learn_opts& lo, const wt_solver_opts&
     rc = WT_OK;
     cudaMemcpyAsync(N.ustar, E.u.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, st);
     zero_level(E, l, E.u.lv[q]);
+    op(E, OP_RESID, l, E.u.lv[q], E.f.lv[q], E.res.lv[q]);
     for (int c = 0; c < lo.cycles; ++c) {
       const int64_t idx = (int64_t)k * lo.cycles + c;
+      vcycle64(E, o);
+      k_axpy_d<<<nb(NN), TPB, 0, st>>>(NN, E.u.lv[q], E.corr.lv[q]);
       op(E, OP_RESID, l, E.u.lv[q], E.f.lv[q], E.res.lv[q]);
       k_lp_gather<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, E.res.lv[q], N.pr + idx * ns);
       k_lp_diff<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.ustar, E.u.lv[q], N.pe + idx * ns);
-      lp_rms(N, st, nullptr, N.pr + idx * ns, N.rs);
-      cudaMemcpyAsync(N.pscale + idx, N.rs, 8, cudaMemcpyDeviceToDevice, st);
-      vcycle64(E, o);
-      k_axpy_d<<<nb(NN), TPB, 0, st>>>(NN, E.u.lv[q], E.corr.lv[q]);
+      lp_rms(N, st, nullptr, N.pr + idx * ns, N.pscale + idx);
     }
   }
-  k_lp_negate<<<lpg(np), LP_TPB, 0, st>>>(np, N.pscale, N.pscale + np);  // sign-flipped pairs
   cudaMemcpyAsync(E.u.lv[q], N.usave, 8 * NN, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(E.f.lv[q], N.fsave, 8 * NN, cudaMemcpyDeviceToDevice, st);
   cudaError_t e = cudaStreamSynchronize(st);
@@ -279,7 +285,6 @@ int lp_train(Ell& E, LPNet& N, const wt_learn_opts& lo, wt_learn_report& rep) {
   std::mt19937_64 g(lo.seed ^ 0x5bd1e995ull);
   std::vector<int> perm(np);
   for (int k = 0; k < np; ++k) perm[k] = k;
-  std::uniform_int_distribution<int> coin(0, 1);
   int step = 0;
   const double PI = std::acos(-1.0);
   for (int ep = 0; ep < std::max(1, lo.epochs); ++ep) {
@@ -287,10 +292,8 @@ int lp_train(Ell& E, LPNet& N, const wt_learn_opts& lo, wt_learn_report& rep) {
     for (int k : perm) {
       const float lr =
           (float)(lo.lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(PI * step / std::max(1, steps - 1)))));
-      // each pair is seen with either sign (the network is made odd at use)
-      const double* sc = N.pscale + k + (coin(g) ? np : 0);
-      lp_forward(E, N, nullptr, N.pr + (int64_t)k * ns, sc);
-      lp_backward(E, N, N.pe + (int64_t)k * ns, sc, losses + step);
+      lp_forward(E, N, nullptr, N.pr + (int64_t)k * ns, N.pscale + k);
+      lp_backward(E, N, N.pe + (int64_t)k * ns, N.pscale + k, losses + step);
       lp_adam(E, N, lr);
       ++step;
     }
@@ -319,18 +322,23 @@ enum { PRE_NONE = 0, PRE_NET = 1, PRE_MG = 2 };
 
 // One FCG iteration as a stream sequence (captured once per preconditioner):
 // z = M(r); Lz; beta and the new direction; alpha and the update; ||r||.
+// M: -1 (PRE_NONE), the V-cycle V (PRE_MG), or V then the network's correction
+// of the residual V leaves, z = c + net(r - L c), c = V(r) (PRE_NET).
 void fcg_iteration(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
   cudaStream_t st = E.s();
   const int q = E.le - E.ls, l = E.le, ns = N.ns;
   const double* hinv = E.h->at(l).hex_inv;
   if (pre == PRE_NONE) {
     k_fcg_neg<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.r, N.z);
-  } else if (pre == PRE_NET) {
-    lp_precondition(E, N, N.slot, N.r, N.z);
   } else {
     cudaMemcpyAsync(E.res.lv[q], N.r, 8 * N.NN, cudaMemcpyDeviceToDevice, st);
     vcycle64(E, o);
-    cudaMemcpyAsync(N.z, E.corr.lv[q], 8 * N.NN, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(pre == PRE_NET ? N.c : N.z, E.corr.lv[q], 8 * N.NN, cudaMemcpyDeviceToDevice, st);
+    if (pre == PRE_NET) {
+      op(E, OP_APPLY, l, N.c, nullptr, N.lz);
+      k_lp_sub<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.r, N.lz, N.r2);
+      lp_precondition(E, N, N.slot, N.r2, N.c, N.z);
+    }
   }
   op(E, OP_APPLY, l, N.z, nullptr, N.lz);
   auto wdot = [&](const double* a, const double* b, int slotv) {
@@ -350,7 +358,7 @@ void fcg_iteration(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
 
 int fcg_launch(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
   cudaGraphExec_t& ex = N.it_exec[pre];
-  const int key = pre == PRE_MG ? o.down_iter * 1000000 + o.up_iter * 10000 + o.coarse_iter : 0;
+  const int key = pre != PRE_NONE ? o.down_iter * 1000000 + o.up_iter * 10000 + o.coarse_iter : 0;
   if (!ex || N.it_key[pre] != key) {
     if (ex) {
       cudaGraphExecDestroy(ex);
@@ -379,8 +387,9 @@ void fcg_restart(Ell& E, LPNet& N) {
 
 // Flexible CG on level_end to ir_tol (relative to ||f||, the solver's l2).
 // With the network (PRE_NET) the V-cycle takes over when the residual has not
-// halved over the last kWin iterations, or when a step breaks down (<p, Lp> not
-// negative or not finite).
+// halved over the last kWin iterations, has grown tenfold above its smallest
+// value, or a step breaks down (<p, Lp> not negative or not finite); if the
+// residual is then above the initial one, u restarts from the initial guess.
 int fcg_solve(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, int pre) {
   if (!E.lp) {
     if (int rc = lp_build(E, 1)) return rc;
@@ -393,7 +402,9 @@ int fcg_solve(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, int pre) {
   fcg_restart(E, N);
   double err = l2(E, l, N.r) / nf;
   rep.nrm_res_init[q] = err;
+  if (pre == PRE_NET) cudaMemcpyAsync(N.usave, E.u.lv[q], 8 * N.NN, cudaMemcpyDeviceToDevice, E.s());
   std::vector<double> hist{err};
+  double best = err;
   int it = 0, since = 0, net_its = 0, breaks = 0;
   int mode = pre;
   int rc = WT_OK;
@@ -409,11 +420,14 @@ int fcg_solve(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, int pre) {
     err = sc[FCG_RNORM] / nf;
     hist.push_back(err);
     const bool broke = sc[FCG_BREAK] != 0.0 || !std::isfinite(err);
-    const bool stalled = since >= kWin && err > 0.5 * hist[hist.size() - 1 - kWin];
+    const bool stalled = (since >= kWin && err > 0.5 * hist[hist.size() - 1 - kWin]) || err > 10.0 * best;
+    best = std::min(best, err);
     if (mode == PRE_NET && (broke || stalled)) {
       mode = PRE_MG;
       rep.precond_fallback = it;
       since = 0;
+      if (!(err <= rep.nrm_res_init[q]))
+        cudaMemcpyAsync(E.u.lv[q], N.usave, 8 * N.NN, cudaMemcpyDeviceToDevice, E.s());
       fcg_restart(E, N);
       ++rep.restarts;
       err = l2(E, l, N.r) / nf;
@@ -506,7 +520,7 @@ int wt_learned_infer(wt_handle* h, const double* r, double* z) {
   if (!r || !z) return WT_ERR_ARG;
   cudaStream_t st = E->s();
   CKE(cudaMemcpyAsync(N->rc, r, 8 * (size_t)N->ns, cudaMemcpyHostToDevice, st));
-  lp_precondition(*E, *N, nullptr, N->rc, N->ec);
+  lp_precondition(*E, *N, nullptr, N->rc, nullptr, N->ec);
   CKE(cudaMemcpyAsync(z, N->ec, 8 * (size_t)N->ns, cudaMemcpyDeviceToHost, st));
   CKE(cudaStreamSynchronize(st));
   return WT_OK;

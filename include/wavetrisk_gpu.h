@@ -129,11 +129,12 @@ int wt_profile_rk4(wt_handle* h, double dt, int nsteps, double* ms_per_launch, i
  * arrays concatenated from level_start to level_end. */
 enum { WT_SOLVER_FMG = 0, WT_SOLVER_SRJ = 1, WT_SOLVER_MIXED_IR = 2, WT_SOLVER_MG64 = 3,
        /* Flexible CG (truncated to one previous direction, area-weighted inner
-        * product) on level_end, ir_tol / ir_max as for WT_SOLVER_MIXED_IR:
-        * preconditioned by the FP64 V-cycle followed by the learned network's
-        * correction of the residual the V-cycle leaves, with the V-cycle alone
-        * as the fallback when that fails to contract (FCG_LEARNED); by the
-        * FP64 V-cycle alone (FCG_MG, the method without the network); or
+        * product, FP64 recurrences) on level_end, ir_tol / ir_max as for
+        * WT_SOLVER_MIXED_IR: preconditioned by the FP32 V-cycle of the mixed
+        * solve followed by the learned network's correction of the residual
+        * the V-cycle leaves, with plain FP64 multigrid (the FP64 V-cycle) as
+        * the fallback when that fails to contract (FCG_LEARNED); by the FP32
+        * V-cycle alone (FCG_MG, the method without the network); or
         * unpreconditioned (FCG).  No reference counterpart. */
        WT_SOLVER_FCG_LEARNED = 4, WT_SOLVER_FCG = 5, WT_SOLVER_FCG_MG = 6 };
 
@@ -185,7 +186,7 @@ int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report
 
 /* ------------------------------------------------ learned preconditioner ---- */
 /* A hexagonal-stencil convolution network (7 taps: a node and its six
- * neighbours; 2 -> 32 -> 32 -> 1 channels) mapping a residual r of level_end,
+ * neighbours; 2 -> 8 -> 8 -> 1 channels) mapping a residual r of level_end,
  * scaled by its rms, to an approximation of the error e with L e = r, trained
  * on the residuals a V-cycle leaves and used to correct them
  * (WT_SOLVER_FCG_LEARNED).  Its inputs are r and r times a depth feature

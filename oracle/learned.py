@@ -8,7 +8,7 @@ so this restates the network the CUDA kernels define:
           source (lozenge, row j, column i order);
   taps  : the node and its neighbours (+1,0), (+1,+1), (0,+1), (-1,0),
           (-1,-1), (0,-1), resolved through the ghost remap; -1 outside;
-  net   : x = [r / rms(r), (r / rms(r)) (|H| / 2750 - 1)] -> 32 -> 32 -> 1
+  net   : x = [r / rms(r), (r / rms(r)) (|H| / 2750 - 1)] -> 8 -> 8 -> 1
           channels, each a 7-tap convolution with BF16-rounded weights, no
           biases, identity activations (linear in r);
   use   : z = rms(r) y own, own = 0 at the pole slots (slots outside
@@ -21,7 +21,7 @@ Everything is evaluated in float64 from float32-rounded inputs, so the CUDA
 FP32 results agree to FP32 accumulation-order differences."""
 import numpy as np
 
-TAPS, C, CIN = 7, 32, 2
+TAPS, C, CIN = 7, 8, 2
 DI = (0, 1, 1, 0, -1, -1, 0)
 DJ = (0, 0, 1, 1, 0, -1, -1)
 SHAPES = [("W1", (TAPS, CIN, C)), ("W2", (TAPS, C, C)), ("W3", (TAPS, C, 1))]

@@ -1,5 +1,5 @@
 // Learned preconditioner of the free-surface solve: a hexagonal-stencil
-// convolution network over the nodes of one level, 2 -> 32 -> 32 -> 1 channels.
+// convolution network over the nodes of one level, 2 -> 8 -> 8 -> 1 channels.
 // Each layer sums over seven taps (the node and its six neighbours in lozenge
 // directions (+1,0), (+1,+1), (0,+1), (-1,0), (-1,-1), (0,-1), read through the
 // ghost remap) and its input channels:
@@ -10,13 +10,13 @@
 // residuals to any residual.  It corrects what a multigrid V-cycle leaves: the
 // preconditioner is z = c + net(r - L c) with c the V-cycle's correction, and
 // the network's output is masked to 0 at the pole slots (slots of [0, n]^2
-// outside [0, n)^2, whose lozenge-frame taps are degenerate).  The weights are FP32 master copies rounded to BF16 for every use
-// (BF16 weights, FP32 activations and accumulation).  Nodes are numbered
-// compactly: the slots of [0, n]^2 of every lozenge that are their own ghost
-// source; a tap that leaves that set reads 0.  Activations are channel-major,
-// in[c * ns + s].
+// outside [0, n)^2, whose lozenge-frame taps are degenerate).  The weights
+// are FP32 master copies rounded to BF16 for every use (BF16 weights, FP32
+// activations and accumulation).  Nodes are numbered compactly: the slots of
+// [0, n]^2 of every lozenge that are their own ghost source; a tap that
+// leaves that set reads 0.  Activations are channel-major, in[c * ns + s].
 //
-// Parameter layout (kLpParams floats): W1[7][2][32], W2[7][32][32], W3[7][32][1].
+// Parameter layout (kLpParams floats): W1[7][2][8], W2[7][8][8], W3[7][8][1].
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -25,7 +25,7 @@
 
 namespace wtl {
 
-constexpr int kTaps = 7, kC = 32, kIn = 2;
+constexpr int kTaps = 7, kC = 8, kIn = 2;
 constexpr int kW1 = 0, kW2 = kW1 + kTaps * kIn * kC, kW3 = kW2 + kTaps * kC * kC, kLpParams = kW3 + kTaps * kC;
 constexpr int kDepthRef = 2750;  // depth feature |H| / 2750 m - 1
 

@@ -35,8 +35,8 @@ struct LPNet {
   // V-cycle's correction and the residual it leaves)
   int adam_t = 0;
   double inv_area = 1.0;  // 1 / sum of the node areas 1 / hex_inv
-  cudaGraphExec_t it_exec[3] = {nullptr, nullptr, nullptr};
-  int it_key[3] = {-1, -1, -1};
+  cudaGraphExec_t it_exec[4] = {nullptr, nullptr, nullptr, nullptr};
+  int it_key[4] = {-1, -1, -1, -1};
   std::vector<void*> allocs, pair_allocs;
   int nbd() const { return (ns + LP_DOT - 1) / LP_DOT; }
 };
@@ -318,22 +318,30 @@ int lp_train(Ell& E, LPNet& N, const wt_learn_opts& lo, wt_learn_report& rep) {
 }
 
 // ------------------------------------------------------- flexible CG ----
-enum { PRE_NONE = 0, PRE_NET = 1, PRE_MG = 2 };
+enum { PRE_NONE = 0, PRE_NET = 1, PRE_MG = 2, PRE_MG64 = 3 };
 
 // One FCG iteration as a stream sequence (captured once per preconditioner):
 // z = M(r); Lz; beta and the new direction; alpha and the update; ||r||.
-// M: -1 (PRE_NONE), the V-cycle V (PRE_MG), or V then the network's correction
-// of the residual V leaves, z = c + net(r - L c), c = V(r) (PRE_NET).
+// M: -1 (PRE_NONE); the FP32 V-cycle V of the mixed solve (PRE_MG); V then the
+// network's correction of the residual V leaves, z = c + net(r - L c),
+// c = V(r) (PRE_NET); or the FP64 V-cycle, plain multigrid (PRE_MG64, the
+// fallback).  The recurrences stay FP64 whatever the preconditioner.
 void fcg_iteration(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
   cudaStream_t st = E.s();
   const int q = E.le - E.ls, l = E.le, ns = N.ns;
   const double* hinv = E.h->at(l).hex_inv;
   if (pre == PRE_NONE) {
     k_fcg_neg<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.r, N.z);
-  } else {
+  } else if (pre == PRE_MG64) {
     cudaMemcpyAsync(E.res.lv[q], N.r, 8 * N.NN, cudaMemcpyDeviceToDevice, st);
     vcycle64(E, o);
-    cudaMemcpyAsync(pre == PRE_NET ? N.c : N.z, E.corr.lv[q], 8 * N.NN, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(N.z, E.corr.lv[q], 8 * N.NN, cudaMemcpyDeviceToDevice, st);
+  } else {
+    double* c = pre == PRE_NET ? N.c : N.z;
+    k_d2f<<<nb(N.NN), TPB, 0, st>>>(N.NN, N.r, E.r32.lvf[q]);
+    vcycle32(E, o);
+    cudaMemsetAsync(c, 0, 8 * N.NN, st);
+    k_axpy_f2d<<<nb(N.NN), TPB, 0, st>>>(N.NN, c, E.c32.lvf[q]);
     if (pre == PRE_NET) {
       op(E, OP_APPLY, l, N.c, nullptr, N.lz);
       k_lp_sub<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.r, N.lz, N.r2);
@@ -386,7 +394,7 @@ void fcg_restart(Ell& E, LPNet& N) {
 }
 
 // Flexible CG on level_end to ir_tol (relative to ||f||, the solver's l2).
-// With the network (PRE_NET) the V-cycle takes over when the residual has not
+// With the network (PRE_NET) plain FP64 multigrid takes over when the residual has not
 // halved over the last kWin iterations, has grown tenfold above its smallest
 // value, or a step breaks down (<p, Lp> not negative or not finite); if the
 // residual is then above the initial one, u restarts from the initial guess.
@@ -423,7 +431,7 @@ int fcg_solve(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, int pre) {
     const bool stalled = (since >= kWin && err > 0.5 * hist[hist.size() - 1 - kWin]) || err > 10.0 * best;
     best = std::min(best, err);
     if (mode == PRE_NET && (broke || stalled)) {
-      mode = PRE_MG;
+      mode = PRE_MG64;
       rep.precond_fallback = it;
       since = 0;
       if (!(err <= rep.nrm_res_init[q]))

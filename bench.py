@@ -221,7 +221,7 @@ def elliptic_case(lmax, repeats=3):
     # the learned preconditioner: trained once on this level on residual/error
     # pairs of the FP64 multigrid (training time reported apart from the solves)
     S.learned_setup(1)
-    tr = S.learned_train(n_rhs=8, cycles=4, epochs=15, lr=2e-3, seed=1)
+    tr = S.learned_train(n_rhs=16, cycles=4, epochs=40, lr=2e-3, seed=1)
     out["learned_training"] = {"pairs": tr.pairs, "adam_steps": tr.steps, "loss_first_epoch": tr.loss_first_epoch,
                                "loss_last_epoch": tr.loss_last_epoch, "ms_generate": tr.ms_generate,
                                "ms_train": tr.ms_train}

@@ -135,3 +135,30 @@ def test_mixed_precision_reaches_1e_10(hier):
     rep = S.solve(solver_opts("mixed", 1e-10, down_iter=2, up_iter=2, coarse_iter=20))
     assert rep.status == 0 and rep.true_rel_residual <= 1e-10, (rep.true_rel_residual, rep.outer_iterations)
     S.close()
+
+
+def test_solvers_interleaved_keep_converging(hier):
+    """The reference-path FMG/SRJ swap work buffers between calls; the mixed and
+    FP64 refinement solves (whose V-cycle is a captured graph) and the learned
+    FCG must converge whatever ran before them on the same handle."""
+    levels, topos, off = hier
+    S = EllipticSolver(levels, topos)
+    f = np.zeros(off[-1])
+    f[off[-2]:off[-1]] = elliptic_rhs(levels[-1], seed=5)
+    S.upload(f=f)
+    S.restrict()
+    _, fr = S.download()
+    S.learned_setup(1)
+    S.learned_train(n_rhs=2, cycles=2, epochs=2)
+    kw = dict(down_iter=2, up_iter=2, coarse_iter=20)
+    seq = [("mg64", kw), ("fmg", dict(max_vcycle=50, coarse_iter=300)), ("mg64", kw), ("mixed", kw),
+           ("fmg", dict(max_vcycle=50, coarse_iter=300)), ("srj", dict(max_srj_iter=4000, coarse_iter=300)),
+           ("mixed", kw), ("mg64", kw), ("fcg_learned", kw), ("fmg", dict(max_vcycle=50, coarse_iter=300)),
+           ("mg64", kw), ("fcg_mg", kw)]
+    for name, k in seq:
+        S.upload(u=np.zeros(off[-1]), f=fr)
+        rep = S.solve(solver_opts(name, 1e-10, **k))
+        assert rep.true_rel_residual <= 1e-9, (name, rep.true_rel_residual)
+        if name in ("mg64", "mixed", "fcg_learned", "fcg_mg"):
+            assert rep.status == 0 and rep.true_rel_residual <= 1e-10, name
+    S.close()

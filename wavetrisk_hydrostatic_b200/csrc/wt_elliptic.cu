@@ -53,6 +53,7 @@ struct Ell {
   double* scal = nullptr;  // device scalars
   cudaGraphExec_t cycle_exec[2] = {nullptr, nullptr};  // captured correction cycles (FP32, FP64)
   int cycle_key[2] = {-1, -1};
+  const double* cycle_res[2] = {nullptr, nullptr};  // res buffer of level_end each cycle graph reads
   int nbmax = 0;
   std::vector<void*> allocs;
   void* lp = nullptr;  // learned preconditioner (wt_learned.cuh)

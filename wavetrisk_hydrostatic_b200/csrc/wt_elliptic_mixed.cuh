@@ -178,10 +178,13 @@ int mixed_ir(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, bool fp64 =
     if (it == 0) rep.nrm_res_init[q] = err;
     if (err <= o.ir_tol || it == o.ir_max) break;
     // The correction cycle has no host decision: it is captured once per
-    // configuration and replayed as one graph launch per refinement step.
+    // configuration and replayed as one graph launch per refinement step.  The
+    // residual above is written through the current res pointer, which the
+    // reference-path V-cycle (v_cycle) swaps with au: a graph captured with
+    // the other buffer is captured again.
     cudaGraphExec_t& ex = E.cycle_exec[fp64 ? 1 : 0];
     const int key = o.down_iter * 1000000 + o.up_iter * 10000 + o.coarse_iter;
-    if (!ex || E.cycle_key[fp64 ? 1 : 0] != key) {
+    if (!ex || E.cycle_key[fp64 ? 1 : 0] != key || E.cycle_res[fp64 ? 1 : 0] != E.res.lv[q]) {
       if (ex) { cudaGraphExecDestroy(ex); ex = nullptr; }
       cudaGraph_t g;
       cudaStreamBeginCapture(E.s(), cudaStreamCaptureModeThreadLocal);
@@ -199,6 +202,7 @@ int mixed_ir(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, bool fp64 =
       cudaGraphDestroy(g);
       if (ce != cudaSuccess) return wt_handle_fail("cycle instantiate", ce);
       E.cycle_key[fp64 ? 1 : 0] = key;
+      E.cycle_res[fp64 ? 1 : 0] = E.res.lv[q];
     }
     cudaError_t le = cudaGraphLaunch(ex, E.s());
     if (le != cudaSuccess) return wt_handle_fail("cycle launch", le);

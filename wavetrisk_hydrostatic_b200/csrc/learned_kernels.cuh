@@ -132,6 +132,60 @@ __global__ void __launch_bounds__(128) k_lp_conv(int ns, const int* __restrict__
   for (int co = 0; co < COUT; ++co) out[co * ns + s] = acc[co];
 }
 
+// The first layer with the input built on the fly, for the solver: the input
+// of tap node u is v = (r - lc)(slot[u]) (FP64 difference, then FP32) and
+// v * depth feature; the values k_lp_input gives for r - lc at rscale 1.
+__global__ void __launch_bounds__(128) k_lp_conv_in(int ns, const int* __restrict__ tap, const int* __restrict__ slot,
+                                                    const double* __restrict__ r, const double* __restrict__ lc,
+                                                    const double* __restrict__ topo, const float* __restrict__ W,
+                                                    float* __restrict__ out) {
+  __shared__ float sw[kTaps * kIn * kC];
+  for (int q = threadIdx.x; q < kTaps * kIn * kC; q += blockDim.x) sw[q] = W[q];
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  float acc[kC];
+#pragma unroll
+  for (int co = 0; co < kC; ++co) acc[co] = 0.0f;
+  for (int t = 0; t < kTaps; ++t) {
+    const int u = tap[t * ns + s];
+    if (u < 0) continue;
+    const int id = slot[u];
+    const float v = (float)(r[id] - lc[id]);
+    const float x[kIn] = {v, v * (float)(fabs(topo[id]) / (double)kDepthRef - 1.0)};
+#pragma unroll
+    for (int ci = 0; ci < kIn; ++ci) {
+      const float* w = sw + (t * kIn + ci) * kC;
+#pragma unroll
+      for (int co = 0; co < kC; ++co) acc[co] = fmaf(w[co], x[ci], acc[co]);
+    }
+  }
+#pragma unroll
+  for (int co = 0; co < kC; ++co) out[co * ns + s] = acc[co];
+}
+
+// The last layer fused with the solver's output: z(slot[s]) = base(slot[s]) +
+// own * y(s), y the 1-channel convolution of in.
+__global__ void __launch_bounds__(128) k_lp_conv_out(int ns, const int* __restrict__ tap, const int* __restrict__ slot,
+                                                     const float* __restrict__ in, const float* __restrict__ W,
+                                                     const float* __restrict__ own, const double* __restrict__ base,
+                                                     double* __restrict__ z) {
+  __shared__ float sw[kTaps * kC];
+  for (int q = threadIdx.x; q < kTaps * kC; q += blockDim.x) sw[q] = W[q];
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  float acc = 0.0f;
+  for (int t = 0; t < kTaps; ++t) {
+    const int u = tap[t * ns + s];
+    if (u < 0) continue;
+#pragma unroll
+    for (int ci = 0; ci < kC; ++ci) acc = fmaf(sw[t * kC + ci], in[ci * ns + u], acc);
+  }
+  const int id = slot[s];
+  z[id] = base[id] + (double)(own[s] * acc);
+}
+
 // z = base + own * rscale * y into slot[s] of a level array (nullptr:
 // compact; base == nullptr: 0), own = 1 on the owned nodes, 0 at the poles.
 __global__ void k_lp_output(int ns, const int* __restrict__ slot, const float* __restrict__ y,
@@ -143,12 +197,6 @@ __global__ void k_lp_output(int ns, const int* __restrict__ slot, const float* _
   z[id] = (base ? base[id] : 0.0) + (double)(own[s] * y[s]) * *rscale;
 }
 
-// out = x - y on the node slots (the residual a V-cycle correction leaves).
-__global__ void k_lp_sub(int ns, const int* __restrict__ slot, const double* __restrict__ x,
-                         const double* __restrict__ y, double* __restrict__ out) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < ns) out[slot[s]] = x[slot[s]] - y[slot[s]];
-}
 
 // Training loss: the error of the network in the energy norm of the solve,
 //   loss = <d, -L d>_W / |W|,  d = own y - e / rscale,  W = 1 / hex_inv (cell area),

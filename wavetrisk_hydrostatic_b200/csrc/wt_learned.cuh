@@ -30,9 +30,9 @@ struct LPNet {
   double *pr = nullptr, *pe = nullptr, *pscale = nullptr;  // training pairs
   int npairs = 0;
   double *r = nullptr, *z = nullptr, *lz = nullptr, *p = nullptr, *lp = nullptr, *ustar = nullptr,
-         *usave = nullptr, *fsave = nullptr, *c = nullptr, *r2 = nullptr;
-  // level arrays (usave: also u at the start of a learned solve; c, r2: the
-  // V-cycle's correction and the residual it leaves)
+         *usave = nullptr, *fsave = nullptr, *c = nullptr;
+  // level arrays (usave: also u at the start of a learned solve; c: the
+  // V-cycle's correction)
   int adam_t = 0;
   double inv_area = 1.0;  // 1 / sum of the node areas 1 / hex_inv
   cudaGraphExec_t it_exec[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -150,7 +150,7 @@ int lp_build(Ell& E, uint64_t seed) {
   al(&N->losses, 1);
   al(&N->rc, ns);
   al(&N->ec, ns);
-  for (double** p : {&N->r, &N->z, &N->lz, &N->p, &N->lp, &N->ustar, &N->usave, &N->fsave, &N->c, &N->r2})
+  for (double** p : {&N->r, &N->z, &N->lz, &N->p, &N->lp, &N->ustar, &N->usave, &N->fsave, &N->c})
     al(p, D.NN);
   if (rc == WT_OK) {
     cudaMemcpy(N->slot, slot.data(), 4 * (size_t)ns, cudaMemcpyHostToDevice);
@@ -343,9 +343,13 @@ void fcg_iteration(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
     cudaMemsetAsync(c, 0, 8 * N.NN, st);
     k_axpy_f2d<<<nb(N.NN), TPB, 0, st>>>(N.NN, c, E.c32.lvf[q]);
     if (pre == PRE_NET) {
+      // z = c + net(r - L c): the network is linear, so it runs on the
+      // unscaled residual; its input and output are fused into the first and
+      // last layers (k_lp_input + k_lp_conv, k_lp_conv + k_lp_output)
       op(E, OP_APPLY, l, N.c, nullptr, N.lz);
-      k_lp_sub<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.r, N.lz, N.r2);
-      lp_precondition(E, N, N.slot, N.r2, N.c, N.z);
+      k_lp_conv_in<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.slot, N.r, N.lz, E.h->at(l).topo, N.wr + kW1, N.h1);
+      k_lp_conv<kC, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h1, N.wr + kW2, N.h2);
+      k_lp_conv_out<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.slot, N.h2, N.wr + kW3, N.own, N.c, N.z);
     }
   }
   op(E, OP_APPLY, l, N.z, nullptr, N.lz);

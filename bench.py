@@ -57,6 +57,10 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--kernels-only", action="store_true")
     p.add_argument("--wavelets-only", action="store_true")
+    p.add_argument("--elliptic-only", action="store_true",
+                   help="only the free-surface solve on uniform J5..J<level> (every method, the learned "
+                        "preconditioner trained first); each timed solve is an NVTX range named after its method")
+    p.add_argument("--learned-epochs", type=int, default=40, help="training epochs of the learned preconditioner")
     p.add_argument("--trace", default=None, metavar="PATH",
                    help="record a CUDA kernel timeline of --steps adaptive steps (after --warmup) into PATH "
                         "(Chrome trace) and print its summary instead of the bench line")
@@ -196,7 +200,7 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
     return out
 
 
-def elliptic_case(lmax, repeats=3):
+def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False):
     """Free-surface solve on the uniform hierarchy J5..lmax to relative residual
     1e-10: the reference's FMG and SRJ, the FP64 V-cycle in FP64 refinement
     (plain FP64 multigrid) and FP32 V-cycles in FP64 refinement.  Best of
@@ -221,7 +225,7 @@ def elliptic_case(lmax, repeats=3):
     # the learned preconditioner: trained once on this level on residual/error
     # pairs of the FP64 multigrid (training time reported apart from the solves)
     S.learned_setup(1)
-    tr = S.learned_train(n_rhs=16, cycles=4, epochs=40, lr=2e-3, seed=1)
+    tr = S.learned_train(n_rhs=16, cycles=4, epochs=epochs, lr=2e-3, seed=1)
     out["learned_training"] = {"pairs": tr.pairs, "adam_steps": tr.steps, "loss_first_epoch": tr.loss_first_epoch,
                                "loss_last_epoch": tr.loss_last_epoch, "ms_generate": tr.ms_generate,
                                "ms_train": tr.ms_train}
@@ -238,7 +242,12 @@ def elliptic_case(lmax, repeats=3):
         best, rep = None, None
         for _ in range(repeats):
             S.upload(u=np.zeros(off[-1]), f=fr)
+            if nvtx:
+                import torch
+                torch.cuda.nvtx.range_push(name)
             rep = S.solve(o)
+            if nvtx:
+                torch.cuda.nvtx.range_pop()
             best = rep.ms if best is None else min(best, rep.ms)
         out[name] = {"ms": best, "rel_residual": rep.true_rel_residual, "status": rep.status,
                      "outer_iterations": rep.outer_iterations}
@@ -852,6 +861,8 @@ def main():
         bench_trace(args)
     elif args.wavelets_only:
         bench_wavelets(args)
+    elif args.elliptic_only:
+        print(json.dumps(elliptic_case(args.level, epochs=args.learned_epochs, nvtx=True)))
     else:
         bench_ours(args)
 

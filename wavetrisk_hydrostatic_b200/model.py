@@ -436,7 +436,7 @@ class EllipticSolver(DeviceGrid):
         return float(loss[0]), g
 
     def learned_train(self, n_rhs: int = 16, cycles: int = 4, epochs: int = 40, lr: float = 2e-3, seed: int = 1,
-                      down_iter: int = 2, up_iter: int = 2, coarse_iter: int = 20) -> "N.wt_learn_report":
+                      down_iter: int = 2, up_iter: int = 2, coarse_iter: int = 6) -> "N.wt_learn_report":
         """Pairs from the FP64 multigrid, then Adam on the GPU (wt_learned_train)."""
         o = N.wt_learn_opts(n_rhs, cycles, epochs, lr, seed, down_iter, up_iter, coarse_iter)
         rep = N.wt_learn_report()

@@ -184,6 +184,17 @@ int wt_elliptic_l2(wt_handle* h, int level, int which, double* out);
  * stops at ir_max above ir_tol. */
 int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report* rep);
 
+/* V-cycle schedule autotuner: solves the resident problem with `base` and each
+ * candidate schedule (down_iter, up_iter, coarse_iter; cand = 3*ncand ints, or
+ * NULL for the built-in set: down = up in {1, 2, 3}, coarse in {2, 4, 6, 10,
+ * 20}), `repeats` times each from the resident u, and writes the fastest that
+ * reaches base->ir_tol into *best (with its best wall time in *best_ms).  For
+ * methods that solve on level_end only: WT_SOLVER_MIXED_IR, _MG64,
+ * _FCG_LEARNED, _FCG_MG.  u and f are kept.  No reference counterpart (the
+ * reference's schedule is fixed by its module parameters). */
+int wt_elliptic_autotune(wt_handle* h, const wt_solver_opts* base, const int* cand, int ncand, int repeats,
+                         wt_solver_opts* best, double* best_ms);
+
 /* ------------------------------------------------ learned preconditioner ---- */
 /* A hexagonal-stencil convolution network (7 taps: a node and its six
  * neighbours; 2 -> 8 -> 8 -> 1 channels) mapping a residual r of level_end,

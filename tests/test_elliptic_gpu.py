@@ -162,3 +162,23 @@ def test_solvers_interleaved_keep_converging(hier):
         if name in ("mg64", "mixed", "fcg_learned", "fcg_mg"):
             assert rep.status == 0 and rep.true_rel_residual <= 1e-10, name
     S.close()
+
+
+def test_autotune_picks_a_converging_candidate_and_keeps_u_f(hier):
+    levels, topos, off = hier
+    S = EllipticSolver(levels, topos)
+    f = np.zeros(off[-1])
+    f[off[-2]:off[-1]] = elliptic_rhs(levels[-1], seed=6)
+    S.upload(f=f)
+    S.restrict()
+    u0 = random_ml(levels, 3) * 1e-3
+    _, fr = S.download()
+    S.upload(u=u0, f=fr)
+    cands = [(2, 2, 20), (2, 2, 6), (1, 1, 6)]
+    best, ms = S.autotune("mg64", 1e-10, candidates=cands, repeats=2)
+    assert (best.down_iter, best.up_iter, best.coarse_iter) in cands and best.method == 3 and ms > 0
+    u1, f1 = S.download()
+    assert np.array_equal(u1, u0) and np.array_equal(f1, fr)
+    rep = S.solve(best)
+    assert rep.status == 0 and rep.true_rel_residual <= 1e-10
+    S.close()

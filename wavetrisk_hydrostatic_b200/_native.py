@@ -131,6 +131,8 @@ _DEVICE_SIGS = {
     "wt_elliptic_prolong": [_vp, C.c_int],
     "wt_elliptic_l2": [_vp, C.c_int, C.c_int, _dp],
     "wt_elliptic_solve": [_vp, C.POINTER(wt_solver_opts), C.POINTER(wt_solver_report)],
+    "wt_elliptic_autotune": [_vp, C.POINTER(wt_solver_opts), C.POINTER(C.c_int), C.c_int, C.c_int,
+                             C.POINTER(wt_solver_opts), _dp],
     "wt_learned_setup": [_vp, C.c_ulonglong],
     "wt_learned_num_params": [],
     "wt_learned_params": [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float)],

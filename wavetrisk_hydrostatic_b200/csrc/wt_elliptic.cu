@@ -516,4 +516,57 @@ int wt_elliptic_solve(wt_handle* h, const wt_solver_opts* opts, wt_solver_report
   return WT_OK;
 }
 
+int wt_elliptic_autotune(wt_handle* h, const wt_solver_opts* base, const int* cand, int ncand, int repeats,
+                         wt_solver_opts* best, double* best_ms) {
+  if (!h || !h->ell || !base || !best || !best_ms || repeats < 1) return WT_ERR_ARG;
+  const int m = base->method;
+  if (m != WT_SOLVER_MIXED_IR && m != WT_SOLVER_MG64 && m != WT_SOLVER_FCG_LEARNED && m != WT_SOLVER_FCG_MG)
+    return WT_ERR_ARG;
+  Ell& E = *static_cast<Ell*>(h->ell);
+  std::vector<int> set;
+  if (cand) {
+    if (ncand < 1) return WT_ERR_ARG;
+    set.assign(cand, cand + 3 * ncand);
+  } else {
+    for (int d = 1; d <= 3; ++d)
+      for (int c : {2, 4, 6, 10, 20}) set.insert(set.end(), {d, d, c});
+  }
+  const int q = E.le - E.ls;
+  const int64_t NN = E.L[q].NN;
+  double* u0 = nullptr;
+  CKE(cudaMalloc(&u0, 8 * NN));
+  cudaMemcpyAsync(u0, E.u.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, E.s());
+  double tbest = -1.0;
+  int rc = WT_OK;
+  for (size_t k = 0; k + 2 < set.size() && rc == WT_OK; k += 3) {
+    wt_solver_opts o = *base;
+    o.down_iter = set[k];
+    o.up_iter = set[k + 1];
+    o.coarse_iter = set[k + 2];
+    if (o.down_iter < 0 || o.up_iter < 0 || o.coarse_iter < 0) continue;
+    double t = -1.0;
+    for (int r = 0; r < repeats; ++r) {
+      cudaMemcpyAsync(E.u.lv[q], u0, 8 * NN, cudaMemcpyDeviceToDevice, E.s());
+      wt_solver_report rep;
+      const int src = wt_elliptic_solve(h, &o, &rep);
+      if (src == WT_ERR_CUDA) rc = src;
+      if (src != WT_OK) {
+        t = -1.0;
+        break;
+      }
+      t = t < 0 ? rep.ms : std::min(t, rep.ms);
+    }
+    if (t >= 0 && (tbest < 0 || t < tbest)) {
+      tbest = t;
+      *best = o;
+    }
+  }
+  cudaMemcpyAsync(E.u.lv[q], u0, 8 * NN, cudaMemcpyDeviceToDevice, E.s());
+  cudaStreamSynchronize(E.s());
+  cudaFree(u0);
+  if (rc != WT_OK) return rc;
+  *best_ms = tbest;
+  return tbest < 0 ? WT_ERR_NOT_CONVERGED : WT_OK;
+}
+
 }  // extern "C"

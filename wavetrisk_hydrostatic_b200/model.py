@@ -390,6 +390,22 @@ class EllipticSolver(DeviceGrid):
         N.check("wt_elliptic_l2", N.lib().wt_elliptic_l2(self.h, level, which, C.byref(v)))
         return v.value
 
+    def autotune(self, method: str, tol: float = 1e-10, candidates=None, repeats: int = 3, **kw):
+        """Fastest V-cycle schedule (down_iter, up_iter, coarse_iter) of `method`
+        on the resident problem (wt_elliptic_autotune): (opts, best ms).
+        candidates: iterable of (down, up, coarse), or None for the built-in set."""
+        base = solver_opts(method, tol, **kw)
+        cand, n = None, 0
+        if candidates is not None:
+            arr = np.ascontiguousarray(np.asarray(list(candidates), dtype=np.int32).reshape(-1, 3))
+            n = arr.shape[0]
+            cand = arr.ctypes.data_as(C.POINTER(C.c_int))
+        best = N.wt_solver_opts()
+        ms = C.c_double()
+        N.check("wt_elliptic_autotune", N.lib().wt_elliptic_autotune(self.h, C.byref(base), cand, n, int(repeats),
+                                                                     C.byref(best), C.byref(ms)))
+        return best, ms.value
+
     # ---- learned preconditioner (network on level_end) ----
     def learned_setup(self, seed: int = 1) -> int:
         """He-initialised network; returns its node count ns."""

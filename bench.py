@@ -200,7 +200,7 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
     return out
 
 
-def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False):
+def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False, eval_seeds=None):
     """Free-surface solve on the uniform hierarchy J5..lmax to relative residual
     1e-10: the reference's FMG and SRJ, the FP64 V-cycle in FP64 refinement
     (plain FP64 multigrid) and FP32 V-cycles in FP64 refinement.  Best of
@@ -259,6 +259,7 @@ def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False):
     # down = up in {1, 2, 3} sweeps, coarse in {2, 4, 6, 10, 20}), timed the same way
     # (the network is trained again, on the residual/error pairs of the V-cycle tuned for FCG without it,
     # before its own schedule is tuned: it learns what that V-cycle leaves)
+    tuned = {}
     for name in ("mg64", "mixed", "fcg_mg", "fcg_learned"):
         if name == "fcg_learned":
             d, u_, c = out["fcg_mg_tuned"]["schedule"]
@@ -274,10 +275,36 @@ def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False):
             S.upload(u=np.zeros(off[-1]), f=fr)
             rep = S.solve(o)
             best = rep.ms if best is None else min(best, rep.ms)
+        tuned[name] = o
         out[name + "_tuned"] = {"ms": best, "schedule": [o.down_iter, o.up_iter, o.coarse_iter],
                                 "rel_residual": rep.true_rel_residual, "status": rep.status,
                                 "iterations": rep.iterations[q] if name.startswith("fcg") else rep.outer_iterations}
     out["learned_speedup_vs_fp64_mg_tuned"] = out["mg64_tuned"]["ms"] / out["fcg_learned_tuned"]["ms"]
+    if eval_seeds:
+        # right-hand sides the network never saw (its training ones come from its own seeded generator)
+        ev = {name: {"ms": [], "iterations": [], "worst_rel_residual": 0.0, "fallbacks": 0, "failures": 0}
+              for name in tuned}
+        for sd in range(100, 100 + eval_seeds):
+            g2 = np.zeros(off[-1])
+            g2[off[-2]:off[-1]] = elliptic_rhs(levels[-1], seed=sd)
+            S.upload(u=np.zeros(off[-1]), f=g2)
+            S.restrict()
+            _, gr = S.download()
+            for name, o in tuned.items():
+                S.upload(u=np.zeros(off[-1]), f=gr)
+                rep = S.solve(o)
+                e = ev[name]
+                e["ms"].append(rep.ms)
+                e["iterations"].append(rep.iterations[q] if name.startswith("fcg") else rep.outer_iterations)
+                e["worst_rel_residual"] = max(e["worst_rel_residual"], rep.true_rel_residual)
+                e["fallbacks"] += int(rep.precond_fallback > 0)
+                e["failures"] += int(rep.status != 0)
+        out["unseen_rhs_eval"] = {"seeds": eval_seeds, **{
+            name: {"mean_ms": float(np.mean(e["ms"])), "mean_iterations": float(np.mean(e["iterations"])),
+                   "worst_rel_residual": e["worst_rel_residual"], "fallbacks": e["fallbacks"],
+                   "failures": e["failures"]} for name, e in ev.items()}}
+        out["unseen_rhs_eval"]["learned_speedup_vs_fp64_mg"] = (
+            out["unseen_rhs_eval"]["mg64"]["mean_ms"] / out["unseen_rhs_eval"]["fcg_learned"]["mean_ms"])
     out["mixed_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["mixed"]["ms"]
     out["mixed_speedup_vs_fmg"] = out["fmg"]["ms"] / out["mixed"]["ms"]
     out["learned_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["fcg_learned"]["ms"]
@@ -549,7 +576,7 @@ def bench_ours(args):
                 "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,
             })
         for lmax in (6, 7, 8):
-            extra.append(elliptic_case(lmax))
+            extra.append(elliptic_case(lmax, eval_seeds=16 if lmax == 8 else None))
         for (lmin, lmax, nzw) in ((5, 7, 16), (5, 8, 32)):
             extra.append(wavelet_case(lmin, lmax, nzw, device=device))
 
@@ -648,7 +675,7 @@ def bench_ours_uniform(args):
                 "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,
             })
         for lmax in (6, 7, 8):
-            extra.append(elliptic_case(lmax))
+            extra.append(elliptic_case(lmax, eval_seeds=16 if lmax == 8 else None))
         for (lmin, lmax, nzw) in ((5, 7, 16), (5, 8, 32)):
             extra.append(wavelet_case(lmin, lmax, nzw, device=device))
 
@@ -887,7 +914,8 @@ def main():
     elif args.wavelets_only:
         bench_wavelets(args)
     elif args.elliptic_only:
-        print(json.dumps(elliptic_case(args.level, epochs=args.learned_epochs, nvtx=True)))
+        print(json.dumps(elliptic_case(args.level, epochs=args.learned_epochs, nvtx=True,
+                                       eval_seeds=16 if args.level == 8 else None)))
     else:
         bench_ours(args)
 

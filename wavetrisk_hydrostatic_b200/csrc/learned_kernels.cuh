@@ -349,24 +349,80 @@ __global__ void k_fcg_neg(int ns, const int* __restrict__ slot, const double* __
   if (s < ns) z[slot[s]] = -r[slot[s]];
 }
 
-// New direction, truncated to one previous direction:
-// beta = <z, Lp'> / <p', Lp'>, p = z - beta p', Lp = Lz - beta Lp';
-// on a restart (FCG_DELTA_PREV == 0) p = z, Lp = Lz.
-__global__ void k_fcg_dir(int ns, const int* __restrict__ slot, const double* __restrict__ fcg,
-                          const double* __restrict__ z, const double* __restrict__ lz, double* __restrict__ p,
-                          double* __restrict__ lp) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  const double dprev = fcg[FCG_DELTA_PREV];
-  const int id = slot[s];
-  if (dprev == 0.0) {
-    p[id] = z[id];
-    lp[id] = lz[id];
-    return;
+// New direction, truncated to one previous direction: beta = <z, Lp'> / <p', Lp'>,
+// p = z - beta p', Lp = Lz - beta Lp' (on a restart, FCG_DELTA_PREV == 0: p = z,
+// Lp = Lz); fused with the two inner products the step needs, block partials of
+// <p, r>_W and <p, Lp>_W (W = 1 / hinv) into pa and pb.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_fcg_dir_dots(int ns, const int* __restrict__ slot,
+                                                     const double* __restrict__ fcg, const double* __restrict__ z,
+                                                     const double* __restrict__ lz, const double* __restrict__ r,
+                                                     const double* __restrict__ hinv, double* __restrict__ p,
+                                                     double* __restrict__ lp, double* __restrict__ pa,
+                                                     double* __restrict__ pb) {
+  __shared__ double sa[NT / 32], sb[NT / 32];
+  const int s = blockIdx.x * NT + threadIdx.x;
+  double va = 0.0, vb = 0.0;
+  if (s < ns) {
+    const double dprev = fcg[FCG_DELTA_PREV];
+    const int id = slot[s];
+    double pn, lpn;
+    if (dprev == 0.0) {
+      pn = z[id];
+      lpn = lz[id];
+    } else {
+      const double beta = fcg[FCG_ZLP] / dprev;
+      pn = z[id] - beta * p[id];
+      lpn = lz[id] - beta * lp[id];
+    }
+    p[id] = pn;
+    lp[id] = lpn;
+    va = pn * r[id] / hinv[id];
+    vb = pn * lpn / hinv[id];
   }
-  const double beta = fcg[FCG_ZLP] / dprev;
-  p[id] = z[id] - beta * p[id];
-  lp[id] = lz[id] - beta * lp[id];
+  for (int o = 16; o > 0; o >>= 1) {
+    va += __shfl_down_sync(0xffffffffu, va, o);
+    vb += __shfl_down_sync(0xffffffffu, vb, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sa[threadIdx.x >> 5] = va;
+    sb[threadIdx.x >> 5] = vb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < NT / 32; ++q) {
+      a += sa[q];
+      b += sb[q];
+    }
+    pa[blockIdx.x] = a;
+    pb[blockIdx.x] = b;
+  }
+}
+
+// out[0] = sum of pa, out[1] = sum of pb (nb partials each, fixed order).
+__global__ void k_lp_sum2(const double* __restrict__ pa, const double* __restrict__ pb, int nb,
+                          double* __restrict__ out0, double* __restrict__ out1) {
+  __shared__ double sa[256], sb[256];
+  double a = 0.0, b = 0.0;
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+    a += pa[q];
+    b += pb[q];
+  }
+  sa[threadIdx.x] = a;
+  sb[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      sa[threadIdx.x] += sa[threadIdx.x + o];
+      sb[threadIdx.x] += sb[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *out0 = sa[0];
+    *out1 = sb[0];
+  }
 }
 
 // Step: alpha = <p, r> / <p, Lp>; u += alpha p; r -= alpha Lp.  <p, Lp> must be

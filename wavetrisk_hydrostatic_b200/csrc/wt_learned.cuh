@@ -25,7 +25,7 @@ struct LPNet {
   float* own = nullptr; // ns: 1 on owned nodes, 0 at the pole slots
   float *w = nullptr, *wr = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
   float *x = nullptr, *h1 = nullptr, *h2 = nullptr, *y = nullptr, *dy = nullptr, *dh1 = nullptr, *dh2 = nullptr;
-  double *rs = nullptr, *fcg = nullptr, *partial = nullptr, *losses = nullptr;
+  double *rs = nullptr, *fcg = nullptr, *partial = nullptr, *partial2 = nullptr, *losses = nullptr;
   double *rc = nullptr, *ec = nullptr;  // one compact pair (grad / infer)
   double *pr = nullptr, *pe = nullptr, *pscale = nullptr;  // training pairs
   int npairs = 0;
@@ -147,6 +147,7 @@ int lp_build(Ell& E, uint64_t seed) {
   al(&N->rs, 1);
   al(&N->fcg, FCG_N);
   al(&N->partial, N->nbd());
+  al(&N->partial2, N->nbd());
   al(&N->losses, 1);
   al(&N->rc, ns);
   al(&N->ec, ns);
@@ -358,9 +359,10 @@ void fcg_iteration(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
     k_lp_sum<<<1, 256, 0, st>>>(N.partial, N.nbd(), N.fcg + slotv, 0, 1.0);
   };
   wdot(N.z, N.lp, FCG_ZLP);
-  k_fcg_dir<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.fcg, N.z, N.lz, N.p, N.lp);
-  wdot(N.p, N.r, FCG_PR);
-  wdot(N.p, N.lp, FCG_DELTA);
+  // the new direction and <p, r>, <p, Lp> in one pass
+  k_fcg_dir_dots<LP_DOT><<<N.nbd(), LP_DOT, 0, st>>>(ns, N.slot, N.fcg, N.z, N.lz, N.r, hinv, N.p, N.lp, N.partial,
+                                                     N.partial2);
+  k_lp_sum2<<<1, 256, 0, st>>>(N.partial, N.partial2, N.nbd(), N.fcg + FCG_PR, N.fcg + FCG_DELTA);
   k_fcg_step<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.slot, N.fcg, N.p, N.lp, E.u.lv[q], N.r);
   EllLev V = E.view(l);
   const unsigned g = nb(10 * E.m(l) * E.m(l));

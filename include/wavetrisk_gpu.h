@@ -4,7 +4,7 @@
  * mask, multigrid free-surface solve) on the padded lozenge layout.
  *
  * Every entry point is plain C: pointers, sizes and an int status.  A Fortran
- * host binds them with ISO_C_BINDING.  All arrays are
+ * host binds them with ISO_C_BINDING (bind(C) interfaces).  All arrays are
  * double precision unless stated otherwise.
  *
  * Layout of one grid level l (n = 2^l nodes per lozenge side, P = n + 4):

@@ -9,7 +9,7 @@ links or calls it.
 Parity status: unpinned against the reference binary (the reference is Fortran
 and no Fortran compiler exists in the build container); pinned instead by the
 properties the reference relies on (conservation, identities, analytic cases),
-checked in tests/test_oracle.py.
+checked in tests/test_*_oracle.py and tests/test_grid.py.
 """
 from __future__ import annotations
 

@@ -164,6 +164,56 @@ def test_solvers_interleaved_keep_converging(hier):
     S.close()
 
 
+def test_graph_solvers_after_odd_reference_sweeps(hier):
+    """FMG with one pre-sweep (an odd number of u/tmp swaps on every level
+    above level_start) and SRJ stopped after an odd sweep count leave the
+    solver's u, tmp, res and au pointers rotated.  Every captured-graph solver
+    run after them, twice each and with odd V-cycle sweep counts, must give
+    the same solution as on a handle that never ran the reference path."""
+    levels, topos, off = hier
+    f = np.zeros(off[-1])
+    f[off[-2]:off[-1]] = elliptic_rhs(levels[-1], seed=6)
+    kw = dict(down_iter=3, up_iter=3, coarse_iter=5)
+    graph_methods = ("mixed", "mg64", "fcg_mg", "fcg_learned")
+
+    def fresh(params=None):
+        S = EllipticSolver(levels, topos)
+        S.upload(f=f)
+        S.restrict()
+        _, fr = S.download()
+        S.learned_setup(1)
+        if params is None:
+            S.learned_train(n_rhs=2, cycles=2, epochs=2, down_iter=3, up_iter=3, coarse_iter=5)
+        else:
+            S.learned_params(set_to=params)     # the same network on both handles
+        return S, fr
+
+    S0, fr = fresh()
+    params = S0.learned_params()
+    clean = {}
+    for name in graph_methods:
+        S0.upload(u=np.zeros(off[-1]), f=fr)
+        rep = S0.solve(solver_opts(name, 1e-10, **kw))
+        assert rep.status == 0 and rep.true_rel_residual <= 1e-10, name
+        clean[name] = S0.download()[0][off[-2]:off[-1]].copy()
+    S0.close()
+
+    S, fr = fresh(params)
+    disturb = [("fmg", dict(pre_iter=1, post_iter=2, max_vcycle=50, coarse_iter=300)),
+               ("srj", dict(max_srj_iter=7, coarse_iter=300))]
+    for dname, dk in disturb:
+        S.upload(u=np.zeros(off[-1]), f=fr)
+        S.solve(solver_opts(dname, 1e-10, **dk))
+        for name in graph_methods:
+            for _ in range(2):
+                S.upload(u=np.zeros(off[-1]), f=fr)
+                rep = S.solve(solver_opts(name, 1e-10, **kw))
+                assert rep.status == 0 and rep.true_rel_residual <= 1e-10, (dname, name, rep.true_rel_residual)
+                u = S.download()[0][off[-2]:off[-1]]
+                assert np.array_equal(u, clean[name]), (dname, name, rel(u, clean[name]))
+    S.close()
+
+
 def test_autotune_picks_a_converging_candidate_and_keeps_u_f(hier):
     levels, topos, off = hier
     S = EllipticSolver(levels, topos)

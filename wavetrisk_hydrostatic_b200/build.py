@@ -7,6 +7,7 @@ Both compile without a GPU.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -59,18 +60,17 @@ def build_lib(force: bool = False) -> str:
     deps = _deps()
     if not force and not _newer(LIB, deps):
         return LIB
-    objs = []
+    jobs = []
     for src in CU_SOURCES:
         path = os.path.join(CSRC, src)
-        if not os.path.exists(path):
-            continue
-        obj = os.path.join(BUILD, src + ".o")
-        _run([NVCC, *ARCH, *NVCC_FLAGS, "-c", path, "-o", obj])
-        objs.append(obj)
+        if os.path.exists(path):
+            jobs.append([NVCC, *ARCH, *NVCC_FLAGS, "-c", path, "-o", os.path.join(BUILD, src + ".o")])
     for src in CPP_SOURCES:
-        obj = os.path.join(BUILD, src + ".o")
-        _run(["g++", *CXX_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj])
-        objs.append(obj)
+        jobs.append(["g++", *CXX_FLAGS, "-c", os.path.join(CSRC, src), "-o", os.path.join(BUILD, src + ".o")])
+    # the translation units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+        list(ex.map(_run, jobs))
+    objs = [j[-1] for j in jobs]
     tmp = LIB + ".tmp"
     _run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"])
     shutil.move(tmp, LIB)

@@ -53,7 +53,7 @@ struct Ell {
   double* scal = nullptr;  // device scalars
   cudaGraphExec_t cycle_exec[2] = {nullptr, nullptr};  // captured correction cycles (FP32, FP64)
   int cycle_key[2] = {-1, -1};
-  const double* cycle_res[2] = {nullptr, nullptr};  // res buffer of level_end each cycle graph reads
+  std::vector<const void*> cycle_ptrs[2];  // rotating() at each cycle graph's capture
   int nbmax = 0;
   std::vector<void*> allocs;
   void* lp = nullptr;  // learned preconditioner (wt_learned.cuh)
@@ -66,7 +66,56 @@ struct Ell {
   }
   int m(int l) const { return L[l - ls].n + 1; }
   cudaStream_t s() const { return h->stream; }
+
+  // The buffers whose roles the solvers rotate by swapping pointers: jacobi's
+  // u/tmp and corr/tmp ping-pong, v_cycle's res/au swap and the FP32 cycle's
+  // c32/t32 ping-pong.  A captured graph holds the addresses it was captured
+  // with, so it may be replayed only while these are as they were then.
+  std::vector<const void*> rotating() const {
+    std::vector<const void*> v;
+    for (const MField* F : {&u, &tmp, &corr, &res, &au})
+      for (double* p : F->lv) v.push_back(p);
+    for (const MField* F : {&c32, &t32})
+      for (float* p : F->lvf) v.push_back(p);
+    return v;
+  }
+  void set_rotating(const std::vector<const void*>& v) {
+    size_t k = 0;
+    for (MField* F : {&u, &tmp, &corr, &res, &au})
+      for (double*& p : F->lv) p = const_cast<double*>(static_cast<const double*>(v[k++]));
+    for (MField* F : {&c32, &t32})
+      for (float*& p : F->lvf) p = const_cast<float*>(static_cast<const float*>(v[k++]));
+  }
 };
+
+// Captures body() on the solver's stream into ex.  The sweeps inside body()
+// swap pointers while they are captured; afterwards the host-side pointers are
+// put back to what they were at the start, which is the state every replay
+// of the graph starts from, and that state is stored in *ptrs as the graph's
+// key (a replay is valid while E.rotating() == *ptrs).
+template <class Body>
+int capture_graph(Ell& E, cudaGraphExec_t& ex, std::vector<const void*>& ptrs, const char* what, Body body) {
+  if (ex) {
+    cudaGraphExecDestroy(ex);
+    ex = nullptr;
+  }
+  std::vector<const void*> start = E.rotating();
+  cudaGraph_t g;
+  cudaError_t ce = cudaStreamBeginCapture(E.s(), cudaStreamCaptureModeThreadLocal);
+  if (ce != cudaSuccess) return wt_handle_fail(what, ce);
+  body();
+  ce = cudaStreamEndCapture(E.s(), &g);
+  E.set_rotating(start);
+  if (ce != cudaSuccess) return wt_handle_fail(what, ce);
+  ce = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    ex = nullptr;
+    return wt_handle_fail(what, ce);
+  }
+  ptrs = std::move(start);
+  return WT_OK;
+}
 
 template <class T>
 int dalloc(Ell& E, T** p, int64_t n) {

@@ -178,31 +178,26 @@ int mixed_ir(Ell& E, const wt_solver_opts& o, wt_solver_report& rep, bool fp64 =
     if (it == 0) rep.nrm_res_init[q] = err;
     if (err <= o.ir_tol || it == o.ir_max) break;
     // The correction cycle has no host decision: it is captured once per
-    // configuration and replayed as one graph launch per refinement step.  The
-    // residual above is written through the current res pointer, which the
-    // reference-path V-cycle (v_cycle) swaps with au: a graph captured with
-    // the other buffer is captured again.
-    cudaGraphExec_t& ex = E.cycle_exec[fp64 ? 1 : 0];
+    // schedule and replayed as one graph launch per refinement step, while the
+    // buffers it was captured with still hold their roles (the reference-path
+    // solvers FMG and SRJ swap u/tmp and res/au between calls).
+    const int w = fp64 ? 1 : 0;
+    cudaGraphExec_t& ex = E.cycle_exec[w];
     const int key = o.down_iter * 1000000 + o.up_iter * 10000 + o.coarse_iter;
-    if (!ex || E.cycle_key[fp64 ? 1 : 0] != key || E.cycle_res[fp64 ? 1 : 0] != E.res.lv[q]) {
-      if (ex) { cudaGraphExecDestroy(ex); ex = nullptr; }
-      cudaGraph_t g;
-      cudaStreamBeginCapture(E.s(), cudaStreamCaptureModeThreadLocal);
-      if (fp64) {
-        vcycle64(E, o);
-        k_axpy_d<<<nb(NN), TPB, 0, E.s()>>>(NN, E.u.lv[q], E.corr.lv[q]);
-      } else {
-        k_d2f<<<nb(NN), TPB, 0, E.s()>>>(NN, E.res.lv[q], E.r32.lvf[q]);
-        vcycle32(E, o);
-        k_axpy_f2d<<<nb(NN), TPB, 0, E.s()>>>(NN, E.u.lv[q], E.c32.lvf[q]);
-      }
-      cudaError_t ce = cudaStreamEndCapture(E.s(), &g);
-      if (ce != cudaSuccess) return wt_handle_fail("cycle capture", ce);
-      ce = cudaGraphInstantiate(&ex, g, 0);
-      cudaGraphDestroy(g);
-      if (ce != cudaSuccess) return wt_handle_fail("cycle instantiate", ce);
-      E.cycle_key[fp64 ? 1 : 0] = key;
-      E.cycle_res[fp64 ? 1 : 0] = E.res.lv[q];
+    if (!ex || E.cycle_key[w] != key || E.cycle_ptrs[w] != E.rotating()) {
+      E.cycle_key[w] = -1;
+      int rc = capture_graph(E, ex, E.cycle_ptrs[w], "cycle graph", [&] {
+        if (fp64) {
+          vcycle64(E, o);
+          k_axpy_d<<<nb(NN), TPB, 0, E.s()>>>(NN, E.u.lv[q], E.corr.lv[q]);
+        } else {
+          k_d2f<<<nb(NN), TPB, 0, E.s()>>>(NN, E.res.lv[q], E.r32.lvf[q]);
+          vcycle32(E, o);
+          k_axpy_f2d<<<nb(NN), TPB, 0, E.s()>>>(NN, E.u.lv[q], E.c32.lvf[q]);
+        }
+      });
+      if (rc != WT_OK) return rc;
+      E.cycle_key[w] = key;
     }
     cudaError_t le = cudaGraphLaunch(ex, E.s());
     if (le != cudaSuccess) return wt_handle_fail("cycle launch", le);

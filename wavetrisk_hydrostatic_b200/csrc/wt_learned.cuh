@@ -37,6 +37,7 @@ struct LPNet {
   double inv_area = 1.0;  // 1 / sum of the node areas 1 / hex_inv
   cudaGraphExec_t it_exec[4] = {nullptr, nullptr, nullptr, nullptr};
   int it_key[4] = {-1, -1, -1, -1};
+  std::vector<const void*> it_ptrs[4];  // Ell::rotating() at each graph's capture
   std::vector<void*> allocs, pair_allocs;
   int nbd() const { return (ns + LP_DOT - 1) / LP_DOT; }
 };
@@ -373,19 +374,12 @@ void fcg_iteration(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
 int fcg_launch(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
   cudaGraphExec_t& ex = N.it_exec[pre];
   const int key = pre != PRE_NONE ? o.down_iter * 1000000 + o.up_iter * 10000 + o.coarse_iter : 0;
-  if (!ex || N.it_key[pre] != key) {
-    if (ex) {
-      cudaGraphExecDestroy(ex);
-      ex = nullptr;
-    }
-    cudaGraph_t g;
-    cudaStreamBeginCapture(E.s(), cudaStreamCaptureModeThreadLocal);
-    fcg_iteration(E, N, o, pre);
-    cudaError_t ce = cudaStreamEndCapture(E.s(), &g);
-    if (ce != cudaSuccess) return wt_handle_fail("fcg capture", ce);
-    ce = cudaGraphInstantiate(&ex, g, 0);
-    cudaGraphDestroy(g);
-    if (ce != cudaSuccess) return wt_handle_fail("fcg instantiate", ce);
+  // re-captured when the schedule changed or a reference-path solver has
+  // rotated u, res or the V-cycle's work buffers since the capture
+  if (!ex || N.it_key[pre] != key || N.it_ptrs[pre] != E.rotating()) {
+    N.it_key[pre] = -1;
+    int rc = capture_graph(E, ex, N.it_ptrs[pre], "fcg graph", [&] { fcg_iteration(E, N, o, pre); });
+    if (rc != WT_OK) return rc;
     N.it_key[pre] = key;
   }
   cudaError_t le = cudaGraphLaunch(ex, E.s());

@@ -11,6 +11,7 @@
 // cudaFree, no allocating library routine.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 
 #include "../../include/wavetrisk_gpu.h"
@@ -28,8 +29,12 @@ constexpr int NOALLOC_MAX_BLOCKS = 4096;   // 32 KiB of partial sums: levels up 
 // (different streams) overwrite each other's partials and race.
 static __device__ __align__(256) double g_noalloc_partial[NOALLOC_MAX_BLOCKS];
 
+// Device address of g_noalloc_partial per device, looked up on the first call
+// made with that device current.  Two host threads making their first call on
+// one device at once may both look it up; each stores the same address, and
+// the atomics make that a benign race instead of a data race.
 constexpr int MAX_DEVICES = 64;
-double* g_partial_addr[MAX_DEVICES] = {nullptr};
+std::atomic<double*> g_partial_addr[MAX_DEVICES] = {};
 
 __global__ void k_noalloc_sq(int n, int P, int nd, const int* __restrict__ nsrc, const double* __restrict__ s,
                              double* __restrict__ partial) {
@@ -96,18 +101,18 @@ extern "C" int wt_elliptic_l2_noalloc(int level, int domain_level, const int* ns
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return wt_handle_fail("wt_elliptic_l2_noalloc: cudaGetDevice", e);
   if (dev < 0 || dev >= MAX_DEVICES) return WT_ERR_ARG;
-  if (!g_partial_addr[dev]) {
+  double* partial = g_partial_addr[dev].load(std::memory_order_acquire);
+  if (!partial) {
     // The array's name in host code is only a host-side stand-in; the device
     // address is looked up once per device, with that device current.
-    double* p = nullptr;
-    e = cudaGetSymbolAddress((void**)&p, g_noalloc_partial);
+    e = cudaGetSymbolAddress((void**)&partial, g_noalloc_partial);
     if (e != cudaSuccess) return wt_handle_fail("wt_elliptic_l2_noalloc: cudaGetSymbolAddress", e);
-    g_partial_addr[dev] = p;
+    g_partial_addr[dev].store(partial, std::memory_order_release);
   }
   const int nd = (n >> domain_level) > 0 ? (n >> domain_level) : 1;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  k_noalloc_sq<<<(unsigned)nblocks, NOALLOC_TPB, 0, s>>>(n, P, nd, nsrc, field, g_partial_addr[dev]);
-  k_noalloc_final<<<1, 256, 0, s>>>(g_partial_addr[dev], (int)nblocks, result);
+  k_noalloc_sq<<<(unsigned)nblocks, NOALLOC_TPB, 0, s>>>(n, P, nd, nsrc, field, partial);
+  k_noalloc_final<<<1, 256, 0, s>>>(partial, (int)nblocks, result);
   e = cudaGetLastError();
   if (e != cudaSuccess) return wt_handle_fail("wt_elliptic_l2_noalloc: launch", e);
   return WT_OK;

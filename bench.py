@@ -1,24 +1,28 @@
-"""Benchmark: simulated days per wall-clock hour of the TRiSK RK4 stepper.
+"""Benchmark: simulated days per wall-clock hour of the adaptive ocean time step.
 
-Workload (N=1): uniform icosahedral J7 grid (163,842 cells, 491,520 edges),
-16 Boussinesq layers -- the adaptive J4..J7, 16-layer run with every point
-active (wavelet adaptivity is not part of this stepper yet) -- flat 4000 m
-bottom, zonal jet + seeded white-noise free surface, explicit RK4 with
-dt = 300 s (the reference's time_step ->
-dt_step => RK4 -> trend_ml path).  A "step" is one RK4 step: four trend
-evaluations, each fused with its sub-step (3 kernels per stage, ghosts read
-through remap tables).  With --gpus N>1 every rank advances its own ensemble
-member (independent seeds, no collective): weak scaling, value = member-days
-per hour summed over ranks.
+Workload (N=1, the default): the adaptive run J5..J9 (2,621,442 cells at J9),
+32 Boussinesq layers, every patch of the hierarchy present (a fully refined
+tree; masks, compression and adapt every step), flat 4000 m bottom with a
+seeded Gaussian seamount (2000 m, 50 km), zonal jet + 8 seeded Gaussian bumps
+(300 km, 0.05 m) in the layer thicknesses, wavelet threshold tolerance 5e-3,
+explicit RK4 with dt = 37.5 s (150 s at J7 scaled with the finest grid
+spacing, the reference's CFL rule dt = cfl dx_min / c).  One step is the
+reference's time_step (src/main.f90:405-444): RK4 of the hierarchy with
+WT_after_step per stage, adapt's mask sequence and compression, and the
+inverse transform, replayed as one captured CUDA graph.  With --gpus N>1
+every rank advances its own ensemble member (independent seeds, no
+collective): weak scaling, value = member-days per hour summed over ranks.
 
 --impl reference times the CPU restatement of the reference's path (the
 reference is Fortran; no Fortran compiler exists on the build or GPU hosts)
-on the host cores, one worker thread per lozenge domain up to the core count.
+on the host cores, on bounded samples of the same workload (the whole step
+on every level with a subset of the layers, extrapolated to 32 layers).
 
---kernels-only times the device-resident stepper alone on --level/--nz (no
-CPU baseline, host-buffer path or extra workloads); it is the small case the
-kernel profiles are captured on.  --wavelets-only does the same for the
-wavelet transforms on the hierarchy --level-2 .. --level.
+--mode uniform times the single-level TRiSK RK4 stepper (uniform J7 x 16
+by default).  --kernels-only times that stepper alone on --level/--nz (the
+small case kernel profiles are captured on); --wavelets-only does the same
+for the wavelet transforms on the hierarchy --level-2 .. --level;
+--elliptic-only runs the free-surface solve comparison on J5..--level.
 """
 from __future__ import annotations
 
@@ -34,9 +38,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 DT = 300.0      # uniform stepper (explicit RK4, J5 config)
-DT_AD = 150.0   # adaptive run
 TOL_AD = 5e-3   # wavelet threshold tolerance of the adaptive run
 DAY = 86400.0
+
+
+def dt_adaptive(lmax):
+    """Explicit RK4 step of the adaptive run: 150 s at J7, scaled with the
+    finest grid spacing (dt = cfl dx_min / c with the same cfl at every
+    max_level, initialize_dt_viscosity_case in test/seamount/test_case_module.f90)."""
+    return 150.0 * 2.0 ** (7 - lmax)
 
 
 def sim_days_per_hour(steps, seconds, dt=DT):
@@ -50,9 +60,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--mode", default="adaptive", choices=["adaptive", "uniform"])
-    p.add_argument("--lmin", type=int, default=4)
-    p.add_argument("--level", type=int, default=7)
-    p.add_argument("--nz", type=int, default=16)
+    p.add_argument("--lmin", type=int, default=None, help="min level of the adaptive run (default 5)")
+    p.add_argument("--level", type=int, default=None, help="max level (default 9 adaptive, 7 uniform)")
+    p.add_argument("--nz", type=int, default=None, help="layers (default 32 adaptive, 16 uniform)")
     p.add_argument("--no-extra", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--kernels-only", action="store_true")
@@ -64,7 +74,15 @@ def parse():
     p.add_argument("--trace", default=None, metavar="PATH",
                    help="record a CUDA kernel timeline of --steps adaptive steps (after --warmup) into PATH "
                         "(Chrome trace) and print its summary instead of the bench line")
-    return p.parse_args()
+    a = p.parse_args()
+    adaptive = a.mode == "adaptive" and not (a.kernels_only or a.wavelets_only or a.elliptic_only)
+    if a.lmin is None:
+        a.lmin = 5
+    if a.level is None:
+        a.level = 9 if adaptive else 7
+    if a.nz is None:
+        a.nz = 32 if adaptive else 16
+    return a
 
 
 class ClockSampler:
@@ -320,9 +338,11 @@ def workload_config(args, world=1):
         return {
             "workload": f"adaptive run J{args.lmin}..J{args.level} ({cells} cells at J{args.level}), {args.nz} "
                         f"Boussinesq layers, every patch of the hierarchy present (fully refined tree; masks and "
-                        f"adapt every step), jet + 8 seeded Gaussian bumps (300 km, 0.05 m), tol {TOL_AD} "
-                        f"thresholds, explicit RK4 dt={DT_AD:g} s, WT_after_step per stage",
-            "min_level": args.lmin, "max_level": args.level, "layers": args.nz, "dt_s": DT_AD, "tol": TOL_AD,
+                        f"adapt every step), 4000 m bottom with a seeded Gaussian seamount (2000 m, 50 km), jet + "
+                        f"8 seeded Gaussian bumps (300 km, 0.05 m), tol {TOL_AD} thresholds, explicit RK4 "
+                        f"dt={dt_adaptive(args.level):g} s, WT_after_step per stage",
+            "min_level": args.lmin, "max_level": args.level, "layers": args.nz, "dt_s": dt_adaptive(args.level),
+            "tol": TOL_AD,
             "parallelism": f"replicas x{world} (independent ensemble members)" if world > 1 else "single GPU",
             "l2": "flushed (256 MB write) between timed steps, outside the timed region",
         }
@@ -417,24 +437,33 @@ def algorithmic_bytes_trend_ml(level, nz, n_on=None, n_own=None):
     return nz * (inner * 2 * 8 + own * 3 * 8 + on * 12 * 8 + NN * 10 * 8) + inner * 4 + on * 10 * 8
 
 
+def adaptive_states(levels, nz, seed, ph):
+    """Initial states of the adaptive run on every level: seamount bathymetry,
+    layers following it, jet and bumps (the same seeds on every level)."""
+    from wavetrisk_hydrostatic_b200.cases import bump_state, seamount_topography
+
+    return [bump_state(g, nz, seed=seed, ph=ph, topo=seamount_topography(g, seed=seed)) for g in levels]
+
+
 def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile=True):
-    """The adaptive run on the fully refined hierarchy lmin..lmax: jet +
-    8 Gaussian bumps, tol 5e-3 thresholds (initialize_thresholds_case), one
-    step = RK4 of the hierarchy (dt 150 s) + adapt + inverse transform.
-    CUDA-event time per step on the handle's stream."""
+    """The adaptive run on the fully refined hierarchy lmin..lmax (seamount,
+    jet + 8 Gaussian bumps, tol 5e-3 thresholds of initialize_thresholds_case),
+    one step = RK4 of the hierarchy + adapt + inverse transform.  CUDA-event
+    time per step on the handle's stream."""
     import numpy as np
     import torch
 
     from wavetrisk_hydrostatic_b200 import Grid, OceanParams
     from wavetrisk_hydrostatic_b200 import _native as Nt
     from wavetrisk_hydrostatic_b200.adaptive import AdaptiveOcean
-    from wavetrisk_hydrostatic_b200.cases import bump_state
 
+    DT_AD = dt_adaptive(lmax)
     ph = OceanParams()
     G = Grid(lmin, lmax, radius=6371e3)
     levels = [G.level(l) for l in range(lmin, lmax + 1)]
-    states = [bump_state(g, nz, seed=seed, ph=ph) for g in levels]
+    states = adaptive_states(levels, nz, seed, ph)
     model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=TOL_AD)
+    del states
     dev = model.dev
     stream = torch.cuda.ExternalStream(dev.stream, device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
@@ -465,24 +494,22 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
     if profile:
         pm = (Nt.C.c_double * 7)()
         pc = (Nt.C.c_int * 7)()
-        Nt.check("wt_profile_rk4_multi", Nt.lib().wt_profile_rk4_multi(dev.h, DT_AD, 2, pm, pc))
+        Nt.check("wt_profile_rk4_multi", Nt.lib().wt_profile_rk4_multi(dev.h, DT_AD, 1, pm, pc))
         names = ["step1_top", "step1_coarse", "restrict", "trend_ml_top", "trend_ml_coarse", "rk_sub", "wt_after_step"]
         out["phase_ms"] = {names[p]: pm[p] for p in range(7)}
         out["phase_count_per_step"] = {names[p]: pc[p] for p in range(7)}
     if e2e:
-        pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
-        bufs = []
-        for g in levels:
-            bufs.append({"mass": pin((nz, g.NN)), "temp": pin((nz, g.NN)), "velo": pin((nz, 3 * g.NN)),
-                         "mask_n": torch.empty(g.NN, dtype=torch.int32, pin_memory=True).numpy(),
-                         "mask_e": torch.empty(3 * g.NN, dtype=torch.int32, pin_memory=True).numpy()})
+        # The host keeps the finest level's prognostic state and the masks of
+        # every level (its masks of record): each step uploads that state from
+        # pinned host buffers, steps, and downloads the new state and all masks.
+        pin = lambda shape, dt=torch.float64: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+        top = levels[-1]
+        sbuf = {"mass": pin((nz, top.NN)), "temp": pin((nz, top.NN)), "velo": pin((nz, 3 * top.NN))}
+        mbuf = [{"mask_n": pin(g.NN, torch.int32), "mask_e": pin(3 * g.NN, torch.int32)} for g in levels]
         ids = dev.FIELDS
         L = Nt.lib()
-
-        # one batch each way per step (wt_upload_fields / wt_download_fields), finest level first
-        up = [(g.level, k, b[k]) for g, b in reversed(list(zip(levels, bufs))) for k in ("mass", "temp", "velo")]
-        dn = [(g.level, k, b[k]) for g, b in reversed(list(zip(levels, bufs)))
-              for k in ("mass", "temp", "velo", "mask_n", "mask_e")]
+        up = [(lmax, k, sbuf[k]) for k in ("mass", "temp", "velo")]
+        dn = up + [(g.level, k, b[k]) for g, b in reversed(list(zip(levels, mbuf))) for k in ("mask_n", "mask_e")]
 
         def batch(items):
             n = len(items)
@@ -508,8 +535,8 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
         t1 = time.perf_counter()
         out["e2e_s"] = t1 - t0
         out["e2e_steps"] = nsteps_e2e
-        out["h2d_bytes_per_step"] = int(sum(b[k].nbytes for b in bufs for k in ("mass", "temp", "velo")))
-        out["d2h_bytes_per_step"] = int(sum(b[k].nbytes for b in bufs for k in b))
+        out["h2d_bytes_per_step"] = int(sum(a.nbytes for _, _, a in up))
+        out["d2h_bytes_per_step"] = int(sum(a.nbytes for _, _, a in dn))
     out["cells_finest"] = 10 * 4 ** lmax + 2
     model.close()
     return out
@@ -557,6 +584,7 @@ def bench_ours(args):
     clocks = sampler.stop() if sampler else None
     ms_max = allreduce_max(pg, r["ms_total"], device)
     e2e_max = allreduce_max(pg, r["e2e_s"], device)
+    DT_AD = dt_adaptive(args.level)
     value = world * sim_days_per_hour(args.steps, ms_max / 1e3, DT_AD)
     e2e_value = world * sim_days_per_hour(r["e2e_steps"], e2e_max, DT_AD)
 
@@ -608,12 +636,13 @@ def bench_ours(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f64",
-            "data": "synthetic (seeded jet + Gaussian bumps)",
+            "data": "synthetic (seeded seamount, jet and Gaussian bumps)",
             "config": workload_config(args, world),
             "e2e": {"value": e2e_value, "unit": "simulated days per wall-clock hour",
                     "h2d_bytes_per_step": r["h2d_bytes_per_step"], "d2h_bytes_per_step": r["d2h_bytes_per_step"],
                     "path": "C-ABI wt_upload_fields / wt_adaptive_step / wt_download_fields, pinned host "
-                            "buffers: every level's state in, every level's state and masks out, every step"},
+                            "buffers: the finest level's state (every layer) in, that state and every level's "
+                            "masks out, every step"},
             "gpu_launches": adaptive_launches(L) * args.steps,
             "roofline": {"bound": "hbm", "kernel": "k_trend_tma<MODE_ML> (level_end)", "achieved": ach, "peak": hbm,
                          "unit": "GB/s", "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
@@ -731,11 +760,12 @@ def cpu_baseline(args, quick=False):
     import numpy as np
 
     import oracle
-    from wavetrisk_hydrostatic_b200 import Grid, OceanParams, jet_state
+    from oracle.grid import Grid as OGrid
+    from wavetrisk_hydrostatic_b200.cases import OceanParams, jet_state
 
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
-    g = Grid(args.level, args.level, radius=6371e3).level(args.level)
+    g = OGrid(args.level, args.level, radius=6371e3).level(args.level)
     ph = OceanParams()
     st = jet_state(g, args.nz, seed=1, ph=ph)
     oracle.rk4(g, args.nz, ph, st, DT, 1)
@@ -753,62 +783,134 @@ def cpu_baseline(args, quick=False):
             "sample": f"{steps} RK4 steps of the same workload ({t_used:.1f} s of CPU time)"}
 
 
-def cpu_baseline_adaptive(args, quick=False):
-    """The oracle's adaptive step on the same hierarchy (multi-level trend,
-    RK4, WT_after_step, adapt's mask sequence, compression, inverse
-    transform) on all host threads, timed over whole steps until the budget is
-    used."""
-    import numpy as np
+class AdaptiveCpuSampler:
+    """CPU restatement (oracle) of the adaptive step on the workload's full
+    hierarchy, timed on bounded samples.  A sample is one whole adaptive step
+    (multi-level trend and RK4 with WT_after_step per stage, adapt's mask
+    sequence, compression, inverse transform) on every level and every node,
+    computed with `nz_s` of the workload's layers.  The step's cost is
+    A + B nz (the trend, RK and wavelet work is per layer, the mask sequence
+    and the per-node set-up are not); B is calibrated from one step at
+    nz_s and one at 2 nz_s, and a sample's time t(nz_s) is extrapolated to
+    t(nz) = t(nz_s) + (nz - nz_s) B.  The oracle's wavelet transforms run one
+    layer per worker thread, so at 2-4 layers their time grows less than in
+    proportion and B errs low: the extrapolated CPU time is if anything an
+    underestimate.  Geometry and states come from the oracle-side builders."""
 
-    import oracle
-    from oracle.wavelet import Hierarchy
-    from wavetrisk_hydrostatic_b200 import Grid, OceanParams
-    from wavetrisk_hydrostatic_b200.cases import bump_state
+    def __init__(self, lmin, lmax, nz, nz_s=2, seed=1):
+        import numpy as np
 
-    threads = os.cpu_count() or 1
-    oracle.set_threads(threads)
-    ph = OceanParams()
-    lmin, lmax, nz = args.lmin, args.level, args.nz
-    G = Grid(lmin, lmax, radius=6371e3)
-    levels = [G.level(l) for l in range(lmin, lmax + 1)]
-    states = [bump_state(g, nz, seed=1, ph=ph) for g in levels]
-    keys = (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v"))
-    dz = states[-1]["mean_m"][:, 0] / ph.ref_density
-    thr = TOL_AD * np.stack([ph.ref_density * dz, np.full(nz, 1e16), np.full(nz, 1.0)])
-    H = Hierarchy(levels, nz)
-    for name, key in keys:
-        H.set(lmax, key, states[-1][name])
-    H.forward()
-    H.mask_build(thr, 0, lmax)
-    H.compress()
-    H.inverse()
-    budget = args.cpu_seconds if not quick else min(args.cpu_seconds, 10.0)
-    steps, t_used = 0, 0.0
-    while t_used < budget:
-        t0 = time.perf_counter()
-        cur = [dict(states[q], **{n: H.field(g.level, k).copy() for n, k in keys}) for q, g in enumerate(levels)]
-        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in levels]
-        oracle.rk4_multi(levels, nz, ph, cur, masks, DT_AD, 1, H=H)
-        H.mask_build(thr, 0, lmax)
+        import oracle
+        from oracle.grid import Grid as OGrid
+        from wavetrisk_hydrostatic_b200.cases import OceanParams
+
+        self.np = np
+        self.oracle = oracle
+        self.threads = os.cpu_count() or 1
+        oracle.set_threads(self.threads)
+        self.ph = OceanParams()
+        self.lmin, self.lmax, self.nz, self.nz_s, self.seed = lmin, lmax, nz, nz_s, seed
+        G = OGrid(lmin, lmax, radius=6371e3)
+        self.levels = [G.level(l) for l in range(lmin, lmax + 1)]
+        self.slope = None
+        self.ctx = {}
+
+    def _setup(self, nz):
+        from oracle.wavelet import Hierarchy
+
+        np, ph = self.np, self.ph
+        states = adaptive_states(self.levels, nz, self.seed, ph)
+        thr = TOL_AD * np.stack([ph.ref_density * np.full(nz, ph.depth / nz), np.full(nz, 1e16), np.full(nz, 1.0)])
+        H = Hierarchy(self.levels, nz)
+        for name, key in (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v")):
+            H.set(self.lmax, key, states[-1][name])
+        H.forward()
+        H.mask_build(thr, 0, self.lmax)
         H.compress()
         H.inverse()
-        t_used += time.perf_counter() - t0
-        steps += 1
-    return {"value": sim_days_per_hour(steps, t_used, DT_AD), "unit": "simulated days per wall-clock hour",
-            "cores": oracle.get_threads(), "kind": "port",
-            "sample": f"{steps} adaptive steps of the same workload ({t_used:.1f} s): the multi-level trend "
-                      f"over lozenges and the wavelet transforms over layers on {oracle.get_threads()} threads, "
-                      f"the mask sequence on one"}
+        for st in states:
+            for k in ("mass", "temp", "velo"):
+                st.pop(k)
+        self.ctx[nz] = (states, thr, H)
+
+    def step(self, nz):
+        """Seconds of one adaptive step with nz layers."""
+        if nz not in self.ctx:
+            self._setup(nz)
+        states, thr, H = self.ctx[nz]
+        keys = (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v"))
+        t0 = time.perf_counter()
+        cur = [dict(states[q], **{n: H.field(g.level, k).copy() for n, k in keys}) for q, g in enumerate(self.levels)]
+        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in self.levels]
+        self.oracle.rk4_multi(self.levels, nz, self.ph, cur, masks, dt_adaptive(self.lmax), 1, H=H)
+        H.mask_build(thr, 0, self.lmax)
+        H.compress()
+        H.inverse()
+        return time.perf_counter() - t0
+
+    def calibrate(self):
+        t1 = self.step(self.nz_s)
+        t2 = self.step(2 * self.nz_s)
+        self.slope = max(0.0, (t2 - t1) / self.nz_s)
+        self.ctx.pop(2 * self.nz_s, None)
+        return t1, t2
+
+    def sample(self):
+        """One sample: (seconds at nz_s layers, extrapolated seconds at nz layers)."""
+        t = self.step(self.nz_s)
+        return t, t + (self.nz - self.nz_s) * self.slope
+
+    def describe(self, n, secs):
+        return (f"{n} samples, each one whole adaptive step of the J{self.lmin}..J{self.lmax} hierarchy (every level "
+                f"and node) with {self.nz_s} of the {self.nz} layers ({secs:.1f} s of CPU time in all), extrapolated "
+                f"to {self.nz} layers with the per-layer cost {self.slope:.3f} s measured between {self.nz_s} and "
+                f"{2 * self.nz_s} layers; CPU restatement (oracle), multi-level trend over the 10 lozenges and "
+                f"wavelets over layers on {self.threads} threads, mask sequence on one")
+
+
+def cpu_baseline_adaptive(args, quick=False):
+    """The oracle's adaptive step on the same workload: calibration, then
+    samples until the time budget is used (at least one)."""
+    S = AdaptiveCpuSampler(args.lmin, args.level, args.nz)
+    S.calibrate()
+    budget = args.cpu_seconds if not quick else min(args.cpu_seconds, 10.0)
+    n, used, est = 0, 0.0, 0.0
+    while n == 0 or used < budget:
+        t, t32 = S.sample()
+        n, used, est = n + 1, used + t, est + t32
+    return {"value": sim_days_per_hour(n, est, dt_adaptive(args.level)), "unit": "simulated days per wall-clock hour",
+            "cores": S.threads, "kind": "port", "sample": S.describe(n, used),
+            "seconds_per_step": est / n}
 
 
 def bench_reference(args):
+    """The reference arm: the CPU restatement of the path on the host cores,
+    on the same workload, metric and config as our arm.  Warm-up samples
+    (the first two calibrate the per-layer cost) and timed samples as
+    cpu_baseline describes; value = simulated days per hour of the
+    extrapolated whole-workload steps."""
     world, rank, local, pg = dist_init(args)
     if rank != 0:
         if pg is not None:
             pg.destroy_process_group()
         return
     steps = max(1, args.steps)
-    cb = cpu_baseline(args)
+    if args.mode == "adaptive":
+        S = AdaptiveCpuSampler(args.lmin, args.level, args.nz)
+        S.calibrate()
+        for _ in range(max(0, args.warmup - 2)):
+            S.sample()
+        used, est = 0.0, 0.0
+        for _ in range(steps):
+            t, t32 = S.sample()
+            used, est = used + t, est + t32
+        value = sim_days_per_hour(steps, est, dt_adaptive(args.level))
+        cb = {"value": value, "unit": "simulated days per wall-clock hour", "cores": S.threads, "kind": "port",
+              "sample": S.describe(steps, used), "seconds_per_step": est / steps}
+        data = "synthetic (seeded seamount, jet and Gaussian bumps)"
+    else:
+        cb = cpu_baseline(args)
+        data = "synthetic (seeded jet + white-noise free surface)"
     line = {
         "impl": "reference",
         "metric": "sim-days/hour",
@@ -821,10 +923,9 @@ def bench_reference(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded jet + Gaussian bumps)" if args.mode == "adaptive"
-                else "synthetic (seeded jet + white-noise free surface)",
-        "config": dict(workload_config(args, world),
-                       note="CPU restatement of the reference path (no Fortran compiler on the host)"),
+        "data": data,
+        "config": workload_config(args, world),
+        "note": "CPU restatement of the reference path (no Fortran compiler on the build or GPU hosts)",
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -857,20 +958,18 @@ def bench_trace(args):
 
     from wavetrisk_hydrostatic_b200 import Grid, OceanParams
     from wavetrisk_hydrostatic_b200.adaptive import AdaptiveOcean
-    from wavetrisk_hydrostatic_b200.cases import bump_state
 
     torch.cuda.set_device(0)
     ph = OceanParams()
     G = Grid(args.lmin, args.level, radius=6371e3)
     levels = [G.level(l) for l in range(args.lmin, args.level + 1)]
-    model = AdaptiveOcean(G, args.lmin, args.level, args.nz, [bump_state(g, args.nz, seed=1, ph=ph) for g in levels],
-                          ph, tol=TOL_AD)
+    model = AdaptiveOcean(G, args.lmin, args.level, args.nz, adaptive_states(levels, args.nz, 1, ph), ph, tol=TOL_AD)
     for _ in range(args.warmup):
-        model.step(DT_AD)
+        model.step(dt_adaptive(args.level))
     torch.cuda.synchronize()
     with profile(activities=[ProfilerActivity.CUDA]) as prof:
         for _ in range(args.steps):
-            model.step(DT_AD)
+            model.step(dt_adaptive(args.level))
         torch.cuda.synchronize()
     prof.export_chrome_trace(args.trace)
     ev = [e for e in json.load(open(args.trace))["traceEvents"] if e.get("cat") == "kernel"]

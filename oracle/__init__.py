@@ -6,6 +6,11 @@ file:line).  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
 leg import this package, and only as the checker.  The product library never
 links or calls it.
 
+Geometry: every routine takes its geometry and ghost tables from the oracle's
+own grid builder (oracle_grid.cpp through grid.own), never from the level
+objects it is given; a product level only names the grid parameters and the
+level number.
+
 Parity status: unpinned against the reference binary (the reference is Fortran
 and no Fortran compiler exists in the build container); pinned instead by the
 properties the reference relies on (conservation, identities, analytic cases),
@@ -59,6 +64,8 @@ class _Level:
     """Keeps the numpy arrays alive for the lifetime of the ctypes struct."""
 
     def __init__(self, g):
+        from .grid import own
+        g = own(g)
         self.keep = [np.ascontiguousarray(x) for x in
                      (g.len, g.pedlen, g.part, g.hex_inv, g.triarea, g.coriolis)]
         self.hn = np.ascontiguousarray(g.halo_node, dtype=np.int64)
@@ -117,6 +124,8 @@ def trend_multi(levels, nz, ph, states, masks):
     level_end), every level present.  states[q]: dict of mass, temp, velo,
     mean_m, mean_t, topo of levels[q]; masks[q]: (mask_n, mask_e) int32.
     Returns per level (dmass, dtemp, dvelo, state_after_halo)."""
+    from .grid import own
+    levels = [own(g) for g in levels]
     L = lib()
     L.orc_trend_multi.argtypes = [C.POINTER(orc_mlevel), C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
     L.orc_trend_multi.restype = C.c_int

@@ -23,6 +23,8 @@ def _p(a, t=_dp):
 
 class _Level:
     def __init__(self, g):
+        from .grid import own
+        g = own(g)
         self.keep = [_c(g.len), _c(g.pedlen), _c(g.hex_inv), np.ascontiguousarray(g.halo_node, dtype=np.int64),
                      np.ascontiguousarray(g.halo_edge, dtype=np.int64)]
         ln, pl, hi, hn, he = self.keep
@@ -67,6 +69,8 @@ def step1_flux(g, itype, velo, mass, mean_m, scalar=None):
 
 def step1_vort(g, velo):
     """step1 itype 8 + post_vort on one layer's velocity: vorticity (2*NN, LORT then UPLT)."""
+    from .grid import own
+    g = own(g)
     L = lib()
     lv = _Level(g)
     vort = np.zeros(2 * g.NN)
@@ -79,7 +83,9 @@ def step1_vort(g, velo):
 
 
 def _multi(levels, nz, states, masks, etas, div_olds):
+    from .grid import own
     from .restrict import orc_rlevel
+    levels = [own(g) for g in levels]
     i32 = C.POINTER(C.c_int32)
 
     class orc_bml(C.Structure):

@@ -37,6 +37,8 @@ class Hierarchy:
     """Keeps the per-level numpy buffers alive behind an orc_elevel array."""
 
     def __init__(self, levels, topos, grav=9.80616, dt=600.0, theta1=1.0, theta2=1.0, domain_level=2, **solver):
+        from .grid import own
+        levels = [own(g) for g in levels]
         self.L = _bind()
         self.keep = []
         self.arr = (orc_elevel * len(levels))()

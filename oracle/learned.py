@@ -49,7 +49,9 @@ def pack(d):
 
 
 def node_src(lv):
-    """Ghost remap of a LevelGeom: nsrc[k] = source slot of slot k."""
+    """Ghost remap of a level: nsrc[k] = source slot of slot k."""
+    from .grid import own
+    lv = own(lv)
     nsrc = np.arange(lv.NN)
     nsrc[lv.halo_node[:, 0]] = lv.halo_node[:, 1]
     return nsrc

@@ -49,6 +49,8 @@ class Pair:
     FIELDS = ("scal", "dscal", "flux", "dvelo")
 
     def __init__(self, par, chd, nz):
+        from .grid import own
+        par, chd = own(par), own(chd)
         self.L = _bind()
         self.nz = nz
         self.geo = (par, chd)
@@ -87,6 +89,8 @@ class Pair:
 def div(g, flux):
     """Flux divergence at every node (i, j) in [0, n]^2 of every lozenge
     (div, src/ops.f90:1340-1355); other nodes 0.  flux: (..., 3*NN), ghost-copied."""
+    from .grid import own
+    g = own(g)
     NN, P = g.NN, g.P
     f = flux.reshape(flux.shape[:-1] + (3, NN))
     out = np.zeros(flux.shape[:-1] + (NN,))

@@ -45,6 +45,8 @@ class Hierarchy:
     FIELDS = ("s_m", "s_t", "s_v", "w_m", "w_t", "w_v")
 
     def __init__(self, levels, nz):
+        from .grid import own
+        levels = [own(g) for g in levels]
         self.L = _bind()
         self.levels = levels
         self.nz = nz

@@ -6,7 +6,8 @@ dt = 0, and grad_eta of a uniform free surface is zero."""
 import numpy as np
 
 from oracle import barotropic as ob
-from wavetrisk_hydrostatic_b200 import Grid, OceanParams, jet_state
+from oracle.grid import Grid
+from wavetrisk_hydrostatic_b200 import OceanParams, jet_state
 from wavetrisk_hydrostatic_b200.grid import halo_nodes
 
 

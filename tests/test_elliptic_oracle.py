@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from oracle.elliptic import Hierarchy
-from wavetrisk_hydrostatic_b200 import Grid
+from oracle.grid import Grid
 from wavetrisk_hydrostatic_b200.cases import bathymetry, elliptic_rhs
 from wavetrisk_hydrostatic_b200.grid import halo_nodes
 

@@ -5,7 +5,7 @@ import numpy as np
 import torch
 
 from oracle import learned as LO
-from wavetrisk_hydrostatic_b200 import Grid
+from oracle.grid import Grid
 from wavetrisk_hydrostatic_b200.cases import bathymetry
 
 

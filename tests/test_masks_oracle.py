@@ -8,7 +8,7 @@ thresholds every child patch is required."""
 import numpy as np
 
 from oracle.wavelet import ADJZONE, TOLRNZ, Hierarchy
-from wavetrisk_hydrostatic_b200 import Grid
+from oracle.grid import Grid
 from wavetrisk_hydrostatic_b200.cases import jet_state
 
 LS, LE, NZ, PS = 3, 5, 2, 4

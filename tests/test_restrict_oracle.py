@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from oracle.restrict import ADJZONE, RESTRCT, Pair, _nodes, div
-from wavetrisk_hydrostatic_b200 import Grid
+from oracle.grid import Grid
 from wavetrisk_hydrostatic_b200.grid import halo_edges, halo_nodes
 
 

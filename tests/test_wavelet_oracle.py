@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from oracle.wavelet import ADJZONE, FROZEN, TOLRNZ, Hierarchy
-from wavetrisk_hydrostatic_b200 import Grid
+from oracle.grid import Grid
 from wavetrisk_hydrostatic_b200.cases import edge_velocity, solid_body_rotation
 from wavetrisk_hydrostatic_b200.grid import halo_edges, halo_nodes
 

@@ -44,7 +44,9 @@ class AdaptiveOcean:
         top = states[-1]
         for name in ("mass", "temp", "velo"):
             self.dev.upload(max_level, name, top[name])
-        dz = top["mean_m"][:, 0] / self.ph.ref_density
+        # initialize_thresholds_case: the mass scale of layer k is rho0 dz_k with
+        # dz_k from the maximum depth (equal layers), whatever the bathymetry
+        dz = np.full(nz, self.ph.depth / nz)
         lnorm = np.stack([self.ph.ref_density * dz, np.full(nz, 1e16), np.full(nz, udim)])
         self.threshold_def = tol * lnorm
         self.threshold = self.threshold_def.copy()

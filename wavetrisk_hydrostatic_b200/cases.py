@@ -49,22 +49,45 @@ def _proj_jet(p, q, u0, lat0, width):
     return u * np.einsum("ij,ij->j", ez, v / vn)
 
 
+def seamount_topography(g: LevelGeom, seed: int = 0, depth: float = 4000.0, height: float = 2000.0,
+                        radius: float = 50e3) -> np.ndarray:
+    """Flat bottom at -depth with a Gaussian seamount of the given height and
+    radius (m) centred at a seeded point of the sphere (the bathymetry of the
+    reference's seamount case, test/seamount/test_case_module.f90, with a
+    seeded centre): topography = -depth + height exp(-(r/radius)^2), r the
+    great-circle distance, at every node of the level (ghosts from their own
+    coordinates; padding slots without coordinates get the flat depth)."""
+    rng = np.random.default_rng(20_000 + seed)
+    c = rng.standard_normal(3)
+    c /= np.linalg.norm(c)
+    nrm = np.linalg.norm(g.node, axis=0)
+    ok = nrm > 0
+    R = float(nrm[g.owned][0])
+    topo = np.full(g.NN, -depth)
+    ang = np.arccos(np.clip(c @ (g.node[:, ok] / nrm[ok]), -1.0, 1.0))
+    topo[ok] += height * np.exp(-((R * ang) / radius) ** 2)
+    return topo
+
+
 def jet_state(g: LevelGeom, nz: int, seed: int = 0, ph: OceanParams | None = None,
-              u0: float = 1.0, eta_amp: float = 1e-3, rho_bottom: float = 1027.0, rho_top: float = 1024.0):
-    """Uniform-level layered ocean state: flat bottom, linear layer densities, zonal
-    jet at 45N in the top layer decaying linearly to 0 at the bottom, seeded white
+              u0: float = 1.0, eta_amp: float = 1e-3, rho_bottom: float = 1027.0, rho_top: float = 1024.0,
+              topo: np.ndarray | None = None):
+    """Uniform-level layered ocean state: flat bottom (or the given topography,
+    layers of equal thickness H/nz following it as the reference's init_mean
+    sets them with b_vert_mass = 1/nz), linear layer densities, zonal jet at
+    45N in the top layer decaying linearly to 0 at the bottom, seeded white
     noise free surface.  Returns dict of float64 arrays in the C-ABI layout."""
     ph = ph or OceanParams()
     NN = g.NN
     rng = np.random.default_rng(seed)
-    dz = ph.depth / nz
+    topo = np.full(NN, -ph.depth) if topo is None else np.asarray(topo, dtype=np.float64)
+    dz = -topo / nz
     rho = rho_bottom + (rho_top - rho_bottom) * np.arange(nz) / max(nz - 1, 1)   # k=1 is the bottom layer
     mean_m = np.empty((nz, NN))
     mean_t = np.empty((nz, NN))
     for k in range(nz):
         mean_m[k] = ph.ref_density * dz
         mean_t[k] = mean_m[k] * (1.0 - rho[k] / ph.ref_density)
-    topo = np.full(NN, -ph.depth)
     eta = np.zeros(NN)
     own = g.owned
     eta[own] = eta_amp * rng.standard_normal(int(own.sum()))

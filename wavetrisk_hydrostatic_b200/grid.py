@@ -39,6 +39,7 @@ class LevelGeom:
     iu_wgt: np.ndarray | None = None   # (9, NN) outer velocity weights I_u_wgt (levels above min_level-1)
     rf_wgt: np.ndarray | None = None   # (3, NN) flux-restriction weights R_F_wgt (levels above min_level-1)
     rf_conflict: float = 0.0           # largest difference between two writers of one R_F_wgt slot
+    grid_spec: tuple | None = None     # (min_level, max_level, domain_level, radius, omega) of the grid
     _owned: np.ndarray | None = field(default=None, repr=False)
 
     def idx(self, d, i, j):
@@ -113,6 +114,7 @@ class Grid:
             iu_wgt=get("iu_wgt", (9, NN)) if l > self.min_level - 1 else None,
             rf_wgt=get("rf_wgt", (3, NN)) if l > self.min_level - 1 else None,
             rf_conflict=float(get("rf_conflict", (1,))[0]) if l > self.min_level - 1 else 0.0,
+            grid_spec=(self.min_level, self.max_level, self.domain_level, self.radius, self.omega),
         )
         self._levels[l] = g
         return g

@@ -783,112 +783,101 @@ def cpu_baseline(args, quick=False):
             "sample": f"{steps} RK4 steps of the same workload ({t_used:.1f} s of CPU time)"}
 
 
+def hierarchy_nodes(lmin, lmax):
+    return sum(10 * 4 ** l + 2 for l in range(lmin, lmax + 1))
+
+
 class AdaptiveCpuSampler:
-    """CPU restatement (oracle) of the adaptive step on the workload's full
-    hierarchy, timed on bounded samples.  A sample is one whole adaptive step
-    (multi-level trend and RK4 with WT_after_step per stage, adapt's mask
-    sequence, compression, inverse transform) on every level and every node,
-    computed with `nz_s` of the workload's layers.  The step's cost is
-    A + B nz (the trend, RK and wavelet work is per layer, the mask sequence
-    and the per-node set-up are not); B is calibrated from one step at
-    nz_s and one at 2 nz_s, and a sample's time t(nz_s) is extrapolated to
-    t(nz) = t(nz_s) + (nz - nz_s) B.  The oracle's wavelet transforms run one
-    layer per worker thread, so at 2-4 layers their time grows less than in
-    proportion and B errs low: the extrapolated CPU time is if anything an
-    underestimate.  Geometry and states come from the oracle-side builders."""
+    """CPU restatement (oracle) of the adaptive step, timed on bounded
+    samples of the workload.  A sample is one whole adaptive step (multi-level
+    trend and RK4 with WT_after_step per stage, adapt's mask sequence,
+    compression, inverse transform) with every one of the workload's layers
+    on the hierarchy lmin..lmax-2, i.e. the same computation at a quarter of
+    the resolution; its time is scaled to lmin..lmax by the ratio of the node
+    counts of the two hierarchies (about 16).  The oracle computes every node
+    of every level, so its cost per node-layer does not depend on the
+    resolution: on 8 threads it measured 0.894, 0.922 and 0.908 us per
+    node-layer and step for J5..J6, J5..J7 and J5..J8 with 32 layers.
+    Geometry comes from the oracle's own grid builder."""
 
-    def __init__(self, lmin, lmax, nz, nz_s=2, seed=1):
-        import numpy as np
-
+    def __init__(self, lmin, lmax, nz, seed=1):
         import oracle
         from oracle.grid import Grid as OGrid
         from wavetrisk_hydrostatic_b200.cases import OceanParams
 
-        self.np = np
         self.oracle = oracle
         self.threads = os.cpu_count() or 1
         oracle.set_threads(self.threads)
+        self.threads = oracle.get_threads()
         self.ph = OceanParams()
-        self.lmin, self.lmax, self.nz, self.nz_s, self.seed = lmin, lmax, nz, nz_s, seed
-        G = OGrid(lmin, lmax, radius=6371e3)
-        self.levels = [G.level(l) for l in range(lmin, lmax + 1)]
-        self.slope = None
-        self.ctx = {}
+        self.lmin, self.lmax, self.nz, self.seed = lmin, lmax, nz, seed
+        self.ls = max(lmin + 1, lmax - 2)
+        self.scale = hierarchy_nodes(lmin, lmax) / hierarchy_nodes(lmin, self.ls)
+        G = OGrid(lmin, self.ls, radius=6371e3)
+        self.levels = [G.level(l) for l in range(lmin, self.ls + 1)]
+        self._setup()
 
-    def _setup(self, nz):
+    def _setup(self):
+        import numpy as np
         from oracle.wavelet import Hierarchy
 
-        np, ph = self.np, self.ph
+        ph, nz = self.ph, self.nz
         states = adaptive_states(self.levels, nz, self.seed, ph)
-        thr = TOL_AD * np.stack([ph.ref_density * np.full(nz, ph.depth / nz), np.full(nz, 1e16), np.full(nz, 1.0)])
+        self.thr = TOL_AD * np.stack([ph.ref_density * np.full(nz, ph.depth / nz), np.full(nz, 1e16),
+                                      np.full(nz, 1.0)])
         H = Hierarchy(self.levels, nz)
         for name, key in (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v")):
-            H.set(self.lmax, key, states[-1][name])
+            H.set(self.ls, key, states[-1][name])
         H.forward()
-        H.mask_build(thr, 0, self.lmax)
+        H.mask_build(self.thr, 0, self.ls)
         H.compress()
         H.inverse()
         for st in states:
             for k in ("mass", "temp", "velo"):
                 st.pop(k)
-        self.ctx[nz] = (states, thr, H)
-
-    def step(self, nz):
-        """Seconds of one adaptive step with nz layers."""
-        if nz not in self.ctx:
-            self._setup(nz)
-        states, thr, H = self.ctx[nz]
-        keys = (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v"))
-        t0 = time.perf_counter()
-        cur = [dict(states[q], **{n: H.field(g.level, k).copy() for n, k in keys}) for q, g in enumerate(self.levels)]
-        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in self.levels]
-        self.oracle.rk4_multi(self.levels, nz, self.ph, cur, masks, dt_adaptive(self.lmax), 1, H=H)
-        H.mask_build(thr, 0, self.lmax)
-        H.compress()
-        H.inverse()
-        return time.perf_counter() - t0
-
-    def calibrate(self):
-        t1 = self.step(self.nz_s)
-        t2 = self.step(2 * self.nz_s)
-        self.slope = max(0.0, (t2 - t1) / self.nz_s)
-        self.ctx.pop(2 * self.nz_s, None)
-        return t1, t2
+        self.states, self.H = states, H
 
     def sample(self):
-        """One sample: (seconds at nz_s layers, extrapolated seconds at nz layers)."""
-        t = self.step(self.nz_s)
-        return t, t + (self.nz - self.nz_s) * self.slope
+        """One sample: (seconds of the step at lmin..lmax-2, the same scaled to lmin..lmax)."""
+        H = self.H
+        keys = (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v"))
+        t0 = time.perf_counter()
+        cur = [dict(self.states[q], **{n: H.field(g.level, k).copy() for n, k in keys})
+               for q, g in enumerate(self.levels)]
+        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in self.levels]
+        self.oracle.rk4_multi(self.levels, self.nz, self.ph, cur, masks, dt_adaptive(self.lmax), 1, H=H)
+        H.mask_build(self.thr, 0, self.ls)
+        H.compress()
+        H.inverse()
+        t = time.perf_counter() - t0
+        return t, t * self.scale
 
     def describe(self, n, secs):
-        return (f"{n} samples, each one whole adaptive step of the J{self.lmin}..J{self.lmax} hierarchy (every level "
-                f"and node) with {self.nz_s} of the {self.nz} layers ({secs:.1f} s of CPU time in all), extrapolated "
-                f"to {self.nz} layers with the per-layer cost {self.slope:.3f} s measured between {self.nz_s} and "
-                f"{2 * self.nz_s} layers; CPU restatement (oracle), multi-level trend over the 10 lozenges and "
-                f"wavelets over layers on {self.threads} threads, mask sequence on one")
+        return (f"{n} samples, each one whole adaptive step with all {self.nz} layers on the hierarchy "
+                f"J{self.lmin}..J{self.ls} ({secs:.1f} s of CPU time in all), scaled by the node count "
+                f"x{self.scale:.2f} to J{self.lmin}..J{self.lmax}; CPU restatement (oracle), multi-level trend "
+                f"over the 10 lozenges and wavelets over layers on {self.threads} threads, mask sequence on one")
 
 
 def cpu_baseline_adaptive(args, quick=False):
-    """The oracle's adaptive step on the same workload: calibration, then
-    samples until the time budget is used (at least one)."""
+    """The oracle's adaptive step on the same workload: one warm-up sample,
+    then samples until the time budget is used (at least two)."""
     S = AdaptiveCpuSampler(args.lmin, args.level, args.nz)
-    S.calibrate()
+    S.sample()
     budget = args.cpu_seconds if not quick else min(args.cpu_seconds, 10.0)
     n, used, est = 0, 0.0, 0.0
-    while n == 0 or used < budget:
-        t, t32 = S.sample()
-        n, used, est = n + 1, used + t, est + t32
+    while n < 2 or used < budget:
+        t, tf = S.sample()
+        n, used, est = n + 1, used + t, est + tf
     return {"value": sim_days_per_hour(n, est, dt_adaptive(args.level)), "unit": "simulated days per wall-clock hour",
-            "cores": S.threads, "kind": "port", "sample": S.describe(n, used),
-            "seconds_per_step": est / n}
+            "cores": S.threads, "kind": "port", "sample": S.describe(n, used), "seconds_per_step": est / n}
 
 
 def bench_reference(args):
     """The reference arm: the CPU restatement of the path on the host cores,
-    on the same workload, metric and config as our arm.  Warm-up samples
-    (the first two calibrate the per-layer cost) and timed samples as
-    cpu_baseline describes; value = simulated days per hour of the
-    extrapolated whole-workload steps."""
+    on the same workload, metric and config as our arm: --warmup untimed and
+    --steps timed samples as AdaptiveCpuSampler describes; value = simulated
+    days per hour of the scaled whole-workload steps."""
     world, rank, local, pg = dist_init(args)
     if rank != 0:
         if pg is not None:
@@ -897,13 +886,12 @@ def bench_reference(args):
     steps = max(1, args.steps)
     if args.mode == "adaptive":
         S = AdaptiveCpuSampler(args.lmin, args.level, args.nz)
-        S.calibrate()
-        for _ in range(max(0, args.warmup - 2)):
+        for _ in range(max(1, args.warmup)):
             S.sample()
         used, est = 0.0, 0.0
         for _ in range(steps):
-            t, t32 = S.sample()
-            used, est = used + t, est + t32
+            t, tf = S.sample()
+            used, est = used + t, est + tf
         value = sim_days_per_hour(steps, est, dt_adaptive(args.level))
         cb = {"value": value, "unit": "simulated days per wall-clock hour", "cores": S.threads, "kind": "port",
               "sample": S.describe(steps, used), "seconds_per_step": est / steps}

@@ -69,7 +69,15 @@ class Pool {
     stop();
     n = n < 1 ? 1 : (n > 10 ? 10 : n);
     nthreads_ = n;
-    for (int t = 1; t < n; ++t) workers_.emplace_back([this, t] { loop(t); });
+    // a new worker waits for the next run: it starts from the current
+    // generation, not from 0 (a stale generation would replay the last run's
+    // function, which no longer exists)
+    uint64_t g0;
+    {
+      std::unique_lock<std::mutex> lk(m_);
+      g0 = gen_;
+    }
+    for (int t = 1; t < n; ++t) workers_.emplace_back([this, t, g0] { loop(t, g0); });
   }
   int threads() const { return nthreads_; }
   void run(const std::function<void(int)>& fn) {
@@ -85,8 +93,7 @@ class Pool {
   }
   ~Pool() { stop(); }
  private:
-  void loop(int t) {
-    uint64_t seen = 0;
+  void loop(int t, uint64_t seen) {
     for (;;) {
       const std::function<void(int)>* fn;
       {

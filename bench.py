@@ -160,7 +160,7 @@ def barrier(pg):
 
 
 # ---------------------------------------------------------------- ours ----
-def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=True, kernels=True):
+def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=True, kernels=True, flux_bits=64):
     import numpy as np
     import torch
 
@@ -173,6 +173,8 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
     st = jet_state(g, nz, seed=seed, ph=ph)
     model = TriskModel(g, nz, st["topo"], ph)
     model.upload(st)
+    if flux_bits != 64:
+        model.flux_precision(flux_bits)
     stream = torch.cuda.ExternalStream(model.stream, device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # 256 MB > 126 MB L2
     for _ in range(warmup):
@@ -187,7 +189,7 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
         ev[s][1].record(stream)
     model.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in ev)
-    out = {"ms_total": ms, "ms_per_step": ms / steps}
+    out = {"ms_total": ms, "ms_per_step": ms / steps, "final_state": model.download()}
 
     if kernels:
         # Per-kernel launch durations of the same stepper, launched kernel by kernel
@@ -559,6 +561,7 @@ def algorithmic_bytes_trend_rk(level, nz):
 def bench_ours(args):
     if args.mode == "uniform":
         return bench_ours_uniform(args)
+    import numpy as np
     import torch
 
     world, rank, local, pg = dist_init(args)
@@ -603,6 +606,23 @@ def bench_ours(args):
                 "trend_rk_GBps": ab / (kt["trend_rk"] / 1e3) / 1e9,
                 "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,
             })
+            if lv in (7, 8):   # the same run with FP32 flux stencils, error against the FP64 run
+                rm = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False, flux_bits=32)
+                ref, got = rr["final_state"], rm["final_state"]
+                err = {k: float(np.abs(got[k] - ref[k]).max() / max(np.abs(ref[k]).max(), 1e-300))
+                       for k in ("mass", "temp", "velo")}
+                km = rm["kernel_ms_per_launch"]
+                extra.append({
+                    "workload": f"uniform J{lv}, {nz} layers, RK4 dt=300 s with the step1 flux stencils in FP32 "
+                                f"(WT_TUNE_FLUX_PRECISION=32; FP64 trends, conservation and RK accumulation)",
+                    "ms_per_step": rm["ms_per_step"], "value": sim_days_per_hour(steps, rm["ms_total"] / 1e3),
+                    "unit": "simulated days per wall-clock hour",
+                    "speedup_vs_fp64": rr["ms_per_step"] / rm["ms_per_step"],
+                    "max_rel_error_vs_fp64_after_steps": {"steps": steps, **err},
+                    "kernel_ms_per_launch": km,
+                    "step1_plus_trend_ms_fp64": kt["step1"] + kt["trend_rk"],
+                    "step1_plus_trend_ms_fp32_fluxes": km["step1"] + km["trend_rk"],
+                })
         for lmax in (6, 7, 8):
             extra.append(elliptic_case(lmax, eval_seeds=16 if lmax == 8 else None))
         for (lmin, lmax, nzw) in ((5, 7, 16), (5, 8, 32)):

@@ -339,7 +339,17 @@ int wt_lnorm(wt_handle* h, int order, double* out);
  * WT_after_step (no counterpart in the reference, which computes every node of
  * every existing patch; the states and masks are the same either way); 0
  * computes every node. */
-enum { WT_TUNE_WAVELET_LAYERS = 1, WT_TUNE_SKIP_INACTIVE = 2 };
+/* WT_TUNE_FLUX_PRECISION (per handle, 64 = default): 32 runs the flux
+ * stencils of step1 (potential vorticity, mass and Theta fluxes, kinetic
+ * energy: src/ops.f90:276-366, 472-522, post_step1 :526-737) of the
+ * single-level stepper (wt_trend, wt_rk4_step, wt_rk4_step_host) in FP32 with
+ * FP32 results, and keeps FP64 for the column pass, the Bernoulli function's
+ * geopotential and pressure parts, the divergence, Qperp, the gradients and
+ * the RK accumulation.  The first switch to 32 allocates the FP32 work
+ * arrays.  The hierarchy's steps (wt_trend_multi, wt_rk4_multi,
+ * wt_adaptive_step, wt_rk4_split_explicit) stay FP64 and return WT_ERR_STATE
+ * while it is 32.  No reference counterpart (the reference is FP64 only). */
+enum { WT_TUNE_WAVELET_LAYERS = 1, WT_TUNE_SKIP_INACTIVE = 2, WT_TUNE_FLUX_PRECISION = 3 };
 int wt_tune(wt_handle* h, int param, int value);
 /* compress_wavelets (src/adapt.f90:79-103): zero the wavelets of inactive points. */
 int wt_compress(wt_handle* h);

@@ -11,6 +11,7 @@
 
 #include "../../include/wavetrisk_gpu.h"
 #include "trisk_kernels.cuh"
+#include "trisk_mixed.cuh"
 #include "trisk_tma.cuh"
 #include "wt_handle.cuh"
 
@@ -252,6 +253,9 @@ int wt_destroy(wt_handle* h) {
                       h->dm, h->dt, h->dv, h->qe, h->hfm, h->hft, h->bern, h->phik, h->pterm, h->theta};
   for (double* p : arrays)
     if (p) cudaFree(p);
+  float* arrays32[] = {h->qe32, h->hfm32, h->hft32, h->ke32, h->theta32};
+  for (float* p : arrays32)
+    if (p) cudaFree(p);
   h->release_extra();
   if (h->dflag) cudaFree(h->dflag);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -260,6 +264,31 @@ int wt_destroy(wt_handle* h) {
 }
 
 void* wt_stream(wt_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+// WT_TUNE_FLUX_PRECISION (wt_tune): the single-level stepper's flux stencils
+// in FP64 (64) or FP32 (32).  The FP32 work arrays are allocated on the first
+// switch to 32; the captured step graph is dropped so the next step records
+// the other kernels.
+int wt_set_flux_precision(wt_handle* h, int bits) {
+  if (!h || (bits != 64 && bits != 32)) return WT_ERR_ARG;
+  if (bits == h->flux_bits) return WT_OK;
+  if (bits == 32 && !h->qe32) {
+    const int64_t nn = (int64_t)h->nz * h->top().NN;
+    float** arrays[] = {&h->qe32, &h->hfm32, &h->hft32, &h->ke32, &h->theta32};
+    const int64_t sizes[] = {3 * nn, 3 * nn, 3 * nn, nn, nn};
+    for (int q = 0; q < 5; ++q) {
+      cudaError_t e = cudaMalloc(arrays[q], sizeof(float) * sizes[q]);
+      if (e == cudaSuccess) e = cudaMemset(*arrays[q], 0, sizeof(float) * sizes[q]);
+      if (e != cudaSuccess) return wt_handle_fail("flux fp32 arrays", e);
+    }
+  }
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+  }
+  h->flux_bits = bits;
+  return WT_OK;
+}
 
 int wt_synchronize(wt_handle* h) {
   if (!h) return WT_ERR_ARG;
@@ -354,6 +383,25 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
   TB(1);
   k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, h->mean_m, h->mean_t, h->phik, h->pterm, nullptr);
   TE(1);
+  if (h->flux_bits == 32) {  // FP32 flux stencils, FP64 trends and sub-step (trisk_mixed.cuh)
+    TB(2);
+    k_step1_f32<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t,
+                                                   Step1OutF{h->qe32, h->hfm32, h->hft32, h->ke32, h->theta32});
+    TE(2);
+    TrendIOF io{};
+    io.theta = h->theta32; io.qe = h->qe32; io.hfm = h->hfm32; io.hft = h->hft32; io.ke = h->ke32;
+    io.phik = h->phik; io.pterm = h->pterm;
+    io.base_m = bm; io.base_t = bt; io.base_v = bv; io.dst_m = om; io.dst_t = ot; io.dst_v = ov; io.h = hstep;
+    io.dm = h->dm; io.dtt = h->dt; io.dv = h->dv;
+    TB(5);
+    if (mode == MODE_RK)
+      k_trend_mixed<MODE_RK><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
+    else
+      k_trend_mixed<MODE_TREND><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
+    TE(5);
+    CK(cudaGetLastError());
+    return WT_OK;
+  }
   Step1Out so{h->qe, h->hfm, h->hft, h->bern, h->theta};
   TB(2);
   if (h->trend_variant == 0) {

@@ -55,6 +55,10 @@ struct wt_handle {
   wtk::Step1Maps s1maps[3]{};  // step1 input maps for the state buffers (mass,temp,velo), (m1,t1,v1), (m2,t2,v2)
   int* dflag = nullptr;     // device error flag: 1 = a kernel's staged copies did not complete
   int trend_variant = 0;    // 0: TMA-staged k_step1_tma/k_trend_tma, 1: k_step1/k_trend (loads through L1)
+  // WT_TUNE_FLUX_PRECISION: 64 (default) or 32, the FP32 step1 of the
+  // single-level stepper (trisk_mixed.cuh) with its FP32 results below
+  int flux_bits = 64;
+  float *qe32 = nullptr, *hfm32 = nullptr, *hft32 = nullptr, *ke32 = nullptr, *theta32 = nullptr;
   bool state_halo_done = false;
   cudaGraphExec_t graph_exec = nullptr;
   double graph_dt = 0.0;

@@ -305,7 +305,7 @@ extern "C" {
 
 int wt_trend_multi(wt_handle* h) {
   if (!h) return WT_ERR_ARG;
-  if (!h->wav) return WT_ERR_STATE;
+  if (!h->wav || h->flux_bits != 64) return WT_ERR_STATE;  // the hierarchy's steps are FP64 only
   if (int rc = ensure(h)) return rc;
   if (int rc = trend_multi(h, hierarchy_state(h))) return rc;
   CKM(cudaStreamSynchronize(h->stream));
@@ -395,7 +395,7 @@ extern "C" {
 // surface (wt_barotropic_upload_level) and the masks as they are.
 int wt_rk4_split_explicit(wt_handle* h, double dt, double theta1) {
   if (!h) return WT_ERR_ARG;
-  if (!h->wav) return WT_ERR_STATE;
+  if (!h->wav || h->flux_bits != 64) return WT_ERR_STATE;  // the hierarchy's steps are FP64 only
   if (int rc = ensure(h)) return rc;
   if (int rc = rk4_split_explicit(h, dt, theta1)) return rc;
   CKM(cudaStreamSynchronize(h->stream));
@@ -408,7 +408,7 @@ int wt_rk4_split_explicit(wt_handle* h, double dt, double theta1) {
 // WT_after_step on the new stage state, with the masks held fixed.
 int wt_rk4_multi(wt_handle* h, double dt, int nsteps) {
   if (!h || nsteps < 0) return WT_ERR_ARG;
-  if (!h->wav) return WT_ERR_STATE;
+  if (!h->wav || h->flux_bits != 64) return WT_ERR_STATE;  // the hierarchy's steps are FP64 only
   if (int rc = ensure(h)) return rc;
   if (int rc = rk4_multi(h, dt, nsteps, nullptr)) return rc;
   CKM(cudaStreamSynchronize(h->stream));
@@ -424,7 +424,7 @@ int wt_rk4_multi(wt_handle* h, double dt, int nsteps) {
 // max_level change) and replayed; the thresholds are uploaded before each call.
 int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level_fill, int max_level, int nsteps) {
   if (!h || !threshold || nsteps < 0) return WT_ERR_ARG;
-  if (!h->wav) return WT_ERR_STATE;
+  if (!h->wav || h->flux_bits != 64) return WT_ERR_STATE;  // the hierarchy's steps are FP64 only
   if (int rc = ensure(h)) return rc;
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   for (int l = h->level_start; l <= h->level_end; ++l) {  // allocate before any capture
@@ -480,7 +480,7 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
 // sub-step is fused), 6 WT_after_step); count[p] = occurrences per step.
 int wt_profile_rk4_multi(wt_handle* h, double dt, int nsteps, double* ms, int* count) {
   if (!h || nsteps < 1 || !ms || !count) return WT_ERR_ARG;
-  if (!h->wav) return WT_ERR_STATE;
+  if (!h->wav || h->flux_bits != 64) return WT_ERR_STATE;  // the hierarchy's steps are FP64 only
   if (int rc = ensure(h)) return rc;
   PhaseTimer tm{h->stream, {}, {}};
   if (int rc = rk4_multi(h, dt, nsteps, &tm)) return rc;

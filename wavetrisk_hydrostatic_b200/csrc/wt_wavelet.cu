@@ -883,7 +883,10 @@ int wt_lnorm(wt_handle* h, int order, double* out) {
 // Launch-shape tuning of the wavelet kernels: WT_TUNE_WAVELET_LAYERS = layers
 // per thread of the layer-group kernels (1 .. 64; 0 restores the default
 // chosen from the layer count).  Process-wide.
+int wt_set_flux_precision(wt_handle* h, int bits);
+
 int wt_tune(wt_handle* h, int param, int value) {
+  if (param == WT_TUNE_FLUX_PRECISION) return wt_set_flux_precision(h, value);
   if (param == WT_TUNE_WAVELET_LAYERS) {
     if (value < 0 || value > 64) return WT_ERR_ARG;
     g_lpt_set = value;

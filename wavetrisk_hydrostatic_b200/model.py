@@ -120,6 +120,11 @@ class TriskModel(DeviceGrid):
     def synchronize(self) -> None:
         N.check("wt_synchronize", N.lib().wt_synchronize(self.h))
 
+    def flux_precision(self, bits: int) -> None:
+        """WT_TUNE_FLUX_PRECISION: 32 runs step1's flux stencils in FP32 (FP64
+        trends, conservation and RK accumulation); 64 is the FP64 path."""
+        N.check("wt_tune", N.lib().wt_tune(self.h, 3, int(bits)))
+
     # -- barotropic pieces of the mode-split step (src/barotropic_2d.f90) --
     def barotropic_upload(self, eta: np.ndarray | None = None, div_old: np.ndarray | None = None) -> None:
         N.check("wt_barotropic_upload", N.lib().wt_barotropic_upload(

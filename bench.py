@@ -160,7 +160,8 @@ def barrier(pg):
 
 
 # ---------------------------------------------------------------- ours ----
-def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=True, kernels=True, flux_bits=64):
+def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=True, kernels=True, flux_bits=64,
+             dt=DT):
     import numpy as np
     import torch
 
@@ -178,14 +179,14 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
     stream = torch.cuda.ExternalStream(model.stream, device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # 256 MB > 126 MB L2
     for _ in range(warmup):
-        model.rk4(DT, 1)
+        model.rk4(dt, 1)
     model.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     for s in range(steps):
         with torch.cuda.stream(stream):
             flush.fill_(float(s))           # L2 flush between timed steps, outside the timed region
         ev[s][0].record(stream)
-        model.rk4(DT, 1)
+        model.rk4(dt, 1)
         ev[s][1].record(stream)
     model.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in ev)
@@ -196,7 +197,7 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
         # with CUDA events on the handle's stream (same steps, no graph).
         kt = (Nt.C.c_double * 16)()
         nk = Nt.C.c_int(0)
-        Nt.check("wt_profile_rk4", Nt.lib().wt_profile_rk4(model.h, DT, steps, kt, Nt.C.byref(nk)))
+        Nt.check("wt_profile_rk4", Nt.lib().wt_profile_rk4(model.h, dt, steps, kt, Nt.C.byref(nk)))
         names = ["halo_state", "column", "step1", "post_step1", "halo_flux", "trend_rk"]
         out["kernel_ms_per_launch"] = {names[k]: kt[k] for k in range(min(nk.value, len(names))) if kt[k] > 0}
 
@@ -205,11 +206,11 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
         pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
         m, t, v = pin((nz, NN)), pin((nz, NN)), pin((nz, 3 * NN))
         m[:] = st["mass"]; t[:] = st["temp"]; v[:] = st["velo"]
-        model.rk4_host(DT, 1, m, t, v)
+        model.rk4_host(dt, 1, m, t, v)
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
         for _ in range(steps):
-            model.rk4_host(DT, 1, m, t, v)
+            model.rk4_host(dt, 1, m, t, v)
         t1 = time.perf_counter()
         out["e2e_s"] = t1 - t0
         out["h2d_bytes_per_step"] = int(m.nbytes + t.nbytes + v.nbytes)
@@ -594,28 +595,29 @@ def bench_ours(args):
     extra = []
     if not args.no_extra and rank == 0 and world == 1:
         for (lv, nz, steps) in [(7, 16, 50), (5, 8, 100), (8, 32, 10)]:
-            rr = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False)
+            dtu = DT if lv == 5 else dt_adaptive(lv)   # 300 s is the plain method's; J7, J8 at their CFL step
+            rr = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False, dt=dtu)
             kt = rr["kernel_ms_per_launch"]
             ab = algorithmic_bytes_trend_rk(lv, nz)
             extra.append({
-                "workload": f"uniform J{lv} ({rr['cells']} cells), {nz} layers, single-level RK4 dt=300 s "
+                "workload": f"uniform J{lv} ({rr['cells']} cells), {nz} layers, single-level RK4 dt={dtu:g} s "
                             f"(the fused uniform stepper)",
-                "ms_per_step": rr["ms_per_step"], "value": sim_days_per_hour(steps, rr["ms_total"] / 1e3),
+                "ms_per_step": rr["ms_per_step"], "value": sim_days_per_hour(steps, rr["ms_total"] / 1e3, dtu),
                 "unit": "simulated days per wall-clock hour",
                 "kernel_ms_per_launch": kt,
                 "trend_rk_GBps": ab / (kt["trend_rk"] / 1e3) / 1e9,
                 "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,
             })
             if lv in (7, 8):   # the same run with FP32 flux stencils, error against the FP64 run
-                rm = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False, flux_bits=32)
+                rm = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False, flux_bits=32, dt=dtu)
                 ref, got = rr["final_state"], rm["final_state"]
                 err = {k: float(np.abs(got[k] - ref[k]).max() / max(np.abs(ref[k]).max(), 1e-300))
                        for k in ("mass", "temp", "velo")}
                 km = rm["kernel_ms_per_launch"]
                 extra.append({
-                    "workload": f"uniform J{lv}, {nz} layers, RK4 dt=300 s with the step1 flux stencils in FP32 "
-                                f"(WT_TUNE_FLUX_PRECISION=32; FP64 trends, conservation and RK accumulation)",
-                    "ms_per_step": rm["ms_per_step"], "value": sim_days_per_hour(steps, rm["ms_total"] / 1e3),
+                    "workload": f"uniform J{lv}, {nz} layers, RK4 dt={dtu:g} s with the step1 flux stencils in "
+                                f"FP32 (WT_TUNE_FLUX_PRECISION=32; FP64 trends, conservation and RK accumulation)",
+                    "ms_per_step": rm["ms_per_step"], "value": sim_days_per_hour(steps, rm["ms_total"] / 1e3, dtu),
                     "unit": "simulated days per wall-clock hour",
                     "speedup_vs_fp64": rr["ms_per_step"] / rm["ms_per_step"],
                     "max_rel_error_vs_fp64_after_steps": {"steps": steps, **err},
@@ -713,12 +715,13 @@ def bench_ours_uniform(args):
     extra = []
     if not args.no_extra and rank == 0 and world == 1:
         for (lv, nz, steps) in [(5, 8, 100), (8, 32, 10)]:
-            rr = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False)
+            dtu = DT if lv == 5 else dt_adaptive(lv)
+            rr = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False, dt=dtu)
             kt = rr["kernel_ms_per_launch"]
             ab = algorithmic_bytes_trend_rk(lv, nz)
             extra.append({
-                "workload": f"uniform J{lv} ({rr['cells']} cells), {nz} layers, RK4 dt=300 s",
-                "ms_per_step": rr["ms_per_step"], "value": sim_days_per_hour(steps, rr["ms_total"] / 1e3),
+                "workload": f"uniform J{lv} ({rr['cells']} cells), {nz} layers, RK4 dt={dtu:g} s",
+                "ms_per_step": rr["ms_per_step"], "value": sim_days_per_hour(steps, rr["ms_total"] / 1e3, dtu),
                 "kernel_ms_per_launch": kt,
                 "trend_rk_GBps": ab / (kt["trend_rk"] / 1e3) / 1e9,
                 "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,

@@ -5,10 +5,13 @@ white-noise free surface, RK4 with dt 300 s, 100 steps.
 
 Reported per step (printed with -s): the largest error of the layer mass,
 Theta mass and velocity relative to each field's largest magnitude, and the
-relative change of the total mass.  Bounds: the one-trend error is at FP32
-rounding of the fluxes (< 1e-5 relative), the state after 100 steps within
-1e-5 of the FP64 oracle's, and the total mass of every layer conserved to
-FP64 rounding (the FP64 divergence of shared FP32 fluxes telescopes)."""
+relative change of the total mass.  Measured on B200: one trend 4.3e-5
+(mass tendency: the divergence is a difference of six fluxes of 1e9, each
+rounded to FP32) and 1.0e-7 (velocity tendency); the state stays within
+3e-5 of the FP64 oracle's every step (2e-7 after 100 steps) and the total
+mass of every layer is conserved to 4e-15 (the FP64 divergence of shared FP32
+fluxes telescopes).  Bounds: 1e-4 for one trend and for the state after
+every step, 1e-6 after 100 steps, 1e-13 for the total mass."""
 import numpy as np
 import pytest
 
@@ -44,7 +47,7 @@ def test_mixed_trend_within_fp32_rounding_of_fp64():
     edges = np.concatenate([own, own + g.NN, own + 2 * g.NN])
     errs = [_rel(d32[0][:, own], d64[0][:, own]), _rel(d32[2][:, edges], d64[2][:, edges])]
     print("one trend, FP32 fluxes vs FP64: dmass", errs[0], "dvelo", errs[1])
-    assert max(errs) < 1e-5 and max(errs) > 0
+    assert max(errs) < 1e-4 and max(errs) > 0   # the mass divergence: differences of O(1e9) FP32 fluxes
     model.close()
 
 
@@ -75,7 +78,8 @@ def test_mixed_plain_method_100_steps_against_fp64_oracle():
                   f"total mass change {dmass:.1e}")
         worst = max(worst, *e)
         assert dmass < 1e-13, (s, dmass)
-    assert worst < 1e-5, worst
+    assert worst < 1e-4, worst
+    assert max(e) < 1e-6, e     # after 100 steps
     model.close()
 
 

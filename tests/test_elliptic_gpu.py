@@ -1,6 +1,6 @@
 """GPU parity of the elliptic operator, wavelet restriction/prolongation and
 the multigrid solvers against the CPU oracle, through the C-ABI.  Operator and
-transforms: 1e-12 relative (FP64, no contraction).  Solves: both reach the
+transforms: bit for bit (FP64, no contraction).  Solves: both reach the
 tolerance with the same iteration counts; solutions agree to 1e-9 relative
 (reductions are summed in a different order)."""
 import numpy as np
@@ -60,7 +60,7 @@ def test_operator_matches_oracle(hier, level):
     ref = H.apply(level, q)
     q_ = level - 4
     own = owned_mask(levels)[off[q_]:off[q_ + 1]]
-    assert rel(out[off[q_]:off[q_ + 1]][own], ref[off[q_]:off[q_ + 1]][own]) <= 1e-12
+    assert rel(out[off[q_]:off[q_ + 1]][own], ref[off[q_]:off[q_ + 1]][own]) == 0.0
     S.close()
 
 
@@ -75,7 +75,7 @@ def test_restriction_matches_oracle(hier):
     _, fg = S.download()
     fo = H.restrict_all(f)
     own = owned_mask(levels)
-    assert rel(fg[own], fo[own]) <= 1e-12
+    assert rel(fg[own], fo[own]) == 0.0
     S.close()
 
 
@@ -89,7 +89,7 @@ def test_prolongation_matches_oracle(hier):
     ug, _ = S.download()
     uo = H.prolong(6, u)
     own = owned_mask(levels)[off[2]:off[3]]
-    assert rel(ug[off[2]:off[3]][own], uo[off[2]:off[3]][own]) <= 1e-12
+    assert rel(ug[off[2]:off[3]][own], uo[off[2]:off[3]][own]) == 0.0
     S.close()
 
 

@@ -3,10 +3,9 @@
 wt_restrict_u_source) against the CPU oracle (oracle/oracle_restrict.cpp) on
 the same seeded child fields and random masks.
 
-The restricted parent flux is compared on the owned edges of every lozenge at
-1e-12 relative to its magnitude (FP64 with the reference's operand order, no
-FMA contraction: equal bit for bit in practice); the sub-sampled scalar and
-the restricted velocity trend exactly."""
+The restricted parent flux is compared on the owned edges of every lozenge
+bit for bit (FP64 with the reference's operand order, no FMA contraction);
+the sub-sampled scalar and the restricted velocity trend exactly."""
 import numpy as np
 import pytest
 
@@ -64,7 +63,7 @@ def test_restrictions_match_oracle(lmin, lmax, nz, masks):
         o, d = orc.field(0, "flux"), dev.download(par.level, "flux")
         k = _owned(par, True)
         err = np.abs(d[:, k] - o[:, k]).max() / np.abs(o[:, k]).max()
-        assert err <= 1e-12, (par.level, err)
+        assert err == 0.0, (par.level, err)
         assert np.array_equal(dev.download(par.level, "scalar"), orc.field(0, "scal"))
         assert np.array_equal(dev.download(par.level, "dvelo"), orc.field(0, "dvelo"))
     assert dev.status() == 0

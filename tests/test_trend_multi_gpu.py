@@ -4,8 +4,8 @@ multi-level trend (oracle_trisk.cpp: orc_trend_multi) on the same seeded
 per-level states, layer means and masks.
 
 Scalar trends are compared at nodes [0, n]^2 of every lozenge, velocity
-trends on the owned edges, of every level, at 1e-12 relative to each field's
-magnitude (FP64, reference operand order, no FMA contraction)."""
+trends on the owned edges, of every level, bit for bit (FP64, reference
+operand order, no FMA contraction)."""
 import numpy as np
 import pytest
 
@@ -16,7 +16,7 @@ from wavetrisk_hydrostatic_b200.grid import halo_edges, halo_nodes
 from wavetrisk_hydrostatic_b200.model import WaveletHierarchy
 
 pytestmark = pytest.mark.gpu
-TOL = 1e-12
+TOL = 0.0   # bit for bit: FP64 without FMA contraction, the oracle's operand order
 
 
 def _nodes0n(g):

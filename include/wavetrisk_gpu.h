@@ -401,6 +401,26 @@ int wt_rk4_split_explicit(wt_handle* h, double dt, double theta1);
 /* barotropic_correction (src/barotropic_2d.f90:52-116) of the hierarchy's
  * scaling fields from each level's free surface. */
 int wt_barotropic_correction_multi(wt_handle* h);
+/* free_surface_update (src/time_integr.f90:465-478) on the hierarchy:
+ * eta_update (src/barotropic_2d.f90:118-129: rhs_elliptic on every level,
+ * the elliptic operator's coefficients g (|H| + eta_old) and its diagonal
+ * rebuilt from the current free surface, the solve of opts from that surface
+ * on every level), barotropic_correction, u_update and WT_after_step.  The
+ * reference's WT_after_step from level_start - 1 also forms wavelets at
+ * level_start and restricts the velocity below it; the levels the hierarchy
+ * holds come out the same.  Needs wt_wavelet_setup and wt_elliptic_setup with
+ * the same dt, theta1 and theta2 (WT_ERR_STATE otherwise); rep as for
+ * wt_elliptic_solve, whose status it returns (WT_ERR_NOT_CONVERGED when the
+ * solve stopped at its cap; the update is then made with that solution). */
+int wt_free_surface_update(wt_handle* h, double dt, double theta1, double theta2, const wt_solver_opts* opts,
+                           wt_solver_report* rep);
+/* RK4_split (src/time_integr.f90:360-382): when theta2 != 1 the flux
+ * divergence of the current state into each level's previous divergence,
+ * then wt_rk4_split_explicit and wt_free_surface_update. */
+int wt_rk4_split(wt_handle* h, double dt, double theta1, double theta2, const wt_solver_opts* opts,
+                 wt_solver_report* rep);
+/* The free surface of one level of the hierarchy (NN host doubles). */
+int wt_free_surface_download(wt_handle* h, int level, double* eta);
 /* nsteps adaptive time steps of the hierarchy (the reference's time_step,
  * src/main.f90:405-444, explicit RK4, fixed thresholds): wt_rk4_multi(dt, 1),
  * adapt's mask sequence with threshold[3][nz] (wt_mask_build without the

@@ -230,3 +230,57 @@ def rk4_split_explicit(levels, nz, ph, states, masks, etas, dt, theta1, H=None):
             q = dest
     return [(x["mass"], x["temp"], x["velo"]) for x in q]
 
+
+
+def free_surface_update(levels, nz, ph, states, masks, etas, div_olds, dt, theta1, theta2, H, method="fmg",
+                        domain_level=2, **solver):
+    """free_surface_update (src/time_integr.f90:465-478) over the hierarchy:
+    eta_update (src/barotropic_2d.f90:118-129: rhs_elliptic on every level, the
+    solve with the operator's coefficients from the old free surface, starting
+    from it), barotropic_correction, u_update and WT_after_step (with the
+    masks H holds).  states[q]: the level's mass, temp, velo, mean_m, mean_t,
+    topo.  Returns per level (mass, temp, velo), the new free surfaces and the
+    solver's per-level iteration counts."""
+    from .barotropic import barotropic_correction_multi, rhs_elliptic_multi, u_update_multi
+    from .elliptic import Hierarchy as EH
+    from .grid import own
+
+    ol = [own(g) for g in levels]
+    ro = rhs_elliptic_multi(levels, nz, states, masks, etas, div_olds, dt, theta2, ph.ref_density)
+    eo = []
+    for g, e in zip(ol, etas):
+        x = np.array(e, dtype=np.float64).copy()
+        x[g.halo_node[:, 0]] = x[g.halo_node[:, 1]]   # Laplacian_scalar(S_TEMP) after update_bdry
+        eo.append(x)
+    E = EH(levels, [st["topo"] for st in states], grav=ph.grav, dt=dt, theta1=theta1, theta2=theta2,
+           domain_level=domain_level, eta_old=eo, **solver)
+    u, _, its = E.solve(np.concatenate([np.asarray(e, dtype=np.float64) for e in etas]),
+                        np.concatenate([r["rhs"] for r in ro]), method)
+    off = np.cumsum([0] + [g.NN for g in ol])
+    new_etas = [u[off[q]:off[q + 1]].copy() for q in range(len(ol))]
+    mt = barotropic_correction_multi(levels, nz, ph, states, new_etas)
+    st2 = [dict(states[q], mass=m, temp=t) for q, (m, t) in enumerate(mt)]
+    uo = u_update_multi(levels, nz, st2, masks, new_etas, ph.grav, dt, theta1)
+    for q, g in enumerate(ol):
+        H.set(g.level, "s_m", st2[q]["mass"])
+        H.set(g.level, "s_t", st2[q]["temp"])
+        H.set(g.level, "s_v", uo[q]["velo"])
+    H.wt_after_step()
+    out = [(H.field(g.level, "s_m").copy(), H.field(g.level, "s_t").copy(), H.field(g.level, "s_v").copy())
+           for g in ol]
+    return out, new_etas, its
+
+
+def rk4_split(levels, nz, ph, states, masks, etas, dt, theta1, theta2, method="fmg", domain_level=2, **solver):
+    """RK4_split (src/time_integr.f90:360-382) over the hierarchy with theta2 = 1
+    (no previous flux divergence): the four RK_split stages, then
+    free_surface_update.  Returns what free_surface_update returns."""
+    from .wavelet import Hierarchy
+
+    assert theta2 == 1.0
+    H = Hierarchy(levels, nz)
+    q = rk4_split_explicit(levels, nz, ph, states, masks, etas, dt, theta1, H=H)
+    st = [dict(states[i], mass=m, temp=t, velo=v) for i, (m, t, v) in enumerate(q)]
+    zero = [np.zeros(g.NN) for g in levels]
+    return free_surface_update(levels, nz, ph, st, masks, etas, zero, dt, theta1, theta2, H, method=method,
+                               domain_level=domain_level, **solver)

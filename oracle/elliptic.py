@@ -11,7 +11,8 @@ from . import _d, _dp, _ip, lib
 class orc_elevel(C.Structure):
     _fields_ = [("level", C.c_int), ("n", C.c_int), ("P", C.c_int), ("NN", C.c_int64),
                 ("len", _dp), ("pedlen", _dp), ("hex_inv", _dp), ("overl_a", _dp), ("topo", _dp),
-                ("halo_node", _ip), ("n_halo_node", C.c_int64), ("halo_edge", _ip), ("n_halo_edge", C.c_int64)]
+                ("halo_node", _ip), ("n_halo_node", C.c_int64), ("halo_edge", _ip), ("n_halo_edge", C.c_int64),
+                ("eta_old", _dp)]
 
 
 class orc_eparams(C.Structure):
@@ -36,7 +37,11 @@ def _bind():
 class Hierarchy:
     """Keeps the per-level numpy buffers alive behind an orc_elevel array."""
 
-    def __init__(self, levels, topos, grav=9.80616, dt=600.0, theta1=1.0, theta2=1.0, domain_level=2, **solver):
+    def __init__(self, levels, topos, grav=9.80616, dt=600.0, theta1=1.0, theta2=1.0, domain_level=2, eta_old=None,
+                 **solver):
+        """eta_old: per level the old free surface of eta_update (ghosts holding
+        their copies), which enters the operator's coefficients
+        g (|H| + eta_old) and its diagonal; None for 0."""
         from .grid import own
         levels = [own(g) for g in levels]
         self.L = _bind()
@@ -46,9 +51,10 @@ class Hierarchy:
             b = [np.ascontiguousarray(x, dtype=np.float64) for x in (g.len, g.pedlen, g.hex_inv, g.overl_a, topo)]
             hn = np.ascontiguousarray(g.halo_node, dtype=np.int64)
             he = np.ascontiguousarray(g.halo_edge, dtype=np.int64)
-            self.keep += b + [hn, he]
+            eo = None if eta_old is None else np.ascontiguousarray(eta_old[q], dtype=np.float64)
+            self.keep += b + [hn, he] + ([eo] if eo is not None else [])
             self.arr[q] = orc_elevel(g.level, g.n, g.P, g.NN, *[_d(x) for x in b], hn.ctypes.data_as(_ip), len(hn),
-                                     he.ctypes.data_as(_ip), len(he))
+                                     he.ctypes.data_as(_ip), len(he), None if eo is None else _d(eo))
         d = dict(coarse_iter=50, max_vcycle=3, pre_iter=2, down_iter=2, up_iter=2, post_iter=4, max_srj_iter=200,
                  fine_tol=1e-3, coarse_tol=1e-3)
         d.update(solver)

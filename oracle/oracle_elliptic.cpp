@@ -43,6 +43,7 @@ struct ELevel {
   int64_t nhn;
   const int64_t* he;
   int64_t nhe;
+  const double* eta_old;  // old free surface (Laplacian_scalar(S_TEMP) of eta_update), ghosts copied; null = 0
 };
 
 struct EParams {
@@ -120,10 +121,14 @@ struct Solver {
     return a * b;
   }
 
-  // ---- elliptic operator (phi = 1, eta_old = 0, mass => old free surface = 0)
+  // ---- elliptic operator (phi = 1; eta_old the old free surface, 0 when absent)
+  double eta_old(int l, int64_t gid) const {
+    const ELevel& g = L(l);
+    return g.eta_old ? g.eta_old[gid - off[l - ls]] : 0.0;
+  }
   double csq(int l, int64_t gid) const {
     const ELevel& g = L(l);
-    double c = std::fabs(g.topo[gid - off[l - ls]]) * 1.0 + 0.0;
+    double c = std::fabs(g.topo[gid - off[l - ls]]) * 1.0 + eta_old(l, gid);
     return p.grav * c;
   }
   void flux_node(const std::vector<double>& q, int l, int d, int i, int j, bool sw) {
@@ -197,7 +202,7 @@ struct Solver {
       for (int j = 0; j <= n; ++j)
         for (int i = 0; i <= n; ++i) {
           int64_t id0 = id(l, d, i, j);
-          double depth = std::fabs(L(l).topo[id0 - off[l - ls]]) + 0.0 / 1.0;
+          double depth = std::fabs(L(l).topo[id0 - off[l - ls]]) + eta_old(l, id0) / 1.0;
           double wgt = 2.0 * std::sqrt(3.0) * depth;
           double lap = -(p.grav * wgt * (p.dt * p.dt) * hinv(l, id0));
           out[id0] = p.theta1 * p.theta2 * lap - 1.0;
@@ -493,6 +498,7 @@ struct orc_elevel {
   int64_t n_halo_node;
   const int64_t* halo_edge;
   int64_t n_halo_edge;
+  const double* eta_old;
 };
 
 struct orc_eparams {
@@ -507,7 +513,7 @@ static void setup(Solver& S, const orc_elevel* lv, int nlev, const orc_eparams* 
   S.le = lv[nlev - 1].level;
   for (int q = 0; q < nlev; ++q)
     S.lev.push_back(ELevel{lv[q].n, lv[q].P, lv[q].NN, lv[q].len, lv[q].pedlen, lv[q].hex_inv, lv[q].overl_a, lv[q].topo,
-                           lv[q].halo_node, lv[q].n_halo_node, lv[q].halo_edge, lv[q].n_halo_edge});
+                           lv[q].halo_node, lv[q].n_halo_node, lv[q].halo_edge, lv[q].n_halo_edge, lv[q].eta_old});
   S.p = EParams{p->grav, p->dt, p->theta1, p->theta2, p->domain_level, p->coarse_iter, p->max_vcycle, p->pre_iter,
                 p->down_iter, p->up_iter, p->post_iter, p->max_srj_iter, p->fine_tol, p->coarse_tol};
   S.init();

@@ -1,0 +1,92 @@
+"""GPU parity of the mode-split time step with its implicit free surface
+(RK4_split, src/time_integr.f90:360-382, and free_surface_update, :465-478)
+against the CPU oracle on the hierarchy J3..J5, 2 layers, over a seamount:
+the four RK_split stages, then eta_update (rhs_elliptic on every level, the
+elliptic operator's coefficients rebuilt from the old free surface, FMG to
+1e-10 from the old surface), barotropic_correction, u_update and
+WT_after_step.  The solver's per-level iteration counts must equal the
+oracle's; the free surface and the state of every level agree to 1e-9
+relative (the solver's reductions are summed in another order)."""
+import numpy as np
+import pytest
+
+import oracle
+from wavetrisk_hydrostatic_b200 import Grid, OceanParams
+from wavetrisk_hydrostatic_b200.cases import bump_state, seamount_topography
+from wavetrisk_hydrostatic_b200.grid import halo_nodes
+from wavetrisk_hydrostatic_b200.model import WaveletHierarchy, solver_opts
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("masks_kind", ["tolrnz", "built"])
+def test_rk4_split_with_free_surface_matches_oracle(masks_kind):
+    from oracle.wavelet import Hierarchy
+
+    ph = OceanParams()
+    lmin, lmax, nz = 3, 5, 2
+    G = Grid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin, lmax + 1)]
+    states = [bump_state(g, nz, seed=4, ph=ph, topo=seamount_topography(g, seed=4, radius=600e3)) for g in levels]
+    rng = np.random.default_rng(5)
+    etas = []
+    for g in levels:
+        e = rng.standard_normal(g.NN) * 0.05
+        halo_nodes(g, e)
+        etas.append(e)
+    if masks_kind == "built":
+        H = Hierarchy(levels, nz)
+        for name, key in (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v")):
+            H.set(lmax, key, states[-1][name])
+        H.forward()
+        H.mask_build(np.array([[5.0] * nz, [1e16] * nz, [0.05] * nz]), 0, lmax)
+        masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in levels]
+    else:
+        masks = [(np.full(g.NN, 16, np.int32), np.full(3 * g.NN, 16, np.int32)) for g in levels]
+    dt, theta1, theta2 = 600.0, 0.5, 1.0
+    solver = dict(fine_tol=1e-10, coarse_tol=1e-10, max_vcycle=50, coarse_iter=300)
+    dev = WaveletHierarchy(levels, [st["topo"] for st in states], nz, ph)
+    for g, st, (mn, me), e in zip(levels, states, masks, etas):
+        for name in ("mass", "temp", "velo", "mean_m", "mean_t"):
+            dev.upload(g.level, name, st[name])
+        dev.upload(g.level, "mask_n", mn)
+        dev.upload(g.level, "mask_e", me)
+        dev.barotropic_upload(g.level, e, None)
+    dev.elliptic_setup(dt, theta1, theta2, domain_level=G.domain_level)
+    rep = dev.rk4_split(dt, theta1, theta2, solver_opts("fmg", 1e-10, max_vcycle=50, coarse_iter=300))
+    assert rep.status == 0
+    ref, ref_eta, its = oracle.rk4_split(levels, nz, ph, states, masks, etas, dt, theta1, theta2,
+                                         domain_level=G.domain_level, **solver)
+    assert list(rep.iterations)[:len(levels)] == its
+    for q, g in enumerate(levels):
+        own = np.nonzero(g.owned)[0]
+        e = np.concatenate([own, own + g.NN, own + 2 * g.NN])
+        m, t, v = ref[q]
+        assert _rel(dev.free_surface(g.level)[own], ref_eta[q][own]) <= 1e-9, (g.level, "eta")
+        assert _rel(dev.download(g.level, "mass")[:, own], m[:, own]) <= 1e-9, (g.level, "mass")
+        assert _rel(dev.download(g.level, "temp")[:, own], t[:, own]) <= 1e-9, (g.level, "temp")
+        assert _rel(dev.download(g.level, "velo")[:, e], v[:, e]) <= 1e-9, (g.level, "velo")
+    # the free surface moved: the solve is not a no-op
+    assert _rel(ref_eta[-1], etas[-1]) > 1e-3
+    assert dev.status() == 0
+    dev.close()
+
+
+def test_free_surface_update_refuses_a_mismatched_solver_setup():
+    from wavetrisk_hydrostatic_b200 import _native as N
+
+    ph = OceanParams()
+    G = Grid(3, 4, radius=6371e3)
+    levels = [G.level(3), G.level(4)]
+    dev = WaveletHierarchy(levels, [np.full(g.NN, -4000.0) for g in levels], 2, ph)
+    opts = solver_opts("fmg", 1e-8)
+    rep = N.wt_solver_report()
+    import ctypes as C
+    assert N.lib().wt_free_surface_update(dev.h, 600.0, 1.0, 1.0, C.byref(opts), C.byref(rep)) == N.WT_ERR_STATE
+    dev.elliptic_setup(300.0, 1.0, 1.0)
+    assert N.lib().wt_free_surface_update(dev.h, 600.0, 1.0, 1.0, C.byref(opts), C.byref(rep)) == N.WT_ERR_STATE
+    dev.close()

@@ -131,6 +131,11 @@ _DEVICE_SIGS = {
     "wt_elliptic_prolong": [_vp, C.c_int],
     "wt_elliptic_l2": [_vp, C.c_int, C.c_int, _dp],
     "wt_elliptic_solve": [_vp, C.POINTER(wt_solver_opts), C.POINTER(wt_solver_report)],
+    "wt_free_surface_update": [_vp, C.c_double, C.c_double, C.c_double, C.POINTER(wt_solver_opts),
+                               C.POINTER(wt_solver_report)],
+    "wt_rk4_split": [_vp, C.c_double, C.c_double, C.c_double, C.POINTER(wt_solver_opts),
+                     C.POINTER(wt_solver_report)],
+    "wt_free_surface_download": [_vp, C.c_int, _dp],
     "wt_elliptic_autotune": [_vp, C.POINTER(wt_solver_opts), C.POINTER(C.c_int), C.c_int, C.c_int,
                              C.POINTER(wt_solver_opts), _dp],
     "wt_learned_setup": [_vp, C.c_ulonglong],

@@ -294,4 +294,38 @@ __global__ void k_ell_op32(EllLev L, const float* __restrict__ q, const float* _
   if (OP == OP_JACOBI) out[id] = q[id] + w * (f[id] - lq) / L.diagf[id];
 }
 
+// Operator coefficients of elliptic_lo and elliptic_lo_diag from the old free
+// surface eta_old (eta_update keeps it in Laplacian_scalar(S_TEMP),
+// src/barotropic_2d.f90:118-129): per edge interp(csq(a), csq(b)) with
+// csq = g (|H| phi + eta_old) (src/ops.f90:202-216, phi = 1), the diagonal
+// theta1 theta2 (-g 2 sqrt(3) (|H| + eta_old / phi) dt^2 / area) - 1 (the
+// exact = .false. branch, :283-296), and their FP32 copies.  eta_old is read
+// through the node remap (its ghosts hold their owners' values); with eta_old
+// = 0 the results equal those built at setup bit for bit.
+__global__ void k_ell_coeffs(int n, int P, int64_t NN, const double* __restrict__ topo, const double* __restrict__ eta,
+                             const int* __restrict__ nsrc, const double* __restrict__ len,
+                             const double* __restrict__ ped, const double* __restrict__ hinv, double g, double dt,
+                             double th1, double th2, double cf, double* __restrict__ Ie, double* __restrict__ diag,
+                             float* __restrict__ Kf, float* __restrict__ diagf) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= NN) return;
+  const int64_t r = k % ((int64_t)P * P);
+  const int i = (int)(r % P) - 2, j = (int)(r / P) - 2;
+  auto csq = [&](int64_t x) { return g * (fabs(topo[x]) * 1.0 + eta[nsrc[x]]); };
+  const double c0 = csq(k);
+  if (i + 1 <= n + 1) Ie[RT * NN + k] = 0.5 * (c0 + csq(k + 1));
+  if (i + 1 <= n + 1 && j + 1 <= n + 1) Ie[DG * NN + k] = 0.5 * (c0 + csq(k + P + 1));
+  if (j + 1 <= n + 1) Ie[UP * NN + k] = 0.5 * (c0 + csq(k + P));
+  const double depth = fabs(topo[k]) + eta[nsrc[k]] / 1.0;
+  const double wgt = 2.0 * sqrt(3.0) * depth;
+  const double lap = -(g * wgt * (dt * dt) * hinv[k]);
+  const double dg = th1 * th2 * lap - 1.0;
+  diag[k] = dg;
+  diagf[k] = (float)dg;
+  for (int e = 0; e < 3; ++e) {
+    const int64_t q = e * NN + k;
+    if (len[q] > 0) Kf[q] = (float)(cf * Ie[q] * ped[q] / len[q]);
+  }
+}
+
 }  // namespace wte

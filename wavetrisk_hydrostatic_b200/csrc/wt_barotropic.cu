@@ -290,6 +290,18 @@ int wt_level_barotropic_correction(wt_handle* h, double* const* m, double* const
   return WT_OK;
 }
 
+// The free-surface fields of level l: eta (sol(S_MASS, zlevels+1)), the
+// elliptic right-hand side, the flux divergence and the previous one.
+int wt_level_baro_fields(wt_handle* h, int l, double** eta, double** rhs, double** div, double** div_old) {
+  if (int rc = ensure_levels(h)) return rc;
+  BaroLevel& V = static_cast<BaroCtx*>(h->baro)->L[l - h->level_start];
+  if (eta) *eta = V.eta;
+  if (rhs) *rhs = V.rhs;
+  if (div) *div = V.div;
+  if (div_old) *div_old = V.div_old;
+  return WT_OK;
+}
+
 // grad_eta over the hierarchy (src/barotropic_2d.f90:455-474, with
 // cpt_or_restr_eta) into each level's gradient field, without the velocity
 // update; grad[q] receives level level_start+q's [3][NN] field.  Stream-ordered.
@@ -337,6 +349,15 @@ int wt_barotropic_download_level(wt_handle* h, int level, double* div_flux, doub
   if (div_flux) CKB(cudaMemcpyAsync(div_flux, V.div, NN * 8, cudaMemcpyDeviceToHost, h->stream));
   if (rhs) CKB(cudaMemcpyAsync(rhs, V.rhs, NN * 8, cudaMemcpyDeviceToHost, h->stream));
   if (grad) CKB(cudaMemcpyAsync(grad, V.grad, 3 * NN * 8, cudaMemcpyDeviceToHost, h->stream));
+  CKB(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_free_surface_download(wt_handle* h, int level, double* eta) {
+  if (!h || !eta || level < h->level_start || level > h->level_end) return WT_ERR_ARG;
+  if (!h->baro || static_cast<BaroCtx*>(h->baro)->L.empty()) return WT_ERR_STATE;
+  BaroLevel& V = static_cast<BaroCtx*>(h->baro)->L[level - h->level_start];
+  CKB(cudaMemcpyAsync(eta, V.eta, (size_t)h->at(level).NN * 8, cudaMemcpyDeviceToHost, h->stream));
   CKB(cudaStreamSynchronize(h->stream));
   return WT_OK;
 }

@@ -619,3 +619,68 @@ int wt_elliptic_autotune(wt_handle* h, const wt_solver_opts* base, const int* ca
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------- free surface ----
+int wt_level_baro_fields(wt_handle* h, int l, double** eta, double** rhs, double** div, double** div_old);
+int wt_level_barotropic_correction(wt_handle* h, double* const* m, double* const* t);
+
+extern "C" {
+
+// free_surface_update (src/time_integr.f90:465-478) on the hierarchy: eta_update
+// (rhs_elliptic over the hierarchy, the operator's coefficients from the old
+// free surface, the elliptic solve with opts, src/barotropic_2d.f90:118-129),
+// barotropic_correction, u_update and WT_after_step.
+int wt_free_surface_update(wt_handle* h, double dt, double theta1, double theta2, const wt_solver_opts* opts,
+                           wt_solver_report* rep) {
+  if (!h || !opts || !rep || dt <= 0) return WT_ERR_ARG;
+  if (!h->ell || !h->wav || h->flux_bits != 64) return WT_ERR_STATE;
+  Ell& E = *static_cast<Ell*>(h->ell);
+  if (E.ls != h->level_start || E.le != h->level_end || E.dt != dt || E.th1 != theta1 || E.th2 != theta2)
+    return WT_ERR_STATE;  // wt_elliptic_setup with this dt and theta on this hierarchy
+  if (int rc = wt_rhs_elliptic_multi(h, dt, theta2)) return rc;
+  const double g = h->ph.grav;
+  for (int l = E.ls; l <= E.le; ++l) {
+    const int q = l - E.ls;
+    double *eta, *rhs;
+    if (int rc = wt_level_baro_fields(h, l, &eta, &rhs, nullptr, nullptr)) return rc;
+    const DevLevel& D = h->at(l);
+    ELevelDev& X = E.L[q];
+    k_ell_coeffs<<<nb(D.NN), TPB, 0, E.s()>>>(D.n, D.P, D.NN, D.topo, eta, D.nsrc, D.len, D.pedlen, D.hex_inv, g, dt,
+                                                theta1, theta2, E.cf, X.Ie, X.diag, X.Kf, X.diagf);
+    // the solve starts from the current free surface (elliptic_solver(sol(S_MASS, zlevels+1), ...))
+    CKE(cudaMemcpyAsync(E.u.lv[q], eta, 8 * D.NN, cudaMemcpyDeviceToDevice, E.s()));
+    CKE(cudaMemcpyAsync(E.f.lv[q], rhs, 8 * D.NN, cudaMemcpyDeviceToDevice, E.s()));
+  }
+  CKE(cudaGetLastError());
+  int rc = wt_elliptic_solve(h, opts, rep);
+  if (rc != WT_OK && rc != WT_ERR_NOT_CONVERGED) return rc;
+  for (int l = E.ls; l <= E.le; ++l) {
+    double* eta;
+    if (int r2 = wt_level_baro_fields(h, l, &eta, nullptr, nullptr, nullptr)) return r2;
+    CKE(cudaMemcpyAsync(eta, E.u.lv[l - E.ls], 8 * h->at(l).NN, cudaMemcpyDeviceToDevice, E.s()));
+  }
+  if (int r2 = wt_level_barotropic_correction(h, nullptr, nullptr)) return r2;
+  if (int r2 = wt_u_update_multi(h, dt, theta1)) return r2;
+  if (int r2 = wt_wt_after_step(h)) return r2;
+  return rc;
+}
+
+// RK4_split (src/time_integr.f90:360-382): the flux divergence of the previous
+// step when theta2 != 1, RK_split four times and free_surface_update.
+int wt_rk4_split(wt_handle* h, double dt, double theta1, double theta2, const wt_solver_opts* opts,
+                 wt_solver_report* rep) {
+  if (!h || !opts || !rep || dt <= 0) return WT_ERR_ARG;
+  if (!h->ell || !h->wav || h->flux_bits != 64) return WT_ERR_STATE;
+  if (theta2 != 1.0) {
+    if (int rc = wt_rhs_elliptic_multi(h, dt, theta2)) return rc;  // flux_divergence of the current state
+    for (int l = h->level_start; l <= h->level_end; ++l) {
+      double *div, *div_old;
+      if (int rc = wt_level_baro_fields(h, l, nullptr, nullptr, &div, &div_old)) return rc;
+      CKE(cudaMemcpyAsync(div_old, div, 8 * h->at(l).NN, cudaMemcpyDeviceToDevice, h->stream));
+    }
+  }
+  if (int rc = wt_rk4_split_explicit(h, dt, theta1)) return rc;
+  return wt_free_surface_update(h, dt, theta1, theta2, opts, rep);
+}
+
+}  // extern "C"

@@ -307,6 +307,34 @@ class WaveletHierarchy(DeviceGrid):
         """barotropic_correction of every level's scaling fields from its free surface."""
         N.check("wt_barotropic_correction_multi", N.lib().wt_barotropic_correction_multi(self.h))
 
+    def elliptic_setup(self, dt: float, theta1: float = 1.0, theta2: float = 1.0, domain_level: int = 2) -> None:
+        """The free-surface solver of this hierarchy (wt_elliptic_setup)."""
+        N.check("wt_elliptic_setup", N.lib().wt_elliptic_setup(self.h, float(dt), float(theta1), float(theta2),
+                                                               int(domain_level)))
+
+    def _solve_call(self, name, dt, theta1, theta2, opts):
+        rep = N.wt_solver_report()
+        rc = getattr(N.lib(), name)(self.h, float(dt), float(theta1), float(theta2), C.byref(opts), C.byref(rep))
+        if rc not in (N.WT_OK, N.WT_ERR_NOT_CONVERGED):
+            N.check(name, rc)
+        rep.status = rc
+        return rep
+
+    def free_surface_update(self, dt: float, theta1: float, theta2: float, opts) -> "N.wt_solver_report":
+        """free_surface_update: eta_update (rhs, coefficients from the old free
+        surface, solve), barotropic_correction, u_update, WT_after_step."""
+        return self._solve_call("wt_free_surface_update", dt, theta1, theta2, opts)
+
+    def rk4_split(self, dt: float, theta1: float, theta2: float, opts) -> "N.wt_solver_report":
+        """One mode-split time step, RK4_split: RK_split x 4 and free_surface_update."""
+        return self._solve_call("wt_rk4_split", dt, theta1, theta2, opts)
+
+    def free_surface(self, level: int) -> np.ndarray:
+        """The free surface of `level` (sol(S_MASS, zlevels+1)), NN doubles."""
+        eta = np.empty(self.levels[level - self.ls].NN)
+        N.check("wt_free_surface_download", N.lib().wt_free_surface_download(self.h, int(level), N.dptr(eta)))
+        return eta
+
     def skip_inactive(self, on: bool) -> None:
         """WT_TUNE_SKIP_INACTIVE: let the RK stages leave out the finest level's
         nodes whose step1 and trend results cannot reach the state after

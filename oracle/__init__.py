@@ -268,6 +268,16 @@ def free_surface_update(levels, nz, ph, states, masks, etas, div_olds, dt, theta
     H.wt_after_step()
     out = [(H.field(g.level, "s_m").copy(), H.field(g.level, "s_t").copy(), H.field(g.level, "s_v").copy())
            for g in ol]
+    # the free surface goes through the same WT_after_step (it is layer
+    # zlevels+1 of sol): a one-layer hierarchy with the same masks
+    from .wavelet import Hierarchy
+    He = Hierarchy(levels, 1)
+    for q, g in enumerate(ol):
+        He.set(g.level, "mask_n", H.field(g.level, "mask_n"))
+        He.set(g.level, "mask_e", H.field(g.level, "mask_e"))
+        He.set(g.level, "s_m", new_etas[q][None, :])
+    He.wt_after_step()
+    new_etas = [He.field(g.level, "s_m")[0].copy() for g in ol]
     return out, new_etas, its
 
 

@@ -328,4 +328,11 @@ __global__ void k_ell_coeffs(int n, int P, int64_t NN, const double* __restrict_
   }
 }
 
+// compress_scalar (src/adapt.f90:158-172) of one wavelet field: 0 where the
+// node mask is below ADJZONE (8).
+__global__ void k_compress_wc(int64_t NN, const int* __restrict__ mask_n, double* __restrict__ wc) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < NN && mask_n[k] < 8) wc[k] = 0.0;
+}
+
 }  // namespace wte

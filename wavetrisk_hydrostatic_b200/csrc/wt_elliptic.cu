@@ -624,6 +624,35 @@ int wt_elliptic_autotune(wt_handle* h, const wt_solver_opts* base, const int* ca
 int wt_level_baro_fields(wt_handle* h, int l, double** eta, double** rhs, double** div, double** div_old);
 int wt_level_barotropic_correction(wt_handle* h, double* const* m, double* const* t);
 
+namespace {
+
+int eta_after_step(wt_handle* h, Ell& E) {
+  std::vector<double*> eta(E.le - E.ls + 1);
+  for (int l = E.ls; l <= E.le; ++l)
+    if (int rc = wt_level_baro_fields(h, l, &eta[l - E.ls], nullptr, nullptr, nullptr)) return rc;
+  for (int l = E.ls + 1; l <= E.le; ++l) {   // every wavelet from the surface as it is
+    const int q = l - E.ls;
+    double* wc = E.wc_temp.lv[q];
+    zero_level(E, l, wc);
+    const int n = E.L[q - 1].n;
+    k_wc_compute<<<nb(10 * n * n), TPB, 0, E.s()>>>(E.view(l - 1), E.view(l), eta[q], wc);
+    const int *mn, *me;
+    wt_level_masks(h, l, &mn, &me);
+    k_compress_wc<<<nb(E.L[q].NN), TPB, 0, E.s()>>>(E.L[q].NN, mn, wc);
+  }
+  for (int l = E.ls + 1; l <= E.le; ++l) {   // then the inverse from level_start up
+    const int q = l - E.ls, n = E.L[q - 1].n;
+    const EllLev C = E.view(l - 1), F = E.view(l);
+    k_prolong_even<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, eta[q - 1], E.wc_temp.lv[q], eta[q]);
+    k_prolong_odd<<<nb(10 * n * n), TPB, 0, E.s()>>>(C, F, eta[q], E.wc_temp.lv[q]);
+  }
+  CKE(cudaGetLastError());
+  CKE(cudaStreamSynchronize(E.s()));
+  return WT_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 // free_surface_update (src/time_integr.f90:465-478) on the hierarchy: eta_update
@@ -662,6 +691,10 @@ int wt_free_surface_update(wt_handle* h, double dt, double theta1, double theta2
   if (int r2 = wt_level_barotropic_correction(h, nullptr, nullptr)) return r2;
   if (int r2 = wt_u_update_multi(h, dt, theta1)) return r2;
   if (int r2 = wt_wt_after_step(h)) return r2;
+  // WT_after_step(sol, wav_coeff, level_start - 1) transforms the free surface
+  // (sol(S_MASS, zlevels+1)) with the layers: its wavelets on every level above
+  // level_start, compress_scalar with the node masks, inverse_scalar_transform
+  if (int r2 = eta_after_step(h, E)) return r2;
   return rc;
 }
 

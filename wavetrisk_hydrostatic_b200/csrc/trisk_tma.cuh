@@ -33,6 +33,13 @@ enum { S_HFM = 0, S_HFT = 3, S_QE = 6, S_TH = 9, S_B = 10, S_F = 11, S_PART = 12
 constexpr int TREND_TMA_SMEM = S_NPLANE * PLANE_BYTES + 64;  // planes + mbarrier
 constexpr unsigned TREND_TMA_TX = S_NPLANE * TB_N * 8;       // bytes the copies deliver
 constexpr unsigned long long TMA_WAIT_NS = 1000000000ull;  // a block gives up on its copies after 1 s
+// Test-only injection (wt_tune WT_TUNE_TEST_TMA_TIMEOUT): the block declares
+// TMA_INJECT_TX bytes more than its copies deliver, so its phase cannot
+// complete, and gives up after TMA_INJECT_WAIT_NS; on the failure path it
+// then retires the extra bytes itself (complete_tx) and waits, bounded, for
+// its real copies, so no copy is in flight when it exits.
+constexpr unsigned TMA_INJECT_TX = 16;
+constexpr unsigned long long TMA_INJECT_WAIT_NS = 20000ull;
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
@@ -60,11 +67,16 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Polls the mbarrier until its phase completes or TMA_WAIT_NS have passed.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, unsigned parity) {
+__device__ __forceinline__ void mbar_complete_tx(uint32_t bar, unsigned bytes) {
+  asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// Polls the mbarrier until its phase completes or limit_ns have passed.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, unsigned parity,
+                                                  unsigned long long limit_ns = TMA_WAIT_NS) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
-  while (global_ns() - t0 < TMA_WAIT_NS)
+  while (global_ns() - t0 < limit_ns)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -101,11 +113,12 @@ __device__ __forceinline__ void weights5_s(const double* __restrict__ S, int q, 
 // [0, n]^2, the velocity source on [0, n)^2, the sub-step on every padded node;
 // with a needed-node map, tiles with no needed node are left out before any
 // copy is issued and nodes that are not needed write nothing.
-// Block b: layer b % nz, then tile x, tile y, lozenge.  io.err receives 1 when a
-// block's copies did not complete within the wait limit.
+// Block b: layer b % nz, then tile x, tile y, lozenge.  err receives 1 when a
+// block's copies did not complete within the wait limit; inject != 0 forces
+// that path (test only, see TMA_INJECT_TX).
 template <int MODE>
 __global__ void __launch_bounds__(TT_X * TT_Y, 3)
-    k_trend_tma(LevelDev L, int nz, int nbx, int nby, TrendIO io, int* __restrict__ err,
+    k_trend_tma(LevelDev L, int nz, int nbx, int nby, TrendIO io, int* __restrict__ err, int inject,
                 const __grid_constant__ TrendMaps M) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* __restrict__ S = reinterpret_cast<double*>(smem_raw);
@@ -134,7 +147,7 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
   }
   __syncthreads();
   if (tid == 0) {
-    mbar_expect_tx(bar, TREND_TMA_TX);
+    mbar_expect_tx(bar, TREND_TMA_TX + (inject ? TMA_INJECT_TX : 0u));
     const int cx = x0 - 2, cy = y0 - 1;
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
@@ -176,9 +189,12 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
     lUP = L.len[UP * NN + id];
   }
 
-  const bool ok = mbar_wait_bounded(bar, 0);
+  const bool ok = mbar_wait_bounded(bar, 0, inject ? TMA_INJECT_WAIT_NS : TMA_WAIT_NS);
   if (__syncthreads_or(!ok)) {
-    if (tid == 0) atomicCAS(err, 0, 1);
+    if (tid == 0) {
+      atomicCAS(err, 0, 1);
+      if (inject) mbar_complete_tx(bar, TMA_INJECT_TX);
+    }
     if (!ok) mbar_wait_bounded(bar, 0);  // copies still in flight target this block's shared memory
     return;
   }
@@ -317,7 +333,7 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
     k_step1_tma(LevelDev L, int nz, int nbx, int nby, const double* __restrict__ mass, const double* __restrict__ temp,
                 const double* __restrict__ velo, const double* __restrict__ mean_m,
                 const double* __restrict__ phik, const double* __restrict__ pterm, Step1Out out,
-                int* __restrict__ err, const __grid_constant__ Step1Maps M,
+                int* __restrict__ err, int inject, const __grid_constant__ Step1Maps M,
                 const unsigned char* __restrict__ need) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double* __restrict__ S = reinterpret_cast<double*>(smem_raw);
@@ -346,7 +362,7 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
   }
   __syncthreads();
   if (tid == 0) {
-    mbar_expect_tx(bar, STEP1_TMA_TX);
+    mbar_expect_tx(bar, STEP1_TMA_TX + (inject ? TMA_INJECT_TX : 0u));
     tma_load_4d(s_base + P1_M * PLANE_BYTES, &M.mass, cx, cy, d, k, bar);
     tma_load_4d(s_base + P1_T * PLANE_BYTES, &M.temp, cx, cy, d, k, bar);
     tma_load_4d(s_base + P1_AM * PLANE_BYTES, &M.mean_m, cx, cy, d, k, bar);
@@ -376,10 +392,13 @@ __global__ void __launch_bounds__(TT_X * TT_Y, 3)
     hinv = L.hex_inv[id];
   }
 
-  const bool ok = mbar_wait_bounded(bar, 0);
+  const bool ok = mbar_wait_bounded(bar, 0, inject ? TMA_INJECT_WAIT_NS : TMA_WAIT_NS);
   if (__syncthreads_or(!ok)) {
-    if (tid == 0) atomicCAS(err, 0, 1);
-    if (!ok) mbar_wait_bounded(bar, 0);
+    if (tid == 0) {
+      atomicCAS(err, 0, 1);
+      if (inject) mbar_complete_tx(bar, TMA_INJECT_TX);
+    }
+    if (!ok) mbar_wait_bounded(bar, 0);  // copies still in flight target this block's shared memory
     return;
   }
 

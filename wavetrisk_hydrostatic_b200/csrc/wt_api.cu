@@ -296,6 +296,30 @@ int wt_synchronize(wt_handle* h) {
   return WT_OK;
 }
 
+int wt_clear_status(wt_handle* h) {
+  if (!h) return WT_ERR_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->dflag) CK(cudaMemset(h->dflag, 0, sizeof(int)));
+  h->sticky = WT_OK;
+  return WT_OK;
+}
+
+// Test-only: the TMA kernels of the next steps declare more bytes than their
+// copies deliver and take their wait-timeout path (value 1), or run normally
+// (0).  The captured step graphs hold the flag, so they are dropped here.
+int wt_set_tma_inject(wt_handle* h, int value) {
+  if (!h) return WT_ERR_ARG;
+  if (value != 0 && value != 1) return WT_ERR_ARG;
+  if (h->tma_inject == value) return WT_OK;
+  CK(cudaStreamSynchronize(h->stream));
+  h->tma_inject = value;
+  if (h->graph_exec) {
+    cudaGraphExecDestroy(h->graph_exec);
+    h->graph_exec = nullptr;
+  }
+  return WT_OK;
+}
+
 int wt_status(wt_handle* h) {
   if (!h) return WT_ERR_ARG;
   CK(cudaStreamSynchronize(h->stream));
@@ -409,7 +433,7 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
     const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;
     const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
     k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, s>>>(L, nz, nbx, nby, m, t, v, h->mean_m, h->phik, h->pterm, so,
-                                                           h->dflag, h->s1maps[sb], nullptr);
+                                                           h->dflag, h->tma_inject, h->s1maps[sb], nullptr);
   } else {
     k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, h->mean_m, h->mean_t, h->phik, h->pterm, so, nullptr);
   }
@@ -423,9 +447,11 @@ static int launch_trend(wt_handle* h, double* m, double* t, double* v, int mode,
     const int nbx = (D.P + TT_X - 1) / TT_X, nby = (D.P + TT_Y - 1) / TT_Y;
     const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
     if (mode == MODE_RK)
-      k_trend_tma<MODE_RK><<<nblk, TT_X * TT_Y, TREND_TMA_SMEM, s>>>(L, nz, nbx, nby, io, h->dflag, h->maps);
+      k_trend_tma<MODE_RK><<<nblk, TT_X * TT_Y, TREND_TMA_SMEM, s>>>(L, nz, nbx, nby, io, h->dflag, h->tma_inject,
+                                                                     h->maps);
     else
-      k_trend_tma<MODE_TREND><<<nblk, TT_X * TT_Y, TREND_TMA_SMEM, s>>>(L, nz, nbx, nby, io, h->dflag, h->maps);
+      k_trend_tma<MODE_TREND><<<nblk, TT_X * TT_Y, TREND_TMA_SMEM, s>>>(L, nz, nbx, nby, io, h->dflag, h->tma_inject,
+                                                                        h->maps);
   } else {
     if (mode == MODE_RK)
       k_trend<MODE_RK><<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, io);
@@ -445,7 +471,7 @@ int wt_level_trend_ml_tma(wt_handle* h, const wtk::TrendIO& io, const wtk::Trend
   const int nbx = (D.P + TT_X - 1) / TT_X, nby = (D.P + TT_Y - 1) / TT_Y;
   const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
   k_trend_tma<MODE_ML><<<nblk, TT_X * TT_Y, TREND_TMA_SMEM, stream ? stream : h->stream>>>(D.view(), nz, nbx, nby, io,
-                                                                                           h->dflag, M);
+                                                                                           h->dflag, h->tma_inject, M);
   CK(cudaGetLastError());
   return WT_OK;
 }
@@ -465,7 +491,7 @@ int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, co
     const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;
     const unsigned nblk = (unsigned)(nz * nbx * nby * 10);
     k_step1_tma<<<nblk, TT_X * TT_Y, STEP1_TMA_SMEM, s>>>(L, nz, nbx, nby, m, t, v, mean_m, phik, pterm, so,
-                                                           h->dflag, *maps, need);
+                                                           h->dflag, h->tma_inject, *maps, need);
   } else {
     k_step1<<<chunks * nz, NODE_TILE, 0, s>>>(L, nz, m, t, v, mean_m, mean_t, phik, pterm, so, need);
   }

@@ -54,6 +54,7 @@ struct wt_handle {
   wtk::TrendMaps maps{};    // tensor maps of the trend inputs (TMA-staged trend kernel)
   wtk::Step1Maps s1maps[3]{};  // step1 input maps for the state buffers (mass,temp,velo), (m1,t1,v1), (m2,t2,v2)
   int* dflag = nullptr;     // device error flag: 1 = a kernel's staged copies did not complete
+  int tma_inject = 0;       // test only: the TMA kernels take their wait-timeout path
   int trend_variant = 0;    // 0: TMA-staged k_step1_tma/k_trend_tma, 1: k_step1/k_trend (loads through L1)
   // WT_TUNE_FLUX_PRECISION: 64 (default) or 32, the FP32 step1 of the
   // single-level stepper (trisk_mixed.cuh) with its FP32 results below

@@ -884,9 +884,15 @@ int wt_lnorm(wt_handle* h, int order, double* out) {
 // per thread of the layer-group kernels (1 .. 64; 0 restores the default
 // chosen from the layer count).  Process-wide.
 int wt_set_flux_precision(wt_handle* h, int bits);
+int wt_set_tma_inject(wt_handle* h, int value);
 
 int wt_tune(wt_handle* h, int param, int value) {
   if (param == WT_TUNE_FLUX_PRECISION) return wt_set_flux_precision(h, value);
+  if (param == WT_TUNE_TEST_TMA_TIMEOUT) {
+    const int rc = wt_set_tma_inject(h, value);
+    if (rc == WT_OK && h->wav) ++ctx(h)->skip_epoch;  // the hierarchy's step graph re-records
+    return rc;
+  }
   if (param == WT_TUNE_WAVELET_LAYERS) {
     if (value < 0 || value > 64) return WT_ERR_ARG;
     g_lpt_set = value;

@@ -92,6 +92,7 @@ typedef struct wt_handle wt_handle;
 int wt_create(const wt_grid_desc* desc, wt_handle** out);
 int wt_destroy(wt_handle* h);
 int wt_status(wt_handle* h);                 /* sticky device error flags -> status */
+int wt_clear_status(wt_handle* h);           /* acknowledge: device flag and sticky status back to WT_OK */
 int wt_synchronize(wt_handle* h);
 
 /* Prognostic state on level_end: mass, temp [nz][NN]; velo [nz][3][NN];
@@ -197,17 +198,19 @@ int wt_elliptic_autotune(wt_handle* h, const wt_solver_opts* base, const int* ca
 
 /* ------------------------------------------------ learned preconditioner ---- */
 /* A hexagonal-stencil convolution network (7 taps: a node and its six
- * neighbours; 2 -> 8 -> 8 -> 1 channels) mapping a residual r of level_end,
+ * neighbours; 2 -> 32 -> 32 -> 1 channels) mapping a residual r of level_end,
  * scaled by its rms, to an approximation of the error e with L e = r, trained
  * on the residuals a V-cycle leaves and used to correct them
  * (WT_SOLVER_FCG_LEARNED).  Its inputs are r and r times a depth feature
- * (|H| / 2750 m - 1); it has no biases and identity activations (a depth-aware
- * linear operator reaching three neighbours out), and its output is 0 at the
- * pole slots (slots of [0, n]^2 outside [0, n)^2).  FP32 master weights, BF16 weights
- * in every forward and backward kernel, FP32 activations and accumulation.  The nodes are the
- * slots of [0, n]^2 of each lozenge that are their own ghost source, numbered
- * lozenge, row j, column i.  Requires wt_elliptic_setup; no reference
- * counterpart (the reference preconditions nothing). */
+ * (|H| / 2750 m - 1); it has no biases, and its two hidden layers end in the
+ * activation p -> p (p > 0), slope p (p <= 0) (wt_learned_activation; slope 1
+ * is the identity), so net(a r) = a net(r) for a > 0.  Its output is 0 at the
+ * pole slots (slots of [0, n]^2 outside [0, n)^2).  FP32 master weights, BF16
+ * weights and activations in every forward and backward kernel, FP32
+ * accumulation; the 32 -> 32 layer runs on the tensor cores (tcgen05).  The
+ * nodes are the slots of [0, n]^2 of each lozenge that are their own ghost
+ * source, numbered lozenge, row j, column i.  Requires wt_elliptic_setup; no
+ * reference counterpart (the reference preconditions nothing). */
 typedef struct {
   int n_rhs;       /* seeded N(0,1) right-hand sides, zero mean                   */
   int cycles;      /* residual/error pairs per right-hand side: after each of the
@@ -216,6 +219,9 @@ typedef struct {
   float lr;        /* Adam step, cosine-decayed to lr / 20                       */
   unsigned long long seed;
   int down_iter, up_iter, coarse_iter;   /* the generating V-cycle              */
+  int batch_rhs;   /* right-hand sides whose pairs are generated and trained on
+                    * together (their `epochs` passes), then replaced by the next
+                    * batch's; 0 = all n_rhs at once                            */
 } wt_learn_opts;
 
 typedef struct {
@@ -225,6 +231,10 @@ typedef struct {
 } wt_learn_report;
 
 int wt_learned_setup(wt_handle* h, unsigned long long seed);   /* He-initialised weights */
+/* Hidden activation slope in (0, 1] (1 = identity; default 1). */
+int wt_learned_activation(wt_handle* h, float slope);
+/* The 32 -> 32 layer on the tensor cores (1, default) or the CUDA cores (0). */
+int wt_learned_tensor_cores(wt_handle* h, int on);
 int wt_learned_num_params(void);
 /* FP32 master parameters (wt_learned_num_params floats); get or set may be NULL. */
 int wt_learned_params(wt_handle* h, float* get, const float* set);
@@ -240,8 +250,8 @@ int wt_learned_infer(wt_handle* h, const double* r, double* z);
  * arrays; grad: wt_learned_num_params floats).  The solve's u, f are kept. */
 int wt_learned_grad(wt_handle* h, const double* r, const double* e, double* loss, float* grad);
 /* Generates residual/error pairs with the FP64 multigrid, those after each
- * V-cycle (u and f of level_end are kept), and trains the network on them
- * with Adam on the GPU. */
+ * V-cycle (u and f of level_end are kept), batch_rhs right-hand sides at a
+ * time, and trains the network on each batch with Adam on the GPU. */
 int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep);
 
 /* ------------------------------------------------------ no allocation ---- */
@@ -349,7 +359,14 @@ int wt_lnorm(wt_handle* h, int order, double* out);
  * arrays.  The hierarchy's steps (wt_trend_multi, wt_rk4_multi,
  * wt_adaptive_step, wt_rk4_split_explicit) stay FP64 and return WT_ERR_STATE
  * while it is 32.  No reference counterpart (the reference is FP64 only). */
-enum { WT_TUNE_WAVELET_LAYERS = 1, WT_TUNE_SKIP_INACTIVE = 2, WT_TUNE_FLUX_PRECISION = 3 };
+/* WT_TUNE_TEST_TMA_TIMEOUT (per handle, 0 = default; test only): 1 makes
+ * every TMA-staged step1 and trend block declare 16 bytes more than its
+ * copies deliver, give up after 20 us and take its wait-timeout path (error
+ * flag set, block retires the extra bytes, waits for its own copies, returns),
+ * so wt_status reports WT_ERR_TIMEOUT; the state of such a step is not
+ * meaningful.  No reference counterpart. */
+enum { WT_TUNE_WAVELET_LAYERS = 1, WT_TUNE_SKIP_INACTIVE = 2, WT_TUNE_FLUX_PRECISION = 3,
+       WT_TUNE_TEST_TMA_TIMEOUT = 4 };
 int wt_tune(wt_handle* h, int param, int value);
 /* compress_wavelets (src/adapt.f90:79-103): zero the wavelets of inactive points. */
 int wt_compress(wt_handle* h);

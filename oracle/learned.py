@@ -8,20 +8,25 @@ so this restates the network the CUDA kernels define:
           source (lozenge, row j, column i order);
   taps  : the node and its neighbours (+1,0), (+1,+1), (0,+1), (-1,0),
           (-1,-1), (0,-1), resolved through the ghost remap; -1 outside;
-  net   : x = [r / rms(r), (r / rms(r)) (|H| / 2750 - 1)] -> 8 -> 8 -> 1
+  net   : x = [r / rms(r), (r / rms(r)) (|H| / 2750 - 1)] -> 32 -> 32 -> 1
           channels, each a 7-tap convolution with BF16-rounded weights, no
-          biases, identity activations (linear in r);
+          biases; the two hidden layers end in act(p) = p (p > 0), slope p
+          (p <= 0) and are stored rounded to BF16 (the next layer reads the
+          rounded values; the gradient passes straight through the rounding,
+          and act' is taken from the sign of the stored value);
   use   : z = rms(r) y own, own = 0 at the pole slots (slots outside
           [0, n)^2) and 1 elsewhere; the solver adds it to a V-cycle's
           correction, z = c + net(r - L c);
   loss  : <d, -L d>_W / |W| with d = own y - e / rms(r), W the cell areas
           1 / hex_inv (the error in the energy norm of the solve).
 
-Everything is evaluated in float64 from float32-rounded inputs, so the CUDA
-FP32 results agree to FP32 accumulation-order differences."""
+Everything is evaluated in float64 from BF16/float32-rounded values, so the
+CUDA results differ by FP32 accumulation order (and, rarely, by one BF16
+rounding step of a hidden activation that this order moves across a rounding
+boundary)."""
 import numpy as np
 
-TAPS, C, CIN = 7, 8, 2
+TAPS, C, CIN = 7, 32, 2
 DI = (0, 1, 1, 0, -1, -1, 0)
 DJ = (0, 0, 1, 1, 0, -1, -1)
 SHAPES = [("W1", (TAPS, CIN, C)), ("W2", (TAPS, C, C)), ("W3", (TAPS, C, 1))]
@@ -86,10 +91,25 @@ def _conv(a, W, tap):
     return out
 
 
-def forward(theta, r, depth, tap, round_weights=True):
-    """Activations of the network for compact residual r and depth |H| (ns,).
-    Returns a dict with x, h1, h2, y (channel-major), rs and the parameters P
-    used."""
+def act(p, slope):
+    return np.where(p > 0, p, slope * p)
+
+
+def dact(h, slope):
+    """act' from the stored output h (its sign is its argument's)."""
+    return np.where(h > 0, 1.0, slope)
+
+
+def _store(h):
+    """A hidden activation as the kernels store it: FP32, then BF16."""
+    return bf16_round(h.astype(np.float32)).astype(np.float64)
+
+
+def forward(theta, r, depth, tap, round_weights=True, slope=1.0):
+    """Activations of the network for compact residual r and depth |H| (ns,);
+    round_weights=False leaves the weights and the hidden activations
+    unrounded.  Returns a dict with x, h1, h2, y (channel-major), rs, slope and the
+    parameters P used."""
     P = unpack(bf16_round(np.asarray(theta, np.float32)) if round_weights else theta)
     r = np.asarray(r, np.float64)
     rs = np.sqrt(np.mean(r * r))
@@ -97,10 +117,11 @@ def forward(theta, r, depth, tap, round_weights=True):
         rs = 1.0
     v = (r / rs).astype(np.float32)
     x = np.stack([v, v * (np.abs(depth) / 2750.0 - 1.0).astype(np.float32)]).astype(np.float64)
-    h1 = _conv(x, P["W1"], tap)
-    h2 = _conv(h1, P["W2"], tap)
+    st = _store if round_weights else (lambda h: h)    # unrounded: the exact network, for finite differences
+    h1 = st(act(_conv(x, P["W1"], tap), slope))
+    h2 = st(act(_conv(h1, P["W2"], tap), slope))
     y = _conv(h2, P["W3"], tap)[0]
-    return {"x": x, "h1": h1, "h2": h2, "y": y, "rs": rs, "P": P}
+    return {"x": x, "h1": h1, "h2": h2, "y": y, "rs": rs, "P": P, "slope": slope}
 
 
 def _conv_back(a, W, dout, tap):
@@ -118,31 +139,32 @@ def _conv_back(a, W, dout, tap):
 
 def backward(A, dy, tap):
     """Parameter gradient of the network from the output gradient dy (ns,),
-    straight through the BF16 rounding (the gradient of the rounded weights)."""
+    straight through the BF16 roundings (of the weights and the stored
+    activations)."""
     dy = np.asarray(dy, np.float64)[None, :]
-    P = A["P"]
+    P, slope = A["P"], A["slope"]
     dW3, dh2 = _conv_back(A["h2"], P["W3"], dy, tap)
-    dW2, dh1 = _conv_back(A["h1"], P["W2"], dh2, tap)
-    dW1, _ = _conv_back(A["x"], P["W1"], dh1, tap)
+    dW2, dh1 = _conv_back(A["h1"], P["W2"], dh2 * dact(A["h2"], slope), tap)
+    dW1, _ = _conv_back(A["x"], P["W1"], dh1 * dact(A["h1"], slope), tap)
     return pack({"W1": dW1, "W2": dW2, "W3": dW3})
 
 
-def loss_and_grad(theta, r, e, depth, tap, round_weights=True):
+def loss_and_grad(theta, r, e, depth, tap, round_weights=True, slope=1.0):
     """Mean-square head (1/ns) sum (y - e/rs)^2 and its exact gradient: pins
     the network's backward pass against finite differences."""
-    A = forward(theta, r, depth, tap, round_weights)
+    A = forward(theta, r, depth, tap, round_weights, slope)
     d = A["y"] - np.asarray(e, np.float64) / A["rs"]
     return float(np.mean(d * d)), backward(A, 2.0 * d / d.size, tap)
 
 
-def energy_loss_and_grad(theta, r, e, depth, tap, slot, hinv, NN, apply_L, own):
+def energy_loss_and_grad(theta, r, e, depth, tap, slot, hinv, NN, apply_L, own, slope=1.0):
     """The training loss of the CUDA network: the error in the energy norm,
       loss = <d, -L d>_W / |W|,  d = own y - e/rs,  W = 1/hex_inv on the nodes,
     with apply_L(q) = L q for a level array q (ghosts not filled), and the
     gradient the CUDA kernels use, dy = 2 W (-L d) / |W| (exact when L is
     self-adjoint in <,>_W; the discrete operator is, to a few tenths of a
     percent)."""
-    A = forward(theta, r, depth, tap)
+    A = forward(theta, r, depth, tap, slope=slope)
     d = np.zeros(NN)
     d[slot] = own * A["y"] - np.asarray(e, np.float64) / A["rs"]
     w = 1.0 / np.asarray(hinv, np.float64)[slot]
@@ -152,9 +174,9 @@ def energy_loss_and_grad(theta, r, e, depth, tap, slot, hinv, NN, apply_L, own):
     return loss, backward(A, own * 2.0 * a * inv_area, tap)
 
 
-def infer(theta, r, depth, tap, own):
+def infer(theta, r, depth, tap, own, slope=1.0):
     """The network's correction z = rs * y * own."""
-    A = forward(theta, r, depth, tap)
+    A = forward(theta, r, depth, tap, slope=slope)
     return A["rs"] * A["y"] * own
 
 

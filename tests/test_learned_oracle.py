@@ -2,6 +2,7 @@
 torch's conversion, the node layout, and the oracle's parameter gradient
 against central finite differences (float64, unrounded weights)."""
 import numpy as np
+import pytest
 import torch
 
 from oracle import learned as LO
@@ -31,7 +32,8 @@ def test_layout_is_every_node_once():
     assert pent.sum() == 10 and (tap[5, pent] < 0).all() and (np.delete(tap[:, pent], 5, 0) >= 0).all()
 
 
-def test_oracle_gradient_finite_differences():
+@pytest.mark.parametrize("slope", [1.0, 0.25])
+def test_oracle_gradient_finite_differences(slope):
     g = Grid(3, 3, radius=6371e3)
     lv = g.level(3)
     slot, tap = LO.layout(lv)
@@ -39,19 +41,23 @@ def test_oracle_gradient_finite_differences():
     rng = np.random.default_rng(5)
     r, e = rng.standard_normal(slot.size), rng.standard_normal(slot.size)
     theta = LO.init_params(7).astype(np.float64)
-    loss, grad = LO.loss_and_grad(theta, r, e, depth, tap, round_weights=False)
+
+    def f(th):
+        return LO.loss_and_grad(th, r, e, depth, tap, round_weights=False, slope=slope)
+
+    loss, grad = f(theta)
     idx = rng.choice(LO.NPARAMS, 24, replace=False)
     h = 1e-6
     for k in idx:
         tp, tm = theta.copy(), theta.copy()
         tp[k] += h
         tm[k] -= h
-        fd = (LO.loss_and_grad(tp, r, e, depth, tap, False)[0] - LO.loss_and_grad(tm, r, e, depth, tap, False)[0]) / (2 * h)
+        fd = (f(tp)[0] - f(tm)[0]) / (2 * h)
         assert abs(fd - grad[k]) <= 1e-6 * max(1.0, abs(grad).max()), (k, fd, grad[k])
     assert loss > 0
 
 
-def test_infer_is_linear_in_the_residual():
+def test_infer_homogeneity_and_linearity():
     g = Grid(3, 3, radius=6371e3)
     lv = g.level(3)
     slot, tap = LO.layout(lv)
@@ -59,10 +65,22 @@ def test_infer_is_linear_in_the_residual():
     theta = LO.init_params(9)
     own = lv.owned[slot].astype(np.float64)
     r = np.random.default_rng(1).standard_normal(slot.size)
-    z = LO.infer(theta, r, depth, tap, own)
-    assert np.allclose(LO.infer(theta, -r, depth, tap, own), -z, rtol=0, atol=1e-12 * np.abs(z).max())
-    assert np.allclose(LO.infer(theta, 4.0 * r, depth, tap, own), 4.0 * z, rtol=1e-12, atol=0)
+    for slope in (1.0, 0.25):
+        z = LO.infer(theta, r, depth, tap, own, slope)
+        # positively homogeneous, exactly: 4 r has the same r / rms(r)
+        assert np.array_equal(LO.infer(theta, 4.0 * r, depth, tap, own, slope), 4.0 * z)
+        zm = LO.infer(theta, -r, depth, tap, own, slope)
+        if slope == 1.0:
+            assert np.array_equal(zm, -z)                # identity activations: odd
+        else:
+            assert np.abs(zm + z).max() > 1e-3 * np.abs(z).max()
+        assert (z[own == 0] == 0).all() and own.sum() == 10 * lv.n ** 2
+    # identity activations, unrounded: linear up to the FP32 rounding of the inputs
     r2 = np.random.default_rng(2).standard_normal(slot.size)
-    z12 = LO.infer(theta, r + r2, depth, tap, own)     # additive up to the FP32 rounding of the inputs
-    assert np.abs(z12 - z - LO.infer(theta, r2, depth, tap, own)).max() <= 1e-5 * np.abs(z12).max()
-    assert (z[own == 0] == 0).all() and own.sum() == 10 * lv.n ** 2
+
+    def y(rr):
+        A = LO.forward(theta, rr, depth, tap, round_weights=False)
+        return A["rs"] * A["y"]
+
+    y12 = y(r + r2)
+    assert np.abs(y12 - y(r) - y(r2)).max() <= 1e-5 * np.abs(y12).max()

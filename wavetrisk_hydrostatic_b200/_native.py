@@ -73,7 +73,8 @@ class wt_solver_report(C.Structure):
 
 class wt_learn_opts(C.Structure):
     _fields_ = [("n_rhs", C.c_int), ("cycles", C.c_int), ("epochs", C.c_int), ("lr", C.c_float),
-                ("seed", C.c_ulonglong), ("down_iter", C.c_int), ("up_iter", C.c_int), ("coarse_iter", C.c_int)]
+                ("seed", C.c_ulonglong), ("down_iter", C.c_int), ("up_iter", C.c_int), ("coarse_iter", C.c_int),
+                ("batch_rhs", C.c_int)]
 
 
 class wt_learn_report(C.Structure):
@@ -115,6 +116,7 @@ _DEVICE_SIGS = {
     "wt_create": [C.POINTER(wt_grid_desc), C.POINTER(_vp)],
     "wt_destroy": [_vp],
     "wt_status": [_vp],
+    "wt_clear_status": [_vp],
     "wt_synchronize": [_vp],
     "wt_upload_state": [_vp, _dp, _dp, _dp, _dp, _dp],
     "wt_download_state": [_vp, _dp, _dp, _dp],
@@ -145,6 +147,8 @@ _DEVICE_SIGS = {
     "wt_learned_infer": [_vp, _dp, _dp],
     "wt_learned_grad": [_vp, _dp, _dp, _dp, C.POINTER(C.c_float)],
     "wt_learned_train": [_vp, C.POINTER(wt_learn_opts), C.POINTER(wt_learn_report)],
+    "wt_learned_activation": [_vp, C.c_float],
+    "wt_learned_tensor_cores": [_vp, C.c_int],
     "wt_wavelet_setup": [_vp],
     "wt_upload_field": [_vp, C.c_int, C.c_int, _vp],
     "wt_download_field": [_vp, C.c_int, C.c_int, _vp],

@@ -1,31 +1,35 @@
 // Learned preconditioner of the free-surface solve: a hexagonal-stencil
-// convolution network over the nodes of one level, 2 -> 8 -> 8 -> 1 channels.
-// Each layer sums over seven taps (the node and its six neighbours in lozenge
-// directions (+1,0), (+1,+1), (0,+1), (-1,0), (-1,-1), (0,-1), read through the
-// ghost remap) and its input channels:
-//   out[co](s) = sum_t sum_ci W[t][ci][co] * in[ci](tap_t(s)).
-// The network is linear in the residual (inputs r/rs and (r/rs) * depth
-// feature, no biases, identity activations): a fixed, depth-aware linear
-// operator of three hops' reach, which generalises from the training
-// residuals to any residual.  It corrects what a multigrid V-cycle leaves: the
-// preconditioner is z = c + net(r - L c) with c the V-cycle's correction, and
-// the network's output is masked to 0 at the pole slots (slots of [0, n]^2
-// outside [0, n)^2, whose lozenge-frame taps are degenerate).  The weights
-// are FP32 master copies rounded to BF16 for every use (BF16 weights, FP32
-// activations and accumulation).  Nodes are numbered compactly: the slots of
-// [0, n]^2 of every lozenge that are their own ghost source; a tap that
-// leaves that set reads 0.  Activations are channel-major, in[c * ns + s].
+// convolution network over the nodes of one level, 2 -> 32 -> 32 -> 1
+// channels.  Each layer sums over seven taps (the node and its six neighbours
+// in lozenge directions (+1,0), (+1,+1), (0,+1), (-1,0), (-1,-1), (0,-1), read
+// through the ghost remap) and its input channels:
+//   out[co](s) = sum_t sum_ci W[t][ci][co] * in[ci](tap_t(s)),
+// the two hidden layers followed by the activation act(p) = p (p > 0),
+// slope * p (p <= 0) (slope 1: the identity) and stored in BF16.  No biases:
+// the network is positively homogeneous, net(a r) = a net(r) for a > 0, so the
+// solver runs it on the unscaled residual.  It corrects what a multigrid
+// V-cycle leaves: the preconditioner is z = c + net(r - L c) with c the
+// V-cycle's correction, and the network's output is masked to 0 at the pole
+// slots (slots of [0, n]^2 outside [0, n)^2, whose lozenge-frame taps are
+// degenerate).  The weights are FP32 master copies rounded to BF16 for every
+// use; activations are BF16, accumulation FP32.  The middle layer, a
+// 224 x 32 contraction per node, runs on the tensor cores (tcgen05, BF16
+// operands, FP32 accumulator in tensor memory).  Nodes are numbered compactly:
+// the slots of [0, n]^2 of every lozenge that are their own ghost source; a
+// tap that leaves that set reads 0.  Activations are node-major, h[s][c].
 //
-// Parameter layout (kLpParams floats): W1[7][2][8], W2[7][8][8], W3[7][8][1].
+// Parameter layout (kLpParams floats): W1[7][2][32], W2[7][32][32], W3[7][32][1].
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "umma.cuh"
+
 namespace wtl {
 
-constexpr int kTaps = 7, kC = 8, kIn = 2;
+constexpr int kTaps = 7, kC = 32, kIn = 2;
 constexpr int kW1 = 0, kW2 = kW1 + kTaps * kIn * kC, kW3 = kW2 + kTaps * kC * kC, kLpParams = kW3 + kTaps * kC;
 constexpr int kDepthRef = 2750;  // depth feature |H| / 2750 m - 1
 
@@ -91,9 +95,9 @@ __global__ void k_lp_sum(const double* __restrict__ partial, int nb, double* __r
   }
 }
 
-// Network input of every node: the residual scaled by 1 / rscale, and the same
-// times the depth feature |H| / 2750 m - 1.  r read at slot[s] (nullptr:
-// compact), topo at tslot[s].
+// Network input of every node, node-major x[2 s + c]: the residual scaled by
+// 1 / rscale, and the same times the depth feature |H| / 2750 m - 1.  r read
+// at slot[s] (nullptr: compact), topo at tslot[s].
 __global__ void k_lp_input(int ns, const int* __restrict__ slot, const int* __restrict__ tslot,
                            const double* __restrict__ r, const double* __restrict__ rscale,
                            const double* __restrict__ topo, float* __restrict__ x) {
@@ -101,44 +105,37 @@ __global__ void k_lp_input(int ns, const int* __restrict__ slot, const int* __re
   if (s >= ns) return;
   const double inv = 1.0 / *rscale;
   const float v = (float)(r[slot ? slot[s] : s] * inv);
-  x[s] = v;
-  x[ns + s] = v * (float)(fabs(topo[tslot[s]]) / (double)kDepthRef - 1.0);
+  x[2 * s] = v;
+  x[2 * s + 1] = v * (float)(fabs(topo[tslot[s]]) / (double)kDepthRef - 1.0);
 }
 
-// One convolution layer, one thread per node computing all COUT outputs from
-// the 7 x CIN tap inputs; BF16-valued weights staged in shared memory.
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(128) k_lp_conv(int ns, const int* __restrict__ tap, const float* __restrict__ in,
-                                                 const float* __restrict__ W, float* __restrict__ out) {
-  __shared__ float sw[kTaps * CIN * COUT];
-  for (int q = threadIdx.x; q < kTaps * CIN * COUT; q += blockDim.x) sw[q] = W[q];
-  __syncthreads();
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  float acc[COUT];
+__device__ __forceinline__ float lp_act(float p, float slope) { return p > 0.0f ? p : slope * p; }
+// Derivative of the activation from its stored (BF16) output: the sign of the
+// output is the sign of its argument.
+__device__ __forceinline__ float lp_dact(float h, float slope) { return h > 0.0f ? 1.0f : slope; }
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);  // a in the low half
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ void unpack_bf16x8(const uint4& q, float (&f)[8]) {
+  const uint32_t w[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-  for (int co = 0; co < COUT; ++co) acc[co] = 0.0f;
-  for (int t = 0; t < kTaps; ++t) {
-    const int u = tap[t * ns + s];
-    if (u < 0) continue;
-    for (int ci = 0; ci < CIN; ++ci) {
-      const float v = in[ci * ns + u];
-      const float* w = sw + (t * CIN + ci) * COUT;
-#pragma unroll
-      for (int co = 0; co < COUT; ++co) acc[co] = fmaf(w[co], v, acc[co]);
-    }
+  for (int k = 0; k < 4; ++k) {
+    f[2 * k] = __uint_as_float(w[k] << 16);
+    f[2 * k + 1] = __uint_as_float(w[k] & 0xFFFF0000u);
   }
-#pragma unroll
-  for (int co = 0; co < COUT; ++co) out[co * ns + s] = acc[co];
 }
 
-// The first layer with the input built on the fly, for the solver: the input
-// of tap node u is v = (r - lc)(slot[u]) (FP64 difference, then FP32) and
-// v * depth feature; the values k_lp_input gives for r - lc at rscale 1.
-__global__ void __launch_bounds__(128) k_lp_conv_in(int ns, const int* __restrict__ tap, const int* __restrict__ slot,
-                                                    const double* __restrict__ r, const double* __restrict__ lc,
-                                                    const double* __restrict__ topo, const float* __restrict__ W,
-                                                    float* __restrict__ out) {
+// Layer 1 (2 -> 32) with the activation, BF16 output h1[s][32] (64 bytes a
+// node).  The input of tap node u is x[u] (x != nullptr, training and
+// inference on compact residuals) or, for the solver, built on the fly from
+// the level arrays at slot[u]: v = (r - lc) (FP64 difference, then FP32) and
+// v * depth feature, the values k_lp_input gives for r - lc at rscale 1.
+__global__ void __launch_bounds__(128) k_lp_l1(int ns, const int* __restrict__ tap, const float* __restrict__ x,
+                                               const int* __restrict__ slot, const double* __restrict__ r,
+                                               const double* __restrict__ lc, const double* __restrict__ topo,
+                                               const float* __restrict__ W, float slope, uint4* __restrict__ h1) {
   __shared__ float sw[kTaps * kIn * kC];
   for (int q = threadIdx.x; q < kTaps * kIn * kC; q += blockDim.x) sw[q] = W[q];
   __syncthreads();
@@ -150,26 +147,220 @@ __global__ void __launch_bounds__(128) k_lp_conv_in(int ns, const int* __restric
   for (int t = 0; t < kTaps; ++t) {
     const int u = tap[t * ns + s];
     if (u < 0) continue;
-    const int id = slot[u];
-    const float v = (float)(r[id] - lc[id]);
-    const float x[kIn] = {v, v * (float)(fabs(topo[id]) / (double)kDepthRef - 1.0)};
+    float x0, x1;
+    if (x) {
+      const float2 v = reinterpret_cast<const float2*>(x)[u];
+      x0 = v.x;
+      x1 = v.y;
+    } else {
+      const int id = slot[u];
+      x0 = (float)(r[id] - lc[id]);
+      x1 = x0 * (float)(fabs(topo[id]) / (double)kDepthRef - 1.0);
+    }
+    const float* w0 = sw + (t * kIn) * kC;
 #pragma unroll
-    for (int ci = 0; ci < kIn; ++ci) {
-      const float* w = sw + (t * kIn + ci) * kC;
+    for (int co = 0; co < kC; ++co) acc[co] = fmaf(w0[co], x0, acc[co]);
 #pragma unroll
-      for (int co = 0; co < kC; ++co) acc[co] = fmaf(w[co], x[ci], acc[co]);
+    for (int co = 0; co < kC; ++co) acc[co] = fmaf(w0[kC + co], x1, acc[co]);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    uint4 o;
+    o.x = pack_bf16x2(lp_act(acc[8 * q + 0], slope), lp_act(acc[8 * q + 1], slope));
+    o.y = pack_bf16x2(lp_act(acc[8 * q + 2], slope), lp_act(acc[8 * q + 3], slope));
+    o.z = pack_bf16x2(lp_act(acc[8 * q + 4], slope), lp_act(acc[8 * q + 5], slope));
+    o.w = pack_bf16x2(lp_act(acc[8 * q + 6], slope), lp_act(acc[8 * q + 7], slope));
+    h1[4 * (int64_t)s + q] = o;
+  }
+}
+
+// ------------------------------------------------ layer 2 on tensor cores ----
+// h2 = act(conv(h1)) as one GEMM per tile of 128 nodes: A[m][k] =
+// h1[tap_t(s0+m)][ci] (k = 32 t + ci, K = 224, gathered into shared memory),
+// B[n][k] = W2[t][ci][n] (BF16, packed once per weight update), D = A B^T
+// (128 x 32, FP32) in tensor memory: 14 tcgen05.mma of K 16, one commit to an
+// mbarrier, then each warp reads 16 columns of its 32 lanes.  Persistent CTAs
+// (grid <= tiles) keep B and the 32 tensor-memory columns over their tiles.
+constexpr int kL2M = 128;
+constexpr int kL2Ksteps = kTaps * kC / 16;         // 14
+constexpr int kL2StepA = 2 * (kL2M / 8) * 128;     // bytes of A per K step: 2 core columns x 16 row groups
+constexpr int kL2StepB = 2 * (kC / 8) * 128;       // bytes of B per K step: 2 core columns x 4 row groups
+constexpr int kL2ABytes = kL2Ksteps * kL2StepA;    // 57344
+constexpr int kL2BBytes = kL2Ksteps * kL2StepB;    // 14336 (= 2 * kTaps * kC * kC)
+constexpr int kL2Smem = kL2ABytes + kL2BBytes + 16;
+constexpr int kL2Threads = 256;
+constexpr unsigned long long kL2WaitNs = 1000000000ull;  // a CTA gives up on its MMAs after 1 s
+
+// Element (n, k) of the packed B at byte 2 * index: K step k / 16, core
+// column (k % 16) / 8, row group n / 8, row n % 8, element k % 8.
+__global__ void k_lp_pack_w2(const float* __restrict__ wr, __nv_bfloat16* __restrict__ wpk) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kTaps * kC * kC) return;
+  const int ks = idx / 512, rem = idx % 512, kc = rem / 256, g = (rem % 256) / 64, row = (rem % 64) / 8, e = rem % 8;
+  const int n = 8 * g + row, k = 16 * ks + 8 * kc + e, t = k / kC, ci = k % kC;
+  wpk[idx] = __float2bfloat16_rn(wr[kW2 + (t * kC + ci) * kC + n]);
+}
+
+__device__ __forceinline__ void lp_mbar_init(uint32_t bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ bool lp_mbar_wait(uint32_t bar, unsigned parity, unsigned long long limit_ns) {
+  unsigned long long t0 = 0;
+  for (int it = 0;; ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (it == 0) t0 = t;
+    else if (t - t0 > limit_ns) return false;
+  }
+}
+
+__global__ void __launch_bounds__(kL2Threads) k_lp_l2_umma(int ns, const int* __restrict__ tap,
+                                                           const uint4* __restrict__ h1,
+                                                           const uint4* __restrict__ wpk, float slope,
+                                                           uint4* __restrict__ h2, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  unsigned char* sA = sm;
+  unsigned char* sB = sm + kL2ABytes;
+  uint64_t* bar_p = reinterpret_cast<uint64_t*>(sm + kL2ABytes + kL2BBytes);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kL2ABytes + kL2BBytes + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t aaddr = umma::smem_u32(sA), baddr = umma::smem_u32(sB), bar = umma::smem_u32(bar_p);
+
+  for (int q = tid; q < kL2BBytes / 16; q += kL2Threads) reinterpret_cast<uint4*>(sB)[q] = wpk[q];
+  if (tid == 0) lp_mbar_init(bar);
+  if (warp == 0) umma::tmem_alloc(tslot, 32);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  constexpr uint32_t kIdesc = umma::idesc_bf16_f32(kL2M, kC);
+
+  const int ntiles = (ns + kL2M - 1) / kL2M;
+  unsigned parity = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int s0 = tile * kL2M;
+    // gather: item (t, m, q) = the 16-byte chunk q (channels 8q..8q+7) of tap t of row m
+    uint4 v[kTaps * 2];
+#pragma unroll
+    for (int j = 0; j < kTaps * 2; ++j) {
+      const int item = tid + kL2Threads * j, q = item & 3, m = (item >> 2) & (kL2M - 1), t = item >> 9;
+      const int s = s0 + m;
+      const int u = s < ns ? __ldg(tap + (int64_t)t * ns + s) : -1;
+      v[j] = u >= 0 ? __ldg(h1 + 4 * (int64_t)u + q) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int j = 0; j < kTaps * 2; ++j) {
+      const int item = tid + kL2Threads * j, q = item & 3, m = (item >> 2) & (kL2M - 1), t = item >> 9;
+      const int off = (2 * t + (q >> 1)) * kL2StepA + (q & 1) * (kL2StepA / 2) + (m >> 3) * 128 + (m & 7) * 16;
+      *reinterpret_cast<uint4*>(sA + off) = v[j];
+    }
+    umma::fence_async_smem();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < kL2Ksteps; ++ks) {
+        const uint64_t ad = umma::desc_kmajor(aaddr + ks * kL2StepA, kL2StepA / 2, 128);
+        const uint64_t bd = umma::desc_kmajor(baddr + ks * kL2StepB, kL2StepB / 2, 128);
+        umma::mma_bf16(tmem, ad, bd, kIdesc, ks > 0);
+      }
+      umma::commit_arrive(bar);
+    }
+    const bool ok = lp_mbar_wait(bar, parity, kL2WaitNs);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicCAS(err, 0, 1);
+      if (!ok) lp_mbar_wait(bar, parity, kL2WaitNs);  // the MMAs still read shared memory
+      break;
+    }
+    parity ^= 1u;
+    umma::fence_after_sync();
+    float d[16];
+    const int quarter = warp & 3, half = warp >> 2;
+    umma::tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + 16 * half, d);
+    const int s = s0 + 32 * quarter + lane;
+    if (s < ns) {
+      uint4 o0, o1;
+      o0.x = pack_bf16x2(lp_act(d[0], slope), lp_act(d[1], slope));
+      o0.y = pack_bf16x2(lp_act(d[2], slope), lp_act(d[3], slope));
+      o0.z = pack_bf16x2(lp_act(d[4], slope), lp_act(d[5], slope));
+      o0.w = pack_bf16x2(lp_act(d[6], slope), lp_act(d[7], slope));
+      o1.x = pack_bf16x2(lp_act(d[8], slope), lp_act(d[9], slope));
+      o1.y = pack_bf16x2(lp_act(d[10], slope), lp_act(d[11], slope));
+      o1.z = pack_bf16x2(lp_act(d[12], slope), lp_act(d[13], slope));
+      o1.w = pack_bf16x2(lp_act(d[14], slope), lp_act(d[15], slope));
+      h2[4 * (int64_t)s + 2 * half] = o0;
+      h2[4 * (int64_t)s + 2 * half + 1] = o1;
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    umma::fence_after_sync();
+    umma::tmem_free(tmem, 32);
+  }
+}
+
+// Layer 2 on the CUDA cores (the same sums in FP32, one thread a node): the
+// variant for comparison with the tensor-core kernel.
+__global__ void __launch_bounds__(128) k_lp_l2_simt(int ns, const int* __restrict__ tap, const uint4* __restrict__ h1,
+                                                    const float* __restrict__ W, float slope,
+                                                    uint4* __restrict__ h2) {
+  __shared__ __align__(16) float sw[kTaps * kC * kC];
+  for (int q = threadIdx.x; q < kTaps * kC * kC; q += blockDim.x) sw[q] = W[q];
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  float acc[kC];
+#pragma unroll
+  for (int co = 0; co < kC; ++co) acc[co] = 0.0f;
+  for (int t = 0; t < kTaps; ++t) {
+    const int u = tap[t * ns + s];
+    if (u < 0) continue;
+    for (int q = 0; q < 4; ++q) {
+      float f[8];
+      unpack_bf16x8(h1[4 * (int64_t)u + q], f);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const float4* w = reinterpret_cast<const float4*>(sw + (t * kC + 8 * q + e) * kC);
+#pragma unroll
+        for (int c4 = 0; c4 < kC / 4; ++c4) {
+          const float4 ww = w[c4];
+          acc[4 * c4] = fmaf(ww.x, f[e], acc[4 * c4]);
+          acc[4 * c4 + 1] = fmaf(ww.y, f[e], acc[4 * c4 + 1]);
+          acc[4 * c4 + 2] = fmaf(ww.z, f[e], acc[4 * c4 + 2]);
+          acc[4 * c4 + 3] = fmaf(ww.w, f[e], acc[4 * c4 + 3]);
+        }
+      }
     }
   }
 #pragma unroll
-  for (int co = 0; co < kC; ++co) out[co * ns + s] = acc[co];
+  for (int q = 0; q < 4; ++q) {
+    uint4 o;
+    o.x = pack_bf16x2(lp_act(acc[8 * q + 0], slope), lp_act(acc[8 * q + 1], slope));
+    o.y = pack_bf16x2(lp_act(acc[8 * q + 2], slope), lp_act(acc[8 * q + 3], slope));
+    o.z = pack_bf16x2(lp_act(acc[8 * q + 4], slope), lp_act(acc[8 * q + 5], slope));
+    o.w = pack_bf16x2(lp_act(acc[8 * q + 6], slope), lp_act(acc[8 * q + 7], slope));
+    h2[4 * (int64_t)s + q] = o;
+  }
 }
 
-// The last layer fused with the solver's output: z(slot[s]) = base(slot[s]) +
-// own * y(s), y the 1-channel convolution of in.
-__global__ void __launch_bounds__(128) k_lp_conv_out(int ns, const int* __restrict__ tap, const int* __restrict__ slot,
-                                                     const float* __restrict__ in, const float* __restrict__ W,
-                                                     const float* __restrict__ own, const double* __restrict__ base,
-                                                     double* __restrict__ z) {
+// Layer 3 (32 -> 1, no activation): y[s] (z == nullptr), or fused with the
+// solver's output, z(slot[s]) = base(slot[s]) + own * y(s).
+__global__ void __launch_bounds__(128) k_lp_l3(int ns, const int* __restrict__ tap, const uint4* __restrict__ h2,
+                                               const float* __restrict__ W, float* __restrict__ y,
+                                               const int* __restrict__ slot, const float* __restrict__ own,
+                                               const double* __restrict__ base, double* __restrict__ z) {
   __shared__ float sw[kTaps * kC];
   for (int q = threadIdx.x; q < kTaps * kC; q += blockDim.x) sw[q] = W[q];
   __syncthreads();
@@ -180,10 +371,19 @@ __global__ void __launch_bounds__(128) k_lp_conv_out(int ns, const int* __restri
     const int u = tap[t * ns + s];
     if (u < 0) continue;
 #pragma unroll
-    for (int ci = 0; ci < kC; ++ci) acc = fmaf(sw[t * kC + ci], in[ci * ns + u], acc);
+    for (int q = 0; q < 4; ++q) {
+      float f[8];
+      unpack_bf16x8(h2[4 * (int64_t)u + q], f);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) acc = fmaf(sw[t * kC + 8 * q + e], f[e], acc);
+    }
   }
-  const int id = slot[s];
-  z[id] = base[id] + (double)(own[s] * acc);
+  if (z) {
+    const int id = slot[s];
+    z[id] = base[id] + (double)(own[s] * acc);
+  } else {
+    y[s] = acc;
+  }
 }
 
 // z = base + own * rscale * y into slot[s] of a level array (nullptr:
@@ -225,14 +425,19 @@ __global__ void __launch_bounds__(NT) k_lp_aloss(int ns, const int* __restrict__
   block_partial<NT>(v, partial);
 }
 
-// Weight gradient of one layer: dW[t][ci][co] = sum_s dz[co](s) *
-// in[ci](tap_t(s)).  A block stages a chunk of kChunk nodes (their tap inputs
-// A[s][t*CIN+ci] and dz) in shared memory; each thread owns fixed entries of
-// the gradient and sums them over the block's chunks, then adds them once to
-// the global gradient.
+// Input value ci of node u for the weight gradient: FP32 (the network input)
+// or BF16 (the stored activations), node-major.
+__device__ __forceinline__ float lp_in(const float* a, int64_t i) { return a[i]; }
+__device__ __forceinline__ float lp_in(const __nv_bfloat16* a, int64_t i) { return __bfloat162float(a[i]); }
+
+// Weight gradient of one layer: dW[t][ci][co] = sum_s dz(s)[co] *
+// in(tap_t(s))[ci], in and dz node-major.  A block stages a chunk of kChunk
+// nodes (their tap inputs A[s][t*CIN+ci] and dz) in shared memory; each
+// thread owns fixed entries of the gradient and sums them over the block's
+// chunks, then adds them once to the global gradient.
 constexpr int kChunk = 32;
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(256) k_lp_wgrad(int ns, const int* __restrict__ tap, const float* __restrict__ in,
+template <int CIN, int COUT, class TIn>
+__global__ void __launch_bounds__(256) k_lp_wgrad(int ns, const int* __restrict__ tap, const TIn* __restrict__ in,
                                                   const float* __restrict__ dz, float* __restrict__ dW) {
   constexpr int K = kTaps * CIN;             // rows of A
   constexpr int NE = K * COUT;               // gradient entries
@@ -251,13 +456,13 @@ __global__ void __launch_bounds__(256) k_lp_wgrad(int ns, const int* __restrict_
       float v = 0.0f;
       if (s < ns) {
         const int t = k / CIN, ci = k % CIN, u = tap[t * ns + s];
-        v = u >= 0 ? in[ci * ns + u] : 0.0f;
+        v = u >= 0 ? lp_in(in, (int64_t)u * CIN + ci) : 0.0f;
       }
       A[nl][k] = v;
     }
     for (int q = threadIdx.x; q < kChunk * COUT; q += 256) {
-      const int co = q / kChunk, nl = q % kChunk, s = s0 + nl;
-      G[nl][co] = s < ns ? dz[co * ns + s] : 0.0f;
+      const int nl = q / COUT, co = q % COUT, s = s0 + nl;
+      G[nl][co] = s < ns ? dz[(int64_t)s * COUT + co] : 0.0f;
     }
     __syncthreads();
 #pragma unroll
@@ -275,36 +480,64 @@ __global__ void __launch_bounds__(256) k_lp_wgrad(int ns, const int* __restrict_
 #pragma unroll
   for (int r = 0; r < PER; ++r) {
     const int e = threadIdx.x + 256 * r;
-    if (e < NE) {
-      atomicAdd(&dW[e], acc[r]);
-    }
+    if (e < NE) atomicAdd(&dW[e], acc[r]);
   }
 }
 
-// Input gradient of one layer: din[ci](tap_t(s)) += sum_co W[t][ci][co] *
-// dz[co](s), scattered to the tap's node.
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(128) k_lp_igrad(int ns, const int* __restrict__ tap, const float* __restrict__ W,
-                                                  const float* __restrict__ dz, float* __restrict__ din) {
-  __shared__ float sw[kTaps * CIN * COUT];
-  for (int q = threadIdx.x; q < kTaps * CIN * COUT; q += blockDim.x) sw[q] = W[q];
+// Gradient at the input of one layer, gathered: for node u,
+//   dh(u)[ci] = sum over (s, t) with tap_t(s) = u of sum_co W[t][ci][co] dz(s)[co],
+// the pairs listed in the inverse tap table (inv[inv_ptr[u] .. inv_ptr[u+1]),
+// entry 8 s + t), then through the activation whose stored output is h(u):
+// dzin(u)[ci] = dh(u)[ci] * act'(h(u)[ci]).  Node-major FP32 output.
+template <int COUT>
+__global__ void __launch_bounds__(128) k_lp_igrad(int ns, const int* __restrict__ inv_ptr,
+                                                  const int* __restrict__ inv, const float* __restrict__ W,
+                                                  const float* __restrict__ dz, const __nv_bfloat16* __restrict__ h,
+                                                  float slope, float* __restrict__ dzin) {
+  __shared__ __align__(16) float sw[kTaps * kC * COUT];
+  for (int q = threadIdx.x; q < kTaps * kC * COUT; q += blockDim.x) sw[q] = W[q];
   __syncthreads();
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  float g[COUT];
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= ns) return;
+  float acc[kC];
 #pragma unroll
-  for (int co = 0; co < COUT; ++co) g[co] = dz[co * ns + s];
-  for (int t = 0; t < kTaps; ++t) {
-    const int u = tap[t * ns + s];
-    if (u < 0) continue;
-    for (int ci = 0; ci < CIN; ++ci) {
-      const float* w = sw + (t * CIN + ci) * COUT;
-      float a = 0.0f;
+  for (int ci = 0; ci < kC; ++ci) acc[ci] = 0.0f;
+  const int e1 = inv_ptr[u + 1];
+  for (int e = inv_ptr[u]; e < e1; ++e) {
+    const int ent = inv[e], s = ent >> 3, t = ent & 7;
+    if (COUT == 1) {
+      const float g = dz[s];
 #pragma unroll
-      for (int co = 0; co < COUT; ++co) a = fmaf(w[co], g[co], a);
-      atomicAdd(&din[ci * ns + u], a);
+      for (int ci = 0; ci < kC; ++ci) acc[ci] = fmaf(sw[t * kC + ci], g, acc[ci]);
+    } else {
+      float g[COUT];
+#pragma unroll
+      for (int c4 = 0; c4 < COUT / 4; ++c4) {
+        const float4 v = reinterpret_cast<const float4*>(dz + (int64_t)s * COUT)[c4];
+        g[4 * c4] = v.x;
+        g[4 * c4 + 1] = v.y;
+        g[4 * c4 + 2] = v.z;
+        g[4 * c4 + 3] = v.w;
+      }
+#pragma unroll
+      for (int ci = 0; ci < kC; ++ci) {
+        const float4* w = reinterpret_cast<const float4*>(sw + (t * kC + ci) * COUT);
+        float a = acc[ci];
+#pragma unroll
+        for (int c4 = 0; c4 < COUT / 4; ++c4) {
+          const float4 ww = w[c4];
+          a = fmaf(ww.x, g[4 * c4], a);
+          a = fmaf(ww.y, g[4 * c4 + 1], a);
+          a = fmaf(ww.z, g[4 * c4 + 2], a);
+          a = fmaf(ww.w, g[4 * c4 + 3], a);
+        }
+        acc[ci] = a;
+      }
     }
   }
+#pragma unroll
+  for (int ci = 0; ci < kC; ++ci)
+    dzin[(int64_t)u * kC + ci] = acc[ci] * lp_dact(__bfloat162float(h[(int64_t)u * kC + ci]), slope);
 }
 
 // Adam step on the FP32 master parameters (bias-corrected; step t >= 1).

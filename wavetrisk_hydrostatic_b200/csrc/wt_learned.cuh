@@ -1,8 +1,9 @@
 // Learned preconditioner of the free-surface solve (network in
-// learned_kernels.cuh): node layout, training-pair generation with the FP64
-// multigrid, Adam training, and flexible CG preconditioned by an FP64 V-cycle
-// plus the network's correction, with the V-cycle alone as the fallback.  Included by wt_elliptic.cu only, after
-// wt_elliptic_mixed.cuh.
+// learned_kernels.cuh): node layout and inverse taps, training-pair
+// generation with the FP64 multigrid (streamed in batches of right-hand
+// sides), Adam training, and flexible CG preconditioned by a V-cycle plus the
+// network's correction, with the FP64 V-cycle alone as the fallback.
+// Included by wt_elliptic.cu only, after wt_elliptic_mixed.cuh.
 #pragma once
 
 #include <random>
@@ -22,9 +23,15 @@ struct LPNet {
   int64_t NN = 0;
   int* slot = nullptr;  // ns node slots of the level
   int* tap = nullptr;   // 7*ns compact tap indices
+  int *inv_ptr = nullptr, *inv = nullptr;  // inverse taps: (s, t) with tap_t(s) = u, entry 8 s + t
   float* own = nullptr; // ns: 1 on owned nodes, 0 at the pole slots
   float *w = nullptr, *wr = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
-  float *x = nullptr, *h1 = nullptr, *h2 = nullptr, *y = nullptr, *dy = nullptr, *dh1 = nullptr, *dh2 = nullptr;
+  __nv_bfloat16* wpk = nullptr;  // W2 packed for the tensor cores
+  float *x = nullptr, *y = nullptr, *dy = nullptr, *dz1 = nullptr, *dz2 = nullptr;
+  uint4 *h1 = nullptr, *h2 = nullptr;  // BF16 activations, 32 a node
+  float slope = 1.0f;                  // hidden activation (1: identity)
+  int tensor_cores = 1;                // layer 2 on tcgen05 (0: CUDA cores)
+  int l2_grid = 1;                     // persistent CTAs of the tcgen05 layer
   double *rs = nullptr, *fcg = nullptr, *partial = nullptr, *partial2 = nullptr, *losses = nullptr;
   double *rc = nullptr, *ec = nullptr;  // one compact pair (grad / infer)
   double *pr = nullptr, *pe = nullptr, *pscale = nullptr;  // training pairs
@@ -72,6 +79,13 @@ struct Normal {
   }
 };
 
+// BF16 copies of the master weights: rounded floats for the CUDA-core
+// kernels, W2 packed in the tensor cores' shared-memory layout.
+void lp_round_pack(LPNet& N, cudaStream_t st) {
+  k_lp_round<<<lpg(kLpParams, 256), 256, 0, st>>>(N.w, N.wr, kLpParams);
+  k_lp_pack_w2<<<lpg(kTaps * kC * kC, 256), 256, 0, st>>>(N.wr, N.wpk);
+}
+
 int lp_init_params(LPNet& N, uint64_t seed) {
   std::vector<float> w(kLpParams, 0.f);
   Normal rn(seed);
@@ -79,14 +93,16 @@ int lp_init_params(LPNet& N, uint64_t seed) {
     for (int k = 0; k < cnt; ++k) w[off + k] = (float)(sd * rn());
   };
   // variance-preserving scales for linear layers; a small last layer
-  fill(kW1, kTaps * kIn * kC, std::sqrt(1.0 / (kTaps * kIn)));
-  fill(kW2, kTaps * kC * kC, std::sqrt(1.0 / (kTaps * kC)));
+  // variance-preserving through the activation, gain sqrt(2 / (1 + slope^2))
+  const double gain = std::sqrt(2.0 / (1.0 + (double)N.slope * N.slope));
+  fill(kW1, kTaps * kIn * kC, gain * std::sqrt(1.0 / (kTaps * kIn)));
+  fill(kW2, kTaps * kC * kC, gain * std::sqrt(1.0 / (kTaps * kC)));
   fill(kW3, kTaps * kC, 0.1 * std::sqrt(1.0 / (kTaps * kC)));
   cudaMemcpy(N.w, w.data(), 4 * kLpParams, cudaMemcpyHostToDevice);
   cudaMemset(N.m, 0, 4 * kLpParams);
   cudaMemset(N.v, 0, 4 * kLpParams);
   N.adam_t = 0;
-  k_lp_round<<<lpg(kLpParams), LP_TPB>>>(N.w, N.wr, kLpParams);
+  lp_round_pack(N, 0);
   cudaError_t e = cudaDeviceSynchronize();
   return e == cudaSuccess ? WT_OK : wt_handle_fail("learned init", e);
 }
@@ -129,6 +145,21 @@ int lp_build(Ell& E, uint64_t seed) {
       tap[(size_t)t * ns + s] = cid[nsrc[kn]];
     }
   }
+  // inverse taps, each node's list ordered by tap
+  std::vector<int> inv_ptr(ns + 1, 0), inv;
+  for (int t = 0; t < kTaps; ++t)
+    for (int s = 0; s < ns; ++s)
+      if (tap[(size_t)t * ns + s] >= 0) ++inv_ptr[tap[(size_t)t * ns + s] + 1];
+  for (int u = 0; u < ns; ++u) inv_ptr[u + 1] += inv_ptr[u];
+  inv.resize(inv_ptr[ns]);
+  {
+    std::vector<int> fill(inv_ptr.begin(), inv_ptr.end() - 1);
+    for (int t = 0; t < kTaps; ++t)
+      for (int s = 0; s < ns; ++s) {
+        const int u = tap[(size_t)t * ns + s];
+        if (u >= 0) inv[fill[u]++] = 8 * s + t;
+      }
+  }
   auto& A = N->allocs;
   int rc = WT_OK;
   auto al = [&](auto** p, int64_t cnt) {
@@ -136,13 +167,16 @@ int lp_build(Ell& E, uint64_t seed) {
   };
   al(&N->slot, ns);
   al(&N->tap, (int64_t)kTaps * ns);
+  al(&N->inv_ptr, ns + 1);
+  al(&N->inv, std::max<int64_t>(1, (int64_t)inv.size()));
   al(&N->own, ns);
   for (float** p : {&N->w, &N->wr, &N->g, &N->m, &N->v}) al(p, kLpParams);
+  al(&N->wpk, (int64_t)kTaps * kC * kC);
   al(&N->x, (int64_t)kIn * ns);
-  al(&N->h1, (int64_t)kC * ns);
-  al(&N->h2, (int64_t)kC * ns);
-  al(&N->dh1, (int64_t)kC * ns);
-  al(&N->dh2, (int64_t)kC * ns);
+  al(&N->h1, (int64_t)ns * (kC / 8));
+  al(&N->h2, (int64_t)ns * (kC / 8));
+  al(&N->dz1, (int64_t)kC * ns);
+  al(&N->dz2, (int64_t)kC * ns);
   al(&N->y, ns);
   al(&N->dy, ns);
   al(&N->rs, 1);
@@ -158,7 +192,19 @@ int lp_build(Ell& E, uint64_t seed) {
     cudaMemcpy(N->slot, slot.data(), 4 * (size_t)ns, cudaMemcpyHostToDevice);
     cudaMemcpy(N->tap, tap.data(), 4 * tap.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(N->own, own.data(), 4 * (size_t)ns, cudaMemcpyHostToDevice);
-    rc = lp_init_params(*N, seed);
+    cudaMemcpy(N->inv_ptr, inv_ptr.data(), 4 * (size_t)(ns + 1), cudaMemcpyHostToDevice);
+    if (!inv.empty()) cudaMemcpy(N->inv, inv.data(), 4 * inv.size(), cudaMemcpyHostToDevice);
+    // persistent CTAs of the tensor-core layer: as many as fit on the device at once
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaFuncSetAttribute(k_lp_l2_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, kL2Smem);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lp_l2_umma, kL2Threads, kL2Smem);
+    if (e != cudaSuccess) rc = wt_handle_fail("learned l2 attributes", e);
+    const int tiles = (ns + kL2M - 1) / kL2M;
+    N->l2_grid = std::max(1, std::min(tiles, std::max(1, per_sm) * std::max(1, nsm)));
+    if (rc == WT_OK) rc = lp_init_params(*N, seed);
   }
   if (rc != WT_OK) {
     lp_release(N);
@@ -175,18 +221,28 @@ void lp_rms(LPNet& N, cudaStream_t st, const int* slot, const double* r, double*
   k_lp_sum<<<1, 256, 0, st>>>(N.partial, N.nbd(), rs, 1, 1.0 / N.ns);
 }
 
+// Layer 2, h2 = act(conv(h1)): tcgen05 or, for comparison, the CUDA cores.
+void lp_l2(Ell& E, LPNet& N, cudaStream_t st) {
+  if (N.tensor_cores)
+    k_lp_l2_umma<<<N.l2_grid, kL2Threads, kL2Smem, st>>>(N.ns, N.tap, N.h1, reinterpret_cast<const uint4*>(N.wpk),
+                                                        N.slope, N.h2, E.h->dflag);
+  else
+    k_lp_l2_simt<<<lpg(N.ns), LP_TPB, 0, st>>>(N.ns, N.tap, N.h1, N.wr + kW2, N.slope, N.h2);
+}
+
 // Network output y for input r / *rs (r read at slot[s]; nullptr: compact).
 void lp_forward(Ell& E, LPNet& N, const int* slot, const double* r, const double* rs) {
   cudaStream_t st = E.s();
   const int ns = N.ns;
   k_lp_input<<<lpg(ns), LP_TPB, 0, st>>>(ns, slot, N.slot, r, rs, E.h->at(N.l).topo, N.x);
-  k_lp_conv<kIn, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.x, N.wr + kW1, N.h1);
-  k_lp_conv<kC, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h1, N.wr + kW2, N.h2);
-  k_lp_conv<kC, 1><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h2, N.wr + kW3, N.y);
+  k_lp_l1<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.x, nullptr, nullptr, nullptr, nullptr, N.wr + kW1, N.slope,
+                                      N.h1);
+  lp_l2(E, N, st);
+  k_lp_l3<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h2, N.wr + kW3, N.y, nullptr, nullptr, nullptr, nullptr);
 }
 
 // The network's correction z = base + own * rs * net(r/rs), rs = rms(r) (the
-// scaling keeps FP32 in range; the network is linear).  r read and z written
+// scaling keeps FP32 in range; the network is positively homogeneous).  r read and z written
 // at slot[s] (nullptr: compact); base may be nullptr.
 void lp_precondition(Ell& E, LPNet& N, const int* slot, const double* r, const double* base, double* z) {
   cudaStream_t st = E.s();
@@ -206,45 +262,48 @@ void lp_backward(Ell& E, LPNet& N, const double* e, const double* rs, double* lo
                                                  N.dy, N.partial);
   k_lp_sum<<<1, 256, 0, st>>>(N.partial, N.nbd(), loss, 0, N.inv_area);
   cudaMemsetAsync(N.g, 0, 4 * kLpParams, st);
-  cudaMemsetAsync(N.dh1, 0, 4 * (size_t)kC * ns, st);
-  cudaMemsetAsync(N.dh2, 0, 4 * (size_t)kC * ns, st);
   const unsigned gw = std::min<unsigned>((ns + kChunk - 1) / kChunk, 148 * 4);
-  k_lp_wgrad<kC, 1><<<gw, 256, 0, st>>>(ns, N.tap, N.h2, N.dy, N.g + kW3);
-  k_lp_igrad<kC, 1><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.wr + kW3, N.dy, N.dh2);
-  k_lp_wgrad<kC, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.h1, N.dh2, N.g + kW2);
-  k_lp_igrad<kC, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.wr + kW2, N.dh2, N.dh1);
-  k_lp_wgrad<kIn, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.x, N.dh1, N.g + kW1);
+  const auto* h1 = reinterpret_cast<const __nv_bfloat16*>(N.h1);
+  const auto* h2 = reinterpret_cast<const __nv_bfloat16*>(N.h2);
+  k_lp_wgrad<kC, 1><<<gw, 256, 0, st>>>(ns, N.tap, h2, N.dy, N.g + kW3);
+  k_lp_igrad<1><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.inv_ptr, N.inv, N.wr + kW3, N.dy, h2, N.slope, N.dz2);
+  k_lp_wgrad<kC, kC><<<gw, 256, 0, st>>>(ns, N.tap, h1, N.dz2, N.g + kW2);
+  k_lp_igrad<kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.inv_ptr, N.inv, N.wr + kW2, N.dz2, h1, N.slope, N.dz1);
+  k_lp_wgrad<kIn, kC><<<gw, 256, 0, st>>>(ns, N.tap, N.x, N.dz1, N.g + kW1);
 }
 
 void lp_adam(Ell& E, LPNet& N, float lr) {
   cudaStream_t st = E.s();
   ++N.adam_t;
   k_lp_adam<<<lpg(kLpParams, 256), 256, 0, st>>>(kLpParams, N.w, N.g, N.m, N.v, lr, 0.9f, 0.999f, 1e-8f, N.adam_t);
-  k_lp_round<<<lpg(kLpParams, 256), 256, 0, st>>>(N.w, N.wr, kLpParams);
+  lp_round_pack(N, st);
 }
 
-// Residual/error pairs from FP64 multigrid: for each seeded right-hand side,
-// the solution u* to 1e-11, then from u = 0 the residual f - L u and error
-// u* - u after each of `cycles` V-cycles (what a V-cycle leaves, which the
-// network learns to correct).  u and f of the level are kept.
-int lp_generate(Ell& E, LPNet& N, const wt_learn_opts& lo, const wt_solver_opts& mg) {
+// Residual/error pairs from FP64 multigrid: for each seeded right-hand side
+// k0 <= k < k1, the solution u* to 1e-11, then from u = 0 the residual
+// f - L u and error u* - u after each of `cycles` V-cycles (what a V-cycle
+// leaves, which the network learns to correct).  u and f of the level are
+// kept.  The pair buffers hold one batch and are reused across batches.
+int lp_generate(Ell& E, LPNet& N, const wt_learn_opts& lo, const wt_solver_opts& mg, int k0, int k1) {
   const int q = E.le - E.ls, ns = N.ns, l = E.le;
   const int64_t NN = N.NN;
   cudaStream_t st = E.s();
-  lp_free_pairs(&N);
-  const int np = lo.n_rhs * lo.cycles;
+  const int np = (k1 - k0) * lo.cycles;
   int rc = WT_OK;
-  if ((rc = lpalloc(N.pair_allocs, &N.pr, (int64_t)np * ns))) return rc;
-  if ((rc = lpalloc(N.pair_allocs, &N.pe, (int64_t)np * ns))) return rc;
-  if ((rc = lpalloc(N.pair_allocs, &N.pscale, np))) return rc;
-  N.npairs = np;
+  if (N.npairs < np) {
+    lp_free_pairs(&N);
+    if ((rc = lpalloc(N.pair_allocs, &N.pr, (int64_t)np * ns))) return rc;
+    if ((rc = lpalloc(N.pair_allocs, &N.pe, (int64_t)np * ns))) return rc;
+    if ((rc = lpalloc(N.pair_allocs, &N.pscale, np))) return rc;
+    N.npairs = np;
+  }
   cudaMemcpyAsync(N.usave, E.u.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(N.fsave, E.f.lv[q], 8 * NN, cudaMemcpyDeviceToDevice, st);
   std::vector<double> fc(ns);
   wt_solver_opts o = mg;
   o.ir_tol = 1e-11;
   o.ir_max = std::max(o.ir_max, 60);
-  for (int k = 0; k < lo.n_rhs; ++k) {
+  for (int k = k0; k < k1; ++k) {
     Normal rn(lo.seed * 1000003ull + 7919ull * (uint64_t)k + 1);
     double mean = 0.0;
     for (double& v : fc) mean += (v = rn());
@@ -261,7 +320,7 @@ int lp_generate(Ell& E, LPNet& N, const wt_learn_opts& lo, const wt_solver_opts&
     zero_level(E, l, E.u.lv[q]);
     op(E, OP_RESID, l, E.u.lv[q], E.f.lv[q], E.res.lv[q]);
     for (int c = 0; c < lo.cycles; ++c) {
-      const int64_t idx = (int64_t)k * lo.cycles + c;
+      const int64_t idx = (int64_t)(k - k0) * lo.cycles + c;
       vcycle64(E, o);
       k_axpy_d<<<nb(NN), TPB, 0, st>>>(NN, E.u.lv[q], E.corr.lv[q]);
       op(E, OP_RESID, l, E.u.lv[q], E.f.lv[q], E.res.lv[q]);
@@ -277,46 +336,27 @@ int lp_generate(Ell& E, LPNet& N, const wt_learn_opts& lo, const wt_solver_opts&
   return rc;
 }
 
-int lp_train(Ell& E, LPNet& N, const wt_learn_opts& lo, wt_learn_report& rep) {
-  cudaStream_t st = E.s();
-  const int np = N.npairs, ns = N.ns;
-  const int steps = std::max(1, lo.epochs) * np;
-  double* losses = nullptr;
-  std::vector<void*> tmp;
-  if (int rc = lpalloc(tmp, &losses, steps)) return rc;
-  std::mt19937_64 g(lo.seed ^ 0x5bd1e995ull);
+// `epochs` Adam passes over the np pairs of the current batch, one pair a
+// step, in a shuffled order; the step size follows one cosine decay from lr
+// to lr / 20 over all `total` steps of the training, of which `step` are done.
+// The loss of each step goes to losses[step].
+void lp_train_batch(Ell& E, LPNet& N, const wt_learn_opts& lo, int np, std::mt19937_64& g, int& step, int total,
+                    double* losses) {
+  const int ns = N.ns;
   std::vector<int> perm(np);
   for (int k = 0; k < np; ++k) perm[k] = k;
-  int step = 0;
   const double PI = std::acos(-1.0);
   for (int ep = 0; ep < std::max(1, lo.epochs); ++ep) {
     std::shuffle(perm.begin(), perm.end(), g);
     for (int k : perm) {
       const float lr =
-          (float)(lo.lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(PI * step / std::max(1, steps - 1)))));
+          (float)(lo.lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(PI * step / std::max(1, total - 1)))));
       lp_forward(E, N, nullptr, N.pr + (int64_t)k * ns, N.pscale + k);
       lp_backward(E, N, N.pe + (int64_t)k * ns, N.pscale + k, losses + step);
       lp_adam(E, N, lr);
       ++step;
     }
   }
-  std::vector<double> h(steps);
-  cudaMemcpyAsync(h.data(), losses, 8 * (size_t)steps, cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  for (void* p : tmp) cudaFree(p);
-  if (e != cudaSuccess) return wt_handle_fail("learned train", e);
-  double a = 0, b = 0;
-  for (int k = 0; k < np; ++k) {
-    a += h[k];
-    b += h[steps - np + k];
-  }
-  rep.pairs = np;
-  rep.steps = steps;
-  rep.loss_first_epoch = a / np;
-  rep.loss_last_epoch = b / np;
-  for (int k = 0; k < steps; ++k)
-    if (!std::isfinite(h[k])) return WT_ERR_NONFINITE;
-  return WT_OK;
 }
 
 // ------------------------------------------------------- flexible CG ----
@@ -345,13 +385,14 @@ void fcg_iteration(Ell& E, LPNet& N, const wt_solver_opts& o, int pre) {
     cudaMemsetAsync(c, 0, 8 * N.NN, st);
     k_axpy_f2d<<<nb(N.NN), TPB, 0, st>>>(N.NN, c, E.c32.lvf[q]);
     if (pre == PRE_NET) {
-      // z = c + net(r - L c): the network is linear, so it runs on the
-      // unscaled residual; its input and output are fused into the first and
-      // last layers (k_lp_input + k_lp_conv, k_lp_conv + k_lp_output)
+      // z = c + net(r - L c): the network is positively homogeneous, so it
+      // runs on the unscaled residual; its input and output are fused into
+      // the first and last layers
       op(E, OP_APPLY, l, N.c, nullptr, N.lz);
-      k_lp_conv_in<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.slot, N.r, N.lz, E.h->at(l).topo, N.wr + kW1, N.h1);
-      k_lp_conv<kC, kC><<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h1, N.wr + kW2, N.h2);
-      k_lp_conv_out<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.slot, N.h2, N.wr + kW3, N.own, N.c, N.z);
+      k_lp_l1<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, nullptr, N.slot, N.r, N.lz, E.h->at(l).topo, N.wr + kW1,
+                                          N.slope, N.h1);
+      lp_l2(E, N, st);
+      k_lp_l3<<<lpg(ns), LP_TPB, 0, st>>>(ns, N.tap, N.h2, N.wr + kW3, nullptr, N.slot, N.own, N.c, N.z);
     }
   }
   op(E, OP_APPLY, l, N.z, nullptr, N.lz);
@@ -504,7 +545,7 @@ int wt_learned_params(wt_handle* h, float* get, const float* set) {
   CKE(cudaStreamSynchronize(E->s()));
   if (set) {
     CKE(cudaMemcpy(N->w, set, 4 * kLpParams, cudaMemcpyHostToDevice));
-    k_lp_round<<<lpg(kLpParams), LP_TPB, 0, E->s()>>>(N->w, N->wr, kLpParams);
+    lp_round_pack(*N, E->s());
     CKE(cudaStreamSynchronize(E->s()));
   }
   if (get) CKE(cudaMemcpy(get, N->w, 4 * kLpParams, cudaMemcpyDeviceToHost));
@@ -556,7 +597,8 @@ int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep)
   Ell* E;
   LPNet* N;
   if (int rc = lp_get(h, &E, &N)) return rc;
-  if (!o || !rep || o->n_rhs < 1 || o->cycles < 1 || o->epochs < 1 || !(o->lr > 0)) return WT_ERR_ARG;
+  if (!o || !rep || o->n_rhs < 1 || o->cycles < 1 || o->epochs < 1 || !(o->lr > 0) || o->batch_rhs < 0)
+    return WT_ERR_ARG;
   std::memset(rep, 0, sizeof(*rep));
   wt_solver_opts mg{};
   mg.method = WT_SOLVER_MG64;
@@ -564,17 +606,77 @@ int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep)
   mg.up_iter = o->up_iter > 0 ? o->up_iter : 2;
   mg.coarse_iter = o->coarse_iter > 0 ? o->coarse_iter : 20;
   mg.ir_max = 60;
+  const int batch = o->batch_rhs > 0 ? std::min(o->batch_rhs, o->n_rhs) : o->n_rhs;
+  const int total = o->epochs * o->n_rhs * o->cycles;
+  double* losses = nullptr;
+  std::vector<void*> tmp;
+  if (int rc = lpalloc(tmp, &losses, total)) return rc;
+  std::mt19937_64 g(o->seed ^ 0x5bd1e995ull);
   CKE(cudaStreamSynchronize(E->s()));
-  auto t0 = std::chrono::steady_clock::now();
-  int rc = lp_generate(*E, *N, *o, mg);
-  auto t1 = std::chrono::steady_clock::now();
-  if (rc == WT_OK) rc = lp_train(*E, *N, *o, *rep);
-  auto t2 = std::chrono::steady_clock::now();
-  rep->ms_generate = std::chrono::duration<double, std::milli>(t1 - t0).count();
-  rep->ms_train = std::chrono::duration<double, std::milli>(t2 - t1).count();
+  double ms_gen = 0.0, ms_train = 0.0;
+  int rc = WT_OK, step = 0, first_np = 0, last_np = 0;
+  for (int k0 = 0; k0 < o->n_rhs && rc == WT_OK; k0 += batch) {
+    const int k1 = std::min(o->n_rhs, k0 + batch), np = (k1 - k0) * o->cycles;
+    auto t0 = std::chrono::steady_clock::now();
+    rc = lp_generate(*E, *N, *o, mg, k0, k1);
+    auto t1 = std::chrono::steady_clock::now();
+    if (rc == WT_OK) {
+      lp_train_batch(*E, *N, *o, np, g, step, total, losses);
+      cudaError_t e = cudaStreamSynchronize(E->s());
+      if (e != cudaSuccess) rc = wt_handle_fail("learned train", e);
+    }
+    auto t2 = std::chrono::steady_clock::now();
+    ms_gen += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    ms_train += std::chrono::duration<double, std::milli>(t2 - t1).count();
+    if (k0 == 0) first_np = np;
+    last_np = np;
+  }
+  std::vector<double> hl(total, 0.0);
+  if (rc == WT_OK) {
+    cudaError_t e = cudaMemcpy(hl.data(), losses, 8 * (size_t)total, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = wt_handle_fail("learned losses", e);
+  }
+  for (void* p : tmp) cudaFree(p);
   lp_free_pairs(N);
+  rep->ms_generate = ms_gen;
+  rep->ms_train = ms_train;
+  if (rc != WT_OK) return rc;
+  // mean loss over the first pass of the first batch and the last pass of the last one
+  double a = 0, b = 0;
+  for (int k = 0; k < first_np; ++k) a += hl[k];
+  for (int k = 0; k < last_np; ++k) b += hl[total - last_np + k];
+  rep->pairs = o->n_rhs * o->cycles;
+  rep->steps = total;
+  rep->loss_first_epoch = a / std::max(1, first_np);
+  rep->loss_last_epoch = b / std::max(1, last_np);
+  for (int k = 0; k < total; ++k)
+    if (!std::isfinite(hl[k])) return WT_ERR_NONFINITE;
   CKE(cudaGetLastError());
-  return rc;
+  return WT_OK;
+}
+
+// Hidden activation slope (1: identity); takes effect at the next use.
+int wt_learned_activation(wt_handle* h, float slope) {
+  Ell* E;
+  LPNet* N;
+  if (int rc = lp_get(h, &E, &N)) return rc;
+  if (!(slope > 0.0f) || slope > 1.0f) return WT_ERR_ARG;
+  CKE(cudaStreamSynchronize(E->s()));
+  N->slope = slope;
+  for (int k = 0; k < 4; ++k) N->it_key[k] = -1;  // the FCG graphs hold the slope
+  return WT_OK;
+}
+
+// Layer 2 on the tensor cores (1, default) or the CUDA cores (0).
+int wt_learned_tensor_cores(wt_handle* h, int on) {
+  Ell* E;
+  LPNet* N;
+  if (int rc = lp_get(h, &E, &N)) return rc;
+  if (on != 0 && on != 1) return WT_ERR_ARG;
+  CKE(cudaStreamSynchronize(E->s()));
+  N->tensor_cores = on;
+  for (int k = 0; k < 4; ++k) N->it_key[k] = -1;
+  return WT_OK;
 }
 
 }  // extern "C"

@@ -81,6 +81,15 @@ class DeviceGrid:
     def status(self) -> int:
         return N.lib().wt_status(self.h)
 
+    def clear_status(self) -> None:
+        """Acknowledge a device-side error: flag and sticky status back to 0."""
+        N.check("wt_clear_status", N.lib().wt_clear_status(self.h))
+
+    def test_tma_timeout(self, on: bool) -> None:
+        """WT_TUNE_TEST_TMA_TIMEOUT (test only): the TMA-staged kernels take
+        their wait-timeout path while on."""
+        N.check("wt_tune", N.lib().wt_tune(self.h, 4, 1 if on else 0))
+
 
 class TriskModel(DeviceGrid):
     """Uniform-level layered ocean model (incompressible, explicit RK4)."""
@@ -484,10 +493,20 @@ class EllipticSolver(DeviceGrid):
                                                            g.ctypes.data_as(C.POINTER(C.c_float))))
         return float(loss[0]), g
 
+    def learned_activation(self, slope: float) -> None:
+        """Hidden activation slope in (0, 1] (1: identity)."""
+        N.check("wt_learned_activation", N.lib().wt_learned_activation(self.h, float(slope)))
+
+    def learned_tensor_cores(self, on: bool) -> None:
+        """The 32 -> 32 layer on the tensor cores (default) or the CUDA cores."""
+        N.check("wt_learned_tensor_cores", N.lib().wt_learned_tensor_cores(self.h, 1 if on else 0))
+
     def learned_train(self, n_rhs: int = 16, cycles: int = 4, epochs: int = 40, lr: float = 2e-3, seed: int = 1,
-                      down_iter: int = 2, up_iter: int = 2, coarse_iter: int = 6) -> "N.wt_learn_report":
-        """Pairs from the FP64 multigrid, then Adam on the GPU (wt_learned_train)."""
-        o = N.wt_learn_opts(n_rhs, cycles, epochs, lr, seed, down_iter, up_iter, coarse_iter)
+                      down_iter: int = 2, up_iter: int = 2, coarse_iter: int = 6,
+                      batch_rhs: int = 0) -> "N.wt_learn_report":
+        """Pairs from the FP64 multigrid, batch_rhs right-hand sides at a time
+        (0: all), each batch trained with Adam on the GPU (wt_learned_train)."""
+        o = N.wt_learn_opts(n_rhs, cycles, epochs, lr, seed, down_iter, up_iter, coarse_iter, batch_rhs)
         rep = N.wt_learn_report()
         N.check("wt_learned_train", N.lib().wt_learned_train(self.h, C.byref(o), C.byref(rep)))
         return rep

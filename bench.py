@@ -70,7 +70,14 @@ def parse():
     p.add_argument("--elliptic-only", action="store_true",
                    help="only the free-surface solve on uniform J5..J<level> (every method, the learned "
                         "preconditioner trained first); each timed solve is an NVTX range named after its method")
-    p.add_argument("--learned-epochs", type=int, default=40, help="training epochs of the learned preconditioner")
+    p.add_argument("--learned-layers", action="store_true",
+                   help="only the learned network's forward pass on uniform J<level>, layer by layer, with its "
+                        "32 -> 32 layer on the tensor cores and on the CUDA cores")
+    p.add_argument("--learned-pairs", type=int, default=None, metavar="N",
+                   help="--elliptic-only: train the learned preconditioner on N residual/error pairs (8 a "
+                        "right-hand side, 50 right-hand sides a batch, one pass) instead of the level's default")
+    p.add_argument("--eval-seeds", type=int, default=None,
+                   help="--elliptic-only: unseen right-hand sides to evaluate on (default 64 at J8, none below)")
     p.add_argument("--trace", default=None, metavar="PATH",
                    help="record a CUDA kernel timeline of --steps adaptive steps (after --warmup) into PATH "
                         "(Chrome trace) and print its summary instead of the bench line")
@@ -221,11 +228,25 @@ def run_case(level, nz, steps, warmup, seed, device, stream_timing=True, e2e=Tru
     return out
 
 
-def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False, eval_seeds=None):
+LEARNED_TRAIN = {
+    # (right-hand sides, pairs per right-hand side, right-hand sides per batch, Adam passes per batch)
+    6: (32, 4, 32, 10),
+    7: (64, 4, 32, 6),
+    8: (2500, 8, 50, 1),   # 20 000 residual/error pairs, streamed
+}
+LEARNED_SLOPE = 0.25
+
+
+def elliptic_case(lmax, repeats=3, nvtx=False, eval_seeds=None, train=None, slope=LEARNED_SLOPE):
     """Free-surface solve on the uniform hierarchy J5..lmax to relative residual
     1e-10: the reference's FMG and SRJ, the FP64 V-cycle in FP64 refinement
-    (plain FP64 multigrid) and FP32 V-cycles in FP64 refinement.  Best of
-    `repeats` device-timed solves (the report's ms) from a zero first guess."""
+    (plain FP64 multigrid), FP32 V-cycles in FP64 refinement, flexible CG
+    without and with the V-cycle, and flexible CG preconditioned by the V-cycle
+    plus the learned network (2 -> 32 -> 32 -> 1 channels, its middle layer on
+    the tensor cores).  Best of `repeats` device-timed solves (the report's ms)
+    from a zero first guess, at a fixed V-cycle schedule and at the schedule the
+    autotuner picks for each method; then, with eval_seeds, the mean over that
+    many right-hand sides none of the methods was tuned or trained on."""
     import numpy as np
 
     from wavetrisk_hydrostatic_b200 import Grid
@@ -243,25 +264,10 @@ def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False, eval_seeds=None):
     _, fr = S.download()
     out = {"workload": f"Helmholtz free-surface solve, uniform J{lmax} ({10 * 4 ** lmax + 2} cells), "
                        f"hierarchy J5..J{lmax}, seeded bathymetry 500-5000 m, dt 600 s, rel. residual 1e-10"}
-    # the learned preconditioner: trained once on this level on residual/error
-    # pairs of the FP64 multigrid (training time reported apart from the solves)
-    S.learned_setup(1)
-    tr = S.learned_train(n_rhs=16, cycles=4, epochs=epochs, lr=2e-3, seed=1, coarse_iter=6)
-    out["learned_training"] = {"pairs": tr.pairs, "adam_steps": tr.steps, "loss_first_epoch": tr.loss_first_epoch,
-                               "loss_last_epoch": tr.loss_last_epoch, "ms_generate": tr.ms_generate,
-                               "ms_train": tr.ms_train}
     it = dict(ir_max=2000)
-    methods = [("fmg", solver_opts("fmg", 1e-10, max_vcycle=50, coarse_iter=300)),
-               ("srj", solver_opts("srj", 1e-10, max_srj_iter=4000, coarse_iter=300)),
-               # every multigrid-based method with the V-cycle that is fastest for plain FP64 multigrid
-               # (2 + 2 Jacobi sweeps, 6 on the coarsest level; 20 coarse sweeps cost every method time)
-               ("mg64", solver_opts("mg64", 1e-10, down_iter=2, up_iter=2, coarse_iter=6)),
-               ("mixed", solver_opts("mixed", 1e-10, down_iter=2, up_iter=2, coarse_iter=6)),
-               ("fcg_learned", solver_opts("fcg_learned", 1e-10, down_iter=2, up_iter=2, coarse_iter=6, **it)),
-               ("fcg", solver_opts("fcg", 1e-10, **it)),
-               ("fcg_mg", solver_opts("fcg_mg", 1e-10, down_iter=2, up_iter=2, coarse_iter=6, **it))]
     q = len(levels) - 1
-    for name, o in methods:
+
+    def timed(name, o, key=None):
         best, rep = None, None
         for _ in range(repeats):
             S.upload(u=np.zeros(off[-1]), f=fr)
@@ -272,34 +278,52 @@ def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False, eval_seeds=None):
             if nvtx:
                 torch.cuda.nvtx.range_pop()
             best = rep.ms if best is None else min(best, rep.ms)
-        out[name] = {"ms": best, "rel_residual": rep.true_rel_residual, "status": rep.status,
-                     "outer_iterations": rep.outer_iterations}
+        r = {"ms": best, "rel_residual": rep.true_rel_residual, "status": rep.status,
+             "iterations": rep.iterations[q] if name.startswith("fcg") else rep.outer_iterations}
         if name.startswith("fcg"):
-            out[name].update(iterations=rep.iterations[q], restarts=rep.restarts, fallback_at=rep.precond_fallback)
-    # every multigrid-based method again at the V-cycle schedule the autotuner picks for it (built-in set:
+            r.update(restarts=rep.restarts, fallback_at=rep.precond_fallback)
+        out[key or name] = r
+        return r
+
+    fixed = dict(down_iter=2, up_iter=2, coarse_iter=6)   # the V-cycle fastest for plain FP64 multigrid
+    for name, o in (("fmg", solver_opts("fmg", 1e-10, max_vcycle=50, coarse_iter=300)),
+                    ("srj", solver_opts("srj", 1e-10, max_srj_iter=4000, coarse_iter=300)),
+                    ("mg64", solver_opts("mg64", 1e-10, **fixed)),
+                    ("mixed", solver_opts("mixed", 1e-10, **fixed)),
+                    ("fcg", solver_opts("fcg", 1e-10, **it)),
+                    ("fcg_mg", solver_opts("fcg_mg", 1e-10, **fixed, **it))):
+        timed(name, o)
+    # every multigrid-based method at the V-cycle schedule the autotuner picks for it (built-in set:
     # down = up in {1, 2, 3} sweeps, coarse in {2, 4, 6, 10, 20}), timed the same way
-    # (the network is trained again, on the residual/error pairs of the V-cycle tuned for FCG without it,
-    # before its own schedule is tuned: it learns what that V-cycle leaves)
     tuned = {}
-    for name in ("mg64", "mixed", "fcg_mg", "fcg_learned"):
-        if name == "fcg_learned":
-            d, u_, c = out["fcg_mg_tuned"]["schedule"]
-            S.learned_setup(1)
-            tr2 = S.learned_train(n_rhs=16, cycles=4, epochs=epochs, lr=2e-3, seed=1, down_iter=d, up_iter=u_,
-                                  coarse_iter=c)
-            out["learned_training_tuned"] = {"schedule": [d, u_, c], "loss_last_epoch": tr2.loss_last_epoch,
-                                             "ms_train": tr2.ms_train}
+
+    def tune(name):
         S.upload(u=np.zeros(off[-1]), f=fr)
         o, _ = S.autotune(name, 1e-10, repeats=2, ir_max=2000 if name.startswith("fcg") else 60)
-        best, rep = None, None
-        for _ in range(repeats):
-            S.upload(u=np.zeros(off[-1]), f=fr)
-            rep = S.solve(o)
-            best = rep.ms if best is None else min(best, rep.ms)
         tuned[name] = o
-        out[name + "_tuned"] = {"ms": best, "schedule": [o.down_iter, o.up_iter, o.coarse_iter],
-                                "rel_residual": rep.true_rel_residual, "status": rep.status,
-                                "iterations": rep.iterations[q] if name.startswith("fcg") else rep.outer_iterations}
+        timed(name, o, name + "_tuned")["schedule"] = [o.down_iter, o.up_iter, o.coarse_iter]
+
+    for name in ("mg64", "mixed", "fcg_mg"):
+        tune(name)
+    # the learned preconditioner: trained once, on residual/error pairs of the V-cycle tuned for FCG without
+    # it (what that V-cycle leaves is what it learns to correct); training time is reported apart
+    n_rhs, cycles, batch, epochs = train or LEARNED_TRAIN.get(lmax, (32, 4, 32, 6))
+    d, u_, c = out["fcg_mg_tuned"]["schedule"]
+    S.learned_setup(1)
+    S.learned_activation(slope)
+    tr = S.learned_train(n_rhs=n_rhs, cycles=cycles, epochs=epochs, lr=2e-3, seed=1, down_iter=d, up_iter=u_,
+                         coarse_iter=c, batch_rhs=batch)
+    out["learned_training"] = {"network": "2 -> 32 -> 32 -> 1, 7 taps, BF16 weights and activations, FP32 "
+                                          f"accumulation, activation slope {slope}, 32->32 layer on tcgen05",
+                               "pairs": tr.pairs, "adam_steps": tr.steps, "batch_rhs": batch,
+                               "pair_schedule": [d, u_, c], "loss_first_epoch": tr.loss_first_epoch,
+                               "loss_last_epoch": tr.loss_last_epoch, "ms_generate": tr.ms_generate,
+                               "ms_train": tr.ms_train}
+    timed("fcg_learned", solver_opts("fcg_learned", 1e-10, **fixed, **it))
+    tune("fcg_learned")
+    S.learned_tensor_cores(False)                # the same network with its middle layer on the CUDA cores
+    timed("fcg_learned", tuned["fcg_learned"], "fcg_learned_tuned_cuda_cores")
+    S.learned_tensor_cores(True)
     out["learned_speedup_vs_fp64_mg_tuned"] = out["mg64_tuned"]["ms"] / out["fcg_learned_tuned"]["ms"]
     if eval_seeds:
         # right-hand sides the network never saw (its training ones come from its own seeded generator)
@@ -324,8 +348,9 @@ def elliptic_case(lmax, repeats=3, epochs=40, nvtx=False, eval_seeds=None):
             name: {"mean_ms": float(np.mean(e["ms"])), "mean_iterations": float(np.mean(e["iterations"])),
                    "worst_rel_residual": e["worst_rel_residual"], "fallbacks": e["fallbacks"],
                    "failures": e["failures"]} for name, e in ev.items()}}
-        out["unseen_rhs_eval"]["learned_speedup_vs_fp64_mg"] = (
-            out["unseen_rhs_eval"]["mg64"]["mean_ms"] / out["unseen_rhs_eval"]["fcg_learned"]["mean_ms"])
+        ue = out["unseen_rhs_eval"]
+        ue["learned_speedup_vs_fp64_mg"] = ue["mg64"]["mean_ms"] / ue["fcg_learned"]["mean_ms"]
+        ue["mixed_speedup_vs_fp64_mg"] = ue["mg64"]["mean_ms"] / ue["mixed"]["mean_ms"]
     out["mixed_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["mixed"]["ms"]
     out["mixed_speedup_vs_fmg"] = out["fmg"]["ms"] / out["mixed"]["ms"]
     out["learned_speedup_vs_fp64_mg"] = out["mg64"]["ms"] / out["fcg_learned"]["ms"]
@@ -626,7 +651,7 @@ def bench_ours(args):
                     "step1_plus_trend_ms_fp32_fluxes": km["step1"] + km["trend_rk"],
                 })
         for lmax in (6, 7, 8):
-            extra.append(elliptic_case(lmax, eval_seeds=16 if lmax == 8 else None))
+            extra.append(elliptic_case(lmax, eval_seeds=64 if lmax == 8 else None))
         for (lmin, lmax, nzw) in ((5, 7, 16), (5, 8, 32)):
             extra.append(wavelet_case(lmin, lmax, nzw, device=device))
 
@@ -727,7 +752,7 @@ def bench_ours_uniform(args):
                 "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,
             })
         for lmax in (6, 7, 8):
-            extra.append(elliptic_case(lmax, eval_seeds=16 if lmax == 8 else None))
+            extra.append(elliptic_case(lmax, eval_seeds=64 if lmax == 8 else None))
         for (lmin, lmax, nzw) in ((5, 7, 16), (5, 8, 32)):
             extra.append(wavelet_case(lmin, lmax, nzw, device=device))
 
@@ -1013,6 +1038,41 @@ def bench_wavelets(args):
           flush=True)
 
 
+def learned_layers_case(lmax, reps=20):
+    """The learned network's forward pass on uniform J<lmax>, layer by layer
+    (mean device time over reps launches on a seeded residual), with the
+    32 -> 32 layer on the tensor cores and on the CUDA cores.  Layer 2 per
+    node: 2 * 224 * 32 flops; algorithmic bytes 64 (the node's own BF16 input
+    row, the six tap rows being other nodes' rows) + 64 (output) + 28 (7 tap
+    indices).  At J9 the activations (168 MB each) exceed the 126 MB L2."""
+    import numpy as np
+
+    from wavetrisk_hydrostatic_b200 import Grid
+    from wavetrisk_hydrostatic_b200.cases import bathymetry
+    from wavetrisk_hydrostatic_b200.model import EllipticSolver
+
+    g = Grid(5, lmax, radius=6371e3)
+    levels = [g.level(l) for l in range(5, lmax + 1)]
+    S = EllipticSolver(levels, [bathymetry(lv, seed=1) for lv in levels])
+    ns = S.learned_setup(1)
+    S.learned_activation(LEARNED_SLOPE)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    hbm, tc = float(peaks["hbm_gbs"]), float(peaks["bf16_tflops"])
+    out = {"workload": f"learned preconditioner forward pass, uniform J{lmax} ({ns} nodes), 2 -> 32 -> 32 -> 1 "
+                       f"channels, 7 taps, BF16 activations", "nodes": ns}
+    flops2, bytes2 = 2.0 * 224 * 32 * ns, (64 + 64 + 28) * ns
+    for name, on in (("tensor_cores", True), ("cuda_cores", False)):
+        S.learned_tensor_cores(on)
+        ms = S.learned_layer_times(reps)
+        out[name] = {"layer_ms": ms, "layer2_TFLOPs": flops2 / (ms[1] / 1e3) / 1e12,
+                     "layer2_GBps": bytes2 / (ms[1] / 1e3) / 1e9}
+        out[name]["layer2_frac_of_measured_hbm"] = out[name]["layer2_GBps"] / hbm
+        out[name]["layer2_frac_of_measured_bf16"] = out[name]["layer2_TFLOPs"] / tc
+    out["layer2_speedup_tensor_vs_cuda_cores"] = out["cuda_cores"]["layer_ms"][1] / out["tensor_cores"]["layer_ms"][1]
+    S.close()
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1023,9 +1083,12 @@ def main():
         bench_trace(args)
     elif args.wavelets_only:
         bench_wavelets(args)
+    elif args.learned_layers:
+        print(json.dumps(learned_layers_case(args.level)), flush=True)
     elif args.elliptic_only:
-        print(json.dumps(elliptic_case(args.level, epochs=args.learned_epochs, nvtx=True,
-                                       eval_seeds=16 if args.level == 8 else None)))
+        tr = None if args.learned_pairs is None else (max(1, args.learned_pairs // 8), 8, 50, 1)
+        ev = args.eval_seeds if args.eval_seeds is not None else (64 if args.level == 8 else None)
+        print(json.dumps(elliptic_case(args.level, nvtx=True, eval_seeds=ev, train=tr)))
     else:
         bench_ours(args)
 

@@ -235,6 +235,9 @@ int wt_learned_setup(wt_handle* h, unsigned long long seed);   /* He-initialised
 int wt_learned_activation(wt_handle* h, float slope);
 /* The 32 -> 32 layer on the tensor cores (1, default) or the CUDA cores (0). */
 int wt_learned_tensor_cores(wt_handle* h, int on);
+/* Mean device time of each layer of the forward pass over reps launches, on a
+ * seeded residual (ms[3]: layer 1 with its input, layer 2, layer 3). */
+int wt_learned_layer_times(wt_handle* h, int reps, float* ms);
 int wt_learned_num_params(void);
 /* FP32 master parameters (wt_learned_num_params floats); get or set may be NULL. */
 int wt_learned_params(wt_handle* h, float* get, const float* set);

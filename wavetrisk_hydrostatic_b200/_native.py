@@ -149,6 +149,7 @@ _DEVICE_SIGS = {
     "wt_learned_train": [_vp, C.POINTER(wt_learn_opts), C.POINTER(wt_learn_report)],
     "wt_learned_activation": [_vp, C.c_float],
     "wt_learned_tensor_cores": [_vp, C.c_int],
+    "wt_learned_layer_times": [_vp, C.c_int, C.POINTER(C.c_float)],
     "wt_wavelet_setup": [_vp],
     "wt_upload_field": [_vp, C.c_int, C.c_int, _vp],
     "wt_download_field": [_vp, C.c_int, C.c_int, _vp],

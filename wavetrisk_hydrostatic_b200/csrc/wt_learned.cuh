@@ -6,6 +6,7 @@
 // Included by wt_elliptic.cu only, after wt_elliptic_mixed.cuh.
 #pragma once
 
+#include <functional>
 #include <random>
 
 #include "learned_kernels.cuh"
@@ -651,6 +652,52 @@ int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep)
   rep->loss_last_epoch = b / std::max(1, last_np);
   for (int k = 0; k < total; ++k)
     if (!std::isfinite(hl[k])) return WT_ERR_NONFINITE;
+  CKE(cudaGetLastError());
+  return WT_OK;
+}
+
+// Per-layer device time of the network's forward pass on a seeded residual
+// (mean over reps launches of each layer, CUDA events on the solver's
+// stream): ms[0] layer 1 with the input, ms[1] layer 2 (tensor cores or CUDA
+// cores as set), ms[2] layer 3.
+int wt_learned_layer_times(wt_handle* h, int reps, float* ms) {
+  Ell* E;
+  LPNet* N;
+  if (int rc = lp_get(h, &E, &N)) return rc;
+  if (reps < 1 || !ms) return WT_ERR_ARG;
+  cudaStream_t st = E->s();
+  const int ns = N->ns;
+  std::vector<double> r(ns);
+  Normal rn(12345);
+  for (double& v : r) v = rn();
+  CKE(cudaMemcpyAsync(N->rc, r.data(), 8 * (size_t)ns, cudaMemcpyHostToDevice, st));
+  lp_rms(*N, st, nullptr, N->rc, N->rs);
+  k_lp_input<<<lpg(ns), LP_TPB, 0, st>>>(ns, nullptr, N->slot, N->rc, N->rs, E->h->at(N->l).topo, N->x);
+  cudaEvent_t ev[2];
+  CKE(cudaEventCreate(&ev[0]));
+  CKE(cudaEventCreate(&ev[1]));
+  auto l1 = [&] {
+    k_lp_l1<<<lpg(ns), LP_TPB, 0, st>>>(ns, N->tap, N->x, nullptr, nullptr, nullptr, nullptr, N->wr + kW1, N->slope,
+                                        N->h1);
+  };
+  auto l2 = [&] { lp_l2(*E, *N, st); };
+  auto l3 = [&] {
+    k_lp_l3<<<lpg(ns), LP_TPB, 0, st>>>(ns, N->tap, N->h2, N->wr + kW3, N->y, nullptr, nullptr, nullptr, nullptr);
+  };
+  int q = 0;
+  const std::function<void()> layers[3] = {l1, l2, l3};
+  for (const auto& f : layers) {
+    f();  // warm-up
+    CKE(cudaEventRecord(ev[0], st));
+    for (int k = 0; k < reps; ++k) f();
+    CKE(cudaEventRecord(ev[1], st));
+    CKE(cudaEventSynchronize(ev[1]));
+    float t = 0.f;
+    CKE(cudaEventElapsedTime(&t, ev[0], ev[1]));
+    ms[q++] = t / reps;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
   CKE(cudaGetLastError());
   return WT_OK;
 }

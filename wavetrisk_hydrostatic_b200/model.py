@@ -501,6 +501,12 @@ class EllipticSolver(DeviceGrid):
         """The 32 -> 32 layer on the tensor cores (default) or the CUDA cores."""
         N.check("wt_learned_tensor_cores", N.lib().wt_learned_tensor_cores(self.h, 1 if on else 0))
 
+    def learned_layer_times(self, reps: int = 20) -> list[float]:
+        """Mean device ms of the forward pass's three layers (wt_learned_layer_times)."""
+        ms = (C.c_float * 3)()
+        N.check("wt_learned_layer_times", N.lib().wt_learned_layer_times(self.h, int(reps), ms))
+        return [float(v) for v in ms]
+
     def learned_train(self, n_rhs: int = 16, cycles: int = 4, epochs: int = 40, lr: float = 2e-3, seed: int = 1,
                       down_iter: int = 2, up_iter: int = 2, coarse_iter: int = 6,
                       batch_rhs: int = 0) -> "N.wt_learn_report":

@@ -90,3 +90,27 @@ def test_free_surface_update_refuses_a_mismatched_solver_setup():
     dev.elliptic_setup(300.0, 1.0, 1.0)
     assert N.lib().wt_free_surface_update(dev.h, 600.0, 1.0, 1.0, C.byref(opts), C.byref(rep)) == N.WT_ERR_STATE
     dev.close()
+
+
+def test_mode_split_adaptive_steps_run():
+    """ModeSplitOcean (RK4_split + adapt + inverse transform, the ensemble's
+    member step) on J3..J5 x 2 over a seamount: every step's free-surface solve
+    converges and the state and free surface stay finite and bounded."""
+    from wavetrisk_hydrostatic_b200.adaptive import ModeSplitOcean
+
+    ph = OceanParams()
+    G = Grid(3, 5, radius=6371e3)
+    levels = [G.level(l) for l in range(3, 6)]
+    states = [bump_state(g, 2, seed=6, ph=ph, topo=seamount_topography(g, seed=6, radius=600e3)) for g in levels]
+    model = ModeSplitOcean(G, 3, 5, 2, states, 1200.0, ph, tol=5e-3)
+    for _ in range(5):
+        rep = model.step()
+        assert rep.status == 0 and rep.true_rel_residual <= 1e-8
+    assert model.dev.status() == 0
+    for name in ("mass", "temp", "velo"):
+        assert np.isfinite(model.dev.download(5, name)).all()
+    eta = model.dev.free_surface(5)
+    assert np.isfinite(eta).all() and np.abs(eta).max() < 10.0
+    for (mn, me), g in zip(model.masks(), levels):   # every mask entry is one of adapt's values
+        assert mn.min() >= 0 and mn.max() <= 16 and me.min() >= 0 and me.max() <= 16
+    model.close()

@@ -181,6 +181,9 @@ __global__ void __launch_bounds__(128) k_lp_l1(int ns, const int* __restrict__ t
 // (128 x 32, FP32) in tensor memory: 14 tcgen05.mma of K 16, one commit to an
 // mbarrier, then each warp reads 16 columns of its 32 lanes.  Persistent CTAs
 // (grid <= tiles) keep B and the 32 tensor-memory columns over their tiles.
+// The gather is a set of 16-byte cp.async copies of whole 8-channel chunks
+// (zero-filled for taps outside the node set), issued before the previous
+// tile's epilogue so its latency overlaps it.
 constexpr int kL2M = 128;
 constexpr int kL2Ksteps = kTaps * kC / 16;         // 14
 constexpr int kL2StepA = 2 * (kL2M / 8) * 128;     // bytes of A per K step: 2 core columns x 16 row groups
@@ -224,6 +227,47 @@ __device__ __forceinline__ bool lp_mbar_wait(uint32_t bar, unsigned parity, unsi
   }
 }
 
+// 16-byte global -> shared copy (cp.async, L2 only); src_bytes 0 fills zeros.
+__device__ __forceinline__ void cp16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Gather item j of this thread: the 16-byte chunk q (channels 8q..8q+7) of
+// tap t of tile row m, item = tid + kL2Threads j.
+constexpr int kL2Items = kTaps * kL2M * 4 / kL2Threads;  // 14
+__device__ __forceinline__ void l2_item(int tid, int j, int& t, int& m, int& q) {
+  const int item = tid + kL2Threads * j;
+  q = item & 3;
+  m = (item >> 2) & (kL2M - 1);
+  t = item >> 9;
+}
+__device__ __forceinline__ void l2_taps(const int* __restrict__ tap, int ns, int tile, int ntiles, int tid,
+                                        int (&tp)[kL2Items]) {
+#pragma unroll
+  for (int j = 0; j < kL2Items; ++j) {
+    int t, m, q;
+    l2_item(tid, j, t, m, q);
+    const int s = tile * kL2M + m;
+    tp[j] = (tile < ntiles && s < ns) ? __ldg(tap + (int64_t)t * ns + s) : -1;
+  }
+}
+__device__ __forceinline__ void l2_gather(uint32_t aaddr, const uint4* __restrict__ h1, int tid,
+                                          const int (&tp)[kL2Items]) {
+#pragma unroll
+  for (int j = 0; j < kL2Items; ++j) {
+    int t, m, q;
+    l2_item(tid, j, t, m, q);
+    const int off = (2 * t + (q >> 1)) * kL2StepA + (q & 1) * (kL2StepA / 2) + (m >> 3) * 128 + (m & 7) * 16;
+    const int u = tp[j];
+    cp16(aaddr + off, u >= 0 ? (const void*)(h1 + 4 * (int64_t)u + q) : (const void*)h1, u >= 0 ? 16u : 0u);
+  }
+}
+
+// Persistent CTAs over the tiles, the gather of tile i+1 (cp.async straight
+// into the operand layout) in flight while tile i's accumulator is read back
+// and stored; the tap indices are fetched a tile further ahead.
 __global__ void __launch_bounds__(kL2Threads) k_lp_l2_umma(int ns, const int* __restrict__ tap,
                                                            const uint4* __restrict__ h1,
                                                            const uint4* __restrict__ wpk, float slope,
@@ -235,8 +279,16 @@ __global__ void __launch_bounds__(kL2Threads) k_lp_l2_umma(int ns, const int* __
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kL2ABytes + kL2BBytes + 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t aaddr = umma::smem_u32(sA), baddr = umma::smem_u32(sB), bar = umma::smem_u32(bar_p);
+  const int ntiles = (ns + kL2M - 1) / kL2M;
+  const int stride = gridDim.x;
+  int tile = blockIdx.x;
 
-  for (int q = tid; q < kL2BBytes / 16; q += kL2Threads) reinterpret_cast<uint4*>(sB)[q] = wpk[q];
+  int tp[kL2Items];
+  l2_taps(tap, ns, tile, ntiles, tid, tp);
+  for (int q = tid; q < kL2BBytes / 16; q += kL2Threads) cp16(baddr + 16 * q, wpk + q, 16u);
+  l2_gather(aaddr, h1, tid, tp);
+  cp_commit();
+  l2_taps(tap, ns, tile + stride, ntiles, tid, tp);
   if (tid == 0) lp_mbar_init(bar);
   if (warp == 0) umma::tmem_alloc(tslot, 32);
   umma::fence_before_sync();
@@ -245,25 +297,9 @@ __global__ void __launch_bounds__(kL2Threads) k_lp_l2_umma(int ns, const int* __
   const uint32_t tmem = *tslot;
   constexpr uint32_t kIdesc = umma::idesc_bf16_f32(kL2M, kC);
 
-  const int ntiles = (ns + kL2M - 1) / kL2M;
   unsigned parity = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int s0 = tile * kL2M;
-    // gather: item (t, m, q) = the 16-byte chunk q (channels 8q..8q+7) of tap t of row m
-    uint4 v[kTaps * 2];
-#pragma unroll
-    for (int j = 0; j < kTaps * 2; ++j) {
-      const int item = tid + kL2Threads * j, q = item & 3, m = (item >> 2) & (kL2M - 1), t = item >> 9;
-      const int s = s0 + m;
-      const int u = s < ns ? __ldg(tap + (int64_t)t * ns + s) : -1;
-      v[j] = u >= 0 ? __ldg(h1 + 4 * (int64_t)u + q) : make_uint4(0u, 0u, 0u, 0u);
-    }
-#pragma unroll
-    for (int j = 0; j < kTaps * 2; ++j) {
-      const int item = tid + kL2Threads * j, q = item & 3, m = (item >> 2) & (kL2M - 1), t = item >> 9;
-      const int off = (2 * t + (q >> 1)) * kL2StepA + (q & 1) * (kL2StepA / 2) + (m >> 3) * 128 + (m & 7) * 16;
-      *reinterpret_cast<uint4*>(sA + off) = v[j];
-    }
+  for (; tile < ntiles; tile += stride) {
+    cp_wait_all();
     umma::fence_async_smem();
     umma::fence_before_sync();
     __syncthreads();
@@ -284,11 +320,18 @@ __global__ void __launch_bounds__(kL2Threads) k_lp_l2_umma(int ns, const int* __
       break;
     }
     parity ^= 1u;
+    // the operand buffer is free: start the next tile's gather, then its successor's taps
+    const int next = tile + stride;
+    if (next < ntiles) {
+      l2_gather(aaddr, h1, tid, tp);
+      cp_commit();
+      l2_taps(tap, ns, next + stride, ntiles, tid, tp);
+    }
     umma::fence_after_sync();
     float d[16];
     const int quarter = warp & 3, half = warp >> 2;
     umma::tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + 16 * half, d);
-    const int s = s0 + 32 * quarter + lane;
+    const int s = tile * kL2M + 32 * quarter + lane;
     if (s < ns) {
       uint4 o0, o1;
       o0.x = pack_bf16x2(lp_act(d[0], slope), lp_act(d[1], slope));
@@ -303,6 +346,7 @@ __global__ void __launch_bounds__(kL2Threads) k_lp_l2_umma(int ns, const int* __
       h2[4 * (int64_t)s + 2 * half + 1] = o1;
     }
   }
+  cp_wait_all();  // a CTA leaving early (timeout) still has its copies land before it exits
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) {

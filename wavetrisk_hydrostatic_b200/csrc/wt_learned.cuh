@@ -201,10 +201,14 @@ int lp_build(Ell& E, uint64_t seed) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaError_t e = cudaFuncSetAttribute(k_lp_l2_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, kL2Smem);
     if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_lp_l2_umma, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lp_l2_umma, kL2Threads, kL2Smem);
     if (e != cudaSuccess) rc = wt_handle_fail("learned l2 attributes", e);
+    // three CTAs fit an SM by shared memory (70 KB each) and registers
     const int tiles = (ns + kL2M - 1) / kL2M;
-    N->l2_grid = std::max(1, std::min(tiles, std::max(1, per_sm) * std::max(1, nsm)));
+    N->l2_grid = std::max(1, std::min(tiles, std::max(3, per_sm) * std::max(1, nsm)));
     if (rc == WT_OK) rc = lp_init_params(*N, seed);
   }
   if (rc != WT_OK) {

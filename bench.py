@@ -640,6 +640,23 @@ def bench_ours(args):
                 "trend_rk_GBps": ab / (kt["trend_rk"] / 1e3) / 1e9,
                 "trend_rk_frac": ab / (kt["trend_rk"] / 1e3) / 1e9 / hbm,
             })
+            if lv == 5:   # the reference's CPU-runnable case: the CPU restatement's step on this host beside it
+                import oracle
+                from wavetrisk_hydrostatic_b200 import Grid, OceanParams, jet_state
+                g5 = Grid(5, 5, radius=6371e3).level(5)
+                ph5 = OceanParams()
+                cur = jet_state(g5, nz, seed=7, ph=ph5)
+                t_cpu, n_cpu = 0.0, 0
+                while n_cpu < 3 or t_cpu < 3.0:
+                    t0 = time.perf_counter()
+                    m5, t5, v5 = oracle.rk4(g5, nz, ph5, cur, dtu, 1)
+                    t_cpu += time.perf_counter() - t0
+                    n_cpu += 1
+                    cur = dict(cur, mass=m5, temp=t5, velo=v5)
+                extra[-1]["cpu_baseline"] = {"ms_per_step": 1e3 * t_cpu / n_cpu,
+                                             "value": sim_days_per_hour(n_cpu, t_cpu, dtu),
+                                             "cores": oracle.get_threads(), "kind": "port",
+                                             "cpu_model": cpu_model(), "sample": f"{n_cpu} RK4 steps"}
             if lv in (7, 8):   # the same run with FP32 flux stencils, error against the FP64 run
                 rm = run_case(lv, nz, steps, 2, seed=7, device=device, e2e=False, flux_bits=32, dt=dtu)
                 ref, got = rr["final_state"], rm["final_state"]
@@ -914,6 +931,18 @@ class AdaptiveCpuSampler:
                 f"over the 10 lozenges and wavelets over layers on {self.threads} threads, mask sequence on one")
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or None."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline_adaptive(args, quick=False):
     """The oracle's adaptive step on the same workload: one warm-up sample,
     then samples until the time budget is used (at least two)."""
@@ -925,7 +954,8 @@ def cpu_baseline_adaptive(args, quick=False):
         t, tf = S.sample()
         n, used, est = n + 1, used + t, est + tf
     return {"value": sim_days_per_hour(n, est, dt_adaptive(args.level)), "unit": "simulated days per wall-clock hour",
-            "cores": S.threads, "kind": "port", "sample": S.describe(n, used), "seconds_per_step": est / n}
+            "cores": S.threads, "kind": "port", "sample": S.describe(n, used), "seconds_per_step": est / n,
+            "cpu_model": cpu_model(), "host_threads": os.cpu_count()}
 
 
 def bench_reference(args):
@@ -949,7 +979,8 @@ def bench_reference(args):
             used, est = used + t, est + tf
         value = sim_days_per_hour(steps, est, dt_adaptive(args.level))
         cb = {"value": value, "unit": "simulated days per wall-clock hour", "cores": S.threads, "kind": "port",
-              "sample": S.describe(steps, used), "seconds_per_step": est / steps}
+              "sample": S.describe(steps, used), "seconds_per_step": est / steps, "cpu_model": cpu_model(),
+              "host_threads": os.cpu_count()}
         data = "synthetic (seeded seamount, jet and Gaussian bumps)"
     else:
         cb = cpu_baseline(args)

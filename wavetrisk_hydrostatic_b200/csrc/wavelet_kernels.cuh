@@ -221,6 +221,29 @@ __global__ void k_compress(WLev L, int nz) {
       if (L.mask_e[e * L.NN + x] < ADJZONE) L.wv[(int64_t)k * 3 * L.NN + e * L.NN + x] = 0.0;
 }
 
+// compress_wavelets after a mask change whose wavelets were compressed under
+// the previous masks (old_n, old_e): the slots kept before and dropped now are
+// the only ones not holding 0 already, so only they are zeroed (the result is
+// k_compress's).  One thread per node, every layer.
+__global__ void k_compress_delta(WLev L, const int* __restrict__ old_n, const int* __restrict__ old_e, int nz) {
+  int k, d, i, j;
+  if (!decode(1, L.n + 1, k, d, i, j)) return;
+  const int x = nid(L, d, i, j);
+  const bool zn = old_n[x] >= ADJZONE && L.mask_n[x] < ADJZONE;
+  bool ze[3] = {false, false, false};
+  if (i < L.n && j < L.n)
+    for (int e = 0; e < 3; ++e) ze[e] = old_e[e * L.NN + x] >= ADJZONE && L.mask_e[e * L.NN + x] < ADJZONE;
+  if (!(zn || ze[0] || ze[1] || ze[2])) return;
+  for (int kk = 0; kk < nz; ++kk) {
+    if (zn) {
+      L.wm[(int64_t)kk * L.NN + x] = 0.0;
+      L.wt[(int64_t)kk * L.NN + x] = 0.0;
+    }
+    for (int e = 0; e < 3; ++e)
+      if (ze[e]) L.wv[(int64_t)kk * 3 * L.NN + e * L.NN + x] = 0.0;
+  }
+}
+
 // Ghost copy of one level's layered node and edge fields (for host downloads).
 __global__ void k_halo_level(int nz, int NN, const int2* __restrict__ hn, int n_hn, const int3* __restrict__ he, int n_he,
                              double* a, double* b, double* v) {

@@ -135,6 +135,9 @@ const unsigned char* wt_level_rec(wt_handle* h, int level);
 // and inverse transform of the hierarchy, and the threshold upload (wt_wavelet.cu).
 int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq);
 void wt_level_compress(wt_handle* h);
+int wt_level_mask_snapshot_alloc(wt_handle* h);
+void wt_level_mask_snapshot(wt_handle* h);
+void wt_level_compress_delta(wt_handle* h);
 // zero every wavelet array if a host upload wrote wavelets since the last
 // zeroing (stream-ordered; WT_after_step then writes only the slots it computes)
 void wt_level_clean_wavelets(wt_handle* h);

@@ -438,6 +438,7 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
   // writes only the kept slots (the wavelets on entry are not read otherwise)
   if (!wt_level_zero_ok(h)) wt_level_compress(h);
   if (int rc = wt_level_need_refresh(h)) return rc;  // likewise a current needed-node map
+  if (int rc = wt_level_mask_snapshot_alloc(h)) return rc;
   if (!M->step_graph || M->g_dt != dt || M->g_fill != level_fill || M->g_max != max_level ||
       M->g_epoch != wt_level_skip_epoch(h)) {
     if (M->step_graph) {
@@ -449,10 +450,16 @@ int wt_adaptive_step(wt_handle* h, double dt, const double* threshold, int level
     // adapt reads wavelets and masks only, and the inverse transform after it
     // rebuilds every level above level_start: the last stage's own inverse is
     // left out
+    // the last stage's WT_after_step leaves the wavelets compressed under the
+    // masks of this step, so compress_wavelets under the new masks only has to
+    // zero the slots the new masks drop (the masks are kept before adapt)
     int rc = rk4_multi(h, dt, 1, nullptr, false);
-    if (!rc) rc = wt_level_mask_sequence(h, level_fill, max_level, 0, nullptr);
     if (!rc) {
-      wt_level_compress(h);
+      wt_level_mask_snapshot(h);
+      rc = wt_level_mask_sequence(h, level_fill, max_level, 0, nullptr);
+    }
+    if (!rc) {
+      wt_level_compress_delta(h);
       wt_level_inverse(h);
     }
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);

@@ -16,6 +16,7 @@ struct WavLevel {
   double *sm = nullptr, *st = nullptr, *sv = nullptr;  // scaling (owned below level_end)
   double *wm = nullptr, *wt = nullptr, *wv = nullptr;
   int *mask_n = nullptr, *mask_e = nullptr;
+  int *old_n = nullptr, *old_e = nullptr;  // the masks before the adaptive step's mask sequence
   double *scal = nullptr, *dscal = nullptr, *flux = nullptr, *dvelo = nullptr;  // work fields, on first use
   double *mean_m = nullptr, *mean_t = nullptr;  // layer means below level_end, on first use
   int* rf_pi = nullptr;     // flux-restriction plan into this level (k_rf_plan), below level_end

@@ -700,6 +700,42 @@ int wt_level_need_refresh(wt_handle* h) {
 }
 
 void wt_level_compress(wt_handle* h) { compress(h); }
+
+// Arrays for the masks before a mask sequence, levels above level_start.
+int wt_level_mask_snapshot_alloc(wt_handle* h) {
+  WavCtx* W = ctx(h);
+  for (int l = h->level_start + 1; l <= h->level_end; ++l) {
+    WavLevel& V = W->L[l - h->level_start];
+    if (V.old_n) continue;
+    CKW(W->alloc(&V.old_n, (size_t)h->at(l).NN));
+    CKW(W->alloc(&V.old_e, (size_t)3 * h->at(l).NN));
+  }
+  return WT_OK;
+}
+
+// The masks now, kept for wt_level_compress_delta (stream-ordered).
+void wt_level_mask_snapshot(wt_handle* h) {
+  WavCtx* W = ctx(h);
+  for (int l = h->level_start + 1; l <= h->level_end; ++l) {
+    WavLevel& V = W->L[l - h->level_start];
+    const size_t nn = (size_t)h->at(l).NN;
+    cudaMemcpyAsync(V.old_n, V.mask_n, 4 * nn, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(V.old_e, V.mask_e, 12 * nn, cudaMemcpyDeviceToDevice, h->stream);
+  }
+}
+
+// compress_wavelets when the wavelets were compressed under the snapshot's
+// masks: zero only the slots those masks kept and the current ones drop.
+void wt_level_compress_delta(wt_handle* h) {
+  WavCtx* W = ctx(h);
+  for (int l = h->level_start + 1; l <= h->level_end; ++l) {
+    const WavLevel& V = W->L[l - h->level_start];
+    const int n = h->at(l).n;
+    k_compress_delta<<<nb((int64_t)10 * (n + 1) * (n + 1)), TPB, 0, h->stream>>>(view(h, l), V.old_n, V.old_e,
+                                                                                   h->nz);
+  }
+  W->zero_ok = true;
+}
 void wt_level_clean_wavelets(wt_handle* h) {
   if (!ctx(h)->wav_dirty) return;
   zero_wavelets(h);

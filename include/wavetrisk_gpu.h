@@ -257,6 +257,23 @@ int wt_learned_grad(wt_handle* h, const double* r, const double* e, double* loss
  * time, and trains the network on each batch with Adam on the GPU. */
 int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep);
 
+/* ---------------------------------------------------- vertical remap ---- */
+/* remap_vertical_coordinates (src/remap.f90:18-76) for the incompressible
+ * case (remap_incompressible, :147-216): every layered level of the handle
+ * (level_end; every level of the hierarchy after wt_wavelet_setup) is remapped
+ * from its Lagrangian layers to the hybrid grid z_k = a_vert[k] eta + b_vert[k]
+ * z_s (a_vert, b_vert: nz + 1 host values, index 0 at the bottom; eta the
+ * column's free surface from its layer masses, z_s the topography).  Buoyancy
+ * is remapped on each node's column and the three edge velocities on the
+ * columns averaged with the node at each edge's far end; the new masses are
+ * rho0 dz.  remap_type selects the column reconstruction: WT_REMAP_0
+ * (remap0, piecewise constant, :259-285), WT_REMAP_1 (remap1, piecewise linear
+ * with interface reconciliation, :287-380), WT_REMAP_2PPM (remap2PPM, :382-495).
+ * Porosity 1 (no penalization).  The host decides when to remap
+ * (src/main.f90:447-454).  nz <= 64. */
+enum { WT_REMAP_0 = 0, WT_REMAP_1 = 1, WT_REMAP_2PPM = 2 };
+int wt_remap_vertical(wt_handle* h, int remap_type, const double* a_vert, const double* b_vert);
+
 /* ------------------------------------------------------ no allocation ---- */
 /* Weighted l2 norm of one level (the solver's l2, src/lin_solve.f90:433-464)
  * for callers that cannot allocate device memory: a host loop running inside

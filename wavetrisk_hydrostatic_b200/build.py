@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 CXX_FLAGS = ["-O2", "-ffp-contract=off", "-fPIC", "-std=c++17"]
 
-CU_SOURCES = ["wt_api.cu", "wt_elliptic.cu", "wt_noalloc.cu", "wt_wavelet.cu", "wt_barotropic.cu", "wt_trend_ml.cu"]
+CU_SOURCES = ["wt_api.cu", "wt_elliptic.cu", "wt_noalloc.cu", "wt_wavelet.cu", "wt_barotropic.cu", "wt_trend_ml.cu", "wt_remap.cu"]
 CPP_SOURCES = ["grid.cpp", "grid_api.cpp"]
 
 

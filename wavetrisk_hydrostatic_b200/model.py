@@ -81,6 +81,15 @@ class DeviceGrid:
     def status(self) -> int:
         return N.lib().wt_status(self.h)
 
+    def remap_vertical(self, remap_type: str, a_vert: np.ndarray, b_vert: np.ndarray) -> None:
+        """remap_vertical_coordinates of every layered level (wt_remap_vertical):
+        remap_type '0', '1' or '2PPM'; a_vert, b_vert the nz + 1 hybrid
+        coefficients from the bottom."""
+        code = {"0": 0, "1": 1, "2PPM": 2}[remap_type]
+        a = np.ascontiguousarray(a_vert, dtype=np.float64)
+        b = np.ascontiguousarray(b_vert, dtype=np.float64)
+        N.check("wt_remap_vertical", N.lib().wt_remap_vertical(self.h, code, N.dptr(a), N.dptr(b)))
+
     def clear_status(self) -> None:
         """Acknowledge a device-side error: flag and sticky status back to 0."""
         N.check("wt_clear_status", N.lib().wt_clear_status(self.h))

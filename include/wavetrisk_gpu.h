@@ -451,6 +451,13 @@ int wt_barotropic_correction_multi(wt_handle* h);
  * solve stopped at its cap; the update is then made with that solution). */
 int wt_free_surface_update(wt_handle* h, double dt, double theta1, double theta2, const wt_solver_opts* opts,
                            wt_solver_report* rep);
+/* The free surface's part of adapt (src/adapt.f90:79-103 compress_wavelets and
+ * the inverse transform after it, src/main.f90:441; the free surface is layer
+ * zlevels+1 of sol): its wavelets from the last wt_free_surface_update /
+ * wt_rk4_split, compressed under the current masks, then its inverse
+ * transform.  Call after wt_mask_build; WT_ERR_STATE before any free-surface
+ * update. */
+int wt_free_surface_adapt(wt_handle* h);
 /* RK4_split (src/time_integr.f90:360-382): when theta2 != 1 the flux
  * divergence of the current state into each level's previous divergence,
  * then wt_rk4_split_explicit and wt_free_surface_update. */

@@ -233,14 +233,16 @@ def rk4_split_explicit(levels, nz, ph, states, masks, etas, dt, theta1, H=None):
 
 
 def free_surface_update(levels, nz, ph, states, masks, etas, div_olds, dt, theta1, theta2, H, method="fmg",
-                        domain_level=2, **solver):
+                        domain_level=2, keep_eta_hierarchy=False, **solver):
     """free_surface_update (src/time_integr.f90:465-478) over the hierarchy:
     eta_update (src/barotropic_2d.f90:118-129: rhs_elliptic on every level, the
     solve with the operator's coefficients from the old free surface, starting
     from it), barotropic_correction, u_update and WT_after_step (with the
     masks H holds).  states[q]: the level's mass, temp, velo, mean_m, mean_t,
     topo.  Returns per level (mass, temp, velo), the new free surfaces and the
-    solver's per-level iteration counts."""
+    solver's per-level iteration counts (and, with keep_eta_hierarchy, the
+    one-layer wavelet hierarchy holding the free surface and its wavelets,
+    for free_surface_adapt)."""
     from .barotropic import barotropic_correction_multi, rhs_elliptic_multi, u_update_multi
     from .elliptic import Hierarchy as EH
     from .grid import own
@@ -278,10 +280,26 @@ def free_surface_update(levels, nz, ph, states, masks, etas, div_olds, dt, theta
         He.set(g.level, "s_m", new_etas[q][None, :])
     He.wt_after_step()
     new_etas = [He.field(g.level, "s_m")[0].copy() for g in ol]
+    if keep_eta_hierarchy:
+        return out, new_etas, its, He
     return out, new_etas, its
 
 
-def rk4_split(levels, nz, ph, states, masks, etas, dt, theta1, theta2, method="fmg", domain_level=2, **solver):
+def free_surface_adapt(levels, He, masks):
+    """The free surface's part of adapt (src/adapt.f90:79-103 compress_wavelets
+    and the inverse transform after it, src/main.f90:441): the wavelets He kept
+    from free_surface_update, compressed under the new masks, then the inverse
+    transform.  Returns the new free surface of every level."""
+    for g, (mn, me) in zip(levels, masks):
+        He.set(g.level, "mask_n", mn)
+        He.set(g.level, "mask_e", me)
+    He.compress()
+    He.inverse()
+    return [He.field(g.level, "s_m")[0].copy() for g in levels]
+
+
+def rk4_split(levels, nz, ph, states, masks, etas, dt, theta1, theta2, method="fmg", domain_level=2,
+              keep_eta_hierarchy=False, **solver):
     """RK4_split (src/time_integr.f90:360-382) over the hierarchy with theta2 = 1
     (no previous flux divergence): the four RK_split stages, then
     free_surface_update.  Returns what free_surface_update returns."""
@@ -293,4 +311,4 @@ def rk4_split(levels, nz, ph, states, masks, etas, dt, theta1, theta2, method="f
     st = [dict(states[i], mass=m, temp=t, velo=v) for i, (m, t, v) in enumerate(q)]
     zero = [np.zeros(g.NN) for g in levels]
     return free_surface_update(levels, nz, ph, st, masks, etas, zero, dt, theta1, theta2, H, method=method,
-                               domain_level=domain_level, **solver)
+                               domain_level=domain_level, keep_eta_hierarchy=keep_eta_hierarchy, **solver)

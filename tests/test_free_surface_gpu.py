@@ -59,8 +59,8 @@ def test_rk4_split_with_free_surface_matches_oracle(masks_kind):
     dev.elliptic_setup(dt, theta1, theta2, domain_level=G.domain_level)
     rep = dev.rk4_split(dt, theta1, theta2, solver_opts("fmg", 1e-10, max_vcycle=50, coarse_iter=300))
     assert rep.status == 0
-    ref, ref_eta, its = oracle.rk4_split(levels, nz, ph, states, masks, etas, dt, theta1, theta2,
-                                         domain_level=G.domain_level, **solver)
+    ref, ref_eta, its, He = oracle.rk4_split(levels, nz, ph, states, masks, etas, dt, theta1, theta2,
+                                             domain_level=G.domain_level, keep_eta_hierarchy=True, **solver)
     assert list(rep.iterations)[:len(levels)] == its
     for q, g in enumerate(levels):
         own = np.nonzero(g.owned)[0]
@@ -72,6 +72,15 @@ def test_rk4_split_with_free_surface_matches_oracle(masks_kind):
         assert _rel(dev.download(g.level, "velo")[:, e], v[:, e]) <= 1e-9, (g.level, "velo")
     # the free surface moved: the solve is not a no-op
     assert _rel(ref_eta[-1], etas[-1]) > 1e-3
+    # adapt: new masks from the layers, then the free surface compressed under
+    # them and rebuilt (wt_free_surface_adapt against the oracle's)
+    dev.mask_build(np.array([[2.0] * nz, [1e16] * nz, [0.02] * nz]), 0, lmax)
+    new_masks = [(dev.download(g.level, "mask_n"), dev.download(g.level, "mask_e")) for g in levels]
+    dev.free_surface_adapt()
+    ref_eta2 = oracle.free_surface_adapt(levels, He, new_masks)
+    for q, g in enumerate(levels):
+        own = np.nonzero(g.owned)[0]
+        assert _rel(dev.free_surface(g.level)[own], ref_eta2[q][own]) <= 1e-9, (g.level, "eta after adapt")
     assert dev.status() == 0
     dev.close()
 

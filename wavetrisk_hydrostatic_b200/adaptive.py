@@ -102,12 +102,11 @@ class ModeSplitOcean(AdaptiveOcean):
     WT_after_step, then the implicit free-surface solve with coefficients from
     the old free surface, barotropic_correction, u_update and the free
     surface's own WT_after_step), then adapt (masks from the layers' mass,
-    Theta and velocity thresholds, compression) and the inverse transform.
-    The initial free surface of every level is the sum of its layers' mass
-    perturbations over rho0, so layers and free surface start consistent.
-    Not in the reference's sequence here: adapt's masks do not test the free
-    surface's wavelets (the layers' thresholds decide), and the free surface is
-    compressed and reconstructed only inside free_surface_update."""
+    Theta and velocity thresholds, as mask_tol_vars tests layers 1..zlevels
+    only; compression) and the inverse transform, both also of the free
+    surface (layer zlevels+1 of sol, wt_free_surface_adapt).  The initial free
+    surface of every level is the sum of its layers' mass perturbations over
+    rho0, so layers and free surface start consistent."""
 
     def __init__(self, grid: Grid, min_level: int, max_level: int, nz: int, states: list[dict], dt: float,
                  ph: OceanParams | None = None, theta1: float = 1.0, theta2: float = 1.0, solver=None, **kw):
@@ -133,6 +132,7 @@ class ModeSplitOcean(AdaptiveOcean):
         del req
         self.dev.compress()
         self.dev.inverse()
+        self.dev.free_surface_adapt()
         self.istep += 1
         self.last_report = rep
         return rep

@@ -48,6 +48,8 @@ struct Ell {
   int domain_level = 2;
   std::vector<ELevelDev> L;
   MField u, f, res, corr, pf, wc_mass, wc_temp, tmp, au, rr, r0, pp, ss, ap, as_, cc, rr2;
+  MField eta_wc;                   // the free surface's wavelets of its last WT_after_step
+  bool eta_wc_valid = false;
   MField u32, f32, r32, c32, t32;  // FP32 V-cycle work
   double* partial = nullptr;
   double* scal = nullptr;  // device scalars
@@ -233,7 +235,7 @@ extern "C" int wt_elliptic_setup(wt_handle* h, double dt, double theta1, double 
     E->nbmax = std::max<int>(E->nbmax, (int)nb(10 * (int64_t)(D.n + 1) * (D.n + 1)));
   }
   MField* fields[] = {&E->u, &E->f, &E->res, &E->corr, &E->pf, &E->wc_mass, &E->wc_temp, &E->tmp, &E->au,
-                      &E->rr, &E->r0, &E->pp, &E->ss, &E->ap, &E->as_, &E->cc, &E->rr2};
+                      &E->rr, &E->r0, &E->pp, &E->ss, &E->ap, &E->as_, &E->cc, &E->rr2, &E->eta_wc};
   for (MField* F : fields)
     if (rc == WT_OK) rc = alloc_field(*E, *F);
   MField* f32[] = {&E->u32, &E->f32, &E->r32, &E->c32, &E->t32};
@@ -626,29 +628,49 @@ int wt_level_barotropic_correction(wt_handle* h, double* const* m, double* const
 
 namespace {
 
-int eta_after_step(wt_handle* h, Ell& E) {
-  std::vector<double*> eta(E.le - E.ls + 1);
-  for (int l = E.ls; l <= E.le; ++l)
-    if (int rc = wt_level_baro_fields(h, l, &eta[l - E.ls], nullptr, nullptr, nullptr)) return rc;
-  for (int l = E.ls + 1; l <= E.le; ++l) {   // every wavelet from the surface as it is
+// The free surface's inverse transform from its wavelets in E.eta_wc,
+// compressed first under the current masks (compress_scalar), from
+// level_start up (Prolong_scalar + Reconstruct_scalar).
+int eta_inverse(wt_handle* h, Ell& E, const std::vector<double*>& eta) {
+  for (int l = E.ls + 1; l <= E.le; ++l) {
     const int q = l - E.ls;
-    double* wc = E.wc_temp.lv[q];
-    zero_level(E, l, wc);
-    const int n = E.L[q - 1].n;
-    k_wc_compute<<<nb(10 * n * n), TPB, 0, E.s()>>>(E.view(l - 1), E.view(l), eta[q], wc);
     const int *mn, *me;
     wt_level_masks(h, l, &mn, &me);
-    k_compress_wc<<<nb(E.L[q].NN), TPB, 0, E.s()>>>(E.L[q].NN, mn, wc);
+    k_compress_wc<<<nb(E.L[q].NN), TPB, 0, E.s()>>>(E.L[q].NN, mn, E.eta_wc.lv[q]);
   }
-  for (int l = E.ls + 1; l <= E.le; ++l) {   // then the inverse from level_start up
+  for (int l = E.ls + 1; l <= E.le; ++l) {   // from level_start up
     const int q = l - E.ls, n = E.L[q - 1].n;
     const EllLev C = E.view(l - 1), F = E.view(l);
-    k_prolong_even<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, eta[q - 1], E.wc_temp.lv[q], eta[q]);
-    k_prolong_odd<<<nb(10 * n * n), TPB, 0, E.s()>>>(C, F, eta[q], E.wc_temp.lv[q]);
+    k_prolong_even<<<nb(10 * (n + 1) * (n + 1)), TPB, 0, E.s()>>>(C, F, eta[q - 1], E.eta_wc.lv[q], eta[q]);
+    k_prolong_odd<<<nb(10 * n * n), TPB, 0, E.s()>>>(C, F, eta[q], E.eta_wc.lv[q]);
   }
   CKE(cudaGetLastError());
   CKE(cudaStreamSynchronize(E.s()));
   return WT_OK;
+}
+
+int eta_fields(wt_handle* h, Ell& E, std::vector<double*>& eta) {
+  eta.resize(E.le - E.ls + 1);
+  for (int l = E.ls; l <= E.le; ++l)
+    if (int rc = wt_level_baro_fields(h, l, &eta[l - E.ls], nullptr, nullptr, nullptr)) return rc;
+  return WT_OK;
+}
+
+// WT_after_step of the free surface (it is layer zlevels+1 of sol): every
+// wavelet from the surface as it is, compress_scalar, inverse transform.
+// The wavelets stay in E.eta_wc for the inverse transform after adapt.
+int eta_after_step(wt_handle* h, Ell& E) {
+  E.eta_wc_valid = true;
+  std::vector<double*> eta;
+  if (int rc = eta_fields(h, E, eta)) return rc;
+  for (int l = E.ls + 1; l <= E.le; ++l) {
+    const int q = l - E.ls;
+    double* wc = E.eta_wc.lv[q];
+    zero_level(E, l, wc);
+    const int n = E.L[q - 1].n;
+    k_wc_compute<<<nb(10 * n * n), TPB, 0, E.s()>>>(E.view(l - 1), E.view(l), eta[q], wc);
+  }
+  return eta_inverse(h, E, eta);
 }
 
 }  // namespace
@@ -700,6 +722,19 @@ int wt_free_surface_update(wt_handle* h, double dt, double theta1, double theta2
 
 // RK4_split (src/time_integr.f90:360-382): the flux divergence of the previous
 // step when theta2 != 1, RK_split four times and free_surface_update.
+// The free surface's part of adapt's compress_wavelets and of the inverse
+// transform after it (src/adapt.f90:79-103, src/main.f90:441): its wavelets
+// from the last free_surface_update, compressed under the current masks, then
+// the inverse transform.  Call after wt_mask_build.
+int wt_free_surface_adapt(wt_handle* h) {
+  if (!h || !h->ell || !h->wav) return WT_ERR_STATE;
+  Ell& E = *static_cast<Ell*>(h->ell);
+  if (E.ls != h->level_start || E.le != h->level_end || !E.eta_wc_valid) return WT_ERR_STATE;
+  std::vector<double*> eta;
+  if (int rc = eta_fields(h, E, eta)) return rc;
+  return eta_inverse(h, E, eta);
+}
+
 int wt_rk4_split(wt_handle* h, double dt, double theta1, double theta2, const wt_solver_opts* opts,
                  wt_solver_report* rep) {
   if (!h || !opts || !rep || dt <= 0) return WT_ERR_ARG;

@@ -347,6 +347,11 @@ class WaveletHierarchy(DeviceGrid):
         """One mode-split time step, RK4_split: RK_split x 4 and free_surface_update."""
         return self._solve_call("wt_rk4_split", dt, theta1, theta2, opts)
 
+    def free_surface_adapt(self) -> None:
+        """The free surface's compression under the current masks and its
+        inverse transform (adapt's part for layer zlevels+1 of sol)."""
+        N.check("wt_free_surface_adapt", N.lib().wt_free_surface_adapt(self.h))
+
     def free_surface(self, level: int) -> np.ndarray:
         """The free surface of `level` (sol(S_MASS, zlevels+1)), NN doubles."""
         eta = np.empty(self.levels[level - self.ls].NN)

@@ -11,10 +11,14 @@ own grid builder (oracle_grid.cpp through grid.own), never from the level
 objects it is given; a product level only names the grid parameters and the
 level number.
 
-Parity status: unpinned against the reference binary (the reference is Fortran
-and no Fortran compiler exists in the build container); pinned instead by the
-properties the reference relies on (conservation, identities, analytic cases),
-checked in tests/test_*_oracle.py and tests/test_grid.py.
+Parity status: not pinned against a reference binary (the reference is
+Fortran, and neither the build container nor the GPU host has a Fortran
+compiler).  Pinned instead by its own grid builder, bit-identical to the
+product's separate restatement (tests/test_oracle_grid.py), by known answers
+(the analytic elliptic problem's second-order convergence, div curl = 0, the
+energy-neutral Coriolis term, Restrict(Prolong) = I: tests/test_known_answers.py)
+and by the properties the reference relies on (conservation, identities:
+tests/test_*_oracle.py, tests/test_grid.py).
 """
 from __future__ import annotations
 

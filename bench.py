@@ -533,6 +533,15 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
         names = ["step1_top", "step1_coarse", "restrict", "trend_ml_top", "trend_ml_coarse", "rk_sub", "wt_after_step"]
         out["phase_ms"] = {names[p]: pm[p] for p in range(7)}
         out["phase_count_per_step"] = {names[p]: pc[p] for p in range(7)}
+        # the roofline kernel timed with every node computed: the timed steps let the
+        # finest level's trend leave out the tiles no needed node is in, so there it does
+        # less than the algorithmic bytes count (NVTX range "roofline" for ncu)
+        dev.skip_inactive(False)
+        torch.cuda.nvtx.range_push("roofline")
+        Nt.check("wt_profile_rk4_multi", Nt.lib().wt_profile_rk4_multi(dev.h, DT_AD, 1, pm, pc))
+        torch.cuda.nvtx.range_pop()
+        dev.skip_inactive(True)
+        out["phase_ms_dense"] = {names[p]: pm[p] for p in range(7)}
     if e2e:
         # The host keeps the finest level's prognostic state and the masks of
         # every level (its masks of record): each step uploads that state from
@@ -685,12 +694,16 @@ def bench_ours(args):
         tot = sum(share.values())
         dom = max(share, key=lambda k: share[k])
         ab = algorithmic_bytes_trend_ml(args.level, args.nz, n_on=r["masks"][-1]["trsk_nodes_0n"])
-        ach = ab / (pm["trend_ml_top"] / 1e3) / 1e9
+        t_dense = r["phase_ms_dense"]["trend_ml_top"]
+        ach = ab / (t_dense / 1e3) / 1e9
         traffic = None
         tf = os.path.join(ROOT, "profiles", "trend_ml_traffic.json")
         if os.path.exists(tf):
             try:
-                traffic = json.load(open(tf)).get(f"J{args.level}_nz{args.nz}")
+                tj = json.load(open(tf))
+                traffic = tj.get(f"J{args.level}_nz{args.nz}")
+                if traffic is None and tj.get("dense_ratio_J7_nz32"):   # scaled by the algorithmic bytes
+                    traffic = int(tj["dense_ratio_J7_nz32"] * ab)
             except Exception:
                 traffic = None
         cpu = cpu_baseline(args, quick=True)
@@ -718,6 +731,14 @@ def bench_ours(args):
             "roofline": {"bound": "hbm", "kernel": "k_trend_tma<MODE_ML> (level_end)", "achieved": ach, "peak": hbm,
                          "unit": "GB/s", "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
                          "algorithmic_bytes_per_launch": ab,
+                         "kernel_ms_dense": t_dense,
+                         "kernel_ms_in_timed_steps": pm["trend_ml_top"],
+                         "timing": "CUDA events around the kernel's launches in one profiled RK4 step with every node "
+                                   "computed (the timed steps leave out tiles with no needed node, doing less than "
+                                   "the algorithmic bytes count: kernel_ms_in_timed_steps)",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same dense launch "
+                                           "at J7 x 32, scaled to this level by the algorithmic bytes "
+                                           "(profiles/trend_ml_traffic.json)" if traffic else None,
                          "dominant_phase_by_time": dom,
                          "phase_share": {k: v / tot for k, v in share.items()},
                          "phase_ms_per_occurrence": pm, "phase_count_per_step": pc},

@@ -1,15 +1,16 @@
 """Benchmark: simulated days per wall-clock hour of the adaptive ocean time step.
 
 Workload (N=1, the default): the adaptive run J5..J9 (2,621,442 cells at J9),
-32 Boussinesq layers, every patch of the hierarchy present (a fully refined
-tree; masks, compression and adapt every step), flat 4000 m bottom with a
-seeded Gaussian seamount (2000 m, 50 km), zonal jet + 8 seeded Gaussian bumps
-(300 km, 0.05 m) in the layer thicknesses, wavelet threshold tolerance 5e-3,
-explicit RK4 with dt = 37.5 s (150 s at J7 scaled with the finest grid
-spacing, the reference's CFL rule dt = cfl dx_min / c).  One step is the
-reference's time_step (src/main.f90:405-444): RK4 of the hierarchy with
-WT_after_step per stage, adapt's mask sequence and compression, and the
-inverse transform, replayed as one captured CUDA graph.  With --gpus N>1
+32 Boussinesq layers, flat 4000 m bottom with a seeded Gaussian seamount
+(2000 m, 50 km), zonal jet + 8 seeded Gaussian bumps (300 km, 0.05 m) in the
+layer thicknesses, wavelet threshold tolerance 5e-3, explicit RK4 with
+dt = 37.5 s (150 s at J7 scaled with the finest grid spacing, the reference's
+CFL rule dt = cfl dx_min / c).  The initial grid is refined level by level as
+the reference's initialize does (a partially refined patch tree, 4 x 4 node
+patches).  One step is the reference's time_step (src/main.f90:405-444): RK4
+of the hierarchy with WT_after_step per stage, adapt's mask sequence with
+refine() of the patch tree and compression, and the inverse transform,
+replayed as one captured CUDA graph.  With --gpus N>1
 every rank advances its own ensemble member (independent seeds, no
 collective): weak scaling, value = member-days per hour summed over ranks.
 
@@ -481,10 +482,11 @@ def adaptive_states(levels, nz, seed, ph):
 
 
 def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile=True):
-    """The adaptive run on the fully refined hierarchy lmin..lmax (seamount,
-    jet + 8 Gaussian bumps, tol 5e-3 thresholds of initialize_thresholds_case),
-    one step = RK4 of the hierarchy + adapt + inverse transform.  CUDA-event
-    time per step on the handle's stream."""
+    """The adaptive run lmin..lmax (seamount, jet + 8 Gaussian bumps, tol 5e-3
+    thresholds of initialize_thresholds_case), its initial grid refined level
+    by level as the reference's initialize does, one step = RK4 of the
+    hierarchy + adapt (with refine() of the patch tree) + inverse transform.
+    CUDA-event time per step on the handle's stream."""
     import numpy as np
     import torch
 
@@ -496,8 +498,10 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
     ph = OceanParams()
     G = Grid(lmin, lmax, radius=6371e3)
     levels = [G.level(l) for l in range(lmin, lmax + 1)]
-    states = adaptive_states(levels, nz, seed, ph)
-    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=TOL_AD)
+    states = adaptive_states([G.level(lmin - 1)] + levels, nz, seed, ph)
+    t_init = time.perf_counter()
+    model = AdaptiveOcean(G, lmin, lmax, nz, states[1:], ph, tol=TOL_AD, root_state=states[0])
+    t_init = time.perf_counter() - t_init
     del states
     dev = model.dev
     stream = torch.cuda.ExternalStream(dev.stream, device=device)
@@ -526,6 +530,9 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
                     "active_edges": int(np.count_nonzero(me[e] >= 8)), "edges": int(e.size),
                     "trsk_nodes_0n": int(np.count_nonzero(mn[inner] >= 2))})
     out["masks"] = act
+    out["tree"] = tree_summary(model, levels)
+    out["tree"]["init_s"] = round(t_init, 2)
+    out["tree"]["init_log"] = [list(x) for x in model.init_log]
     if profile:
         pm = (Nt.C.c_double * 7)()
         pc = (Nt.C.c_int * 7)()
@@ -584,6 +591,21 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
     out["cells_finest"] = 10 * 4 ** lmax + 2
     model.close()
     return out
+
+
+def tree_summary(model, levels):
+    """The patch tree after the run: its level_end and, per level, the patches
+    that exist out of all and the owned nodes they hold."""
+    ps = model.patch_size
+    per = []
+    nodes = 0
+    for g in levels:
+        ex = model.patches(g.level)
+        per.append({"level": g.level, "patches": int(ex.sum()), "of": int(ex.size)})
+        nodes += int(ex.sum()) * ps * ps
+    dense = sum(10 * g.n * g.n for g in levels)
+    return {"level_end": model.level_end(), "patch_size": ps, "levels": per, "tree_nodes": nodes,
+            "dense_nodes": dense, "tree_fraction": nodes / dense}
 
 
 def algorithmic_bytes_trend_rk(level, nz):
@@ -743,6 +765,7 @@ def bench_ours(args):
                          "phase_share": {k: v / tot for k, v in share.items()},
                          "phase_ms_per_occurrence": pm, "phase_count_per_step": pc},
             "masks_after_run": r["masks"],
+            "patch_tree": r["tree"],
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
@@ -1058,7 +1081,9 @@ def bench_trace(args):
     ph = OceanParams()
     G = Grid(args.lmin, args.level, radius=6371e3)
     levels = [G.level(l) for l in range(args.lmin, args.level + 1)]
-    model = AdaptiveOcean(G, args.lmin, args.level, args.nz, adaptive_states(levels, args.nz, 1, ph), ph, tol=TOL_AD)
+    states = adaptive_states([G.level(args.lmin - 1)] + levels, args.nz, 1, ph)
+    model = AdaptiveOcean(G, args.lmin, args.level, args.nz, states[1:], ph, tol=TOL_AD, root_state=states[0])
+    del states
     for _ in range(args.warmup):
         model.step(dt_adaptive(args.level))
     torch.cuda.synchronize()
@@ -1127,7 +1152,8 @@ def ensemble_case(members=16, days=1.0, nz=32, lmin=5, rank=0, world=1, device=N
     for m in mine:
         lmax = lmax_of[m]
         levels = [G.level(l) for l in range(lmin, lmax + 1)]
-        states = adaptive_states(levels, nz, 100 + m, ph)
+        states = adaptive_states([G.level(lmin - 1)] + levels, nz, 100 + m, ph)
+        root_state, states = states[0], states[1:]
         g = levels[-1]
         own = g.owned
         area = 1.0 / g.hex_inv[own]
@@ -1139,7 +1165,7 @@ def ensemble_case(members=16, days=1.0, nz=32, lmin=5, rank=0, world=1, device=N
         mass0 = total_mass(states[-1]["mass"])
         dt = dt_split(lmax)
         steps = int(round(days * DAY / dt))
-        model = ModeSplitOcean(G, lmin, lmax, nz, states, dt, ph, tol=TOL_AD,
+        model = ModeSplitOcean(G, lmin, lmax, nz, states, dt, ph, tol=TOL_AD, root_state=root_state,
                                solver=solver_opts(solver, 1e-9, down_iter=2, up_iter=2, coarse_iter=6))
         del states
         stream = torch.cuda.ExternalStream(model.dev.stream, device=device)

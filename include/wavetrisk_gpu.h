@@ -354,6 +354,48 @@ int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill);
  * hierarchy exists (a fully refined tree). */
 int wt_mask_build(wt_handle* h, const double* threshold, int level_fill, int max_level, int patch_size,
                   unsigned char* child_required);
+
+/* ---- The patch tree of a partially refined hierarchy (src/refine_patch.f90).
+ * Level l holds 10 * (n_l / patch_size)^2 patches of patch_size^2 owned nodes
+ * (PATCH_SIZE, src/patch.f90:6), one byte each, lozenge-major [10][rows][cols].
+ * Every level's fields stay allocated; the tree decides which patches exist,
+ * and the levels above its level_end hold ZERO masks, which the mask-tested
+ * transforms, restrictions and mask sweeps leave out as the reference leaves
+ * out levels it has not made.  Once a tree exists, wt_adaptive_step refines it
+ * on the device inside its graph (while the tree's level_end is the
+ * hierarchy's top). */
+/* add_second_level (src/refine_patch.f90:247-268) as init_structures calls it
+ * (src/main.f90:482-524): every patch of level_start exists, none above, the
+ * tree's level_end is level_start.  patch_size: even, dividing n_level_start. */
+int wt_tree_init(wt_handle* h, int patch_size);
+/* The tree's level_end (levels above it have no patch). */
+int wt_tree_level_end(wt_handle* h, int* level_end);
+/* One level's patch bytes: exist (1 = the patch exists) and fresh (1 = made
+ * by the last refine); either may be NULL. */
+int wt_tree_download(wt_handle* h, int level, unsigned char* exist, unsigned char* fresh);
+/* Grid sync after a host-side refine or a restart (load_adapt_mpi,
+ * src/io.f90:971): the host's tree replaces the device's: exist holds
+ * every level's bytes, level_start first; level_start must be complete. */
+int wt_grid_sync(wt_handle* h, const unsigned char* exist, int level_end);
+/* adapt (src/adapt.f90:14-65) on the tree: init_masks_zero, mask_active,
+ * mask_adj_same_scale and mask_restrict_same_scale up to the tree's
+ * level_end; refine() (src/refine_patch.f90:12-49: check_child_required of
+ * every existing patch below max_level, a child patch per flagged quadrant,
+ * level_end + 1 when one of level level_end + 1 is made); then
+ * mask_adj_finer_scale, complete_masks and mask_trsk up to the new level_end,
+ * and compress_wavelets.  Returns the new level_end and whether a patch was
+ * made (either pointer may be NULL). */
+int wt_adapt(wt_handle* h, const double* threshold, int level_fill, int max_level, int* level_end, int* refined);
+/* count_active (src/main.f90:137-172) over the patches the last refine made:
+ * counts[0] node wavelets (mass and Theta of every layer) with |w| >=
+ * threshold(v, k), counts[1] edge wavelets (velocity). */
+int wt_count_active(wt_handle* h, const double* threshold, long long* counts);
+/* out[0] patches of the level, out[1] of them made by the last refine, out[2]
+ * owned nodes outside the tree with a node or edge mask that is not ZERO. */
+int wt_tree_stats(wt_handle* h, int level, long long* out);
+/* mask_adj_child (src/mask.f90:314-466) of the parents of `level` alone, as
+ * init_structures applies it to the root level (src/main.f90:514). */
+int wt_mask_adj_child(wt_handle* h, int level);
 /* cal_lnorm (src/lnorms.f90:7-58) of the hierarchy's scaling fields over
  * levels level_start..level_end: out[v*nz + k] for v = mass, Theta, velocity;
  * scalars are mean + perturbation over nodes [0, n]^2, velocities over the

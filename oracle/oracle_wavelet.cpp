@@ -813,6 +813,13 @@ struct W {
   }
   // adapt (src/adapt.f90:14-65) without tree surgery: every patch exists.
   void mask_build(const double* thr, int level_fill, int max_level, int ps, uint8_t* required) {
+    mask_phase1(thr, level_fill, max_level, ps, required, le - 1);
+    mask_phase2();
+  }
+  // adapt up to refine(): init_masks_zero, mask_active, mask_adj_same_scale,
+  // mask_restrict_same_scale, then check_child_required of the parent levels
+  // ls .. req_hi (refine visits every existing patch, level_end's included).
+  void mask_phase1(const double* thr, int level_fill, int max_level, int ps, uint8_t* required, int req_hi) {
     init_masks_zero();
     // mask_active
     for (int l = ls; l <= le; ++l) {
@@ -834,11 +841,16 @@ struct W {
     comm_masks();
     if (required) {
       uint8_t* o = required;
-      for (int l = ls; l <= le - 1; ++l) {
+      for (int l = ls; l <= req_hi; ++l) {
         child_required(l, ps, o);
         o += (int64_t)10 * (L(l).n / ps) * (L(l).n / ps) * 4;
       }
     }
+  }
+  // adapt after refine() (post_refine's comm_masks, mask_adj_finer_scale,
+  // complete_masks, mask_trsk) on levels ls .. le, le being the level_end that
+  // refine left.
+  void mask_phase2() {
     comm_masks();  // post_refine
     for (int l = le - 1; l >= ls; --l) {
       mask_adj_child(l);
@@ -918,6 +930,31 @@ int orc_mask_build(orc_wlevel* lv, int ls, int le, int nz, const double* thresho
                    int patch_size, uint8_t* child_required) {
   W w{lv, ls, le, nz};
   w.mask_build(threshold, level_fill, max_level, patch_size, child_required);
+  return 0;
+}
+
+// The two halves of adapt's mask sequence around refine(): the first on levels
+// ls..le with the check_child_required flags of parent levels ls..req_hi, the
+// second on ls..le as refine left level_end.
+int orc_mask_phase1(orc_wlevel* lv, int ls, int le, int nz, const double* threshold, int level_fill, int max_level,
+                    int patch_size, uint8_t* child_required, int req_hi) {
+  W w{lv, ls, le, nz};
+  w.mask_phase1(threshold, level_fill, max_level, patch_size, child_required, req_hi);
+  return 0;
+}
+
+int orc_mask_phase2(orc_wlevel* lv, int ls, int le, int nz) {
+  W w{lv, ls, le, nz};
+  w.mask_phase2();
+  return 0;
+}
+
+// mask_adj_child of the parents of level l (l in [ls, le-1]) alone, as
+// init_structures applies it to the root level (src/main.f90:514).
+int orc_mask_adj_child(orc_wlevel* lv, int ls, int le, int nz, int l) {
+  if (l < ls || l >= le) return 1;
+  W w{lv, ls, le, nz};
+  w.mask_adj_child(l);
   return 0;
 }
 

@@ -32,6 +32,9 @@ def _bind():
         getattr(L, name).argtypes = [P, C.c_int, C.c_int, C.c_int]
     L.orc_mask_tol.argtypes = [P, C.c_int, C.c_int, C.c_int, _dp, C.c_int]
     L.orc_mask_build.argtypes = [P, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    L.orc_mask_phase1.argtypes = [P, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int]
+    L.orc_mask_phase2.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    L.orc_mask_adj_child.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int]
     return L
 
 
@@ -79,11 +82,12 @@ class Hierarchy:
     def set(self, level, name, value):
         self.f[level - self.ls][name][...] = value
 
-    def forward(self):
-        self.L.orc_wt_forward(self.arr, self.ls, self.le, self.nz)
+    def forward(self, le=None):
+        """forward_wavelet_transform over levels ls .. le (default: the top)."""
+        self.L.orc_wt_forward(self.arr, self.ls, self.le if le is None else le, self.nz)
 
-    def inverse(self):
-        self.L.orc_wt_inverse(self.arr, self.ls, self.le, self.nz)
+    def inverse(self, le=None):
+        self.L.orc_wt_inverse(self.arr, self.ls, self.le if le is None else le, self.nz)
 
     def mask_tol(self, threshold, level_fill):
         thr = np.ascontiguousarray(threshold, dtype=np.float64).reshape(3, self.nz)
@@ -99,8 +103,28 @@ class Hierarchy:
                               int(patch_size), None if out is None else out.ctypes.data)
         return out
 
-    def compress(self):
-        self.L.orc_compress(self.arr, self.ls, self.le, self.nz)
+    def mask_phase1(self, threshold, level_fill, max_level, patch_size, le, req_hi):
+        """adapt's mask sequence up to refine() on levels ls .. le; returns the
+        check_child_required flags of parent levels ls .. req_hi (uint8, level
+        by level, lozenge-major, 4 quadrants a parent patch)."""
+        thr = np.ascontiguousarray(threshold, dtype=np.float64).reshape(3, self.nz)
+        n = sum(10 * (g.n // patch_size) ** 2 * 4 for g in self.levels[:req_hi - self.ls + 1])
+        out = np.zeros(max(n, 1), dtype=np.uint8)
+        self.L.orc_mask_phase1(self.arr, self.ls, int(le), self.nz, _p(thr), int(level_fill), int(max_level),
+                               int(patch_size), out.ctypes.data, int(req_hi))
+        return out[:n]
+
+    def mask_phase2(self, le):
+        """adapt's mask sequence after refine() on levels ls .. le."""
+        self.L.orc_mask_phase2(self.arr, self.ls, int(le), self.nz)
+
+    def mask_adj_child(self, level):
+        """mask_adj_child of the parents of `level` alone."""
+        if self.L.orc_mask_adj_child(self.arr, self.ls, self.le, self.nz, int(level)):
+            raise ValueError("mask_adj_child: level out of range")
+
+    def compress(self, le=None):
+        self.L.orc_compress(self.arr, self.ls, self.le if le is None else le, self.nz)
 
     def wt_after_step(self):
         self.L.orc_wt_after_step(self.arr, self.ls, self.le, self.nz)

@@ -34,7 +34,7 @@ def test_adaptive_steps_match_oracle(lmin, lmax, nz, tol, upload):
     G = Grid(lmin, lmax, radius=6371e3)
     levels = [G.level(l) for l in range(lmin, lmax + 1)]
     states = [bump_state(g, nz, seed=1, ph=ph) for g in levels]
-    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=tol)
+    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=tol, init="dense")
     # oracle: the same sequence of calls
     H = Hierarchy(levels, nz)
     for name, key in KEYS:
@@ -89,7 +89,7 @@ def test_adaptive_long_run_masks_every_step(lmin, lmax, nz, dt, nsteps):
     G = Grid(lmin, lmax, radius=6371e3)
     levels = [G.level(l) for l in range(lmin, lmax + 1)]
     states = [bump_state(g, nz, seed=2, ph=ph) for g in levels]
-    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3)
+    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3, init="dense")
     H = Hierarchy(levels, nz)
     for name, key in KEYS:
         H.set(lmax, key, states[-1][name])
@@ -135,8 +135,8 @@ def test_skipping_inactive_nodes_changes_nothing(lmin, lmax, nz, dt, nsteps):
     G = Grid(lmin, lmax, radius=6371e3)
     levels = [G.level(l) for l in range(lmin, lmax + 1)]
     states = [bump_state(g, nz, seed=3, ph=ph) for g in levels]
-    a = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3)
-    b = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3)
+    a = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3, init="dense")
+    b = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3, init="dense")
     b.dev.skip_inactive(False)
     for s in range(nsteps):
         a.step(dt)

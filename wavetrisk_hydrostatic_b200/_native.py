@@ -164,6 +164,14 @@ _DEVICE_SIGS = {
     "wt_mask_tol_vars": [_vp, _dp, C.c_int],
     "wt_compress": [_vp],
     "wt_mask_build": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p],
+    "wt_tree_init": [_vp, C.c_int],
+    "wt_tree_level_end": [_vp, C.POINTER(C.c_int)],
+    "wt_tree_download": [_vp, C.c_int, C.c_void_p, C.c_void_p],
+    "wt_grid_sync": [_vp, C.c_void_p, C.c_int],
+    "wt_adapt": [_vp, _dp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "wt_count_active": [_vp, _dp, C.POINTER(C.c_longlong)],
+    "wt_tree_stats": [_vp, C.c_int, C.POINTER(C.c_longlong)],
+    "wt_mask_adj_child": [_vp, C.c_int],
     "wt_wt_after_step": [_vp],
     "wt_step1_vort": [_vp, C.c_int, _dp],
     "wt_barotropic_upload_level": [_vp, C.c_int, _dp, _dp],

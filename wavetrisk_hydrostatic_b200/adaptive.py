@@ -1,20 +1,28 @@
-"""Host driver of the adaptive ocean time step on a fully refined hierarchy.
+"""Host driver of the adaptive ocean time step on a hierarchy of levels whose
+patch tree is partially refined.
 
-It mirrors the reference's time loop for an explicit (non-mode-split)
-incompressible run, time_step in src/main.f90:405-444:
+It mirrors the reference's explicit (non-mode-split) incompressible run:
+initialize (src/main.f90:36-135) builds the initial grid level by level
+(count_active, adapt with refine(), until level_end reaches max_level or the
+patches just made hold no significant wavelet), then time_step
+(src/main.f90:405-444) does
 
     dt_step (RK4 with trend_ml and WT_after_step per stage)
-    adapt (set_thresholds, the mask sequence, compress_wavelets)
+    adapt (set_thresholds, the mask sequence with refine(), compress_wavelets)
     inverse_wavelet_transform (wav_coeff, sol)
 
-on levels [min_level, max_level] with every patch present: refine() has no
-patch to create, so adapt reduces to its mask sequence (check_child_required
-is still returned).  The thresholds follow initialize_thresholds_case and
-set_thresholds_case of the reference's ocean test cases
-(test/seamount/test_case_module.f90:554-608): tol * (rho0 dz_k, 1e16, Udim)
-by default, or tol * cal_lnorm("inf") with the same floors and the 1 % / 99 %
-blending after step 10 when dynamic.  Everything below runs on the device
-through the C-ABI (include/wavetrisk_gpu.h); this class only sequences it.
+Every level's fields are allocated on the device; the patch tree (one byte
+per PATCH_SIZE^2 patch, refined on the device, include/wavetrisk_gpu.h) says
+which patches exist, and the levels above its level_end hold ZERO masks.  The
+thresholds follow initialize_thresholds_case and set_thresholds_case of the
+reference's ocean test cases (test/seamount/test_case_module.f90:554-608): tol *
+(rho0 dz_k, 1e16, Udim) by default, or tol * cal_lnorm("inf") with the same
+floors and the 1 % / 99 % blending after step 10 when dynamic.  Everything
+below runs on the device through the C-ABI; this class only sequences it.
+
+init="dense" keeps the earlier start-up instead: the initial condition on the
+finest level, its wavelets on every level at once, one adapt and the inverse
+transform, with every patch present.
 """
 from __future__ import annotations
 
@@ -24,14 +32,27 @@ from .cases import OceanParams
 from .grid import Grid, halo_nodes
 from .model import WaveletHierarchy, solver_opts
 
+TOLRNZ, ZERO = 16, 0
+
+
+def patch_size_for(min_level: int) -> int:
+    """PATCH_SIZE = 2^PATCH_LEVEL with PATCH_LEVEL = MIN_LEVEL - DOMAIN_LEVEL - 1
+    (src/shared.f90:33) and DOMAIN_LEVEL from the reference's parameter files
+    (src/param_J3.f90 .. param_J9.f90: 0, 1, 2, 3 for MIN_LEVEL 3..6, then 2)."""
+    domain_level = {3: 0, 4: 1, 5: 2, 6: 3}.get(min_level, 2)
+    return 2 ** (min_level - domain_level - 1)
+
 
 class AdaptiveOcean:
     def __init__(self, grid: Grid, min_level: int, max_level: int, nz: int, states: list[dict],
                  ph: OceanParams | None = None, tol: float = 5e-3, udim: float = 1.0, level_fill: int = 0,
-                 dynamic_thresholds: bool = False):
+                 dynamic_thresholds: bool = False, init: str = "reference", root_state: dict | None = None):
         """states[q]: dict of mass, temp, velo, mean_m, mean_t, topo of level
-        min_level + q; the scaling fields of the finest level are the initial
-        condition, the coarser ones are recomputed by the forward transform."""
+        min_level + q, the initial condition evaluated on that level;
+        root_state the same on level min_level - 1 (init="reference": the
+        reference keeps that level below level_start, and its forward transform
+        takes level_start's wavelets from it).  init="dense": only the finest
+        level's scaling fields are read."""
         self.ph = ph or OceanParams()
         self.levels = [grid.level(l) for l in range(min_level, max_level + 1)]
         self.nz, self.tol, self.udim = nz, tol, udim
@@ -51,10 +72,82 @@ class AdaptiveOcean:
         self.threshold_def = tol * lnorm
         self.threshold = self.threshold_def.copy()
         self.istep = 0
-        # initial grid: wavelets of the initial condition, masks, compression, inverse transform
-        self.dev.forward()
-        self.adapt()
-        self.dev.inverse()
+        self.patch_size = patch_size_for(min_level)
+        self.tree = False
+        self.init_log = []
+        if init == "reference":
+            if root_state is None:
+                raise ValueError("init='reference' needs root_state: the initial condition on level min_level-1")
+            self._reference_init(grid, states, root_state)
+        elif init == "dense":
+            # initial grid: wavelets of the initial condition, masks, compression, inverse transform
+            self.dev.forward()
+            self.adapt()
+            self.dev.inverse()
+        else:
+            raise ValueError(f"unknown init {init!r}")
+
+    def _reference_init(self, grid: Grid, states: list[dict], root_state: dict) -> None:
+        """initialize (src/main.f90:36-135) for fixed thresholds.
+
+        init_structures (src/main.f90:482-524): masks TOLRNZ on the root level
+        (init_masks, src/mask.f90:704-720), level_start's patches made
+        (add_second_level), mask_adj_child of the root; level_end =
+        level_start.  Then count_active (the initial condition on every level
+        and forward_wavelet_transform down to the root, src/main.f90:137-172)
+        and adapt until level_end reaches max_level or the patches the last
+        adapt made hold no significant wavelet; then adapt and count_active
+        once more.  The root level lives in a second two-level hierarchy
+        (root, level_start) that gives level_start its wavelets."""
+        ls, nz, dev = self.min_level, self.nz, self.dev
+        root = grid.level(ls - 1)
+        R = WaveletHierarchy([root, self.levels[0]], [root_state["topo"], states[0]["topo"]], nz, self.ph)
+        try:
+            for g in self.levels:
+                dev.upload(g.level, "mask_n", ZERO)
+                dev.upload(g.level, "mask_e", ZERO)
+            R.upload(root.level, "mask_n", TOLRNZ)
+            R.upload(root.level, "mask_e", TOLRNZ)
+            R.upload(ls, "mask_n", ZERO)
+            R.upload(ls, "mask_e", ZERO)
+            R.mask_adj_child(root.level)
+            dev.upload(ls, "mask_n", R.download(ls, "mask_n"))
+            dev.upload(ls, "mask_e", R.download(ls, "mask_e"))
+            dev.tree_init(self.patch_size)
+            self.tree = True
+
+            def count_active():
+                dev.upload_many([(g.level, name, st[name]) for g, st in zip(self.levels, states)
+                                 for name in ("mass", "temp", "velo")])
+                dev.forward()
+                R.upload_many([(ls, name, dev.download(ls, name)) for name in ("mass", "temp", "velo", "mask_n",
+                                                                               "mask_e")]
+                              + [(root.level, name, root_state[name]) for name in ("mass", "temp", "velo")])
+                R.forward()
+                dev.upload_many([(ls, name, R.download(ls, name)) for name in ("wc_mass", "wc_temp", "wc_velo")])
+
+            count_active()
+            while dev.tree_level_end() < self.max_level:
+                self.set_thresholds()
+                le, _ = dev.adapt(self.threshold, self.level_fill, self.max_level)
+                count_active()
+                nn, ne = dev.count_active(self.threshold)
+                self.init_log.append((le, nn, ne))
+                if nn == 0 and ne == 0:
+                    break
+            self.set_thresholds()
+            dev.adapt(self.threshold, self.level_fill, self.max_level)
+            count_active()
+        finally:
+            R.close()
+
+    def level_end(self) -> int:
+        """The patch tree's level_end (the hierarchy's top without a tree)."""
+        return self.dev.tree_level_end() if self.tree else self.max_level
+
+    def patches(self, level: int):
+        """Patch existence of `level` ([10][n/ps][n/ps] bool), or None without a tree."""
+        return self.dev.tree(level, self.patch_size)[0] if self.tree else None
 
     def set_thresholds(self) -> None:
         """set_thresholds_case (test/seamount/test_case_module.f90:554-581)."""
@@ -67,9 +160,14 @@ class AdaptiveOcean:
         self.threshold = 0.01 * new + 0.99 * self.threshold if self.istep >= 10 else new.copy()
 
     def adapt(self, patch_size: int = 0):
-        """adapt (src/adapt.f90:14-65) on the dense hierarchy; returns the
-        check_child_required flags when patch_size > 0."""
+        """adapt (src/adapt.f90:14-65): with a patch tree the mask sequence with
+        refine() inside and compression (returns None); without one the mask
+        sequence on the whole hierarchy, returning the check_child_required
+        flags when patch_size > 0."""
         self.set_thresholds()
+        if self.tree:
+            self.dev.adapt(self.threshold, self.level_fill, self.max_level)
+            return None
         req = self.dev.mask_build(self.threshold, self.level_fill, self.max_level, patch_size)
         self.dev.compress()
         return req
@@ -79,7 +177,8 @@ class AdaptiveOcean:
         fixed thresholds the whole step is one graph replay on the device
         (wt_adaptive_step); dynamic thresholds need cal_lnorm of the new state
         on the host between the RK4 and the mask sequence."""
-        if not self.dynamic:
+        if not self.dynamic and (not self.tree or self.dev.tree_level_end() == self.max_level):
+            # the step graph refines the tree on the device while its level_end is the top
             self.set_thresholds()
             self.dev.adaptive_step(dt, self.threshold, self.level_fill, self.max_level)
         else:
@@ -128,9 +227,11 @@ class ModeSplitOcean(AdaptiveOcean):
             raise ValueError("the free-surface solver is set up for dt = %g" % self.dt)
         self.set_thresholds()
         rep = self.dev.rk4_split(self.dt, self.theta1, self.theta2, self.solver)
-        req = self.dev.mask_build(self.threshold, self.level_fill, self.max_level, 0)
-        del req
-        self.dev.compress()
+        if self.tree:
+            self.dev.adapt(self.threshold, self.level_fill, self.max_level)
+        else:
+            self.dev.mask_build(self.threshold, self.level_fill, self.max_level, 0)
+            self.dev.compress()
         self.dev.inverse()
         self.dev.free_surface_adapt()
         self.istep += 1

@@ -68,6 +68,20 @@ struct WavCtx {
   bool need_ok = false;
   bool skip_inactive = true;
   int skip_epoch = 0;
+  // patch tree (wt_tree_init; tree_ps = 0: none, every patch exists): per
+  // level a byte per patch of tree_ps^2 owned nodes at tree + tree_off[q]
+  // (tree_kernels.cuh), the patches the last refine made at fresh +
+  // tree_off[q], the check_child_required flags of parent level
+  // level_start + q at treq + treq_off[q], and the tree's level_end on the
+  // device (tree_le) and as last read by the host (tree_level_end)
+  int tree_ps = 0;
+  unsigned char* tree = nullptr;
+  unsigned char* fresh = nullptr;
+  unsigned char* treq = nullptr;
+  std::vector<size_t> tree_off, treq_off;
+  int* tree_le = nullptr;
+  int tree_level_end = 0;
+  unsigned long long* tree_cnt = nullptr;  // [2] counters of k_tree_count_new / k_tree_outside
   template <class T>
   cudaError_t alloc(T** p, size_t count) {
     cudaError_t e = cudaMalloc(p, count * sizeof(T));

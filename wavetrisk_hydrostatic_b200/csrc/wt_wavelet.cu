@@ -14,6 +14,7 @@
 #include "wavelet_kernels.cuh"
 #include "wavelet_layers.cuh"
 #include "need_map.cuh"
+#include "tree_kernels.cuh"
 #include "wt_handle.cuh"
 #include "wt_wavctx.cuh"
 
@@ -556,12 +557,17 @@ int wt_mask_tol_vars(wt_handle* h, const double* threshold, int level_fill) {
 // adapt (src/adapt.f90:14-65) without tree surgery, on the dense hierarchy.
 }  // extern "C"
 
-// adapt's mask sequence (src/adapt.f90:14-65) on the dense hierarchy, stream-
-// ordered and without host synchronisation (so that it can be captured in a
-// graph); the thresholds are already in the context's device buffer.  With
-// dreq non-null, check_child_required flags go there (patch_size > 0).
-int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq) {
-  const int ls = h->level_start, le = h->level_end;
+// adapt's mask sequence (src/adapt.f90:14-65) up to refine(), stream-ordered
+// and without host synchronisation (capturable), on levels level_start .. le:
+// init_masks_zero, mask_active (le is level_end: nodes [0, n] there, [-1, n+1]
+// below), mask_adj_same_scale and mask_restrict_same_scale; then, with dreq
+// non-null, check_child_required of the parent levels level_start .. req_hi
+// into dreq (patch_size > 0).  The thresholds are already in the context's
+// device buffer.  Levels above le are the tree's missing levels: their masks
+// stay ZERO.
+static int mask_phase1(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq, int le,
+                int req_hi) {
+  const int ls = h->level_start;
   cudaStream_t s = h->stream;
   const bool child_required = dreq != nullptr;
   for (int l = ls + 1; l <= le; ++l) k_mask_zero<<<nb(3 * h->at(l).NN), TPB, 0, s>>>(view(h, l));
@@ -582,12 +588,39 @@ int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patc
   comm_masks(h);
   if (child_required) {
     int64_t o = 0;
-    for (int l = ls; l <= le - 1; ++l) {
+    for (int l = ls; l <= req_hi; ++l) {
       const int64_t cnt = (int64_t)10 * (h->at(l).n / patch_size) * (h->at(l).n / patch_size) * 4;
       k_child_required<<<nb(cnt), TPB, 0, s>>>(view(h, l), patch_size, dreq + o);
       o += cnt;
     }
   }
+  CKW(cudaGetLastError());
+  return WT_OK;
+}
+
+// refine() on the device tree from the flags in W->treq (tree_kernels.cuh):
+// parent levels req_hi down to level_start, so that every launch reads parent
+// bytes no earlier launch of this refine wrote; clears the new-patch marks
+// first.  Stream-ordered.
+static void tree_refine(wt_handle* h, int req_hi) {
+  WavCtx* W = ctx(h);
+  const int ls = h->level_start, ps = W->tree_ps;
+  cudaStream_t s = h->stream;
+  cudaMemsetAsync(W->fresh, 0, W->tree_off.back(), s);
+  for (int l = req_hi; l >= ls; --l) {
+    const int q = l - ls, np = h->at(l).n / ps;
+    k_tree_refine<<<nb((int64_t)10 * np * np * 4), TPB, 0, s>>>(W->treq + W->treq_off[q], W->tree + W->tree_off[q],
+                                                               W->tree + W->tree_off[q + 1],
+                                                               W->fresh + W->tree_off[q + 1], np, l, W->tree_le);
+  }
+}
+
+// adapt's mask sequence after refine() on levels level_start .. le (the
+// level_end refine left): post_refine's comm_masks, mask_adj_finer_scale,
+// complete_masks and mask_trsk; then the needed-node maps of the new masks.
+static int mask_phase2(wt_handle* h, int le) {
+  const int ls = h->level_start;
+  cudaStream_t s = h->stream;
   comm_masks(h);  // post_refine
   for (int l = le - 1; l >= ls; --l) {
     k_mask_adj_child<<<nodes_blocks(h->at(l).n + 1), TPB, 0, s>>>(view(h, l), view(h, l + 1));
@@ -616,6 +649,27 @@ int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patc
   CKW(cudaGetLastError());
   ctx(h)->zero_ok = false;  // new masks: compress_wavelets has not run under them
   return wt_level_need_build(h);
+}
+
+// adapt's mask sequence (src/adapt.f90:14-65) on every level of the hierarchy,
+// stream-ordered and without host synchronisation (so that it can be captured
+// in a graph).  With dreq non-null, check_child_required flags of parent
+// levels level_start .. level_end-1 go there (patch_size > 0).  With a patch
+// tree whose level_end is the hierarchy's, refine() runs on the device between
+// the two halves, as in the reference (the flags then go to the tree's own
+// buffer when dreq is null).
+int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq) {
+  const int le = h->level_end;
+  WavCtx* W = ctx(h);
+  const bool tree = W->tree_ps > 0 && W->tree_level_end == le && !dreq;
+  const int req_hi = std::min(le, max_level) - 1;
+  if (tree) {
+    if (int rc = mask_phase1(h, level_fill, max_level, W->tree_ps, W->treq, le, req_hi)) return rc;
+    tree_refine(h, req_hi);
+  } else if (int rc = mask_phase1(h, level_fill, max_level, patch_size, dreq, le, le - 1)) {
+    return rc;
+  }
+  return mask_phase2(h, le);
 }
 
 // The needed-node maps of the levels above level_start from the current masks
@@ -945,6 +999,174 @@ int wt_tune(wt_handle* h, int param, int value) {
     return WT_OK;
   }
   return WT_ERR_ARG;
+}
+
+}  // extern "C"
+
+// ---- the patch tree of a partially refined hierarchy (src/refine_patch.f90)
+
+extern "C" {
+
+int wt_tree_init(wt_handle* h, int patch_size) {
+  if (int rc = ready(h)) return rc;
+  const int ls = h->level_start, le = h->level_end;
+  if (patch_size < 2 || (patch_size & 1) || h->at(ls).n % patch_size) return WT_ERR_ARG;
+  WavCtx* W = ctx(h);
+  if (W->tree && W->tree_ps != patch_size) return WT_ERR_STATE;  // one patch size per handle
+  if (!W->tree) {
+    const size_t nl = W->L.size();
+    W->tree_off.assign(nl + 1, 0);
+    W->treq_off.assign(nl, 0);
+    size_t t = 0, r = 0;
+    for (int l = ls; l <= le; ++l) {
+      const size_t np = (size_t)(h->at(l).n / patch_size);
+      W->tree_off[l - ls] = t;
+      W->treq_off[l - ls] = r;
+      t += 10 * np * np;
+      r += 10 * np * np * 4;
+    }
+    W->tree_off[nl] = t;
+    CKW(W->alloc(&W->tree, t));
+    CKW(W->alloc(&W->fresh, t));
+    CKW(W->alloc(&W->treq, r));
+    CKW(W->alloc(&W->tree_le, 1));
+    CKW(W->alloc(&W->tree_cnt, 2));
+  }
+  W->tree_ps = patch_size;
+  // add_second_level: every patch of level_start; none above
+  CKW(cudaMemsetAsync(W->tree, 0, W->tree_off.back(), h->stream));
+  CKW(cudaMemsetAsync(W->tree, 1, W->tree_off[1], h->stream));
+  CKW(cudaMemsetAsync(W->fresh, 0, W->tree_off.back(), h->stream));
+  CKW(cudaMemcpyAsync(W->tree_le, &h->level_start, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  W->tree_level_end = ls;
+  ++W->skip_epoch;  // the hierarchy's step graph re-records (refine inside it or not)
+  return WT_OK;
+}
+
+int wt_tree_level_end(wt_handle* h, int* level_end) {
+  if (int rc = ready(h)) return rc;
+  WavCtx* W = ctx(h);
+  if (!W->tree_ps || !level_end) return W->tree_ps ? WT_ERR_ARG : WT_ERR_STATE;
+  CKW(cudaMemcpyAsync(level_end, W->tree_le, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  if (W->tree_level_end != *level_end) {
+    W->tree_level_end = *level_end;
+    ++W->skip_epoch;
+  }
+  return WT_OK;
+}
+
+int wt_tree_download(wt_handle* h, int level, unsigned char* exist, unsigned char* fresh) {
+  if (int rc = ready(h)) return rc;
+  WavCtx* W = ctx(h);
+  if (!W->tree_ps) return WT_ERR_STATE;
+  if (level < h->level_start || level > h->level_end) return WT_ERR_ARG;
+  const int q = level - h->level_start;
+  const size_t n = W->tree_off[q + 1] - W->tree_off[q];
+  if (exist) CKW(cudaMemcpyAsync(exist, W->tree + W->tree_off[q], n, cudaMemcpyDeviceToHost, h->stream));
+  if (fresh) CKW(cudaMemcpyAsync(fresh, W->fresh + W->tree_off[q], n, cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_grid_sync(wt_handle* h, const unsigned char* exist, int level_end) {
+  if (int rc = ready(h)) return rc;
+  WavCtx* W = ctx(h);
+  if (!W->tree_ps) return WT_ERR_STATE;
+  if (!exist || level_end < h->level_start || level_end > h->level_end) return WT_ERR_ARG;
+  for (size_t x = 0; x < W->tree_off[1]; ++x)
+    if (!exist[x]) return WT_ERR_ARG;  // level_start is complete
+  CKW(cudaMemcpyAsync(W->tree, exist, W->tree_off.back(), cudaMemcpyHostToDevice, h->stream));
+  CKW(cudaMemsetAsync(W->fresh, 0, W->tree_off.back(), h->stream));
+  CKW(cudaMemcpyAsync(W->tree_le, &level_end, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  if (W->tree_level_end != level_end) ++W->skip_epoch;
+  W->tree_level_end = level_end;
+  return WT_OK;
+}
+
+int wt_adapt(wt_handle* h, const double* threshold, int level_fill, int max_level, int* level_end, int* refined) {
+  if (int rc = ready(h)) return rc;
+  WavCtx* W = ctx(h);
+  if (!W->tree_ps) return WT_ERR_STATE;
+  if (!threshold) return WT_ERR_ARG;
+  const int ls = h->level_start, le1 = W->tree_level_end;
+  const int req_hi = std::min(std::min(le1, max_level - 1), h->level_end - 1);
+  CKW(cudaMemcpyAsync(W->thr, threshold, 3 * h->nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  if (int rc = mask_phase1(h, level_fill, max_level, W->tree_ps, W->treq, le1, req_hi)) return rc;
+  if (req_hi >= ls) {
+    tree_refine(h, req_hi);
+  } else {
+    CKW(cudaMemsetAsync(W->fresh, 0, W->tree_off.back(), h->stream));
+  }
+  int le2 = le1;
+  CKW(cudaMemcpyAsync(&le2, W->tree_le, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<unsigned char> fr(W->tree_off.back());
+  CKW(cudaMemcpyAsync(fr.data(), W->fresh, fr.size(), cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  if (le2 != le1) ++W->skip_epoch;
+  W->tree_level_end = le2;
+  if (int rc = mask_phase2(h, le2)) return rc;
+  compress(h);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  if (level_end) *level_end = le2;
+  if (refined) *refined = std::any_of(fr.begin(), fr.end(), [](unsigned char c) { return c != 0; }) ? 1 : 0;
+  return WT_OK;
+}
+
+int wt_count_active(wt_handle* h, const double* threshold, long long* counts) {
+  if (int rc = ready(h)) return rc;
+  WavCtx* W = ctx(h);
+  if (!W->tree_ps) return WT_ERR_STATE;
+  if (!threshold || !counts) return WT_ERR_ARG;
+  CKW(cudaMemcpyAsync(W->thr, threshold, 3 * h->nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CKW(cudaMemsetAsync(W->tree_cnt, 0, 2 * sizeof(unsigned long long), h->stream));
+  for (int l = h->level_start + 1; l <= h->level_end; ++l) {
+    const int n = h->at(l).n;
+    k_tree_count_new<<<nb((int64_t)10 * n * n), TPB, 0, h->stream>>>(
+        view(h, l), W->fresh + W->tree_off[l - h->level_start], W->tree_ps, h->nz, W->thr, W->tree_cnt);
+  }
+  unsigned long long c[2] = {0, 0};
+  CKW(cudaMemcpyAsync(c, W->tree_cnt, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  counts[0] = (long long)c[0];
+  counts[1] = (long long)c[1];
+  return WT_OK;
+}
+
+int wt_tree_stats(wt_handle* h, int level, long long* out) {
+  if (int rc = ready(h)) return rc;
+  WavCtx* W = ctx(h);
+  if (!W->tree_ps) return WT_ERR_STATE;
+  if (!out || level < h->level_start || level > h->level_end) return WT_ERR_ARG;
+  const int q = level - h->level_start, n = h->at(level).n;
+  const size_t np2 = W->tree_off[q + 1] - W->tree_off[q];
+  std::vector<unsigned char> ex(np2), fr(np2);
+  CKW(cudaMemsetAsync(W->tree_cnt, 0, 2 * sizeof(unsigned long long), h->stream));
+  k_tree_outside<<<nb((int64_t)10 * n * n), TPB, 0, h->stream>>>(view(h, level), W->tree + W->tree_off[q], W->tree_ps,
+                                                                 W->tree_cnt);
+  unsigned long long c[2] = {0, 0};
+  CKW(cudaMemcpyAsync(ex.data(), W->tree + W->tree_off[q], np2, cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaMemcpyAsync(fr.data(), W->fresh + W->tree_off[q], np2, cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaMemcpyAsync(c, W->tree_cnt, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  out[0] = (long long)std::count(ex.begin(), ex.end(), (unsigned char)1);
+  out[1] = (long long)std::count(fr.begin(), fr.end(), (unsigned char)1);
+  out[2] = (long long)c[0];
+  return WT_OK;
+}
+
+int wt_mask_adj_child(wt_handle* h, int level) {
+  if (int rc = ready(h)) return rc;
+  if (level < h->level_start || level >= h->level_end) return WT_ERR_ARG;
+  k_mask_adj_child<<<nodes_blocks(h->at(level).n + 1), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1));
+  ctx(h)->zero_ok = false;
+  ctx(h)->need_ok = false;
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
 }
 
 }  // extern "C"

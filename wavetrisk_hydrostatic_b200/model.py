@@ -272,6 +272,54 @@ class WaveletHierarchy(DeviceGrid):
     def compress(self) -> None:
         N.check("wt_compress", N.lib().wt_compress(self.h))
 
+    # ---- patch tree (src/refine_patch.f90)
+    def tree_init(self, patch_size: int) -> None:
+        N.check("wt_tree_init", N.lib().wt_tree_init(self.h, int(patch_size)))
+
+    def tree_level_end(self) -> int:
+        le = C.c_int(0)
+        N.check("wt_tree_level_end", N.lib().wt_tree_level_end(self.h, C.byref(le)))
+        return le.value
+
+    def tree(self, level: int, patch_size: int):
+        """(exist, fresh) patch bytes of `level` as bool arrays [10][n/ps][n/ps]."""
+        npp = self.levels[level - self.ls].n // patch_size
+        ex = np.empty((10, npp, npp), dtype=np.uint8)
+        fr = np.empty_like(ex)
+        N.check("wt_tree_download", N.lib().wt_tree_download(self.h, int(level), ex.ctypes.data, fr.ctypes.data))
+        return ex.astype(bool), fr.astype(bool)
+
+    def grid_sync(self, exist_levels, level_end: int) -> None:
+        """Upload a host tree: exist_levels[q] the patch bytes of level ls + q."""
+        buf = np.ascontiguousarray(np.concatenate([np.asarray(e, dtype=np.uint8).ravel() for e in exist_levels]))
+        N.check("wt_grid_sync", N.lib().wt_grid_sync(self.h, buf.ctypes.data, int(level_end)))
+
+    def adapt(self, threshold: np.ndarray, level_fill: int, max_level: int):
+        """adapt on the tree (mask sequence with refine() inside, compression);
+        returns (level_end, refined)."""
+        thr = _c(np.asarray(threshold).reshape(3, self.nz))
+        le, rf = C.c_int(0), C.c_int(0)
+        N.check("wt_adapt", N.lib().wt_adapt(self.h, N.dptr(thr), int(level_fill), int(max_level), C.byref(le),
+                                             C.byref(rf)))
+        return le.value, bool(rf.value)
+
+    def count_active(self, threshold: np.ndarray):
+        """count_active over the patches the last refine made: (node, edge) counts."""
+        thr = _c(np.asarray(threshold).reshape(3, self.nz))
+        out = (C.c_longlong * 2)()
+        N.check("wt_count_active", N.lib().wt_count_active(self.h, N.dptr(thr), out))
+        return int(out[0]), int(out[1])
+
+    def tree_stats(self, level: int):
+        """(patches, patches made by the last refine, owned nodes outside the
+        tree with a mask that is not ZERO) of `level`."""
+        out = (C.c_longlong * 3)()
+        N.check("wt_tree_stats", N.lib().wt_tree_stats(self.h, int(level), out))
+        return int(out[0]), int(out[1]), int(out[2])
+
+    def mask_adj_child(self, level: int) -> None:
+        N.check("wt_mask_adj_child", N.lib().wt_mask_adj_child(self.h, int(level)))
+
     def wt_after_step(self) -> None:
         N.check("wt_wt_after_step", N.lib().wt_wt_after_step(self.h))
 

@@ -391,7 +391,9 @@ int wt_adapt(wt_handle* h, const double* threshold, int level_fill, int max_leve
  * threshold(v, k), counts[1] edge wavelets (velocity). */
 int wt_count_active(wt_handle* h, const double* threshold, long long* counts);
 /* out[0] patches of the level, out[1] of them made by the last refine, out[2]
- * owned nodes outside the tree with a node or edge mask that is not ZERO. */
+ * owned nodes outside the tree with a node or edge mask that is not ZERO,
+ * out[3] owned nodes in the level's needed-node map (-1 without one).  No
+ * reference counterpart (diagnostics). */
 int wt_tree_stats(wt_handle* h, int level, long long* out);
 /* mask_adj_child (src/mask.f90:314-466) of the parents of `level` alone, as
  * init_structures applies it to the root level (src/main.f90:514). */

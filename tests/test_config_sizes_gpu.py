@@ -3,15 +3,17 @@ configurations, through the C-ABI.
 
 * Plain method (uniform J5, 8 layers, jet + white-noise free surface, RK4
   dt 300 s): the state after every one of 100 steps, bit for bit.
-* Adaptive J4..J7, 16 layers (jet + 8 Gaussian bumps, tol 5e-3, dt 150 s):
-  every mask of every level after every one of 20 steps, bit for bit; the
-  scaling fields of every level at the end, bit for bit.
+* Adaptive J4..J7, 16 layers (jet + 8 Gaussian bumps, tol 5e-3, dt 150 s),
+  the initial grid refined level by level as the reference's initialize
+  does: the patch tree and every mask of every level after every one of 20
+  steps, bit for bit; the scaling fields of every level at the end, bit for
+  bit.
 * Elliptic: the operator at J7 and J8, restriction J8 -> J5 and prolongation
   into J7 and J8 on the hierarchy J5..J8; FMG and SRJ at J7 with the oracle's
   iteration counts.
 * The benchmark's adaptive workload at J5..J8, 32 layers (seamount, jet and
-  bumps, dt 75 s): masks after every one of 3 steps bit for bit, fields at the
-  end bit for bit.
+  bumps, dt 75 s, the reference's initial refinement): tree and masks after
+  every one of 3 steps bit for bit, fields at the end bit for bit.
 
 The FP64 kernels are compiled without FMA contraction and follow the oracle's
 operand order, so their results are compared with np.array_equal; the
@@ -22,9 +24,9 @@ import pytest
 
 import oracle
 from oracle.elliptic import Hierarchy as EHier
-from oracle.wavelet import Hierarchy
+from oracle.tree import ReferenceInit, adapt
 from wavetrisk_hydrostatic_b200 import Grid, OceanParams, jet_state
-from wavetrisk_hydrostatic_b200.adaptive import AdaptiveOcean
+from wavetrisk_hydrostatic_b200.adaptive import AdaptiveOcean, patch_size_for
 from wavetrisk_hydrostatic_b200.cases import bathymetry, bump_state, elliptic_rhs, seamount_topography
 from wavetrisk_hydrostatic_b200.grid import halo_nodes
 from wavetrisk_hydrostatic_b200.model import EllipticSolver, TriskModel, solver_opts
@@ -60,38 +62,38 @@ def test_plain_method_j5x8_100_steps_every_step():
 
 
 def _adaptive_pair(lmin, lmax, nz, make, ph):
-    """The device model and the oracle hierarchy after the initial adapt, and
-    the per-level inputs the oracle's steps need besides the state."""
+    """The device model and the oracle hierarchy after the reference's initial
+    refinement (the patch tree grown level by level from level_start + 1),
+    and the per-level inputs the oracle's steps need besides the state."""
     G = Grid(lmin, lmax, radius=6371e3)
+    root = G.level(lmin - 1)
     levels = [G.level(l) for l in range(lmin, lmax + 1)]
-    states = [make(g) for g in levels]
-    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3)
-    H = Hierarchy(levels, nz)
-    for name, key in KEYS:
-        H.set(lmax, key, states[-1][name])
-    H.forward()
-    H.mask_build(model.threshold_def, 0, lmax)
-    H.compress()
-    H.inverse()
+    ics = {g.level: make(g) for g in [root] + levels}
+    states = [ics[g.level] for g in levels]
+    model = AdaptiveOcean(G, lmin, lmax, nz, states, ph, tol=5e-3, root_state=ics[root.level])
+    RI = ReferenceInit(root, levels, nz, ics, model.threshold_def, lmax, ps=patch_size_for(lmin)).run()
     base = [{k: v for k, v in st.items() if k not in ("mass", "temp", "velo")} for st in states]
-    return levels, model, H, base
+    return levels, model, RI, base
 
 
-def _run_adaptive(levels, model, H, nz, ph, dt, nsteps, base):
+def _run_adaptive(levels, model, RI, nz, ph, dt, nsteps, base):
     lmax = levels[-1].level
+    H, tree = RI.H, RI.tree
     for s in range(nsteps):
         cur = [dict(base[q], **{n: H.field(g.level, k).copy() for n, k in KEYS}) for q, g in enumerate(levels)]
         masks = [(H.field(g.level, "mask_n").copy(), H.field(g.level, "mask_e").copy()) for g in levels]
         oracle.rk4_multi(levels, nz, ph, cur, masks, dt, 1, H=H)
-        H.mask_build(model.threshold_def, 0, lmax)
-        H.compress()
+        adapt(H, tree, model.threshold_def, lmax)
         H.inverse()
         model.step(dt)
+        assert model.level_end() == tree.level_end, s
         for g, (mn, me) in zip(levels, model.masks()):
+            assert np.array_equal(model.patches(g.level), tree.exist[g.level]), (s, g.level, "tree")
             assert np.array_equal(mn, H.field(g.level, "mask_n")), (s, g.level, "mask_n")
             assert np.array_equal(me, H.field(g.level, "mask_e")), (s, g.level, "mask_e")
-    for g in levels:
-        own, edges = _owned_idx(g)
+    for g in levels:  # on the nodes of existing patches, where the state after a step is complete
+        own = np.nonzero(g.owned & tree.node_map(g))[0]
+        edges = np.concatenate([own, own + g.NN, own + 2 * g.NN])
         for name, key in KEYS:
             k = edges if name == "velo" else own
             d, o = model.dev.download(g.level, name)[:, k], H.field(g.level, key)[:, k]
@@ -103,8 +105,8 @@ def test_adaptive_j4_j7_x16_20_steps_masks_every_step():
     oracle.set_threads(10)
     ph = OceanParams()
     nz = 16
-    levels, model, H, base = _adaptive_pair(4, 7, nz, lambda g: bump_state(g, nz, seed=1, ph=ph), ph)
-    _run_adaptive(levels, model, H, nz, ph, 150.0, 20, base)
+    levels, model, RI, base = _adaptive_pair(4, 7, nz, lambda g: bump_state(g, nz, seed=1, ph=ph), ph)
+    _run_adaptive(levels, model, RI, nz, ph, 150.0, 20, base)
     model.close()
 
 
@@ -113,8 +115,8 @@ def test_benchmark_workload_j5_j8_x32_3_steps():
     ph = OceanParams()
     nz = 32
     make = lambda g: bump_state(g, nz, seed=1, ph=ph, topo=seamount_topography(g, seed=1))
-    levels, model, H, base = _adaptive_pair(5, 8, nz, make, ph)
-    _run_adaptive(levels, model, H, nz, ph, 75.0, 3, base)
+    levels, model, RI, base = _adaptive_pair(5, 8, nz, make, ph)
+    _run_adaptive(levels, model, RI, nz, ph, 75.0, 3, base)
     model.close()
 
 

@@ -5,8 +5,10 @@ oracle's restatement (oracle/tree.py) on the same seeded inputs.
 
 After the initialisation and after every step: the tree (every level's patch
 bytes), its level_end, every mask of every level bit for bit; the scaling
-fields of every level bit for bit on owned nodes and edges; and no mask that
-is not ZERO outside the tree (the reference has no node there)."""
+fields of every level bit for bit on the nodes of existing patches and their
+edges (the device limits its work to the tree, so the state is complete
+there, as the reference's is); and no mask that is not ZERO outside the tree
+(the reference has no node there)."""
 import numpy as np
 import pytest
 
@@ -21,8 +23,11 @@ pytestmark = pytest.mark.gpu
 KEYS = (("mass", "s_m"), ("temp", "s_t"), ("velo", "s_v"))
 
 
-def _owned(g):
-    own = np.nonzero(g.owned)[0]
+def _owned(g, tree=None):
+    """Owned nodes (those of existing patches with a tree: after a step the
+    state is complete there, as the reference's is) and their edges."""
+    sel = g.owned if tree is None else g.owned & tree.node_map(g)
+    own = np.nonzero(sel)[0]
     return own, np.concatenate([own, own + g.NN, own + 2 * g.NN])
 
 
@@ -46,7 +51,7 @@ def _check(levels, model, RI, tag, fields=True):
         assert np.array_equal(me, H.field(g.level, "mask_e")), (tag, g.level, "mask_e")
         assert model.dev.tree_stats(g.level)[2] == 0, (tag, g.level, "mask outside the tree")
         if fields:
-            own, edges = _owned(g)
+            own, edges = _owned(g, tree)
             for name, key in KEYS:
                 k = edges if name == "velo" else own
                 d, o = model.dev.download(g.level, name)[:, k], H.field(g.level, key)[:, k]

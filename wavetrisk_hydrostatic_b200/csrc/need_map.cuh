@@ -158,3 +158,95 @@ __global__ void k_map_up(MapLev C, MapLev Pa, const unsigned char* __restrict__ 
 }
 
 }  // namespace wtw
+
+namespace wtw {
+
+// The patch tree's part in the maps (tree_kernels.cuh): the reference
+// computes, transforms and keeps values only on the nodes of existing
+// patches, and reads the 2-node ring of boundary patches around them.
+struct TreeLev {
+  int n, P, NN;
+  const int* nsrc;
+  const unsigned char* exist;  // [10][n/ps][n/ps] patch bytes of this level
+};
+
+// Whether padded slot y of a level is a node of an existing patch (through its
+// ghost source); the pole slots, which no patch's [0, n)^2 holds, count as
+// existing.
+__device__ __forceinline__ bool tree_node(const TreeLev& T, int ps, int y) {
+  const int s = __ldg(T.nsrc + y);
+  const int PP = T.P * T.P;
+  const int d = s / PP, r = s - d * PP;
+  const int i = r % T.P - 2, j = r / T.P - 2;
+  if (i < 0 || j < 0 || i >= T.n || j >= T.n) return true;
+  const int np = T.n / ps;
+  return T.exist[((int64_t)d * np + j / ps) * np + i / ps] != 0;
+}
+
+// Whether a node of an existing patch lies within 2 nodes (i and j each) of
+// padded slot (d, i, j), i, j in [0, n): the patch nodes and their 2-node ring.
+__device__ __forceinline__ bool tree_near(const TreeLev& T, int ps, int d, int i, int j) {
+  for (int b = -2; b <= 2; ++b)
+    for (int a = -2; a <= 2; ++a)
+      if (tree_node(T, ps, (d * T.P + j + b + 2) * T.P + i + a + 2)) return true;
+  return false;
+}
+
+// need &= the tree's nodes and their ring, on the owned nodes [0, n)^2 of one
+// level (the lozenge-corner regions the seed forces stay in).
+__global__ void k_need_tree(TreeLev T, int ps, unsigned char* __restrict__ need) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= T.NN || !need[x]) return;
+  const int PP = T.P * T.P;
+  const int d = x / PP, r = x - d * PP;
+  const int i = r % T.P - 2, j = r / T.P - 2, n = T.n;
+  if (i < 0 || j < 0 || i >= n || j >= n) return;
+  const int cr = NEED_R + 1;
+  if ((i <= cr || i >= n - 1 - cr) && (j <= cr || j >= n - 1 - cr)) return;
+  if (!tree_near(T, ps, d, i, j)) need[x] = 0;
+}
+
+// The parents the inverse transform after adapt rebuilds with a patch tree:
+// those of the next RK stage (recpar, in) and every parent one of whose
+// children within 2 nodes of the coincident child is a node of an existing
+// patch of the child level, so that the state after the step is complete on
+// the tree.  Own-source parent slots only (the kernels read through nsrc).
+__global__ void k_map_tree_par(MapLev Lp, TreeLev Tc, int ps, const unsigned char* __restrict__ in,
+                               unsigned char* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= Lp.NN) return;
+  unsigned char v = in[x];
+  if (!v && __ldg(Lp.nsrc + x) == x) {
+    const int PP = Lp.P * Lp.P;
+    const int d = x / PP, r = x - d * PP;
+    const int ip = r % Lp.P - 2, jp = r / Lp.P - 2;
+    if (ip >= 0 && jp >= 0 && ip <= Lp.n && jp <= Lp.n) v = tree_near(Tc, ps, d, 2 * ip < Tc.n ? 2 * ip : Tc.n - 1,
+                                                                     2 * jp < Tc.n ? 2 * jp : Tc.n - 1);
+    else
+      v = 1;
+  }
+  out[x] = v;
+}
+
+}  // namespace wtw
+
+namespace wtw {
+
+// A level's work list from its needed-node map: every padded slot x with
+// need[nsrc[x]] set, appended by warp-aggregated atomics (the order varies
+// from build to build; each slot's results do not depend on it).  *count
+// must be 0 on entry.
+__global__ void k_list_build(MapLev L, const unsigned char* __restrict__ need, int* __restrict__ ids,
+                             int* __restrict__ count) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool on = x < L.NN && need[__ldg(L.nsrc + x)] != 0;
+  const unsigned m = __ballot_sync(0xffffffffu, on);
+  if (!m) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(m, base, leader);
+  if (on) ids[base + __popc(m & ((1u << lane) - 1))] = x;
+}
+
+}  // namespace wtw

@@ -50,6 +50,11 @@ __global__ void k_halo_state(int nz, int64_t NN, const int2* __restrict__ hn, in
 // integrate_pressure_up (src/ops.f90:1094-1131), incompressible case, for every
 // node (i, j) in [0, n]^2 of every lozenge.  Writes the layer geopotential
 // Phi_k = interp(geopot, geopot_lower) and press/(rho0*phi).
+__device__ __forceinline__ void column_node(const LevelDev& L, const Phys& ph, int nz, const double* __restrict__ mass,
+                                            const double* __restrict__ temp, const double* __restrict__ mean_m,
+                                            const double* __restrict__ mean_t, double* __restrict__ phik,
+                                            double* __restrict__ pterm, int id, int i, int j);
+
 __global__ void __launch_bounds__(NODE_TILE) k_column(LevelDev L, Phys ph, int nz, const double* __restrict__ mass,
                                                       const double* __restrict__ temp, const double* __restrict__ mean_m,
                                                       const double* __restrict__ mean_t, double* __restrict__ phik,
@@ -61,6 +66,25 @@ __global__ void __launch_bounds__(NODE_TILE) k_column(LevelDev L, Phys ph, int n
   if (!layer_node(L, 1, k0, id, i, j)) return;
   if (i < 0 || j < 0 || i > L.n || j > L.n) return;
   if (need && !need[__ldg(L.nsrc + id)]) return;
+  column_node(L, ph, nz, mass, temp, mean_m, mean_t, phik, pterm, id, i, j);
+}
+
+// The same over a work list (persistent blocks).
+__global__ void __launch_bounds__(NODE_TILE) k_column_list(LevelDev L, Phys ph, int nz, const double* __restrict__ mass,
+                                                           const double* __restrict__ temp,
+                                                           const double* __restrict__ mean_m,
+                                                           const double* __restrict__ mean_t, double* __restrict__ phik,
+                                                           double* __restrict__ pterm, NodeList W) {
+  for_list(L, 1, W, [&](int, int id, int i, int j) {
+    if (i < 0 || j < 0 || i > L.n || j > L.n) return;
+    column_node(L, ph, nz, mass, temp, mean_m, mean_t, phik, pterm, id, i, j);
+  });
+}
+
+__device__ __forceinline__ void column_node(const LevelDev& L, const Phys& ph, int nz, const double* __restrict__ mass,
+                                            const double* __restrict__ temp, const double* __restrict__ mean_m,
+                                            const double* __restrict__ mean_t, double* __restrict__ phik,
+                                            double* __restrict__ pterm, int id, int i, int j) {
   const int src = (i < L.n && j < L.n) ? id : L.nsrc[id];
   double sp = 0.0;
   for (int k = 0; k < nz; ++k) {
@@ -191,6 +215,12 @@ __device__ __noinline__ void post_corner(const LevelDev L, int c, int d, int64_t
 // reference's sequential sweep leaves behind; the four corner threads then
 // apply post_step1.  The node's potential temperature Theta/rho
 // (src/ops.f90:798, theta_e's node factor) is stored for the velocity trend.
+__device__ __forceinline__ void step1_node(const LevelDev& L, int nz, const double* __restrict__ mass,
+                                           const double* __restrict__ temp, const double* __restrict__ velo,
+                                           const double* __restrict__ mean_m, const double* __restrict__ mean_t,
+                                           const double* __restrict__ phik, const double* __restrict__ pterm,
+                                           const Step1Out& out, int k, int id, int i, int j);
+
 __global__ void __launch_bounds__(NODE_TILE, 3)
     k_step1(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
             const double* __restrict__ velo, const double* __restrict__ mean_m, const double* __restrict__ mean_t,
@@ -200,6 +230,26 @@ __global__ void __launch_bounds__(NODE_TILE, 3)
   if (!layer_node(L, nz, k, id, i, j)) return;
   if (i < 0 || j < 0 || i > L.n || j > L.n) return;
   if (need && !need[__ldg(L.nsrc + id)]) return;  // needed-node map (need_map.cuh)
+  step1_node(L, nz, mass, temp, velo, mean_m, mean_t, phik, pterm, out, k, id, i, j);
+}
+
+// The same over a work list (persistent blocks).
+__global__ void __launch_bounds__(NODE_TILE, 3)
+    k_step1_list(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
+                 const double* __restrict__ velo, const double* __restrict__ mean_m,
+                 const double* __restrict__ mean_t, const double* __restrict__ phik,
+                 const double* __restrict__ pterm, Step1Out out, NodeList W) {
+  for_list(L, nz, W, [&](int k, int id, int i, int j) {
+    if (i < 0 || j < 0 || i > L.n || j > L.n) return;
+    step1_node(L, nz, mass, temp, velo, mean_m, mean_t, phik, pterm, out, k, id, i, j);
+  });
+}
+
+__device__ __forceinline__ void step1_node(const LevelDev& L, int nz, const double* __restrict__ mass,
+                                           const double* __restrict__ temp, const double* __restrict__ velo,
+                                           const double* __restrict__ mean_m, const double* __restrict__ mean_t,
+                                           const double* __restrict__ phik, const double* __restrict__ pterm,
+                                           const Step1Out& out, int k, int id, int i, int j) {
   const int NN = L.NN;
   const int P = L.P;
   const int idN = id + P, idE = id + 1, idS = id - P, idW = id - 1, idNE = id + P + 1, idSW = id - P - 1;

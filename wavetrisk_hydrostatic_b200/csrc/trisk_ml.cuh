@@ -41,10 +41,24 @@ struct TrendML {
 
 constexpr int ML_TRSK = 2, ML_ADJZONE = 8;
 
+__device__ __forceinline__ void trend_ml_node(const LevelDev& L, int nz, const TrendML& io, int k, int id, int i,
+                                              int j);
+
 __global__ void __launch_bounds__(NODE_TILE, 4) k_trend_ml(LevelDev L, int nz, TrendML io) {
   int k, id, i, j;
   if (!layer_node(L, nz, k, id, i, j)) return;
   if (io.need && !io.need[__ldg(L.nsrc + id)]) return;
+  trend_ml_node(L, nz, io, k, id, i, j);
+}
+
+// The same over a work list (persistent blocks): the list holds the padded
+// slots of the needed-node map.
+__global__ void __launch_bounds__(NODE_TILE, 3) k_trend_ml_list(LevelDev L, int nz, TrendML io, NodeList W) {
+  for_list(L, nz, W, [&](int k, int id, int i, int j) { trend_ml_node(L, nz, io, k, id, i, j); });
+}
+
+__device__ __forceinline__ void trend_ml_node(const LevelDev& L, int nz, const TrendML& io, int k, int id, int i,
+                                              int j) {
   const int P = L.P;
   const int NN = L.NN;
   const int n = L.n;

@@ -1,8 +1,10 @@
 // Inline readers shared by the layer kernels: interpolation, node indexing,
 // the layer-fastest block mapping and reads of the state through the ghost
-// remap tables.  Device functions only, so several translation units may
-// include it.
+// remap tables; device functions and one inline host helper (the grid of a
+// persistent kernel), so several translation units may include it.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 
 #include "trisk_types.cuh"
@@ -23,17 +25,53 @@ __device__ __forceinline__ int64_t nid(const LevelDev& L, int d, int i, int j) {
 // levels with 6*NN >= 2^31).
 constexpr int NODE_TILE = 256;
 
-__device__ __forceinline__ bool layer_node(const LevelDev& L, int nz, int& k, int& id, int& i, int& j) {
-  const int chunk = blockIdx.x / nz;
-  k = blockIdx.x - chunk * nz;
-  id = chunk * NODE_TILE + threadIdx.x;
-  if (id >= L.NN) return false;
+__device__ __forceinline__ void node_ij(const LevelDev& L, int id, int& i, int& j) {
   const int pp = L.P * L.P;
   const int r = id - (id / pp) * pp;
   const int jp = r / L.P;
   j = jp - 2;
   i = r - jp * L.P - 2;
+}
+
+__device__ __forceinline__ bool layer_node(const LevelDev& L, int nz, int& k, int& id, int& i, int& j) {
+  const int chunk = blockIdx.x / nz;
+  k = blockIdx.x - chunk * nz;
+  id = chunk * NODE_TILE + threadIdx.x;
+  if (id >= L.NN) return false;
+  node_ij(L, id, i, j);
   return true;
+}
+
+// Grid of a persistent kernel: the blocks of NODE_TILE threads the device
+// keeps resident at once (never more than `dense`, the blocks of the dense
+// launch it replaces).  Host code.
+template <class K>
+inline unsigned persistent_grid(K kernel, unsigned dense) {
+  int dev = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, NODE_TILE, 0) != cudaSuccess || per < 1)
+    return dense;
+  const unsigned g = (unsigned)sms * (unsigned)per;
+  return g < dense ? g : dense;
+}
+
+// Persistent loop over a work list: items (chunk of NODE_TILE entries, layer)
+// layer-fastest as in the dense launches, strided by the grid; f(k, id, i, j)
+// for every entry of the block's chunks.
+template <class F>
+__device__ __forceinline__ void for_list(const LevelDev& L, int nz, const NodeList& W, F f) {
+  const int cnt = __ldg(W.count);
+  const int64_t items = (int64_t)((cnt + NODE_TILE - 1) / NODE_TILE) * nz;
+  for (int64_t w = blockIdx.x; w < items; w += gridDim.x) {
+    const int chunk = (int)(w / nz), k = (int)(w - (int64_t)chunk * nz);
+    const int e = chunk * NODE_TILE + threadIdx.x;
+    if (e >= cnt) continue;
+    const int id = __ldg(W.ids + e);
+    int i, j;
+    node_ij(L, id, i, j);
+    f(k, id, i, j);
+  }
 }
 
 // Readers of the state through the ghost remap.

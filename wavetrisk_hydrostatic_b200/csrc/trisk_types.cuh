@@ -9,6 +9,14 @@ namespace wtk {
 enum { RT = 0, DG = 1, UP = 2 };
 enum { LORT = 0, UPLT = 1 };
 
+// A level's work list: the padded slots a kernel computes (those of the
+// needed-node map), their count on the device, built inside the step's graph
+// (need_map.cuh: k_list_build).
+struct NodeList {
+  const int* ids;
+  const int* count;
+};
+
 struct LevelDev {
   int n, P;
   int NN;  // 10*P*P; 6*NN < 2^31, so offsets inside one layer fit an int

@@ -25,6 +25,7 @@ inline unsigned blocks_for(int64_t n, int tpb = TPB) { return (unsigned)((n + tp
 
 }  // namespace
 
+
 int wt_handle_fail(const char* where, cudaError_t e) {
   std::fprintf(stderr, "wavetrisk_gpu: %s: %s\n", where, cudaGetErrorString(e));
   return e == cudaErrorMemoryAllocation ? WT_ERR_ALLOC : WT_ERR_CUDA;
@@ -479,14 +480,22 @@ int wt_level_trend_ml_tma(wt_handle* h, const wtk::TrendIO& io, const wtk::Trend
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
                    double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream,
-                   const unsigned char* need) {
+                   const unsigned char* need, const wtk::NodeList* list) {
   const DevLevel& D = h->at(level);
   const LevelDev L = D.view();
   const int nz = h->nz;
   cudaStream_t s = stream ? stream : h->stream;
   const unsigned chunks = blocks_for(D.NN, NODE_TILE);
-  k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, mean_m, mean_t, phik, pterm, need);
   Step1Out so{qe, hfm, hft, bern, theta};
+  if (list && list->ids) {  // the needed slots only, persistent blocks over the level's work list
+    k_column_list<<<persistent_grid(k_column_list, chunks), NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, mean_m, mean_t,
+                                                                               phik, pterm, *list);
+    k_step1_list<<<persistent_grid(k_step1_list, chunks * nz), NODE_TILE, 0, s>>>(L, nz, m, t, v, mean_m, mean_t,
+                                                                                  phik, pterm, so, *list);
+    CK(cudaGetLastError());
+    return WT_OK;
+  }
+  k_column<<<chunks, NODE_TILE, 0, s>>>(L, h->ph, nz, m, t, mean_m, mean_t, phik, pterm, need);
   if (maps && level == h->level_end && h->trend_variant == 0) {
     const int nbx = (D.n + 1 + TT_X - 1) / TT_X, nby = (D.n + 1 + TT_Y - 1) / TT_Y;
     const unsigned nblk = (unsigned)(nz * nbx * nby * 10);

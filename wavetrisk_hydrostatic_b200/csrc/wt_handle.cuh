@@ -101,7 +101,7 @@ int wt_level_trend_ml_tma(wt_handle* h, const wtk::TrendIO& io, const wtk::Trend
 int wt_level_step1(wt_handle* h, int level, const double* m, const double* t, const double* v, const double* mean_m,
                    const double* mean_t, double* phik, double* pterm, double* qe, double* hfm, double* hft,
                    double* bern, double* theta, const wtk::Step1Maps* maps, cudaStream_t stream,
-                   const unsigned char* need = nullptr);
+                   const unsigned char* need = nullptr, const wtk::NodeList* list = nullptr);
 // The step1 input maps of a top-level state (WT_ERR_STATE when the handle runs the L1 kernels) (wt_api.cu).
 int wt_make_step1_maps(wt_handle* h, const double* m, const double* t, const double* v, wtk::Step1Maps* out);
 // scalar_cpt_restr / flux_cpt_restr of the nz layers of the given fields from
@@ -131,6 +131,8 @@ int wt_level_wav_forward_pair(wt_handle* h, int level);
 // would be overwritten before anything reads it)
 int wt_level_wav_finish(wt_handle* h, bool partial = false, bool rebuild = true);
 const unsigned char* wt_level_rec(wt_handle* h, int level);
+// the parents the inverse after adapt rebuilds (patch tree), or null: every parent
+const unsigned char* wt_level_rec_final(wt_handle* h, int level);
 // adapt's mask sequence without host synchronisation (capturable), compression
 // and inverse transform of the hierarchy, and the threshold upload (wt_wavelet.cu).
 int wt_level_mask_sequence(wt_handle* h, int level_fill, int max_level, int patch_size, unsigned char* dreq);
@@ -150,6 +152,8 @@ bool wt_level_zero_ok(wt_handle* h);
 // changes to WT_TUNE_SKIP_INACTIVE.
 int wt_level_need_build(wt_handle* h);
 const unsigned char* wt_level_need(wt_handle* h, int level);
+// the work list of a level's needed-node map ({null, null} without a map)
+wtk::NodeList wt_level_list(wt_handle* h, int level);
 int wt_level_skip_epoch(wt_handle* h);
 // barotropic_correction of the given per-level scaling fields (hierarchy's own
 // when m is null) and grad_eta per level, without the velocity update
@@ -162,6 +166,9 @@ int wt_level_grad_eta(wt_handle* h, const double** grad);
 int wt_level_ready_wait(wt_handle* h, int level, cudaStream_t st);
 // build the map if skipping is on and the masks changed since the last build
 int wt_level_need_refresh(wt_handle* h);
+// The inverse transform after adapt (stream-ordered): with a patch tree it
+// rebuilds the parents the next step reads and those of the tree's nodes, so
+// that the state is complete on the tree; without one every parent.
 void wt_level_inverse(wt_handle* h);
 int wt_level_set_thresholds(wt_handle* h, const double* threshold);
 // The scaling fields (mass, Theta, velocity) of a level (wt_wavelet.cu).

@@ -186,6 +186,8 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
   // With WT_after_step following (wav), a level's results above level_start are
   // read only where its needed-node map says so (need_map.cuh).
   auto need = [&](int l) -> const unsigned char* { return (wav && dest && !grad) ? wt_level_need(h, l) : nullptr; };
+  // and then over the level's work list, the needed slots only (persistent blocks)
+  auto list = [&](int l) { return need(l) ? wt_level_list(h, l) : wtk::NodeList{nullptr, nullptr}; };
   // Column + step1 of a level read only that level's state and write only its
   // own work fields, so the coarser levels' run beside the finest level's on
   // side streams (parallel branches of a captured graph).  The phase timer
@@ -204,8 +206,9 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
       } else {
         CKM(cudaStreamWaitEvent(M->side[q], M->fork, 0));
       }
+      const wtk::NodeList wl = list(l);
       if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft, V.bern,
-                                  V.theta, nullptr, M->side[q], need(l)))
+                                  V.theta, nullptr, M->side[q], need(l), &wl))
         return rc;
       CKM(cudaEventRecord(M->done[q], M->side[q]));
     }
@@ -233,8 +236,9 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
           maps = &M->q1maps;
         }
       }
+      const wtk::NodeList wl = list(l);
       if (int rc = wt_level_step1(h, l, S.m[q], S.t[q], S.v[q], mm, mt, V.phik, V.pterm, V.qe, V.hfm, V.hft,
-                                  V.bern, V.theta, maps, nullptr, need(l)))
+                                  V.bern, V.theta, maps, nullptr, need(l), &wl))
         return rc;
       PE(tm, l == h->level_end ? PH_STEP1_TOP : PH_STEP1_COARSE);
       if (concurrent) CKM(cudaEventRecord(M->s1top, h->stream));
@@ -280,7 +284,11 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
     io.need = need(l);
     const unsigned chunks = (unsigned)((D.NN + wtk::NODE_TILE - 1) / wtk::NODE_TILE);
     PB(tm);
-    if (l == h->level_end && M->tmaps_ok && base && dest) {  // TMA-staged, the same arithmetic
+    const wtk::NodeList wl = list(l);
+    if (wl.ids) {  // the needed slots only, persistent blocks over the level's work list
+      wtk::k_trend_ml_list<<<wtk::persistent_grid(wtk::k_trend_ml_list, chunks * nz), wtk::NODE_TILE, 0,
+                             h->stream>>>(D.view(), nz, io, wl);
+    } else if (l == h->level_end && M->tmaps_ok && base && dest) {  // TMA-staged, the same arithmetic
       wtk::TrendIO t{};
       t.theta = V.theta; t.qe = V.qe; t.hfm = V.hfm; t.hft = V.hft; t.bern = V.bern; t.phik = V.phik;
       t.base_m = io.base_m; t.base_t = io.base_t; t.base_v = io.base_v;

@@ -64,7 +64,18 @@ struct WavCtx {
   // parent level (need_map.cuh), at recpar + rec_off[q]; rscr: scratch maps
   unsigned char* recpar = nullptr;
   std::vector<size_t> rec_off;
+  size_t rec_tot = 0;
+  // with a patch tree: the parents the inverse transform after adapt rebuilds
+  // (recpar and every parent of a node of an existing patch), at recfin +
+  // rec_off[q]; recfin_ok once built with the current maps
+  unsigned char* recfin = nullptr;
+  bool recfin_ok = false;
   unsigned char* rscr[2] = {nullptr, nullptr};
+  // work lists of the levels above level_start (need_map.cuh: k_list_build):
+  // the slots of the needed-node map at list + need_off[q], their count at
+  // list_cnt[q], built with the maps
+  int* list = nullptr;
+  int* list_cnt = nullptr;
   bool need_ok = false;
   bool skip_inactive = true;
   int skip_epoch = 0;

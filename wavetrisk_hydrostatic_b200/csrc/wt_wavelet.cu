@@ -136,7 +136,9 @@ void launch_velo_wc(wt_handle* h, int l, cudaStream_t s, cudaStream_t si) {
 // scalars and the velocity reconstruct independently of each other, so the
 // scalar chain (Prolong_scalar, Reconstruct_scalar per level) runs on a side
 // stream beside the velocity chain (outer, then inner edges per level).
-void inverse(wt_handle* h, bool partial = false) {
+// partial 0: every parent; 1: those of wt_level_rec (an intermediate RK
+// stage); 2: those of wt_level_rec_final (after adapt, with a patch tree)
+void inverse(wt_handle* h, int partial = 0) {
   const int nz = h->nz;
   WavCtx* W = ctx(h);
   cudaStream_t s = h->stream, sa = W->side[0];
@@ -147,7 +149,7 @@ void inverse(wt_handle* h, bool partial = false) {
     const int np = h->at(l).n, q = l + 1 - h->level_start;
     const WLev P = view(h, l), C = view(h, l + 1);
     const int64_t par1 = (int64_t)10 * (np + 1) * (np + 1), par0 = (int64_t)10 * np * np;
-    const unsigned char* rec = partial ? wt_level_rec(h, l) : nullptr;
+    const unsigned char* rec = partial == 1 ? wt_level_rec(h, l) : partial == 2 ? wt_level_rec_final(h, l) : nullptr;
     k_prolong_l<<<nbl(par1, nz), TPBL, 0, sa>>>(P, C, nz, lpt_for(nz), rec);
     k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, sa>>>(P, C, np, nz, lpt_for(nz), rec);
     cudaEventRecord(W->ready_s[q], sa);
@@ -222,7 +224,7 @@ int wt_level_wav_finish(wt_handle* h, bool partial, bool rebuild) {
     CKW(cudaStreamWaitEvent(h->stream, W->ev[1 + k], 0));
   }
   W->zero_ok = true;  // every level pair's forward wavelets are launched
-  if (rebuild) inverse(h, partial);
+  if (rebuild) inverse(h, partial ? 1 : 0);
   CKW(cudaGetLastError());
   return WT_OK;
 }
@@ -302,6 +304,8 @@ int wt_wavelet_setup(wt_handle* h) {
     }
     CKW(W->alloc(&W->need[0], tot));
     CKW(W->alloc(&W->need[1], tot));
+    CKW(W->alloc(&W->list, tot));
+    CKW(W->alloc(&W->list_cnt, W->L.size()));
     size_t ptot = 0, mx = 0;
     W->rec_off.assign(W->L.size(), 0);
     for (int l = h->level_start; l <= h->level_end; ++l) {
@@ -312,6 +316,7 @@ int wt_wavelet_setup(wt_handle* h) {
       mx = std::max(mx, (size_t)h->at(l).NN);
     }
     CKW(W->alloc(&W->recpar, ptot));
+    W->rec_tot = ptot;
     CKW(W->alloc(&W->rscr[0], mx));
     CKW(W->alloc(&W->rscr[1], mx));
   }
@@ -698,6 +703,16 @@ int wt_level_need_build(wt_handle* h) {
   cudaStream_t s = h->stream;
   k_need_seed<<<g, TPB, 0, s>>>(S);
   for (int r = 0; r < NEED_R; ++r) k_need_dilate<<<g, TPB, 0, s>>>(S, r);
+  // with a patch tree: only the nodes of existing patches and their 2-node ring
+  const bool tree = W->tree_ps > 0;
+  auto tl = [&](int l) {
+    const DevLevel& D = h->at(l);
+    return TreeLev{D.n, D.P, (int)D.NN, D.nsrc, W->tree + W->tree_off[l - h->level_start]};
+  };
+  if (tree)
+    for (int l = h->level_start + 1; l <= h->level_end; ++l)
+      k_need_tree<<<nb(h->at(l).NN), TPB, 0, s>>>(tl(l), W->tree_ps,
+                                                  W->need[NEED_R & 1] + W->need_off[l - h->level_start]);
   // parents rebuilt by the intermediate stages' inverse transforms, finest first
   auto ml = [&](int l) {
     const DevLevel& D = h->at(l);
@@ -716,9 +731,19 @@ int wt_level_need_build(wt_handle* h) {
     k_map_up<<<nb(Lp.NN), TPB, 0, s>>>(Lc, Lp, A, B);
     k_map_dilate<<<nb(Lp.NN), TPB, 0, s>>>(Lp, B, A);
     k_map_dilate<<<nb(Lp.NN), TPB, 0, s>>>(Lp, A, rp);  // recpar(l)
+    if (tree && W->recfin)
+      k_map_tree_par<<<nb(Lp.NN), TPB, 0, s>>>(Lp, tl(c), W->tree_ps, rp, W->recfin + W->rec_off[l - h->level_start]);
+  }
+  // work lists of the levels above level_start
+  cudaMemsetAsync(W->list_cnt, 0, W->L.size() * sizeof(int), s);
+  for (int l = h->level_start + 1; l <= h->level_end; ++l) {
+    const int q = l - h->level_start;
+    k_list_build<<<nb(h->at(l).NN), TPB, 0, s>>>(ml(l), W->need[NEED_R & 1] + W->need_off[q], W->list + W->need_off[q],
+                                                 W->list_cnt + q);
   }
   CKW(cudaGetLastError());
   W->need_ok = true;
+  W->recfin_ok = tree && W->recfin;
   return WT_OK;
 }
 
@@ -729,6 +754,14 @@ const unsigned char* wt_level_rec(wt_handle* h, int level) {
   if (level >= h->level_end || !W->recpar || !W->skip_inactive || !W->need_ok) return nullptr;
   return W->recpar + W->rec_off[level - h->level_start];
 }
+// The parents of level that the inverse transform after adapt rebuilds: with a
+// patch tree those the next step reads and those of the tree's nodes (recfin),
+// else null (every parent).
+const unsigned char* wt_level_rec_final(wt_handle* h, int level) {
+  WavCtx* W = ctx(h);
+  if (level >= h->level_end || !W->recfin || !W->recfin_ok || !W->skip_inactive || !W->need_ok) return nullptr;
+  return W->recfin + W->rec_off[level - h->level_start];
+}
 
 // The map level's step1 and trend may skip by, or null (level_start, no map,
 // skipping turned off, or masks uploaded since the last build).
@@ -738,6 +771,14 @@ const unsigned char* wt_level_need(wt_handle* h, int level) {
   return W->need[NEED_R & 1] + W->need_off[level - h->level_start];  // the last dilation's output
 }
 int wt_level_skip_epoch(wt_handle* h) { return ctx(h)->skip_epoch; }
+// The work list of level (the slots of its needed-node map), or {null, null}
+// when wt_level_need gives no map.
+wtk::NodeList wt_level_list(wt_handle* h, int level) {
+  WavCtx* W = ctx(h);
+  if (!wt_level_need(h, level) || !W->list) return wtk::NodeList{nullptr, nullptr};
+  const int q = level - h->level_start;
+  return wtk::NodeList{W->list + W->need_off[q], W->list_cnt + q};
+}
 
 // Make stream st wait until the last inverse transform has completed level's state.
 int wt_level_ready_wait(wt_handle* h, int level, cudaStream_t st) {
@@ -797,7 +838,7 @@ void wt_level_clean_wavelets(wt_handle* h) {
   ctx(h)->zero_ok = true;  // every slot is 0
 }
 bool wt_level_zero_ok(wt_handle* h) { return ctx(h)->zero_ok; }
-void wt_level_inverse(wt_handle* h) { inverse(h); }
+void wt_level_inverse(wt_handle* h) { inverse(h, 2); }
 int wt_level_set_thresholds(wt_handle* h, const double* threshold) {
   CKW(cudaMemcpyAsync(ctx(h)->thr, threshold, 3 * h->nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   return WT_OK;
@@ -1031,6 +1072,7 @@ int wt_tree_init(wt_handle* h, int patch_size) {
     CKW(W->alloc(&W->treq, r));
     CKW(W->alloc(&W->tree_le, 1));
     CKW(W->alloc(&W->tree_cnt, 2));
+    if (W->recpar) CKW(W->alloc(&W->recfin, W->rec_tot));
   }
   W->tree_ps = patch_size;
   // add_second_level: every patch of level_start; none above
@@ -1041,6 +1083,7 @@ int wt_tree_init(wt_handle* h, int patch_size) {
   CKW(cudaStreamSynchronize(h->stream));
   W->tree_level_end = ls;
   ++W->skip_epoch;  // the hierarchy's step graph re-records (refine inside it or not)
+  W->need_ok = false;  // the maps are limited to the tree
   return WT_OK;
 }
 
@@ -1083,6 +1126,7 @@ int wt_grid_sync(wt_handle* h, const unsigned char* exist, int level_end) {
   CKW(cudaStreamSynchronize(h->stream));
   if (W->tree_level_end != level_end) ++W->skip_epoch;
   W->tree_level_end = level_end;
+  W->need_ok = false;
   return WT_OK;
 }
 
@@ -1155,6 +1199,18 @@ int wt_tree_stats(wt_handle* h, int level, long long* out) {
   out[0] = (long long)std::count(ex.begin(), ex.end(), (unsigned char)1);
   out[1] = (long long)std::count(fr.begin(), fr.end(), (unsigned char)1);
   out[2] = (long long)c[0];
+  // owned nodes in the level's needed-node map (-1 without a current map)
+  out[3] = -1;
+  if (const unsigned char* nd = wt_level_need(h, level)) {
+    const DevLevel& D = h->at(level);
+    std::vector<unsigned char> m(D.NN);
+    CKW(cudaMemcpy(m.data(), nd, D.NN, cudaMemcpyDeviceToHost));
+    long long k = 0;
+    for (int d = 0; d < 10; ++d)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) k += m[((int64_t)d * D.P + j + 2) * D.P + i + 2] != 0;
+    out[3] = k;
+  }
   return WT_OK;
 }
 

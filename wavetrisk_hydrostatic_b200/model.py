@@ -312,10 +312,11 @@ class WaveletHierarchy(DeviceGrid):
 
     def tree_stats(self, level: int):
         """(patches, patches made by the last refine, owned nodes outside the
-        tree with a mask that is not ZERO) of `level`."""
-        out = (C.c_longlong * 3)()
+        tree with a mask that is not ZERO, owned nodes in the needed-node map
+        or -1) of `level`."""
+        out = (C.c_longlong * 4)()
         N.check("wt_tree_stats", N.lib().wt_tree_stats(self.h, int(level), out))
-        return int(out[0]), int(out[1]), int(out[2])
+        return tuple(int(x) for x in out)
 
     def mask_adj_child(self, level: int) -> None:
         N.check("wt_mask_adj_child", N.lib().wt_mask_adj_child(self.h, int(level)))

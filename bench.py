@@ -455,20 +455,26 @@ def adaptive_launches(L):
     return 4 * stage - 4 * (L - 1) + masks + (L - 1) + 4 * (L - 1)
 
 
-def algorithmic_bytes_trend_ml(level, nz, n_on=None, n_own=None):
+def algorithmic_bytes_trend_ml(level, nz, n_on=None, n_own=None, n_listed=None):
     """Compulsory bytes of one multi-level trend launch on a level with the
-    fused RK sub-step (k_trend_ml, or k_trend_tma<MODE_ML> on the finest level,
-    which stages every input plane of a tile, so its traffic is higher).  Every node of [0, n]^2 reads its mask and writes dmass and dTheta
-    (2 words a layer); every owned node writes the velocity source (3); the
-    n_on nodes with mask_n >= TRSK also read theta, qe(3), hflux_mass(3),
-    hflux_Theta(3), Bernoulli and Phi (12 words a layer) and len(3), part(6),
-    hex_inv once; every padded node reads the RK base state and writes the stage
-    state (5 + 5 words a layer).  Without n_on every node counts as active."""
+    fused RK sub-step (k_trend_ml, k_trend_ml_list over the level's work list,
+    or k_trend_tma<MODE_ML> on the finest level, which stages every input plane
+    of a tile, so its traffic is higher).  Every node of [0, n]^2 reads its mask
+    and writes dmass and dTheta (2 words a layer); every owned node writes the
+    velocity source (3); the n_on nodes with mask_n >= TRSK also read theta,
+    qe(3), hflux_mass(3), hflux_Theta(3), Bernoulli and Phi (12 words a layer)
+    and len(3), part(6), hex_inv once; every padded node reads the RK base state
+    and writes the stage state (5 + 5 words a layer).  Without n_on every node
+    counts as active.  n_listed: the work list's owned nodes, which then stand
+    for the nodes of [0, n]^2, the owned nodes and the padded nodes alike (the
+    list's few ghost-ring slots are left out, so the figure is a lower bound)."""
     n = 2 ** level
     P = n + 4
     NN = 10 * P * P
     inner = 10 * (n + 1) ** 2
     own = 10 * n * n if n_own is None else n_own
+    if n_listed is not None:
+        inner = own = NN = n_listed
     on = inner if n_on is None else n_on
     return nz * (inner * 2 * 8 + own * 3 * 8 + on * 12 * 8 + NN * 10 * 8) + inner * 4 + on * 10 * 8
 
@@ -536,7 +542,10 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
     if profile:
         pm = (Nt.C.c_double * 7)()
         pc = (Nt.C.c_int * 7)()
+        # NVTX range "roofline_list" for ncu: the profiled step with the timed steps' maps and lists
+        torch.cuda.nvtx.range_push("roofline_list")
         Nt.check("wt_profile_rk4_multi", Nt.lib().wt_profile_rk4_multi(dev.h, DT_AD, 1, pm, pc))
+        torch.cuda.nvtx.range_pop()
         names = ["step1_top", "step1_coarse", "restrict", "trend_ml_top", "trend_ml_coarse", "rk_sub", "wt_after_step"]
         out["phase_ms"] = {names[p]: pm[p] for p in range(7)}
         out["phase_count_per_step"] = {names[p]: pc[p] for p in range(7)}
@@ -550,32 +559,35 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
         dev.skip_inactive(True)
         out["phase_ms_dense"] = {names[p]: pm[p] for p in range(7)}
     if e2e:
-        # The host keeps the finest level's prognostic state and the masks of
-        # every level (its masks of record): each step uploads that state from
-        # pinned host buffers, steps, and downloads the new state and all masks.
+        # The host keeps what the reference's host holds between steps: the
+        # finest level's prognostic state on its existing patches (packed patch
+        # by patch, wt_download_tree_state), every level's masks and the finest
+        # level's patch bytes.  Each step uploads that state from pinned host
+        # buffers, steps, and downloads the new state, the masks and the tree.
         pin = lambda shape, dt=torch.float64: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
         top = levels[-1]
-        sbuf = {"mass": pin((nz, top.NN)), "temp": pin((nz, top.NN)), "velo": pin((nz, 3 * top.NN))}
+        bufs = dev.tree_state_buffers(alloc=pin)
         mbuf = [{"mask_n": pin(g.NN, torch.int32), "mask_e": pin(3 * g.NN, torch.int32)} for g in levels]
+        tbuf = pin(10 * (top.n // model.patch_size) ** 2, torch.uint8)
         ids = dev.FIELDS
         L = Nt.lib()
-        up = [(lmax, k, sbuf[k]) for k in ("mass", "temp", "velo")]
-        dn = up + [(g.level, k, b[k]) for g, b in reversed(list(zip(levels, mbuf))) for k in ("mask_n", "mask_e")]
-
-        def batch(items):
-            n = len(items)
-            return (n, (Nt.C.c_int * n)(*[l for l, _, _ in items]), (Nt.C.c_int * n)(*[ids[k] for _, k, _ in items]),
-                    (Nt.C.c_void_p * n)(*[a.ctypes.data for _, _, a in items]))
-
-        bu, bd = batch(up), batch(dn)
+        dn = [(g.level, k, b[k]) for g, b in reversed(list(zip(levels, mbuf))) for k in ("mask_n", "mask_e")]
+        bd = (len(dn), (Nt.C.c_int * len(dn))(*[l for l, _, _ in dn]),
+              (Nt.C.c_int * len(dn))(*[ids[k] for _, k, _ in dn]), (Nt.C.c_void_p * len(dn))(*[a.ctypes.data for _, _, a in dn]))
+        state = {"n": dev.download_tree_state(bufs)}
+        h2d, d2h = [], []
+        per_patch = 5 * nz * model.patch_size ** 2 * 8
 
         def put():
-            Nt.check("wt_upload_fields", L.wt_upload_fields(dev.h, *bu))
+            dev.upload_tree_state(bufs, state["n"])
+            h2d.append(state["n"] * per_patch)
 
         def get():
+            state["n"] = dev.download_tree_state(bufs)
             Nt.check("wt_download_fields", L.wt_download_fields(dev.h, *bd))
+            Nt.check("wt_tree_download", L.wt_tree_download(dev.h, lmax, tbuf.ctypes.data, None))
+            d2h.append(state["n"] * per_patch + sum(a.nbytes for _, _, a in dn) + tbuf.nbytes)
 
-        get()
         nsteps_e2e = max(1, steps // 2)
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
@@ -586,8 +598,8 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
         t1 = time.perf_counter()
         out["e2e_s"] = t1 - t0
         out["e2e_steps"] = nsteps_e2e
-        out["h2d_bytes_per_step"] = int(sum(a.nbytes for _, _, a in up))
-        out["d2h_bytes_per_step"] = int(sum(a.nbytes for _, _, a in dn))
+        out["h2d_bytes_per_step"] = int(sum(h2d) / len(h2d))
+        out["d2h_bytes_per_step"] = int(sum(d2h) / len(d2h))
     out["cells_finest"] = 10 * 4 ** lmax + 2
     model.close()
     return out
@@ -601,7 +613,9 @@ def tree_summary(model, levels):
     nodes = 0
     for g in levels:
         ex = model.patches(g.level)
-        per.append({"level": g.level, "patches": int(ex.sum()), "of": int(ex.size)})
+        st = model.dev.tree_stats(g.level)
+        per.append({"level": g.level, "patches": int(ex.sum()), "of": int(ex.size), "needed_owned_nodes": st[3],
+                    "owned_nodes": 10 * g.n * g.n})
         nodes += int(ex.sum()) * ps * ps
     dense = sum(10 * g.n * g.n for g in levels)
     return {"level_end": model.level_end(), "patch_size": ps, "levels": per, "tree_nodes": nodes,
@@ -715,17 +729,21 @@ def bench_ours(args):
         share = {k: pm[k] * pc[k] for k in pm}
         tot = sum(share.values())
         dom = max(share, key=lambda k: share[k])
-        ab = algorithmic_bytes_trend_ml(args.level, args.nz, n_on=r["masks"][-1]["trsk_nodes_0n"])
+        # the roofline kernel: the finest level's k_trend_ml_list (its work list
+        # = the needed slots), timed in the profiled step that takes the same maps
+        listed = r["tree"]["levels"][-1]["needed_owned_nodes"]
+        ab = algorithmic_bytes_trend_ml(args.level, args.nz, n_on=r["masks"][-1]["trsk_nodes_0n"], n_listed=listed)
+        t_list = pm["trend_ml_top"]
+        ach = ab / (t_list / 1e3) / 1e9
+        ab_dense = algorithmic_bytes_trend_ml(args.level, args.nz)
         t_dense = r["phase_ms_dense"]["trend_ml_top"]
-        ach = ab / (t_dense / 1e3) / 1e9
         traffic = None
-        tf = os.path.join(ROOT, "profiles", "trend_ml_traffic.json")
+        tf = os.path.join(ROOT, "profiles", "trend_ml_list_traffic.json")
         if os.path.exists(tf):
             try:
                 tj = json.load(open(tf))
-                traffic = tj.get(f"J{args.level}_nz{args.nz}")
-                if traffic is None and tj.get("dense_ratio_J7_nz32"):   # scaled by the algorithmic bytes
-                    traffic = int(tj["dense_ratio_J7_nz32"] * ab)
+                if tj.get("traffic_per_algorithmic_byte"):   # measured on a smaller case, scaled by the bytes
+                    traffic = int(tj["traffic_per_algorithmic_byte"] * ab)
             except Exception:
                 traffic = None
         cpu = cpu_baseline(args, quick=True)
@@ -746,21 +764,24 @@ def bench_ours(args):
             "config": workload_config(args, world),
             "e2e": {"value": e2e_value, "unit": "simulated days per wall-clock hour",
                     "h2d_bytes_per_step": r["h2d_bytes_per_step"], "d2h_bytes_per_step": r["d2h_bytes_per_step"],
-                    "path": "C-ABI wt_upload_fields / wt_adaptive_step / wt_download_fields, pinned host "
-                            "buffers: the finest level's state (every layer) in, that state and every level's "
-                            "masks out, every step"},
+                    "path": "C-ABI wt_upload_tree_state / wt_adaptive_step / wt_download_tree_state + "
+                            "wt_download_fields + wt_tree_download, pinned host buffers: the finest level's state "
+                            "(every layer) on its existing patches in, that state, every level's masks and the "
+                            "finest level's patch bytes out, every step (bytes: averages over the steps)"},
             "gpu_launches": adaptive_launches(L) * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "k_trend_tma<MODE_ML> (level_end)", "achieved": ach, "peak": hbm,
-                         "unit": "GB/s", "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": ab,
-                         "kernel_ms_dense": t_dense,
-                         "kernel_ms_in_timed_steps": pm["trend_ml_top"],
-                         "timing": "CUDA events around the kernel's launches in one profiled RK4 step with every node "
-                                   "computed (the timed steps leave out tiles with no needed node, doing less than "
-                                   "the algorithmic bytes count: kernel_ms_in_timed_steps)",
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same dense launch "
-                                           "at J7 x 32, scaled to this level by the algorithmic bytes "
-                                           "(profiles/trend_ml_traffic.json)" if traffic else None,
+            "roofline": {"bound": "hbm", "kernel": "k_trend_ml_list (level_end, over its work list)", "achieved": ach,
+                         "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": ab, "listed_owned_nodes": listed,
+                         "kernel_ms": t_list,
+                         "timing": "CUDA events around the kernel's launches in one profiled RK4 step (phase by phase, "
+                                   "the same needed-node maps and work lists as the timed steps)",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel on the "
+                                           "J5..J7 x 32 workload, per algorithmic byte, scaled to this launch "
+                                           "(profiles/trend_ml_list_traffic.json)" if traffic else None,
+                         "dense_tma_kernel": {"kernel": "k_trend_tma<MODE_ML> with every node computed (maps off)",
+                                              "ms": t_dense, "algorithmic_bytes": ab_dense,
+                                              "achieved_GBps": ab_dense / (t_dense / 1e3) / 1e9,
+                                              "frac": ab_dense / (t_dense / 1e3) / 1e9 / hbm},
                          "dominant_phase_by_time": dom,
                          "phase_share": {k: v / tot for k, v in share.items()},
                          "phase_ms_per_occurrence": pm, "phase_count_per_step": pc},

@@ -395,6 +395,17 @@ int wt_count_active(wt_handle* h, const double* threshold, long long* counts);
  * out[3] owned nodes in the level's needed-node map (-1 without one).  No
  * reference counterpart (diagnostics). */
 int wt_tree_stats(wt_handle* h, int level, long long* out);
+/* level_end's state on the existing patches only, as the reference's host
+ * holds it (its patch storage, src/domain.f90): for every existing patch of
+ * level_end in lozenge-major order, its patch_size^2 owned nodes row by row,
+ * layer by layer; mass and temp [n_patches][nz][ps*ps], velo
+ * [n_patches][nz][3][ps*ps] doubles.  The download returns the patch count
+ * (WT_ERR_ARG, with *n_patches set, when it exceeds capacity); the upload
+ * needs the count of the device's current tree. */
+int wt_download_tree_state(wt_handle* h, double* mass, double* temp, double* velo, long long capacity,
+                           long long* n_patches);
+int wt_upload_tree_state(wt_handle* h, const double* mass, const double* temp, const double* velo,
+                         long long n_patches);
 /* mask_adj_child (src/mask.f90:314-466) of the parents of `level` alone, as
  * init_structures applies it to the root level (src/main.f90:514). */
 int wt_mask_adj_child(wt_handle* h, int level);

@@ -46,7 +46,9 @@ def test_tma_wait_timeout_is_reported_and_the_handle_recovers():
 
 def test_tma_wait_timeout_on_the_hierarchy_step():
     """The finest level's k_step1_tma / k_trend_tma<MODE_ML> inside the
-    hierarchy's captured RK4 graph (wt_rk4_multi) on J5..J6."""
+    hierarchy's captured RK4 graph (wt_rk4_multi) on J5..J6, with the
+    needed-node maps off: with them the levels run persistent kernels over
+    their work lists, and the TMA-staged kernels only without."""
     from wavetrisk_hydrostatic_b200.model import WaveletHierarchy
 
     lmin, lmax, nz, dt = 5, 6, 2, 300.0
@@ -55,6 +57,7 @@ def test_tma_wait_timeout_on_the_hierarchy_step():
     levels = [G.level(l) for l in range(lmin, lmax + 1)]
     states = [jet_state(g, nz, seed=5 + q, ph=ph) for q, g in enumerate(levels)]
     dev = WaveletHierarchy(levels, [s["topo"] for s in states], nz, ph)
+    dev.skip_inactive(False)
 
     def load():
         for g, s in zip(levels, states):

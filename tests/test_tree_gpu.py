@@ -125,3 +125,42 @@ def test_grid_sync_round_trip():
     with pytest.raises(WtError):
         model.dev.grid_sync(bad, levels[-1].level)
     model.close()
+
+
+def test_packed_tree_state_round_trip():
+    """wt_download_tree_state gives level_end's state on its existing patches,
+    patch by patch in lozenge-major order; wt_upload_tree_state writes packed
+    values back to exactly those nodes."""
+    ph = OceanParams()
+    nz = 3
+    G, levels, ics, model, RI = _pair(3, 5, nz, lambda g: bump_state(g, nz, seed=2, ph=ph), ph)
+    model.step(300.0)
+    g, ps = levels[-1], model.patch_size
+    bufs = model.dev.tree_state_buffers()
+    n = model.dev.download_tree_state(bufs)
+    ex = model.patches(g.level)
+    assert n == int(ex.sum()) > 0
+    full = {k: model.dev.download(g.level, k) for k in ("mass", "temp", "velo")}
+    d, pj, pi = np.nonzero(ex)
+    s = np.arange(ps * ps)
+    ii = (pi[:, None] * ps + s[None, :] % ps)
+    jj = (pj[:, None] * ps + s[None, :] // ps)
+    x = g.idx(d[:, None], ii, jj)                       # [patch][node]
+    assert np.array_equal(bufs[0][:n], full["mass"][:, x].transpose(1, 0, 2))
+    assert np.array_equal(bufs[1][:n], full["temp"][:, x].transpose(1, 0, 2))
+    v = full["velo"].reshape(nz, 3, g.NN)[:, :, x]      # [nz][3][patch][node]
+    assert np.array_equal(bufs[2][:n], v.transpose(2, 0, 1, 3))
+    # upload changed values: only the patch nodes change
+    new = tuple(b.copy() for b in bufs)
+    for b in new:
+        b[:n] += 1.0
+    model.dev.upload_tree_state(new, n)
+    after = {k: model.dev.download(g.level, k) for k in ("mass", "temp", "velo")}
+    mask = np.zeros(g.NN, dtype=bool)
+    mask[x.ravel()] = True
+    own = g.owned
+    assert np.array_equal(after["mass"][:, mask], full["mass"][:, mask] + 1.0)
+    assert np.array_equal(after["mass"][:, own & ~mask], full["mass"][:, own & ~mask])
+    with pytest.raises(WtError):
+        model.dev.upload_tree_state(new, n + 1)
+    model.close()

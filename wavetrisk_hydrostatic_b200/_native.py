@@ -172,6 +172,8 @@ _DEVICE_SIGS = {
     "wt_count_active": [_vp, _dp, C.POINTER(C.c_longlong)],
     "wt_tree_stats": [_vp, C.c_int, C.POINTER(C.c_longlong)],
     "wt_mask_adj_child": [_vp, C.c_int],
+    "wt_download_tree_state": [_vp, _dp, _dp, _dp, C.c_longlong, C.POINTER(C.c_longlong)],
+    "wt_upload_tree_state": [_vp, _dp, _dp, _dp, C.c_longlong],
     "wt_wt_after_step": [_vp],
     "wt_step1_vort": [_vp, C.c_int, _dp],
     "wt_barotropic_upload_level": [_vp, C.c_int, _dp, _dp],

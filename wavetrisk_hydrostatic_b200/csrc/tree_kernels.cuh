@@ -91,3 +91,74 @@ __global__ void k_tree_outside(WLev g, const unsigned char* __restrict__ exist, 
 }
 
 }  // namespace wtw
+
+namespace wtw {
+
+// The existing patches of one level as a list of patch indices in
+// lozenge-major order (one block: each thread counts a contiguous run of the
+// patch bytes, a block-wide scan gives its offset, then it writes its run),
+// so that the host and the device agree on the packed order.  Launch with
+// one block of TREE_SCAN threads.
+constexpr int TREE_SCAN = 1024;
+__global__ void __launch_bounds__(TREE_SCAN) k_patch_list(const unsigned char* __restrict__ exist, int npatch,
+                                                          int* __restrict__ ids, int* __restrict__ count) {
+  __shared__ int part[TREE_SCAN];
+  const int t = threadIdx.x;
+  const int run = (npatch + TREE_SCAN - 1) / TREE_SCAN;
+  const int a = min(npatch, t * run), b = min(npatch, a + run);
+  int c = 0;
+  for (int x = a; x < b; ++x) c += exist[x] != 0;
+  part[t] = c;
+  __syncthreads();
+  for (int o = 1; o < TREE_SCAN; o <<= 1) {  // inclusive Hillis-Steele scan
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int w = part[t] - c;
+  for (int x = a; x < b; ++x)
+    if (exist[x]) ids[w++] = x;
+  if (t == TREE_SCAN - 1) *count = part[t];
+}
+
+// The level's state on the listed patches, packed patch by patch: mass and
+// Theta [patch][layer][ps*ps], velocity [patch][layer][edge][ps*ps], the ps*ps
+// owned nodes of a patch row by row.  One thread per (patch, layer, node);
+// scatter = false gathers the level into the packed arrays, true scatters them
+// back.
+template <bool SCATTER>
+__global__ void k_tree_pack(int n, int P, int NN, int ps, int nz, const int* __restrict__ ids,
+                            const int* __restrict__ count, double* __restrict__ m, double* __restrict__ t,
+                            double* __restrict__ v, double* __restrict__ pm, double* __restrict__ pt,
+                            double* __restrict__ pv) {
+  const int ps2 = ps * ps;
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t tot = (int64_t)__ldg(count) * nz * ps2;
+  if (g >= tot) return;
+  const int s = (int)(g % ps2);
+  const int64_t pk = g / ps2;  // patch * nz + layer
+  const int k = (int)(pk % nz);
+  const int p = __ldg(ids + pk / nz);
+  const int np = n / ps;
+  const int d = p / (np * np), r = p - d * np * np;
+  const int i = (r % np) * ps + s % ps, j = (r / np) * ps + s / ps;
+  const int64_t x = ((int64_t)d * P + j + 2) * P + i + 2;
+  const int64_t o = (int64_t)k * NN + x;
+  if (SCATTER) {
+    m[o] = pm[g];
+    t[o] = pt[g];
+  } else {
+    pm[g] = m[o];
+    pt[g] = t[o];
+  }
+  for (int e = 0; e < 3; ++e) {
+    const int64_t ov = ((int64_t)k * 3 + e) * NN + x, gv = (pk * 3 + e) * ps2 + s;
+    if (SCATTER)
+      v[ov] = pv[gv];
+    else
+      pv[gv] = v[ov];
+  }
+}
+
+}  // namespace wtw

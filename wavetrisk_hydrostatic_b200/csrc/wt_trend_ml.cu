@@ -185,7 +185,10 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
   const int nz = h->nz;
   // With WT_after_step following (wav), a level's results above level_start are
   // read only where its needed-node map says so (need_map.cuh).
-  auto need = [&](int l) -> const unsigned char* { return (wav && dest && !grad) ? wt_level_need(h, l) : nullptr; };
+  // The phase profile (tm) takes the same maps, so that its times are those of the steps.
+  auto need = [&](int l) -> const unsigned char* {
+    return ((wav || tm) && dest && !grad) ? wt_level_need(h, l) : nullptr;
+  };
   // and then over the level's work list, the needed slots only (persistent blocks)
   auto list = [&](int l) { return need(l) ? wt_level_list(h, l) : wtk::NodeList{nullptr, nullptr}; };
   // Column + step1 of a level read only that level's state and write only its
@@ -336,8 +339,7 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm, bool last_inv
     q1.v.push_back(V.v1);
   }
   const double hs[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
-  if (!tm)
-    if (int rc = wt_level_need_refresh(h)) return rc;
+  if (int rc = wt_level_need_refresh(h)) return rc;
   for (int s = 0; s < nsteps; ++s)
     for (int stage = 0; stage < 4; ++stage) {
       const States& src = stage == 0 ? q : q1;

@@ -93,6 +93,11 @@ struct WavCtx {
   int* tree_le = nullptr;
   int tree_level_end = 0;
   unsigned long long* tree_cnt = nullptr;  // [2] counters of k_tree_count_new / k_tree_outside
+  // packed transfers of level_end's state on its patches (wt_download_tree_state):
+  // the patch list, its count and the packed arrays, allocated on first use
+  int* plist = nullptr;
+  int* pcount = nullptr;
+  double* pack = nullptr;
   template <class T>
   cudaError_t alloc(T** p, size_t count) {
     cudaError_t e = cudaMalloc(p, count * sizeof(T));

@@ -1214,6 +1214,91 @@ int wt_tree_stats(wt_handle* h, int level, long long* out) {
   return WT_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// The patch list of level_end and its count on the host; the packed arrays'
+// base pointers (mass, Theta, velocity) in the staging buffer.
+int tree_pack_prepare(wt_handle* h, long long* n, double** pm, double** pt, double** pv) {
+  WavCtx* W = ctx(h);
+  const int le = h->level_end, q = le - h->level_start, ps = W->tree_ps;
+  const DevLevel& D = h->at(le);
+  const int npatch = (int)(W->tree_off[q + 1] - W->tree_off[q]);
+  const size_t per = (size_t)h->nz * ps * ps;  // doubles of one field of one patch
+  if (!W->pack) {
+    CKW(W->alloc(&W->plist, (size_t)npatch));
+    CKW(W->alloc(&W->pcount, 1));
+    CKW(W->alloc(&W->pack, (size_t)npatch * per * 5));
+  }
+  k_patch_list<<<1, TREE_SCAN, 0, h->stream>>>(W->tree + W->tree_off[q], npatch, W->plist, W->pcount);
+  int c = 0;
+  CKW(cudaMemcpyAsync(&c, W->pcount, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CKW(cudaStreamSynchronize(h->stream));
+  *n = c;
+  *pm = W->pack;
+  *pt = W->pack + (size_t)c * per;
+  *pv = W->pack + (size_t)c * per * 2;
+  (void)D;
+  return WT_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int wt_download_tree_state(wt_handle* h, double* mass, double* temp, double* velo, long long capacity,
+                           long long* n_patches) {
+  if (int rc = ready(h)) return rc;
+  WavCtx* W = ctx(h);
+  if (!W->tree_ps) return WT_ERR_STATE;
+  if (!mass || !temp || !velo || !n_patches) return WT_ERR_ARG;
+  long long n = 0;
+  double *pm, *pt, *pv;
+  if (int rc = tree_pack_prepare(h, &n, &pm, &pt, &pv)) return rc;
+  *n_patches = n;
+  if (n > capacity) return WT_ERR_ARG;
+  const DevLevel& D = h->at(h->level_end);
+  const int ps = W->tree_ps;
+  const size_t per = (size_t)h->nz * ps * ps;
+  const int64_t tot = (int64_t)n * per;
+  if (tot > 0) {
+    k_tree_pack<false><<<nb(tot), TPB, 0, h->stream>>>(D.n, D.P, (int)D.NN, ps, h->nz, W->plist, W->pcount, h->mass,
+                                                       h->temp, h->velo, pm, pt, pv);
+    CKW(cudaMemcpyAsync(mass, pm, tot * 8, cudaMemcpyDeviceToHost, h->stream));
+    CKW(cudaMemcpyAsync(temp, pt, tot * 8, cudaMemcpyDeviceToHost, h->stream));
+    CKW(cudaMemcpyAsync(velo, pv, 3 * tot * 8, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
+int wt_upload_tree_state(wt_handle* h, const double* mass, const double* temp, const double* velo,
+                         long long n_patches) {
+  if (int rc = ready(h)) return rc;
+  WavCtx* W = ctx(h);
+  if (!W->tree_ps) return WT_ERR_STATE;
+  if (!mass || !temp || !velo) return WT_ERR_ARG;
+  long long n = 0;
+  double *pm, *pt, *pv;
+  if (int rc = tree_pack_prepare(h, &n, &pm, &pt, &pv)) return rc;
+  if (n != n_patches) return WT_ERR_ARG;  // packed for another tree
+  const DevLevel& D = h->at(h->level_end);
+  const int ps = W->tree_ps;
+  const size_t per = (size_t)h->nz * ps * ps;
+  const int64_t tot = (int64_t)n * per;
+  if (tot > 0) {
+    CKW(cudaMemcpyAsync(pm, mass, tot * 8, cudaMemcpyHostToDevice, h->stream));
+    CKW(cudaMemcpyAsync(pt, temp, tot * 8, cudaMemcpyHostToDevice, h->stream));
+    CKW(cudaMemcpyAsync(pv, velo, 3 * tot * 8, cudaMemcpyHostToDevice, h->stream));
+    k_tree_pack<true><<<nb(tot), TPB, 0, h->stream>>>(D.n, D.P, (int)D.NN, ps, h->nz, W->plist, W->pcount, h->mass,
+                                                      h->temp, h->velo, pm, pt, pv);
+  }
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  h->state_halo_done = false;
+  return WT_OK;
+}
+
 int wt_mask_adj_child(wt_handle* h, int level) {
   if (int rc = ready(h)) return rc;
   if (level < h->level_start || level >= h->level_end) return WT_ERR_ARG;

@@ -275,6 +275,31 @@ class WaveletHierarchy(DeviceGrid):
     # ---- patch tree (src/refine_patch.f90)
     def tree_init(self, patch_size: int) -> None:
         N.check("wt_tree_init", N.lib().wt_tree_init(self.h, int(patch_size)))
+        self.patch_size = int(patch_size)
+
+    def tree_state_buffers(self, alloc=np.empty):
+        """Packed arrays of level_end's state for every patch of the level
+        (mass, temp [patches][nz][ps*ps], velo [patches][nz][3][ps*ps]);
+        alloc(shape) makes each (e.g. pinned host memory)."""
+        ps, g = self.patch_size, self.levels[-1]
+        npatch = 10 * (g.n // ps) ** 2
+        return (alloc((npatch, self.nz, ps * ps)), alloc((npatch, self.nz, ps * ps)),
+                alloc((npatch, self.nz, 3, ps * ps)))
+
+    def download_tree_state(self, bufs) -> int:
+        """level_end's state on its existing patches into the packed arrays
+        bufs (tree_state_buffers); returns the patch count (the arrays' first
+        that many rows)."""
+        m, t, v = bufs
+        n = C.c_longlong(0)
+        N.check("wt_download_tree_state", N.lib().wt_download_tree_state(
+            self.h, N.dptr(m), N.dptr(t), N.dptr(v), m.shape[0], C.byref(n)))
+        return n.value
+
+    def upload_tree_state(self, bufs, n_patches: int) -> None:
+        m, t, v = bufs
+        N.check("wt_upload_tree_state", N.lib().wt_upload_tree_state(self.h, N.dptr(m), N.dptr(t), N.dptr(v),
+                                                                     int(n_patches)))
 
     def tree_level_end(self) -> int:
         le = C.c_int(0)

@@ -373,8 +373,9 @@ def workload_config(args, world=1):
     if args.mode == "adaptive":
         return {
             "workload": f"adaptive run J{args.lmin}..J{args.level} ({cells} cells at J{args.level}), {args.nz} "
-                        f"Boussinesq layers, every patch of the hierarchy present (fully refined tree; masks and "
-                        f"adapt every step), 4000 m bottom with a seeded Gaussian seamount (2000 m, 50 km), jet + "
+                        f"Boussinesq layers, partially refined patch tree (4x4-node patches) refined level by "
+                        f"level at the start as the reference's initialize does and by adapt every step, 4000 m "
+                        f"bottom with a seeded Gaussian seamount (2000 m, 50 km), jet + "
                         f"8 seeded Gaussian bumps (300 km, 0.05 m), tol {TOL_AD} thresholds, explicit RK4 "
                         f"dt={dt_adaptive(args.level):g} s, WT_after_step per stage",
             "min_level": args.lmin, "max_level": args.level, "layers": args.nz, "dt_s": dt_adaptive(args.level),
@@ -510,6 +511,7 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
     t_init = time.perf_counter() - t_init
     del states
     dev = model.dev
+    tree_init = tree_summary(model, levels)
     stream = torch.cuda.ExternalStream(dev.stream, device=device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
     for _ in range(warmup):
@@ -537,6 +539,7 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
                     "trsk_nodes_0n": int(np.count_nonzero(mn[inner] >= 2))})
     out["masks"] = act
     out["tree"] = tree_summary(model, levels)
+    out["tree_init"] = tree_init
     out["tree"]["init_s"] = round(t_init, 2)
     out["tree"]["init_log"] = [list(x) for x in model.init_log]
     if profile:
@@ -746,7 +749,7 @@ def bench_ours(args):
                     traffic = int(tj["traffic_per_algorithmic_byte"] * ab)
             except Exception:
                 traffic = None
-        cpu = cpu_baseline(args, quick=True)
+        cpu = cpu_baseline(args, quick=True, tree_fraction=r["tree_init"]["tree_fraction"])
         L = args.level - args.lmin + 1
         line = {
             "metric": "sim-days/hour",
@@ -787,6 +790,7 @@ def bench_ours(args):
                          "phase_ms_per_occurrence": pm, "phase_count_per_step": pc},
             "masks_after_run": r["masks"],
             "patch_tree": r["tree"],
+            "patch_tree_initial": r["tree_init"],
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
@@ -857,7 +861,7 @@ def bench_ours_uniform(args):
                 traffic = json.load(open(tf)).get(f"J{args.level}_nz{args.nz}")
             except Exception:
                 traffic = None
-        cpu = cpu_baseline(args, quick=True)
+        cpu = cpu_baseline(args, quick=True, tree_fraction=r["tree_init"]["tree_fraction"])
         line = {
             "metric": "sim-days/hour",
             "value": value,
@@ -890,10 +894,10 @@ def bench_ours_uniform(args):
 
 
 # ----------------------------------------------------------- reference ----
-def cpu_baseline(args, quick=False):
+def cpu_baseline(args, quick=False, tree_fraction=None):
     """Times the CPU restatement (oracle) on a bounded sample of the workload."""
     if args.mode == "adaptive":
-        return cpu_baseline_adaptive(args, quick)
+        return cpu_baseline_adaptive(args, quick, tree_fraction)
     import numpy as np
 
     import oracle
@@ -937,7 +941,7 @@ class AdaptiveCpuSampler:
     node-layer and step for J5..J6, J5..J7 and J5..J8 with 32 layers.
     Geometry comes from the oracle's own grid builder."""
 
-    def __init__(self, lmin, lmax, nz, seed=1):
+    def __init__(self, lmin, lmax, nz, seed=1, tree_fraction=None):
         import oracle
         from oracle.grid import Grid as OGrid
         from wavetrisk_hydrostatic_b200.cases import OceanParams
@@ -949,7 +953,11 @@ class AdaptiveCpuSampler:
         self.ph = OceanParams()
         self.lmin, self.lmax, self.nz, self.seed = lmin, lmax, nz, seed
         self.ls = max(lmin + 1, lmax - 2)
-        self.scale = hierarchy_nodes(lmin, lmax) / hierarchy_nodes(lmin, self.ls)
+        # the reference computes the nodes of its existing patches only: the
+        # workload's initial patch tree holds this fraction of the hierarchy's nodes
+        self.tree_fraction = oracle_tree_fraction(lmin, lmax, nz, seed) if tree_fraction is None else tree_fraction
+        self.dense_scale = hierarchy_nodes(lmin, lmax) / hierarchy_nodes(lmin, self.ls)
+        self.scale = self.dense_scale * self.tree_fraction
         G = OGrid(lmin, self.ls, radius=6371e3)
         self.levels = [G.level(l) for l in range(lmin, self.ls + 1)]
         self._setup()
@@ -991,9 +999,35 @@ class AdaptiveCpuSampler:
 
     def describe(self, n, secs):
         return (f"{n} samples, each one whole adaptive step with all {self.nz} layers on the hierarchy "
-                f"J{self.lmin}..J{self.ls} ({secs:.1f} s of CPU time in all), scaled by the node count "
-                f"x{self.scale:.2f} to J{self.lmin}..J{self.lmax}; CPU restatement (oracle), multi-level trend "
-                f"over the 10 lozenges and wavelets over layers on {self.threads} threads, mask sequence on one")
+                f"J{self.lmin}..J{self.ls} ({secs:.1f} s of CPU time in all; the oracle computes every node), "
+                f"scaled by the node count x{self.dense_scale:.2f} to J{self.lmin}..J{self.lmax} and by the "
+                f"fraction of those nodes in the existing patches of the workload's initial patch tree "
+                f"({self.tree_fraction:.4f}), which is what the reference computes; CPU restatement (oracle), "
+                f"multi-level trend over the 10 lozenges and wavelets over layers on {self.threads} threads, "
+                f"mask sequence on one")
+
+
+def oracle_tree_fraction(lmin, lmax, nz, seed):
+    """The fraction of the hierarchy's owned nodes that lie in existing
+    patches after the reference's initial refinement of the workload, from the
+    oracle's restatement (oracle/tree.py); the GPU's tree is bit-identical to
+    it (tests/test_tree_gpu.py)."""
+    import numpy as np
+
+    from oracle.grid import Grid as OGrid
+    from oracle.tree import ReferenceInit
+    from wavetrisk_hydrostatic_b200.adaptive import patch_size_for
+    from wavetrisk_hydrostatic_b200.cases import OceanParams
+
+    ph = OceanParams()
+    G = OGrid(lmin, lmax, radius=6371e3)
+    levels = [G.level(l) for l in range(lmin - 1, lmax + 1)]
+    ics = {g.level: st for g, st in zip(levels, adaptive_states(levels, nz, seed, ph))}
+    thr = TOL_AD * np.stack([ph.ref_density * np.full(nz, ph.depth / nz), np.full(nz, 1e16), np.full(nz, 1.0)])
+    ps = patch_size_for(lmin)
+    RI = ReferenceInit(levels[0], levels[1:], nz, ics, thr, lmax, ps=ps).run()
+    nodes = sum(int(e.sum()) * ps * ps for e in RI.tree.exist.values())
+    return nodes / sum(10 * 4 ** l for l in range(lmin, lmax + 1))
 
 
 def cpu_model():
@@ -1008,10 +1042,10 @@ def cpu_model():
     return None
 
 
-def cpu_baseline_adaptive(args, quick=False):
+def cpu_baseline_adaptive(args, quick=False, tree_fraction=None):
     """The oracle's adaptive step on the same workload: one warm-up sample,
     then samples until the time budget is used (at least two)."""
-    S = AdaptiveCpuSampler(args.lmin, args.level, args.nz)
+    S = AdaptiveCpuSampler(args.lmin, args.level, args.nz, tree_fraction=tree_fraction)
     S.sample()
     budget = args.cpu_seconds if not quick else min(args.cpu_seconds, 10.0)
     n, used, est = 0, 0.0, 0.0
@@ -1020,6 +1054,8 @@ def cpu_baseline_adaptive(args, quick=False):
         n, used, est = n + 1, used + t, est + tf
     return {"value": sim_days_per_hour(n, est, dt_adaptive(args.level)), "unit": "simulated days per wall-clock hour",
             "cores": S.threads, "kind": "port", "sample": S.describe(n, used), "seconds_per_step": est / n,
+            "tree_fraction": S.tree_fraction,
+            "dense_value": sim_days_per_hour(n, est / S.tree_fraction, dt_adaptive(args.level)),
             "cpu_model": cpu_model(), "host_threads": os.cpu_count()}
 
 
@@ -1044,8 +1080,9 @@ def bench_reference(args):
             used, est = used + t, est + tf
         value = sim_days_per_hour(steps, est, dt_adaptive(args.level))
         cb = {"value": value, "unit": "simulated days per wall-clock hour", "cores": S.threads, "kind": "port",
-              "sample": S.describe(steps, used), "seconds_per_step": est / steps, "cpu_model": cpu_model(),
-              "host_threads": os.cpu_count()}
+              "sample": S.describe(steps, used), "seconds_per_step": est / steps, "tree_fraction": S.tree_fraction,
+              "dense_value": sim_days_per_hour(steps, est / S.tree_fraction, dt_adaptive(args.level)),
+              "cpu_model": cpu_model(), "host_threads": os.cpu_count()}
         data = "synthetic (seeded seamount, jet and Gaussian bumps)"
     else:
         cb = cpu_baseline(args)

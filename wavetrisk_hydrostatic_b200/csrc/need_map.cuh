@@ -250,3 +250,31 @@ __global__ void k_list_build(MapLev L, const unsigned char* __restrict__ need, i
 }
 
 }  // namespace wtw
+
+namespace wtw {
+
+// A parent level's work list: every padded parent slot of [0, np]^2 whose
+// source the map says is rebuilt (rec[nsrc[x]]), appended by warp-aggregated
+// atomics (order free).  *count must be 0 on entry.
+__global__ void k_parent_list_build(MapLev Lp, const unsigned char* __restrict__ rec, int* __restrict__ ids,
+                                    int* __restrict__ count) {
+  const int m = Lp.n + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool on = false;
+  int x = 0;
+  if (t < 10 * m * m) {
+    const int d = t / (m * m), r = t - d * m * m;
+    const int jp = r / m, ip = r - jp * m;
+    x = (d * Lp.P + jp + 2) * Lp.P + ip + 2;
+    on = rec[__ldg(Lp.nsrc + x)] != 0;
+  }
+  const unsigned msk = __ballot_sync(0xffffffffu, on);
+  if (!msk) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(msk) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(msk));
+  base = __shfl_sync(msk, base, leader);
+  if (on) ids[base + __popc(msk & ((1u << lane) - 1))] = x;
+}
+
+}  // namespace wtw

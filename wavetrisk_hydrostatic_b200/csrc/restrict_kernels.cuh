@@ -337,39 +337,15 @@ __device__ __forceinline__ double sm_eval_s(const int (*si)[32], const double (*
 // fc0/fc1 and dscalar dc0/dc1) on the restricted parent edges (mask_e >=
 // RESTRCT).  Block (32, ny): 32 consecutive parent edges of the plan, ny
 // threads per edge taking layers y, y + ny, ...; blocks without a restricted
-// edge return before staging.  Same expression trees and operand order as
+// edge return before staging.  With a work list (PL), persistent blocks take
+// 32 of the listed parents' edges at a time.  Same expression trees and operand order as
 // part_coarse_flux + coarse_flux + interp_flux of the reference.
-__global__ void __launch_bounds__(256) k_restr_flux3(WLev P, int m, int nz, const int* __restrict__ pi,
-                                                     const double* __restrict__ pd, double* __restrict__ fp0,
-                                                     double* __restrict__ fp1, const double* __restrict__ fc0,
-                                                     const double* __restrict__ fc1, const double* __restrict__ dc0,
-                                                     const double* __restrict__ dc1, int NNc) {
-  __shared__ int si[RF_NI][32];
-  __shared__ double sd[RF_ND][32];
-  const int64_t ne = (int64_t)3 * 10 * m * m;
-  const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
-  const int64_t u0 = (int64_t)blockIdx.x * 32;
-  const int64_t u = u0 + x;
-  int ip = 0, jp = 0, d = 0, e = 0;
-  bool on = false;
-  if (u < ne) {
-    ip = (int)(u % m);
-    jp = (int)((u / m) % m);
-    d = (int)((u / ((int64_t)m * m)) % 10);
-    e = (int)(u / ((int64_t)10 * m * m));
-    on = P.mask_e[e * P.NN + nid(P, d, ip, jp)] >= M_RESTRCT;
-  }
-  if (!__syncthreads_or(on)) return;
-  const int nv = (int)min((int64_t)32, ne - u0);
-  for (int q = y; q < RF_NI + RF_ND; q += ny)
-    if (x < nv) {
-      if (q < RF_NI)
-        si[q][x] = pi[q * ne + u];
-      else
-        sd[q - RF_NI][x] = pd[(q - RF_NI) * ne + u];
-    }
-  __syncthreads();
-  if (!on) return;
+__device__ __forceinline__ void restr_flux_one(const WLev& P, int nz, const int (*si)[32], const double (*sd)[32],
+                                               int x, int d, int ip, int jp, int e, double* __restrict__ fp0,
+                                               double* __restrict__ fp1, const double* __restrict__ fc0,
+                                               const double* __restrict__ fc1, const double* __restrict__ dc0,
+                                               const double* __restrict__ dc1, int NNc) {
+  const int y = threadIdx.y, ny = blockDim.y;
   const bool pa = (e & 1) != 0, pb = ((e + 1) & 1) != 0;
   const int64_t so = (int64_t)e * P.NN + nid(P, d, ip, jp);
   const double ar0 = sd[12][x], ar1 = sd[13][x], o0 = sd[14][x], o1 = sd[15][x], o2 = sd[16][x], o3 = sd[17][x];
@@ -400,9 +376,80 @@ __global__ void __launch_bounds__(256) k_restr_flux3(WLev P, int m, int nz, cons
   }
 }
 
-// scalar_cpt_restr over parents [0, n]^2, every layer.
-__global__ void k_restr_scalar(WLev P, WLev C, int nz) {
+__global__ void __launch_bounds__(256) k_restr_flux3(WLev P, int m, int nz, const int* __restrict__ pi,
+                                                     const double* __restrict__ pd, double* __restrict__ fp0,
+                                                     double* __restrict__ fp1, const double* __restrict__ fc0,
+                                                     const double* __restrict__ fc1, const double* __restrict__ dc0,
+                                                     const double* __restrict__ dc1, int NNc, ParentList PL) {
+  __shared__ int si[RF_NI][32];
+  __shared__ double sd[RF_ND][32];
+  const int64_t ne = (int64_t)3 * 10 * m * m;
+  const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
+  if (PL.ids) {
+    const int cnt = __ldg(PL.count);
+    for (int c = blockIdx.x; c < (3 * cnt + 31) / 32; c += gridDim.x) {
+      const int it = c * 32 + x, e = it % 3;
+      int d = 0, ip = 0, jp = 0;
+      bool on = it < 3 * cnt && list_parent(P.n, __ldg(PL.ids + it / 3), m, d, ip, jp) &&
+                P.mask_e[e * P.NN + nid(P, d, ip, jp)] >= M_RESTRCT;
+      if (__syncthreads_or(on)) {
+        const int64_t u = (((int64_t)e * 10 + d) * m + jp) * m + ip;
+        if (on)
+          for (int q = y; q < RF_NI + RF_ND; q += ny) {
+            if (q < RF_NI)
+              si[q][x] = pi[q * ne + u];
+            else
+              sd[q - RF_NI][x] = pd[(q - RF_NI) * ne + u];
+          }
+        __syncthreads();
+        if (on) restr_flux_one(P, nz, si, sd, x, d, ip, jp, e, fp0, fp1, fc0, fc1, dc0, dc1, NNc);
+      }
+      __syncthreads();
+    }
+    return;
+  }
+  const int64_t u0 = (int64_t)blockIdx.x * 32;
+  const int64_t u = u0 + x;
+  int ip = 0, jp = 0, d = 0, e = 0;
+  bool on = false;
+  if (u < ne) {
+    ip = (int)(u % m);
+    jp = (int)((u / m) % m);
+    d = (int)((u / ((int64_t)m * m)) % 10);
+    e = (int)(u / ((int64_t)10 * m * m));
+    on = P.mask_e[e * P.NN + nid(P, d, ip, jp)] >= M_RESTRCT;
+  }
+  if (!__syncthreads_or(on)) return;
+  const int nv = (int)min((int64_t)32, ne - u0);
+  for (int q = y; q < RF_NI + RF_ND; q += ny)
+    if (x < nv) {
+      if (q < RF_NI)
+        si[q][x] = pi[q * ne + u];
+      else
+        sd[q - RF_NI][x] = pd[(q - RF_NI) * ne + u];
+    }
+  __syncthreads();
+  if (!on) return;
+  restr_flux_one(P, nz, si, sd, x, d, ip, jp, e, fp0, fp1, fc0, fc1, dc0, dc1, NNc);
+}
+
+// scalar_cpt_restr over parents [0, n]^2, every layer (with a work list, its
+// parents only, persistent threads).
+__global__ void k_restr_scalar(WLev P, WLev C, int nz, ParentList PL) {
   const int m = P.n + 1;
+  if (PL.ids) {
+    const int cnt = __ldg(PL.count);
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)cnt * nz;
+         t += (int64_t)gridDim.x * blockDim.x) {
+      const int k = (int)(t / cnt), e = (int)(t - (int64_t)k * cnt);
+      int d, ip, jp;
+      if (!list_parent(P.n, __ldg(PL.ids + e), m, d, ip, jp)) continue;
+      const int idp = nid(P, d, ip, jp);
+      if (P.mask_n[idp] >= M_RESTRCT)
+        P.scal[(int64_t)k * P.NN + idp] = C.scal[(int64_t)k * C.NN + nid(C, d, 2 * ip, 2 * jp)];
+    }
+    return;
+  }
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)nz * 10 * m * m) return;
   const int ip = (int)(t % m), jp = (int)((t / m) % m), d = (int)((t / ((int64_t)m * m)) % 10);

@@ -20,6 +20,48 @@ enum { RT = 0, DG = 1, UP = 2 };
 enum { LORT = 0, UPLT = 1 };
 constexpr int FROZEN = 32, TOLRNZ = 16, ADJZONE = 8, ZERO = 0;
 
+// A parent level's work list with a patch tree: the padded parent slots of
+// [0, n]^2 that an interscale kernel may have work at (those the inverse after
+// adapt rebuilds: the next step's parents and those of the tree's nodes, which
+// hold every child slot a mask reaches), their count on the device; built with
+// the needed-node maps (need_map.cuh: k_parent_list_build).  ids null: none.
+struct ParentList {
+  const int* ids;
+  const int* count;
+};
+
+// Persistent loop over a parent list for the kernels with one thread per
+// (parent, group of lpt layers): items group-major as parent_of's, strided by
+// the grid; f(d, ip, jp, k0, k1) for the listed parents of [0, m)^2 (m = n or
+// n + 1 of the parent level, whose padded side is np + 4).
+template <class F>
+__device__ __forceinline__ void for_parents(int np, int m, int nz, int lpt, const ParentList& PL, F f) {
+  const int cnt = __ldg(PL.count);
+  const int ng = (nz + lpt - 1) / lpt;
+  const int P = np + 4, PP = P * P;
+  const int64_t tot = (int64_t)cnt * ng;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int g = (int)(t / cnt), e = (int)(t - (int64_t)g * cnt);
+    const int x = __ldg(PL.ids + e);
+    const int d = x / PP, r = x - d * PP;
+    const int ip = r % P - 2, jp = r / P - 2;
+    if (ip < 0 || jp < 0 || ip >= m || jp >= m) continue;
+    const int k0 = g * lpt;
+    f(d, ip, jp, k0, min(nz, k0 + lpt));
+  }
+}
+
+// The parent (d, ip, jp) of work-list entry x (a padded slot of a parent
+// level of side np), or false outside [0, m)^2.
+__device__ __forceinline__ bool list_parent(int np, int x, int m, int& d, int& ip, int& jp) {
+  const int P = np + 4, PP = P * P;
+  d = x / PP;
+  const int r = x - d * PP;
+  ip = r % P - 2;
+  jp = r / P - 2;
+  return ip >= 0 && jp >= 0 && ip < m && jp < m;
+}
+
 // One level of the hierarchy on the device.
 struct WLev {
   int n, P, NN;
@@ -331,7 +373,24 @@ __global__ void k_mask_halo_all(MaskHaloSet S) {
 // scalars and three edges (read through the ghost remaps), and the flags are
 // OR-ed in shared memory before the y = 0 thread updates the masks.
 // thr[v*nz + k]: v = 0 mass, 1 Theta, 2 velocity.
-__global__ void k_mask_tol_y(WLev L, int nz, int st, int en, const double* __restrict__ thr, int below_fill) {
+// Whether padded slot y (its own source) lies in an existing patch of the
+// level (exist: [10][n/ps][n/ps] patch bytes); the pole slots count as in.
+__device__ __forceinline__ bool slot_in_tree(const WLev& L, const unsigned char* __restrict__ exist, int ps, int y) {
+  const int PP = L.P * L.P;
+  const int d = y / PP, r = y - d * PP;
+  const int i = r % L.P - 2, j = r / L.P - 2;
+  if (i < 0 || j < 0 || i >= L.n || j >= L.n) return true;
+  const int np = L.n / ps;
+  return exist[((int64_t)d * np + j / ps) * np + i / ps] != 0;
+}
+
+// With a patch tree (exist non-null), a node whose own wavelets and whose
+// edges' wavelets all belong to nodes outside the tree is left out: the
+// compression that produced the wavelets kept none there (masks never reach
+// outside the tree), and init_masks_zero left its masks ZERO, which a pass
+// with zero wavelets keeps.
+__global__ void k_mask_tol_y(WLev L, int nz, int st, int en, const double* __restrict__ thr, int below_fill,
+                             const unsigned char* __restrict__ exist, int ps) {
   __shared__ int fl[8][32];  // ny <= 8
   const int m = L.n + en - st;
   const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
@@ -356,7 +415,13 @@ __global__ void k_mask_tol_y(WLev L, int nz, int st, int en, const double* __res
     int ce[3];
 #pragma unroll
     for (int e = 0; e < 3; ++e) ce[e] = __ldg(L.esrc + e * L.NN + x_);
-    for (int k = y; k < nz; k += ny) {
+    bool read = true;
+    if (exist && !below_fill) {
+      read = slot_in_tree(L, exist, ps, cn);
+#pragma unroll
+      for (int e = 0; e < 3; ++e) read = read || slot_in_tree(L, exist, ps, (ce[e] >> 1) % L.NN);
+    }
+    for (int k = y; k < nz && read; k += ny) {
       const double wm = L.wm[(int64_t)k * L.NN + cn], wt = L.wt[(int64_t)k * L.NN + cn];
       if (fabs(wm) >= thr[0 * nz + k] || below_fill) f |= 1;
       if (fabs(wt) >= thr[1 * nz + k] || below_fill) f |= 1;

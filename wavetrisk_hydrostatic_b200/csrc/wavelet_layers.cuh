@@ -98,111 +98,131 @@ __device__ __forceinline__ void child_interps(NodeInterp N[3], const WLev& C, in
 // current masks), so only the kept slots are written.  CMP 0: the forward
 // transform (wavelets zeroed beforehand, no compression).
 template <int CMP>
-__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int np, int nz, int lpt) {
-  int d, ip, jp;
-  int k0, k1;
-  if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  const int ci[3] = {i + 1, i + 1, i}, cj[3] = {j, j + 1, j + 1};
-  bool on[3];
-  int self[3], at[3];
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    on[q] = mn(C, d, ci[q], cj[q]) >= ADJZONE;
-    self[q] = wn_code(C, d, ci[q], cj[q]);
-    at[q] = nid(C, d, ci[q], cj[q]);
-  }
-  if (!(on[0] || on[1] || on[2])) {
-    if (CMP == 1)
-      for (int k = k0; k < k1; ++k)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          C.wm[(int64_t)k * C.NN + at[q]] = 0.0;
-          C.wt[(int64_t)k * C.NN + at[q]] = 0.0;
-        }
+__global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_scalar_wc_l(WLev C, int np, int nz, int lpt, ParentList PL) {
+  auto body = [&](int d, int ip, int jp, int k0, int k1) {
+    const int i = 2 * ip, j = 2 * jp;
+    const int ci[3] = {i + 1, i + 1, i}, cj[3] = {j, j + 1, j + 1};
+    bool on[3];
+    int self[3], at[3];
+  #pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      on[q] = mn(C, d, ci[q], cj[q]) >= ADJZONE;
+      self[q] = wn_code(C, d, ci[q], cj[q]);
+      at[q] = nid(C, d, ci[q], cj[q]);
+    }
+    if (!(on[0] || on[1] || on[2])) {
+      if (CMP == 1)
+        for (int k = k0; k < k1; ++k)
+  #pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            C.wm[(int64_t)k * C.NN + at[q]] = 0.0;
+            C.wt[(int64_t)k * C.NN + at[q]] = 0.0;
+          }
+      return;
+    }
+    NodeInterp N[3];
+    child_interps(N, C, d, i, j);
+    for (int k = k0; k < k1; ++k)
+  #pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+        double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+  #pragma unroll
+        for (int q = 0; q < 3; ++q)
+          if (on[q])
+            wc[at[q]] = wn(s, self[q]) - node_eval(N[q], s);
+          else if (CMP == 1)
+            wc[at[q]] = 0.0;
+      }
+  };
+  if (PL.ids) {
+    for_parents(np, np, nz, lpt, PL, body);
     return;
   }
-  NodeInterp N[3];
-  child_interps(N, C, d, i, j);
-  for (int k = k0; k < k1; ++k)
-#pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
-      double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
-#pragma unroll
-      for (int q = 0; q < 3; ++q)
-        if (on[q])
-          wc[at[q]] = wn(s, self[q]) - node_eval(N[q], s);
-        else if (CMP == 1)
-          wc[at[q]] = 0.0;
-    }
+  int d, ip, jp, k0, k1;
+  if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
+  body(d, ip, jp, k0, k1);
 }
 
 // Reconstruct_scalar (src/wavelet.f90:614-640), parents [0, np)^2.
 __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_recon_scalar_l(WLev Pa, WLev C, int np, int nz, int lpt,
-                                                                         const unsigned char* __restrict__ rec) {
-  int d, ip, jp;
-  int k0, k1;
-  if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
-  if (!rebuilt(rec, Pa, d, ip, jp)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  const int ci[3] = {i + 1, i + 1, i}, cj[3] = {j, j + 1, j + 1};
-  int self[3], at[3];
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    self[q] = wn_code(C, d, ci[q], cj[q]);
-    at[q] = nid(C, d, ci[q], cj[q]);
-  }
-  NodeInterp N[3];
-  child_interps(N, C, d, i, j);
-  for (int k = k0; k < k1; ++k)
-#pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
-      double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
-      double r[3];
-#pragma unroll
-      for (int q = 0; q < 3; ++q) r[q] = node_eval(N[q], s) + wn(wc, self[q]);
-#pragma unroll
-      for (int q = 0; q < 3; ++q) s[at[q]] = r[q];
+                                                                         const unsigned char* __restrict__ rec,
+                                                                         ParentList PL) {
+  auto body = [&](int d, int ip, int jp, int k0, int k1) {
+    if (!rebuilt(rec, Pa, d, ip, jp)) return;
+    const int i = 2 * ip, j = 2 * jp;
+    const int ci[3] = {i + 1, i + 1, i}, cj[3] = {j, j + 1, j + 1};
+    int self[3], at[3];
+  #pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      self[q] = wn_code(C, d, ci[q], cj[q]);
+      at[q] = nid(C, d, ci[q], cj[q]);
     }
+    NodeInterp N[3];
+    child_interps(N, C, d, i, j);
+    for (int k = k0; k < k1; ++k)
+  #pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+        double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+        double r[3];
+  #pragma unroll
+        for (int q = 0; q < 3; ++q) r[q] = node_eval(N[q], s) + wn(wc, self[q]);
+  #pragma unroll
+        for (int q = 0; q < 3; ++q) s[at[q]] = r[q];
+      }
+  };
+  if (PL.ids) {
+    for_parents(np, np, nz, lpt, PL, body);
+    return;
+  }
+  int d, ip, jp, k0, k1;
+  if (!parent_of(np, nz, lpt, d, ip, jp, k0, k1)) return;
+  body(d, ip, jp, k0, k1);
 }
 
 // Prolong_scalar (src/wavelet.f90:571-612), parents [0, np]^2: the eleven
 // lifting terms the reference sums.
 __global__ void __launch_bounds__(128, WL_MINB_SCALAR) k_prolong_l(WLev Pa, WLev C, int nz, int lpt,
-                                                                    const unsigned char* __restrict__ rec) {
+                                                                    const unsigned char* __restrict__ rec,
+                                                                    ParentList PL) {
   const int np = Pa.n;
-  int d, ip, jp;
-  int k0, k1;
-  if (!parent_of(np + 1, nz, lpt, d, ip, jp, k0, k1)) return;
-  if (!rebuilt(rec, Pa, d, ip, jp)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  if (mn(C, d, i, j) == FROZEN) return;
-  const int ti[11] = {i + 1, i + 1, i + 2, i, i - 1, i - 1, i - 2, i - 1, i, i - 1, i + 1};
-  const int tj[11] = {j, j + 1, j + 1, j + 1, j, j + 1, j - 1, j - 1, j - 1, j - 2, j - 1};
-  const int tk[11] = {1, 2, 3, 1, 2, 3, 4, 1, 2, 3, 4};
-  double w[11];
-  int c[11];
-#pragma unroll
-  for (int q = 0; q < 11; ++q) {
-    w[q] = oa(C, d, ti[q], tj[q], tk[q]);
-    c[q] = wn_code(C, d, ti[q], tj[q]);
-  }
-  const double hp = hv(Pa, d, ip, jp);
-  const int cp = wn_code(Pa, d, ip, jp);
-  const int at = nid(C, d, i, j);
-  for (int k = k0; k < k1; ++k)
-#pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
-      const double* sp = (v == 0 ? Pa.sm : Pa.st) + (int64_t)k * Pa.NN;
-      double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
-      double sum = wn(wc, c[0]) * w[0];
-#pragma unroll
-      for (int q = 1; q < 11; ++q) sum = sum + wn(wc, c[q]) * w[q];
-      s[at] = wn(sp, cp) - sum * hp;
+  auto body = [&](int d, int ip, int jp, int k0, int k1) {
+    if (!rebuilt(rec, Pa, d, ip, jp)) return;
+    const int i = 2 * ip, j = 2 * jp;
+    if (mn(C, d, i, j) == FROZEN) return;
+    const int ti[11] = {i + 1, i + 1, i + 2, i, i - 1, i - 1, i - 2, i - 1, i, i - 1, i + 1};
+    const int tj[11] = {j, j + 1, j + 1, j + 1, j, j + 1, j - 1, j - 1, j - 1, j - 2, j - 1};
+    const int tk[11] = {1, 2, 3, 1, 2, 3, 4, 1, 2, 3, 4};
+    double w[11];
+    int c[11];
+  #pragma unroll
+    for (int q = 0; q < 11; ++q) {
+      w[q] = oa(C, d, ti[q], tj[q], tk[q]);
+      c[q] = wn_code(C, d, ti[q], tj[q]);
     }
+    const double hp = hv(Pa, d, ip, jp);
+    const int cp = wn_code(Pa, d, ip, jp);
+    const int at = nid(C, d, i, j);
+    for (int k = k0; k < k1; ++k)
+  #pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const double* wc = (v == 0 ? C.wm : C.wt) + (int64_t)k * C.NN;
+        const double* sp = (v == 0 ? Pa.sm : Pa.st) + (int64_t)k * Pa.NN;
+        double* s = (v == 0 ? C.sm : C.st) + (int64_t)k * C.NN;
+        double sum = wn(wc, c[0]) * w[0];
+  #pragma unroll
+        for (int q = 1; q < 11; ++q) sum = sum + wn(wc, c[q]) * w[q];
+        s[at] = wn(sp, cp) - sum * hp;
+      }
+  };
+  if (PL.ids) {
+    for_parents(np, np + 1, nz, lpt, PL, body);
+    return;
+  }
+  int d, ip, jp, k0, k1;
+  if (!parent_of(np + 1, nz, lpt, d, ip, jp, k0, k1)) return;
+  body(d, ip, jp, k0, k1);
 }
 
 // Interp_outer_velo (src/wavelet.f90:1064-1094) of the outer child edge e of
@@ -262,54 +282,60 @@ __device__ __forceinline__ double outer_eval(const OuterInterp& O, const double*
 // (0 where the slot's own mask is below ADJZONE) is applied to them, after the
 // pentagon corrections in the corner parents.
 template <int CMP>
-__global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa, WLev C, int nz, int lpt) {
-  int d, ip, jp;
-  int k0, k1;
+__global__ void __launch_bounds__(128, WL_MINB_OUTER) k_velo_wc_outer_l(WLev Pa, WLev C, int nz, int lpt, ParentList PL) {
+  auto body = [&](int d, int ip, int jp, int k0, int k1) {
+    const int i = 2 * ip, j = 2 * jp;
+    const bool corner = (ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1);
+    for (int e = 0; e < 3; ++e) {
+      const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
+      const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
+      const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
+      if (me(C, e, d, a2, b2) < ADJZONE) {
+        if (CMP == 1)
+          for (int k = k0; k < k1; ++k) {
+            C.wv[(int64_t)k * 3 * C.NN + x2] = 0.0;
+            C.wv[(int64_t)k * 3 * C.NN + x1] = 0.0;
+          }
+        else if (CMP == 2 && me(C, e, d, a1, b1) >= ADJZONE)  // a kept slot that the pair leaves at 0
+          for (int k = k0; k < k1; ++k) C.wv[(int64_t)k * 3 * C.NN + x1] = 0.0;
+        continue;
+      }
+      const bool keep1 = CMP == 0 || corner || me(C, e, d, a1, b1) >= ADJZONE;
+      OuterInterp O;
+      outer_interp(O, Pa, C, d, ip, jp, a2, b2, e);
+      const int cv = we_code(C, e, d, a2, b2);
+      for (int k = k0; k < k1; ++k) {
+        const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+        const double* v = C.sv + (int64_t)k * 3 * C.NN;
+        double* wc = C.wv + (int64_t)k * 3 * C.NN;
+        double t0;
+        const double u = outer_eval(O, vp, t0);
+        const double w = we(v, cv) - u;
+        wc[x2] = w;
+        wc[x1] = keep1 ? -w : 0.0;
+      }
+    }
+    if (corner) {
+      for (int k = k0; k < k1; ++k)
+        penta_compute(Pa, C, Pa.sv + (int64_t)k * 3 * Pa.NN, C.wv + (int64_t)k * 3 * C.NN, d, ip, jp);
+      if (CMP)
+        for (int e = 0; e < 3; ++e)
+  #pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int a = i + c_end_pt[e][h][0], b = j + c_end_pt[e][h][1];
+            if (me(C, e, d, a, b) >= ADJZONE) continue;
+            const int x = e * C.NN + nid(C, d, a, b);
+            for (int k = k0; k < k1; ++k) C.wv[(int64_t)k * 3 * C.NN + x] = 0.0;
+          }
+    }
+  };
+  if (PL.ids) {
+    for_parents(Pa.n, Pa.n, nz, lpt, PL, body);
+    return;
+  }
+  int d, ip, jp, k0, k1;
   if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  const bool corner = (ip == 0 || ip == Pa.n - 1) && (jp == 0 || jp == Pa.n - 1);
-  for (int e = 0; e < 3; ++e) {
-    const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
-    const int a2 = i + c_end_pt[e][1][0], b2 = j + c_end_pt[e][1][1];
-    const int x2 = e * C.NN + nid(C, d, a2, b2), x1 = e * C.NN + nid(C, d, a1, b1);
-    if (me(C, e, d, a2, b2) < ADJZONE) {
-      if (CMP == 1)
-        for (int k = k0; k < k1; ++k) {
-          C.wv[(int64_t)k * 3 * C.NN + x2] = 0.0;
-          C.wv[(int64_t)k * 3 * C.NN + x1] = 0.0;
-        }
-      else if (CMP == 2 && me(C, e, d, a1, b1) >= ADJZONE)  // a kept slot that the pair leaves at 0
-        for (int k = k0; k < k1; ++k) C.wv[(int64_t)k * 3 * C.NN + x1] = 0.0;
-      continue;
-    }
-    const bool keep1 = CMP == 0 || corner || me(C, e, d, a1, b1) >= ADJZONE;
-    OuterInterp O;
-    outer_interp(O, Pa, C, d, ip, jp, a2, b2, e);
-    const int cv = we_code(C, e, d, a2, b2);
-    for (int k = k0; k < k1; ++k) {
-      const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
-      const double* v = C.sv + (int64_t)k * 3 * C.NN;
-      double* wc = C.wv + (int64_t)k * 3 * C.NN;
-      double t0;
-      const double u = outer_eval(O, vp, t0);
-      const double w = we(v, cv) - u;
-      wc[x2] = w;
-      wc[x1] = keep1 ? -w : 0.0;
-    }
-  }
-  if (corner) {
-    for (int k = k0; k < k1; ++k)
-      penta_compute(Pa, C, Pa.sv + (int64_t)k * 3 * Pa.NN, C.wv + (int64_t)k * 3 * C.NN, d, ip, jp);
-    if (CMP)
-      for (int e = 0; e < 3; ++e)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int a = i + c_end_pt[e][h][0], b = j + c_end_pt[e][h][1];
-          if (me(C, e, d, a, b) >= ADJZONE) continue;
-          const int x = e * C.NN + nid(C, d, a, b);
-          for (int k = k0; k < k1; ++k) C.wv[(int64_t)k * 3 * C.NN + x] = 0.0;
-        }
-  }
+  body(d, ip, jp, k0, k1);
 }
 
 // Interp_inner_velo (src/wavelet.f90:1005-1062) of parent (ip, jp): parent
@@ -377,43 +403,49 @@ __device__ __forceinline__ void inner_eval(const InnerInterp& I, const double* _
 // Compute_velo_wavelets' inner edges (src/wavelet.f90:672-710), parents
 // [0, np)^2; CMP as for k_scalar_wc_l.
 template <int CMP>
-__global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa, WLev C, int nz, int lpt) {
-  int d, ip, jp;
-  int k0, k1;
-  if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
-  const int i = 2 * ip, j = 2 * jp;
-  const int ge[6] = {UP, DG, RT, RT, DG, UP};
-  const int gi[6] = {i + 1, i + 1, i + 1, i, i, i + 1};
-  const int gj[6] = {j, j, j + 1, j + 1, j + 1, j + 1};
-  bool on[6];
-  bool any = false;
-#pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    on[q] = me(C, ge[q], d, gi[q], gj[q]) >= ADJZONE;
-    any = any || on[q];
-  }
-  if (!any) {
-    if (CMP == 1)
-      for (int k = k0; k < k1; ++k)
-#pragma unroll
-        for (int q = 0; q < 6; ++q) C.wv[(int64_t)k * 3 * C.NN + ge[q] * C.NN + nid(C, d, gi[q], gj[q])] = 0.0;
+__global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa, WLev C, int nz, int lpt, ParentList PL) {
+  auto body = [&](int d, int ip, int jp, int k0, int k1) {
+    const int i = 2 * ip, j = 2 * jp;
+    const int ge[6] = {UP, DG, RT, RT, DG, UP};
+    const int gi[6] = {i + 1, i + 1, i + 1, i, i, i + 1};
+    const int gj[6] = {j, j, j + 1, j + 1, j + 1, j + 1};
+    bool on[6];
+    bool any = false;
+  #pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      on[q] = me(C, ge[q], d, gi[q], gj[q]) >= ADJZONE;
+      any = any || on[q];
+    }
+    if (!any) {
+      if (CMP == 1)
+        for (int k = k0; k < k1; ++k)
+  #pragma unroll
+          for (int q = 0; q < 6; ++q) C.wv[(int64_t)k * 3 * C.NN + ge[q] * C.NN + nid(C, d, gi[q], gj[q])] = 0.0;
+      return;
+    }
+    InnerInterp I;
+    inner_interp(I, Pa, C, d, ip, jp);
+    for (int k = k0; k < k1; ++k) {
+      const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
+      const double* v = C.sv + (int64_t)k * 3 * C.NN;
+      double* wc = C.wv + (int64_t)k * 3 * C.NN;
+      double u[6];
+      inner_eval(I, vp, v, u);
+  #pragma unroll
+      for (int q = 0; q < 6; ++q)
+        if (on[q])
+          wc[I.xt[q]] = we(v, I.ct[q]) - u[q];
+        else if (CMP == 1)
+          wc[I.xt[q]] = 0.0;
+    }
+  };
+  if (PL.ids) {
+    for_parents(Pa.n, Pa.n, nz, lpt, PL, body);
     return;
   }
-  InnerInterp I;
-  inner_interp(I, Pa, C, d, ip, jp);
-  for (int k = k0; k < k1; ++k) {
-    const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
-    const double* v = C.sv + (int64_t)k * 3 * C.NN;
-    double* wc = C.wv + (int64_t)k * 3 * C.NN;
-    double u[6];
-    inner_eval(I, vp, v, u);
-#pragma unroll
-    for (int q = 0; q < 6; ++q)
-      if (on[q])
-        wc[I.xt[q]] = we(v, I.ct[q]) - u[q];
-      else if (CMP == 1)
-        wc[I.xt[q]] = 0.0;
-  }
+  int d, ip, jp, k0, k1;
+  if (!parent_of(Pa.n, nz, lpt, d, ip, jp, k0, k1)) return;
+  body(d, ip, jp, k0, k1);
 }
 
 // ---------------------------------------------------------------------------
@@ -555,26 +587,25 @@ __device__ __forceinline__ void plan_parent(int64_t u, int m, int& d, int& ip, i
   ip = r - jp * m;
 }
 
-// Reconstruct_outer_velo (src/wavelet.f90:954-976) from the outer plan,
-// parents [0, np]^2, then Reconstruct_velo_penta by the corner parents.
-__global__ void __launch_bounds__(256) k_recon_outer_p(WLev Pa, WLev C, int nz, const int* __restrict__ pi,
-                                                       const double* __restrict__ pd,
-                                                       const unsigned char* __restrict__ rec) {
-  __shared__ int si[OP_NI][32];
-  __shared__ double sd[OP_ND][32];
-  const int np = Pa.n, m = np + 1;
-  const int64_t ne = (int64_t)10 * m * m, u0 = (int64_t)blockIdx.x * 32;
-  const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
-  int d = 0, ip = 0, jp = 0;
-  bool live = u0 + x < ne;
-  if (live) {
-    plan_parent(u0 + x, m, d, ip, jp);
-    live = rebuilt(rec, Pa, d, ip, jp);
-  }
-  if (!__syncthreads_or(live)) return;
-  stage_plan<OP_NI, OP_ND>(si, sd, pi, pd, ne, u0, (int)min((int64_t)32, ne - u0));
-  __syncthreads();
-  if (!live) return;
+// Plan rows of the block's parents gathered one row per thread (the parents
+// of a work list are not consecutive plan rows).
+template <int NI, int ND>
+__device__ __forceinline__ void gather_plan(int (*si)[32], double (*sd)[32], const int* __restrict__ pi,
+                                            const double* __restrict__ pd, int64_t ne, int64_t u, bool live) {
+  const int x = threadIdx.x;
+  if (live)
+    for (int q = threadIdx.y; q < NI + ND; q += blockDim.y) {
+      if (q < NI)
+        si[q][x] = pi[q * ne + u];
+      else
+        sd[q - NI][x] = pd[(q - NI) * ne + u];
+    }
+}
+
+// Reconstruct_outer_velo of the staged parent x of the block (d, ip, jp).
+__device__ __forceinline__ void recon_outer_one(const WLev& Pa, const WLev& C, int nz, const int (*si)[32],
+                                                const double (*sd)[32], int x, int d, int ip, int jp) {
+  const int np = Pa.n, y = threadIdx.y, ny = blockDim.y;
   const int i = 2 * ip, j = 2 * jp;
   for (int e = 0; e < 3; ++e) {
     const int a1 = i + c_end_pt[e][0][0], b1 = j + c_end_pt[e][0][1];
@@ -597,6 +628,46 @@ __global__ void __launch_bounds__(256) k_recon_outer_p(WLev Pa, WLev C, int nz, 
       penta_reconstruct(Pa, C, Pa.sv + (int64_t)k * 3 * Pa.NN, C.sv + (int64_t)k * 3 * C.NN, d, ip, jp);
 }
 
+// Reconstruct_outer_velo (src/wavelet.f90:954-976) from the outer plan,
+// parents [0, np]^2, then Reconstruct_velo_penta by the corner parents.  With
+// a work list (PL), persistent blocks take 32 listed parents at a time.
+__global__ void __launch_bounds__(256) k_recon_outer_p(WLev Pa, WLev C, int nz, const int* __restrict__ pi,
+                                                       const double* __restrict__ pd,
+                                                       const unsigned char* __restrict__ rec, ParentList PL) {
+  __shared__ int si[OP_NI][32];
+  __shared__ double sd[OP_ND][32];
+  const int np = Pa.n, m = np + 1;
+  const int64_t ne = (int64_t)10 * m * m;
+  const int x = threadIdx.x;
+  if (PL.ids) {
+    const int cnt = __ldg(PL.count);
+    for (int c = blockIdx.x; c < (cnt + 31) / 32; c += gridDim.x) {
+      const int e = c * 32 + x;
+      int d = 0, ip = 0, jp = 0;
+      bool live = e < cnt && list_parent(Pa.n, __ldg(PL.ids + e), m, d, ip, jp) && rebuilt(rec, Pa, d, ip, jp);
+      if (__syncthreads_or(live)) {
+        gather_plan<OP_NI, OP_ND>(si, sd, pi, pd, ne, ((int64_t)d * m + jp) * m + ip, live);
+        __syncthreads();
+        if (live) recon_outer_one(Pa, C, nz, si, sd, x, d, ip, jp);
+      }
+      __syncthreads();
+    }
+    return;
+  }
+  const int64_t u0 = (int64_t)blockIdx.x * 32;
+  int d = 0, ip = 0, jp = 0;
+  bool live = u0 + x < ne;
+  if (live) {
+    plan_parent(u0 + x, m, d, ip, jp);
+    live = rebuilt(rec, Pa, d, ip, jp);
+  }
+  if (!__syncthreads_or(live)) return;
+  stage_plan<OP_NI, OP_ND>(si, sd, pi, pd, ne, u0, (int)min((int64_t)32, ne - u0));
+  __syncthreads();
+  if (!live) return;
+  recon_outer_one(Pa, C, nz, si, sd, x, d, ip, jp);
+}
+
 // target edges of the inner plan: UP(i+1,j) DG(i+1,j) RT(i+1,j+1) RT(i,j+1) DG(i,j+1) UP(i+1,j+1)
 __device__ __forceinline__ int inner_target(const WLev& C, int q, int d, int i, int j) {
   const int ge[6] = {UP, DG, RT, RT, DG, UP};
@@ -605,26 +676,10 @@ __device__ __forceinline__ int inner_target(const WLev& C, int q, int d, int i, 
   return ge[q] * C.NN + nid(C, d, gi[q], gj[q]);
 }
 
-// Reconstruct_inner_velo (src/wavelet.f90:978-1003) from the inner plan,
-// parents [0, np)^2.
-__global__ void __launch_bounds__(256, WL_PLAN_MINB) k_recon_inner_p(WLev Pa, WLev C, int nz, const int* __restrict__ pi,
-                                                       const double* __restrict__ pd,
-                                                       const unsigned char* __restrict__ rec) {
-  __shared__ int si[IP_NI][32];
-  __shared__ double sd[IP_ND][32];
-  const int m = Pa.n;
-  const int64_t ne = (int64_t)10 * m * m, u0 = (int64_t)blockIdx.x * 32;
-  const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
-  int d = 0, ip = 0, jp = 0;
-  bool live = u0 + x < ne;
-  if (live) {
-    plan_parent(u0 + x, m, d, ip, jp);
-    live = rebuilt(rec, Pa, d, ip, jp);
-  }
-  if (!__syncthreads_or(live)) return;
-  stage_plan<IP_NI, IP_ND>(si, sd, pi, pd, ne, u0, (int)min((int64_t)32, ne - u0));
-  __syncthreads();
-  if (!live) return;
+// Reconstruct_inner_velo of the staged parent x of the block (d, ip, jp).
+__device__ __forceinline__ void recon_inner_one(const WLev& Pa, const WLev& C, int nz, const int (*si)[32],
+                                                const double (*sd)[32], int x, int d, int ip, int jp) {
+  const int y = threadIdx.y, ny = blockDim.y;
   const int i = 2 * ip, j = 2 * jp;
   for (int k = y; k < nz; k += ny) {
     const double* vp = Pa.sv + (int64_t)k * 3 * Pa.NN;
@@ -635,6 +690,46 @@ __global__ void __launch_bounds__(256, WL_PLAN_MINB) k_recon_inner_p(WLev Pa, WL
 #pragma unroll
     for (int q = 0; q < 6; ++q) v[inner_target(C, q, d, i, j)] = uu[q] + we(wc, si[15 + q][x]);
   }
+}
+
+// Reconstruct_inner_velo (src/wavelet.f90:978-1003) from the inner plan,
+// parents [0, np)^2.  With a work list (PL), persistent blocks take 32 listed
+// parents at a time.
+__global__ void __launch_bounds__(256, WL_PLAN_MINB) k_recon_inner_p(WLev Pa, WLev C, int nz, const int* __restrict__ pi,
+                                                       const double* __restrict__ pd,
+                                                       const unsigned char* __restrict__ rec, ParentList PL) {
+  __shared__ int si[IP_NI][32];
+  __shared__ double sd[IP_ND][32];
+  const int m = Pa.n;
+  const int64_t ne = (int64_t)10 * m * m;
+  const int x = threadIdx.x;
+  if (PL.ids) {
+    const int cnt = __ldg(PL.count);
+    for (int c = blockIdx.x; c < (cnt + 31) / 32; c += gridDim.x) {
+      const int e = c * 32 + x;
+      int d = 0, ip = 0, jp = 0;
+      bool live = e < cnt && list_parent(Pa.n, __ldg(PL.ids + e), m, d, ip, jp) && rebuilt(rec, Pa, d, ip, jp);
+      if (__syncthreads_or(live)) {
+        gather_plan<IP_NI, IP_ND>(si, sd, pi, pd, ne, ((int64_t)d * m + jp) * m + ip, live);
+        __syncthreads();
+        if (live) recon_inner_one(Pa, C, nz, si, sd, x, d, ip, jp);
+      }
+      __syncthreads();
+    }
+    return;
+  }
+  const int64_t u0 = (int64_t)blockIdx.x * 32;
+  int d = 0, ip = 0, jp = 0;
+  bool live = u0 + x < ne;
+  if (live) {
+    plan_parent(u0 + x, m, d, ip, jp);
+    live = rebuilt(rec, Pa, d, ip, jp);
+  }
+  if (!__syncthreads_or(live)) return;
+  stage_plan<IP_NI, IP_ND>(si, sd, pi, pd, ne, u0, (int)min((int64_t)32, ne - u0));
+  __syncthreads();
+  if (!live) return;
+  recon_inner_one(Pa, C, nz, si, sd, x, d, ip, jp);
 }
 
 }  // namespace wtw

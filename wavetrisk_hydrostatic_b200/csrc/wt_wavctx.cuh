@@ -70,6 +70,10 @@ struct WavCtx {
   // rec_off[q]; recfin_ok once built with the current maps
   unsigned char* recfin = nullptr;
   bool recfin_ok = false;
+  // with a patch tree: each parent level's work list (wavelet_kernels.cuh:
+  // ParentList) at plist_par + rec_off[q], its count at plist_cnt[q]
+  int* plist_par = nullptr;
+  int* plist_cnt = nullptr;
   unsigned char* rscr[2] = {nullptr, nullptr};
   // work lists of the levels above level_start (need_map.cuh: k_list_build):
   // the slots of the needed-node map at list + need_off[q], their count at

@@ -37,6 +37,20 @@ inline unsigned nbl(int64_t n, int nz) {
 
 int fail(const char* where, cudaError_t e) { return wt_handle_fail(where, e); }
 
+// Grid of a persistent kernel over a work list: the blocks of `threads`
+// threads the device keeps resident at once, at most `dense`.
+template <class K>
+unsigned pgrid(K kernel, int threads, unsigned dense) {
+  int dev = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess || per < 1)
+    return dense;
+  const unsigned g = (unsigned)sms * (unsigned)per;
+  return g < dense ? g : dense;
+}
+const ParentList kNoList{nullptr, nullptr};
+
 #define CKW(x)                                  \
   do {                                          \
     cudaError_t e_ = (x);                       \
@@ -112,11 +126,20 @@ void zero_wavelets(wt_handle* h) {
   }
 }
 
+}  // namespace
+ParentList wt_level_plist(wt_handle* h, int level);
+namespace {
+
 // Scalar wavelets of level l+1 (Compute_scalar_wavelets over parents [0, n_l)).
+// With CMP 2 (only the kept slots written) and a parent work list, the listed
+// parents only, persistent threads.
 template <int CMP>
 void launch_scalar_wc(wt_handle* h, int l, cudaStream_t s) {
   const int np = h->at(l).n, nz = h->nz;
-  k_scalar_wc_l<CMP><<<nbl((int64_t)10 * np * np, nz), TPBL, 0, s>>>(view(h, l + 1), np, nz, lpt_for(nz));
+  const ParentList PL = CMP == 2 ? wt_level_plist(h, l) : kNoList;
+  const unsigned dense = nbl((int64_t)10 * np * np, nz);
+  k_scalar_wc_l<CMP><<<PL.ids ? pgrid(k_scalar_wc_l<CMP>, TPBL, dense) : dense, TPBL, 0, s>>>(view(h, l + 1), np, nz,
+                                                                                             lpt_for(nz), PL);
 }
 
 // Blocks of 32 plan rows by min(nz, 8) layer threads (the plan kernels).
@@ -128,8 +151,11 @@ template <int CMP>
 void launch_velo_wc(wt_handle* h, int l, cudaStream_t s, cudaStream_t si) {
   const int np = h->at(l).n, nz = h->nz;
   const unsigned g = nbl((int64_t)10 * np * np, nz);
-  k_velo_wc_outer_l<CMP><<<g, TPBL, 0, s>>>(view(h, l), view(h, l + 1), nz, lpt_for(nz));
-  k_velo_wc_inner_l<CMP><<<g, TPBL, 0, si>>>(view(h, l), view(h, l + 1), nz, lpt_for(nz));
+  const ParentList PL = CMP == 2 ? wt_level_plist(h, l) : kNoList;
+  k_velo_wc_outer_l<CMP><<<PL.ids ? pgrid(k_velo_wc_outer_l<CMP>, TPBL, g) : g, TPBL, 0, s>>>(
+      view(h, l), view(h, l + 1), nz, lpt_for(nz), PL);
+  k_velo_wc_inner_l<CMP><<<PL.ids ? pgrid(k_velo_wc_inner_l<CMP>, TPBL, g) : g, TPBL, 0, si>>>(
+      view(h, l), view(h, l + 1), nz, lpt_for(nz), PL);
 }
 
 // inverse_wavelet_transform (src/wavelet.f90:208-296) from level_start.  The
@@ -150,12 +176,20 @@ void inverse(wt_handle* h, int partial = 0) {
     const WLev P = view(h, l), C = view(h, l + 1);
     const int64_t par1 = (int64_t)10 * (np + 1) * (np + 1), par0 = (int64_t)10 * np * np;
     const unsigned char* rec = partial == 1 ? wt_level_rec(h, l) : partial == 2 ? wt_level_rec_final(h, l) : nullptr;
-    k_prolong_l<<<nbl(par1, nz), TPBL, 0, sa>>>(P, C, nz, lpt_for(nz), rec);
-    k_recon_scalar_l<<<nbl(par0, nz), TPBL, 0, sa>>>(P, C, np, nz, lpt_for(nz), rec);
+    // a partial rebuild over the parent work list (its parents include every rebuilt one)
+    const ParentList PL = rec ? wt_level_plist(h, l) : kNoList;
+    const dim3 pb = plan_block(nz);
+    const int pt = (int)(pb.x * pb.y);
+    k_prolong_l<<<PL.ids ? pgrid(k_prolong_l, TPBL, nbl(par1, nz)) : nbl(par1, nz), TPBL, 0, sa>>>(P, C, nz, lpt_for(nz),
+                                                                                                  rec, PL);
+    k_recon_scalar_l<<<PL.ids ? pgrid(k_recon_scalar_l, TPBL, nbl(par0, nz)) : nbl(par0, nz), TPBL, 0, sa>>>(
+        P, C, np, nz, lpt_for(nz), rec, PL);
     cudaEventRecord(W->ready_s[q], sa);
     const WavLevel& V = W->L[l - h->level_start];
-    k_recon_outer_p<<<plan_grid(par1), plan_block(nz), 0, s>>>(P, C, nz, V.op_i, V.op_d, rec);
-    k_recon_inner_p<<<plan_grid(par0), plan_block(nz), 0, s>>>(P, C, nz, V.ip_i, V.ip_d, rec);
+    k_recon_outer_p<<<PL.ids ? pgrid(k_recon_outer_p, pt, plan_grid(par1)) : plan_grid(par1), pb, 0, s>>>(
+        P, C, nz, V.op_i, V.op_d, rec, PL);
+    k_recon_inner_p<<<PL.ids ? pgrid(k_recon_inner_p, pt, plan_grid(par0)) : plan_grid(par0), pb, 0, s>>>(
+        P, C, nz, V.ip_i, V.ip_d, rec, PL);
     cudaEventRecord(W->ready_v[q], s);
   }
   cudaEventRecord(W->ev[1], sa);
@@ -532,9 +566,12 @@ void comm_masks(wt_handle* h) {
 void mask_tol(wt_handle* h, int l, int st, int en, int level_fill) {
   const int m = h->at(l).n + en - st;
   const dim3 blk(32, std::min(h->nz, 8));
-  k_mask_tol_y<<<(unsigned)(((int64_t)10 * m * m + 31) / 32), blk, 0, h->stream>>>(view(h, l), h->nz, st, en,
-                                                                                     ctx(h)->thr,
-                                                                                     l < level_fill ? 1 : 0);
+  WavCtx* W = ctx(h);
+  // with a patch tree, the nodes outside it are left out (levels above level_start)
+  const unsigned char* ex = (W->tree_ps > 0 && l > h->level_start) ? W->tree + W->tree_off[l - h->level_start] : nullptr;
+  k_mask_tol_y<<<(unsigned)(((int64_t)10 * m * m + 31) / 32), blk, 0, h->stream>>>(view(h, l), h->nz, st, en, W->thr,
+                                                                                     l < level_fill ? 1 : 0, ex,
+                                                                                     W->tree_ps);
 }
 inline unsigned nodes_blocks(int m) { return nb((int64_t)10 * m * m); }
 }  // namespace
@@ -734,6 +771,15 @@ int wt_level_need_build(wt_handle* h) {
     if (tree && W->recfin)
       k_map_tree_par<<<nb(Lp.NN), TPB, 0, s>>>(Lp, tl(c), W->tree_ps, rp, W->recfin + W->rec_off[l - h->level_start]);
   }
+  // with a patch tree, the parent levels' work lists from recfin
+  if (tree && W->recfin) {
+    cudaMemsetAsync(W->plist_cnt, 0, W->L.size() * sizeof(int), s);
+    for (int l = h->level_start; l < h->level_end; ++l) {
+      const int q = l - h->level_start, m = h->at(l).n + 1;
+      k_parent_list_build<<<nb((int64_t)10 * m * m), TPB, 0, s>>>(ml(l), W->recfin + W->rec_off[q],
+                                                                  W->plist_par + W->rec_off[q], W->plist_cnt + q);
+    }
+  }
   // work lists of the levels above level_start
   cudaMemsetAsync(W->list_cnt, 0, W->L.size() * sizeof(int), s);
   for (int l = h->level_start + 1; l <= h->level_end; ++l) {
@@ -754,6 +800,16 @@ const unsigned char* wt_level_rec(wt_handle* h, int level) {
   if (level >= h->level_end || !W->recpar || !W->skip_inactive || !W->need_ok) return nullptr;
   return W->recpar + W->rec_off[level - h->level_start];
 }
+// The work list of parent level `level` (a patch tree and current maps), else
+// {null, null}: the interscale kernels then launch over every parent.
+ParentList wt_level_plist(wt_handle* h, int level) {
+  WavCtx* W = ctx(h);
+  if (level >= h->level_end || !W->plist_par || !W->recfin_ok || !W->skip_inactive || !W->need_ok)
+    return ParentList{nullptr, nullptr};
+  const int q = level - h->level_start;
+  return ParentList{W->plist_par + W->rec_off[q], W->plist_cnt + q};
+}
+
 // The parents of level that the inverse transform after adapt rebuilds: with a
 // patch tree those the next step reads and those of the tree's nodes (recfin),
 // else null (every parent).
@@ -896,7 +952,10 @@ int wt_level_restrict_scalar(wt_handle* h, int level, double* par, const double*
   P.scal = par;
   C.scal = const_cast<double*>(chd);
   const int m = h->at(level).n + 1;
-  k_restr_scalar<<<nb((int64_t)nz * 10 * m * m), TPB, 0, stream ? stream : h->stream>>>(P, C, nz);
+  const ParentList PL = wt_level_plist(h, level);
+  const unsigned dense = nb((int64_t)nz * 10 * m * m);
+  k_restr_scalar<<<PL.ids ? pgrid(k_restr_scalar, TPB, dense) : dense, TPB, 0, stream ? stream : h->stream>>>(P, C, nz,
+                                                                                                              PL);
   CKW(cudaGetLastError());
   return WT_OK;
 }
@@ -910,9 +969,10 @@ int restrict_flux(wt_handle* h, int level, double* par0, double* par1, const dou
   const int m = h->at(level).n;
   const int64_t ne = (int64_t)3 * 10 * m * m;
   const dim3 blk(32, std::min(nz, 8));
-  k_restr_flux3<<<(unsigned)((ne + 31) / 32), blk, 0, h->stream>>>(view(h, level), m, nz, V.rf_pi, V.rf_pd, par0,
-                                                                    par1, chd0, chd1, dsc0, dsc1,
-                                                                    (int)h->at(level + 1).NN);
+  const ParentList PL = wt_level_plist(h, level);
+  const unsigned dense = (unsigned)((ne + 31) / 32);
+  k_restr_flux3<<<PL.ids ? pgrid(k_restr_flux3, (int)(blk.x * blk.y), dense) : dense, blk, 0, h->stream>>>(
+      view(h, level), m, nz, V.rf_pi, V.rf_pd, par0, par1, chd0, chd1, dsc0, dsc1, (int)h->at(level + 1).NN, PL);
   CKW(cudaGetLastError());
   return WT_OK;
 }
@@ -942,7 +1002,8 @@ int restrict_pair(wt_handle* h, int level, std::initializer_list<int> fields) {
 int wt_restrict_scalar(wt_handle* h, int level) {
   if (int rc = restrict_pair(h, level, {WT_WORK_SCALAR})) return rc;
   const int m = h->at(level).n + 1;
-  k_restr_scalar<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz);
+  k_restr_scalar<<<nb((int64_t)h->nz * 10 * m * m), TPB, 0, h->stream>>>(view(h, level), view(h, level + 1), h->nz,
+                                                                          kNoList);
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   return WT_OK;
@@ -1072,7 +1133,11 @@ int wt_tree_init(wt_handle* h, int patch_size) {
     CKW(W->alloc(&W->treq, r));
     CKW(W->alloc(&W->tree_le, 1));
     CKW(W->alloc(&W->tree_cnt, 2));
-    if (W->recpar) CKW(W->alloc(&W->recfin, W->rec_tot));
+    if (W->recpar) {
+      CKW(W->alloc(&W->recfin, W->rec_tot));
+      CKW(W->alloc(&W->plist_par, W->rec_tot));
+      CKW(W->alloc(&W->plist_cnt, W->L.size()));
+    }
   }
   W->tree_ps = patch_size;
   // add_second_level: every patch of level_start; none above

@@ -522,7 +522,9 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
         with torch.cuda.stream(stream):
             flush.fill_(float(s))
         ev[s][0].record(stream)
+        torch.cuda.nvtx.range_push("step")   # for an ncu launch list of the timed steps
         model.step(DT_AD)
+        torch.cuda.nvtx.range_pop()
         ev[s][1].record(stream)
     torch.cuda.synchronize(device)
     ms = sum(a.elapsed_time(b) for a, b in ev)

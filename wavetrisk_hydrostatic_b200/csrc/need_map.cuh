@@ -230,51 +230,90 @@ __global__ void k_map_tree_par(MapLev Lp, TreeLev Tc, int ps, const unsigned cha
 
 }  // namespace wtw
 
+
+
 namespace wtw {
 
-// A level's work list from its needed-node map: every padded slot x with
-// need[nsrc[x]] set, appended by warp-aggregated atomics (the order varies
-// from build to build; each slot's results do not depend on it).  *count
-// must be 0 on entry.
-__global__ void k_list_build(MapLev L, const unsigned char* __restrict__ need, int* __restrict__ ids,
-                             int* __restrict__ count) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool on = x < L.NN && need[__ldg(L.nsrc + x)] != 0;
-  const unsigned m = __ballot_sync(0xffffffffu, on);
-  if (!m) return;
-  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(count, __popc(m));
-  base = __shfl_sync(m, base, leader);
-  if (on) ids[base + __popc(m & ((1u << lane) - 1))] = x;
+// Work lists in ascending slot order (so that a warp of a list kernel takes
+// neighbouring rows of a patch and their stencils share cache lines), by a
+// three-pass compaction over blocks of LIST_B candidates: per-block counts, one
+// scan of the counts, then each block writes its entries at its offset.
+constexpr int LIST_B = 1024;
+
+// Candidates of a level's node list: every padded slot x, on where
+// need[nsrc[x]] is set.
+struct NodeCand {
+  int NN;
+  const int* nsrc;
+  const unsigned char* map;
+  __device__ __forceinline__ int n() const { return NN; }
+  __device__ __forceinline__ bool on(int t, int& x) const {
+    x = t;
+    return map[__ldg(nsrc + t)] != 0;
+  }
+};
+// Candidates of a parent level's list: the slots of [0, np]^2, on where
+// rec[nsrc[x]] is set.
+struct ParentCand {
+  int np, P;
+  const int* nsrc;
+  const unsigned char* map;
+  __device__ __forceinline__ int n() const { return 10 * (np + 1) * (np + 1); }
+  __device__ __forceinline__ bool on(int t, int& x) const {
+    const int m = np + 1, d = t / (m * m), r = t - d * m * m;
+    const int jp = r / m, ip = r - jp * m;
+    x = (d * P + jp + 2) * P + ip + 2;
+    return map[__ldg(nsrc + x)] != 0;
+  }
+};
+
+template <class Cand>
+__global__ void __launch_bounds__(LIST_B) k_list_count(Cand c, int* __restrict__ bcnt) {
+  const int t = blockIdx.x * LIST_B + threadIdx.x;
+  int x;
+  const bool on = t < c.n() && c.on(t, x);
+  const int k = __syncthreads_count(on);
+  if (threadIdx.x == 0) bcnt[blockIdx.x] = k;
 }
 
-}  // namespace wtw
-
-namespace wtw {
-
-// A parent level's work list: every padded parent slot of [0, np]^2 whose
-// source the map says is rebuilt (rec[nsrc[x]]), appended by warp-aggregated
-// atomics (order free).  *count must be 0 on entry.
-__global__ void k_parent_list_build(MapLev Lp, const unsigned char* __restrict__ rec, int* __restrict__ ids,
-                                    int* __restrict__ count) {
-  const int m = Lp.n + 1;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool on = false;
-  int x = 0;
-  if (t < 10 * m * m) {
-    const int d = t / (m * m), r = t - d * m * m;
-    const int jp = r / m, ip = r - jp * m;
-    x = (d * Lp.P + jp + 2) * Lp.P + ip + 2;
-    on = rec[__ldg(Lp.nsrc + x)] != 0;
+// Exclusive scan of nb block counts into boff, the total into *count (one block).
+__global__ void __launch_bounds__(LIST_B) k_list_scan(int nb, const int* __restrict__ bcnt, int* __restrict__ boff,
+                                                      int* __restrict__ count) {
+  __shared__ int part[LIST_B];
+  const int t = threadIdx.x;
+  const int run = (nb + LIST_B - 1) / LIST_B;
+  const int a = min(nb, t * run), b = min(nb, a + run);
+  int c = 0;
+  for (int q = a; q < b; ++q) c += bcnt[q];
+  part[t] = c;
+  __syncthreads();
+  for (int o = 1; o < LIST_B; o <<= 1) {
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
   }
-  const unsigned msk = __ballot_sync(0xffffffffu, on);
-  if (!msk) return;
-  const int lane = threadIdx.x & 31, leader = __ffs(msk) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(count, __popc(msk));
-  base = __shfl_sync(msk, base, leader);
-  if (on) ids[base + __popc(msk & ((1u << lane) - 1))] = x;
+  int w = part[t] - c;
+  for (int q = a; q < b; ++q) {
+    boff[q] = w;
+    w += bcnt[q];
+  }
+  if (t == LIST_B - 1) *count = part[t];
+}
+
+template <class Cand>
+__global__ void __launch_bounds__(LIST_B) k_list_write(Cand c, const int* __restrict__ boff, int* __restrict__ ids) {
+  __shared__ int wsum[LIST_B / 32];
+  const int t = blockIdx.x * LIST_B + threadIdx.x;
+  int x = 0;
+  const bool on = t < c.n() && c.on(t, x);
+  const unsigned m = __ballot_sync(0xffffffffu, on);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(m);
+  __syncthreads();
+  int before = 0;
+  for (int q = 0; q < w; ++q) before += wsum[q];
+  if (on) ids[boff[blockIdx.x] + before + __popc(m & ((1u << lane) - 1))] = x;
 }
 
 }  // namespace wtw

@@ -11,7 +11,7 @@ enum { LORT = 0, UPLT = 1 };
 
 // A level's work list: the padded slots a kernel computes (those of the
 // needed-node map), their count on the device, built inside the step's graph
-// (need_map.cuh: k_list_build).
+// (need_map.cuh: k_list_count, k_list_scan, k_list_write).
 struct NodeList {
   const int* ids;
   const int* count;

@@ -24,7 +24,7 @@ constexpr int FROZEN = 32, TOLRNZ = 16, ADJZONE = 8, ZERO = 0;
 // [0, n]^2 that an interscale kernel may have work at (those the inverse after
 // adapt rebuilds: the next step's parents and those of the tree's nodes, which
 // hold every child slot a mask reaches), their count on the device; built with
-// the needed-node maps (need_map.cuh: k_parent_list_build).  ids null: none.
+// the needed-node maps (need_map.cuh: k_list_count/_scan/_write).  ids null: none.
 struct ParentList {
   const int* ids;
   const int* count;

@@ -74,8 +74,11 @@ struct WavCtx {
   // ParentList) at plist_par + rec_off[q], its count at plist_cnt[q]
   int* plist_par = nullptr;
   int* plist_cnt = nullptr;
+  // block counts and offsets of the list compaction (need_map.cuh: k_list_*)
+  int* lscr = nullptr;
+  size_t lscr_n = 0;
   unsigned char* rscr[2] = {nullptr, nullptr};
-  // work lists of the levels above level_start (need_map.cuh: k_list_build):
+  // work lists of the levels above level_start (need_map.cuh: k_list_*):
   // the slots of the needed-node map at list + need_off[q], their count at
   // list_cnt[q], built with the maps
   int* list = nullptr;

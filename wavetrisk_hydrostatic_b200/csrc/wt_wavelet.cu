@@ -51,6 +51,27 @@ unsigned pgrid(K kernel, int threads, unsigned dense) {
 }
 const ParentList kNoList{nullptr, nullptr};
 
+// Blocks of LIST_B candidates of the largest level (the list compaction's scratch).
+size_t mx_nn_blocks(wt_handle* h) {
+  size_t mx = 0;
+  for (int l = h->level_start; l <= h->level_end; ++l) mx = std::max(mx, (size_t)h->at(l).NN);
+  return (mx + LIST_B - 1) / LIST_B;
+}
+
+// An ascending work list of the candidates c into ids, its count into *count
+// (stream-ordered; scratch: the context's block counts and offsets).
+template <class Cand>
+void build_list(wt_handle* h, const Cand& c, int n, int* ids, int* count) {
+  WavCtx* W = ctx(h);
+  const int nb = (n + LIST_B - 1) / LIST_B;
+  int* bcnt = W->lscr;
+  int* boff = W->lscr + W->lscr_n / 2;
+  cudaStream_t s = h->stream;
+  k_list_count<<<nb, LIST_B, 0, s>>>(c, bcnt);
+  k_list_scan<<<1, LIST_B, 0, s>>>(nb, bcnt, boff, count);
+  k_list_write<<<nb, LIST_B, 0, s>>>(c, boff, ids);
+}
+
 #define CKW(x)                                  \
   do {                                          \
     cudaError_t e_ = (x);                       \
@@ -340,6 +361,8 @@ int wt_wavelet_setup(wt_handle* h) {
     CKW(W->alloc(&W->need[1], tot));
     CKW(W->alloc(&W->list, tot));
     CKW(W->alloc(&W->list_cnt, W->L.size()));
+    W->lscr_n = 2 * (mx_nn_blocks(h) + 1);
+    CKW(W->alloc(&W->lscr, W->lscr_n));
     size_t ptot = 0, mx = 0;
     W->rec_off.assign(W->L.size(), 0);
     for (int l = h->level_start; l <= h->level_end; ++l) {
@@ -772,20 +795,19 @@ int wt_level_need_build(wt_handle* h) {
       k_map_tree_par<<<nb(Lp.NN), TPB, 0, s>>>(Lp, tl(c), W->tree_ps, rp, W->recfin + W->rec_off[l - h->level_start]);
   }
   // with a patch tree, the parent levels' work lists from recfin
-  if (tree && W->recfin) {
-    cudaMemsetAsync(W->plist_cnt, 0, W->L.size() * sizeof(int), s);
+  if (tree && W->recfin)
     for (int l = h->level_start; l < h->level_end; ++l) {
       const int q = l - h->level_start, m = h->at(l).n + 1;
-      k_parent_list_build<<<nb((int64_t)10 * m * m), TPB, 0, s>>>(ml(l), W->recfin + W->rec_off[q],
-                                                                  W->plist_par + W->rec_off[q], W->plist_cnt + q);
+      const DevLevel& D = h->at(l);
+      build_list(h, ParentCand{D.n, D.P, D.nsrc, W->recfin + W->rec_off[q]}, 10 * m * m, W->plist_par + W->rec_off[q],
+                 W->plist_cnt + q);
     }
-  }
   // work lists of the levels above level_start
-  cudaMemsetAsync(W->list_cnt, 0, W->L.size() * sizeof(int), s);
   for (int l = h->level_start + 1; l <= h->level_end; ++l) {
     const int q = l - h->level_start;
-    k_list_build<<<nb(h->at(l).NN), TPB, 0, s>>>(ml(l), W->need[NEED_R & 1] + W->need_off[q], W->list + W->need_off[q],
-                                                 W->list_cnt + q);
+    const DevLevel& D = h->at(l);
+    build_list(h, NodeCand{(int)D.NN, D.nsrc, W->need[NEED_R & 1] + W->need_off[q]}, (int)D.NN,
+               W->list + W->need_off[q], W->list_cnt + q);
   }
   CKW(cudaGetLastError());
   W->need_ok = true;

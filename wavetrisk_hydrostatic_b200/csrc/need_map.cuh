@@ -20,7 +20,7 @@
 namespace wtw {
 
 #ifndef WT_NEED_R
-#define WT_NEED_R 6
+#define WT_NEED_R 4
 #endif
 constexpr int NEED_R = WT_NEED_R;
 constexpr int NEED_MAXL = 16;

@@ -392,36 +392,55 @@ __device__ __forceinline__ bool slot_in_tree(const WLev& L, const unsigned char*
 __global__ void k_mask_tol_y(WLev L, int nz, int st, int en, const double* __restrict__ thr, int below_fill,
                              const unsigned char* __restrict__ exist, int ps) {
   __shared__ int fl[8][32];  // ny <= 8
+  __shared__ int s_x[32], s_cn[32], s_ce[3][32];
+  __shared__ unsigned char s_in[32], s_go[32];
   const int m = L.n + en - st;
   const int x = threadIdx.x, y = threadIdx.y, ny = blockDim.y;
-  const int64_t t = (int64_t)blockIdx.x * 32 + x;
-  bool in = t < (int64_t)10 * m * m;
-  int d = 0, i = 0, j = 0;
-  if (in) {
-    d = (int)(t / ((int64_t)m * m));
-    const int r = (int)(t - (int64_t)d * m * m);
-    j = r / m + st;
-    i = r % m + st;
-    in = inr(L, i, j);
+  if (y == 0) {  // the node of column x, once for the block's layer threads
+    const int64_t t = (int64_t)blockIdx.x * 32 + x;
+    bool in = t < (int64_t)10 * m * m;
+    int d = 0, i = 0, j = 0;
+    if (in) {
+      d = (int)(t / ((int64_t)m * m));
+      const int r = (int)(t - (int64_t)d * m * m);
+      j = r / m + st;
+      i = r % m + st;
+      in = inr(L, i, j);
+    }
+    int x_ = 0, cn = 0, ce[3] = {0, 0, 0};
+    if (in) {
+      x_ = nid(L, d, i, j);
+      in = L.mask_n[x_] != FROZEN;
+    }
+    bool read = in;
+    if (in) {
+      cn = __ldg(L.nsrc + x_);
+#pragma unroll
+      for (int e = 0; e < 3; ++e) ce[e] = __ldg(L.esrc + e * L.NN + x_);
+      if (exist && !below_fill) {
+        read = slot_in_tree(L, exist, ps, cn);
+#pragma unroll
+        for (int e = 0; e < 3; ++e) read = read || slot_in_tree(L, exist, ps, (ce[e] >> 1) % L.NN);
+      }
+    }
+    s_in[x] = in;
+    s_go[x] = read;
+    s_x[x] = x_;
+    s_cn[x] = cn;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) s_ce[e][x] = ce[e];
   }
-  int x_ = 0;
-  if (in) {
-    x_ = nid(L, d, i, j);
-    in = L.mask_n[x_] != FROZEN;
-  }
+  __syncthreads();
+  const bool in = s_in[x], go = s_go[x];
+  // with a tree, a block none of whose nodes reads a wavelet changes no mask
+  if (exist && !below_fill && !__syncthreads_or(go)) return;
+  const int x_ = s_x[x], cn = s_cn[x];
   int f = 0;
-  if (in) {
-    const int cn = __ldg(L.nsrc + x_);
+  if (go) {
     int ce[3];
 #pragma unroll
-    for (int e = 0; e < 3; ++e) ce[e] = __ldg(L.esrc + e * L.NN + x_);
-    bool read = true;
-    if (exist && !below_fill) {
-      read = slot_in_tree(L, exist, ps, cn);
-#pragma unroll
-      for (int e = 0; e < 3; ++e) read = read || slot_in_tree(L, exist, ps, (ce[e] >> 1) % L.NN);
-    }
-    for (int k = y; k < nz && read; k += ny) {
+    for (int e = 0; e < 3; ++e) ce[e] = s_ce[e][x];
+    for (int k = y; k < nz; k += ny) {
       const double wm = L.wm[(int64_t)k * L.NN + cn], wt = L.wt[(int64_t)k * L.NN + cn];
       if (fabs(wm) >= thr[0 * nz + k] || below_fill) f |= 1;
       if (fabs(wt) >= thr[1 * nz + k] || below_fill) f |= 1;

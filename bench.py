@@ -435,25 +435,28 @@ def wavelet_case(lmin, lmax, nz, repeats=5, device=None):
     return out
 
 
-def adaptive_launches(L):
-    """Kernels launched by one adaptive step of L levels (AdaptiveOcean.step
-    with fixed thresholds, max_level = level_end): RK4 of the hierarchy (per
-    stage: column + step1 and k_trend_ml (with the RK sub-step) per level,
-    three restrictions per coarse level (Bernoulli, Exner, both fluxes),
-    WT_after_step with three wavelet kernels per coarse level (scalar,
-    outer and inner velocity, compression fused) and four inverse-transform
-    kernels per coarse level), wt_mask_build's sweeps (each comm_masks is
-    one launch over all levels, 3L + 3 of them), compression and the inverse
-    transform.  The mask sequence ends with the needed-node maps of the
-    levels above level_start (a seed and six dilation launches) and the
-    reconstruct maps of the intermediate stages' inverse transforms (six
-    launches per coarser level)."""
-    stage = 3 * L + 3 * (L - 1) + 3 * (L - 1) + 4 * (L - 1)
-    comm = 3 * L + 3
-    masks = ((L - 1) + 1 + 2 * (L - 1) + L + (L - 1) + 2 * (L - 1) + 2 * (L - 2) + 1 + 2 * (L - 2) + 1 + L
-             + comm + (7 + 6 * (L - 1) if L > 1 else 0))
-    # the last stage's inverse transform is left out (the one after adapt rebuilds the levels)
-    return 4 * stage - 4 * (L - 1) + masks + (L - 1) + 4 * (L - 1)
+def adaptive_launches(L, need_r=4):
+    """Kernels launched by one adaptive step of L levels with a patch tree
+    (AdaptiveOcean.step with fixed thresholds once the tree's level_end is the
+    top: one graph replay); C = L - 1 parent levels, the same number of levels
+    above level_start.
+    * RK4, per stage: column, step1 and trend of every level (the levels above
+      level_start over their work lists), two scalar and one flux restriction
+      and three forward-wavelet kernels per parent level; four inverse kernels
+      per parent level after each of the first three stages and after adapt.
+    * adapt's mask sequence (init_masks_zero, mask_active, the sweeps with
+      refine() of the tree, complete_masks, mask_trsk and 3C + 6 comm_masks).
+    * The maps: one seed, need_r dilations and the cut to the tree; per parent
+      level seven reconstruct-map launches; three launches per work list (one
+      per level above level_start and one per parent level).
+    * compress_wavelets of the dropped slots.
+    The ncu launch list of one step (profiles/adaptive_J5-J9x32_step_launch_list.md)
+    counts 360 for L = 5."""
+    C = L - 1
+    stage = 12 * L + 12 * C + 12 * C + 16 * C
+    masks = C + 3 * L + 13 * C + 4
+    maps = 1 + need_r + C + 7 * C + 3 * C + 3 * C
+    return stage + masks + maps + C
 
 
 def algorithmic_bytes_trend_ml(level, nz, n_on=None, n_own=None, n_listed=None):

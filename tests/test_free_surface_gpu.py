@@ -101,17 +101,22 @@ def test_free_surface_update_refuses_a_mismatched_solver_setup():
     dev.close()
 
 
-def test_mode_split_adaptive_steps_run():
+@pytest.mark.parametrize("init", ["dense", "reference"])
+def test_mode_split_adaptive_steps_run(init):
     """ModeSplitOcean (RK4_split + adapt + inverse transform, the ensemble's
-    member step) on J3..J5 x 2 over a seamount: every step's free-surface solve
-    converges and the state and free surface stay finite and bounded."""
+    member step) on J3..J5 x 2 over a seamount, from the dense start and from
+    the reference's initial refinement (patch tree refined by adapt): every
+    step's free-surface solve converges and the state and free surface stay
+    finite and bounded."""
     from wavetrisk_hydrostatic_b200.adaptive import ModeSplitOcean
 
     ph = OceanParams()
     G = Grid(3, 5, radius=6371e3)
-    levels = [G.level(l) for l in range(3, 6)]
+    levels = [G.level(l) for l in range(2, 6)]
     states = [bump_state(g, 2, seed=6, ph=ph, topo=seamount_topography(g, seed=6, radius=600e3)) for g in levels]
-    model = ModeSplitOcean(G, 3, 5, 2, states, 1200.0, ph, tol=5e-3, init="dense")
+    root, states, levels = states[0], states[1:], levels[1:]
+    model = ModeSplitOcean(G, 3, 5, 2, states, 1200.0, ph, tol=5e-3, init=init,
+                           root_state=root if init == "reference" else None)
     for _ in range(5):
         rep = model.step()
         assert rep.status == 0 and rep.true_rel_residual <= 1e-8

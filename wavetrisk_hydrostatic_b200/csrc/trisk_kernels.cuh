@@ -75,10 +75,12 @@ __global__ void __launch_bounds__(NODE_TILE) k_column_list(LevelDev L, Phys ph, 
                                                            const double* __restrict__ mean_m,
                                                            const double* __restrict__ mean_t, double* __restrict__ phik,
                                                            double* __restrict__ pterm, NodeList W) {
-  for_list(L, 1, W, [&](int, int id, int i, int j) {
-    if (i < 0 || j < 0 || i > L.n || j > L.n) return;
+  const int cnt = __ldg(W.count);
+  for (int64_t w = blockIdx.x; w < list_items(cnt, 1); w += gridDim.x) {
+    int k, id, i, j;
+    if (!list_entry(L, 1, W, cnt, w, k, id, i, j) || i < 0 || j < 0 || i > L.n || j > L.n) continue;
     column_node(L, ph, nz, mass, temp, mean_m, mean_t, phik, pterm, id, i, j);
-  });
+  }
 }
 
 __device__ __forceinline__ void column_node(const LevelDev& L, const Phys& ph, int nz, const double* __restrict__ mass,
@@ -234,15 +236,17 @@ __global__ void __launch_bounds__(NODE_TILE, 3)
 }
 
 // The same over a work list (persistent blocks).
-__global__ void __launch_bounds__(NODE_TILE, 3)
+__global__ void __launch_bounds__(NODE_TILE, 4)
     k_step1_list(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
                  const double* __restrict__ velo, const double* __restrict__ mean_m,
                  const double* __restrict__ mean_t, const double* __restrict__ phik,
                  const double* __restrict__ pterm, Step1Out out, NodeList W) {
-  for_list(L, nz, W, [&](int k, int id, int i, int j) {
-    if (i < 0 || j < 0 || i > L.n || j > L.n) return;
+  const int cnt = __ldg(W.count);
+  for (int64_t w = blockIdx.x; w < list_items(cnt, nz); w += gridDim.x) {
+    int k, id, i, j;
+    if (!list_entry(L, nz, W, cnt, w, k, id, i, j) || i < 0 || j < 0 || i > L.n || j > L.n) continue;
     step1_node(L, nz, mass, temp, velo, mean_m, mean_t, phik, pterm, out, k, id, i, j);
-  });
+  }
 }
 
 __device__ __forceinline__ void step1_node(const LevelDev& L, int nz, const double* __restrict__ mass,

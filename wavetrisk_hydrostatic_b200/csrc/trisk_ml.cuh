@@ -54,7 +54,11 @@ __global__ void __launch_bounds__(NODE_TILE, 4) k_trend_ml(LevelDev L, int nz, T
 // The same over a work list (persistent blocks): the list holds the padded
 // slots of the needed-node map.
 __global__ void __launch_bounds__(NODE_TILE, 3) k_trend_ml_list(LevelDev L, int nz, TrendML io, NodeList W) {
-  for_list(L, nz, W, [&](int k, int id, int i, int j) { trend_ml_node(L, nz, io, k, id, i, j); });
+  const int cnt = __ldg(W.count);
+  for (int64_t w = blockIdx.x; w < list_items(cnt, nz); w += gridDim.x) {
+    int k, id, i, j;
+    if (list_entry(L, nz, W, cnt, w, k, id, i, j)) trend_ml_node(L, nz, io, k, id, i, j);
+  }
 }
 
 __device__ __forceinline__ void trend_ml_node(const LevelDev& L, int nz, const TrendML& io, int k, int id, int i,

@@ -56,22 +56,21 @@ inline unsigned persistent_grid(K kernel, unsigned dense) {
   return g < dense ? g : dense;
 }
 
-// Persistent loop over a work list: items (chunk of NODE_TILE entries, layer)
-// layer-fastest as in the dense launches, strided by the grid; f(k, id, i, j)
-// for every entry of the block's chunks.
-template <class F>
-__device__ __forceinline__ void for_list(const LevelDev& L, int nz, const NodeList& W, F f) {
-  const int cnt = __ldg(W.count);
-  const int64_t items = (int64_t)((cnt + NODE_TILE - 1) / NODE_TILE) * nz;
-  for (int64_t w = blockIdx.x; w < items; w += gridDim.x) {
-    const int chunk = (int)(w / nz), k = (int)(w - (int64_t)chunk * nz);
-    const int e = chunk * NODE_TILE + threadIdx.x;
-    if (e >= cnt) continue;
-    const int id = __ldg(W.ids + e);
-    int i, j;
-    node_ij(L, id, i, j);
-    f(k, id, i, j);
-  }
+// Work-list items: (chunk of NODE_TILE entries, layer) layer-fastest as in
+// the dense launches; a persistent kernel strides w over [0, list_items) by the
+// grid and takes entry (k, id, i, j) of item w where list_entry says so.
+__device__ __forceinline__ int64_t list_items(int cnt, int nz) {
+  return (int64_t)((cnt + NODE_TILE - 1) / NODE_TILE) * nz;
+}
+__device__ __forceinline__ bool list_entry(const LevelDev& L, int nz, const NodeList& W, int cnt, int64_t w, int& k,
+                                           int& id, int& i, int& j) {
+  const int chunk = (int)(w / nz);
+  k = (int)(w - (int64_t)chunk * nz);
+  const int e = chunk * NODE_TILE + threadIdx.x;
+  if (e >= cnt) return false;
+  id = __ldg(W.ids + e);
+  node_ij(L, id, i, j);
+  return true;
 }
 
 // Readers of the state through the ghost remap.

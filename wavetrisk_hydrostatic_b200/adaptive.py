@@ -26,6 +26,8 @@ transform, with every patch present.
 """
 from __future__ import annotations
 
+import json
+
 import numpy as np
 
 from .cases import OceanParams
@@ -58,7 +60,8 @@ class AdaptiveOcean:
         self.nz, self.tol, self.udim = nz, tol, udim
         self.min_level, self.max_level, self.level_fill = min_level, max_level, level_fill
         self.dynamic = dynamic_thresholds
-        self.dev = WaveletHierarchy(self.levels, [st["topo"] for st in states], nz, self.ph)
+        self.topos = [np.asarray(st["topo"], dtype=np.float64) for st in states]
+        self.dev = WaveletHierarchy(self.levels, self.topos, nz, self.ph)
         for g, st in zip(self.levels, states):
             for name in ("mean_m", "mean_t"):
                 self.dev.upload(g.level, name, st[name])
@@ -189,6 +192,57 @@ class AdaptiveOcean:
 
     def masks(self):
         return [(self.dev.download(g.level, "mask_n"), self.dev.download(g.level, "mask_e")) for g in self.levels]
+
+    # every device field the next step reads (the RK stage buffers and the maps are rebuilt from these)
+    CHECKPOINT_FIELDS = ("mass", "temp", "velo", "wc_mass", "wc_temp", "wc_velo", "mask_n", "mask_e", "mean_m",
+                         "mean_t")
+
+    def save(self, path: str) -> None:
+        """Checkpoint for an exact resume: every level's scaling fields, wavelets, masks and layer means, the
+        patch tree, the topography, the thresholds and the step count, in one .npz file.  A run resumed by
+        load() takes the same steps, bit for bit, as the run that was saved.  (The reference's
+        dump_adapt_mpi, src/io.f90:792-935, stores a pruned tree and the wavelets only and rebuilds the rest
+        on restart; its file format is not this one.)"""
+        arrays = {}
+        for g in self.levels:
+            for name in self.CHECKPOINT_FIELDS:
+                arrays[f"L{g.level}_{name}"] = self.dev.download(g.level, name)
+            arrays[f"L{g.level}_topo"] = self.topos[g.level - self.min_level]
+            if self.tree:
+                arrays[f"L{g.level}_patches"] = self.dev.tree(g.level, self.patch_size)[0].astype(np.uint8)
+        meta = {"kind": "AdaptiveOcean", "min_level": self.min_level, "max_level": self.max_level, "nz": self.nz,
+                "tol": self.tol, "udim": self.udim, "level_fill": self.level_fill, "dynamic": self.dynamic,
+                "istep": self.istep, "tree": self.tree, "patch_size": self.patch_size,
+                "level_end": self.level_end(), "threshold": self.threshold.tolist(),
+                "threshold_def": self.threshold_def.tolist(), "ph": vars(self.ph)}
+        np.savez(path, meta=np.array(json.dumps(meta)), **arrays)
+
+    @classmethod
+    def load(cls, path: str, grid: Grid) -> "AdaptiveOcean":
+        """A model resumed from save()'s file on the grid it was made on."""
+        z = np.load(path, allow_pickle=False)
+        meta = json.loads(str(z["meta"]))
+        if meta.get("kind") != "AdaptiveOcean":
+            raise ValueError(f"{path}: not an AdaptiveOcean checkpoint")
+        self = cls.__new__(cls)
+        self.ph = OceanParams(**meta["ph"])
+        self.min_level, self.max_level, self.nz = meta["min_level"], meta["max_level"], meta["nz"]
+        self.tol, self.udim, self.level_fill = meta["tol"], meta["udim"], meta["level_fill"]
+        self.dynamic, self.istep = meta["dynamic"], meta["istep"]
+        self.patch_size, self.tree, self.init_log = meta["patch_size"], False, []
+        self.levels = [grid.level(l) for l in range(self.min_level, self.max_level + 1)]
+        self.topos = [z[f"L{g.level}_topo"] for g in self.levels]
+        self.dev = WaveletHierarchy(self.levels, self.topos, self.nz, self.ph)
+        self.threshold = np.array(meta["threshold"])
+        self.threshold_def = np.array(meta["threshold_def"])
+        for g in self.levels:
+            for name in self.CHECKPOINT_FIELDS:
+                self.dev.upload(g.level, name, z[f"L{g.level}_{name}"])
+        if meta["tree"]:
+            self.dev.tree_init(self.patch_size)
+            self.dev.grid_sync([z[f"L{g.level}_patches"] for g in self.levels], meta["level_end"])
+            self.tree = True
+        return self
 
     def close(self) -> None:
         self.dev.close()

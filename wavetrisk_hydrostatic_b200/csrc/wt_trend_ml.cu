@@ -177,7 +177,7 @@ States hierarchy_state(wt_handle* h) {
 // step1 start as soon as that transform has rebuilt the level, beside the finer
 // levels' reconstruction.
 // With grad (per level), the velocity sub-step is u_star's base + hs * (trend +
-// th1 * grad) (src/barotropic_2d.f90:29-50), every node computed.
+// th1 * grad) (src/barotropic_2d.f90:29-50).
 int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const States* base = nullptr,
                 const States* dest = nullptr, double hs = 0.0, bool wav = false, bool after_inverse = false,
                 const double* const* grad = nullptr, double th1 = 0.0) {
@@ -185,10 +185,10 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
   const int nz = h->nz;
   // With WT_after_step following (wav), a level's results above level_start are
   // read only where its needed-node map says so (need_map.cuh).
-  // The phase profile (tm) takes the same maps, so that its times are those of the steps.
-  auto need = [&](int l) -> const unsigned char* {
-    return ((wav || tm) && dest && !grad) ? wt_level_need(h, l) : nullptr;
-  };
+  // The phase profile (tm) takes the same maps, so that its times are those of the steps.  The
+  // mode-split stages (grad) take them too: their extra terms (barotropic_correction, grad_eta) run on
+  // every node, and each stage's inverse transform rebuilds every level above level_start.
+  auto need = [&](int l) -> const unsigned char* { return ((wav || tm) && dest) ? wt_level_need(h, l) : nullptr; };
   // and then over the level's work list, the needed slots only (persistent blocks)
   auto list = [&](int l) { return need(l) ? wt_level_list(h, l) : wtk::NodeList{nullptr, nullptr}; };
   // Column + step1 of a level read only that level's state and write only its
@@ -369,7 +369,9 @@ namespace {
 // over the hierarchy, without free_surface_update: per stage
 // barotropic_correction of the stage's source state, trend_ml, scalar_star and
 // u_star (src/barotropic_2d.f90:9-50; the base is always the solution, as the
-// reference's sol), and WT_after_step of the stage state.  Every node computed.
+// reference's sol), and WT_after_step of the stage state.  The trends run over
+// the levels' work lists (needed-node maps); each stage's inverse transform
+// rebuilds every level above level_start.
 int rk4_split_explicit(wt_handle* h, double dt, double theta1) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const States q = hierarchy_state(h);

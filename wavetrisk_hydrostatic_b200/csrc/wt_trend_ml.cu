@@ -187,7 +187,7 @@ int trend_multi(wt_handle* h, const States& S, PhaseTimer* tm = nullptr, const S
   // read only where its needed-node map says so (need_map.cuh).
   // The phase profile (tm) takes the same maps, so that its times are those of the steps.  The
   // mode-split stages (grad) take them too: their extra terms (barotropic_correction, grad_eta) run on
-  // every node, and each stage's inverse transform rebuilds every level above level_start.
+  // every node and read the stage's values only where the next trend does.
   auto need = [&](int l) -> const unsigned char* { return ((wav || tm) && dest) ? wt_level_need(h, l) : nullptr; };
   // and then over the level's work list, the needed slots only (persistent blocks)
   auto list = [&](int l) { return need(l) ? wt_level_list(h, l) : wtk::NodeList{nullptr, nullptr}; };
@@ -370,8 +370,9 @@ namespace {
 // barotropic_correction of the stage's source state, trend_ml, scalar_star and
 // u_star (src/barotropic_2d.f90:9-50; the base is always the solution, as the
 // reference's sol), and WT_after_step of the stage state.  The trends run over
-// the levels' work lists (needed-node maps); each stage's inverse transform
-// rebuilds every level above level_start.
+// the levels' work lists (needed-node maps); the first three stages' inverse
+// transforms rebuild the parents the next stage reads, the last one every
+// parent.
 int rk4_split_explicit(wt_handle* h, double dt, double theta1) {
   MLCtx* M = static_cast<MLCtx*>(h->ml);
   const States q = hierarchy_state(h);
@@ -391,7 +392,9 @@ int rk4_split_explicit(wt_handle* h, double dt, double theta1) {
     wt_level_wav_bind(h, dest.m.data(), dest.t.data(), dest.v.data());
     wt_level_clean_wavelets(h);
     int rc = trend_multi(h, src, nullptr, &q, &dest, hs[stage], true, false, grad.data(), theta1);
-    if (!rc) rc = wt_level_wav_finish(h, false);
+    // the intermediate stages' inverse rebuilds the parents the next stage reads; the last stage's every one
+    // (free_surface_update reads the whole state)
+    if (!rc) rc = wt_level_wav_finish(h, stage < 3);
     wt_level_wav_unbind(h);
     if (rc) return rc;
   }

@@ -236,7 +236,10 @@ __global__ void __launch_bounds__(NODE_TILE, 3)
 }
 
 // The same over a work list (persistent blocks).
-__global__ void __launch_bounds__(NODE_TILE, 4)
+#ifndef WT_STEP1_LIST_MINB
+#define WT_STEP1_LIST_MINB 4
+#endif
+__global__ void __launch_bounds__(NODE_TILE, WT_STEP1_LIST_MINB)
     k_step1_list(LevelDev L, int nz, const double* __restrict__ mass, const double* __restrict__ temp,
                  const double* __restrict__ velo, const double* __restrict__ mean_m,
                  const double* __restrict__ mean_t, const double* __restrict__ phik,

@@ -53,7 +53,11 @@ __global__ void __launch_bounds__(NODE_TILE, 4) k_trend_ml(LevelDev L, int nz, T
 
 // The same over a work list (persistent blocks): the list holds the padded
 // slots of the needed-node map.
-__global__ void __launch_bounds__(NODE_TILE, 3) k_trend_ml_list(LevelDev L, int nz, TrendML io, NodeList W) {
+#ifndef WT_ML_LIST_MINB
+#define WT_ML_LIST_MINB 3
+#endif
+__global__ void __launch_bounds__(NODE_TILE, WT_ML_LIST_MINB)
+    k_trend_ml_list(LevelDev L, int nz, TrendML io, NodeList W) {
   const int cnt = __ldg(W.count);
   for (int64_t w = blockIdx.x; w < list_items(cnt, nz); w += gridDim.x) {
     int k, id, i, j;

@@ -117,7 +117,9 @@ int wt_level_mean(wt_handle* h, int level, int field, double** out);
 void wt_level_masks(wt_handle* h, int level, const int** mask_n, const int** mask_e);
 // WT_after_step on the given per-level scaling fields (level_start first), or on
 // the hierarchy's own when the arrays are null; stream-ordered (wt_wavelet.cu).
-int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v);
+// mode selects the parents the inverse transform rebuilds, as in
+// wt_level_wav_finish.
+int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v, int mode = 0);
 // WT_after_step in pieces, for callers that launch each level pair's forward
 // wavelets as soon as both levels' fields are written: bind the stage's scaling
 // fields, wt_level_clean_wavelets, wt_level_wav_forward_pair for every l in
@@ -125,11 +127,12 @@ int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double
 void wt_level_wav_bind(wt_handle* h, double* const* m, double* const* t, double* const* v);
 void wt_level_wav_unbind(wt_handle* h);
 int wt_level_wav_forward_pair(wt_handle* h, int level);
-// partial: the inverse rebuilds only the parents of wt_level_rec (an
-// intermediate RK stage, whose state the next stage reads only where needed);
+// mode 0: the inverse rebuilds every parent; 1: only the parents of
+// wt_level_rec (an intermediate RK stage, whose state the next stage reads only
+// where needed); 2: those of wt_level_rec_final (the step's last inverse).
 // rebuild false: join the forward wavelets and leave the inverse out (its result
 // would be overwritten before anything reads it)
-int wt_level_wav_finish(wt_handle* h, bool partial = false, bool rebuild = true);
+int wt_level_wav_finish(wt_handle* h, int mode = 0, bool rebuild = true);
 const unsigned char* wt_level_rec(wt_handle* h, int level);
 // the parents the inverse after adapt rebuilds (patch tree), or null: every parent
 const unsigned char* wt_level_rec_final(wt_handle* h, int level);

@@ -344,10 +344,11 @@ int rk4_multi(wt_handle* h, double dt, int nsteps, PhaseTimer* tm, bool last_inv
     for (int stage = 0; stage < 4; ++stage) {
       const States& src = stage == 0 ? q : q1;
       const States& dest = stage == 3 ? q : q1;
-      if (tm) {  // phase by phase
+      if (tm) {  // phase by phase, each stage's inverse over the parents the timed step rebuilds
         if (int rc = trend_multi(h, src, tm, &q, &dest, hs[stage])) return rc;
         PB(tm);
-        if (int rc = wt_level_after_step(h, dest.m.data(), dest.t.data(), dest.v.data())) return rc;
+        if (int rc = wt_level_after_step(h, dest.m.data(), dest.t.data(), dest.v.data(), stage < 3 ? 1 : 2))
+          return rc;
         PE(tm, PH_AFTER_STEP);
         continue;
       }

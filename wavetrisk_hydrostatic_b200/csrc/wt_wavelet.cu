@@ -272,14 +272,14 @@ int wt_level_wav_forward_pair(wt_handle* h, int l) {
 
 // The end of WT_after_step once every level pair's forward wavelets are
 // launched: join the side streams, then the inverse transform.
-int wt_level_wav_finish(wt_handle* h, bool partial, bool rebuild) {
+int wt_level_wav_finish(wt_handle* h, int mode, bool rebuild) {
   WavCtx* W = ctx(h);
   for (int k = 1; k < 4; ++k) {
     CKW(cudaEventRecord(W->ev[1 + k], W->side[k]));
     CKW(cudaStreamWaitEvent(h->stream, W->ev[1 + k], 0));
   }
   W->zero_ok = true;  // every level pair's forward wavelets are launched
-  if (rebuild) inverse(h, partial ? 1 : 0);
+  if (rebuild) inverse(h, mode);
   CKW(cudaGetLastError());
   return WT_OK;
 }
@@ -287,12 +287,12 @@ int wt_level_wav_finish(wt_handle* h, bool partial, bool rebuild) {
 // WT_after_step (src/adapt.f90:192-237) on the scaling fields m[q], t[q], v[q]
 // of level level_start+q (the hierarchy's own scaling fields when the arrays
 // are null).
-int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v) {
+int wt_level_after_step(wt_handle* h, double* const* m, double* const* t, double* const* v, int mode) {
   if (m) wt_level_wav_bind(h, m, t, v);
   wt_level_clean_wavelets(h);
   int rc = WT_OK;
   for (int l = h->level_start; l <= h->level_end - 1 && !rc; ++l) rc = wt_level_wav_forward_pair(h, l);
-  if (!rc) rc = wt_level_wav_finish(h);
+  if (!rc) rc = wt_level_wav_finish(h, mode);
   if (m) wt_level_wav_unbind(h);
   return rc;
 }

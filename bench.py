@@ -597,14 +597,23 @@ def adaptive_case(lmin, lmax, nz, steps, warmup, seed, device, e2e=True, profile
             d2h.append(state["n"] * per_patch + sum(a.nbytes for _, _, a in dn) + tbuf.nbytes)
 
         nsteps_e2e = max(1, steps // 2)
+        part = [0.0, 0.0, 0.0]  # upload, step, download (each call returns after its stream)
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
         for _ in range(nsteps_e2e):
+            ta = time.perf_counter()
             put()
+            tb = time.perf_counter()
             model.step(DT_AD)
+            tc = time.perf_counter()
             get()
+            td = time.perf_counter()
+            part[0] += tb - ta
+            part[1] += tc - tb
+            part[2] += td - tc
         t1 = time.perf_counter()
         out["e2e_s"] = t1 - t0
+        out["e2e_parts_ms"] = {k: 1e3 * v / nsteps_e2e for k, v in zip(("upload", "step", "download"), part)}
         out["e2e_steps"] = nsteps_e2e
         out["h2d_bytes_per_step"] = int(sum(h2d) / len(h2d))
         out["d2h_bytes_per_step"] = int(sum(d2h) / len(d2h))
@@ -775,7 +784,8 @@ def bench_ours(args):
                     "path": "C-ABI wt_upload_tree_state / wt_adaptive_step / wt_download_tree_state + "
                             "wt_download_fields + wt_tree_download, pinned host buffers: the finest level's state "
                             "(every layer) on its existing patches in, that state, every level's masks and the "
-                            "finest level's patch bytes out, every step (bytes: averages over the steps)"},
+                            "finest level's patch bytes out, every step (bytes: averages over the steps)",
+                    "parts_ms_per_step": r["e2e_parts_ms"]},
             "gpu_launches": adaptive_launches(L) * args.steps,
             "roofline": {"bound": "hbm", "kernel": "k_trend_ml_list (level_end, over its work list)", "achieved": ach,
                          "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,

@@ -467,9 +467,11 @@ __global__ void __launch_bounds__(128, WL_MINB_INNER) k_velo_wc_inner_l(WLev Pa,
 // (a2, b2)'s code), double slots e*9 + (0-8: weights).
 constexpr int OP_NI = 42, OP_ND = 27;
 // Minimum resident blocks per SM of the inner-edge plan kernels (register cap):
-// uncapped they take about 148 registers, one block per SM.
+// uncapped they take about 148 registers, one block per SM.  Over the parent
+// work lists of the adaptive J5..J9 x 32 step, 3 blocks (80 registers, about
+// 50 bytes spilled) beat 2 (122 registers): 11.95 vs 12.18 ms a step.
 #ifndef WL_PLAN_MINB
-#define WL_PLAN_MINB 2
+#define WL_PLAN_MINB 3
 #endif
 // Inner plan, parents [0, np)^2 (u = (d*np + jp)*np + ip): int slots parent
 // codes (0-4), child circulation codes (5-14), target codes (15-20); double

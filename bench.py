@@ -75,6 +75,8 @@ def parse():
                    help="the adaptive mode-split ensemble (RK4_split + adapt) of --members members for --days days")
     p.add_argument("--members", type=int, default=16)
     p.add_argument("--days", type=float, default=1.0)
+    p.add_argument("--remap", default="2PPM", choices=["none", "0", "1", "2PPM"],
+                   help="--ensemble: the layer remap taken when the relative layer mass drops below 0.9")
     p.add_argument("--learned-layers", action="store_true",
                    help="only the learned network's forward pass on uniform J<level>, layer by layer, with its "
                         "32 -> 32 layer on the tensor cores and on the CUDA cores")
@@ -1203,13 +1205,17 @@ def dt_split(lmax):
     return 4.0 * dt_adaptive(lmax)
 
 
-def ensemble_case(members=16, days=1.0, nz=32, lmin=5, rank=0, world=1, device=None, solver="mixed"):
+def ensemble_case(members=16, days=1.0, nz=32, lmin=5, rank=0, world=1, device=None, solver="mixed",
+                  remap="2PPM"):
     """The adaptive mode-split ensemble: members with max levels J7, J8, J9
     in turn, each over its own seeded seamount and jet + bumps, J5..J<max> x nz
     layers, stepped by RK4_split (the implicit free surface solved every step)
-    + adapt + inverse transform for `days` simulated days.  Members are dealt
-    to ranks (member m on rank m % world); each runs on its own handle, one
-    after the other.  CUDA-event time of the steps (set-up excluded)."""
+    + adapt + inverse transform for `days` simulated days, with the layers
+    remapped (remap type `remap`, None for none) whenever the smallest relative
+    layer mass drops below 0.9, as the reference's time_step does.  Members
+    are dealt to ranks (member m on rank m % world); each runs on its own
+    handle, one after the other.  CUDA-event time of the steps (set-up
+    excluded, the min-mass tests and remaps included)."""
     import numpy as np
     import torch
 
@@ -1239,7 +1245,8 @@ def ensemble_case(members=16, days=1.0, nz=32, lmin=5, rank=0, world=1, device=N
         dt = dt_split(lmax)
         steps = int(round(days * DAY / dt))
         model = ModeSplitOcean(G, lmin, lmax, nz, states, dt, ph, tol=TOL_AD, root_state=root_state,
-                               solver=solver_opts(solver, 1e-9, down_iter=2, up_iter=2, coarse_iter=6))
+                               solver=solver_opts(solver, 1e-9, down_iter=2, up_iter=2, coarse_iter=6),
+                               remap=remap)
         del states
         stream = torch.cuda.ExternalStream(model.dev.stream, device=device)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1259,7 +1266,8 @@ def ensemble_case(members=16, days=1.0, nz=32, lmin=5, rank=0, world=1, device=N
         mn = model.masks()[-1][0]
         out.append({"member": m, "levels": [lmin, lmax], "dt_s": dt, "steps": steps, "ms": ms,
                     "ms_per_step": ms / max(1, steps), "status": model.dev.status(),
-                    "solver_unconverged_steps": unconverged,
+                    "solver_unconverged_steps": unconverged, "remaps": model.remaps,
+                    "last_min_mass": model.min_mass,
                     "solver_mean_iterations": float(np.mean(its)) if its else 0.0,
                     "finite": bool(np.isfinite(mass).all() and np.isfinite(velo).all() and np.isfinite(eta).all()),
                     "max_abs_velocity": float(np.abs(velo[:, np.concatenate([np.nonzero(g.owned)[0] + e * g.NN
@@ -1317,7 +1325,8 @@ def bench_ensemble(args):
     if world > 1:
         import torch.distributed as dist
         dist.init_process_group("nccl", device_id=device)
-    res = ensemble_case(args.members, args.days, args.nz if args.nz else 32, rank=rank, world=world, device=device)
+    res = ensemble_case(args.members, args.days, args.nz if args.nz else 32, rank=rank, world=world, device=device,
+                        remap=None if args.remap == "none" else args.remap)
     ms = sum(r["ms"] for r in res)
     if world > 1:
         t = torch.tensor([ms], device=device, dtype=torch.float64)
@@ -1333,7 +1342,9 @@ def bench_ensemble(args):
                           "ms_total_slowest_rank": ms, "scaling": "strong",
                           "config": {"workload": f"{args.members}-member adaptive mode-split ensemble, J5..J7/J8/J9 "
                                                  f"in turn x {args.nz or 32} layers, seeded seamount + jet + bumps, "
-                                                 f"RK4_split + adapt + inverse transform, {args.days} simulated day(s)",
+                                                 f"RK4_split + adapt + inverse transform, layers remapped "
+                                                 f"({args.remap}) below relative mass 0.9, {args.days} "
+                                                 f"simulated day(s)",
                                      "dtype": "f64"},
                           "members": res}), flush=True)
 

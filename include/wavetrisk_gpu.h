@@ -273,6 +273,16 @@ int wt_learned_train(wt_handle* h, const wt_learn_opts* o, wt_learn_report* rep)
  * (src/main.f90:447-454).  nz <= 64. */
 enum { WT_REMAP_0 = 0, WT_REMAP_1 = 1, WT_REMAP_2PPM = 2 };
 int wt_remap_vertical(wt_handle* h, int remap_type, const double* a_vert, const double* b_vert);
+/* cpt_min_mass (src/main.f90:625-693, with cal_min_mass, incompressible case,
+ * A/B hybrid grid, porosity 1): the smallest relative layer mass
+ * (mean + perturbation) / (ref_density dz_k) over the layers of every node of
+ * every level whose node mask is at least ADJZONE (every node of a handle
+ * without masks), dz_k = b_vert[k+1] z_s - b_vert[k] z_s from the b_vert of
+ * wt_remap_vertical.  *min_mass = 0 where a layer mass is not positive or not
+ * a number (the reference aborts there), 1e16 when no node counts.  The host
+ * remaps when it drops below min_mass_remap (0.9 by default,
+ * src/main.f90:447-454). */
+int wt_min_mass(wt_handle* h, const double* b_vert, double* min_mass);
 
 /* ------------------------------------------------------ no allocation ---- */
 /* Weighted l2 norm of one level (the solver's l2, src/lin_solve.f90:433-464)

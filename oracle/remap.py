@@ -172,3 +172,32 @@ def remap_level(lv, nz, state, remap_type, a_vert, b_vert, rho0):
     mass[:, x] = rho_dz - mm[:, x]
     temp[:, x] = rho_dz * tn[1:] - mt[:, x]
     return mass, temp, velo
+
+
+def min_mass_level(lv, nz, state, b_vert, rho0, mask_n=None):
+    """cal_min_mass (src/main.f90:642-693), incompressible case, A/B hybrid
+    grid, porosity 1, over the own-source nodes of [0, n]^2 of one level whose
+    node mask is at least ADJZONE (8; every node without masks): the smallest
+    (sol + sol_mean) / (rho0 dz_k) with dz_k = b_vert[k+1] z_s - b_vert[k] z_s.
+    A layer mass that is not positive, or a ratio that is not, gives 0 (where
+    the reference aborts); no node gives 1e16, the reference's start value."""
+    lv = own(lv)
+    n, P, NN = lv.n, lv.P, lv.NN
+    nsrc = np.arange(NN)
+    nsrc[lv.halo_node[:, 0]] = lv.halo_node[:, 1]
+    d, j, i = np.meshgrid(np.arange(10), np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    x = ((d * P + j + 2) * P + i + 2).ravel()
+    x = x[nsrc[x] == x]
+    if mask_n is not None:
+        x = x[np.asarray(mask_n)[x] >= 8]
+    if x.size == 0:
+        return 1e16
+    b = np.asarray(b_vert, dtype=np.float64)
+    zs = np.asarray(state["topo"], dtype=np.float64)[x]
+    rho_dz = np.asarray(state["mass"])[:, x] + np.asarray(state["mean_m"])[:, x]
+    dz = b[1:, None] * zs[None, :] - b[:-1, None] * zs[None, :]
+    with np.errstate(all="ignore"):
+        rel = rho_dz / (rho0 * dz)
+    if not ((rho_dz > 0.0) & (rel > 0.0)).all():
+        return 0.0
+    return float(rel.min())

@@ -90,3 +90,35 @@ def test_remap_matches_oracle_bit_for_bit(kind):
     if kind != "1":
         assert np.isfinite(out["mass"][:, nodes]).all() and np.isfinite(out["velo"][:, edges]).all()
     assert np.abs(om[:, own] - st["mass"][:, own]).max() > 1.0      # the remap moved mass
+
+
+@pytest.mark.gpu
+def test_min_mass_matches_oracle():
+    """cpt_min_mass on the device (wt_min_mass) against the oracle's
+    cal_min_mass, exactly, on Lagrangian layers moved off the hybrid grid; and
+    0 once a layer has collapsed."""
+    from wavetrisk_hydrostatic_b200 import Grid, OceanParams
+    from wavetrisk_hydrostatic_b200.cases import bump_state, seamount_topography
+    from wavetrisk_hydrostatic_b200.grid import halo_nodes
+    from wavetrisk_hydrostatic_b200.model import TriskModel
+
+    nz, level = 8, 5
+    ph = OceanParams()
+    g = Grid(level, level, radius=6371e3).level(level)
+    st = bump_state(g, nz, seed=3, ph=ph, topo=seamount_topography(g, seed=3, radius=600e3))
+    rng = np.random.default_rng(5)
+    for k in range(nz):
+        st["mass"][k] += st["mean_m"][k] * 0.3 * (rng.random(g.NN) - 0.5)
+        halo_nodes(g, st["mass"][k])
+    b = 1.0 - np.arange(nz + 1) / nz
+    m = TriskModel(g, nz, st["topo"], ph)
+    m.upload(st)
+    got = m.min_mass(b)
+    want = R.min_mass_level(g, nz, st, b, ph.ref_density)
+    assert got == want and 0.8 < got < 0.9
+    own = np.nonzero(g.owned)[0]
+    st["mass"][3, own[17]] = -st["mean_m"][3, own[17]] * 1.5   # a collapsed layer
+    m.upload(st)
+    assert m.min_mass(b) == 0.0 == R.min_mass_level(g, nz, st, b, ph.ref_density)
+    assert m.status() == 0
+    m.close()

@@ -149,6 +149,7 @@ _DEVICE_SIGS = {
     "wt_learned_train": [_vp, C.POINTER(wt_learn_opts), C.POINTER(wt_learn_report)],
     "wt_learned_activation": [_vp, C.c_float],
     "wt_remap_vertical": [_vp, C.c_int, _dp, _dp],
+    "wt_min_mass": [_vp, _dp, _dp],
     "wt_free_surface_adapt": [_vp],
     "wt_learned_tensor_cores": [_vp, C.c_int],
     "wt_learned_layer_times": [_vp, C.c_int, C.POINTER(C.c_float)],

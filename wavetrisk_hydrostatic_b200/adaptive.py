@@ -259,13 +259,24 @@ class ModeSplitOcean(AdaptiveOcean):
     only; compression) and the inverse transform, both also of the free
     surface (layer zlevels+1 of sol, wt_free_surface_adapt).  The initial free
     surface of every level is the sum of its layers' mass perturbations over
-    rho0, so layers and free surface start consistent."""
+    rho0, so layers and free surface start consistent.
+
+    remap ('0', '1' or '2PPM', default none): after each step, as the
+    reference's time_step (src/main.f90:447-454), the Lagrangian layers are
+    remapped to the hybrid grid z_k = a_k eta + b_k z_s of the initial layers
+    (a_k = k/nz, b_k = 1 - a_k from the bottom) when the smallest relative
+    layer mass (cpt_min_mass) is below min_mass_remap."""
 
     def __init__(self, grid: Grid, min_level: int, max_level: int, nz: int, states: list[dict], dt: float,
-                 ph: OceanParams | None = None, theta1: float = 1.0, theta2: float = 1.0, solver=None, **kw):
+                 ph: OceanParams | None = None, theta1: float = 1.0, theta2: float = 1.0, solver=None,
+                 remap: str | None = None, min_mass_remap: float = 0.9, **kw):
         ph = ph or OceanParams()
         super().__init__(grid, min_level, max_level, nz, states, ph, **kw)
         self.dt, self.theta1, self.theta2 = float(dt), float(theta1), float(theta2)
+        self.remap, self.min_mass_remap, self.remaps = remap, float(min_mass_remap), 0
+        self.b_vert = 1.0 - np.arange(nz + 1) / nz
+        self.a_vert = 1.0 - self.b_vert
+        self.min_mass = None
         self.solver = solver if solver is not None else solver_opts("mixed", 1e-9, down_iter=2, up_iter=2,
                                                                      coarse_iter=6)
         for g, st in zip(self.levels, states):
@@ -288,6 +299,11 @@ class ModeSplitOcean(AdaptiveOcean):
             self.dev.compress()
         self.dev.inverse()
         self.dev.free_surface_adapt()
+        if self.remap:
+            self.min_mass = self.dev.min_mass(self.b_vert)
+            if self.min_mass < self.min_mass_remap:
+                self.dev.remap_vertical(self.remap, self.a_vert, self.b_vert)
+                self.remaps += 1
         self.istep += 1
         self.last_report = rep
         return rep

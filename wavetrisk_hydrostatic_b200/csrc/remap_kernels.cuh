@@ -239,4 +239,46 @@ __global__ void __launch_bounds__(128) k_remap_incompressible(RemapLevel L, int 
   }
 }
 
+// cal_min_mass (src/main.f90:642-693), incompressible case on the A/B hybrid
+// grid with porosity 1: the smallest rho_dz_k / (rho0 dz_k) over the layers of
+// the level's own nodes in [0, n]^2 (the owned nodes and the pole slots) whose
+// node mask is at least ADJZONE (8; every such node when mask_n is null), with
+// dz_k = (b_vert[k+1] - b_vert[k]) z_s the layer of the zero-perturbation grid
+// and rho_dz_k = mean_m + mass.  A layer mass that is not positive or not a
+// number counts as 0 (where the reference aborts: "A layer has collapsed").
+// The minimum is kept as the bits of a non-negative double, which atomicMin
+// orders as the values.
+__global__ void __launch_bounds__(128) k_min_mass(RemapLevel L, int nz, const double* __restrict__ bv, double rho0,
+                                                  const int* __restrict__ mask_n,
+                                                  unsigned long long* __restrict__ out) {
+  const int m = L.n + 1;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long key = ~0ull;
+  if (t < (int64_t)10 * m * m) {
+    const int d = (int)(t / ((int64_t)m * m));
+    const int r = (int)(t - (int64_t)d * m * m);
+    const int j = r / m, i = r - j * m;
+    const int x = (d * L.P + j + 2) * L.P + i + 2;
+    if (L.nsrc[x] == x && (!mask_n || mask_n[x] >= 8)) {
+      const double zs = L.topo[x];
+      double mn = 1e16;
+      for (int k = 0; k < nz; ++k) {
+        const double rho_dz = L.mass[(int64_t)k * L.NN + x] + L.mean_m[(int64_t)k * L.NN + x];
+        const double rel = rho_dz / (rho0 * (bv[k + 1] * zs - bv[k] * zs));
+        if (!(rho_dz > 0.0) || !(rel > 0.0)) {  // collapsed, or not a number
+          mn = 0.0;
+          break;
+        }
+        mn = fmin(mn, rel);
+      }
+      key = (unsigned long long)__double_as_longlong(mn);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long v = __shfl_down_sync(0xffffffffu, key, o);
+    key = v < key ? v : key;
+  }
+  if ((threadIdx.x & 31) == 0 && key != ~0ull) atomicMin(out, key);
+}
+
 }  // namespace wtr

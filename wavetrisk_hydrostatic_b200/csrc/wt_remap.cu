@@ -3,6 +3,7 @@
 // (the reference does it when the smallest relative layer mass drops below
 // min_mass_remap, src/main.f90:447-454) and which reconstruction to use.
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "../../include/wavetrisk_gpu.h"
@@ -12,6 +13,7 @@
 int wt_handle_fail(const char* what, cudaError_t e);
 int wt_level_mean(wt_handle* h, int level, int field, double** out);
 void wt_level_state(wt_handle* h, int level, double** m, double** t, double** v);
+void wt_level_masks(wt_handle* h, int level, const int** mask_n, const int** mask_e);
 
 extern "C" {
 
@@ -57,6 +59,51 @@ int wt_remap_vertical(wt_handle* h, int remap_type, const double* a_vert, const 
   if (rc != WT_OK) return rc;
   if (e != cudaSuccess) return wt_handle_fail("remap", e);
   h->state_halo_done = false;
+  return WT_OK;
+}
+
+int wt_min_mass(wt_handle* h, const double* b_vert, double* min_mass) {
+  if (!h || !b_vert || !min_mass) return WT_ERR_ARG;
+  const int nz = h->nz;
+  if (nz < 1) return WT_ERR_ARG;
+  if (h->flux_bits != 64) return WT_ERR_STATE;
+  cudaStream_t s = h->stream;
+  const int l0 = h->wav ? h->level_start : h->level_end;
+  double* bv = nullptr;
+  cudaError_t e = cudaMalloc(&bv, 8 * (size_t)(nz + 2));
+  unsigned long long* key = reinterpret_cast<unsigned long long*>(bv + nz + 1);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(bv, b_vert, 8 * (size_t)(nz + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(key, 0xff, 8, s);
+  int rc = WT_OK;
+  for (int l = l0; l <= h->level_end && e == cudaSuccess && rc == WT_OK; ++l) {
+    const DevLevel& D = h->at(l);
+    double *m, *t, *v, *mm;
+    if (l == h->level_end) {
+      m = h->mass;
+    } else {
+      wt_level_state(h, l, &m, &t, &v);
+    }
+    if ((rc = wt_level_mean(h, l, WT_FIELD_MEAN_MASS, &mm))) break;
+    const int *mask_n = nullptr, *mask_e = nullptr;
+    if (h->wav) wt_level_masks(h, l, &mask_n, &mask_e);
+    wtr::RemapLevel L{D.n, D.P, D.NN, D.nsrc, D.topo, mm, nullptr, nullptr, m, nullptr, nullptr};
+    const int64_t cnt = (int64_t)10 * (D.n + 1) * (D.n + 1);
+    wtr::k_min_mass<<<(unsigned)((cnt + 127) / 128), 128, 0, s>>>(L, nz, bv, h->ph.ref_density, mask_n, key);
+    e = cudaGetLastError();
+  }
+  unsigned long long k = ~0ull;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&k, key, 8, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(bv);
+  if (rc != WT_OK) return rc;
+  if (e != cudaSuccess) return wt_handle_fail("min_mass", e);
+  if (k == ~0ull) {
+    *min_mass = 1e16;  // no node counted: the reference's starting value
+  } else {
+    double x;
+    std::memcpy(&x, &k, 8);
+    *min_mass = x;
+  }
   return WT_OK;
 }
 

@@ -90,6 +90,14 @@ class DeviceGrid:
         b = np.ascontiguousarray(b_vert, dtype=np.float64)
         N.check("wt_remap_vertical", N.lib().wt_remap_vertical(self.h, code, N.dptr(a), N.dptr(b)))
 
+    def min_mass(self, b_vert: np.ndarray) -> float:
+        """cpt_min_mass (wt_min_mass): the smallest relative layer mass against the
+        zero-perturbation grid b_vert z_s, over the nodes the masks keep."""
+        b = np.ascontiguousarray(b_vert, dtype=np.float64)
+        out = np.zeros(1)
+        N.check("wt_min_mass", N.lib().wt_min_mass(self.h, N.dptr(b), N.dptr(out)))
+        return float(out[0])
+
     def clear_status(self) -> None:
         """Acknowledge a device-side error: flag and sticky status back to 0."""
         N.check("wt_clear_status", N.lib().wt_clear_status(self.h))

@@ -396,6 +396,13 @@ int wt_grid_sync(wt_handle* h, const unsigned char* exist, int level_end);
  * and compress_wavelets.  Returns the new level_end and whether a patch was
  * made (either pointer may be NULL). */
 int wt_adapt(wt_handle* h, const double* threshold, int level_fill, int max_level, int* level_end, int* refined);
+/* inverse_wavelet_transform after adapt (time_step, src/main.f90:444) on the
+ * tree: rebuilds the parents whose children the next step reads (the needed
+ * nodes of the masks wt_adapt left) and those of the tree's nodes, as the
+ * inverse inside wt_adaptive_step does; the scaling values outside the tree,
+ * which no step reads, keep what they held.  Without a tree, or with the
+ * needed-node maps off, every parent (wt_inverse_wt). */
+int wt_inverse_tree(wt_handle* h);
 /* count_active (src/main.f90:137-172) over the patches the last refine made:
  * counts[0] node wavelets (mass and Theta of every layer) with |w| >=
  * threshold(v, k), counts[1] edge wavelets (velocity). */

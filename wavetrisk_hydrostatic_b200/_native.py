@@ -162,6 +162,7 @@ _DEVICE_SIGS = {
     "wt_download_fields": [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(_vp)],
     "wt_forward_wt": [_vp],
     "wt_inverse_wt": [_vp],
+    "wt_inverse_tree": [_vp],
     "wt_mask_tol_vars": [_vp, _dp, C.c_int],
     "wt_compress": [_vp],
     "wt_mask_build": [_vp, _dp, C.c_int, C.c_int, C.c_int, C.c_void_p],

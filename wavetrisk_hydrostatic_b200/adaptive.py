@@ -187,7 +187,10 @@ class AdaptiveOcean:
         else:
             self.dev.rk4_multi(dt, 1)
             self.adapt()
-            self.dev.inverse()
+            if self.tree:   # as the graph's inverse: the parents the next step reads and the tree's
+                self.dev.inverse_tree()
+            else:
+                self.dev.inverse()
         self.istep += 1
 
     def masks(self):
@@ -294,10 +297,11 @@ class ModeSplitOcean(AdaptiveOcean):
         rep = self.dev.rk4_split(self.dt, self.theta1, self.theta2, self.solver)
         if self.tree:
             self.dev.adapt(self.threshold, self.level_fill, self.max_level)
+            self.dev.inverse_tree()
         else:
             self.dev.mask_build(self.threshold, self.level_fill, self.max_level, 0)
             self.dev.compress()
-        self.dev.inverse()
+            self.dev.inverse()
         self.dev.free_surface_adapt()
         if self.remap:
             self.min_mass = self.dev.min_mass(self.b_vert)

@@ -1247,6 +1247,15 @@ int wt_adapt(wt_handle* h, const double* threshold, int level_fill, int max_leve
   return WT_OK;
 }
 
+int wt_inverse_tree(wt_handle* h) {
+  if (int rc = ready(h)) return rc;
+  if (int rc = wt_level_need_refresh(h)) return rc;  // maps of the current masks (wt_adapt leaves them built)
+  inverse(h, 2);
+  CKW(cudaGetLastError());
+  CKW(cudaStreamSynchronize(h->stream));
+  return WT_OK;
+}
+
 int wt_count_active(wt_handle* h, const double* threshold, long long* counts) {
   if (int rc = ready(h)) return rc;
   WavCtx* W = ctx(h);

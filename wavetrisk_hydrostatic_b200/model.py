@@ -261,6 +261,11 @@ class WaveletHierarchy(DeviceGrid):
     def inverse(self) -> None:
         N.check("wt_inverse_wt", N.lib().wt_inverse_wt(self.h))
 
+    def inverse_tree(self) -> None:
+        """The inverse transform after adapt on the patch tree (wt_inverse_tree):
+        the parents the next step reads and those of the tree's nodes."""
+        N.check("wt_inverse_tree", N.lib().wt_inverse_tree(self.h))
+
     def mask_tol_vars(self, threshold: np.ndarray, level_fill: int) -> None:
         thr = _c(np.asarray(threshold).reshape(3, self.nz))
         N.check("wt_mask_tol_vars", N.lib().wt_mask_tol_vars(self.h, N.dptr(thr), int(level_fill)))

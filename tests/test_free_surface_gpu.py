@@ -128,3 +128,32 @@ def test_mode_split_adaptive_steps_run(init):
     for (mn, me), g in zip(model.masks(), levels):   # every mask entry is one of adapt's values
         assert mn.min() >= 0 and mn.max() <= 16 and me.min() >= 0 and me.max() <= 16
     model.close()
+
+
+def test_mode_split_remaps_below_min_mass():
+    """The reference's remap trigger in the mode-split step (min_mass <
+    min_mass_remap, src/main.f90:447-454): with the threshold above every
+    relative layer mass each step remaps, and the layers' total mass stays
+    what the free surface says (the remap moves mass only within columns)."""
+    from wavetrisk_hydrostatic_b200.adaptive import ModeSplitOcean
+
+    ph = OceanParams()
+    G = Grid(3, 5, radius=6371e3)
+    levels = [G.level(l) for l in range(2, 6)]
+    states = [bump_state(g, 4, seed=8, ph=ph, topo=seamount_topography(g, seed=8, radius=600e3)) for g in levels]
+    root, states, levels = states[0], states[1:], levels[1:]
+    g = levels[-1]
+    own = np.nonzero(g.owned)[0]
+    area = 1.0 / g.hex_inv[own]
+    model = ModeSplitOcean(G, 3, 5, 4, states, 1200.0, ph, tol=5e-3, root_state=root, min_mass_remap=2.0)
+    mean = model.dev.download(5, "mean_m")[:, own]
+    m0 = float(np.sum((mean + states[-1]["mass"][:, own]) * area))
+    for s in range(3):
+        rep = model.step()
+        assert rep.status == 0
+        assert model.remaps == s + 1 and 0.5 < model.min_mass < 2.0
+    assert model.dev.status() == 0
+    mass = model.dev.download(5, "mass")
+    assert np.isfinite(mass).all() and np.isfinite(model.dev.download(5, "velo")).all()
+    assert abs(float(np.sum((mean + mass[:, own]) * area)) - m0) <= 1e-7 * m0
+    model.close()

@@ -264,15 +264,17 @@ class ModeSplitOcean(AdaptiveOcean):
     surface of every level is the sum of its layers' mass perturbations over
     rho0, so layers and free surface start consistent.
 
-    remap ('0', '1' or '2PPM', default none): after each step, as the
-    reference's time_step (src/main.f90:447-454), the Lagrangian layers are
-    remapped to the hybrid grid z_k = a_k eta + b_k z_s of the initial layers
-    (a_k = k/nz, b_k = 1 - a_k from the bottom) when the smallest relative
-    layer mass (cpt_min_mass) is below min_mass_remap."""
+    remap ('0', '1' or '2PPM'; None turns it off): after each step, as the
+    reference's time_step does by default (remap = .true., src/main.f90:
+    447-454), the Lagrangian layers are remapped to the hybrid grid
+    z_k = a_k eta + b_k z_s of the initial layers (a_k = k/nz, b_k = 1 - a_k
+    from the bottom) when the smallest relative layer mass (cpt_min_mass) is
+    below min_mass_remap.  The default 2PPM stands in for the reference's
+    default PPR reconstruction, which is not built."""
 
     def __init__(self, grid: Grid, min_level: int, max_level: int, nz: int, states: list[dict], dt: float,
                  ph: OceanParams | None = None, theta1: float = 1.0, theta2: float = 1.0, solver=None,
-                 remap: str | None = None, min_mass_remap: float = 0.9, **kw):
+                 remap: str | None = "2PPM", min_mass_remap: float = 0.9, **kw):
         ph = ph or OceanParams()
         super().__init__(grid, min_level, max_level, nz, states, ph, **kw)
         self.dt, self.theta1, self.theta2 = float(dt), float(theta1), float(theta2)

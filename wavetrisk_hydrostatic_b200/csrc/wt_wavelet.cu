@@ -1224,6 +1224,14 @@ int wt_adapt(wt_handle* h, const double* threshold, int level_fill, int max_leve
   if (!threshold) return WT_ERR_ARG;
   const int ls = h->level_start, le1 = W->tree_level_end;
   const int req_hi = std::min(std::min(le1, max_level - 1), h->level_end - 1);
+  // wavelets already compressed under the masks now (as after an RK stage's
+  // WT_after_step): compress_wavelets only has to zero the slots the new masks
+  // drop, as in the step graph
+  const bool delta = W->zero_ok;
+  if (delta) {
+    if (int rc = wt_level_mask_snapshot_alloc(h)) return rc;
+    wt_level_mask_snapshot(h);
+  }
   CKW(cudaMemcpyAsync(W->thr, threshold, 3 * h->nz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   if (int rc = mask_phase1(h, level_fill, max_level, W->tree_ps, W->treq, le1, req_hi)) return rc;
   if (req_hi >= ls) {
@@ -1239,7 +1247,10 @@ int wt_adapt(wt_handle* h, const double* threshold, int level_fill, int max_leve
   if (le2 != le1) ++W->skip_epoch;
   W->tree_level_end = le2;
   if (int rc = mask_phase2(h, le2)) return rc;
-  compress(h);
+  if (delta)
+    wt_level_compress_delta(h);
+  else
+    compress(h);
   CKW(cudaGetLastError());
   CKW(cudaStreamSynchronize(h->stream));
   if (level_end) *level_end = le2;

@@ -1,6 +1,6 @@
 """The multi-rank host logic of bench.py on CPU with the gloo backend,
 world size 2: the max-over-ranks timing reduction, and the reference arm
-launched the way the driver launches it (torch.distributed.run, rendezvous on
+launched as a multi-GPU bench run is (torch.distributed.run, rendezvous on
 127.0.0.1), where rank 0 alone prints one JSON line and every rank exits 0."""
 import json
 import os
